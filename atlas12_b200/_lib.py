@@ -1,0 +1,186 @@
+"""ctypes binding of libatlasgpu.so (include/atlasgpu.h).
+
+The library is built in-tree (atlas12_b200/libatlasgpu.so).  There is no CPU
+fallback: if the library cannot be loaded every entry point raises.
+"""
+import atexit
+import ctypes
+import os
+import weakref
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libatlasgpu.so")
+
+OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ENONFINITE, ESTATE = 0, -1, -2, -3, -4, -5, -6
+PREC_FP64, PREC_MIXED = 0, 1
+NXTAU = 51
+
+
+class AtlasGPUError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"atlasgpu status {code}: {msg}")
+        self.code = code
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int), ("stream", ctypes.c_void_p)]
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("ratio", ctypes.c_double), ("ratiolg", ctypes.c_double), ("wbegin", ctypes.c_double),
+                ("length", ctypes.c_int32), ("ixwlbeg", ctypes.c_int32)]
+
+
+class Accum(ctypes.Structure):
+    _fields_ = [(n, ctypes.POINTER(ctypes.c_double)) for n in
+                ("rjmins", "rdabh", "rdiagj", "flxrad", "raden", "h_total", "accrad", "abross")] + \
+               [("pradk0", ctypes.c_double)]
+
+
+LTE_LINE = np.dtype([("nbuff", "<i4"), ("cgf", "<f4"), ("nelion", "<i4"), ("elo", "<f4"),
+                     ("gamrf", "<f4"), ("gamsf", "<f4"), ("gamwf", "<f4"), ("code", "<f4")])
+assert LTE_LINE.itemsize == 32
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "atlasgpu_device_count": (_I, []),
+    "atlasgpu_create": (_I, [ctypes.POINTER(_P), ctypes.POINTER(Opts)]),
+    "atlasgpu_destroy": (_I, [_P]),
+    "atlasgpu_last_error": (ctypes.c_char_p, [_P]),
+    "atlasgpu_set_precision": (_I, [_P, _I]),
+    "atlasgpu_set_stream": (_I, [_P, _P]),
+    "atlasgpu_synchronize": (_I, [_P]),
+    "atlasgpu_launch_count": (_I64, [_P]),
+    "atlasgpu_enable_timing": (_I, [_P, _I]),
+    "atlasgpu_kernel_ms": (_D, [_P, ctypes.c_char_p]),
+    "atlasgpu_set_operators": (_I, [_P, _P, _P, _P, _P, _P]),
+    "atlasgpu_synthe_grid": (_I, [_D, _D, _D, ctypes.POINTER(Grid)]),
+    "atlasgpu_synthe_bin": (_I, [_P, _P, _I64, _D, _I32, _P]),
+    "atlasgpu_synthe_bin_dev": (_I, [_P, _P, _I64, _D, _I32, _P, ctypes.POINTER(_I64)]),
+    "atlasgpu_synthe_continuum": (_I, [_P, _P, _I, _P, _I, _I, _D, _D, _I, _P]),
+    "atlasgpu_synthe_line_opacity": (_I, [_P, _P, _I64, _I, _I, _D, _P, _P, _P, _I, _P, _P, _P, _I, _P]),
+    "atlasgpu_synthe_line_opacity_dev": (_I, [_P, _P, _I64, _I, _I, _D, _P, _P, _P, _I, _P, _P, _P, _I, _P]),
+    "atlasgpu_synthe_spectrum": (_I, [_P, _P, _I, _P, _P, _I, _I, _P, _P, _D, _D, _I, _P, _P, _P]),
+    "atlasgpu_synthe_spectrum_dev": (_I, [_P, _P, _I, _P, _P, _I, _I, _P, _P, _D, _D, _I, _P, _P, _P]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libatlasgpu.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise AtlasGPUError(ESTATE, f"{LIB_PATH} not built (run __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name, None)
+            if f is None:
+                continue
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    L = lib()
+    return {n for n in SIGNATURES if hasattr(L, n)}
+
+
+def ptr(a):
+    """Data pointer of a numpy array (contiguous) or a torch tensor."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    assert a.flags["C_CONTIGUOUS"], "arrays must be C-contiguous"
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def device_count():
+    return int(lib().atlasgpu_device_count())
+
+
+_live = weakref.WeakSet()
+
+
+@atexit.register
+def _close_all():
+    # release device memory before the interpreter (and the CUDA runtime) shut down
+    for c in list(_live):
+        try:
+            c.close()
+        except Exception:
+            pass
+
+
+class Context:
+    """Owns one atlasgpu_ctx (one CUDA stream on one device)."""
+
+    def __init__(self, device=0, precision=PREC_MIXED, stream=None):
+        self._h = _P()
+        o = Opts(device, precision, stream)
+        rc = lib().atlasgpu_create(ctypes.byref(self._h), ctypes.byref(o))
+        if rc != OK:
+            raise AtlasGPUError(rc, "atlasgpu_create failed (device %d)" % device)
+        self.device = device
+        _live.add(self)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def check(self, rc):
+        if rc != OK:
+            raise AtlasGPUError(rc, lib().atlasgpu_last_error(self._h).decode())
+        return rc
+
+    def call(self, name, *args):
+        return self.check(getattr(lib(), name)(self._h, *args))
+
+    def close(self):
+        if self._h:
+            lib().atlasgpu_destroy(self._h)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_precision(self, p):
+        self.call("atlasgpu_set_precision", int(p))
+
+    def set_stream(self, stream):
+        self.call("atlasgpu_set_stream", stream)
+
+    def synchronize(self):
+        self.call("atlasgpu_synchronize")
+
+    def launches(self):
+        return int(lib().atlasgpu_launch_count(self._h))
+
+    def enable_timing(self, on=True):
+        self.call("atlasgpu_enable_timing", 1 if on else 0)
+
+    def kernel_ms(self, name):
+        return float(lib().atlasgpu_kernel_ms(self._h, name.encode()))
+
+    def set_operators(self, xtau8, coefj, coefh, ch_j, ck_j):
+        """coefj/coefh as 2-D arrays COEF[L-1, M-1]; passed column-major."""
+        self._ops = [np.ascontiguousarray(xtau8, np.float64),
+                     np.ascontiguousarray(np.asarray(coefj, np.float64).ravel(order="F")),
+                     np.ascontiguousarray(np.asarray(coefh, np.float64).ravel(order="F")),
+                     np.ascontiguousarray(ch_j, np.float64), np.ascontiguousarray(ck_j, np.float64)]
+        self.call("atlasgpu_set_operators", *[ptr(a) for a in self._ops])

@@ -1,0 +1,130 @@
+// api_common.cuh -- the context object behind the C ABI and its helpers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+struct atlasgpu_ctx {
+  int device = 0;
+  int precision = ATLASGPU_PREC_MIXED;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  int64_t launches = 0;
+  bool timing = false;
+  std::map<std::string, double> kms;
+  // named device buffers, grow-only
+  std::map<std::string, std::pair<void*, size_t>> bufs;
+  atlasgpu::JoshOps* ops = nullptr;  // device
+  bool ops_set = false;
+  int nsm = 148;
+  size_t smem_optin = 0;
+};
+
+namespace atlasgpu {
+
+inline int fail(atlasgpu_ctx* c, int code, const char* fmt, ...) {
+  char b[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(b, sizeof b, fmt, ap);
+  va_end(ap);
+  if (c) c->err = b;
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return ::atlasgpu::fail(ctx, ATLASGPU_ECUDA, "%s: %s (%s:%d)", #call,              \
+                              cudaGetErrorString(e_), __FILE__, __LINE__);                \
+  } while (0)
+
+#define CKL(ctx_)                                                                         \
+  do {                                                                                    \
+    cudaError_t e_ = cudaGetLastError();                                                  \
+    if (e_ != cudaSuccess)                                                                \
+      return ::atlasgpu::fail(ctx_, ATLASGPU_ECUDA, "launch: %s (%s:%d)",                \
+                              cudaGetErrorString(e_), __FILE__, __LINE__);                \
+    (ctx_)->launches++;                                                                   \
+  } while (0)
+
+// grow-only named device buffer
+inline int buf(atlasgpu_ctx* ctx, const char* name, size_t bytes, void** out) {
+  auto it = ctx->bufs.find(name);
+  if (it != ctx->bufs.end() && it->second.second >= bytes) {
+    *out = it->second.first;
+    return 0;
+  }
+  if (it != ctx->bufs.end()) {
+    cudaFree(it->second.first);
+    ctx->bufs.erase(it);
+  }
+  void* p = nullptr;
+  size_t want = bytes < 256 ? 256 : bytes;
+  if (cudaMalloc(&p, want) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, ATLASGPU_ENOMEM, "cudaMalloc(%zu) failed for %s", want, name);
+  }
+  ctx->bufs[name] = {p, want};
+  *out = p;
+  return 0;
+}
+
+template <class T>
+inline int bufT(atlasgpu_ctx* ctx, const char* name, size_t count, T** out) {
+  void* p;
+  int r = buf(ctx, name, count * sizeof(T), &p);
+  *out = (T*)p;
+  return r;
+}
+
+// CUDA-event timing of one named launch family (only when enabled)
+struct Timer {
+  atlasgpu_ctx* ctx;
+  const char* name;
+  cudaEvent_t a = nullptr, b = nullptr;
+  Timer(atlasgpu_ctx* c, const char* n) : ctx(c), name(n) {
+    if (ctx->timing) {
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, ctx->stream);
+    }
+  }
+  void stop() {
+    if (ctx->timing && a) {
+      cudaEventRecord(b, ctx->stream);
+      cudaEventSynchronize(b);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      ctx->kms[name] = ms;
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+      a = b = nullptr;
+    }
+  }
+  ~Timer() { stop(); }
+};
+
+inline int grid_for(atlasgpu_ctx* ctx, int64_t work, int threads, int per_sm = 8) {
+  int64_t g = (work + threads - 1) / threads;
+  int64_t cap = (int64_t)ctx->nsm * per_sm;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+inline bool finite_all(const double* p, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (!(p[i] - p[i] == 0.0)) return false;
+  return true;
+}
+
+}  // namespace atlasgpu

@@ -1,0 +1,437 @@
+// api_synthe.cu -- C ABI: context management and the SYNTHE entry points.
+#include <cmath>
+#include <cstdlib>
+
+#include "api_common.cuh"
+#include "synthe.cuh"
+
+using namespace atlasgpu;
+
+extern "C" {
+
+int atlasgpu_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int atlasgpu_create(atlasgpu_ctx** out, const atlasgpu_opts* opts) {
+  if (!out) return ATLASGPU_EINVAL;
+  *out = nullptr;
+  atlasgpu_ctx* ctx = new atlasgpu_ctx();
+  if (opts) {
+    ctx->device = opts->device;
+    ctx->precision = opts->precision;
+    ctx->stream = (cudaStream_t)opts->stream;
+  }
+  if (ctx->precision != ATLASGPU_PREC_FP64 && ctx->precision != ATLASGPU_PREC_MIXED) {
+    delete ctx;
+    return ATLASGPU_EINVAL;
+  }
+  if (cudaSetDevice(ctx->device) != cudaSuccess) {
+    cudaGetLastError();
+    delete ctx;
+    return ATLASGPU_ECUDA;
+  }
+  if (!ctx->stream) {
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      delete ctx;
+      return ATLASGPU_ECUDA;
+    }
+    ctx->own_stream = true;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, ctx->device) == cudaSuccess) {
+    ctx->nsm = prop.multiProcessorCount;
+    ctx->smem_optin = prop.sharedMemPerBlockOptin;
+  }
+  if (cudaMalloc(&ctx->ops, sizeof(JoshOps)) != cudaSuccess) {
+    cudaGetLastError();
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return ATLASGPU_ENOMEM;
+  }
+  *out = ctx;
+  return ATLASGPU_OK;
+}
+
+int atlasgpu_destroy(atlasgpu_ctx* ctx) {
+  if (!ctx) return ATLASGPU_EINVAL;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->bufs) cudaFree(kv.second.first);
+  if (ctx->ops) cudaFree(ctx->ops);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return ATLASGPU_OK;
+}
+
+const char* atlasgpu_last_error(atlasgpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int atlasgpu_set_precision(atlasgpu_ctx* ctx, int precision) {
+  if (!ctx) return ATLASGPU_EINVAL;
+  if (precision != ATLASGPU_PREC_FP64 && precision != ATLASGPU_PREC_MIXED)
+    return fail(ctx, ATLASGPU_EINVAL, "precision %d", precision);
+  ctx->precision = precision;
+  return ATLASGPU_OK;
+}
+
+int atlasgpu_set_stream(atlasgpu_ctx* ctx, void* stream) {
+  if (!ctx) return ATLASGPU_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (ctx->own_stream) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    ctx->own_stream = false;
+  }
+  if (stream) {
+    ctx->stream = (cudaStream_t)stream;
+  } else {
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ctx->own_stream = true;
+  }
+  return ATLASGPU_OK;
+}
+
+int atlasgpu_synchronize(atlasgpu_ctx* ctx) {
+  if (!ctx) return ATLASGPU_EINVAL;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return ATLASGPU_OK;
+}
+
+int64_t atlasgpu_launch_count(atlasgpu_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int atlasgpu_enable_timing(atlasgpu_ctx* ctx, int on) {
+  if (!ctx) return ATLASGPU_EINVAL;
+  ctx->timing = on != 0;
+  return ATLASGPU_OK;
+}
+
+double atlasgpu_kernel_ms(atlasgpu_ctx* ctx, const char* name) {
+  if (!ctx || !name) return -1.0;
+  auto it = ctx->kms.find(name);
+  return it == ctx->kms.end() ? -1.0 : it->second;
+}
+
+int atlasgpu_set_operators(atlasgpu_ctx* ctx, const double* xtau8, const double* coefj,
+                           const double* coefh, const double* ch_j, const double* ck_j) {
+  if (!ctx || !xtau8 || !coefj || !coefh || !ch_j || !ck_j)
+    return fail(ctx, ATLASGPU_EINVAL, "set_operators: null argument");
+  if (!finite_all(xtau8, kNx) || !finite_all(coefj, kNx * kNx) || !finite_all(coefh, kNx * kNx) ||
+      !finite_all(ch_j, kNx) || !finite_all(ck_j, kNx))
+    return fail(ctx, ATLASGPU_ENONFINITE, "set_operators: non-finite operator entry");
+  for (int i = 1; i < kNx; ++i)
+    if (!(xtau8[i] > xtau8[i - 1])) return fail(ctx, ATLASGPU_EINVAL, "XTAU8 not increasing");
+  JoshOps h;
+  memcpy(h.xtau, xtau8, sizeof h.xtau);
+  memcpy(h.ch, ch_j, sizeof h.ch);
+  memcpy(h.ck, ck_j, sizeof h.ck);
+  memcpy(h.coefj, coefj, sizeof h.coefj);
+  memcpy(h.coefh, coefh, sizeof h.coefh);
+  cudaSetDevice(ctx->device);
+  CK(cudaMemcpyAsync(ctx->ops, &h, sizeof h, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->ops_set = true;
+  return ATLASGPU_OK;
+}
+
+// ---------------------------------------------------------------- grid/bin
+int atlasgpu_synthe_grid(double wlbeg, double wlend, double resolu, atlasgpu_grid* g) {
+  if (!g || !(wlbeg > 0.0) || !(wlend > wlbeg) || !(resolu > 0.0)) return ATLASGPU_EINVAL;
+  g->ratio = 1.0 + 1.0 / resolu;
+  g->ratiolg = log(g->ratio);
+  g->length = (int32_t)(log(wlend / wlbeg) / g->ratiolg);
+  g->ixwlbeg = (int32_t)(log(wlbeg) / g->ratiolg);
+  g->wbegin = exp((double)g->ixwlbeg * g->ratiolg);
+  if (g->wbegin < wlbeg) {
+    g->ixwlbeg = g->ixwlbeg + 1;
+    g->wbegin = exp((double)g->ixwlbeg * g->ratiolg);
+  }
+  return ATLASGPU_OK;
+}
+
+static int bin_core(atlasgpu_ctx* ctx, const double* d_wl, int64_t n, double ratiolg,
+                    int32_t ixwlbeg, int32_t* d_nb, int64_t* flagged_host, int64_t cap,
+                    int64_t* nflag_out) {
+  unsigned long long* d_nf;
+  int64_t* d_fl;
+  int r;
+  if ((r = bufT(ctx, "bin_nflag", 1, &d_nf))) return r;
+  if ((r = bufT(ctx, "bin_flag", (size_t)cap, &d_fl))) return r;
+  CK(cudaMemsetAsync(d_nf, 0, sizeof(unsigned long long), ctx->stream));
+  {
+    Timer tm(ctx, "synthe_bin");
+    k_bin<<<grid_for(ctx, n, 256, 16), 256, 0, ctx->stream>>>(d_wl, n, ratiolg, ixwlbeg, d_nb,
+                                                               d_fl, d_nf, cap);
+    CKL(ctx);
+  }
+  unsigned long long nf = 0;
+  CK(cudaMemcpyAsync(&nf, d_nf, sizeof nf, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if ((int64_t)nf > cap) return fail(ctx, ATLASGPU_EINVAL, "bin: %llu boundary cases exceed %lld", nf, (long long)cap);
+  if (flagged_host && nf) CK(cudaMemcpy(flagged_host, d_fl, nf * sizeof(int64_t), cudaMemcpyDeviceToHost));
+  *nflag_out = (int64_t)nf;
+  return 0;
+}
+
+int atlasgpu_synthe_bin_dev(atlasgpu_ctx* ctx, const double* d_wlvac, int64_t n, double ratiolg,
+                            int32_t ixwlbeg, int32_t* d_nbuff, int64_t* n_flagged) {
+  if (!ctx || n < 0 || (n > 0 && (!d_wlvac || !d_nbuff)) || !(ratiolg > 0.0))
+    return fail(ctx, ATLASGPU_EINVAL, "synthe_bin_dev: bad argument");
+  if (n == 0) {
+    if (n_flagged) *n_flagged = 0;
+    return 0;
+  }
+  cudaSetDevice(ctx->device);
+  const int64_t cap = 1 << 20;
+  std::vector<int64_t> fl(cap);
+  int64_t nf = 0;
+  int r = bin_core(ctx, d_wlvac, n, ratiolg, ixwlbeg, d_nbuff, fl.data(), cap, &nf);
+  if (r) return r;
+  // boundary cases: the host C library log decides (bit-exact with the reader)
+  for (int64_t k = 0; k < nf; ++k) {
+    double w;
+    CK(cudaMemcpy(&w, d_wlvac + fl[k], sizeof w, cudaMemcpyDeviceToHost));
+    const int32_t nb = (int32_t)(log(w) / ratiolg + 0.5) - ixwlbeg + 1;
+    CK(cudaMemcpy(d_nbuff + fl[k], &nb, sizeof nb, cudaMemcpyHostToDevice));
+  }
+  if (n_flagged) *n_flagged = nf;
+  return 0;
+}
+
+int atlasgpu_synthe_bin(atlasgpu_ctx* ctx, const double* wlvac, int64_t n, double ratiolg,
+                        int32_t ixwlbeg, int32_t* nbuff_out) {
+  if (!ctx || n < 0 || (n > 0 && (!wlvac || !nbuff_out)) || !(ratiolg > 0.0))
+    return fail(ctx, ATLASGPU_EINVAL, "synthe_bin: bad argument");
+  if (n == 0) return 0;
+  cudaSetDevice(ctx->device);
+  double* d_wl;
+  int32_t* d_nb;
+  int r;
+  if ((r = bufT(ctx, "bin_wl", (size_t)n, &d_wl)) || (r = bufT(ctx, "bin_nb", (size_t)n, &d_nb))) return r;
+  CK(cudaMemcpyAsync(d_wl, wlvac, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  const int64_t cap = 1 << 20;
+  std::vector<int64_t> fl(cap);
+  int64_t nf = 0;
+  if ((r = bin_core(ctx, d_wl, n, ratiolg, ixwlbeg, d_nb, fl.data(), cap, &nf))) return r;
+  CK(cudaMemcpy(nbuff_out, d_nb, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  for (int64_t k = 0; k < nf; ++k)
+    nbuff_out[fl[k]] = (int32_t)(log(wlvac[fl[k]]) / ratiolg + 0.5) - ixwlbeg + 1;
+  return 0;
+}
+
+// ---------------------------------------------------------------- continuum
+int atlasgpu_synthe_continuum(atlasgpu_ctx* ctx, const double* wledge, int nedge,
+                              const double* continall, int stride, int nrhox, double wbegin,
+                              double ratio, int length, float* continuum_out) {
+  if (!ctx || !wledge || !continall || !continuum_out || nedge < 2 || nrhox < 1 ||
+      nrhox > kKwMax || length < 1 || stride < 3 * (nedge - 1))
+    return fail(ctx, ATLASGPU_EINVAL, "synthe_continuum: bad argument");
+  for (int i = 1; i < nedge; ++i)
+    if (!(wledge[i] > wledge[i - 1])) return fail(ctx, ATLASGPU_EINVAL, "wledge not increasing");
+  if (!finite_all(continall, (size_t)nrhox * stride))
+    return fail(ctx, ATLASGPU_ENONFINITE, "synthe_continuum: non-finite table entry");
+  cudaSetDevice(ctx->device);
+  double *d_we, *d_ca;
+  float* d_out;
+  int r;
+  if ((r = bufT(ctx, "cont_we", nedge, &d_we)) || (r = bufT(ctx, "cont_ca", (size_t)nrhox * stride, &d_ca)) ||
+      (r = bufT(ctx, "cont_out", (size_t)nrhox * length, &d_out)))
+    return r;
+  CK(cudaMemcpyAsync(d_we, wledge, nedge * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(d_ca, continall, (size_t)nrhox * stride * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  {
+    Timer tm(ctx, "synthe_continuum");
+    dim3 g((length + 255) / 256 < 4096 ? (length + 255) / 256 : 4096, nrhox);
+    k_continuum<<<g, 256, 0, ctx->stream>>>(d_we, nedge, d_ca, stride, nrhox, wbegin, ratio, length, d_out);
+    CKL(ctx);
+  }
+  CK(cudaMemcpyAsync(continuum_out, d_out, (size_t)nrhox * length * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+// ---------------------------------------------------------------- line opacity
+int atlasgpu_synthe_line_opacity_dev(atlasgpu_ctx* ctx, const atlasgpu_lte_line* d_lines, int64_t n,
+                                     int length, int nrhox, double resolu, const float* d_cont,
+                                     const double* d_xnfdop, const double* d_dopple, int nspec,
+                                     const double* d_xne, const double* d_txnxn, const double* d_hckt,
+                                     int maxprof, float* d_opac) {
+  if (!ctx || n < 0 || length < 1 || nrhox < 1 || nrhox > kKwMax || nspec < 1 || maxprof < 1 ||
+      !(resolu > 0.0) || !d_cont || !d_xnfdop || !d_dopple || !d_xne || !d_txnxn || !d_hckt ||
+      !d_opac || (n > 0 && !d_lines))
+    return fail(ctx, ATLASGPU_EINVAL, "synthe_line_opacity: bad argument");
+  cudaSetDevice(ctx->device);
+  const int ntiles = (length + kTile - 1) / kTile;
+  double* acc;
+  int r;
+  if ((r = bufT(ctx, "lo_acc", (size_t)nrhox * length, &acc))) return r;
+  CK(cudaMemsetAsync(acc, 0, (size_t)nrhox * length * sizeof(double), ctx->stream));
+  const int64_t nn = n > 0 ? n : 1;
+  // depth batch so that the far-line lists stay within ~4 GB
+  int nj = (int)std::min<int64_t>(nrhox, std::max<int64_t>(1, (4ll << 30) / (nn * (int64_t)sizeof(FarLine))));
+  FarLine* far;
+  unsigned* nfar;
+  int* tdiff;
+  int64_t *off, *fillptr, *tot, *base;
+  if ((r = bufT(ctx, "lo_far", (size_t)nj * nn, &far)) || (r = bufT(ctx, "lo_nfar", nj, &nfar)) ||
+      (r = bufT(ctx, "lo_tdiff", (size_t)nj * (ntiles + 1), &tdiff)) ||
+      (r = bufT(ctx, "lo_off", (size_t)nj * (ntiles + 1), &off)) ||
+      (r = bufT(ctx, "lo_fill", (size_t)nj * ntiles, &fillptr)) || (r = bufT(ctx, "lo_tot", nj, &tot)) ||
+      (r = bufT(ctx, "lo_base", nj, &base)))
+    return r;
+  std::vector<int64_t> htot(nj), hbase(nj);
+  for (int j0 = 0; j0 < nrhox; j0 += nj) {
+    const int nb = std::min(nj, nrhox - j0);
+    CK(cudaMemsetAsync(nfar, 0, nb * sizeof(unsigned), ctx->stream));
+    CK(cudaMemsetAsync(tdiff, 0, (size_t)nb * (ntiles + 1) * sizeof(int), ctx->stream));
+    if (n > 0) {
+      CoreArgs a{d_lines, n, length, nrhox, nspec, maxprof, j0, nb, resolu, d_cont, d_xnfdop,
+                 d_dopple, d_xne, d_txnxn, d_hckt, acc, far, nfar, tdiff, ntiles};
+      Timer tm(ctx, "synthe_core");
+      const int64_t groups = n * nb;
+      k_core<8><<<grid_for(ctx, groups * 8, 256, 16), 256, 0, ctx->stream>>>(a);
+      CKL(ctx);
+    }
+    k_far_scan<<<nb, 32, 0, ctx->stream>>>(tdiff, ntiles, off, fillptr, tot);
+    CKL(ctx);
+    CK(cudaMemcpyAsync(htot.data(), tot, nb * sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    int64_t run = 0;
+    for (int k = 0; k < nb; ++k) {
+      hbase[k] = run;
+      run += htot[k];
+    }
+    int* csr;
+    if ((r = bufT(ctx, "lo_csr", (size_t)std::max<int64_t>(run, 1), &csr))) return r;
+    CK(cudaMemcpyAsync(base, hbase.data(), nb * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
+    {
+      Timer tm(ctx, "synthe_farfill");
+      dim3 g(std::max(1, std::min(ctx->nsm * 4 / std::max(1, nb) + 1, 1024)), nb);
+      k_far_fill<<<g, 256, 0, ctx->stream>>>(far, nfar, nn, length, base, fillptr, ntiles, csr);
+      CKL(ctx);
+    }
+    {
+      Timer tm(ctx, "synthe_farwing");
+      dim3 g(ntiles, nb);
+      if (ctx->precision == ATLASGPU_PREC_MIXED)
+        k_farwing<true><<<g, kFarThreads, 0, ctx->stream>>>(far, nn, off, base, csr, ntiles, length, j0, acc, d_opac);
+      else
+        k_farwing<false><<<g, kFarThreads, 0, ctx->stream>>>(far, nn, off, base, csr, ntiles, length, j0, acc, d_opac);
+      CKL(ctx);
+    }
+  }
+  return 0;
+}
+
+int atlasgpu_synthe_line_opacity(atlasgpu_ctx* ctx, const atlasgpu_lte_line* lines, int64_t n,
+                                 int length, int nrhox, double resolu, const float* continuum,
+                                 const double* xnfdop, const double* dopple, int nspec,
+                                 const double* xne, const double* txnxn, const double* hckt,
+                                 int maxprof, float* opacity_out) {
+  if (!ctx || n < 0 || (n > 0 && !lines) || !continuum || !xnfdop || !dopple || !xne || !txnxn ||
+      !hckt || !opacity_out || length < 1 || nrhox < 1 || nrhox > kKwMax || nspec < 1)
+    return fail(ctx, ATLASGPU_EINVAL, "synthe_line_opacity: bad argument");
+  for (int64_t i = 0; i < n; ++i)
+    if (lines[i].nelion < 1 || lines[i].nelion > nspec)
+      return fail(ctx, ATLASGPU_EINVAL, "line %lld: nelion %d outside 1..%d", (long long)i, lines[i].nelion, nspec);
+  cudaSetDevice(ctx->device);
+  atlasgpu_lte_line* d_l;
+  float *d_c, *d_o;
+  double *d_xd, *d_dp, *d_xne, *d_tx, *d_hc;
+  int r;
+  const size_t nd = (size_t)nrhox * nspec;
+  if ((r = bufT(ctx, "h_lines", (size_t)std::max<int64_t>(n, 1), &d_l)) ||
+      (r = bufT(ctx, "h_cont", (size_t)nrhox * length, &d_c)) ||
+      (r = bufT(ctx, "h_opac", (size_t)nrhox * length, &d_o)) || (r = bufT(ctx, "h_xnfdop", nd, &d_xd)) ||
+      (r = bufT(ctx, "h_dopple", nd, &d_dp)) || (r = bufT(ctx, "h_xne", nrhox, &d_xne)) ||
+      (r = bufT(ctx, "h_txnxn", nrhox, &d_tx)) || (r = bufT(ctx, "h_hckt", nrhox, &d_hc)))
+    return r;
+  cudaStream_t s = ctx->stream;
+  if (n > 0) CK(cudaMemcpyAsync(d_l, lines, n * sizeof(atlasgpu_lte_line), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_c, continuum, (size_t)nrhox * length * sizeof(float), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_xd, xnfdop, nd * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_dp, dopple, nd * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_xne, xne, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_tx, txnxn, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_hc, hckt, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  if ((r = atlasgpu_synthe_line_opacity_dev(ctx, d_l, n, length, nrhox, resolu, d_c, d_xd, d_dp, nspec,
+                                            d_xne, d_tx, d_hc, maxprof, d_o)))
+    return r;
+  CK(cudaMemcpyAsync(opacity_out, d_o, (size_t)nrhox * length * sizeof(float), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+// ---------------------------------------------------------------- spectrum
+static int spectrum_launch(atlasgpu_ctx* ctx, const SpecArgs& a) {
+  int nwarp = 4;
+  const size_t per = sizeof(SpecWS);
+  while (nwarp > 1 && sizeof(double) * kKwMax + nwarp * per > ctx->smem_optin) --nwarp;
+  const size_t smem = sizeof(double) * kKwMax + nwarp * per;
+  CK(cudaFuncSetAttribute(k_spectrum, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int blocks = std::min<int64_t>((a.length + nwarp - 1) / nwarp, (int64_t)ctx->nsm * 8);
+  Timer tm(ctx, "josh_spectrum");
+  k_spectrum<<<blocks, 32 * nwarp, smem, ctx->stream>>>(a);
+  CKL(ctx);
+  return 0;
+}
+
+int atlasgpu_synthe_spectrum_dev(atlasgpu_ctx* ctx, const double* d_wledge, int nedge,
+                                 const double* d_contabs, const double* d_contscat, int stride,
+                                 int nrhox, const double* d_rhox, const double* d_hkt, double wbegin,
+                                 double ratio, int length, const float* d_opac, double* d_flux,
+                                 double* d_cont) {
+  if (!ctx || !ctx->ops_set) return fail(ctx, ATLASGPU_ESTATE, "synthe_spectrum: operators not set");
+  if (nedge < 2 || nrhox < 4 || nrhox > kKwMax || length < 1 || stride < 3 * (nedge - 1) || !d_wledge ||
+      !d_contabs || !d_contscat || !d_rhox || !d_hkt || !d_opac || !d_flux || !d_cont)
+    return fail(ctx, ATLASGPU_EINVAL, "synthe_spectrum: bad argument");
+  cudaSetDevice(ctx->device);
+  SpecArgs a{ctx->ops, d_wledge, d_contabs, d_contscat, d_rhox, d_hkt, nedge, stride, nrhox, length,
+             wbegin, ratio, d_opac, d_flux, d_cont};
+  return spectrum_launch(ctx, a);
+}
+
+int atlasgpu_synthe_spectrum(atlasgpu_ctx* ctx, const double* wledge, int nedge, const double* contabs,
+                             const double* contscat, int stride, int nrhox, const double* rhox,
+                             const double* hkt, double wbegin, double ratio, int length,
+                             const float* opacity, double* flux, double* cont) {
+  if (!ctx || !wledge || !contabs || !contscat || !rhox || !hkt || !opacity || !flux || !cont ||
+      nedge < 2 || nrhox < 4 || nrhox > kKwMax || length < 1 || stride < 3 * (nedge - 1))
+    return fail(ctx, ATLASGPU_EINVAL, "synthe_spectrum: bad argument");
+  for (int i = 1; i < nedge; ++i)
+    if (!(wledge[i] > wledge[i - 1])) return fail(ctx, ATLASGPU_EINVAL, "wledge not increasing");
+  if (!finite_all(contabs, (size_t)nrhox * stride) || !finite_all(contscat, (size_t)nrhox * stride) ||
+      !finite_all(rhox, nrhox) || !finite_all(hkt, nrhox))
+    return fail(ctx, ATLASGPU_ENONFINITE, "synthe_spectrum: non-finite input");
+  cudaSetDevice(ctx->device);
+  double *d_we, *d_ca, *d_cs, *d_rx, *d_hk, *d_fl, *d_ct;
+  float* d_op;
+  int r;
+  const size_t nt = (size_t)nrhox * stride;
+  if ((r = bufT(ctx, "s_we", nedge, &d_we)) || (r = bufT(ctx, "s_ca", nt, &d_ca)) ||
+      (r = bufT(ctx, "s_cs", nt, &d_cs)) || (r = bufT(ctx, "s_rx", nrhox, &d_rx)) ||
+      (r = bufT(ctx, "s_hk", nrhox, &d_hk)) || (r = bufT(ctx, "s_fl", length, &d_fl)) ||
+      (r = bufT(ctx, "s_ct", length, &d_ct)) || (r = bufT(ctx, "s_op", (size_t)nrhox * length, &d_op)))
+    return r;
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(d_we, wledge, nedge * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_ca, contabs, nt * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_cs, contscat, nt * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_rx, rhox, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_hk, hkt, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_op, opacity, (size_t)nrhox * length * sizeof(float), cudaMemcpyHostToDevice, s));
+  if ((r = atlasgpu_synthe_spectrum_dev(ctx, d_we, nedge, d_ca, d_cs, stride, nrhox, d_rx, d_hk, wbegin,
+                                        ratio, length, d_op, d_fl, d_ct)))
+    return r;
+  CK(cudaMemcpyAsync(flux, d_fl, length * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(cont, d_ct, length * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+}  // extern "C"

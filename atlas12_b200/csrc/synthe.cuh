@@ -1,0 +1,363 @@
+// synthe.cuh -- SYNTHE hot-path kernels (sm_100a).
+//
+//  k_bin        line -> grid index (mod_mklinelist.f90:898-899)
+//  k_continuum  continuum per depth on the grid (synthe.f90:483-516)
+//  k_core       gates, line centre and Voigt core walk of every (line, depth)
+//               pair (synthe.f90:559-640), core values scattered with FP64
+//               atomics; far-wing lines recorded for k_farwing
+//  k_far_*      per-(depth, tile) inverted index of the far-wing lines
+//  k_farwing    gather of the x_wing/n^2 far wings (synthe.f90:641-650)
+//               tile by tile in registers, plus the core accumulator, written
+//               as the REAL(4) opacity matrix
+//  k_spectrum   the wavelength loop (synthe.f90:698-718, 797-902): two
+//               warp-cooperative JOSH(1,1) solves per wavelength
+#pragma once
+#include "common.cuh"
+#include "josh.cuh"
+#include "voigt.cuh"
+
+namespace atlasgpu {
+
+constexpr int kTile = 1024;      // bins per far-wing tile
+constexpr int kFarThreads = 256; // threads per far-wing tile CTA
+
+struct FarLine {
+  int c;    // line centre nbuff (1-based)
+  int n10;  // n10dop: core extent
+  int m;    // maxstep: far-wing extent
+  int pad;
+  double x; // x_wing = profile(n10dop) * n10dop**2
+};
+
+// ---------------------------------------------------------------- binning
+__global__ void k_bin(const double* __restrict__ wl, int64_t n, double ratiolg, int ixwlbeg,
+                      int32_t* __restrict__ nbuff, int64_t* __restrict__ flagged,
+                      unsigned long long* __restrict__ nflag, int64_t flag_cap) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double q = log(wl[i]) / ratiolg + 0.5;
+    const int ixwl = (int)q;
+    nbuff[i] = ixwl - ixwlbeg + 1;
+    // a 1-ulp difference in log moves q by < 1e-9: re-evaluate near-integers on the host
+    if (fabs(q - rint(q)) < 1.0e-8) {
+      const unsigned long long k = atomicAdd(nflag, 1ull);
+      if ((int64_t)k < flag_cap) flagged[k] = i;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- continuum
+__global__ void k_continuum(const double* __restrict__ wledge, int nedge,
+                            const double* __restrict__ continall, int stride, int nrhox,
+                            double wbegin, double ratio, int length, float* __restrict__ out) {
+  const int j = blockIdx.y;
+  const double* ab = continall + (size_t)j * stride;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < length; i += gridDim.x * blockDim.x) {
+    const double w = wbegin * powi(ratio, i);
+    // iedge = 1 + #{e in [2, nedge-1] : wledge(e) <= w}
+    int lo = 1, hi = nedge - 1;  // answer in [1, nedge-1]
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;  // candidate iedge
+      if (wledge[mid - 1] <= w) lo = mid;
+      else hi = mid - 1;
+    }
+    const int ie = lo;
+    const double wl0 = wledge[ie - 1], wl1 = wledge[ie];
+    const double h = (wl0 + wl1) * 0.5;
+    const double dd = powi(wl1 - wl0, 2) * 0.5;
+    const double* q = ab + 3 * (ie - 1);
+    const double v = ((w - h) * (w - wl1) * q[0] + (wl0 - w) * (w - wl1) * 2.0 * q[1] +
+                      (w - wl0) * (w - h) * q[2]) / dd;
+    float cf = (float)v;
+    if (cf < -15.0f) cf = -15.0f;
+    out[(size_t)j * length + i] = (float)exp10((double)cf);
+  }
+}
+
+// ---------------------------------------------------------------- core pass
+struct CoreArgs {
+  const atlasgpu_lte_line* lines;
+  int64_t n;
+  int length, nrhox, nspec, maxprof, j0, nj;  // depths [j0, j0+nj)
+  double resolu;
+  const float* cont;     // [nrhox][length]
+  const double *xnfdop, *dopple;  // [nrhox][nspec]
+  const double *xne, *txnxn, *hckt;
+  double* acc;           // [nrhox][length] core accumulator
+  FarLine* far;          // [nj][n]
+  unsigned int* nfar;    // [nj]
+  int* tdiff;            // [nj][ntiles+1]
+  int ntiles;
+};
+
+template <int G>
+__global__ void __launch_bounds__(256) k_core(CoreArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int g = lane % G;                 // lane within the group
+  const int gbase = lane - g;             // first lane of the group
+  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << gbase);
+  const int64_t npairs = a.n * a.nj;
+  const int64_t gid0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
+  const int64_t gstride = (int64_t)gridDim.x * blockDim.x / G;
+  for (int64_t p = gid0; p < npairs; p += gstride) {
+    const int jj = (int)(p / a.n);
+    const int64_t il = p - (int64_t)jj * a.n;
+    const int j = a.j0 + jj;
+    const atlasgpu_lte_line L = a.lines[il];
+    const int nb = L.nbuff;
+    const int nel = L.nelion - 1;
+    if (nel < 0 || nel >= a.nspec) continue;  // invalid species: no opacity
+    const int ic = nb < 1 ? 1 : (nb > a.length ? a.length : nb);
+    const double xd = a.xnfdop[(size_t)j * a.nspec + nel];
+    const double dp = a.dopple[(size_t)j * a.nspec + nel];
+    double kappa0 = (double)L.cgf * xd;
+    const double kapmin = (double)a.cont[(size_t)j * a.length + ic - 1] * kLineCutoff;
+    if (kappa0 < kapmin) continue;
+    kappa0 = kappa0 * exp(-(double)L.elo * a.hckt[j]);
+    if (kappa0 < kapmin) continue;
+    const double adamp =
+        ((double)L.gamrf + (double)L.gamsf * a.xne[j] + (double)L.gamwf * a.txnxn[j]) / dp;
+    const int n10 = (int)(10.0 * dp * a.resolu);
+    double* accj = a.acc + (size_t)j * a.length;
+    if (g == 0 && nb >= 1 && nb <= a.length)
+      atomicAdd(accj + nb - 1, kappa0 * voigt_weideman(0.0, adamp));
+    const double dv = 1.0 / dp / a.resolu;
+    // With MAXPROF < n10dop the reference scatters only min(n10dop, maxstep)
+    // core points when no point falls below kapmin; that limit is known only
+    // after the walk, so such pairs walk once to decide and once to scatter.
+    const bool defer = a.maxprof < n10;
+    int nstop = 0;  // 0: no sub-threshold point in the core
+    double plast = 0.0;
+    for (int s0 = 1; s0 <= n10 && nstop == 0; s0 += G) {
+      const int s = s0 + g;
+      const bool valid = s <= n10;
+      double pv = 0.0;
+      if (valid) pv = kappa0 * voigt_weideman((double)s * dv, adamp);
+      const unsigned below = __ballot_sync(gmask, valid && pv < kapmin) & gmask;
+      int slim = n10;
+      if (below) {
+        nstop = s0 + (__ffs(below >> gbase) - 1);
+        slim = nstop;
+      }
+      if (!defer && valid && s <= slim) {
+        const int r = nb + s, b = nb - s;
+        if (r >= 1 && r <= a.length) atomicAdd(accj + r - 1, pv);
+        if (b >= 1 && b <= a.length) atomicAdd(accj + b - 1, pv);
+      }
+      if (s == n10) plast = pv;
+    }
+    if (defer) {
+      const int lim = nstop ? nstop : a.maxprof;
+      for (int s = 1 + g; s <= lim; s += G) {
+        const double pv = kappa0 * voigt_weideman((double)s * dv, adamp);
+        const int r = nb + s, b = nb - s;
+        if (r >= 1 && r <= a.length) atomicAdd(accj + r - 1, pv);
+        if (b >= 1 && b <= a.length) atomicAdd(accj + b - 1, pv);
+      }
+    }
+    if (nstop == 0 && n10 >= 1) {
+      // far wing: x_wing/n**2 for n10dop < n <= maxstep
+      const int src = gbase + ((n10 - 1) % G);
+      plast = __shfl_sync(gmask, plast, src);
+      const double xw = plast * ((double)n10 * (double)n10);
+      // INT(SQRT(x_wing/kapmin))+1 capped at MAXPROF; saturate before the
+      // integer conversion (the reference's INT overflows for huge ratios)
+      const double q = sqrt(xw / kapmin);
+      const int maxstep = q >= (double)a.maxprof ? a.maxprof : min((int)q + 1, a.maxprof);
+      const int lo = max(nb - maxstep, 1), hi = min(nb + maxstep, a.length);
+      if (maxstep > n10 && lo <= hi && g == 0) {
+        const unsigned slot = atomicAdd(a.nfar + jj, 1u);
+        FarLine f;
+        f.c = nb;
+        f.n10 = n10;
+        f.m = maxstep;
+        f.pad = 0;
+        f.x = xw;
+        a.far[(size_t)jj * a.n + slot] = f;
+        int* td = a.tdiff + (size_t)jj * (a.ntiles + 1);
+        atomicAdd(td + (lo - 1) / kTile, 1);
+        atomicAdd(td + (hi - 1) / kTile + 1, -1);
+      }
+    }
+  }
+}
+
+// per depth: tile counts from the difference array, exclusive offsets
+__global__ void k_far_scan(int* __restrict__ tdiff, int ntiles, int64_t* __restrict__ off,
+                           int64_t* __restrict__ fillptr, int64_t* __restrict__ total) {
+  // one block per depth; sequential over tiles in chunks (ntiles is small)
+  const int jj = blockIdx.x;
+  if (threadIdx.x != 0) return;
+  int* td = tdiff + (size_t)jj * (ntiles + 1);
+  int64_t* o = off + (size_t)jj * (ntiles + 1);
+  int64_t* fp = fillptr + (size_t)jj * ntiles;
+  int cnt = 0;
+  int64_t run = 0;
+  for (int t = 0; t < ntiles; ++t) {
+    cnt += td[t];
+    o[t] = run;
+    fp[t] = run;
+    run += cnt;
+  }
+  o[ntiles] = run;
+  total[jj] = run;
+}
+
+__global__ void k_far_fill(const FarLine* __restrict__ far, const unsigned* __restrict__ nfar,
+                           int64_t nlines, int length, const int64_t* __restrict__ base,
+                           int64_t* __restrict__ fillptr, int ntiles, int* __restrict__ csr) {
+  const int jj = blockIdx.y;
+  const unsigned nf = nfar[jj];
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (unsigned s = warp; s < nf; s += nwarps) {
+    const FarLine f = far[(size_t)jj * nlines + s];
+    const int lo = max(f.c - f.m, 1), hi = min(f.c + f.m, length);
+    const int t0 = (lo - 1) / kTile, t1 = (hi - 1) / kTile;
+    for (int t = t0 + lane; t <= t1; t += 32) {
+      const int64_t pos = atomicAdd((unsigned long long*)(fillptr + (size_t)jj * ntiles + t), 1ull);
+      csr[base[jj] + pos] = (int)s;
+    }
+  }
+}
+
+// far-wing gather + core accumulator -> REAL(4) opacity; zeroes acc for reuse
+template <bool kMixed>
+__global__ void __launch_bounds__(kFarThreads) k_farwing(const FarLine* __restrict__ far,
+                                                         int64_t nlines,
+                                                         const int64_t* __restrict__ off,
+                                                         const int64_t* __restrict__ base,
+                                                         const int* __restrict__ csr, int ntiles,
+                                                         int length, int j0,
+                                                         double* __restrict__ acc,
+                                                         float* __restrict__ opac) {
+  const int jj = blockIdx.y, t = blockIdx.x, j = j0 + jj;
+  constexpr int kPer = kTile / kFarThreads;
+  const int i0 = t * kTile + threadIdx.x + 1;  // 1-based bins i0 + k*kFarThreads
+  double sum[kPer];
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) sum[k] = 0.0;
+  const int64_t* o = off + (size_t)jj * (ntiles + 1);
+  const int64_t e0 = base[jj] + o[t], e1 = base[jj] + o[t + 1];
+  const FarLine* fj = far + (size_t)jj * nlines;
+  for (int64_t e = e0; e < e1; ++e) {
+    const FarLine f = fj[csr[e]];
+    if (kMixed) {
+      const float xf = (float)f.x;
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) {
+        const int d = abs(i0 + k * kFarThreads - f.c);
+        if (d > f.n10 && d <= f.m) {
+          const float df = (float)d;
+          sum[k] += (double)(xf * __frcp_rn(df * df));
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) {
+        const int d = abs(i0 + k * kFarThreads - f.c);
+        if (d > f.n10 && d <= f.m) {
+          const double dd = (double)d;
+          sum[k] += f.x / (dd * dd);
+        }
+      }
+    }
+  }
+  double* accj = acc + (size_t)j * length;
+  float* oj = opac + (size_t)j * length;
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) {
+    const int i = i0 + k * kFarThreads;
+    if (i <= length) {
+      oj[i - 1] = (float)(accj[i - 1] + sum[k]);
+      accj[i - 1] = 0.0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- spectrum
+struct SpecArgs {
+  const JoshOps* ops;
+  const double *wledge, *contabs, *contscat, *rhox, *hkt;
+  int nedge, stride, nrhox, length;
+  double wbegin, ratio;
+  const float* opac;  // [nrhox][length]
+  double *flux, *cont;
+};
+
+struct SpecWS {
+  JoshWS w;
+  double acont[kKwMax], sigmac[kKwMax], aline[kKwMax], sigmal[kKwMax], sline[kKwMax],
+      bnu[kKwMax];
+};
+
+__global__ void __launch_bounds__(128) k_spectrum(SpecArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nwarp = blockDim.x >> 5;
+  double* rhox_s = reinterpret_cast<double*>(smem_raw);
+  SpecWS* wsa = reinterpret_cast<SpecWS*>(smem_raw + sizeof(double) * kKwMax);
+  SpecWS& S = wsa[wid];
+  for (int j = threadIdx.x; j < a.nrhox; j += blockDim.x) rhox_s[j] = a.rhox[j];
+  __syncthreads();
+  const JoshOps& ops = *a.ops;
+  const int nr = a.nrhox;
+  for (int iw = blockIdx.x * nwarp + wid; iw < a.length; iw += gridDim.x * nwarp) {
+    const double wave8 = a.wbegin * powi(a.ratio, iw);
+    // iedge_sv = 1 + #{e >= 2 : wledge(e) <= wave}  (setup_opacity_sv walk)
+    int lo = 1, hi = a.nedge - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (a.wledge[mid - 1] <= wave8) lo = mid;
+      else hi = mid - 1;
+    }
+    const int ie = lo;
+    const double wl0 = a.wledge[ie - 1], wl1 = a.wledge[ie];
+    const double half = (wl0 + wl1) * 0.5, del = powi(wl1 - wl0, 2) * 0.5;
+    const double c1 = (wave8 - half) * (wave8 - wl1) / del;
+    const double c2 = (wl0 - wave8) * (wave8 - wl1) * 2.0 / del;
+    const double c3 = (wave8 - wl0) * (wave8 - half) / del;
+    const double freq = kClightNms / wave8;
+    const double freq15 = freq / 1.0e15;
+    const double f3 = powi(freq15, 3);
+    for (int j = lane; j < nr; j += 32) {
+      const double* ca = a.contabs + (size_t)j * a.stride + 3 * (ie - 1);
+      const double* cs = a.contscat + (size_t)j * a.stride + 3 * (ie - 1);
+      S.acont[j] = exp10(c1 * ca[0] + c2 * ca[1] + c3 * ca[2]);
+      S.sigmac[j] = exp10(c1 * cs[0] + c2 * cs[1] + c3 * cs[2]);
+      const double ehvkt = exp(-freq * a.hkt[j]);
+      const double stim = 1.0 - ehvkt;
+      const double bnu = kBnuPrefac * f3 * ehvkt / stim;
+      S.bnu[j] = bnu;
+      S.aline[j] = 0.0;
+      S.sigmal[j] = 0.0;
+      S.sline[j] = bnu;
+    }
+    wsync();
+    double surf = 0.0, hnu = 0.0;
+    w_josh(ops, rhox_s, nr, S.acont, S.aline, S.sigmac, S.sigmal, S.bnu, S.sline, S.bnu, S.w,
+           nullptr, &surf, lane);
+    surf = __shfl_sync(0xffffffffu, surf, 0);
+    for (int j = lane; j < nr; j += 32) {
+      const double ehvkt = exp(-freq * a.hkt[j]);
+      const double stim = 1.0 - ehvkt;
+      const float asyn =
+          (float)((double)a.opac[(size_t)j * a.length + iw] * (1.0 - exp(-freq * a.hkt[j])));
+      S.aline[j] = (double)asyn * (1.0 - 0.0);
+      S.sline[j] = S.bnu[j] * stim / (1.0 - ehvkt);
+      S.sigmal[j] = 0.0;
+    }
+    wsync();
+    w_josh(ops, rhox_s, nr, S.acont, S.aline, S.sigmac, S.sigmal, S.bnu, S.sline, S.bnu, S.w,
+           nullptr, &hnu, lane);
+    if (lane == 0) {
+      const double resid = hnu / surf;
+      a.flux[iw] = resid * surf;
+      a.cont[iw] = surf;
+    }
+    wsync();
+  }
+}
+
+}  // namespace atlasgpu

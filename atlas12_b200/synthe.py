@@ -1,0 +1,112 @@
+"""Host-side mirror of SYNTHE's hot path (synthe.f90), on the CUDA C ABI.
+
+Names and argument meaning follow the reference driver:
+
+* ``synthe_grid``      -- the log-lambda grid (synthe.f90:316-324)
+* ``bin_lines``        -- nbuff of every line (mod_mklinelist.f90:898-899)
+* ``continuum``        -- continuum(nbuff) per depth (synthe.f90:483-516)
+* ``line_opacity``     -- opacity_matrix(length, nrhox) (synthe.f90:559-686)
+* ``spectrum``         -- the wavelength loop, two JOSH per point
+                          (synthe.f90:698-718, 797-902)
+* ``Synthe.run``       -- all of the above for one model, as PROGRAM SYNTHE
+
+Arrays are numpy; ``opacity_matrix`` is returned as [nrhox, length] float32,
+the memory layout of the reference's (length, nrhox) REAL(4) array.
+Errors raise AtlasGPUError with the library's message (the reference prints
+and calls EXIT(1)).
+"""
+import numpy as np
+
+from . import _lib
+from ._lib import LTE_LINE, Context, ptr
+
+MAXPROF = 1000000  # synthe_module.f90:219
+RESOLU_MIN = 300000.0  # synthe.f90 refuses coarser grids
+
+
+def synthe_grid(wlbeg, wlend, resolu):
+    if resolu < RESOLU_MIN:
+        raise ValueError(f"resolu below the supported floor: {resolu} < {RESOLU_MIN}")
+    g = _lib.Grid()
+    rc = _lib.lib().atlasgpu_synthe_grid(float(wlbeg), float(wlend), float(resolu), g)
+    if rc != 0:
+        raise _lib.AtlasGPUError(rc, "require 0 < wlbeg < wlend")
+    return dict(ratio=g.ratio, ratiolg=g.ratiolg, wbegin=g.wbegin, length=g.length, ixwlbeg=g.ixwlbeg)
+
+
+def make_lte_lines(nbuff, cgf, nelion, elo, gamrf, gamsf, gamwf, code=None):
+    """Pack SoA line parameters into the 32-byte BIND(C) lte_line records."""
+    n = len(nbuff)
+    rec = np.zeros(n, dtype=LTE_LINE)
+    rec["nbuff"], rec["cgf"], rec["nelion"], rec["elo"] = nbuff, cgf, nelion, elo
+    rec["gamrf"], rec["gamsf"], rec["gamwf"] = gamrf, gamsf, gamwf
+    if code is not None:
+        rec["code"] = code
+    return rec
+
+
+class Synthe:
+    """One SYNTHE synthesis on one GPU context."""
+
+    def __init__(self, ctx: Context, operators):
+        self.ctx = ctx
+        ctx.set_operators(operators["xtau8"], operators["coefj"], operators["coefh"],
+                          operators["ch_j"], operators["ck_j"])
+
+    def bin_lines(self, wlvac, grid):
+        wl = np.ascontiguousarray(wlvac, np.float64)
+        out = np.zeros(wl.size, np.int32)
+        self.ctx.call("atlasgpu_synthe_bin", ptr(wl), wl.size, grid["ratiolg"], grid["ixwlbeg"], ptr(out))
+        return out
+
+    def continuum(self, wledge, continall, grid):
+        we = np.ascontiguousarray(wledge, np.float64)
+        ca = np.ascontiguousarray(continall, np.float64)
+        nrhox, stride = ca.shape
+        out = np.zeros((nrhox, grid["length"]), np.float32)
+        self.ctx.call("atlasgpu_synthe_continuum", ptr(we), we.size, ptr(ca), stride, nrhox,
+                      grid["wbegin"], grid["ratio"], grid["length"], ptr(out))
+        return out
+
+    def line_opacity(self, lines, grid, resolu, continuum, xnfdop, dopple, xne, txnxn, hckt, maxprof=MAXPROF):
+        lines = np.ascontiguousarray(lines, dtype=LTE_LINE)
+        cont = np.ascontiguousarray(continuum, np.float32)
+        xd = np.ascontiguousarray(xnfdop, np.float64)
+        dp = np.ascontiguousarray(dopple, np.float64)
+        nrhox, nspec = xd.shape
+        vecs = [np.ascontiguousarray(v, np.float64) for v in (xne, txnxn, hckt)]
+        out = np.zeros((nrhox, grid["length"]), np.float32)
+        self.ctx.call("atlasgpu_synthe_line_opacity", ptr(lines), lines.size, grid["length"], nrhox,
+                      float(resolu), ptr(cont), ptr(xd), ptr(dp), nspec, *[ptr(v) for v in vecs],
+                      int(maxprof), ptr(out))
+        return out
+
+    def spectrum(self, wledge, contabs, contscat, rhox, hkt, grid, opacity):
+        we = np.ascontiguousarray(wledge, np.float64)
+        ca = np.ascontiguousarray(contabs, np.float64)
+        cs = np.ascontiguousarray(contscat, np.float64)
+        nrhox, stride = ca.shape
+        rx = np.ascontiguousarray(rhox, np.float64)
+        hk = np.ascontiguousarray(hkt, np.float64)
+        op = np.ascontiguousarray(opacity, np.float32)
+        flux = np.zeros(grid["length"])
+        cont = np.zeros(grid["length"])
+        self.ctx.call("atlasgpu_synthe_spectrum", ptr(we), we.size, ptr(ca), ptr(cs), stride, nrhox, ptr(rx),
+                      ptr(hk), grid["wbegin"], grid["ratio"], grid["length"], ptr(op), ptr(flux), ptr(cont))
+        return flux, cont
+
+    def run(self, case):
+        """PROGRAM SYNTHE on a prepared case dict (see synthetic.synthe_case):
+        returns (wavelength_angstrom, flux, continuum_flux, opacity_matrix)."""
+        grid = synthe_grid(case["wlbeg"], case["wlend"], case["resolu"])
+        L = case["lines"]
+        nb = self.bin_lines(L["wlvac"], grid)
+        lines = make_lte_lines(nb, L["cgf"], L["nelion"], L["elo"], L["gamrf"], L["gamsf"], L["gamwf"])
+        atm = case["atm"]
+        cont = self.continuum(case["wledge"], case["continall"], grid)
+        op = self.line_opacity(lines, grid, case["resolu"], cont, atm["xnfdop"], atm["dopple"], atm["xne"],
+                               atm["txnxn"], atm["hckt"])
+        flux, cflux = self.spectrum(case["wledge"], case["contabs"], case["contscat"], atm["rhox"], atm["hkt"],
+                                    grid, op)
+        wave = grid["wbegin"] * grid["ratio"] ** np.arange(grid["length"]) * 10.0
+        return wave, flux, cflux, op

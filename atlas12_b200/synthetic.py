@@ -1,0 +1,157 @@
+"""Seeded synthetic workloads with the shapes of the named configurations.
+
+There is no network and the reference's line lists are not distributed with
+it, so every workload is synthetic (numpy.random.default_rng(seed)):
+
+* SYNTHE (one atmosphere): 72-depth Eddington grey model (Teff, log g), lines
+  with lambda uniform in a window, log gf ~ N(-2, 1.5) and E_low ~ U(0, 8) eV
+  for atoms, log gf ~ N(-4, 1) and E_low ~ U(0, 3) eV for molecules,
+  log gamma_rad / Stark / vdW ~ N(8, 0.3) / N(-5.5, 0.5) / N(-7.5, 0.3)
+  normalised by 4 pi nu as the gfall reader does (mod_mklinelist.f90:996-1006).
+* ATLAS12 opacity sampling: LINEDATA records with int16 fields
+  NINT(log10(x)*1000 + 16384) (atlas12_modules.f90:19497-19501).
+
+Populations and continuum come from atlas12_b200.surrogate.
+"""
+import numpy as np
+
+from . import surrogate as sg
+
+C_NM = 2.99792458e17
+EV_CM = 8065.543937
+
+
+def synthe_edges(wlbeg, wlend):
+    """Continuum edge list covering [wlbeg, wlend] with the H I edges that fall
+    inside, ~2 nm apart, padded on both sides (wledge_m analogue)."""
+    lo, hi = wlbeg * 0.98, wlend * 1.02
+    n = max(int((hi - lo) / 2.0), 4)
+    e = list(np.linspace(lo, hi, n + 1))
+    for h in (91.175, 364.70, 820.6):
+        if lo < h < hi:
+            e.append(h)
+    return np.unique(np.array(e))
+
+
+def synthe_continuum_tables(wledge, t, p, e=None):
+    """log10 kappa tables on (left edge, mid, right edge) of every interval,
+    [nrhox, 3*(nedge-1)]: continall (abs+scat), contabs, contscat."""
+    ne = wledge.size
+    pts = []
+    for i in range(ne - 1):
+        a, b = wledge[i], wledge[i + 1]
+        eps = (b - a) * 1e-9
+        pts += [a + eps, 0.5 * (a + b), b - eps]
+    ka, sgm = sg.continuum_opacity(np.array(pts), t, p, e)
+    return (np.log10(ka + sgm).T.copy(), np.log10(ka).T.copy(), np.log10(sgm).T.copy())
+
+
+def synthe_atmosphere(teff=5777.0, logg=4.44, vturb=1.5, nrhox=72, ross=None):
+    m = sg.grey_model(teff, logg, nrhox=nrhox, ross=ross)
+    pop = sg.populations(m["t"], m["p"], vturb)
+    t = m["t"]
+    hkt = sg.HPLANCK / (sg.KBOL * t)
+    hckt = hkt * sg.CLIGHT
+    # SYNTHE keeps these as REAL(4) values (synthe.f90:374-392)
+    xne32 = pop["xne"].astype(np.float32).astype(np.float64)
+    nh = pop["xnfp"][:, 0] * 2.0
+    txnxn = ((nh + 0.42 * 0.085 * nh) * (t.astype(np.float32) / 10000.0) ** 0.3).astype(np.float32)
+    xnfdop = np.where(pop["dopple"] > 0, pop["xnfp"] / pop["rho"][:, None] / np.maximum(pop["dopple"], 1e-300), 0.0)
+    return dict(model=m, t=t, p=m["p"], rhox=m["rhox"], rho=pop["rho"], hkt=hkt, hckt=hckt,
+                xne=xne32, txnxn=txnxn.astype(np.float64), xnfdop=xnfdop, dopple=pop["dopple"],
+                eos=pop, teff=teff, logg=logg)
+
+
+def synthe_lines(n, wlbeg, wlend, seed=1, mol_frac=0.0):
+    """Raw line parameters (vacuum nm, gf, elo cm^-1, damping) before binning."""
+    rng = np.random.default_rng(seed)
+    wl = np.sort(rng.uniform(wlbeg, wlend, n))
+    is_mol = rng.uniform(size=n) < mol_frac
+    loggf = np.where(is_mol, rng.normal(-4.0, 1.0, n), rng.normal(-2.0, 1.5, n))
+    elo_ev = np.where(is_mol, rng.uniform(0.0, 3.0, n), rng.uniform(0.0, 8.0, n))
+    lgr = rng.normal(8.0, 0.3, n)
+    lgs = rng.normal(-5.5, 0.5, n)
+    lgw = rng.normal(-7.5, 0.3, n)
+    atoms = [sg.nelion(z, s) for z in sg.METALS[:, 0] for s in (1, 2)]
+    mols = [sg.mol_nelion(s) for s in sg.MOLECULES[:, 0]]
+    nel = np.where(is_mol, rng.choice(mols, n), rng.choice(atoms, n)).astype(np.int32)
+    # reader conversions (mod_mklinelist.f90:996-1006)
+    frelin = 2.99792458e17 / wl
+    gf = (10.0 ** loggf.astype(np.float32)).astype(np.float32)
+    cgf = (0.026538 / 1.77245 * gf.astype(np.float64) / frelin).astype(np.float32)
+    frq4pi = 12.5664 * frelin
+    return dict(wlvac=wl, cgf=cgf, nelion=nel, elo=(elo_ev * EV_CM).astype(np.float32),
+                gamrf=(10.0 ** lgr / frq4pi).astype(np.float32),
+                gamsf=(10.0 ** lgs / frq4pi).astype(np.float32),
+                gamwf=(10.0 ** lgw / frq4pi).astype(np.float32))
+
+
+def synthe_case(nlines=20000, wlbeg=400.0, wlend=410.0, resolu=500000.0, seed=1, teff=5777.0,
+                logg=4.44, vturb=1.5, mol_frac=0.0, nrhox=72, ross=None):
+    """Complete SYNTHE input set (the small CPU-runnable case by default)."""
+    atm = synthe_atmosphere(teff, logg, vturb, nrhox, ross=ross)
+    wledge = synthe_edges(wlbeg, wlend)
+    cont_all, cont_abs, cont_scat = synthe_continuum_tables(wledge, atm["t"], atm["p"], atm["eos"])
+    lines = synthe_lines(nlines, wlbeg, wlend, seed=seed, mol_frac=mol_frac)
+    return dict(atm=atm, wledge=wledge, continall=cont_all, contabs=cont_abs, contscat=cont_scat,
+                lines=lines, wlbeg=wlbeg, wlend=wlend, resolu=resolu)
+
+
+# ---------------------------------------------------------------- ATLAS12
+def encode_i16(x):
+    """NINT(log10(x)*1000 + 16384) clipped to INTEGER(2) (atlas12_modules.f90:19497-19501)."""
+    v = np.rint(np.log10(x) * 1000.0 + 16384.0)
+    return np.clip(v, -32768, 32767).astype(np.int16)
+
+
+def pack_linedata(iwl, ielion, ielo, igflog, igr, igs, igw):
+    """LINEREC = [IWL | IELION,IELO | IGFLOG,IGR | IGS,IGW] (atlas12_modules.f90:1950-1977)."""
+    def pair(lo, hi):
+        return (lo.astype(np.int16).view(np.uint16).astype(np.uint32) |
+                (hi.astype(np.int16).view(np.uint16).astype(np.uint32) << 16)).view(np.int32)
+    return np.stack([iwl.astype(np.int32), pair(ielion, ielo), pair(igflog, igr), pair(igs, igw)], axis=1)
+
+
+def atlas_lines(n, wl_lo, wl_hi, seed=2, mol_frac=0.0):
+    """LINEDATA for the opacity-sampling line loop, lambda log-uniform."""
+    rng = np.random.default_rng(seed)
+    ratiolg = np.log(1.0 + 1.0 / 2000000.0)
+    wl = np.sort(np.exp(rng.uniform(np.log(wl_lo), np.log(wl_hi), n)))
+    iwl = np.floor(np.log(wl) / ratiolg + 0.5).astype(np.int64)
+    is_mol = rng.uniform(size=n) < mol_frac
+    loggf = np.where(is_mol, rng.normal(-4.0, 1.0, n), rng.normal(-2.0, 1.5, n))
+    elo_ev = np.where(is_mol, rng.uniform(0.0, 3.0, n), rng.uniform(0.0, 8.0, n))
+    atoms = [sg.nelion(z, s) for z in sg.METALS[:, 0] for s in (1, 2)]
+    mols = [sg.mol_nelion(s) for s in sg.MOLECULES[:, 0]]
+    nel = np.where(is_mol, rng.choice(mols, n), rng.choice(atoms, n))
+    # IELION = 10*NELION (+ isotope digit 0); gammas are per-unit-frequency
+    # widths times 4 pi c / lambda -> GAMMA = TABLOG(IG)*WLVAC*(1/(4 pi c)).
+    gr = 10.0 ** rng.normal(8.0, 0.3, n)
+    gs = 10.0 ** rng.normal(-5.5, 0.5, n)
+    gw = 10.0 ** rng.normal(-7.5, 0.3, n)
+    return pack_linedata(iwl, (nel * 10).astype(np.int16), encode_i16(elo_ev * EV_CM),
+                         encode_i16(10.0 ** loggf), encode_i16(gr), encode_i16(gs), encode_i16(gw))
+
+
+def atlas_waveset(nustart=9599, numnu=30000):
+    """WAVESET(NU) = 10**(1 + 1e-4*(NU+NUSTART-1)) and RCOSET trapezoid weights
+    (atlas12c.f90:451-491)."""
+    nu = np.arange(1, numnu + 1)
+    ws = 10.0 ** (1.0 + 0.0001 * (nu + nustart - 1))
+    f = C_NM / ws
+    rc = np.zeros(numnu)
+    rc[0] = (f[0] - f[1]) * 1.5
+    rc[1:-1] = (f[:-2] - f[2:]) * 0.5
+    rc[-1] = (f[-2] + f[-1]) * 0.25
+    return ws, rc
+
+
+def geometric_waveset(wl_lo=9.0, wl_hi=160000.0, numnu=30000):
+    """log-spaced grid over the stated span with the same trapezoid weights."""
+    ws = np.geomspace(wl_lo, wl_hi, numnu)
+    f = C_NM / ws
+    rc = np.zeros(numnu)
+    rc[0] = (f[0] - f[1]) * 1.5
+    rc[1:-1] = (f[:-2] - f[2:]) * 0.5
+    rc[-1] = (f[-2] + f[-1]) * 0.25
+    return ws, rc

@@ -1,0 +1,1028 @@
+/*
+ * oracle.c -- CPU restatement of the ATLAS12 / SYNTHE hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (see oracle.h): the checker for the CUDA path,
+ * never the product.  Every function cites the reference routine it
+ * restates (paths inside cconroy20/atlas12).  Statement order and operand
+ * order follow the reference so that IEEE results agree to the last few
+ * ulps; the file is compiled with -ffp-contract=off.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define KW_MAX 128
+
+/* mod_constants (atlas12_modules.f90:315-355) */
+static const double PI_ = 3.141592653589793;
+static const double SQRTPI = 1.7724538509055159;
+static const double INVSQRTPI = 0.5641895835477563;
+static const double CLIGHT_NMS = 2.99792458e17;
+static const double HPLANCK = 6.62607015e-27;
+static const double CLIGHT = 2.99792458e10;
+static const double LINE_CUTOFF = 1.0e-3;      /* :175 */
+static const double EULER_M1 = 0.922784335098467; /* :2373 */
+
+static double bnu_prefac(void) { return 2.0 * HPLANCK / (CLIGHT * CLIGHT) * 1.0e45; }
+
+/* gfortran lowers REAL(8)**INTEGER to libgcc's binary exponentiation. */
+double orc_powi(double x, int m) {
+  unsigned n = m < 0 ? (unsigned)(-m) : (unsigned)m;
+  double y = (n % 2) ? x : 1.0;
+  while (n >>= 1) {
+    x = x * x;
+    if (n % 2) y = y * x;
+  }
+  return m < 0 ? 1.0 / y : y;
+}
+
+/* ======================================================================
+ * Numerics
+ * ==================================================================== */
+
+/* PARCOE, atlas12_modules.f90:5358-5434 */
+void orc_parcoe(const double *f, const double *x, double *a, double *b,
+                double *c, int n) {
+  int j;
+  double d, wt;
+  c[0] = 0.0;
+  b[0] = (f[1] - f[0]) / (x[1] - x[0]);
+  a[0] = f[0] - x[0] * b[0];
+  c[n - 1] = 0.0;
+  b[n - 1] = (f[n - 1] - f[n - 2]) / (x[n - 1] - x[n - 2]);
+  a[n - 1] = f[n - 1] - x[n - 1] * b[n - 1];
+  if (n == 2) return;
+  if (n == 3) {
+    a[1] = a[2];
+    b[1] = b[2];
+    c[1] = c[2];
+    return;
+  }
+  for (j = 1; j <= n - 2; ++j) {
+    d = (f[j] - f[j - 1]) / (x[j] - x[j - 1]);
+    c[j] = f[j + 1] / ((x[j + 1] - x[j]) * (x[j + 1] - x[j - 1])) -
+           f[j] / ((x[j] - x[j - 1]) * (x[j + 1] - x[j])) +
+           f[j - 1] / ((x[j] - x[j - 1]) * (x[j + 1] - x[j - 1]));
+    b[j] = d - (x[j] + x[j - 1]) * c[j];
+    a[j] = f[j - 1] - x[j - 1] * d + x[j] * x[j - 1] * c[j];
+  }
+  c[1] = 0.0;
+  b[1] = (f[2] - f[1]) / (x[2] - x[1]);
+  a[1] = f[1] - x[1] * b[1];
+  c[2] = 0.0;
+  b[2] = (f[3] - f[2]) / (x[3] - x[2]);
+  a[2] = f[2] - x[2] * b[2];
+  for (j = 1; j <= n - 2; ++j) {
+    if (c[j] != 0.0) {
+      wt = fabs(c[j + 1]) / (fabs(c[j + 1]) + fabs(c[j]));
+      a[j] = a[j + 1] + wt * (a[j] - a[j + 1]);
+      b[j] = b[j + 1] + wt * (b[j] - b[j + 1]);
+      c[j] = c[j + 1] + wt * (c[j] - c[j + 1]);
+    }
+  }
+  a[n - 2] = a[n - 1];
+  b[n - 2] = b[n - 1];
+  c[n - 2] = c[n - 1];
+}
+
+/* INTEG (IQUAD=0 branch), atlas12_modules.f90:5293-5324 */
+void orc_integ(const double *x, const double *f, double *fint, int n,
+               double start) {
+  double a[KW_MAX], b[KW_MAX], c[KW_MAX];
+  orc_parcoe(f, x, a, b, c, n);
+  fint[0] = start;
+  for (int i = 0; i < n - 1; ++i) {
+    double xlo = x[i], xhi = x[i + 1];
+    fint[i + 1] = fint[i] + (a[i] + b[i] * 0.5 * (xhi + xlo) +
+                             c[i] / 3.0 * ((xhi + xlo) * xhi + xlo * xlo)) *
+                                (xhi - xlo);
+  }
+}
+
+/* DERIV, atlas12_modules.f90:5228-5266 */
+void orc_deriv(const double *x, const double *f, double *dfdx, int n) {
+  dfdx[0] = (f[1] - f[0]) / (x[1] - x[0]);
+  dfdx[n - 1] = (f[n - 1] - f[n - 2]) / (x[n - 1] - x[n - 2]);
+  if (n == 2) return;
+  double s = fabs(x[1] - x[0]) / (x[1] - x[0]);
+  for (int j = 1; j <= n - 2; ++j) {
+    double scale = fmax(fmax(fabs(f[j - 1]), fabs(f[j])), fabs(f[j + 1])) / fabs(x[j]);
+    if (scale == 0.0) scale = 1.0;
+    double dr = (f[j + 1] - f[j]) / (x[j + 1] - x[j]) / scale;
+    double dl = (f[j] - f[j - 1]) / (x[j] - x[j - 1]) / scale;
+    double tr = dr / (s * sqrt(1.0 + dr * dr) + 1.0);
+    double tl = dl / (s * sqrt(1.0 + dl * dl) + 1.0);
+    dfdx[j] = (tr + tl) / (1.0 - tr * tl) * scale;
+  }
+}
+
+/* MAP1, atlas12_modules.f90:5570-5692.  L is kept 1-based as in the source. */
+int orc_map1(const double *xold, const double *fold, int nold,
+             const double *xnew, double *fnew, int nnew) {
+#define XO(i) xold[(i)-1]
+#define FO(i) fold[(i)-1]
+  double a = 0, b = 0, c = 0, abac = 0, bbac = 0, cbac = 0, afor = 0, bfor = 0,
+         cfor = 0, d, wt;
+  int l = 2, ll = 0, l1, l2;
+  for (int k = 0; k < nnew; ++k) {
+    int past = 0;
+    while (xnew[k] >= XO(l)) {
+      l = l + 1;
+      if (l > nold) {
+        past = 1;
+        break;
+      }
+    }
+    if (!past && l == ll) {
+      fnew[k] = a + (b + c * xnew[k]) * xnew[k];
+      continue;
+    }
+    if (l <= 3 || past) {
+      l = l < nold ? l : nold;
+      if (!past && l == ll) {
+        fnew[k] = a + (b + c * xnew[k]) * xnew[k];
+        continue;
+      }
+      c = 0.0;
+      b = (FO(l) - FO(l - 1)) / (XO(l) - XO(l - 1));
+      a = FO(l) - XO(l) * b;
+      ll = l;
+      fnew[k] = a + b * xnew[k];
+      continue;
+    }
+    l1 = l - 1;
+    if (l == ll + 1 && l != 3 && l != 4) {
+      cbac = cfor;
+      bbac = bfor;
+      abac = afor;
+    } else {
+      l2 = l - 2;
+      d = (FO(l1) - FO(l2)) / (XO(l1) - XO(l2));
+      cbac = FO(l) / ((XO(l) - XO(l1)) * (XO(l) - XO(l2))) +
+             (FO(l2) / (XO(l) - XO(l2)) - FO(l1) / (XO(l) - XO(l1))) /
+                 (XO(l1) - XO(l2));
+      bbac = d - (XO(l1) + XO(l2)) * cbac;
+      abac = FO(l2) - XO(l2) * d + XO(l1) * XO(l2) * cbac;
+    }
+    if (l >= nold) {
+      a = abac;
+      b = bbac;
+      c = cbac;
+      ll = l;
+      fnew[k] = a + (b + c * xnew[k]) * xnew[k];
+      continue;
+    }
+    d = (FO(l) - FO(l1)) / (XO(l) - XO(l1));
+    cfor = FO(l + 1) / ((XO(l + 1) - XO(l)) * (XO(l + 1) - XO(l1))) +
+           (FO(l1) / (XO(l + 1) - XO(l1)) - FO(l) / (XO(l + 1) - XO(l))) /
+               (XO(l) - XO(l1));
+    bfor = d - (XO(l) + XO(l1)) * cfor;
+    afor = FO(l1) - XO(l1) * d + XO(l) * XO(l1) * cfor;
+    wt = 0.0;
+    if (fabs(cfor) != 0.0) wt = fabs(cfor) / (fabs(cfor) + fabs(cbac));
+    a = afor + wt * (abac - afor);
+    b = bfor + wt * (bbac - bfor);
+    c = cfor + wt * (cbac - cfor);
+    ll = l;
+    fnew[k] = a + (b + c * xnew[k]) * xnew[k];
+  }
+  return ll - 1;
+#undef XO
+#undef FO
+}
+
+/* SOLVIT, atlas12_modules.f90:5739-5847.  A column-major n x n. */
+void orc_solvit(double *A, int n, double *B, int *ipivot) {
+#define AA(r, c) A[((c)-1) * n + (r)-1]
+#define BB(r) B[(r)-1]
+  const double PIVOT_TOL = 1.0e-30;
+  int i, j, k, m;
+  double pivot, t, c;
+  for (i = 1; i <= n - 1; ++i) {
+    m = i;
+    for (k = i + 1; k <= n; ++k)
+      if (fabs(AA(k, i)) > fabs(AA(m, i))) m = k;
+    ipivot[i - 1] = m;
+    if (m != i) {
+      for (k = i + 1; k <= n; ++k) {
+        t = AA(i, k);
+        AA(i, k) = AA(m, k);
+        AA(m, k) = t;
+      }
+    }
+    if (fabs(AA(m, i)) < PIVOT_TOL) AA(m, i) = copysign(PIVOT_TOL, AA(m, i));
+    pivot = 1.0 / AA(m, i);
+    AA(m, i) = AA(i, i);
+    AA(i, i) = pivot;
+    for (k = i + 1; k <= n; ++k) AA(k, i) = AA(k, i) * pivot;
+    for (j = i + 1; j <= n; ++j) {
+      c = AA(i, j);
+      if (c == 0.0) continue;
+      for (k = i + 1; k <= n; ++k) AA(k, j) = AA(k, j) - AA(k, i) * c;
+    }
+  }
+  if (fabs(AA(n, n)) < PIVOT_TOL) AA(n, n) = copysign(PIVOT_TOL, AA(n, n));
+  AA(n, n) = 1.0 / AA(n, n);
+  for (i = 1; i <= n - 1; ++i) {
+    m = ipivot[i - 1];
+    if (m != i) {
+      t = BB(m);
+      BB(m) = BB(i);
+      BB(i) = t;
+    }
+    c = BB(i);
+    for (k = i + 1; k <= n; ++k) BB(k) = BB(k) - AA(k, i) * c;
+  }
+  for (j = n; j >= 2; --j) {
+    BB(j) = BB(j) * AA(j, j);
+    c = BB(j);
+    for (k = 1; k <= j - 1; ++k) BB(k) = BB(k) - AA(k, j) * c;
+  }
+  BB(1) = BB(1) * AA(1, 1);
+#undef AA
+#undef BB
+}
+
+/* EXPI, atlas12_modules.f90:21103-21225 (Cody & Thacher 1968 rational fits).
+ * The reference caches E1 between calls; the cache does not change values. */
+double orc_expi(int n, double x) {
+  static const double A0 = -44178.5471728217, A1 = 57721.7247139444,
+                      A2 = 9938.31388962037, A3 = 1842.11088668000,
+                      A4 = 101.093806161906, A5 = 5.03416184097568;
+  static const double B0 = 76537.3323337614, B1 = 32597.1881290275,
+                      B2 = 6106.10794245759, B3 = 635.419418378382,
+                      B4 = 37.2298352833327;
+  static const double C0 = 4.65627107975096e-7, C1 = 0.999979577051595,
+                      C2 = 9.04161556946329, C3 = 24.3784088791317,
+                      C4 = 23.0192559391333, C5 = 6.90522522784444,
+                      C6 = 0.430967839469389;
+  static const double D1 = 10.0411643829054, D2 = 32.4264210695138,
+                      D3 = 41.2807841891424, D4 = 20.4494785013794,
+                      D5 = 3.31909213593302, D6 = 0.103400130404874;
+  static const double E0 = -0.999999999998447, E1C = -26.6271060431811,
+                      E2 = -241.055827097015, E3 = -895.927957772937,
+                      E4 = -1298.85688746484, E5 = -545.374158883133,
+                      E6 = -5.66575206533869;
+  static const double F1 = 28.6271060422192, F2 = 292.310039388533,
+                      F3 = 1332.78537748257, F4 = 2777.61949509163,
+                      F5 = 2404.01713225909, F6 = 631.657483280800;
+  double ex = exp(-x), e1;
+  if (x > 4.0) {
+    e1 = (ex + ex * (E0 + (E1C + (E2 + (E3 + (E4 + (E5 + E6 / x) / x) / x) / x) / x) / x) /
+                   (x + F1 + (F2 + (F3 + (F4 + (F5 + F6 / x) / x) / x) / x) / x)) /
+         x;
+  } else if (x > 1.0) {
+    e1 = ex * (C6 + (C5 + (C4 + (C3 + (C2 + (C1 + C0 * x) * x) * x) * x) * x) * x) /
+         (D6 + (D5 + (D4 + (D3 + (D2 + (D1 + x) * x) * x) * x) * x) * x);
+  } else if (x > 0.0) {
+    e1 = (A0 + (A1 + (A2 + (A3 + (A4 + A5 * x) * x) * x) * x) * x) /
+             (B0 + (B1 + (B2 + (B3 + (B4 + x) * x) * x) * x) * x) -
+         log(x);
+  } else {
+    e1 = 0.0;
+  }
+  double r = e1;
+  if (n == 1) return r;
+  for (int i = 1; i <= n - 1; ++i) r = (ex - x * r) / (double)i;
+  return r;
+}
+
+/* ======================================================================
+ * Voigt functions
+ * ==================================================================== */
+
+/* Weideman (1994) N=32 coefficients: computed by tests/golden/make_golden.py
+ * from the published construction (FFT of exp(-t^2)(L^2+t^2) on
+ * t = L tan(theta/2)), Horner order.  They coincide bit-for-bit with the
+ * reference's AWEI table (synthe_module.f90:91-126). */
+static const double WEI_L = 4.75682846001088411;
+static const double WEI_A[32] = {
+    -1.30317978630500875e-12, 3.74088129316536249e-12, 8.03036789996388945e-12,
+    -2.15436320778387687e-11, -5.54423594816646238e-11, 1.16582510935237737e-10,
+    4.15374309183345315e-10, -5.23102048119632885e-10, -3.20801509172336887e-09,
+    8.12488945684665156e-10, 2.37975567798974168e-08, 2.29304390650999664e-08,
+    -1.48130789151209774e-07, -4.18407637021697758e-07, 4.25583313757500854e-07,
+    4.40153173157854990e-06, 6.82103194400198485e-06, -2.14096192017107501e-05,
+    -1.30754492546153456e-04, -2.45329802700214317e-04, 3.92591360700703107e-04,
+    4.51954110534921738e-03, 1.90061557848454077e-02, 5.73044035298372195e-02,
+    1.40607162268937685e-01, 2.95444510715087316e-01, 5.46013972063934094e-01,
+    9.01925489364799882e-01, 1.34554416923454490e+00, 1.82566962963248147e+00,
+    2.26353729990026764e+00, 2.57225340812456960e+00};
+
+/* voigt_profile, synthe_module.f90:463-537, without the final REAL(4). */
+double orc_voigt_weideman(double v, double a) {
+  double x = fabs(v), y = a, s = x + y;
+  if (s > 15.0) {
+    double dr = x * x - y * y - 0.5;
+    double di = 2.0 * x * y;
+    double d2 = dr * dr + di * di;
+    return (-y * dr + x * di) / (SQRTPI * d2);
+  }
+  double dr = WEI_L + y, di = -x;
+  double nr = WEI_L - y, ni = x;
+  double d2 = dr * dr + di * di;
+  double zr = (nr * dr + ni * di) / d2;
+  double zi = (ni * dr - nr * di) / d2;
+  double pr = WEI_A[0], pim = 0.0, tmp;
+  for (int k = 1; k < 32; ++k) {
+    tmp = pr * zr - pim * zi + WEI_A[k];
+    pim = pr * zi + pim * zr;
+    pr = tmp;
+  }
+  double sq_r = dr * dr - di * di;
+  double sq_i = 2.0 * dr * di;
+  double sq_d = sq_r * sq_r + sq_i * sq_i;
+  double term1 = 2.0 * (pr * sq_r + pim * sq_i) / sq_d;
+  double term2 = dr / (SQRTPI * d2);
+  return term1 + term2;
+}
+
+float orc_voigt_profile(float v, float a) {
+  return (float)orc_voigt_weideman((double)fabsf(v), (double)a);
+}
+
+/* TABVOIGT, atlas12_modules.f90:19796-19851 */
+void orc_tabvoigt(double vsteps, int n, const double *tabvi,
+                  const double *tabh1, int ntab, double *h0tab, double *h1tab,
+                  double *h2tab) {
+  for (int i = 1; i <= n; ++i) h0tab[i - 1] = (double)(i - 1) / vsteps;
+  orc_map1(tabvi, tabh1, ntab, h0tab, h1tab, n);
+  for (int i = 1; i <= n; ++i) {
+    double vv = orc_powi((double)(i - 1) / vsteps, 2);
+    h0tab[i - 1] = exp(-vv);
+    h2tab[i - 1] = h0tab[i - 1] - (vv + vv) * h0tab[i - 1];
+  }
+}
+
+/* VOIGT, atlas12_modules.f90:21033-21097 (tables 1-based via IV) */
+double orc_voigt_kurucz(double v, double a, const double *h0, const double *h1,
+                        const double *h2) {
+  int iv = (int)(v * 200.0 + 1.5);
+  if (a < 0.2) {
+    if (v <= 10.0) return (h2[iv - 1] * a + h1[iv - 1]) * a + h0[iv - 1];
+    return 0.5642 * a / orc_powi(v, 2);
+  } else if (a <= 1.4 && a + v <= 3.2) {
+    double vv = v * v;
+    double hh1 = h1[iv - 1] + h0[iv - 1] * 1.12838;
+    double hh2 = h2[iv - 1] + hh1 * 1.12838 - h0[iv - 1];
+    double hh3 = (1.0 - h2[iv - 1]) * 0.37613 - hh1 * 0.66667 * vv + hh2 * 1.12838;
+    double hh4 = (3.0 * hh3 - hh1) * 0.37613 + h0[iv - 1] * 0.66667 * vv * vv;
+    return ((((hh4 * a + hh3) * a + hh2) * a + hh1) * a + h0[iv - 1]) *
+           (((-.122727278 * a + .532770573) * a - .96284325) * a + .979895032);
+  } else {
+    double aa = a * a, vv = v * v;
+    double u = (aa + vv) * 1.4142;
+    double r = a * 0.79788 / u;
+    if (a <= 100.0) {
+      double aau = aa / u, vvu = vv / u, uu = u * u;
+      r = ((((aau - 10.0 * vvu) * aau * 3.0 + 15.0 * vvu * vvu) + 3.0 * vv - aa) / uu + 1.0) * r;
+    }
+    return r;
+  }
+}
+
+/* ======================================================================
+ * SYNTHE grid, binning, continuum, line opacity
+ * ==================================================================== */
+
+/* synthe.f90:316-324 */
+void orc_synthe_grid(double wlbeg, double wlend, double resolu, orc_grid_t *g) {
+  g->ratio = 1.0 + 1.0 / resolu;
+  g->ratiolg = log(g->ratio);
+  g->length = (int32_t)(log(wlend / wlbeg) / g->ratiolg);
+  g->ixwlbeg = (int32_t)(log(wlbeg) / g->ratiolg);
+  g->wbegin = exp((double)g->ixwlbeg * g->ratiolg);
+  if (g->wbegin < wlbeg) {
+    g->ixwlbeg = g->ixwlbeg + 1;
+    g->wbegin = exp((double)g->ixwlbeg * g->ratiolg);
+  }
+}
+
+/* mod_mklinelist.f90:898-899 */
+int32_t orc_synthe_nbuff(double wlvac, double ratiolg, int32_t ixwlbeg) {
+  int32_t ixwl = (int32_t)(log(wlvac) / ratiolg + 0.5);
+  return ixwl - ixwlbeg + 1;
+}
+
+/* synthe.f90:483-516: quadratic interpolation in log10 kappa across the
+ * continuum edges, floor at -15, then 10**x (REAL(4) in REF32). */
+void orc_synthe_continuum(int mode, const double *wledge, int nedge,
+                          const double *continall, int ncont_stride, int nrhox,
+                          double wbegin, double ratio, int length, void *out) {
+  double *half = (double *)malloc(sizeof(double) * nedge);
+  double *del = (double *)malloc(sizeof(double) * nedge);
+  for (int ie = 2; ie <= nedge; ++ie) {
+    half[ie - 2] = (wledge[ie - 2] + wledge[ie - 1]) * 0.5;
+    del[ie - 2] = orc_powi(wledge[ie - 1] - wledge[ie - 2], 2) * 0.5;
+  }
+  for (int j = 0; j < nrhox; ++j) {
+    const double *ab = continall + (size_t)j * ncont_stride;
+    int iedge = 1;
+    for (int i = 1; i <= length; ++i) {
+      double w = wbegin * orc_powi(ratio, i - 1);
+      while (w >= wledge[iedge] && iedge < nedge - 1) iedge = iedge + 1;
+      const double *q = ab + 3 * (iedge - 1);
+      double wl0 = wledge[iedge - 1], wl1 = wledge[iedge];
+      double h = half[iedge - 1], dd = del[iedge - 1];
+      double v = ((w - h) * (w - wl1) * q[0] + (wl0 - w) * (w - wl1) * 2.0 * q[1] +
+                  (w - wl0) * (w - h) * q[2]) /
+                 dd;
+      if (mode == ORC_REF32) {
+        float cf = (float)v;
+        if (cf < -15.0f) cf = -15.0f;
+        ((float *)out)[(size_t)j * length + i - 1] = powf(10.0f, cf);
+      } else {
+        if (v < -15.0) v = -15.0;
+        ((double *)out)[(size_t)j * length + i - 1] = pow(10.0, v);
+      }
+    }
+  }
+  free(half);
+  free(del);
+}
+
+/* Scatter one line's profile into buf (1-based bins).  synthe.f90:652-682 */
+#define SCATTER(BUF, T)                                                        \
+  do {                                                                         \
+    if (nb + nstep < 1 || nb - nstep > length) break;                          \
+    if (nb < length) {                                                         \
+      int maxred = (length - nb) < nstep ? (length - nb) : nstep;              \
+      int mb = 1 > (1 - nb) ? 1 : (1 - nb);                                    \
+      for (int is = mb; is <= maxred; ++is) BUF[nb + is - 1] += (T)prof[is];    \
+      if (nb <= 1) break;                                                      \
+    }                                                                          \
+    int maxblue = (nb - 1) < nstep ? (nb - 1) : nstep;                         \
+    int mb2 = 1 > (nb - length) ? 1 : (nb - length);                           \
+    for (int is = mb2; is <= maxblue; ++is) BUF[nb - is - 1] += (T)prof[is];    \
+  } while (0)
+
+/* SYNTHE LTE line loop, synthe.f90:559-683 (NLTE tags and the Ca I 4227
+ * developer switch are off in production: NLTE_MODE=0, CA4227_MODE=0). */
+void orc_synthe_line_opacity(int mode, const orc_lines_t *L, int length,
+                             int nrhox, double resolu, const void *continuum,
+                             const double *xnfdop, const double *dopple,
+                             int nspec, const double *xne, const double *txnxn,
+                             const double *hckt, int maxprof,
+                             double *opacity_f64_out, float *opacity_out) {
+  /* the core walk runs to n10dop even when MAXPROF is smaller */
+  double dmax = 0.0;
+  for (size_t k = 0; k < (size_t)nrhox * nspec; ++k) dmax = fmax(dmax, dopple[k]);
+  size_t cap = (size_t)maxprof + (size_t)(10.0 * dmax * resolu) + 2;
+  double *prof = (double *)malloc(sizeof(double) * cap);
+  float *pf = (float *)malloc(sizeof(float) * cap);
+  float *bufs = (float *)malloc(sizeof(float) * (size_t)length);
+  double *bufd = (double *)malloc(sizeof(double) * (size_t)length);
+  for (int j = 0; j < nrhox; ++j) {
+    const double *xd = xnfdop + (size_t)j * nspec;
+    const double *dp = dopple + (size_t)j * nspec;
+    memset(bufs, 0, sizeof(float) * length);
+    memset(bufd, 0, sizeof(double) * length);
+    for (int64_t il = 0; il < L->n; ++il) {
+      int nb = L->nbuff[il];
+      int nel = L->nelion[il] - 1;
+      int ic = nb < 1 ? 1 : (nb > length ? length : nb);
+      int nstep, n10dop = (int)(10.0 * dp[nel] * resolu);
+      if (mode == ORC_REF32) {
+        const float *cont = (const float *)continuum + (size_t)j * length;
+        float kappa0 = L->cgf[il] * (float)xd[nel];
+        float kapmin = cont[ic - 1] * (float)LINE_CUTOFF;
+        if (kappa0 < kapmin) continue;
+        kappa0 = kappa0 * (float)exp(-(double)L->elo[il] * hckt[j]);
+        if (kappa0 < kapmin) continue;
+        float gw = L->gamwf[il] * (float)txnxn[j];
+        float adamp = (float)(((double)L->gamrf[il] + (double)L->gamsf[il] * xne[j] + (double)gw) / dp[nel]);
+        float dopple_nel = (float)dp[nel];
+        if (nb >= 1 && nb <= length) bufs[nb - 1] += kappa0 * orc_voigt_profile(0.0f, adamp);
+        float dvoigt = 1.0f / dopple_nel / (float)resolu;
+        for (nstep = 1; nstep <= n10dop; ++nstep) {
+          pf[nstep] = kappa0 * orc_voigt_profile((float)nstep * dvoigt, adamp);
+          if (pf[nstep] < kapmin) break;
+        }
+        if (nstep > n10dop) {
+          float xs = (float)n10dop;
+          float x_wing = pf[n10dop] * (xs * xs);
+          float qs = sqrtf(x_wing / kapmin);
+          int maxstep = qs >= (float)maxprof ? maxprof : (int)qs + 1;
+          if (maxstep > maxprof) maxstep = maxprof;
+          for (nstep = n10dop + 1; nstep <= maxstep; ++nstep) {
+            float s = (float)nstep;
+            pf[nstep] = x_wing / (s * s);
+          }
+          nstep = maxstep;
+        }
+        /* accumulate the REAL(4) profile in REAL(4) */
+        {
+          float *BUF = bufs;
+          do {
+            if (nb + nstep < 1 || nb - nstep > length) break;
+            if (nb < length) {
+              int maxred = (length - nb) < nstep ? (length - nb) : nstep;
+              int mb = 1 > (1 - nb) ? 1 : (1 - nb);
+              for (int is = mb; is <= maxred; ++is) BUF[nb + is - 1] += pf[is];
+              if (nb <= 1) break;
+            }
+            int maxblue = (nb - 1) < nstep ? (nb - 1) : nstep;
+            int mb2 = 1 > (nb - length) ? 1 : (nb - length);
+            for (int is = mb2; is <= maxblue; ++is) BUF[nb - is - 1] += pf[is];
+          } while (0);
+        }
+      } else {
+        const float *cont = (const float *)continuum + (size_t)j * length;
+        double kappa0 = (double)L->cgf[il] * xd[nel];
+        double kapmin = (double)cont[ic - 1] * LINE_CUTOFF;
+        if (kappa0 < kapmin) continue;
+        kappa0 = kappa0 * exp(-(double)L->elo[il] * hckt[j]);
+        if (kappa0 < kapmin) continue;
+        double adamp = ((double)L->gamrf[il] + (double)L->gamsf[il] * xne[j] +
+                        (double)L->gamwf[il] * txnxn[j]) / dp[nel];
+        if (nb >= 1 && nb <= length) bufd[nb - 1] += kappa0 * orc_voigt_weideman(0.0, adamp);
+        double dvoigt = 1.0 / dp[nel] / resolu;
+        for (nstep = 1; nstep <= n10dop; ++nstep) {
+          prof[nstep] = kappa0 * orc_voigt_weideman((double)nstep * dvoigt, adamp);
+          if (prof[nstep] < kapmin) break;
+        }
+        if (nstep > n10dop) {
+          double x_wing = prof[n10dop] * ((double)n10dop * (double)n10dop);
+          double qs = sqrt(x_wing / kapmin);
+          int maxstep = qs >= (double)maxprof ? maxprof : (int)qs + 1;
+          if (maxstep > maxprof) maxstep = maxprof;
+          for (nstep = n10dop + 1; nstep <= maxstep; ++nstep)
+            prof[nstep] = x_wing / ((double)nstep * (double)nstep);
+          nstep = maxstep;
+        }
+        SCATTER(bufd, double);
+      }
+    }
+    for (int i = 0; i < length; ++i) {
+      double v = (mode == ORC_REF32) ? (double)bufs[i] : bufd[i];
+      if (opacity_f64_out) opacity_f64_out[(size_t)j * length + i] = v;
+      if (opacity_out) opacity_out[(size_t)j * length + i] = (float)v;
+    }
+  }
+  free(prof);
+  free(pf);
+  free(bufs);
+  free(bufd);
+}
+
+/* ======================================================================
+ * JOSH, atlas12_modules.f90:18398-18776 (IFSURF 0 and 1 paths)
+ * ==================================================================== */
+void orc_josh(const orc_ops_t *ops, int ifscat, int ifsurf, orc_josh_t *s) {
+  const int NX = ORC_NXTAU, NR = s->nrhox;
+  const double *xtau8 = ops->xtau;
+  double xs[ORC_NXTAU], xsbar[ORC_NXTAU], xalpha[ORC_NXTAU];
+  double xsbar8[ORC_NXTAU], xalpha8[ORC_NXTAU], xs8[ORC_NXTAU];
+  double xh[ORC_NXTAU], xjs[ORC_NXTAU], amat[ORC_NXTAU * ORC_NXTAU];
+  double snubar[KW_MAX];
+  int ipiv[ORC_NXTAU];
+  int j, l, m, maxj = 0;
+  s->edd_iters = 0;
+  for (j = 0; j < NR; ++j) {
+    s->abtot[j] = s->acont[j] + s->aline[j] + s->sigmac[j] + s->sigmal[j];
+    s->alpha[j] = (s->sigmac[j] + s->sigmal[j]) / s->abtot[j];
+    snubar[j] = (s->acont[j] * s->scont[j] + s->aline[j] * s->sline[j]) /
+                (s->acont[j] + s->aline[j]);
+  }
+  orc_integ(s->rhox, s->abtot, s->taunu, NR, s->abtot[0] * s->rhox[0]);
+  if (ifscat == 0) {
+    /* IFSCAT=0 never occurs on the hot path (IFSCAT=1 default :1293);
+     * restated for IFSURF=1 only. */
+    for (j = 0; j < NR; ++j) s->snu[j] = snubar[j];
+    maxj = orc_map1(s->taunu, s->snu, NR, xtau8, xs8, NX);
+    for (l = 0; l < NX; ++l) xs[l] = xs8[l];
+    double h = 0.0;
+    for (m = 0; m < NX; ++m) h = h + ops->ch[m] * xs[m];
+    s->hnu[0] = h;
+    s->maxj = maxj;
+    return;
+  }
+  if (s->taunu[0] > xtau8[NX - 1]) maxj = 1;
+  if (maxj != 1) {
+    maxj = orc_map1(s->taunu, snubar, NR, xtau8, xsbar8, NX);
+    maxj = orc_map1(s->taunu, s->alpha, NR, xtau8, xalpha8, NX);
+    for (l = 0; l < NX; ++l) {
+      xalpha8[l] = fmax(xalpha8[l], 0.0);
+      xsbar8[l] = fmax(xsbar8[l], 1.0e-38);
+      xalpha[l] = xalpha8[l];
+      xsbar[l] = xsbar8[l];
+      if (xtau8[l] < s->taunu[0]) {
+        xsbar8[l] = fmax(snubar[0], 1.0e-38);
+        xalpha8[l] = fmax(s->alpha[0], 0.0);
+        xsbar[l] = xsbar8[l];
+        xalpha[l] = xalpha8[l];
+      }
+    }
+    double amax = xalpha[0];
+    for (l = 1; l < NX; ++l) amax = fmax(amax, xalpha[l]);
+    if (amax <= 0.0) {
+      for (l = 0; l < NX; ++l) xs[l] = fmax(xsbar[l], 1.0e-37);
+    } else {
+      for (l = 0; l < NX; ++l) {
+        for (m = 0; m < NX; ++m) amat[m * NX + l] = -xalpha[l] * ops->coefj[m * NX + l];
+        amat[l * NX + l] = amat[l * NX + l] + 1.0;
+        xs[l] = (1.0 - xalpha[l]) * xsbar[l];
+      }
+      orc_solvit(amat, NX, xs, ipiv);
+      for (l = 0; l < NX; ++l) xs[l] = fmax(xs[l], 1.0e-37);
+    }
+    if (ifsurf == 1) {
+      double h = 0.0;
+      for (m = 0; m < NX; ++m) h = h + ops->ch[m] * xs[m];
+      s->hnu[0] = h;
+      s->maxj = maxj;
+      return;
+    }
+    for (m = 0; m < NX; ++m) xs8[m] = xs[m];
+    orc_map1(xtau8, xs8, NX, s->taunu, s->snu, maxj);
+  }
+  if (maxj != NR) {
+    int maxj1 = maxj + 1;
+    if (maxj == 1) maxj1 = 1;
+    for (j = maxj1; j <= NR; ++j) s->snu[j - 1] = snubar[j - 1];
+    m = maxj - 1 > 1 ? maxj - 1 : 1;
+    int nm1 = NR - m + 1, nmj = NR - maxj + 1;
+    double error = 0.0;
+    for (l = 1; l <= 50; ++l) {
+      error = 0.0;
+      int ifneg = 0;
+      s->edd_iters = l;
+      for (j = m; j <= NR; ++j) {
+        if (s->snu[j - 1] <= 0.0) {
+          ifneg = 1;
+          for (int jj = m; jj <= NR; ++jj) {
+            snubar[jj - 1] = s->bnu[jj - 1];
+            s->snu[jj - 1] = s->bnu[jj - 1];
+          }
+          break;
+        }
+      }
+      orc_deriv(s->taunu + m - 1, s->snu + m - 1, s->hnu + m - 1, nm1);
+      for (j = m; j <= NR; ++j) {
+        if (s->hnu[j - 1] <= 0.0) {
+          ifneg = 1;
+          for (int jj = m; jj <= NR; ++jj) {
+            snubar[jj - 1] = s->bnu[jj - 1];
+            s->snu[jj - 1] = s->bnu[jj - 1];
+          }
+          orc_deriv(s->taunu + m - 1, s->snu + m - 1, s->hnu + m - 1, nm1);
+          break;
+        }
+      }
+      for (j = m; j <= NR; ++j) s->hnu[j - 1] = s->hnu[j - 1] / 3.0;
+      orc_deriv(s->taunu + maxj - 1, s->hnu + maxj - 1, s->jmins + maxj - 1, nmj);
+      for (j = maxj1; j <= NR; ++j) {
+        if (ifneg == 1) s->jmins[j - 1] = 0.0;
+        s->jnu[j - 1] = s->jmins[j - 1] + s->snu[j - 1];
+        double snew = (1.0 - s->alpha[j - 1]) * snubar[j - 1] + s->alpha[j - 1] * s->jnu[j - 1];
+        error = fabs(snew - s->snu[j - 1]) / snew + error;
+        s->snu[j - 1] = snew;
+      }
+      if (error < 0.00001) break;
+    }
+  }
+  s->maxj = maxj;
+  if (maxj == 1) {
+    s->knu1 = s->jnu[0] / 3.0;
+    return;
+  }
+  double xjs8[ORC_NXTAU], xh8[ORC_NXTAU];
+  for (l = 0; l < NX; ++l) {
+    xjs[l] = -xs[l];
+    for (m = 0; m < NX; ++m) xjs[l] = xjs[l] + ops->coefj[m * NX + l] * xs[m];
+    xjs8[l] = xjs[l];
+    xh[l] = 0.0;
+    for (m = 0; m < NX; ++m) xh[l] = xh[l] + ops->coefh[m * NX + l] * xs[m];
+    xh8[l] = xh[l];
+  }
+  orc_map1(xtau8, xjs8, NX, s->taunu, s->jmins, maxj);
+  orc_map1(xtau8, xh8, NX, s->taunu, s->hnu, maxj);
+  double xk = 0.0;
+  for (m = 0; m < NX; ++m) xk = xk + ops->ck[m] * xs[m];
+  s->knu1 = xk;
+  for (j = 0; j < maxj; ++j) {
+    s->snu[j] = fmax(s->snu[j], 1.0e-38);
+    s->jnu[j] = fmax(s->jmins[j] + s->snu[j], 1.0e-38);
+  }
+}
+
+/* ======================================================================
+ * SYNTHE spectrum: synthe.f90:698-718 + setup_opacity_sv :797-833 +
+ * process_wavelength_point :848-902 (LTE, fscat=0, bfudge=1, IFSURF=1)
+ * ==================================================================== */
+void orc_synthe_spectrum(const orc_ops_t *ops, const double *wledge, int nedge,
+                         const double *contabs, const double *contscat,
+                         int ncont_stride, int nrhox, const double *rhox,
+                         const double *hkt, double wbegin, double ratio,
+                         int length, const float *opacity, int iw0, int iw1,
+                         double *flux, double *cont) {
+  double half[4096], del[4096];
+  for (int ie = 2; ie <= nedge; ++ie) {
+    half[ie - 2] = (wledge[ie - 2] + wledge[ie - 1]) * 0.5;
+    del[ie - 2] = orc_powi(wledge[ie - 1] - wledge[ie - 2], 2) * 0.5;
+  }
+  double acont[KW_MAX], sigmac[KW_MAX], aline[KW_MAX], sigmal[KW_MAX],
+      sline[KW_MAX], scont[KW_MAX], bnu[KW_MAX], ehvkt[KW_MAX], stim[KW_MAX];
+  double abtot[KW_MAX], alpha[KW_MAX], taunu[KW_MAX], snu[KW_MAX], jnu[KW_MAX],
+      hnu[KW_MAX], jmins[KW_MAX];
+  float asyn[KW_MAX];
+  const double BP = bnu_prefac();
+  int iedge = 1;
+  /* the reference walks iedge_sv from 1 over every lambda in order; for a
+   * sub-range start the search from the beginning as well */
+  for (int iw = 1; iw <= iw1; ++iw) {
+    double wave8 = wbegin * orc_powi(ratio, iw - 1);
+    while (wave8 >= wledge[iedge]) iedge = iedge + 1;
+    if (iw < iw0) continue;
+    double freq8 = CLIGHT_NMS / wave8;
+    for (int j = 0; j < nrhox; ++j)
+      asyn[j] = (float)((double)opacity[(size_t)j * length + iw - 1] * (1.0 - exp(-freq8 * hkt[j])));
+    double wv = wave8;
+    double c1 = (wv - half[iedge - 1]) * (wv - wledge[iedge]) / del[iedge - 1];
+    double c2 = (wledge[iedge - 1] - wv) * (wv - wledge[iedge]) * 2.0 / del[iedge - 1];
+    double c3 = (wv - wledge[iedge - 1]) * (wv - half[iedge - 1]) / del[iedge - 1];
+    for (int j = 0; j < nrhox; ++j) {
+      const double *ca = contabs + (size_t)j * ncont_stride + 3 * (iedge - 1);
+      const double *cs = contscat + (size_t)j * ncont_stride + 3 * (iedge - 1);
+      acont[j] = pow(10.0, c1 * ca[0] + c2 * ca[1] + c3 * ca[2]);
+      sigmac[j] = pow(10.0, c1 * cs[0] + c2 * cs[1] + c3 * cs[2]);
+    }
+    double freq = CLIGHT_NMS / wv;
+    double freq15 = freq / 1.0e15;
+    for (int j = 0; j < nrhox; ++j) {
+      ehvkt[j] = exp(-freq * hkt[j]);
+      stim[j] = 1.0 - ehvkt[j];
+      bnu[j] = BP * orc_powi(freq15, 3) * ehvkt[j] / stim[j];
+      aline[j] = 0.0;
+      sigmal[j] = 0.0;
+      sline[j] = bnu[j];
+      scont[j] = bnu[j];
+    }
+    orc_josh_t st = {rhox, acont, aline, sigmac, sigmal, scont, sline, bnu, nrhox,
+                     abtot, alpha, taunu, snu, jnu, hnu, jmins, 0.0, 0, 0};
+    orc_josh(ops, 1, 1, &st);
+    double surf = hnu[0];
+    for (int j = 0; j < nrhox; ++j) {
+      aline[j] = (double)asyn[j] * (1.0 - 0.0);
+      sline[j] = bnu[j] * stim[j] / (1.0 - ehvkt[j]);
+      sigmal[j] = (double)asyn[j] * 0.0;
+    }
+    orc_josh(ops, 1, 1, &st);
+    double resid = hnu[0] / surf;
+    flux[iw - iw0] = resid * surf;
+    cont[iw - iw0] = surf;
+  }
+}
+
+/* ======================================================================
+ * ATLAS12 LINOP1, atlas12_modules.f90:18132-18374
+ * ==================================================================== */
+/* TABLOG, atlas12_modules.f90:2083-2086: 10**((I-16384)*0.001) for every
+ * INTEGER(2) I, stored at [I + 32768]. */
+void orc_build_tablog(double *out) {
+  for (int k = 0; k < 65536; ++k) out[k] = pow(10.0, (double)((k - 32768) - 16384) * 0.001);
+}
+
+static inline double tablog_(const orc_atlas_tables_t *tb, int16_t i) {
+  return tb->tablog[(int)i + 32768];
+}
+
+static void linop_wings(const orc_atlas_tables_t *tb, double center, double adamp,
+                        double dopwave, double wlvac, int nu, int numnu,
+                        const double *waveset, double tc, double *xl, int kw) {
+  /* xl points at XLINES(J,1); XLINES(J,IW) = xl[(IW-1)*kw] */
+  const int MAX_WING = 100;
+  const double *H0 = tb->h0tab, *H1 = tb->h1tab, *H2 = tb->h2tab;
+  int iwmax = nu + MAX_WING < numnu ? nu + MAX_WING : numnu;
+  for (int iw = nu; iw <= iwmax; ++iw) {
+    double cv;
+    if (adamp > 0.20) {
+      cv = center * orc_voigt_kurucz((waveset[iw - 1] - wlvac) / dopwave, adamp, H0, H1, H2);
+    } else {
+      double vv = (waveset[iw - 1] - wlvac) / dopwave;
+      if (vv > 10.0) {
+        cv = center * INVSQRTPI * adamp / orc_powi(vv, 2);
+      } else {
+        int iv = (int)(vv * 200.0 + 1.5);
+        cv = center * ((H2[iv - 1] * adamp + H1[iv - 1]) * adamp + H0[iv - 1]);
+      }
+    }
+    xl[(size_t)(iw - 1) * kw] += cv;
+    if (cv < tc) break;
+  }
+  for (int i = 1; i <= MAX_WING; ++i) {
+    int iw = nu - i;
+    if (iw <= 0) break;
+    double cv;
+    if (adamp > 0.20) {
+      cv = center * orc_voigt_kurucz((wlvac - waveset[iw - 1]) / dopwave, adamp, H0, H1, H2);
+    } else {
+      double vv = (wlvac - waveset[iw - 1]) / dopwave;
+      if (vv > 10.0) {
+        cv = center * INVSQRTPI * adamp / orc_powi(vv, 2);
+      } else {
+        int iv = (int)(vv * 200.0 + 1.5);
+        cv = center * ((H2[iv - 1] * adamp + H1[iv - 1]) * adamp + H0[iv - 1]);
+      }
+    }
+    xl[(size_t)(iw - 1) * kw] += cv;
+    if (cv < tc) break;
+  }
+}
+
+int64_t orc_atlas_linop1(const orc_atlas_tables_t *tb, const int32_t *linedata,
+                         int64_t nlines, int nrhox, int kw, const double *xnfdop,
+                         const double *dopple, int nspec, const double *xne,
+                         const double *txnxn, const double *hckt,
+                         const double *tabcont, const int32_t *iwavetab,
+                         int nwave, const double *waveset, int numnu,
+                         double *xlines) {
+  const double CEN_PREFAC4 = 0.026538 / SQRTPI / CLIGHT_NMS;
+  const double FOURPI_C_INV = 1.0 / (4.0 * PI_ * CLIGHT_NMS);
+  const double RATIOLG = log(1.0 + 1.0 / 2000000.0);
+  int ifj[KW_MAX + 2];
+  ifj[0] = 0;
+  memset(xlines, 0, sizeof(double) * (size_t)numnu * kw);
+  int nucont = 1, nu = 1, iwlold = 0;
+  double start = waveset[0] - 1.0, stop = waveset[numnu - 1] + 1.0;
+  int64_t lineused = 0;
+  double gammar = 0, gammas = 0, gammaw = 0;
+  for (int64_t line = 0; line < nlines; ++line) {
+    const int32_t *rec = linedata + 4 * line;
+    int32_t iwl = rec[0];
+    int16_t ielion = (int16_t)(rec[1] & 0xffff), ielo = (int16_t)((uint32_t)rec[1] >> 16);
+    int16_t igflog = (int16_t)(rec[2] & 0xffff), igr = (int16_t)((uint32_t)rec[2] >> 16);
+    int16_t igs = (int16_t)(rec[3] & 0xffff), igw = (int16_t)((uint32_t)rec[3] >> 16);
+    if (iwl < iwlold) {
+      nucont = 1;
+      nu = 1;
+    }
+    while (iwl >= iwavetab[nucont - 1]) {
+      nucont = nucont + 1;
+      if (nucont > nwave + 1) {
+        nucont = nwave + 1;
+        break;
+      }
+    }
+    int nelion = abs(ielion / 10);
+    if (nelion < 1 || nelion > nspec) {
+      iwlold = iwl;
+      continue;
+    }
+    double wlvac = exp(iwl * RATIOLG);
+    double wlvac4 = wlvac;
+    if (wlvac < start || wlvac > stop) {
+      iwlold = iwl;
+      continue;
+    }
+    /* The reference's CYCLE inside this DO WHILE walks past NUMNU for lines
+     * redward of WAVESET(NUMNU-1) (reads beyond the grid); the restatement
+     * clamps at NUMNU.  Synthetic inputs keep lines inside the grid. */
+    while (nu <= numnu && wlvac >= waveset[nu - 1]) nu = nu + 1;
+    if (nu > numnu) nu = numnu;
+    double cgf = CEN_PREFAC4 * wlvac4 * tablog_(tb, igflog);
+    double elo = tablog_(tb, ielo);
+    double adamp = 0.0;
+    int ifline = 0;
+    const double *xdn = xnfdop + (size_t)(nelion - 1) * kw;
+    const double *dpn = dopple + (size_t)(nelion - 1) * kw;
+    const double *tcv = tabcont + (size_t)(nucont - 1) * kw;
+    for (int J = 8; J <= nrhox; J += 8) {
+      ifj[J] = 0;
+      double center = cgf * xdn[J - 1];
+      if (center < tcv[J - 1]) continue;
+      center = center * exp(-elo * hckt[J - 1]);
+      if (center < tcv[J - 1]) continue;
+      ifj[J] = 1;
+      ifline = 1;
+      if (adamp == 0.0) {
+        gammar = tablog_(tb, igr) * wlvac4 * FOURPI_C_INV;
+        gammas = tablog_(tb, igs) * wlvac4 * FOURPI_C_INV;
+        gammaw = tablog_(tb, igw) * wlvac4 * FOURPI_C_INV;
+      }
+      adamp = (gammar + gammas * xne[J - 1] + gammaw * txnxn[J - 1]) / dpn[J - 1];
+      double dopwave = dpn[J - 1] * wlvac4;
+      linop_wings(tb, center, adamp, dopwave, wlvac, nu, numnu, waveset, tcv[J - 1],
+                  xlines + (J - 1), kw);
+    }
+    for (int K = 8; K <= nrhox; K += 8) {
+      if (ifj[K - 8] + ifj[K] == 0) continue;
+      for (int J = K - 7; J <= K - 1; ++J) {
+        double center = cgf * xdn[J - 1];
+        if (center < tcv[J - 1]) continue;
+        center = center * exp(-elo * hckt[J - 1]);
+        if (center < tcv[J - 1]) continue;
+        adamp = (gammar + gammas * xne[J - 1] + gammaw * txnxn[J - 1]) / dpn[J - 1];
+        double dopwave = dpn[J - 1] * wlvac4;
+        linop_wings(tb, center, adamp, dopwave, wlvac, nu, numnu, waveset, tcv[J - 1],
+                    xlines + (J - 1), kw);
+      }
+    }
+    if (ifline == 1) lineused = lineused + 1;
+    iwlold = iwl;
+  }
+  return lineused;
+}
+
+/* ======================================================================
+ * ATLAS12 RUN_RT_PASS frequency loop with TCORR/RADIAP/ROSS mode 2,
+ * atlas12_modules.f90:3880-3951, :2457-2522, :5072-5097, :5178-5190.
+ * KAPP is replaced by the caller's per-frequency ACONT/SIGMAC/SCONT
+ * (scont NULL => SCONT = BNU); ALINE = XLINES*STIM, SIGMAL = 0, SLINE = BNU.
+ * acc arrays are accumulated into (call with zeroed arrays for mode 1).
+ * ==================================================================== */
+void orc_atlas_rt_pass(const orc_ops_t *ops, int numnu, const double *waveset,
+                       const double *rcoset, const double *acont,
+                       const double *sigmac, const double *scont, int kw,
+                       const double *xlines, int nrhox, const double *rhox,
+                       const double *t, const double *hkt, double teff, int nu0,
+                       int nu1, orc_accum_t *acc, double *hsurf) {
+  const double BP = bnu_prefac();
+  double ehvkt[KW_MAX], stim[KW_MAX], bnu[KW_MAX], aline[KW_MAX], sigmal[KW_MAX],
+      sline[KW_MAX], sc[KW_MAX];
+  double abtot[KW_MAX], alpha[KW_MAX], taunu[KW_MAX], snu[KW_MAX], jnu[KW_MAX],
+      hnu[KW_MAX], jmins[KW_MAX], dabtot[KW_MAX];
+  for (int nu = nu0; nu <= nu1; ++nu) {
+    double wave = waveset[nu - 1];
+    double freq = CLIGHT_NMS / wave;
+    double rcowt = rcoset[nu - 1];
+    double freq15 = freq / 1.0e15;
+    const double *ac = acont + (size_t)(nu - 1) * kw;
+    const double *sg = sigmac + (size_t)(nu - 1) * kw;
+    for (int j = 0; j < nrhox; ++j) {
+      ehvkt[j] = exp(-freq * hkt[j]);
+      stim[j] = 1.0 - ehvkt[j];
+      bnu[j] = BP * orc_powi(freq15, 3) * ehvkt[j] / stim[j];
+      sc[j] = scont ? scont[(size_t)(nu - 1) * kw + j] : bnu[j];
+      aline[j] = 0.0 + xlines[(size_t)(nu - 1) * kw + j] * stim[j];
+      sigmal[j] = 0.0;
+      sline[j] = bnu[j];
+      jnu[j] = 0.0;
+      hnu[j] = 0.0;
+      jmins[j] = 0.0;
+      snu[j] = 0.0;
+    }
+    orc_josh_t st = {rhox, ac, aline, sg, sigmal, sc, sline, bnu, nrhox,
+                     abtot, alpha, taunu, snu, jnu, hnu, jmins, 0.0, 0, 0};
+    orc_josh(ops, 1, 0, &st);
+    int neg = 0;
+    for (int j = 0; j < nrhox; ++j)
+      if (snu[j] < 0.0 || jnu[j] < 0.0 || hnu[j] < 0.0) {
+        neg = 1;
+        break;
+      }
+    if (neg) {
+      for (int j = 0; j < nrhox; ++j) {
+        jnu[j] = fmax(jnu[j], 1.0e-99);
+        snu[j] = fmax(snu[j], 1.0e-99);
+        hnu[j] = fmax(hnu[j], 1.0e-99);
+      }
+    }
+    if (hsurf) hsurf[nu - nu0] = hnu[0];
+    /* TCORR mode 2 */
+    orc_deriv(rhox, abtot, dabtot, nrhox);
+    for (int j = 0; j < nrhox; ++j) {
+      acc->rdabh[j] = acc->rdabh[j] + dabtot[j] / abtot[j] * hnu[j] * rcowt;
+      acc->rjmins[j] = acc->rjmins[j] + abtot[j] * jmins[j] * rcowt;
+      acc->flxrad[j] = acc->flxrad[j] + hnu[j] * rcowt;
+    }
+    double term2 = 0.0, d = 0.0;
+    for (int j = 1; j <= nrhox; ++j) {
+      double term1 = term2;
+      if (j != nrhox) d = taunu[j] - taunu[j - 1];
+      d = fmax(1.0e-10, d);
+      if (d <= 0.01) {
+        term2 = (EULER_M1 - log(d)) * d / 4.0 + orc_powi(d, 2) / 12.0 -
+                orc_powi(d, 3) / 96.0 + orc_powi(d, 4) / 720.0;
+      } else {
+        double ex = 0.0;
+        if (d < 10.0) ex = orc_expi(3, d);
+        if (teff <= 4250.0 && d > 0.005 && d < 0.02) ex = 0.0;
+        term2 = 0.5 * (d + ex - 0.5) / d;
+      }
+      double diagj = term1 + term2;
+      double dbdt;
+      if (numnu == 1)
+        dbdt = 0.0; /* single-frequency branch is not on the hot path */
+      else
+        dbdt = bnu[j - 1] * freq * hkt[j - 1] / t[j - 1] / fmax(stim[j - 1], 1.0e-30);
+      acc->rdiagj[j - 1] = acc->rdiagj[j - 1] +
+                           abtot[j - 1] * (diagj - 1.0) / (1.0 - alpha[j - 1] * diagj) *
+                               (1.0 - alpha[j - 1]) * dbdt * rcowt;
+    }
+    /* RADIAP mode 2 */
+    for (int j = 0; j < nrhox; ++j) {
+      acc->raden[j] = acc->raden[j] + jnu[j] * rcowt;
+      acc->h_total[j] = acc->h_total[j] + hnu[j] * rcowt;
+      acc->accrad[j] = acc->accrad[j] + abtot[j] * hnu[j] * rcowt;
+    }
+    acc->pradk0 = acc->pradk0 + st.knu1 * rcowt;
+    /* ROSS mode 2 */
+    for (int j = 0; j < nrhox; ++j) {
+      double dbdt = bnu[j] * freq * hkt[j] / t[j] / stim[j];
+      acc->abross[j] = acc->abross[j] + dbdt / abtot[j] * rcowt;
+    }
+  }
+}

@@ -1,0 +1,156 @@
+/*
+ * oracle.h -- CPU restatement of the ATLAS12 / SYNTHE hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA
+ * path in atlas12_b200/csrc: only tests/, __graft_entry__.smoke() and the
+ * CPU-baseline leg of bench.py may load it.  The product never links it.
+ *
+ * Parity status: pinned.  The reference (Fortran 90) cannot be compiled in
+ * this image (no Fortran compiler), so every routine below is a line-level
+ * restatement of the cited reference source, pinned against the reference's
+ * own data constants (operator matrices, quadrature weights, Voigt tables)
+ * extracted by tests/golden/make_golden.py and against independent
+ * known-answer tests (scipy wofz / expn / numpy.linalg.solve, analytic
+ * transfer solutions).  Citations are file:line inside cconroy20/atlas12.
+ *
+ * Two arithmetic modes for the SYNTHE line loop:
+ *   ORC_REF32 : the reference's REAL(4) semantics, lines summed sequentially
+ *               in line order (synthe.f90:559-683);
+ *   ORC_FP64  : every quantity in double (the all-FP64 accuracy oracle).
+ */
+#ifndef ATLAS12_ORACLE_H
+#define ATLAS12_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_NXTAU 51
+#define ORC_REF32 0
+#define ORC_FP64 1
+
+/* ---- numerics (atlas12_modules.f90) ---------------------------------- */
+void orc_parcoe(const double *f, const double *x, double *a, double *b,
+                double *c, int n);                              /* :5358-5434 */
+void orc_integ(const double *x, const double *f, double *fint, int n,
+               double start);                                   /* :5293-5324 */
+void orc_deriv(const double *x, const double *f, double *dfdx, int n); /* :5228 */
+int orc_map1(const double *xold, const double *fold, int nold,
+             const double *xnew, double *fnew, int nnew);       /* :5570-5692 */
+void orc_solvit(double *a, int n, double *b, int *ipivot);      /* :5739-5847 */
+double orc_expi(int n, double x);                               /* :21103-21225 */
+double orc_powi(double x, int m);      /* gfortran REAL(8)**INTEGER */
+
+/* ---- Voigt functions ------------------------------------------------- */
+double orc_voigt_weideman(double v, double a); /* synthe_module.f90:463-537, FP64 */
+float orc_voigt_profile(float v, float a);     /* same, REAL(4) interface */
+void orc_tabvoigt(double vsteps, int n, const double *tabvi,
+                  const double *tabh1, int ntab, double *h0tab,
+                  double *h1tab, double *h2tab);      /* :19796-19851 */
+double orc_voigt_kurucz(double v, double a, const double *h0tab,
+                        const double *h1tab, const double *h2tab); /* :21033 */
+
+/* ---- SYNTHE grid + binning (synthe.f90:316-324, mod_mklinelist:898) -- */
+typedef struct {
+  double ratio, ratiolg, wbegin;
+  int32_t length, ixwlbeg;
+} orc_grid_t;
+void orc_synthe_grid(double wlbeg, double wlend, double resolu, orc_grid_t *g);
+int32_t orc_synthe_nbuff(double wlvac, double ratiolg, int32_t ixwlbeg);
+
+/* ---- SYNTHE continuum per depth (synthe.f90:483-516) ------------------
+ * continall: [nrhox][3*(nedge-1)] log10 kappa (row = depth)
+ * out      : [nrhox][length]  (float for REF32, double for FP64) */
+void orc_synthe_continuum(int mode, const double *wledge, int nedge,
+                          const double *continall, int ncont_stride,
+                          int nrhox, double wbegin, double ratio,
+                          int length, void *out);
+
+/* ---- SYNTHE LTE line opacity (synthe.f90:559-683) --------------------
+ * Lines are SoA; nelion is 1-based into the per-depth xnfdop/dopple rows
+ * of width nspec.  continuum is the REAL(4) array of orc_synthe_continuum
+ * (mode REF32) for both modes: the modes differ in the arithmetic of this
+ * stage, not in its inputs.
+ * opacity_out: [nrhox][length] float (both modes round the final sum). */
+typedef struct {
+  const int32_t *nbuff;
+  const float *cgf;
+  const int32_t *nelion;
+  const float *elo, *gamrf, *gamsf, *gamwf;
+  int64_t n;
+} orc_lines_t;
+void orc_synthe_line_opacity(int mode, const orc_lines_t *L, int length,
+                             int nrhox, double resolu, const void *continuum,
+                             const double *xnfdop, const double *dopple,
+                             int nspec, const double *xne,
+                             const double *txnxn, const double *hckt,
+                             int maxprof, double *opacity_f64_out,
+                             float *opacity_out);
+
+/* ---- JOSH (atlas12_modules.f90:18398-18776) ------------------------- */
+typedef struct {
+  double xtau[ORC_NXTAU];
+  double coefj[ORC_NXTAU * ORC_NXTAU]; /* column-major, COEFJ(L,M) at [(M-1)*51+L-1] */
+  double coefh[ORC_NXTAU * ORC_NXTAU];
+  double ch[ORC_NXTAU], ck[ORC_NXTAU];
+} orc_ops_t;
+
+typedef struct {
+  /* inputs (nrhox) */
+  const double *rhox, *acont, *aline, *sigmac, *sigmal, *scont, *sline, *bnu;
+  int nrhox;
+  /* outputs (nrhox) */
+  double *abtot, *alpha, *taunu, *snu, *jnu, *hnu, *jmins;
+  double knu1;
+  int maxj, edd_iters;
+} orc_josh_t;
+void orc_josh(const orc_ops_t *ops, int ifscat, int ifsurf, orc_josh_t *s);
+
+/* ---- SYNTHE spectrum (synthe.f90:698-718, 797-902) -------------------
+ * contabs/contscat: [nrhox][3*(nedge-1)] log10 tables (contabs_sv layout
+ * flattened as (k, iedge) per depth).  opacity: [nrhox][length] float.
+ * Writes flux[length], cont[length]. */
+void orc_synthe_spectrum(const orc_ops_t *ops, const double *wledge,
+                         int nedge, const double *contabs,
+                         const double *contscat, int ncont_stride, int nrhox,
+                         const double *rhox, const double *hkt,
+                         double wbegin, double ratio, int length,
+                         const float *opacity, int iw0, int iw1,
+                         double *flux, double *cont);
+
+/* ---- ATLAS LINOP1 (atlas12_modules.f90:18132-18374) ------------------
+ * linedata: [n][4] int32 (LINEREC); xnfdop, dopple: [nspec][kw] column-major
+ * (index (nelion-1)*kw + j-1, i.e. XNFDOP(J,NELION)); tabcont [nwave+1][kw];
+ * tablog[65536] indexed by (uint16)I; xlines_out [numnu][kw] (XLINES(J,NU)). */
+typedef struct {
+  const double *h0tab, *h1tab, *h2tab; /* 2001 */
+  const double *tablog;                /* 65536, index = int16 + 32768 */
+} orc_atlas_tables_t;
+void orc_build_tablog(double *out65536);
+int64_t orc_atlas_linop1(const orc_atlas_tables_t *tb, const int32_t *linedata,
+                         int64_t nlines, int nrhox, int kw, const double *xnfdop,
+                         const double *dopple, int nspec, const double *xne,
+                         const double *txnxn, const double *hckt,
+                         const double *tabcont, const int32_t *iwavetab,
+                         int nwave, const double *waveset, int numnu,
+                         double *xlines);
+
+/* ---- ATLAS RT pass, mode-2 integrals (atlas12_modules.f90:3880-3951) --- */
+typedef struct {
+  double *rjmins, *rdabh, *rdiagj, *flxrad;  /* TCORR mode 2 */
+  double *raden, *h_total, *accrad;           /* RADIAP mode 2 */
+  double *abross;                             /* ROSS mode 2 */
+  double pradk0;
+} orc_accum_t;
+void orc_atlas_rt_pass(const orc_ops_t *ops, int numnu, const double *waveset,
+                       const double *rcoset, const double *acont,
+                       const double *sigmac, const double *scont, int kw,
+                       const double *xlines, int nrhox, const double *rhox,
+                       const double *t, const double *hkt, double teff,
+                       int nu0, int nu1, orc_accum_t *acc, double *hsurf);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

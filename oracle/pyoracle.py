@@ -1,0 +1,309 @@
+"""ctypes wrapper around the CPU oracle (oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, as the checker.  The product (atlas12_b200)
+never imports this module.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
+_ip = ctypes.POINTER(ctypes.c_int32)
+NXTAU = 51
+REF32, FP64 = 0, 1
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def _declare(L):
+    L.orc_integ.argtypes = [_dp, _dp, _dp, ctypes.c_int, ctypes.c_double]
+    L.orc_parcoe.argtypes = [_dp, _dp, _dp, _dp, _dp, ctypes.c_int]
+    L.orc_deriv.argtypes = [_dp, _dp, _dp, ctypes.c_int]
+    L.orc_map1.argtypes = [_dp, _dp, ctypes.c_int, _dp, _dp, ctypes.c_int]
+    L.orc_map1.restype = ctypes.c_int
+    L.orc_solvit.argtypes = [_dp, ctypes.c_int, _dp, _ip]
+    L.orc_expi.argtypes = [ctypes.c_int, ctypes.c_double]
+    L.orc_expi.restype = ctypes.c_double
+    L.orc_voigt_weideman.argtypes = [ctypes.c_double, ctypes.c_double]
+    L.orc_voigt_weideman.restype = ctypes.c_double
+    L.orc_voigt_profile.argtypes = [ctypes.c_float, ctypes.c_float]
+    L.orc_voigt_profile.restype = ctypes.c_float
+    L.orc_tabvoigt.argtypes = [ctypes.c_double, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp, _dp]
+    L.orc_voigt_kurucz.argtypes = [ctypes.c_double, ctypes.c_double, _dp, _dp, _dp]
+    L.orc_voigt_kurucz.restype = ctypes.c_double
+    L.orc_synthe_nbuff.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int32]
+    L.orc_synthe_nbuff.restype = ctypes.c_int32
+    L.orc_build_tablog.argtypes = [_dp]
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ptr(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+# ---------------------------------------------------------------- numerics
+def integ(x, f, start):
+    x, f = _d(x), _d(f)
+    out = np.zeros_like(x)
+    lib().orc_integ(_ptr(x), _ptr(f), _ptr(out), x.size, float(start))
+    return out
+
+
+def deriv(x, f):
+    x, f = _d(x), _d(f)
+    out = np.zeros_like(x)
+    lib().orc_deriv(_ptr(x), _ptr(f), _ptr(out), x.size)
+    return out
+
+
+def map1(xold, fold, xnew):
+    xold, fold, xnew = _d(xold), _d(fold), _d(xnew)
+    out = np.zeros_like(xnew)
+    r = lib().orc_map1(_ptr(xold), _ptr(fold), xold.size, _ptr(xnew), _ptr(out), xnew.size)
+    return out, r
+
+
+def solvit(A, b):
+    n = A.shape[0]
+    a = np.asfortranarray(A, dtype=np.float64).copy(order="F")
+    x = _d(b).copy()
+    piv = np.zeros(n, dtype=np.int32)
+    lib().orc_solvit(a.ctypes.data_as(_dp), n, _ptr(x), _ptr(piv, _ip))
+    return x
+
+
+def expi(n, x):
+    return lib().orc_expi(int(n), float(x))
+
+
+def voigt_weideman(v, a):
+    return lib().orc_voigt_weideman(float(v), float(a))
+
+
+def voigt_profile(v, a):
+    return lib().orc_voigt_profile(float(v), float(a))
+
+
+def tabvoigt(tabvi, tabh1, vsteps=200.0, n=2001):
+    tabvi, tabh1 = _d(tabvi), _d(tabh1)
+    h0, h1, h2 = (np.zeros(n) for _ in range(3))
+    lib().orc_tabvoigt(vsteps, n, _ptr(tabvi), _ptr(tabh1), tabvi.size, _ptr(h0), _ptr(h1), _ptr(h2))
+    return h0, h1, h2
+
+
+def voigt_kurucz(v, a, h0, h1, h2):
+    return lib().orc_voigt_kurucz(float(v), float(a), _ptr(h0), _ptr(h1), _ptr(h2))
+
+
+def build_tablog():
+    out = np.zeros(65536)
+    lib().orc_build_tablog(_ptr(out))
+    return out
+
+
+def nbuff(wlvac, ratiolg, ixwlbeg):
+    return lib().orc_synthe_nbuff(float(wlvac), float(ratiolg), int(ixwlbeg))
+
+
+# ---------------------------------------------------------------- structs
+class _Grid(ctypes.Structure):
+    _fields_ = [("ratio", ctypes.c_double), ("ratiolg", ctypes.c_double), ("wbegin", ctypes.c_double),
+                ("length", ctypes.c_int32), ("ixwlbeg", ctypes.c_int32)]
+
+
+class Ops(ctypes.Structure):
+    _fields_ = [("xtau", ctypes.c_double * NXTAU), ("coefj", ctypes.c_double * (NXTAU * NXTAU)),
+                ("coefh", ctypes.c_double * (NXTAU * NXTAU)), ("ch", ctypes.c_double * NXTAU),
+                ("ck", ctypes.c_double * NXTAU)]
+
+    @classmethod
+    def from_tables(cls, t):
+        o = cls()
+        o.xtau[:] = list(t["xtau8"])
+        o.coefj[:] = list(np.asarray(t["coefj"]).ravel(order="F"))
+        o.coefh[:] = list(np.asarray(t["coefh"]).ravel(order="F"))
+        o.ch[:] = list(t["ch_j"])
+        o.ck[:] = list(t["ck_j"])
+        return o
+
+
+class _Lines(ctypes.Structure):
+    _fields_ = [("nbuff", _ip), ("cgf", _fp), ("nelion", _ip), ("elo", _fp), ("gamrf", _fp),
+                ("gamsf", _fp), ("gamwf", _fp), ("n", ctypes.c_int64)]
+
+
+class _Josh(ctypes.Structure):
+    _fields_ = [(n, _dp) for n in ("rhox", "acont", "aline", "sigmac", "sigmal", "scont", "sline", "bnu")] + \
+               [("nrhox", ctypes.c_int)] + \
+               [(n, _dp) for n in ("abtot", "alpha", "taunu", "snu", "jnu", "hnu", "jmins")] + \
+               [("knu1", ctypes.c_double), ("maxj", ctypes.c_int), ("edd_iters", ctypes.c_int)]
+
+
+class _Accum(ctypes.Structure):
+    _fields_ = [(n, _dp) for n in ("rjmins", "rdabh", "rdiagj", "flxrad", "raden", "h_total",
+                                     "accrad", "abross")] + [("pradk0", ctypes.c_double)]
+
+
+class _AtlasTables(ctypes.Structure):
+    _fields_ = [("h0tab", _dp), ("h1tab", _dp), ("h2tab", _dp), ("tablog", _dp)]
+
+
+def _declare2(L):
+    L.orc_synthe_grid.argtypes = [ctypes.c_double] * 3 + [ctypes.POINTER(_Grid)]
+    L.orc_synthe_continuum.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_void_p]
+    L.orc_synthe_line_opacity.argtypes = [ctypes.c_int, ctypes.POINTER(_Lines), ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_double, ctypes.c_void_p, _dp, _dp, ctypes.c_int, _dp, _dp,
+                                          _dp, ctypes.c_int, _dp, _fp]
+    L.orc_josh.argtypes = [ctypes.POINTER(Ops), ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Josh)]
+    L.orc_synthe_spectrum.argtypes = [ctypes.POINTER(Ops), _dp, ctypes.c_int, _dp, _dp, ctypes.c_int,
+                                      ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                      _fp, ctypes.c_int, ctypes.c_int, _dp, _dp]
+    L.orc_atlas_linop1.argtypes = [ctypes.POINTER(_AtlasTables), _ip, ctypes.c_int64, ctypes.c_int,
+                                   ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp, _dp, _dp, _ip,
+                                   ctypes.c_int, _dp, ctypes.c_int, _dp]
+    L.orc_atlas_linop1.restype = ctypes.c_int64
+    L.orc_atlas_rt_pass.argtypes = [ctypes.POINTER(Ops), ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_void_p,
+                                    ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double,
+                                    ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Accum), _dp]
+
+
+_declared2 = False
+
+
+def _lib2():
+    global _declared2
+    L = lib()
+    if not _declared2:
+        _declare2(L)
+        _declared2 = True
+    return L
+
+
+# ---------------------------------------------------------------- SYNTHE
+def synthe_grid(wlbeg, wlend, resolu):
+    g = _Grid()
+    _lib2().orc_synthe_grid(wlbeg, wlend, resolu, ctypes.byref(g))
+    return dict(ratio=g.ratio, ratiolg=g.ratiolg, wbegin=g.wbegin, length=g.length, ixwlbeg=g.ixwlbeg)
+
+
+def synthe_continuum(mode, wledge, continall, wbegin, ratio, length):
+    wledge, continall = _d(wledge), _d(continall)
+    nrhox, stride = continall.shape
+    out = np.zeros((nrhox, length), dtype=np.float32 if mode == REF32 else np.float64)
+    _lib2().orc_synthe_continuum(mode, _ptr(wledge), wledge.size, _ptr(continall), stride, nrhox,
+                                 wbegin, ratio, length, out.ctypes.data_as(ctypes.c_void_p))
+    return out
+
+
+def synthe_line_opacity(mode, lines, length, atm, continuum, resolu, maxprof=1000000):
+    """lines: dict of SoA arrays; atm: dict(xnfdop[nrhox,nspec], dopple, xne, txnxn, hckt)."""
+    arrs = dict(nbuff=np.ascontiguousarray(lines["nbuff"], np.int32),
+                cgf=np.ascontiguousarray(lines["cgf"], np.float32),
+                nelion=np.ascontiguousarray(lines["nelion"], np.int32),
+                elo=np.ascontiguousarray(lines["elo"], np.float32),
+                gamrf=np.ascontiguousarray(lines["gamrf"], np.float32),
+                gamsf=np.ascontiguousarray(lines["gamsf"], np.float32),
+                gamwf=np.ascontiguousarray(lines["gamwf"], np.float32))
+    L = _Lines(_ptr(arrs["nbuff"], _ip), _ptr(arrs["cgf"], _fp), _ptr(arrs["nelion"], _ip),
+               _ptr(arrs["elo"], _fp), _ptr(arrs["gamrf"], _fp), _ptr(arrs["gamsf"], _fp),
+               _ptr(arrs["gamwf"], _fp), arrs["nbuff"].size)
+    xnfdop, dopple = _d(atm["xnfdop"]), _d(atm["dopple"])
+    nrhox, nspec = xnfdop.shape
+    xne, txnxn, hckt = _d(atm["xne"]), _d(atm["txnxn"]), _d(atm["hckt"])
+    cont = np.ascontiguousarray(continuum)
+    out64 = np.zeros((nrhox, length))
+    out32 = np.zeros((nrhox, length), dtype=np.float32)
+    _lib2().orc_synthe_line_opacity(mode, ctypes.byref(L), length, nrhox, resolu,
+                                    cont.ctypes.data_as(ctypes.c_void_p), _ptr(xnfdop), _ptr(dopple), nspec,
+                                    _ptr(xne), _ptr(txnxn), _ptr(hckt), maxprof, _ptr(out64), _ptr(out32, _fp))
+    return out32, out64
+
+
+def josh(ops, ifscat, ifsurf, rhox, acont, aline, sigmac, sigmal, scont, sline, bnu):
+    ins = [_d(v) for v in (rhox, acont, aline, sigmac, sigmal, scont, sline, bnu)]
+    nr = ins[0].size
+    outs = [np.zeros(nr) for _ in range(7)]
+    st = _Josh(*[_ptr(v) for v in ins], nr, *[_ptr(v) for v in outs], 0.0, 0, 0)
+    _lib2().orc_josh(ctypes.byref(ops), ifscat, ifsurf, ctypes.byref(st))
+    names = ("abtot", "alpha", "taunu", "snu", "jnu", "hnu", "jmins")
+    r = dict(zip(names, outs))
+    r.update(knu1=st.knu1, maxj=st.maxj, edd_iters=st.edd_iters)
+    return r
+
+
+def synthe_spectrum(ops, wledge, contabs, contscat, rhox, hkt, wbegin, ratio, opacity, iw0=1, iw1=None):
+    wledge, contabs, contscat, rhox, hkt = (_d(v) for v in (wledge, contabs, contscat, rhox, hkt))
+    op = np.ascontiguousarray(opacity, np.float32)
+    nrhox, length = op.shape
+    iw1 = length if iw1 is None else iw1
+    n = iw1 - iw0 + 1
+    flux, cont = np.zeros(n), np.zeros(n)
+    _lib2().orc_synthe_spectrum(ctypes.byref(ops), _ptr(wledge), wledge.size, _ptr(contabs), _ptr(contscat),
+                                contabs.shape[1], nrhox, _ptr(rhox), _ptr(hkt), wbegin, ratio, length,
+                                _ptr(op, _fp), iw0, iw1, _ptr(flux), _ptr(cont))
+    return flux, cont
+
+
+# ---------------------------------------------------------------- ATLAS
+def atlas_linop1(h0, h1, h2, tablog, linedata, atm, tabcont, iwavetab, waveset):
+    """atm: dict(xnfdop[nspec,kw], dopple[nspec,kw], xne[kw], txnxn[kw], hckt[kw]) -> xlines[numnu,kw]."""
+    h0, h1, h2, tablog = (_d(v) for v in (h0, h1, h2, tablog))
+    tb = _AtlasTables(_ptr(h0), _ptr(h1), _ptr(h2), _ptr(tablog))
+    ld = np.ascontiguousarray(linedata, np.int32)
+    xnfdop, dopple = _d(atm["xnfdop"]), _d(atm["dopple"])
+    nspec, kw = xnfdop.shape
+    nrhox = int(atm.get("nrhox", kw))
+    xne, txnxn, hckt = _d(atm["xne"]), _d(atm["txnxn"]), _d(atm["hckt"])
+    tabcont = _d(tabcont)
+    iw = np.ascontiguousarray(iwavetab, np.int32)
+    waveset = _d(waveset)
+    xl = np.zeros((waveset.size, kw))
+    used = _lib2().orc_atlas_linop1(ctypes.byref(tb), _ptr(ld, _ip), ld.shape[0], nrhox, kw, _ptr(xnfdop),
+                                    _ptr(dopple), nspec, _ptr(xne), _ptr(txnxn), _ptr(hckt), _ptr(tabcont),
+                                    _ptr(iw, _ip), iw.size - 1, _ptr(waveset), waveset.size, _ptr(xl))
+    return xl, used
+
+
+def atlas_rt_pass(ops, waveset, rcoset, acont, sigmac, xlines, rhox, t, hkt, teff, scont=None, nu0=1, nu1=None):
+    waveset, rcoset, acont, sigmac, xlines, rhox, t, hkt = (
+        _d(v) for v in (waveset, rcoset, acont, sigmac, xlines, rhox, t, hkt))
+    numnu, kw = acont.shape
+    nrhox = rhox.size
+    nu1 = numnu if nu1 is None else nu1
+    acc = {k: np.zeros(nrhox) for k in ("rjmins", "rdabh", "rdiagj", "flxrad", "raden", "h_total",
+                                         "accrad", "abross")}
+    A = _Accum(*[_ptr(acc[k]) for k in ("rjmins", "rdabh", "rdiagj", "flxrad", "raden", "h_total",
+                                        "accrad", "abross")], 0.0)
+    hs = np.zeros(nu1 - nu0 + 1)
+    sc = None if scont is None else _d(scont)
+    _lib2().orc_atlas_rt_pass(ctypes.byref(ops), numnu, _ptr(waveset), _ptr(rcoset), _ptr(acont), _ptr(sigmac),
+                              None if sc is None else sc.ctypes.data_as(ctypes.c_void_p), kw, _ptr(xlines), nrhox,
+                              _ptr(rhox), _ptr(t), _ptr(hkt), teff, nu0, nu1, ctypes.byref(A), _ptr(hs))
+    acc["pradk0"] = A.pradk0
+    return acc, hs

@@ -1,0 +1,78 @@
+"""Extract the reference's own data constants into a test fixture.
+
+Run in a container where the reference checkout is mounted (it is read, never
+modified).  Writes tests/golden/reference_tables.npz with:
+
+  coefj, coefh   51x51 J and H operators, from data/blockj.dat, blockh.dat
+                 (BLOCKJ/BLOCKH, atlas12_modules.f90:18792-18860: 2601 REAL*4
+                 values after a 3-line header, column-major, promoted to
+                 REAL*8) -- stored as coef[L-1, M-1] = COEF(L, M)
+  xtau8, ch_j, ck_j   JOSH's fixed 51-point tau grid and surface H / K
+                 quadrature weights (atlas12_modules.f90:18409-18451)
+  tabvi, tabh1   TABVOIGT's 81-point H1(v) table (atlas12_modules.f90:19805-19835)
+  awei, lwei     Weideman N=32 coefficients (synthe_module.f90:91-126), kept
+                 only to pin the product's own derivation of them
+  wavetab        KAPCONT's 361-point continuum-cutoff grid (atlas12_modules.f90:1811-1857)
+
+Usage:  python tests/golden/make_golden.py [reference_root]
+"""
+import ctypes
+import os
+import re
+import sys
+
+import numpy as np
+
+ROOT = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+_libc = ctypes.CDLL(None)
+_libc.strtof.restype = ctypes.c_float
+_libc.strtof.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_char_p)]
+
+
+def read_real4_block(path):
+    """List-directed READ of REAL*4 after 3 header lines (strtof = correctly rounded)."""
+    with open(path) as f:
+        lines = f.read().splitlines()[3:]
+    toks = " ".join(lines).replace(",", " ").split()
+    vals = np.array([_libc.strtof(t.encode(), None) for t in toks[:2601]], dtype=np.float32)
+    assert vals.size == 2601, path
+    # COEF = reshape(dble(C), (/51,51/)): column-major
+    return vals.astype(np.float64).reshape(51, 51, order="F")
+
+
+def fortran_array(src, name, count):
+    i = src.index(name)
+    j = src.index("/)", i) if "(/" in src[i:i + 200] else src.index("]", i)
+    body = src[i:j]
+    body = body[body.index("(/") + 2:] if "(/" in body else body[body.index("[") + 1:]
+    body = re.sub(r"!.*", "", body)
+    nums = re.findall(r"[-+]?\d*\.\d+(?:[DdEe][-+]?\d+)?|[-+]?\d+\.(?:[DdEe][-+]?\d+)?", body)
+    vals = np.array([float(x.replace("D", "e").replace("d", "e")) for x in nums])
+    assert vals.size == count, (name, vals.size)
+    return vals
+
+
+def main():
+    mod = open(os.path.join(ROOT, "src", "atlas12_modules.f90")).read()
+    syn = open(os.path.join(ROOT, "src", "synthe_module.f90")).read()
+    out = dict(
+        coefj=read_real4_block(os.path.join(ROOT, "data", "blockj.dat")),
+        coefh=read_real4_block(os.path.join(ROOT, "data", "blockh.dat")),
+        ch_j=fortran_array(mod, "CH_J(NXTAU) =", 51),
+        ck_j=fortran_array(mod, "CK_J(NXTAU) =", 51),
+        xtau8=fortran_array(mod, "XTAU8(NXTAU) =", 51),
+        tabvi=fortran_array(mod, "TABVI(81) =", 81),
+        tabh1=fortran_array(mod, "TABH1(81) =", 81),
+        awei=fortran_array(syn, "AWEI(32) =", 32),
+        lwei=np.array([float(re.search(r"LWEI = ([0-9.D+-]+)", syn).group(1).replace("D", "e"))]),
+        wavetab=fortran_array(mod, "WAVETAB(NWAVE) =", 361),
+    )
+    np.savez(os.path.join(HERE, "reference_tables.npz"), **out)
+    for k, v in out.items():
+        print(k, v.shape)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,138 @@
+"""SYNTHE hot path on the GPU (through the C ABI) against the CPU oracle.
+
+Tolerances:
+  * nbuff (binning): bit-exact.
+  * continuum (REAL(4)): 2 ulp (device exp10 vs the C library powf).
+  * kappa_line: |GPU - oracle_fp64| <= 1e-5 * (kappa_line + kappa_cont) per bin
+    for both precisions (typically ~1e-7 mixed, ~1e-12 fp64); against the
+    reference's REAL(4) sequential sums (oracle ref32) <= 1e-4 * (k + k_c).
+  * flux: relative 1e-4 against the oracle on the same opacity.
+"""
+import numpy as np
+import pytest
+
+from atlas12_b200 import _lib, synthetic
+from atlas12_b200 import synthe as S
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small_case():
+    return synthetic.synthe_case(nlines=3000, wlbeg=400.0, wlend=402.0, seed=5)
+
+
+@pytest.fixture(scope="module")
+def prepared(po, small_case):
+    case = small_case
+    g = po.synthe_grid(case["wlbeg"], case["wlend"], case["resolu"])
+    nb = np.array([po.nbuff(w, g["ratiolg"], g["ixwlbeg"]) for w in case["lines"]["wlvac"]], np.int32)
+    lines = dict(case["lines"], nbuff=nb)
+    cont = po.synthe_continuum(po.REF32, case["wledge"], case["continall"], g["wbegin"], g["ratio"], g["length"])
+    o32, o32_64 = po.synthe_line_opacity(po.REF32, lines, g["length"], case["atm"], cont, case["resolu"])
+    o64, o64_64 = po.synthe_line_opacity(po.FP64, lines, g["length"], case["atm"], cont, case["resolu"])
+    return dict(case=case, grid=g, lines=lines, cont=cont, ref32=o32_64, fp64=o64_64)
+
+
+def _rec(lines):
+    return S.make_lte_lines(lines["nbuff"], lines["cgf"], lines["nelion"], lines["elo"], lines["gamrf"],
+                            lines["gamsf"], lines["gamwf"])
+
+
+def _kappa_err(got, ref, cont):
+    return np.max(np.abs(got.astype(np.float64) - ref) / (ref + cont.astype(np.float64)))
+
+
+def test_bin_bitexact_including_boundaries(po, gpu_ctx, tables):
+    syn = S.Synthe(gpu_ctx, tables)
+    g = S.synthe_grid(300.0, 1000.0, 500000.0)
+    rng = np.random.default_rng(11)
+    wl = np.sort(rng.uniform(300.0, 1000.0, 200000))
+    k = rng.integers(g["ixwlbeg"], g["ixwlbeg"] + g["length"], 2000)
+    edge = np.exp((k + 0.5) * g["ratiolg"])              # on the rounding boundary
+    near = np.nextafter(edge, edge * (1 + rng.choice([-1, 1], edge.size)))
+    onpt = g["wbegin"] * g["ratio"] ** rng.integers(0, g["length"], 2000)
+    allw = np.concatenate([wl, edge, near, onpt])
+    got = syn.bin_lines(allw, g)
+    ref = np.array([po.nbuff(w, g["ratiolg"], g["ixwlbeg"]) for w in allw], np.int32)
+    np.testing.assert_array_equal(got, ref)
+
+
+def test_continuum_matches_oracle(prepared, gpu_ctx, tables):
+    p = prepared
+    syn = S.Synthe(gpu_ctx, tables)
+    got = syn.continuum(p["case"]["wledge"], p["case"]["continall"], p["grid"])
+    np.testing.assert_allclose(got, p["cont"], rtol=2.5e-7)
+
+
+@pytest.mark.parametrize("prec", [_lib.PREC_FP64, _lib.PREC_MIXED])
+def test_line_opacity_matches_fp64_oracle(prepared, gpu_ctx, tables, prec):
+    p = prepared
+    gpu_ctx.set_precision(prec)
+    syn = S.Synthe(gpu_ctx, tables)
+    atm = p["case"]["atm"]
+    got = syn.line_opacity(_rec(p["lines"]), p["grid"], p["case"]["resolu"], p["cont"], atm["xnfdop"],
+                           atm["dopple"], atm["xne"], atm["txnxn"], atm["hckt"])
+    gpu_ctx.set_precision(_lib.PREC_MIXED)
+    e64 = _kappa_err(got, p["fp64"], p["cont"])
+    e32 = _kappa_err(got, p["ref32"], p["cont"])
+    assert e64 <= 1e-5, e64
+    assert e32 <= 1e-4, e32
+    assert np.all(np.isfinite(got)) and got.max() > 0
+
+
+def test_line_opacity_edge_cases(po, prepared, gpu_ctx, tables):
+    p = prepared
+    syn = S.Synthe(gpu_ctx, tables)
+    atm = p["case"]["atm"]
+    g = p["grid"]
+    # empty line list
+    empty = S.make_lte_lines(*[np.zeros(0)] * 7)
+    out = syn.line_opacity(empty, g, p["case"]["resolu"], p["cont"], atm["xnfdop"], atm["dopple"], atm["xne"],
+                           atm["txnxn"], atm["hckt"])
+    assert out.shape == p["cont"].shape and not out.any()
+    # lines off both ends of the grid (wings reach in) and a small profile cap
+    L = dict(p["lines"])
+    L = {k: v[:400].copy() for k, v in L.items()}
+    L["nbuff"][:100] -= g["length"] + 50
+    L["nbuff"][100:200] += g["length"] + 50
+    for maxprof in (1000000, 60):
+        ref = po.synthe_line_opacity(po.FP64, L, g["length"], atm, p["cont"], p["case"]["resolu"],
+                                     maxprof=maxprof)[1]
+        got = syn.line_opacity(_rec(L), g, p["case"]["resolu"], p["cont"], atm["xnfdop"], atm["dopple"],
+                               atm["xne"], atm["txnxn"], atm["hckt"], maxprof=maxprof)
+        assert _kappa_err(got, ref, p["cont"]) <= 1e-5
+
+
+def test_spectrum_matches_oracle(po, ops, prepared, gpu_ctx, tables):
+    p = prepared
+    case, g = p["case"], p["grid"]
+    syn = S.Synthe(gpu_ctx, tables)
+    op = p["ref32"].astype(np.float32)
+    atm = case["atm"]
+    flux, cont = syn.spectrum(case["wledge"], case["contabs"], case["contscat"], atm["rhox"], atm["hkt"], g, op)
+    sel = np.linspace(1, g["length"], 300).astype(int)
+    rf = np.zeros(sel.size)
+    rc = np.zeros(sel.size)
+    for i, iw in enumerate(sel):
+        f, c = po.synthe_spectrum(ops, case["wledge"], case["contabs"], case["contscat"], atm["rhox"], atm["hkt"],
+                                  g["wbegin"], g["ratio"], op, iw0=int(iw), iw1=int(iw))
+        rf[i], rc[i] = f[0], c[0]
+    np.testing.assert_allclose(flux[sel - 1], rf, rtol=1e-4)
+    np.testing.assert_allclose(cont[sel - 1], rc, rtol=1e-4)
+    assert np.all(flux > 0) and np.all(flux <= cont * (1 + 1e-9))
+
+
+def test_full_c1_pipeline(po, gpu_ctx, tables):
+    """The CPU-runnable configuration end to end: 20k lines, 12,346 points."""
+    case = synthetic.synthe_case()
+    syn = S.Synthe(gpu_ctx, tables)
+    wave, flux, cflux, op = syn.run(case)
+    g = po.synthe_grid(case["wlbeg"], case["wlend"], case["resolu"])
+    assert op.shape == (72, g["length"]) == (72, 12346)
+    nb = np.array([po.nbuff(w, g["ratiolg"], g["ixwlbeg"]) for w in case["lines"]["wlvac"]], np.int32)
+    lines = dict(case["lines"], nbuff=nb)
+    cont = po.synthe_continuum(po.REF32, case["wledge"], case["continall"], g["wbegin"], g["ratio"], g["length"])
+    ref = po.synthe_line_opacity(po.FP64, lines, g["length"], case["atm"], cont, case["resolu"])[1]
+    assert _kappa_err(op, ref, cont) <= 1e-5
+    assert np.all(np.isfinite(flux)) and np.all(flux > 0)
