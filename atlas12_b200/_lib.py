@@ -70,7 +70,40 @@ SIGNATURES = {
     "atlasgpu_synthe_line_opacity_dev": (_I, [_P, _P, _I64, _I, _I, _D, _P, _P, _P, _I, _P, _P, _P, _I, _P]),
     "atlasgpu_synthe_spectrum": (_I, [_P, _P, _I, _P, _P, _I, _I, _P, _P, _D, _D, _I, _P, _P, _P]),
     "atlasgpu_synthe_spectrum_dev": (_I, [_P, _P, _I, _P, _P, _I, _I, _P, _P, _D, _D, _I, _P, _P, _P]),
+    "atlasgpu_atlas_set_voigt_tables": (_I, [_P, _P, _P, _P, _I]),
+    "atlasgpu_atlas_linop": (_I, [_P, _P, _I64, _I, _I, _P, _P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P,
+                                  ctypes.POINTER(_I64)]),
+    "atlasgpu_atlas_rt_pass": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _D,
+                                    ctypes.POINTER(Accum), _P]),
+    "atlasgpu_atlas_finish": (_I, [_P, ctypes.c_void_p, ctypes.POINTER(Accum), ctypes.POINTER(_D)]),
+    "atlasgpu_model_create": (_I, [_P, ctypes.c_void_p, ctypes.POINTER(_P)]),
+    "atlasgpu_model_iterate": (_I, [_P, _P, _I, _D, _I, ctypes.POINTER(_I), _P]),
+    "atlasgpu_model_get": (_I, [_P, _P, _P, _P, _P, _P, _P, _P]),
+    "atlasgpu_model_set_structure": (_I, [_P, _P, _P, _P, _P]),
+    "atlasgpu_model_destroy": (_I, [_P, _P]),
+    "atlasgpu_surrogate_eval": (_I, [_P, _I, _P, _P, _D, _I, _P, _P, _P, _P, _P]),
 }
+
+_DP = ctypes.POINTER(ctypes.c_double)
+
+
+class FinishState(ctypes.Structure):
+    """atlasgpu_finish_state (include/atlasgpu.h)."""
+    _fields_ = [("nrhox", _I), ("iter", _I), ("teff", _D), ("grav", _D), ("pradk0", _D)] + \
+               [(n, _DP) for n in ("t", "rhox", "p", "xne", "abross", "prad", "vturb", "pturb", "tauros",
+                                   "accrad", "raden", "oldt1", "flxerr", "dtflux", "dtlamb", "dtsurf", "t1")] + \
+               [("ross_n", _I), ("ross_max", _I), ("ross_zerot", _D), ("ross_slopet", _D), ("ross_zerop", _D),
+                ("ross_slopep", _D), ("ross_t", _DP), ("ross_p", _DP), ("ross_k", _DP)]
+
+
+class ModelDesc(ctypes.Structure):
+    """atlasgpu_model_desc (include/atlasgpu.h)."""
+    _fields_ = [("teff", _D), ("logg", _D), ("vturb_kms", _D), ("nrhox", _I),
+                ("t", _DP), ("p", _DP), ("rhox", _DP), ("tauros", _DP),
+                ("waveset", _DP), ("rcoset", _DP), ("numnu", _I),
+                ("cutoff_wave", _DP), ("nwave", _I),
+                ("linedata", ctypes.POINTER(ctypes.c_int32)), ("nlines", _I64),
+                ("h0tab", _DP), ("h1tab", _DP), ("h2tab", _DP)]
 
 _lib = None
 

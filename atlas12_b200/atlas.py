@@ -1,0 +1,206 @@
+"""Host-side mirror of ATLAS12's hot path (atlas12c.f90 + RUN_RT_PASS), on the C ABI.
+
+Reference names and meanings:
+
+* ``waveset_rcoset``  -- WAVESET and the RCOSET trapezoid weights (atlas12c.f90:451-491)
+* ``tabvoigt``        -- H0/H1/H2 tables at 200 steps per Doppler width (TABVOIGT)
+* ``Atlas.linop1``    -- XLINES(J,NU) from LINEDATA (LINOP1)
+* ``Atlas.rt_pass``   -- the frequency loop with JOSH and the mode-2 sums (RUN_RT_PASS)
+* ``Atlas.finish``    -- ROSS(3), RADIAP(3), TCORR(3) on one model
+* ``AtlasModel``      -- one atmosphere iterated on the device (the ITERAT loop,
+                         atlas12c.f90:496-606) with the synthetic surrogate physics
+
+Arrays follow the reference layouts seen from C: XLINES(kw, numnu) is
+[numnu, kw], XNFDOP(kw, mion) is [mion, kw].
+"""
+import ctypes
+
+import numpy as np
+from scipy.special import dawsn
+
+from . import _lib, surrogate, synthetic
+from ._lib import Accum, Context, FinishState, ModelDesc, ptr
+
+LINE_CUTOFF = 1.0e-3
+RATIOLG_LINES = np.log(1.0 + 1.0 / 2000000.0)
+ACC_NAMES = ("rjmins", "rdabh", "rdiagj", "flxrad", "raden", "h_total", "accrad", "abross")
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def tabvoigt(vsteps=200.0, n=2001):
+    """H0 = exp(-v^2), H1 = -2/sqrt(pi) (1 - 2 v F(v)) (F = Dawson's integral),
+    H2 = (1 - 2 v^2) exp(-v^2) on v = (i-1)/vsteps.  The reference tabulates H1
+    from an 81-point table remapped with MAP1 (TABVOIGT); this driver evaluates
+    the function itself."""
+    v = np.arange(n) / vsteps
+    h0 = np.exp(-v * v)
+    h1 = -2.0 / np.sqrt(np.pi) * (1.0 - 2.0 * v * dawsn(v))
+    h2 = h0 - (v * v + v * v) * h0
+    return h0, h1, h2
+
+
+def cutoff_grid(n=361, lo=9.0, hi=400000.0):
+    """KAPCONT's continuum-cutoff wavelengths (nm): a log-spaced stand-in for WAVETAB."""
+    return np.geomspace(lo, hi, n)
+
+
+def iwavetab(cutwave):
+    """IWAVETAB = INT(LOG(WAVE)/RATIOLG + 0.5) plus the 2**30 sentinel (KAPCONT :19096)."""
+    iw = np.empty(cutwave.size + 1, dtype=np.int32)
+    iw[:-1] = (np.log(cutwave) / RATIOLG_LINES + 0.5).astype(np.int64)
+    iw[-1] = 2 ** 30
+    return iw
+
+
+class Atlas:
+    """The ATLAS12 kernels on one context (parity-level entry points)."""
+
+    def __init__(self, ctx: Context, operators, h0=None, h1=None, h2=None):
+        self.ctx = ctx
+        ctx.set_operators(operators["xtau8"], operators["coefj"], operators["coefh"], operators["ch_j"],
+                          operators["ck_j"])
+        if h0 is None:
+            h0, h1, h2 = tabvoigt()
+        self.tables = [np.ascontiguousarray(x, np.float64) for x in (h0, h1, h2)]
+        ctx.call("atlasgpu_atlas_set_voigt_tables", *[ptr(x) for x in self.tables], 2001)
+
+    def linop1(self, linedata, nrhox, xnfdop, dopple, xne, txnxn, hckt, tabcont, iwt, waveset):
+        ld = np.ascontiguousarray(linedata, np.int32)
+        xd = np.ascontiguousarray(xnfdop, np.float64)
+        dp = np.ascontiguousarray(dopple, np.float64)
+        nspec, kw = xd.shape
+        vec = [np.ascontiguousarray(v, np.float64) for v in (xne, txnxn, hckt)]
+        tc = np.ascontiguousarray(tabcont, np.float64)
+        iw = np.ascontiguousarray(iwt, np.int32)
+        ws = np.ascontiguousarray(waveset, np.float64)
+        out = np.zeros((ws.size, kw))
+        used = ctypes.c_int64(0)
+        self.ctx.call("atlasgpu_atlas_linop", ptr(ld), ld.shape[0], int(nrhox), kw, ptr(xd), ptr(dp), nspec,
+                      *[ptr(v) for v in vec], ptr(tc), ptr(iw), iw.size - 1, ptr(ws), ws.size, ptr(out),
+                      ctypes.byref(used))
+        return out, used.value
+
+    def rt_pass(self, waveset, rcoset, acont, sigmac, xlines, rhox, t, hkt, teff, scont=None):
+        ws, rc = (np.ascontiguousarray(v, np.float64) for v in (waveset, rcoset))
+        ac, sg, xl = (np.ascontiguousarray(v, np.float64) for v in (acont, sigmac, xlines))
+        sc = None if scont is None else np.ascontiguousarray(scont, np.float64)
+        numnu, kw = ac.shape
+        rx, tt, hk = (np.ascontiguousarray(v, np.float64) for v in (rhox, t, hkt))
+        nrhox = rx.size
+        acc = {k: np.zeros(nrhox) for k in ACC_NAMES}
+        A = Accum(*[_dp(acc[k]) for k in ACC_NAMES], 0.0)
+        hs = np.zeros(numnu)
+        self.ctx.call("atlasgpu_atlas_rt_pass", numnu, ptr(ws), ptr(rc), ptr(ac), ptr(sg), ptr(sc), kw, ptr(xl),
+                      nrhox, ptr(rx), ptr(tt), ptr(hk), float(teff), ctypes.byref(A), ptr(hs))
+        acc["pradk0"] = A.pradk0
+        return acc, hs
+
+    def finish(self, model, acc, iteration, store):
+        """model: dict of [nrhox] arrays (t, rhox, p, xne, abross, prad, vturb, pturb, tauros, accrad,
+        raden, oldt1) updated in place; store: RossStore (ROSSTAB history, updated).
+        Returns (max |FLXERR|, dict of the .iter columns)."""
+        n = model["t"].size
+        out = {k: np.zeros(n) for k in ("flxerr", "dtflux", "dtlamb", "dtsurf", "t1")}
+        names = ("t", "rhox", "p", "xne", "abross", "prad", "vturb", "pturb", "tauros", "accrad", "raden", "oldt1")
+        for k in names:
+            model[k] = np.ascontiguousarray(model[k], np.float64)
+        st = FinishState(n, int(iteration), float(model["teff"]), float(model["grav"]), float(acc["pradk0"]),
+                         *[_dp(model[k]) for k in names], *[_dp(out[k]) for k in out],
+                         store.n, store.maxtab, *store.norm, _dp(store.t), _dp(store.p), _dp(store.k))
+        a = {k: np.ascontiguousarray(acc[k], np.float64).copy() for k in ACC_NAMES}
+        A = Accum(*[_dp(a[k]) for k in ACC_NAMES], float(acc["pradk0"]))
+        err = ctypes.c_double(0)
+        self.ctx.call("atlasgpu_atlas_finish", ctypes.byref(st), ctypes.byref(A), ctypes.byref(err))
+        model["pradk0"] = st.pradk0
+        store.n = st.ross_n
+        store.norm = [st.ross_zerot, st.ross_slopet, st.ross_zerop, st.ross_slopep]
+        return err.value, out
+
+
+class RossStore:
+    """ROSSTAB's growing table of the model's own (log T, log P, log kappa_R)
+    points (ROSSTAB_MAXTAB = kw*60 with kw = 80)."""
+
+    def __init__(self, maxtab=80 * 60):
+        self.n = 0
+        self.maxtab = maxtab
+        self.norm = [0.0, 1.0, 0.0, 1.0]
+        self.t = np.zeros(maxtab)
+        self.p = np.zeros(maxtab)
+        self.k = np.zeros(maxtab)
+
+    def copy(self):
+        c = RossStore(self.maxtab)
+        c.n, c.norm = self.n, list(self.norm)
+        c.t, c.p, c.k = self.t.copy(), self.p.copy(), self.k.copy()
+        return c
+
+
+class AtlasModel:
+    """One ATLAS12 atmosphere iterated entirely on the device.
+
+    The starting structure is the Eddington grey model on TAUSTD (or a given
+    structure); populations and continuum come from atlas12_b200.surrogate.
+    """
+
+    def __init__(self, ctx: Context, operators, teff=5777.0, logg=4.44, vturb=1.5, linedata=None,
+                 waveset=None, rcoset=None, nrhox=72, ross=None, start=None, h_tables=None):
+        self.ctx = ctx
+        ctx.set_operators(operators["xtau8"], operators["coefj"], operators["coefh"], operators["ch_j"],
+                          operators["ck_j"])
+        self.ross = ross or surrogate.RossTable()
+        m = start or surrogate.grey_model(teff, logg, nrhox=nrhox, ross=self.ross)
+        if waveset is None:
+            waveset, rcoset = synthetic.geometric_waveset()
+        self.waveset = np.ascontiguousarray(waveset, np.float64)
+        self.rcoset = np.ascontiguousarray(rcoset, np.float64)
+        self.cutwave = cutoff_grid()
+        ld = np.zeros((0, 4), np.int32) if linedata is None else np.ascontiguousarray(linedata, np.int32)
+        h0, h1, h2 = h_tables or tabvoigt()
+        self._keep = [np.ascontiguousarray(x, np.float64) for x in (m["t"], m["p"], m["rhox"], m["tauros"])]
+        self._keep += [np.ascontiguousarray(x, np.float64) for x in (h0, h1, h2)]
+        self._keep += [ld]
+        t, p, rx, tau, h0, h1, h2, ld = self._keep
+        self.nrhox = t.size
+        self.teff = teff
+        d = ModelDesc(teff, logg, vturb, self.nrhox, _dp(t), _dp(p), _dp(rx), _dp(tau), _dp(self.waveset),
+                      _dp(self.rcoset), self.waveset.size, _dp(self.cutwave), self.cutwave.size,
+                      ld.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ld.shape[0], _dp(h0), _dp(h1), _dp(h2))
+        self._h = ctypes.c_void_p()
+        ctx.call("atlasgpu_model_create", ctypes.byref(d), ctypes.byref(self._h))
+
+    def iterate(self, max_iter=30, tol_percent=0.1, graph=True):
+        """Iterate until max |FLXERR| <= tol_percent (percent) or max_iter.
+        Returns (iterations run, per-iteration max |FLXERR|)."""
+        hist = np.zeros(max(max_iter, 1))
+        done = ctypes.c_int(0)
+        self.ctx.call("atlasgpu_model_iterate", self._h, int(max_iter), float(tol_percent), 1 if graph else 0,
+                      ctypes.byref(done), ptr(hist))
+        return done.value, hist[:done.value]
+
+    def structure(self):
+        n = self.nrhox
+        out = {k: np.zeros(n) for k in ("t", "rhox", "p", "xne", "flxerr")}
+        hs = np.zeros(self.waveset.size)
+        self.ctx.call("atlasgpu_model_get", self._h, *[ptr(out[k]) for k in ("t", "rhox", "p", "xne", "flxerr")],
+                      ptr(hs))
+        out["hsurf"] = hs
+        return out
+
+    def set_structure(self, t, p, rhox):
+        arrs = [np.ascontiguousarray(x, np.float64) for x in (t, p, rhox)]
+        self.ctx.call("atlasgpu_model_set_structure", self._h, *[ptr(a) for a in arrs])
+
+    def close(self):
+        if self._h:
+            _lib.lib().atlasgpu_model_destroy(self.ctx.handle, self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

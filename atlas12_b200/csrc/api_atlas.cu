@@ -1,0 +1,343 @@
+// api_atlas.cu -- C ABI: the ATLAS12 entry points (LINOP1, RT pass, finish)
+// and the device-resident model iteration.
+#include <cmath>
+#include <vector>
+
+#include "api_common.cuh"
+#include "atlas.cuh"
+#include "tcorr.cuh"
+
+using namespace atlasgpu;
+
+namespace {
+
+constexpr int kTabN = 2001;
+
+int ensure_tablog(atlasgpu_ctx* ctx, double** out) {
+  double* d;
+  const bool fresh = ctx->bufs.find("tablog") == ctx->bufs.end();
+  int r = bufT(ctx, "tablog", 65536, &d);
+  if (r) return r;
+  if (fresh) {
+    // TABLOG(I) = 10**((I-16384)*0.001) for every INTEGER(2) I, with the C
+    // library pow that the reference's ** calls
+    std::vector<double> h(65536);
+    for (int k = 0; k < 65536; ++k) h[k] = pow(10.0, (double)((k - 32768) - 16384) * 0.001);
+    CK(cudaMemcpy(d, h.data(), 65536 * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  *out = d;
+  return 0;
+}
+
+}  // namespace
+
+namespace atlasgpu {
+// Line preparation with the host fix of near-tie frequency brackets.
+int atlas_prep_lines(atlasgpu_ctx* ctx, const int32_t* d_ld, const int32_t* h_ld, int64_t n,
+               const double* d_tablog, const double* d_ws, const double* h_ws, int numnu,
+               const int32_t* d_iwt, int nwave, int nspec, AtlasLine* d_lines) {
+  unsigned long long* d_nf;
+  int64_t* d_fl;
+  const int64_t cap = 1 << 16;
+  int r;
+  if ((r = bufT(ctx, "ap_nflag", 1, &d_nf)) || (r = bufT(ctx, "ap_flag", cap, &d_fl))) return r;
+  CK(cudaMemsetAsync(d_nf, 0, sizeof(unsigned long long), ctx->stream));
+  AtlasPrepArgs a{d_ld, n, d_tablog, d_ws, numnu, d_iwt, nwave, nspec, d_lines, d_fl, d_nf, cap};
+  {
+    Timer tm(ctx, "atlas_prep");
+    k_atlas_prep<<<grid_for(ctx, n, 256, 16), 256, 0, ctx->stream>>>(a);
+    CKL(ctx);
+  }
+  unsigned long long nf = 0;
+  CK(cudaMemcpyAsync(&nf, d_nf, sizeof nf, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if ((int64_t)nf > cap) return fail(ctx, ATLASGPU_EINVAL, "prep: %llu near-tie lines", nf);
+  if (nf) {
+    std::vector<int64_t> fl(nf);
+    CK(cudaMemcpy(fl.data(), d_fl, nf * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    const double RATIOLG = log(1.0 + 1.0 / 2000000.0);
+    for (unsigned long long k = 0; k < nf; ++k) {
+      const int64_t i = fl[k];
+      int32_t rec[4];
+      if (h_ld) memcpy(rec, h_ld + 4 * i, sizeof rec);
+      else CK(cudaMemcpy(rec, d_ld + 4 * i, sizeof rec, cudaMemcpyDeviceToHost));
+      AtlasLine L;
+      CK(cudaMemcpy(&L, d_lines + i, sizeof L, cudaMemcpyDeviceToHost));
+      const double wl = exp(rec[0] * RATIOLG);  // the reference's EXP
+      int nu = 1;
+      while (nu < numnu && wl >= h_ws[nu - 1]) ++nu;
+      auto tablog = [](int32_t word, int hi) {
+        const int16_t v = (int16_t)(hi ? ((uint32_t)word >> 16) : (word & 0xffff));
+        return pow(10.0, (double)((int)v - 16384) * 0.001);
+      };
+      const double CEN_PREFAC4 = 0.026538 / kSqrtPi / kClightNms;
+      const double FOURPI_C_INV = 1.0 / (4.0 * kPi * kClightNms);
+      L.cgf = CEN_PREFAC4 * wl * tablog(rec[2], 0);
+      L.gr = tablog(rec[2], 1) * wl * FOURPI_C_INV;
+      L.gs = tablog(rec[3], 0) * wl * FOURPI_C_INV;
+      L.gw = tablog(rec[3], 1) * wl * FOURPI_C_INV;
+      L.wlvac = wl;
+      L.nu = nu;
+      CK(cudaMemcpy(d_lines + i, &L, sizeof L, cudaMemcpyHostToDevice));
+    }
+  }
+  return 0;
+}
+}  // namespace atlasgpu
+
+namespace {
+
+__global__ void k_transpose(const double* __restrict__ in, int rows, int cols, double* __restrict__ out) {
+  // out[c][r] = in[r][c]
+  __shared__ double tile[32][33];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = r0 + k, c = c0 + threadIdx.x;
+    if (r < rows && c < cols) tile[k][threadIdx.x] = in[(size_t)r * cols + c];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int c = c0 + k, r = r0 + threadIdx.x;
+    if (r < rows && c < cols) out[(size_t)c * rows + r] = tile[threadIdx.x][k];
+  }
+}
+
+int transpose(atlasgpu_ctx* ctx, const double* in, int rows, int cols, double* out) {
+  dim3 g((cols + 31) / 32, (rows + 31) / 32), b(32, 8);
+  k_transpose<<<g, b, 0, ctx->stream>>>(in, rows, cols, out);
+  CKL(ctx);
+  return 0;
+}
+
+int rt_launch(atlasgpu_ctx* ctx, RtArgs& a, bool surr, double* d_sum, int* nwarps_out) {
+  int nwarp = 4;
+  const size_t per = sizeof(RtWS);
+  while (nwarp > 1 && sizeof(double) * kKwMax + nwarp * per > ctx->smem_optin) --nwarp;
+  const size_t smem = sizeof(double) * kKwMax + nwarp * per;
+  // enough warps to fill every SM several times, frequencies contiguous per warp
+  const int target_warps = ctx->nsm * nwarp * 6;
+  a.nu_per_warp = std::max(1, (a.numnu + target_warps - 1) / target_warps);
+  const int nw = (a.numnu + a.nu_per_warp - 1) / a.nu_per_warp;
+  const int blocks = (nw + nwarp - 1) / nwarp;
+  const int nwl = blocks * nwarp;
+  double* part;
+  int r;
+  if ((r = bufT(ctx, surr ? "rt_part_m" : "rt_part", (size_t)nwl * (kAcc * a.kw + 1), &part))) return r;
+  a.partial = part;
+  if (surr) {
+    CK(cudaFuncSetAttribute(k_atlas_rt<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  } else {
+    CK(cudaFuncSetAttribute(k_atlas_rt<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+  {
+    Timer tm(ctx, "atlas_rt");
+    if (surr) k_atlas_rt<true><<<blocks, 32 * nwarp, smem, ctx->stream>>>(a);
+    else k_atlas_rt<false><<<blocks, 32 * nwarp, smem, ctx->stream>>>(a);
+    CKL(ctx);
+  }
+  {
+    Timer tm(ctx, "atlas_reduce");
+    k_atlas_reduce<<<(kAcc * a.kw + 1 + 127) / 128, 128, 0, ctx->stream>>>(part, nwl, a.kw, 0, d_sum);
+    CKL(ctx);
+  }
+  if (nwarps_out) *nwarps_out = nwl;
+  return 0;
+}
+
+__global__ void k_finish_one(ModelState* s, double* acc, int kw, int n, int iter, double teff,
+                             double grav, RossStore* R, double* work) {
+  if (blockIdx.x == 0) w_atlas_finish(*s, acc, kw, n, iter, teff, grav, R, work, threadIdx.x & 31);
+}
+
+}  // namespace
+
+extern "C" {
+
+int atlasgpu_atlas_set_voigt_tables(atlasgpu_ctx* ctx, const double* h0, const double* h1,
+                                    const double* h2, int n) {
+  if (!ctx || !h0 || !h1 || !h2 || n != kTabN) return fail(ctx, ATLASGPU_EINVAL, "voigt tables: n must be 2001");
+  if (!finite_all(h0, n) || !finite_all(h1, n) || !finite_all(h2, n))
+    return fail(ctx, ATLASGPU_ENONFINITE, "voigt tables: non-finite entry");
+  cudaSetDevice(ctx->device);
+  double *d0, *d1, *d2, *tl;
+  int r;
+  if ((r = bufT(ctx, "tab_h0", n, &d0)) || (r = bufT(ctx, "tab_h1", n, &d1)) || (r = bufT(ctx, "tab_h2", n, &d2)) ||
+      (r = ensure_tablog(ctx, &tl)))
+    return r;
+  CK(cudaMemcpy(d0, h0, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d1, h1, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d2, h2, n * sizeof(double), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int atlasgpu_atlas_linop(atlasgpu_ctx* ctx, const int32_t* linedata, int64_t n, int nrhox, int kw,
+                         const double* xnfdop, const double* dopple, int nspec, const double* xne,
+                         const double* txnxn, const double* hckt, const double* tabcont,
+                         const int32_t* iwavetab, int nwave, const double* waveset, int numnu,
+                         double* xlines_out, int64_t* lines_used) {
+  if (!ctx || n < 0 || (n > 0 && !linedata) || nrhox < 8 || kw < nrhox || kw > kKwMax || nspec < 1 ||
+      !xnfdop || !dopple || !xne || !txnxn || !hckt || !tabcont || !iwavetab || nwave < 1 || !waveset ||
+      numnu < 2 || !xlines_out)
+    return fail(ctx, ATLASGPU_EINVAL, "atlas_linop: bad argument");
+  if (ctx->bufs.find("tab_h0") == ctx->bufs.end())
+    return fail(ctx, ATLASGPU_ESTATE, "atlas_linop: Voigt tables not set");
+  for (int i = 1; i < numnu; ++i)
+    if (!(waveset[i] > waveset[i - 1])) return fail(ctx, ATLASGPU_EINVAL, "WAVESET not increasing");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  int32_t *d_ld, *d_iw;
+  double *d_xd, *d_dp, *d_xne, *d_tx, *d_hc, *d_tc, *d_ws, *d_xl, *d_out, *tl;
+  AtlasLine* d_lines;
+  unsigned long long* d_cnt;
+  int r;
+  const size_t nd = (size_t)nspec * kw;
+  const int64_t nn = std::max<int64_t>(n, 1);
+  if ((r = bufT(ctx, "al_ld", (size_t)nn * 4, &d_ld)) || (r = bufT(ctx, "al_iw", nwave + 1, &d_iw)) ||
+      (r = bufT(ctx, "al_xd", nd, &d_xd)) || (r = bufT(ctx, "al_dp", nd, &d_dp)) ||
+      (r = bufT(ctx, "al_xne", kw, &d_xne)) || (r = bufT(ctx, "al_tx", kw, &d_tx)) ||
+      (r = bufT(ctx, "al_hc", kw, &d_hc)) || (r = bufT(ctx, "al_tc", (size_t)(nwave + 1) * kw, &d_tc)) ||
+      (r = bufT(ctx, "al_ws", numnu, &d_ws)) || (r = bufT(ctx, "al_xl", (size_t)kw * numnu, &d_xl)) ||
+      (r = bufT(ctx, "al_out", (size_t)kw * numnu, &d_out)) || (r = bufT(ctx, "al_lines", nn, &d_lines)) ||
+      (r = bufT(ctx, "al_cnt", 2, &d_cnt)) || (r = ensure_tablog(ctx, &tl)))
+    return r;
+  if (n > 0) CK(cudaMemcpyAsync(d_ld, linedata, n * 4 * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_iw, iwavetab, (nwave + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_xd, xnfdop, nd * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_dp, dopple, nd * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_xne, xne, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_tx, txnxn, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_hc, hckt, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_tc, tabcont, (size_t)(nwave + 1) * kw * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_ws, waveset, numnu * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(d_xl, 0, (size_t)kw * numnu * sizeof(double), s));
+  CK(cudaMemsetAsync(d_cnt, 0, 2 * sizeof(unsigned long long), s));
+  if (n > 0) {
+    if ((r = atlas_prep_lines(ctx, d_ld, linedata, n, tl, d_ws, waveset, numnu, d_iw, nwave, nspec, d_lines))) return r;
+    LinopArgs a{d_lines, n, nrhox, kw, nspec, numnu, d_xd, d_dp, d_xne, d_tx, d_hc, d_tc, d_ws,
+                (const double*)ctx->bufs["tab_h0"].first, (const double*)ctx->bufs["tab_h1"].first,
+                (const double*)ctx->bufs["tab_h2"].first, d_xl, d_cnt, d_cnt + 1};
+    Timer tm(ctx, "atlas_linop");
+    k_atlas_linop<<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
+    CKL(ctx);
+  }
+  if ((r = transpose(ctx, d_xl, kw, numnu, d_out))) return r;
+  CK(cudaMemcpyAsync(xlines_out, d_out, (size_t)kw * numnu * sizeof(double), cudaMemcpyDeviceToHost, s));
+  unsigned long long cnt[2];
+  CK(cudaMemcpyAsync(cnt, d_cnt, sizeof cnt, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (lines_used) *lines_used = (int64_t)cnt[1];
+  return 0;
+}
+
+int atlasgpu_atlas_rt_pass(atlasgpu_ctx* ctx, int numnu, const double* waveset, const double* rcoset,
+                           const double* acont, const double* sigmac, const double* scont, int kw,
+                           const double* xlines, int nrhox, const double* rhox, const double* t,
+                           const double* hkt, double teff, atlasgpu_accum* out, double* hsurf_out) {
+  if (!ctx || !ctx->ops_set) return fail(ctx, ATLASGPU_ESTATE, "atlas_rt_pass: operators not set");
+  if (numnu < 1 || !waveset || !rcoset || !acont || !sigmac || kw < nrhox || kw > kKwMax || nrhox < 4 ||
+      !xlines || !rhox || !t || !hkt || !out)
+    return fail(ctx, ATLASGPU_EINVAL, "atlas_rt_pass: bad argument");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const size_t nt = (size_t)numnu * kw;
+  double *d_ws, *d_rc, *d_ac, *d_sg, *d_sc = nullptr, *d_xl0, *d_xl, *d_rx, *d_t, *d_hk, *d_hs, *d_sum;
+  int r;
+  if ((r = bufT(ctx, "rt_ws", numnu, &d_ws)) || (r = bufT(ctx, "rt_rc", numnu, &d_rc)) ||
+      (r = bufT(ctx, "rt_ac", nt, &d_ac)) || (r = bufT(ctx, "rt_sg", nt, &d_sg)) ||
+      (r = bufT(ctx, "rt_xl0", nt, &d_xl0)) || (r = bufT(ctx, "rt_xl", nt, &d_xl)) ||
+      (r = bufT(ctx, "rt_rx", kw, &d_rx)) || (r = bufT(ctx, "rt_t", kw, &d_t)) || (r = bufT(ctx, "rt_hk", kw, &d_hk)) ||
+      (r = bufT(ctx, "rt_hs", numnu, &d_hs)) || (r = bufT(ctx, "rt_sum", kAcc * kw + 1, &d_sum)))
+    return r;
+  if (scont && (r = bufT(ctx, "rt_sc", nt, &d_sc))) return r;
+  CK(cudaMemcpyAsync(d_ws, waveset, numnu * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_rc, rcoset, numnu * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_ac, acont, nt * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_sg, sigmac, nt * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (scont) CK(cudaMemcpyAsync(d_sc, scont, nt * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_xl0, xlines, nt * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_rx, rhox, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_t, t, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_hk, hkt, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  if ((r = transpose(ctx, d_xl0, numnu, kw, d_xl))) return r;
+  RtArgs a{ctx->ops, nullptr, numnu, nrhox, kw, d_ws, d_rc, d_ac, d_sg, d_sc, d_xl, d_rx, d_t, d_hk, teff,
+           1, nullptr, d_hs, nullptr};
+  if ((r = rt_launch(ctx, a, false, d_sum, nullptr))) return r;
+  std::vector<double> hsum(kAcc * kw + 1);
+  CK(cudaMemcpyAsync(hsum.data(), d_sum, hsum.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (hsurf_out) CK(cudaMemcpyAsync(hsurf_out, d_hs, numnu * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  double* dst[kAcc] = {out->rjmins, out->rdabh, out->rdiagj, out->flxrad, out->raden, out->h_total, out->accrad, out->abross};
+  for (int q = 0; q < kAcc; ++q)
+    if (dst[q]) memcpy(dst[q], hsum.data() + q * kw, nrhox * sizeof(double));
+  out->pradk0 = hsum[kAcc * kw];
+  return 0;
+}
+
+int atlasgpu_atlas_finish(atlasgpu_ctx* ctx, atlasgpu_finish_state* st, const atlasgpu_accum* acc,
+                          double* max_flxerr) {
+  if (!ctx || !st || !acc || st->nrhox < 8 || st->nrhox > kKwMax || !st->ross_t || !st->ross_p || !st->ross_k ||
+      st->ross_max < 1 || st->ross_n < 0 || st->ross_n > st->ross_max)
+    return fail(ctx, ATLASGPU_EINVAL, "atlas_finish: bad argument");
+  const int n = st->nrhox, kw = n;
+  double* hv[17] = {st->t, st->rhox, st->p, st->xne, st->abross, st->prad, st->vturb, st->pturb,
+                    st->tauros, st->accrad, st->raden, st->oldt1, st->flxerr, st->dtflux, st->dtlamb,
+                    st->dtsurf, st->t1};
+  for (int q = 0; q < 17; ++q)
+    if (!hv[q]) return fail(ctx, ATLASGPU_EINVAL, "atlas_finish: null array %d", q);
+  const double* ha[kAcc] = {acc->rjmins, acc->rdabh, acc->rdiagj, acc->flxrad, acc->raden, acc->h_total, acc->accrad, acc->abross};
+  for (int q = 0; q < kAcc; ++q)
+    if (!ha[q]) return fail(ctx, ATLASGPU_EINVAL, "atlas_finish: null accumulator %d", q);
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  double *d_arr, *d_acc, *d_work, *d_ross;
+  ModelState* d_ms;
+  RossStore* d_rs;
+  int r;
+  const size_t nr = (size_t)st->ross_max;
+  if ((r = bufT(ctx, "fin_arr", 17 * kw, &d_arr)) || (r = bufT(ctx, "fin_acc", kAcc * kw + 1, &d_acc)) ||
+      (r = bufT(ctx, "fin_work", 24 * kw, &d_work)) || (r = bufT(ctx, "fin_ross", 3 * nr, &d_ross)) ||
+      (r = bufT(ctx, "fin_ms", 1, &d_ms)) || (r = bufT(ctx, "fin_rs", 1, &d_rs)))
+    return r;
+  std::vector<double> h(17 * kw), ha2(kAcc * kw + 1);
+  for (int q = 0; q < 17; ++q) memcpy(h.data() + q * kw, hv[q], n * sizeof(double));
+  for (int q = 0; q < kAcc; ++q) memcpy(ha2.data() + q * kw, ha[q], n * sizeof(double));
+  ha2[kAcc * kw] = acc->pradk0;
+  ModelState ms;
+  double** f[17] = {&ms.t, &ms.rhox, &ms.p, &ms.xne, &ms.abross, &ms.prad, &ms.vturb, &ms.pturb, &ms.tauros,
+                    &ms.accrad, &ms.raden, &ms.oldt1, &ms.flxerr, &ms.dtflux, &ms.dtlamb, &ms.dtsurf, &ms.t1};
+  for (int q = 0; q < 17; ++q) *f[q] = d_arr + q * kw;
+  ms.pradk0 = st->pradk0;
+  ms.maxerr = 0;
+  CK(cudaMemcpyAsync(d_arr, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_acc, ha2.data(), ha2.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_ross, st->ross_t, nr * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_ross + nr, st->ross_p, nr * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_ross + 2 * nr, st->ross_k, nr * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_ms, &ms, sizeof ms, cudaMemcpyHostToDevice, s));
+  RossStore R{st->ross_n, st->ross_max, st->ross_zerot, st->ross_slopet, st->ross_zerop, st->ross_slopep,
+              d_ross, d_ross + nr, d_ross + 2 * nr};
+  CK(cudaMemcpyAsync(d_rs, &R, sizeof R, cudaMemcpyHostToDevice, s));
+  {
+    Timer tm(ctx, "atlas_finish");
+    k_finish_one<<<1, 32, 0, s>>>(d_ms, d_acc, kw, n, st->iter, st->teff, st->grav, d_rs, d_work);
+    CKL(ctx);
+  }
+  CK(cudaMemcpyAsync(h.data(), d_arr, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&ms, d_ms, sizeof ms, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&R, d_rs, sizeof R, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(st->ross_t, d_ross, nr * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(st->ross_p, d_ross + nr, nr * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(st->ross_k, d_ross + 2 * nr, nr * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  st->ross_n = R.n;
+  st->ross_zerot = R.zerot;
+  st->ross_slopet = R.slopet;
+  st->ross_zerop = R.zerop;
+  st->ross_slopep = R.slopep;
+  for (int q = 0; q < 17; ++q) memcpy(hv[q], h.data() + q * kw, n * sizeof(double));
+  st->pradk0 = ms.pradk0;
+  if (max_flxerr) *max_flxerr = ms.maxerr;
+  return 0;
+}
+
+}  // extern "C"

@@ -127,4 +127,9 @@ inline bool finite_all(const double* p, size_t n) {
   return true;
 }
 
+struct AtlasLine;
+int atlas_prep_lines(atlasgpu_ctx* ctx, const int32_t* d_ld, const int32_t* h_ld, int64_t n,
+                     const double* d_tablog, const double* d_ws, const double* h_ws, int numnu,
+                     const int32_t* d_iwt, int nwave, int nspec, AtlasLine* d_lines);
+
 }  // namespace atlasgpu

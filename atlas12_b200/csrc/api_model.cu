@@ -1,0 +1,424 @@
+// api_model.cu -- device-resident ATLAS12 model: the iteration loop of
+// atlas12c.f90:496-606 with every step on the device, one CUDA graph per
+// iteration.  The EOS / populations / continuum come from the synthetic
+// surrogate (surrogate.cuh) that stands in for the off-path physics.
+#include <cmath>
+#include <vector>
+
+#include "api_common.cuh"
+#include "atlas.cuh"
+#include "tcorr.cuh"
+
+using namespace atlasgpu;
+
+namespace {
+constexpr int kNState = 17;         // ModelState vectors
+constexpr int kRossMax = 80 * 60;   // ROSSTAB_MAXTAB = kw*60 with the reference's kw = 80
+}  // namespace
+
+struct atlasgpu_model {
+  int nrhox, kw, numnu, nwave, nspec;
+  int64_t nlines;
+  double teff, grav, vturb;
+  // device memory
+  double* state;         // [kNState][kw]
+  ModelState* ms;        // device struct pointing into state
+  double *xnfdop, *dopple;  // [nspec][kw]
+  double *xne_eos, *txnxn, *hkt, *hckt, *rho;  // [kw]
+  ContCoef* cc;          // [kw]
+  double *waveset, *rcoset, *cutwave, *tabcont;  // tabcont [nwave+1][kw]
+  int32_t* iwavetab;
+  int32_t* linedata;
+  AtlasLine* lines;
+  double* xl;            // [kw][numnu]
+  double *partial, *sum, *work, *hsurf;
+  double *h0, *h1, *h2, *ross;  // ross: ROSSTAB points [3][kRossMax]
+  RossStore* R;                  // device
+  int* iter_dev;         // iterations completed
+  double* maxerr_dev;    // last max |FLXERR|
+  unsigned long long* cnt;
+  int nwarp_rt, blocks_rt, nwl;
+  size_t smem_rt;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  bool kapcont_done = false;
+};
+
+namespace {
+
+// hydrostatics (iteration > 1), surrogate EOS / populations, Planck factors
+__global__ void k_model_eos(ModelState* ms, const int* iter_dev, int nrhox, int kw, double grav,
+                            double vturb_cms, double* xnfdop, double* dopple, double* xne_eos,
+                            double* txnxn, double* hkt, double* hckt, double* rho, ContCoef* cc) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nrhox) return;
+  const int iter = *iter_dev + 1;
+  const double t = ms->t[j];
+  double p = ms->p[j];
+  if (iter > 1) {
+    // P = GRAV*RHOX - PRAD - PTURB - PCON (atlas12c.f90:513-519), PCON = 0
+    p = grav * ms->rhox[j] - ms->prad[j] - ms->pturb[j] - 0.0;
+    if (p <= 0.0) p = fmax(grav * ms->rhox[j] * 1.0e-4, 1.0e-10);
+    ms->p[j] = p;
+  }
+  ContCoef c;
+  const EosOut e = surrogate_depth(t, p, vturb_cms, j, kw, xnfdop, dopple, &c);
+  cc[j] = c;
+  xne_eos[j] = e.xne;
+  ms->xne[j] = e.xne;
+  rho[j] = e.rho;
+  const double tk = kKbol * t;
+  hkt[j] = kHplanck / tk;
+  hckt[j] = hkt[j] * kClight;
+  // TXNXN = (XNF(H I) + 0.42 XNF(He I) + 0.85 XNF(H2)) (T/1e4)^0.3
+  txnxn[j] = (e.nh * (1.0 - e.xh) + 0.42 * 0.085 * e.nh) * pow(t / 10000.0, 0.3);
+}
+
+// KAPCONT (atlas12_modules.f90:19072-19138) on the surrogate continuum
+__global__ void k_model_kapcont(const double* cutwave, int nwave, const double* waveset, int nrhox,
+                                int kw, const double* hkt, const ContCoef* cc, double* tabcont) {
+  const int nu = blockIdx.x;  // 0..nwave-1
+  const double wave = cutwave[nu];
+  const double freq = kClightNms / wave;
+  for (int j = threadIdx.x; j < nrhox; j += blockDim.x) {
+    double acont = 1.0e10, sigmac = 0.0;
+    if (wave > waveset[0]) surrogate_kapp(cc[j], wave, acont, sigmac);
+    const double stim = 1.0 - exp(-freq * hkt[j]);
+    const double v = (acont + sigmac) * kLineCutoff / stim;
+    tabcont[(size_t)nu * kw + j] = v;
+    if (nu == nwave - 1) tabcont[(size_t)nwave * kw + j] = v;
+  }
+}
+
+__global__ void k_model_finish(ModelState* ms, double* acc, int kw, int n, int* iter_dev, double teff,
+                               double grav, RossStore* R, double* work, double* maxerr) {
+  if (blockIdx.x != 0) return;
+  const int lane = threadIdx.x & 31;
+  const int iter = *iter_dev + 1;
+  const double e = w_atlas_finish(*ms, acc, kw, n, iter, teff, grav, R, work, lane);
+  if (lane == 0) {
+    *maxerr = e;
+    *iter_dev = iter;
+  }
+}
+
+__global__ void k_surrogate_eval(int nrhox, const double* t, const double* p, double vturb_cms, int nw,
+                                 const double* wave, double* xnfdop, double* dopple, ContCoef* cc,
+                                 double* kabs, double* sigma, double* xne, double* rho) {
+  const int j = blockIdx.x;
+  if (j >= nrhox) return;
+  if (threadIdx.x == 0) {
+    const EosOut e = surrogate_depth(t[j], p[j], vturb_cms, j, nrhox, xnfdop, dopple, cc + j);
+    xne[j] = e.xne;
+    rho[j] = e.rho;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nw; i += blockDim.x) {
+    double ka, sg;
+    surrogate_kapp(cc[j], wave[i], ka, sg);
+    kabs[(size_t)i * nrhox + j] = ka;
+    sigma[(size_t)i * nrhox + j] = sg;
+  }
+}
+
+int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m) {
+  cudaStream_t s = ctx->stream;
+  k_model_eos<<<1, 128, 0, s>>>(m->ms, m->iter_dev, m->nrhox, m->kw, m->grav, m->vturb * 1.0e5,
+                                m->xnfdop, m->dopple, m->xne_eos, m->txnxn, m->hkt, m->hckt, m->rho, m->cc);
+  CKL(ctx);
+  if (!m->kapcont_done) {
+    k_model_kapcont<<<m->nwave, 128, 0, s>>>(m->cutwave, m->nwave, m->waveset, m->nrhox, m->kw, m->hkt,
+                                             m->cc, m->tabcont);
+    CKL(ctx);
+  }
+  CK(cudaMemsetAsync(m->xl, 0, (size_t)m->kw * m->numnu * sizeof(double), s));
+  if (m->nlines > 0) {
+    LinopArgs la{m->lines, m->nlines, m->nrhox, m->kw, m->nspec, m->numnu, m->xnfdop, m->dopple,
+                 m->xne_eos, m->txnxn, m->hckt, m->tabcont, m->waveset, m->h0, m->h1, m->h2, m->xl,
+                 nullptr, m->cnt};
+    k_atlas_linop<<<grid_for(ctx, m->nlines * 32, 256, 16), 256, 0, s>>>(la);
+    CKL(ctx);
+  }
+  RtArgs ra{ctx->ops, m->cc, m->numnu, m->nrhox, m->kw, m->waveset, m->rcoset, nullptr, nullptr, nullptr,
+            m->xl, (const double*)m->state + 1 * m->kw, (const double*)m->state + 0 * m->kw, m->hkt,
+            m->teff, 1, m->partial, m->hsurf, nullptr};
+  const int target = ctx->nsm * m->nwarp_rt * 6;
+  ra.nu_per_warp = std::max(1, (m->numnu + target - 1) / target);
+  k_atlas_rt<true><<<m->blocks_rt, 32 * m->nwarp_rt, m->smem_rt, s>>>(ra);
+  CKL(ctx);
+  k_atlas_reduce<<<(kAcc * m->kw + 1 + 127) / 128, 128, 0, s>>>(m->partial, m->nwl, m->kw, 0, m->sum);
+  CKL(ctx);
+  k_model_finish<<<1, 32, 0, s>>>(m->ms, m->sum, m->kw, m->nrhox, m->iter_dev, m->teff, m->grav, m->R,
+                                  m->work, m->maxerr_dev);
+  CKL(ctx);
+  return 0;
+}
+
+template <class T>
+int dalloc(atlasgpu_ctx* ctx, T** p, size_t n) {
+  if (cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, ATLASGPU_ENOMEM, "model: cudaMalloc of %zu bytes", n * sizeof(T));
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int atlasgpu_surrogate_eval(atlasgpu_ctx* ctx, int nrhox, const double* t, const double* p, double vturb_kms,
+                            int nw, const double* wave, double* kabs, double* sigma, double* xne,
+                            double* xnfdop) {
+  if (!ctx || nrhox < 1 || nrhox > kKwMax || nw < 1 || !t || !p || !wave || !kabs || !sigma || !xne)
+    return fail(ctx, ATLASGPU_EINVAL, "surrogate_eval: bad argument");
+  cudaSetDevice(ctx->device);
+  double *dt, *dp, *dw, *dxd, *ddp, *dka, *dsg, *dxne, *drho;
+  ContCoef* dcc;
+  int r;
+  const size_t ns = (size_t)kSurrNspec * nrhox;
+  if ((r = bufT(ctx, "se_t", nrhox, &dt)) || (r = bufT(ctx, "se_p", nrhox, &dp)) || (r = bufT(ctx, "se_w", nw, &dw)) ||
+      (r = bufT(ctx, "se_xd", ns, &dxd)) || (r = bufT(ctx, "se_dp", ns, &ddp)) ||
+      (r = bufT(ctx, "se_ka", (size_t)nw * nrhox, &dka)) || (r = bufT(ctx, "se_sg", (size_t)nw * nrhox, &dsg)) ||
+      (r = bufT(ctx, "se_xne", nrhox, &dxne)) || (r = bufT(ctx, "se_rho", nrhox, &drho)) ||
+      (r = bufT(ctx, "se_cc", nrhox, &dcc)))
+    return r;
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(dt, t, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dp, p, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dw, wave, nw * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(dxd, 0, ns * sizeof(double), s));
+  k_surrogate_eval<<<nrhox, 128, 0, s>>>(nrhox, dt, dp, vturb_kms * 1.0e5, nw, dw, dxd, ddp, dcc, dka, dsg, dxne, drho);
+  CKL(ctx);
+  CK(cudaMemcpyAsync(kabs, dka, (size_t)nw * nrhox * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(sigma, dsg, (size_t)nw * nrhox * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(xne, dxne, nrhox * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (xnfdop) CK(cudaMemcpyAsync(xnfdop, dxd, ns * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlasgpu_model** out) {
+  if (!ctx || !d || !out) return fail(ctx, ATLASGPU_EINVAL, "model_create: null argument");
+  *out = nullptr;
+  if (!ctx->ops_set) return fail(ctx, ATLASGPU_ESTATE, "model_create: operators not set");
+  if (d->nrhox < 16 || d->nrhox > kKwMax || d->numnu < 2 || d->nwave < 1 || d->nlines < 0 || !d->t || !d->p ||
+      !d->rhox || !d->tauros || !d->waveset || !d->rcoset || !d->cutoff_wave || (d->nlines > 0 && !d->linedata) ||
+      !d->h0tab || !d->h1tab || !d->h2tab || !(d->teff > 0) || !(d->vturb_kms >= 0))
+    return fail(ctx, ATLASGPU_EINVAL, "model_create: bad descriptor");
+  for (int i = 1; i < d->numnu; ++i)
+    if (!(d->waveset[i] > d->waveset[i - 1])) return fail(ctx, ATLASGPU_EINVAL, "WAVESET not increasing");
+  for (int i = 1; i < d->nwave; ++i)
+    if (!(d->cutoff_wave[i] > d->cutoff_wave[i - 1])) return fail(ctx, ATLASGPU_EINVAL, "cutoff grid not increasing");
+  cudaSetDevice(ctx->device);
+  atlasgpu_model* m = new atlasgpu_model();
+  m->nrhox = d->nrhox;
+  m->kw = d->nrhox;
+  m->numnu = d->numnu;
+  m->nwave = d->nwave;
+  m->nspec = kSurrNspec;
+  m->nlines = d->nlines;
+  m->teff = d->teff;
+  m->grav = pow(10.0, d->logg);
+  m->vturb = d->vturb_kms;
+  const int kw = m->kw;
+  int r = 0;
+  const size_t nr = (size_t)3 * kRossMax;
+  if ((r = dalloc(ctx, &m->state, kNState * kw)) || (r = dalloc(ctx, &m->ms, 1)) ||
+      (r = dalloc(ctx, &m->xnfdop, (size_t)m->nspec * kw)) || (r = dalloc(ctx, &m->dopple, (size_t)m->nspec * kw)) ||
+      (r = dalloc(ctx, &m->xne_eos, kw)) || (r = dalloc(ctx, &m->txnxn, kw)) || (r = dalloc(ctx, &m->hkt, kw)) ||
+      (r = dalloc(ctx, &m->hckt, kw)) || (r = dalloc(ctx, &m->rho, kw)) || (r = dalloc(ctx, &m->cc, kw)) ||
+      (r = dalloc(ctx, &m->waveset, m->numnu)) || (r = dalloc(ctx, &m->rcoset, m->numnu)) ||
+      (r = dalloc(ctx, &m->cutwave, m->nwave)) || (r = dalloc(ctx, &m->tabcont, (size_t)(m->nwave + 1) * kw)) ||
+      (r = dalloc(ctx, &m->iwavetab, m->nwave + 1)) || (r = dalloc(ctx, &m->linedata, (size_t)m->nlines * 4)) ||
+      (r = dalloc(ctx, &m->lines, (size_t)m->nlines)) || (r = dalloc(ctx, &m->xl, (size_t)kw * m->numnu)) ||
+      (r = dalloc(ctx, &m->sum, kAcc * kw + 1)) || (r = dalloc(ctx, &m->work, 24 * kw)) ||
+      (r = dalloc(ctx, &m->hsurf, m->numnu)) || (r = dalloc(ctx, &m->h0, 2001)) || (r = dalloc(ctx, &m->h1, 2001)) ||
+      (r = dalloc(ctx, &m->h2, 2001)) || (r = dalloc(ctx, &m->ross, nr)) || (r = dalloc(ctx, &m->R, 1)) || (r = dalloc(ctx, &m->iter_dev, 1)) ||
+      (r = dalloc(ctx, &m->maxerr_dev, 1)) || (r = dalloc(ctx, &m->cnt, 2))) {
+    atlasgpu_model_destroy(ctx, m);
+    return r;
+  }
+  // RT launch shape
+  m->nwarp_rt = 4;
+  while (m->nwarp_rt > 1 && sizeof(double) * kKwMax + m->nwarp_rt * sizeof(RtWS) > ctx->smem_optin) --m->nwarp_rt;
+  m->smem_rt = sizeof(double) * kKwMax + m->nwarp_rt * sizeof(RtWS);
+  const int target = ctx->nsm * m->nwarp_rt * 6;
+  const int npw = std::max(1, (m->numnu + target - 1) / target);
+  const int nw = (m->numnu + npw - 1) / npw;
+  m->blocks_rt = (nw + m->nwarp_rt - 1) / m->nwarp_rt;
+  m->nwl = m->blocks_rt * m->nwarp_rt;
+  if ((r = dalloc(ctx, &m->partial, (size_t)m->nwl * (kAcc * kw + 1)))) {
+    atlasgpu_model_destroy(ctx, m);
+    return r;
+  }
+  CK(cudaFuncSetAttribute(k_atlas_rt<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->smem_rt));
+  cudaStream_t s = ctx->stream;
+  // state vectors: t, rhox, p, xne, abross, prad, vturb, pturb, tauros, accrad, raden, oldt1, flxerr,
+  // dtflux, dtlamb, dtsurf, t1
+  std::vector<double> h(kNState * kw, 0.0);
+  for (int j = 0; j < kw; ++j) {
+    h[0 * kw + j] = d->t[j];
+    h[1 * kw + j] = d->rhox[j];
+    h[2 * kw + j] = d->p[j];
+    h[6 * kw + j] = d->vturb_kms * 1.0e5;
+    h[8 * kw + j] = d->tauros[j];
+  }
+  ModelState ms;
+  double** f[kNState] = {&ms.t, &ms.rhox, &ms.p, &ms.xne, &ms.abross, &ms.prad, &ms.vturb, &ms.pturb, &ms.tauros,
+                         &ms.accrad, &ms.raden, &ms.oldt1, &ms.flxerr, &ms.dtflux, &ms.dtlamb, &ms.dtsurf, &ms.t1};
+  for (int q = 0; q < kNState; ++q) *f[q] = m->state + q * kw;
+  ms.pradk0 = 0.0;
+  ms.maxerr = 0.0;
+  CK(cudaMemcpyAsync(m->state, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(m->ms, &ms, sizeof ms, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(m->xnfdop, 0, (size_t)m->nspec * kw * sizeof(double), s));
+  // dopple must be nonzero where a line may look: fill with 1 (the populations are 0 there)
+  {
+    std::vector<double> one((size_t)m->nspec * kw, 1.0);
+    CK(cudaMemcpy(m->dopple, one.data(), one.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpyAsync(m->waveset, d->waveset, m->numnu * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(m->rcoset, d->rcoset, m->numnu * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(m->cutwave, d->cutoff_wave, m->nwave * sizeof(double), cudaMemcpyHostToDevice, s));
+  std::vector<int32_t> iwt(m->nwave + 1);
+  const double RATIOLG = log(1.0 + 1.0 / 2000000.0);
+  for (int i = 0; i < m->nwave; ++i) iwt[i] = (int32_t)(log(d->cutoff_wave[i]) / RATIOLG + 0.5);
+  iwt[m->nwave] = 1 << 30;
+  CK(cudaMemcpyAsync(m->iwavetab, iwt.data(), iwt.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  if (m->nlines > 0)
+    CK(cudaMemcpyAsync(m->linedata, d->linedata, (size_t)m->nlines * 4 * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(m->h0, d->h0tab, 2001 * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(m->h1, d->h1tab, 2001 * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(m->h2, d->h2tab, 2001 * sizeof(double), cudaMemcpyHostToDevice, s));
+  {
+    RossStore R0{0, kRossMax, 0.0, 1.0, 0.0, 1.0, m->ross, m->ross + kRossMax, m->ross + 2 * kRossMax};
+    CK(cudaMemcpy(m->R, &R0, sizeof R0, cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemsetAsync(m->iter_dev, 0, sizeof(int), s));
+  CK(cudaMemsetAsync(m->cnt, 0, 2 * sizeof(unsigned long long), s));
+  // TABLOG and the per-line preparation (iteration invariant)
+  double* tl;
+  {
+    const bool fresh = ctx->bufs.find("tablog") == ctx->bufs.end();
+    if ((r = bufT(ctx, "tablog", 65536, &tl))) {
+      atlasgpu_model_destroy(ctx, m);
+      return r;
+    }
+    if (fresh) {
+      std::vector<double> ht(65536);
+      for (int k = 0; k < 65536; ++k) ht[k] = pow(10.0, (double)((k - 32768) - 16384) * 0.001);
+      CK(cudaMemcpy(tl, ht.data(), 65536 * sizeof(double), cudaMemcpyHostToDevice));
+    }
+  }
+  if (m->nlines > 0 && (r = atlas_prep_lines(ctx, m->linedata, d->linedata, m->nlines, tl, m->waveset, d->waveset,
+                                              m->numnu, m->iwavetab, m->nwave, m->nspec, m->lines))) {
+    atlasgpu_model_destroy(ctx, m);
+    return r;
+  }
+  CK(cudaStreamSynchronize(s));
+  *out = m;
+  return 0;
+}
+
+int atlasgpu_model_iterate(atlasgpu_ctx* ctx, atlasgpu_model* m, int max_iter, double tol, int use_graph,
+                           int* iters_done, double* hist) {
+  if (!ctx || !m || max_iter < 0) return fail(ctx, ATLASGPU_EINVAL, "model_iterate: bad argument");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  int done = 0, r;
+  Timer tm(ctx, "model_iterate");
+  for (int it = 0; it < max_iter; ++it) {
+    if (!m->kapcont_done) {
+      // first iteration of the model: KAPCONT included, not captured
+      if ((r = enqueue_iteration(ctx, m))) return r;
+      m->kapcont_done = true;
+    } else if (use_graph) {
+      if (!m->gexec) {
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const int64_t l0 = ctx->launches;
+        r = enqueue_iteration(ctx, m);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(s, &g);
+        if (r) return r;
+        if (ec != cudaSuccess) return fail(ctx, ATLASGPU_ECUDA, "graph capture: %s", cudaGetErrorString(ec));
+        m->graph = g;
+        CK(cudaGraphInstantiate(&m->gexec, g, 0));
+        ctx->launches = l0;  // counted when replayed
+      }
+      CK(cudaGraphLaunch(m->gexec, s));
+      ctx->launches += 5;
+    } else {
+      if ((r = enqueue_iteration(ctx, m))) return r;
+    }
+    double e = 0.0;
+    CK(cudaMemcpyAsync(&e, m->maxerr_dev, sizeof e, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (hist) hist[it] = e;
+    ++done;
+    if (!(e == e)) return fail(ctx, ATLASGPU_ENONFINITE, "model_iterate: FLXERR is not finite at iteration %d", done);
+    if (tol > 0.0 && e <= tol) break;
+  }
+  tm.stop();
+  if (iters_done) *iters_done = done;
+  return 0;
+}
+
+int atlasgpu_model_get(atlasgpu_ctx* ctx, atlasgpu_model* m, double* t, double* rhox, double* p, double* xne,
+                       double* flxerr, double* hsurf) {
+  if (!ctx || !m) return fail(ctx, ATLASGPU_EINVAL, "model_get: null");
+  cudaSetDevice(ctx->device);
+  const int kw = m->kw;
+  std::vector<double> h(kNState * kw);
+  CK(cudaMemcpyAsync(h.data(), m->state, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (hsurf) CK(cudaMemcpyAsync(hsurf, m->hsurf, m->numnu * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (t) memcpy(t, h.data() + 0 * kw, m->nrhox * sizeof(double));
+  if (rhox) memcpy(rhox, h.data() + 1 * kw, m->nrhox * sizeof(double));
+  if (p) memcpy(p, h.data() + 2 * kw, m->nrhox * sizeof(double));
+  if (xne) memcpy(xne, h.data() + 3 * kw, m->nrhox * sizeof(double));
+  if (flxerr) memcpy(flxerr, h.data() + 12 * kw, m->nrhox * sizeof(double));
+  return 0;
+}
+
+int atlasgpu_model_set_structure(atlasgpu_ctx* ctx, atlasgpu_model* m, const double* t, const double* p,
+                                 const double* rhox) {
+  if (!ctx || !m || !t || !p || !rhox) return fail(ctx, ATLASGPU_EINVAL, "model_set_structure: null");
+  cudaSetDevice(ctx->device);
+  const int kw = m->kw;
+  std::vector<double> h(kNState * kw);
+  CK(cudaMemcpy(h.data(), m->state, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int j = 0; j < m->nrhox; ++j) {
+    h[0 * kw + j] = t[j];
+    h[1 * kw + j] = rhox[j];
+    h[2 * kw + j] = p[j];
+    h[5 * kw + j] = 0.0;   // PRAD
+    h[11 * kw + j] = 0.0;  // OLDT1
+    h[8 * kw + j] = pow(10.0, -6.875 + 0.125 * j);
+  }
+  CK(cudaMemcpy(m->state, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemset(m->iter_dev, 0, sizeof(int)));
+  RossStore R0{0, kRossMax, 0.0, 1.0, 0.0, 1.0, m->ross, m->ross + kRossMax, m->ross + 2 * kRossMax};
+  CK(cudaMemcpy(m->R, &R0, sizeof R0, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int atlasgpu_model_destroy(atlasgpu_ctx* ctx, atlasgpu_model* m) {
+  if (!m) return ATLASGPU_EINVAL;
+  if (ctx) {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+  }
+  if (m->gexec) cudaGraphExecDestroy(m->gexec);
+  if (m->graph) cudaGraphDestroy(m->graph);
+  void* ps[] = {m->state, m->ms, m->xnfdop, m->dopple, m->xne_eos, m->txnxn, m->hkt, m->hckt, m->rho, m->cc,
+                m->waveset, m->rcoset, m->cutwave, m->tabcont, m->iwavetab, m->linedata, m->lines, m->xl,
+                m->partial, m->sum, m->work, m->hsurf, m->h0, m->h1, m->h2, m->ross, m->R, m->iter_dev,
+                m->maxerr_dev, m->cnt};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  delete m;
+  return ATLASGPU_OK;
+}
+
+}  // extern "C"

@@ -30,7 +30,7 @@ struct FarLine {
 };
 
 // ---------------------------------------------------------------- binning
-__global__ void k_bin(const double* __restrict__ wl, int64_t n, double ratiolg, int ixwlbeg,
+static __global__ void k_bin(const double* __restrict__ wl, int64_t n, double ratiolg, int ixwlbeg,
                       int32_t* __restrict__ nbuff, int64_t* __restrict__ flagged,
                       unsigned long long* __restrict__ nflag, int64_t flag_cap) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -47,7 +47,7 @@ __global__ void k_bin(const double* __restrict__ wl, int64_t n, double ratiolg, 
 }
 
 // ---------------------------------------------------------------- continuum
-__global__ void k_continuum(const double* __restrict__ wledge, int nedge,
+static __global__ void k_continuum(const double* __restrict__ wledge, int nedge,
                             const double* __restrict__ continall, int stride, int nrhox,
                             double wbegin, double ratio, int length, float* __restrict__ out) {
   const int j = blockIdx.y;
@@ -91,7 +91,7 @@ struct CoreArgs {
 };
 
 template <int G>
-__global__ void __launch_bounds__(256) k_core(CoreArgs a) {
+static __global__ void __launch_bounds__(256) k_core(CoreArgs a) {
   const int lane = threadIdx.x & 31;
   const int g = lane % G;                 // lane within the group
   const int gbase = lane - g;             // first lane of the group
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(256) k_core(CoreArgs a) {
 }
 
 // per depth: tile counts from the difference array, exclusive offsets
-__global__ void k_far_scan(int* __restrict__ tdiff, int ntiles, int64_t* __restrict__ off,
+static __global__ void k_far_scan(int* __restrict__ tdiff, int ntiles, int64_t* __restrict__ off,
                            int64_t* __restrict__ fillptr, int64_t* __restrict__ total) {
   // one block per depth; sequential over tiles in chunks (ntiles is small)
   const int jj = blockIdx.x;
@@ -203,7 +203,7 @@ __global__ void k_far_scan(int* __restrict__ tdiff, int ntiles, int64_t* __restr
   total[jj] = run;
 }
 
-__global__ void k_far_fill(const FarLine* __restrict__ far, const unsigned* __restrict__ nfar,
+static __global__ void k_far_fill(const FarLine* __restrict__ far, const unsigned* __restrict__ nfar,
                            int64_t nlines, int length, const int64_t* __restrict__ base,
                            int64_t* __restrict__ fillptr, int ntiles, int* __restrict__ csr) {
   const int jj = blockIdx.y;
@@ -224,7 +224,7 @@ __global__ void k_far_fill(const FarLine* __restrict__ far, const unsigned* __re
 
 // far-wing gather + core accumulator -> REAL(4) opacity; zeroes acc for reuse
 template <bool kMixed>
-__global__ void __launch_bounds__(kFarThreads) k_farwing(const FarLine* __restrict__ far,
+static __global__ void __launch_bounds__(kFarThreads) k_farwing(const FarLine* __restrict__ far,
                                                          int64_t nlines,
                                                          const int64_t* __restrict__ off,
                                                          const int64_t* __restrict__ base,
@@ -292,7 +292,7 @@ struct SpecWS {
       bnu[kKwMax];
 };
 
-__global__ void __launch_bounds__(128) k_spectrum(SpecArgs a) {
+static __global__ void __launch_bounds__(128) k_spectrum(SpecArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int nwarp = blockDim.x >> 5;

@@ -15,7 +15,7 @@
 
 namespace atlasgpu {
 
-__constant__ double kWeiA[32] = {
+static __constant__ double kWeiA[32] = {
     -1.30317978630500875e-12, 3.74088129316536249e-12, 8.03036789996388945e-12,
     -2.15436320778387687e-11, -5.54423594816646238e-11, 1.16582510935237737e-10,
     4.15374309183345315e-10, -5.23102048119632885e-10, -3.20801509172336887e-09,

@@ -11,7 +11,8 @@ in for them with a small, smooth, physically-shaped model:
   partition functions; molecules from a Guldberg-Waage-like T scaling;
 * electron density: hydrogen + metal ionisation (Saha), ideal gas;
 * continuum absorption: H- bound-free and free-free, H I bound-free from
-  n = 1, 2, 3 (Lyman, Balmer, Paschen edges), all with simple analytic
+  n = 1, 2, 3 (Lyman, Balmer, Paschen edges), metal bound-free from the
+  neutral ground states (edges at 1239.84/chi nm), all with simple analytic
   cross-section shapes; scattering: Thomson + H I Rayleigh;
 * Rosseland mean: tabulated from the same continuum on a (log T, log P) grid.
 
@@ -59,6 +60,7 @@ MOLECULES = np.array([
     (45, 63.87, -9.0, 14.0),  # TiO
 ])
 MW6 = 139 * 6  # SYNTHE's flattened species axis (mw*6)
+MBF_SIGMA = 2.0e-17  # metal ground-state photo-ionisation cross-section at the edge (cm^2)
 
 
 def nelion(z, ion_stage):
@@ -162,10 +164,17 @@ def continuum_opacity(wave_nm, t, p, e=None):
         pop = nh1 * 2.0 * n * n * np.exp(-13.598 * (1.0 - 1.0 / (n * n)) * EV_ERG / (KBOL * t)) / 2.0
         sig = np.where(w <= edge, 7.9e-18 / n ** 5 * (w / edge) ** 3 * n ** 3 / 1.0, 0.0)
         kh = kh + pop * sig
+    # metal bound-free from the neutral ground states, edges at 1239.84/chi nm
+    kmet = np.zeros(np.broadcast(w, t).shape)
+    for z, m, chi, leps, u1, u2 in METALS:
+        r = _saha(t[0], e["xne"], chi, u1, u2)[None, :]
+        n1 = nh * 10.0 ** (leps - 12.0) / (1.0 + r)
+        edge = 1239.84198 / chi
+        kmet = kmet + np.where(w <= edge, n1 * MBF_SIGMA * (w / edge) ** 3, 0.0)
     # Thomson + Rayleigh(H I)
     sray = 5.8e-24 * (121.6 / np.maximum(w, 125.0)) ** 4 * nh1
     sigma = (6.6524587051e-25 * ne + sray) / rho
-    kabs = (khm + kff + kh) / rho + 1e-12
+    kabs = (khm + kff + kh + kmet) / rho + 1e-12
     return kabs, sigma
 
 
@@ -180,7 +189,7 @@ class RossTable:
     """log kappa_Ross on a (log T, log P) grid from the surrogate continuum
     (the ROSSTAB analogue consumed by TTAUP)."""
 
-    def __init__(self, lt0=np.log10(1500.0), lt1=np.log10(60000.0), lp0=-4.0, lp1=10.0, nt=96, np_=112):
+    def __init__(self, lt0=np.log10(1000.0), lt1=np.log10(60000.0), lp0=-4.0, lp1=10.0, nt=104, np_=112):
         self.lt = np.linspace(lt0, lt1, nt)
         self.lp = np.linspace(lp0, lp1, np_)
         wave = np.geomspace(9.0, 160000.0, 2400)

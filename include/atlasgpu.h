@@ -152,6 +152,107 @@ int atlasgpu_synthe_spectrum_dev(atlasgpu_ctx *ctx, const double *d_wledge, int 
                                  const double *d_hkt, double wbegin, double ratio, int length,
                                  const float *d_opacity, double *d_flux, double *d_cont);
 
+
+/* ---- ATLAS12 ---------------------------------------------------------- */
+/* Voigt tables of TABVOIGT(200, 2001) (atlas12_modules.f90:19796-19851), as
+ * the driver computes them at start-up (atlas12c.f90:236).  n = 2001.  Also
+ * builds TABLOG (:2083-2086) on the host with the C library pow. */
+int atlasgpu_atlas_set_voigt_tables(atlasgpu_ctx *ctx, const double *h0tab, const double *h1tab,
+                                    const double *h2tab, int n);
+
+/* LINOP1 (atlas12_modules.f90:18132-18374): line opacity XLINES(J,NU) from
+ * the stored LINEDATA records.
+ *   linedata [n][4] int32 (LINEREC, :1950-1977)
+ *   xnfdop, dopple [nspec][kw] (XNFDOP(J,NELION), DOPPLE(J,NELION))
+ *   xne, txnxn, hckt [nrhox]; tabcont [nwave+1][kw]; iwavetab [nwave+1]
+ *   waveset [numnu]; xlines_out [numnu][kw]
+ * lines_used (may be NULL) receives LINEUSED (lines above TABCONT at some
+ * coarse depth).  Lines redward of WAVESET(NUMNU-1) take NU = NUMNU (the
+ * reference's walk runs past the grid there). */
+int atlasgpu_atlas_linop(atlasgpu_ctx *ctx, const int32_t *linedata, int64_t n, int nrhox, int kw,
+                         const double *xnfdop, const double *dopple, int nspec, const double *xne,
+                         const double *txnxn, const double *hckt, const double *tabcont,
+                         const int32_t *iwavetab, int nwave, const double *waveset, int numnu,
+                         double *xlines_out, int64_t *lines_used);
+
+/* RUN_RT_PASS frequency loop (atlas12_modules.f90:3880-3951): per NU the
+ * Planck terms, ALINE = XLINES*STIM, JOSH(1,0) (:18398-18776), the negative
+ * floor and the TCORR/RADIAP/ROSS mode-2 sums.  acont/sigmac [numnu][kw]
+ * from KAPP, scont [numnu][kw] or NULL for SCONT = BNU; xlines [numnu][kw].
+ * out: sums over all frequencies (zeroed by the call, i.e. mode 1 included);
+ * hsurf_out [numnu] = HNU(1) per frequency (the .flux record). */
+int atlasgpu_atlas_rt_pass(atlasgpu_ctx *ctx, int numnu, const double *waveset, const double *rcoset,
+                           const double *acont, const double *sigmac, const double *scont, int kw,
+                           const double *xlines, int nrhox, const double *rhox, const double *t,
+                           const double *hkt, double teff, atlasgpu_accum *out, double *hsurf_out);
+
+/* Model arrays for the end of an iteration, [nrhox] each, updated in place. */
+typedef struct {
+  int nrhox, iter;
+  double teff, grav, pradk0;
+  double *t, *rhox, *p, *xne, *abross, *prad, *vturb, *pturb, *tauros, *accrad, *raden, *oldt1;
+  double *flxerr, *dtflux, *dtlamb, *dtsurf, *t1; /* outputs: the .iter columns */
+  /* ROSSTAB store (atlas12_modules.f90:5937-6228), in/out: ross_n points of
+   * normalised (log T, log P, log10 kappa_R) in ross_t/p/k [ross_max], with
+   * the normalisation fixed by the first store (ross_n = 0 on iteration 1) */
+  int ross_n, ross_max;
+  double ross_zerot, ross_slopet, ross_zerop, ross_slopep;
+  double *ross_t, *ross_p, *ross_k;
+} atlasgpu_finish_state;
+
+/* ROSS(3), the ROSSTAB store, RADIAP(3) and TCORR(3) (atlas12_modules.f90:
+ * 5193-5198, 5937-6228, 5108-5135, 2528-2977) with TTAUP (:6303-6523),
+ * radiative branch, on the device.  acc = the mode-2 sums from atlasgpu_atlas_rt_pass.  max_flxerr
+ * receives max |FLXERR| in percent (the convergence metric). */
+int atlasgpu_atlas_finish(atlasgpu_ctx *ctx, atlasgpu_finish_state *s, const atlasgpu_accum *acc,
+                          double *max_flxerr);
+
+/* ---- device-resident ATLAS12 model ----------------------------------
+ * One atmosphere kept on the device for the whole iteration (atlas12c.f90
+ * :496-606): hydrostatics, populations and continuum from the documented
+ * synthetic surrogate (they stand in for the off-path EOS and KAPP),
+ * KAPCONT once, then per iteration LINOP1, the RT pass, the reduction and
+ * the finish, as one captured CUDA graph. */
+typedef struct atlasgpu_model atlasgpu_model;
+typedef struct {
+  double teff, logg, vturb_kms;
+  int nrhox;                               /* <= 100 */
+  const double *t, *p, *rhox, *tauros;     /* starting model [nrhox] */
+  const double *waveset, *rcoset;          /* [numnu] */
+  int numnu;
+  const double *cutoff_wave;               /* KAPCONT grid [nwave] (nm) */
+  int nwave;
+  const int32_t *linedata;                 /* [nlines][4] */
+  int64_t nlines;
+  const double *h0tab, *h1tab, *h2tab;     /* TABVOIGT tables, 2001 */
+} atlasgpu_model_desc;
+
+int atlasgpu_model_create(atlasgpu_ctx *ctx, const atlasgpu_model_desc *desc, atlasgpu_model **out);
+/* Run up to max_iter iterations; stop after the first whose max |FLXERR| <=
+ * tol_percent (tol <= 0: run all).  iters_done and maxerr_hist[max_iter]
+ * (may be NULL) receive the count and the per-iteration metric.
+ * use_graph != 0 replays one captured graph per iteration. */
+int atlasgpu_model_iterate(atlasgpu_ctx *ctx, atlasgpu_model *m, int max_iter, double tol_percent,
+                           int use_graph, int *iters_done, double *maxerr_hist);
+/* Copy the current structure (each [nrhox], any may be NULL) and the last
+ * iteration's HNU(1) per frequency ([numnu], may be NULL). */
+int atlasgpu_model_get(atlasgpu_ctx *ctx, atlasgpu_model *m, double *t, double *rhox, double *p,
+                       double *xne, double *flxerr, double *hsurf);
+/* Overwrite the structure (T, P, RHOX [nrhox]) and restart the iteration
+ * count (a warm start). */
+int atlasgpu_model_set_structure(atlasgpu_ctx *ctx, atlasgpu_model *m, const double *t,
+                                 const double *p, const double *rhox);
+int atlasgpu_model_destroy(atlasgpu_ctx *ctx, atlasgpu_model *m);
+
+/* The surrogate physics on the device for given T, P [nrhox]: continuum
+ * absorption and scattering kabs, sigma [nw][nrhox] at wave [nw] (nm),
+ * electron density xne [nrhox] and XNFDOP [270][nrhox] (may be NULL).  No
+ * reference counterpart: it exposes the stand-in for KAPP / the EOS that the
+ * device-resident model uses, so that it can be checked. */
+int atlasgpu_surrogate_eval(atlasgpu_ctx *ctx, int nrhox, const double *t, const double *p,
+                            double vturb_kms, int nw, const double *wave, double *kabs, double *sigma,
+                            double *xne, double *xnfdop);
+
 #ifdef __cplusplus
 }
 #endif

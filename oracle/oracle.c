@@ -1026,3 +1026,288 @@ void orc_atlas_rt_pass(const orc_ops_t *ops, int numnu, const double *waveset,
     }
   }
 }
+
+/* ======================================================================
+ * ROSS(3) :5193-5198, RADIAP(3) :5108-5135, TCORR(3) :2528-2977 (radiative
+ * branch), TTAUP :6303-6523, with ROSSTAB a caller table.
+ * ==================================================================== */
+static const double SIGMA_SB = 5.670374419e-5;
+
+/* ROSSTAB(0,0,0): append the current (T, P, ABROSS) profile */
+void orc_rosstab_store(orc_tcorr_t *s) {
+  int n = s->nrhox;
+  if (s->nross == 0) {
+    s->zerot = log10(s->t[0]);
+    s->zerop = log10(s->p[0]);
+    s->slopet = log10(s->t[n - 1]) - s->zerot;
+    s->slopep = log10(s->p[n - 1]) - s->zerop;
+  }
+  for (int j = 0; j < n; ++j) {
+    s->nross = s->nross + 1;
+    if (s->nross > s->maxtab) {
+      s->nross = s->maxtab;
+      break;
+    }
+    int k = s->nross - 1;
+    s->tabt[k] = (log10(s->t[j]) - s->zerot) / s->slopet;
+    s->tabp[k] = (log10(s->p[j]) - s->zerop) / s->slopep;
+    s->tabk[k] = log10(s->abross[j]);
+  }
+}
+
+/* ROSSTAB(T, P, V) lookup, IROSSTAB = 1: nearest stored point in each of the
+ * four (T, P) quadrants, bilinear when all four exist, else inverse distance */
+double orc_rosstab(const orc_tcorr_t *s, double temp, double pres) {
+  double tl = (log10(temp) - s->zerot) / s->slopet;
+  double pl = (log10(pres) - s->zerop) / s->slopep;
+  double rpp = 1e30, rpm = 1e30, rmp = 1e30, rmm = 1e30;
+  int ipp = 0, ipm = 0, imp = 0, imm = 0;
+  for (int i = 1; i <= s->nross; ++i) {
+    double dt = s->tabt[i - 1] - tl, dp = s->tabp[i - 1] - pl;
+    double r2 = orc_powi(dt, 2) + orc_powi(dp, 2);
+    if (dt >= 0.0) {
+      if (dp >= 0.0) {
+        if (r2 < rpp) { rpp = r2; ipp = i; }
+      } else {
+        if (r2 < rpm) { rpm = r2; ipm = i; }
+      }
+    } else {
+      if (dp >= 0.0) {
+        if (r2 < rmp) { rmp = r2; imp = i; }
+      } else {
+        if (r2 < rmm) { rmm = r2; imm = i; }
+      }
+    }
+  }
+  double R;
+  if (ipp && ipm && imp && imm) {
+    double Tpp = s->tabt[ipp - 1], Ppp = s->tabp[ipp - 1], Rpp = s->tabk[ipp - 1];
+    double Tpm = s->tabt[ipm - 1], Ppm = s->tabp[ipm - 1], Rpm = s->tabk[ipm - 1];
+    double Tmp = s->tabt[imp - 1], Pmp = s->tabp[imp - 1], Rmp = s->tabk[imp - 1];
+    double Tmm = s->tabt[imm - 1], Pmm = s->tabp[imm - 1], Rmm = s->tabk[imm - 1];
+    double rhi = ((tl - Tmp) * Rpp + (Tpp - tl) * Rmp) / (Tpp - Tmp);
+    double phi = ((tl - Tmp) * Ppp + (Tpp - tl) * Pmp) / (Tpp - Tmp);
+    double rlo = ((tl - Tmm) * Rpm + (Tpm - tl) * Rmm) / (Tpm - Tmm);
+    double plo = ((tl - Tmm) * Ppm + (Tpm - tl) * Pmm) / (Tpm - Tmm);
+    R = ((pl - plo) * rhi + (phi - pl) * rlo) / (phi - plo);
+  } else {
+    double dpp = sqrt(rpp) + 1.0e-5, dpm = sqrt(rpm) + 1.0e-5, dmp = sqrt(rmp) + 1.0e-5,
+           dmm = sqrt(rmm) + 1.0e-5;
+    double rwt = 1.0 / dpp + 1.0 / dpm + 1.0 / dmp + 1.0 / dmm;
+    R = (s->tabk[(ipp > 1 ? ipp : 1) - 1] / dpp + s->tabk[(ipm > 1 ? ipm : 1) - 1] / dpm +
+         s->tabk[(imp > 1 ? imp : 1) - 1] / dmp + s->tabk[(imm > 1 ? imm : 1) - 1] / dmm) / rwt;
+  }
+  return pow(10.0, R);
+}
+
+void orc_ttaup(const orc_tcorr_t *s, const double *tin, const double *tau, double *abstd,
+               double *ptotal, double *pout, const double *prad, int n) {
+  const int MAX_CORRECTOR = 50, STALL_DECREASE = 3, RELAX_TRIGGER = 4;
+  const double CONV_TOL = 1.0e-4, DPLOG_MAX = 10.0, OPACITY_REBOOT = 2.0, STALL_RATIO = 0.9;
+  const double RELAX_LADDER[4] = {0.5, 0.3, 0.1, 0.05};
+  const double g = s->grav;
+  double dlgtau = log(tau[1] / tau[0]);
+  double plog1 = 0, plog2 = 0, plog3 = 0, plog4 = 0, dplog1 = 0, dplog2 = 0, dplog3 = 0;
+  double plog = 0, pnew, dplog = 0, err, perr, best_err, best_plog;
+  abstd[0] = 0.1;
+  if (prad[0] > 0.0) abstd[0] = fmin(0.1, g * tau[0] / prad[0] / 2.0);
+  double abstd1_init = abstd[0];
+  for (int J = 1; J <= n; ++J) {
+    int j = J - 1;
+    if (J == 1) plog = log(g / abstd[0] * tau[0]);
+    else if (J <= 4) plog = plog1 + dplog1;
+    else plog = (3.0 * plog4 + 8.0 * dplog1 - 4.0 * dplog2 + 8.0 * dplog3) / 3.0;
+    err = 1.0;
+    perr = 1.0;
+    best_err = HUGE_VAL;
+    best_plog = plog;
+    int N = 0, conv = 0, nstall = 0, rl = 1;
+    double relax = 0.5;
+    for (;;) {
+      ptotal[j] = exp(plog);
+      pout[j] = ptotal[j] + (prad[0] - prad[j]) + (0.0 - 0.0);
+      if (pout[j] <= 0.0) {
+        pout[j] = ptotal[j] * 1.0e-4;
+        if (pout[j] <= 0.0) pout[j] = 1.0e-10;
+      }
+      abstd[j] = orc_rosstab(s, tin[j], pout[j]);
+      dplog = g / abstd[j] * tau[j] / ptotal[j] * dlgtau;
+      dplog = fmax(0.0, fmin(DPLOG_MAX, dplog));
+      N = N + 1;
+      if (N == 1) continue;
+      if (J == 1) pnew = log(g / abstd[0] * tau[0]);
+      else if (J <= 4) pnew = (plog + 2.0 * plog1 + dplog + dplog1) / 3.0;
+      else
+        pnew = (126.0 * plog1 - 14.0 * plog3 + 9.0 * plog4 + 42.0 * dplog + 108.0 * dplog1 -
+                54.0 * dplog2 + 24.0 * dplog3) / 121.0;
+      perr = err;
+      err = fabs(pnew - plog);
+      if (err < best_err) {
+        best_err = err;
+        best_plog = pnew;
+      }
+      if (N > STALL_DECREASE && err > STALL_RATIO * perr) {
+        nstall = nstall + 1;
+        if (nstall >= RELAX_TRIGGER && rl < 4) {
+          rl = rl + 1;
+          nstall = 0;
+        }
+      } else {
+        nstall = nstall - 1 > 0 ? nstall - 1 : 0;
+      }
+      relax = RELAX_LADDER[rl - 1];
+      plog = (1.0 - relax) * plog + relax * pnew;
+      if (err <= CONV_TOL) {
+        conv = 1;
+        break;
+      }
+      if (N >= MAX_CORRECTOR) break;
+    }
+    if (!conv) {
+      plog = best_plog;
+      ptotal[j] = exp(plog);
+      pout[j] = ptotal[j] + (prad[0] - prad[j]);
+      if (pout[j] <= 0.0) pout[j] = fmax(ptotal[j] * 1.0e-4, 1.0e-10);
+      abstd[j] = orc_rosstab(s, tin[j], pout[j]);
+      dplog = g / abstd[j] * tau[j] / ptotal[j] * dlgtau;
+      dplog = fmax(0.0, fmin(DPLOG_MAX, dplog));
+    }
+    if (J == 1 && (abstd[0] / abstd1_init > OPACITY_REBOOT || abstd1_init / abstd[0] > OPACITY_REBOOT)) {
+      abstd1_init = abstd[0];
+      plog = log(g / abstd[0] * tau[0]);
+      ptotal[0] = exp(plog);
+      pout[0] = ptotal[0];
+      if (pout[0] > 0.0) {
+        abstd[0] = orc_rosstab(s, tin[0], pout[0]);
+        plog = log(g / abstd[0] * tau[0]);
+        ptotal[0] = exp(plog);
+        pout[0] = ptotal[0];
+      }
+      dplog = g / abstd[0] * tau[0] / ptotal[0] * dlgtau;
+      dplog = fmax(0.0, fmin(DPLOG_MAX, dplog));
+    }
+    plog4 = plog3;
+    plog3 = plog2;
+    plog2 = plog1;
+    plog1 = plog;
+    dplog3 = dplog2;
+    dplog2 = dplog1;
+    dplog1 = dplog;
+  }
+}
+
+double orc_atlas_finish(orc_tcorr_t *s) {
+  const int n = s->nrhox;
+  const double FOUR_SIGMA_OVER_PI = 4.0 * SIGMA_SB / PI_;
+  const double FOURPI_OVER_C = 4.0 * PI_ / CLIGHT;
+  const double FLUX = SIGMA_SB * orc_powi(s->teff, 4) / (4.0 * PI_);
+  const double ABROSS_FLOOR = 1.0e-30, RDIAGJ_FLOOR = 1.0e-30, HRATIO_DTLAMB_OFF = 1.0e-3;
+  double dtdrhx[KW_MAX], dabros[KW_MAX], codrhx[KW_MAX], G[KW_MAX], gflux[KW_MAX], dtau[KW_MAX];
+  double flxdrv[KW_MAX], dum[KW_MAX], tinteg[KW_MAX], tplus[KW_MAX], taustd[KW_MAX];
+  double tnew1[KW_MAX], tnew2[KW_MAX], prdnew[KW_MAX], ab1[KW_MAX], ab2[KW_MAX], pt1[KW_MAX],
+      pt2[KW_MAX], p1[KW_MAX], p2[KW_MAX], ppp[KW_MAX], rrr[KW_MAX], drhox[KW_MAX];
+  double remap[10][KW_MAX];
+  int j;
+  /* ROSS(3) */
+  for (j = 0; j < n; ++j) s->abross[j] = FOUR_SIGMA_OVER_PI * orc_powi(s->t[j], 3) / s->abross[j];
+  orc_integ(s->rhox, s->abross, s->tauros, n, s->abross[0] * s->rhox[0]);
+  orc_rosstab_store(s); /* RX = ROSSTAB(0,0,0), atlas12c.f90:586 */
+  /* RADIAP(3) */
+  double errormax = 0.0;
+  for (j = 0; j < n; ++j) {
+    s->raden[j] = s->raden[j] * FOURPI_OVER_C;
+    s->accrad[j] = s->accrad[j] * FOURPI_OVER_C;
+    if (s->h_total[j] / FLUX > 1.0) s->accrad[j] = s->accrad[j] * FLUX / s->h_total[j];
+    errormax = fmax(errormax, s->h_total[j] / FLUX);
+  }
+  s->pradk0 = s->pradk0 * FOURPI_OVER_C;
+  if (errormax > 1.0) s->pradk0 = s->pradk0 / errormax;
+  orc_integ(s->rhox, s->accrad, s->prad, n, s->accrad[0] * s->rhox[0]);
+  /* TCORR(3) */
+  orc_deriv(s->rhox, s->t, dtdrhx, n);
+  orc_deriv(s->rhox, s->abross, dabros, n);
+  for (j = 0; j < n; ++j) {
+    double abs_ = fmax(s->abross[j], ABROSS_FLOOR);
+    s->rdabh[j] = s->rdabh[j] - s->flxrad[j] * dabros[j] / abs_;
+    codrhx[j] = (s->rdabh[j] + 0.0) / (s->flxrad[j] + 0.0);
+  }
+  codrhx[0] = 0.0;
+  codrhx[1] = 0.0;
+  orc_integ(s->rhox, codrhx, G, n, 0.0);
+  for (j = 0; j < n; ++j) {
+    G[j] = exp(G[j]);
+    gflux[j] = G[j] * (s->flxrad[j] + 0.0 - FLUX) / (s->flxrad[j] + 0.0);
+  }
+  orc_integ(s->tauros, gflux, dtau, n, 0.0);
+  for (j = 0; j < n; ++j) {
+    dtau[j] = dtau[j] / G[j];
+    dtau[j] = fmax(-s->tauros[j] / 3.0, fmin(s->tauros[j] / 3.0, dtau[j]));
+    s->dtflux[j] = -dtau[j] * dtdrhx[j] / fmax(s->abross[j], ABROSS_FLOOR);
+  }
+  const double MAX_DT = 0.04 * s->teff;
+  double maxerr = 0.0;
+  for (j = 0; j < n; ++j) {
+    s->flxerr[j] = (s->flxrad[j] + 0.0 - FLUX) / FLUX * 100.0;
+    maxerr = fmax(maxerr, fabs(s->flxerr[j]));
+  }
+  orc_deriv(s->tauros, s->flxerr, flxdrv, n);
+  for (j = 0; j < n; ++j) {
+    double hratio = 0.0 / (0.0 + fmax(s->flxrad[j], 1.0e-30));
+    if (hratio < HRATIO_DTLAMB_OFF) flxdrv[j] = s->rjmins[j] / fmax(s->abross[j], ABROSS_FLOOR) / FLUX * 100.0;
+    s->dtlamb[j] = -flxdrv[j] * FLUX / 100.0 / fmax(fabs(s->rdiagj[j]), RDIAGJ_FLOOR) *
+                   copysign(1.0, s->rdiagj[j]) * fmax(s->abross[j], ABROSS_FLOOR);
+    s->dtlamb[j] = fmax(-MAX_DT, fmin(MAX_DT, s->dtlamb[j]));
+  }
+  double dtsur = (FLUX - s->flxrad[0]) / FLUX * 0.25 * s->t[0];
+  dtsur = fmax(-MAX_DT, fmin(MAX_DT, dtsur));
+  for (j = 0; j < n; ++j) dum[j] = s->dtflux[j] + s->dtlamb[j];
+  orc_integ(s->tauros, dum, tinteg, n, 0.0);
+  double xn = 0.1, tone, ttwo;
+  orc_map1(s->tauros, tinteg, n, &xn, &tone, 1);
+  xn = 2.0;
+  orc_map1(s->tauros, tinteg, n, &xn, &ttwo, 1);
+  double tav = (ttwo - tone) / 2.0;
+  if (dtsur * tav <= 0.0) tav = 0.0;
+  if (fabs(tav) > fabs(dtsur)) tav = dtsur;
+  dtsur = dtsur - tav;
+  for (j = 0; j < n; ++j) {
+    s->dtsurf[j] = dtsur;
+    s->t1[j] = s->dtflux[j] + s->dtlamb[j] + s->dtsurf[j];
+  }
+  for (j = 0; j < n; ++j) {
+    if (s->iter == 1) {
+    } else if (s->oldt1[j] * s->t1[j] > 0.0 && fabs(s->oldt1[j]) > fabs(s->t1[j])) {
+      s->t1[j] = s->t1[j] * 1.25;
+    } else if (s->oldt1[j] * s->t1[j] < 0.0) {
+      s->t1[j] = s->t1[j] * 0.5;
+    }
+    s->oldt1[j] = s->t1[j];
+  }
+  for (j = 0; j < n; ++j) {
+    tplus[j] = s->t[j] + s->t1[j];
+    taustd[j] = pow(10.0, -6.875 + (double)j * 0.125);
+  }
+  orc_map1(s->tauros, s->t, n, taustd, tnew1, n);
+  orc_map1(s->tauros, s->prad, n, taustd, prdnew, n);
+  orc_ttaup(s, tnew1, taustd, ab1, pt1, p1, prdnew, n);
+  orc_map1(s->tauros, tplus, n, taustd, tnew2, n);
+  orc_ttaup(s, tnew2, taustd, ab2, pt2, p2, prdnew, n);
+  for (j = 0; j < n; ++j) ppp[j] = (pt2[j] - pt1[j]) / pt1[j];
+  orc_map1(taustd, ppp, n, s->tauros, rrr, n);
+  for (j = 0; j < n; ++j) drhox[j] = rrr[j] * s->rhox[j];
+  for (j = 0; j < n; ++j) s->t[j] = s->t[j] + s->t1[j];
+  for (int i = 2; i <= n; ++i) {
+    int jj = n + 1 - i;
+    s->t[jj - 1] = fmin(s->t[jj - 1], s->t[jj] - 1.0);
+  }
+  for (j = 0; j < n; ++j) s->t[j] = fmax(s->t[j], 1200.0);
+  for (j = 0; j < n; ++j) s->rhox[j] = s->rhox[j] + drhox[j];
+  double *src[9] = {s->rhox, s->t, s->p, s->xne, s->abross, s->prad, s->vturb, s->pturb, s->accrad};
+  for (int q = 0; q < 9; ++q) orc_map1(s->tauros, src[q], n, taustd, remap[q], n);
+  for (j = 0; j < n; ++j)
+    if (s->tauros[0] > taustd[j] && remap[4][j] < 0.0) remap[4][j] = s->abross[0];
+  for (int q = 0; q < 8; ++q)
+    for (j = 0; j < n; ++j) src[q][j] = remap[q][j];
+  for (j = 0; j < n; ++j) s->tauros[j] = taustd[j];
+  return maxerr;
+}

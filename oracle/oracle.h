@@ -154,3 +154,27 @@ void orc_atlas_rt_pass(const orc_ops_t *ops, int numnu, const double *waveset,
 }
 #endif
 #endif
+
+/* ---- ATLAS12 iteration finish: ROSS(3), RADIAP(3), TCORR(3) ----------
+ * Radiative branch (IFCONV = 0: CONVEC not called, CNVFLX = 0, CZ_CONSTRUCT
+ * returns at once, no smoothing; USE_DTGRAD = .FALSE.).  ROSSTAB keeps the
+ * model's own kappa_R history (stored after ROSS(3), looked up by TTAUP).
+ * Arrays [nrhox] are updated in place as the Fortran module arrays are.
+ * Returns max |FLXERR| (percent). */
+typedef struct {
+  int nrhox, iter;
+  double teff, grav, pradk0;
+  double *t, *rhox, *p, *xne, *abross, *prad, *vturb, *pturb, *tauros, *accrad, *raden, *oldt1;
+  double *rjmins, *rdabh, *rdiagj, *flxrad, *h_total; /* mode-2 sums (rdabh modified) */
+  double *flxerr, *dtflux, *dtlamb, *dtsurf, *t1;     /* outputs */
+  /* ROSSTAB store (atlas12_modules.f90:5937-6228, IROSSTAB = 1): points
+   * (normalised log T, log P, log10 kappa_R) appended after every ROSS(3) */
+  int nross, maxtab;
+  double zerot, slopet, zerop, slopep;
+  double *tabt, *tabp, *tabk; /* [maxtab] */
+} orc_tcorr_t;
+void orc_rosstab_store(orc_tcorr_t *s);
+double orc_rosstab(const orc_tcorr_t *s, double t, double p);
+void orc_ttaup(const orc_tcorr_t *s, const double *tin, const double *tau, double *abstd,
+               double *ptotal, double *pout, const double *prad, int n);
+double orc_atlas_finish(orc_tcorr_t *s);

@@ -307,3 +307,65 @@ def atlas_rt_pass(ops, waveset, rcoset, acont, sigmac, xlines, rhox, t, hkt, tef
                               _ptr(rhox), _ptr(t), _ptr(hkt), teff, nu0, nu1, ctypes.byref(A), _ptr(hs))
     acc["pradk0"] = A.pradk0
     return acc, hs
+
+
+# ---------------------------------------------------------------- ATLAS finish
+_DPp = ctypes.POINTER(ctypes.c_double)
+
+
+class _Tcorr(ctypes.Structure):
+    _fields_ = [("nrhox", ctypes.c_int), ("iter", ctypes.c_int), ("teff", ctypes.c_double),
+                ("grav", ctypes.c_double), ("pradk0", ctypes.c_double)] + \
+               [(n, _DPp) for n in ("t", "rhox", "p", "xne", "abross", "prad", "vturb", "pturb", "tauros",
+                                    "accrad", "raden", "oldt1", "rjmins", "rdabh", "rdiagj", "flxrad", "h_total",
+                                    "flxerr", "dtflux", "dtlamb", "dtsurf", "t1")] + \
+               [("nross", ctypes.c_int), ("maxtab", ctypes.c_int), ("zerot", ctypes.c_double),
+                ("slopet", ctypes.c_double), ("zerop", ctypes.c_double), ("slopep", ctypes.c_double),
+                ("tabt", _DPp), ("tabp", _DPp), ("tabk", _DPp)]
+
+
+class RossStore:
+    """ROSSTAB's growing (log T, log P, log kappa_R) table (KW*60 entries, KW = 80)."""
+
+    def __init__(self, maxtab=80 * 60):
+        self.n = 0
+        self.maxtab = maxtab
+        self.norm = [0.0, 1.0, 0.0, 1.0]
+        self.t = np.zeros(maxtab)
+        self.p = np.zeros(maxtab)
+        self.k = np.zeros(maxtab)
+
+    def copy(self):
+        c = RossStore(self.maxtab)
+        c.n, c.norm = self.n, list(self.norm)
+        c.t, c.p, c.k = self.t.copy(), self.p.copy(), self.k.copy()
+        return c
+
+
+def atlas_finish(model, acc, iteration, store):
+    """ROSS(3)/ROSSTAB store/RADIAP(3)/TCORR(3) restatement; model dict and the
+    RossStore updated in place."""
+    L = lib()
+    L.orc_atlas_finish.argtypes = [ctypes.POINTER(_Tcorr)]
+    L.orc_atlas_finish.restype = ctypes.c_double
+    n = model["t"].size
+    names = ("t", "rhox", "p", "xne", "abross", "prad", "vturb", "pturb", "tauros", "accrad", "raden", "oldt1")
+    for k in names:
+        model[k] = np.ascontiguousarray(model[k], np.float64)
+    a = {k: np.ascontiguousarray(acc[k], np.float64).copy() for k in ("rjmins", "rdabh", "rdiagj", "flxrad",
+                                                                      "h_total", "raden", "accrad", "abross")}
+    # ROSS/RADIAP mode 3 turn the accumulated sums into the model quantities in place
+    model["abross"] = a["abross"]
+    model["raden"] = a["raden"]
+    model["accrad"] = a["accrad"]
+    out = {k: np.zeros(n) for k in ("flxerr", "dtflux", "dtlamb", "dtsurf", "t1")}
+    s = _Tcorr(n, int(iteration), float(model["teff"]), float(model["grav"]), float(acc["pradk0"]),
+               *[_ptr(model[k]) for k in names], *[_ptr(a[k]) for k in ("rjmins", "rdabh", "rdiagj", "flxrad",
+                                                                         "h_total")],
+               *[_ptr(out[k]) for k in out], store.n, store.maxtab, *store.norm, _ptr(store.t), _ptr(store.p),
+               _ptr(store.k))
+    err = L.orc_atlas_finish(ctypes.byref(s))
+    store.n = s.nross
+    store.norm = [s.zerot, s.slopet, s.zerop, s.slopep]
+    model["pradk0"] = s.pradk0
+    return err, out

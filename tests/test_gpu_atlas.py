@@ -1,0 +1,147 @@
+"""ATLAS12 hot path on the GPU (through the C ABI) against the CPU oracle.
+
+Tolerances (all FP64 on both sides; differences come from FMA contraction and
+the order of the FP64 atomic/partial sums):
+  * XLINES: relative 1e-9 per element (a flipped wing-stop decision would be ~1e-3)
+  * RT-pass sums: relative 1e-9; HNU(1) per frequency: relative 1e-6
+  * finish (T, RHOX, P after TCORR(3) and the remap): relative 1e-9
+"""
+import numpy as np
+import pytest
+
+from atlas12_b200 import _lib, atlas, surrogate, synthetic
+
+pytestmark = pytest.mark.gpu
+
+NSPEC = 270
+
+
+@pytest.fixture(scope="module")
+def atlas_case():
+    ross = surrogate.RossTable()
+    m = surrogate.grey_model(5777.0, 4.44, ross=ross)
+    pop = surrogate.populations(m["t"], m["p"], 1.5)
+    nr = m["t"].size
+    xnfdop = np.zeros((NSPEC, nr))
+    dopple = np.ones((NSPEC, nr))
+    nsp = min(NSPEC, pop["xnfp"].shape[1])
+    xd = np.where(pop["dopple"] > 0, pop["xnfp"] / np.maximum(pop["dopple"], 1e-300) / pop["rho"][:, None], 0.0)
+    xnfdop[:nsp] = xd[:, :nsp].T
+    dopple[:nsp] = np.where(pop["dopple"][:, :nsp].T > 0, pop["dopple"][:, :nsp].T, 1.0)
+    t = m["t"]
+    hkt = surrogate.HPLANCK / (surrogate.KBOL * t)
+    hckt = hkt * surrogate.CLIGHT
+    txnxn = (pop["nh"] * (1 - pop["xh"]) + 0.42 * 0.085 * pop["nh"]) * (t / 1e4) ** 0.3
+    ws, rc = synthetic.geometric_waveset(9.0, 160000.0, 3000)
+    cut = atlas.cutoff_grid()
+    iw = atlas.iwavetab(cut)
+    ka, sg = surrogate.continuum_opacity(cut, t, m["p"], pop)
+    stim_c = 1.0 - np.exp(-(surrogate.CLIGHT_NMS / cut)[:, None] * hkt[None, :])
+    tab = (ka + sg) * atlas.LINE_CUTOFF / stim_c
+    tab[cut <= ws[0]] = (1e10 + 0.0) * atlas.LINE_CUTOFF / stim_c[cut <= ws[0]]
+    tabcont = np.vstack([tab, tab[-1:]])
+    acont, sigmac = surrogate.continuum_opacity(ws, t, m["p"], pop)
+    lines = synthetic.atlas_lines(20000, ws[2], ws[-3], seed=4)
+    return dict(m=m, pop=pop, xnfdop=xnfdop, dopple=dopple, xne=pop["xne"], txnxn=txnxn, hkt=hkt, hckt=hckt,
+                ws=ws, rc=rc, cut=cut, iw=iw, tabcont=tabcont, acont=acont, sigmac=sigmac, lines=lines, ross=ross)
+
+
+@pytest.fixture(scope="module")
+def h_tables(po, tables):
+    return po.tabvoigt(tables["tabvi"], tables["tabh1"])
+
+
+@pytest.fixture(scope="module")
+def oracle_linop(po, atlas_case, h_tables):
+    c = atlas_case
+    atm = dict(xnfdop=c["xnfdop"], dopple=c["dopple"], xne=c["xne"], txnxn=c["txnxn"], hckt=c["hckt"])
+    return po.atlas_linop1(*h_tables, po.build_tablog(), c["lines"], atm, c["tabcont"], c["iw"], c["ws"])
+
+
+def test_linop_matches_oracle(gpu_ctx, tables, atlas_case, h_tables, oracle_linop):
+    c = atlas_case
+    A = atlas.Atlas(gpu_ctx, tables, *h_tables)
+    xl, used = A.linop1(c["lines"], 72, c["xnfdop"], c["dopple"], c["xne"], c["txnxn"], c["hckt"], c["tabcont"],
+                        c["iw"], c["ws"])
+    ref, ref_used = oracle_linop
+    assert used == ref_used and used > 100
+    assert np.count_nonzero(ref) > 1000
+    scale = np.maximum(np.abs(ref), 1e-300)
+    assert np.max(np.abs(xl - ref) / scale) < 1e-9
+
+
+def test_linop_empty_and_out_of_grid(gpu_ctx, tables, atlas_case, h_tables, po):
+    c = atlas_case
+    A = atlas.Atlas(gpu_ctx, tables, *h_tables)
+    xl, used = A.linop1(np.zeros((0, 4), np.int32), 72, c["xnfdop"], c["dopple"], c["xne"], c["txnxn"], c["hckt"],
+                        c["tabcont"], c["iw"], c["ws"])
+    assert used == 0 and not xl.any()
+    # lines outside START..STOP and with an out-of-range species are skipped
+    ld = c["lines"][:50].copy()
+    ld[:10, 0] = 1000                            # ~ 1.0005 nm, blue of the grid
+    ld[10:20, 1] = (ld[10:20, 1] & ~0xffff) | 9999  # NELION = 999 > nspec
+    atm = dict(xnfdop=c["xnfdop"], dopple=c["dopple"], xne=c["xne"], txnxn=c["txnxn"], hckt=c["hckt"])
+    ref, ru = po.atlas_linop1(*h_tables, po.build_tablog(), ld, atm, c["tabcont"], c["iw"], c["ws"])
+    got, gu = A.linop1(ld, 72, c["xnfdop"], c["dopple"], c["xne"], c["txnxn"], c["hckt"], c["tabcont"], c["iw"],
+                       c["ws"])
+    assert gu == ru
+    np.testing.assert_allclose(got, ref, rtol=1e-9, atol=0)
+
+
+def test_rt_pass_matches_oracle(po, ops, gpu_ctx, tables, atlas_case, oracle_linop):
+    c = atlas_case
+    xl = oracle_linop[0]
+    m = c["m"]
+    ref, rhs = po.atlas_rt_pass(ops, c["ws"], c["rc"], c["acont"], c["sigmac"], xl, m["rhox"], m["t"], c["hkt"],
+                                5777.0)
+    A = atlas.Atlas(gpu_ctx, tables)
+    got, ghs = A.rt_pass(c["ws"], c["rc"], c["acont"], c["sigmac"], xl, m["rhox"], m["t"], c["hkt"], 5777.0)
+    for k in atlas.ACC_NAMES:
+        np.testing.assert_allclose(got[k], ref[k], rtol=1e-9, err_msg=k)
+    assert abs(got["pradk0"] - ref["pradk0"]) <= 1e-9 * abs(ref["pradk0"])
+    # per-frequency H(1): where the Eddington sweep runs, its stop test (summed
+    # error < 1e-5) is summed in a different order, which can change the last
+    # sweep and H(1) by up to ~1e-7
+    np.testing.assert_allclose(ghs, rhs, rtol=1e-6)
+
+
+def test_finish_matches_oracle(po, ops, gpu_ctx, tables, atlas_case, oracle_linop):
+    c = atlas_case
+    m = c["m"]
+    acc, _ = po.atlas_rt_pass(ops, c["ws"], c["rc"], c["acont"], c["sigmac"], oracle_linop[0], m["rhox"], m["t"],
+                              c["hkt"], 5777.0)
+    nr = m["t"].size
+
+    def state():
+        return dict(t=m["t"].copy(), rhox=m["rhox"].copy(), p=m["p"].copy(), xne=c["xne"].copy(),
+                    abross=np.zeros(nr), prad=np.zeros(nr), vturb=np.full(nr, 1.5e5), pturb=np.zeros(nr),
+                    tauros=m["tauros"].copy(), accrad=np.zeros(nr), raden=np.zeros(nr), oldt1=np.zeros(nr),
+                    teff=5777.0, grav=m["grav"])
+
+    A = atlas.Atlas(gpu_ctx, tables)
+    store_o, store_g = po.RossStore(), atlas.RossStore()
+    for it in (1, 2, 3):
+        so, sg = state(), state()
+        so["oldt1"] = np.linspace(-20, 30, nr)  # OLDT1 is updated in place: one copy each
+        sg["oldt1"] = np.linspace(-20, 30, nr)
+        eo, oo = po.atlas_finish(so, acc, it, store_o)
+        eg, og = A.finish(sg, acc, it, store_g)
+        assert store_g.n == store_o.n == 72 * it
+        np.testing.assert_allclose(store_g.k[:store_g.n], store_o.k[:store_o.n], rtol=1e-12)
+        assert abs(eg - eo) <= 1e-9 * max(eo, 1e-3)
+        for k in ("t", "rhox", "p", "xne", "prad", "tauros"):
+            np.testing.assert_allclose(sg[k], so[k], rtol=1e-9, err_msg=k)
+        for k in ("flxerr", "dtflux", "dtlamb", "t1"):
+            np.testing.assert_allclose(og[k], oo[k], rtol=1e-8, atol=1e-9, err_msg=k)
+
+
+def test_model_iteration_reduces_flux_error(gpu_ctx, tables):
+    ws, rc = synthetic.geometric_waveset(9.0, 160000.0, 6000)
+    lines = synthetic.atlas_lines(20000, ws[2], ws[-3], seed=4)
+    model = atlas.AtlasModel(gpu_ctx, tables, teff=5777.0, logg=4.44, linedata=lines, waveset=ws, rcoset=rc)
+    n, hist = model.iterate(max_iter=12, tol_percent=0.0, graph=True)
+    s = model.structure()
+    model.close()
+    assert n == 12 and np.all(np.isfinite(hist))
+    assert hist[-1] < 0.5 * hist[0], hist
+    assert np.all(np.diff(s["t"]) > 0) and s["t"].min() >= 1200.0
