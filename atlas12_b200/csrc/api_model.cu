@@ -121,11 +121,18 @@ __global__ void k_surrogate_eval(int nrhox, const double* t, const double* p, do
   }
 }
 
-int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m) {
+// One iteration on the context stream.  With timed = true (never while a
+// graph is being captured) each launch is bracketed by CUDA events.
+int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
   cudaStream_t s = ctx->stream;
-  k_model_eos<<<1, 128, 0, s>>>(m->ms, m->iter_dev, m->nrhox, m->kw, m->grav, m->vturb * 1.0e5,
-                                m->xnfdop, m->dopple, m->xne_eos, m->txnxn, m->hkt, m->hckt, m->rho, m->cc);
-  CKL(ctx);
+  const bool was = ctx->timing;
+  ctx->timing = was && timed;
+  {
+    Timer tm(ctx, "model_eos");
+    k_model_eos<<<1, 128, 0, s>>>(m->ms, m->iter_dev, m->nrhox, m->kw, m->grav, m->vturb * 1.0e5, m->xnfdop,
+                                  m->dopple, m->xne_eos, m->txnxn, m->hkt, m->hckt, m->rho, m->cc);
+    CKL(ctx);
+  }
   if (!m->kapcont_done) {
     k_model_kapcont<<<m->nwave, 128, 0, s>>>(m->cutwave, m->nwave, m->waveset, m->nrhox, m->kw, m->hkt,
                                              m->cc, m->tabcont);
@@ -136,6 +143,7 @@ int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m) {
     LinopArgs la{m->lines, m->nlines, m->nrhox, m->kw, m->nspec, m->numnu, m->xnfdop, m->dopple,
                  m->xne_eos, m->txnxn, m->hckt, m->tabcont, m->waveset, m->h0, m->h1, m->h2, m->xl,
                  nullptr, m->cnt};
+    Timer tm(ctx, "atlas_linop");
     k_atlas_linop<<<grid_for(ctx, m->nlines * 32, 256, 16), 256, 0, s>>>(la);
     CKL(ctx);
   }
@@ -144,14 +152,38 @@ int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m) {
             m->teff, 1, m->partial, m->hsurf, nullptr};
   const int target = ctx->nsm * m->nwarp_rt * 6;
   ra.nu_per_warp = std::max(1, (m->numnu + target - 1) / target);
-  k_atlas_rt<true><<<m->blocks_rt, 32 * m->nwarp_rt, m->smem_rt, s>>>(ra);
-  CKL(ctx);
-  k_atlas_reduce<<<(kAcc * m->kw + 1 + 127) / 128, 128, 0, s>>>(m->partial, m->nwl, m->kw, 0, m->sum);
-  CKL(ctx);
-  k_model_finish<<<1, 32, 0, s>>>(m->ms, m->sum, m->kw, m->nrhox, m->iter_dev, m->teff, m->grav, m->R,
-                                  m->work, m->maxerr_dev);
-  CKL(ctx);
+  {
+    Timer tm(ctx, "atlas_rt");
+    k_atlas_rt<true><<<m->blocks_rt, 32 * m->nwarp_rt, m->smem_rt, s>>>(ra);
+    CKL(ctx);
+  }
+  {
+    Timer tm(ctx, "atlas_reduce");
+    k_atlas_reduce<<<(kAcc * m->kw + 1 + 127) / 128, 128, 0, s>>>(m->partial, m->nwl, m->kw, 0, m->sum);
+    CKL(ctx);
+  }
+  {
+    Timer tm(ctx, "atlas_finish");
+    k_model_finish<<<1, 32, 0, s>>>(m->ms, m->sum, m->kw, m->nrhox, m->iter_dev, m->teff, m->grav, m->R,
+                                    m->work, m->maxerr_dev);
+    CKL(ctx);
+  }
+  ctx->timing = was;
   return 0;
+}
+
+__global__ void k_fp64_fma(double* out, int iters) {
+  // 8 independent DFMA chains per thread
+  double a[8];
+  for (int k = 0; k < 8; ++k) a[k] = 1.0 + 1e-9 * (threadIdx.x + k);
+  const double b = 0.999999999, c = 1e-12;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = fma(a[k], b, c);
+  }
+  double s = 0.0;
+  for (int k = 0; k < 8; ++k) s += a[k];
+  if (s == 12345.678) out[0] = s;  // keep the chains alive
 }
 
 template <class T>
@@ -331,13 +363,13 @@ int atlasgpu_model_iterate(atlasgpu_ctx* ctx, atlasgpu_model* m, int max_iter, d
   for (int it = 0; it < max_iter; ++it) {
     if (!m->kapcont_done) {
       // first iteration of the model: KAPCONT included, not captured
-      if ((r = enqueue_iteration(ctx, m))) return r;
+      if ((r = enqueue_iteration(ctx, m, true))) return r;
       m->kapcont_done = true;
     } else if (use_graph) {
       if (!m->gexec) {
         CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         const int64_t l0 = ctx->launches;
-        r = enqueue_iteration(ctx, m);
+        r = enqueue_iteration(ctx, m, false);
         cudaGraph_t g = nullptr;
         const cudaError_t ec = cudaStreamEndCapture(s, &g);
         if (r) return r;
@@ -349,7 +381,7 @@ int atlasgpu_model_iterate(atlasgpu_ctx* ctx, atlasgpu_model* m, int max_iter, d
       CK(cudaGraphLaunch(m->gexec, s));
       ctx->launches += 5;
     } else {
-      if ((r = enqueue_iteration(ctx, m))) return r;
+      if ((r = enqueue_iteration(ctx, m, true))) return r;
     }
     double e = 0.0;
     CK(cudaMemcpyAsync(&e, m->maxerr_dev, sizeof e, cudaMemcpyDeviceToHost, s));
@@ -398,6 +430,7 @@ int atlasgpu_model_set_structure(atlasgpu_ctx* ctx, atlasgpu_model* m, const dou
   }
   CK(cudaMemcpy(m->state, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemset(m->iter_dev, 0, sizeof(int)));
+  m->kapcont_done = false;  // KAPCONT runs again on the new structure's first iteration
   RossStore R0{0, kRossMax, 0.0, 1.0, 0.0, 1.0, m->ross, m->ross + kRossMax, m->ross + 2 * kRossMax};
   CK(cudaMemcpy(m->R, &R0, sizeof R0, cudaMemcpyHostToDevice));
   return 0;
@@ -419,6 +452,29 @@ int atlasgpu_model_destroy(atlasgpu_ctx* ctx, atlasgpu_model* m) {
     if (p) cudaFree(p);
   delete m;
   return ATLASGPU_OK;
+}
+
+double atlasgpu_fp64_peak_tflops(atlasgpu_ctx* ctx) {
+  if (!ctx) return -1.0;
+  cudaSetDevice(ctx->device);
+  double* d;
+  if (bufT(ctx, "peak_out", 1, &d)) return -1.0;
+  const int iters = 4096, threads = 256, blocks = ctx->nsm * 8;
+  k_fp64_fma<<<blocks, threads, 0, ctx->stream>>>(d, 64);  // warm-up
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, ctx->stream);
+  k_fp64_fma<<<blocks, threads, 0, ctx->stream>>>(d, iters);
+  cudaEventRecord(b, ctx->stream);
+  cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (cudaGetLastError() != cudaSuccess || ms <= 0.f) return -1.0;
+  const double flops = 2.0 * 8.0 * iters * (double)threads * blocks;
+  return flops / (ms * 1e-3) / 1e12;
 }
 
 }  // extern "C"

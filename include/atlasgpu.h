@@ -244,6 +244,11 @@ int atlasgpu_model_set_structure(atlasgpu_ctx *ctx, atlasgpu_model *m, const dou
                                  const double *p, const double *rhox);
 int atlasgpu_model_destroy(atlasgpu_ctx *ctx, atlasgpu_model *m);
 
+/* Measured FP64 FMA throughput of the device (TFLOP/s, 2 flops per FMA):
+ * the denominator of the FP64-pipe roofline of the transfer kernels.  No
+ * reference counterpart.  Returns a negative value on failure. */
+double atlasgpu_fp64_peak_tflops(atlasgpu_ctx *ctx);
+
 /* The surrogate physics on the device for given T, P [nrhox]: continuum
  * absorption and scattering kabs, sigma [nw][nrhox] at wave [nw] (nm),
  * electron density xne [nrhox] and XNFDOP [270][nrhox] (may be NULL).  No

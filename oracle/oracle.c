@@ -12,6 +12,9 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #define KW_MAX 128
 
@@ -933,12 +936,12 @@ int64_t orc_atlas_linop1(const orc_atlas_tables_t *tb, const int32_t *linedata,
  * (scont NULL => SCONT = BNU); ALINE = XLINES*STIM, SIGMAL = 0, SLINE = BNU.
  * acc arrays are accumulated into (call with zeroed arrays for mode 1).
  * ==================================================================== */
-void orc_atlas_rt_pass(const orc_ops_t *ops, int numnu, const double *waveset,
-                       const double *rcoset, const double *acont,
-                       const double *sigmac, const double *scont, int kw,
-                       const double *xlines, int nrhox, const double *rhox,
-                       const double *t, const double *hkt, double teff, int nu0,
-                       int nu1, orc_accum_t *acc, double *hsurf) {
+static void rt_pass_range(const orc_ops_t *ops, int numnu, const double *waveset,
+                          const double *rcoset, const double *acont,
+                          const double *sigmac, const double *scont, int kw,
+                          const double *xlines, int nrhox, const double *rhox,
+                          const double *t, const double *hkt, double teff, int nu0,
+                          int nu1, orc_accum_t *acc, double *hsurf) {
   const double BP = bnu_prefac();
   double ehvkt[KW_MAX], stim[KW_MAX], bnu[KW_MAX], aline[KW_MAX], sigmal[KW_MAX],
       sline[KW_MAX], sc[KW_MAX];
@@ -1025,6 +1028,53 @@ void orc_atlas_rt_pass(const orc_ops_t *ops, int numnu, const double *waveset,
       acc->abross[j] = acc->abross[j] + dbdt / abtot[j] * rcowt;
     }
   }
+}
+
+/* The frequency loop split into contiguous chunks over the host threads
+ * (OMP_NUM_THREADS); each chunk sums in frequency order into private
+ * accumulators, which are added in chunk order. */
+void orc_atlas_rt_pass(const orc_ops_t *ops, int numnu, const double *waveset,
+                       const double *rcoset, const double *acont,
+                       const double *sigmac, const double *scont, int kw,
+                       const double *xlines, int nrhox, const double *rhox,
+                       const double *t, const double *hkt, double teff, int nu0,
+                       int nu1, orc_accum_t *acc, double *hsurf) {
+  int nth = 1;
+#ifdef _OPENMP
+  nth = omp_get_max_threads();
+#endif
+  if (nth > nu1 - nu0 + 1) nth = nu1 - nu0 + 1;
+  if (nth <= 1) {
+    rt_pass_range(ops, numnu, waveset, rcoset, acont, sigmac, scont, kw, xlines, nrhox, rhox,
+                  t, hkt, teff, nu0, nu1, acc, hsurf);
+    return;
+  }
+  double *priv = (double *)calloc((size_t)nth * (8 * KW_MAX + 1), sizeof(double));
+#pragma omp parallel num_threads(nth)
+  {
+    int id = 0;
+#ifdef _OPENMP
+    id = omp_get_thread_num();
+#endif
+    int len = nu1 - nu0 + 1;
+    int a = nu0 + (int)((long)len * id / nth), b = nu0 + (int)((long)len * (id + 1) / nth) - 1;
+    double *p = priv + (size_t)id * (8 * KW_MAX + 1);
+    orc_accum_t loc = {p, p + KW_MAX, p + 2 * KW_MAX, p + 3 * KW_MAX, p + 4 * KW_MAX,
+                       p + 5 * KW_MAX, p + 6 * KW_MAX, p + 7 * KW_MAX, 0.0};
+    if (a <= b)
+      rt_pass_range(ops, numnu, waveset, rcoset, acont, sigmac, scont, kw, xlines, nrhox, rhox,
+                    t, hkt, teff, a, b, &loc, hsurf ? hsurf + (a - nu0) : NULL);
+    p[8 * KW_MAX] = loc.pradk0;
+  }
+  double *dst[8] = {acc->rjmins, acc->rdabh, acc->rdiagj, acc->flxrad,
+                    acc->raden, acc->h_total, acc->accrad, acc->abross};
+  for (int id = 0; id < nth; ++id) {
+    double *p = priv + (size_t)id * (8 * KW_MAX + 1);
+    for (int q = 0; q < 8; ++q)
+      for (int j = 0; j < nrhox; ++j) dst[q][j] = dst[q][j] + p[q * KW_MAX + j];
+    acc->pradk0 = acc->pradk0 + p[8 * KW_MAX];
+  }
+  free(priv);
 }
 
 /* ======================================================================
