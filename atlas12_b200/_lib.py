@@ -83,6 +83,7 @@ SIGNATURES = {
     "atlasgpu_model_destroy": (_I, [_P, _P]),
     "atlasgpu_surrogate_eval": (_I, [_P, _I, _P, _P, _D, _I, _P, _P, _P, _P, _P]),
     "atlasgpu_fp64_peak_tflops": (_D, [_P]),
+    "atlasgpu_atlas_rt_pass_noalloc": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _D, _P, _P]),
 }
 
 _DP = ctypes.POINTER(ctypes.c_double)

@@ -1,0 +1,88 @@
+// api_noalloc.cu -- the frequency loop of the ATLAS12 RT pass for callers
+// that cannot allocate device memory.
+//
+// Some callers manage every byte of device memory themselves and may not call
+// cudaMalloc: a Fortran driver that owns its device arrays through its own
+// allocator or memory pool, code running inside a memory budget enforced by
+// the host application, or a process that must not grow its footprint after
+// start-up.  atlasgpu_atlas_rt_pass_noalloc serves them: the caller passes all
+// inputs and outputs as device pointers, and the only scratch the pass needs
+// (one row of partial sums per warp) lives in a fixed file-scope device array.
+//
+// That array is part of the library image: every GPU that loads the library
+// holds it (kNoAllocWarps x (8*kKwMax + 1) doubles = 6.6 MB) until the
+// process exits.  All calls share it and it keeps the last call's contents;
+// every row a call reads is written by that call first, so nothing needs
+// clearing, but two calls that overlap on the GPU (different streams, or
+// different host threads on one device) race on it and must be serialised by
+// the caller.
+#include "api_common.cuh"
+#include "atlas.cuh"
+
+using namespace atlasgpu;
+
+namespace {
+
+constexpr int kNoAllocWarps = 1024;               // maximum warps (rows of partials)
+constexpr int kNoAllocRow = kAcc * kKwMax + 1;    // one row: 8 sums per depth + PRADK0
+
+static __device__ __align__(256) double g_noalloc_partial[(size_t)kNoAllocWarps * kNoAllocRow];
+
+constexpr int kMaxDevices = 64;
+double* g_partial_addr[kMaxDevices] = {nullptr};  // device address of the array, per device
+
+}  // namespace
+
+extern "C" {
+
+int atlasgpu_atlas_rt_pass_noalloc(atlasgpu_ctx* ctx, int numnu, const double* d_waveset,
+                                   const double* d_rcoset, const double* d_acont, const double* d_sigmac,
+                                   const double* d_scont, int kw, const double* d_xlines_t, int nrhox,
+                                   const double* d_rhox, const double* d_t, const double* d_hkt, double teff,
+                                   double* d_sums, double* d_hsurf) {
+  if (!ctx) return ATLASGPU_EINVAL;
+  if (!ctx->ops_set) return fail(ctx, ATLASGPU_ESTATE, "rt_pass_noalloc: operators not set");
+  if (numnu < 1 || nrhox < 4 || kw < nrhox)
+    return fail(ctx, ATLASGPU_EINVAL, "rt_pass_noalloc: numnu %d, nrhox %d, kw %d", numnu, nrhox, kw);
+  if (kw > kKwMax)
+    return fail(ctx, ATLASGPU_EINVAL, "rt_pass_noalloc: kw = %d exceeds the fixed scratch limit of %d depths",
+                kw, kKwMax);
+  if (!d_waveset || !d_rcoset || !d_acont || !d_sigmac || !d_xlines_t || !d_rhox || !d_t || !d_hkt || !d_sums ||
+      !d_hsurf)
+    return fail(ctx, ATLASGPU_EINVAL, "rt_pass_noalloc: null device pointer");
+  if (ctx->device < 0 || ctx->device >= kMaxDevices)
+    return fail(ctx, ATLASGPU_EINVAL, "rt_pass_noalloc: device %d beyond %d", ctx->device, kMaxDevices);
+  CK(cudaSetDevice(ctx->device));
+  // set-up, once per device, with that device current: the host-side name of
+  // the array is not a device address, so ask the runtime for the address
+  if (!g_partial_addr[ctx->device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partial);
+    if (e != cudaSuccess || !p)
+      return fail(ctx, ATLASGPU_ECUDA, "rt_pass_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    g_partial_addr[ctx->device] = (double*)p;
+  }
+  double* partial = g_partial_addr[ctx->device];
+  // launch shape: at most kNoAllocWarps warps, contiguous frequencies per warp
+  int nwarp = 4;
+  while (nwarp > 1 && sizeof(double) * kKwMax + nwarp * sizeof(RtWS) > ctx->smem_optin) --nwarp;
+  const size_t smem = sizeof(double) * kKwMax + nwarp * sizeof(RtWS);
+  int target = ctx->nsm * nwarp * 6;
+  if (target > kNoAllocWarps) target = kNoAllocWarps;
+  const int npw = (numnu + target - 1) / target;
+  const int nw = (numnu + npw - 1) / npw;
+  const int blocks = (nw + nwarp - 1) / nwarp;
+  const int nwl = blocks * nwarp;
+  if (nwl > kNoAllocWarps)
+    return fail(ctx, ATLASGPU_EINVAL, "rt_pass_noalloc: %d warps exceed the scratch limit %d", nwl, kNoAllocWarps);
+  CK(cudaFuncSetAttribute(k_atlas_rt<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  RtArgs a{ctx->ops, nullptr, numnu, nrhox, kw, d_waveset, d_rcoset, d_acont, d_sigmac, d_scont, d_xlines_t,
+           d_rhox, d_t, d_hkt, teff, npw, partial, d_hsurf, nullptr};
+  k_atlas_rt<false><<<blocks, 32 * nwarp, smem, ctx->stream>>>(a);
+  CKL(ctx);
+  k_atlas_reduce<<<(kAcc * kw + 1 + 127) / 128, 128, 0, ctx->stream>>>(partial, nwl, kw, 0, d_sums);
+  CKL(ctx);
+  return ATLASGPU_OK;
+}
+
+}  // extern "C"

@@ -244,6 +244,29 @@ int atlasgpu_model_set_structure(atlasgpu_ctx *ctx, atlasgpu_model *m, const dou
                                  const double *p, const double *rhox);
 int atlasgpu_model_destroy(atlasgpu_ctx *ctx, atlasgpu_model *m);
 
+/* The RT-pass frequency loop for callers that cannot allocate device memory.
+ * No counterpart in the reference (it is a second entry to the work of
+ * atlasgpu_atlas_rt_pass).  Every input and output is a device pointer owned
+ * by the caller: d_waveset, d_rcoset [numnu]; d_acont, d_sigmac, d_scont
+ * [numnu][kw] (d_scont may be NULL: SCONT = BNU); d_xlines_t = XLINES
+ * transposed, [kw][numnu] (the layout the device LINOP1 writes); d_rhox,
+ * d_t, d_hkt [nrhox]; d_sums [8*kw + 1] receives RJMINS, RDABH, RDIAGJ,
+ * FLXRAD, RADEN, H_TOTAL, ACCRAD, ABROSS ([q*kw + j]) and PRADK0 ([8*kw]);
+ * d_hsurf [numnu] receives HNU(1) per frequency.
+ * The call allocates nothing: its scratch is a fixed device array of
+ * 1024 x 801 doubles (6.6 MB) in the library image, held by every GPU that
+ * loads the library until the process exits.  kw above 100 is rejected.
+ * The first call on a device looks the array's address up once (make that
+ * first call before any stream capture).  All calls share the array, so calls
+ * that overlap on the GPU race: serialise them.  Runs on the context stream
+ * and returns without waiting. */
+int atlasgpu_atlas_rt_pass_noalloc(atlasgpu_ctx *ctx, int numnu, const double *d_waveset,
+                                   const double *d_rcoset, const double *d_acont,
+                                   const double *d_sigmac, const double *d_scont, int kw,
+                                   const double *d_xlines_t, int nrhox, const double *d_rhox,
+                                   const double *d_t, const double *d_hkt, double teff,
+                                   double *d_sums, double *d_hsurf);
+
 /* Measured FP64 FMA throughput of the device (TFLOP/s, 2 flops per FMA):
  * the denominator of the FP64-pipe roofline of the transfer kernels.  No
  * reference counterpart.  Returns a negative value on failure. */
