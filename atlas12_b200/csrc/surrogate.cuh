@@ -44,6 +44,10 @@ struct ContCoef {
   double mbf[kNMetal];  // neutral-metal density * cross-section / rho
 };
 constexpr double kMbfSigma = 2.0e-17;  // surrogate.MBF_SIGMA
+// Fraction of the metal / molecule populations seen by the ATLAS12 line list
+// (surrogate.ATLAS_LINE_POP): the device surrogate serves only the ATLAS12
+// model, whose purely radiative structure stays convergent at this strength.
+constexpr double kAtlasLinePop = 0.01;
 
 struct EosOut {
   double xne, rho, nh, xh;
@@ -83,12 +87,12 @@ __device__ inline EosOut surrogate_depth(double t, double p, double vturb_cms, i
     const double n = nh * exp10(kMetal[m][3] - 12.0);
     const int z = (int)kMetal[m][0];
     const double d = dop(kMetal[m][1]);
-    put((z - 1) * 6 + 1, n / (1.0 + r) / kMetal[m][4], d);
-    put((z - 1) * 6 + 2, n * r / (1.0 + r) / kMetal[m][5], d);
+    put((z - 1) * 6 + 1, n / (1.0 + r) / kMetal[m][4] * kAtlasLinePop, d);
+    put((z - 1) * 6 + 2, n * r / (1.0 + r) / kMetal[m][5] * kAtlasLinePop, d);
   }
   for (int m = 0; m < kNMol; ++m) {
     const int slot = (int)kMol[m][0];
-    const double v = nh * exp10(kMol[m][2]) * fmin(pow(5000.0 / t, kMol[m][3]), 1e6) / 1000.0;
+    const double v = nh * exp10(kMol[m][2]) * fmin(pow(5000.0 / t, kMol[m][3]), 1e6) / 1000.0 * kAtlasLinePop;
     put((slot - 1) * 6 + 1, v, dop(kMol[m][1]));
   }
   // continuum coefficients (surrogate.continuum_opacity)

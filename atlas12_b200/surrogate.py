@@ -61,6 +61,15 @@ MOLECULES = np.array([
 ])
 MW6 = 139 * 6  # SYNTHE's flattened species axis (mw*6)
 MBF_SIGMA = 2.0e-17  # metal ground-state photo-ionisation cross-section at the edge (cm^2)
+# Fraction of each metal / molecule population that the ATLAS12 synthetic line
+# list draws on.  The ATLAS12 model here is purely radiative (the reference's
+# convective flux, CONVEC, is outside the hot path), and a radiative solar
+# model blanketed by 500,000 full-strength synthetic lines has no radiative-
+# equilibrium solution reachable from the grey start: the deep layers heat
+# without bound.  At 1/100 the grey start converges to max|FLXERR| <= 0.1 %
+# in about 30 iterations.  SYNTHE's synthetic atmospheres use the full
+# populations (line_pop = 1).
+ATLAS_LINE_POP = 0.01
 
 
 def nelion(z, ion_stage):
@@ -108,9 +117,11 @@ def eos(t, p):
     return dict(ntot=ntot, nh=nh, xne=ne, rho=rho, xh=xh)
 
 
-def populations(t, p, vturb_kms):
+def populations(t, p, vturb_kms, line_pop=1.0):
     """Per-depth species number densities / partition function (XNFPEL analogue)
-    and Doppler widths.  Returns dict of [nrhox, MW6] arrays plus eos fields."""
+    and Doppler widths.  Returns dict of [nrhox, MW6] arrays plus eos fields.
+    line_pop scales the metal and molecule entries (ATLAS_LINE_POP for the
+    ATLAS12 model, 1 for SYNTHE); hydrogen and the EOS are unaffected."""
     t = np.asarray(t, dtype=np.float64)
     e = eos(t, p)
     nr = t.size
@@ -128,12 +139,12 @@ def populations(t, p, vturb_kms):
         r = _saha(t, e["xne"], chi, u1, u2)
         n = e["nh"] * 10.0 ** (leps - 12.0)
         i1, i2 = nelion(z, 1) - 1, nelion(z, 2) - 1
-        xnfp[:, i1] = n / (1.0 + r) / u1
-        xnfp[:, i2] = n * r / (1.0 + r) / u2
+        xnfp[:, i1] = n / (1.0 + r) / u1 * line_pop
+        xnfp[:, i2] = n * r / (1.0 + r) / u2 * line_pop
         dop[:, i1] = dop[:, i2] = _dop(m)
     for slot, m, labund, texp in MOLECULES:
         i = mol_nelion(slot) - 1
-        xnfp[:, i] = e["nh"] * 10.0 ** labund * np.minimum((5000.0 / t) ** texp, 1e6) / 1000.0
+        xnfp[:, i] = e["nh"] * 10.0 ** labund * np.minimum((5000.0 / t) ** texp, 1e6) / 1000.0 * line_pop
         dop[:, i] = _dop(m)
     e.update(xnfp=xnfp, dopple=dop)
     return e

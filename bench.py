@@ -183,7 +183,7 @@ def oracle_iteration_factory(po, atlas, ops, W):
         if it > 1:
             p = st["grav"] * st["rhox"] - st["prad"]
             st["p"] = np.where(p <= 0, np.maximum(st["grav"] * st["rhox"] * 1e-4, 1e-10), p)
-        pop = sg.populations(st["t"], st["p"], CFG["vturb_kms"])
+        pop = sg.populations(st["t"], st["p"], CFG["vturb_kms"], sg.ATLAS_LINE_POP)
         t = st["t"]
         xd = np.zeros((270, nr))
         dp = np.ones((270, nr))
@@ -203,9 +203,10 @@ def oracle_iteration_factory(po, atlas, ops, W):
         xl, _ = po.atlas_linop1(h0, h1, h2, tl, W["lines"], atm, state["tabcont"], iw, W["ws"])
         ac, sgm = sg.continuum_opacity(W["ws"], t, st["p"], pop)
         acc, _ = po.atlas_rt_pass(ops, W["ws"], W["rc"], ac, sgm, xl, st["rhox"], t, hkt, CFG["teff"])
-        err, _ = po.atlas_finish(st, acc, it, store)
+        err, st["finish"] = po.atlas_finish(st, acc, it, store)
         return err
 
+    step.state = st
     return step
 
 

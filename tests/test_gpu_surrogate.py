@@ -17,7 +17,7 @@ def test_device_surrogate_matches_numpy(gpu_ctx):
     xne, xd = np.zeros(nr), np.zeros((270, nr))
     gpu_ctx.call("atlasgpu_surrogate_eval", nr, ptr(t), ptr(p), 1.5, nw, ptr(wave), ptr(ka), ptr(sg), ptr(xne), ptr(xd))
     rk, rs = surrogate.continuum_opacity(wave, t, p)
-    pop = surrogate.populations(t, p, 1.5)
+    pop = surrogate.populations(t, p, 1.5, surrogate.ATLAS_LINE_POP)
     np.testing.assert_allclose(xne, pop["xne"], rtol=1e-10)
     np.testing.assert_allclose(ka, rk, rtol=1e-9)
     np.testing.assert_allclose(sg, rs, rtol=1e-10)
