@@ -369,3 +369,40 @@ def atlas_finish(model, acc, iteration, store):
     store.norm = [s.zerot, s.slopet, s.zerop, s.slopep]
     model["pradk0"] = s.pradk0
     return err, out
+
+
+def _tcorr_for(store, t, p, abross, grav, keep):
+    """A _Tcorr over (t, p, abross) carrying the ROSSTAB store; arrays kept alive in keep."""
+    n = np.asarray(t).size
+    cols = {k: np.zeros(n) for k in ("t", "rhox", "p", "xne", "abross", "prad", "vturb", "pturb", "tauros",
+                                     "accrad", "raden", "oldt1", "rjmins", "rdabh", "rdiagj", "flxrad",
+                                     "h_total", "flxerr", "dtflux", "dtlamb", "dtsurf", "t1")}
+    cols["t"][:], cols["p"][:], cols["abross"][:] = t, p, abross
+    keep.append(cols)
+    return _Tcorr(n, 1, 0.0, float(grav), 0.0, *[_ptr(cols[k]) for k in cols], store.n, store.maxtab,
+                  *store.norm, _ptr(store.t), _ptr(store.p), _ptr(store.k))
+
+
+def rosstab_store(store, t, p, abross):
+    """ROSSTAB store (IROSSTAB = 1) of one model's (T, P, ABROSS) into store."""
+    keep = []
+    s = _tcorr_for(store, t, p, abross, 0.0, keep)
+    L = lib()
+    L.orc_rosstab_store.argtypes = [ctypes.POINTER(_Tcorr)]
+    L.orc_rosstab_store(ctypes.byref(s))
+    store.n = s.nross
+    store.norm = [s.zerot, s.slopet, s.zerop, s.slopep]
+
+
+def ttaup(store, t, tau, grav, prad):
+    """TTAUP: hydrostatic P(tau) for T(tau) with kappa_R from the ROSSTAB store.
+    Returns (abstd, ptotal, p)."""
+    keep = []
+    n = np.asarray(t).size
+    s = _tcorr_for(store, t, np.zeros(n), np.zeros(n), grav, keep)
+    t, tau, prad = _d(t), _d(tau), _d(prad)
+    ab, pt, po = np.zeros(n), np.zeros(n), np.zeros(n)
+    L = lib()
+    L.orc_ttaup.argtypes = [ctypes.POINTER(_Tcorr)] + [ctypes.c_void_p] * 6 + [ctypes.c_int]
+    L.orc_ttaup(ctypes.byref(s), _ptr(t), _ptr(tau), _ptr(ab), _ptr(pt), _ptr(po), _ptr(prad), n)
+    return ab, pt, po

@@ -13,6 +13,11 @@ modified).  Writes tests/golden/reference_tables.npz with:
   awei, lwei     Weideman N=32 coefficients (synthe_module.f90:91-126), kept
                  only to pin the product's own derivation of them
   wavetab        KAPCONT's 361-point continuum-cutoff grid (atlas12_modules.f90:1811-1857)
+  deck           the reference's converged solar model (workdir/ap00t5777g4.44at12.dat,
+                 Teff 5777 K, log g 4.44, 72 depths, iteration 45): READ DECK6
+                 columns RHOX, T, P, XNE, ABROSS, ACCRAD, VTURB as printed, [72, 7],
+                 plus deck_pradk = PRADK -- output of the reference itself, used
+                 to pin INTEG / ROSSTAB / TTAUP
 
 Usage:  python tests/golden/make_golden.py [reference_root]
 """
@@ -54,6 +59,16 @@ def fortran_array(src, name, count):
     return vals
 
 
+def read_deck(path):
+    """READ DECK6 block and PRADK of an ATLAS12 model file."""
+    lines = open(path).read().splitlines()
+    i = next(k for k, l in enumerate(lines) if l.startswith("READ DECK6"))
+    n = int(lines[i].split()[2].rstrip(","))
+    rows = np.array([[float(x) for x in lines[i + 1 + j].split()[:7]] for j in range(n)])
+    pradk = float(next(l for l in lines if l.startswith("PRADK")).split()[1])
+    return rows, np.array([pradk])
+
+
 def main():
     mod = open(os.path.join(ROOT, "src", "atlas12_modules.f90")).read()
     syn = open(os.path.join(ROOT, "src", "synthe_module.f90")).read()
@@ -69,6 +84,7 @@ def main():
         lwei=np.array([float(re.search(r"LWEI = ([0-9.D+-]+)", syn).group(1).replace("D", "e"))]),
         wavetab=fortran_array(mod, "WAVETAB(NWAVE) =", 361),
     )
+    out["deck"], out["deck_pradk"] = read_deck(os.path.join(ROOT, "workdir", "ap00t5777g4.44at12.dat"))
     np.savez(os.path.join(HERE, "reference_tables.npz"), **out)
     for k, v in out.items():
         print(k, v.shape)

@@ -152,3 +152,36 @@ def test_synthe_grid_and_binning(po):
     for i in (1, 17, 12346):
         w = g["wbegin"] * g["ratio"] ** (i - 1)
         assert po.nbuff(w, g["ratiolg"], g["ixwlbeg"]) == i
+
+
+# ---- pins against the reference's own converged solar model (READ DECK6 of
+# workdir/ap00t5777g4.44at12.dat: Teff 5777 K, log g 4.44, 72 depths) ----
+
+def test_integ_reproduces_reference_tau_grid(po, tables):
+    """ROSS(3)'s TAUROS = INTEG(RHOX, ABROSS, ABROSS(1)*RHOX(1)) on the converged
+    deck returns the standard grid log tau = -6.875 + 0.125 (j-1) that the
+    reference remapped the model onto (TAU1LG/STEPLG, atlas12_modules.f90:1792),
+    to the deck's print precision (4 digits of ABROSS)."""
+    d = tables["deck"]
+    rhox, ab = d[:, 0], d[:, 4]
+    tau = po.integ(rhox, ab, ab[0] * rhox[0])
+    std = -6.875 + 0.125 * np.arange(d.shape[0])
+    assert np.max(np.abs(np.log10(tau) - std)) < 2e-4
+
+
+def test_ttaup_reproduces_reference_deck(po, tables):
+    """TTAUP (atlas12_modules.f90:6303-6523) with ROSSTAB holding the deck's
+    own (T, P, ABROSS) integrates hydrostatic equilibrium on the standard tau
+    grid back to the deck's P and RHOX (printed to 4 digits) and looks up its
+    ABROSS."""
+    d = tables["deck"]
+    rhox, t, p, ab = d[:, 0], d[:, 1], d[:, 2], d[:, 4]
+    g = 10.0 ** 4.44
+    store = po.RossStore()
+    po.rosstab_store(store, t, p, ab)
+    assert store.n == d.shape[0]
+    tau = 10.0 ** (-6.875 + 0.125 * np.arange(d.shape[0]))
+    abstd, ptot, pout = po.ttaup(store, t, tau, g, np.zeros_like(t))
+    assert np.max(np.abs(pout / p - 1.0)) < 3e-3
+    assert np.max(np.abs(ptot / (g * rhox) - 1.0)) < 3e-3
+    assert np.max(np.abs(abstd / ab - 1.0)) < 2e-3
