@@ -11,7 +11,8 @@ import weakref
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libatlasgpu.so")
+# ATLASGPU_LIB selects another build of the same library (e.g. an instrumented one)
+LIB_PATH = os.environ.get("ATLASGPU_LIB") or os.path.join(HERE, "libatlasgpu.so")
 
 OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ENONFINITE, ESTATE = 0, -1, -2, -3, -4, -5, -6
 PREC_FP64, PREC_MIXED = 0, 1

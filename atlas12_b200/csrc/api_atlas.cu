@@ -137,16 +137,17 @@ int rt_launch(atlasgpu_ctx* ctx, RtArgs& a, bool surr, double* d_sum, int* nwarp
   }
   {
     Timer tm(ctx, "atlas_reduce");
-    k_atlas_reduce<<<(kAcc * a.kw + 1 + 127) / 128, 128, 0, ctx->stream>>>(part, nwl, a.kw, 0, d_sum);
+    launch_reduce(part, nwl, a.kw, d_sum, ctx->stream);
     CKL(ctx);
   }
   if (nwarps_out) *nwarps_out = nwl;
   return 0;
 }
 
-__global__ void k_finish_one(ModelState* s, double* acc, int kw, int n, int iter, double teff,
-                             double grav, RossStore* R, double* work) {
-  if (blockIdx.x == 0) w_atlas_finish(*s, acc, kw, n, iter, teff, grav, R, work, threadIdx.x & 31);
+__global__ void __launch_bounds__(kFinThreads) k_finish_one(ModelState* s, double* acc, int kw, int n, int iter,
+                                                             double teff, double grav, RossStore* R) {
+  extern __shared__ __align__(16) double fin_smem[];
+  if (blockIdx.x == 0) b_atlas_finish(s, acc, kw, n, iter, teff, grav, R, fin_smem);
 }
 
 }  // namespace
@@ -279,6 +280,10 @@ int atlasgpu_atlas_finish(atlasgpu_ctx* ctx, atlasgpu_finish_state* st, const at
       st->ross_max < 1 || st->ross_n < 0 || st->ross_n > st->ross_max)
     return fail(ctx, ATLASGPU_EINVAL, "atlas_finish: bad argument");
   const int n = st->nrhox, kw = n;
+  const size_t fsm = fin_smem_bytes(kw, st->ross_max);
+  if (fsm > (size_t)ctx->smem_optin)
+    return fail(ctx, ATLASGPU_EINVAL, "atlas_finish: ross_max %d exceeds the on-chip ROSSTAB capacity",
+                st->ross_max);
   double* hv[17] = {st->t, st->rhox, st->p, st->xne, st->abross, st->prad, st->vturb, st->pturb,
                     st->tauros, st->accrad, st->raden, st->oldt1, st->flxerr, st->dtflux, st->dtlamb,
                     st->dtsurf, st->t1};
@@ -289,13 +294,13 @@ int atlasgpu_atlas_finish(atlasgpu_ctx* ctx, atlasgpu_finish_state* st, const at
     if (!ha[q]) return fail(ctx, ATLASGPU_EINVAL, "atlas_finish: null accumulator %d", q);
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
-  double *d_arr, *d_acc, *d_work, *d_ross;
+  double *d_arr, *d_acc, *d_ross;
   ModelState* d_ms;
   RossStore* d_rs;
   int r;
   const size_t nr = (size_t)st->ross_max;
   if ((r = bufT(ctx, "fin_arr", 17 * kw, &d_arr)) || (r = bufT(ctx, "fin_acc", kAcc * kw + 1, &d_acc)) ||
-      (r = bufT(ctx, "fin_work", 24 * kw, &d_work)) || (r = bufT(ctx, "fin_ross", 3 * nr, &d_ross)) ||
+      (r = bufT(ctx, "fin_ross", 3 * nr, &d_ross)) ||
       (r = bufT(ctx, "fin_ms", 1, &d_ms)) || (r = bufT(ctx, "fin_rs", 1, &d_rs)))
     return r;
   std::vector<double> h(17 * kw), ha2(kAcc * kw + 1);
@@ -319,7 +324,8 @@ int atlasgpu_atlas_finish(atlasgpu_ctx* ctx, atlasgpu_finish_state* st, const at
   CK(cudaMemcpyAsync(d_rs, &R, sizeof R, cudaMemcpyHostToDevice, s));
   {
     Timer tm(ctx, "atlas_finish");
-    k_finish_one<<<1, 32, 0, s>>>(d_ms, d_acc, kw, n, st->iter, st->teff, st->grav, d_rs, d_work);
+    CK(cudaFuncSetAttribute(k_finish_one, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+    k_finish_one<<<1, kFinThreads, fsm, s>>>(d_ms, d_acc, kw, n, st->iter, st->teff, st->grav, d_rs);
     CKL(ctx);
   }
   CK(cudaMemcpyAsync(h.data(), d_arr, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -31,7 +31,7 @@ struct atlasgpu_model {
   int32_t* linedata;
   AtlasLine* lines;
   double* xl;            // [kw][numnu]
-  double *partial, *sum, *work, *hsurf;
+  double *partial, *sum, *hsurf;
   double *h0, *h1, *h2, *ross;  // ross: ROSSTAB points [3][kRossMax]
   RossStore* R;                  // device
   int* iter_dev;         // iterations completed
@@ -90,13 +90,15 @@ __global__ void k_model_kapcont(const double* cutwave, int nwave, const double* 
   }
 }
 
-__global__ void k_model_finish(ModelState* ms, double* acc, int kw, int n, int* iter_dev, double teff,
-                               double grav, RossStore* R, double* work, double* maxerr) {
+__global__ void __launch_bounds__(kFinThreads) k_model_finish(ModelState* ms, double* acc, int kw, int n,
+                                                               int* iter_dev, double teff, double grav,
+                                                               RossStore* R, double* maxerr) {
+  extern __shared__ __align__(16) double fin_smem[];
   if (blockIdx.x != 0) return;
-  const int lane = threadIdx.x & 31;
   const int iter = *iter_dev + 1;
-  const double e = w_atlas_finish(*ms, acc, kw, n, iter, teff, grav, R, work, lane);
-  if (lane == 0) {
+  __syncthreads();  // every thread has read the count before thread 0 advances it
+  const double e = b_atlas_finish(ms, acc, kw, n, iter, teff, grav, R, fin_smem);
+  if (threadIdx.x == 0) {
     *maxerr = e;
     *iter_dev = iter;
   }
@@ -159,13 +161,13 @@ int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
   }
   {
     Timer tm(ctx, "atlas_reduce");
-    k_atlas_reduce<<<(kAcc * m->kw + 1 + 127) / 128, 128, 0, s>>>(m->partial, m->nwl, m->kw, 0, m->sum);
+    launch_reduce(m->partial, m->nwl, m->kw, m->sum, s);
     CKL(ctx);
   }
   {
     Timer tm(ctx, "atlas_finish");
-    k_model_finish<<<1, 32, 0, s>>>(m->ms, m->sum, m->kw, m->nrhox, m->iter_dev, m->teff, m->grav, m->R,
-                                    m->work, m->maxerr_dev);
+    k_model_finish<<<1, kFinThreads, fin_smem_bytes(m->kw, kRossMax), s>>>(
+        m->ms, m->sum, m->kw, m->nrhox, m->iter_dev, m->teff, m->grav, m->R, m->maxerr_dev);
     CKL(ctx);
   }
   ctx->timing = was;
@@ -264,7 +266,7 @@ int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlas
       (r = dalloc(ctx, &m->cutwave, m->nwave)) || (r = dalloc(ctx, &m->tabcont, (size_t)(m->nwave + 1) * kw)) ||
       (r = dalloc(ctx, &m->iwavetab, m->nwave + 1)) || (r = dalloc(ctx, &m->linedata, (size_t)m->nlines * 4)) ||
       (r = dalloc(ctx, &m->lines, (size_t)m->nlines)) || (r = dalloc(ctx, &m->xl, (size_t)kw * m->numnu)) ||
-      (r = dalloc(ctx, &m->sum, kAcc * kw + 1)) || (r = dalloc(ctx, &m->work, 24 * kw)) ||
+      (r = dalloc(ctx, &m->sum, kAcc * kw + 1)) ||
       (r = dalloc(ctx, &m->hsurf, m->numnu)) || (r = dalloc(ctx, &m->h0, 2001)) || (r = dalloc(ctx, &m->h1, 2001)) ||
       (r = dalloc(ctx, &m->h2, 2001)) || (r = dalloc(ctx, &m->ross, nr)) || (r = dalloc(ctx, &m->R, 1)) || (r = dalloc(ctx, &m->iter_dev, 1)) ||
       (r = dalloc(ctx, &m->maxerr_dev, 1)) || (r = dalloc(ctx, &m->cnt, 2))) {
@@ -285,6 +287,13 @@ int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlas
     return r;
   }
   CK(cudaFuncSetAttribute(k_atlas_rt<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->smem_rt));
+  if (fin_smem_bytes(kw, kRossMax) > (size_t)ctx->smem_optin) {
+    atlasgpu_model_destroy(ctx, m);
+    return fail(ctx, ATLASGPU_EINVAL, "model_create: finish needs %zu B of shared memory",
+                fin_smem_bytes(kw, kRossMax));
+  }
+  CK(cudaFuncSetAttribute(k_model_finish, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)fin_smem_bytes(kw, kRossMax)));
   cudaStream_t s = ctx->stream;
   // state vectors: t, rhox, p, xne, abross, prad, vturb, pturb, tauros, accrad, raden, oldt1, flxerr,
   // dtflux, dtlamb, dtsurf, t1
@@ -446,7 +455,7 @@ int atlasgpu_model_destroy(atlasgpu_ctx* ctx, atlasgpu_model* m) {
   if (m->graph) cudaGraphDestroy(m->graph);
   void* ps[] = {m->state, m->ms, m->xnfdop, m->dopple, m->xne_eos, m->txnxn, m->hkt, m->hckt, m->rho, m->cc,
                 m->waveset, m->rcoset, m->cutwave, m->tabcont, m->iwavetab, m->linedata, m->lines, m->xl,
-                m->partial, m->sum, m->work, m->hsurf, m->h0, m->h1, m->h2, m->ross, m->R, m->iter_dev,
+                m->partial, m->sum, m->hsurf, m->h0, m->h1, m->h2, m->ross, m->R, m->iter_dev,
                 m->maxerr_dev, m->cnt};
   for (void* p : ps)
     if (p) cudaFree(p);

@@ -80,7 +80,7 @@ int atlasgpu_atlas_rt_pass_noalloc(atlasgpu_ctx* ctx, int numnu, const double* d
            d_rhox, d_t, d_hkt, teff, npw, partial, d_hsurf, nullptr};
   k_atlas_rt<false><<<blocks, 32 * nwarp, smem, ctx->stream>>>(a);
   CKL(ctx);
-  k_atlas_reduce<<<(kAcc * kw + 1 + 127) / 128, 128, 0, ctx->stream>>>(partial, nwl, kw, 0, d_sums);
+  launch_reduce(partial, nwl, kw, d_sums, ctx->stream);
   CKL(ctx);
   return ATLASGPU_OK;
 }

@@ -386,16 +386,44 @@ static __global__ void __launch_bounds__(128) k_atlas_rt(RtArgs a) {
   if (lane == 0) out[kAcc * a.kw] = pradk0;
 }
 
-// fixed-order sum of the per-warp partials: out[kAcc*kw + 1]
-static __global__ void k_atlas_reduce(const double* __restrict__ partial, int nwarps, int kw, int n,
-                               double* __restrict__ out) {
+// fixed-order sum of the per-warp partials: out[kAcc*kw + 1].  A block owns
+// 32 consecutive sums (threadIdx.x) and splits the rows over 32 row groups
+// (threadIdx.y: rows y, y+32, ...); the 32 group sums are then added in group
+// order.  The order is fixed by the launch shape, so the result does not
+// depend on scheduling.
+constexpr int kRedCols = 32, kRedRows = 32;
+static __global__ void __launch_bounds__(kRedCols* kRedRows)
+    k_atlas_reduce(const double* __restrict__ partial, int nwarps, int kw, int n, double* __restrict__ out) {
+  __shared__ double s[kRedRows][kRedCols + 1];
   const int stride = kAcc * kw + 1;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < stride; e += gridDim.x * blockDim.x) {
-    double s = 0.0;
-    for (int w = 0; w < nwarps; ++w) s += partial[(size_t)w * stride + e];
-    out[e] = s;
+  const int e = blockIdx.x * kRedCols + threadIdx.x;
+  double v = 0.0;
+  if (e < stride) {
+    int w = threadIdx.y;
+    // four independent loads in flight per step, added in row order
+    for (; w + 3 * kRedRows < nwarps; w += 4 * kRedRows) {
+      const double a0 = partial[(size_t)w * stride + e];
+      const double a1 = partial[(size_t)(w + kRedRows) * stride + e];
+      const double a2 = partial[(size_t)(w + 2 * kRedRows) * stride + e];
+      const double a3 = partial[(size_t)(w + 3 * kRedRows) * stride + e];
+      v = (((v + a0) + a1) + a2) + a3;
+    }
+    for (; w < nwarps; w += kRedRows) v += partial[(size_t)w * stride + e];
+  }
+  s[threadIdx.y][threadIdx.x] = v;
+  __syncthreads();
+  if (threadIdx.y == 0 && e < stride) {
+    double t = 0.0;
+    for (int y = 0; y < kRedRows; ++y) t += s[y][threadIdx.x];
+    out[e] = t;
   }
   (void)n;
+}
+
+inline void launch_reduce(const double* partial, int nwarps, int kw, double* out, cudaStream_t st) {
+  const int stride = kAcc * kw + 1;
+  k_atlas_reduce<<<(stride + kRedCols - 1) / kRedCols, dim3(kRedCols, kRedRows), 0, st>>>(partial, nwarps, kw, 0,
+                                                                                            out);
 }
 
 }  // namespace atlasgpu

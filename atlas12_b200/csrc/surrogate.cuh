@@ -33,9 +33,6 @@ static __constant__ double kMol[kNMol][4] = {{41, 13.02, -7.0, 8.0},
                                       {44, 17.01, -7.5, 9.0},
                                       {45, 63.87, -9.0, 14.0}};
 
-__device__ inline double saha(double t, double ne, double chi, double u1, double u2) {
-  return 2.4147e15 * pow(t, 1.5) / fmax(ne, 1.0) * (2.0 * u2 / u1) * exp(-chi * kEvErg / (kKbol * t));
-}
 
 // per-depth continuum coefficients: kabs(w) = hm*abf(w) + ff*(w/1000)^2 +
 // sum_n pop[n]*sig_n(w) + 1e-12 ;  sigma(w) = es + ray*5.8e-24*(121.6/max(w,125))^4
@@ -57,23 +54,38 @@ struct EosOut {
 // column (depth j).  Returns EOS fields and fills the continuum coefficients.
 __device__ inline EosOut surrogate_depth(double t, double p, double vturb_cms, int j, int kw,
                                          double* xnfdop, double* dopple, ContCoef* cc) {
-  const double ntot = p / (kKbol * t);
+  // the T-only factors of every Saha ratio, evaluated once (same operand
+  // order as surrogate._saha, so the ratios are the same numbers)
+  const double st = 2.4147e15 * pow(t, 1.5);
+  const double kt = kKbol * t;
+  const double bh = (2.0 * 1.0 / 2.0), eh = exp(-13.598 * kEvErg / kt);
+  double bm[kNMetal], em[kNMetal], am[kNMetal];
+#pragma unroll
+  for (int m = 0; m < kNMetal; ++m) {
+    bm[m] = 2.0 * kMetal[m][5] / kMetal[m][4];
+    em[m] = exp(-kMetal[m][2] * kEvErg / kt);
+    am[m] = exp10(kMetal[m][3] - 12.0);
+  }
+  const double ntot = p / kt;
   double ne = fmax(ntot * 1e-4, 1.0);
   double nh = 0, xh = 0;
   for (int it = 0; it < 30; ++it) {
     nh = ntot / (1.1 + ne / ntot);
-    const double rh = saha(t, ne, 13.598, 2.0, 1.0);
+    const double sn = st / fmax(ne, 1.0);
+    const double rh = sn * bh * eh;
     xh = rh / (1.0 + rh);
     double sm = 0.0;
+#pragma unroll
     for (int m = 0; m < kNMetal; ++m) {
-      const double rm = saha(t, ne, kMetal[m][2], kMetal[m][4], kMetal[m][5]);
-      sm += exp10(kMetal[m][3] - 12.0) * (rm / (1.0 + rm));
+      const double rm = sn * bm[m] * em[m];
+      sm += am[m] * (rm / (1.0 + rm));
     }
     const double ne_new = nh * xh + nh * sm + 1.0;
     ne = sqrt(ne * ne_new);
   }
   nh = ntot / (1.1 + ne / ntot);
   const double rho = nh * 1.4 * kAmu;
+  const double sn = st / fmax(ne, 1.0);
   auto dop = [&](double m) { return sqrt(2.0 * kKbol * t / (m * kAmu) + vturb_cms * vturb_cms) / kClight; };
   auto put = [&](int nel, double xnfp, double d) {
     xnfdop[(size_t)(nel - 1) * kw + j] = xnfp / d / rho;
@@ -82,13 +94,15 @@ __device__ inline EosOut surrogate_depth(double t, double p, double vturb_cms, i
   const double dh = dop(1.008);
   put(1, nh * (1 - xh) / 2.0, dh);
   put(2, nh * xh, dh);
+#pragma unroll
   for (int m = 0; m < kNMetal; ++m) {
-    const double r = saha(t, ne, kMetal[m][2], kMetal[m][4], kMetal[m][5]);
-    const double n = nh * exp10(kMetal[m][3] - 12.0);
+    const double r = sn * bm[m] * em[m];
+    const double n = nh * am[m];
     const int z = (int)kMetal[m][0];
     const double d = dop(kMetal[m][1]);
     put((z - 1) * 6 + 1, n / (1.0 + r) / kMetal[m][4] * kAtlasLinePop, d);
     put((z - 1) * 6 + 2, n * r / (1.0 + r) / kMetal[m][5] * kAtlasLinePop, d);
+    cc->mbf[m] = nh * am[m] / (1.0 + r) * kMbfSigma / rho;
   }
   for (int m = 0; m < kNMol; ++m) {
     const int slot = (int)kMol[m][0];
@@ -105,10 +119,6 @@ __device__ inline EosOut surrogate_depth(double t, double p, double vturb_cms, i
     cc->pop[n - 1] = nh1 * 2.0 * n * n * exp(-13.598 * (1.0 - 1.0 / (n * n)) * kEvErg / (kKbol * t)) / 2.0 / rho;
   cc->es = 6.6524587051e-25 * ne / rho;
   cc->ray = nh1 / rho;
-  for (int m = 0; m < kNMetal; ++m) {
-    const double r = saha(t, ne, kMetal[m][2], kMetal[m][4], kMetal[m][5]);
-    cc->mbf[m] = nh * exp10(kMetal[m][3] - 12.0) / (1.0 + r) * kMbfSigma / rho;
-  }
   EosOut o{ne, rho, nh, xh};
   return o;
 }
@@ -116,7 +126,7 @@ __device__ inline EosOut surrogate_depth(double t, double p, double vturb_cms, i
 __device__ __forceinline__ void surrogate_kapp(const ContCoef& c, double w, double& kabs, double& sigma) {
   double x = w / 1642.0;
   x = x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x);
-  const double abf = 4.0e-17 * 6.0 * pow(x, 1.5) * pow(1.0 - x, 1.5) * 4.0;
+  const double abf = 4.0e-17 * 6.0 * (x * sqrt(x)) * ((1.0 - x) * sqrt(1.0 - x)) * 4.0;
   double k = c.hm * abf + c.ff * (w / 1000.0) * (w / 1000.0);
   const double edges[3] = {91.175, 364.70, 820.6};
 #pragma unroll

@@ -1,9 +1,11 @@
 // tcorr.cuh -- end of an ATLAS12 iteration on the device: ROSS(3), RADIAP(3)
 // and the radiative branch of TCORR(3) with TTAUP's RHOX correction and the
-// remap onto the standard Rosseland grid.  One warp per model: this is a
-// 72-depth serial recurrence (atlas12_modules.f90 :5193-5198, :5108-5135,
-// :2528-2977, :6303-6523), cheap next to the frequency loop, and keeping it
-// on the device lets a whole iteration run as one captured CUDA graph.
+// remap onto the standard Rosseland grid.  One CTA per model: a 72-depth
+// serial recurrence (atlas12_modules.f90 :5193-5198, :5108-5135, :2528-2977,
+// :6303-6523) run by one thread on shared-memory copies of the model, and the
+// two TTAUP integrations run side by side with their ROSSTAB searches split
+// over a thread group.  Keeping it on the device lets a whole iteration run
+// as one captured CUDA graph.
 //
 // Radiative branch: IFCONV = 0 (no CONVEC, CNVFLX = 0, CZ_CONSTRUCT returns
 // at once), no smoothing (J1SMOOTH = 0), USE_DTGRAD = .FALSE.  TTAUP's
@@ -14,6 +16,7 @@
 namespace atlasgpu {
 
 constexpr double kSigmaSB = 5.670374419e-5;
+constexpr int kAcc8 = 8;  // mode-2 sums per depth (RJMINS ... ABROSS), then PRADK0
 
 // ---- serial numerics (one thread) -------------------------------------
 __device__ inline void s_parcoe(const double* f, const double* x, double* a, double* b, double* c,
@@ -175,6 +178,35 @@ __device__ inline void s_rosstab_store(RossStore& R, const double* t, const doub
     R.n = R.n + 1;
   }
 }
+// ---- the finish as one CTA ---------------------------------------------
+// kFinThreads threads: thread 0 runs the serial recurrences on shared-memory
+// copies of the model; the two TTAUP integrations (current and corrected
+// T) run at the same time, one per group of kFinGroup threads, each ROSSTAB
+// lookup split across its group.  Every thread of a group runs TTAUP's
+// control flow on identical values (a lookup's result is folded in the same
+// order by every thread), so the groups need no broadcast of scalars.
+constexpr int kFinThreads = 512;
+constexpr int kFinGroup = 256;
+constexpr int kFinGroupWarps = kFinGroup / 32;
+constexpr int kFinVec = 17;   // model vectors kept on chip
+constexpr int kFinWork = 26;  // scratch vectors
+
+// per-group fold buffer of the per-warp quadrant minima (double-buffered so
+// that one barrier per lookup suffices)
+struct FinFold {
+  double r[2][kFinGroupWarps][4];
+  int i[2][kFinGroupWarps][4];
+};
+
+// shared-memory bytes of b_atlas_finish for kw depths and cap ROSSTAB points
+__host__ __device__ inline size_t fin_smem_bytes(int kw, int cap) {
+  return sizeof(double) * ((size_t)(kFinVec + kFinWork + kAcc8) * kw + 1 + 3 * (size_t)cap) +
+         2 * sizeof(FinFold) + 64;
+}
+
+__device__ __forceinline__ void group_bar(int id) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kFinGroup) : "memory");
+}
 
 // lexicographic (r2, index) minimum: the sequential scan keeps the first minimum
 __device__ __forceinline__ void wmin2(double& r, int& i) {
@@ -189,13 +221,23 @@ __device__ __forceinline__ void wmin2(double& r, int& i) {
   }
 }
 
-// ROSSTAB(T, P, V) lookup: all 32 lanes scan, every lane returns the value
-__device__ inline double w_rosstab(const RossStore& R, double temp, double pres, int lane) {
+// ROSSTAB(T, P, V) lookup (atlas12_modules.f90:5937-6228): nearest stored point
+// in each (log T, log P) quadrant, bilinear blend of the four (inverse-
+// distance weights when a quadrant is empty).  R's arrays are in shared
+// memory; every thread of the group returns the value.
+struct RossView {
+  int n;
+  double zerot, slopet, zerop, slopep;
+  const double *t, *p, *k;
+};
+
+__device__ inline double b_rosstab(const RossView& R, double temp, double pres, int gtid, FinFold& fold,
+                                   int& parity, int bar) {
   const double tl = (log10(temp) - R.zerot) / R.slopet;
   const double pl = (log10(pres) - R.zerop) / R.slopep;
   double r[4] = {1e30, 1e30, 1e30, 1e30};  // PP, PM, MP, MM
   int id[4] = {1 << 30, 1 << 30, 1 << 30, 1 << 30};
-  for (int i = lane; i < R.n; i += 32) {
+  for (int i = gtid; i < R.n; i += kFinGroup) {
     const double dt = R.t[i] - tl, dp = R.p[i] - pl;
     const double r2 = dt * dt + dp * dp;
     const int q = (dt >= 0.0) ? (dp >= 0.0 ? 0 : 1) : (dp >= 0.0 ? 2 : 3);
@@ -205,10 +247,32 @@ __device__ inline double w_rosstab(const RossStore& R, double temp, double pres,
     }
   }
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    wmin2(r[q], id[q]);
-    if (id[q] == (1 << 30)) id[q] = 0;
+  for (int q = 0; q < 4; ++q) wmin2(r[q], id[q]);
+  const int w = gtid >> 5;
+  if ((gtid & 31) == 0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      fold.r[parity][w][q] = r[q];
+      fold.i[parity][w][q] = id[q];
+    }
   }
+  group_bar(bar);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    double rr = fold.r[parity][0][q];
+    int ii = fold.i[parity][0][q];
+    for (int v = 1; v < kFinGroupWarps; ++v) {
+      const double orr = fold.r[parity][v][q];
+      const int oi = fold.i[parity][v][q];
+      if (orr < rr || (orr == rr && oi < ii)) {
+        rr = orr;
+        ii = oi;
+      }
+    }
+    r[q] = rr;
+    id[q] = ii == (1 << 30) ? 0 : ii;
+  }
+  parity ^= 1;
   double res;
   if (id[0] && id[1] && id[2] && id[3]) {
     const double Tpp = R.t[id[0] - 1], Ppp = R.p[id[0] - 1], Rpp = R.k[id[0] - 1];
@@ -230,14 +294,13 @@ __device__ inline double w_rosstab(const RossStore& R, double temp, double pres,
   return exp10(res);
 }
 
-// TTAUP (radiative: P_turb = 0).  Every lane of the warp runs it on identical
-// data (the ROSSTAB scans are split across lanes); values are carried in
-// registers and only lane 0 stores the output arrays, so no lane ever reads
-// an element another lane may be rewriting.
-__device__ inline void w_ttaup(const RossStore& R, double g, const double* tin, const double* tau,
+// TTAUP (atlas12_modules.f90:6303-6523; radiative: P_turb = 0) by one group.
+// Values are carried in registers; thread 0 of the group stores the outputs.
+__device__ inline void b_ttaup(const RossView& R, double g, const double* tin, const double* tau,
                                double* abstd, double* ptotal, double* pout, const double* prad, int n,
-                               int lane) {
+                               int gtid, FinFold& fold, int bar) {
   const double RELAX[4] = {0.5, 0.3, 0.1, 0.05};
+  int parity = 0;
   const double dlgtau = log(tau[1] / tau[0]);
   const double prad0 = prad[0];
   double plog1 = 0, plog2 = 0, plog3 = 0, plog4 = 0, dplog1 = 0, dplog2 = 0, dplog3 = 0;
@@ -262,7 +325,7 @@ __device__ inline void w_ttaup(const RossStore& R, double g, const double* tin, 
         poj = ptj * 1.0e-4;
         if (poj <= 0.0) poj = 1.0e-10;
       }
-      abj = w_rosstab(R, tj, poj, lane);
+      abj = b_rosstab(R, tj, poj, gtid, fold, parity, bar);
       if (J == 1) ab0 = abj;
       dplog = g / abj * tauj / ptj * dlgtau;
       dplog = fmax(0.0, fmin(10.0, dplog));
@@ -302,7 +365,7 @@ __device__ inline void w_ttaup(const RossStore& R, double g, const double* tin, 
       ptj = exp(plog);
       poj = ptj + (prad0 - pradj);
       if (poj <= 0.0) poj = fmax(ptj * 1.0e-4, 1.0e-10);
-      abj = w_rosstab(R, tj, poj, lane);
+      abj = b_rosstab(R, tj, poj, gtid, fold, parity, bar);
       if (J == 1) ab0 = abj;
       dplog = g / abj * tauj / ptj * dlgtau;
       dplog = fmax(0.0, fmin(10.0, dplog));
@@ -313,7 +376,7 @@ __device__ inline void w_ttaup(const RossStore& R, double g, const double* tin, 
       ptj = exp(plog);
       poj = ptj;
       if (poj > 0.0) {
-        ab0 = w_rosstab(R, tin[0], poj, lane);
+        ab0 = b_rosstab(R, tin[0], poj, gtid, fold, parity, bar);
         abj = ab0;
         plog = log(g / ab0 * tau[0]);
         ptj = exp(plog);
@@ -322,7 +385,7 @@ __device__ inline void w_ttaup(const RossStore& R, double g, const double* tin, 
       dplog = g / ab0 * tau[0] / ptj * dlgtau;
       dplog = fmax(0.0, fmin(10.0, dplog));
     }
-    if (lane == 0) {
+    if (gtid == 0) {
       abstd[j] = abj;
       ptotal[j] = ptj;
       pout[j] = poj;
@@ -345,18 +408,45 @@ struct ModelState {
   double maxerr;
 };
 
-// finish one iteration: acc = the reduced mode-2 sums [kAcc*kw + 1]
-// (order rjmins, rdabh, rdiagj, flxrad, raden, h_total, accrad, abross, pradk0)
-// Called by all 32 lanes of one warp: lane 0 runs the serial recurrences,
-// the warp runs the two TTAUP integrations together (ROSSTAB scans split
-// across lanes).  R lives in device memory; the maximum |FLXERR| is returned
-// to every lane.
-__device__ inline double w_atlas_finish(ModelState& s, double* acc, int kw, int n, int iter,
-                                        double teff, double grav, RossStore* R, double* work,
-                                        int lane) {
+// finish one iteration.  gacc = the reduced mode-2 sums [kAcc*kw + 1] (order
+// rjmins, rdabh, rdiagj, flxrad, raden, h_total, accrad, abross, pradk0;
+// rdabh is updated in place as TCORR(3) does); gms / gR in device memory,
+// updated in place.  Launched with kFinThreads threads and
+// fin_smem_bytes(kw, gR->maxtab) bytes of dynamic shared memory (smem).
+// Returns max |FLXERR| (percent) to every thread.
+__device__ inline double b_atlas_finish(ModelState* gms, double* gacc, int kw, int n, int iter, double teff,
+                                        double grav, RossStore* gR, double* smem) {
+  const int tid = threadIdx.x;
   const double FOUR_SIGMA_OVER_PI = 4.0 * kSigmaSB / kPi;
   const double FOURPI_OVER_C = 4.0 * kPi / kClight;
   const double FLUX = kSigmaSB * powi(teff, 4) / (4.0 * kPi);
+  const int cap = gR->maxtab;
+  // shared-memory layout
+  double* V = smem;                           // [kFinVec][kw]
+  double* acc = V + kFinVec * kw;             // [kAcc8*kw + 1]
+  double* work = acc + kAcc8 * kw + 1;        // [kFinWork][kw]
+  double* rt = work + kFinWork * kw;          // ROSSTAB [3][cap]
+  double* rp = rt + cap;
+  double* rk = rp + cap;
+  FinFold* fold = reinterpret_cast<FinFold*>(rk + cap);  // [2]
+  __shared__ double s_scal[8];  // zerot, slopet, zerop, slopep, maxerr, pradk0
+  __shared__ int s_n[2];        // ROSSTAB points before / after the store
+  double* gv[kFinVec] = {gms->t, gms->rhox, gms->p, gms->xne, gms->abross, gms->prad, gms->vturb, gms->pturb,
+                         gms->tauros, gms->accrad, gms->raden, gms->oldt1, gms->flxerr, gms->dtflux,
+                         gms->dtlamb, gms->dtsurf, gms->t1};
+  const int n0 = gR->n;
+  for (int e = tid; e < kFinVec * n; e += blockDim.x) V[(e / n) * kw + e % n] = gv[e / n][e % n];
+  for (int e = tid; e < kAcc8 * kw + 1; e += blockDim.x) acc[e] = gacc[e];
+  for (int e = tid; e < n0; e += blockDim.x) {
+    rt[e] = gR->t[e];
+    rp[e] = gR->p[e];
+    rk[e] = gR->k[e];
+  }
+  __syncthreads();
+  ModelState s;
+  double** f[kFinVec] = {&s.t, &s.rhox, &s.p, &s.xne, &s.abross, &s.prad, &s.vturb, &s.pturb, &s.tauros,
+                         &s.accrad, &s.raden, &s.oldt1, &s.flxerr, &s.dtflux, &s.dtlamb, &s.dtsurf, &s.t1};
+  for (int q = 0; q < kFinVec; ++q) *f[q] = V + q * kw;
   double* rjmins = acc + 0 * kw;
   double* rdabh = acc + 1 * kw;
   double* rdiagj = acc + 2 * kw;
@@ -365,128 +455,150 @@ __device__ inline double w_atlas_finish(ModelState& s, double* acc, int kw, int 
   double* h_total = acc + 5 * kw;
   double* accrad = acc + 6 * kw;
   double* abross = acc + 7 * kw;
-  double pradk0 = acc[8 * kw];
-  // scratch [24][kw]
-  double* W[24];
-  for (int q = 0; q < 24; ++q) W[q] = work + q * kw;
+  double* W[kFinWork];
+  for (int q = 0; q < kFinWork; ++q) W[q] = work + q * kw;
   double *wa = W[0], *wb = W[1], *wc = W[2], *dtdrhx = W[3], *dabros = W[4], *codrhx = W[5],
          *G = W[6], *gflux = W[7], *dtau = W[8], *flxdrv = W[9], *dum = W[10], *tinteg = W[11],
          *tplus = W[12], *taustd = W[13], *tnew1 = W[14], *tnew2 = W[15], *prdnew = W[16],
          *ab1 = W[17], *pt1 = W[18], *p1 = W[19], *pt2 = W[20], *ppp = W[21], *rrr = W[22],
-         *rmp = W[23];
-  double maxerr = 0.0;
-  if (lane == 0) {
-  // ROSS(3)
-  for (int j = 0; j < n; ++j) s.abross[j] = FOUR_SIGMA_OVER_PI * powi(s.t[j], 3) / abross[j];
-  s_integ(s.rhox, s.abross, s.tauros, n, s.abross[0] * s.rhox[0], wa, wb, wc);
-  s_rosstab_store(*R, s.t, s.p, s.abross, n);  // RX = ROSSTAB(0,0,0), atlas12c.f90:586
-  // RADIAP(3)
-  double errormax = 0.0;
-  for (int j = 0; j < n; ++j) {
-    s.raden[j] = raden[j] * FOURPI_OVER_C;
-    s.accrad[j] = accrad[j] * FOURPI_OVER_C;
-    if (h_total[j] / FLUX > 1.0) s.accrad[j] = s.accrad[j] * FLUX / h_total[j];
-    errormax = fmax(errormax, h_total[j] / FLUX);
-  }
-  pradk0 = pradk0 * FOURPI_OVER_C;
-  if (errormax > 1.0) pradk0 = pradk0 / errormax;
-  s.pradk0 = pradk0;
-  s_integ(s.rhox, s.accrad, s.prad, n, s.accrad[0] * s.rhox[0], wa, wb, wc);
-  // TCORR(3)
-  s_deriv(s.rhox, s.t, dtdrhx, n);
-  s_deriv(s.rhox, s.abross, dabros, n);
-  for (int j = 0; j < n; ++j) {
-    rdabh[j] = rdabh[j] - flxrad[j] * dabros[j] / fmax(s.abross[j], 1.0e-30);
-    codrhx[j] = (rdabh[j] + 0.0) / (flxrad[j] + 0.0);
-  }
-  codrhx[0] = 0.0;
-  codrhx[1] = 0.0;
-  s_integ(s.rhox, codrhx, G, n, 0.0, wa, wb, wc);
-  for (int j = 0; j < n; ++j) {
-    G[j] = exp(G[j]);
-    gflux[j] = G[j] * (flxrad[j] + 0.0 - FLUX) / (flxrad[j] + 0.0);
-  }
-  s_integ(s.tauros, gflux, dtau, n, 0.0, wa, wb, wc);
-  for (int j = 0; j < n; ++j) {
-    dtau[j] = dtau[j] / G[j];
-    dtau[j] = fmax(-s.tauros[j] / 3.0, fmin(s.tauros[j] / 3.0, dtau[j]));
-    s.dtflux[j] = -dtau[j] * dtdrhx[j] / fmax(s.abross[j], 1.0e-30);
-  }
-  const double MAX_DT = 0.04 * teff;
-  for (int j = 0; j < n; ++j) {
-    s.flxerr[j] = (flxrad[j] + 0.0 - FLUX) / FLUX * 100.0;
-    maxerr = fmax(maxerr, fabs(s.flxerr[j]));
-  }
-  s_deriv(s.tauros, s.flxerr, flxdrv, n);
-  for (int j = 0; j < n; ++j) {
-    // HRATIO = 0 in radiative layers: FLXDRV from the thermal imbalance
-    flxdrv[j] = rjmins[j] / fmax(s.abross[j], 1.0e-30) / FLUX * 100.0;
-    double d = -flxdrv[j] * FLUX / 100.0 / fmax(fabs(rdiagj[j]), 1.0e-30) * copysign(1.0, rdiagj[j]) *
-               fmax(s.abross[j], 1.0e-30);
-    s.dtlamb[j] = fmax(-MAX_DT, fmin(MAX_DT, d));
-  }
-  double dtsur = (FLUX - flxrad[0]) / FLUX * 0.25 * s.t[0];
-  dtsur = fmax(-MAX_DT, fmin(MAX_DT, dtsur));
-  for (int j = 0; j < n; ++j) dum[j] = s.dtflux[j] + s.dtlamb[j];
-  s_integ(s.tauros, dum, tinteg, n, 0.0, wa, wb, wc);
-  double xq = 0.1, tone, ttwo;
-  s_map1(s.tauros, tinteg, n, &xq, &tone, 1);
-  xq = 2.0;
-  s_map1(s.tauros, tinteg, n, &xq, &ttwo, 1);
-  double tav = (ttwo - tone) / 2.0;
-  if (dtsur * tav <= 0.0) tav = 0.0;
-  if (fabs(tav) > fabs(dtsur)) tav = dtsur;
-  dtsur = dtsur - tav;
-  for (int j = 0; j < n; ++j) {
-    s.dtsurf[j] = dtsur;
-    double t1 = s.dtflux[j] + s.dtlamb[j] + dtsur;
-    if (iter == 1) {
-    } else if (s.oldt1[j] * t1 > 0.0 && fabs(s.oldt1[j]) > fabs(t1)) {
-      t1 = t1 * 1.25;
-    } else if (s.oldt1[j] * t1 < 0.0) {
-      t1 = t1 * 0.5;
+         *rmp = W[23], *ab2 = W[24], *p2 = W[25];
+  if (tid == 0) {
+    RossStore R{n0, cap, gR->zerot, gR->slopet, gR->zerop, gR->slopep, rt, rp, rk};
+    double maxerr = 0.0;
+    // ROSS(3)
+    for (int j = 0; j < n; ++j) s.abross[j] = FOUR_SIGMA_OVER_PI * powi(s.t[j], 3) / abross[j];
+    s_integ(s.rhox, s.abross, s.tauros, n, s.abross[0] * s.rhox[0], wa, wb, wc);
+    s_rosstab_store(R, s.t, s.p, s.abross, n);  // RX = ROSSTAB(0,0,0), atlas12c.f90:586
+    // RADIAP(3)
+    double errormax = 0.0;
+    for (int j = 0; j < n; ++j) {
+      s.raden[j] = raden[j] * FOURPI_OVER_C;
+      s.accrad[j] = accrad[j] * FOURPI_OVER_C;
+      if (h_total[j] / FLUX > 1.0) s.accrad[j] = s.accrad[j] * FLUX / h_total[j];
+      errormax = fmax(errormax, h_total[j] / FLUX);
     }
-    s.oldt1[j] = t1;
-    s.t1[j] = t1;
+    double pradk0 = acc[kAcc8 * kw] * FOURPI_OVER_C;
+    if (errormax > 1.0) pradk0 = pradk0 / errormax;
+    s_integ(s.rhox, s.accrad, s.prad, n, s.accrad[0] * s.rhox[0], wa, wb, wc);
+    // TCORR(3)
+    s_deriv(s.rhox, s.t, dtdrhx, n);
+    s_deriv(s.rhox, s.abross, dabros, n);
+    for (int j = 0; j < n; ++j) {
+      rdabh[j] = rdabh[j] - flxrad[j] * dabros[j] / fmax(s.abross[j], 1.0e-30);
+      codrhx[j] = (rdabh[j] + 0.0) / (flxrad[j] + 0.0);
+    }
+    codrhx[0] = 0.0;
+    codrhx[1] = 0.0;
+    s_integ(s.rhox, codrhx, G, n, 0.0, wa, wb, wc);
+    for (int j = 0; j < n; ++j) {
+      G[j] = exp(G[j]);
+      gflux[j] = G[j] * (flxrad[j] + 0.0 - FLUX) / (flxrad[j] + 0.0);
+    }
+    s_integ(s.tauros, gflux, dtau, n, 0.0, wa, wb, wc);
+    for (int j = 0; j < n; ++j) {
+      dtau[j] = dtau[j] / G[j];
+      dtau[j] = fmax(-s.tauros[j] / 3.0, fmin(s.tauros[j] / 3.0, dtau[j]));
+      s.dtflux[j] = -dtau[j] * dtdrhx[j] / fmax(s.abross[j], 1.0e-30);
+    }
+    const double MAX_DT = 0.04 * teff;
+    for (int j = 0; j < n; ++j) {
+      s.flxerr[j] = (flxrad[j] + 0.0 - FLUX) / FLUX * 100.0;
+      maxerr = fmax(maxerr, fabs(s.flxerr[j]));
+    }
+    s_deriv(s.tauros, s.flxerr, flxdrv, n);
+    for (int j = 0; j < n; ++j) {
+      // HRATIO = 0 in radiative layers: FLXDRV from the thermal imbalance
+      flxdrv[j] = rjmins[j] / fmax(s.abross[j], 1.0e-30) / FLUX * 100.0;
+      double d = -flxdrv[j] * FLUX / 100.0 / fmax(fabs(rdiagj[j]), 1.0e-30) * copysign(1.0, rdiagj[j]) *
+                 fmax(s.abross[j], 1.0e-30);
+      s.dtlamb[j] = fmax(-MAX_DT, fmin(MAX_DT, d));
+    }
+    double dtsur = (FLUX - flxrad[0]) / FLUX * 0.25 * s.t[0];
+    dtsur = fmax(-MAX_DT, fmin(MAX_DT, dtsur));
+    for (int j = 0; j < n; ++j) dum[j] = s.dtflux[j] + s.dtlamb[j];
+    s_integ(s.tauros, dum, tinteg, n, 0.0, wa, wb, wc);
+    double xq = 0.1, tone, ttwo;
+    s_map1(s.tauros, tinteg, n, &xq, &tone, 1);
+    xq = 2.0;
+    s_map1(s.tauros, tinteg, n, &xq, &ttwo, 1);
+    double tav = (ttwo - tone) / 2.0;
+    if (dtsur * tav <= 0.0) tav = 0.0;
+    if (fabs(tav) > fabs(dtsur)) tav = dtsur;
+    dtsur = dtsur - tav;
+    for (int j = 0; j < n; ++j) {
+      s.dtsurf[j] = dtsur;
+      double t1 = s.dtflux[j] + s.dtlamb[j] + dtsur;
+      if (iter == 1) {
+      } else if (s.oldt1[j] * t1 > 0.0 && fabs(s.oldt1[j]) > fabs(t1)) {
+        t1 = t1 * 1.25;
+      } else if (s.oldt1[j] * t1 < 0.0) {
+        t1 = t1 * 0.5;
+      }
+      s.oldt1[j] = t1;
+      s.t1[j] = t1;
+    }
+    for (int j = 0; j < n; ++j) {
+      tplus[j] = s.t[j] + s.t1[j];
+      taustd[j] = exp10(-6.875 + (double)j * 0.125);
+    }
+    s_map1(s.tauros, s.t, n, taustd, tnew1, n);
+    s_map1(s.tauros, s.prad, n, taustd, prdnew, n);
+    s_map1(s.tauros, tplus, n, taustd, tnew2, n);
+    s_scal[0] = R.zerot;
+    s_scal[1] = R.slopet;
+    s_scal[2] = R.zerop;
+    s_scal[3] = R.slopep;
+    s_scal[4] = maxerr;
+    s_scal[5] = pradk0;
+    s_n[0] = n0;
+    s_n[1] = R.n;
   }
-  for (int j = 0; j < n; ++j) {
-    tplus[j] = s.t[j] + s.t1[j];
-    taustd[j] = exp10(-6.875 + (double)j * 0.125);
+  __syncthreads();
+  {
+    const RossView RV{s_n[1], s_scal[0], s_scal[1], s_scal[2], s_scal[3], rt, rp, rk};
+    const int grp = tid / kFinGroup, gtid = tid % kFinGroup;
+    if (grp == 0) b_ttaup(RV, grav, tnew1, taustd, ab1, pt1, p1, prdnew, n, gtid, fold[0], 1);
+    else if (grp == 1) b_ttaup(RV, grav, tnew2, taustd, ab2, pt2, p2, prdnew, n, gtid, fold[1], 2);
   }
-  s_map1(s.tauros, s.t, n, taustd, tnew1, n);
-  s_map1(s.tauros, s.prad, n, taustd, prdnew, n);
-  s_map1(s.tauros, tplus, n, taustd, tnew2, n);
-  s.maxerr = maxerr;
+  __syncthreads();
+  if (tid == 0) {
+    for (int j = 0; j < n; ++j) ppp[j] = (pt2[j] - pt1[j]) / pt1[j];
+    s_map1(taustd, ppp, n, s.tauros, rrr, n);
+    for (int j = 0; j < n; ++j) s.t[j] = s.t[j] + s.t1[j];
+    for (int i = 2; i <= n; ++i) {
+      const int jj = n + 1 - i;
+      s.t[jj - 1] = fmin(s.t[jj - 1], s.t[jj] - 1.0);
+    }
+    for (int j = 0; j < n; ++j) s.t[j] = fmax(s.t[j], 1200.0);
+    for (int j = 0; j < n; ++j) s.rhox[j] = s.rhox[j] + rrr[j] * s.rhox[j];
+    double* src[8] = {s.rhox, s.t, s.p, s.xne, s.abross, s.prad, s.vturb, s.pturb};
+    const double ab_surf = s.abross[0];
+    for (int q = 0; q < 8; ++q) {
+      s_map1(s.tauros, src[q], n, taustd, rmp, n);
+      if (q == 4)
+        for (int j = 0; j < n; ++j)
+          if (s.tauros[0] > taustd[j] && rmp[j] < 0.0) rmp[j] = ab_surf;
+      for (int j = 0; j < n; ++j) src[q][j] = rmp[j];
+    }
+    for (int j = 0; j < n; ++j) s.tauros[j] = taustd[j];
+    gms->pradk0 = s_scal[5];
+    gms->maxerr = s_scal[4];
+    gR->n = s_n[1];
+    gR->zerot = s_scal[0];
+    gR->slopet = s_scal[1];
+    gR->zerop = s_scal[2];
+    gR->slopep = s_scal[3];
   }
-  __syncwarp(0xffffffffu);
-  const RossStore Rl = *R;
-  w_ttaup(Rl, grav, tnew1, taustd, ab1, pt1, p1, prdnew, n, lane);
-  __syncwarp(0xffffffffu);
-  w_ttaup(Rl, grav, tnew2, taustd, ab1, pt2, p1, prdnew, n, lane);
-  __syncwarp(0xffffffffu);
-  if (lane == 0) {
-  for (int j = 0; j < n; ++j) ppp[j] = (pt2[j] - pt1[j]) / pt1[j];
-  s_map1(taustd, ppp, n, s.tauros, rrr, n);
-  for (int j = 0; j < n; ++j) s.t[j] = s.t[j] + s.t1[j];
-  for (int i = 2; i <= n; ++i) {
-    const int jj = n + 1 - i;
-    s.t[jj - 1] = fmin(s.t[jj - 1], s.t[jj] - 1.0);
+  __syncthreads();
+  // write back the model, TCORR's RDABH and the new ROSSTAB points
+  for (int e = tid; e < kFinVec * n; e += blockDim.x) gv[e / n][e % n] = V[(e / n) * kw + e % n];
+  for (int e = tid; e < n; e += blockDim.x) gacc[kw + e] = rdabh[e];
+  for (int e = s_n[0] + tid; e < s_n[1]; e += blockDim.x) {
+    gR->t[e] = rt[e];
+    gR->p[e] = rp[e];
+    gR->k[e] = rk[e];
   }
-  for (int j = 0; j < n; ++j) s.t[j] = fmax(s.t[j], 1200.0);
-  for (int j = 0; j < n; ++j) s.rhox[j] = s.rhox[j] + rrr[j] * s.rhox[j];
-  double* src[8] = {s.rhox, s.t, s.p, s.xne, s.abross, s.prad, s.vturb, s.pturb};
-  const double ab_surf = s.abross[0];
-  for (int q = 0; q < 8; ++q) {
-    s_map1(s.tauros, src[q], n, taustd, rmp, n);
-    if (q == 4)
-      for (int j = 0; j < n; ++j)
-        if (s.tauros[0] > taustd[j] && rmp[j] < 0.0) rmp[j] = ab_surf;
-    for (int j = 0; j < n; ++j) src[q][j] = rmp[j];
-  }
-  for (int j = 0; j < n; ++j) s.tauros[j] = taustd[j];
-  }
-  __syncwarp(0xffffffffu);
-  return s.maxerr;
+  return s_scal[4];
 }
 
 }  // namespace atlasgpu

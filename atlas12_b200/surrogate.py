@@ -165,7 +165,7 @@ def continuum_opacity(wave_nm, t, p, e=None):
     pe = ne * KBOL * t
     # H- bound-free: cross-section shape peaking near 850 nm, threshold 1642 nm
     x = np.clip(w / 1642.0, 0.0, 1.0)
-    abf = 4.0e-17 * 6.0 * x ** 1.5 * (1.0 - x) ** 1.5 * 4.0
+    abf = 4.0e-17 * 6.0 * (x * np.sqrt(x)) * ((1.0 - x) * np.sqrt(1.0 - x)) * 4.0
     khm = 4.158e-10 * abf * pe * theta ** 2.5 * 10.0 ** (0.754 * theta) * nh1
     # H- free-free ~ lambda^2
     kff = 1.0e-26 * pe * nh1 * (w / 1000.0) ** 2 * (0.5 + 1.5 * theta)
