@@ -87,39 +87,14 @@ int atlas_prep_lines(atlasgpu_ctx* ctx, const int32_t* d_ld, const int32_t* h_ld
 
 namespace {
 
-__global__ void k_transpose(const double* __restrict__ in, int rows, int cols, double* __restrict__ out) {
-  // out[c][r] = in[r][c]
-  __shared__ double tile[32][33];
-  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
-  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-    const int r = r0 + k, c = c0 + threadIdx.x;
-    if (r < rows && c < cols) tile[k][threadIdx.x] = in[(size_t)r * cols + c];
-  }
-  __syncthreads();
-  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-    const int c = c0 + k, r = r0 + threadIdx.x;
-    if (r < rows && c < cols) out[(size_t)c * rows + r] = tile[threadIdx.x][k];
-  }
-}
-
-int transpose(atlasgpu_ctx* ctx, const double* in, int rows, int cols, double* out) {
-  dim3 g((cols + 31) / 32, (rows + 31) / 32), b(32, 8);
-  k_transpose<<<g, b, 0, ctx->stream>>>(in, rows, cols, out);
-  CKL(ctx);
-  return 0;
-}
-
 int rt_launch(atlasgpu_ctx* ctx, RtArgs& a, bool surr, double* d_sum, int* nwarps_out) {
-  int nwarp = 4;
-  const size_t per = sizeof(RtWS);
-  while (nwarp > 1 && sizeof(double) * kKwMax + nwarp * per > ctx->smem_optin) --nwarp;
-  const size_t smem = sizeof(double) * kKwMax + nwarp * per;
-  // enough warps to fill every SM several times, frequencies contiguous per warp
-  const int target_warps = ctx->nsm * nwarp * 6;
-  a.nu_per_warp = std::max(1, (a.numnu + target_warps - 1) / target_warps);
-  const int nw = (a.numnu + a.nu_per_warp - 1) / a.nu_per_warp;
-  const int blocks = (nw + nwarp - 1) / nwarp;
-  const int nwl = blocks * nwarp;
+  const size_t smem = rt_smem_bytes();
+  // enough groups to fill every SM several times, frequencies contiguous per group
+  const int target = ctx->nsm * 3 * kRtGroups * 4;
+  a.nu_per_warp = std::max(1, (a.numnu + target - 1) / target);
+  const int ng = (a.numnu + a.nu_per_warp - 1) / a.nu_per_warp;
+  const int blocks = (ng + kRtGroups - 1) / kRtGroups;
+  const int nwl = blocks * kRtGroups;
   double* part;
   int r;
   if ((r = bufT(ctx, surr ? "rt_part_m" : "rt_part", (size_t)nwl * (kAcc * a.kw + 1), &part))) return r;
@@ -131,8 +106,8 @@ int rt_launch(atlasgpu_ctx* ctx, RtArgs& a, bool surr, double* d_sum, int* nwarp
   }
   {
     Timer tm(ctx, "atlas_rt");
-    if (surr) k_atlas_rt<true><<<blocks, 32 * nwarp, smem, ctx->stream>>>(a);
-    else k_atlas_rt<false><<<blocks, 32 * nwarp, smem, ctx->stream>>>(a);
+    if (surr) k_atlas_rt<true><<<blocks, kRtThreads, smem, ctx->stream>>>(a);
+    else k_atlas_rt<false><<<blocks, kRtThreads, smem, ctx->stream>>>(a);
     CKL(ctx);
   }
   {
@@ -187,7 +162,7 @@ int atlasgpu_atlas_linop(atlasgpu_ctx* ctx, const int32_t* linedata, int64_t n, 
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
   int32_t *d_ld, *d_iw;
-  double *d_xd, *d_dp, *d_xne, *d_tx, *d_hc, *d_tc, *d_ws, *d_xl, *d_out, *tl;
+  double *d_xd, *d_dp, *d_xne, *d_tx, *d_hc, *d_tc, *d_ws, *d_xl, *tl;
   AtlasLine* d_lines;
   unsigned long long* d_cnt;
   int r;
@@ -198,7 +173,7 @@ int atlasgpu_atlas_linop(atlasgpu_ctx* ctx, const int32_t* linedata, int64_t n, 
       (r = bufT(ctx, "al_xne", kw, &d_xne)) || (r = bufT(ctx, "al_tx", kw, &d_tx)) ||
       (r = bufT(ctx, "al_hc", kw, &d_hc)) || (r = bufT(ctx, "al_tc", (size_t)(nwave + 1) * kw, &d_tc)) ||
       (r = bufT(ctx, "al_ws", numnu, &d_ws)) || (r = bufT(ctx, "al_xl", (size_t)kw * numnu, &d_xl)) ||
-      (r = bufT(ctx, "al_out", (size_t)kw * numnu, &d_out)) || (r = bufT(ctx, "al_lines", nn, &d_lines)) ||
+      (r = bufT(ctx, "al_lines", nn, &d_lines)) ||
       (r = bufT(ctx, "al_cnt", 2, &d_cnt)) || (r = ensure_tablog(ctx, &tl)))
     return r;
   if (n > 0) CK(cudaMemcpyAsync(d_ld, linedata, n * 4 * sizeof(int32_t), cudaMemcpyHostToDevice, s));
@@ -221,8 +196,7 @@ int atlasgpu_atlas_linop(atlasgpu_ctx* ctx, const int32_t* linedata, int64_t n, 
     k_atlas_linop<<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
     CKL(ctx);
   }
-  if ((r = transpose(ctx, d_xl, kw, numnu, d_out))) return r;
-  CK(cudaMemcpyAsync(xlines_out, d_out, (size_t)kw * numnu * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(xlines_out, d_xl, (size_t)kw * numnu * sizeof(double), cudaMemcpyDeviceToHost, s));
   unsigned long long cnt[2];
   CK(cudaMemcpyAsync(cnt, d_cnt, sizeof cnt, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -241,11 +215,11 @@ int atlasgpu_atlas_rt_pass(atlasgpu_ctx* ctx, int numnu, const double* waveset, 
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
   const size_t nt = (size_t)numnu * kw;
-  double *d_ws, *d_rc, *d_ac, *d_sg, *d_sc = nullptr, *d_xl0, *d_xl, *d_rx, *d_t, *d_hk, *d_hs, *d_sum;
+  double *d_ws, *d_rc, *d_ac, *d_sg, *d_sc = nullptr, *d_xl0, *d_rx, *d_t, *d_hk, *d_hs, *d_sum;
   int r;
   if ((r = bufT(ctx, "rt_ws", numnu, &d_ws)) || (r = bufT(ctx, "rt_rc", numnu, &d_rc)) ||
       (r = bufT(ctx, "rt_ac", nt, &d_ac)) || (r = bufT(ctx, "rt_sg", nt, &d_sg)) ||
-      (r = bufT(ctx, "rt_xl0", nt, &d_xl0)) || (r = bufT(ctx, "rt_xl", nt, &d_xl)) ||
+      (r = bufT(ctx, "rt_xl0", nt, &d_xl0)) ||
       (r = bufT(ctx, "rt_rx", kw, &d_rx)) || (r = bufT(ctx, "rt_t", kw, &d_t)) || (r = bufT(ctx, "rt_hk", kw, &d_hk)) ||
       (r = bufT(ctx, "rt_hs", numnu, &d_hs)) || (r = bufT(ctx, "rt_sum", kAcc * kw + 1, &d_sum)))
     return r;
@@ -259,9 +233,8 @@ int atlasgpu_atlas_rt_pass(atlasgpu_ctx* ctx, int numnu, const double* waveset, 
   CK(cudaMemcpyAsync(d_rx, rhox, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(d_t, t, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(d_hk, hkt, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
-  if ((r = transpose(ctx, d_xl0, numnu, kw, d_xl))) return r;
-  RtArgs a{ctx->ops, nullptr, numnu, nrhox, kw, d_ws, d_rc, d_ac, d_sg, d_sc, d_xl, d_rx, d_t, d_hk, teff,
-           1, nullptr, d_hs, nullptr};
+  RtArgs a{ctx->ops, nullptr, numnu, nrhox, kw, d_ws, d_rc, d_ac, d_sg, d_sc, d_xl0, d_rx, d_t, d_hk, teff,
+           1, 1, kw, nullptr, d_hs, nullptr};
   if ((r = rt_launch(ctx, a, false, d_sum, nullptr))) return r;
   std::vector<double> hsum(kAcc * kw + 1);
   CK(cudaMemcpyAsync(hsum.data(), d_sum, hsum.size() * sizeof(double), cudaMemcpyDeviceToHost, s));

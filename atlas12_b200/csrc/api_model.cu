@@ -30,14 +30,14 @@ struct atlasgpu_model {
   int32_t* iwavetab;
   int32_t* linedata;
   AtlasLine* lines;
-  double* xl;            // [kw][numnu]
+  double* xl;            // XLINES(J, NU): [numnu][kw]
   double *partial, *sum, *hsurf;
   double *h0, *h1, *h2, *ross;  // ross: ROSSTAB points [3][kRossMax]
   RossStore* R;                  // device
   int* iter_dev;         // iterations completed
   double* maxerr_dev;    // last max |FLXERR|
   unsigned long long* cnt;
-  int nwarp_rt, blocks_rt, nwl;
+  int blocks_rt, nwl, nu_per_group;
   size_t smem_rt;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -151,12 +151,10 @@ int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
   }
   RtArgs ra{ctx->ops, m->cc, m->numnu, m->nrhox, m->kw, m->waveset, m->rcoset, nullptr, nullptr, nullptr,
             m->xl, (const double*)m->state + 1 * m->kw, (const double*)m->state + 0 * m->kw, m->hkt,
-            m->teff, 1, m->partial, m->hsurf, nullptr};
-  const int target = ctx->nsm * m->nwarp_rt * 6;
-  ra.nu_per_warp = std::max(1, (m->numnu + target - 1) / target);
+            m->teff, m->nu_per_group, 1, m->kw, m->partial, m->hsurf, nullptr};
   {
     Timer tm(ctx, "atlas_rt");
-    k_atlas_rt<true><<<m->blocks_rt, 32 * m->nwarp_rt, m->smem_rt, s>>>(ra);
+    k_atlas_rt<true><<<m->blocks_rt, kRtThreads, m->smem_rt, s>>>(ra);
     CKL(ctx);
   }
   {
@@ -274,14 +272,12 @@ int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlas
     return r;
   }
   // RT launch shape
-  m->nwarp_rt = 4;
-  while (m->nwarp_rt > 1 && sizeof(double) * kKwMax + m->nwarp_rt * sizeof(RtWS) > ctx->smem_optin) --m->nwarp_rt;
-  m->smem_rt = sizeof(double) * kKwMax + m->nwarp_rt * sizeof(RtWS);
-  const int target = ctx->nsm * m->nwarp_rt * 6;
-  const int npw = std::max(1, (m->numnu + target - 1) / target);
-  const int nw = (m->numnu + npw - 1) / npw;
-  m->blocks_rt = (nw + m->nwarp_rt - 1) / m->nwarp_rt;
-  m->nwl = m->blocks_rt * m->nwarp_rt;
+  m->smem_rt = rt_smem_bytes();
+  const int target = ctx->nsm * 3 * kRtGroups * 4;
+  m->nu_per_group = std::max(1, (m->numnu + target - 1) / target);
+  const int ng = (m->numnu + m->nu_per_group - 1) / m->nu_per_group;
+  m->blocks_rt = (ng + kRtGroups - 1) / kRtGroups;
+  m->nwl = m->blocks_rt * kRtGroups;
   if ((r = dalloc(ctx, &m->partial, (size_t)m->nwl * (kAcc * kw + 1)))) {
     atlasgpu_model_destroy(ctx, m);
     return r;

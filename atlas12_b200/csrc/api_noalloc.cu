@@ -7,10 +7,11 @@
 // the host application, or a process that must not grow its footprint after
 // start-up.  atlasgpu_atlas_rt_pass_noalloc serves them: the caller passes all
 // inputs and outputs as device pointers, and the only scratch the pass needs
-// (one row of partial sums per warp) lives in a fixed file-scope device array.
+// (one row of partial sums per thread group) lives in a fixed file-scope
+// device array.
 //
 // That array is part of the library image: every GPU that loads the library
-// holds it (kNoAllocWarps x (8*kKwMax + 1) doubles = 6.6 MB) until the
+// holds it (kNoAllocRows x (8*kKwMax + 1) doubles = 6.6 MB) until the
 // process exits.  All calls share it and it keeps the last call's contents;
 // every row a call reads is written by that call first, so nothing needs
 // clearing, but two calls that overlap on the GPU (different streams, or
@@ -23,10 +24,10 @@ using namespace atlasgpu;
 
 namespace {
 
-constexpr int kNoAllocWarps = 1024;               // maximum warps (rows of partials)
+constexpr int kNoAllocRows = 1024;                // maximum thread groups (rows of partials)
 constexpr int kNoAllocRow = kAcc * kKwMax + 1;    // one row: 8 sums per depth + PRADK0
 
-static __device__ __align__(256) double g_noalloc_partial[(size_t)kNoAllocWarps * kNoAllocRow];
+static __device__ __align__(256) double g_noalloc_partial[(size_t)kNoAllocRows * kNoAllocRow];
 
 constexpr int kMaxDevices = 64;
 double* g_partial_addr[kMaxDevices] = {nullptr};  // device address of the array, per device
@@ -63,22 +64,22 @@ int atlasgpu_atlas_rt_pass_noalloc(atlasgpu_ctx* ctx, int numnu, const double* d
     g_partial_addr[ctx->device] = (double*)p;
   }
   double* partial = g_partial_addr[ctx->device];
-  // launch shape: at most kNoAllocWarps warps, contiguous frequencies per warp
-  int nwarp = 4;
-  while (nwarp > 1 && sizeof(double) * kKwMax + nwarp * sizeof(RtWS) > ctx->smem_optin) --nwarp;
-  const size_t smem = sizeof(double) * kKwMax + nwarp * sizeof(RtWS);
-  int target = ctx->nsm * nwarp * 6;
-  if (target > kNoAllocWarps) target = kNoAllocWarps;
+  // launch shape: at most kNoAllocRows thread groups (rows of partials),
+  // contiguous frequencies per group
+  const size_t smem = rt_smem_bytes();
+  int target = ctx->nsm * 3 * kRtGroups * 4;
+  if (target > kNoAllocRows) target = kNoAllocRows;
   const int npw = (numnu + target - 1) / target;
-  const int nw = (numnu + npw - 1) / npw;
-  const int blocks = (nw + nwarp - 1) / nwarp;
-  const int nwl = blocks * nwarp;
-  if (nwl > kNoAllocWarps)
-    return fail(ctx, ATLASGPU_EINVAL, "rt_pass_noalloc: %d warps exceed the scratch limit %d", nwl, kNoAllocWarps);
+  const int ng = (numnu + npw - 1) / npw;
+  const int blocks = (ng + kRtGroups - 1) / kRtGroups;
+  const int nwl = blocks * kRtGroups;
+  if (nwl > kNoAllocRows)
+    return fail(ctx, ATLASGPU_EINVAL, "rt_pass_noalloc: %d thread groups exceed the scratch limit %d", nwl,
+                kNoAllocRows);
   CK(cudaFuncSetAttribute(k_atlas_rt<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   RtArgs a{ctx->ops, nullptr, numnu, nrhox, kw, d_waveset, d_rcoset, d_acont, d_sigmac, d_scont, d_xlines_t,
-           d_rhox, d_t, d_hkt, teff, npw, partial, d_hsurf, nullptr};
-  k_atlas_rt<false><<<blocks, 32 * nwarp, smem, ctx->stream>>>(a);
+           d_rhox, d_t, d_hkt, teff, npw, numnu, 1, partial, d_hsurf, nullptr};
+  k_atlas_rt<false><<<blocks, kRtThreads, smem, ctx->stream>>>(a);
   CKL(ctx);
   launch_reduce(partial, nwl, kw, d_sums, ctx->stream);
   CKL(ctx);

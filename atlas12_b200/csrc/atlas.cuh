@@ -106,62 +106,63 @@ struct LinopArgs {
   const double* tabcont;          // [nwave+1][kw]
   const double* waveset;
   const double *h0, *h1, *h2;     // 2001
-  double* xl;                     // [kw][numnu]  (transposed XLINES)
+  double* xl;                     // XLINES(J, NU): [numnu][kw]
   unsigned long long* npairs;     // diagnostics: walked (line, depth) pairs
   unsigned long long* used;       // LINEUSED: lines above TABCONT at a coarse depth
 };
 
-// one (line, depth) wing walk by a warp: lanes over wing points
-__device__ __forceinline__ void linop_wings_warp(const LinopArgs& a, int J, double center,
-                                                 double adamp, double dopwave, double wlvac,
-                                                 int nu, double tc, int lane) {
-  double* xlj = a.xl + (size_t)(J - 1) * a.numnu;
+// LINOP1's profile value at one wing point: tabulated H(v, a) for
+// ADAMP <= 0.2 and v <= 10, the Lorentz wing 1/sqrt(pi) a / v^2 beyond,
+// the full VOIGT for ADAMP > 0.2 (atlas12_modules.f90:18290-18345)
+__device__ __forceinline__ double linop_cv(const LinopArgs& a, double center, double adamp, double vv) {
+  if (adamp > 0.20) return center * voigt_kurucz(vv, adamp, a.h0, a.h1, a.h2);
+  if (vv > 10.0) return center * kInvSqrtPi * adamp / (vv * vv);
+  const int iv = (int)(vv * 200.0 + 1.5);
+  return center * ((a.h2[iv - 1] * adamp + a.h1[iv - 1]) * adamp + a.h0[iv - 1]);
+}
+
+// The rest of one (line, depth) walk after a lane gave up on it, by the
+// whole warp (lanes over wing points), add-then-test as in the reference:
+// red points rnext..iwmax unless rdone, blue offsets bnext..100 unless bdone.
+static __device__ __noinline__ void linop_finish_warp(const LinopArgs& a, int J, double center, double adamp,
+                                               double dopwave, double wlvac, int nu, double tc, int rnext,
+                                               bool rdone, int bnext, bool bdone, int lane) {
+  double* xl = a.xl + (J - 1);
   const int iwmax = min(nu + 100, a.numnu);
-  // red wing: IW = NU .. min(NU+100, NUMNU), add then test
-  for (int base = nu; base <= iwmax; base += 32) {
-    const int iw = base + lane;
-    double cv = 0.0;
-    const bool valid = iw <= iwmax;
-    if (valid) {
-      const double vv = (a.waveset[iw - 1] - wlvac) / dopwave;
-      if (adamp > 0.20) {
-        cv = center * voigt_kurucz(vv, adamp, a.h0, a.h1, a.h2);
-      } else if (vv > 10.0) {
-        cv = center * kInvSqrtPi * adamp / (vv * vv);
-      } else {
-        const int iv = (int)(vv * 200.0 + 1.5);
-        cv = center * ((a.h2[iv - 1] * adamp + a.h1[iv - 1]) * adamp + a.h0[iv - 1]);
-      }
+  if (!rdone) {
+    for (int base = rnext; base <= iwmax; base += 32) {
+      const int iw = base + lane;
+      const bool valid = iw <= iwmax;
+      double cv = 0.0;
+      if (valid) cv = linop_cv(a, center, adamp, (a.waveset[iw - 1] - wlvac) / dopwave);
+      const unsigned stop = __ballot_sync(0xffffffffu, valid && cv < tc);
+      const int last = stop ? base + __ffs(stop) - 1 : iwmax;
+      if (valid && iw <= last) atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
+      if (stop) break;
     }
-    const unsigned stop = __ballot_sync(0xffffffffu, valid && cv < tc);
-    const int last = stop ? base + __ffs(stop) - 1 : iwmax;  // last point added
-    if (valid && iw <= last) atomicAdd(xlj + iw - 1, cv);
-    if (stop) break;
   }
-  // blue wing: IW = NU-1 .. NU-100 (>= 1)
-  for (int i0 = 1; i0 <= 100; i0 += 32) {
-    const int i = i0 + lane;
-    const int iw = nu - i;
-    const bool valid = i <= 100 && iw >= 1;
-    double cv = 0.0;
-    if (valid) {
-      const double vv = (wlvac - a.waveset[iw - 1]) / dopwave;
-      if (adamp > 0.20) {
-        cv = center * voigt_kurucz(vv, adamp, a.h0, a.h1, a.h2);
-      } else if (vv > 10.0) {
-        cv = center * kInvSqrtPi * adamp / (vv * vv);
-      } else {
-        const int iv = (int)(vv * 200.0 + 1.5);
-        cv = center * ((a.h2[iv - 1] * adamp + a.h1[iv - 1]) * adamp + a.h0[iv - 1]);
-      }
+  if (!bdone) {
+    for (int i0 = bnext; i0 <= 100; i0 += 32) {
+      const int i = i0 + lane;
+      const int iw = nu - i;
+      const bool valid = i <= 100 && iw >= 1;
+      double cv = 0.0;
+      if (valid) cv = linop_cv(a, center, adamp, (wlvac - a.waveset[iw - 1]) / dopwave);
+      const unsigned stop = __ballot_sync(0xffffffffu, valid && cv < tc);
+      const unsigned inval = __ballot_sync(0xffffffffu, !valid);
+      const int ilast = stop ? i0 + __ffs(stop) - 1 : 100;
+      if (valid && i <= ilast) atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
+      if (stop || inval) break;
     }
-    const unsigned stop = __ballot_sync(0xffffffffu, valid && cv < tc);
-    const unsigned inval = __ballot_sync(0xffffffffu, !valid);
-    const int ilast = stop ? i0 + __ffs(stop) - 1 : 100;
-    if (valid && i <= ilast) atomicAdd(xlj + iw - 1, cv);
-    if (stop || inval) break;
   }
 }
+
+// Warp per line, lane per depth.  Most (line, depth) wing walks stop after a
+// point or two (the C2 grid is ~50 Doppler widths per step), so each lane
+// walks its own depth's red and blue wings for up to kLinopLanePts points,
+// and the few walks still going are finished by the whole warp.  Lanes of a
+// warp touch XLINES(J, IW) at consecutive J: one coalesced atomic per step.
+constexpr int kLinopLanePts = 4;
 
 static __global__ void __launch_bounds__(256) k_atlas_linop(LinopArgs a) {
   const int lane = threadIdx.x & 31;
@@ -174,7 +175,7 @@ static __global__ void __launch_bounds__(256) k_atlas_linop(LinopArgs a) {
     const double* xdn = a.xnfdop + (size_t)(L.nelion - 1) * a.kw;
     const double* dpn = a.dopple + (size_t)(L.nelion - 1) * a.kw;
     const double* tcv = a.tabcont + (size_t)(L.nucont - 1) * a.kw;
-    // phase 1 gates: coarse depths 8, 16, ... (lane k -> depth 8(k+1))
+    // coarse gates: depths 8, 16, ... (lane k -> depth 8(k+1)); bit k = IFJ at depth 8(k+1)
     int pass = 0;
     {
       const int J = 8 * (lane + 1);
@@ -186,37 +187,81 @@ static __global__ void __launch_bounds__(256) k_atlas_linop(LinopArgs a) {
         }
       }
     }
-    const unsigned ifj = __ballot_sync(0xffffffffu, pass);  // bit k: IFJ(8(k+1)+1)
+    const unsigned ifj = __ballot_sync(0xffffffffu, pass);
     if (ifj == 0) continue;
     if (lane == 0) atomicAdd(a.used, 1ull);
-    // walk every depth that passes: coarse depths, then fine depths of blocks
-    // whose neighbouring coarse gates (IFJ(K-7), IFJ(K+1)) are set
-    for (int K = 8; K <= a.nrhox; K += 8) {
-      const int k = K / 8 - 1;
-      const bool cur = (ifj >> k) & 1u;
-      const bool prev = k > 0 && ((ifj >> (k - 1)) & 1u);
-      // fine depths K-7..K-1 (processed after all coarse in the reference; the
-      // order of additions into different XLINES(J,*) rows does not interact)
-      if (cur || prev) {
-        for (int J = K - 7; J <= K - 1; ++J) {
-          double center = L.cgf * xdn[J - 1];
-          if (center < tcv[J - 1]) continue;
-          center = center * exp(-L.elo * a.hckt[J - 1]);
-          if (center < tcv[J - 1]) continue;
-          const double adamp = (L.gr + L.gs * a.xne[J - 1] + L.gw * a.txnxn[J - 1]) / dpn[J - 1];
-          linop_wings_warp(a, J, center, adamp, dpn[J - 1] * L.wlvac, L.wlvac, L.nu, tcv[J - 1], lane);
-          ++walked;
+    const int iwmax = min(L.nu + 100, a.numnu);
+    for (int J0 = 1; J0 <= a.nrhox; J0 += 32) {
+      const int J = J0 + lane;
+      bool walk = false;
+      double center = 0.0, tc = 0.0;
+      const int K = 8 * ((J + 7) / 8);  // the coarse depth closing J's block
+      if (J <= a.nrhox && K <= a.nrhox) {
+        const int k = K / 8 - 1;
+        const bool cur = (ifj >> k) & 1u;
+        tc = tcv[J - 1];
+        if (J == K) {
+          walk = cur;
+          if (walk) center = L.cgf * xdn[J - 1] * exp(-L.elo * a.hckt[J - 1]);
+        } else if (cur || (k > 0 && ((ifj >> (k - 1)) & 1u))) {
+          // fine depth K-7..K-1 of a block next to a passing coarse depth
+          center = L.cgf * xdn[J - 1];
+          if (center >= tc) {
+            center = center * exp(-L.elo * a.hckt[J - 1]);
+            walk = center >= tc;
+          }
         }
       }
-      if (cur) {
-        const int J = K;
-        const double center = L.cgf * xdn[J - 1] * exp(-L.elo * a.hckt[J - 1]);
-        const double adamp = (L.gr + L.gs * a.xne[J - 1] + L.gw * a.txnxn[J - 1]) / dpn[J - 1];
-        linop_wings_warp(a, J, center, adamp, dpn[J - 1] * L.wlvac, L.wlvac, L.nu, tcv[J - 1], lane);
+      if (!__any_sync(0xffffffffu, walk)) continue;
+      double adamp = 0.0, dopwave = 1.0;
+      if (walk) {
+        adamp = (L.gr + L.gs * a.xne[J - 1] + L.gw * a.txnxn[J - 1]) / dpn[J - 1];
+        dopwave = dpn[J - 1] * L.wlvac;
         ++walked;
+      }
+      double* xlj = a.xl + (J - 1);
+      bool rdone = !walk, bdone = !walk;
+      int rnext = L.nu, bnext = 1;
+      for (int s = 0; s < kLinopLanePts && __any_sync(0xffffffffu, !rdone || !bdone); ++s) {
+        if (!rdone) {
+          const int iw = rnext;
+          const double cv = linop_cv(a, center, adamp, (a.waveset[iw - 1] - L.wlvac) / dopwave);
+          atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
+          if (cv < tc || iw >= iwmax) rdone = true;
+          else rnext = iw + 1;
+        }
+        if (!bdone) {
+          const int iw = L.nu - bnext;
+          if (iw < 1) {
+            bdone = true;
+          } else {
+            const double cv = linop_cv(a, center, adamp, (L.wlvac - a.waveset[iw - 1]) / dopwave);
+            atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
+            if (cv < tc || bnext >= 100) bdone = true;
+            else bnext = bnext + 1;
+          }
+        }
+      }
+      // walks still going: the warp finishes them one at a time
+      unsigned ov = __ballot_sync(0xffffffffu, !rdone || !bdone);
+      while (ov) {
+        const int src = __ffs(ov) - 1;
+        ov &= ov - 1;
+        const int Js = __shfl_sync(0xffffffffu, J, src);
+        const double cs = __shfl_sync(0xffffffffu, center, src);
+        const double as = __shfl_sync(0xffffffffu, adamp, src);
+        const double ds = __shfl_sync(0xffffffffu, dopwave, src);
+        const double ts = __shfl_sync(0xffffffffu, tc, src);
+        const int rn = __shfl_sync(0xffffffffu, rnext, src);
+        const int bn = __shfl_sync(0xffffffffu, bnext, src);
+        const bool rd = __shfl_sync(0xffffffffu, (int)rdone, src) != 0;
+        const bool bd = __shfl_sync(0xffffffffu, (int)bdone, src) != 0;
+        linop_finish_warp(a, Js, cs, as, ds, L.wlvac, L.nu, ts, rn, rd, bn, bd, lane);
       }
     }
   }
+  // walked (line, depth) pairs, summed over the warp's lanes
+  for (int o = 16; o > 0; o >>= 1) walked += __shfl_xor_sync(0xffffffffu, walked, o);
   if (lane == 0 && walked && a.npairs) atomicAdd(a.npairs, walked);
 }
 
@@ -263,11 +308,12 @@ struct RtArgs {
   int numnu, nrhox, kw;
   const double *waveset, *rcoset;
   const double *acont, *sigmac, *scont;  // [numnu][kw]; scont may be null (=> BNU)
-  const double* xl;                      // [kw][numnu] transposed XLINES
+  const double* xl;                      // XLINES: element (J, NU) at xl[(J-1)*xl_sj + (NU-1)*xl_snu]
   const double *rhox, *t, *hkt;
   double teff;
-  int nu_per_warp;
-  double* partial;   // [nwarps][kAcc*kw + 1]
+  int nu_per_warp;    // contiguous frequencies per group
+  int xl_sj, xl_snu;  // XLINES strides (depth, frequency)
+  double* partial;   // [groups][kAcc*kw + 1]
   double* hsurf;     // [numnu] HNU(1) per frequency (the .flux record)
   int* sweeps;       // [numnu] Eddington sweeps (diagnostic; may be null)
 };
@@ -279,31 +325,41 @@ struct RtWS {
       stim[kKwMax], dab[kKwMax];
 };
 
+// One pair group (64 threads) per frequency, kRtGroups groups per CTA.  The
+// group's 51 matrix rows live in registers (pair scatter_solve), so the
+// shared-memory footprint is the depth vectors only.
+constexpr int kRtGroups = 2;
+constexpr int kRtThreads = kRtGroups * PairG::N;
+
+__host__ __device__ inline size_t rt_smem_bytes() { return sizeof(double) * kKwMax + kRtGroups * sizeof(RtWS); }
+
 template <bool kSurr>
-static __global__ void __launch_bounds__(128) k_atlas_rt(RtArgs a) {
+static __global__ void __launch_bounds__(kRtThreads, 3) k_atlas_rt(RtArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int gid = threadIdx.x / PairG::N;
   double* rhox_s = reinterpret_cast<double*>(smem_raw);
-  RtWS& S = reinterpret_cast<RtWS*>(smem_raw + sizeof(double) * kKwMax)[wid];
+  RtWS& S = reinterpret_cast<RtWS*>(smem_raw + sizeof(double) * kKwMax)[gid];
   for (int j = threadIdx.x; j < a.nrhox; j += blockDim.x) rhox_s[j] = a.rhox[j];
   __syncthreads();
+  PairG g(threadIdx.x % PairG::N, 1 + gid, S.w.red);
+  constexpr int C = (kKwMax + PairG::N - 1) / PairG::N;
   const JoshOps& ops = *a.ops;
   const int nr = a.nrhox;
-  const int gw = blockIdx.x * nwarp + wid;
+  const int gw = blockIdx.x * kRtGroups + gid;  // partial-sum row of this group
   const int nu0 = gw * a.nu_per_warp + 1;
   const int nu1 = min(nu0 + a.nu_per_warp - 1, a.numnu);
-  double acc[kAcc][4];
+  double acc[kAcc][C];
 #pragma unroll
   for (int q = 0; q < kAcc; ++q)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) acc[q][c] = 0.0;
+    for (int c = 0; c < C; ++c) acc[q][c] = 0.0;
   double pradk0 = 0.0;
   for (int nu = nu0; nu <= nu1; ++nu) {
     const double wave = a.waveset[nu - 1];
     const double freq = kClightNms / wave;
     const double rcowt = a.rcoset[nu - 1];
     const double f3 = powi(freq / 1.0e15, 3);
-    for (int j = lane; j < nr; j += 32) {
+    for (int j = g.r; j < nr; j += PairG::N) {
       const double ehvkt = exp(-freq * a.hkt[j]);
       const double stim = 1.0 - ehvkt;
       const double bnu = kBnuPrefac * f3 * ehvkt / stim;
@@ -320,29 +376,29 @@ static __global__ void __launch_bounds__(128) k_atlas_rt(RtArgs a) {
         S.sigmac[j] = a.sigmac[(size_t)(nu - 1) * a.kw + j];
         S.scont[j] = a.scont ? a.scont[(size_t)(nu - 1) * a.kw + j] : bnu;
       }
-      S.aline[j] = 0.0 + a.xl[(size_t)j * a.numnu + nu - 1] * stim;
+      S.aline[j] = 0.0 + a.xl[(size_t)j * a.xl_sj + (size_t)(nu - 1) * a.xl_snu] * stim;
       S.sigmal[j] = 0.0;
     }
-    wsync();
-    const int sw = w_josh(ops, rhox_s, nr, S.acont, S.aline, S.sigmac, S.sigmal, S.scont, S.f.bnu,
-                          S.f.bnu, S.w, &S.f, nullptr, lane);
-    if (a.sweeps && lane == 0) a.sweeps[nu - 1] = sw;
+    g.sync();
+    const int sw = g_josh(g, ops, rhox_s, nr, S.acont, S.aline, S.sigmac, S.sigmal, S.scont, S.f.bnu,
+                          S.f.bnu, S.w, nullptr, &S.f, nullptr);
+    if (a.sweeps && g.r == 0) a.sweeps[nu - 1] = sw;
     // negative floor (RUN_RT_PASS :3926-3937)
     bool neg = false;
-    for (int j = lane; j < nr; j += 32) neg |= (S.f.snu[j] < 0.0 || S.f.jnu[j] < 0.0 || S.f.hnu[j] < 0.0);
-    if (__any_sync(0xffffffffu, neg)) {
-      for (int j = lane; j < nr; j += 32) {
+    for (int j = g.r; j < nr; j += PairG::N) neg |= (S.f.snu[j] < 0.0 || S.f.jnu[j] < 0.0 || S.f.hnu[j] < 0.0);
+    if (g.any(neg)) {
+      for (int j = g.r; j < nr; j += PairG::N) {
         S.f.jnu[j] = fmax(S.f.jnu[j], 1.0e-99);
         S.f.snu[j] = fmax(S.f.snu[j], 1.0e-99);
         S.f.hnu[j] = fmax(S.f.hnu[j], 1.0e-99);
       }
-      wsync();
+      g.sync();
     }
-    if (lane == 0) a.hsurf[nu - 1] = S.f.hnu[0];
+    if (g.r == 0) a.hsurf[nu - 1] = S.f.hnu[0];
     // TCORR mode 2: d(abtot)/d(rhox)
-    w_deriv(rhox_s, S.w.abtot, S.dab, nr, lane);
+    g_deriv(g, rhox_s, S.w.abtot, S.dab, nr);
     // TERM2 per depth (E3 diagonal of Lambda); D(NRHOX) repeats D(NRHOX-1)
-    for (int j = lane; j < nr; j += 32) {
+    for (int j = g.r; j < nr; j += PairG::N) {
       const int jd = j < nr - 1 ? j : nr - 2;
       double d = S.w.taunu[jd + 1] - S.w.taunu[jd];
       d = fmax(1.0e-10, d);
@@ -358,9 +414,11 @@ static __global__ void __launch_bounds__(128) k_atlas_rt(RtArgs a) {
       }
       S.w.t1[j] = term2;
     }
-    wsync();
-    int c = 0;
-    for (int j = lane; j < nr; j += 32, ++c) {
+    g.sync();
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const int j = g.r + c * PairG::N;
+      if (j >= nr) break;
       const double ab = S.w.abtot[j], al = S.w.alpha[j], h = S.f.hnu[j];
       acc[1][c] += S.dab[j] / ab * h * rcowt;                 // RDABH
       acc[0][c] += ab * S.f.jmins[j] * rcowt;                 // RJMINS
@@ -376,14 +434,18 @@ static __global__ void __launch_bounds__(128) k_atlas_rt(RtArgs a) {
       acc[7][c] += dbdt2 / ab * rcowt;                        // ABROSS
     }
     pradk0 += S.f.knu1 * rcowt;
-    wsync();
+    g.sync();
   }
   double* out = a.partial + (size_t)gw * (kAcc * a.kw + 1);
-  int c = 0;
-  for (int j = lane; j < nr; j += 32, ++c)
 #pragma unroll
-    for (int q = 0; q < kAcc; ++q) out[q * a.kw + j] = acc[q][c];
-  if (lane == 0) out[kAcc * a.kw] = pradk0;
+  for (int c = 0; c < C; ++c) {
+    const int j = g.r + c * PairG::N;
+    if (j < nr) {
+#pragma unroll
+      for (int q = 0; q < kAcc; ++q) out[q * a.kw + j] = acc[q][c];
+    }
+  }
+  if (g.r == 0) out[kAcc * a.kw] = pradk0;
 }
 
 // fixed-order sum of the per-warp partials: out[kAcc*kw + 1].  A block owns

@@ -1,7 +1,8 @@
-// josh.cuh -- warp-cooperative JOSH radiative transfer (FP64) for sm_100a.
+// josh.cuh -- cooperative JOSH radiative transfer (FP64) for sm_100a.
 //
-// One warp solves one frequency.  Depth vectors (<= kKwMax) and the 51x51
-// scattering system live in the warp's shared-memory workspace; lanes split
+// A thread group solves one frequency: either one warp (WarpG) or a pair of
+// warps (PairG, 64 threads synchronised by a named barrier).  Depth vectors
+// (<= kKwMax) live in the group's shared-memory workspace; threads split
 // depths, grid points, matrix rows or columns.  Every routine restates the
 // reference formula for each output element (atlas12_modules.f90):
 //   PARCOE :5358-5434, INTEG :5293-5324, DERIV :5228-5266, MAP1 :5570-5692,
@@ -12,18 +13,70 @@
 // per point from the bracket indices of the neighbouring outputs, so each
 // output gets the formula the sequential walk would have used.
 // Running sums whose order decides later branches (the INTEG cumulative sum)
-// are summed in the reference order by one lane.
+// are summed in the reference order by one thread.
+//
+// The 51x51 scattering system: a warp group factors it in shared memory
+// (w_solvit); a pair group keeps one matrix row per thread in registers and
+// broadcasts only the pivot row (pair_solve), which takes the 21 KB matrix
+// out of shared memory and the row updates off the shared-memory pipe.
 #pragma once
 #include "common.cuh"
 
 namespace atlasgpu {
 
+// ---------------------------------------------------------------- groups
+struct WarpG {
+  static constexpr int N = 32;
+  int r;  // lane
+  __device__ explicit WarpG(int lane) : r(lane) {}
+  __device__ __forceinline__ void sync() const { __syncwarp(0xffffffffu); }
+  __device__ __forceinline__ double max(double v) { return warp_max(v); }
+  __device__ __forceinline__ double sum(double v) { return warp_sum(v); }
+  __device__ __forceinline__ bool any(bool p) { return __any_sync(0xffffffffu, p); }
+};
+
+// Two warps on named barrier `bar`; red = 4 doubles of the group's shared
+// scratch (two slots per warp, alternated so one barrier per reduction
+// suffices: a slot is rewritten only after every thread has passed the
+// barrier of the reduction in between).
+struct PairG {
+  static constexpr int N = 64;
+  int r;  // 0..63
+  int bar;
+  double* red;
+  int par;
+  __device__ PairG(int rank, int barrier, double* scratch) : r(rank), bar(barrier), red(scratch), par(0) {}
+  __device__ __forceinline__ void sync() const {
+    asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(N) : "memory");
+  }
+  __device__ __forceinline__ double sum(double v) {
+    v = warp_sum(v);
+    if ((r & 31) == 0) red[par * 2 + (r >> 5)] = v;
+    sync();
+    const double s = red[par * 2] + red[par * 2 + 1];
+    par ^= 1;
+    return s;
+  }
+  __device__ __forceinline__ double max(double v) {
+    v = warp_max(v);
+    if ((r & 31) == 0) red[par * 2 + (r >> 5)] = v;
+    sync();
+    const double s = fmax(red[par * 2], red[par * 2 + 1]);
+    par ^= 1;
+    return s;
+  }
+  __device__ __forceinline__ bool any(bool p) { return max(__any_sync(0xffffffffu, p) ? 1.0 : 0.0) > 0.0; }
+};
+
 struct JoshWS {
-  double A[kNx * kLd];  // scattering system, column-major, ld = kLd
   double xs[kNx], xsbar[kNx], xalpha[kNx], xw[kNx];
   double abtot[kKwMax], alpha[kKwMax], snubar[kKwMax], taunu[kKwMax];
   double t1[kKwMax], t2[kKwMax], t3[kKwMax];  // scratch (PARCOE a,b,c / terms)
+  double prow[kNx + 1];                       // pivot row broadcast (pair groups)
+  double red[4];                              // group reductions (pair groups)
   int lidx[kKwMax + 4];                       // MAP1 bracket indices
+  int piv[2];                                 // pivot (value slot, position) exchange
+  double pval[2];
 };
 
 // Full-solution extras for IFSURF = 0 (ATLAS)
@@ -37,10 +90,12 @@ __device__ __forceinline__ void wsync() { __syncwarp(0xffffffffu); }
 
 // ---------------------------------------------------------------- PARCOE/INTEG
 // Coefficients into (a, b, c); n >= 4 assumed (n = NRHOX >= 4 on the hot path).
-__device__ inline void w_parcoe(const double* f, const double* x, double* a, double* b, double* c,
-                                int n, int lane) {
+template <class G>
+__device__ inline void g_parcoe(G& g, const double* f, const double* x, double* a, double* b, double* c,
+                                int n) {
+  constexpr int C = (kKwMax + G::N - 1) / G::N;
   // steps 1-3: endpoints linear, j = 1, 2 linear, interior parabolic
-  for (int j = lane; j < n; j += 32) {
+  for (int j = g.r; j < n; j += G::N) {
     double aj, bj, cj;
     if (j == 0 || j == 1 || j == 2 || j == n - 1) {
       const int i0 = (j == n - 1) ? n - 2 : j;
@@ -59,11 +114,11 @@ __device__ inline void w_parcoe(const double* f, const double* x, double* a, dou
     b[j] = bj;
     c[j] = cj;
   }
-  wsync();
+  g.sync();
   // step 4: blend each interval with its right neighbour's unsmoothed fit
-  double na[4], nb[4], nc[4];
+  double na[C], nb[C], nc[C];
   int cnt = 0;
-  for (int j = lane; j < n; j += 32, ++cnt) {
+  for (int j = g.r; j < n; j += G::N, ++cnt) {
     na[cnt] = a[j];
     nb[cnt] = b[j];
     nc[cnt] = c[j];
@@ -74,38 +129,38 @@ __device__ inline void w_parcoe(const double* f, const double* x, double* a, dou
       nc[cnt] = c[j + 1] + wt * (c[j] - c[j + 1]);
     }
   }
-  wsync();
+  g.sync();
   cnt = 0;
-  for (int j = lane; j < n; j += 32, ++cnt) {
+  for (int j = g.r; j < n; j += G::N, ++cnt) {
     a[j] = na[cnt];
     b[j] = nb[cnt];
     c[j] = nc[cnt];
   }
-  wsync();
+  g.sync();
   // step 5: penultimate interval takes the endpoint linear fit
-  if (lane == 0) {
+  if (g.r == 0) {
     a[n - 2] = a[n - 1];
     b[n - 2] = b[n - 1];
     c[n - 2] = c[n - 1];
   }
-  wsync();
+  g.sync();
 }
 
 // fint = running parabolic integral of f over x, fint[0] = start
-__device__ inline void w_integ(const double* x, const double* f, double* fint, int n, double start,
-                               JoshWS& ws, int lane) {
+template <class G>
+__device__ inline void g_integ(G& g, const double* x, const double* f, double* fint, int n, double start,
+                               JoshWS& ws) {
   double *a = ws.t1, *b = ws.t2, *c = ws.t3;
-  w_parcoe(f, x, a, b, c, n, lane);
-  for (int i = lane; i < n - 1; i += 32) {
+  g_parcoe(g, f, x, a, b, c, n);
+  for (int i = g.r; i < n - 1; i += G::N) {
     const double xlo = x[i], xhi = x[i + 1];
-    // reuse a[] for the interval terms after reading this interval's a,b,c
     const double term = (a[i] + b[i] * 0.5 * (xhi + xlo) +
                          c[i] / 3.0 * ((xhi + xlo) * xhi + xlo * xlo)) *
                         (xhi - xlo);
     b[i] = term;
   }
-  wsync();
-  if (lane == 0) {
+  g.sync();
+  if (g.r == 0) {
     double s = start;
     fint[0] = s;
     for (int i = 0; i < n - 1; ++i) {
@@ -113,15 +168,17 @@ __device__ inline void w_integ(const double* x, const double* f, double* fint, i
       fint[i + 1] = s;
     }
   }
-  wsync();
+  g.sync();
 }
 
 // ---------------------------------------------------------------- DERIV
-__device__ inline void w_deriv(const double* x, const double* f, double* dfdx, int n, int lane) {
+template <class G>
+__device__ inline void g_deriv(G& g, const double* x, const double* f, double* dfdx, int n) {
+  constexpr int C = (kKwMax + G::N - 1) / G::N;
   const double s = fabs(x[1] - x[0]) / (x[1] - x[0]);
-  double v[4];
+  double v[C];
   int cnt = 0;
-  for (int j = lane; j < n; j += 32, ++cnt) {
+  for (int j = g.r; j < n; j += G::N, ++cnt) {
     if (j == 0) {
       v[cnt] = (f[1] - f[0]) / (x[1] - x[0]);
     } else if (j == n - 1) {
@@ -136,10 +193,10 @@ __device__ inline void w_deriv(const double* x, const double* f, double* dfdx, i
       v[cnt] = (tr + tl) / (1.0 - tr * tl) * scale;
     }
   }
-  wsync();  // dfdx may alias f in callers
+  g.sync();  // dfdx may alias f in callers
   cnt = 0;
-  for (int j = lane; j < n; j += 32, ++cnt) dfdx[j] = v[cnt];
-  wsync();
+  for (int j = g.r; j < n; j += G::N, ++cnt) dfdx[j] = v[cnt];
+  g.sync();
 }
 
 // ---------------------------------------------------------------- MAP1
@@ -169,10 +226,11 @@ __device__ __forceinline__ void map1_for(const double* xo, const double* fo, int
 }
 
 // Returns MAP1 (index of the last old interval used).  xnew ascending.
-__device__ inline int w_map1(const double* xo, const double* fo, int nold, const double* xn,
-                             double* fn, int nnew, int* lidx, int lane) {
+template <class G>
+__device__ inline int g_map1(G& g, const double* xo, const double* fo, int nold, const double* xn,
+                             double* fn, int nnew, int* lidx) {
   // bracket: L_k = min{L >= 2 : XOLD(L) > XNEW(k)}, nold+1 when past the end
-  for (int k = lane; k < nnew; k += 32) {
+  for (int k = g.r; k < nnew; k += G::N) {
     const double v = xn[k];
     int lo = 2, hi = nold + 1;  // search in [2, nold+1)
     while (lo < hi) {
@@ -182,8 +240,8 @@ __device__ inline int w_map1(const double* xo, const double* fo, int nold, const
     }
     lidx[k] = lo;
   }
-  wsync();
-  for (int k = lane; k < nnew; k += 32) {
+  g.sync();
+  for (int k = g.r; k < nnew; k += G::N) {
     const int Lraw = lidx[k];
     const bool past = Lraw > nold;
     const double v = xn[k];
@@ -219,18 +277,20 @@ __device__ inline int w_map1(const double* xo, const double* fo, int nold, const
     }
     fn[k] = A + (B + C * v) * v;
   }
-  wsync();
+  g.sync();
   const int Llast = lidx[nnew - 1];
   const int ll = Llast > nold ? nold : Llast;
-  wsync();
+  g.sync();
   return ll - 1;
 }
 
 // ---------------------------------------------------------------- SOLVIT
-// Gaussian elimination with partial pivoting on ws.A (kNx x kNx, ld kLd),
-// right-hand side / solution in b.  Reference pivot rule: first maximum.
+constexpr double kPivotTol = 1.0e-30;
+
+// Gaussian elimination with partial pivoting on A (kNx x kNx, column-major,
+// ld kLd, shared memory), right-hand side / solution in b.  Reference pivot
+// rule: first maximum.  One warp.
 __device__ inline void w_solvit(double* __restrict__ A, double* __restrict__ b, int lane) {
-  constexpr double PIVOT_TOL = 1.0e-30;
   constexpr int n = kNx;
   int mypiv0 = 0, mypiv1 = 0;  // pivot of column i for i = lane, lane+32
   for (int i = 0; i < n - 1; ++i) {
@@ -269,7 +329,7 @@ __device__ inline void w_solvit(double* __restrict__ A, double* __restrict__ b, 
     wsync();
     // (c) reciprocal pivot on the diagonal
     double pv = A[i * kLd + m];
-    if (fabs(pv) < PIVOT_TOL) pv = copysign(PIVOT_TOL, pv);
+    if (fabs(pv) < kPivotTol) pv = copysign(kPivotTol, pv);
     const double pivot = 1.0 / pv;
     const double aii = A[i * kLd + i];
     wsync();
@@ -298,7 +358,7 @@ __device__ inline void w_solvit(double* __restrict__ A, double* __restrict__ b, 
   }
   if (lane == 0) {
     double v = A[(n - 1) * kLd + n - 1];
-    if (fabs(v) < PIVOT_TOL) v = copysign(PIVOT_TOL, v);
+    if (fabs(v) < kPivotTol) v = copysign(kPivotTol, v);
     A[(n - 1) * kLd + n - 1] = 1.0 / v;
   }
   wsync();
@@ -330,33 +390,141 @@ __device__ inline void w_solvit(double* __restrict__ A, double* __restrict__ b, 
   wsync();
 }
 
+// (I - diag(XALPHA) COEFJ) XS = (1 - XALPHA) XSBAR by one warp: the matrix
+// AMAT(L,M) = -XALPHA(L)*COEFJ(L,M) (+1 on the diagonal) in shared memory A.
+__device__ inline void scatter_solve(WarpG& g, const JoshOps& ops, JoshWS& ws, double* A) {
+  for (int m = 0; m < kNx; ++m) {
+    for (int l = g.r; l < kNx; l += 32) {
+      double v = -ws.xalpha[l] * ops.coefj[m * kNx + l];
+      if (l == m) v = v + 1.0;
+      A[m * kLd + l] = v;
+    }
+  }
+  for (int l = g.r; l < kNx; l += 32) ws.xs[l] = (1.0 - ws.xalpha[l]) * ws.xsbar[l];
+  g.sync();
+  w_solvit(A, ws.xs, g.r);
+}
+
+// The same system by a pair group, thread r < 51 holding row r of
+// [AMAT | rhs] in registers.  The elimination follows SOLVIT's arithmetic:
+// the pivot of step i is the first maximum |A(k,i)| over the rows at
+// positions i..50 (rows are swapped logically: each thread tracks the
+// position of its row), the pivot is replaced by its reciprocal (clamped at
+// 1e-30), multipliers are A(k,i) * (1/pivot), the right-hand side is
+// eliminated with the same multipliers in step order, and back substitution
+// runs column by column from the last.
+static __device__ __forceinline__ void scatter_solve(PairG& g, const JoshOps& ops, JoshWS& ws, double* /*unused*/) {
+  constexpr int n = kNx;
+  const bool own = g.r < n;
+  double a[n + 1];
+  {
+    const int l = own ? g.r : 0;
+    const double xa = ws.xalpha[l];
+#pragma unroll
+    for (int m = 0; m < n; ++m) {
+      double v = -xa * ops.coefj[m * kNx + l];
+      if (l == m) v = v + 1.0;
+      a[m] = v;
+    }
+    a[n] = (1.0 - xa) * ws.xsbar[l];
+  }
+  int pos = own ? g.r : n + 1;  // current row position
+  bool done = !own;
+  double rp = 0.0;  // reciprocal pivot of this row once it is the pivot
+#pragma unroll
+  for (int i = 0; i < n - 1; ++i) {
+    // (a) pivot: max |A(pos, i)| over pending rows, ties to the lowest position
+    double best = done ? -1.0 : fabs(a[i]);
+    int bpos = done ? (1 << 20) : pos;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int op = __shfl_xor_sync(0xffffffffu, bpos, o);
+      if (ob > best || (ob == best && op < bpos)) {
+        best = ob;
+        bpos = op;
+      }
+    }
+    if ((g.r & 31) == 0) {
+      ws.pval[g.r >> 5] = best;
+      ws.piv[g.r >> 5] = bpos;
+    }
+    g.sync();
+    {
+      const double b0 = ws.pval[0], b1 = ws.pval[1];
+      const int p0 = ws.piv[0], p1 = ws.piv[1];
+      bpos = (b1 > b0 || (b1 == b0 && p1 < p0)) ? p1 : p0;
+    }
+    const bool me = !done && pos == bpos;
+    // (b) the row at position i moves to the pivot's position
+    if (!done && !me && pos == i) pos = bpos;
+    // (c) the pivot row, with its reciprocal pivot, to every thread
+    if (me) {
+      double pv = a[i];
+      if (fabs(pv) < kPivotTol) pv = copysign(kPivotTol, pv);
+      rp = 1.0 / pv;
+      ws.prow[i] = rp;
+#pragma unroll
+      for (int j = i + 1; j <= n; ++j) ws.prow[j] = a[j];
+      pos = i;
+      done = true;
+    }
+    g.sync();
+    // (d, e) multiplier and trailing update of the pending rows (rhs included)
+    if (!done) {
+      const double l = a[i] * ws.prow[i];
+#pragma unroll
+      for (int j = i + 1; j <= n; ++j) a[j] = a[j] - l * ws.prow[j];
+    }
+  }
+  // the last pending row takes position n-1
+  if (!done) {
+    pos = n - 1;
+    double v = a[n - 1];
+    if (fabs(v) < kPivotTol) v = copysign(kPivotTol, v);
+    rp = 1.0 / v;
+  }
+  // back substitution: X(j) = B(j) * (1/pivot), then B(k) -= A(k,j) X(j), k < j
+  double b = a[n];
+#pragma unroll
+  for (int j = n - 1; j >= 0; --j) {
+    if (own && pos == j) {
+      b = b * rp;
+      ws.xs[j] = b;
+    }
+    g.sync();
+    if (own && pos < j) b = b - a[j] * ws.xs[j];
+  }
+  g.sync();
+}
+
 // ---------------------------------------------------------------- JOSH
 // Inputs in ws.*: abtot/alpha/snubar are formed here from the opacity
 // vectors.  rhox is shared by the CTA.  ifsurf = 1 returns H(1); ifsurf = 0
 // fills full (SNU, JNU, HNU, JMINS, KNU(1), MAXJ) as the reference does.
+// A: shared-memory matrix for a warp group (unused by a pair group).
 // Returns the number of Eddington sweeps run (0 if none).
-__device__ inline int w_josh(const JoshOps& ops, const double* rhox, int nr, const double* acont,
+template <class G>
+__device__ inline int g_josh(G& g, const JoshOps& ops, const double* rhox, int nr, const double* acont,
                              const double* aline, const double* sigmac, const double* sigmal,
-                             const double* scont, const double* sline, const double* bnu,
-                             JoshWS& ws,
-                             JoshWSFull* full, double* hsurf, int lane) {
-  for (int j = lane; j < nr; j += 32) {
+                             const double* scont, const double* sline, const double* bnu, JoshWS& ws,
+                             double* A, JoshWSFull* full, double* hsurf) {
+  for (int j = g.r; j < nr; j += G::N) {
     const double ab = acont[j] + aline[j] + sigmac[j] + sigmal[j];
     ws.abtot[j] = ab;
     ws.alpha[j] = (sigmac[j] + sigmal[j]) / ab;
     ws.snubar[j] = (acont[j] * scont[j] + aline[j] * sline[j]) / (acont[j] + aline[j]);
   }
-  wsync();
-  w_integ(rhox, ws.abtot, ws.taunu, nr, ws.abtot[0] * rhox[0], ws, lane);
+  g.sync();
+  g_integ(g, rhox, ws.abtot, ws.taunu, nr, ws.abtot[0] * rhox[0], ws);
   int maxj = 0;
   if (ws.taunu[0] > ops.xtau[kNx - 1]) maxj = 1;
   if (maxj != 1) {
-    maxj = w_map1(ws.taunu, ws.snubar, nr, ops.xtau, ws.xsbar, kNx, ws.lidx, lane);
-    maxj = w_map1(ws.taunu, ws.alpha, nr, ops.xtau, ws.xalpha, kNx, ws.lidx, lane);
+    maxj = g_map1(g, ws.taunu, ws.snubar, nr, ops.xtau, ws.xsbar, kNx, ws.lidx);
+    maxj = g_map1(g, ws.taunu, ws.alpha, nr, ops.xtau, ws.xalpha, kNx, ws.lidx);
     const double tau1 = ws.taunu[0];
-    double amax = 0.0;
-    bool any = false;
-    for (int l = lane; l < kNx; l += 32) {
+    double amax = -1.0;
+    for (int l = g.r; l < kNx; l += G::N) {
       double xa = fmax(ws.xalpha[l], 0.0);
       double xb = fmax(ws.xsbar[l], 1.0e-38);
       if (ops.xtau[l] < tau1) {
@@ -365,40 +533,29 @@ __device__ inline int w_josh(const JoshOps& ops, const double* rhox, int nr, con
       }
       ws.xalpha[l] = xa;
       ws.xsbar[l] = xb;
-      if (!any || xa > amax) amax = xa;
-      any = true;
+      amax = fmax(amax, xa);
     }
-    amax = warp_max(any ? amax : -1.0);
-    wsync();
+    amax = g.max(amax);
+    g.sync();
     if (amax <= 0.0) {
-      for (int l = lane; l < kNx; l += 32) ws.xs[l] = fmax(ws.xsbar[l], 1.0e-37);
-      wsync();
+      for (int l = g.r; l < kNx; l += G::N) ws.xs[l] = fmax(ws.xsbar[l], 1.0e-37);
+      g.sync();
     } else {
-      // AMAT(L,M) = -XALPHA(L)*COEFJ(L,M), +1 on the diagonal; lanes own rows
-      for (int m = 0; m < kNx; ++m) {
-        for (int l = lane; l < kNx; l += 32) {
-          double v = -ws.xalpha[l] * ops.coefj[m * kNx + l];
-          if (l == m) v = v + 1.0;
-          ws.A[m * kLd + l] = v;
-        }
-      }
-      for (int l = lane; l < kNx; l += 32) ws.xs[l] = (1.0 - ws.xalpha[l]) * ws.xsbar[l];
-      wsync();
-      w_solvit(ws.A, ws.xs, lane);
-      for (int l = lane; l < kNx; l += 32) ws.xs[l] = fmax(ws.xs[l], 1.0e-37);
-      wsync();
+      scatter_solve(g, ops, ws, A);
+      for (int l = g.r; l < kNx; l += G::N) ws.xs[l] = fmax(ws.xs[l], 1.0e-37);
+      g.sync();
     }
     if (full == nullptr) {
       // IFSURF = 1: H(1) = sum CH_J * XS in the reference order
-      if (lane == 0) {
+      if (g.r == 0) {
         double h = 0.0;
         for (int m = 0; m < kNx; ++m) h = h + ops.ch[m] * ws.xs[m];
         *hsurf = h;
       }
-      wsync();
+      g.sync();
       return 0;
     }
-    w_map1(ops.xtau, ws.xs, kNx, ws.taunu, full->snu, maxj, ws.lidx, lane);
+    g_map1(g, ops.xtau, ws.xs, kNx, ws.taunu, full->snu, maxj, ws.lidx);
   }
   // JOSH with IFSURF = 1 and MAXJ = 1 falls through to the Eddington sweep
   // IFSURF = 1 with an optically thick surface borrows the scratch vectors
@@ -411,40 +568,40 @@ __device__ inline int w_josh(const JoshOps& ops, const double* rhox, int nr, con
   double* jnu = F ? F->jnu : nullptr;
   if (maxj != nr) {
     const int maxj1 = (maxj == 1) ? 1 : maxj + 1;
-    for (int j = maxj1 - 1 + lane; j < nr; j += 32) snu[j] = ws.snubar[j];
-    wsync();
+    for (int j = maxj1 - 1 + g.r; j < nr; j += G::N) snu[j] = ws.snubar[j];
+    g.sync();
     const int m = maxj - 1 > 1 ? maxj - 1 : 1;
     const int nm1 = nr - m + 1, nmj = nr - maxj + 1;
     for (int l = 1; l <= 50; ++l) {
       sweeps = l;
       // negative SNU -> reset to BNU
       bool neg = false;
-      for (int j = m - 1 + lane; j < nr; j += 32) neg |= (snu[j] <= 0.0);
-      int ifneg = __any_sync(0xffffffffu, neg) ? 1 : 0;
+      for (int j = m - 1 + g.r; j < nr; j += G::N) neg |= (snu[j] <= 0.0);
+      int ifneg = g.any(neg) ? 1 : 0;
       if (ifneg) {
-        for (int j = m - 1 + lane; j < nr; j += 32) {
+        for (int j = m - 1 + g.r; j < nr; j += G::N) {
           ws.snubar[j] = bnu[j];
           snu[j] = bnu[j];
         }
-        wsync();
+        g.sync();
       }
-      w_deriv(ws.taunu + m - 1, snu + m - 1, hnu + m - 1, nm1, lane);
+      g_deriv(g, ws.taunu + m - 1, snu + m - 1, hnu + m - 1, nm1);
       bool hneg = false;
-      for (int j = m - 1 + lane; j < nr; j += 32) hneg |= (hnu[j] <= 0.0);
-      if (__any_sync(0xffffffffu, hneg)) {
+      for (int j = m - 1 + g.r; j < nr; j += G::N) hneg |= (hnu[j] <= 0.0);
+      if (g.any(hneg)) {
         ifneg = 1;
-        for (int j = m - 1 + lane; j < nr; j += 32) {
+        for (int j = m - 1 + g.r; j < nr; j += G::N) {
           ws.snubar[j] = bnu[j];
           snu[j] = bnu[j];
         }
-        wsync();
-        w_deriv(ws.taunu + m - 1, snu + m - 1, hnu + m - 1, nm1, lane);
+        g.sync();
+        g_deriv(g, ws.taunu + m - 1, snu + m - 1, hnu + m - 1, nm1);
       }
-      for (int j = m - 1 + lane; j < nr; j += 32) hnu[j] = hnu[j] / 3.0;
-      wsync();
-      w_deriv(ws.taunu + maxj - 1, hnu + maxj - 1, jmins + maxj - 1, nmj, lane);
+      for (int j = m - 1 + g.r; j < nr; j += G::N) hnu[j] = hnu[j] / 3.0;
+      g.sync();
+      g_deriv(g, ws.taunu + maxj - 1, hnu + maxj - 1, jmins + maxj - 1, nmj);
       double err = 0.0;
-      for (int j = maxj1 - 1 + lane; j < nr; j += 32) {
+      for (int j = maxj1 - 1 + g.r; j < nr; j += G::N) {
         if (ifneg) jmins[j] = 0.0;
         const double jv = jmins[j] + snu[j];
         if (jnu) jnu[j] = jv;
@@ -452,8 +609,8 @@ __device__ inline int w_josh(const JoshOps& ops, const double* rhox, int nr, con
         err += fabs(snew - snu[j]) / snew;
         snu[j] = snew;
       }
-      err = warp_sum(err);
-      wsync();
+      err = g.sum(err);
+      g.sync();
       if (err < 0.00001) break;
     }
   }
@@ -461,15 +618,15 @@ __device__ inline int w_josh(const JoshOps& ops, const double* rhox, int nr, con
     if (F) {
       F->knu1 = jnu[0] / 3.0;
       F->maxj = maxj;
-    } else if (lane == 0) {
+    } else if (g.r == 0) {
       *hsurf = hnu[0];
     }
-    wsync();
+    g.sync();
     return sweeps;
   }
   // (IFSURF = 1 never reaches here with MAXJ != 1: it returned above.)
   // J - S and H on the 51-point grid, mapped back onto the first MAXJ depths
-  for (int l = lane; l < kNx; l += 32) {
+  for (int l = g.r; l < kNx; l += G::N) {
     double xj = -ws.xs[l];
     double xh = 0.0;
     for (int mm = 0; mm < kNx; ++mm) {
@@ -479,20 +636,20 @@ __device__ inline int w_josh(const JoshOps& ops, const double* rhox, int nr, con
     ws.xw[l] = xj;
     ws.xsbar[l] = xh;  // XSBAR no longer needed: holds XH
   }
-  wsync();
-  w_map1(ops.xtau, ws.xw, kNx, ws.taunu, F->jmins, maxj, ws.lidx, lane);
-  w_map1(ops.xtau, ws.xsbar, kNx, ws.taunu, F->hnu, maxj, ws.lidx, lane);
-  if (lane == 0) {
+  g.sync();
+  g_map1(g, ops.xtau, ws.xw, kNx, ws.taunu, F->jmins, maxj, ws.lidx);
+  g_map1(g, ops.xtau, ws.xsbar, kNx, ws.taunu, F->hnu, maxj, ws.lidx);
+  if (g.r == 0) {
     double xk = 0.0;
     for (int mm = 0; mm < kNx; ++mm) xk = xk + ops.ck[mm] * ws.xs[mm];
     F->knu1 = xk;
     F->maxj = maxj;
   }
-  for (int j = lane; j < maxj; j += 32) {
+  for (int j = g.r; j < maxj; j += G::N) {
     F->snu[j] = fmax(F->snu[j], 1.0e-38);
     F->jnu[j] = fmax(F->jmins[j] + F->snu[j], 1.0e-38);
   }
-  wsync();
+  g.sync();
   return sweeps;
 }
 

@@ -123,7 +123,7 @@ __device__ inline EosOut surrogate_depth(double t, double p, double vturb_cms, i
   return o;
 }
 
-__device__ __forceinline__ void surrogate_kapp(const ContCoef& c, double w, double& kabs, double& sigma) {
+static __device__ __noinline__ void surrogate_kapp(const ContCoef& c, double w, double& kabs, double& sigma) {
   double x = w / 1642.0;
   x = x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x);
   const double abf = 4.0e-17 * 6.0 * (x * sqrt(x)) * ((1.0 - x) * sqrt(1.0 - x)) * 4.0;

@@ -288,6 +288,7 @@ struct SpecArgs {
 
 struct SpecWS {
   JoshWS w;
+  double A[kNx * kLd];  // the warp's scattering matrix
   double acont[kKwMax], sigmac[kKwMax], aline[kKwMax], sigmal[kKwMax], sline[kKwMax],
       bnu[kKwMax];
 };
@@ -295,6 +296,7 @@ struct SpecWS {
 static __global__ void __launch_bounds__(128) k_spectrum(SpecArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  WarpG g(lane);
   const int nwarp = blockDim.x >> 5;
   double* rhox_s = reinterpret_cast<double*>(smem_raw);
   SpecWS* wsa = reinterpret_cast<SpecWS*>(smem_raw + sizeof(double) * kKwMax);
@@ -336,8 +338,8 @@ static __global__ void __launch_bounds__(128) k_spectrum(SpecArgs a) {
     }
     wsync();
     double surf = 0.0, hnu = 0.0;
-    w_josh(ops, rhox_s, nr, S.acont, S.aline, S.sigmac, S.sigmal, S.bnu, S.sline, S.bnu, S.w,
-           nullptr, &surf, lane);
+    g_josh(g, ops, rhox_s, nr, S.acont, S.aline, S.sigmac, S.sigmal, S.bnu, S.sline, S.bnu, S.w, S.A,
+           nullptr, &surf);
     surf = __shfl_sync(0xffffffffu, surf, 0);
     for (int j = lane; j < nr; j += 32) {
       const double ehvkt = exp(-freq * a.hkt[j]);
@@ -349,8 +351,8 @@ static __global__ void __launch_bounds__(128) k_spectrum(SpecArgs a) {
       S.sigmal[j] = 0.0;
     }
     wsync();
-    w_josh(ops, rhox_s, nr, S.acont, S.aline, S.sigmac, S.sigmal, S.bnu, S.sline, S.bnu, S.w,
-           nullptr, &hnu, lane);
+    g_josh(g, ops, rhox_s, nr, S.acont, S.aline, S.sigmac, S.sigmal, S.bnu, S.sline, S.bnu, S.w, S.A,
+           nullptr, &hnu);
     if (lane == 0) {
       const double resid = hnu / surf;
       a.flux[iw] = resid * surf;
