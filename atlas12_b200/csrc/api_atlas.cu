@@ -87,7 +87,7 @@ int atlas_prep_lines(atlasgpu_ctx* ctx, const int32_t* d_ld, const int32_t* h_ld
 
 namespace {
 
-int rt_launch(atlasgpu_ctx* ctx, RtArgs& a, bool surr, double* d_sum, int* nwarps_out) {
+int rt_launch(atlasgpu_ctx* ctx, RtArgs& a, double* d_sum, int* nwarps_out) {
   const size_t smem = rt_smem_bytes();
   // enough groups to fill every SM several times, frequencies contiguous per group
   const int target = ctx->nsm * 3 * kRtGroups * 4;
@@ -97,17 +97,12 @@ int rt_launch(atlasgpu_ctx* ctx, RtArgs& a, bool surr, double* d_sum, int* nwarp
   const int nwl = blocks * kRtGroups;
   double* part;
   int r;
-  if ((r = bufT(ctx, surr ? "rt_part_m" : "rt_part", (size_t)nwl * (kAcc * a.kw + 1), &part))) return r;
+  if ((r = bufT(ctx, "rt_part", (size_t)nwl * (kAcc * a.kw + 1), &part))) return r;
   a.partial = part;
-  if (surr) {
-    CK(cudaFuncSetAttribute(k_atlas_rt<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  } else {
-    CK(cudaFuncSetAttribute(k_atlas_rt<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  }
+  CK(cudaFuncSetAttribute(k_atlas_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   {
     Timer tm(ctx, "atlas_rt");
-    if (surr) k_atlas_rt<true><<<blocks, kRtThreads, smem, ctx->stream>>>(a);
-    else k_atlas_rt<false><<<blocks, kRtThreads, smem, ctx->stream>>>(a);
+    k_atlas_rt<<<blocks, kRtThreads, smem, ctx->stream>>>(a);
     CKL(ctx);
   }
   {
@@ -233,9 +228,9 @@ int atlasgpu_atlas_rt_pass(atlasgpu_ctx* ctx, int numnu, const double* waveset, 
   CK(cudaMemcpyAsync(d_rx, rhox, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(d_t, t, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(d_hk, hkt, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
-  RtArgs a{ctx->ops, nullptr, numnu, nrhox, kw, d_ws, d_rc, d_ac, d_sg, d_sc, d_xl0, d_rx, d_t, d_hk, teff,
+  RtArgs a{ctx->ops, numnu, nrhox, kw, d_ws, d_rc, d_ac, d_sg, d_sc, d_xl0, d_rx, d_t, d_hk, teff,
            1, 1, kw, nullptr, d_hs, nullptr};
-  if ((r = rt_launch(ctx, a, false, d_sum, nullptr))) return r;
+  if ((r = rt_launch(ctx, a, d_sum, nullptr))) return r;
   std::vector<double> hsum(kAcc * kw + 1);
   CK(cudaMemcpyAsync(hsum.data(), d_sum, hsum.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
   if (hsurf_out) CK(cudaMemcpyAsync(hsurf_out, d_hs, numnu * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -26,6 +26,7 @@ struct atlasgpu_model {
   double *xnfdop, *dopple;  // [nspec][kw]
   double *xne_eos, *txnxn, *hkt, *hckt, *rho;  // [kw]
   ContCoef* cc;          // [kw]
+  double *acont, *sigmac;  // the RT pass's continuum [numnu][kw]
   double *waveset, *rcoset, *cutwave, *tabcont;  // tabcont [nwave+1][kw]
   int32_t* iwavetab;
   int32_t* linedata;
@@ -104,6 +105,20 @@ __global__ void __launch_bounds__(kFinThreads) k_model_finish(ModelState* ms, do
   }
 }
 
+// KAPP stand-in for the RT pass: ACONT, SIGMAC [numnu][kw] from the surrogate
+// continuum coefficients of this iteration's structure
+__global__ void k_model_kapp(const double* waveset, int numnu, int nrhox, int kw, const ContCoef* cc,
+                             double* acont, double* sigmac) {
+  const int64_t n = (int64_t)numnu * nrhox;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int nu = (int)(e / nrhox), j = (int)(e % nrhox);
+    double ka, sg;
+    surrogate_kapp(cc[j], waveset[nu], ka, sg);
+    acont[(size_t)nu * kw + j] = ka;
+    sigmac[(size_t)nu * kw + j] = sg;
+  }
+}
+
 __global__ void k_surrogate_eval(int nrhox, const double* t, const double* p, double vturb_cms, int nw,
                                  const double* wave, double* xnfdop, double* dopple, ContCoef* cc,
                                  double* kabs, double* sigma, double* xne, double* rho) {
@@ -149,12 +164,18 @@ int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
     k_atlas_linop<<<grid_for(ctx, m->nlines * 32, 256, 16), 256, 0, s>>>(la);
     CKL(ctx);
   }
-  RtArgs ra{ctx->ops, m->cc, m->numnu, m->nrhox, m->kw, m->waveset, m->rcoset, nullptr, nullptr, nullptr,
+  {
+    Timer tm(ctx, "model_kapp");
+    k_model_kapp<<<grid_for(ctx, (int64_t)m->numnu * m->nrhox, 256, 8), 256, 0, s>>>(
+        m->waveset, m->numnu, m->nrhox, m->kw, m->cc, m->acont, m->sigmac);
+    CKL(ctx);
+  }
+  RtArgs ra{ctx->ops, m->numnu, m->nrhox, m->kw, m->waveset, m->rcoset, m->acont, m->sigmac, nullptr,
             m->xl, (const double*)m->state + 1 * m->kw, (const double*)m->state + 0 * m->kw, m->hkt,
             m->teff, m->nu_per_group, 1, m->kw, m->partial, m->hsurf, nullptr};
   {
     Timer tm(ctx, "atlas_rt");
-    k_atlas_rt<true><<<m->blocks_rt, kRtThreads, m->smem_rt, s>>>(ra);
+    k_atlas_rt<<<m->blocks_rt, kRtThreads, m->smem_rt, s>>>(ra);
     CKL(ctx);
   }
   {
@@ -260,6 +281,7 @@ int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlas
       (r = dalloc(ctx, &m->xnfdop, (size_t)m->nspec * kw)) || (r = dalloc(ctx, &m->dopple, (size_t)m->nspec * kw)) ||
       (r = dalloc(ctx, &m->xne_eos, kw)) || (r = dalloc(ctx, &m->txnxn, kw)) || (r = dalloc(ctx, &m->hkt, kw)) ||
       (r = dalloc(ctx, &m->hckt, kw)) || (r = dalloc(ctx, &m->rho, kw)) || (r = dalloc(ctx, &m->cc, kw)) ||
+      (r = dalloc(ctx, &m->acont, (size_t)m->numnu * kw)) || (r = dalloc(ctx, &m->sigmac, (size_t)m->numnu * kw)) ||
       (r = dalloc(ctx, &m->waveset, m->numnu)) || (r = dalloc(ctx, &m->rcoset, m->numnu)) ||
       (r = dalloc(ctx, &m->cutwave, m->nwave)) || (r = dalloc(ctx, &m->tabcont, (size_t)(m->nwave + 1) * kw)) ||
       (r = dalloc(ctx, &m->iwavetab, m->nwave + 1)) || (r = dalloc(ctx, &m->linedata, (size_t)m->nlines * 4)) ||
@@ -282,7 +304,7 @@ int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlas
     atlasgpu_model_destroy(ctx, m);
     return r;
   }
-  CK(cudaFuncSetAttribute(k_atlas_rt<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->smem_rt));
+  CK(cudaFuncSetAttribute(k_atlas_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->smem_rt));
   if (fin_smem_bytes(kw, kRossMax) > (size_t)ctx->smem_optin) {
     atlasgpu_model_destroy(ctx, m);
     return fail(ctx, ATLASGPU_EINVAL, "model_create: finish needs %zu B of shared memory",
@@ -384,7 +406,7 @@ int atlasgpu_model_iterate(atlasgpu_ctx* ctx, atlasgpu_model* m, int max_iter, d
         ctx->launches = l0;  // counted when replayed
       }
       CK(cudaGraphLaunch(m->gexec, s));
-      ctx->launches += 5;
+      ctx->launches += 6;
     } else {
       if ((r = enqueue_iteration(ctx, m, true))) return r;
     }
@@ -450,6 +472,7 @@ int atlasgpu_model_destroy(atlasgpu_ctx* ctx, atlasgpu_model* m) {
   if (m->gexec) cudaGraphExecDestroy(m->gexec);
   if (m->graph) cudaGraphDestroy(m->graph);
   void* ps[] = {m->state, m->ms, m->xnfdop, m->dopple, m->xne_eos, m->txnxn, m->hkt, m->hckt, m->rho, m->cc,
+                m->acont, m->sigmac,
                 m->waveset, m->rcoset, m->cutwave, m->tabcont, m->iwavetab, m->linedata, m->lines, m->xl,
                 m->partial, m->sum, m->hsurf, m->h0, m->h1, m->h2, m->ross, m->R, m->iter_dev,
                 m->maxerr_dev, m->cnt};

@@ -76,10 +76,10 @@ int atlasgpu_atlas_rt_pass_noalloc(atlasgpu_ctx* ctx, int numnu, const double* d
   if (nwl > kNoAllocRows)
     return fail(ctx, ATLASGPU_EINVAL, "rt_pass_noalloc: %d thread groups exceed the scratch limit %d", nwl,
                 kNoAllocRows);
-  CK(cudaFuncSetAttribute(k_atlas_rt<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  RtArgs a{ctx->ops, nullptr, numnu, nrhox, kw, d_waveset, d_rcoset, d_acont, d_sigmac, d_scont, d_xlines_t,
+  CK(cudaFuncSetAttribute(k_atlas_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  RtArgs a{ctx->ops, numnu, nrhox, kw, d_waveset, d_rcoset, d_acont, d_sigmac, d_scont, d_xlines_t,
            d_rhox, d_t, d_hkt, teff, npw, numnu, 1, partial, d_hsurf, nullptr};
-  k_atlas_rt<false><<<blocks, kRtThreads, smem, ctx->stream>>>(a);
+  k_atlas_rt<<<blocks, kRtThreads, smem, ctx->stream>>>(a);
   CKL(ctx);
   launch_reduce(partial, nwl, kw, d_sums, ctx->stream);
   CKL(ctx);

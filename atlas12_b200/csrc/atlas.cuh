@@ -304,7 +304,6 @@ constexpr int kAcc = 8;  // rjmins, rdabh, rdiagj, flxrad, raden, h_total, accra
 
 struct RtArgs {
   const JoshOps* ops;
-  const ContCoef* cc;                    // surrogate continuum coefficients [kw] (surrogate mode)
   int numnu, nrhox, kw;
   const double *waveset, *rcoset;
   const double *acont, *sigmac, *scont;  // [numnu][kw]; scont may be null (=> BNU)
@@ -321,8 +320,9 @@ struct RtArgs {
 struct RtWS {
   JoshWS w;
   JoshWSFull f;
-  double acont[kKwMax], sigmac[kKwMax], aline[kKwMax], sigmal[kKwMax], scont[kKwMax],
-      stim[kKwMax], dab[kKwMax];
+  double acont[kKwMax], sigmac[kKwMax], aline[kKwMax], stim[kKwMax];
+  double dab[kKwMax];           // SCONT while JOSH runs (when given), then d(abtot)/d(rhox)
+  double U[kNx * (kNx + 1)];    // pivot rows of the 51x51 factorisation
 };
 
 // One pair group (64 threads) per frequency, kRtGroups groups per CTA.  The
@@ -331,15 +331,19 @@ struct RtWS {
 constexpr int kRtGroups = 2;
 constexpr int kRtThreads = kRtGroups * PairG::N;
 
-__host__ __device__ inline size_t rt_smem_bytes() { return sizeof(double) * kKwMax + kRtGroups * sizeof(RtWS); }
+// shared memory: RHOX and a zero vector (SIGMAL) for the CTA, then the groups' workspaces
+__host__ __device__ inline size_t rt_smem_bytes() { return 2 * sizeof(double) * kKwMax + kRtGroups * sizeof(RtWS); }
 
-template <bool kSurr>
 static __global__ void __launch_bounds__(kRtThreads, 3) k_atlas_rt(RtArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int gid = threadIdx.x / PairG::N;
   double* rhox_s = reinterpret_cast<double*>(smem_raw);
-  RtWS& S = reinterpret_cast<RtWS*>(smem_raw + sizeof(double) * kKwMax)[gid];
-  for (int j = threadIdx.x; j < a.nrhox; j += blockDim.x) rhox_s[j] = a.rhox[j];
+  double* zero_s = rhox_s + kKwMax;
+  RtWS& S = reinterpret_cast<RtWS*>(smem_raw + 2 * sizeof(double) * kKwMax)[gid];
+  for (int j = threadIdx.x; j < a.nrhox; j += blockDim.x) {
+    rhox_s[j] = a.rhox[j];
+    zero_s[j] = 0.0;
+  }
   __syncthreads();
   PairG g(threadIdx.x % PairG::N, 1 + gid, S.w.red);
   constexpr int C = (kKwMax + PairG::N - 1) / PairG::N;
@@ -365,23 +369,14 @@ static __global__ void __launch_bounds__(kRtThreads, 3) k_atlas_rt(RtArgs a) {
       const double bnu = kBnuPrefac * f3 * ehvkt / stim;
       S.stim[j] = stim;
       S.f.bnu[j] = bnu;
-      if (kSurr) {
-        double ka, sg;
-        surrogate_kapp(a.cc[j], wave, ka, sg);
-        S.acont[j] = ka;
-        S.sigmac[j] = sg;
-        S.scont[j] = bnu;
-      } else {
-        S.acont[j] = a.acont[(size_t)(nu - 1) * a.kw + j];
-        S.sigmac[j] = a.sigmac[(size_t)(nu - 1) * a.kw + j];
-        S.scont[j] = a.scont ? a.scont[(size_t)(nu - 1) * a.kw + j] : bnu;
-      }
+      S.acont[j] = a.acont[(size_t)(nu - 1) * a.kw + j];
+      S.sigmac[j] = a.sigmac[(size_t)(nu - 1) * a.kw + j];
+      if (a.scont) S.dab[j] = a.scont[(size_t)(nu - 1) * a.kw + j];
       S.aline[j] = 0.0 + a.xl[(size_t)j * a.xl_sj + (size_t)(nu - 1) * a.xl_snu] * stim;
-      S.sigmal[j] = 0.0;
     }
     g.sync();
-    const int sw = g_josh(g, ops, rhox_s, nr, S.acont, S.aline, S.sigmac, S.sigmal, S.scont, S.f.bnu,
-                          S.f.bnu, S.w, nullptr, &S.f, nullptr);
+    const int sw = g_josh(g, ops, rhox_s, nr, S.acont, S.aline, S.sigmac, zero_s, a.scont ? S.dab : S.f.bnu,
+                          S.f.bnu, S.f.bnu, S.w, S.U, &S.f, nullptr);
     if (a.sweeps && g.r == 0) a.sweeps[nu - 1] = sw;
     // negative floor (RUN_RT_PASS :3926-3937)
     bool neg = false;

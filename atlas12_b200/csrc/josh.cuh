@@ -17,8 +17,8 @@
 //
 // The 51x51 scattering system: a warp group factors it in shared memory
 // (w_solvit); a pair group keeps one matrix row per thread in registers and
-// broadcasts only the pivot row (pair_solve), which takes the 21 KB matrix
-// out of shared memory and the row updates off the shared-memory pipe.
+// writes only the pivot rows to shared memory, which takes the row updates
+// off the shared-memory pipe.
 #pragma once
 #include "common.cuh"
 
@@ -72,11 +72,9 @@ struct JoshWS {
   double xs[kNx], xsbar[kNx], xalpha[kNx], xw[kNx];
   double abtot[kKwMax], alpha[kKwMax], snubar[kKwMax], taunu[kKwMax];
   double t1[kKwMax], t2[kKwMax], t3[kKwMax];  // scratch (PARCOE a,b,c / terms)
-  double prow[kNx + 1];                       // pivot row broadcast (pair groups)
   double red[4];                              // group reductions (pair groups)
   int lidx[kKwMax + 4];                       // MAP1 bracket indices
-  int piv[2];                                 // pivot (value slot, position) exchange
-  double pval[2];
+  unsigned pk[2][3];                          // pivot key exchange between the pair's warps
 };
 
 // Full-solution extras for IFSURF = 0 (ATLAS)
@@ -413,10 +411,18 @@ __device__ inline void scatter_solve(WarpG& g, const JoshOps& ops, JoshWS& ws, d
 // 1e-30), multipliers are A(k,i) * (1/pivot), the right-hand side is
 // eliminated with the same multipliers in step order, and back substitution
 // runs column by column from the last.
-static __device__ __forceinline__ void scatter_solve(PairG& g, const JoshOps& ops, JoshWS& ws, double* /*unused*/) {
-  constexpr int n = kNx;
+// Each step shifts the pending rows one column left, so column i is always
+// register a[0] and the loop over steps stays rolled (one short loop body
+// instead of 51 unrolled steps).  The pivot row of step i is stored in
+// U[i][0..51] (U[i][0] = 1/pivot, U[i][t] = column i+t, the rhs at t = 51-i)
+// for the other rows' update and for the back substitution.
+// The pivot search reduces a 64-bit key (|a| bits, then position) with
+// redux.sync per warp and one exchange between the two warps.
+static __device__ __forceinline__ void scatter_solve(PairG& g, const JoshOps& ops, JoshWS& ws, double* U) {
+  constexpr int n = kNx, W = kNx + 1;
+  constexpr unsigned FULL = 0xffffffffu;
   const bool own = g.r < n;
-  double a[n + 1];
+  double a[W];
   {
     const int l = own ? g.r : 0;
     const double xa = ws.xalpha[l];
@@ -430,70 +436,72 @@ static __device__ __forceinline__ void scatter_solve(PairG& g, const JoshOps& op
   }
   int pos = own ? g.r : n + 1;  // current row position
   bool done = !own;
-  double rp = 0.0;  // reciprocal pivot of this row once it is the pivot
-#pragma unroll
   for (int i = 0; i < n - 1; ++i) {
     // (a) pivot: max |A(pos, i)| over pending rows, ties to the lowest position
-    double best = done ? -1.0 : fabs(a[i]);
-    int bpos = done ? (1 << 20) : pos;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const int op = __shfl_xor_sync(0xffffffffu, bpos, o);
-      if (ob > best || (ob == best && op < bpos)) {
-        best = ob;
-        bpos = op;
-      }
+    unsigned hi = 0u, lo = 0u;
+    if (!done) {
+      const unsigned long long bits = (unsigned long long)__double_as_longlong(fabs(a[0]));
+      hi = (unsigned)(bits >> 32) + 1u;  // 0 marks rows already eliminated
+      lo = (unsigned)bits;
     }
+    const unsigned mhi = __reduce_max_sync(FULL, hi);
+    const unsigned mlo = __reduce_max_sync(FULL, hi == mhi ? lo : 0u);
+    const unsigned mpos =
+        __reduce_min_sync(FULL, (hi != 0u && hi == mhi && lo == mlo) ? (unsigned)pos : 0xffffffffu);
     if ((g.r & 31) == 0) {
-      ws.pval[g.r >> 5] = best;
-      ws.piv[g.r >> 5] = bpos;
+      ws.pk[g.r >> 5][0] = mhi;
+      ws.pk[g.r >> 5][1] = mlo;
+      ws.pk[g.r >> 5][2] = mpos;
     }
     g.sync();
+    unsigned bpos;
     {
-      const double b0 = ws.pval[0], b1 = ws.pval[1];
-      const int p0 = ws.piv[0], p1 = ws.piv[1];
-      bpos = (b1 > b0 || (b1 == b0 && p1 < p0)) ? p1 : p0;
+      const unsigned h0 = ws.pk[0][0], l0 = ws.pk[0][1], p0 = ws.pk[0][2];
+      const unsigned h1 = ws.pk[1][0], l1 = ws.pk[1][1], p1 = ws.pk[1][2];
+      const bool second = h1 > h0 || (h1 == h0 && (l1 > l0 || (l1 == l0 && p1 < p0)));
+      bpos = second ? p1 : p0;
     }
-    const bool me = !done && pos == bpos;
+    const bool me = !done && (unsigned)pos == bpos;
     // (b) the row at position i moves to the pivot's position
-    if (!done && !me && pos == i) pos = bpos;
+    if (!done && !me && pos == i) pos = (int)bpos;
     // (c) the pivot row, with its reciprocal pivot, to every thread
+    double* ur = U + i * W;
     if (me) {
-      double pv = a[i];
+      double pv = a[0];
       if (fabs(pv) < kPivotTol) pv = copysign(kPivotTol, pv);
-      rp = 1.0 / pv;
-      ws.prow[i] = rp;
+      ur[0] = 1.0 / pv;
 #pragma unroll
-      for (int j = i + 1; j <= n; ++j) ws.prow[j] = a[j];
+      for (int t = 1; t < W; ++t) ur[t] = a[t];
       pos = i;
       done = true;
     }
     g.sync();
-    // (d, e) multiplier and trailing update of the pending rows (rhs included)
+    // (d, e) multiplier and trailing update of the pending rows, shifted left
     if (!done) {
-      const double l = a[i] * ws.prow[i];
+      const double l = a[0] * ur[0];
 #pragma unroll
-      for (int j = i + 1; j <= n; ++j) a[j] = a[j] - l * ws.prow[j];
+      for (int t = 1; t < W; ++t) a[t - 1] = a[t] - l * ur[t];
+      a[W - 1] = 0.0;
     }
   }
-  // the last pending row takes position n-1
+  // the last pending row takes position n-1: column n-1 in a[0], rhs in a[1]
   if (!done) {
     pos = n - 1;
-    double v = a[n - 1];
+    double v = a[0];
     if (fabs(v) < kPivotTol) v = copysign(kPivotTol, v);
-    rp = 1.0 / v;
+    U[(n - 1) * W] = 1.0 / v;
+    U[(n - 1) * W + 1] = a[1];
   }
+  g.sync();
   // back substitution: X(j) = B(j) * (1/pivot), then B(k) -= A(k,j) X(j), k < j
-  double b = a[n];
-#pragma unroll
+  double b = own ? U[pos * W + (W - 1 - pos)] : 0.0;
   for (int j = n - 1; j >= 0; --j) {
     if (own && pos == j) {
-      b = b * rp;
+      b = b * U[j * W];
       ws.xs[j] = b;
     }
     g.sync();
-    if (own && pos < j) b = b - a[j] * ws.xs[j];
+    if (own && pos < j) b = b - U[pos * W + (j - pos)] * ws.xs[j];
   }
   g.sync();
 }
@@ -502,7 +510,7 @@ static __device__ __forceinline__ void scatter_solve(PairG& g, const JoshOps& op
 // Inputs in ws.*: abtot/alpha/snubar are formed here from the opacity
 // vectors.  rhox is shared by the CTA.  ifsurf = 1 returns H(1); ifsurf = 0
 // fills full (SNU, JNU, HNU, JMINS, KNU(1), MAXJ) as the reference does.
-// A: shared-memory matrix for a warp group (unused by a pair group).
+// A: shared-memory matrix for a warp group, the U rows for a pair group.
 // Returns the number of Eddington sweeps run (0 if none).
 template <class G>
 __device__ inline int g_josh(G& g, const JoshOps& ops, const double* rhox, int nr, const double* acont,
