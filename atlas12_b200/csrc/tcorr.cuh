@@ -12,6 +12,7 @@
 // opacities come from ROSSTAB, the model's own kappa_R history.
 #pragma once
 #include "common.cuh"
+#include "josh.cuh"
 
 namespace atlasgpu {
 
@@ -201,7 +202,7 @@ struct FinFold {
 // shared-memory bytes of b_atlas_finish for kw depths and cap ROSSTAB points
 __host__ __device__ inline size_t fin_smem_bytes(int kw, int cap) {
   return sizeof(double) * ((size_t)(kFinVec + kFinWork + kAcc8) * kw + 1 + 3 * (size_t)cap) +
-         2 * sizeof(FinFold) + 64;
+         2 * sizeof(FinFold) + sizeof(JoshWS) + 64;
 }
 
 __device__ __forceinline__ void group_bar(int id) {
@@ -231,9 +232,9 @@ struct RossView {
   const double *t, *p, *k;
 };
 
-__device__ inline double b_rosstab(const RossView& R, double temp, double pres, int gtid, FinFold& fold,
+// tl = (log10 T - zerot) / slopet, hoisted by the caller (T is fixed per depth)
+__device__ inline double b_rosstab(const RossView& R, double tl, double pres, int gtid, FinFold& fold,
                                    int& parity, int bar) {
-  const double tl = (log10(temp) - R.zerot) / R.slopet;
   const double pl = (log10(pres) - R.zerop) / R.slopep;
   double r[4] = {1e30, 1e30, 1e30, 1e30};  // PP, PM, MP, MM
   int id[4] = {1 << 30, 1 << 30, 1 << 30, 1 << 30};
@@ -311,6 +312,7 @@ __device__ inline void b_ttaup(const RossView& R, double g, const double* tin, c
   for (int J = 1; J <= n; ++J) {
     const int j = J - 1;
     const double tj = tin[j], tauj = tau[j], pradj = prad[j];
+    const double tlj = (log10(tj) - R.zerot) / R.slopet;
     double ptj = 0.0, poj = 0.0, abj = 0.0;
     if (J == 1) plog = log(g / ab0 * tau[0]);
     else if (J <= 4) plog = plog1 + dplog1;
@@ -325,7 +327,7 @@ __device__ inline void b_ttaup(const RossView& R, double g, const double* tin, c
         poj = ptj * 1.0e-4;
         if (poj <= 0.0) poj = 1.0e-10;
       }
-      abj = b_rosstab(R, tj, poj, gtid, fold, parity, bar);
+      abj = b_rosstab(R, tlj, poj, gtid, fold, parity, bar);
       if (J == 1) ab0 = abj;
       dplog = g / abj * tauj / ptj * dlgtau;
       dplog = fmax(0.0, fmin(10.0, dplog));
@@ -365,7 +367,7 @@ __device__ inline void b_ttaup(const RossView& R, double g, const double* tin, c
       ptj = exp(plog);
       poj = ptj + (prad0 - pradj);
       if (poj <= 0.0) poj = fmax(ptj * 1.0e-4, 1.0e-10);
-      abj = b_rosstab(R, tj, poj, gtid, fold, parity, bar);
+      abj = b_rosstab(R, tlj, poj, gtid, fold, parity, bar);
       if (J == 1) ab0 = abj;
       dplog = g / abj * tauj / ptj * dlgtau;
       dplog = fmax(0.0, fmin(10.0, dplog));
@@ -376,7 +378,7 @@ __device__ inline void b_ttaup(const RossView& R, double g, const double* tin, c
       ptj = exp(plog);
       poj = ptj;
       if (poj > 0.0) {
-        ab0 = b_rosstab(R, tin[0], poj, gtid, fold, parity, bar);
+        ab0 = b_rosstab(R, (log10(tin[0]) - R.zerot) / R.slopet, poj, gtid, fold, parity, bar);
         abj = ab0;
         plog = log(g / ab0 * tau[0]);
         ptj = exp(plog);
@@ -462,70 +464,87 @@ __device__ inline double b_atlas_finish(ModelState* gms, double* gacc, int kw, i
          *tplus = W[12], *taustd = W[13], *tnew1 = W[14], *tnew2 = W[15], *prdnew = W[16],
          *ab1 = W[17], *pt1 = W[18], *p1 = W[19], *pt2 = W[20], *ppp = W[21], *rrr = W[22],
          *rmp = W[23], *ab2 = W[24], *p2 = W[25];
-  if (tid == 0) {
-    RossStore R{n0, cap, gR->zerot, gR->slopet, gR->zerop, gR->slopep, rt, rp, rk};
+  JoshWS& jw = *reinterpret_cast<JoshWS*>(fold + 2);  // MAP1 / PARCOE scratch of warp 0
+  if (tid < 32) {
+    // warp 0: the recurrences of ROSS(3), RADIAP(3) and TCORR(3), depths over lanes
+    WarpG w(tid);
+    const int L = tid;
     double maxerr = 0.0;
     // ROSS(3)
-    for (int j = 0; j < n; ++j) s.abross[j] = FOUR_SIGMA_OVER_PI * powi(s.t[j], 3) / abross[j];
-    s_integ(s.rhox, s.abross, s.tauros, n, s.abross[0] * s.rhox[0], wa, wb, wc);
-    s_rosstab_store(R, s.t, s.p, s.abross, n);  // RX = ROSSTAB(0,0,0), atlas12c.f90:586
+    for (int j = L; j < n; j += 32) s.abross[j] = FOUR_SIGMA_OVER_PI * powi(s.t[j], 3) / abross[j];
+    w.sync();
+    g_integ(w, s.rhox, s.abross, s.tauros, n, s.abross[0] * s.rhox[0], jw);
+    RossStore R{n0, cap, gR->zerot, gR->slopet, gR->zerop, gR->slopep, rt, rp, rk};
+    if (L == 0) s_rosstab_store(R, s.t, s.p, s.abross, n);  // RX = ROSSTAB(0,0,0), atlas12c.f90:586
     // RADIAP(3)
     double errormax = 0.0;
-    for (int j = 0; j < n; ++j) {
+    for (int j = L; j < n; j += 32) {
       s.raden[j] = raden[j] * FOURPI_OVER_C;
       s.accrad[j] = accrad[j] * FOURPI_OVER_C;
       if (h_total[j] / FLUX > 1.0) s.accrad[j] = s.accrad[j] * FLUX / h_total[j];
       errormax = fmax(errormax, h_total[j] / FLUX);
     }
+    errormax = w.max(errormax);
     double pradk0 = acc[kAcc8 * kw] * FOURPI_OVER_C;
     if (errormax > 1.0) pradk0 = pradk0 / errormax;
-    s_integ(s.rhox, s.accrad, s.prad, n, s.accrad[0] * s.rhox[0], wa, wb, wc);
+    w.sync();
+    g_integ(w, s.rhox, s.accrad, s.prad, n, s.accrad[0] * s.rhox[0], jw);
     // TCORR(3)
-    s_deriv(s.rhox, s.t, dtdrhx, n);
-    s_deriv(s.rhox, s.abross, dabros, n);
-    for (int j = 0; j < n; ++j) {
+    g_deriv(w, s.rhox, s.t, dtdrhx, n);
+    g_deriv(w, s.rhox, s.abross, dabros, n);
+    for (int j = L; j < n; j += 32) {
       rdabh[j] = rdabh[j] - flxrad[j] * dabros[j] / fmax(s.abross[j], 1.0e-30);
       codrhx[j] = (rdabh[j] + 0.0) / (flxrad[j] + 0.0);
     }
-    codrhx[0] = 0.0;
-    codrhx[1] = 0.0;
-    s_integ(s.rhox, codrhx, G, n, 0.0, wa, wb, wc);
-    for (int j = 0; j < n; ++j) {
+    w.sync();
+    if (L == 0) {
+      codrhx[0] = 0.0;
+      codrhx[1] = 0.0;
+    }
+    w.sync();
+    g_integ(w, s.rhox, codrhx, G, n, 0.0, jw);
+    for (int j = L; j < n; j += 32) {
       G[j] = exp(G[j]);
       gflux[j] = G[j] * (flxrad[j] + 0.0 - FLUX) / (flxrad[j] + 0.0);
     }
-    s_integ(s.tauros, gflux, dtau, n, 0.0, wa, wb, wc);
-    for (int j = 0; j < n; ++j) {
+    w.sync();
+    g_integ(w, s.tauros, gflux, dtau, n, 0.0, jw);
+    const double MAX_DT = 0.04 * teff;
+    for (int j = L; j < n; j += 32) {
       dtau[j] = dtau[j] / G[j];
       dtau[j] = fmax(-s.tauros[j] / 3.0, fmin(s.tauros[j] / 3.0, dtau[j]));
       s.dtflux[j] = -dtau[j] * dtdrhx[j] / fmax(s.abross[j], 1.0e-30);
-    }
-    const double MAX_DT = 0.04 * teff;
-    for (int j = 0; j < n; ++j) {
       s.flxerr[j] = (flxrad[j] + 0.0 - FLUX) / FLUX * 100.0;
       maxerr = fmax(maxerr, fabs(s.flxerr[j]));
     }
-    s_deriv(s.tauros, s.flxerr, flxdrv, n);
-    for (int j = 0; j < n; ++j) {
+    maxerr = w.max(maxerr);
+    w.sync();
+    g_deriv(w, s.tauros, s.flxerr, flxdrv, n);
+    for (int j = L; j < n; j += 32) {
       // HRATIO = 0 in radiative layers: FLXDRV from the thermal imbalance
       flxdrv[j] = rjmins[j] / fmax(s.abross[j], 1.0e-30) / FLUX * 100.0;
       double d = -flxdrv[j] * FLUX / 100.0 / fmax(fabs(rdiagj[j]), 1.0e-30) * copysign(1.0, rdiagj[j]) *
                  fmax(s.abross[j], 1.0e-30);
       s.dtlamb[j] = fmax(-MAX_DT, fmin(MAX_DT, d));
+      dum[j] = s.dtflux[j] + s.dtlamb[j];
     }
+    w.sync();
     double dtsur = (FLUX - flxrad[0]) / FLUX * 0.25 * s.t[0];
     dtsur = fmax(-MAX_DT, fmin(MAX_DT, dtsur));
-    for (int j = 0; j < n; ++j) dum[j] = s.dtflux[j] + s.dtlamb[j];
-    s_integ(s.tauros, dum, tinteg, n, 0.0, wa, wb, wc);
-    double xq = 0.1, tone, ttwo;
-    s_map1(s.tauros, tinteg, n, &xq, &tone, 1);
-    xq = 2.0;
-    s_map1(s.tauros, tinteg, n, &xq, &ttwo, 1);
-    double tav = (ttwo - tone) / 2.0;
-    if (dtsur * tav <= 0.0) tav = 0.0;
-    if (fabs(tav) > fabs(dtsur)) tav = dtsur;
-    dtsur = dtsur - tav;
-    for (int j = 0; j < n; ++j) {
+    g_integ(w, s.tauros, dum, tinteg, n, 0.0, jw);
+    if (L == 0) {
+      double xq = 0.1, tone, ttwo;
+      s_map1(s.tauros, tinteg, n, &xq, &tone, 1);
+      xq = 2.0;
+      s_map1(s.tauros, tinteg, n, &xq, &ttwo, 1);
+      double tav = (ttwo - tone) / 2.0;
+      if (dtsur * tav <= 0.0) tav = 0.0;
+      if (fabs(tav) > fabs(dtsur)) tav = dtsur;
+      jw.red[0] = dtsur - tav;
+    }
+    w.sync();
+    dtsur = jw.red[0];
+    for (int j = L; j < n; j += 32) {
       s.dtsurf[j] = dtsur;
       double t1 = s.dtflux[j] + s.dtlamb[j] + dtsur;
       if (iter == 1) {
@@ -536,22 +555,23 @@ __device__ inline double b_atlas_finish(ModelState* gms, double* gacc, int kw, i
       }
       s.oldt1[j] = t1;
       s.t1[j] = t1;
-    }
-    for (int j = 0; j < n; ++j) {
-      tplus[j] = s.t[j] + s.t1[j];
+      tplus[j] = s.t[j] + t1;
       taustd[j] = exp10(-6.875 + (double)j * 0.125);
     }
-    s_map1(s.tauros, s.t, n, taustd, tnew1, n);
-    s_map1(s.tauros, s.prad, n, taustd, prdnew, n);
-    s_map1(s.tauros, tplus, n, taustd, tnew2, n);
-    s_scal[0] = R.zerot;
-    s_scal[1] = R.slopet;
-    s_scal[2] = R.zerop;
-    s_scal[3] = R.slopep;
-    s_scal[4] = maxerr;
-    s_scal[5] = pradk0;
-    s_n[0] = n0;
-    s_n[1] = R.n;
+    w.sync();
+    g_map1(w, s.tauros, s.t, n, taustd, tnew1, n, jw.lidx);
+    g_map1(w, s.tauros, s.prad, n, taustd, prdnew, n, jw.lidx);
+    g_map1(w, s.tauros, tplus, n, taustd, tnew2, n, jw.lidx);
+    if (L == 0) {
+      s_scal[0] = R.zerot;
+      s_scal[1] = R.slopet;
+      s_scal[2] = R.zerop;
+      s_scal[3] = R.slopep;
+      s_scal[4] = maxerr;
+      s_scal[5] = pradk0;
+      s_n[0] = n0;
+      s_n[1] = R.n;
+    }
   }
   __syncthreads();
   {
@@ -561,33 +581,48 @@ __device__ inline double b_atlas_finish(ModelState* gms, double* gacc, int kw, i
     else if (grp == 1) b_ttaup(RV, grav, tnew2, taustd, ab2, pt2, p2, prdnew, n, gtid, fold[1], 2);
   }
   __syncthreads();
-  if (tid == 0) {
-    for (int j = 0; j < n; ++j) ppp[j] = (pt2[j] - pt1[j]) / pt1[j];
-    s_map1(taustd, ppp, n, s.tauros, rrr, n);
-    for (int j = 0; j < n; ++j) s.t[j] = s.t[j] + s.t1[j];
-    for (int i = 2; i <= n; ++i) {
-      const int jj = n + 1 - i;
-      s.t[jj - 1] = fmin(s.t[jj - 1], s.t[jj] - 1.0);
+  if (tid < 32) {
+    WarpG w(tid);
+    const int L = tid;
+    for (int j = L; j < n; j += 32) ppp[j] = (pt2[j] - pt1[j]) / pt1[j];
+    w.sync();
+    g_map1(w, taustd, ppp, n, s.tauros, rrr, n, jw.lidx);
+    for (int j = L; j < n; j += 32) s.t[j] = s.t[j] + s.t1[j];
+    w.sync();
+    if (L == 0) {
+      // monotone T from the bottom up, then the 1200 K floor
+      for (int i = 2; i <= n; ++i) {
+        const int jj = n + 1 - i;
+        s.t[jj - 1] = fmin(s.t[jj - 1], s.t[jj] - 1.0);
+      }
     }
-    for (int j = 0; j < n; ++j) s.t[j] = fmax(s.t[j], 1200.0);
-    for (int j = 0; j < n; ++j) s.rhox[j] = s.rhox[j] + rrr[j] * s.rhox[j];
+    w.sync();
+    for (int j = L; j < n; j += 32) {
+      s.t[j] = fmax(s.t[j], 1200.0);
+      s.rhox[j] = s.rhox[j] + rrr[j] * s.rhox[j];
+    }
+    w.sync();
     double* src[8] = {s.rhox, s.t, s.p, s.xne, s.abross, s.prad, s.vturb, s.pturb};
     const double ab_surf = s.abross[0];
     for (int q = 0; q < 8; ++q) {
-      s_map1(s.tauros, src[q], n, taustd, rmp, n);
-      if (q == 4)
-        for (int j = 0; j < n; ++j)
-          if (s.tauros[0] > taustd[j] && rmp[j] < 0.0) rmp[j] = ab_surf;
-      for (int j = 0; j < n; ++j) src[q][j] = rmp[j];
+      g_map1(w, s.tauros, src[q], n, taustd, rmp, n, jw.lidx);
+      for (int j = L; j < n; j += 32) {
+        double v = rmp[j];
+        if (q == 4 && s.tauros[0] > taustd[j] && v < 0.0) v = ab_surf;
+        src[q][j] = v;
+      }
+      w.sync();
     }
-    for (int j = 0; j < n; ++j) s.tauros[j] = taustd[j];
-    gms->pradk0 = s_scal[5];
-    gms->maxerr = s_scal[4];
-    gR->n = s_n[1];
-    gR->zerot = s_scal[0];
-    gR->slopet = s_scal[1];
-    gR->zerop = s_scal[2];
-    gR->slopep = s_scal[3];
+    for (int j = L; j < n; j += 32) s.tauros[j] = taustd[j];
+    if (L == 0) {
+      gms->pradk0 = s_scal[5];
+      gms->maxerr = s_scal[4];
+      gR->n = s_n[1];
+      gR->zerot = s_scal[0];
+      gR->slopet = s_scal[1];
+      gR->zerop = s_scal[2];
+      gR->slopep = s_scal[3];
+    }
   }
   __syncthreads();
   // write back the model, TCORR's RDABH and the new ROSSTAB points
