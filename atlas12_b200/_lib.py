@@ -72,6 +72,7 @@ SIGNATURES = {
     "atlasgpu_synthe_spectrum": (_I, [_P, _P, _I, _P, _P, _I, _I, _P, _P, _D, _D, _I, _P, _P, _P]),
     "atlasgpu_synthe_spectrum_dev": (_I, [_P, _P, _I, _P, _P, _I, _I, _P, _P, _D, _D, _I, _P, _P, _P]),
     "atlasgpu_atlas_set_voigt_tables": (_I, [_P, _P, _P, _P, _I]),
+    "atlasgpu_atlas_tabvoigt": (_I, [_D, _I, _P, _P, _I, _P, _P, _P]),
     "atlasgpu_atlas_linop": (_I, [_P, _P, _I64, _I, _I, _P, _P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P,
                                   ctypes.POINTER(_I64)]),
     "atlasgpu_atlas_rt_pass": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _D,

@@ -16,7 +16,6 @@ Arrays follow the reference layouts seen from C: XLINES(kw, numnu) is
 import ctypes
 
 import numpy as np
-from scipy.special import dawsn
 
 from . import _lib, surrogate, synthetic
 from ._lib import Accum, Context, FinishState, ModelDesc, ptr
@@ -30,15 +29,17 @@ def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
-def tabvoigt(vsteps=200.0, n=2001):
-    """H0 = exp(-v^2), H1 = -2/sqrt(pi) (1 - 2 v F(v)) (F = Dawson's integral),
-    H2 = (1 - 2 v^2) exp(-v^2) on v = (i-1)/vsteps.  The reference tabulates H1
-    from an 81-point table remapped with MAP1 (TABVOIGT); this driver evaluates
-    the function itself."""
-    v = np.arange(n) / vsteps
-    h0 = np.exp(-v * v)
-    h1 = -2.0 / np.sqrt(np.pi) * (1.0 - 2.0 * v * dawsn(v))
-    h2 = h0 - (v * v + v * v) * h0
+def tabvoigt(operators, vsteps=200.0, n=2001):
+    """TABVOIGT (atlas12_modules.f90:19796-19851): H0, H1, H2 at vsteps points per
+    Doppler width, H1 mapped (MAP1) from the reference's TABVI/TABH1 table
+    (operators["tabvi"], operators["tabh1"]), computed by the library."""
+    tv = np.ascontiguousarray(operators["tabvi"], np.float64)
+    th = np.ascontiguousarray(operators["tabh1"], np.float64)
+    h0, h1, h2 = np.zeros(n), np.zeros(n), np.zeros(n)
+    rc = _lib.lib().atlasgpu_atlas_tabvoigt(float(vsteps), int(n), ptr(tv), ptr(th), tv.size, ptr(h0), ptr(h1),
+                                           ptr(h2))
+    if rc != _lib.OK:
+        raise _lib.AtlasGPUError(rc, "atlasgpu_atlas_tabvoigt: bad table")
     return h0, h1, h2
 
 
@@ -63,7 +64,7 @@ class Atlas:
         ctx.set_operators(operators["xtau8"], operators["coefj"], operators["coefh"], operators["ch_j"],
                           operators["ck_j"])
         if h0 is None:
-            h0, h1, h2 = tabvoigt()
+            h0, h1, h2 = tabvoigt(operators)
         self.tables = [np.ascontiguousarray(x, np.float64) for x in (h0, h1, h2)]
         ctx.call("atlasgpu_atlas_set_voigt_tables", *[ptr(x) for x in self.tables], 2001)
 
@@ -151,15 +152,17 @@ class AtlasModel:
         self.ctx = ctx
         ctx.set_operators(operators["xtau8"], operators["coefj"], operators["coefh"], operators["ch_j"],
                           operators["ck_j"])
-        self.ross = ross or surrogate.RossTable()
-        m = start or surrogate.grey_model(teff, logg, nrhox=nrhox, ross=self.ross)
+        if start is None:
+            ross = ross or surrogate.RossTable()
+            start = surrogate.grey_model(teff, logg, nrhox=nrhox, ross=ross)
+        m = start
         if waveset is None:
             waveset, rcoset = synthetic.geometric_waveset()
         self.waveset = np.ascontiguousarray(waveset, np.float64)
         self.rcoset = np.ascontiguousarray(rcoset, np.float64)
         self.cutwave = cutoff_grid()
         ld = np.zeros((0, 4), np.int32) if linedata is None else np.ascontiguousarray(linedata, np.int32)
-        h0, h1, h2 = h_tables or tabvoigt()
+        h0, h1, h2 = h_tables or tabvoigt(operators)
         self._keep = [np.ascontiguousarray(x, np.float64) for x in (m["t"], m["p"], m["rhox"], m["tauros"])]
         self._keep += [np.ascontiguousarray(x, np.float64) for x in (h0, h1, h2)]
         self._keep += [ld]

@@ -124,6 +124,23 @@ __global__ void __launch_bounds__(kFinThreads) k_finish_one(ModelState* s, doubl
 
 extern "C" {
 
+int atlasgpu_atlas_tabvoigt(double vsteps, int n, const double* tabvi, const double* tabh1, int ntab,
+                            double* h0, double* h1, double* h2) {
+  if (!tabvi || !tabh1 || !h0 || !h1 || !h2 || n < 2 || ntab < 4 || !(vsteps > 0.0)) return ATLASGPU_EINVAL;
+  for (int i = 1; i < ntab; ++i)
+    if (!(tabvi[i] > tabvi[i - 1])) return ATLASGPU_EINVAL;
+  // H1 = MAP1 of the tabulated H1(v) onto v = (i-1)/vsteps, H0 = exp(-v^2),
+  // H2 = H0 - 2 v^2 H0 (atlas12_modules.f90:19796-19851)
+  for (int i = 1; i <= n; ++i) h0[i - 1] = (double)(i - 1) / vsteps;
+  s_map1(tabvi, tabh1, ntab, h0, h1, n);
+  for (int i = 1; i <= n; ++i) {
+    const double vv = powi((double)(i - 1) / vsteps, 2);
+    h0[i - 1] = exp(-vv);
+    h2[i - 1] = h0[i - 1] - (vv + vv) * h0[i - 1];
+  }
+  return ATLASGPU_OK;
+}
+
 int atlasgpu_atlas_set_voigt_tables(atlasgpu_ctx* ctx, const double* h0, const double* h1,
                                     const double* h2, int n) {
   if (!ctx || !h0 || !h1 || !h2 || n != kTabN) return fail(ctx, ATLASGPU_EINVAL, "voigt tables: n must be 2001");

@@ -83,7 +83,7 @@ __device__ inline void s_deriv(const double* x, const double* f, double* d, int 
 }
 
 // MAP1 as a sequential walk (1-based L as in the reference)
-__device__ inline int s_map1(const double* xo, const double* fo, int nold, const double* xn,
+__host__ __device__ inline int s_map1(const double* xo, const double* fo, int nold, const double* xn,
                              double* fn, int nnew) {
 #define XO(i) xo[(i)-1]
 #define FO(i) fo[(i)-1]

@@ -134,10 +134,9 @@ def run_reference(args):
     from atlas12_b200 import atlas
     W = workload()
     t = operators()
-    ops = po.Ops.from_tables(t)
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    step = oracle_iteration_factory(po, atlas, ops, W)
+    step = oracle_iteration_factory(po, atlas, t, W)
     for _ in range(args.warmup):
         step()
     times = []
@@ -161,10 +160,11 @@ def run_reference(args):
     return 0
 
 
-def oracle_iteration_factory(po, atlas, ops, W):
+def oracle_iteration_factory(po, atlas, tables, W):
     """One ATLAS12 iteration of the oracle on the grey start (state carried)."""
     from atlas12_b200 import surrogate as sg
-    h0, h1, h2 = atlas.tabvoigt()
+    ops = po.Ops.from_tables(tables)
+    h0, h1, h2 = po.tabvoigt(tables["tabvi"], tables["tabh1"])
     tl = po.build_tablog()
     cut = atlas.cutoff_grid()
     iw = atlas.iwavetab(cut)
@@ -359,7 +359,7 @@ def cpu_baseline(W, ops_t, iters_gpu):
     from atlas12_b200 import atlas
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    step = oracle_iteration_factory(po, atlas, po.Ops.from_tables(ops_t), W)
+    step = oracle_iteration_factory(po, atlas, ops_t, W)
     step()
     t0 = time.perf_counter()
     step()

@@ -154,6 +154,13 @@ int atlasgpu_synthe_spectrum_dev(atlasgpu_ctx *ctx, const double *d_wledge, int 
 
 
 /* ---- ATLAS12 ---------------------------------------------------------- */
+/* TABVOIGT (atlas12_modules.f90:19796-19851) on the host: H0 = exp(-v^2),
+ * H1 = MAP1 of the tabulated H1 (tabvi, tabh1 [ntab], the reference's TABVI
+ * and TABH1 data, :19805-19835) onto v = (i-1)/vsteps, H2 = H0 - 2 v^2 H0,
+ * each [n].  No device work; needs no context. */
+int atlasgpu_atlas_tabvoigt(double vsteps, int n, const double *tabvi, const double *tabh1, int ntab,
+                            double *h0, double *h1, double *h2);
+
 /* Voigt tables of TABVOIGT(200, 2001) (atlas12_modules.f90:19796-19851), as
  * the driver computes them at start-up (atlas12c.f90:236).  n = 2001.  Also
  * builds TABLOG (:2083-2086) on the host with the C library pow. */

@@ -2,6 +2,8 @@
 import os
 import re
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
@@ -29,3 +31,12 @@ def test_grid_is_host_only():
     from atlas12_b200 import synthe
     g = synthe.synthe_grid(400.0, 410.0, 500000.0)
     assert g["length"] == 12346 and g["ixwlbeg"] > 0
+
+
+def test_tabvoigt_matches_oracle(tables, po):
+    """TABVOIGT is host code in the library: it must equal the oracle's restatement."""
+    from atlas12_b200 import atlas
+    got = atlas.tabvoigt(tables)
+    ref = po.tabvoigt(tables["tabvi"], tables["tabh1"])
+    for g, r in zip(got, ref):
+        np.testing.assert_array_equal(g, r)
