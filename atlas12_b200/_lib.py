@@ -83,8 +83,17 @@ SIGNATURES = {
     "atlasgpu_model_get": (_I, [_P, _P, _P, _P, _P, _P, _P, _P]),
     "atlasgpu_model_set_structure": (_I, [_P, _P, _P, _P, _P]),
     "atlasgpu_model_destroy": (_I, [_P, _P]),
+    "atlasgpu_model_set_params": (_I, [_P, _P, _D, _D, _D, _D]),
     "atlasgpu_surrogate_eval": (_I, [_P, _I, _P, _P, _D, _I, _P, _P, _P, _P, _P]),
     "atlasgpu_fp64_peak_tflops": (_D, [_P]),
+    "atlasgpu_mlp_create": (_I, [_P, _I, _I, _I, _I, ctypes.c_uint64, ctypes.POINTER(_P)]),
+    "atlasgpu_mlp_destroy": (_I, [_P, _P]),
+    "atlasgpu_mlp_nparam": (_I64, [_P]),
+    "atlasgpu_mlp_get_params": (_I, [_P, _P, _P]),
+    "atlasgpu_mlp_set_params": (_I, [_P, _P, _P]),
+    "atlasgpu_mlp_forward": (_I, [_P, _P, _P, _I, _P]),
+    "atlasgpu_mlp_loss_grad": (_I, [_P, _P, _P, _P, _I, _P, _P]),
+    "atlasgpu_mlp_train": (_I, [_P, _P, _P, _P, _I, _I, _I, ctypes.c_float, ctypes.c_uint64, _P]),
     "atlasgpu_atlas_rt_pass_noalloc": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _D, _P, _P]),
 }
 
@@ -107,7 +116,7 @@ class ModelDesc(ctypes.Structure):
                 ("waveset", _DP), ("rcoset", _DP), ("numnu", _I),
                 ("cutoff_wave", _DP), ("nwave", _I),
                 ("linedata", ctypes.POINTER(ctypes.c_int32)), ("nlines", _I64),
-                ("h0tab", _DP), ("h1tab", _DP), ("h2tab", _DP)]
+                ("h0tab", _DP), ("h1tab", _DP), ("h2tab", _DP), ("mh", _D)]
 
 _lib = None
 

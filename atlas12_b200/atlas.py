@@ -148,12 +148,12 @@ class AtlasModel:
     """
 
     def __init__(self, ctx: Context, operators, teff=5777.0, logg=4.44, vturb=1.5, linedata=None,
-                 waveset=None, rcoset=None, nrhox=72, ross=None, start=None, h_tables=None):
+                 waveset=None, rcoset=None, nrhox=72, ross=None, start=None, h_tables=None, mh=0.0):
         self.ctx = ctx
         ctx.set_operators(operators["xtau8"], operators["coefj"], operators["coefh"], operators["ch_j"],
                           operators["ck_j"])
         if start is None:
-            ross = ross or surrogate.RossTable()
+            ross = ross or surrogate.RossTable(mh=mh)
             start = surrogate.grey_model(teff, logg, nrhox=nrhox, ross=ross)
         m = start
         if waveset is None:
@@ -171,7 +171,8 @@ class AtlasModel:
         self.teff = teff
         d = ModelDesc(teff, logg, vturb, self.nrhox, _dp(t), _dp(p), _dp(rx), _dp(tau), _dp(self.waveset),
                       _dp(self.rcoset), self.waveset.size, _dp(self.cutwave), self.cutwave.size,
-                      ld.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ld.shape[0], _dp(h0), _dp(h1), _dp(h2))
+                      ld.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ld.shape[0], _dp(h0), _dp(h1), _dp(h2),
+                      float(mh))
         self._h = ctypes.c_void_p()
         ctx.call("atlasgpu_model_create", ctypes.byref(d), ctypes.byref(self._h))
 
@@ -192,6 +193,11 @@ class AtlasModel:
                       ptr(hs))
         out["hsurf"] = hs
         return out
+
+    def set_params(self, teff, logg, vturb, mh=0.0):
+        """New stellar parameters on the same line list and grid; follow with set_structure."""
+        self.teff = teff
+        self.ctx.call("atlasgpu_model_set_params", self._h, float(teff), float(logg), float(vturb), float(mh))
 
     def set_structure(self, t, p, rhox):
         arrs = [np.ascontiguousarray(x, np.float64) for x in (t, p, rhox)]

@@ -19,7 +19,7 @@ constexpr int kRossMax = 80 * 60;   // ROSSTAB_MAXTAB = kw*60 with the reference
 struct atlasgpu_model {
   int nrhox, kw, numnu, nwave, nspec;
   int64_t nlines;
-  double teff, grav, vturb;
+  double teff, grav, vturb, mh;
   // device memory
   double* state;         // [kNState][kw]
   ModelState* ms;        // device struct pointing into state
@@ -49,7 +49,7 @@ namespace {
 
 // hydrostatics (iteration > 1), surrogate EOS / populations, Planck factors
 __global__ void k_model_eos(ModelState* ms, const int* iter_dev, int nrhox, int kw, double grav,
-                            double vturb_cms, double* xnfdop, double* dopple, double* xne_eos,
+                            double vturb_cms, double mh, double* xnfdop, double* dopple, double* xne_eos,
                             double* txnxn, double* hkt, double* hckt, double* rho, ContCoef* cc) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nrhox) return;
@@ -63,7 +63,7 @@ __global__ void k_model_eos(ModelState* ms, const int* iter_dev, int nrhox, int 
     ms->p[j] = p;
   }
   ContCoef c;
-  const EosOut e = surrogate_depth(t, p, vturb_cms, j, kw, xnfdop, dopple, &c);
+  const EosOut e = surrogate_depth(t, p, vturb_cms, mh, j, kw, xnfdop, dopple, &c);
   cc[j] = c;
   xne_eos[j] = e.xne;
   ms->xne[j] = e.xne;
@@ -125,7 +125,7 @@ __global__ void k_surrogate_eval(int nrhox, const double* t, const double* p, do
   const int j = blockIdx.x;
   if (j >= nrhox) return;
   if (threadIdx.x == 0) {
-    const EosOut e = surrogate_depth(t[j], p[j], vturb_cms, j, nrhox, xnfdop, dopple, cc + j);
+    const EosOut e = surrogate_depth(t[j], p[j], vturb_cms, 0.0, j, nrhox, xnfdop, dopple, cc + j);
     xne[j] = e.xne;
     rho[j] = e.rho;
   }
@@ -146,7 +146,8 @@ int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
   ctx->timing = was && timed;
   {
     Timer tm(ctx, "model_eos");
-    k_model_eos<<<1, 128, 0, s>>>(m->ms, m->iter_dev, m->nrhox, m->kw, m->grav, m->vturb * 1.0e5, m->xnfdop,
+    k_model_eos<<<1, 128, 0, s>>>(m->ms, m->iter_dev, m->nrhox, m->kw, m->grav, m->vturb * 1.0e5, m->mh,
+                                  m->xnfdop,
                                   m->dopple, m->xne_eos, m->txnxn, m->hkt, m->hckt, m->rho, m->cc);
     CKL(ctx);
   }
@@ -274,6 +275,7 @@ int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlas
   m->teff = d->teff;
   m->grav = pow(10.0, d->logg);
   m->vturb = d->vturb_kms;
+  m->mh = d->mh;
   const int kw = m->kw;
   int r = 0;
   const size_t nr = (size_t)3 * kRossMax;
@@ -460,6 +462,26 @@ int atlasgpu_model_set_structure(atlasgpu_ctx* ctx, atlasgpu_model* m, const dou
   m->kapcont_done = false;  // KAPCONT runs again on the new structure's first iteration
   RossStore R0{0, kRossMax, 0.0, 1.0, 0.0, 1.0, m->ross, m->ross + kRossMax, m->ross + 2 * kRossMax};
   CK(cudaMemcpy(m->R, &R0, sizeof R0, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int atlasgpu_model_set_params(atlasgpu_ctx* ctx, atlasgpu_model* m, double teff, double logg,
+                              double vturb_kms, double mh) {
+  if (!ctx || !m || !(teff > 0.0) || !(vturb_kms >= 0.0)) return fail(ctx, ATLASGPU_EINVAL, "model_set_params");
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  m->teff = teff;
+  m->grav = pow(10.0, logg);
+  m->vturb = vturb_kms;
+  m->mh = mh;
+  std::vector<double> v(m->kw, vturb_kms * 1.0e5);
+  CK(cudaMemcpy(m->state + 6 * m->kw, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+  // the captured iteration holds the old scalars: capture again on next use
+  if (m->gexec) cudaGraphExecDestroy(m->gexec);
+  if (m->graph) cudaGraphDestroy(m->graph);
+  m->gexec = nullptr;
+  m->graph = nullptr;
+  m->kapcont_done = false;
   return 0;
 }
 

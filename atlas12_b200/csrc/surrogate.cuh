@@ -50,9 +50,9 @@ struct EosOut {
   double xne, rho, nh, xh;
 };
 
-// surrogate.eos + populations for one depth.  xnfdop/dopple: [nspec][kw]
+// surrogate.eos + populations for one depth (mh = [M/H]).  xnfdop/dopple: [nspec][kw]
 // column (depth j).  Returns EOS fields and fills the continuum coefficients.
-__device__ inline EosOut surrogate_depth(double t, double p, double vturb_cms, int j, int kw,
+__device__ inline EosOut surrogate_depth(double t, double p, double vturb_cms, double mh, int j, int kw,
                                          double* xnfdop, double* dopple, ContCoef* cc) {
   // the T-only factors of every Saha ratio, evaluated once (same operand
   // order as surrogate._saha, so the ratios are the same numbers)
@@ -64,7 +64,7 @@ __device__ inline EosOut surrogate_depth(double t, double p, double vturb_cms, i
   for (int m = 0; m < kNMetal; ++m) {
     bm[m] = 2.0 * kMetal[m][5] / kMetal[m][4];
     em[m] = exp(-kMetal[m][2] * kEvErg / kt);
-    am[m] = exp10(kMetal[m][3] - 12.0);
+    am[m] = exp10(kMetal[m][3] - 12.0 + mh);  // [M/H] scales every metal
   }
   const double ntot = p / kt;
   double ne = fmax(ntot * 1e-4, 1.0);

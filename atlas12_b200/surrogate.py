@@ -97,12 +97,13 @@ def _saha(t, ne, chi, u1, u2):
     return 2.4147e15 * t ** 1.5 / np.maximum(ne, 1.0) * (2.0 * u2 / u1) * np.exp(-chi * EV_ERG / (KBOL * t))
 
 
-def eos(t, p):
-    """Ideal-gas surrogate EOS -> dict(ntot, nh, xne, rho, xh) per depth."""
+def eos(t, p, mh=0.0):
+    """Ideal-gas surrogate EOS -> dict(ntot, nh, xne, rho, xh) per depth.
+    mh = [M/H]: every metal abundance scaled by 10**mh."""
     t = np.asarray(t, dtype=np.float64)
     p = np.asarray(p, dtype=np.float64)
     ntot = p / (KBOL * t)
-    eps = 10.0 ** (METALS[:, 3] - 12.0)
+    eps = 10.0 ** (METALS[:, 3] - 12.0 + mh)
     ne = np.maximum(ntot * 1e-4, 1.0)
     for _ in range(30):  # fixed-point on n_e
         nh = ntot / (1.1 + ne / ntot)
@@ -114,16 +115,16 @@ def eos(t, p):
         ne = np.sqrt(ne * ne_new)
     nh = ntot / (1.1 + ne / ntot)
     rho = nh * 1.4 * AMU
-    return dict(ntot=ntot, nh=nh, xne=ne, rho=rho, xh=xh)
+    return dict(ntot=ntot, nh=nh, xne=ne, rho=rho, xh=xh, mh=mh)
 
 
-def populations(t, p, vturb_kms, line_pop=1.0):
+def populations(t, p, vturb_kms, line_pop=1.0, mh=0.0):
     """Per-depth species number densities / partition function (XNFPEL analogue)
     and Doppler widths.  Returns dict of [nrhox, MW6] arrays plus eos fields.
     line_pop scales the metal and molecule entries (ATLAS_LINE_POP for the
     ATLAS12 model, 1 for SYNTHE); hydrogen and the EOS are unaffected."""
     t = np.asarray(t, dtype=np.float64)
-    e = eos(t, p)
+    e = eos(t, p, mh)
     nr = t.size
     xnfp = np.zeros((nr, MW6))
     dop = np.zeros((nr, MW6))
@@ -137,7 +138,7 @@ def populations(t, p, vturb_kms, line_pop=1.0):
     dop[:, 0] = dop[:, 1] = _dop(1.008)
     for z, m, chi, leps, u1, u2 in METALS:
         r = _saha(t, e["xne"], chi, u1, u2)
-        n = e["nh"] * 10.0 ** (leps - 12.0)
+        n = e["nh"] * 10.0 ** (leps - 12.0 + mh)
         i1, i2 = nelion(z, 1) - 1, nelion(z, 2) - 1
         xnfp[:, i1] = n / (1.0 + r) / u1 * line_pop
         xnfp[:, i2] = n * r / (1.0 + r) / u2 * line_pop
@@ -150,12 +151,14 @@ def populations(t, p, vturb_kms, line_pop=1.0):
     return e
 
 
-def continuum_opacity(wave_nm, t, p, e=None):
-    """Surrogate continuum -> (kappa_abs, sigma) in cm^2/g, shape [nwave, nrhox]."""
+def continuum_opacity(wave_nm, t, p, e=None, mh=0.0):
+    """Surrogate continuum -> (kappa_abs, sigma) in cm^2/g, shape [nwave, nrhox].
+    e: an eos()/populations() result (carries its [M/H]); else eos(t, p, mh)."""
     w = np.asarray(wave_nm, dtype=np.float64)[:, None]
     t = np.asarray(t, dtype=np.float64)[None, :]
     if e is None:
-        e = eos(t[0], p)
+        e = eos(t[0], p, mh)
+    mh = e.get("mh", 0.0)
     nh = e["nh"][None, :]
     ne = e["xne"][None, :]
     rho = e["rho"][None, :]
@@ -179,7 +182,7 @@ def continuum_opacity(wave_nm, t, p, e=None):
     kmet = np.zeros(np.broadcast(w, t).shape)
     for z, m, chi, leps, u1, u2 in METALS:
         r = _saha(t[0], e["xne"], chi, u1, u2)[None, :]
-        n1 = nh * 10.0 ** (leps - 12.0) / (1.0 + r)
+        n1 = nh * 10.0 ** (leps - 12.0 + mh) / (1.0 + r)
         edge = 1239.84198 / chi
         kmet = kmet + np.where(w <= edge, n1 * MBF_SIGMA * (w / edge) ** 3, 0.0)
     # Thomson + Rayleigh(H I)
@@ -190,27 +193,31 @@ def continuum_opacity(wave_nm, t, p, e=None):
 
 
 def planck_dbdt(wave_nm, t):
+    """dB_nu/dT; 0 where h nu / kT overflows."""
     nu = CLIGHT_NMS / np.asarray(wave_nm)[:, None]
     x = HPLANCK * nu / (KBOL * np.asarray(t)[None, :])
-    b = 2.0 * HPLANCK * nu ** 3 / CLIGHT ** 2 / np.expm1(x)
-    return b * x / np.asarray(t)[None, :] * np.exp(x) / np.expm1(x)
+    with np.errstate(over="ignore", invalid="ignore"):
+        b = 2.0 * HPLANCK * nu ** 3 / CLIGHT ** 2 / np.expm1(x)
+        d = b * x / np.asarray(t)[None, :] * np.exp(x) / np.expm1(x)
+    return np.where(np.isfinite(d), d, 0.0)
 
 
 class RossTable:
     """log kappa_Ross on a (log T, log P) grid from the surrogate continuum
     (the ROSSTAB analogue consumed by TTAUP)."""
 
-    def __init__(self, lt0=np.log10(1000.0), lt1=np.log10(60000.0), lp0=-4.0, lp1=10.0, nt=104, np_=112):
+    def __init__(self, lt0=np.log10(1000.0), lt1=np.log10(60000.0), lp0=-4.0, lp1=10.0, nt=104, np_=112,
+                 mh=0.0, nwave=2400):
         self.lt = np.linspace(lt0, lt1, nt)
         self.lp = np.linspace(lp0, lp1, np_)
-        wave = np.geomspace(9.0, 160000.0, 2400)
+        wave = np.geomspace(9.0, 160000.0, nwave)
         nu = CLIGHT_NMS / wave
         dnu = np.abs(np.gradient(nu))
         tab = np.zeros((nt, np_))
         for i, lt in enumerate(self.lt):
             tt = np.full(np_, 10.0 ** lt)
             pp = 10.0 ** self.lp
-            ka, sg = continuum_opacity(wave, tt, pp)
+            ka, sg = continuum_opacity(wave, tt, pp, mh=mh)
             d = planck_dbdt(wave, tt) * dnu[:, None]
             tab[i] = np.log10(np.sum(d, axis=0) / np.sum(d / (ka + sg), axis=0))
         self.table = tab

@@ -1,0 +1,235 @@
+"""Learned warm start for the ATLAS12 iteration.
+
+A small MLP (4 -> 256 -> 256 -> 216, FP32, tanh) maps the stellar parameters
+(Teff, log g, [M/H], vturb) to a starting structure on the standard Rosseland
+grid: log10 T, log10 P and log10 Ne at each of the 72 depths.  It is trained on
+converged models that this library's own ATLAS12 iteration produces, with the
+library's forward / backward / Adam kernels (csrc/mlp.cu).  The plain grey
+start stays the fallback, and the unmodified iteration still judges
+convergence, so the network can only shorten the iteration.
+
+    ws = WarmStart.load(path, ctx)
+    start = ws.start(teff, logg, mh, vturb)      # dict t, p, rhox, tauros, xne
+    model.set_params(teff, logg, vturb, mh); model.set_structure(start["t"], start["p"], start["rhox"])
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib, surrogate
+from ._lib import ptr
+
+NRHOX = 72
+TAUSTD = 10.0 ** (-6.875 + 0.125 * np.arange(NRHOX))
+SHAPE = (4, 256, 256, 3 * NRHOX)
+# parameter box of the training grid: Teff, log g, [M/H], vturb (km/s)
+BOX = np.array([[3500.0, 8000.0], [1.0, 5.0], [-2.0, 0.5], [0.5, 3.0]])
+
+
+def sample_params(n, seed, box=BOX):
+    """n parameter sets uniform in the box (seeded)."""
+    rng = np.random.default_rng(seed)
+    return box[:, 0] + (box[:, 1] - box[:, 0]) * rng.uniform(size=(n, 4))
+
+
+def encode_inputs(params, box=BOX):
+    """Parameters to [-1, 1] over the box."""
+    p = np.atleast_2d(np.asarray(params, dtype=np.float64))
+    return (2.0 * (p - box[:, 0]) / (box[:, 1] - box[:, 0]) - 1.0).astype(np.float32)
+
+
+class MLP:
+    """The device network (csrc/mlp.cu) on one context."""
+
+    def __init__(self, ctx, shape=SHAPE, seed=1):
+        self.ctx = ctx
+        self.shape = tuple(shape)
+        self._h = ctypes.c_void_p()
+        ctx.call("atlasgpu_mlp_create", *[int(s) for s in self.shape], ctypes.c_uint64(seed), ctypes.byref(self._h))
+        self.nparam = int(_lib.lib().atlasgpu_mlp_nparam(self._h))
+
+    def params(self):
+        out = np.zeros(self.nparam, np.float32)
+        self.ctx.call("atlasgpu_mlp_get_params", self._h, ptr(out))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.nparam
+        self.ctx.call("atlasgpu_mlp_set_params", self._h, ptr(p))
+
+    def forward(self, x):
+        x = np.ascontiguousarray(np.atleast_2d(x), np.float32)
+        y = np.zeros((x.shape[0], self.shape[3]), np.float32)
+        self.ctx.call("atlasgpu_mlp_forward", self._h, ptr(x), x.shape[0], ptr(y))
+        return y
+
+    def loss_grad(self, x, t):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.zeros(self.nparam, np.float32)
+        loss = ctypes.c_float(0.0)
+        self.ctx.call("atlasgpu_mlp_loss_grad", self._h, ptr(x), ptr(t), x.shape[0], ptr(g), ctypes.byref(loss))
+        return float(loss.value), g
+
+    def train(self, x, t, epochs, batch=64, lr=1e-3, seed=7):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        hist = np.zeros(max(epochs, 1), np.float32)
+        self.ctx.call("atlasgpu_mlp_train", self._h, ptr(x), ptr(t), x.shape[0], int(epochs), int(batch),
+                      ctypes.c_float(lr), ctypes.c_uint64(seed), ptr(hist))
+        return hist[:epochs]
+
+    def close(self):
+        if self._h:
+            _lib.lib().atlasgpu_mlp_destroy(self.ctx.handle, self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def structure_targets(t, p, xne):
+    """[n, 216] = log10 T, log10 P, log10 Ne per depth."""
+    return np.concatenate([np.log10(t), np.log10(p), np.log10(np.maximum(xne, 1.0))], axis=1)
+
+
+class WarmStart:
+    """Trained network plus the output standardisation."""
+
+    def __init__(self, mlp, ymean, ystd):
+        self.mlp = mlp
+        self.ymean = np.asarray(ymean, np.float64)
+        self.ystd = np.asarray(ystd, np.float64)
+
+    @classmethod
+    def fit(cls, ctx, params, t, p, xne, epochs=2000, batch=64, lr=1e-3, seed=1):
+        """Train on converged structures (each [n, 72]); returns (WarmStart, loss history)."""
+        y = structure_targets(t, p, xne)
+        ymean, ystd = y.mean(0), np.maximum(y.std(0), 1e-3)
+        mlp = MLP(ctx, seed=seed)
+        hist = mlp.train(encode_inputs(params), ((y - ymean) / ystd).astype(np.float32), epochs, batch, lr,
+                         seed + 1)
+        return cls(mlp, ymean, ystd), hist
+
+    def predict(self, params):
+        y = self.mlp.forward(encode_inputs(params)).astype(np.float64) * self.ystd + self.ymean
+        n = NRHOX
+        return 10.0 ** y[:, :n], 10.0 ** y[:, n:2 * n], 10.0 ** y[:, 2 * n:]
+
+    def start(self, teff, logg, mh, vturb):
+        """Starting structure on TAUSTD: T, P from the network, RHOX = P / g."""
+        t, p, xne = self.predict([[teff, logg, mh, vturb]])
+        t, p = t[0], p[0]
+        # the network's T need not be monotone; the iteration's own rule applies
+        for j in range(NRHOX - 2, -1, -1):
+            t[j] = min(t[j], t[j + 1] - 1.0)
+        return dict(t=np.maximum(t, 1200.0), p=p, rhox=p / 10.0 ** logg, tauros=TAUSTD.copy(), xne=xne[0])
+
+    def save(self, path):
+        np.savez(path, params=self.mlp.params(), shape=np.array(self.mlp.shape), ymean=self.ymean,
+                 ystd=self.ystd, box=BOX)
+
+    @classmethod
+    def load(cls, path, ctx):
+        d = np.load(path)
+        mlp = MLP(ctx, shape=tuple(int(s) for s in d["shape"]))
+        mlp.set_params(d["params"])
+        return cls(mlp, d["ymean"], d["ystd"])
+
+
+_ross_cache = {}
+
+
+def grey_start(teff, logg, mh, nrhox=NRHOX):
+    """The plain grey start at [M/H] (Rosseland tables cached per 0.1 dex)."""
+    key = round(float(mh), 1)
+    if key not in _ross_cache:
+        _ross_cache[key] = surrogate.RossTable(mh=key, nwave=600)
+    return surrogate.grey_model(teff, logg, nrhox=nrhox, ross=_ross_cache[key])
+
+
+def run_models(model, params, starts=None, max_iter=80, tol=0.1):
+    """Iterate `model` (an AtlasModel on the shared line list and grid) for each
+    parameter set from its grey start (or starts[i]).  Returns per-model
+    iterations, final max |FLXERR| and the final T, P, XNE [n, 72]."""
+    n = len(params)
+    iters = np.zeros(n, np.int32)
+    err = np.zeros(n)
+    T, P, NE = (np.zeros((n, model.nrhox)) for _ in range(3))
+    for i, (teff, logg, mh, vt) in enumerate(params):
+        s = starts[i] if starts is not None else grey_start(teff, logg, mh, model.nrhox)
+        model.set_params(teff, logg, vt, mh)
+        model.set_structure(s["t"], s["p"], s["rhox"])
+        try:
+            k, hist = model.iterate(max_iter=max_iter, tol_percent=tol, graph=True)
+            st = model.structure()
+            iters[i], err[i] = k, hist[-1] if k else np.inf
+            T[i], P[i], NE[i] = st["t"], st["p"], st["xne"]
+        except _lib.AtlasGPUError:
+            iters[i], err[i] = max_iter, np.inf
+    return iters, err, T, P, NE
+
+
+def _workload_model(ctx, tables, numnu=30000, nlines=500000, seed=2):
+    """An AtlasModel on the C2-style line list and grid (shared by every model)."""
+    from . import atlas, synthetic
+    ws, rc = synthetic.geometric_waveset(9.0, 160000.0, numnu)
+    lines = synthetic.atlas_lines(nlines, ws[2], ws[-3], seed=seed)
+    return atlas.AtlasModel(ctx, tables, linedata=lines, waveset=ws, rcoset=rc, start=grey_start(5777.0, 4.44, 0.0))
+
+
+def main(argv=None):
+    """generate: converged models over the parameter box; train: fit the network.
+
+    python -m atlas12_b200.warmstart generate --n 2000 --seed 11 --out models.npz
+    python -m atlas12_b200.warmstart train --data models.npz --out warmstart.npz
+    """
+    import argparse
+    import os
+    import time
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("cmd", choices=["generate", "train"])
+    ap.add_argument("--n", type=int, default=2000)
+    ap.add_argument("--seed", type=int, default=11)
+    ap.add_argument("--max-iter", type=int, default=80)
+    ap.add_argument("--data", default=None)
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--epochs", type=int, default=3000)
+    ap.add_argument("--budget-s", type=float, default=1e9, help="stop generating after this many seconds")
+    a = ap.parse_args(argv)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    t = np.load(os.path.join(root, "tests", "golden", "reference_tables.npz"))
+    tables = {k: t[k] for k in t.files}
+    ctx = _lib.Context(0, _lib.PREC_MIXED)
+    if a.cmd == "generate":
+        model = _workload_model(ctx, tables)
+        params = sample_params(a.n, a.seed)
+        t0 = time.time()
+        out = dict(params=[], iters=[], err=[], t=[], p=[], xne=[])
+        for i in range(0, a.n, 50):
+            if time.time() - t0 > a.budget_s:
+                break
+            it, er, T, P, NE = run_models(model, params[i:i + 50], max_iter=a.max_iter)
+            for k, v in zip(("params", "iters", "err", "t", "p", "xne"), (params[i:i + 50], it, er, T, P, NE)):
+                out[k].append(v)
+            done = sum(len(x) for x in out["iters"])
+            conv = sum(int(np.sum(e <= 0.1)) for e in out["err"])
+            print(f"{done} models, {conv} converged, {time.time() - t0:.0f} s", flush=True)
+        np.savez(a.out, **{k: np.concatenate(v) for k, v in out.items()})
+        model.close()
+    else:
+        d = np.load(a.data)
+        ok = d["err"] <= 0.1
+        ws, hist = WarmStart.fit(ctx, d["params"][ok], d["t"][ok], d["p"][ok], d["xne"][ok], epochs=a.epochs)
+        ws.save(a.out)
+        print(f"trained on {int(ok.sum())} converged models; loss {hist[0]:.4g} -> {hist[-1]:.4g}", flush=True)
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()

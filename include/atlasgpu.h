@@ -232,6 +232,7 @@ typedef struct {
   const int32_t *linedata;                 /* [nlines][4] */
   int64_t nlines;
   const double *h0tab, *h1tab, *h2tab;     /* TABVOIGT tables, 2001 */
+  double mh;                               /* [M/H]: metal abundances scaled by 10**mh */
 } atlasgpu_model_desc;
 
 int atlasgpu_model_create(atlasgpu_ctx *ctx, const atlasgpu_model_desc *desc, atlasgpu_model **out);
@@ -249,6 +250,11 @@ int atlasgpu_model_get(atlasgpu_ctx *ctx, atlasgpu_model *m, double *t, double *
  * count (a warm start). */
 int atlasgpu_model_set_structure(atlasgpu_ctx *ctx, atlasgpu_model *m, const double *t,
                                  const double *p, const double *rhox);
+/* New stellar parameters for the next model on the same line list and grid
+ * (call atlasgpu_model_set_structure after it); no reference counterpart:
+ * the reference runs one model per process. */
+int atlasgpu_model_set_params(atlasgpu_ctx *ctx, atlasgpu_model *m, double teff, double logg,
+                              double vturb_kms, double mh);
 int atlasgpu_model_destroy(atlasgpu_ctx *ctx, atlasgpu_model *m);
 
 /* The RT-pass frequency loop for callers that cannot allocate device memory.
@@ -273,6 +279,31 @@ int atlasgpu_atlas_rt_pass_noalloc(atlasgpu_ctx *ctx, int numnu, const double *d
                                    const double *d_xlines_t, int nrhox, const double *d_rhox,
                                    const double *d_t, const double *d_hkt, double teff,
                                    double *d_sums, double *d_hsurf);
+
+/* ---- learned warm start ----------------------------------------------
+ * A dense tanh MLP nin -> nh1 -> nh2 -> nout (FP32) that maps stellar
+ * parameters to a starting structure; trained on the device on converged
+ * models of this library's own ATLAS12 iteration.  No reference counterpart
+ * (the reference starts from a tabulated model).  Parameters are one flat
+ * vector [W1 (nh1 x nin), b1, W2 (nh2 x nh1), b2, W3 (nout x nh2), b3], W
+ * row-major [out][in]; x [n][nin], targets/outputs [n][nout] (host).
+ * Loss: mean squared error over samples and outputs. */
+typedef struct atlasgpu_mlp atlasgpu_mlp;
+int atlasgpu_mlp_create(atlasgpu_ctx *ctx, int nin, int nh1, int nh2, int nout, uint64_t seed,
+                        atlasgpu_mlp **out);
+int atlasgpu_mlp_destroy(atlasgpu_ctx *ctx, atlasgpu_mlp *p);
+int64_t atlasgpu_mlp_nparam(atlasgpu_mlp *p);
+int atlasgpu_mlp_get_params(atlasgpu_ctx *ctx, atlasgpu_mlp *p, float *out);
+int atlasgpu_mlp_set_params(atlasgpu_ctx *ctx, atlasgpu_mlp *p, const float *in);
+int atlasgpu_mlp_forward(atlasgpu_ctx *ctx, atlasgpu_mlp *p, const float *x, int n, float *y);
+/* Loss and its gradient over the n samples (grad [nparam], may be NULL). */
+int atlasgpu_mlp_loss_grad(atlasgpu_ctx *ctx, atlasgpu_mlp *p, const float *x, const float *t, int n,
+                           float *grad, float *loss);
+/* Adam (lr, beta 0.9/0.999, eps 1e-8) over `epochs` shuffled passes in
+ * minibatches of `batch`; loss_hist [epochs] (may be NULL) receives each
+ * epoch's last minibatch loss. */
+int atlasgpu_mlp_train(atlasgpu_ctx *ctx, atlasgpu_mlp *p, const float *x, const float *t, int n,
+                       int epochs, int batch, float lr, uint64_t seed, float *loss_hist);
 
 /* Measured FP64 FMA throughput of the device (TFLOP/s, 2 flops per FMA):
  * the denominator of the FP64-pipe roofline of the transfer kernels.  No

@@ -185,3 +185,21 @@ def test_ttaup_reproduces_reference_deck(po, tables):
     assert np.max(np.abs(pout / p - 1.0)) < 3e-3
     assert np.max(np.abs(ptot / (g * rhox) - 1.0)) < 3e-3
     assert np.max(np.abs(abstd / ab - 1.0)) < 2e-3
+
+
+def test_mlp_oracle_gradient_is_the_derivative():
+    """The network restatement's analytic gradient against central differences."""
+    import mlp_ref
+    shape = (4, 6, 5, 7)
+    rng = np.random.default_rng(0)
+    n = sum(a * b + a for a, b in ((6, 4), (5, 6), (7, 5)))
+    p = rng.normal(0, 0.5, n)
+    x = rng.uniform(-1, 1, (9, 4))
+    t = rng.normal(0, 1, (9, 7))
+    _, g = mlp_ref.loss_grad(p, x, t, shape)
+    h = 1e-6
+    for i in rng.choice(n, 25, replace=False):
+        e = np.zeros(n)
+        e[i] = h
+        fd = (mlp_ref.loss_grad(p + e, x, t, shape)[0] - mlp_ref.loss_grad(p - e, x, t, shape)[0]) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-7 + 1e-6 * abs(g[i])
