@@ -95,7 +95,18 @@ SIGNATURES = {
     "atlasgpu_mlp_loss_grad": (_I, [_P, _P, _P, _P, _I, _P, _P]),
     "atlasgpu_mlp_train": (_I, [_P, _P, _P, _P, _I, _I, _I, ctypes.c_float, ctypes.c_uint64, _P]),
     "atlasgpu_atlas_rt_pass_noalloc": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _D, _P, _P]),
+    "atlasgpu_batch_create": (_I, [_P, ctypes.c_void_p, _I, ctypes.POINTER(_P)]),
+    "atlasgpu_batch_load": (_I, [_P, _P, _I, _D, _D, _D, _D, _P, _P, _P, _I, _D]),
+    "atlasgpu_batch_step": (_I, [_P, _P, _I]),
+    "atlasgpu_batch_poll": (_I, [_P, _P, _P, _P, _P, ctypes.POINTER(_I)]),
+    "atlasgpu_batch_run": (_I, [_P, _P, _I, _P, _P, _P]),
+    "atlasgpu_batch_get": (_I, [_P, _P, _I, _P, _P, _P, _P, _P, _P, _P]),
+    "atlasgpu_batch_nslots": (_I, [_P]),
+    "atlasgpu_batch_destroy": (_I, [_P, _P]),
 }
+
+SLOT_IDLE, SLOT_RUNNING, SLOT_CONVERGED, SLOT_NONFINITE, SLOT_CAPPED = 0, 1, 2, 3, 4
+BATCH_MAX_ITER = 256
 
 _DP = ctypes.POINTER(ctypes.c_double)
 

@@ -213,3 +213,121 @@ class AtlasModel:
             self.close()
         except Exception:
             pass
+
+
+class AtlasBatch:
+    """Many ATLAS12 atmospheres iterated together on the device
+    (atlasgpu_batch_*): they share one frequency grid, line list and Voigt
+    tables; each slot has its own parameters and structure.
+
+        b = AtlasBatch(ctx, operators, nslots=32, linedata=lines, waveset=ws, rcoset=rc)
+        results = b.run_queue(params, starts)     # work queue over all models
+
+    The reference runs the same models as one process each
+    (scripts/runat12_grid.slurm:1-16).
+    """
+
+    def __init__(self, ctx: Context, operators, nslots, linedata=None, waveset=None, rcoset=None, nrhox=72,
+                 h_tables=None):
+        self.ctx = ctx
+        ctx.set_operators(operators["xtau8"], operators["coefj"], operators["coefh"], operators["ch_j"],
+                          operators["ck_j"])
+        if waveset is None:
+            waveset, rcoset = synthetic.geometric_waveset()
+        self.waveset = np.ascontiguousarray(waveset, np.float64)
+        self.rcoset = np.ascontiguousarray(rcoset, np.float64)
+        self.cutwave = cutoff_grid()
+        ld = np.zeros((0, 4), np.int32) if linedata is None else np.ascontiguousarray(linedata, np.int32)
+        h0, h1, h2 = h_tables or tabvoigt(operators)
+        dummy = np.ones(nrhox)
+        keep = [np.ascontiguousarray(x, np.float64) for x in (dummy, dummy, dummy, dummy, h0, h1, h2)] + [ld]
+        t, p, rx, tau, h0, h1, h2, ld = keep
+        self.nrhox = nrhox
+        self.nslots = int(nslots)
+        d = ModelDesc(5777.0, 4.44, 1.5, nrhox, _dp(t), _dp(p), _dp(rx), _dp(tau), _dp(self.waveset),
+                      _dp(self.rcoset), self.waveset.size, _dp(self.cutwave), self.cutwave.size,
+                      ld.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ld.shape[0], _dp(h0), _dp(h1), _dp(h2), 0.0)
+        self._h = ctypes.c_void_p()
+        ctx.call("atlasgpu_batch_create", ctypes.byref(d), self.nslots, ctypes.byref(self._h))
+
+    def load(self, slot, teff, logg, vturb, mh, start, max_iter=60, tol_percent=0.1):
+        """Start a model in `slot` from start = dict(t, p, rhox) on TAUSTD."""
+        arrs = [np.ascontiguousarray(start[k], np.float64) for k in ("t", "p", "rhox")]
+        self.ctx.call("atlasgpu_batch_load", self._h, int(slot), float(teff), float(logg), float(vturb), float(mh),
+                      *[ptr(a) for a in arrs], int(max_iter), float(tol_percent))
+
+    def step(self, n=1):
+        self.ctx.call("atlasgpu_batch_step", self._h, int(n))
+
+    def poll(self):
+        """(status, iterations done, last max |FLXERR|) per slot, and the number running."""
+        st = np.zeros(self.nslots, np.int32)
+        it = np.zeros(self.nslots, np.int32)
+        er = np.zeros(self.nslots)
+        run = ctypes.c_int(0)
+        self.ctx.call("atlasgpu_batch_poll", self._h, ptr(st), ptr(it), ptr(er), ctypes.byref(run))
+        return st, it, er, run.value
+
+    def run(self, poll_every=4):
+        st = np.zeros(self.nslots, np.int32)
+        it = np.zeros(self.nslots, np.int32)
+        er = np.zeros(self.nslots)
+        self.ctx.call("atlasgpu_batch_run", self._h, int(poll_every), ptr(st), ptr(it), ptr(er))
+        return st, it, er
+
+    def structure(self, slot, iters=None):
+        n = self.nrhox
+        out = {k: np.zeros(n) for k in ("t", "rhox", "p", "xne", "flxerr")}
+        hs = np.zeros(self.waveset.size)
+        hist = np.zeros(_lib.BATCH_MAX_ITER)
+        self.ctx.call("atlasgpu_batch_get", self._h, int(slot), *[ptr(out[k]) for k in ("t", "rhox", "p", "xne",
+                                                                                        "flxerr")], ptr(hs),
+                      ptr(hist))
+        out["hsurf"] = hs
+        if iters is not None:
+            out["hist"] = hist[:iters]
+        return out
+
+    def run_queue(self, params, starts, max_iter=60, tol_percent=0.1, poll_every=2, keep=True):
+        """Iterate every model of `params` ([n, 4]: Teff, log g, [M/H], vturb)
+        from starts[i] (dict t, p, rhox), keeping all slots busy: a slot that
+        finishes is read back and loaded with the next model.  Returns a
+        list of dicts (status, iters, maxerr, and the structure when keep)."""
+        n = len(params)
+        res = [None] * n
+        slot_of = [-1] * self.nslots
+        nxt = 0
+        for s in range(min(self.nslots, n)):
+            teff, logg, mh, vt = params[nxt]
+            self.load(s, teff, logg, vt, mh, starts[nxt], max_iter, tol_percent)
+            slot_of[s] = nxt
+            nxt += 1
+        while any(k >= 0 for k in slot_of):
+            self.step(poll_every)
+            st, it, er, _ = self.poll()
+            for s in range(self.nslots):
+                i = slot_of[s]
+                if i < 0 or st[s] == _lib.SLOT_RUNNING:
+                    continue
+                r = {"status": int(st[s]), "iters": int(it[s]), "maxerr": float(er[s])}
+                if keep:
+                    r.update(self.structure(s, int(it[s])))
+                res[i] = r
+                slot_of[s] = -1
+                if nxt < n:
+                    teff, logg, mh, vt = params[nxt]
+                    self.load(s, teff, logg, vt, mh, starts[nxt], max_iter, tol_percent)
+                    slot_of[s] = nxt
+                    nxt += 1
+        return res
+
+    def close(self):
+        if self._h:
+            _lib.lib().atlasgpu_batch_destroy(self.ctx.handle, self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

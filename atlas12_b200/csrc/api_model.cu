@@ -6,15 +6,9 @@
 #include <vector>
 
 #include "api_common.cuh"
-#include "atlas.cuh"
-#include "tcorr.cuh"
+#include "model.cuh"
 
 using namespace atlasgpu;
-
-namespace {
-constexpr int kNState = 17;         // ModelState vectors
-constexpr int kRossMax = 80 * 60;   // ROSSTAB_MAXTAB = kw*60 with the reference's kw = 80
-}  // namespace
 
 struct atlasgpu_model {
   int nrhox, kw, numnu, nwave, nspec;
@@ -53,42 +47,14 @@ __global__ void k_model_eos(ModelState* ms, const int* iter_dev, int nrhox, int 
                             double* txnxn, double* hkt, double* hckt, double* rho, ContCoef* cc) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nrhox) return;
-  const int iter = *iter_dev + 1;
-  const double t = ms->t[j];
-  double p = ms->p[j];
-  if (iter > 1) {
-    // P = GRAV*RHOX - PRAD - PTURB - PCON (atlas12c.f90:513-519), PCON = 0
-    p = grav * ms->rhox[j] - ms->prad[j] - ms->pturb[j] - 0.0;
-    if (p <= 0.0) p = fmax(grav * ms->rhox[j] * 1.0e-4, 1.0e-10);
-    ms->p[j] = p;
-  }
-  ContCoef c;
-  const EosOut e = surrogate_depth(t, p, vturb_cms, mh, j, kw, xnfdop, dopple, &c);
-  cc[j] = c;
-  xne_eos[j] = e.xne;
-  ms->xne[j] = e.xne;
-  rho[j] = e.rho;
-  const double tk = kKbol * t;
-  hkt[j] = kHplanck / tk;
-  hckt[j] = hkt[j] * kClight;
-  // TXNXN = (XNF(H I) + 0.42 XNF(He I) + 0.85 XNF(H2)) (T/1e4)^0.3
-  txnxn[j] = (e.nh * (1.0 - e.xh) + 0.42 * 0.085 * e.nh) * pow(t / 10000.0, 0.3);
+  model_eos_depth(ms, *iter_dev + 1, j, kw, grav, vturb_cms, mh, xnfdop, dopple, xne_eos, txnxn, hkt, hckt, rho,
+                  cc);
 }
 
 // KAPCONT (atlas12_modules.f90:19072-19138) on the surrogate continuum
 __global__ void k_model_kapcont(const double* cutwave, int nwave, const double* waveset, int nrhox,
                                 int kw, const double* hkt, const ContCoef* cc, double* tabcont) {
-  const int nu = blockIdx.x;  // 0..nwave-1
-  const double wave = cutwave[nu];
-  const double freq = kClightNms / wave;
-  for (int j = threadIdx.x; j < nrhox; j += blockDim.x) {
-    double acont = 1.0e10, sigmac = 0.0;
-    if (wave > waveset[0]) surrogate_kapp(cc[j], wave, acont, sigmac);
-    const double stim = 1.0 - exp(-freq * hkt[j]);
-    const double v = (acont + sigmac) * kLineCutoff / stim;
-    tabcont[(size_t)nu * kw + j] = v;
-    if (nu == nwave - 1) tabcont[(size_t)nwave * kw + j] = v;
-  }
+  model_kapcont_row(blockIdx.x, cutwave, nwave, waveset, nrhox, kw, hkt, cc, tabcont);
 }
 
 __global__ void __launch_bounds__(kFinThreads) k_model_finish(ModelState* ms, double* acc, int kw, int n,
@@ -105,18 +71,10 @@ __global__ void __launch_bounds__(kFinThreads) k_model_finish(ModelState* ms, do
   }
 }
 
-// KAPP stand-in for the RT pass: ACONT, SIGMAC [numnu][kw] from the surrogate
-// continuum coefficients of this iteration's structure
+// KAPP stand-in for the RT pass: ACONT, SIGMAC [numnu][kw]
 __global__ void k_model_kapp(const double* waveset, int numnu, int nrhox, int kw, const ContCoef* cc,
                              double* acont, double* sigmac) {
-  const int64_t n = (int64_t)numnu * nrhox;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int nu = (int)(e / nrhox), j = (int)(e % nrhox);
-    double ka, sg;
-    surrogate_kapp(cc[j], waveset[nu], ka, sg);
-    acont[(size_t)nu * kw + j] = ka;
-    sigmac[(size_t)nu * kw + j] = sg;
-  }
+  model_kapp_range(waveset, numnu, nrhox, kw, cc, acont, sigmac, nullptr);
 }
 
 __global__ void k_surrogate_eval(int nrhox, const double* t, const double* p, double vturb_cms, int nw,

@@ -164,7 +164,7 @@ static __device__ __noinline__ void linop_finish_warp(const LinopArgs& a, int J,
 // warp touch XLINES(J, IW) at consecutive J: one coalesced atomic per step.
 constexpr int kLinopLanePts = 4;
 
-static __global__ void __launch_bounds__(256) k_atlas_linop(LinopArgs a) {
+static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
   const int lane = threadIdx.x & 31;
   const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -265,6 +265,8 @@ static __global__ void __launch_bounds__(256) k_atlas_linop(LinopArgs a) {
   if (lane == 0 && walked && a.npairs) atomicAdd(a.npairs, walked);
 }
 
+static __global__ void __launch_bounds__(256) k_atlas_linop(LinopArgs a) { linop_body(a); }
+
 // ---------------------------------------------------------------- RT pass
 __device__ __forceinline__ double expi3(double x) {
   // EXPI(3, x), atlas12_modules.f90:21103-21225 (Cody & Thacher 1968)
@@ -334,7 +336,7 @@ constexpr int kRtThreads = kRtGroups * PairG::N;
 // shared memory: RHOX and a zero vector (SIGMAL) for the CTA, then the groups' workspaces
 __host__ __device__ inline size_t rt_smem_bytes() { return 2 * sizeof(double) * kKwMax + kRtGroups * sizeof(RtWS); }
 
-static __global__ void __launch_bounds__(kRtThreads, 3) k_atlas_rt(RtArgs a) {
+static __device__ __forceinline__ void rt_body(const RtArgs& a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int gid = threadIdx.x / PairG::N;
   double* rhox_s = reinterpret_cast<double*>(smem_raw);
@@ -443,14 +445,16 @@ static __global__ void __launch_bounds__(kRtThreads, 3) k_atlas_rt(RtArgs a) {
   if (g.r == 0) out[kAcc * a.kw] = pradk0;
 }
 
+static __global__ void __launch_bounds__(kRtThreads, 3) k_atlas_rt(RtArgs a) { rt_body(a); }
+
 // fixed-order sum of the per-warp partials: out[kAcc*kw + 1].  A block owns
 // 32 consecutive sums (threadIdx.x) and splits the rows over 32 row groups
 // (threadIdx.y: rows y, y+32, ...); the 32 group sums are then added in group
 // order.  The order is fixed by the launch shape, so the result does not
 // depend on scheduling.
 constexpr int kRedCols = 32, kRedRows = 32;
-static __global__ void __launch_bounds__(kRedCols* kRedRows)
-    k_atlas_reduce(const double* __restrict__ partial, int nwarps, int kw, int n, double* __restrict__ out) {
+static __device__ __forceinline__ void reduce_body(const double* __restrict__ partial, int nwarps, int kw,
+                                                   double* __restrict__ out) {
   __shared__ double s[kRedRows][kRedCols + 1];
   const int stride = kAcc * kw + 1;
   const int e = blockIdx.x * kRedCols + threadIdx.x;
@@ -474,13 +478,16 @@ static __global__ void __launch_bounds__(kRedCols* kRedRows)
     for (int y = 0; y < kRedRows; ++y) t += s[y][threadIdx.x];
     out[e] = t;
   }
-  (void)n;
+}
+
+static __global__ void __launch_bounds__(kRedCols* kRedRows)
+    k_atlas_reduce(const double* __restrict__ partial, int nwarps, int kw, double* __restrict__ out) {
+  reduce_body(partial, nwarps, kw, out);
 }
 
 inline void launch_reduce(const double* partial, int nwarps, int kw, double* out, cudaStream_t st) {
   const int stride = kAcc * kw + 1;
-  k_atlas_reduce<<<(stride + kRedCols - 1) / kRedCols, dim3(kRedCols, kRedRows), 0, st>>>(partial, nwarps, kw, 0,
-                                                                                            out);
+  k_atlas_reduce<<<(stride + kRedCols - 1) / kRedCols, dim3(kRedCols, kRedRows), 0, st>>>(partial, nwarps, kw, out);
 }
 
 }  // namespace atlasgpu

@@ -280,6 +280,53 @@ int atlasgpu_atlas_rt_pass_noalloc(atlasgpu_ctx *ctx, int numnu, const double *d
                                    const double *d_t, const double *d_hkt, double teff,
                                    double *d_sums, double *d_hsurf);
 
+/* ---- batched ATLAS12 models ----------------------------------------
+ * Replaces the reference's grid runs, which start one atlas12c process per
+ * model (scripts/runat12_grid.slurm:1-16, scripts/atlas12.sh:231), each
+ * running the iteration loop of atlas12c.f90:496-606.  A batch holds
+ * `nslots` atmospheres that share the frequency grid, the line list and the
+ * Voigt tables of the descriptor (its starting model and stellar parameters
+ * are not used); every slot has its own parameters, structure and ROSSTAB
+ * history.  One captured CUDA graph runs one iteration of every RUNNING
+ * slot; a slot leaves the iteration by itself (status word on the device)
+ * when max |FLXERR| <= its tolerance (CONVERGED), when it is not finite
+ * (NONFINITE) or at its iteration cap (CAPPED), so a finished slot can be
+ * loaded with the next model while the others run. */
+#define ATLASGPU_BATCH_MAX_SLOTS 1024
+#define ATLASGPU_BATCH_MAX_ITER 256
+#define ATLASGPU_SLOT_IDLE 0
+#define ATLASGPU_SLOT_RUNNING 1
+#define ATLASGPU_SLOT_CONVERGED 2
+#define ATLASGPU_SLOT_NONFINITE 3
+#define ATLASGPU_SLOT_CAPPED 4
+typedef struct atlasgpu_batch atlasgpu_batch;
+int atlasgpu_batch_create(atlasgpu_ctx *ctx, const atlasgpu_model_desc *shared, int nslots,
+                          atlasgpu_batch **out);
+/* Start a model in `slot` (status RUNNING, iteration count 0) from the
+ * structure T, P, RHOX [nrhox] on TAUSTD (READIN's starting model,
+ * atlas12c.f90:256), with at most max_iter (<= ATLASGPU_BATCH_MAX_ITER)
+ * iterations and convergence at max |FLXERR| <= tol_percent (<= 0: run
+ * max_iter).  Waits for the context stream. */
+int atlasgpu_batch_load(atlasgpu_ctx *ctx, atlasgpu_batch *b, int slot, double teff, double logg,
+                        double vturb_kms, double mh, const double *t, const double *p,
+                        const double *rhox, int max_iter, double tol_percent);
+/* Enqueue n iterations of every RUNNING slot (graph replays; per-launch
+ * timed launches when timing is enabled); returns without waiting. */
+int atlasgpu_batch_step(atlasgpu_ctx *ctx, atlasgpu_batch *b, int n);
+/* Wait, then read every slot's status, iterations done and last max
+ * |FLXERR| (arrays [nslots], any may be NULL) and the number still running. */
+int atlasgpu_batch_poll(atlasgpu_ctx *ctx, atlasgpu_batch *b, int *status, int *iters,
+                        double *maxerr, int *nrunning);
+/* Step and poll (every poll_every iterations) until no slot is RUNNING. */
+int atlasgpu_batch_run(atlasgpu_ctx *ctx, atlasgpu_batch *b, int poll_every, int *status, int *iters,
+                       double *maxerr);
+/* A slot's structure (each [nrhox]), HNU(1) per frequency [numnu] of its last
+ * iteration and its max |FLXERR| history [iterations done]; any may be NULL. */
+int atlasgpu_batch_get(atlasgpu_ctx *ctx, atlasgpu_batch *b, int slot, double *t, double *rhox,
+                       double *p, double *xne, double *flxerr, double *hsurf, double *maxerr_hist);
+int atlasgpu_batch_nslots(atlasgpu_batch *b);
+int atlasgpu_batch_destroy(atlasgpu_ctx *ctx, atlasgpu_batch *b);
+
 /* ---- learned warm start ----------------------------------------------
  * A dense tanh MLP nin -> nh1 -> nh2 -> nout (FP32) that maps stellar
  * parameters to a starting structure; trained on the device on converged

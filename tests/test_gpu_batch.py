@@ -1,0 +1,95 @@
+"""Batched ATLAS12 models (atlasgpu_batch_*) against the single-model path.
+
+Every slot of a batch must follow exactly the iteration a lone model follows
+from the same start: the batch only changes how the work is launched (one
+graph for all slots) and how the frequency sums are grouped before their
+fixed-order reduction.  Tolerance: relative 1e-8 on T, P, RHOX and on each
+iteration's max |FLXERR| after 5 iterations (the frequency-sum grouping
+differs, the rest is the same FP64 arithmetic).
+"""
+import numpy as np
+import pytest
+
+from atlas12_b200 import _lib, atlas, surrogate, synthetic
+
+pytestmark = pytest.mark.gpu
+
+PARAMS = [(5777.0, 4.44, 0.0, 1.5), (6200.0, 4.2, -0.5, 2.0), (5400.0, 4.6, 0.3, 1.0)]
+NIT = 5
+
+
+@pytest.fixture(scope="module")
+def small_grid():
+    ws, rc = synthetic.geometric_waveset(9.0, 160000.0, 2000)
+    lines = synthetic.atlas_lines(5000, ws[2], ws[-3], seed=3)
+    return ws, rc, lines
+
+
+def _start(teff, logg, mh):
+    return surrogate.grey_model(teff, logg, ross=surrogate.RossTable(mh=mh, nwave=600))
+
+
+@pytest.fixture(scope="module")
+def singles(gpu_ctx, tables, small_grid):
+    ws, rc, lines = small_grid
+    out = []
+    m = atlas.AtlasModel(gpu_ctx, tables, linedata=lines, waveset=ws, rcoset=rc)
+    for teff, logg, mh, vt in PARAMS:
+        s = _start(teff, logg, mh)
+        m.set_params(teff, logg, vt, mh)
+        m.set_structure(s["t"], s["p"], s["rhox"])
+        n, hist = m.iterate(max_iter=NIT, tol_percent=0.0, graph=True)
+        assert n == NIT
+        out.append(dict(m.structure(), hist=hist))
+    m.close()
+    return out
+
+
+def test_batch_queue_matches_single_models(gpu_ctx, tables, small_grid, singles):
+    ws, rc, lines = small_grid
+    b = atlas.AtlasBatch(gpu_ctx, tables, nslots=2, linedata=lines, waveset=ws, rcoset=rc)
+    starts = [_start(teff, logg, mh) for teff, logg, mh, _ in PARAMS]
+    # three models through two slots: the third reuses a slot that held another model
+    res = b.run_queue(PARAMS, starts, max_iter=NIT, tol_percent=0.0, poll_every=2)
+    for i, (r, s) in enumerate(zip(res, singles)):
+        assert r["status"] == _lib.SLOT_CAPPED and r["iters"] == NIT, (i, r["status"], r["iters"])
+        for k in ("t", "p", "rhox"):
+            np.testing.assert_allclose(r[k], s[k], rtol=1e-8, err_msg=f"model {i} {k}")
+        np.testing.assert_allclose(r["hist"], s["hist"], rtol=1e-8, err_msg=f"model {i} history")
+        np.testing.assert_allclose(r["hsurf"], s["hsurf"], rtol=1e-8, err_msg=f"model {i} HNU(1)")
+    b.close()
+
+
+def test_batch_slots_stop_by_themselves(gpu_ctx, tables, small_grid):
+    """A converged slot (tol above its error) stops; the others keep their cap;
+    idle slots never run; extra graph replays change nothing."""
+    ws, rc, lines = small_grid
+    b = atlas.AtlasBatch(gpu_ctx, tables, nslots=4, linedata=lines, waveset=ws, rcoset=rc)
+    teff, logg, mh, vt = PARAMS[0]
+    s = _start(teff, logg, mh)
+    b.load(0, teff, logg, vt, mh, s, max_iter=6, tol_percent=1e9)  # converges at its first iteration
+    b.load(1, teff, logg, vt, mh, s, max_iter=3, tol_percent=0.0)
+    b.load(3, teff, logg, vt, mh, s, max_iter=4, tol_percent=0.0)
+    st, it, er = b.run(poll_every=3)
+    assert list(st) == [_lib.SLOT_CONVERGED, _lib.SLOT_CAPPED, _lib.SLOT_IDLE, _lib.SLOT_CAPPED]
+    assert list(it) == [1, 3, 0, 4]
+    t3 = b.structure(3)["t"].copy()
+    b.step(3)
+    st2, it2, _, run = b.poll()
+    assert run == 0 and list(it2) == list(it)
+    np.testing.assert_array_equal(b.structure(3)["t"], t3)
+    b.close()
+
+
+def test_batch_rejects_bad_arguments(gpu_ctx, tables, small_grid):
+    ws, rc, lines = small_grid
+    b = atlas.AtlasBatch(gpu_ctx, tables, nslots=2, linedata=lines[:100], waveset=ws, rcoset=rc)
+    s = _start(5777.0, 4.44, 0.0)
+    with pytest.raises(_lib.AtlasGPUError, match="bad argument"):
+        b.load(2, 5777.0, 4.44, 1.5, 0.0, s)
+    with pytest.raises(_lib.AtlasGPUError, match="bad argument"):
+        b.load(0, 5777.0, 4.44, 1.5, 0.0, s, max_iter=_lib.BATCH_MAX_ITER + 1)
+    bad = dict(s, t=np.where(np.arange(s["t"].size) == 7, -1.0, s["t"]))
+    with pytest.raises(_lib.AtlasGPUError, match="depth 8"):
+        b.load(0, 5777.0, 4.44, 1.5, 0.0, bad)
+    b.close()
