@@ -155,6 +155,10 @@ int atlasgpu_atlas_set_voigt_tables(atlasgpu_ctx* ctx, const double* h0, const d
   CK(cudaMemcpy(d0, h0, n * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(d1, h1, n * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(d2, h2, n * sizeof(double), cudaMemcpyHostToDevice));
+  float4* df;
+  if ((r = bufT(ctx, "tab_hf", n, &df))) return r;
+  const std::vector<float4> hf = pack_voigt_f32(h0, h1, h2, n);
+  CK(cudaMemcpy(df, hf.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
   return 0;
 }
 
@@ -203,9 +207,11 @@ int atlasgpu_atlas_linop(atlasgpu_ctx* ctx, const int32_t* linedata, int64_t n, 
     if ((r = atlas_prep_lines(ctx, d_ld, linedata, n, tl, d_ws, waveset, numnu, d_iw, nwave, nspec, d_lines))) return r;
     LinopArgs a{d_lines, n, nrhox, kw, nspec, numnu, d_xd, d_dp, d_xne, d_tx, d_hc, d_tc, d_ws,
                 (const double*)ctx->bufs["tab_h0"].first, (const double*)ctx->bufs["tab_h1"].first,
-                (const double*)ctx->bufs["tab_h2"].first, d_xl, d_cnt, d_cnt + 1};
+                (const double*)ctx->bufs["tab_h2"].first, (const float4*)ctx->bufs["tab_hf"].first, d_xl, d_cnt,
+                d_cnt + 1};
     Timer tm(ctx, "atlas_linop");
-    k_atlas_linop<<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
+    if (ctx->precision == ATLASGPU_PREC_MIXED) k_atlas_linop<true><<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
+    else k_atlas_linop<false><<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
     CKL(ctx);
   }
   CK(cudaMemcpyAsync(xlines_out, d_xl, (size_t)kw * numnu * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -80,11 +80,12 @@ __global__ void k_batch_kapp(BatchDev d) {
   model_kapp_range(d.waveset, d.numnu, d.nrhox, d.kw, d.cc + (size_t)b * d.kw, d.acont + o, d.sigmac + o, d.xl + o);
 }
 
-__global__ void __launch_bounds__(256) k_batch_linop(const LinopArgs* __restrict__ args, const BatchCtl* ctl) {
+template <bool F32>
+__global__ void __launch_bounds__(256, 3) k_batch_linop(const LinopArgs* __restrict__ args, const BatchCtl* ctl) {
   const int b = blockIdx.y;
   if (!running(ctl, b)) return;
   const LinopArgs a = args[b];
-  linop_body(a);
+  linop_body<F32>(a);
 }
 
 __global__ void __launch_bounds__(kRtThreads, 3) k_batch_rt(const RtArgs* __restrict__ args, const BatchCtl* ctl) {
@@ -140,6 +141,8 @@ struct atlasgpu_batch {
   BatchDev d{};
   // batch-wide device data
   double *waveset = nullptr, *rcoset = nullptr, *cutwave = nullptr, *h0 = nullptr, *h1 = nullptr, *h2 = nullptr;
+  float4* hf = nullptr;
+  int graph_precision = -1;  // precision the captured graph was built with
   double *ross = nullptr, *state = nullptr;
   int32_t *iwavetab = nullptr, *linedata = nullptr;
   AtlasLine* lines = nullptr;
@@ -176,7 +179,10 @@ int enqueue_batch(atlasgpu_ctx* ctx, atlasgpu_batch* B, bool timed) {
   }
   if (B->nlines > 0) {
     Timer tm(ctx, "batch_linop");
-    k_batch_linop<<<dim3(B->grid_linop, nb), 256, 0, s>>>(B->la, B->d.ctl);
+    if (ctx->precision == ATLASGPU_PREC_MIXED)
+      k_batch_linop<true><<<dim3(B->grid_linop, nb), 256, 0, s>>>(B->la, B->d.ctl);
+    else
+      k_batch_linop<false><<<dim3(B->grid_linop, nb), 256, 0, s>>>(B->la, B->d.ctl);
     CKL(ctx);
   }
   {
@@ -214,7 +220,7 @@ int atlasgpu_batch_destroy(atlasgpu_ctx* ctx, atlasgpu_batch* B) {
   const BatchDev& d = B->d;
   void* ps[] = {d.ctl, d.ms, d.R, d.xnfdop, d.dopple, d.xne_eos, d.txnxn, d.hkt, d.hckt, d.rho, d.cc, d.acont,
                 d.sigmac, d.xl, d.tabcont, d.partial, d.sum, d.hist, d.hsurf, B->waveset, B->rcoset, B->cutwave, B->h0,
-                B->h1, B->h2, B->ross, B->state, B->iwavetab, B->linedata, B->lines, B->la, B->ra, B->cnt};
+                B->h1, B->h2, B->hf, B->ross, B->state, B->iwavetab, B->linedata, B->lines, B->la, B->ra, B->cnt};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete B;
@@ -272,7 +278,7 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
       (r = balloc(ctx, &B->waveset, B->numnu)) ||
       (r = balloc(ctx, &B->rcoset, B->numnu)) || (r = balloc(ctx, &B->cutwave, B->nwave)) ||
       (r = balloc(ctx, &B->iwavetab, B->nwave + 1)) || (r = balloc(ctx, &B->h0, 2001)) ||
-      (r = balloc(ctx, &B->h1, 2001)) || (r = balloc(ctx, &B->h2, 2001)) ||
+      (r = balloc(ctx, &B->h1, 2001)) || (r = balloc(ctx, &B->h2, 2001)) || (r = balloc(ctx, &B->hf, 2001)) ||
       (r = balloc(ctx, &B->ross, (size_t)nb * 3 * kRossMax)) || (r = balloc(ctx, &B->state, (size_t)nb * kNState * kw)) ||
       (r = balloc(ctx, &B->linedata, (size_t)B->nlines * 4)) || (r = balloc(ctx, &B->lines, (size_t)B->nlines)) ||
       (r = balloc(ctx, &B->la, nb)) || (r = balloc(ctx, &B->ra, nb)) || (r = balloc(ctx, &B->cnt, 2))) {
@@ -310,7 +316,7 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
     const size_t o = (size_t)b * kw, os = (size_t)b * nsk, on = (size_t)b * nnk;
     la[b] = LinopArgs{B->lines, B->nlines, B->nrhox, kw, B->nspec, B->numnu, d.xnfdop + os, d.dopple + os,
                       d.xne_eos + o, d.txnxn + o, d.hckt + o, d.tabcont + (size_t)b * (B->nwave + 1) * kw,
-                      B->waveset, B->h0, B->h1, B->h2, d.xl + on, nullptr, B->cnt};
+                      B->waveset, B->h0, B->h1, B->h2, B->hf, d.xl + on, nullptr, B->cnt};
     ra[b] = RtArgs{ctx->ops, B->numnu, B->nrhox, kw, B->waveset, B->rcoset, d.acont + on, d.sigmac + on, nullptr,
                    d.xl + on, ms[b].rhox, ms[b].t, d.hkt + o, 0.0, nu_per, 1, kw,
                    d.partial + (size_t)b * d.nwl * stride, d.hsurf + (size_t)b * B->numnu, nullptr};
@@ -342,6 +348,10 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
   CK(cudaMemcpyAsync(B->h0, dsc->h0tab, 2001 * sizeof(double), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(B->h1, dsc->h1tab, 2001 * sizeof(double), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(B->h2, dsc->h2tab, 2001 * sizeof(double), cudaMemcpyHostToDevice, s));
+  {
+    const std::vector<float4> hf = pack_voigt_f32(dsc->h0tab, dsc->h1tab, dsc->h2tab, 2001);
+    CK(cudaMemcpy(B->hf, hf.data(), hf.size() * sizeof(float4), cudaMemcpyHostToDevice));
+  }
   CK(cudaMemsetAsync(B->cnt, 0, 2 * sizeof(unsigned long long), s));
   double* tl;
   {
@@ -417,6 +427,13 @@ int atlasgpu_batch_step(atlasgpu_ctx* ctx, atlasgpu_batch* B, int n) {
       if ((r = enqueue_batch(ctx, B, true))) return r;
       continue;
     }
+    if (B->gexec && B->graph_precision != ctx->precision) {
+      // the graph holds the kernels of the precision it was captured with
+      cudaGraphExecDestroy(B->gexec);
+      cudaGraphDestroy(B->graph);
+      B->gexec = nullptr;
+      B->graph = nullptr;
+    }
     if (!B->gexec) {
       CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       const int64_t l0 = ctx->launches;
@@ -430,6 +447,7 @@ int atlasgpu_batch_step(atlasgpu_ctx* ctx, atlasgpu_batch* B, int n) {
       if (ec != cudaSuccess) return fail(ctx, ATLASGPU_ECUDA, "batch graph capture: %s", cudaGetErrorString(ec));
       B->graph = g;
       CK(cudaGraphInstantiate(&B->gexec, g, 0));
+      B->graph_precision = ctx->precision;
       ctx->launches = l0;  // counted when replayed
     }
     CK(cudaGraphLaunch(B->gexec, s));

@@ -127,6 +127,13 @@ inline bool finite_all(const double* p, size_t n) {
   return true;
 }
 
+// TABVOIGT's H0, H1, H2 packed as FP32 (H0, H1, H2, 0) for the mixed-precision LINOP1 walk
+inline std::vector<float4> pack_voigt_f32(const double* h0, const double* h1, const double* h2, int n) {
+  std::vector<float4> v(n);
+  for (int i = 0; i < n; ++i) v[i] = make_float4((float)h0[i], (float)h1[i], (float)h2[i], 0.0f);
+  return v;
+}
+
 struct AtlasLine;
 int atlas_prep_lines(atlasgpu_ctx* ctx, const int32_t* d_ld, const int32_t* h_ld, int64_t n,
                      const double* d_tablog, const double* d_ws, const double* h_ws, int numnu,

@@ -28,6 +28,7 @@ struct atlasgpu_model {
   double* xl;            // XLINES(J, NU): [numnu][kw]
   double *partial, *sum, *hsurf;
   double *h0, *h1, *h2, *ross;  // ross: ROSSTAB points [3][kRossMax]
+  float4* hf;                    // FP32 (H0, H1, H2, 0)
   RossStore* R;                  // device
   int* iter_dev;         // iterations completed
   double* maxerr_dev;    // last max |FLXERR|
@@ -36,6 +37,7 @@ struct atlasgpu_model {
   size_t smem_rt;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
+  int graph_precision = -1;  // precision the captured graph was built with
   bool kapcont_done = false;
 };
 
@@ -117,10 +119,13 @@ int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
   CK(cudaMemsetAsync(m->xl, 0, (size_t)m->kw * m->numnu * sizeof(double), s));
   if (m->nlines > 0) {
     LinopArgs la{m->lines, m->nlines, m->nrhox, m->kw, m->nspec, m->numnu, m->xnfdop, m->dopple,
-                 m->xne_eos, m->txnxn, m->hckt, m->tabcont, m->waveset, m->h0, m->h1, m->h2, m->xl,
+                 m->xne_eos, m->txnxn, m->hckt, m->tabcont, m->waveset, m->h0, m->h1, m->h2, m->hf, m->xl,
                  nullptr, m->cnt};
     Timer tm(ctx, "atlas_linop");
-    k_atlas_linop<<<grid_for(ctx, m->nlines * 32, 256, 16), 256, 0, s>>>(la);
+    if (ctx->precision == ATLASGPU_PREC_MIXED)
+      k_atlas_linop<true><<<grid_for(ctx, m->nlines * 32, 256, 16), 256, 0, s>>>(la);
+    else
+      k_atlas_linop<false><<<grid_for(ctx, m->nlines * 32, 256, 16), 256, 0, s>>>(la);
     CKL(ctx);
   }
   {
@@ -248,7 +253,7 @@ int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlas
       (r = dalloc(ctx, &m->lines, (size_t)m->nlines)) || (r = dalloc(ctx, &m->xl, (size_t)kw * m->numnu)) ||
       (r = dalloc(ctx, &m->sum, kAcc * kw + 1)) ||
       (r = dalloc(ctx, &m->hsurf, m->numnu)) || (r = dalloc(ctx, &m->h0, 2001)) || (r = dalloc(ctx, &m->h1, 2001)) ||
-      (r = dalloc(ctx, &m->h2, 2001)) || (r = dalloc(ctx, &m->ross, nr)) || (r = dalloc(ctx, &m->R, 1)) || (r = dalloc(ctx, &m->iter_dev, 1)) ||
+      (r = dalloc(ctx, &m->h2, 2001)) || (r = dalloc(ctx, &m->hf, 2001)) || (r = dalloc(ctx, &m->ross, nr)) || (r = dalloc(ctx, &m->R, 1)) || (r = dalloc(ctx, &m->iter_dev, 1)) ||
       (r = dalloc(ctx, &m->maxerr_dev, 1)) || (r = dalloc(ctx, &m->cnt, 2))) {
     atlasgpu_model_destroy(ctx, m);
     return r;
@@ -311,6 +316,10 @@ int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlas
   CK(cudaMemcpyAsync(m->h1, d->h1tab, 2001 * sizeof(double), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(m->h2, d->h2tab, 2001 * sizeof(double), cudaMemcpyHostToDevice, s));
   {
+    const std::vector<float4> hf = pack_voigt_f32(d->h0tab, d->h1tab, d->h2tab, 2001);
+    CK(cudaMemcpy(m->hf, hf.data(), hf.size() * sizeof(float4), cudaMemcpyHostToDevice));
+  }
+  {
     RossStore R0{0, kRossMax, 0.0, 1.0, 0.0, 1.0, m->ross, m->ross + kRossMax, m->ross + 2 * kRossMax};
     CK(cudaMemcpy(m->R, &R0, sizeof R0, cudaMemcpyHostToDevice));
   }
@@ -353,6 +362,12 @@ int atlasgpu_model_iterate(atlasgpu_ctx* ctx, atlasgpu_model* m, int max_iter, d
       if ((r = enqueue_iteration(ctx, m, true))) return r;
       m->kapcont_done = true;
     } else if (use_graph) {
+      if (m->gexec && m->graph_precision != ctx->precision) {
+        cudaGraphExecDestroy(m->gexec);
+        cudaGraphDestroy(m->graph);
+        m->gexec = nullptr;
+        m->graph = nullptr;
+      }
       if (!m->gexec) {
         CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         const int64_t l0 = ctx->launches;
@@ -363,6 +378,7 @@ int atlasgpu_model_iterate(atlasgpu_ctx* ctx, atlasgpu_model* m, int max_iter, d
         if (ec != cudaSuccess) return fail(ctx, ATLASGPU_ECUDA, "graph capture: %s", cudaGetErrorString(ec));
         m->graph = g;
         CK(cudaGraphInstantiate(&m->gexec, g, 0));
+        m->graph_precision = ctx->precision;
         ctx->launches = l0;  // counted when replayed
       }
       CK(cudaGraphLaunch(m->gexec, s));
@@ -454,7 +470,7 @@ int atlasgpu_model_destroy(atlasgpu_ctx* ctx, atlasgpu_model* m) {
   void* ps[] = {m->state, m->ms, m->xnfdop, m->dopple, m->xne_eos, m->txnxn, m->hkt, m->hckt, m->rho, m->cc,
                 m->acont, m->sigmac,
                 m->waveset, m->rcoset, m->cutwave, m->tabcont, m->iwavetab, m->linedata, m->lines, m->xl,
-                m->partial, m->sum, m->hsurf, m->h0, m->h1, m->h2, m->ross, m->R, m->iter_dev,
+                m->partial, m->sum, m->hsurf, m->h0, m->h1, m->h2, m->hf, m->ross, m->R, m->iter_dev,
                 m->maxerr_dev, m->cnt};
   for (void* p : ps)
     if (p) cudaFree(p);

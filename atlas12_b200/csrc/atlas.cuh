@@ -106,27 +106,58 @@ struct LinopArgs {
   const double* tabcont;          // [nwave+1][kw]
   const double* waveset;
   const double *h0, *h1, *h2;     // 2001
+  const float4* hf;               // (H0, H1, H2, 0) in FP32 [2001], for the mixed-precision walk
   double* xl;                     // XLINES(J, NU): [numnu][kw]
   unsigned long long* npairs;     // diagnostics: walked (line, depth) pairs
   unsigned long long* used;       // LINEUSED: lines above TABCONT at a coarse depth
 };
 
-// LINOP1's profile value at one wing point: tabulated H(v, a) for
-// ADAMP <= 0.2 and v <= 10, the Lorentz wing 1/sqrt(pi) a / v^2 beyond,
-// the full VOIGT for ADAMP > 0.2 (atlas12_modules.f90:18290-18345)
-__device__ __forceinline__ double linop_cv(const LinopArgs& a, double center, double adamp, double vv) {
-  if (adamp > 0.20) return center * voigt_kurucz(vv, adamp, a.h0, a.h1, a.h2);
-  if (vv > 10.0) return center * kInvSqrtPi * adamp / (vv * vv);
+// LINOP1's profile value at one wing point, V = (distance in nm) * RDOP with
+// RDOP = 1 / (DOPPLE * WLVAC) taken once per (line, depth): tabulated H(v, a)
+// for ADAMP <= 0.2 and v <= 10, the Lorentz wing 1/sqrt(pi) a / v^2 beyond,
+// the full VOIGT for ADAMP > 0.2 (atlas12_modules.f90:18290-18345).
+// F32 (mixed precision) evaluates the tabulated and Lorentz values in FP32
+// from FP32 copies of the tables (hf = H0, H1, H2); V, the table index and
+// the regime tests stay FP64, so every point uses the table entry the FP64
+// walk uses.
+static __device__ __noinline__ double linop_full_voigt(const LinopArgs& a, double vv, double adamp) {
+  return voigt_kurucz(vv, adamp, a.h0, a.h1, a.h2);
+}
+
+template <bool F32>
+__device__ __forceinline__ double linop_cv(const LinopArgs& a, double center, double adamp, double dl, double rdop) {
+  const double vv = dl * rdop;
+  if (adamp > 0.20) return center * linop_full_voigt(a, vv, adamp);
+  if (vv > 10.0) {
+    if (F32) return (double)((float)center * ((float)(kInvSqrtPi * adamp) * __frcp_rn((float)(vv * vv))));
+    return center * kInvSqrtPi * adamp / (vv * vv);
+  }
   const int iv = (int)(vv * 200.0 + 1.5);
+  if (F32) {
+    const float4 h = a.hf[iv - 1];
+    const float af = (float)adamp;
+    return (double)((float)center * fmaf(fmaf(h.z, af, h.y), af, h.x));
+  }
   return center * ((a.h2[iv - 1] * adamp + a.h1[iv - 1]) * adamp + a.h0[iv - 1]);
+}
+
+// The wing walk stops at the first point whose value is below TABCONT.  In
+// FP32 a value within 1e-5 of the threshold is re-evaluated in FP64 for the
+// decision, so both precisions stop at the same point.
+template <bool F32>
+__device__ __forceinline__ bool linop_below(const LinopArgs& a, double cv, double tc, double center, double adamp,
+                                            double dl, double rdop) {
+  if (F32 && fabs(cv - tc) <= 1.0e-5 * tc) return linop_cv<false>(a, center, adamp, dl, rdop) < tc;
+  return cv < tc;
 }
 
 // The rest of one (line, depth) walk after a lane gave up on it, by the
 // whole warp (lanes over wing points), add-then-test as in the reference:
 // red points rnext..iwmax unless rdone, blue offsets bnext..100 unless bdone.
+template <bool F32>
 static __device__ __noinline__ void linop_finish_warp(const LinopArgs& a, int J, double center, double adamp,
-                                               double dopwave, double wlvac, int nu, double tc, int rnext,
-                                               bool rdone, int bnext, bool bdone, int lane) {
+                                                      double rdop, double wlvac, int nu, double tc, int rnext,
+                                                      bool rdone, int bnext, bool bdone, int lane) {
   double* xl = a.xl + (J - 1);
   const int iwmax = min(nu + 100, a.numnu);
   if (!rdone) {
@@ -134,8 +165,13 @@ static __device__ __noinline__ void linop_finish_warp(const LinopArgs& a, int J,
       const int iw = base + lane;
       const bool valid = iw <= iwmax;
       double cv = 0.0;
-      if (valid) cv = linop_cv(a, center, adamp, (a.waveset[iw - 1] - wlvac) / dopwave);
-      const unsigned stop = __ballot_sync(0xffffffffu, valid && cv < tc);
+      bool below = false;
+      if (valid) {
+        const double dl = a.waveset[iw - 1] - wlvac;
+        cv = linop_cv<F32>(a, center, adamp, dl, rdop);
+        below = linop_below<F32>(a, cv, tc, center, adamp, dl, rdop);
+      }
+      const unsigned stop = __ballot_sync(0xffffffffu, valid && below);
       const int last = stop ? base + __ffs(stop) - 1 : iwmax;
       if (valid && iw <= last) atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
       if (stop) break;
@@ -147,8 +183,13 @@ static __device__ __noinline__ void linop_finish_warp(const LinopArgs& a, int J,
       const int iw = nu - i;
       const bool valid = i <= 100 && iw >= 1;
       double cv = 0.0;
-      if (valid) cv = linop_cv(a, center, adamp, (wlvac - a.waveset[iw - 1]) / dopwave);
-      const unsigned stop = __ballot_sync(0xffffffffu, valid && cv < tc);
+      bool below = false;
+      if (valid) {
+        const double dl = wlvac - a.waveset[iw - 1];
+        cv = linop_cv<F32>(a, center, adamp, dl, rdop);
+        below = linop_below<F32>(a, cv, tc, center, adamp, dl, rdop);
+      }
+      const unsigned stop = __ballot_sync(0xffffffffu, valid && below);
       const unsigned inval = __ballot_sync(0xffffffffu, !valid);
       const int ilast = stop ? i0 + __ffs(stop) - 1 : 100;
       if (valid && i <= ilast) atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
@@ -164,6 +205,7 @@ static __device__ __noinline__ void linop_finish_warp(const LinopArgs& a, int J,
 // warp touch XLINES(J, IW) at consecutive J: one coalesced atomic per step.
 constexpr int kLinopLanePts = 4;
 
+template <bool F32>
 static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
   const int lane = threadIdx.x & 31;
   const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -213,21 +255,23 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
         }
       }
       if (!__any_sync(0xffffffffu, walk)) continue;
-      double adamp = 0.0, dopwave = 1.0;
+      double adamp = 0.0, rdop = 1.0;
       if (walk) {
         adamp = (L.gr + L.gs * a.xne[J - 1] + L.gw * a.txnxn[J - 1]) / dpn[J - 1];
-        dopwave = dpn[J - 1] * L.wlvac;
+        rdop = 1.0 / (dpn[J - 1] * L.wlvac);
         ++walked;
       }
       double* xlj = a.xl + (J - 1);
       bool rdone = !walk, bdone = !walk;
       int rnext = L.nu, bnext = 1;
+#pragma unroll 1
       for (int s = 0; s < kLinopLanePts && __any_sync(0xffffffffu, !rdone || !bdone); ++s) {
         if (!rdone) {
           const int iw = rnext;
-          const double cv = linop_cv(a, center, adamp, (a.waveset[iw - 1] - L.wlvac) / dopwave);
+          const double dl = a.waveset[iw - 1] - L.wlvac;
+          const double cv = linop_cv<F32>(a, center, adamp, dl, rdop);
           atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
-          if (cv < tc || iw >= iwmax) rdone = true;
+          if (linop_below<F32>(a, cv, tc, center, adamp, dl, rdop) || iw >= iwmax) rdone = true;
           else rnext = iw + 1;
         }
         if (!bdone) {
@@ -235,9 +279,10 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
           if (iw < 1) {
             bdone = true;
           } else {
-            const double cv = linop_cv(a, center, adamp, (L.wlvac - a.waveset[iw - 1]) / dopwave);
+            const double dl = L.wlvac - a.waveset[iw - 1];
+            const double cv = linop_cv<F32>(a, center, adamp, dl, rdop);
             atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
-            if (cv < tc || bnext >= 100) bdone = true;
+            if (linop_below<F32>(a, cv, tc, center, adamp, dl, rdop) || bnext >= 100) bdone = true;
             else bnext = bnext + 1;
           }
         }
@@ -250,13 +295,13 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
         const int Js = __shfl_sync(0xffffffffu, J, src);
         const double cs = __shfl_sync(0xffffffffu, center, src);
         const double as = __shfl_sync(0xffffffffu, adamp, src);
-        const double ds = __shfl_sync(0xffffffffu, dopwave, src);
+        const double ds = __shfl_sync(0xffffffffu, rdop, src);
         const double ts = __shfl_sync(0xffffffffu, tc, src);
         const int rn = __shfl_sync(0xffffffffu, rnext, src);
         const int bn = __shfl_sync(0xffffffffu, bnext, src);
         const bool rd = __shfl_sync(0xffffffffu, (int)rdone, src) != 0;
         const bool bd = __shfl_sync(0xffffffffu, (int)bdone, src) != 0;
-        linop_finish_warp(a, Js, cs, as, ds, L.wlvac, L.nu, ts, rn, rd, bn, bd, lane);
+        linop_finish_warp<F32>(a, Js, cs, as, ds, L.wlvac, L.nu, ts, rn, rd, bn, bd, lane);
       }
     }
   }
@@ -265,7 +310,8 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
   if (lane == 0 && walked && a.npairs) atomicAdd(a.npairs, walked);
 }
 
-static __global__ void __launch_bounds__(256) k_atlas_linop(LinopArgs a) { linop_body(a); }
+template <bool F32>
+static __global__ void __launch_bounds__(256, 3) k_atlas_linop(LinopArgs a) { linop_body<F32>(a); }
 
 // ---------------------------------------------------------------- RT pass
 __device__ __forceinline__ double expi3(double x) {

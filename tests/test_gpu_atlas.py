@@ -58,16 +58,25 @@ def oracle_linop(po, atlas_case, h_tables):
     return po.atlas_linop1(*h_tables, po.build_tablog(), c["lines"], atm, c["tabcont"], c["iw"], c["ws"])
 
 
-def test_linop_matches_oracle(gpu_ctx, tables, atlas_case, h_tables, oracle_linop):
+@pytest.mark.parametrize("prec,tol", [(_lib.PREC_FP64, 1e-9), (_lib.PREC_MIXED, 1e-6)])
+def test_linop_matches_oracle(gpu_ctx, tables, atlas_case, h_tables, oracle_linop, prec, tol):
+    """FP64: every element to 1e-9.  Mixed precision (FP32 profile values,
+    FP64 index, regime and stop decisions, FP64 sums): the same wing points
+    (identical nonzero pattern) and every element to 1e-6."""
     c = atlas_case
     A = atlas.Atlas(gpu_ctx, tables, *h_tables)
-    xl, used = A.linop1(c["lines"], 72, c["xnfdop"], c["dopple"], c["xne"], c["txnxn"], c["hckt"], c["tabcont"],
-                        c["iw"], c["ws"])
+    gpu_ctx.set_precision(prec)
+    try:
+        xl, used = A.linop1(c["lines"], 72, c["xnfdop"], c["dopple"], c["xne"], c["txnxn"], c["hckt"],
+                            c["tabcont"], c["iw"], c["ws"])
+    finally:
+        gpu_ctx.set_precision(_lib.PREC_MIXED)
     ref, ref_used = oracle_linop
     assert used == ref_used and used > 100
     assert np.count_nonzero(ref) > 1000
+    np.testing.assert_array_equal(xl != 0, ref != 0)
     scale = np.maximum(np.abs(ref), 1e-300)
-    assert np.max(np.abs(xl - ref) / scale) < 1e-9
+    assert np.max(np.abs(xl - ref) / scale) < tol
 
 
 def test_linop_empty_and_out_of_grid(gpu_ctx, tables, atlas_case, h_tables, po):
@@ -85,7 +94,7 @@ def test_linop_empty_and_out_of_grid(gpu_ctx, tables, atlas_case, h_tables, po):
     got, gu = A.linop1(ld, 72, c["xnfdop"], c["dopple"], c["xne"], c["txnxn"], c["hckt"], c["tabcont"], c["iw"],
                        c["ws"])
     assert gu == ru
-    np.testing.assert_allclose(got, ref, rtol=1e-9, atol=0)
+    np.testing.assert_allclose(got, ref, rtol=1e-6, atol=0)  # mixed precision (FP32 profile values)
 
 
 def test_rt_pass_matches_oracle(po, ops, gpu_ctx, tables, atlas_case, oracle_linop):
