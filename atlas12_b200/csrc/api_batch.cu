@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(256, 3) k_batch_linop(const LinopArgs* __restr
   linop_body<F32>(a);
 }
 
-__global__ void __launch_bounds__(kRtThreads, 3) k_batch_rt(const RtArgs* __restrict__ args, const BatchCtl* ctl) {
+__global__ void __launch_bounds__(kRtThreads, kRtMinBlocks) k_batch_rt(const RtArgs* __restrict__ args, const BatchCtl* ctl) {
   const int b = blockIdx.y;
   if (!running(ctl, b)) return;
   RtArgs a = args[b];

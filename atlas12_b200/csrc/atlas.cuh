@@ -370,21 +370,23 @@ struct RtWS {
   JoshWSFull f;
   double acont[kKwMax], sigmac[kKwMax], aline[kKwMax], stim[kKwMax];
   double dab[kKwMax];           // SCONT while JOSH runs (when given), then d(abtot)/d(rhox)
-  double U[kNx * (kNx + 1)];    // pivot rows of the 51x51 factorisation
+  alignas(16) double U[kNx * (kNx + 1)];  // pivot rows of the 51x51 factorisation (rows 16-byte aligned)
 };
 
 // One pair group (64 threads) per frequency, kRtGroups groups per CTA.  The
-// group's 51 matrix rows live in registers (pair scatter_solve), so the
-// shared-memory footprint is the depth vectors only.
+// group's 51 matrix rows live in registers (pair elimination), so the
+// shared-memory footprint is the depth vectors and the pivot rows.
+using RtG = PairG;
 constexpr int kRtGroups = 2;
-constexpr int kRtThreads = kRtGroups * PairG::N;
+constexpr int kRtThreads = kRtGroups * RtG::N;
+constexpr int kRtMinBlocks = 3;
 
 // shared memory: RHOX and a zero vector (SIGMAL) for the CTA, then the groups' workspaces
 __host__ __device__ inline size_t rt_smem_bytes() { return 2 * sizeof(double) * kKwMax + kRtGroups * sizeof(RtWS); }
 
 static __device__ __forceinline__ void rt_body(const RtArgs& a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int gid = threadIdx.x / PairG::N;
+  const int gid = threadIdx.x / RtG::N;
   double* rhox_s = reinterpret_cast<double*>(smem_raw);
   double* zero_s = rhox_s + kKwMax;
   RtWS& S = reinterpret_cast<RtWS*>(smem_raw + 2 * sizeof(double) * kKwMax)[gid];
@@ -393,8 +395,8 @@ static __device__ __forceinline__ void rt_body(const RtArgs& a) {
     zero_s[j] = 0.0;
   }
   __syncthreads();
-  PairG g(threadIdx.x % PairG::N, 1 + gid, S.w.red);
-  constexpr int C = (kKwMax + PairG::N - 1) / PairG::N;
+  RtG g(threadIdx.x % RtG::N, 1 + gid, S.w.red);
+  constexpr int C = (kKwMax + RtG::N - 1) / RtG::N;
   const JoshOps& ops = *a.ops;
   const int nr = a.nrhox;
   const int gw = blockIdx.x * kRtGroups + gid;  // partial-sum row of this group
@@ -411,7 +413,7 @@ static __device__ __forceinline__ void rt_body(const RtArgs& a) {
     const double freq = kClightNms / wave;
     const double rcowt = a.rcoset[nu - 1];
     const double f3 = powi(freq / 1.0e15, 3);
-    for (int j = g.r; j < nr; j += PairG::N) {
+    for (int j = g.r; j < nr; j += RtG::N) {
       const double ehvkt = exp(-freq * a.hkt[j]);
       const double stim = 1.0 - ehvkt;
       const double bnu = kBnuPrefac * f3 * ehvkt / stim;
@@ -428,9 +430,9 @@ static __device__ __forceinline__ void rt_body(const RtArgs& a) {
     if (a.sweeps && g.r == 0) a.sweeps[nu - 1] = sw;
     // negative floor (RUN_RT_PASS :3926-3937)
     bool neg = false;
-    for (int j = g.r; j < nr; j += PairG::N) neg |= (S.f.snu[j] < 0.0 || S.f.jnu[j] < 0.0 || S.f.hnu[j] < 0.0);
+    for (int j = g.r; j < nr; j += RtG::N) neg |= (S.f.snu[j] < 0.0 || S.f.jnu[j] < 0.0 || S.f.hnu[j] < 0.0);
     if (g.any(neg)) {
-      for (int j = g.r; j < nr; j += PairG::N) {
+      for (int j = g.r; j < nr; j += RtG::N) {
         S.f.jnu[j] = fmax(S.f.jnu[j], 1.0e-99);
         S.f.snu[j] = fmax(S.f.snu[j], 1.0e-99);
         S.f.hnu[j] = fmax(S.f.hnu[j], 1.0e-99);
@@ -441,7 +443,7 @@ static __device__ __forceinline__ void rt_body(const RtArgs& a) {
     // TCORR mode 2: d(abtot)/d(rhox)
     g_deriv(g, rhox_s, S.w.abtot, S.dab, nr);
     // TERM2 per depth (E3 diagonal of Lambda); D(NRHOX) repeats D(NRHOX-1)
-    for (int j = g.r; j < nr; j += PairG::N) {
+    for (int j = g.r; j < nr; j += RtG::N) {
       const int jd = j < nr - 1 ? j : nr - 2;
       double d = S.w.taunu[jd + 1] - S.w.taunu[jd];
       d = fmax(1.0e-10, d);
@@ -460,7 +462,7 @@ static __device__ __forceinline__ void rt_body(const RtArgs& a) {
     g.sync();
 #pragma unroll
     for (int c = 0; c < C; ++c) {
-      const int j = g.r + c * PairG::N;
+      const int j = g.r + c * RtG::N;
       if (j >= nr) break;
       const double ab = S.w.abtot[j], al = S.w.alpha[j], h = S.f.hnu[j];
       acc[1][c] += S.dab[j] / ab * h * rcowt;                 // RDABH
@@ -482,7 +484,7 @@ static __device__ __forceinline__ void rt_body(const RtArgs& a) {
   double* out = a.partial + (size_t)gw * (kAcc * a.kw + 1);
 #pragma unroll
   for (int c = 0; c < C; ++c) {
-    const int j = g.r + c * PairG::N;
+    const int j = g.r + c * RtG::N;
     if (j < nr) {
 #pragma unroll
       for (int q = 0; q < kAcc; ++q) out[q * a.kw + j] = acc[q][c];
@@ -491,7 +493,7 @@ static __device__ __forceinline__ void rt_body(const RtArgs& a) {
   if (g.r == 0) out[kAcc * a.kw] = pradk0;
 }
 
-static __global__ void __launch_bounds__(kRtThreads, 3) k_atlas_rt(RtArgs a) { rt_body(a); }
+static __global__ void __launch_bounds__(kRtThreads, kRtMinBlocks) k_atlas_rt(RtArgs a) { rt_body(a); }
 
 // fixed-order sum of the per-warp partials: out[kAcc*kw + 1].  A block owns
 // 32 consecutive sums (threadIdx.x) and splits the rows over 32 row groups

@@ -35,46 +35,54 @@ struct WarpG {
   __device__ __forceinline__ bool any(bool p) { return __any_sync(0xffffffffu, p); }
 };
 
-// Two warps on named barrier `bar`; red = 4 doubles of the group's shared
-// scratch (two slots per warp, alternated so one barrier per reduction
-// suffices: a slot is rewritten only after every thread has passed the
-// barrier of the reduction in between).
-struct PairG {
-  static constexpr int N = 64;
-  int r;  // 0..63
+// NW warps on named barrier `bar`; red = 2*NW doubles of the group's shared
+// scratch (one slot per warp and parity, alternated so one barrier per
+// reduction suffices: a slot is rewritten only after every thread has passed
+// the barrier of the reduction in between).  Warp partials are combined in
+// warp order, so the result does not depend on scheduling.
+template <int NW>
+struct MultiG {
+  static constexpr int N = 32 * NW;
+  int r;  // 0..N-1
   int bar;
   double* red;
   int par;
-  __device__ PairG(int rank, int barrier, double* scratch) : r(rank), bar(barrier), red(scratch), par(0) {}
+  __device__ MultiG(int rank, int barrier, double* scratch) : r(rank), bar(barrier), red(scratch), par(0) {}
   __device__ __forceinline__ void sync() const {
     asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(N) : "memory");
   }
   __device__ __forceinline__ double sum(double v) {
     v = warp_sum(v);
-    if ((r & 31) == 0) red[par * 2 + (r >> 5)] = v;
+    if ((r & 31) == 0) red[par * NW + (r >> 5)] = v;
     sync();
-    const double s = red[par * 2] + red[par * 2 + 1];
+    double s = red[par * NW];
+#pragma unroll
+    for (int w = 1; w < NW; ++w) s += red[par * NW + w];
     par ^= 1;
     return s;
   }
   __device__ __forceinline__ double max(double v) {
     v = warp_max(v);
-    if ((r & 31) == 0) red[par * 2 + (r >> 5)] = v;
+    if ((r & 31) == 0) red[par * NW + (r >> 5)] = v;
     sync();
-    const double s = fmax(red[par * 2], red[par * 2 + 1]);
+    double s = red[par * NW];
+#pragma unroll
+    for (int w = 1; w < NW; ++w) s = fmax(s, red[par * NW + w]);
     par ^= 1;
     return s;
   }
   __device__ __forceinline__ bool any(bool p) { return max(__any_sync(0xffffffffu, p) ? 1.0 : 0.0) > 0.0; }
 };
+using PairG = MultiG<2>;
 
 struct JoshWS {
   double xs[kNx], xsbar[kNx], xalpha[kNx], xw[kNx];
   double abtot[kKwMax], alpha[kKwMax], snubar[kKwMax], taunu[kKwMax];
   double t1[kKwMax], t2[kKwMax], t3[kKwMax];  // scratch (PARCOE a,b,c / terms)
-  double red[4];                              // group reductions (pair groups)
+  double red[8];                              // group reductions (multi-warp groups)
+  double piv[kNx];                            // pivots of the elimination without interchanges
   int lidx[kKwMax + 4];                       // MAP1 bracket indices
-  unsigned pk[2][3];                          // pivot key exchange between the pair's warps
+  unsigned pk[4][3];                          // pivot key exchange between a group's warps
 };
 
 // Full-solution extras for IFSURF = 0 (ATLAS)
@@ -403,6 +411,51 @@ __device__ inline void scatter_solve(WarpG& g, const JoshOps& ops, JoshWS& ws, d
   w_solvit(A, ws.xs, g.r);
 }
 
+// Pivot-row traffic in 16-byte words: the row owner stores [1/pivot, a[1..51]]
+// and every pending row reads it back, as 26 double2 (U rows are 16-byte
+// aligned: 52 doubles per row on a 16-byte aligned base).
+__device__ __forceinline__ void store_pivot_row(double* ur, double rpiv, const double (&a)[kNx + 1]) {
+  double2* u2 = reinterpret_cast<double2*>(ur);
+  u2[0] = make_double2(rpiv, a[1]);
+#pragma unroll
+  for (int q = 1; q < (kNx + 1) / 2; ++q) u2[q] = make_double2(a[2 * q], a[2 * q + 1]);
+}
+
+// a[t-1] = a[t] - l * ur[t] (t = 1..51), a[51] = 0, with l = a[0] * ur[0]
+__device__ __forceinline__ void eliminate_shift(double (&a)[kNx + 1], const double* ur) {
+  const double2* u2 = reinterpret_cast<const double2*>(ur);
+  const double2 u0 = u2[0];
+  const double l = a[0] * u0.x;
+  a[0] = a[1] - l * u0.y;
+#pragma unroll
+  for (int q = 1; q < (kNx + 1) / 2; ++q) {
+    const double2 u = u2[q];
+    a[2 * q - 1] = a[2 * q] - l * u.x;
+    a[2 * q] = a[2 * q + 1] - l * u.y;
+  }
+  a[kNx] = 0.0;
+}
+
+// Back substitution from the stored pivot rows U (row k: U[k][0] = 1/pivot,
+// U[k][t] = column k+t, the rhs at t = 51-k) by the group's first warp: lane
+// q holds positions q and q+32, X(j) = B(j) * (1/pivot) is passed by shuffle
+// and B(k) -= A(k,j) X(j) for k < j, in SOLVIT's order.  XS receives X.
+__device__ __forceinline__ void u_back_substitute(int r, const double* U, double* xs) {
+  constexpr int n = kNx, W = kNx + 1;
+  if (r >= 32) return;
+  const int k0 = r, k1 = r + 32;
+  double b0 = U[k0 * W + (W - 1 - k0)];
+  double b1 = k1 < n ? U[k1 * W + (W - 1 - k1)] : 0.0;
+  for (int j = n - 1; j >= 0; --j) {
+    const int src = j & 31;
+    double x = (j < 32 ? b0 : b1) * U[j * W];
+    x = __shfl_sync(0xffffffffu, x, src);
+    if (r == src) xs[j] = x;
+    if (k0 < j) b0 = b0 - U[k0 * W + (j - k0)] * x;
+    if (k1 < j) b1 = b1 - U[k1 * W + (j - k1)] * x;
+  }
+}
+
 // The same system by a pair group, thread r < 51 holding row r of
 // [AMAT | rhs] in registers.  The elimination follows SOLVIT's arithmetic:
 // the pivot of step i is the first maximum |A(k,i)| over the rows at
@@ -469,20 +522,13 @@ static __device__ __forceinline__ void scatter_solve(PairG& g, const JoshOps& op
     if (me) {
       double pv = a[0];
       if (fabs(pv) < kPivotTol) pv = copysign(kPivotTol, pv);
-      ur[0] = 1.0 / pv;
-#pragma unroll
-      for (int t = 1; t < W; ++t) ur[t] = a[t];
+      store_pivot_row(ur, 1.0 / pv, a);
       pos = i;
       done = true;
     }
     g.sync();
     // (d, e) multiplier and trailing update of the pending rows, shifted left
-    if (!done) {
-      const double l = a[0] * ur[0];
-#pragma unroll
-      for (int t = 1; t < W; ++t) a[t - 1] = a[t] - l * ur[t];
-      a[W - 1] = 0.0;
-    }
+    if (!done) eliminate_shift(a, ur);
   }
   // the last pending row takes position n-1: column n-1 in a[0], rhs in a[1]
   if (!done) {
@@ -493,17 +539,66 @@ static __device__ __forceinline__ void scatter_solve(PairG& g, const JoshOps& op
     U[(n - 1) * W + 1] = a[1];
   }
   g.sync();
-  // back substitution: X(j) = B(j) * (1/pivot), then B(k) -= A(k,j) X(j), k < j
-  double b = own ? U[pos * W + (W - 1 - pos)] : 0.0;
-  for (int j = n - 1; j >= 0; --j) {
-    if (own && pos == j) {
-      b = b * U[j * W];
-      ws.xs[j] = b;
+  u_back_substitute(g.r, U, ws.xs);
+  g.sync();
+}
+
+// Elimination without interchanges, checked: thread r < 51 holds row r,
+// which becomes the pivot row at step r.  At step i every pending row
+// compares its |A(k,i)| with the pivot |A(i,i)|; SOLVIT's first-maximum rule
+// would pick another row only if some |A(k,i)| is strictly larger.  Returns
+// false (the caller then redoes the system with interchanges) if that ever
+// happened; otherwise the operations were exactly SOLVIT's, in its order.
+// (For these systems it does not happen: AMAT is column diagonally dominant
+// because the columns of COEFJ sum to at most 1 and XALPHA < 1.)
+static __device__ __forceinline__ bool scatter_solve_nopivot(PairG& g, const JoshOps& ops, JoshWS& ws, double* U) {
+  constexpr int n = kNx, W = kNx + 1;
+  const bool own = g.r < n;
+  double a[W];
+  {
+    const int l = own ? g.r : 0;
+    const double xa = ws.xalpha[l];
+#pragma unroll
+    for (int m = 0; m < n; ++m) {
+      double v = -xa * ops.coefj[m * kNx + l];
+      if (l == m) v = v + 1.0;
+      a[m] = v;
+    }
+    a[n] = (1.0 - xa) * ws.xsbar[l];
+  }
+  bool swap = false;
+  for (int i = 0; i < n - 1; ++i) {
+    double* ur = U + i * W;
+    if (g.r == i) {
+      ws.piv[i] = a[0];
+      double pv = a[0];
+      if (fabs(pv) < kPivotTol) pv = copysign(kPivotTol, pv);
+      store_pivot_row(ur, 1.0 / pv, a);
     }
     g.sync();
-    if (own && pos < j) b = b - U[pos * W + (j - pos)] * ws.xs[j];
+    if (own && g.r > i) {
+      swap |= fabs(a[0]) > fabs(ws.piv[i]);
+      eliminate_shift(a, ur);
+    }
   }
+  if (g.r == n - 1) {
+    double v = a[0];
+    if (fabs(v) < kPivotTol) v = copysign(kPivotTol, v);
+    U[(n - 1) * W] = 1.0 / v;
+    U[(n - 1) * W + 1] = a[1];
+  }
+  if (g.any(swap)) return false;
+  u_back_substitute(g.r, U, ws.xs);
   g.sync();
+  return true;
+}
+
+
+__device__ __forceinline__ void solve_scatter(PairG& g, const JoshOps& ops, JoshWS& ws, double* U) {
+  if (!scatter_solve_nopivot(g, ops, ws, U)) scatter_solve(g, ops, ws, U);
+}
+__device__ __forceinline__ void solve_scatter(WarpG& g, const JoshOps& ops, JoshWS& ws, double* A) {
+  scatter_solve(g, ops, ws, A);
 }
 
 // ---------------------------------------------------------------- JOSH
@@ -549,7 +644,7 @@ __device__ inline int g_josh(G& g, const JoshOps& ops, const double* rhox, int n
       for (int l = g.r; l < kNx; l += G::N) ws.xs[l] = fmax(ws.xsbar[l], 1.0e-37);
       g.sync();
     } else {
-      scatter_solve(g, ops, ws, A);
+      solve_scatter(g, ops, ws, A);
       for (int l = g.r; l < kNx; l += G::N) ws.xs[l] = fmax(ws.xs[l], 1.0e-37);
       g.sync();
     }

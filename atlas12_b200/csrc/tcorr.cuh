@@ -470,6 +470,7 @@ __device__ inline double b_atlas_finish(ModelState* gms, double* gacc, int kw, i
     WarpG w(tid);
     const int L = tid;
     double maxerr = 0.0;
+    bool nonfinite = false;
     // ROSS(3)
     for (int j = L; j < n; j += 32) s.abross[j] = FOUR_SIGMA_OVER_PI * powi(s.t[j], 3) / abross[j];
     w.sync();
@@ -516,8 +517,11 @@ __device__ inline double b_atlas_finish(ModelState* gms, double* gacc, int kw, i
       s.dtflux[j] = -dtau[j] * dtdrhx[j] / fmax(s.abross[j], 1.0e-30);
       s.flxerr[j] = (flxrad[j] + 0.0 - FLUX) / FLUX * 100.0;
       maxerr = fmax(maxerr, fabs(s.flxerr[j]));
+      nonfinite |= !(fabs(s.flxerr[j]) <= 1.0e308);
     }
     maxerr = w.max(maxerr);
+    // fmax drops NaN: a non-finite FLXERR anywhere makes the metric NaN
+    if (__any_sync(0xffffffffu, nonfinite)) maxerr = __longlong_as_double(0x7ff8000000000000ll);
     w.sync();
     g_deriv(w, s.tauros, s.flxerr, flxdrv, n);
     for (int j = L; j < n; j += 32) {

@@ -152,82 +152,98 @@ def grey_start(teff, logg, mh, nrhox=NRHOX):
     return surrogate.grey_model(teff, logg, nrhox=nrhox, ross=_ross_cache[key])
 
 
-def run_models(model, params, starts=None, max_iter=80, tol=0.1):
-    """Iterate `model` (an AtlasModel on the shared line list and grid) for each
-    parameter set from its grey start (or starts[i]).  Returns per-model
-    iterations, final max |FLXERR| and the final T, P, XNE [n, 72]."""
+def run_models(batch, params, starts=None, max_iter=80, tol=0.1):
+    """Iterate every parameter set ([n, 4]: Teff, log g, [M/H], vturb) on an
+    AtlasBatch (shared line list and grid) from its grey start (or
+    starts[i]).  Returns per-model iterations, final max |FLXERR| (inf when
+    the model did not converge) and the final T, P, XNE [n, 72]."""
     n = len(params)
-    iters = np.zeros(n, np.int32)
-    err = np.zeros(n)
-    T, P, NE = (np.zeros((n, model.nrhox)) for _ in range(3))
-    for i, (teff, logg, mh, vt) in enumerate(params):
-        s = starts[i] if starts is not None else grey_start(teff, logg, mh, model.nrhox)
-        model.set_params(teff, logg, vt, mh)
-        model.set_structure(s["t"], s["p"], s["rhox"])
-        try:
-            k, hist = model.iterate(max_iter=max_iter, tol_percent=tol, graph=True)
-            st = model.structure()
-            iters[i], err[i] = k, hist[-1] if k else np.inf
-            T[i], P[i], NE[i] = st["t"], st["p"], st["xne"]
-        except _lib.AtlasGPUError:
-            iters[i], err[i] = max_iter, np.inf
+    if starts is None:
+        starts = [grey_start(teff, logg, mh, batch.nrhox) for teff, logg, mh, _ in params]
+    res = batch.run_queue(params, starts, max_iter=max_iter, tol_percent=tol)
+    iters = np.array([r["iters"] for r in res], np.int32)
+    err = np.array([r["maxerr"] if r["status"] == _lib.SLOT_CONVERGED else np.inf for r in res])
+    T, P, NE = (np.array([r[k] for r in res]) for k in ("t", "p", "xne"))
     return iters, err, T, P, NE
 
 
-def _workload_model(ctx, tables, numnu=30000, nlines=500000, seed=2):
-    """An AtlasModel on the C2-style line list and grid (shared by every model)."""
+def workload_batch(ctx, tables, nslots=64, numnu=30000, nlines=500000, seed=2):
+    """An AtlasBatch on the 30,000-frequency, 500,000-line opacity-sampling
+    workload (every model shares the line list and the grid)."""
     from . import atlas, synthetic
     ws, rc = synthetic.geometric_waveset(9.0, 160000.0, numnu)
     lines = synthetic.atlas_lines(nlines, ws[2], ws[-3], seed=seed)
-    return atlas.AtlasModel(ctx, tables, linedata=lines, waveset=ws, rcoset=rc, start=grey_start(5777.0, 4.44, 0.0))
+    return atlas.AtlasBatch(ctx, tables, nslots=nslots, linedata=lines, waveset=ws, rcoset=rc)
+
+
+def compare_starts(batch, ws, params, max_iter=80, tol=0.1):
+    """Iterations to max |FLXERR| <= tol from the grey start and from the
+    network's start, per parameter set (the unmodified iteration judges both).
+    Returns dict of arrays: iters/err for 'grey' and 'mlp'."""
+    out = {}
+    for name, starts in (("grey", None), ("mlp", [ws.start(*p) for p in params])):
+        it, er, _, _, _ = run_models(batch, params, starts, max_iter=max_iter, tol=tol)
+        out[name] = dict(iters=it, err=er)
+    return out
 
 
 def main(argv=None):
-    """generate: converged models over the parameter box; train: fit the network.
+    """generate: converged models over the parameter box; train: fit the
+    network; evaluate: held-out iterations from the grey and the learned start.
 
     python -m atlas12_b200.warmstart generate --n 2000 --seed 11 --out models.npz
     python -m atlas12_b200.warmstart train --data models.npz --out warmstart.npz
+    python -m atlas12_b200.warmstart evaluate --weights warmstart.npz --n 200 --seed 12 --out heldout.npz
     """
     import argparse
     import os
     import time
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("cmd", choices=["generate", "train"])
+    ap.add_argument("cmd", choices=["generate", "train", "evaluate"])
     ap.add_argument("--n", type=int, default=2000)
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--max-iter", type=int, default=80)
+    ap.add_argument("--slots", type=int, default=64)
     ap.add_argument("--data", default=None)
+    ap.add_argument("--weights", default=None)
     ap.add_argument("--out", required=True)
     ap.add_argument("--epochs", type=int, default=3000)
-    ap.add_argument("--budget-s", type=float, default=1e9, help="stop generating after this many seconds")
+    ap.add_argument("--lr", type=float, default=1e-3)
     a = ap.parse_args(argv)
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     t = np.load(os.path.join(root, "tests", "golden", "reference_tables.npz"))
     tables = {k: t[k] for k in t.files}
     ctx = _lib.Context(0, _lib.PREC_MIXED)
+    t0 = time.time()
     if a.cmd == "generate":
-        model = _workload_model(ctx, tables)
+        batch = workload_batch(ctx, tables, a.slots)
         params = sample_params(a.n, a.seed)
-        t0 = time.time()
-        out = dict(params=[], iters=[], err=[], t=[], p=[], xne=[])
-        for i in range(0, a.n, 50):
-            if time.time() - t0 > a.budget_s:
-                break
-            it, er, T, P, NE = run_models(model, params[i:i + 50], max_iter=a.max_iter)
-            for k, v in zip(("params", "iters", "err", "t", "p", "xne"), (params[i:i + 50], it, er, T, P, NE)):
-                out[k].append(v)
-            done = sum(len(x) for x in out["iters"])
-            conv = sum(int(np.sum(e <= 0.1)) for e in out["err"])
-            print(f"{done} models, {conv} converged, {time.time() - t0:.0f} s", flush=True)
-        np.savez(a.out, **{k: np.concatenate(v) for k, v in out.items()})
-        model.close()
-    else:
+        it, er, T, P, NE = run_models(batch, params, max_iter=a.max_iter)
+        np.savez(a.out, params=params, iters=it, err=er, t=T, p=P, xne=NE)
+        conv = np.isfinite(er)
+        print(f"{a.n} models, {int(conv.sum())} converged (mean {it[conv].mean():.1f} iterations), "
+              f"{time.time() - t0:.0f} s", flush=True)
+        batch.close()
+    elif a.cmd == "train":
         d = np.load(a.data)
-        ok = d["err"] <= 0.1
-        ws, hist = WarmStart.fit(ctx, d["params"][ok], d["t"][ok], d["p"][ok], d["xne"][ok], epochs=a.epochs)
+        ok = np.isfinite(d["err"]) & (d["err"] <= 0.1)
+        ws, hist = WarmStart.fit(ctx, d["params"][ok], d["t"][ok], d["p"][ok], d["xne"][ok], epochs=a.epochs,
+                                 lr=a.lr)
         ws.save(a.out)
-        print(f"trained on {int(ok.sum())} converged models; loss {hist[0]:.4g} -> {hist[-1]:.4g}", flush=True)
+        print(f"trained on {int(ok.sum())} converged models; loss {hist[0]:.4g} -> {hist[-1]:.4g}, "
+              f"{time.time() - t0:.0f} s", flush=True)
+    else:
+        ws = WarmStart.load(a.weights, ctx)
+        batch = workload_batch(ctx, tables, a.slots)
+        params = sample_params(a.n, a.seed)
+        r = compare_starts(batch, ws, params, max_iter=a.max_iter)
+        np.savez(a.out, params=params, **{f"{k}_{q}": r[k][q] for k in r for q in r[k]})
+        for k in r:
+            c = np.isfinite(r[k]["err"])
+            print(f"{k}: {int(c.sum())}/{a.n} converged, mean iterations {r[k]['iters'][c].mean():.2f}, "
+                  f"total iterations {int(r[k]['iters'].sum())}", flush=True)
+        batch.close()
     ctx.close()
 
 
