@@ -43,6 +43,11 @@ class Accum(ctypes.Structure):
 LTE_LINE = np.dtype([("nbuff", "<i4"), ("cgf", "<f4"), ("nelion", "<i4"), ("elo", "<f4"),
                      ("gamrf", "<f4"), ("gamsf", "<f4"), ("gamwf", "<f4"), ("code", "<f4")])
 assert LTE_LINE.itemsize == 32
+# unit-19 NLTE / complex-profile record (atlasgpu_nlte_line), 64 bytes
+NLTE_LINE = np.dtype([("wlvac", "<f8"), ("elo", "<f4"), ("gf", "<f4"), ("nblo", "<i4"), ("nbup", "<i4"),
+                      ("nelion", "<i4"), ("itype", "<i4"), ("ncon", "<i4"), ("nelionx", "<i4"), ("gammar", "<f4"),
+                      ("gammas", "<f4"), ("gammaw", "<f4"), ("nbuff", "<i4"), ("lim", "<i4"), ("pad", "<i4")])
+assert NLTE_LINE.itemsize == 64
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -75,6 +80,10 @@ SIGNATURES = {
     "atlasgpu_atlas_tabvoigt": (_I, [_D, _I, _P, _P, _I, _P, _P, _P]),
     "atlasgpu_atlas_linop": (_I, [_P, _P, _I64, _I, _I, _P, _P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P,
                                   ctypes.POINTER(_I64)]),
+    "atlasgpu_synthe_nlte_opacity": (_I, [_P, _P, _I64, _I, _I, _D, _D, _D, _D, _P, _P, _P, _I, _P, _P, _P, _P,
+                                          _P]),
+    "atlasgpu_atlas_xlinop": (_I, [_P, _P, _I64, _I, _I, _P, _P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P,
+                                   ctypes.POINTER(_I64)]),
     "atlasgpu_atlas_rt_pass": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _D,
                                     ctypes.POINTER(Accum), _P]),
     "atlasgpu_atlas_finish": (_I, [_P, ctypes.c_void_p, ctypes.POINTER(Accum), ctypes.POINTER(_D)]),
@@ -84,6 +93,10 @@ SIGNATURES = {
     "atlasgpu_model_set_structure": (_I, [_P, _P, _P, _P, _P]),
     "atlasgpu_model_destroy": (_I, [_P, _P]),
     "atlasgpu_model_set_params": (_I, [_P, _P, _D, _D, _D, _D]),
+    "atlasgpu_model_set_shard": (_I, [_P, _P, _I, _I]),
+    "atlasgpu_model_set_sums_buffer": (_I, [_P, _P, _P]),
+    "atlasgpu_model_iterate_begin": (_I, [_P, _P]),
+    "atlasgpu_model_iterate_end": (_I, [_P, _P, ctypes.POINTER(_D)]),
     "atlasgpu_surrogate_eval": (_I, [_P, _I, _P, _P, _D, _I, _P, _P, _P, _P, _P]),
     "atlasgpu_fp64_peak_tflops": (_D, [_P]),
     "atlasgpu_mlp_create": (_I, [_P, _I, _I, _I, _I, ctypes.c_uint64, ctypes.POINTER(_P)]),

@@ -84,6 +84,27 @@ class Atlas:
                       ctypes.byref(used))
         return out, used.value
 
+    def xlinop(self, records, nrhox, xnfdop, dopple, xne, txnxn, hckt, tabcont, iwt, waveset, contx, xlines=None):
+        """XLINOP's normal-line branch on unit-19 records (NLTE_LINE array,
+        sorted by wavelength), added into a copy of xlines [numnu, kw] (zeros
+        when None).  contx: CONTX(25,16) as [16, 25].  Returns (xlines,
+        number of records of the types this branch does not handle)."""
+        rec = np.ascontiguousarray(records, _lib.NLTE_LINE)
+        xd = np.ascontiguousarray(xnfdop, np.float64)
+        dp = np.ascontiguousarray(dopple, np.float64)
+        nspec, kw = xd.shape
+        vec = [np.ascontiguousarray(v, np.float64) for v in (xne, txnxn, hckt)]
+        tc = np.ascontiguousarray(tabcont, np.float64)
+        iw = np.ascontiguousarray(iwt, np.int32)
+        ws = np.ascontiguousarray(waveset, np.float64)
+        cx = np.ascontiguousarray(contx, np.float64)
+        out = np.zeros((ws.size, kw)) if xlines is None else np.array(xlines, np.float64, copy=True, order="C")
+        other = ctypes.c_int64(0)
+        self.ctx.call("atlasgpu_atlas_xlinop", ptr(rec), rec.shape[0], int(nrhox), kw, ptr(xd), ptr(dp), nspec,
+                      *[ptr(v) for v in vec], ptr(tc), ptr(iw), iw.size - 1, ptr(ws), ws.size, ptr(cx), ptr(out),
+                      ctypes.byref(other))
+        return out, other.value
+
     def rt_pass(self, waveset, rcoset, acont, sigmac, xlines, rhox, t, hkt, teff, scont=None):
         ws, rc = (np.ascontiguousarray(v, np.float64) for v in (waveset, rcoset))
         ac, sg, xl = (np.ascontiguousarray(v, np.float64) for v in (acont, sigmac, xlines))
@@ -203,6 +224,25 @@ class AtlasModel:
         arrs = [np.ascontiguousarray(x, np.float64) for x in (t, p, rhox)]
         self.ctx.call("atlasgpu_model_set_structure", self._h, *[ptr(a) for a in arrs])
 
+    def set_shard(self, nu_first, nu_last):
+        """Restrict LINOP1 and the RT pass to frequencies nu_first..nu_last (1-based, inclusive)."""
+        self.ctx.call("atlasgpu_model_set_shard", self._h, int(nu_first), int(nu_last))
+
+    def set_sums_buffer(self, d_sums):
+        """Frequency sums [8*nrhox + 1] in a caller-owned device buffer (torch tensor; None: internal)."""
+        self._sums_ref = d_sums
+        self.ctx.call("atlasgpu_model_set_sums_buffer", self._h, ptr(d_sums))
+
+    def iterate_begin(self):
+        """Enqueue one iteration up to the (shard's) frequency sums."""
+        self.ctx.call("atlasgpu_model_iterate_begin", self._h)
+
+    def iterate_end(self):
+        """Enqueue the finish from the sums, wait; returns max |FLXERR| (percent)."""
+        e = ctypes.c_double(0.0)
+        self.ctx.call("atlasgpu_model_iterate_end", self._h, ctypes.byref(e))
+        return e.value
+
     def close(self):
         if self._h:
             _lib.lib().atlasgpu_model_destroy(self.ctx.handle, self._h)
@@ -288,20 +328,33 @@ class AtlasBatch:
             out["hist"] = hist[:iters]
         return out
 
-    def run_queue(self, params, starts, max_iter=60, tol_percent=0.1, poll_every=2, keep=True):
+    def run_queue(self, params, starts, max_iter=60, tol_percent=0.1, poll_every=2, keep=True, fallback=None,
+                  first_max_iter=None):
         """Iterate every model of `params` ([n, 4]: Teff, log g, [M/H], vturb)
         from starts[i] (dict t, p, rhox), keeping all slots busy: a slot that
-        finishes is read back and loaded with the next model.  Returns a
-        list of dicts (status, iters, maxerr, and the structure when keep)."""
+        finishes is read back and loaded with the next model.  With
+        `fallback` (a second list of starts, e.g. the grey models), a model
+        whose first attempt ends without converging (non-finite, or capped
+        at first_max_iter iterations) is run again from fallback[i] with
+        max_iter.  Returns a list of dicts (status, iters = iterations of
+        all attempts, maxerr, attempts, and the structure when keep)."""
         n = len(params)
         res = [None] * n
+        spent = [0] * n
         slot_of = [-1] * self.nslots
-        nxt = 0
+        attempt = [0] * self.nslots
+        queue = [(i, 0) for i in range(n)]  # (model, attempt)
+        cap0 = max_iter if (fallback is None or first_max_iter is None) else first_max_iter
+
+        def load(s, i, k):
+            teff, logg, mh, vt = params[i]
+            st = starts[i] if k == 0 else fallback[i]
+            self.load(s, teff, logg, vt, mh, st, cap0 if k == 0 else max_iter, tol_percent)
+            slot_of[s] = i
+            attempt[s] = k
+
         for s in range(min(self.nslots, n)):
-            teff, logg, mh, vt = params[nxt]
-            self.load(s, teff, logg, vt, mh, starts[nxt], max_iter, tol_percent)
-            slot_of[s] = nxt
-            nxt += 1
+            load(s, *queue.pop(0))
         while any(k >= 0 for k in slot_of):
             self.step(poll_every)
             st, it, er, _ = self.poll()
@@ -309,16 +362,17 @@ class AtlasBatch:
                 i = slot_of[s]
                 if i < 0 or st[s] == _lib.SLOT_RUNNING:
                     continue
-                r = {"status": int(st[s]), "iters": int(it[s]), "maxerr": float(er[s])}
-                if keep:
-                    r.update(self.structure(s, int(it[s])))
-                res[i] = r
+                spent[i] += int(it[s])
                 slot_of[s] = -1
-                if nxt < n:
-                    teff, logg, mh, vt = params[nxt]
-                    self.load(s, teff, logg, vt, mh, starts[nxt], max_iter, tol_percent)
-                    slot_of[s] = nxt
-                    nxt += 1
+                if st[s] != _lib.SLOT_CONVERGED and fallback is not None and attempt[s] == 0:
+                    queue.insert(0, (i, 1))
+                else:
+                    r = {"status": int(st[s]), "iters": spent[i], "maxerr": float(er[s]), "attempts": attempt[s] + 1}
+                    if keep:
+                        r.update(self.structure(s, int(it[s])))
+                    res[i] = r
+                if queue:
+                    load(s, *queue.pop(0))
         return res
 
     def close(self):

@@ -222,6 +222,83 @@ int atlasgpu_atlas_linop(atlasgpu_ctx* ctx, const int32_t* linedata, int64_t n, 
   return 0;
 }
 
+int atlasgpu_atlas_xlinop(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* recs, int64_t n, int nrhox, int kw,
+                          const double* xnfdop, const double* dopple, int nspec, const double* xne,
+                          const double* txnxn, const double* hckt, const double* tabcont,
+                          const int32_t* iwavetab, int nwave, const double* waveset, int numnu,
+                          const double* contx, double* xlines_inout, int64_t* n_other) {
+  if (!ctx || n < 0 || (n > 0 && !recs) || nrhox < 8 || kw < nrhox || kw > kKwMax || nspec < 1 || !xnfdop ||
+      !dopple || !xne || !txnxn || !hckt || !tabcont || !iwavetab || nwave < 1 || !waveset || numnu < 2 ||
+      !contx || !xlines_inout)
+    return fail(ctx, ATLASGPU_EINVAL, "atlas_xlinop: bad argument");
+  if (ctx->bufs.find("tab_h0") == ctx->bufs.end())
+    return fail(ctx, ATLASGPU_ESTATE, "atlas_xlinop: Voigt tables not set");
+  for (int i = 1; i < numnu; ++i)
+    if (!(waveset[i] > waveset[i - 1])) return fail(ctx, ATLASGPU_EINVAL, "WAVESET not increasing");
+  int64_t other = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (i > 0 && recs[i].wlvac < recs[i - 1].wlvac)
+      return fail(ctx, ATLASGPU_EINVAL, "atlas_xlinop: records not sorted by wavelength at %lld", (long long)i);
+    const int t = recs[i].itype, nc = recs[i].ncon > 10 ? 0 : recs[i].ncon;
+    if ((t == 0 || t == 3) && nc > 0 && (recs[i].nelionx < 1 || recs[i].nelionx > 16))
+      return fail(ctx, ATLASGPU_EINVAL, "atlas_xlinop: NELIONX %d outside CONTX at record %lld", recs[i].nelionx,
+                  (long long)i);
+    other += (t != 0 && t != 2 && t != 3);
+  }
+  if (n_other) *n_other = other;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  atlasgpu_nlte_line* d_rec;
+  int32_t* d_iw;
+  double *d_xd, *d_dp, *d_xne, *d_tx, *d_hc, *d_tc, *d_ws, *d_xl, *d_cx, *d_lc, *d_em;
+  AtlasLine* d_lines;
+  int r;
+  const size_t nd = (size_t)nspec * kw;
+  const int64_t nn = std::max<int64_t>(n, 1);
+  if ((r = bufT(ctx, "xl_rec", (size_t)nn, &d_rec)) || (r = bufT(ctx, "al_iw", nwave + 1, &d_iw)) ||
+      (r = bufT(ctx, "al_xd", nd, &d_xd)) || (r = bufT(ctx, "al_dp", nd, &d_dp)) ||
+      (r = bufT(ctx, "al_xne", kw, &d_xne)) || (r = bufT(ctx, "al_tx", kw, &d_tx)) ||
+      (r = bufT(ctx, "al_hc", kw, &d_hc)) || (r = bufT(ctx, "al_tc", (size_t)(nwave + 1) * kw, &d_tc)) ||
+      (r = bufT(ctx, "al_ws", numnu, &d_ws)) || (r = bufT(ctx, "al_xl", (size_t)kw * numnu, &d_xl)) ||
+      (r = bufT(ctx, "xl_lines", (size_t)nn, &d_lines)) || (r = bufT(ctx, "xl_contx", 25 * 16, &d_cx)) ||
+      (r = bufT(ctx, "xl_lcontx", (size_t)nn, &d_lc)) || (r = bufT(ctx, "xl_emerge", kw, &d_em)))
+    return r;
+  // EMERGE(J) = RYDBERG_INF / NMERGE**2, NMERGE = NSTARK = 1600 / XNE(J)**(2/15) (:19964-19977)
+  std::vector<double> em(kw, 0.0);
+  for (int j = 0; j < nrhox; ++j) {
+    const double nmerge = 1600.0 / pow(xne[j], 2.0 / 15.0);
+    em[j] = 109737.31568157 / (nmerge * nmerge);
+  }
+  if (n > 0) CK(cudaMemcpyAsync(d_rec, recs, n * sizeof(atlasgpu_nlte_line), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_iw, iwavetab, (nwave + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_xd, xnfdop, nd * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_dp, dopple, nd * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_xne, xne, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_tx, txnxn, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_hc, hckt, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_tc, tabcont, (size_t)(nwave + 1) * kw * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_ws, waveset, numnu * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_xl, xlines_inout, (size_t)kw * numnu * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_cx, contx, 25 * 16 * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_em, em.data(), kw * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (n > 0) {
+    XlinopPrepArgs pa{d_rec, n, d_ws, numnu, d_iw, nwave, nspec, d_cx, d_lines, d_lc};
+    k_xlinop_prep<<<grid_for(ctx, n, 256, 16), 256, 0, s>>>(pa);
+    CKL(ctx);
+    LinopArgs a{d_lines, n, nrhox, kw, nspec, numnu, d_xd, d_dp, d_xne, d_tx, d_hc, d_tc, d_ws,
+                (const double*)ctx->bufs["tab_h0"].first, (const double*)ctx->bufs["tab_h1"].first,
+                (const double*)ctx->bufs["tab_h2"].first, (const float4*)ctx->bufs["tab_hf"].first, d_xl, nullptr,
+                nullptr, 1, 0, 2000, 0.5642, d_lc, d_em};
+    Timer tm(ctx, "atlas_xlinop");
+    if (ctx->precision == ATLASGPU_PREC_MIXED) k_atlas_linop<true><<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
+    else k_atlas_linop<false><<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
+    CKL(ctx);
+  }
+  CK(cudaMemcpyAsync(xlines_inout, d_xl, (size_t)kw * numnu * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
 int atlasgpu_atlas_rt_pass(atlasgpu_ctx* ctx, int numnu, const double* waveset, const double* rcoset,
                            const double* acont, const double* sigmac, const double* scont, int kw,
                            const double* xlines, int nrhox, const double* rhox, const double* t,

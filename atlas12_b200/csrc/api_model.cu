@@ -38,6 +38,8 @@ struct atlasgpu_model {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   int graph_precision = -1;  // precision the captured graph was built with
+  int nu_first = 1, nu_last = 0;  // frequency shard (1-based, inclusive; 0 = NUMNU)
+  double* ext_sums = nullptr;     // caller-owned device buffer for the frequency sums (or null)
   bool kapcont_done = false;
 };
 
@@ -98,9 +100,23 @@ __global__ void k_surrogate_eval(int nrhox, const double* t, const double* p, do
   }
 }
 
-// One iteration on the context stream.  With timed = true (never while a
-// graph is being captured) each launch is bracketed by CUDA events.
-int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
+// RT launch shape for the model's frequency shard: enough pair groups to fill
+// every SM several times, frequencies contiguous per group
+void rt_shape(atlasgpu_ctx* ctx, atlasgpu_model* m) {
+  const int last = m->nu_last > 0 ? m->nu_last : m->numnu;
+  const int len = last - m->nu_first + 1;
+  const int target = ctx->nsm * 3 * kRtGroups * 4;
+  m->nu_per_group = std::max(1, (len + target - 1) / target);
+  const int ng = (len + m->nu_per_group - 1) / m->nu_per_group;
+  m->blocks_rt = (ng + kRtGroups - 1) / kRtGroups;
+}
+
+// The first part of one iteration on the context stream, up to the reduced
+// frequency sums (EOS, KAPCONT on the first iteration, LINOP1, KAPP, the RT
+// pass over the model's shard, the fixed-order reduction).  With timed =
+// true (never while a graph is being captured) each launch is bracketed by
+// CUDA events.
+int enqueue_begin(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
   cudaStream_t s = ctx->stream;
   const bool was = ctx->timing;
   ctx->timing = was && timed;
@@ -120,7 +136,7 @@ int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
   if (m->nlines > 0) {
     LinopArgs la{m->lines, m->nlines, m->nrhox, m->kw, m->nspec, m->numnu, m->xnfdop, m->dopple,
                  m->xne_eos, m->txnxn, m->hckt, m->tabcont, m->waveset, m->h0, m->h1, m->h2, m->hf, m->xl,
-                 nullptr, m->cnt};
+                 nullptr, m->cnt, m->nu_first, m->nu_last};
     Timer tm(ctx, "atlas_linop");
     if (ctx->precision == ATLASGPU_PREC_MIXED)
       k_atlas_linop<true><<<grid_for(ctx, m->nlines * 32, 256, 16), 256, 0, s>>>(la);
@@ -136,7 +152,8 @@ int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
   }
   RtArgs ra{ctx->ops, m->numnu, m->nrhox, m->kw, m->waveset, m->rcoset, m->acont, m->sigmac, nullptr,
             m->xl, (const double*)m->state + 1 * m->kw, (const double*)m->state + 0 * m->kw, m->hkt,
-            m->teff, m->nu_per_group, 1, m->kw, m->partial, m->hsurf, nullptr};
+            m->teff, m->nu_per_group, 1, m->kw, m->partial, m->hsurf, nullptr, m->nu_first, m->nu_last};
+  double* sums = m->ext_sums ? m->ext_sums : m->sum;
   {
     Timer tm(ctx, "atlas_rt");
     k_atlas_rt<<<m->blocks_rt, kRtThreads, m->smem_rt, s>>>(ra);
@@ -144,17 +161,41 @@ int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
   }
   {
     Timer tm(ctx, "atlas_reduce");
-    launch_reduce(m->partial, m->nwl, m->kw, m->sum, s);
-    CKL(ctx);
-  }
-  {
-    Timer tm(ctx, "atlas_finish");
-    k_model_finish<<<1, kFinThreads, fin_smem_bytes(m->kw, kRossMax), s>>>(
-        m->ms, m->sum, m->kw, m->nrhox, m->iter_dev, m->teff, m->grav, m->R, m->maxerr_dev);
+    launch_reduce(m->partial, m->blocks_rt * kRtGroups, m->kw, sums, s);
     CKL(ctx);
   }
   ctx->timing = was;
   return 0;
+}
+
+// The rest of the iteration: ROSS(3), RADIAP(3), TCORR(3) and the remap from
+// the (possibly externally all-reduced) frequency sums.
+int enqueue_finish(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
+  cudaStream_t s = ctx->stream;
+  const bool was = ctx->timing;
+  ctx->timing = was && timed;
+  double* sums = m->ext_sums ? m->ext_sums : m->sum;
+  {
+    Timer tm(ctx, "atlas_finish");
+    k_model_finish<<<1, kFinThreads, fin_smem_bytes(m->kw, kRossMax), s>>>(
+        m->ms, sums, m->kw, m->nrhox, m->iter_dev, m->teff, m->grav, m->R, m->maxerr_dev);
+    CKL(ctx);
+  }
+  ctx->timing = was;
+  return 0;
+}
+
+int enqueue_iteration(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
+  int r;
+  if ((r = enqueue_begin(ctx, m, timed))) return r;
+  return enqueue_finish(ctx, m, timed);
+}
+
+void drop_graph(atlasgpu_model* m) {
+  if (m->gexec) cudaGraphExecDestroy(m->gexec);
+  if (m->graph) cudaGraphDestroy(m->graph);
+  m->gexec = nullptr;
+  m->graph = nullptr;
 }
 
 __global__ void k_fp64_fma(double* out, int iters) {
@@ -260,11 +301,13 @@ int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlas
   }
   // RT launch shape
   m->smem_rt = rt_smem_bytes();
-  const int target = ctx->nsm * 3 * kRtGroups * 4;
-  m->nu_per_group = std::max(1, (m->numnu + target - 1) / target);
-  const int ng = (m->numnu + m->nu_per_group - 1) / m->nu_per_group;
-  m->blocks_rt = (ng + kRtGroups - 1) / kRtGroups;
-  m->nwl = m->blocks_rt * kRtGroups;
+  rt_shape(ctx, m);
+  {
+    // any shard launches at most min(NUMNU, target) groups (rt_shape): size the partials for that
+    const int target = ctx->nsm * 3 * kRtGroups * 4;
+    const int gmax = std::min(m->numnu, target);
+    m->nwl = ((gmax + kRtGroups - 1) / kRtGroups) * kRtGroups;
+  }
   if ((r = dalloc(ctx, &m->partial, (size_t)m->nwl * (kAcc * kw + 1)))) {
     atlasgpu_model_destroy(ctx, m);
     return r;
@@ -456,6 +499,49 @@ int atlasgpu_model_set_params(atlasgpu_ctx* ctx, atlasgpu_model* m, double teff,
   m->gexec = nullptr;
   m->graph = nullptr;
   m->kapcont_done = false;
+  return 0;
+}
+
+int atlasgpu_model_set_shard(atlasgpu_ctx* ctx, atlasgpu_model* m, int nu_first, int nu_last) {
+  if (!ctx || !m || nu_first < 1 || nu_last < nu_first || nu_last > m->numnu)
+    return fail(ctx, ATLASGPU_EINVAL, "model_set_shard: frequencies %d..%d outside 1..%d", nu_first, nu_last,
+                m ? m->numnu : 0);
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  m->nu_first = nu_first;
+  m->nu_last = nu_last;
+  rt_shape(ctx, m);
+  drop_graph(m);
+  return 0;
+}
+
+int atlasgpu_model_set_sums_buffer(atlasgpu_ctx* ctx, atlasgpu_model* m, double* d_sums) {
+  if (!ctx || !m) return fail(ctx, ATLASGPU_EINVAL, "model_set_sums_buffer: null");
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  m->ext_sums = d_sums;
+  drop_graph(m);
+  return 0;
+}
+
+int atlasgpu_model_iterate_begin(atlasgpu_ctx* ctx, atlasgpu_model* m) {
+  if (!ctx || !m) return fail(ctx, ATLASGPU_EINVAL, "model_iterate_begin: null");
+  cudaSetDevice(ctx->device);
+  const int r = enqueue_begin(ctx, m, true);
+  m->kapcont_done = true;
+  return r;
+}
+
+int atlasgpu_model_iterate_end(atlasgpu_ctx* ctx, atlasgpu_model* m, double* maxerr) {
+  if (!ctx || !m) return fail(ctx, ATLASGPU_EINVAL, "model_iterate_end: null");
+  cudaSetDevice(ctx->device);
+  int r;
+  if ((r = enqueue_finish(ctx, m, true))) return r;
+  double e = 0.0;
+  CK(cudaMemcpyAsync(&e, m->maxerr_dev, sizeof e, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (maxerr) *maxerr = e;
+  if (!(e == e)) return fail(ctx, ATLASGPU_ENONFINITE, "model_iterate_end: FLXERR is not finite");
   return 0;
 }
 

@@ -396,6 +396,67 @@ int atlasgpu_synthe_spectrum_dev(atlasgpu_ctx* ctx, const double* d_wledge, int 
   return spectrum_launch(ctx, a);
 }
 
+int atlasgpu_synthe_nlte_opacity(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* recs, int64_t n, int length,
+                                 int nrhox, double wbegin, double ratio, double wlend, double velshift_kms,
+                                 const float* continuum, const double* xnfdop, const double* dopple, int nspec,
+                                 const double* xne, const double* txnxn, const double* hckt, const double* contx,
+                                 float* opacity_inout) {
+  if (!ctx || n < 0 || (n > 0 && !recs) || length < 1 || nrhox < 1 || nrhox > kKwMax || !(wbegin > 0.0) ||
+      !(ratio > 1.0) || !continuum || !xnfdop || !dopple || nspec < 1 || !xne || !txnxn || !hckt || !contx ||
+      !opacity_inout)
+    return fail(ctx, ATLASGPU_EINVAL, "synthe_nlte_opacity: bad argument");
+  for (int64_t i = 0; i < n; ++i) {
+    const int t = recs[i].itype;
+    const bool normal = t == 0 || t == 3 || t <= -3;
+    if (normal && recs[i].ncon > 0 && (recs[i].ncon > 26 || recs[i].nelionx < 1 || recs[i].nelionx > 17))
+      return fail(ctx, ATLASGPU_EINVAL, "synthe_nlte_opacity: NCON %d / NELIONX %d outside CONTX at record %lld",
+                  recs[i].ncon, recs[i].nelionx, (long long)i);
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const size_t nm = (size_t)nrhox * length, nd = (size_t)nrhox * nspec;
+  atlasgpu_nlte_line* d_rec;
+  float *d_cont, *d_op;
+  double *d_xd, *d_dp, *d_xne, *d_tx, *d_hc, *d_em, *d_cx, *d_acc;
+  int r;
+  if ((r = bufT(ctx, "sn_rec", (size_t)std::max<int64_t>(n, 1), &d_rec)) || (r = bufT(ctx, "sn_cont", nm, &d_cont)) ||
+      (r = bufT(ctx, "sn_op", nm, &d_op)) || (r = bufT(ctx, "sn_xd", nd, &d_xd)) || (r = bufT(ctx, "sn_dp", nd, &d_dp)) ||
+      (r = bufT(ctx, "sn_xne", nrhox, &d_xne)) || (r = bufT(ctx, "sn_tx", nrhox, &d_tx)) ||
+      (r = bufT(ctx, "sn_hc", nrhox, &d_hc)) || (r = bufT(ctx, "sn_em", nrhox, &d_em)) ||
+      (r = bufT(ctx, "sn_cx", 26 * 17, &d_cx)) || (r = bufT(ctx, "sn_acc", nm, &d_acc)))
+    return r;
+  // EMERGE(J) = RYDBERG_INF / NMERGE**2 with the reference's REAL(4) INGLIS and NMERGE = INGLIS - 1.5
+  std::vector<double> em(nrhox);
+  for (int j = 0; j < nrhox; ++j) {
+    const float inglis = (float)(1600.0 / pow(xne[j], 2.0 / 15.0));
+    const float nmerge = inglis - 1.5f;
+    em[j] = 109737.31568157 / ((double)nmerge * (double)nmerge);
+  }
+  if (n > 0) CK(cudaMemcpyAsync(d_rec, recs, n * sizeof(atlasgpu_nlte_line), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_cont, continuum, nm * sizeof(float), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_op, opacity_inout, nm * sizeof(float), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_xd, xnfdop, nd * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_dp, dopple, nd * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_xne, xne, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_tx, txnxn, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_hc, hckt, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_em, em.data(), nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_cx, contx, 26 * 17 * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(d_acc, 0, nm * sizeof(double), s));
+  if (n > 0) {
+    NlteArgs a{d_rec, n, length, nrhox, nspec, wbegin, ratio, wlend, 1.0 + velshift_kms / 299792.458, d_cont, d_xd,
+               d_dp, d_xne, d_tx, d_hc, d_em, d_cx, d_acc};
+    Timer tm(ctx, "synthe_nlte");
+    k_synthe_nlte<<<grid_for(ctx, n * nrhox * 32, 256, 16), 256, 0, s>>>(a);
+    CKL(ctx);
+    k_add_f64_to_f32<<<grid_for(ctx, (int64_t)nm, 256, 8), 256, 0, s>>>(d_acc, d_op, (int64_t)nm);
+    CKL(ctx);
+  }
+  CK(cudaMemcpyAsync(opacity_inout, d_op, nm * sizeof(float), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
 int atlasgpu_synthe_spectrum(atlasgpu_ctx* ctx, const double* wledge, int nedge, const double* contabs,
                              const double* contscat, int stride, int nrhox, const double* rhox,
                              const double* hkt, double wbegin, double ratio, int length,

@@ -97,6 +97,58 @@ static __global__ void k_atlas_prep(AtlasPrepArgs a) {
   }
 }
 
+// XLINOP record preparation: the per-record part of XLINOP's read loop
+// (atlas12_modules.f90:19992-20036) -- NUCONT from IWL, NU from WLVAC (both
+// advanced monotonically in the reference; binary searches here, the same on
+// wavelength-sorted records), the TYPE dispatch, and CONTX(NCON,NELIONX) for
+// the continuum-edge cutoff.  Records the normal branch does not walk get
+// NELION = 0.
+struct XlinopPrepArgs {
+  const atlasgpu_nlte_line* rec;
+  int64_t n;
+  const double* waveset;
+  int numnu;
+  const int32_t* iwavetab;  // [nwave+1]
+  int nwave, nspec;
+  const double* contx;      // CONTX(25,16) column-major
+  AtlasLine* out;
+  double* lcontx;           // [n] CONTX(NCON,NELIONX) or 0
+};
+
+static __global__ void k_xlinop_prep(XlinopPrepArgs a) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const atlasgpu_nlte_line r = a.rec[i];
+    AtlasLine L;
+    L.pad = 0;
+    L.wlvac = r.wlvac;
+    L.cgf = (double)r.gf;
+    L.elo = (double)r.elo;
+    L.gr = (double)r.gammar;
+    L.gs = (double)r.gammas;
+    L.gw = (double)r.gammaw;
+    int lo = 1, hi = a.nwave + 1;  // NUCONT = first k with IWL < IWAVETAB(k), clamped to NWAVE+1
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (r.nbuff < a.iwavetab[mid - 1]) hi = mid;
+      else lo = mid + 1;
+    }
+    L.nucont = lo;
+    lo = 1;  // NU = first grid point with WLVAC < WAVESET(NU); NUMNU+1 when none
+    hi = a.numnu + 1;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (r.wlvac < a.waveset[mid - 1]) hi = mid;
+      else lo = mid + 1;
+    }
+    L.nu = lo;
+    const bool normal = r.itype == 0 || r.itype == 3;
+    L.nelion = (normal && r.nelion >= 1 && r.nelion <= a.nspec && L.nu < a.numnu) ? r.nelion : 0;
+    const int ncon = r.ncon > 10 ? 0 : r.ncon;
+    a.lcontx[i] = (ncon > 0) ? a.contx[(size_t)(r.nelionx - 1) * 25 + (ncon - 1)] : 0.0;
+    a.out[i] = L;
+  }
+}
+
 struct LinopArgs {
   const AtlasLine* lines;
   int64_t n;
@@ -110,6 +162,19 @@ struct LinopArgs {
   double* xl;                     // XLINES(J, NU): [numnu][kw]
   unsigned long long* npairs;     // diagnostics: walked (line, depth) pairs
   unsigned long long* used;       // LINEUSED: lines above TABCONT at a coarse depth
+  // frequency shard NU_LO..NU_HI (1-based; 0 => NUMNU) that receives XLINES: a
+  // line is walked only if its +-100-point window meets the shard, and only
+  // points inside the shard are added (the walk itself is unchanged)
+  int nu_lo = 1, nu_hi = 0;
+  // XLINOP's normal-line branch (atlas12_modules.f90:20040-20174) walks the
+  // same way with MAX_WING = 2000, LORENTZ_PREFAC = 0.5642 and a blue-wing
+  // cutoff at the continuum edge WCON = 1e7 / (CONTX(NCON,NELIONX) - EMERGE(J))
+  // per (line, depth): lcontx [n] holds CONTX(NCON,NELIONX) (0: no cutoff),
+  // emerge [kw] EMERGE(J).  LINOP1: 100, 1/sqrt(pi), no cutoff (null).
+  int max_wing = 100;
+  double lorentz = kInvSqrtPi;
+  const double* lcontx = nullptr;
+  const double* emerge = nullptr;
 };
 
 // LINOP1's profile value at one wing point, V = (distance in nm) * RDOP with
@@ -129,8 +194,8 @@ __device__ __forceinline__ double linop_cv(const LinopArgs& a, double center, do
   const double vv = dl * rdop;
   if (adamp > 0.20) return center * linop_full_voigt(a, vv, adamp);
   if (vv > 10.0) {
-    if (F32) return (double)((float)center * ((float)(kInvSqrtPi * adamp) * __frcp_rn((float)(vv * vv))));
-    return center * kInvSqrtPi * adamp / (vv * vv);
+    if (F32) return (double)((float)center * ((float)(a.lorentz * adamp) * __frcp_rn((float)(vv * vv))));
+    return center * a.lorentz * adamp / (vv * vv);
   }
   const int iv = (int)(vv * 200.0 + 1.5);
   if (F32) {
@@ -157,9 +222,10 @@ __device__ __forceinline__ bool linop_below(const LinopArgs& a, double cv, doubl
 template <bool F32>
 static __device__ __noinline__ void linop_finish_warp(const LinopArgs& a, int J, double center, double adamp,
                                                       double rdop, double wlvac, int nu, double tc, int rnext,
-                                                      bool rdone, int bnext, bool bdone, int lane) {
+                                                      bool rdone, int bnext, bool bdone, double wcon, int lane) {
   double* xl = a.xl + (J - 1);
-  const int iwmax = min(nu + 100, a.numnu);
+  const int iwmax = min(nu + a.max_wing, a.numnu);
+  const int nuh = a.nu_hi > 0 ? a.nu_hi : a.numnu;
   if (!rdone) {
     for (int base = rnext; base <= iwmax; base += 32) {
       const int iw = base + lane;
@@ -173,15 +239,16 @@ static __device__ __noinline__ void linop_finish_warp(const LinopArgs& a, int J,
       }
       const unsigned stop = __ballot_sync(0xffffffffu, valid && below);
       const int last = stop ? base + __ffs(stop) - 1 : iwmax;
-      if (valid && iw <= last) atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
+      if (valid && iw <= last && iw >= a.nu_lo && iw <= nuh) atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
       if (stop) break;
     }
   }
   if (!bdone) {
-    for (int i0 = bnext; i0 <= 100; i0 += 32) {
+    for (int i0 = bnext; i0 <= a.max_wing; i0 += 32) {
       const int i = i0 + lane;
       const int iw = nu - i;
-      const bool valid = i <= 100 && iw >= 1;
+      // the walk ends before the grid start and (XLINOP) before the continuum edge
+      const bool valid = i <= a.max_wing && iw >= 1 && !(a.waveset[iw - 1] < wcon);
       double cv = 0.0;
       bool below = false;
       if (valid) {
@@ -191,8 +258,8 @@ static __device__ __noinline__ void linop_finish_warp(const LinopArgs& a, int J,
       }
       const unsigned stop = __ballot_sync(0xffffffffu, valid && below);
       const unsigned inval = __ballot_sync(0xffffffffu, !valid);
-      const int ilast = stop ? i0 + __ffs(stop) - 1 : 100;
-      if (valid && i <= ilast) atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
+      const int ilast = stop ? i0 + __ffs(stop) - 1 : a.max_wing;
+      if (valid && i <= ilast && iw >= a.nu_lo && iw <= nuh) atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
       if (stop || inval) break;
     }
   }
@@ -211,9 +278,11 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
   const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long walked = 0;
+  const int nuh = a.nu_hi > 0 ? a.nu_hi : a.numnu;
   for (int64_t il = w0; il < a.n; il += nw) {
     const AtlasLine L = a.lines[il];
-    if (L.nelion == 0) continue;
+    if (L.nelion == 0 || L.nu + a.max_wing < a.nu_lo || L.nu - a.max_wing > nuh) continue;
+    const double cx = a.lcontx ? a.lcontx[il] : 0.0;
     const double* xdn = a.xnfdop + (size_t)(L.nelion - 1) * a.kw;
     const double* dpn = a.dopple + (size_t)(L.nelion - 1) * a.kw;
     const double* tcv = a.tabcont + (size_t)(L.nucont - 1) * a.kw;
@@ -231,8 +300,8 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
     }
     const unsigned ifj = __ballot_sync(0xffffffffu, pass);
     if (ifj == 0) continue;
-    if (lane == 0) atomicAdd(a.used, 1ull);
-    const int iwmax = min(L.nu + 100, a.numnu);
+    if (lane == 0 && a.used) atomicAdd(a.used, 1ull);
+    const int iwmax = min(L.nu + a.max_wing, a.numnu);
     for (int J0 = 1; J0 <= a.nrhox; J0 += 32) {
       const int J = J0 + lane;
       bool walk = false;
@@ -255,6 +324,12 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
         }
       }
       if (!__any_sync(0xffffffffu, walk)) continue;
+      // XLINOP: no walk at a depth whose continuum edge lies redward of the line
+      double wcon = 0.0;
+      if (walk && cx > 0.0) {
+        wcon = 1.0e7 / (cx - a.emerge[J - 1]);
+        if (L.wlvac < wcon) walk = false;
+      }
       double adamp = 0.0, rdop = 1.0;
       if (walk) {
         adamp = (L.gr + L.gs * a.xne[J - 1] + L.gw * a.txnxn[J - 1]) / dpn[J - 1];
@@ -270,19 +345,19 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
           const int iw = rnext;
           const double dl = a.waveset[iw - 1] - L.wlvac;
           const double cv = linop_cv<F32>(a, center, adamp, dl, rdop);
-          atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
+          if (iw >= a.nu_lo && iw <= nuh) atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
           if (linop_below<F32>(a, cv, tc, center, adamp, dl, rdop) || iw >= iwmax) rdone = true;
           else rnext = iw + 1;
         }
         if (!bdone) {
           const int iw = L.nu - bnext;
-          if (iw < 1) {
+          if (iw < 1 || a.waveset[iw - 1] < wcon) {
             bdone = true;
           } else {
             const double dl = L.wlvac - a.waveset[iw - 1];
             const double cv = linop_cv<F32>(a, center, adamp, dl, rdop);
-            atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
-            if (linop_below<F32>(a, cv, tc, center, adamp, dl, rdop) || bnext >= 100) bdone = true;
+            if (iw >= a.nu_lo && iw <= nuh) atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
+            if (linop_below<F32>(a, cv, tc, center, adamp, dl, rdop) || bnext >= a.max_wing) bdone = true;
             else bnext = bnext + 1;
           }
         }
@@ -301,7 +376,8 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
         const int bn = __shfl_sync(0xffffffffu, bnext, src);
         const bool rd = __shfl_sync(0xffffffffu, (int)rdone, src) != 0;
         const bool bd = __shfl_sync(0xffffffffu, (int)bdone, src) != 0;
-        linop_finish_warp<F32>(a, Js, cs, as, ds, L.wlvac, L.nu, ts, rn, rd, bn, bd, lane);
+        const double wc = __shfl_sync(0xffffffffu, wcon, src);
+        linop_finish_warp<F32>(a, Js, cs, as, ds, L.wlvac, L.nu, ts, rn, rd, bn, bd, wc, lane);
       }
     }
   }
@@ -363,6 +439,8 @@ struct RtArgs {
   double* partial;   // [groups][kAcc*kw + 1]
   double* hsurf;     // [numnu] HNU(1) per frequency (the .flux record)
   int* sweeps;       // [numnu] Eddington sweeps (diagnostic; may be null)
+  // frequency shard NU_FIRST..NU_LAST (1-based; 0 => NUMNU): groups start at NU_FIRST
+  int nu_first = 1, nu_last = 0;
 };
 
 struct RtWS {
@@ -400,8 +478,8 @@ static __device__ __forceinline__ void rt_body(const RtArgs& a) {
   const JoshOps& ops = *a.ops;
   const int nr = a.nrhox;
   const int gw = blockIdx.x * kRtGroups + gid;  // partial-sum row of this group
-  const int nu0 = gw * a.nu_per_warp + 1;
-  const int nu1 = min(nu0 + a.nu_per_warp - 1, a.numnu);
+  const int nu0 = a.nu_first + gw * a.nu_per_warp;
+  const int nu1 = min(nu0 + a.nu_per_warp - 1, a.nu_last > 0 ? a.nu_last : a.numnu);
   double acc[kAcc][C];
 #pragma unroll
   for (int q = 0; q < kAcc; ++q)

@@ -362,4 +362,107 @@ static __global__ void __launch_bounds__(128) k_spectrum(SpecArgs a) {
   }
 }
 
+// ---------------------------------------------------------------- NLTE list
+// compute_line_opacity's normal-metal branch (TYPE 0, 3 and the He I
+// fallthrough TYPE <= -3; synthe_module.f90:3400-3458), FP64.  One warp per
+// (record, depth); lanes take 32 consecutive grid points of a wing, the
+// first lane below the cutoff ends the wing (red: tested before the add,
+// blue: after it).  Points blueward of WCON are skipped, WCON..WTAIL tapers.
+// Grid wavelengths are wbegin * ratio**(i-1) per point (the reference walks
+// them by repeated multiplication; the two agree to ~1e-11 relative).
+struct NlteArgs {
+  const atlasgpu_nlte_line* rec;
+  int64_t n;
+  int length, nrhox, nspec;
+  double wbegin, ratio, wlend, dopratio;
+  const float* cont;                // [nrhox][length]
+  const double *xnfdop, *dopple;    // [nrhox][nspec]
+  const double *xne, *txnxn, *hckt, *emerge;  // [nrhox]
+  const double* contx;              // CONTX(26,17) column-major
+  double* acc;                      // [nrhox][length]
+};
+
+static __global__ void __launch_bounds__(256) k_synthe_nlte(NlteArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t npair = a.n * a.nrhox;
+  for (int64_t p = w0; p < npair; p += nw) {
+    const int64_t il = p / a.nrhox;
+    const int j = (int)(p % a.nrhox);
+    const atlasgpu_nlte_line r = a.rec[il];
+    const int t = r.itype;
+    if (!(t == 0 || t == 3 || t <= -3) || r.nelion < 1 || r.nelion > a.nspec) continue;
+    const float* cont = a.cont + (size_t)j * a.length;
+    double* acc = a.acc + (size_t)j * a.length;
+    const double wl = r.wlvac * a.dopratio;
+    const int nbuff = r.nbuff;
+    const int nel = r.nelion - 1;
+    const double xd = a.xnfdop[(size_t)j * a.nspec + nel], dp = a.dopple[(size_t)j * a.nspec + nel];
+    double kappa0 = (double)r.gf * xd;
+    const int ic = nbuff < 1 ? 1 : (nbuff > a.length ? a.length : nbuff);
+    const double kapmin = (double)cont[ic - 1] * kLineCutoff;
+    if (kappa0 < kapmin) continue;
+    kappa0 = kappa0 * exp(-(double)r.elo * a.hckt[j]);
+    if (kappa0 < kapmin) continue;
+    double wcon = 0.0, wtail = 0.0;
+    if (r.ncon > 0) {
+      const double cx = a.contx[(size_t)(r.nelionx - 1) * 26 + (r.ncon - 1)];
+      wcon = 1.0e7 / (cx - a.emerge[j]) * a.dopratio;
+      wtail = 1.0e7 / (cx - a.emerge[j] - 500.0) * a.dopratio;
+    }
+    const double adamp = ((double)r.gammar + (double)r.gammas * a.xne[j] + (double)r.gammaw * a.txnxn[j]) / dp;
+    const double dopwl = dp * wl;
+    if (wl <= a.wlend) {
+      const int minred = nbuff > 1 ? nbuff : 1;
+      for (int base = minred; base <= a.length; base += 32) {
+        const int ib = base + lane;
+        bool use = false, stop = false;
+        double kappa = 0.0;
+        if (ib <= a.length) {
+          const double wave = a.wbegin * powi(a.ratio, ib - 1);
+          if (wave >= wcon) {
+            use = true;
+            kappa = kappa0 * voigt_weideman(fabs(wave - wl) / dopwl, adamp);
+            if (wave < wtail) kappa = kappa * ((wave - wcon) / (wtail - wcon));
+            stop = kappa < (double)cont[ib - 1] * kLineCutoff;
+          }
+        }
+        const unsigned sb = __ballot_sync(0xffffffffu, stop);
+        const int first = sb ? __ffs(sb) - 1 : 32;
+        if (use && lane < first) atomicAdd(acc + ib - 1, kappa);
+        if (sb) break;
+      }
+      if (minred == 1 || wl < a.wbegin) continue;
+    }
+    const int ib0 = a.length + 1 < nbuff ? a.length + 1 : nbuff;
+    const int maxblue = ib0 - 1;
+    for (int i0 = 1; i0 <= maxblue; i0 += 32) {
+      const int i = i0 + lane;
+      const int ib = ib0 - i;
+      bool use = false, stop = false;
+      double kappa = 0.0;
+      if (i <= maxblue) {
+        const double wave = a.wbegin * powi(a.ratio, ib - 1);
+        if (wave >= wcon) {
+          use = true;
+          kappa = kappa0 * voigt_weideman(fabs(wave - wl) / dopwl, adamp);
+          if (wave < wtail) kappa = kappa * ((wave - wcon) / (wtail - wcon));
+          stop = kappa < (double)cont[ib - 1] * kLineCutoff;
+        }
+      }
+      const unsigned sb = __ballot_sync(0xffffffffu, stop);
+      const int first = sb ? __ffs(sb) - 1 : 32;
+      if (use && lane <= first) atomicAdd(acc + ib - 1, kappa);
+      if (sb) break;
+    }
+  }
+}
+
+// opacity [nrhox][length] (REAL(4)) += the FP64 contribution
+static __global__ void k_add_f64_to_f32(const double* __restrict__ acc, float* __restrict__ out, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    out[e] = (float)((double)out[e] + acc[e]);
+}
+
 }  // namespace atlasgpu

@@ -133,6 +133,44 @@ def atlas_lines(n, wl_lo, wl_hi, seed=2, mol_frac=0.0):
                          encode_i16(10.0 ** loggf), encode_i16(gr), encode_i16(gs), encode_i16(gw))
 
 
+def nlte_records(n, wl_lo, wl_hi, seed=6, strong=0.05, ncon_frac=0.3, types=(0, 3, 2, 1), type_p=(.7, .15, .1, .05)):
+    """Unit-19 records (the NLTE / complex-profile list XLINOP reads), sorted
+    by wavelength, with the ATLAS line distributions plus: a fraction `strong`
+    of lines 4 dex stronger (wings beyond LINOP1's 100 points), a fraction
+    `ncon_frac` with a continuum-edge cutoff (NCON 1..10, NELIONX 1..16), and
+    the line types in `types` with probabilities `type_p`."""
+    from . import _lib
+    rng = np.random.default_rng(seed)
+    ratiolg = np.log(1.0 + 1.0 / 2000000.0)
+    wl = np.sort(np.exp(rng.uniform(np.log(wl_lo), np.log(wl_hi), n)))
+    atoms = [sg.nelion(z, s) for z in sg.METALS[:, 0] for s in (1, 2)]
+    loggf = rng.normal(-2.0, 1.5, n) + np.where(rng.uniform(size=n) < strong, 4.0, 0.0)
+    four_pi_c = 4.0 * np.pi * C_NM
+    r = np.zeros(n, _lib.NLTE_LINE)
+    r["wlvac"] = wl
+    r["elo"] = rng.uniform(0.0, 8.0, n) * EV_CM
+    r["gf"] = 0.026538 / np.sqrt(np.pi) / C_NM * wl * 10.0 ** loggf  # CGF
+    r["nelion"] = rng.choice(atoms, n)
+    r["itype"] = rng.choice(np.array(types), n, p=np.array(type_p) / np.sum(type_p))
+    has = rng.uniform(size=n) < ncon_frac
+    r["ncon"] = np.where(has, rng.integers(1, 11, n), 0)
+    r["nelionx"] = np.where(has, rng.integers(1, 17, n), 0)
+    r["gammar"] = 10.0 ** rng.normal(8.0, 0.3, n) * wl / four_pi_c
+    r["gammas"] = 10.0 ** rng.normal(-5.5, 0.5, n) * wl / four_pi_c
+    r["gammaw"] = 10.0 ** rng.normal(-7.5, 0.3, n) * wl / four_pi_c
+    r["nbuff"] = np.floor(np.log(wl) / ratiolg + 0.5).astype(np.int32)  # IWL
+    return r
+
+
+def contx_table(seed=7):
+    """A CONTX(25,16) edge table [16, 25] (cm^-1) placing continuum edges
+    across the optical and near-UV: for tests of XLINOP's blue-wing cutoff."""
+    rng = np.random.default_rng(seed)
+    t = np.zeros((16, 25))
+    t[:, :10] = rng.uniform(1.0e4, 1.0e5, (16, 10))
+    return t
+
+
 def atlas_waveset(nustart=9599, numnu=30000):
     """WAVESET(NU) = 10**(1 + 1e-4*(NU+NUSTART-1)) and RCOSET trapezoid weights
     (atlas12c.f90:451-491)."""

@@ -1,25 +1,29 @@
 #!/usr/bin/env python3
 """bench.py -- converged ATLAS12 models per hour on B200.
 
-Workload (the opacity-sampling configuration the metric is quoted on): one
-ATLAS12 model with 30,000 log-spaced frequencies over 9 nm - 160 um, 72
-depths, 500,000 synthetic lines (lambda log-uniform, log gf ~ N(-2, 1.5),
-E_low ~ U(0, 8) eV, log gamma_rad/Stark/vdW ~ N(8, .3)/N(-5.5, .5)/N(-7.5, .3)),
-Teff 5777 K, log g 4.44, vturb 1.5 km/s, iterated from the Eddington grey
-start until max |FLXERR| <= 0.1 % (Delta F/F <= 1e-3; cap 60 iterations).
-Populations and continuum come from the documented synthetic surrogate.
+Workload (the opacity-sampling configuration): ATLAS12 models with 30,000
+log-spaced frequencies over 9 nm - 160 um, 72 depths and 500,000 synthetic
+lines (lambda log-uniform, log gf ~ N(-2, 1.5), E_low ~ U(0, 8) eV,
+log gamma_rad/Stark/vdW ~ N(8, .3)/N(-5.5, .5)/N(-7.5, .3)), each iterated
+until max |FLXERR| <= 0.1 % (Delta F/F <= 1e-3).  A step is one set of 32
+models whose stellar parameters are drawn (seeded) from the warm-start box:
+Teff 3500-8000 K, log g 1-5, [M/H] -2..+0.5, vturb 0.5-3 km/s.  Populations
+and continuum come from the documented synthetic surrogate.
 
-A step is one model run to convergence; value = converged models/hr (whole
-job).  Inputs stay resident in HBM during the timed region; L2 is flushed
-between steps.  e2e repeats the measurement through the public API
-(atlas12_b200.atlas.AtlasModel) with host buffers: model creation (upload of
-the line list, grids and tables), the iterations, and the read-back of the
-converged structure are all inside the wall-clock timed region.
+value: converged models per hour (whole job) of this library's path --
+batched models (one captured graph per iteration for all slots),
+mixed-precision LINOP1, and the learned warm start with the grey start as
+fallback -- with inputs resident in HBM, L2 flushed (256 MB write) between
+steps, CUDA events on the library's stream.  plain_fp64: the same 32 models
+one at a time, all-FP64, grey start, one launch at a time (the plain FP64 GPU
+path the patterns are measured against).  e2e: the same step through the
+public API from host buffers (batch creation with the line list upload,
+warm-start prediction, iteration, read-back of every structure).
 
 --impl reference times the CPU restatement of the same path (oracle/, the
 reference's own Fortran cannot be built in this image) on all host threads:
-each step is one full iteration; models/hr uses the iteration count the
-method needs to converge on this workload.
+each step is one full iteration of the grey-start solar model; models/hr
+uses the mean iteration count the plain method needs on the step's models.
 """
 import argparse
 import json
@@ -34,16 +38,21 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-CFG = dict(workload="atlas12-opacity-sampling", numnu=30000, wl_lo=9.0, wl_hi=160000.0, nrhox=72,
-           nlines=500000, teff=5777.0, logg=4.44, vturb_kms=1.5, tol_percent=0.1, max_iter=60, seed=2,
-           start="eddington-grey")
-# iterations the method needs from the grey start on this workload (oracle run, same
-# method); used only to turn the reference arm's per-iteration time into models/hr
-REF_ITERS_TO_CONVERGE = 40
+# mean iterations per model (converged or capped) that the plain grey-start
+# method spends on the step's 32 models, measured on B200 by this bench's
+# plain_fp64 arm; turns the reference arm's per-iteration time into models/hr
+PLAIN_ITERS_PER_MODEL = 50.0
+CFG = dict(workload="atlas12-opacity-sampling model set", numnu=30000, wl_lo=9.0, wl_hi=160000.0, nrhox=72,
+           nlines=500000, line_seed=2, models_per_step=32, param_seed=13,
+           params="Teff U(3500,8000) K, log g U(1,5), [M/H] U(-2,0.5), vturb U(0.5,3) km/s", tol_percent=0.1,
+           max_iter=60, warm_max_iter=30, slots=32, vturb_solar=1.5)
+WARMSTART = os.path.join(ROOT, "atlas12_b200", "data", "warmstart_c2.npz")
 # FP64 flops counted per frequency in the RT kernel: LU 2/3 51^3, triangular
 # solves 2*51^2, system build 2*51^2, J/H/K operators 4*51^2 + 2*51,
 # INTEG/MAP1/DERIV and the mode-2 sums ~ 110 per depth (72 depths)
 FLOPS_PER_NU = int(2 / 3 * 51 ** 3 + 8 * 51 ** 2 + 2 * 51 + 110 * 72)
+# DRAM bytes of one model's RT pass (read + write), ncu on the 30,000-frequency model
+RT_TRAFFIC_PER_MODEL = 56.2e6
 
 
 def parse():
@@ -54,16 +63,18 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 GPU comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--synthe-c3", action="store_true", help="also measure the 20M-line full-optical SYNTHE case")
     return ap.parse_args()
 
 
 def workload():
-    from atlas12_b200 import surrogate, synthetic
+    from atlas12_b200 import surrogate, synthetic, warmstart
     ws, rc = synthetic.geometric_waveset(CFG["wl_lo"], CFG["wl_hi"], CFG["numnu"])
-    lines = synthetic.atlas_lines(CFG["nlines"], ws[2], ws[-3], seed=CFG["seed"])
-    ross = surrogate.RossTable()
-    grey = surrogate.grey_model(CFG["teff"], CFG["logg"], nrhox=CFG["nrhox"], ross=ross)
-    return dict(ws=ws, rc=rc, lines=lines, grey=grey, ross=ross)
+    lines = synthetic.atlas_lines(CFG["nlines"], ws[2], ws[-3], seed=CFG["line_seed"])
+    params = warmstart.sample_params(CFG["models_per_step"], CFG["param_seed"])
+    grey = [warmstart.grey_start(teff, logg, mh, CFG["nrhox"]) for teff, logg, mh, _ in params]
+    solar = surrogate.grey_model(5777.0, 4.44, nrhox=CFG["nrhox"], ross=surrogate.RossTable())
+    return dict(ws=ws, rc=rc, lines=lines, params=params, grey=grey, solar=solar)
 
 
 def operators():
@@ -145,7 +156,7 @@ def run_reference(args):
         step()
         times.append(time.perf_counter() - t0)
     t_it = float(np.mean(times))
-    v = 3600.0 / (t_it * REF_ITERS_TO_CONVERGE)
+    v = 3600.0 / (t_it * PLAIN_ITERS_PER_MODEL)
     line = {"impl": "reference", "metric": "converged models/hr (dF/F<=1e-3)", "value": v, "unit": "models/hr",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_it * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -153,61 +164,30 @@ def run_reference(args):
             "cpu_baseline": {"value": v, "unit": "models/hr", "cores": int(os.environ["OMP_NUM_THREADS"]),
                              "kind": "port",
                              "sample": f"one full ATLAS12 iteration per step (LINOP1 + 30,000-frequency RT pass + "
-                                       f"TCORR(3)) on the host; models/hr = 3600 / (t_iteration x "
-                                       f"{REF_ITERS_TO_CONVERGE} iterations to convergence)"},
+                                       f"TCORR(3)) of the grey-start solar model on the host; models/hr = 3600 / "
+                                       f"(t_iteration x {PLAIN_ITERS_PER_MODEL} iterations per model, the mean the "
+                                       f"plain method spends on the step's models)"},
             "e2e": {"value": v, "unit": "models/hr", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
 def oracle_iteration_factory(po, atlas, tables, W):
-    """One ATLAS12 iteration of the oracle on the grey start (state carried)."""
-    from atlas12_b200 import surrogate as sg
-    ops = po.Ops.from_tables(tables)
-    h0, h1, h2 = po.tabvoigt(tables["tabvi"], tables["tabh1"])
-    tl = po.build_tablog()
-    cut = atlas.cutoff_grid()
-    iw = atlas.iwavetab(cut)
-    g = W["grey"]
-    nr = g["t"].size
-    st = dict(t=g["t"].copy(), rhox=g["rhox"].copy(), p=g["p"].copy(), xne=np.zeros(nr), abross=np.zeros(nr),
-              prad=np.zeros(nr), vturb=np.full(nr, CFG["vturb_kms"] * 1e5), pturb=np.zeros(nr),
-              tauros=g["tauros"].copy(), accrad=np.zeros(nr), raden=np.zeros(nr), oldt1=np.zeros(nr),
-              teff=CFG["teff"], grav=g["grav"])
-    store = po.RossStore()
-    state = {"it": 0, "tabcont": None}
+    """One ATLAS12 iteration of the oracle on the grey-start solar model (state carried)."""
+    from iteration import OracleIteration
+    it = OracleIteration(po, atlas, tables, W["ws"], W["rc"], W["lines"], W["solar"], 5777.0, CFG["vturb_solar"])
+    return it.step
 
-    def step():
-        state["it"] += 1
-        it = state["it"]
-        if it > 1:
-            p = st["grav"] * st["rhox"] - st["prad"]
-            st["p"] = np.where(p <= 0, np.maximum(st["grav"] * st["rhox"] * 1e-4, 1e-10), p)
-        pop = sg.populations(st["t"], st["p"], CFG["vturb_kms"], sg.ATLAS_LINE_POP)
-        t = st["t"]
-        xd = np.zeros((270, nr))
-        dp = np.ones((270, nr))
-        xx = np.where(pop["dopple"] > 0, pop["xnfp"] / np.maximum(pop["dopple"], 1e-300) / pop["rho"][:, None], 0.0)
-        xd[:] = xx[:, :270].T
-        dp[:] = np.where(pop["dopple"][:, :270].T > 0, pop["dopple"][:, :270].T, 1.0)
-        hkt = sg.HPLANCK / (sg.KBOL * t)
-        hckt = hkt * sg.CLIGHT
-        txnxn = (pop["nh"] * (1 - pop["xh"]) + 0.42 * 0.085 * pop["nh"]) * (t / 1e4) ** 0.3
-        st["xne"] = pop["xne"]
-        if state["tabcont"] is None:
-            ka, sgm = sg.continuum_opacity(cut, t, st["p"], pop)
-            stc = 1 - np.exp(-(sg.CLIGHT_NMS / cut)[:, None] * hkt[None, :])
-            tab = (ka + sgm) * 1e-3 / stc
-            state["tabcont"] = np.vstack([tab, tab[-1:]])
-        atm = dict(xnfdop=xd, dopple=dp, xne=pop["xne"], txnxn=txnxn, hckt=hckt)
-        xl, _ = po.atlas_linop1(h0, h1, h2, tl, W["lines"], atm, state["tabcont"], iw, W["ws"])
-        ac, sgm = sg.continuum_opacity(W["ws"], t, st["p"], pop)
-        acc, _ = po.atlas_rt_pass(ops, W["ws"], W["rc"], ac, sgm, xl, st["rhox"], t, hkt, CFG["teff"])
-        err, st["finish"] = po.atlas_finish(st, acc, it, store)
-        return err
 
-    step.state = st
-    return step
+def warm_starts(ctx, params, grey):
+    """Starting structures from the trained network (grey where it is absent)."""
+    from atlas12_b200 import warmstart
+    if not os.path.exists(WARMSTART):
+        return list(grey), False
+    ws = warmstart.WarmStart.load(WARMSTART, ctx)
+    starts = [ws.start(*p) for p in params]
+    ws.mlp.close()
+    return starts, True
 
 
 def run_ours(args):
@@ -224,21 +204,21 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     W = workload()
     ops = operators()
-    g = W["grey"]
+    params, grey = W["params"], W["grey"]
     ctx = _lib.Context(local, _lib.PREC_MIXED, stream=stream.cuda_stream)
-    model = atlas.AtlasModel(ctx, ops, teff=CFG["teff"], logg=CFG["logg"], vturb=CFG["vturb_kms"],
-                             linedata=W["lines"], waveset=W["ws"], rcoset=W["rc"], start=g)
+    starts, learned = warm_starts(ctx, params, grey)
+    batch = atlas.AtlasBatch(ctx, ops, nslots=CFG["slots"], linedata=W["lines"], waveset=W["ws"], rcoset=W["rc"])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    first = CFG["warm_max_iter"] if learned else None
 
-    def one_model(graph=True):
-        model.set_structure(g["t"], g["p"], g["rhox"])
-        return model.iterate(max_iter=CFG["max_iter"], tol_percent=CFG["tol_percent"], graph=graph)
+    def one_step(b=batch, st=starts, keep=False):
+        return b.run_queue(params, st, max_iter=CFG["max_iter"], tol_percent=CFG["tol_percent"], keep=keep,
+                           fallback=grey if learned else None, first_max_iter=first)
 
     for _ in range(max(args.warmup, 1)):
-        one_model()
-    iters, converged = [], 0
+        one_step()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    total_ms = 0.0
+    total_ms, converged, iters, attempts = 0.0, 0, [], []
     clocks = Clocks(local)
     if dist:
         dist.barrier()
@@ -246,14 +226,15 @@ def run_ours(args):
     clocks.start()
     l0 = ctx.launches()
     for _ in range(args.steps):
-        flush.zero_()  # L2 flush between models (256 MB > 126 MB L2)
+        flush.zero_()  # L2 flush between steps (256 MB > 126 MB L2)
         ev0.record(stream)
-        n, hist = one_model()
+        res = one_step()
         ev1.record(stream)
         torch.cuda.synchronize()
         total_ms += ev0.elapsed_time(ev1)
-        iters.append(n)
-        converged += int(n > 0 and hist[-1] <= CFG["tol_percent"])
+        converged += sum(r["status"] == _lib.SLOT_CONVERGED for r in res)
+        iters += [r["iters"] for r in res]
+        attempts += [r["attempts"] for r in res]
     gpu_launches = ctx.launches() - l0
     clk = clocks.stop()
     torch.cuda.synchronize()
@@ -265,91 +246,149 @@ def run_ours(args):
     t_max = float(t_max.item())
     value = float(conv_all.item()) * 3600.0 / (t_max / 1e3)
 
-    # per-kernel times of one iteration (non-graph, CUDA events in the library)
+    # per-kernel times of one batched iteration with every slot running (CUDA events, no graph)
+    for s_ in range(CFG["slots"]):
+        teff, logg, mh, vt = params[s_ % len(params)]
+        batch.load(s_, teff, logg, vt, mh, grey[s_ % len(params)], max_iter=3, tol_percent=0.0)
+    batch.step(1)
     ctx.enable_timing(True)
-    model.set_structure(g["t"], g["p"], g["rhox"])
-    model.iterate(max_iter=3, tol_percent=0.0, graph=False)
-    kms = {k: ctx.kernel_ms(k) for k in ("model_eos", "model_kapp", "atlas_linop", "atlas_rt", "atlas_reduce",
-                                        "atlas_finish")}
+    batch.step(1)
+    names = ("eos", "kapcont", "kapp", "linop", "rt", "reduce", "finish")
+    kms = {k: ctx.kernel_ms("batch_" + k) for k in names}
     ctx.enable_timing(False)
+    batch.run()
+    per_model = {k: v / CFG["slots"] for k, v in kms.items()}
     fp64_peak = float(_lib.lib().atlasgpu_fp64_peak_tflops(ctx.handle))
+    ach = CFG["slots"] * CFG["numnu"] * FLOPS_PER_NU / (kms["rt"] * 1e-3) / 1e12
+    roof = {"kernel": "k_batch_rt (JOSH per frequency, FP64)", "bound": "fp64", "achieved": ach, "peak": fp64_peak,
+            "unit": "TFLOP/s", "frac": ach / fp64_peak if fp64_peak > 0 else None,
+            "traffic": RT_TRAFFIC_PER_MODEL * CFG["slots"],
+            "peak_source": "measured DFMA loop on this GPU (atlasgpu_fp64_peak_tflops); MEASURED_PEAKS.json has no FP64 figure",
+            "work": f"{FLOPS_PER_NU} FP64 flop per frequency x {CFG['numnu']} frequencies x {CFG['slots']} models per launch",
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_batch_rt launch (profiles/)"}
 
-    # plain FP64 GPU path: same method, FP64 everywhere, one launch at a time, grey start
+    # plain FP64 GPU path: the same models one at a time, FP64, grey start, per-launch host loop
     plain = None
     if not args.no_plain:
         ctx.set_precision(_lib.PREC_FP64)
-        one_model(graph=False)
-        pm, pi = 0.0, []
-        for _ in range(min(args.steps, 3)):
-            flush.zero_()
+        model = atlas.AtlasModel(ctx, ops, teff=5777.0, logg=4.44, vturb=1.5, linedata=W["lines"], waveset=W["ws"],
+                                 rcoset=W["rc"], start=W["solar"])
+        pm, pconv, pit = 0.0, 0, []
+        flush.zero_()
+        for (teff, logg, mh, vt), g in zip(params, grey):
+            model.set_params(teff, logg, vt, mh)
+            model.set_structure(g["t"], g["p"], g["rhox"])
             ev0.record(stream)
-            n, hist = one_model(graph=False)
+            try:
+                n, hist = model.iterate(max_iter=CFG["max_iter"], tol_percent=CFG["tol_percent"], graph=False)
+                ok = n > 0 and hist[-1] <= CFG["tol_percent"]
+            except _lib.AtlasGPUError:
+                n, ok = CFG["max_iter"], False
             ev1.record(stream)
             torch.cuda.synchronize()
             pm += ev0.elapsed_time(ev1)
-            pi.append(n)
+            pconv += int(ok)
+            pit.append(n)
+        model.close()
         ctx.set_precision(_lib.PREC_MIXED)
-        plain = {"value": 3600.0 * len(pi) / (pm / 1e3), "unit": "models/hr", "ms_per_model": pm / len(pi),
-                 "iterations": float(np.mean(pi)), "path": "FP64, per-launch host loop, grey start"}
+        plain = {"value": pconv * 3600.0 / (pm / 1e3), "unit": "models/hr", "converged": pconv,
+                 "models": len(params), "ms_per_model": pm / len(params), "mean_iterations": float(np.mean(pit)),
+                 "path": "FP64 everywhere, one model at a time, per-launch host loop, grey start"}
 
-    # e2e through the public API, host buffers in and out
+    # e2e through the public API from host buffers (batch creation uploads the line list and grid)
     e2e_s = 0.0
-    h2d = W["lines"].nbytes + W["ws"].nbytes + W["rc"].nbytes + 361 * 8 + 3 * 2001 * 8 + 4 * CFG["nrhox"] * 8
-    d2h = 5 * CFG["nrhox"] * 8 + CFG["numnu"] * 8
-    ne2e = max(1, min(args.steps, 3))
+    ne2e = max(1, min(args.steps, 2))
+    h2d = d2h = 0
     for _ in range(ne2e):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        m2 = atlas.AtlasModel(ctx, ops, teff=CFG["teff"], logg=CFG["logg"], vturb=CFG["vturb_kms"],
-                              linedata=W["lines"], waveset=W["ws"], rcoset=W["rc"], start=g)
-        m2.iterate(max_iter=CFG["max_iter"], tol_percent=CFG["tol_percent"], graph=True)
-        m2.structure()
+        b2 = atlas.AtlasBatch(ctx, ops, nslots=CFG["slots"], linedata=W["lines"], waveset=W["ws"], rcoset=W["rc"])
+        st2, _ = warm_starts(ctx, params, grey)
+        res = one_step(b2, st2, keep=True)
         torch.cuda.synchronize()
         e2e_s += time.perf_counter() - t0
-        m2.close()
+        b2.close()
+        n_loads = sum(r["attempts"] for r in res)
+        h2d = (W["lines"].nbytes + W["ws"].nbytes + W["rc"].nbytes + 361 * 8 + 3 * 2001 * 8 +
+               n_loads * 3 * CFG["nrhox"] * 8)
+        d2h = len(res) * (5 * CFG["nrhox"] * 8 + CFG["numnu"] * 8)
     e2e_all = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(e2e_all, op=dist.ReduceOp.MAX)
-    e2e_value = world * ne2e * 3600.0 / float(e2e_all.item())
+    e2e_value = world * ne2e * converged / max(args.steps, 1) * 3600.0 / float(e2e_all.item())
 
-    # roofline of the dominant kernel
-    dom = max((k for k in kms if kms[k] > 0), key=lambda k: kms[k])
-    if dom == "atlas_rt":
-        ach = CFG["numnu"] * FLOPS_PER_NU / (kms[dom] * 1e-3) / 1e12
-        roof = {"kernel": "k_atlas_rt", "bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": ach / fp64_peak if fp64_peak > 0 else None, "traffic": None,
-                "peak_source": "measured DFMA loop (atlasgpu_fp64_peak_tflops)",
-                "work": f"{FLOPS_PER_NU} FP64 flop per frequency x {CFG['numnu']}"}
-    else:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
-        byts = CFG["nlines"] * 16 + CFG["nrhox"] * CFG["numnu"] * 8
-        ach = byts / (kms[dom] * 1e-3) / 1e9
-        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": ach / peaks["hbm_gbs"], "traffic": None,
-                "work": "16 B per LINEDATA record + 8 B per XLINES element"}
+    # the single grey-start solar model (30,000 frequencies, 500,000 lines) on the batch path
+    b1 = atlas.AtlasBatch(ctx, ops, nslots=1, linedata=W["lines"], waveset=W["ws"], rcoset=W["rc"])
+    b1.load(0, 5777.0, 4.44, 1.5, 0.0, W["solar"], max_iter=CFG["max_iter"], tol_percent=CFG["tol_percent"])
+    b1.run()
+    b1.load(0, 5777.0, 4.44, 1.5, 0.0, W["solar"], max_iter=CFG["max_iter"], tol_percent=CFG["tol_percent"])
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    st1, it1, er1 = b1.run()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    single = {"ms": ev0.elapsed_time(ev1), "iterations": int(it1[0]), "max_flxerr_percent": float(er1[0]),
+              "start": "Eddington grey, Teff 5777 K, log g 4.44"}
+    b1.close()
+
+    syn = None
+    if rank == 0 and world == 1:
+        # C1: 20,000 atomic lines, 400-410 nm at R = 500,000, 72 depths
+        syn = {"c1": synthe_rates(ctx, ops, 20000, 400.0, 410.0, 0.0)}
+        if args.synthe_c3:
+            # C3: 20M lines (30 % molecular), 300-1000 nm at R = 500,000
+            syn["c3"] = synthe_rates(ctx, ops, 20000000, 300.0, 1000.0, 0.3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(W, ops, float(np.mean(iters)))
+        cpu = cpu_baseline(W, ops, plain["mean_iterations"] if plain else PLAIN_ITERS_PER_MODEL)
     if rank == 0:
         line = {"metric": "converged models/hr (dF/F<=1e-3)", "value": value, "unit": "models/hr",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded lines, surrogate populations/continuum)",
-                "config": dict(CFG, parallelism=f"replicas x{world}", l2="flushed between steps (256 MB write)"),
-                "iterations_to_converge": float(np.mean(iters)), "converged": int(conv_all.item()),
-                "kernel_ms_per_iteration": kms, "roofline": roof, "cpu_baseline": cpu,
-                "plain_fp64": plain, "vs_plain_fp64": (value / plain["value"]) if plain else None,
+                "data": "synthetic (seeded lines and stellar parameters, surrogate populations/continuum)",
+                "config": dict(CFG, parallelism=f"replicas x{world}", start="learned warm start, grey fallback"
+                               if learned else "grey (no trained network found)",
+                               l2="flushed between steps (256 MB write)"),
+                "converged_per_step": float(conv_all.item()) / args.steps / world,
+                "mean_iterations_per_model": float(np.mean(iters)), "mean_attempts": float(np.mean(attempts)),
+                "kernel_ms_per_model_iteration": per_model, "roofline": roof, "cpu_baseline": cpu,
+                "plain_fp64": plain, "vs_plain_fp64": (value / plain["value"]) if plain and plain["value"] else None,
+                "single_model": single, "synthe": syn,
                 "e2e": {"value": e2e_value, "unit": "models/hr", "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h)},
                 "gpu_launches": int(gpu_launches), "clocks": clk}
         print(json.dumps(line), flush=True)
-    model.close()
+    batch.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def synthe_rates(ctx, ops, nlines, wlbeg, wlend, mol_frac, seed=1):
+    """SYNTHE line opacity and spectrum on a synthetic case (CUDA events in the
+    library, second run of each precision): line-depth evaluations per second
+    of the line-opacity kernels (binning and continuum excluded) in mixed
+    precision and all-FP64, and the spectrum's two JOSH solves per lambda."""
+    from atlas12_b200 import _lib, synthe, synthetic
+    case = synthetic.synthe_case(nlines=nlines, wlbeg=wlbeg, wlend=wlend, seed=seed, mol_frac=mol_frac)
+    S = synthe.Synthe(ctx, ops)
+    out = {"lines": nlines, "depths": 72, "window_nm": [wlbeg, wlend], "resolu": case["resolu"]}
+    for name, prec in (("mixed", _lib.PREC_MIXED), ("fp64", _lib.PREC_FP64)):
+        ctx.set_precision(prec)
+        S.run(case)
+        ctx.enable_timing(True)
+        _, flux, _, _ = S.run(case)
+        ms = {k: ctx.kernel_ms(k) for k in ("synthe_core", "synthe_farfill", "synthe_farwing", "josh_spectrum")}
+        ctx.enable_timing(False)
+        line_ms = ms["synthe_core"] + ms["synthe_farfill"] + ms["synthe_farwing"]
+        out[name] = {"line_depth_evals_per_s": nlines * 72 / (line_ms * 1e-3), "line_opacity_ms": line_ms,
+                     "spectrum_ms": ms["josh_spectrum"], "kernel_ms": ms}
+        out["points"] = int(flux.size)
+    ctx.set_precision(_lib.PREC_MIXED)
+    out["mixed_vs_fp64_line_opacity"] = out["fp64"]["line_opacity_ms"] / out["mixed"]["line_opacity_ms"]
+    return out
 
 
 def cpu_baseline(W, ops_t, iters_gpu):

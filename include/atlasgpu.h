@@ -58,6 +58,20 @@ typedef struct {
   float code;     /* species code (carried, unused by the kernels) */
 } atlasgpu_lte_line;
 
+/* BIND(C) twin of the NLTE / complex-profile line record read from unit 19
+ * (nlte_line_t, mod_mklinelist.f90:43-63; read at atlas12_modules.f90:19992),
+ * padded to 64 bytes.  nbuff carries IWL (the integer log wavelength). */
+typedef struct {
+  double wlvac;            /* vacuum wavelength, nm */
+  float elo, gf;           /* lower level energy (cm^-1), CGF */
+  int32_t nblo, nbup;      /* NLTE level indices */
+  int32_t nelion, itype;   /* species index; line type (0, 3 normal; 2 skipped) */
+  int32_t ncon, nelionx;   /* continuum-edge index into CONTX, its species column */
+  float gammar, gammas, gammaw; /* damping / (4 pi nu) */
+  int32_t nbuff, lim;      /* IWL; wing extent index */
+  int32_t pad;
+} atlasgpu_nlte_line;
+
 /* SYNTHE log-lambda grid, synthe.f90:316-324 */
 typedef struct {
   double ratio, ratiolg, wbegin;
@@ -137,6 +151,24 @@ int atlasgpu_synthe_line_opacity_dev(atlasgpu_ctx *ctx, const atlasgpu_lte_line 
                                      const double *d_xne, const double *d_txnxn,
                                      const double *d_hckt, int maxprof, float *d_opacity);
 
+/* The NLTE / complex-profile list's normal-metal lines (TYPE 0, 3 and the He I
+ * fallthrough TYPE <= -3) of compute_line_opacity (synthe_module.f90:3167-3458,
+ * called per depth at synthe.f90:554): wings walked from the record's grid
+ * index nbuff, red wing tested before the add, blue wing after it, stop at
+ * continuum(i)*LINE_CUTOFF; blue of the continuum edge WCON = 1e7 /
+ * (CONTX(NCON,NELIONX) - EMERGE(J)) nothing is added, WCON..WTAIL (500 cm^-1
+ * redder) tapers linearly; lambdas shifted by (1 + velshift/c).  FP64 sums,
+ * added into opacity_inout [nrhox][length] (the LTE opacity matrix).
+ *   recs [n] (nbuff = grid index); continuum [nrhox][length];
+ *   xnfdop, dopple [nrhox][nspec]; xne, txnxn, hckt [nrhox];
+ *   contx [17][26]: CONTX(26,17) column-major.
+ * Hydrogen, autoionising and merged-continuum records are skipped. */
+int atlasgpu_synthe_nlte_opacity(atlasgpu_ctx *ctx, const atlasgpu_nlte_line *recs, int64_t n, int length,
+                                 int nrhox, double wbegin, double ratio, double wlend, double velshift_kms,
+                                 const float *continuum, const double *xnfdop, const double *dopple, int nspec,
+                                 const double *xne, const double *txnxn, const double *hckt, const double *contx,
+                                 float *opacity_inout);
+
 /* Spectrum: the SYNTHE wavelength loop (synthe.f90:698-718) with
  * setup_opacity_sv and process_wavelength_point (:797-902): per lambda two
  * JOSH(1,1) solves, continuum-only and continuum+line.  contabs/contscat
@@ -181,6 +213,24 @@ int atlasgpu_atlas_linop(atlasgpu_ctx *ctx, const int32_t *linedata, int64_t n, 
                          const double *txnxn, const double *hckt, const double *tabcont,
                          const int32_t *iwavetab, int nwave, const double *waveset, int numnu,
                          double *xlines_out, int64_t *lines_used);
+
+/* XLINOP's normal-line branch (TYPE 0 and 3, atlas12_modules.f90:20040-20174):
+ * the LINOP1 walk on unit-19 records with MAX_WING = 2000, LORENTZ_PREFAC =
+ * 0.5642 and the blue-wing cutoff at the continuum edge WCON = 1e7 /
+ * (CONTX(NCON,NELIONX) - EMERGE(J)), EMERGE(J) = RYDBERG_INF / NMERGE(J)**2,
+ * NMERGE = 1600 / XNE(J)**(2/15) (:19964-19977).  Adds into xlines_inout
+ * [numnu][kw] (RUN_RT_PASS calls it after LINOP1, :3893-3894).
+ *   recs [n], sorted by wavelength (the reference advances NU and NUCONT
+ *   monotonically and stops at the first line with NU >= NUMNU)
+ *   contx [16][25]: CONTX(25,16) column-major (XLINOP's edge table)
+ * TYPE 2 records are skipped as in the reference; records of the other
+ * types (hydrogen, autoionizing, merged continuum) are skipped and counted
+ * in n_other (may be NULL). */
+int atlasgpu_atlas_xlinop(atlasgpu_ctx *ctx, const atlasgpu_nlte_line *recs, int64_t n, int nrhox, int kw,
+                          const double *xnfdop, const double *dopple, int nspec, const double *xne,
+                          const double *txnxn, const double *hckt, const double *tabcont,
+                          const int32_t *iwavetab, int nwave, const double *waveset, int numnu,
+                          const double *contx, double *xlines_inout, int64_t *n_other);
 
 /* RUN_RT_PASS frequency loop (atlas12_modules.f90:3880-3951): per NU the
  * Planck terms, ALINE = XLINES*STIM, JOSH(1,0) (:18398-18776), the negative
@@ -255,6 +305,21 @@ int atlasgpu_model_set_structure(atlasgpu_ctx *ctx, atlasgpu_model *m, const dou
  * the reference runs one model per process. */
 int atlasgpu_model_set_params(atlasgpu_ctx *ctx, atlasgpu_model *m, double teff, double logg,
                               double vturb_kms, double mh);
+/* Frequency sharding of one model over several GPUs.  The reference's
+ * frequency loop (RUN_RT_PASS, atlas12_modules.f90:3905-3949) only adds into
+ * the TCORR/RADIAP/ROSS mode-2 accumulators, so it splits into contiguous
+ * ranges whose sums add; ROSS(3)/RADIAP(3)/TCORR(3) (atlas12c.f90:585-590)
+ * then run on the total.  set_shard restricts LINOP1 (XLINES) and the RT pass
+ * to NU_FIRST..NU_LAST (1-based, inclusive); set_sums_buffer makes the model
+ * write its sums [8*kw + 1] to, and finish from, a caller-owned device buffer
+ * (NULL: the model's own); iterate_begin enqueues one iteration up to the
+ * sums, iterate_end enqueues the finish, waits and returns max |FLXERR|.
+ * Between the two the caller adds the shards' sums (an all-reduce on the
+ * context stream). */
+int atlasgpu_model_set_shard(atlasgpu_ctx *ctx, atlasgpu_model *m, int nu_first, int nu_last);
+int atlasgpu_model_set_sums_buffer(atlasgpu_ctx *ctx, atlasgpu_model *m, double *d_sums);
+int atlasgpu_model_iterate_begin(atlasgpu_ctx *ctx, atlasgpu_model *m);
+int atlasgpu_model_iterate_end(atlasgpu_ctx *ctx, atlasgpu_model *m, double *maxerr);
 int atlasgpu_model_destroy(atlasgpu_ctx *ctx, atlasgpu_model *m);
 
 /* The RT-pass frequency loop for callers that cannot allocate device memory.

@@ -930,6 +930,215 @@ int64_t orc_atlas_linop1(const orc_atlas_tables_t *tb, const int32_t *linedata,
 }
 
 /* ======================================================================
+ * XLINOP, normal-line branch (TYPE 0 and 3), atlas12_modules.f90:19873-20174.
+ * The read loop advances NUCONT on IWL and NU on WLVAC (:20017-20031) and
+ * stops at the first record with NU >= NUMNU or WLVAC > WAVESET(NUHI);
+ * TYPE 2 is skipped (:20036-20038); the other types (hydrogen, autoionizing,
+ * merged continuum) are outside this restatement and skipped.  The walk is
+ * LINOP1's with MAX_WING = 2000, LORENTZ_PREFAC = 0.5642 (:19877-19879), and
+ * the blue wing and the whole depth cut at the continuum edge WCON
+ * (:20057-20060, 20074-20075).
+ * ==================================================================== */
+static void xlinop_wings(const orc_atlas_tables_t *tb, double center, double adamp, double dopwave,
+                         double wlvac, int nu, int numnu, const double *waveset, double tc, double wcon,
+                         double *xl, int kw) {
+  const int MAX_WING = 2000;
+  const double LORENTZ_PREFAC = 0.5642;
+  const double *H0 = tb->h0tab, *H1 = tb->h1tab, *H2 = tb->h2tab;
+  int iwmax = nu + MAX_WING < numnu ? nu + MAX_WING : numnu;
+  for (int iw = nu; iw <= iwmax; ++iw) {
+    double cv;
+    if (adamp > 0.20) {
+      cv = center * orc_voigt_kurucz((waveset[iw - 1] - wlvac) / dopwave, adamp, H0, H1, H2);
+    } else {
+      double vv = (waveset[iw - 1] - wlvac) / dopwave;
+      if (vv > 10.0) {
+        cv = center * LORENTZ_PREFAC * adamp / orc_powi(vv, 2);
+      } else {
+        int iv = (int)(vv * 200.0 + 1.5);
+        cv = center * ((H2[iv - 1] * adamp + H1[iv - 1]) * adamp + H0[iv - 1]);
+      }
+    }
+    xl[(size_t)(iw - 1) * kw] += cv;
+    if (cv < tc) break;
+  }
+  for (int i = 1; i <= MAX_WING; ++i) {
+    int iw = nu - i;
+    if (iw <= 0) break;
+    if (waveset[iw - 1] < wcon) break;
+    double cv;
+    if (adamp > 0.20) {
+      cv = center * orc_voigt_kurucz((wlvac - waveset[iw - 1]) / dopwave, adamp, H0, H1, H2);
+    } else {
+      double vv = (wlvac - waveset[iw - 1]) / dopwave;
+      if (vv > 10.0) {
+        cv = center * LORENTZ_PREFAC * adamp / orc_powi(vv, 2);
+      } else {
+        int iv = (int)(vv * 200.0 + 1.5);
+        cv = center * ((H2[iv - 1] * adamp + H1[iv - 1]) * adamp + H0[iv - 1]);
+      }
+    }
+    xl[(size_t)(iw - 1) * kw] += cv;
+    if (cv < tc) break;
+  }
+}
+
+int64_t orc_atlas_xlinop(const orc_atlas_tables_t *tb, const orc_nlte_line_t *recs, int64_t nrec,
+                         int nrhox, int kw, const double *xnfdop, const double *dopple, int nspec,
+                         const double *xne, const double *txnxn, const double *hckt,
+                         const double *tabcont, const int32_t *iwavetab, int nwave,
+                         const double *waveset, int numnu, const double *contx, double *xlines) {
+  const double RYDBERG_INF = 109737.31568157;
+  double emerge[KW_MAX];
+  for (int j = 0; j < nrhox; ++j) {
+    double nstark = 1600.0 / pow(xne[j], 2.0 / 15.0);
+    double nmerge = nstark;
+    emerge[j] = RYDBERG_INF / (nmerge * nmerge);
+  }
+  int ifj[KW_MAX + 2];
+  ifj[0] = 0;
+  int nucont = 1, nu = 1;
+  int64_t line;
+  for (line = 0; line < nrec; ++line) {
+    const orc_nlte_line_t *r = recs + line;
+    double wlvac = r->wlvac;
+    if (wlvac > waveset[numnu - 1]) return line;
+    double wlvac4 = wlvac;
+    int32_t iwl = r->nbuff;
+    while (iwl >= iwavetab[nucont - 1]) {
+      nucont = nucont + 1;
+      if (nucont > nwave + 1) {
+        nucont = nwave + 1;
+        break;
+      }
+    }
+    int stop = 0;
+    while (wlvac >= waveset[nu - 1]) {
+      nu = nu + 1;
+      if (nu >= numnu) {
+        stop = 1;
+        break;
+      }
+    }
+    if (stop) return line;
+    if (r->itype != 0 && r->itype != 3) continue;
+    int nelion = r->nelion;
+    if (nelion < 1 || nelion > nspec) continue;
+    double cgf = (double)r->gf, elo = (double)r->elo;
+    double gammar = (double)r->gammar, gammas = (double)r->gammas, gammaw = (double)r->gammaw;
+    int ncon = r->ncon;
+    const double *xdn = xnfdop + (size_t)(nelion - 1) * kw;
+    const double *dpn = dopple + (size_t)(nelion - 1) * kw;
+    const double *tcv = tabcont + (size_t)(nucont - 1) * kw;
+    for (int pass = 0; pass < 2; ++pass) {
+      /* pass 0: coarse depths 8, 16, ...; pass 1: the gated fine depths */
+      for (int K = 8; K <= nrhox; K += 8) {
+        int j0 = K, j1 = K;
+        if (pass == 0) ifj[K] = 0;
+        else {
+          if (ifj[K - 8] + ifj[K] == 0) continue;
+          j0 = K - 7;
+          j1 = K - 1;
+        }
+        for (int J = j0; J <= j1; ++J) {
+          double center = cgf * xdn[J - 1];
+          if (center < tcv[J - 1]) continue;
+          center = center * exp(-elo * hckt[J - 1]);
+          if (center < tcv[J - 1]) continue;
+          if (pass == 0) ifj[K] = 1;
+          double adamp = (gammar + gammas * xne[J - 1] + gammaw * txnxn[J - 1]) / dpn[J - 1];
+          double dopwave = dpn[J - 1] * wlvac4;
+          double wcon = 0.0;
+          if (ncon > 10) ncon = 0;
+          if (ncon > 0) wcon = 1.0e7 / (contx[(size_t)(r->nelionx - 1) * 25 + (ncon - 1)] - emerge[J - 1]);
+          if (wlvac < wcon) continue;
+          xlinop_wings(tb, center, adamp, dopwave, wlvac, nu, numnu, waveset, tcv[J - 1], wcon,
+                       xlines + (J - 1), kw);
+        }
+      }
+    }
+  }
+  return line;
+}
+
+/* ======================================================================
+ * SYNTHE compute_line_opacity, normal-metal branch (TYPE 0, 3 and the He I
+ * fallthrough TYPE <= -3), synthe_module.f90:3167-3458, in FP64.
+ * EMERGE keeps the reference's REAL(4) INGLIS/NMERGE (:3306-3311); the
+ * wavelength walk keeps its sequential products (:3429-3452): red wing
+ * test-before-add from MAX(1,NBUFF), blue wing add-then-test below NBUFF;
+ * points blueward of WCON are skipped, the WCON..WTAIL ramp tapers.
+ * ==================================================================== */
+void orc_synthe_nlte_opacity(const orc_nlte_line_t *recs, int64_t n, int length, int nrhox,
+                             double wbegin, double ratio, double wlend, double velshift_kms,
+                             const float *continuum, const double *xnfdop, const double *dopple,
+                             int nspec, const double *xne, const double *txnxn, const double *hckt,
+                             const double *contx, double *out) {
+  const double RYDBERG_INF = 109737.31568157, CLIGHT_KMS = 299792.458, CUTOFF = LINE_CUTOFF;
+  const double dopratio = 1.0 + velshift_kms / CLIGHT_KMS;
+  for (int j = 0; j < nrhox; ++j) {
+    float inglis = (float)(1600.0 / pow(xne[j], 2.0 / 15.0));
+    float nmerge = inglis - 1.5f;
+    double emerge = RYDBERG_INF / ((double)nmerge * (double)nmerge);
+    const float *cont = continuum + (size_t)j * length;
+    const double *xd = xnfdop + (size_t)j * nspec, *dp = dopple + (size_t)j * nspec;
+    double *buf = out + (size_t)j * length;
+    for (int64_t il = 0; il < n; ++il) {
+      const orc_nlte_line_t *r = recs + il;
+      int t = r->itype;
+      if (!(t == 0 || t == 3 || t <= -3)) continue;
+      int nel = r->nelion;
+      if (nel < 1 || nel > nspec) continue;
+      double wl = r->wlvac * dopratio;
+      int nbuff = r->nbuff;
+      double kappa0 = (double)r->gf * xd[nel - 1];
+      int ic = nbuff < 1 ? 1 : (nbuff > length ? length : nbuff);
+      double kapmin = (double)cont[ic - 1] * CUTOFF;
+      if (kappa0 < kapmin) continue;
+      kappa0 = kappa0 * exp(-(double)r->elo * hckt[j]);
+      if (kappa0 < kapmin) continue;
+      double wcon = 0.0, wtail = 0.0;
+      if (r->ncon > 0) {
+        double cx = contx[(size_t)(r->nelionx - 1) * 26 + (r->ncon - 1)];
+        wcon = 1.0e7 / (cx - emerge) * dopratio;
+        wtail = 1.0e7 / (cx - emerge - 500.0) * dopratio;
+      }
+      double adamp = ((double)r->gammar + (double)r->gammas * xne[j] + (double)r->gammaw * txnxn[j]) / dp[nel - 1];
+      double dopwl = dp[nel - 1] * wl;
+      if (wl <= wlend) {
+        int minred = nbuff > 1 ? nbuff : 1;
+        double wave = wbegin * orc_powi(ratio, minred - 1);
+        for (int ib = minred; ib <= length; ++ib) {
+          if (wave >= wcon) {
+            double v = fabs(wave - wl) / dopwl;
+            double kappa = kappa0 * orc_voigt_weideman(v, adamp);
+            if (wave < wtail) kappa = kappa * ((wave - wcon) / (wtail - wcon));
+            if (kappa < (double)cont[ib - 1] * CUTOFF) break;
+            buf[ib - 1] += kappa;
+          }
+          wave = wave * ratio;
+        }
+        if (minred == 1) continue;
+        if (wl < wbegin) continue;
+      }
+      int ib = length + 1 < nbuff ? length + 1 : nbuff;
+      int maxblue = ib - 1;
+      double wave = wbegin * orc_powi(ratio, ib - 1);
+      for (int i = 1; i <= maxblue; ++i) {
+        ib = ib - 1;
+        wave = wave / ratio;
+        if (wave < wcon) continue;
+        double v = fabs(wave - wl) / dopwl;
+        double kappa = kappa0 * orc_voigt_weideman(v, adamp);
+        if (wave < wtail) kappa = kappa * ((wave - wcon) / (wtail - wcon));
+        buf[ib - 1] += kappa;
+        if (kappa < (double)cont[ib - 1] * CUTOFF) break;
+      }
+    }
+  }
+}
+
+/* ======================================================================
  * ATLAS12 RUN_RT_PASS frequency loop with TCORR/RADIAP/ROSS mode 2,
  * atlas12_modules.f90:3880-3951, :2457-2522, :5072-5097, :5178-5190.
  * KAPP is replaced by the caller's per-frequency ACONT/SIGMAC/SCONT

@@ -136,6 +136,34 @@ int64_t orc_atlas_linop1(const orc_atlas_tables_t *tb, const int32_t *linedata,
                          int nwave, const double *waveset, int numnu,
                          double *xlines);
 
+/* ---- XLINOP normal-line branch (atlas12_modules.f90:19873-20174) ------ */
+typedef struct {
+  double wlvac;
+  float elo, gf;
+  int32_t nblo, nbup, nelion, itype, ncon, nelionx;
+  float gammar, gammas, gammaw;
+  int32_t nbuff, lim, pad;
+} orc_nlte_line_t;
+/* Adds the TYPE 0/3 records' wings into xlines [numnu][kw]; contx is
+ * CONTX(25,16) column-major.  Returns the number of records read. */
+int64_t orc_atlas_xlinop(const orc_atlas_tables_t *tb, const orc_nlte_line_t *recs, int64_t nrec,
+                         int nrhox, int kw, const double *xnfdop, const double *dopple, int nspec,
+                         const double *xne, const double *txnxn, const double *hckt,
+                         const double *tabcont, const int32_t *iwavetab, int nwave,
+                         const double *waveset, int numnu, const double *contx, double *xlines);
+
+/* ---- SYNTHE compute_line_opacity, normal-metal branch
+ *      (synthe_module.f90:3167-3458), FP64 restatement ------------------
+ * Adds the TYPE 0/3 (and He I, TYPE <= -3) records' opacity at every depth
+ * into out [nrhox][length] (double).  recs use nbuff as the grid index;
+ * continuum [nrhox][length] (float, the REAL(4) continuum); xnfdop, dopple
+ * [nrhox][nspec]; contx CONTX(26,17) column-major. */
+void orc_synthe_nlte_opacity(const orc_nlte_line_t *recs, int64_t n, int length, int nrhox,
+                             double wbegin, double ratio, double wlend, double velshift_kms,
+                             const float *continuum, const double *xnfdop, const double *dopple,
+                             int nspec, const double *xne, const double *txnxn, const double *hckt,
+                             const double *contx, double *out);
+
 /* ---- ATLAS RT pass, mode-2 integrals (atlas12_modules.f90:3880-3951) --- */
 typedef struct {
   double *rjmins, *rdabh, *rdiagj, *flxrad;  /* TCORR mode 2 */

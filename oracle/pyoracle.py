@@ -188,6 +188,15 @@ def _declare2(L):
                                    ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp, _dp, _dp, _ip,
                                    ctypes.c_int, _dp, ctypes.c_int, _dp]
     L.orc_atlas_linop1.restype = ctypes.c_int64
+    L.orc_atlas_xlinop.argtypes = [ctypes.POINTER(_AtlasTables), ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                                   ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp, _dp, _dp, _ip,
+                                   ctypes.c_int, _dp, ctypes.c_int, _dp, _dp]
+    L.orc_atlas_xlinop.restype = ctypes.c_int64
+    L.orc_synthe_nlte_opacity.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                          ctypes.POINTER(ctypes.c_float), _dp, _dp, ctypes.c_int, _dp, _dp, _dp,
+                                          _dp, _dp]
+    L.orc_synthe_nlte_opacity.restype = None
     L.orc_atlas_rt_pass.argtypes = [ctypes.POINTER(Ops), ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_void_p,
                                     ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double,
                                     ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Accum), _dp]
@@ -406,3 +415,45 @@ def ttaup(store, t, tau, grav, prad):
     L.orc_ttaup.argtypes = [ctypes.POINTER(_Tcorr)] + [ctypes.c_void_p] * 6 + [ctypes.c_int]
     L.orc_ttaup(ctypes.byref(s), _ptr(t), _ptr(tau), _ptr(ab), _ptr(pt), _ptr(po), _ptr(prad), n)
     return ab, pt, po
+
+
+# unit-19 NLTE / complex-profile record (nlte_line_t, mod_mklinelist.f90:43-63), padded to 64 bytes
+NLTE_LINE = np.dtype([("wlvac", "<f8"), ("elo", "<f4"), ("gf", "<f4"), ("nblo", "<i4"), ("nbup", "<i4"),
+                      ("nelion", "<i4"), ("itype", "<i4"), ("ncon", "<i4"), ("nelionx", "<i4"), ("gammar", "<f4"),
+                      ("gammas", "<f4"), ("gammaw", "<f4"), ("nbuff", "<i4"), ("lim", "<i4"), ("pad", "<i4")])
+assert NLTE_LINE.itemsize == 64
+
+
+def atlas_xlinop(h0, h1, h2, tablog, recs, atm, tabcont, iwavetab, waveset, contx, xlines=None):
+    """XLINOP's normal-line branch; adds into a copy of xlines [numnu, kw] (zeros when None).
+    contx: CONTX(25,16) as a numpy [16, 25] array (column-major view).  Returns (xlines, records read)."""
+    h0, h1, h2, tablog = (_d(v) for v in (h0, h1, h2, tablog))
+    tb = _AtlasTables(_ptr(h0), _ptr(h1), _ptr(h2), _ptr(tablog))
+    rec = np.ascontiguousarray(recs, NLTE_LINE)
+    xnfdop, dopple = _d(atm["xnfdop"]), _d(atm["dopple"])
+    nspec, kw = xnfdop.shape
+    nrhox = int(atm.get("nrhox", kw))
+    xne, txnxn, hckt = _d(atm["xne"]), _d(atm["txnxn"]), _d(atm["hckt"])
+    tabcont, waveset, cx = _d(tabcont), _d(waveset), _d(contx)
+    iw = np.ascontiguousarray(iwavetab, np.int32)
+    xl = np.zeros((waveset.size, kw)) if xlines is None else _d(xlines).copy()
+    nread = _lib2().orc_atlas_xlinop(ctypes.byref(tb), rec.ctypes.data_as(ctypes.c_void_p), rec.shape[0], nrhox, kw,
+                                     _ptr(xnfdop), _ptr(dopple), nspec, _ptr(xne), _ptr(txnxn), _ptr(hckt),
+                                     _ptr(tabcont), _ptr(iw, _ip), iw.size - 1, _ptr(waveset), waveset.size, _ptr(cx),
+                                     _ptr(xl))
+    return xl, nread
+
+
+def synthe_nlte_opacity(recs, length, wbegin, ratio, wlend, velshift_kms, continuum, atm, contx):
+    """compute_line_opacity's normal-metal branch in FP64: the contribution [nrhox, length] (double).
+    continuum [nrhox, length] float; atm: xnfdop, dopple [nrhox, nspec], xne, txnxn, hckt; contx [17, 26]."""
+    rec = np.ascontiguousarray(recs, NLTE_LINE)
+    cont = np.ascontiguousarray(continuum, np.float32)
+    xnfdop, dopple = _d(atm["xnfdop"]), _d(atm["dopple"])
+    nrhox, nspec = xnfdop.shape
+    out = np.zeros((nrhox, length))
+    _lib2().orc_synthe_nlte_opacity(rec.ctypes.data_as(ctypes.c_void_p), rec.shape[0], length, nrhox, wbegin, ratio,
+                                    wlend, velshift_kms, cont.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                    _ptr(xnfdop), _ptr(dopple), nspec, _ptr(_d(atm["xne"])), _ptr(_d(atm["txnxn"])),
+                                    _ptr(_d(atm["hckt"])), _ptr(_d(contx)), _ptr(out))
+    return out

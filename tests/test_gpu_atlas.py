@@ -154,3 +154,47 @@ def test_model_iteration_reduces_flux_error(gpu_ctx, tables):
     assert n == 12 and np.all(np.isfinite(hist))
     assert hist[-1] < 0.5 * hist[0], hist
     assert np.all(np.diff(s["t"]) > 0) and s["t"].min() >= 1200.0
+
+
+@pytest.mark.parametrize("prec,tol", [(_lib.PREC_FP64, 1e-9), (_lib.PREC_MIXED, 1e-6)])
+def test_xlinop_normal_branch_matches_oracle(po, gpu_ctx, tables, atlas_case, h_tables, prec, tol):
+    """XLINOP's normal-line branch on unit-19 records over a grid fine enough
+    that strong lines walk past LINOP1's 100 points (up to MAX_WING = 2000),
+    with continuum-edge cutoffs, TYPE 2 skips and other types counted.
+    Same tolerances and nonzero pattern as LINOP1."""
+    c = atlas_case
+    ws = np.geomspace(300.0, 600.0, 4000)
+    recs = synthetic.nlte_records(5000, 300.5, 599.5, seed=6, strong=0.1)
+    contx = synthetic.contx_table()
+    atm = dict(xnfdop=c["xnfdop"], dopple=c["dopple"], xne=c["xne"], txnxn=c["txnxn"], hckt=c["hckt"])
+    base = np.zeros((ws.size, 72))
+    base[::7, 3] = 1e-3  # XLINOP adds into the LINOP1 result
+    ref, nread = po.atlas_xlinop(*h_tables, po.build_tablog(), recs, atm, c["tabcont"], c["iw"], ws, contx, base)
+    nocut, _ = po.atlas_xlinop(*h_tables, po.build_tablog(), recs, atm, c["tabcont"], c["iw"], ws,
+                               np.zeros_like(contx), base)
+    assert nread > 4000
+    assert np.count_nonzero(ref != base) > 20000
+    assert np.sum(nocut) > np.sum(ref)  # the continuum-edge cutoff removed blue wings
+    # some walks are longer than LINOP1's 100 points
+    rows = np.nonzero(np.any(ref != base, axis=1))[0]
+    assert np.max(np.diff(rows)) < 50 and np.count_nonzero(np.any(ref != base, axis=1)) > 2000
+    A = atlas.Atlas(gpu_ctx, tables, *h_tables)
+    gpu_ctx.set_precision(prec)
+    try:
+        got, other = A.xlinop(recs, 72, c["xnfdop"], c["dopple"], c["xne"], c["txnxn"], c["hckt"], c["tabcont"],
+                              c["iw"], ws, contx, base)
+    finally:
+        gpu_ctx.set_precision(_lib.PREC_MIXED)
+    assert other == int(np.sum(recs["itype"] == 1))
+    np.testing.assert_array_equal(got != base, ref != base)
+    scale = np.maximum(np.abs(ref), 1e-300)
+    assert np.max(np.abs(got - ref) / scale) < tol
+
+
+def test_xlinop_rejects_unsorted_records(gpu_ctx, tables, atlas_case, h_tables):
+    c = atlas_case
+    recs = synthetic.nlte_records(100, 300.5, 599.5, seed=6)[::-1].copy()
+    A = atlas.Atlas(gpu_ctx, tables, *h_tables)
+    with pytest.raises(_lib.AtlasGPUError, match="not sorted"):
+        A.xlinop(recs, 72, c["xnfdop"], c["dopple"], c["xne"], c["txnxn"], c["hckt"], c["tabcont"], c["iw"],
+                 np.geomspace(300.0, 600.0, 400), synthetic.contx_table())

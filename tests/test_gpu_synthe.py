@@ -136,3 +136,56 @@ def test_full_c1_pipeline(po, gpu_ctx, tables):
     ref = po.synthe_line_opacity(po.FP64, lines, g["length"], case["atm"], cont, case["resolu"])[1]
     assert _kappa_err(op, ref, cont) <= 1e-5
     assert np.all(np.isfinite(flux)) and np.all(flux > 0)
+
+
+def _nlte_records(po, case, g, seed=8):
+    """NLTE-list records from the case's lines: all line types, continuum edges,
+    5 % of lines moved 0.3 nm blue and 5 % 0.3 nm red of the window."""
+    rng = np.random.default_rng(seed)
+    L = case["lines"]
+    n = L["wlvac"].size
+    wl = L["wlvac"] + np.where(rng.uniform(size=n) < 0.05, -0.3, 0.0) + np.where(rng.uniform(size=n) < 0.05, 0.3, 0.0)
+    order = np.argsort(wl)
+    r = np.zeros(n, _lib.NLTE_LINE)
+    r["wlvac"] = wl[order]
+    r["elo"] = L["elo"][order]
+    r["gf"] = L["cgf"][order]
+    r["nelion"] = L["nelion"][order]
+    r["itype"] = rng.choice([0, 3, -3, 2, -1, 1], n, p=[.6, .1, .1, .1, .05, .05])
+    has = rng.uniform(size=n) < 0.3
+    r["ncon"] = np.where(has, rng.integers(1, 11, n), 0)
+    r["nelionx"] = np.where(has, rng.integers(1, 18, n), 0)
+    for a, b in (("gammar", "gamrf"), ("gammas", "gamsf"), ("gammaw", "gamwf")):
+        r[a] = L[b][order]
+    r["nbuff"] = [po.nbuff(w, g["ratiolg"], g["ixwlbeg"]) for w in r["wlvac"]]
+    return r
+
+
+def test_nlte_normal_lines_match_fp64_oracle(po, gpu_ctx, tables, prepared):
+    """compute_line_opacity's normal-metal branch: GPU (FP64 sums, FP32
+    output) against the FP64 restatement, relative to kappa + kappa_cont
+    per bin (1e-6; the FP32 output rounding is ~6e-8)."""
+    p = prepared
+    case, g, cont = p["case"], p["grid"], p["cont"]
+    recs = _nlte_records(po, case, g)
+    assert (recs["nbuff"] < 1).any() and (recs["nbuff"] > g["length"]).any()
+    rng = np.random.default_rng(9)
+    contx = np.zeros((17, 26))
+    # edges (cm^-1) whose WCON = 1e7 / (CONTX - EMERGE) lands inside the 400-402 nm window
+    contx[:, :10] = 1.0e7 / rng.uniform(399.5, 402.5, (17, 10))
+    atm = case["atm"]
+    wlend = case["wlend"]
+    ref = po.synthe_nlte_opacity(recs, g["length"], g["wbegin"], g["ratio"], wlend, 2.5, cont, atm, contx)
+    nocut = po.synthe_nlte_opacity(recs, g["length"], g["wbegin"], g["ratio"], wlend, 2.5, cont, atm,
+                                   np.zeros_like(contx))
+    assert np.count_nonzero(ref) > 0.3 * ref.size and np.sum(nocut) > np.sum(ref)
+    syn = S.Synthe(gpu_ctx, tables)
+    got = syn.nlte_opacity(recs, g, wlend, cont, atm["xnfdop"], atm["dopple"], atm["xne"], atm["txnxn"], atm["hckt"],
+                           contx, np.zeros((72, g["length"]), np.float32), velshift_kms=2.5)
+    err = np.abs(got.astype(np.float64) - ref) / (ref + cont.astype(np.float64))
+    assert err.max() <= 1e-6, err.max()
+    # it adds into the LTE opacity it is given
+    base = np.full((72, g["length"]), 1.0e-3, np.float32)
+    got2 = syn.nlte_opacity(recs, g, wlend, cont, atm["xnfdop"], atm["dopple"], atm["xne"], atm["txnxn"],
+                            atm["hckt"], contx, base, velshift_kms=2.5)
+    np.testing.assert_allclose(got2.astype(np.float64) - 1.0e-3, ref, rtol=1e-5, atol=2e-10)
