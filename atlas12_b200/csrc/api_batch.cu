@@ -249,8 +249,9 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
   B->nlines = dsc->nlines;
   const int kw = B->kw, nb = nslots;
   const size_t stride = (size_t)kAcc * kw + 1;
-  // launch shapes: about four resident waves of RT groups over the whole batch
-  const int target = ctx->nsm * 3 * kRtGroups * 4;
+  // launch shapes: about 32 resident waves of RT groups over the whole batch, so
+  // that the per-frequency cost spread (sweeps, interchanges) evens out
+  const int target = ctx->nsm * 3 * kRtGroups * 32;
   const int groups_per_slot = std::max(1, (target + nb - 1) / nb);
   const int nu_per = std::max(1, (B->numnu + groups_per_slot - 1) / groups_per_slot);
   const int ng = (B->numnu + nu_per - 1) / nu_per;

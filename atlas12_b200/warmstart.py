@@ -98,26 +98,51 @@ def structure_targets(t, p, xne):
 
 
 class WarmStart:
-    """Trained network plus the output standardisation."""
+    """Trained network plus the output standardisation.
 
-    def __init__(self, mlp, ymean, ystd):
+    With residual = True (the default for training) the network predicts
+    log10 T and log10 P relative to the plain grey start of the same
+    parameters, which already carries most of their variation across the box;
+    log10 Ne is predicted absolute (the iteration recomputes it anyway)."""
+
+    def __init__(self, mlp, ymean, ystd, residual=False):
         self.mlp = mlp
         self.ymean = np.asarray(ymean, np.float64)
         self.ystd = np.asarray(ystd, np.float64)
+        self.residual = bool(residual)
+
+    @staticmethod
+    def _grey_logs(params):
+        g = [grey_start(teff, logg, mh) for teff, logg, mh, _ in np.atleast_2d(params)]
+        return np.array([np.log10(x["t"]) for x in g]), np.array([np.log10(x["p"]) for x in g])
 
     @classmethod
-    def fit(cls, ctx, params, t, p, xne, epochs=2000, batch=64, lr=1e-3, seed=1):
-        """Train on converged structures (each [n, 72]); returns (WarmStart, loss history)."""
+    def fit(cls, ctx, params, t, p, xne, epochs=2000, batch=64, lr=1e-3, seed=1, residual=True, lr_tail=None,
+            tail_epochs=0):
+        """Train on converged structures (each [n, 72]); returns (WarmStart, loss history).
+        A second phase of tail_epochs at lr_tail follows when given."""
         y = structure_targets(t, p, xne)
+        if residual:
+            gt, gp = cls._grey_logs(params)
+            y[:, :NRHOX] -= gt
+            y[:, NRHOX:2 * NRHOX] -= gp
         ymean, ystd = y.mean(0), np.maximum(y.std(0), 1e-3)
         mlp = MLP(ctx, seed=seed)
-        hist = mlp.train(encode_inputs(params), ((y - ymean) / ystd).astype(np.float32), epochs, batch, lr,
-                         seed + 1)
-        return cls(mlp, ymean, ystd), hist
+        x = encode_inputs(params)
+        yn = ((y - ymean) / ystd).astype(np.float32)
+        hist = mlp.train(x, yn, epochs, batch, lr, seed + 1)
+        if tail_epochs and lr_tail:
+            hist = np.concatenate([hist, mlp.train(x, yn, tail_epochs, batch, lr_tail, seed + 2)])
+        return cls(mlp, ymean, ystd, residual), hist
 
     def predict(self, params):
+        params = np.atleast_2d(params)
         y = self.mlp.forward(encode_inputs(params)).astype(np.float64) * self.ystd + self.ymean
         n = NRHOX
+        if self.residual:
+            gt, gp = self._grey_logs(params)
+            y[:, :n] += gt
+            y[:, n:2 * n] += gp
         return 10.0 ** y[:, :n], 10.0 ** y[:, n:2 * n], 10.0 ** y[:, 2 * n:]
 
     def start(self, teff, logg, mh, vturb):
@@ -131,14 +156,14 @@ class WarmStart:
 
     def save(self, path):
         np.savez(path, params=self.mlp.params(), shape=np.array(self.mlp.shape), ymean=self.ymean,
-                 ystd=self.ystd, box=BOX)
+                 ystd=self.ystd, box=BOX, residual=np.array(self.residual))
 
     @classmethod
     def load(cls, path, ctx):
         d = np.load(path)
         mlp = MLP(ctx, shape=tuple(int(s) for s in d["shape"]))
         mlp.set_params(d["params"])
-        return cls(mlp, d["ymean"], d["ystd"])
+        return cls(mlp, d["ymean"], d["ystd"], bool(d["residual"]) if "residual" in d.files else False)
 
 
 _ross_cache = {}
@@ -227,12 +252,22 @@ def main(argv=None):
         batch.close()
     elif a.cmd == "train":
         d = np.load(a.data)
-        ok = np.isfinite(d["err"]) & (d["err"] <= 0.1)
-        ws, hist = WarmStart.fit(ctx, d["params"][ok], d["t"][ok], d["p"][ok], d["xne"][ok], epochs=a.epochs,
-                                 lr=a.lr)
+        # converged models with a physical structure (the surface P of a remapped model can dip below 0)
+        ok = (np.isfinite(d["err"]) & (d["err"] <= 0.1) & np.all(d["t"] > 0, axis=1) & np.all(d["p"] > 0, axis=1)
+              & np.all(np.isfinite(d["xne"]), axis=1))
+        idx = np.where(ok)[0]
+        rng = np.random.default_rng(a.seed)
+        val = rng.permutation(idx)[: max(1, idx.size // 10)]
+        trn = np.setdiff1d(idx, val)
+        for name, use in (("validation split", trn), ("all", idx)):
+            ws, hist = WarmStart.fit(ctx, d["params"][use], d["t"][use], d["p"][use], d["xne"][use],
+                                     epochs=a.epochs, lr=a.lr, lr_tail=a.lr / 4, tail_epochs=a.epochs // 2)
+            tv, _, _ = ws.predict(d["params"][val])
+            dex = np.abs(np.log10(tv) - np.log10(d["t"][val]))
+            print(f"{name}: trained on {use.size} converged models, loss {hist[0]:.4g} -> {hist[-1]:.4g}; "
+                  f"held-out {val.size}: median max|dlog T| {np.median(dex.max(1)):.4f} dex", flush=True)
         ws.save(a.out)
-        print(f"trained on {int(ok.sum())} converged models; loss {hist[0]:.4g} -> {hist[-1]:.4g}, "
-              f"{time.time() - t0:.0f} s", flush=True)
+        print(f"{time.time() - t0:.0f} s", flush=True)
     else:
         ws = WarmStart.load(a.weights, ctx)
         batch = workload_batch(ctx, tables, a.slots)
@@ -241,8 +276,10 @@ def main(argv=None):
         np.savez(a.out, params=params, **{f"{k}_{q}": r[k][q] for k in r for q in r[k]})
         for k in r:
             c = np.isfinite(r[k]["err"])
-            print(f"{k}: {int(c.sum())}/{a.n} converged, mean iterations {r[k]['iters'][c].mean():.2f}, "
-                  f"total iterations {int(r[k]['iters'].sum())}", flush=True)
+            it = r[k]["iters"]
+            print(f"{k}: {int(c.sum())}/{a.n} converged, mean iterations {it[c].mean():.2f}, total iterations "
+                  f"{int(it.sum())}; within 30 iterations {int(np.sum(c & (it <= 30)))}, "
+                  f"iterations spent with a 30 cap {int(np.minimum(it, 30).sum())}", flush=True)
         batch.close()
     ctx.close()
 
