@@ -55,8 +55,10 @@ WARMSTART = os.path.join(ROOT, "atlas12_b200", "data", "warmstart_c2.npz")
 # solves 2*51^2, system build 2*51^2, J/H/K operators 4*51^2 + 2*51,
 # INTEG/MAP1/DERIV and the mode-2 sums ~ 110 per depth (72 depths)
 FLOPS_PER_NU = int(2 / 3 * 51 ** 3 + 8 * 51 ** 2 + 2 * 51 + 110 * 72)
-# DRAM bytes of one model's RT pass (read + write), ncu on the 30,000-frequency model
-RT_TRAFFIC_PER_MODEL = 56.2e6
+# DRAM bytes per model of one batched RT launch (ncu, 4-slot capture of this
+# workload): ACONT, SIGMAC, XLINES read (51.8 MB) plus the partial sums written
+# (4.1 MB per model at 32 slots; 27.7 MB at 4)
+RT_TRAFFIC_PER_MODEL = 55.9e6
 
 
 def parse():
@@ -68,6 +70,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 GPU comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--synthe-c3", action="store_true", help="also measure the 20M-line full-optical SYNTHE case")
+    ap.add_argument("--slots", type=int, default=None, help="batch slots (default: one per model of a step)")
     return ap.parse_args()
 
 
@@ -217,6 +220,8 @@ def run_ours(args):
     params, grey = W["params"], W["grey"]
     ctx = _lib.Context(local, _lib.PREC_MIXED, stream=stream.cuda_stream)
     starts, learned = warm_starts(ctx, params, grey)
+    if args.slots:
+        CFG["slots"] = args.slots
     batch = atlas.AtlasBatch(ctx, ops, nslots=CFG["slots"], linedata=W["lines"], waveset=W["ws"], rcoset=W["rc"])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -271,6 +276,8 @@ def run_ours(args):
     roof = {"kernel": "k_batch_rt (JOSH per frequency, FP64)", "bound": "fp64", "achieved": ach, "peak": fp64_peak,
             "unit": "TFLOP/s", "frac": ach / fp64_peak if fp64_peak > 0 else None,
             "traffic": RT_TRAFFIC_PER_MODEL * CFG["slots"],
+            "traffic_scaling": "ncu capture of a 4-slot launch (74.5 MB per model incl. 27.7 MB of partial sums), "
+                               "read traffic scaled by slots, partial sums at this batch's 4.1 MB per model",
             "peak_source": "measured DFMA loop on this GPU (atlasgpu_fp64_peak_tflops); MEASURED_PEAKS.json has no FP64 figure",
             "work": f"{FLOPS_PER_NU} FP64 flop per frequency x {CFG['numnu']} frequencies x {CFG['slots']} models per launch",
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_batch_rt launch (profiles/)"}
