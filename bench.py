@@ -78,7 +78,8 @@ def workload():
     from atlas12_b200 import surrogate, synthetic, warmstart
     ws, rc = synthetic.geometric_waveset(CFG["wl_lo"], CFG["wl_hi"], CFG["numnu"])
     lines = synthetic.atlas_lines(CFG["nlines"], ws[2], ws[-3], seed=CFG["line_seed"])
-    params = warmstart.sample_params(CFG["models_per_step"], CFG["param_seed"])
+    rank = int(os.environ.get("RANK", "0"))
+    params = warmstart.sample_params(CFG["models_per_step"], CFG["param_seed"] + rank)
     grey = [warmstart.grey_start(teff, logg, mh, CFG["nrhox"]) for teff, logg, mh, _ in params]
     solar = surrogate.grey_model(5777.0, 4.44, nrhox=CFG["nrhox"], ross=surrogate.RossTable())
     return dict(ws=ws, rc=rc, lines=lines, params=params, grey=grey, solar=solar)
@@ -284,7 +285,7 @@ def run_ours(args):
 
     # plain FP64 GPU path: the same models one at a time, FP64, grey start, per-launch host loop
     plain = None
-    if not args.no_plain:
+    if not args.no_plain and rank == 0:
         ctx.set_precision(_lib.PREC_FP64)
         model = atlas.AtlasModel(ctx, ops, teff=5777.0, logg=4.44, vturb=1.5, linedata=W["lines"], waveset=W["ws"],
                                  rcoset=W["rc"], start=W["solar"])
@@ -391,11 +392,13 @@ def synthe_rates(ctx, ops, nlines, wlbeg, wlend, mol_frac, seed=1):
     case = synthetic.synthe_case(nlines=nlines, wlbeg=wlbeg, wlend=wlend, seed=seed, mol_frac=mol_frac)
     S = synthe.Synthe(ctx, ops)
     out = {"lines": nlines, "depths": 72, "window_nm": [wlbeg, wlend], "resolu": case["resolu"]}
+    res = {}
     for name, prec in (("mixed", _lib.PREC_MIXED), ("fp64", _lib.PREC_FP64)):
         ctx.set_precision(prec)
         S.run(case)
         ctx.enable_timing(True)
-        _, flux, _, _ = S.run(case)
+        _, flux, _, op = S.run(case)
+        res[name] = (flux, op)
         ms = {k: ctx.kernel_ms(k) for k in ("synthe_core", "synthe_farfill", "synthe_farwing", "josh_spectrum")}
         ctx.enable_timing(False)
         line_ms = ms["synthe_core"] + ms["synthe_farfill"] + ms["synthe_farwing"]
@@ -404,6 +407,13 @@ def synthe_rates(ctx, ops, nlines, wlbeg, wlend, mol_frac, seed=1):
         out["points"] = int(flux.size)
     ctx.set_precision(_lib.PREC_MIXED)
     out["mixed_vs_fp64_line_opacity"] = out["fp64"]["line_opacity_ms"] / out["mixed"]["line_opacity_ms"]
+    # mixed precision against the all-FP64 GPU path (which matches the FP64 oracle to ~1e-12)
+    (fm, om), (f64, o64) = res["mixed"], res["fp64"]
+    cont = S.continuum(case["wledge"], case["continall"], synthe.synthe_grid(wlbeg, wlend, case["resolu"]))
+    out["mixed_error_vs_fp64"] = {
+        "kappa_line_max_rel_to_kappa_plus_cont": float(np.max(np.abs(om.astype(np.float64) - o64) /
+                                                              (o64.astype(np.float64) + cont))),
+        "flux_max_rel": float(np.max(np.abs(fm - f64) / np.abs(f64)))}
     return out
 
 
