@@ -115,6 +115,8 @@ SIGNATURES = {
     "atlasgpu_batch_run": (_I, [_P, _P, _I, _P, _P, _P]),
     "atlasgpu_batch_get": (_I, [_P, _P, _I, _P, _P, _P, _P, _P, _P, _P]),
     "atlasgpu_batch_nslots": (_I, [_P]),
+    "atlasgpu_batch_set_shape": (_I, [_P, _P, _I, _I]),
+    "atlasgpu_batch_get_shape": (_I, [_P, _P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "atlasgpu_batch_destroy": (_I, [_P, _P]),
 }
 

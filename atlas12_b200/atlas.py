@@ -284,6 +284,7 @@ class AtlasBatch:
         t, p, rx, tau, h0, h1, h2, ld = keep
         self.nrhox = nrhox
         self.nslots = int(nslots)
+        self.nlines = int(ld.shape[0])
         d = ModelDesc(5777.0, 4.44, 1.5, nrhox, _dp(t), _dp(p), _dp(rx), _dp(tau), _dp(self.waveset),
                       _dp(self.rcoset), self.waveset.size, _dp(self.cutwave), self.cutwave.size,
                       ld.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ld.shape[0], _dp(h0), _dp(h1), _dp(h2), 0.0)
@@ -298,6 +299,15 @@ class AtlasBatch:
 
     def step(self, n=1):
         self.ctx.call("atlasgpu_batch_step", self._h, int(n))
+
+    def set_shape(self, linop_ctas_per_sm, rt_waves):
+        """Launch shape of the batched LINOP1 and RT kernels (see atlas12_b200.autotune)."""
+        self.ctx.call("atlasgpu_batch_set_shape", self._h, int(linop_ctas_per_sm), int(rt_waves))
+
+    def shape(self):
+        a, b = ctypes.c_int(0), ctypes.c_int(0)
+        self.ctx.call("atlasgpu_batch_get_shape", self._h, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
 
     def poll(self):
         """(status, iterations done, last max |FLXERR|) per slot, and the number running."""

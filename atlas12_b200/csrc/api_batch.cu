@@ -150,6 +150,9 @@ struct atlasgpu_batch {
   RtArgs* ra = nullptr;
   unsigned long long* cnt = nullptr;
   int grid_linop = 1, grid_kapp = 1, blocks_rt = 1;
+  int linop_ctas_per_sm = 16, rt_waves = 32;  // launch shape (atlasgpu_batch_set_shape)
+  size_t partial_rows = 0;                    // allocated partial-sum rows per slot
+  std::vector<RtArgs> ra_host;                // per-slot RT arguments (rebuilt with the shape)
   size_t smem_rt = 0, smem_fin = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -205,6 +208,48 @@ int enqueue_batch(atlasgpu_ctx* ctx, atlasgpu_batch* B, bool timed) {
   return 0;
 }
 
+// Launch shape: LINOP1 CTAs per SM over the whole batch, and RT pair groups
+// sized for about rt_waves resident waves over the batch (each group takes a
+// contiguous run of one slot's frequencies).  Grows the partial-sum buffer
+// when a shape needs more rows, rewrites the per-slot RT arguments and drops
+// the captured graph.
+int apply_shape(atlasgpu_ctx* ctx, atlasgpu_batch* B, int linop_ctas_per_sm, int rt_waves) {
+  const int nb = B->nslots;
+  const size_t stride = (size_t)kAcc * B->kw + 1;
+  const int target = ctx->nsm * 3 * kRtGroups * rt_waves;
+  const int groups_per_slot = std::max(1, (target + nb - 1) / nb);
+  const int nu_per = std::max(1, (B->numnu + groups_per_slot - 1) / groups_per_slot);
+  const int ng = (B->numnu + nu_per - 1) / nu_per;
+  const int blocks = (ng + kRtGroups - 1) / kRtGroups;
+  const size_t rows = (size_t)blocks * kRtGroups;
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (rows > B->partial_rows) {
+    if (B->d.partial) cudaFree(B->d.partial);
+    B->d.partial = nullptr;
+    if (cudaMalloc((void**)&B->d.partial, (size_t)nb * rows * stride * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      B->partial_rows = 0;
+      return fail(ctx, ATLASGPU_ENOMEM, "batch: partial sums for %zu groups per slot", rows);
+    }
+    B->partial_rows = rows;
+  }
+  B->blocks_rt = blocks;
+  B->d.nwl = (int)rows;
+  B->grid_linop = std::max(1, ctx->nsm * linop_ctas_per_sm / nb);
+  B->linop_ctas_per_sm = linop_ctas_per_sm;
+  B->rt_waves = rt_waves;
+  for (int b = 0; b < nb; ++b) {
+    B->ra_host[b].nu_per_warp = nu_per;
+    B->ra_host[b].partial = B->d.partial + (size_t)b * rows * stride;
+  }
+  CK(cudaMemcpy(B->ra, B->ra_host.data(), nb * sizeof(RtArgs), cudaMemcpyHostToDevice));
+  if (B->gexec) cudaGraphExecDestroy(B->gexec);
+  if (B->graph) cudaGraphDestroy(B->graph);
+  B->gexec = nullptr;
+  B->graph = nullptr;
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -249,15 +294,6 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
   B->nlines = dsc->nlines;
   const int kw = B->kw, nb = nslots;
   const size_t stride = (size_t)kAcc * kw + 1;
-  // launch shapes: about 32 resident waves of RT groups over the whole batch, so
-  // that the per-frequency cost spread (sweeps, interchanges) evens out
-  const int target = ctx->nsm * 3 * kRtGroups * 32;
-  const int groups_per_slot = std::max(1, (target + nb - 1) / nb);
-  const int nu_per = std::max(1, (B->numnu + groups_per_slot - 1) / groups_per_slot);
-  const int ng = (B->numnu + nu_per - 1) / nu_per;
-  B->blocks_rt = (ng + kRtGroups - 1) / kRtGroups;
-  B->d.nwl = B->blocks_rt * kRtGroups;
-  B->grid_linop = std::max(1, ctx->nsm * 16 / nb);
   B->grid_kapp = std::max(1, ctx->nsm * 8 / nb);
   BatchDev& d = B->d;
   d.numnu = B->numnu;
@@ -274,7 +310,7 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
       (r = balloc(ctx, &d.rho, (size_t)nb * kw)) || (r = balloc(ctx, &d.cc, (size_t)nb * kw)) ||
       (r = balloc(ctx, &d.acont, nb * nnk)) || (r = balloc(ctx, &d.sigmac, nb * nnk)) ||
       (r = balloc(ctx, &d.xl, nb * nnk)) || (r = balloc(ctx, &d.tabcont, (size_t)nb * (B->nwave + 1) * kw)) ||
-      (r = balloc(ctx, &d.partial, (size_t)nb * d.nwl * stride)) || (r = balloc(ctx, &d.sum, nb * stride)) ||
+      (r = balloc(ctx, &d.sum, nb * stride)) ||
       (r = balloc(ctx, &d.hist, (size_t)nb * kHist)) || (r = balloc(ctx, &d.hsurf, nb * (size_t)B->numnu)) ||
       (r = balloc(ctx, &B->waveset, B->numnu)) ||
       (r = balloc(ctx, &B->rcoset, B->numnu)) || (r = balloc(ctx, &B->cutwave, B->nwave)) ||
@@ -319,14 +355,15 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
                       d.xne_eos + o, d.txnxn + o, d.hckt + o, d.tabcont + (size_t)b * (B->nwave + 1) * kw,
                       B->waveset, B->h0, B->h1, B->h2, B->hf, d.xl + on, nullptr, B->cnt};
     ra[b] = RtArgs{ctx->ops, B->numnu, B->nrhox, kw, B->waveset, B->rcoset, d.acont + on, d.sigmac + on, nullptr,
-                   d.xl + on, ms[b].rhox, ms[b].t, d.hkt + o, 0.0, nu_per, 1, kw,
-                   d.partial + (size_t)b * d.nwl * stride, d.hsurf + (size_t)b * B->numnu, nullptr};
+                   d.xl + on, ms[b].rhox, ms[b].t, d.hkt + o, 0.0, 1, 1, kw, nullptr,
+                   d.hsurf + (size_t)b * B->numnu, nullptr};
   }
+  B->ra_host = ra;
   CK(cudaMemcpyAsync(d.ctl, ctl.data(), nb * sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(d.ms, ms.data(), nb * sizeof(ModelState), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(d.R, R.data(), nb * sizeof(RossStore), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(B->la, la.data(), nb * sizeof(LinopArgs), cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(B->ra, ra.data(), nb * sizeof(RtArgs), cudaMemcpyHostToDevice, s));
+
   CK(cudaMemsetAsync(B->state, 0, (size_t)nb * kNState * kw * sizeof(double), s));
   CK(cudaMemsetAsync(d.xnfdop, 0, nb * nsk * sizeof(double), s));
   {
@@ -373,7 +410,26 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
     return r;
   }
   CK(cudaStreamSynchronize(s));
+  if ((r = apply_shape(ctx, B, B->linop_ctas_per_sm, B->rt_waves))) {
+    atlasgpu_batch_destroy(ctx, B);
+    return r;
+  }
   *out = B;
+  return 0;
+}
+
+int atlasgpu_batch_set_shape(atlasgpu_ctx* ctx, atlasgpu_batch* B, int linop_ctas_per_sm, int rt_waves) {
+  if (!ctx || !B || linop_ctas_per_sm < 1 || linop_ctas_per_sm > 64 || rt_waves < 1 || rt_waves > 256)
+    return fail(ctx, ATLASGPU_EINVAL, "batch_set_shape: linop CTAs per SM %d (1..64), RT waves %d (1..256)",
+                linop_ctas_per_sm, rt_waves);
+  cudaSetDevice(ctx->device);
+  return apply_shape(ctx, B, linop_ctas_per_sm, rt_waves);
+}
+
+int atlasgpu_batch_get_shape(atlasgpu_ctx* ctx, atlasgpu_batch* B, int* linop_ctas_per_sm, int* rt_waves) {
+  if (!ctx || !B) return fail(ctx, ATLASGPU_EINVAL, "batch_get_shape: null");
+  if (linop_ctas_per_sm) *linop_ctas_per_sm = B->linop_ctas_per_sm;
+  if (rt_waves) *rt_waves = B->rt_waves;
   return 0;
 }
 

@@ -217,7 +217,7 @@ def main(argv=None):
     network; evaluate: held-out iterations from the grey and the learned start.
 
     python -m atlas12_b200.warmstart generate --n 2000 --seed 11 --out models.npz
-    python -m atlas12_b200.warmstart train --data models.npz --out warmstart.npz
+    python -m atlas12_b200.warmstart train --data models.npz[,more.npz] --out warmstart.npz
     python -m atlas12_b200.warmstart evaluate --weights warmstart.npz --n 200 --seed 12 --out heldout.npz
     """
     import argparse
@@ -251,7 +251,8 @@ def main(argv=None):
               f"{time.time() - t0:.0f} s", flush=True)
         batch.close()
     elif a.cmd == "train":
-        d = np.load(a.data)
+        parts = [np.load(f) for f in a.data.split(",")]
+        d = {k: np.concatenate([q[k] for q in parts]) for k in ("params", "iters", "err", "t", "p", "xne")}
         # converged models with a physical structure (the surface P of a remapped model can dip below 0)
         ok = (np.isfinite(d["err"]) & (d["err"] <= 0.1) & np.all(d["t"] > 0, axis=1) & np.all(d["p"] > 0, axis=1)
               & np.all(np.isfinite(d["xne"]), axis=1))

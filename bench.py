@@ -224,6 +224,9 @@ def run_ours(args):
     if args.slots:
         CFG["slots"] = args.slots
     batch = atlas.AtlasBatch(ctx, ops, nslots=CFG["slots"], linedata=W["lines"], waveset=W["ws"], rcoset=W["rc"])
+    # launch shape chosen by the autotuner on these models (outside the timed region)
+    from atlas12_b200 import autotune
+    lc, rw, tuned = autotune.tune_batch(batch, params, grey)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def one_step(b=batch, st=starts, keep=False):
@@ -364,6 +367,7 @@ def run_ours(args):
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded lines and stellar parameters, surrogate populations/continuum)",
+                "launch_shape": {"linop_ctas_per_sm": lc, "rt_waves": rw, "autotune": tuned},
                 "config": dict(CFG, parallelism=f"replicas x{world}", start="learned warm start, grey fallback"
                                if learned else "grey (no trained network found)",
                                l2="flushed between steps (256 MB write)"),

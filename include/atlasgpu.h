@@ -390,6 +390,13 @@ int atlasgpu_batch_run(atlasgpu_ctx *ctx, atlasgpu_batch *b, int poll_every, int
 int atlasgpu_batch_get(atlasgpu_ctx *ctx, atlasgpu_batch *b, int slot, double *t, double *rhox,
                        double *p, double *xne, double *flxerr, double *hsurf, double *maxerr_hist);
 int atlasgpu_batch_nslots(atlasgpu_batch *b);
+/* Launch shape of the batched kernels (no reference counterpart): LINOP1 CTAs
+ * per SM over the whole batch (1..64, default 16) and the RT pass's frequency
+ * groups sized for about rt_waves resident waves over the batch (1..256,
+ * default 32).  Results do not depend on the shape beyond the grouping of the
+ * frequency sums.  The next step captures a new graph. */
+int atlasgpu_batch_set_shape(atlasgpu_ctx *ctx, atlasgpu_batch *b, int linop_ctas_per_sm, int rt_waves);
+int atlasgpu_batch_get_shape(atlasgpu_ctx *ctx, atlasgpu_batch *b, int *linop_ctas_per_sm, int *rt_waves);
 int atlasgpu_batch_destroy(atlasgpu_ctx *ctx, atlasgpu_batch *b);
 
 /* ---- learned warm start ----------------------------------------------

@@ -7,6 +7,8 @@ fixed-order reduction.  Tolerance: relative 1e-8 on T, P, RHOX and on each
 iteration's max |FLXERR| after 5 iterations (the frequency-sum grouping
 differs, the rest is the same FP64 arithmetic).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -92,4 +94,28 @@ def test_batch_rejects_bad_arguments(gpu_ctx, tables, small_grid):
     bad = dict(s, t=np.where(np.arange(s["t"].size) == 7, -1.0, s["t"]))
     with pytest.raises(_lib.AtlasGPUError, match="depth 8"):
         b.load(0, 5777.0, 4.44, 1.5, 0.0, bad)
+    b.close()
+
+
+def test_launch_shape_and_autotuner(gpu_ctx, tables, small_grid, singles, tmp_path, monkeypatch):
+    """Every launch shape gives the lone model's iteration (relative 1e-8);
+    the autotuner picks one of its candidates and caches it per workload."""
+    from atlas12_b200 import autotune
+    monkeypatch.setenv("XDG_CACHE_HOME", str(tmp_path))
+    ws, rc, lines = small_grid
+    b = atlas.AtlasBatch(gpu_ctx, tables, nslots=2, linedata=lines, waveset=ws, rcoset=rc)
+    starts = [_start(teff, logg, mh) for teff, logg, mh, _ in PARAMS]
+    for shape in ((8, 8), (32, 64), (1, 1)):
+        b.set_shape(*shape)
+        assert b.shape() == shape
+        res = b.run_queue(PARAMS, starts, max_iter=NIT, tol_percent=0.0)
+        for i, (r, s) in enumerate(zip(res, singles)):
+            np.testing.assert_allclose(r["t"], s["t"], rtol=1e-8, err_msg=f"shape {shape} model {i}")
+    lc, rw, entry = autotune.tune_batch(b, PARAMS, starts)
+    assert lc in autotune.LINOP_CANDIDATES and rw in autotune.RT_CANDIDATES and b.shape() == (lc, rw)
+    assert os.path.exists(autotune.cache_path())
+    b.set_shape(16, 32)
+    assert autotune.tune_batch(b, PARAMS, starts)[:2] == (lc, rw)  # from the cache
+    with pytest.raises(_lib.AtlasGPUError, match="RT waves"):
+        b.set_shape(16, 0)
     b.close()
