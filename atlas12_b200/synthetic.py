@@ -46,9 +46,9 @@ def synthe_continuum_tables(wledge, t, p, e=None):
     return (np.log10(ka + sgm).T.copy(), np.log10(ka).T.copy(), np.log10(sgm).T.copy())
 
 
-def synthe_atmosphere(teff=5777.0, logg=4.44, vturb=1.5, nrhox=72, ross=None):
+def synthe_atmosphere(teff=5777.0, logg=4.44, vturb=1.5, nrhox=72, ross=None, mh=0.0):
     m = sg.grey_model(teff, logg, nrhox=nrhox, ross=ross)
-    pop = sg.populations(m["t"], m["p"], vturb)
+    pop = sg.populations(m["t"], m["p"], vturb, mh=mh)
     t = m["t"]
     hkt = sg.HPLANCK / (sg.KBOL * t)
     hckt = hkt * sg.CLIGHT
@@ -87,14 +87,33 @@ def synthe_lines(n, wlbeg, wlend, seed=1, mol_frac=0.0):
 
 
 def synthe_case(nlines=20000, wlbeg=400.0, wlend=410.0, resolu=500000.0, seed=1, teff=5777.0,
-                logg=4.44, vturb=1.5, mol_frac=0.0, nrhox=72, ross=None):
+                logg=4.44, vturb=1.5, mol_frac=0.0, nrhox=72, ross=None, mh=0.0):
     """Complete SYNTHE input set (the small CPU-runnable case by default)."""
-    atm = synthe_atmosphere(teff, logg, vturb, nrhox, ross=ross)
+    atm = synthe_atmosphere(teff, logg, vturb, nrhox, ross=ross, mh=mh)
     wledge = synthe_edges(wlbeg, wlend)
     cont_all, cont_abs, cont_scat = synthe_continuum_tables(wledge, atm["t"], atm["p"], atm["eos"])
     lines = synthe_lines(nlines, wlbeg, wlend, seed=seed, mol_frac=mol_frac)
     return dict(atm=atm, wledge=wledge, continall=cont_all, contabs=cont_abs, contscat=cont_scat,
                 lines=lines, wlbeg=wlbeg, wlend=wlend, resolu=resolu)
+
+
+def grid_cases(n, seed=4, line_scale=1.0, lo=300.0, hi=1000.0):
+    """The batched-grid workload: n atmospheres with Teff U(3500, 8000) K,
+    log g U(1, 5), [M/H] U(-2, 0.5), each with its own window of U(5, 100) nm
+    inside lo..hi at R = 500,000 and U(0.2, 5)M lines (times line_scale),
+    30 % molecular.  Returns synthe_case dicts (seeded)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        teff, logg, mh = rng.uniform(3500.0, 8000.0), rng.uniform(1.0, 5.0), rng.uniform(-2.0, 0.5)
+        width = rng.uniform(5.0, 100.0)
+        wlbeg = rng.uniform(lo, hi - width)
+        nl = int(rng.uniform(0.2e6, 5.0e6) * line_scale)
+        c = synthe_case(nlines=nl, wlbeg=wlbeg, wlend=wlbeg + width, seed=seed * 1000 + k, teff=teff, logg=logg,
+                        mol_frac=0.3, mh=mh)
+        c["params"] = (teff, logg, mh)
+        out.append(c)
+    return out
 
 
 # ---------------------------------------------------------------- ATLAS12

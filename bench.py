@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--synthe-c3", action="store_true", help="also measure the 20M-line full-optical SYNTHE case")
     ap.add_argument("--slots", type=int, default=None, help="batch slots (default: one per model of a step)")
+    ap.add_argument("--synthe-grid", type=int, default=0,
+                    help="also time N atmospheres of the batched-grid SYNTHE workload, concurrent vs one at a time")
     return ap.parse_args()
 
 
@@ -357,6 +359,8 @@ def run_ours(args):
         if args.synthe_c3:
             # C3: 20M lines (30 % molecular), 300-1000 nm at R = 500,000
             syn["c3"] = synthe_rates(ctx, ops, 20000000, 300.0, 1000.0, 0.3)
+        if args.synthe_grid:
+            syn["grid"] = synthe_grid_rate(local, ops, args.synthe_grid)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -419,6 +423,36 @@ def synthe_rates(ctx, ops, nlines, wlbeg, wlend, mol_frac, seed=1):
                                                               (o64.astype(np.float64) + cont))),
         "flux_max_rel": float(np.max(np.abs(fm - f64) / np.abs(f64)))}
     return out
+
+
+def synthe_grid_rate(device, ops, n, lanes=8):
+    """Spectra of n atmospheres of the batched-grid workload (own windows of
+    5-100 nm at R = 500,000, 0.2-5M lines each): wall time through the public
+    API one after another on one context, and on `lanes` contexts (streams)
+    at once; spectra per hour both ways, and the largest difference between
+    the two runs' fluxes (same arithmetic: 0 up to atomics order)."""
+    from atlas12_b200 import synthe, synthe_batch, synthetic
+    cases = synthetic.grid_cases(n)
+    one = synthe_batch.SyntheBatch(device, ops, lanes=1)
+    many = synthe_batch.SyntheBatch(device, ops, lanes=lanes)
+    tiny = [synthetic.synthe_case(nlines=2000, wlbeg=500.0, wlend=500.5, seed=3)] * lanes
+    one.run(tiny[:1])
+    many.run(tiny)
+    t0 = time.perf_counter()
+    r1 = one.run(cases)
+    t1 = time.perf_counter()
+    r8 = many.run(cases)
+    t2 = time.perf_counter()
+    one.close()
+    many.close()
+    dflux = max(float(np.max(np.abs(a[1] - b[1]) / np.abs(b[1]))) for a, b in zip(r8, r1))
+    pts = int(sum(r[1].size for r in r1))
+    lines = int(sum(c["lines"]["wlvac"].size for c in cases))
+    return {"atmospheres": n, "points": pts, "lines": lines, "lanes": lanes,
+            "sequential_s": t1 - t0, "concurrent_s": t2 - t1,
+            "spectra_per_hr_sequential": n * 3600.0 / (t1 - t0), "spectra_per_hr_concurrent": n * 3600.0 / (t2 - t1),
+            "speedup": (t1 - t0) / (t2 - t1), "max_rel_flux_difference": dflux,
+            "timing": "host wall clock around the public API calls (host inputs, host outputs)"}
 
 
 def cpu_baseline(W, ops_t, iters_gpu, conv_fraction):

@@ -189,3 +189,24 @@ def test_nlte_normal_lines_match_fp64_oracle(po, gpu_ctx, tables, prepared):
     got2 = syn.nlte_opacity(recs, g, wlend, cont, atm["xnfdop"], atm["dopple"], atm["xne"], atm["txnxn"],
                             atm["hckt"], contx, base, velshift_kms=2.5)
     np.testing.assert_allclose(got2.astype(np.float64) - 1.0e-3, ref, rtol=1e-5, atol=2e-10)
+
+
+def test_concurrent_spectra_match_one_at_a_time(gpu_ctx, tables):
+    """Spectra of atmospheres with their own windows and line lists on four
+    concurrent contexts equal those computed one at a time (flux to 1e-6:
+    only the order of the FP64 atomic sums differs)."""
+    from atlas12_b200 import synthe_batch
+    cases = synthetic.grid_cases(6, seed=5, line_scale=0.002, lo=400.0, hi=520.0)
+    for c in cases:  # keep the windows short for the test
+        c["wlend"] = c["wlbeg"] + min(c["wlend"] - c["wlbeg"], 2.0)
+        keep = c["lines"]["wlvac"] < c["wlend"]
+        c["lines"] = {k: v[keep] for k, v in c["lines"].items()}
+    one = synthe_batch.SyntheBatch(0, tables, lanes=1)
+    many = synthe_batch.SyntheBatch(0, tables, lanes=4)
+    r1, r4 = one.run(cases), many.run(cases)
+    one.close()
+    many.close()
+    for a, b in zip(r4, r1):
+        np.testing.assert_array_equal(a[0], b[0])
+        np.testing.assert_allclose(a[1], b[1], rtol=1e-6)
+        np.testing.assert_allclose(a[2], b[2], rtol=1e-6)
