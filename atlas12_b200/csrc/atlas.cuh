@@ -543,18 +543,21 @@ static __device__ __forceinline__ void rt_body(const RtArgs& a) {
       const int j = g.r + c * RtG::N;
       if (j >= nr) break;
       const double ab = S.w.abtot[j], al = S.w.alpha[j], h = S.f.hnu[j];
-      acc[1][c] += S.dab[j] / ab * h * rcowt;                 // RDABH
+      const double rab = 1.0 / ab;
+      acc[1][c] += S.dab[j] * rab * h * rcowt;                // RDABH
       acc[0][c] += ab * S.f.jmins[j] * rcowt;                 // RJMINS
       acc[3][c] += h * rcowt;                                 // FLXRAD
       const double diagj = (j > 0 ? S.w.t1[j - 1] : 0.0) + S.w.t1[j];
       const double hk = a.hkt[j], tt = a.t[j];
-      const double dbdt = S.f.bnu[j] * freq * hk / tt / fmax(S.stim[j], 1.0e-30);
+      // dB/dT = BNU * freq * HKT / T / STIM (floored at 1e-30 for RDIAGJ, as the reference)
+      const double bft = S.f.bnu[j] * freq * hk / tt;
+      const double dbdt = bft / fmax(S.stim[j], 1.0e-30);
       acc[2][c] += ab * (diagj - 1.0) / (1.0 - al * diagj) * (1.0 - al) * dbdt * rcowt;  // RDIAGJ
       acc[4][c] += S.f.jnu[j] * rcowt;                        // RADEN
       acc[5][c] += h * rcowt;                                 // H_TOTAL
       acc[6][c] += ab * h * rcowt;                            // ACCRAD
-      const double dbdt2 = S.f.bnu[j] * freq * hk / tt / S.stim[j];
-      acc[7][c] += dbdt2 / ab * rcowt;                        // ABROSS
+      const double dbdt2 = (S.stim[j] >= 1.0e-30) ? dbdt : bft / S.stim[j];
+      acc[7][c] += dbdt2 * rab * rcowt;                       // ABROSS
     }
     pradk0 += S.f.knu1 * rcowt;
     g.sync();

@@ -411,30 +411,37 @@ __device__ inline void scatter_solve(WarpG& g, const JoshOps& ops, JoshWS& ws, d
   w_solvit(A, ws.xs, g.r);
 }
 
-// Pivot-row traffic in 16-byte words: the row owner stores [1/pivot, a[1..51]]
-// and every pending row reads it back, as 26 double2 (U rows are 16-byte
-// aligned: 52 doubles per row on a 16-byte aligned base).
+// Pivot-row traffic in 16-byte words: the row owner stores [1/pivot, a[1..]]
+// and every pending row reads it back as double2 words (U rows are 16-byte
+// aligned: 52 doubles per row on a 16-byte aligned base).  From step 26 on,
+// only the first 26 entries of a shifted row can be nonzero (columns i..50
+// and the rhs), so those steps move and update NW = 13 words instead of 26.
+template <int NW = (kNx + 1) / 2>
 __device__ __forceinline__ void store_pivot_row(double* ur, double rpiv, const double (&a)[kNx + 1]) {
   double2* u2 = reinterpret_cast<double2*>(ur);
   u2[0] = make_double2(rpiv, a[1]);
 #pragma unroll
-  for (int q = 1; q < (kNx + 1) / 2; ++q) u2[q] = make_double2(a[2 * q], a[2 * q + 1]);
+  for (int q = 1; q < NW; ++q) u2[q] = make_double2(a[2 * q], a[2 * q + 1]);
 }
 
-// a[t-1] = a[t] - l * ur[t] (t = 1..51), a[51] = 0, with l = a[0] * ur[0]
+// a[t-1] = a[t] - l * ur[t] (t = 1..2NW-1), l = a[0] * ur[0]; the entry
+// shifted in from beyond the stored words is zero (a[2NW-1] = 0)
+template <int NW = (kNx + 1) / 2>
 __device__ __forceinline__ void eliminate_shift(double (&a)[kNx + 1], const double* ur) {
   const double2* u2 = reinterpret_cast<const double2*>(ur);
   const double2 u0 = u2[0];
   const double l = a[0] * u0.x;
   a[0] = a[1] - l * u0.y;
 #pragma unroll
-  for (int q = 1; q < (kNx + 1) / 2; ++q) {
+  for (int q = 1; q < NW; ++q) {
     const double2 u = u2[q];
     a[2 * q - 1] = a[2 * q] - l * u.x;
     a[2 * q] = a[2 * q + 1] - l * u.y;
   }
-  a[kNx] = 0.0;
+  a[2 * NW - 1] = 0.0;
 }
+
+constexpr int kHalfStep = (kNx + 1) / 2;  // first step whose pending rows fit in half a row
 
 // Back substitution from the stored pivot rows U (row k: U[k][0] = 1/pivot,
 // U[k][t] = column k+t, the rhs at t = 51-k) by the group's first warp: lane
@@ -522,13 +529,17 @@ static __device__ __forceinline__ void scatter_solve(PairG& g, const JoshOps& op
     if (me) {
       double pv = a[0];
       if (fabs(pv) < kPivotTol) pv = copysign(kPivotTol, pv);
-      store_pivot_row(ur, 1.0 / pv, a);
+      if (i < kHalfStep) store_pivot_row(ur, 1.0 / pv, a);
+      else store_pivot_row<kHalfStep / 2>(ur, 1.0 / pv, a);
       pos = i;
       done = true;
     }
     g.sync();
     // (d, e) multiplier and trailing update of the pending rows, shifted left
-    if (!done) eliminate_shift(a, ur);
+    if (!done) {
+      if (i < kHalfStep) eliminate_shift(a, ur);
+      else eliminate_shift<kHalfStep / 2>(a, ur);
+    }
   }
   // the last pending row takes position n-1: column n-1 in a[0], rhs in a[1]
   if (!done) {
@@ -573,12 +584,14 @@ static __device__ __forceinline__ bool scatter_solve_nopivot(PairG& g, const Jos
       ws.piv[i] = a[0];
       double pv = a[0];
       if (fabs(pv) < kPivotTol) pv = copysign(kPivotTol, pv);
-      store_pivot_row(ur, 1.0 / pv, a);
+      if (i < kHalfStep) store_pivot_row(ur, 1.0 / pv, a);
+      else store_pivot_row<kHalfStep / 2>(ur, 1.0 / pv, a);
     }
     g.sync();
     if (own && g.r > i) {
       swap |= fabs(a[0]) > fabs(ws.piv[i]);
-      eliminate_shift(a, ur);
+      if (i < kHalfStep) eliminate_shift(a, ur);
+      else eliminate_shift<kHalfStep / 2>(a, ur);
     }
   }
   if (g.r == n - 1) {
@@ -729,15 +742,19 @@ __device__ inline int g_josh(G& g, const JoshOps& ops, const double* rhox, int n
   }
   // (IFSURF = 1 never reaches here with MAXJ != 1: it returned above.)
   // J - S and H on the 51-point grid, mapped back onto the first MAXJ depths
+  // four interleaved partial sums per product (instruction-level parallelism
+  // instead of one 51-long dependent chain; the grouping differs from the
+  // reference's sequential sum only at rounding level)
   for (int l = g.r; l < kNx; l += G::N) {
-    double xj = -ws.xs[l];
-    double xh = 0.0;
+    double sj[4] = {0.0, 0.0, 0.0, 0.0}, sh[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
     for (int mm = 0; mm < kNx; ++mm) {
-      xj = xj + ops.coefj[mm * kNx + l] * ws.xs[mm];
-      xh = xh + ops.coefh[mm * kNx + l] * ws.xs[mm];
+      const double x = ws.xs[mm];
+      sj[mm & 3] = sj[mm & 3] + ops.coefj[mm * kNx + l] * x;
+      sh[mm & 3] = sh[mm & 3] + ops.coefh[mm * kNx + l] * x;
     }
-    ws.xw[l] = xj;
-    ws.xsbar[l] = xh;  // XSBAR no longer needed: holds XH
+    ws.xw[l] = -ws.xs[l] + ((sj[0] + sj[1]) + (sj[2] + sj[3]));
+    ws.xsbar[l] = (sh[0] + sh[1]) + (sh[2] + sh[3]);  // XSBAR no longer needed: holds XH
   }
   g.sync();
   g_map1(g, ops.xtau, ws.xw, kNx, ws.taunu, F->jmins, maxj, ws.lidx);
