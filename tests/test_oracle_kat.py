@@ -203,3 +203,77 @@ def test_mlp_oracle_gradient_is_the_derivative():
         e[i] = h
         fd = (mlp_ref.loss_grad(p + e, x, t, shape)[0] - mlp_ref.loss_grad(p - e, x, t, shape)[0]) / (2 * h)
         assert abs(fd - g[i]) <= 1e-7 + 1e-6 * abs(g[i])
+
+
+def test_xlinop_normal_branch_agrees_with_linop1(po, tables):
+    """XLINOP's normal branch (atlas12_modules.f90:20040-20174) is LINOP1's
+    walk (:18236-18370) with MAX_WING 2000, LORENTZ_PREFAC 0.5642 and the
+    continuum-edge cutoff.  Fed the same lines (records holding LINOP1's own
+    decoded wavelength, CGF, ELO and damping), no edge, on a grid coarse
+    enough that no walk reaches 100 points, the two restatements must give
+    the same XLINES: equal where every point is tabulated, within the two
+    Lorentz constants' ratio (1.8e-5) where the far-wing formula is used."""
+    from atlas12_b200 import atlas, surrogate, synthetic
+    h = po.tabvoigt(tables["tabvi"], tables["tabh1"])
+    tl = po.build_tablog()
+    m = surrogate.grey_model(5777.0, 4.44)
+    pop = surrogate.populations(m["t"], m["p"], 1.5, surrogate.ATLAS_LINE_POP)
+    nr = 72
+    xnfdop, dopple = np.zeros((270, nr)), np.ones((270, nr))
+    xd = np.where(pop["dopple"] > 0, pop["xnfp"] / np.maximum(pop["dopple"], 1e-300) / pop["rho"][:, None], 0.0)
+    ns = min(270, pop["xnfp"].shape[1])
+    xnfdop[:ns] = xd[:, :ns].T
+    dopple[:ns] = np.where(pop["dopple"][:, :ns].T > 0, pop["dopple"][:, :ns].T, 1.0)
+    t = m["t"]
+    hkt = surrogate.HPLANCK / (surrogate.KBOL * t)
+    hckt = hkt * surrogate.CLIGHT
+    txnxn = (pop["nh"] * (1 - pop["xh"]) + 0.42 * 0.085 * pop["nh"]) * (t / 1e4) ** 0.3
+    ws, _ = synthetic.geometric_waveset(9.0, 160000.0, 3000)
+    cut = atlas.cutoff_grid()
+    iw = atlas.iwavetab(cut)
+    ka, sg = surrogate.continuum_opacity(cut, t, m["p"], pop)
+    stim = 1.0 - np.exp(-(surrogate.CLIGHT_NMS / cut)[:, None] * hkt[None, :])
+    tab = (ka + sg) * atlas.LINE_CUTOFF / stim
+    tab[cut <= ws[0]] = 1e10 * atlas.LINE_CUTOFF / stim[cut <= ws[0]]
+    tabcont = np.vstack([tab, tab[-1:]])
+    ld = synthetic.atlas_lines(2000, ws[2], ws[-3], seed=4)
+    atm = dict(xnfdop=xnfdop, dopple=dopple, xne=pop["xne"], txnxn=txnxn, hckt=hckt)
+    # the same lines as unit-19 records, with LINOP1's decoding (:18176-18253)
+    ratiolg = np.log(1.0 + 1.0 / 2000000.0)
+    lo16 = (ld[:, 1:] & 0xFFFF).astype(np.uint16).view(np.int16)
+    hi16 = ((ld[:, 1:].view(np.uint32) >> 16) & 0xFFFF).astype(np.uint16).view(np.int16)
+    tab_of = lambda i16: tl[i16.astype(np.int64) + 32768]
+    wl = np.exp(ld[:, 0] * ratiolg)
+    four_pi_c_inv = 1.0 / (4.0 * np.pi * surrogate.CLIGHT_NMS)
+    r = np.zeros(ld.shape[0], po.NLTE_LINE)
+    r["wlvac"] = wl
+    r["nbuff"] = ld[:, 0]
+    r["nelion"] = np.abs(lo16[:, 0] // 10)
+    r["itype"] = 0
+    # REAL(4) record fields: compare against LINOP1 fed the same rounded values
+    cgf = (0.026538 / np.sqrt(np.pi) / surrogate.CLIGHT_NMS * wl * tab_of(lo16[:, 1])).astype(np.float32)
+    elo = tab_of(hi16[:, 0]).astype(np.float32)
+    gr = (tab_of(hi16[:, 1]) * wl * four_pi_c_inv).astype(np.float32)
+    gs = (tab_of(lo16[:, 2]) * wl * four_pi_c_inv).astype(np.float32)
+    gw = (tab_of(hi16[:, 2]) * wl * four_pi_c_inv).astype(np.float32)
+    r["gf"], r["elo"], r["gammar"], r["gammas"], r["gammaw"] = cgf, elo, gr, gs, gw
+    # keep the lines whose every wing walk stays inside LINOP1's 100 points
+    nul = np.searchsorted(ws, wl, side="right") + 1
+    keep = []
+    for i in range(ld.shape[0]):
+        rows = np.nonzero(po.atlas_xlinop(*h, tl, r[i:i + 1], atm, tabcont, iw, ws, np.zeros((16, 25)))[0].any(1))[0]
+        if rows.size == 0 or (rows.max() + 1 - nul[i] < 100 and nul[i] - (rows.min() + 1) < 100):
+            keep.append(i)
+    keep = np.array(keep)
+    assert keep.size > 0.8 * ld.shape[0]
+    ld, r = ld[keep], r[keep]
+    ref, _ = po.atlas_linop1(*h, tl, ld, atm, tabcont, iw, ws)
+    got, nread = po.atlas_xlinop(*h, tl, r, atm, tabcont, iw, ws, np.zeros((16, 25)))
+    assert nread == ld.shape[0]
+    nz = ref != 0
+    assert np.array_equal(nz, got != 0) and nz.sum() > 1000
+    # besides the Lorentz constants (0.5642 vs 1/sqrt(pi): 1.8e-5) only the
+    # REAL(4) rounding of the record fields differs
+    rel = np.abs(got[nz] - ref[nz]) / ref[nz]
+    assert rel.max() < 2.0e-5, rel.max()
+    assert np.median(np.abs(rel - (0.5642 * np.sqrt(np.pi) - 1.0))) < 1e-6
