@@ -45,7 +45,7 @@ sys.path.insert(0, ROOT)
 # it converges, measured on B200 by this bench's plain_fp64 arm; they turn the
 # reference arm's per-iteration time into converged models/hr
 PLAIN_ITERS_PER_MODEL = 29.6
-PLAIN_CONVERGED_FRACTION = 3.0 / 32.0
+PLAIN_CONVERGED_FRACTION = 3.0 / 32.0  # measured: 3 of the 32 within 30 iterations
 CFG = dict(workload="atlas12-opacity-sampling model set", numnu=30000, wl_lo=9.0, wl_hi=160000.0, nrhox=72,
            nlines=500000, line_seed=2, models_per_step=32, param_seed=13,
            params="Teff U(3500,8000) K, log g U(1,5), [M/H] U(-2,0.5), vturb U(0.5,3) km/s", tol_percent=0.1,
