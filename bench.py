@@ -56,9 +56,9 @@ WARMSTART = os.path.join(ROOT, "atlas12_b200", "data", "warmstart_c2.npz")
 # INTEG/MAP1/DERIV and the mode-2 sums ~ 110 per depth (72 depths)
 FLOPS_PER_NU = int(2 / 3 * 51 ** 3 + 8 * 51 ** 2 + 2 * 51 + 110 * 72)
 # DRAM bytes per model of one batched RT launch (ncu, 4-slot capture of this
-# workload): ACONT, SIGMAC, XLINES read (51.8 MB) plus the partial sums written
-# (4.1 MB per model at 32 slots; 27.7 MB at 4)
-RT_TRAFFIC_PER_MODEL = 55.9e6
+# workload at the tuned shape): ACONT, SIGMAC, XLINES read (52.7 MB) plus the
+# partial sums written (8.1 MB per model at 32 slots and 64 waves)
+RT_TRAFFIC_PER_MODEL = 60.8e6
 
 
 def parse():
@@ -282,8 +282,8 @@ def run_ours(args):
     roof = {"kernel": "k_batch_rt (JOSH per frequency, FP64)", "bound": "fp64", "achieved": ach, "peak": fp64_peak,
             "unit": "TFLOP/s", "frac": ach / fp64_peak if fp64_peak > 0 else None,
             "traffic": RT_TRAFFIC_PER_MODEL * CFG["slots"],
-            "traffic_scaling": "ncu capture of a 4-slot launch (74.5 MB per model incl. 27.7 MB of partial sums), "
-                               "read traffic scaled by slots, partial sums at this batch's 4.1 MB per model",
+            "traffic_scaling": "ncu capture of a 4-slot launch (90.2 MB per model incl. 37.5 MB of partial sums), "
+                               "read traffic scaled by slots, partial sums at this batch's 8.1 MB per model",
             "peak_source": "measured DFMA loop on this GPU (atlasgpu_fp64_peak_tflops); MEASURED_PEAKS.json has no FP64 figure",
             "work": f"{FLOPS_PER_NU} FP64 flop per frequency x {CFG['numnu']} frequencies x {CFG['slots']} models per launch",
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_batch_rt launch (profiles/)"}
