@@ -118,9 +118,25 @@ SIGNATURES = {
     "atlasgpu_batch_set_shape": (_I, [_P, _P, _I, _I]),
     "atlasgpu_batch_get_shape": (_I, [_P, _P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "atlasgpu_batch_destroy": (_I, [_P, _P]),
+    "atlasgpu_atlas_select_tables": (_I, [_P, _I, _I, _P, _I, _P, _P, _P, _P, _I]),
+    "atlasgpu_atlas_selectlines": (_I, [_P, _I, _P, _I64, ctypes.c_void_p, _P, _I64, ctypes.POINTER(_I64)]),
+    "atlasgpu_atlas_selectlines_dev": (_I, [_P, _I, _P, _I64, ctypes.c_void_p, _P, _I64, ctypes.POINTER(_I64)]),
 }
 
 SLOT_IDLE, SLOT_RUNNING, SLOT_CONVERGED, SLOT_NONFINITE, SLOT_CAPPED = 0, 1, 2, 3, 4
+
+# SELECTLINES database kinds (ATLASGPU_SEL_*) and their record formats
+SEL_LOWPRED, SEL_LOWOBS, SEL_HI, SEL_DIATOMIC, SEL_TIO, SEL_H2O, SEL_H3PLUS = range(1, 8)
+MOL2_REC = np.dtype([("wl", "<f4"), ("gflog", "<f4"), ("e1", "<f4"), ("e2", "<f4"), ("code", "<i4"),
+                     ("iso", "<i4"), ("gr", "<i4"), ("label", "<i4")])
+assert MOL2_REC.itemsize == 32
+H2O_REC = np.dtype([("iwl", "<i4"), ("ielo", "<i2"), ("igflog", "<i2")])
+assert H2O_REC.itemsize == 8
+
+
+class SelectState(ctypes.Structure):
+    """atlasgpu_select_state (include/atlasgpu.h)."""
+    _fields_ = [("nu", ctypes.c_int32), ("igr", ctypes.c_int32), ("freq", ctypes.c_double)]
 BATCH_MAX_ITER = 256
 
 _DP = ctypes.POINTER(ctypes.c_double)

@@ -9,9 +9,7 @@
 
 using namespace atlasgpu;
 
-namespace {
-
-constexpr int kTabN = 2001;
+namespace atlasgpu {
 
 int ensure_tablog(atlasgpu_ctx* ctx, double** out) {
   double* d;
@@ -28,6 +26,12 @@ int ensure_tablog(atlasgpu_ctx* ctx, double** out) {
   *out = d;
   return 0;
 }
+
+}  // namespace atlasgpu
+
+namespace {
+
+constexpr int kTabN = 2001;
 
 }  // namespace
 

@@ -25,6 +25,12 @@ struct atlasgpu_ctx {
   bool ops_set = false;
   int nsm = 148;
   size_t smem_optin = 0;
+  // SELECTLINES tables (atlasgpu_atlas_select_tables)
+  bool sel_ready = false;
+  int sel_nwave = 0, sel_nspec = 0;
+  double sel_hckt_last = 0.0;
+  std::vector<double> sel_freqtab;   // CLIGHT_NMS / WAVETAB(k)
+  std::vector<int16_t> sel_igrtab;   // H2O's IGR after advancing past bin k
 };
 
 namespace atlasgpu {
@@ -133,6 +139,9 @@ inline std::vector<float4> pack_voigt_f32(const double* h0, const double* h1, co
   for (int i = 0; i < n; ++i) v[i] = make_float4((float)h0[i], (float)h1[i], (float)h2[i], 0.0f);
   return v;
 }
+
+// TABLOG (atlas12_modules.f90:2083-2086) for every INTEGER(2), index I + 32768, on the context
+int ensure_tablog(atlasgpu_ctx* ctx, double** out);
 
 struct AtlasLine;
 int atlas_prep_lines(atlasgpu_ctx* ctx, const int32_t* d_ld, const int32_t* h_ld, int64_t n,

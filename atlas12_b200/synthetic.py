@@ -212,3 +212,107 @@ def geometric_waveset(wl_lo=9.0, wl_hi=160000.0, numnu=30000):
     rc[1:-1] = (f[:-2] - f[2:]) * 0.5
     rc[-1] = (f[-2] + f[-1]) * 0.25
     return ws, rc
+
+
+# ------------------------------------------------------------ SELECTLINES
+def selectlines_tables(wavetab, nspec=1006, kw=80, nrhox=72, seed=11, dead_frac=0.15, faint_frac=0.03):
+    """XNFDOP [nspec, kw], HCKT [nrhox], TABCONT [nwave+1, kw] for SELECTLINES.
+
+    XNFDOPMAX(e, nu) comes out near FREQ(nu) * 10**(3.8 + N(0, 1)), so lines of
+    log gf ~ -2 straddle the CENRATIO = 1 cut; a fraction of the species have
+    no population (XNFDOPMAX = 0) and a few a vanishing one (<= 1e-37).
+    Depths past nrhox hold values that would dominate the maximum if read."""
+    rng = np.random.default_rng(seed)
+    wavetab = np.asarray(wavetab, np.float64)
+    nwave = wavetab.size
+    freq = 2.99792458e17 / np.append(wavetab, wavetab[-1])
+    j = np.arange(kw)
+    h = 0.3 * np.sin(0.37 * j)
+    d = -0.2 * np.cos(0.21 * j)
+    c = -np.log10(freq) + rng.normal(0.0, 0.3, nwave + 1)
+    tabcont = 10.0 ** (c[:, None] + d[None, :])
+    s = 3.8 + rng.normal(0.0, 1.0, nspec) - np.max((h - d)[:nrhox])
+    s[[894, 939]] = 5.6  # TiO and H2O (log gf ~ -4)
+    xnfdop = 10.0 ** (s[:, None] + h[None, :])
+    dead = rng.uniform(size=nspec) < dead_frac
+    dead[[894, 939]] = False
+    xnfdop[dead] = 0.0
+    faint = (rng.uniform(size=nspec) < faint_frac) & ~dead
+    faint[[894, 939]] = False
+    xnfdop[faint] = 1.0e-60
+    xnfdop[:, nrhox:] = 1.0e300
+    tabcont[:, nrhox:] = 1.0e-300
+    t = np.linspace(4000.0, 12000.0, nrhox)
+    hckt = 1.4387773538277204 / t
+    return xnfdop, hckt, tabcont
+
+
+def _wl_iwl(rng, n, lo, hi, sort=True):
+    ratiolg = np.log(1.0 + 1.0 / 2000000.0)
+    wl = np.exp(rng.uniform(np.log(lo), np.log(hi), n))
+    if sort:
+        wl = np.sort(wl)
+    return (np.log(wl) / ratiolg + 0.5).astype(np.int64)
+
+
+def selectlines_records(kind, n, wavetab, seed=12, shuffle_frac=0.0, nspec=1006, bad_frac=0.0):
+    """Seeded records of one SELECTLINES database kind (atlas12_b200._lib.SEL_*).
+
+    LINEREC kinds span WAVETAB (a few below its first bin and past its last),
+    with log gf ~ N(-2, 1.5), E ~ U(0, 64500) cm-1 and random species; MOL2 and
+    H2O records mimic the TiO and H2O lists.  shuffle_frac swaps that fraction
+    of records with a random other one (the NU advance then sees IWL go back);
+    bad_frac plants NELION values outside 1..nspec (LINEREC kinds)."""
+    from ._lib import SEL_DIATOMIC, SEL_TIO, SEL_H2O, SEL_H3PLUS, MOL2_REC, H2O_REC
+    rng = np.random.default_rng(seed)
+    lo, hi = float(wavetab[0]) * 0.97, float(wavetab[-1]) * 1.02
+    if kind == SEL_TIO:
+        r = np.zeros(n, MOL2_REC)
+        r["wl"] = np.sort(np.exp(rng.uniform(np.log(300.0), np.log(5000.0), n))).astype(np.float32)
+        r["gflog"] = rng.normal(-4.0, 1.2, n).astype(np.float32)
+        r["e1"] = rng.uniform(0.0, 30000.0, n).astype(np.float32)
+        r["e2"] = (r["e1"] + rng.normal(0.0, 3000.0, n)).astype(np.float32)
+        r["code"] = np.where(rng.uniform(size=n) < 0.85, 822, rng.choice([606, 101, 823], n))
+        r["iso"] = np.where(rng.uniform(size=n) < 0.9, rng.integers(46, 51, n), rng.choice([45, 51], n))
+        r["gr"] = np.where(rng.uniform(size=n) < 0.5, 0, (100 * rng.normal(8.0, 0.4, n)).astype(np.int32))
+        r["label"] = rng.integers(0, 2, n)
+        bad = rng.uniform(size=n) < 0.002
+        r["wl"][bad] = np.where(rng.uniform(size=bad.sum()) < 0.5, 0.0, -1.0).astype(np.float32)
+        rec = r
+    elif kind == SEL_H2O:
+        r = np.zeros(n, H2O_REC)
+        r["iwl"] = _wl_iwl(rng, n, 500.0, min(hi, 1.0e5))
+        mag = rng.integers(1, 30000, n)
+        r["ielo"] = np.where(rng.uniform(size=n) < 0.5, mag, -mag).astype(np.int16)
+        g = np.clip(np.rint(16384 + 1000 * rng.normal(-4.0, 1.5, n)), 1, 32767).astype(np.int32)
+        r["igflog"] = np.where(rng.uniform(size=n) < 0.5, g, -g).astype(np.int16)
+        rec = r
+    else:
+        iwl = _wl_iwl(rng, n, lo, hi)
+        if kind == SEL_DIATOMIC:
+            # the diatomic species codes SELECTLINES knows (MOLCODES)
+            codes = np.array([8410, 8411, 8460, 8461, 8470, 8471, 8480, 8481, 8482, 8510, 8511, 8512, 8530, 8531,
+                              8532, 8580, 8581, 8582, 8583, 8584, 8620, 8621, 8622, 8623, 8640, 8641, 8642, 8643,
+                              8680, 8681, 8682, 8690, 8691, 8692, 8693, 8700, 8701, 8702, 8703, 8704, 8705, 8890,
+                              8891, 8892, 8896, 8960])
+            ielion = rng.choice(codes, n)
+            loggf = rng.normal(-3.0, 1.5, n)
+        else:
+            nel = rng.integers(1, nspec + 1, n)
+            ielion = np.where(rng.uniform(size=n) < 0.5, 1, -1) * (10 * nel + rng.integers(0, 10, n))
+            if bad_frac > 0:
+                b = rng.uniform(size=n) < bad_frac
+                ielion[b] = rng.choice([0, 5, -7, 10 * (nspec + 1), 10 * (nspec + 3) + 4], b.sum())
+            loggf = rng.normal(-2.0, 1.5, n) if kind != SEL_H3PLUS else rng.normal(-1.0, 1.5, n)
+        elo = rng.uniform(1.0, 64500.0, n)
+        rec = pack_linedata(iwl, ielion.astype(np.int16), encode_i16(elo), encode_i16(10.0 ** loggf),
+                            encode_i16(10.0 ** rng.normal(8.0, 0.3, n)), encode_i16(10.0 ** rng.normal(-5.5, 0.5, n)),
+                            encode_i16(10.0 ** rng.normal(-7.5, 0.3, n)))
+    if shuffle_frac > 0 and n > 1:
+        k = int(n * shuffle_frac)
+        a = rng.integers(0, n, k)
+        b = rng.integers(0, n, k)
+        tmp = rec[a].copy()
+        rec[a] = rec[b]
+        rec[b] = tmp
+    return rec

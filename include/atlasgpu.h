@@ -264,6 +264,59 @@ typedef struct {
 int atlasgpu_atlas_finish(atlasgpu_ctx *ctx, atlasgpu_finish_state *s, const atlasgpu_accum *acc,
                           double *max_flxerr);
 
+/* ---- SELECTLINES: the line databases -> LINEDATA ----------------------
+ * SELECTLINES (atlas12_modules.f90:19171-19781) keeps the lines whose
+ * centre opacity can reach the continuum cutoff: per record, the NU advance
+ * over IWAVETAB (DO WHILE (IWL >= IWAVETAB(NU)), which sets FREQ), then
+ * CENRATIO = CEN_PREFAC * TABLOG(IGFLOG) * XNFDOPMAX(NELION, NU) / FREQ >= 1
+ * and CENRATIO * exp(-E * HCKT(NRHOX)) >= 1, and the record packed as
+ * LINEDATA (PACK_LINEDATA, :1964-1977).  One call runs one database loop;
+ * the driver order (:19262-19767) is the caller's. */
+#define ATLASGPU_SEL_LOWPRED 1  /* gfpred LINEREC [4] int32, unit 11 (:19262-19312) */
+#define ATLASGPU_SEL_LOWOBS 2   /* lowobsat12 LINEREC, unit 111 (:19314-19357) */
+#define ATLASGPU_SEL_HI 3       /* hilines LINEREC, unit 21 (:19359-19402) */
+#define ATLASGPU_SEL_DIATOMIC 4 /* LINEREC as the diatomic reader packs them, sorted by IWL,
+                                   IGFLOG before the isotopologue correction (:19403-19529) */
+#define ATLASGPU_SEL_TIO 5      /* MOL2 records, 32 bytes, after the header (:19531-19648) */
+#define ATLASGPU_SEL_H2O 6      /* {int32 IWL; int16 IELO, IGFLOG}, 8 bytes (:19650-19720) */
+#define ATLASGPU_SEL_H3PLUS 7   /* h3plus LINEREC, unit 61 (:19722-19767) */
+
+/* the module variables a database loop reads at entry and leaves behind:
+ * NU (1-based bin of IWAVETAB), FREQ (Hz) and IGR (INTEGER(2)) */
+typedef struct atlasgpu_select_state {
+  int32_t nu;
+  int32_t igr;
+  double freq;
+} atlasgpu_select_state;
+
+/* The tables every database loop reads, kept on the context: XNFDOPMAX
+ * (:19248-19256, computed on the device from xnfdop [nspec][kw] and tabcont
+ * [nwave+1][kw] over nrhox depths), HCKT(NRHOX) from hckt [nrhox], IWAVETAB
+ * [nwave+1] (nondecreasing, the 2**30 sentinel last) and WAVETAB [nwave]
+ * (nm, for FREQ = CLIGHT_NMS / WAVETAB(NU)).  nwave + 1 <= 1024. */
+int atlasgpu_atlas_select_tables(atlasgpu_ctx *ctx, int nrhox, int kw, const double *xnfdop, int nspec,
+                                 const double *hckt, const double *tabcont, const int32_t *iwavetab,
+                                 const double *wavetab, int nwave);
+
+/* One database loop over n records of kind's format, in file order (host
+ * buffers).  state: in at entry, out as the loop leaves it.  The selected
+ * records go to linedata_out [cap][4] in file order; *n_out their count.
+ * The reference's fatal cases return ATLASGPU_EINVAL with the record index
+ * in atlasgpu_last_error: an unknown diatomic MOLCODE; NELION outside
+ * 1..nspec where the reference indexes XNFDOPMAX with it (every kind but
+ * LOWPRED, which skips such records); IWL at or past the IWAVETAB sentinel;
+ * more than cap selected records (LINEDATA overflow).  Records can be given
+ * in chunks: the state carries the loop from one call to the next. */
+int atlasgpu_atlas_selectlines(atlasgpu_ctx *ctx, int kind, const void *recs, int64_t n,
+                               atlasgpu_select_state *state, int32_t *linedata_out, int64_t cap,
+                               int64_t *n_out);
+
+/* The same with device buffers: d_recs aligned to 16 bytes (8 for H2O),
+ * d_linedata_out [cap][4] aligned to 16 bytes. */
+int atlasgpu_atlas_selectlines_dev(atlasgpu_ctx *ctx, int kind, const void *d_recs, int64_t n,
+                                   atlasgpu_select_state *state, int32_t *d_linedata_out, int64_t cap,
+                                   int64_t *n_out);
+
 /* ---- device-resident ATLAS12 model ----------------------------------
  * One atmosphere kept on the device for the whole iteration (atlas12c.f90
  * :496-606): hydrostatics, populations and continuum from the documented

@@ -1570,3 +1570,185 @@ double orc_atlas_finish(orc_tcorr_t *s) {
   for (j = 0; j < n; ++j) s->tauros[j] = taustd[j];
   return maxerr;
 }
+
+/* ---- SELECTLINES (atlas12_modules.f90:19171-19781) -------------------- */
+
+/* XNFDOPMAX(NELION, NU) = max over J of XNFDOP(J, NELION) / TABCONT(J, NU),
+ * starting from 0 (:19248-19256).  xmax [nwave+1][nspec]. */
+void orc_xnfdopmax(int nrhox, int kw, const double *xnfdop, int nspec, const double *tabcont,
+                   int nwave, double *xmax) {
+  for (int nu = 0; nu <= nwave; ++nu)
+    for (int e = 0; e < nspec; ++e) {
+      double m = 0.0;
+      for (int j = 0; j < nrhox; ++j) {
+        const double r = xnfdop[(size_t)e * kw + j] / tabcont[(size_t)nu * kw + j];
+        if (r > m) m = r;
+      }
+      xmax[(size_t)nu * nspec + e] = m;
+    }
+}
+
+/* INT() of a REAL(8) as x86-64 converts it (cvttsd2si): truncation toward
+ * zero, and the integer-indefinite -2**31 for NaN or a value out of range */
+static int32_t sel_fint(double x) {
+  if (!(x > -2147483649.0 && x < 2147483648.0)) return INT32_MIN;
+  return (int32_t)x;
+}
+/* INTEGER(2) = INTEGER(4): the low 16 bits */
+static int16_t sel_i16(int32_t v) { return (int16_t)(uint16_t)(uint32_t)v; }
+static double sel_tablog(int16_t i) { return pow(10.0, (double)((int32_t)i - 16384) * 0.001); } /* :2083 */
+static void sel_unpack(const int32_t *r, int32_t *iwl, int16_t *f) { /* UNPACK_LINEDATA :1950-1963 */
+  *iwl = r[0];
+  for (int k = 0; k < 3; ++k) {
+    f[2 * k] = (int16_t)(uint16_t)((uint32_t)r[1 + k] & 0xffffu);
+    f[2 * k + 1] = (int16_t)(uint16_t)((uint32_t)r[1 + k] >> 16);
+  }
+}
+static void sel_pack(int32_t *o, int32_t iwl, const int16_t *f) { /* PACK_LINEDATA :1967-1977 */
+  o[0] = iwl;
+  for (int k = 0; k < 3; ++k)
+    o[1 + k] = (int32_t)((uint32_t)(uint16_t)f[2 * k] | ((uint32_t)(uint16_t)f[2 * k + 1] << 16));
+}
+
+/* One database loop of SELECTLINES.  The loop body follows the reference
+ * case by case: the NU advance (DO WHILE IWL >= IWAVETAB(NU), setting FREQ
+ * and, for H2O, IGR), the species index, the XNFDOPMAX / CENRATIO /
+ * Boltzmann tests against HCKT(NRHOX), and the packed record.  Module
+ * variables that outlive the loop (NU, FREQ, IGR) go through st. */
+int64_t orc_atlas_selectlines(const orc_select_tables_t *tb, int kind, const void *recs, int64_t n,
+                              orc_select_state_t *st, const double *xmax, int nspec, double hckt_last,
+                              const int32_t *iwt, const double *wavetab, int nwave,
+                              int32_t *out, int64_t cap, int64_t *bad) {
+  const double CLIGHT_NMS = 2.99792458e17;          /* :325 */
+  const double CEN_PREFAC = 0.026538 / 1.7724538509055159; /* :19178, SQRTPI :317 */
+  const double RATIOLG = log(1.0 + 1.0 / 2000000.0);
+  int nu = st->nu;
+  double freq = st->freq;
+  int16_t igr = (int16_t)st->igr;
+  int64_t ns = 0;
+  *bad = -1;
+  for (int64_t i = 0; i < n; ++i) {
+    int32_t iwl = 0;
+    int16_t f[6] = {0, 0, 0, 0, 0, 0}; /* IELION, IELO, IGFLOG, IGR, IGS, IGW */
+    double elo_exp = 0.0;                 /* the energy in the Boltzmann test */
+    int nelion;
+    if (kind == ORC_SEL_TIO) {
+      const int32_t *w = (const int32_t *)recs + 8 * i;
+      if (w[4] != 822) continue;           /* :19599 */
+      const int iso = w[5] - 45;
+      if (iso < 1 || iso > 5) continue;
+      float wl4, e1, e2, gf4;
+      memcpy(&wl4, &w[0], 4);
+      memcpy(&gf4, &w[1], 4);
+      memcpy(&e1, &w[2], 4);
+      memcpy(&e2, &w[3], 4);
+      const double W = (double)wl4;
+      if (W <= 0.0) continue;
+      iwl = sel_fint(log(W) / RATIOLG + 0.5);
+      while (iwl >= iwt[nu - 1]) {
+        if (nu == nwave + 1) { *bad = i; return ORC_SEL_ESENTINEL; }
+        freq = CLIGHT_NMS / wavetab[nu - 1];
+        ++nu;
+      }
+      const int32_t kgflog = sel_fint(round((double)gf4 * 1000.0)) + 16384;
+      f[2] = sel_i16(kgflog + tb->tio_isocorr[iso - 1] > 1 ? kgflog + tb->tio_isocorr[iso - 1] : 1);
+      nelion = 895;
+      if (nelion > nspec) { *bad = i; return ORC_SEL_ENELION; }
+      const double xm = xmax[(size_t)(nu - 1) * nspec + nelion - 1];
+      if (xm == 0.0) continue;
+      const double cen = CEN_PREFAC * sel_tablog(f[2]) * xm / freq;
+      if (cen < 1.0) continue;
+      const double a1 = fabs((double)e1), a2 = fabs((double)e2);
+      const double elo = a2 < a1 ? a2 : a1;
+      if (cen * exp(-elo * hckt_last) < 1.0) continue;
+      f[0] = (int16_t)(8949 + iso);
+      f[1] = sel_i16(sel_fint(log10(elo > 1.0e-10 ? elo : 1.0e-10) * 1000.0 + 16384.5));
+      const double g = w[6] == 0 ? 2.223e13 / (W * W) : pow(10.0, (double)w[6] * 0.01);
+      igr = sel_i16(sel_fint(log10(g) * 1000.0 + 16384.5));
+      f[3] = igr;
+      f[4] = 1;
+      f[5] = 9384;
+    } else if (kind == ORC_SEL_H2O) {
+      const unsigned char *b = (const unsigned char *)recs + 8 * i;
+      int16_t ielo_in, igf_in;
+      memcpy(&iwl, b, 4);
+      memcpy(&ielo_in, b + 4, 2);
+      memcpy(&igf_in, b + 6, 2);
+      while (iwl >= iwt[nu - 1]) {
+        if (nu == nwave + 1) { *bad = i; return ORC_SEL_ESENTINEL; }
+        freq = CLIGHT_NMS / wavetab[nu - 1];
+        /* GAMMAR = 2.474D-22 * FREQ**2 * 0.001 (a default REAL literal) */
+        const double gammar = 2.474e-22 * (freq * freq) * (double)0.001f;
+        igr = sel_i16(sel_fint(log10(gammar) * 1000.0 + 16384.5));
+        ++nu;
+      }
+      int iso;
+      if (ielo_in > 0 && igf_in > 0) iso = 1;
+      else if (ielo_in > 0) iso = 2;
+      else if (igf_in > 0) iso = 3;
+      else iso = 4;
+      f[0] = (int16_t)(-(9399 + iso));
+      const double elo = (double)abs((int32_t)ielo_in);
+      const int32_t kgflog = abs((int32_t)igf_in);
+      f[2] = sel_i16(kgflog + tb->h2o_isocorr[iso - 1] > 1 ? kgflog + tb->h2o_isocorr[iso - 1] : 1);
+      nelion = 940;
+      if (nelion > nspec) { *bad = i; return ORC_SEL_ENELION; }
+      const double xm = xmax[(size_t)(nu - 1) * nspec + nelion - 1];
+      if (xm == 0.0) continue;
+      const double cen = CEN_PREFAC * sel_tablog(f[2]) * xm / freq;
+      if (cen < 1.0) continue;
+      if (cen * exp(-elo * hckt_last) < 1.0) continue;
+      f[1] = sel_i16(sel_fint(log10(elo) * 1000.0 + 16384.5));
+      f[3] = igr;
+      f[4] = 1;
+      f[5] = 9384;
+    } else {
+      /* LINEREC databases: UNPACK_LINEDATA sets every field, IGR included */
+      const int32_t *r = (const int32_t *)recs + 4 * i;
+      sel_unpack(r, &iwl, f);
+      igr = f[3];
+      while (iwl >= iwt[nu - 1]) {
+        if (nu == nwave + 1) { *bad = i; return ORC_SEL_ESENTINEL; }
+        freq = CLIGHT_NMS / wavetab[nu - 1];
+        ++nu;
+      }
+      if (kind == ORC_SEL_DIATOMIC) {
+        const int32_t molcode = f[0];
+        int imol = -1;
+        for (int k = 0; k < tb->nmol; ++k)
+          if (tb->molcodes[k] == molcode) { imol = k; break; }
+        if (imol < 0) { *bad = i; return ORC_SEL_EMOLCODE; }
+        const int32_t kgflog = f[2];
+        f[2] = sel_i16(kgflog + tb->isox[imol] > 1 ? kgflog + tb->isox[imol] : 1);
+      } else if (kind == ORC_SEL_H3PLUS) {
+        const int32_t kgflog = f[2];
+        f[2] = sel_i16(kgflog - 1272 > 1 ? kgflog - 1272 : 1);
+        f[4] = 1;
+        f[5] = 9384;
+      }
+      nelion = kind == ORC_SEL_H3PLUS ? 895 : abs((int32_t)f[0] / 10);
+      if (nelion < 1 || nelion > nspec) {
+        if (kind == ORC_SEL_LOWPRED) continue; /* :19283-19287 */
+        *bad = i;
+        return ORC_SEL_ENELION;
+      }
+      const double xm = xmax[(size_t)(nu - 1) * nspec + nelion - 1];
+      if (kind == ORC_SEL_LOWPRED || kind == ORC_SEL_LOWOBS) {
+        if (xm <= 1.0e-37) continue;
+      } else if (xm == 0.0) {
+        continue;
+      }
+      const double cen = CEN_PREFAC * sel_tablog(f[2]) * xm / freq;
+      if (cen < 1.0) continue;
+      elo_exp = sel_tablog(f[1]);
+      if (cen * exp(-elo_exp * hckt_last) < 1.0) continue;
+    }
+    if (ns >= cap) { *bad = i; return ORC_SEL_EOVERFLOW; }
+    sel_pack(out + 4 * ns, iwl, f);
+    ++ns;
+  }
+  st->nu = nu;
+  st->freq = freq;
+  st->igr = igr;
+  return ns;
+}

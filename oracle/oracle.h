@@ -178,10 +178,6 @@ void orc_atlas_rt_pass(const orc_ops_t *ops, int numnu, const double *waveset,
                        const double *t, const double *hkt, double teff,
                        int nu0, int nu1, orc_accum_t *acc, double *hsurf);
 
-#ifdef __cplusplus
-}
-#endif
-#endif
 
 /* ---- ATLAS12 iteration finish: ROSS(3), RADIAP(3), TCORR(3) ----------
  * Radiative branch (IFCONV = 0: CONVEC not called, CNVFLX = 0, CZ_CONSTRUCT
@@ -206,3 +202,57 @@ double orc_rosstab(const orc_tcorr_t *s, double t, double p);
 void orc_ttaup(const orc_tcorr_t *s, const double *tin, const double *tau, double *abstd,
                double *ptotal, double *pout, const double *prad, int n);
 double orc_atlas_finish(orc_tcorr_t *s);
+
+/* ---- SELECTLINES (atlas12_modules.f90:19171-19781) -------------------
+ * One database loop of SELECTLINES: the records of one line list, filtered
+ * by the line-centre ratio against XNFDOPMAX and the Boltzmann factor at the
+ * deepest layer, and packed as LINEDATA records (:1964-1977).
+ * kinds and their record formats:
+ *   ORC_SEL_LOWPRED  int32[4] LINEREC, gfpred (unit 11)          :19262-19312
+ *   ORC_SEL_LOWOBS   int32[4] LINEREC, lowobsat12 (unit 111)     :19314-19357
+ *   ORC_SEL_HI       int32[4] LINEREC, hilines (unit 21)         :19359-19402
+ *   ORC_SEL_DIATOMIC int32[4] LINEREC as the diatomic reader packs it, sorted
+ *                    by IWL, IGFLOG before the isotopologue correction
+ *                                                                  :19403-19529
+ *   ORC_SEL_TIO      32-byte MOL2 records after the header        :19531-19648
+ *   ORC_SEL_H2O      8-byte records {int32 IWL; int16 IELO, IGFLOG} :19650-19720
+ *   ORC_SEL_H3PLUS   int32[4] LINEREC, h3plus (unit 61)          :19722-19767
+ * st: the module variables the loop reads and leaves behind (NU, 1-based;
+ * FREQ; IGR).  xmax [nwave+1][nspec] = XNFDOPMAX (orc_xnfdopmax).
+ * Returns the number of records written to out [cap][4], or a negative
+ * code (ORC_SEL_E*) with the offending record index in *bad. */
+#define ORC_SEL_LOWPRED 1
+#define ORC_SEL_LOWOBS 2
+#define ORC_SEL_HI 3
+#define ORC_SEL_DIATOMIC 4
+#define ORC_SEL_TIO 5
+#define ORC_SEL_H2O 6
+#define ORC_SEL_H3PLUS 7
+#define ORC_SEL_ENELION -1   /* NELION outside 1..nspec where the reference indexes with it */
+#define ORC_SEL_EMOLCODE -2  /* diatomic MOLCODE not in MOLCODES (the reference stops) */
+#define ORC_SEL_ESENTINEL -3 /* IWL at or past the IWAVETAB sentinel */
+#define ORC_SEL_EOVERFLOW -4 /* more selected records than cap (LINEDATA overflow) */
+typedef struct {
+  int32_t nu;
+  int32_t igr;
+  double freq;
+} orc_select_state_t;
+/* SELECTLINES's constant tables (:19182-19207), passed in from the fixture
+ * extracted out of the reference source */
+typedef struct {
+  const int32_t *molcodes, *isox; /* MOLCODES(NMOL), ISOX(NMOL) */
+  int nmol;
+  const int32_t *tio_isocorr;     /* TIO_ISOCORR(5) */
+  const int32_t *h2o_isocorr;     /* H2O_ISOCORR(4) */
+} orc_select_tables_t;
+void orc_xnfdopmax(int nrhox, int kw, const double *xnfdop, int nspec, const double *tabcont,
+                   int nwave, double *xmax);                        /* :19248-19256 */
+int64_t orc_atlas_selectlines(const orc_select_tables_t *tb, int kind, const void *recs, int64_t n,
+                              orc_select_state_t *st, const double *xmax, int nspec, double hckt_last,
+                              const int32_t *iwavetab, const double *wavetab, int nwave,
+                              int32_t *out, int64_t cap, int64_t *bad);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

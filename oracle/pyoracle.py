@@ -457,3 +457,62 @@ def synthe_nlte_opacity(recs, length, wbegin, ratio, wlend, velshift_kms, contin
                                     _ptr(xnfdop), _ptr(dopple), nspec, _ptr(_d(atm["xne"])), _ptr(_d(atm["txnxn"])),
                                     _ptr(_d(atm["hckt"])), _ptr(_d(contx)), _ptr(out))
     return out
+
+
+# ------------------------------------------------------------- SELECTLINES
+SEL_LOWPRED, SEL_LOWOBS, SEL_HI, SEL_DIATOMIC, SEL_TIO, SEL_H2O, SEL_H3PLUS = range(1, 8)
+SEL_ERRORS = {-1: "NELION out of range", -2: "unknown MOLCODE", -3: "IWL past the IWAVETAB sentinel",
+              -4: "LINEDATA overflow"}
+MOL2_REC = np.dtype([("wl", "<f4"), ("gflog", "<f4"), ("e1", "<f4"), ("e2", "<f4"), ("code", "<i4"),
+                     ("iso", "<i4"), ("gr", "<i4"), ("label", "<i4")])
+H2O_REC = np.dtype([("iwl", "<i4"), ("ielo", "<i2"), ("igflog", "<i2")])
+CLIGHT_NMS = 2.99792458e17
+
+
+class _SelState(ctypes.Structure):
+    _fields_ = [("nu", ctypes.c_int32), ("igr", ctypes.c_int32), ("freq", ctypes.c_double)]
+
+
+class _SelTables(ctypes.Structure):
+    _fields_ = [("molcodes", _ip), ("isox", _ip), ("nmol", ctypes.c_int), ("tio_isocorr", _ip),
+                ("h2o_isocorr", _ip)]
+
+
+def xnfdopmax(nrhox, xnfdop, tabcont):
+    """XNFDOPMAX [nwave+1, nspec] from xnfdop [nspec, kw] and tabcont [nwave+1, kw]."""
+    xnfdop, tabcont = _d(xnfdop), _d(tabcont)
+    nspec, kw = xnfdop.shape
+    out = np.zeros((tabcont.shape[0], nspec))
+    L = _lib2()
+    L.orc_xnfdopmax.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, _dp]
+    L.orc_xnfdopmax(nrhox, kw, _ptr(xnfdop), nspec, _ptr(tabcont), tabcont.shape[0] - 1, _ptr(out))
+    return out
+
+
+def selectlines(tables, kind, recs, state, xmax, hckt_last, iwavetab, wavetab, cap=None):
+    """One SELECTLINES database loop.  tables: dict with molcodes, isox, tio_isocorr, h2o_isocorr;
+    state: dict(nu, freq, igr), updated in place.  Returns (linedata [m, 4] int32, error code, record)."""
+    recs = np.ascontiguousarray(recs)
+    n = recs.shape[0]
+    cap = n if cap is None else cap
+    mc, ix, ti, hi = (np.ascontiguousarray(tables[k], np.int32)
+                      for k in ("molcodes", "isox", "tio_isocorr", "h2o_isocorr"))
+    tb = _SelTables(_ptr(mc, _ip), _ptr(ix, _ip), mc.size, _ptr(ti, _ip), _ptr(hi, _ip))
+    st = _SelState(int(state["nu"]), int(state["igr"]), float(state["freq"]))
+    xmax = _d(xmax)
+    iw = np.ascontiguousarray(iwavetab, np.int32)
+    wt = _d(wavetab)
+    out = np.zeros((max(cap, 1), 4), np.int32)
+    bad = ctypes.c_int64(-1)
+    L = _lib2()
+    L.orc_atlas_selectlines.argtypes = [ctypes.POINTER(_SelTables), ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
+                                        ctypes.POINTER(_SelState), _dp, ctypes.c_int, ctypes.c_double, _ip, _dp,
+                                        ctypes.c_int, _ip, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+    L.orc_atlas_selectlines.restype = ctypes.c_int64
+    r = L.orc_atlas_selectlines(ctypes.byref(tb), kind, recs.ctypes.data_as(ctypes.c_void_p), n, ctypes.byref(st),
+                                _ptr(xmax), xmax.shape[1], float(hckt_last), _ptr(iw, _ip), _ptr(wt), wt.size,
+                                _ptr(out, _ip), cap, ctypes.byref(bad))
+    if r < 0:
+        return None, int(r), int(bad.value)
+    state.update(nu=st.nu, igr=st.igr, freq=st.freq)
+    return out[:r].copy(), 0, -1

@@ -13,6 +13,9 @@ modified).  Writes tests/golden/reference_tables.npz with:
   awei, lwei     Weideman N=32 coefficients (synthe_module.f90:91-126), kept
                  only to pin the product's own derivation of them
   wavetab        KAPCONT's 361-point continuum-cutoff grid (atlas12_modules.f90:1811-1857)
+  molcodes, isox SELECTLINES's diatomic species codes and isotopologue log gf
+                 corrections in millidex (atlas12_modules.f90:19182-19202)
+  tio_isocorr, h2o_isocorr   the TiO and H2O isotope corrections (:19204, :19207)
   deck           the reference's converged solar model (workdir/ap00t5777g4.44at12.dat,
                  Teff 5777 K, log g 4.44, 72 depths, iteration 45): READ DECK6
                  columns RHOX, T, P, XNE, ABROSS, ACCRAD, VTURB as printed, [72, 7],
@@ -59,6 +62,16 @@ def fortran_array(src, name, count):
     return vals
 
 
+def fortran_int_array(src, name, count):
+    """INTEGER array constructor (/ ... /) following name, comments dropped."""
+    i = src.index(name)
+    body = src[src.index("(/", i) + 2:src.index("/)", i)]
+    body = re.sub(r"!.*", "", body).replace("&", " ")
+    vals = np.array([int(x) for x in re.findall(r"[-+]?\d+", body)], dtype=np.int32)
+    assert vals.size == count, (name, vals.size)
+    return vals
+
+
 def read_deck(path):
     """READ DECK6 block and PRADK of an ATLAS12 model file."""
     lines = open(path).read().splitlines()
@@ -83,6 +96,10 @@ def main():
         awei=fortran_array(syn, "AWEI(32) =", 32),
         lwei=np.array([float(re.search(r"LWEI = ([0-9.D+-]+)", syn).group(1).replace("D", "e"))]),
         wavetab=fortran_array(mod, "WAVETAB(NWAVE) =", 361),
+        molcodes=fortran_int_array(mod, "MOLCODES(NMOL) =", 46),
+        isox=fortran_int_array(mod, "ISOX(NMOL) =", 46),
+        tio_isocorr=fortran_int_array(mod, "TIO_ISOCORR(5) =", 5),
+        h2o_isocorr=fortran_int_array(mod, "H2O_ISOCORR(4) =", 4),
     )
     out["deck"], out["deck_pradk"] = read_deck(os.path.join(ROOT, "workdir", "ap00t5777g4.44at12.dat"))
     np.savez(os.path.join(HERE, "reference_tables.npz"), **out)

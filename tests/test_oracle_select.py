@@ -1,0 +1,234 @@
+"""The oracle's SELECTLINES (oracle.c orc_atlas_selectlines) against a second,
+independent restatement in plain Python loops, on small seeded databases of
+every kind, and the loop's state rules (atlas12_modules.f90:19171-19781).
+
+The reference has no tests or golden vectors for this path and cannot be
+built here; the pins are its own constant tables (MOLCODES, ISOX,
+TIO_ISOCORR, H2O_ISOCORR, WAVETAB extracted from the source by
+tests/golden/make_golden.py) and agreement of two restatements written from
+the source separately.
+"""
+import math
+import struct
+
+import numpy as np
+import pytest
+
+from atlas12_b200 import atlas, synthetic
+
+CLIGHT_NMS = 2.99792458e17
+CEN_PREFAC = 0.026538 / 1.7724538509055159
+RATIOLG = math.log(1.0 + 1.0 / 2000000.0)
+KINDS = range(1, 8)
+
+
+def fint(x):
+    """INT() as x86-64 converts a REAL(8): truncation, -2**31 for NaN / out of range."""
+    if not (-2147483649.0 < x < 2147483648.0):
+        return -2147483648
+    return int(x)
+
+
+def i16(v):
+    v &= 0xFFFF
+    return v - 0x10000 if v >= 0x8000 else v
+
+
+def nint(x):
+    """NINT: nearest, halves away from zero."""
+    a = abs(x)
+    r = math.floor(a)
+    r += 1 if a - r >= 0.5 else 0
+    return int(math.copysign(r, x))
+
+
+def tablog(i):
+    return math.pow(10.0, (i - 16384) * 0.001)
+
+
+def py_select(tb, kind, recs, st, xmax, hckt_last, iwt, wavetab):
+    """Plain-loop SELECTLINES database loop (returns records, error, record)."""
+    nwave = len(wavetab)
+    nspec = xmax.shape[1]
+    nu, freq, igr = st["nu"], st["freq"], st["igr"]
+    out = []
+    molcodes = [int(x) for x in tb["molcodes"]]
+
+    def advance(iwl, h2o=False):
+        nonlocal nu, freq, igr
+        while iwl >= iwt[nu - 1]:
+            if nu == nwave + 1:
+                raise IndexError
+            freq = CLIGHT_NMS / wavetab[nu - 1]
+            if h2o:
+                gammar = 2.474e-22 * (freq * freq) * float(np.float32(0.001))
+                igr = i16(fint(math.log10(gammar) * 1000.0 + 16384.5))
+            nu += 1
+
+    for i in range(len(recs)):
+        try:
+            if kind == 5:
+                r = recs[i]
+                if int(r["code"]) != 822:
+                    continue
+                iso = int(r["iso"]) - 45
+                if iso < 1 or iso > 5:
+                    continue
+                w = float(r["wl"])
+                if w <= 0.0:
+                    continue
+                iwl = fint(math.log(w) / RATIOLG + 0.5)
+                advance(iwl)
+                kg = nint(float(r["gflog"]) * 1000.0) + 16384
+                igf = i16(max(kg + int(tb["tio_isocorr"][iso - 1]), 1))
+                xm = xmax[nu - 1, 894]
+                if xm == 0.0:
+                    continue
+                cen = CEN_PREFAC * tablog(igf) * xm / freq
+                if cen < 1.0:
+                    continue
+                elo = min(abs(float(r["e1"])), abs(float(r["e2"])))
+                if cen * math.exp(-elo * hckt_last) < 1.0:
+                    continue
+                g = 2.223e13 / (w * w) if int(r["gr"]) == 0 else math.pow(10.0, float(int(r["gr"])) * 0.01)
+                igr = i16(fint(math.log10(g) * 1000.0 + 16384.5))
+                f = [8949 + iso, i16(fint(math.log10(max(elo, 1e-10)) * 1000.0 + 16384.5)), igf, igr, 1, 9384]
+            elif kind == 6:
+                r = recs[i]
+                iwl = int(r["iwl"])
+                advance(iwl, h2o=True)
+                ie, ig = int(r["ielo"]), int(r["igflog"])
+                iso = 1 if (ie > 0 and ig > 0) else 2 if ie > 0 else 3 if ig > 0 else 4
+                elo = float(abs(ie))
+                igf = i16(max(abs(ig) + int(tb["h2o_isocorr"][iso - 1]), 1))
+                xm = xmax[nu - 1, 939]
+                if xm == 0.0:
+                    continue
+                cen = CEN_PREFAC * tablog(igf) * xm / freq
+                if cen < 1.0 or cen * math.exp(-elo * hckt_last) < 1.0:
+                    continue
+                f = [-(9399 + iso), i16(fint(math.log10(elo) * 1000.0 + 16384.5)), igf, igr, 1, 9384]
+            else:
+                w = [int(x) for x in recs[i]]
+                iwl = w[0]
+                f = [i16(w[1]), i16(w[1] >> 16), i16(w[2]), i16(w[2] >> 16), i16(w[3]), i16(w[3] >> 16)]
+                igr = f[3]
+                advance(iwl)
+                if kind == 4:
+                    if f[0] not in molcodes:
+                        return None, -2, i
+                    f[2] = i16(max(f[2] + int(tb["isox"][molcodes.index(f[0])]), 1))
+                if kind == 7:
+                    f[2] = i16(max(f[2] - 1272, 1))
+                    f[4], f[5] = 1, 9384
+                nelion = 895 if kind == 7 else abs(int(f[0] / 10))
+                if nelion < 1 or nelion > nspec:
+                    if kind == 1:
+                        continue
+                    return None, -1, i
+                xm = xmax[nu - 1, nelion - 1]
+                if (xm <= 1e-37) if kind in (1, 2) else (xm == 0.0):
+                    continue
+                cen = CEN_PREFAC * tablog(f[2]) * xm / freq
+                if cen < 1.0 or cen * math.exp(-tablog(f[1]) * hckt_last) < 1.0:
+                    continue
+        except IndexError:
+            return None, -3, i
+        out.append([iwl] + [struct.unpack("<i", struct.pack("<hh", f[2 * k], f[2 * k + 1]))[0] for k in range(3)])
+    st.update(nu=nu, freq=freq, igr=igr)
+    return np.array(out, np.int32).reshape(-1, 4), 0, -1
+
+
+@pytest.fixture(scope="module")
+def sel(tables, po):
+    wt = tables["wavetab"]
+    xn, hckt, tc = synthetic.selectlines_tables(wt)
+    return dict(wt=wt, iwt=atlas.iwavetab(wt), xmax=po.xnfdopmax(72, xn, tc), hckt=hckt,
+                tb={k: tables[k] for k in ("molcodes", "isox", "tio_isocorr", "h2o_isocorr")})
+
+
+def test_xnfdopmax_is_the_depth_maximum(po):
+    rng = np.random.default_rng(3)
+    xn = rng.uniform(0.0, 2.0, (5, 9))
+    tc = rng.uniform(0.5, 1.5, (4, 9))
+    got = po.xnfdopmax(7, xn, tc)
+    want = np.max(xn[None, :, :7] / tc[:, None, :7], axis=2)
+    np.testing.assert_array_equal(got, np.maximum(want, 0.0))
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("shuffle", [0.0, 0.05])
+def test_oracle_matches_plain_loop_restatement(sel, po, kind, shuffle):
+    recs = synthetic.selectlines_records(kind, 3000, sel["wt"], seed=20 + kind, shuffle_frac=shuffle)
+    if kind == 5:
+        # log gf with an exact half in millidex: NINT rounds it away from zero
+        recs["gflog"][::7] = np.float32(-3.9375)
+        recs["gflog"][3::7] = np.float32(0.0625)
+    st0 = {"nu": 1, "freq": CLIGHT_NMS / sel["wt"][-1], "igr": 7}
+    s1, s2 = dict(st0), dict(st0)
+    got, e1, b1 = po.selectlines(sel["tb"], kind, recs, s1, sel["xmax"], sel["hckt"][-1], sel["iwt"], sel["wt"])
+    want, e2, b2 = py_select(sel["tb"], kind, recs, s2, sel["xmax"], sel["hckt"][-1], sel["iwt"], sel["wt"])
+    assert (e1, b1) == (e2, b2)
+    assert got.shape[0] > 0
+    np.testing.assert_array_equal(got, want)
+    assert s1 == s2
+
+
+@pytest.mark.parametrize("kind", [2, 3])
+def test_out_of_range_species_stop_the_loop(sel, po, kind):
+    """LOWOBS and HILINES index XNFDOPMAX with any NELION: the oracle stops at the
+    first such record; LOWPRED skips them."""
+    recs = synthetic.selectlines_records(kind, 2000, sel["wt"], seed=5, bad_frac=0.01)
+    bad_rows = [i for i in range(len(recs)) if not 1 <= abs(int(int(np.int16(recs[i, 1] & 0xFFFF)) / 10)) <= 1006]
+    st = {"nu": 1, "freq": 1.0, "igr": 0}
+    out, err, bad = po.selectlines(sel["tb"], kind, recs, st, sel["xmax"], sel["hckt"][-1], sel["iwt"], sel["wt"])
+    assert err == -1 and bad == bad_rows[0]
+    st = {"nu": 1, "freq": 1.0, "igr": 0}
+    out, err, bad = po.selectlines(sel["tb"], 1, recs, st, sel["xmax"], sel["hckt"][-1], sel["iwt"], sel["wt"])
+    assert err == 0
+
+
+def test_chunks_continue_the_loop(sel, po):
+    """The state (NU, FREQ, IGR) carries a loop across calls: chunks = one call."""
+    for kind in KINDS:
+        recs = synthetic.selectlines_records(kind, 5000, sel["wt"], seed=40 + kind, shuffle_frac=0.01)
+        st = {"nu": 1, "freq": 3.0e15, "igr": -3}
+        whole, _, _ = po.selectlines(sel["tb"], kind, recs, st, sel["xmax"], sel["hckt"][-1], sel["iwt"], sel["wt"])
+        st2 = {"nu": 1, "freq": 3.0e15, "igr": -3}
+        parts = [po.selectlines(sel["tb"], kind, recs[a:b], st2, sel["xmax"], sel["hckt"][-1], sel["iwt"],
+                                sel["wt"])[0] for a, b in ((0, 1), (1, 1777), (1777, 1777), (1777, 5000))]
+        np.testing.assert_array_equal(np.concatenate(parts), whole)
+        assert st == st2
+
+
+def test_sentinel_and_overflow(sel, po):
+    recs = synthetic.selectlines_records(1, 100, sel["wt"], seed=9)
+    recs[60, 0] = 2 ** 30
+    st = {"nu": 1, "freq": 1.0, "igr": 0}
+    assert po.selectlines(sel["tb"], 1, recs, st, sel["xmax"], sel["hckt"][-1], sel["iwt"], sel["wt"])[1:] == (-3, 60)
+    recs = synthetic.selectlines_records(7, 1000, sel["wt"], seed=9)
+    st = {"nu": 1, "freq": 1.0, "igr": 0}
+    n = po.selectlines(sel["tb"], 7, recs, st, sel["xmax"], sel["hckt"][-1], sel["iwt"], sel["wt"])[0].shape[0]
+    st = {"nu": 1, "freq": 1.0, "igr": 0}
+    assert po.selectlines(sel["tb"], 7, recs, st, sel["xmax"], sel["hckt"][-1], sel["iwt"], sel["wt"],
+                          cap=n - 1)[1] == -4
+
+
+def test_unknown_molcode_stops(sel, po):
+    recs = synthetic.selectlines_records(4, 300, sel["wt"], seed=2)
+    recs[123, 1] = (recs[123, 1] & ~0xFFFF) | 8420  # not a MOLCODE
+    st = {"nu": 1, "freq": 1.0, "igr": 0}
+    assert po.selectlines(sel["tb"], 4, recs, st, sel["xmax"], sel["hckt"][-1], sel["iwt"], sel["wt"])[1:] == (-2, 123)
+
+
+def test_host_record_conversion():
+    """LINEREC kinds go to the library as int32 [n, 4]; MOL2 / H2O keep their layout."""
+    from atlas12_b200 import _lib, linelists
+    r = linelists.SelectLines._records(1, np.arange(40, dtype=np.int64).reshape(10, 4))
+    assert r.dtype == np.int32 and r.shape == (10, 4) and r.flags["C_CONTIGUOUS"]
+    t = np.zeros(3, _lib.MOL2_REC)
+    assert linelists.SelectLines._records(5, t).nbytes == 96
+    with pytest.raises(ValueError):
+        linelists.SelectLines._records(6, t)
+    with pytest.raises(ValueError):
+        linelists.SelectLines._records(2, np.zeros((5, 3), np.int32))
