@@ -71,6 +71,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--synthe-c3", action="store_true", help="also measure the 20M-line full-optical SYNTHE case")
     ap.add_argument("--slots", type=int, default=None, help="batch slots (default: one per model of a step)")
+    ap.add_argument("--no-select", action="store_true", help="skip the SELECTLINES line-database rates")
     ap.add_argument("--synthe-grid", type=int, default=0,
                     help="also time N atmospheres of the batched-grid SYNTHE workload, concurrent vs one at a time")
     return ap.parse_args()
@@ -362,6 +363,10 @@ def run_ours(args):
         if args.synthe_grid:
             syn["grid"] = synthe_grid_rate(local, ops, args.synthe_grid)
 
+    sel = None
+    if rank == 0 and world == 1 and not args.no_select:
+        sel = selectlines_rates(ctx, ops, cpu=not args.no_cpu)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(W, ops, plain["mean_iterations"] if plain else PLAIN_ITERS_PER_MODEL,
@@ -379,7 +384,7 @@ def run_ours(args):
                 "mean_iterations_per_model": float(np.mean(iters)),
                 "kernel_ms_per_model_iteration": per_model, "roofline": roof, "cpu_baseline": cpu,
                 "plain_fp64": plain, "vs_plain_fp64": (value / plain["value"]) if plain and plain["value"] else None,
-                "single_model": single, "synthe": syn,
+                "single_model": single, "synthe": syn, "selectlines": sel,
                 "e2e": {"value": e2e_value, "unit": "models/hr", "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h)},
                 "gpu_launches": int(gpu_launches), "clocks": clk}
@@ -389,6 +394,79 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+# SELECTLINES workloads: one database loop per record format, each input
+# 320 MB (larger than L2), records in file (wavelength) order
+SELECT_CASES = [("gfpred LINEREC (16 B)", 1, 20_000_000), ("TiO MOL2 (32 B)", 5, 10_000_000),
+                ("H2O (8 B)", 6, 40_000_000)]
+# DRAM bytes of one 12M-record LINEREC launch (ncu): 216 MB, 18.0 B per record
+SELECT_TRAFFIC_PER_LINEREC = 18.0
+
+
+def hbm_peak():
+    """Measured copy bandwidth of this pool's B200s, else the stated fallback (GB/s)."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs"
+    except (OSError, KeyError, ValueError, TypeError):
+        return 6650.0, "fallback 6.65 TB/s (no MEASURED_PEAKS.json)"
+
+
+def selectlines_rates(ctx, ops, cpu=True, reps=3):
+    """SELECTLINES (one database loop) per record format: the selection
+    kernel's time (CUDA events in the library, best of reps after a warm-up,
+    inputs resident in HBM), its HBM roofline (records read + LINEDATA
+    written), the host entry point end to end (records from host memory,
+    LINEDATA back), and the oracle on a 2M-record sample (one core)."""
+    import torch
+    from atlas12_b200 import atlas, linelists, synthetic
+    wt = ops["wavetab"]
+    xn, hckt, tc = synthetic.selectlines_tables(wt)
+    S = linelists.SelectLines(ctx, 72, xn, hckt, tc, atlas.iwavetab(wt), wt)
+    peak, src = hbm_peak()
+    out = {"tables": "synthetic XNFDOP/TABCONT over the reference's WAVETAB (361 bins), 1006 species, 72 depths",
+           "peak_gbs": peak, "peak_source": src, "cases": []}
+    ctx.enable_timing(True)
+    for name, kind, n in SELECT_CASES:
+        recs = synthetic.selectlines_records(kind, n, wt, seed=1)
+        raw = np.ascontiguousarray(recs).view(np.uint8)
+        d_in = torch.from_numpy(raw).cuda()
+        d_out = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+        ms = []
+        for _ in range(reps + 1):
+            st = linelists.initial_state(wt)
+            m = S.select_dev(kind, d_in, n, st, d_out, n)
+            ms.append(ctx.kernel_ms("k_selectlines"))
+        k_ms = min(ms[1:])
+        algo = raw.nbytes + 16 * m
+        t0 = time.perf_counter()
+        st = linelists.initial_state(wt)
+        host_out = S.select(kind, recs, st)
+        e2e = time.perf_counter() - t0
+        case = {"database": name, "records": n, "selected": m, "kernel_ms": k_ms,
+                "records_per_s": n / (k_ms * 1e-3), "algorithmic_bytes": int(algo),
+                "roofline": {"bound": "hbm", "achieved": algo / (k_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": algo / (k_ms * 1e-3) / 1e9 / peak,
+                             "traffic": SELECT_TRAFFIC_PER_LINEREC * n if kind == 1 else None},
+                "e2e": {"records_per_s": n / e2e, "h2d_bytes": int(raw.nbytes),
+                        "d2h_bytes": int(host_out.nbytes)}}
+        if cpu:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import pyoracle as po
+            sub = recs[:2_000_000]
+            tb = {k: ops[k] for k in ("molcodes", "isox", "tio_isocorr", "h2o_isocorr")}
+            xmax = po.xnfdopmax(72, xn, tc)
+            t0 = time.perf_counter()
+            po.selectlines(tb, kind, sub, linelists.initial_state(wt), xmax, hckt[-1], atlas.iwavetab(wt), wt)
+            dt = time.perf_counter() - t0
+            case["cpu_baseline"] = {"records_per_s": len(sub) / dt, "cores": 1, "kind": "port",
+                                    "sample": f"first {len(sub)} records of the same database"}
+        out["cases"].append(case)
+        del d_in, d_out
+    ctx.enable_timing(False)
+    return out
 
 
 def synthe_rates(ctx, ops, nlines, wlbeg, wlend, mol_frac, seed=1):
