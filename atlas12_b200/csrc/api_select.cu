@@ -45,8 +45,16 @@ size_t rec_bytes(int kind) { return kind == kSelTio ? 32 : kind == kSelH2o ? 8 :
 
 size_t sel_smem(int kind) { return std::max<size_t>(rec_bytes(kind), 16) * (kSelTile + kSelThreads); }
 
+// pass A (tile maxima of UB), the scan of NU at each tile's entry, pass B
 template <int K>
 int launch_select(atlasgpu_ctx* ctx, const SelArgs& a, int ntiles) {
+  int* d_tub;
+  int r;
+  if ((r = bufT(ctx, "sel_tub", ntiles, &d_tub))) return r;
+  k_sel_tile_ub<K><<<ntiles, kSelThreads, 0, ctx->stream>>>(a, d_tub);
+  CKL(ctx);
+  k_sel_scan<true><<<1, 1024, 0, ctx->stream>>>(d_tub, ntiles, a.nu0, const_cast<long long*>(a.tile_nu));
+  CKL(ctx);
   const size_t smem = sel_smem(K);
   CK(cudaFuncSetAttribute(k_selectlines<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_selectlines<K><<<ntiles, kSelThreads, smem, ctx->stream>>>(a);
@@ -115,27 +123,33 @@ int tio_overrides(atlasgpu_ctx* ctx, const void* d_recs, int64_t n, const long l
   return 0;
 }
 
-// The selection pass and the host's decisions.  last_rec_igr: the IGR field
-// of the last input record (LINEREC kinds), which UNPACK_LINEDATA leaves in
-// the module variable.
-int select_core(atlasgpu_ctx* ctx, int kind, const void* d_recs, int64_t n, atlasgpu_select_state* st, int4* d_out,
-                int64_t cap, int64_t* n_out, int16_t last_rec_igr) {
+// Records per pass of the kernels (scratch: 16 bytes per record)
+constexpr int64_t kSelChunk = int64_t(1) << 27;
+
+// One chunk through passes A-C and the host's decisions.  Output at d_out
+// (at most cap records); *n_out the count; error records offset by rec0.
+int select_chunk(atlasgpu_ctx* ctx, int kind, const void* d_recs, int64_t n, atlasgpu_select_state* st, int4* d_out,
+                 int64_t cap, int64_t* n_out, int64_t rec0) {
   const int nwave = ctx->sel_nwave;
   const long long* d_ovr_idx = nullptr;
   const int* d_ovr_iwl = nullptr;
   int novr = 0, r;
   if (kind == kSelTio && (r = tio_overrides(ctx, d_recs, n, &d_ovr_idx, &d_ovr_iwl, &novr))) return r;
 
-  const long long ntiles = (n + kSelTile - 1) / kSelTile;
-  unsigned long long *d_desc, *d_err;
-  unsigned* d_misc;  // ticket, nfix, timeout
+  const int ntiles = (int)((n + kSelTile - 1) / kSelTile);
+  int *d_tub, *d_cnt;
+  long long *d_nu, *d_off;
+  int4* d_scr;
+  unsigned long long* d_err;
+  unsigned* d_nfix;
   SelFix* d_fix;
-  if ((r = bufT(ctx, "sel_desc", 2 * ntiles, &d_desc)) || (r = bufT(ctx, "sel_err", 1, &d_err)) ||
-      (r = bufT(ctx, "sel_misc", 4, &d_misc)) || (r = bufT(ctx, "sel_fix", kFixCap, &d_fix)))
+  if ((r = bufT(ctx, "sel_tub", ntiles, &d_tub)) || (r = bufT(ctx, "sel_tcnt", ntiles, &d_cnt)) ||
+      (r = bufT(ctx, "sel_tnu", ntiles + 1, &d_nu)) || (r = bufT(ctx, "sel_toff", ntiles + 1, &d_off)) ||
+      (r = bufT(ctx, "sel_scratch", (size_t)ntiles * kSelTile, &d_scr)) || (r = bufT(ctx, "sel_err", 1, &d_err)) ||
+      (r = bufT(ctx, "sel_nfix", 1, &d_nfix)) || (r = bufT(ctx, "sel_fix", kFixCap, &d_fix)))
     return r;
-  CK(cudaMemsetAsync(d_desc, 0, 2 * ntiles * sizeof(unsigned long long), ctx->stream));
   CK(cudaMemsetAsync(d_err, 0xff, sizeof(unsigned long long), ctx->stream));
-  CK(cudaMemsetAsync(d_misc, 0, 4 * sizeof(unsigned), ctx->stream));
+  CK(cudaMemsetAsync(d_nfix, 0, sizeof(unsigned), ctx->stream));
 
   SelArgs a{};
   a.recs = d_recs;
@@ -166,40 +180,43 @@ int select_core(atlasgpu_ctx* ctx, int kind, const void* d_recs, int64_t n, atla
   a.ovr_idx = d_ovr_idx;
   a.ovr_iwl = d_ovr_iwl;
   a.novr = novr;
-  a.desc_nu = d_desc;
-  a.desc_cnt = d_desc + ntiles;
-  a.ticket = d_misc;
-  a.out = d_out;
-  a.cap = cap;
+  a.tile_nu = d_nu;
+  a.tile_count = d_cnt;
+  a.scratch = d_scr;
   a.fix = d_fix;
-  a.nfix = d_misc + 1;
+  a.nfix = d_nfix;
   a.fixcap = kFixCap;
   a.err = d_err;
-  a.timeout = d_misc + 2;
   {
     Timer tk(ctx, "k_selectlines");
-    if ((r = dispatch(ctx, kind, a, (int)ntiles))) return r;
+    if ((r = dispatch(ctx, kind, a, ntiles))) return r;
+    k_sel_scan<false><<<1, 1024, 0, ctx->stream>>>(d_cnt, ntiles, 0, d_off);
+    CKL(ctx);
+    k_sel_move<<<std::min(ntiles, ctx->nsm * 8), 256, 0, ctx->stream>>>(d_scr, d_cnt, d_off, ntiles, d_out, cap);
+    CKL(ctx);
   }
+  k_sel_fixpos<<<(kFixCap + 255) / 256, 256, 0, ctx->stream>>>(d_fix, d_nfix, kFixCap, d_off);
+  CKL(ctx);
 
-  unsigned long long last[2], err;
-  unsigned misc[4];
-  CK(cudaMemcpyAsync(&last[0], d_desc + ntiles - 1, 8, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaMemcpyAsync(&last[1], d_desc + 2 * ntiles - 1, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  long long last[2];
+  unsigned long long err;
+  unsigned nfix;
+  CK(cudaMemcpyAsync(&last[0], d_nu + ntiles, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(&last[1], d_off + ntiles, 8, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaMemcpyAsync(&err, d_err, 8, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaMemcpyAsync(misc, d_misc, sizeof misc, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(&nfix, d_nfix, sizeof nfix, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  if (misc[2]) return fail(ctx, ATLASGPU_ETIMEOUT, "selectlines: a tile descriptor wait gave up");
   if (err != ~0ull)
-    return fail(ctx, ATLASGPU_EINVAL, "selectlines: record %lld: %s", (long long)(err >> 8), err_text((int)(err & 0xff)));
-  const int nu = (int)(last[0] & kSelValue);
-  int64_t total = (int64_t)(last[1] & kSelValue);
+    return fail(ctx, ATLASGPU_EINVAL, "selectlines: record %lld: %s", (long long)(err >> 8) + (long long)rec0,
+                err_text((int)(err & 0xff)));
+  const int nu = (int)last[0];
+  int64_t total = (int64_t)last[1];
   if (total > cap)
-    return fail(ctx, ATLASGPU_EINVAL, "selectlines: LINEDATA overflow (%lld selected, cap %lld)", (long long)total,
-                (long long)cap);
-  if (misc[1] > kFixCap) return fail(ctx, ATLASGPU_EINVAL, "selectlines: %u records near a rounding boundary", misc[1]);
+    return fail(ctx, ATLASGPU_EINVAL, "selectlines: LINEDATA overflow (record set beyond cap %lld)", (long long)cap);
+  if (nfix > kFixCap) return fail(ctx, ATLASGPU_EINVAL, "selectlines: %u records near a rounding boundary", nfix);
 
   // the host's decisions: fields first (positions before any removal), then the Boltzmann tests
-  std::vector<SelFix> fx(misc[1]);
+  std::vector<SelFix> fx(nfix);
   if (!fx.empty()) CK(cudaMemcpy(fx.data(), d_fix, fx.size() * sizeof(SelFix), cudaMemcpyDeviceToHost));
   std::vector<long long> drop;
   for (const SelFix& f : fx) {
@@ -233,22 +250,37 @@ int select_core(atlasgpu_ctx* ctx, int kind, const void* d_recs, int64_t n, atla
     CK(cudaStreamSynchronize(ctx->stream));
   }
 
-  // the module variables the loop leaves behind
+  // the module variables the loop leaves behind (IGR of the LINEREC kinds: by the caller)
   const bool adv = nu > st->nu;
   if (adv) st->freq = ctx->sel_freqtab[nu - 2];
   if (kind == kSelH2o) {
     if (adv) st->igr = ctx->sel_igrtab[nu - 2];
-  } else if (kind == kSelTio) {
-    if (total > 0) {
-      int4 rec;
-      CK(cudaMemcpy(&rec, d_out + total - 1, sizeof rec, cudaMemcpyDeviceToHost));
-      st->igr = (int16_t)((unsigned)rec.z >> 16);
-    }
-  } else {
-    st->igr = last_rec_igr;
+  } else if (kind == kSelTio && total > 0) {
+    int4 rec;
+    CK(cudaMemcpy(&rec, d_out + total - 1, sizeof rec, cudaMemcpyDeviceToHost));
+    st->igr = (int16_t)((unsigned)rec.z >> 16);
   }
   st->nu = nu;
   *n_out = total;
+  return 0;
+}
+
+// All records, a chunk at a time with the loop state carried over.
+// last_rec_igr: the IGR field of the last input record (LINEREC kinds),
+// which UNPACK_LINEDATA leaves in the module variable.
+int select_core(atlasgpu_ctx* ctx, int kind, const void* d_recs, int64_t n, atlasgpu_select_state* st, int4* d_out,
+                int64_t cap, int64_t* n_out, int16_t last_rec_igr) {
+  const size_t rb = rec_bytes(kind);
+  int64_t written = 0;
+  for (int64_t c0 = 0; c0 < n; c0 += kSelChunk) {
+    const int64_t cn = std::min(kSelChunk, n - c0);
+    int64_t m = 0;
+    int r = select_chunk(ctx, kind, (const char*)d_recs + c0 * rb, cn, st, d_out + written, cap - written, &m, c0);
+    if (r) return r;
+    written += m;
+  }
+  if (kind != kSelTio && kind != kSelH2o) st->igr = last_rec_igr;
+  *n_out = written;
   return 0;
 }
 

@@ -1,23 +1,25 @@
 // select.cuh -- SELECTLINES (atlas12_modules.f90:19171-19781) on the device:
 // the filter that turns the line databases into the LINEDATA records LINOP1
-// walks.  One pass over the records, HBM-bound:
+// walks.  HBM-bound streaming passes over tiles of 2048 records, with no
+// CTA waiting on another:
 //
 //  * the NU advance (DO WHILE (IWL >= IWAVETAB(NU)) ...) is a running
 //    maximum: after a record, NU = max(NU at entry, UB(max IWL so far)) with
-//    UB(x) = the first bin whose IWAVETAB exceeds x, so it is a max-scan over
-//    UB of the records in file order;
-//  * the selected records are compacted in file order, a sum-scan;
-//  * both scans are single pass: each CTA takes the next tile (a ticket),
-//    publishes its tile aggregate and looks back over its predecessors'
-//    descriptors (decoupled look-back), once for NU and once for the count.
+//    UB(x) = the first bin whose IWAVETAB exceeds x.  k_sel_tile_ub takes
+//    each tile's maximum UB and k_sel_scan the exclusive maximum over tiles,
+//    so a tile knows NU at its entry;
+//  * k_selectlines filters each tile at its records' NU and writes the
+//    selected LINEDATA compacted at the tile's own place in a scratch array,
+//    with the tile's count; k_sel_scan sums the counts and k_sel_move puts
+//    every tile's records at its offset, in file order.
 //
 // The tests follow the reference's arithmetic in FP64 with explicit
 // round-to-nearest operations.  Three quantities pass through a
 // transcendental the C library evaluates on the host (exp in the Boltzmann
 // test, log / log10 in the TiO and H2O fields).  Where the device result is
 // within a guard band of a decision boundary the record is listed for the
-// host, which decides with the C library: the TiO IWL before the pass (an
-// override table), the Boltzmann test and the IELO / IGR fields after it
+// host, which decides with the C library: the TiO IWL before the passes (an
+// override table), the Boltzmann test and the IELO / IGR fields after them
 // (a fix list with output positions).
 #pragma once
 #include <type_traits>
@@ -29,11 +31,8 @@ namespace atlasgpu {
 constexpr int kSelThreads = 256;
 constexpr int kSelItems = 8;
 constexpr int kSelTile = kSelThreads * kSelItems;  // records per tile
-constexpr int kSelGroup = 4;                       // records whose table loads are issued together
+constexpr int kSelGroup = 2;                       // records whose table loads are issued together
 constexpr int kSelMaxWave = 1024;                  // IWAVETAB entries held in shared memory
-constexpr unsigned long long kSelFlagA = 1ull << 62;  // tile aggregate published
-constexpr unsigned long long kSelFlagP = 2ull << 62;  // inclusive prefix published
-constexpr unsigned long long kSelValue = (1ull << 62) - 1;
 constexpr double kSelKeepBand = 1.0e-12;  // |CENRATIO*exp(...) - 1| left to the host
 constexpr double kSelIntBand = 1.0e-6;    // distance of an INT() argument from an integer left to the host
 
@@ -80,16 +79,13 @@ struct SelArgs {
   const long long* ovr_idx;  // TiO records whose IWL the host decided, sorted
   const int* ovr_iwl;
   int novr;
-  unsigned long long* desc_nu;   // [ntiles] look-back descriptors
-  unsigned long long* desc_cnt;  // [ntiles]
-  unsigned int* ticket;
-  int4* out;
-  long long cap;
+  const long long* tile_nu;  // [ntiles] NU at entry to each tile (exclusive maximum of UB, NU at entry first)
+  int* tile_count;      // [ntiles] selected records per tile
+  int4* scratch;        // [ntiles * kSelTile] each tile's LINEDATA, compacted at the tile's start
   SelFix* fix;
   unsigned int* nfix;
   unsigned int fixcap;
   unsigned long long* err;  // min over (record << 8 | code)
-  unsigned int* timeout;
 };
 
 __device__ __forceinline__ int sel_fint(double x) {
@@ -98,63 +94,6 @@ __device__ __forceinline__ int sel_fint(double x) {
 }
 __device__ __forceinline__ short sel_i16(int v) { return (short)(unsigned short)(unsigned)v; }
 __device__ __forceinline__ bool sel_near_int(double x) { return fabs(x - rint(x)) <= kSelIntBand; }
-
-__device__ __forceinline__ unsigned long long sel_ld_acquire(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void sel_st_release(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-// bounded wait for a descriptor; on timeout the identity (0) as an
-// inclusive prefix, and the call reports ATLASGPU_ETIMEOUT
-__device__ __forceinline__ unsigned long long sel_wait(const unsigned long long* p, unsigned int* timeout) {
-  for (unsigned it = 0;; ++it) {
-    const unsigned long long v = sel_ld_acquire(p);
-    if (v >> 62) return v;
-    // after one wait has given up, the others do not wait again
-    if (it >= (1u << 22) || ((it & 1023u) == 1023u && *(volatile unsigned int*)timeout)) {
-      atomicExch(timeout, 1u);
-      return kSelFlagP;
-    }
-    __nanosleep(it < 32 ? 32 : 256);
-  }
-}
-
-// Exclusive prefix of tile `tile` over desc under op (max when MAX, else
-// sum), walking 32 predecessors at a time; warp 0 calls it.  init is the
-// value before tile 0.  Publishes this tile's inclusive prefix.
-template <bool MAX>
-__device__ unsigned long long sel_lookback(unsigned long long* desc, int tile, unsigned long long agg,
-                                           unsigned long long init, unsigned int* timeout) {
-  const int lane = threadIdx.x & 31;
-  unsigned long long excl = init;
-  if (tile > 0) {
-    if (lane == 0) sel_st_release(desc + tile, kSelFlagA | agg);
-    excl = 0;
-    for (int j = tile - 1;; j -= 32) {
-      const int idx = j - lane;
-      const unsigned long long d = idx >= 0 ? sel_wait(desc + idx, timeout) : kSelFlagP;
-      const unsigned pmask = __ballot_sync(0xffffffffu, (d >> 62) == 2ull);
-      const int first = pmask ? __ffs(pmask) - 1 : 32;
-      unsigned long long v = lane <= first ? (d & kSelValue) : 0ull;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
-        v = MAX ? (w > v ? w : v) : v + w;
-      }
-      excl = MAX ? (v > excl ? v : excl) : excl + v;
-      if (pmask) break;
-    }
-  }
-  if (lane == 0) {
-    const unsigned long long inc = MAX ? (agg > excl ? agg : excl) : excl + agg;
-    sel_st_release(desc + tile, kSelFlagP | inc);
-  }
-  return excl;
-}
 
 // TiO's IWL = INT(LOG(WLVAC)/RATIOLG + 0.5) and whether the record takes
 // part in the NU advance (molecule 822, Ti isotope 46-50, WLVAC > 0)
@@ -212,9 +151,9 @@ struct SelRecType<kSelH2o> {
   using T = SelH2o;
 };
 
-// padded shared-memory slot of the k-th record of a tile: each thread's
-// kSelItems consecutive records are followed by one spare, so the blocked
-// reads of a warp fall in different banks
+// padded slot of the k-th record of a tile: each thread's kSelItems
+// consecutive records are followed by one spare, so the blocked reads of a
+// warp fall in different banks
 __device__ __forceinline__ int sel_slot(int k) { return k + k / kSelItems; }
 
 // UB(x): the first 1-based bin k with IWAVETAB(k) > x, over the shared copy
@@ -523,9 +462,95 @@ __device__ __forceinline__ void sel_push_fixes(const SelArgs& a, const typename 
   }
 }
 
-// The selection pass: one tile of kSelTile records per CTA.
+// Pass A: the largest UB of each tile's records (the NU a tile leaves
+// behind, before the carry from earlier tiles).  Record k of the tile is
+// read by thread k % 256: the maximum does not depend on the order.
 template <int KIND>
-__global__ void __launch_bounds__(kSelThreads, 3) k_selectlines(SelArgs a) {
+__global__ void __launch_bounds__(kSelThreads) k_sel_tile_ub(SelArgs a, int* __restrict__ tile_ub) {
+  using R = typename SelRecType<KIND>::T;
+  __shared__ int s_iwt[kSelMaxWave];
+  __shared__ int s_warp[kSelThreads / 32];
+  const int t = threadIdx.x, tile = blockIdx.x;
+  for (int k = t; k <= a.nwave; k += kSelThreads) s_iwt[k] = a.iwt[k];
+  __syncthreads();
+  const long long base = (long long)tile * kSelTile;
+  const int cnt = (int)min((long long)kSelTile, a.n - base);
+  const R* g = reinterpret_cast<const R*>(a.recs) + base;
+  int m = 0;
+#pragma unroll 4
+  for (int k = t; k < cnt; k += kSelThreads) {
+    int iwl;
+    if (sel_advance_iwl<KIND>(g[k], a, base + k, &iwl)) {
+      const int u = min(sel_ub(s_iwt, a.nwave, iwl, 0), a.nwave + 1);
+      m = u > m ? u : m;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((t & 31) == 0) s_warp[t >> 5] = m;
+  __syncthreads();
+  if (t == 0) {
+    int r = 0;
+    for (int w = 0; w < kSelThreads / 32; ++w) r = max(r, s_warp[w]);
+    tile_ub[tile] = r;
+  }
+}
+
+// Exclusive scan over n tile values by one CTA of 1024 threads, in chunks:
+// the maximum with `init` folded in first (MAX), or the sum from 0.  out[n]
+// receives the total.
+template <bool MAX>
+__global__ void __launch_bounds__(1024) k_sel_scan(const int* __restrict__ in, int n, long long init,
+                                                   long long* __restrict__ out) {
+  __shared__ long long s_warp[32];
+  __shared__ long long s_carry;
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  if (t == 0) s_carry = MAX ? init : 0;
+  __syncthreads();
+  for (int c0 = 0; c0 < n; c0 += 1024) {
+    const int i = c0 + t;
+    long long v = i < n ? (long long)in[i] : 0;
+    long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x = MAX ? (y > x ? y : x) : x + y;
+    }
+    if (lane == 31) s_warp[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      long long w = s_warp[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w = MAX ? (y > w ? y : w) : w + y;
+      }
+      s_warp[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    const long long carry = s_carry;
+    const long long before = wid > 0 ? s_warp[wid - 1] : (MAX ? 0 : 0);
+    const long long xin = __shfl_up_sync(0xffffffffu, x, 1);
+    long long ex = lane > 0 ? (MAX ? (before > xin ? before : xin) : before + xin) : before;
+    ex = MAX ? (ex > carry ? ex : carry) : ex + carry;
+    if (i < n) out[i] = ex;
+    __syncthreads();
+    if (t == 1023) {
+      const long long inc = MAX ? (ex > v ? ex : v) : ex + v;
+      s_carry = inc;
+    }
+    __syncthreads();
+  }
+  if (t == 0) out[n] = s_carry;
+}
+
+// Pass B: the filter.  One tile of kSelTile records per CTA, staged
+// coalesced in shared memory; thread t takes records 8t..8t+7.  NU at the
+// tile's entry comes from the scan of pass A.  The selected records'
+// LINEDATA goes to the tile's place in the scratch array, compacted in file
+// order, with the host's cases listed at their scratch positions.
+template <int KIND>
+__global__ void __launch_bounds__(kSelThreads, 4) k_selectlines(SelArgs a) {
   using R = typename SelRecType<KIND>::T;
   using Slot = SelSlotT<R>;
   extern __shared__ __align__(16) unsigned char sel_smem[];
@@ -533,24 +558,20 @@ __global__ void __launch_bounds__(kSelThreads, 3) k_selectlines(SelArgs a) {
   __shared__ int s_iwt[kSelMaxWave];
   __shared__ int s_molcor[KIND == kSelDiatomic ? kSelMolN : 1];
   __shared__ int s_warp[kSelThreads / 32];
-  __shared__ int s_tile;
-  __shared__ unsigned long long s_excl;
   auto rec = [&](int k) -> const R& { return *reinterpret_cast<const R*>(&s_slot[sel_slot(k)]); };
 
-  const int t = threadIdx.x;
-  if (t == 0) s_tile = (int)atomicAdd(a.ticket, 1u);
+  const int t = threadIdx.x, tile = blockIdx.x;
   for (int k = t; k <= a.nwave; k += kSelThreads) s_iwt[k] = a.iwt[k];
   if constexpr (KIND == kSelDiatomic)
     for (int k = t; k < kSelMolN; k += kSelThreads) s_molcor[k] = a.molcor[k];
-  __syncthreads();
-  const int tile = s_tile;
   const long long base = (long long)tile * kSelTile;
   const int cnt = (int)min((long long)kSelTile, a.n - base);
   const R* g = reinterpret_cast<const R*>(a.recs) + base;
   for (int k = t; k < cnt; k += kSelThreads) *reinterpret_cast<R*>(&s_slot[sel_slot(k)]) = g[k];
+  const int tile_nu = (int)a.tile_nu[tile];
   __syncthreads();
 
-  // pass 1: UB of each record's IWL, running max in file order
+  // UB of each record's IWL, running maximum in file order
   int run = 0, hint = 0;
   int ubs[kSelItems];
 #pragma unroll
@@ -573,16 +594,10 @@ __global__ void __launch_bounds__(kSelThreads, 3) k_selectlines(SelArgs a) {
   }
   int agg;
   const int pre = block_scan_excl<kSelThreads>(run, s_warp, &agg, true);
-  if (t < 32) {
-    const unsigned long long e = sel_lookback<true>(a.desc_nu, tile, (unsigned long long)agg,
-                                                    (unsigned long long)a.nu0, a.timeout);
-    if (t == 0) s_excl = e;
-  }
-  __syncthreads();
-  const int nu_in = (int)s_excl > pre ? (int)s_excl : pre;  // NU before this thread's records
+  const int nu_in = tile_nu > pre ? tile_nu : pre;  // NU before this thread's records
 
-  // pass 2: the filter at each record's NU, operands gathered a group at a
-  // time; a selected record's LINEDATA replaces it in its slot
+  // the filter at each record's NU, operands gathered a group at a time; a
+  // selected record's LINEDATA replaces it in its slot
   int nu = nu_in;
   unsigned sel = 0, keep = 0, fixbits = 0;
   int mycount = 0;
@@ -617,28 +632,46 @@ __global__ void __launch_bounds__(kSelThreads, 3) k_selectlines(SelArgs a) {
   }
   int total;
   const int opre = block_scan_excl<kSelThreads>(mycount, s_warp, &total, false);
-  if (t < 32) {
-    const unsigned long long e = sel_lookback<false>(a.desc_cnt, tile, (unsigned long long)total, 0ull, a.timeout);
-    if (t == 0) s_excl = e;
-  }
-  __syncthreads();
-  const long long obase = (long long)s_excl;
+  if (t == 0) a.tile_count[tile] = total;
 
-  // store the selected records in file order; list the host's cases (the
-  // original record comes from global memory: its slot now holds LINEDATA)
-  long long q = obase + opre;
+  // the tile's LINEDATA to its scratch place in file order; the host's cases
+  // (the original record comes from global memory: its slot holds LINEDATA)
+  int4* sc = a.scratch + base;
+  int q = opre;
   nu = nu_in;
 #pragma unroll
   for (int i = 0; i < kSelItems; ++i) {
     nu = ubs[i] > nu ? ubs[i] : nu;
     if (sel >> i & 1u) {
       const int k = t * kSelItems + i;
-      if (q < a.cap) a.out[q] = *reinterpret_cast<const int4*>(&s_slot[sel_slot(k)]);
+      sc[q] = *reinterpret_cast<const int4*>(&s_slot[sel_slot(k)]);
       const unsigned fx = (fixbits >> (2 * i)) & 3u;
-      if ((keep >> i & 1u) || fx) sel_push_fixes<KIND>(a, g[k], base + k, q, nu, keep >> i & 1u, fx, s_molcor);
+      if ((keep >> i & 1u) || fx) sel_push_fixes<KIND>(a, g[k], base + k, base + q, nu, keep >> i & 1u, fx, s_molcor);
       ++q;
     }
   }
+}
+
+// Pass C: every tile's LINEDATA from its scratch place to its offset (the
+// exclusive sum of the counts); positions at or past cap are not written
+__global__ void __launch_bounds__(256) k_sel_move(const int4* __restrict__ scratch, const int* __restrict__ count,
+                                                  const long long* __restrict__ off, int ntiles, int4* out,
+                                                  long long cap) {
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int c = count[tile];
+    const long long o = off[tile];
+    const int4* src = scratch + (long long)tile * kSelTile;
+    for (int k = threadIdx.x; k < c; k += blockDim.x)
+      if (o + k < cap) out[o + k] = src[k];
+  }
+}
+
+// the fix list's scratch positions -> output positions
+__global__ void k_sel_fixpos(SelFix* fix, const unsigned* nfix, unsigned fixcap, const long long* __restrict__ off) {
+  const unsigned e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= min(*nfix, fixcap)) return;
+  const long long p = fix[e].pos;
+  fix[e].pos = off[p / kSelTile] + p % kSelTile;
 }
 
 // drop the records at sorted positions rm [nrm] from in [n] into out

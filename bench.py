@@ -400,8 +400,9 @@ def run_ours(args):
 # 320 MB (larger than L2), records in file (wavelength) order
 SELECT_CASES = [("gfpred LINEREC (16 B)", 1, 20_000_000), ("TiO MOL2 (32 B)", 5, 10_000_000),
                 ("H2O (8 B)", 6, 40_000_000)]
-# DRAM bytes of one 12M-record LINEREC launch (ncu): 216 MB, 18.0 B per record
-SELECT_TRAFFIC_PER_LINEREC = 18.0
+# DRAM bytes of one 12M-record LINEREC call, all its kernels (ncu): 437 MB,
+# 36.4 B per record (the tile-maximum pass reads the records a second time)
+SELECT_TRAFFIC_PER_LINEREC = 36.4
 
 
 def hbm_peak():
@@ -415,11 +416,12 @@ def hbm_peak():
 
 
 def selectlines_rates(ctx, ops, cpu=True, reps=3):
-    """SELECTLINES (one database loop) per record format: the selection
-    kernel's time (CUDA events in the library, best of reps after a warm-up,
-    inputs resident in HBM), its HBM roofline (records read + LINEDATA
-    written), the host entry point end to end (records from host memory,
-    LINEDATA back), and the oracle on a 2M-record sample (one core)."""
+    """SELECTLINES (one database loop) per record format: the device passes'
+    time (CUDA events in the library around all of them, best of reps after
+    a warm-up, inputs resident in HBM), their HBM roofline (records read +
+    LINEDATA written), the host entry point end to end (records from host
+    memory, LINEDATA back; best of two calls), and the oracle on a 2M-record
+    sample (one core)."""
     import torch
     from atlas12_b200 import atlas, linelists, synthetic
     wt = ops["wavetab"]
@@ -441,10 +443,12 @@ def selectlines_rates(ctx, ops, cpu=True, reps=3):
             ms.append(ctx.kernel_ms("k_selectlines"))
         k_ms = min(ms[1:])
         algo = raw.nbytes + 16 * m
-        t0 = time.perf_counter()
-        st = linelists.initial_state(wt)
-        host_out = S.select(kind, recs, st)
-        e2e = time.perf_counter() - t0
+        e2e = float("inf")
+        for _ in range(2):  # the first call also grows the context's buffers
+            t0 = time.perf_counter()
+            st = linelists.initial_state(wt)
+            host_out = S.select(kind, recs, st)
+            e2e = min(e2e, time.perf_counter() - t0)
         case = {"database": name, "records": n, "selected": m, "kernel_ms": k_ms,
                 "records_per_s": n / (k_ms * 1e-3), "algorithmic_bytes": int(algo),
                 "roofline": {"bound": "hbm", "achieved": algo / (k_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
