@@ -84,11 +84,14 @@ class Atlas:
                       ctypes.byref(used))
         return out, used.value
 
-    def xlinop(self, records, nrhox, xnfdop, dopple, xne, txnxn, hckt, tabcont, iwt, waveset, contx, xlines=None):
-        """XLINOP's normal-line branch on unit-19 records (NLTE_LINE array,
-        sorted by wavelength), added into a copy of xlines [numnu, kw] (zeros
-        when None).  contx: CONTX(25,16) as [16, 25].  Returns (xlines,
-        number of records of the types this branch does not handle)."""
+    def xlinop(self, records, nrhox, xnfdop, dopple, xne, txnxn, hckt, tabcont, iwt, waveset, contx, xlines=None,
+               xnfp=None, rho=None):
+        """XLINOP on unit-19 records (NLTE_LINE array, sorted by wavelength),
+        added into a copy of xlines [numnu, kw] (zeros when None).  contx:
+        CONTX(25,16) as [16, 25].  With xnfp [nspec, kw] and rho [kw] also the
+        autoionizing and merged-continuum records.  Returns (xlines, number of
+        records of the types not handled: hydrogen, and those two without
+        populations)."""
         rec = np.ascontiguousarray(records, _lib.NLTE_LINE)
         xd = np.ascontiguousarray(xnfdop, np.float64)
         dp = np.ascontiguousarray(dopple, np.float64)
@@ -100,9 +103,11 @@ class Atlas:
         cx = np.ascontiguousarray(contx, np.float64)
         out = np.zeros((ws.size, kw)) if xlines is None else np.array(xlines, np.float64, copy=True, order="C")
         other = ctypes.c_int64(0)
+        xp = None if xnfp is None else np.ascontiguousarray(xnfp, np.float64)
+        rh = None if rho is None else np.ascontiguousarray(rho, np.float64)
         self.ctx.call("atlasgpu_atlas_xlinop", ptr(rec), rec.shape[0], int(nrhox), kw, ptr(xd), ptr(dp), nspec,
-                      *[ptr(v) for v in vec], ptr(tc), ptr(iw), iw.size - 1, ptr(ws), ws.size, ptr(cx), ptr(out),
-                      ctypes.byref(other))
+                      *[ptr(v) for v in vec], ptr(tc), ptr(iw), iw.size - 1, ptr(ws), ws.size, ptr(cx), ptr(xp),
+                      ptr(rh), ptr(out), ctypes.byref(other))
         return out, other.value
 
     def rt_pass(self, waveset, rcoset, acont, sigmac, xlines, rhox, t, hkt, teff, scont=None):

@@ -230,11 +230,13 @@ int atlasgpu_atlas_xlinop(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* recs, int
                           const double* xnfdop, const double* dopple, int nspec, const double* xne,
                           const double* txnxn, const double* hckt, const double* tabcont,
                           const int32_t* iwavetab, int nwave, const double* waveset, int numnu,
-                          const double* contx, double* xlines_inout, int64_t* n_other) {
+                          const double* contx, const double* xnfp, const double* rho, double* xlines_inout,
+                          int64_t* n_other) {
   if (!ctx || n < 0 || (n > 0 && !recs) || nrhox < 8 || kw < nrhox || kw > kKwMax || nspec < 1 || !xnfdop ||
       !dopple || !xne || !txnxn || !hckt || !tabcont || !iwavetab || nwave < 1 || !waveset || numnu < 2 ||
-      !contx || !xlines_inout)
+      !contx || !xlines_inout || (!xnfp) != (!rho))
     return fail(ctx, ATLASGPU_EINVAL, "atlas_xlinop: bad argument");
+  const bool pops = xnfp != nullptr;
   if (ctx->bufs.find("tab_h0") == ctx->bufs.end())
     return fail(ctx, ATLASGPU_ESTATE, "atlas_xlinop: Voigt tables not set");
   for (int i = 1; i < numnu; ++i)
@@ -247,7 +249,7 @@ int atlasgpu_atlas_xlinop(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* recs, int
     if ((t == 0 || t == 3) && nc > 0 && (recs[i].nelionx < 1 || recs[i].nelionx > 16))
       return fail(ctx, ATLASGPU_EINVAL, "atlas_xlinop: NELIONX %d outside CONTX at record %lld", recs[i].nelionx,
                   (long long)i);
-    other += (t != 0 && t != 2 && t != 3);
+    other += t == -1 || (!pops && t != 0 && t != 2 && t != 3);
   }
   if (n_other) *n_other = other;
   cudaSetDevice(ctx->device);
@@ -297,6 +299,15 @@ int atlasgpu_atlas_xlinop(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* recs, int
     if (ctx->precision == ATLASGPU_PREC_MIXED) k_atlas_linop<true><<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
     else k_atlas_linop<false><<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
     CKL(ctx);
+    if (pops) {
+      double *d_xp, *d_rho;
+      if ((r = bufT(ctx, "xl_xnfp", nd, &d_xp)) || (r = bufT(ctx, "xl_rho", kw, &d_rho))) return r;
+      CK(cudaMemcpyAsync(d_xp, xnfp, nd * sizeof(double), cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(d_rho, rho, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+      XShoreArgs xa{d_rec, d_lines, n, nrhox, kw, nspec, numnu, d_ws, d_tc, d_xp, d_rho, d_hc, d_em, d_xl};
+      k_xlinop_shore<<<grid_for(ctx, n * nrhox * 32, 256, 16), 256, 0, s>>>(xa);
+      CKL(ctx);
+    }
   }
   CK(cudaMemcpyAsync(xlines_inout, d_xl, (size_t)kw * numnu * sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));

@@ -149,6 +149,92 @@ static __global__ void k_xlinop_prep(XlinopPrepArgs a) {
   }
 }
 
+// XLINOP's autoionizing (TYPE 1, Fano profile, atlas12_modules.f90:20201-20226)
+// and merged-continuum (any other TYPE but 0, 2, 3 and -1, :20228-20245)
+// records: one warp per (record, depth), 32 grid points per step; the same
+// operations as the reference per point, FP64 atomics into XLINES.
+struct XShoreArgs {
+  const atlasgpu_nlte_line* rec;
+  const AtlasLine* lines;  // NU and NUCONT of every record (k_xlinop_prep)
+  int64_t n;
+  int nrhox, kw, nspec, numnu;
+  const double* waveset;
+  const double* tabcont;    // [nwave+1][kw]
+  const double *xnfp, *rho;  // XNFP(J,NELION) [nspec][kw], RHO(J) [kw]
+  const double *hckt, *emerge;
+  double* xl;               // XLINES(J, NU): [numnu][kw]
+};
+
+static __global__ void __launch_bounds__(256) k_xlinop_shore(XShoreArgs a) {
+  constexpr double kRydbergInf = 109737.31568157;
+  const int lane = threadIdx.x & 31;
+  const int64_t npairs = a.n * a.nrhox;
+  const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t p = w0; p < npairs; p += nw) {
+    const int64_t i = p / a.nrhox;
+    const int j = (int)(p - i * a.nrhox);
+    const atlasgpu_nlte_line r = a.rec[i];
+    const int t = r.itype;
+    if (t == 0 || t == 2 || t == 3 || t == -1) continue;
+    const int nu = a.lines[i].nu, nucont = a.lines[i].nucont;
+    if (nu >= a.numnu || r.nelion < 1 || r.nelion > a.nspec) continue;
+    const double xnfp = a.xnfp[(size_t)(r.nelion - 1) * a.kw + j], rho = a.rho[j];
+    const double bz = exp(-((double)r.elo * a.hckt[j]));
+    double* xl = a.xl + j;
+    if (t == 1) {
+      const double tc = a.tabcont[(size_t)(nucont - 1) * a.kw + j];
+      const double g = (double)r.gf, ashore = (double)r.gammas, bshore = (double)r.gammaw;
+      const double gammar = (double)r.gammar;
+      const double frelin = __ddiv_rn(kClightNms, r.wlvac);
+      double center = __ddiv_rn(__dmul_rn(__dmul_rn(bshore, g), xnfp), rho);
+      if (center < tc) continue;
+      center = __dmul_rn(center, bz);
+      if (center < tc) continue;
+      // red wing NU .. min(NU + 2000, NUMNU), blue wing NU-1 .. max(NU-2000, 1)
+      for (int side = 0; side < 2; ++side) {
+        const int first = side == 0 ? nu : nu - 1;
+        const int count = side == 0 ? min(nu + 2000, a.numnu) - nu + 1 : min(2000, nu - 1);
+        for (int s0 = 0; s0 < count; s0 += 32) {
+          const int s = s0 + lane;
+          const bool valid = s < count;
+          const int iw = side == 0 ? first + s : first - s;
+          double cv = 0.0;
+          if (valid) {
+            const double ep = __ddiv_rn(
+                __dmul_rn(2.0, __dsub_rn(__ddiv_rn(kClightNms, a.waveset[iw - 1]), frelin)), gammar);
+            cv = __ddiv_rn(__ddiv_rn(__dmul_rn(center, __dadd_rn(__dmul_rn(ashore, ep), bshore)),
+                                     __dadd_rn(__dmul_rn(ep, ep), 1.0)),
+                           bshore);
+          }
+          const unsigned below = __ballot_sync(0xffffffffu, valid && cv < tc);
+          const int stop = below ? __ffs(below) - 1 : 32;  // the first point below TABCONT is added, then the wing ends
+          if (valid && lane <= stop) atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
+          if (below) break;
+        }
+      }
+    } else {
+      const double z = r.nelion == 4 ? 2.0 : 1.0;
+      const double nlast = (double)t;
+      const double rw = __ddiv_rn(1.0e7, r.wlvac);
+      const double wshift =
+          __ddiv_rn(1.0e7, __dsub_rn(rw, __ddiv_rn(__dmul_rn(kRydbergInf, __dmul_rn(z, z)), __dmul_rn(nlast, nlast))));
+      const double wmerge = __ddiv_rn(1.0e7, __dsub_rn(rw, __dmul_rn(a.emerge[j], __dmul_rn(z, z))));
+      const double wmax = wmerge > wshift ? wmerge : wshift;
+      const double con = __ddiv_rn(__dmul_rn(__dmul_rn((double)r.gf, xnfp), bz), rho);
+      const int hi = min(nu + 1000, a.numnu);
+      for (int iw0 = nu; iw0 <= hi; iw0 += 32) {
+        const int iw = iw0 + lane;
+        const bool in = iw <= hi && !(wmax < a.waveset[iw - 1]);
+        const unsigned out = __ballot_sync(0xffffffffu, iw <= hi && !in);
+        const int stop = out ? __ffs(out) - 1 : 32;  // the walk ends at the first point past WMAX
+        if (in && lane < stop) atomicAdd(xl + (size_t)(iw - 1) * a.kw, con);
+        if (out) break;
+      }
+    }
+  }
+}
+
 struct LinopArgs {
   const AtlasLine* lines;
   int64_t n;

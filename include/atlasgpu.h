@@ -214,7 +214,7 @@ int atlasgpu_atlas_linop(atlasgpu_ctx *ctx, const int32_t *linedata, int64_t n, 
                          const int32_t *iwavetab, int nwave, const double *waveset, int numnu,
                          double *xlines_out, int64_t *lines_used);
 
-/* XLINOP's normal-line branch (TYPE 0 and 3, atlas12_modules.f90:20040-20174):
+/* XLINOP (atlas12_modules.f90:19873-20250).  The normal-line branch (TYPE 0 and 3, :20040-20174):
  * the LINOP1 walk on unit-19 records with MAX_WING = 2000, LORENTZ_PREFAC =
  * 0.5642 and the blue-wing cutoff at the continuum edge WCON = 1e7 /
  * (CONTX(NCON,NELIONX) - EMERGE(J)), EMERGE(J) = RYDBERG_INF / NMERGE(J)**2,
@@ -223,14 +223,19 @@ int atlasgpu_atlas_linop(atlasgpu_ctx *ctx, const int32_t *linedata, int64_t n, 
  *   recs [n], sorted by wavelength (the reference advances NU and NUCONT
  *   monotonically and stops at the first line with NU >= NUMNU)
  *   contx [16][25]: CONTX(25,16) column-major (XLINOP's edge table)
- * TYPE 2 records are skipped as in the reference; records of the other
- * types (hydrogen, autoionizing, merged continuum) are skipped and counted
- * in n_other (may be NULL). */
+ * With xnfp [nspec][kw] (XNFP(J,NELION)) and rho [kw] (RHO(J)) also the
+ * autoionizing lines (TYPE 1, Fano profile over MAX_WING = 2000 points,
+ * :20201-20226) and the merged-continuum records (every other TYPE but -1,
+ * NLAST = TYPE, flat up to the dissolution limit, at most 1001 points,
+ * :20228-20245); both NULL: those are skipped and counted in n_other.
+ * TYPE 2 records are skipped as in the reference; hydrogen (TYPE -1, the
+ * HPROF4 Stark profile) is skipped and counted in n_other (may be NULL). */
 int atlasgpu_atlas_xlinop(atlasgpu_ctx *ctx, const atlasgpu_nlte_line *recs, int64_t n, int nrhox, int kw,
                           const double *xnfdop, const double *dopple, int nspec, const double *xne,
                           const double *txnxn, const double *hckt, const double *tabcont,
                           const int32_t *iwavetab, int nwave, const double *waveset, int numnu,
-                          const double *contx, double *xlines_inout, int64_t *n_other);
+                          const double *contx, const double *xnfp, const double *rho, double *xlines_inout,
+                          int64_t *n_other);
 
 /* RUN_RT_PASS frequency loop (atlas12_modules.f90:3880-3951): per NU the
  * Planck terms, ALINE = XLINES*STIM, JOSH(1,0) (:18398-18776), the negative

@@ -983,11 +983,45 @@ static void xlinop_wings(const orc_atlas_tables_t *tb, double center, double ada
   }
 }
 
+/* XLINOP's autoionizing lines (TYPE 1, Fano profile, :20201-20226):
+ * CENTER = BSHORE*G*XNFP(J,NELION)/RHO(J) with the two TABCONT gates around
+ * the Boltzmann factor, then both wings up to MAX_WING = 2000 points of
+ * CENTER*(ASHORE*EPSIL + BSHORE)/(EPSIL**2 + 1)/BSHORE, EPSIL =
+ * 2*(FREQ - FRELIN)/GAMMAR, each stopping after the first point below
+ * TABCONT(J, NUCONT). */
+static void xlinop_fano(const orc_nlte_line_t *r, int nu, int numnu, const double *waveset, double xnfp,
+                        double rho, double elo_hckt, double tc, double *xl, int kw) {
+  const double CLIGHT_NMS = 2.99792458e17;
+  const double g = (double)r->gf, ashore = (double)r->gammas, bshore = (double)r->gammaw;
+  const double gammar = (double)r->gammar;
+  const double frelin = CLIGHT_NMS / r->wlvac;
+  double center = bshore * g * xnfp / rho;
+  if (center < tc) return;
+  center = center * exp(-elo_hckt);
+  if (center < tc) return;
+  const int hi = nu + 2000 < numnu ? nu + 2000 : numnu;
+  for (int iw = nu; iw <= hi; ++iw) {
+    const double epsil = 2.0 * (CLIGHT_NMS / waveset[iw - 1] - frelin) / gammar;
+    const double cv = center * (ashore * epsil + bshore) / (epsil * epsil + 1.0) / bshore;
+    xl[(size_t)(iw - 1) * kw] += cv;
+    if (cv < tc) break;
+  }
+  for (int i = 1; i <= 2000; ++i) {
+    const int iw = nu - i;
+    if (iw <= 0) break;
+    const double epsil = 2.0 * (CLIGHT_NMS / waveset[iw - 1] - frelin) / gammar;
+    const double cv = center * (ashore * epsil + bshore) / (epsil * epsil + 1.0) / bshore;
+    xl[(size_t)(iw - 1) * kw] += cv;
+    if (cv < tc) break;
+  }
+}
+
 int64_t orc_atlas_xlinop(const orc_atlas_tables_t *tb, const orc_nlte_line_t *recs, int64_t nrec,
                          int nrhox, int kw, const double *xnfdop, const double *dopple, int nspec,
                          const double *xne, const double *txnxn, const double *hckt,
                          const double *tabcont, const int32_t *iwavetab, int nwave,
-                         const double *waveset, int numnu, const double *contx, double *xlines) {
+                         const double *waveset, int numnu, const double *contx, const double *xnfp,
+                         const double *rho, double *xlines) {
   const double RYDBERG_INF = 109737.31568157;
   double emerge[KW_MAX];
   for (int j = 0; j < nrhox; ++j) {
@@ -1021,7 +1055,36 @@ int64_t orc_atlas_xlinop(const orc_atlas_tables_t *tb, const orc_nlte_line_t *re
       }
     }
     if (stop) return line;
-    if (r->itype != 0 && r->itype != 3) continue;
+    if (r->itype == 2 || r->itype == -1) continue; /* coronal: skipped; hydrogen: not restated */
+    if (r->itype != 0 && r->itype != 3) {
+      /* autoionizing (TYPE 1) and merged-continuum (any other TYPE, NLAST =
+       * TYPE, :20228-20245) records read XNFP(J, NELION) and RHO(J) */
+      const int nel = r->nelion;
+      if (!xnfp || !rho || nel < 1 || nel > nspec) continue;
+      const double *xp = xnfp + (size_t)(nel - 1) * kw;
+      const double elo = (double)r->elo;
+      if (r->itype == 1) {
+        for (int J = 1; J <= nrhox; ++J)
+          xlinop_fano(r, nu, numnu, waveset, xp[J - 1], rho[J - 1], elo * hckt[J - 1],
+                      tabcont[(size_t)(nucont - 1) * kw + J - 1], xlines + (J - 1), kw);
+      } else {
+        const double z = nel == 4 ? 2.0 : 1.0;
+        const double nlast = (double)r->itype;
+        const double wshift = 1.0e7 / (1.0e7 / wlvac - RYDBERG_INF * (z * z) / (nlast * nlast));
+        const double xsectg = (double)r->gf;
+        for (int J = 1; J <= nrhox; ++J) {
+          const double wmerge = 1.0e7 / (1.0e7 / wlvac - emerge[J - 1] * (z * z));
+          const double wmax = wmerge > wshift ? wmerge : wshift;
+          const double con = xsectg * xp[J - 1] * exp(-elo * hckt[J - 1]) / rho[J - 1];
+          const int hi = nu + 1000 < numnu ? nu + 1000 : numnu;
+          for (int iw = nu; iw <= hi; ++iw) {
+            if (wmax < waveset[iw - 1]) break;
+            xlines[(size_t)(iw - 1) * kw + J - 1] += con;
+          }
+        }
+      }
+      continue;
+    }
     int nelion = r->nelion;
     if (nelion < 1 || nelion > nspec) continue;
     double cgf = (double)r->gf, elo = (double)r->elo;

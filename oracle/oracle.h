@@ -145,12 +145,16 @@ typedef struct {
   int32_t nbuff, lim, pad;
 } orc_nlte_line_t;
 /* Adds the TYPE 0/3 records' wings into xlines [numnu][kw]; contx is
- * CONTX(25,16) column-major.  Returns the number of records read. */
+ * CONTX(25,16) column-major.  With xnfp [nspec][kw] (XNFP(J,NELION)) and rho
+ * [kw] also the autoionizing (TYPE 1) and merged-continuum (other TYPEs)
+ * records (:20201-20245); NULL skips them.  Hydrogen (TYPE -1) is not
+ * restated.  Returns the number of records read. */
 int64_t orc_atlas_xlinop(const orc_atlas_tables_t *tb, const orc_nlte_line_t *recs, int64_t nrec,
                          int nrhox, int kw, const double *xnfdop, const double *dopple, int nspec,
                          const double *xne, const double *txnxn, const double *hckt,
                          const double *tabcont, const int32_t *iwavetab, int nwave,
-                         const double *waveset, int numnu, const double *contx, double *xlines);
+                         const double *waveset, int numnu, const double *contx, const double *xnfp,
+                         const double *rho, double *xlines);
 
 /* ---- SYNTHE compute_line_opacity, normal-metal branch
  *      (synthe_module.f90:3167-3458), FP64 restatement ------------------

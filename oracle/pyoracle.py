@@ -190,7 +190,7 @@ def _declare2(L):
     L.orc_atlas_linop1.restype = ctypes.c_int64
     L.orc_atlas_xlinop.argtypes = [ctypes.POINTER(_AtlasTables), ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
                                    ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp, _dp, _dp, _ip,
-                                   ctypes.c_int, _dp, ctypes.c_int, _dp, _dp]
+                                   ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, _dp]
     L.orc_atlas_xlinop.restype = ctypes.c_int64
     L.orc_synthe_nlte_opacity.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -425,8 +425,9 @@ assert NLTE_LINE.itemsize == 64
 
 
 def atlas_xlinop(h0, h1, h2, tablog, recs, atm, tabcont, iwavetab, waveset, contx, xlines=None):
-    """XLINOP's normal-line branch; adds into a copy of xlines [numnu, kw] (zeros when None).
-    contx: CONTX(25,16) as a numpy [16, 25] array (column-major view).  Returns (xlines, records read)."""
+    """XLINOP; adds into a copy of xlines [numnu, kw] (zeros when None).  contx: CONTX(25,16) as a
+    numpy [16, 25] array (column-major view).  With atm["xnfp"] [nspec, kw] and atm["rho"] [kw] also
+    the autoionizing and merged-continuum records.  Returns (xlines, records read)."""
     h0, h1, h2, tablog = (_d(v) for v in (h0, h1, h2, tablog))
     tb = _AtlasTables(_ptr(h0), _ptr(h1), _ptr(h2), _ptr(tablog))
     rec = np.ascontiguousarray(recs, NLTE_LINE)
@@ -437,10 +438,14 @@ def atlas_xlinop(h0, h1, h2, tablog, recs, atm, tabcont, iwavetab, waveset, cont
     tabcont, waveset, cx = _d(tabcont), _d(waveset), _d(contx)
     iw = np.ascontiguousarray(iwavetab, np.int32)
     xl = np.zeros((waveset.size, kw)) if xlines is None else _d(xlines).copy()
+    xp = rh = None
+    if atm.get("xnfp") is not None:
+        xnfp_a, rho_a = _d(atm["xnfp"]), _d(atm["rho"])
+        xp, rh = _ptr(xnfp_a), _ptr(rho_a)
     nread = _lib2().orc_atlas_xlinop(ctypes.byref(tb), rec.ctypes.data_as(ctypes.c_void_p), rec.shape[0], nrhox, kw,
                                      _ptr(xnfdop), _ptr(dopple), nspec, _ptr(xne), _ptr(txnxn), _ptr(hckt),
                                      _ptr(tabcont), _ptr(iw, _ip), iw.size - 1, _ptr(waveset), waveset.size, _ptr(cx),
-                                     _ptr(xl))
+                                     xp, rh, _ptr(xl))
     return xl, nread
 
 

@@ -191,6 +191,49 @@ def test_xlinop_normal_branch_matches_oracle(po, gpu_ctx, tables, atlas_case, h_
     assert np.max(np.abs(got - ref) / scale) < tol
 
 
+@pytest.mark.parametrize("prec,tol", [(_lib.PREC_FP64, 1e-9), (_lib.PREC_MIXED, 1e-6)])
+def test_xlinop_autoionizing_and_merged_continuum_match_oracle(po, gpu_ctx, tables, atlas_case, h_tables, prec,
+                                                                tol):
+    """XLINOP with populations: the autoionizing lines (TYPE 1, Fano profile
+    with ASHORE = GAMMAS, BSHORE = GAMMAW) and the merged-continuum records
+    (TYPE 7, 12, -3: NLAST = TYPE; NELION 4 takes Z = 2) on top of the normal
+    lines; hydrogen (TYPE -1) is the only type left out and counted."""
+    c = atlas_case
+    ws = np.geomspace(300.0, 600.0, 4000)
+    recs = synthetic.nlte_records(4000, 300.5, 599.5, seed=9, strong=0.1, types=(0, 3, 2, 1, -1, 7, 12, -3),
+                                  type_p=(.45, .1, .05, .2, .05, .05, .05, .05))
+    rng = np.random.default_rng(10)
+    f = recs["itype"] == 1
+    recs["gammaw"][f] = 10.0 ** rng.uniform(3.0, 6.0, f.sum())                # BSHORE
+    recs["gammas"][f] = recs["gammaw"][f] * rng.uniform(-2.0, 2.0, f.sum())   # ASHORE
+    recs["gammar"][f] = 10.0 ** rng.uniform(11.0, 13.0, f.sum())             # GAMMAR (Hz)
+    m = np.isin(recs["itype"], (7, 12, -3))
+    recs["nelion"][np.nonzero(m)[0][::4]] = 4
+    pop = c["pop"]
+    nsp = min(NSPEC, pop["xnfp"].shape[1])
+    xnfp = np.zeros((NSPEC, 72))
+    xnfp[:nsp] = pop["xnfp"][:, :nsp].T
+    rho = pop["rho"]
+    contx = synthetic.contx_table()
+    atm = dict(xnfdop=c["xnfdop"], dopple=c["dopple"], xne=c["xne"], txnxn=c["txnxn"], hckt=c["hckt"])
+    plain, _ = po.atlas_xlinop(*h_tables, po.build_tablog(), recs, atm, c["tabcont"], c["iw"], ws, contx)
+    ref, nread = po.atlas_xlinop(*h_tables, po.build_tablog(), recs, dict(atm, xnfp=xnfp, rho=rho), c["tabcont"],
+                                 c["iw"], ws, contx)
+    assert nread > 3000
+    assert np.count_nonzero(ref != plain) > 2000  # the two branches add where the normal lines do not
+    A = atlas.Atlas(gpu_ctx, tables, *h_tables)
+    gpu_ctx.set_precision(prec)
+    try:
+        got, other = A.xlinop(recs, 72, c["xnfdop"], c["dopple"], c["xne"], c["txnxn"], c["hckt"], c["tabcont"],
+                              c["iw"], ws, contx, xnfp=xnfp, rho=rho)
+    finally:
+        gpu_ctx.set_precision(_lib.PREC_MIXED)
+    assert other == int(np.sum(recs["itype"] == -1))
+    np.testing.assert_array_equal(got != 0, ref != 0)
+    scale = np.maximum(np.abs(ref), 1e-300)
+    assert np.max(np.abs(got - ref) / scale) < tol
+
+
 def test_xlinop_rejects_unsorted_records(gpu_ctx, tables, atlas_case, h_tables):
     c = atlas_case
     recs = synthetic.nlte_records(100, 300.5, 599.5, seed=6)[::-1].copy()
