@@ -80,8 +80,8 @@ SIGNATURES = {
     "atlasgpu_atlas_tabvoigt": (_I, [_D, _I, _P, _P, _I, _P, _P, _P]),
     "atlasgpu_atlas_linop": (_I, [_P, _P, _I64, _I, _I, _P, _P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P,
                                   ctypes.POINTER(_I64)]),
-    "atlasgpu_synthe_nlte_opacity": (_I, [_P, _P, _I64, _I, _I, _D, _D, _D, _D, _P, _P, _P, _I, _P, _P, _P, _P,
-                                          _P]),
+    "atlasgpu_synthe_nlte_opacity": (_I, [_P, _P, _I64, _I, _I, _D, _D, _D, _D, _P, _P, _P, _P, _I, _P, _P, _P,
+                                          _P, _P]),
     "atlasgpu_atlas_xlinop": (_I, [_P, _P, _I64, _I, _I, _P, _P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P,
                                    _P, ctypes.POINTER(_I64)]),
     "atlasgpu_atlas_rt_pass": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _D,

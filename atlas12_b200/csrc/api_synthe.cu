@@ -398,9 +398,9 @@ int atlasgpu_synthe_spectrum_dev(atlasgpu_ctx* ctx, const double* d_wledge, int 
 
 int atlasgpu_synthe_nlte_opacity(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* recs, int64_t n, int length,
                                  int nrhox, double wbegin, double ratio, double wlend, double velshift_kms,
-                                 const float* continuum, const double* xnfdop, const double* dopple, int nspec,
-                                 const double* xne, const double* txnxn, const double* hckt, const double* contx,
-                                 float* opacity_inout) {
+                                 const float* continuum, const double* xnfdop, const double* dopple,
+                                 const double* xnfpel, int nspec, const double* xne, const double* txnxn,
+                                 const double* hckt, const double* contx, float* opacity_inout) {
   if (!ctx || n < 0 || (n > 0 && !recs) || length < 1 || nrhox < 1 || nrhox > kKwMax || !(wbegin > 0.0) ||
       !(ratio > 1.0) || !continuum || !xnfdop || !dopple || nspec < 1 || !xne || !txnxn || !hckt || !contx ||
       !opacity_inout)
@@ -446,6 +446,12 @@ int atlasgpu_synthe_nlte_opacity(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* re
   if (n > 0) {
     NlteArgs a{d_rec, n, length, nrhox, nspec, wbegin, ratio, wlend, 1.0 + velshift_kms / 299792.458, d_cont, d_xd,
                d_dp, d_xne, d_tx, d_hc, d_em, d_cx, d_acc};
+    if (xnfpel) {
+      double* d_xp;
+      if ((r = bufT(ctx, "sn_xp", nd, &d_xp))) return r;
+      CK(cudaMemcpyAsync(d_xp, xnfpel, nd * sizeof(double), cudaMemcpyHostToDevice, s));
+      a.xnfpel = d_xp;
+    }
     Timer tm(ctx, "synthe_nlte");
     k_synthe_nlte<<<grid_for(ctx, n * nrhox * 32, 256, 16), 256, 0, s>>>(a);
     CKL(ctx);

@@ -380,7 +380,61 @@ struct NlteArgs {
   const double *xne, *txnxn, *hckt, *emerge;  // [nrhox]
   const double* contx;              // CONTX(26,17) column-major
   double* acc;                      // [nrhox][length]
+  const double* xnfpel = nullptr;   // [nrhox][nspec] XNFPEL = populations / RHO; null: Shore lines skipped
 };
+
+// compute_line_opacity's autoionizing (Shore) lines, synthe_module.f90:3609-3650:
+// KAPPA0 = GAMMAW*GF*XNFPEL with the two continuum gates around the Boltzmann
+// factor, then the Fano profile KAPPA0*(GAMMAS*EPSIL + GAMMAW)/(EPSIL**2+1)/GAMMAW,
+// EPSIL = 2*(FREQ - FRELIN)/GAMMAR, red wing from nbuff to the grid end and blue
+// wing to its start, each point added and then tested against
+// continuum(i)*LINE_CUTOFF.  One warp per (record, depth), 32 points per step.
+static __device__ __forceinline__ void synthe_shore_pair(const NlteArgs& a, const atlasgpu_nlte_line& r, int j,
+                                                         int lane) {
+  const int nel = r.nelion - 1;
+  const float* cont = a.cont + (size_t)j * a.length;
+  double* acc = a.acc + (size_t)j * a.length;
+  const double wl = r.wlvac * a.dopratio;
+  const int nbuff = r.nbuff;
+  const double gr = (double)r.gammar, gs = (double)r.gammas, gw = (double)r.gammaw;
+  double kappa0 = gw * (double)r.gf * a.xnfpel[(size_t)j * a.nspec + nel];
+  const int ic = nbuff < 1 ? 1 : (nbuff > a.length ? a.length : nbuff);
+  const double kapmin = (double)cont[ic - 1] * kLineCutoff;
+  if (kappa0 < kapmin) return;
+  kappa0 = kappa0 * exp(-(double)r.elo * a.hckt[j]);
+  if (kappa0 < kapmin) return;
+  const double frelin = kClightNms / wl;
+  auto kappa_at = [&](int ib) {
+    const double freq = kClightNms / (a.wbegin * powi(a.ratio, ib - 1));
+    const double eps = 2.0 * (freq - frelin) / gr;
+    return kappa0 * (gs * eps + gw) / (eps * eps + 1.0) / gw;
+  };
+  if (wl <= a.wlend) {
+    const int minred = nbuff > 1 ? nbuff : 1;
+    for (int base = minred; base <= a.length; base += 32) {
+      const int ib = base + lane;
+      const bool in = ib <= a.length;
+      const double k = in ? kappa_at(ib) : 0.0;
+      const unsigned sb = __ballot_sync(0xffffffffu, in && k < (double)cont[ib - 1] * kLineCutoff);
+      const int first = sb ? __ffs(sb) - 1 : 32;
+      if (in && lane <= first) atomicAdd(acc + ib - 1, k);
+      if (sb) break;
+    }
+    if (nbuff == 1 || wl < a.wbegin) return;
+  }
+  const int ib0 = a.length + 1 < nbuff ? a.length + 1 : nbuff;
+  const int maxblue = ib0 - 1;
+  for (int i0 = 1; i0 <= maxblue; i0 += 32) {
+    const int i = i0 + lane;
+    const int ib = ib0 - i;
+    const bool in = i <= maxblue;
+    const double k = in ? kappa_at(ib) : 0.0;
+    const unsigned sb = __ballot_sync(0xffffffffu, in && k < (double)cont[ib - 1] * kLineCutoff);
+    const int first = sb ? __ffs(sb) - 1 : 32;
+    if (in && lane <= first) atomicAdd(acc + ib - 1, k);
+    if (sb) break;
+  }
+}
 
 static __global__ void __launch_bounds__(256) k_synthe_nlte(NlteArgs a) {
   const int lane = threadIdx.x & 31;
@@ -392,6 +446,10 @@ static __global__ void __launch_bounds__(256) k_synthe_nlte(NlteArgs a) {
     const int j = (int)(p % a.nrhox);
     const atlasgpu_nlte_line r = a.rec[il];
     const int t = r.itype;
+    if (t == 1 && a.xnfpel && r.nelion >= 1 && r.nelion <= a.nspec) {
+      synthe_shore_pair(a, r, j, lane);
+      continue;
+    }
     if (!(t == 0 || t == 3 || t <= -3) || r.nelion < 1 || r.nelion > a.nspec) continue;
     const float* cont = a.cont + (size_t)j * a.length;
     double* acc = a.acc + (size_t)j * a.length;

@@ -96,10 +96,11 @@ class Synthe:
         return flux, cont
 
     def nlte_opacity(self, records, grid, wlend, continuum, xnfdop, dopple, xne, txnxn, hckt, contx, opacity,
-                     velshift_kms=0.0):
+                     velshift_kms=0.0, xnfpel=None):
         """compute_line_opacity's normal-metal lines (NLTE_LINE records, nbuff
-        = grid index) added into a copy of opacity [nrhox, length] (float32).
-        contx: CONTX(26,17) as [17, 26]."""
+        = grid index) added into a copy of opacity [nrhox, length] (float32);
+        with xnfpel [nrhox, nspec] (populations / RHO) also the autoionizing
+        (Shore) lines.  contx: CONTX(26,17) as [17, 26]."""
         rec = np.ascontiguousarray(records, _lib.NLTE_LINE)
         cont = np.ascontiguousarray(continuum, np.float32)
         xd = np.ascontiguousarray(xnfdop, np.float64)
@@ -107,10 +108,11 @@ class Synthe:
         nrhox, nspec = xd.shape
         vec = [np.ascontiguousarray(v, np.float64) for v in (xne, txnxn, hckt)]
         out = np.array(opacity, np.float32, copy=True, order="C")
+        xp = None if xnfpel is None else np.ascontiguousarray(xnfpel, np.float64)
         self.ctx.call("atlasgpu_synthe_nlte_opacity", ptr(rec), rec.shape[0], int(grid["length"]), nrhox,
                       float(grid["wbegin"]), float(grid["ratio"]), float(wlend), float(velshift_kms), ptr(cont),
-                      ptr(xd), ptr(dp), nspec, *[ptr(v) for v in vec], ptr(np.ascontiguousarray(contx, np.float64)),
-                      ptr(out))
+                      ptr(xd), ptr(dp), ptr(xp), nspec, *[ptr(v) for v in vec],
+                      ptr(np.ascontiguousarray(contx, np.float64)), ptr(out))
         return out
 
     def run(self, case):

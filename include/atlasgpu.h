@@ -162,12 +162,16 @@ int atlasgpu_synthe_line_opacity_dev(atlasgpu_ctx *ctx, const atlasgpu_lte_line 
  *   recs [n] (nbuff = grid index); continuum [nrhox][length];
  *   xnfdop, dopple [nrhox][nspec]; xne, txnxn, hckt [nrhox];
  *   contx [17][26]: CONTX(26,17) column-major.
- * Hydrogen, autoionising and merged-continuum records are skipped. */
+ * With xnfpel [nrhox][nspec] (XNFPEL = populations / RHO, synthe.f90:533-542)
+ * also the autoionizing (Shore) lines, TYPE 1 (:3609-3650): the Fano profile
+ * with GAMMAS, GAMMAW as the Shore parameters, each wing point added and then
+ * tested; xnfpel NULL skips them.  Hydrogen and merged-continuum records are
+ * skipped. */
 int atlasgpu_synthe_nlte_opacity(atlasgpu_ctx *ctx, const atlasgpu_nlte_line *recs, int64_t n, int length,
                                  int nrhox, double wbegin, double ratio, double wlend, double velshift_kms,
-                                 const float *continuum, const double *xnfdop, const double *dopple, int nspec,
-                                 const double *xne, const double *txnxn, const double *hckt, const double *contx,
-                                 float *opacity_inout);
+                                 const float *continuum, const double *xnfdop, const double *dopple,
+                                 const double *xnfpel, int nspec, const double *xne, const double *txnxn,
+                                 const double *hckt, const double *contx, float *opacity_inout);
 
 /* Spectrum: the SYNTHE wavelength loop (synthe.f90:698-718) with
  * setup_opacity_sv and process_wavelength_point (:797-902): per lambda two

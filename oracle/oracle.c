@@ -1135,8 +1135,8 @@ int64_t orc_atlas_xlinop(const orc_atlas_tables_t *tb, const orc_nlte_line_t *re
 void orc_synthe_nlte_opacity(const orc_nlte_line_t *recs, int64_t n, int length, int nrhox,
                              double wbegin, double ratio, double wlend, double velshift_kms,
                              const float *continuum, const double *xnfdop, const double *dopple,
-                             int nspec, const double *xne, const double *txnxn, const double *hckt,
-                             const double *contx, double *out) {
+                             const double *xnfpel, int nspec, const double *xne, const double *txnxn,
+                             const double *hckt, const double *contx, double *out) {
   const double RYDBERG_INF = 109737.31568157, CLIGHT_KMS = 299792.458, CUTOFF = LINE_CUTOFF;
   const double dopratio = 1.0 + velshift_kms / CLIGHT_KMS;
   for (int j = 0; j < nrhox; ++j) {
@@ -1149,6 +1149,47 @@ void orc_synthe_nlte_opacity(const orc_nlte_line_t *recs, int64_t n, int length,
     for (int64_t il = 0; il < n; ++il) {
       const orc_nlte_line_t *r = recs + il;
       int t = r->itype;
+      if (t == 1 && xnfpel) {
+        /* autoionizing (Shore) line, synthe_module.f90:3609-3650: GAMMAS and
+         * GAMMAW hold the Shore parameters; the red wing adds then tests */
+        const int nel = r->nelion;
+        if (nel < 1 || nel > nspec) continue;
+        const double wl = r->wlvac * dopratio;
+        const int nbuff = r->nbuff;
+        const double gr = (double)r->gammar, gs = (double)r->gammas, gw = (double)r->gammaw;
+        double kappa0 = gw * (double)r->gf * xnfpel[(size_t)j * nspec + nel - 1];
+        const int ic = nbuff < 1 ? 1 : (nbuff > length ? length : nbuff);
+        const double kapmin = (double)cont[ic - 1] * CUTOFF;
+        if (kappa0 < kapmin) continue;
+        kappa0 = kappa0 * exp(-(double)r->elo * hckt[j]);
+        if (kappa0 < kapmin) continue;
+        const double frelin = CLIGHT_NMS / wl;
+        if (wl <= wlend) {
+          const int minred = nbuff > 1 ? nbuff : 1;
+          double freq = CLIGHT_NMS / (wbegin * orc_powi(ratio, minred - 1));
+          for (int ib = minred; ib <= length; ++ib) {
+            const double eps = 2.0 * (freq - frelin) / gr;
+            const double kappa = kappa0 * (gs * eps + gw) / (eps * eps + 1.0) / gw;
+            buf[ib - 1] += kappa;
+            if (kappa < (double)cont[ib - 1] * CUTOFF) break;
+            freq = freq / ratio;
+          }
+          if (nbuff == 1) continue;
+          if (wl < wbegin) continue;
+        }
+        int ib = length + 1 < nbuff ? length + 1 : nbuff;
+        const int maxblue = ib - 1;
+        double freq = CLIGHT_NMS / (wbegin * orc_powi(ratio, ib - 1));
+        for (int i = 1; i <= maxblue; ++i) {
+          ib = ib - 1;
+          freq = freq * ratio;
+          const double eps = 2.0 * (freq - frelin) / gr;
+          const double kappa = kappa0 * (gs * eps + gw) / (eps * eps + 1.0) / gw;
+          buf[ib - 1] += kappa;
+          if (kappa < (double)cont[ib - 1] * CUTOFF) break;
+        }
+        continue;
+      }
       if (!(t == 0 || t == 3 || t <= -3)) continue;
       int nel = r->nelion;
       if (nel < 1 || nel > nspec) continue;

@@ -157,7 +157,9 @@ int64_t orc_atlas_xlinop(const orc_atlas_tables_t *tb, const orc_nlte_line_t *re
                          const double *rho, double *xlines);
 
 /* ---- SYNTHE compute_line_opacity, normal-metal branch
- *      (synthe_module.f90:3167-3458), FP64 restatement ------------------
+ *      (synthe_module.f90:3167-3458) and, with xnfpel [nrhox][nspec]
+ *      (XNFPEL = populations / RHO, synthe.f90:533-542), the autoionizing
+ *      (Shore) lines (:3609-3650); FP64 restatement ---------------------
  * Adds the TYPE 0/3 (and He I, TYPE <= -3) records' opacity at every depth
  * into out [nrhox][length] (double).  recs use nbuff as the grid index;
  * continuum [nrhox][length] (float, the REAL(4) continuum); xnfdop, dopple
@@ -165,8 +167,8 @@ int64_t orc_atlas_xlinop(const orc_atlas_tables_t *tb, const orc_nlte_line_t *re
 void orc_synthe_nlte_opacity(const orc_nlte_line_t *recs, int64_t n, int length, int nrhox,
                              double wbegin, double ratio, double wlend, double velshift_kms,
                              const float *continuum, const double *xnfdop, const double *dopple,
-                             int nspec, const double *xne, const double *txnxn, const double *hckt,
-                             const double *contx, double *out);
+                             const double *xnfpel, int nspec, const double *xne, const double *txnxn,
+                             const double *hckt, const double *contx, double *out);
 
 /* ---- ATLAS RT pass, mode-2 integrals (atlas12_modules.f90:3880-3951) --- */
 typedef struct {

@@ -194,8 +194,8 @@ def _declare2(L):
     L.orc_atlas_xlinop.restype = ctypes.c_int64
     L.orc_synthe_nlte_opacity.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
-                                          ctypes.POINTER(ctypes.c_float), _dp, _dp, ctypes.c_int, _dp, _dp, _dp,
-                                          _dp, _dp]
+                                          ctypes.POINTER(ctypes.c_float), _dp, _dp, _dp, ctypes.c_int, _dp, _dp,
+                                          _dp, _dp, _dp]
     L.orc_synthe_nlte_opacity.restype = None
     L.orc_atlas_rt_pass.argtypes = [ctypes.POINTER(Ops), ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_void_p,
                                     ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double,
@@ -450,17 +450,20 @@ def atlas_xlinop(h0, h1, h2, tablog, recs, atm, tabcont, iwavetab, waveset, cont
 
 
 def synthe_nlte_opacity(recs, length, wbegin, ratio, wlend, velshift_kms, continuum, atm, contx):
-    """compute_line_opacity's normal-metal branch in FP64: the contribution [nrhox, length] (double).
-    continuum [nrhox, length] float; atm: xnfdop, dopple [nrhox, nspec], xne, txnxn, hckt; contx [17, 26]."""
+    """compute_line_opacity's normal-metal branch (and, with atm["xnfpel"] [nrhox, nspec], the Shore
+    lines) in FP64: the contribution [nrhox, length] (double).  continuum [nrhox, length] float;
+    atm: xnfdop, dopple [nrhox, nspec], xne, txnxn, hckt; contx [17, 26]."""
     rec = np.ascontiguousarray(recs, NLTE_LINE)
     cont = np.ascontiguousarray(continuum, np.float32)
     xnfdop, dopple = _d(atm["xnfdop"]), _d(atm["dopple"])
+    xp = None if atm.get("xnfpel") is None else _d(atm["xnfpel"])
     nrhox, nspec = xnfdop.shape
     out = np.zeros((nrhox, length))
     _lib2().orc_synthe_nlte_opacity(rec.ctypes.data_as(ctypes.c_void_p), rec.shape[0], length, nrhox, wbegin, ratio,
                                     wlend, velshift_kms, cont.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
-                                    _ptr(xnfdop), _ptr(dopple), nspec, _ptr(_d(atm["xne"])), _ptr(_d(atm["txnxn"])),
-                                    _ptr(_d(atm["hckt"])), _ptr(_d(contx)), _ptr(out))
+                                    _ptr(xnfdop), _ptr(dopple), None if xp is None else _ptr(xp), nspec,
+                                    _ptr(_d(atm["xne"])), _ptr(_d(atm["txnxn"])), _ptr(_d(atm["hckt"])),
+                                    _ptr(_d(contx)), _ptr(out))
     return out
 
 

@@ -191,6 +191,35 @@ def test_nlte_normal_lines_match_fp64_oracle(po, gpu_ctx, tables, prepared):
     np.testing.assert_allclose(got2.astype(np.float64) - 1.0e-3, ref, rtol=1e-5, atol=2e-10)
 
 
+def test_nlte_shore_lines_match_fp64_oracle(po, gpu_ctx, tables, prepared):
+    """compute_line_opacity's autoionizing (Shore) lines with XNFPEL given:
+    the Fano profile from GAMMAS, GAMMAW and GAMMAR, red wing added before
+    its test, on top of the normal lines; GPU against the FP64 restatement
+    (1e-6 of kappa + kappa_cont per bin)."""
+    p = prepared
+    case, g, cont = p["case"], p["grid"], p["cont"]
+    recs = _nlte_records(po, case, g)
+    rng = np.random.default_rng(21)
+    f = rng.uniform(size=recs.size) < 0.3
+    recs["itype"][f] = 1
+    recs["gammaw"][f] = 10.0 ** rng.uniform(4.0, 6.0, f.sum())               # BSHORE
+    recs["gammas"][f] = recs["gammaw"][f] * rng.uniform(-2.0, 2.0, f.sum())  # ASHORE
+    recs["gammar"][f] = 10.0 ** rng.uniform(10.0, 12.0, f.sum())            # GAMMAR (Hz)
+    contx = np.zeros((17, 26))
+    atm = case["atm"]
+    xnfpel = atm["xnfdop"] * atm["dopple"]
+    wlend = case["wlend"]
+    plain = po.synthe_nlte_opacity(recs, g["length"], g["wbegin"], g["ratio"], wlend, 0.0, cont, atm, contx)
+    ref = po.synthe_nlte_opacity(recs, g["length"], g["wbegin"], g["ratio"], wlend, 0.0, cont,
+                                 dict(atm, xnfpel=xnfpel), contx)
+    assert np.count_nonzero(ref != plain) > 0.1 * ref.size
+    syn = S.Synthe(gpu_ctx, tables)
+    got = syn.nlte_opacity(recs, g, wlend, cont, atm["xnfdop"], atm["dopple"], atm["xne"], atm["txnxn"], atm["hckt"],
+                           contx, np.zeros((72, g["length"]), np.float32), xnfpel=xnfpel)
+    err = np.abs(got.astype(np.float64) - ref) / (ref + cont.astype(np.float64))
+    assert err.max() <= 1e-6, err.max()
+
+
 def test_concurrent_spectra_match_one_at_a_time(gpu_ctx, tables):
     """Spectra of atmospheres with their own windows and line lists on four
     concurrent contexts equal those computed one at a time (flux to 1e-6:
