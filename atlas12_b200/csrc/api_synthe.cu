@@ -396,6 +396,41 @@ int atlasgpu_synthe_spectrum_dev(atlasgpu_ctx* ctx, const double* d_wledge, int 
   return spectrum_launch(ctx, a);
 }
 
+namespace {
+// The grid indices of a merged-continuum edge at one depth
+// (synthe_module.f90:3664-3689, vacuum wavelengths): NBUFF1 the first point
+// redward of the line, NBUFF2 at WMERGE, NBUFF3 at WTAIL = 500 cm^-1 redder;
+// WMERGE from the REAL(4) Inglis-Teller NMERGE (:3344-3347), H I with
+// RYDBERG_H.  The REAL(4) edge test uses the C library expf as the
+// reference's REAL(4) EXP does.  Returns 0 when the edge misses the grid.
+int merged_bins(double wl, int nlast, int nelion, double xne, double wbegin, double ratio, int length, int* n1,
+                int* n2, int* n3) {
+  const double ratiolg = log(ratio);
+  const int ixwlbeg = (int)lrint(log(wbegin) / ratiolg);
+  const float inglis = (float)(1600.0 / pow(xne, 2.0 / 15.0));
+  const float nmerge = inglis - 1.5f;
+  const double ryd = nelion == 1 ? 109677.583403 : 109737.31568157;  // RYDBERG_H, RYDBERG_INF
+  const double em = ryd / ((double)nmerge * (double)nmerge);
+  const double wshift = 1.0e7 / (1.0e7 / wl - ryd / ((double)nlast * (double)nlast));
+  double wmerge = 1.0e7 / (1.0e7 / wl - em);
+  if (wmerge < 0.0) wmerge = wshift + wshift;
+  wmerge = std::max(wmerge, wshift);
+  wmerge = std::min(wshift + wshift, wmerge);
+  double wtail = 1.0e7 / (1.0e7 / wmerge - 500.0);
+  if (wtail < 0.0) wtail = wmerge + wmerge;
+  wtail = std::min(wmerge + wmerge, wtail);
+  int ixwl = (int)(log(wl) / ratiolg);
+  const float edgeblue = expf((float)ixwl * (float)ratiolg);
+  if (edgeblue > (float)wl) ixwl -= 1;
+  *n1 = ixwl + 1 - ixwlbeg + 1;
+  *n2 = (int)(log(wmerge) / ratiolg + 0.5) - ixwlbeg + 1;
+  *n3 = (int)(log(wtail) / ratiolg + 0.5) - ixwlbeg + 1;
+  if (*n1 > length || *n3 < 1) return 0;
+  *n1 = std::max(*n1, 1);
+  return 1;
+}
+}  // namespace
+
 int atlasgpu_synthe_nlte_opacity(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* recs, int64_t n, int length,
                                  int nrhox, double wbegin, double ratio, double wlend, double velshift_kms,
                                  const float* continuum, const double* xnfdop, const double* dopple,
@@ -451,6 +486,31 @@ int atlasgpu_synthe_nlte_opacity(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* re
       if ((r = bufT(ctx, "sn_xp", nd, &d_xp))) return r;
       CK(cudaMemcpyAsync(d_xp, xnfpel, nd * sizeof(double), cudaMemcpyHostToDevice, s));
       a.xnfpel = d_xp;
+      // merged-continuum edges: their grid indices per depth, from the C library
+      std::vector<int> mord((size_t)n, -1);
+      std::vector<int4> mb;
+      const double dopratio = a.dopratio;
+      for (int64_t i = 0; i < n; ++i) {
+        const atlasgpu_nlte_line& rec = recs[i];
+        if (rec.itype < 4 || rec.nelion < 1 || rec.nelion > nspec) continue;
+        mord[i] = (int)(mb.size() / nrhox);
+        for (int j = 0; j < nrhox; ++j) {
+          int4 b;
+          b.w = merged_bins(rec.wlvac * dopratio, rec.itype, rec.nelion, xne[j], wbegin, ratio, length, &b.x, &b.y,
+                            &b.z);
+          mb.push_back(b);
+        }
+      }
+      if (!mb.empty()) {
+        int* d_mo;
+        int4* d_mb;
+        if ((r = bufT(ctx, "sn_mord", (size_t)n, &d_mo)) || (r = bufT(ctx, "sn_mbins", mb.size(), &d_mb))) return r;
+        CK(cudaMemcpyAsync(d_mo, mord.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_mb, mb.data(), mb.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));  // the host vectors go out of scope
+        a.mord = d_mo;
+        a.mbins = d_mb;
+      }
     }
     Timer tm(ctx, "synthe_nlte");
     k_synthe_nlte<<<grid_for(ctx, n * nrhox * 32, 256, 16), 256, 0, s>>>(a);

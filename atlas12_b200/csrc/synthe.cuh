@@ -381,6 +381,11 @@ struct NlteArgs {
   const double* contx;              // CONTX(26,17) column-major
   double* acc;                      // [nrhox][length]
   const double* xnfpel = nullptr;   // [nrhox][nspec] XNFPEL = populations / RHO; null: Shore lines skipped
+  // merged-continuum edges (TYPE >= 4): per record its ordinal m (-1: none)
+  // and per (m, depth) the grid indices NBUFF1, NBUFF2, NBUFF3 and a flag
+  // (0: the edge misses the grid), computed on the host with the C library
+  const int* mord = nullptr;
+  const int4* mbins = nullptr;
 };
 
 // compute_line_opacity's autoionizing (Shore) lines, synthe_module.f90:3609-3650:
@@ -448,6 +453,25 @@ static __global__ void __launch_bounds__(256) k_synthe_nlte(NlteArgs a) {
     const int t = r.itype;
     if (t == 1 && a.xnfpel && r.nelion >= 1 && r.nelion <= a.nspec) {
       synthe_shore_pair(a, r, j, lane);
+      continue;
+    }
+    if (t >= 4) {
+      // merged-continuum edge (synthe_module.f90:3652-3696): flat to NBUFF2,
+      // then tapering to zero at NBUFF3
+      if (!a.mbins) continue;
+      const int m = a.mord[il];
+      if (m < 0) continue;
+      const int4 b = a.mbins[(size_t)m * a.nrhox + j];
+      if (!b.w) continue;
+      const double kappa = (double)r.gf * a.xnfpel[(size_t)j * a.nspec + r.nelion - 1] *
+                           exp(-(double)r.elo * a.hckt[j]);
+      const double dn = (double)(b.z - b.y);
+      const int hi = b.z < a.length ? b.z : a.length;
+      double* acc = a.acc + (size_t)j * a.length;
+      for (int ib = b.x + lane; ib <= hi; ib += 32) {
+        const double tail = ib > b.y ? (double)(b.z - ib) / dn : 1.0;
+        atomicAdd(acc + ib - 1, kappa * tail);
+      }
       continue;
     }
     if (!(t == 0 || t == 3 || t <= -3) || r.nelion < 1 || r.nelion > a.nspec) continue;

@@ -165,8 +165,10 @@ int atlasgpu_synthe_line_opacity_dev(atlasgpu_ctx *ctx, const atlasgpu_lte_line 
  * With xnfpel [nrhox][nspec] (XNFPEL = populations / RHO, synthe.f90:533-542)
  * also the autoionizing (Shore) lines, TYPE 1 (:3609-3650): the Fano profile
  * with GAMMAS, GAMMAW as the Shore parameters, each wing point added and then
- * tested; xnfpel NULL skips them.  Hydrogen and merged-continuum records are
- * skipped. */
+ * tested; and the merged-continuum edges, TYPE = NLAST >= 4 (:3652-3696, vacuum
+ * wavelengths): flat from the line to WMERGE, tapering to zero at WTAIL, the
+ * grid indices computed on the host with the C library.  xnfpel NULL skips
+ * both.  Hydrogen records are skipped. */
 int atlasgpu_synthe_nlte_opacity(atlasgpu_ctx *ctx, const atlasgpu_nlte_line *recs, int64_t n, int length,
                                  int nrhox, double wbegin, double ratio, double wlend, double velshift_kms,
                                  const float *continuum, const double *xnfdop, const double *dopple,

@@ -1132,6 +1132,39 @@ int64_t orc_atlas_xlinop(const orc_atlas_tables_t *tb, const orc_nlte_line_t *re
  * test-before-add from MAX(1,NBUFF), blue wing add-then-test below NBUFF;
  * points blueward of WCON are skipped, the WCON..WTAIL ramp tapers.
  * ==================================================================== */
+/* The grid indices of a merged-continuum edge at one depth
+ * (synthe_module.f90:3664-3689, IFVAC = 1): NBUFF1 the first point redward
+ * of the line, NBUFF2 at WMERGE, NBUFF3 at WTAIL.  EMERGE and EMERGEH from
+ * the REAL(4) Inglis-Teller NMERGE = 1600/XNE**(2/15) - 1.5 (:3344-3347);
+ * NELION 1 (H I) takes RYDBERG_H.  Returns 0 when the edge misses the grid. */
+static int orc_synthe_merged_bins(double wl, int nlast, int nelion, double xne, double wbegin, double ratio,
+                                  int *n1, int *n2, int *n3, int length) {
+  const double RYDBERG_INF = 109737.31568157, RYDBERG_H = 109677.583403;
+  const double ratiolg = log(ratio);
+  const int ixwlbeg = (int)lrint(log(wbegin) / ratiolg);
+  const float inglis = (float)(1600.0 / pow(xne, 2.0 / 15.0));
+  const float nmerge = inglis - 1.5f;
+  const double ryd = nelion == 1 ? RYDBERG_H : RYDBERG_INF;
+  const double em = ryd / ((double)nmerge * (double)nmerge);
+  double wshift = 1.0e7 / (1.0e7 / wl - ryd / ((double)nlast * (double)nlast));
+  double wmerge = 1.0e7 / (1.0e7 / wl - em);
+  if (wmerge < 0.0) wmerge = wshift + wshift;
+  wmerge = wmerge > wshift ? wmerge : wshift;
+  wmerge = (wshift + wshift) < wmerge ? (wshift + wshift) : wmerge;
+  double wtail = 1.0e7 / (1.0e7 / wmerge - 500.0);
+  if (wtail < 0.0) wtail = wmerge + wmerge;
+  wtail = (wmerge + wmerge) < wtail ? (wmerge + wmerge) : wtail;
+  int ixwl = (int)(log(wl) / ratiolg);
+  const float edgeblue = expf((float)ixwl * (float)ratiolg);
+  if (edgeblue > (float)wl) ixwl = ixwl - 1;
+  *n1 = ixwl + 1 - ixwlbeg + 1;
+  *n2 = (int)(log(wmerge) / ratiolg + 0.5) - ixwlbeg + 1;
+  *n3 = (int)(log(wtail) / ratiolg + 0.5) - ixwlbeg + 1;
+  if (*n1 > length || *n3 < 1) return 0;
+  if (*n1 < 1) *n1 = 1;
+  return 1;
+}
+
 void orc_synthe_nlte_opacity(const orc_nlte_line_t *recs, int64_t n, int length, int nrhox,
                              double wbegin, double ratio, double wlend, double velshift_kms,
                              const float *continuum, const double *xnfdop, const double *dopple,
@@ -1187,6 +1220,24 @@ void orc_synthe_nlte_opacity(const orc_nlte_line_t *recs, int64_t n, int length,
           const double kappa = kappa0 * (gs * eps + gw) / (eps * eps + 1.0) / gw;
           buf[ib - 1] += kappa;
           if (kappa < (double)cont[ib - 1] * CUTOFF) break;
+        }
+        continue;
+      }
+      if (t >= 4 && xnfpel) {
+        /* merged-continuum edge, synthe_module.f90:3652-3696 (vacuum
+         * wavelengths, IFVAC = 1): flat opacity from the line to WMERGE,
+         * tapering linearly to zero at WTAIL (500 cm^-1 redder) */
+        const int nel = r->nelion;
+        if (nel < 1 || nel > nspec) continue;
+        int n1, n2, n3;
+        if (!orc_synthe_merged_bins(r->wlvac * dopratio, t, nel, xne[j], wbegin, ratio, &n1, &n2, &n3, length))
+          continue;
+        const double kappa = (double)r->gf * xnfpel[(size_t)j * nspec + nel - 1] * exp(-(double)r->elo * hckt[j]);
+        const double dn = (double)(n3 - n2);
+        double tail = 1.0;
+        for (int ib = n1; ib <= (n3 < length ? n3 : length); ++ib) {
+          if (ib > n2) tail = (double)(n3 - ib) / dn;
+          buf[ib - 1] += kappa * tail;
         }
         continue;
       }

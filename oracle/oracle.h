@@ -159,7 +159,8 @@ int64_t orc_atlas_xlinop(const orc_atlas_tables_t *tb, const orc_nlte_line_t *re
 /* ---- SYNTHE compute_line_opacity, normal-metal branch
  *      (synthe_module.f90:3167-3458) and, with xnfpel [nrhox][nspec]
  *      (XNFPEL = populations / RHO, synthe.f90:533-542), the autoionizing
- *      (Shore) lines (:3609-3650); FP64 restatement ---------------------
+ *      (Shore) lines (:3609-3650) and the merged-continuum edges (TYPE >= 4,
+ *      :3652-3696, vacuum wavelengths); FP64 restatement ----------------
  * Adds the TYPE 0/3 (and He I, TYPE <= -3) records' opacity at every depth
  * into out [nrhox][length] (double).  recs use nbuff as the grid index;
  * continuum [nrhox][length] (float, the REAL(4) continuum); xnfdop, dopple

@@ -191,20 +191,25 @@ def test_nlte_normal_lines_match_fp64_oracle(po, gpu_ctx, tables, prepared):
     np.testing.assert_allclose(got2.astype(np.float64) - 1.0e-3, ref, rtol=1e-5, atol=2e-10)
 
 
-def test_nlte_shore_lines_match_fp64_oracle(po, gpu_ctx, tables, prepared):
-    """compute_line_opacity's autoionizing (Shore) lines with XNFPEL given:
-    the Fano profile from GAMMAS, GAMMAW and GAMMAR, red wing added before
-    its test, on top of the normal lines; GPU against the FP64 restatement
-    (1e-6 of kappa + kappa_cont per bin)."""
+def test_nlte_shore_and_merged_lines_match_fp64_oracle(po, gpu_ctx, tables, prepared):
+    """compute_line_opacity with XNFPEL given: the autoionizing (Shore) lines
+    (Fano profile from GAMMAS, GAMMAW and GAMMAR, red wing added before its
+    test) and the merged-continuum edges (TYPE = NLAST >= 4, flat to WMERGE,
+    tapering to WTAIL; NELION 1 with RYDBERG_H), on top of the normal lines;
+    GPU against the FP64 restatement (1e-6 of kappa + kappa_cont per bin)."""
     p = prepared
     case, g, cont = p["case"], p["grid"], p["cont"]
     recs = _nlte_records(po, case, g)
     rng = np.random.default_rng(21)
-    f = rng.uniform(size=recs.size) < 0.3
+    u = rng.uniform(size=recs.size)
+    f = u < 0.3
     recs["itype"][f] = 1
     recs["gammaw"][f] = 10.0 ** rng.uniform(4.0, 6.0, f.sum())               # BSHORE
     recs["gammas"][f] = recs["gammaw"][f] * rng.uniform(-2.0, 2.0, f.sum())  # ASHORE
     recs["gammar"][f] = 10.0 ** rng.uniform(10.0, 12.0, f.sum())            # GAMMAR (Hz)
+    mrg = (u >= 0.3) & (u < 0.33)
+    recs["itype"][mrg] = rng.choice([4, 9, 30, 100], mrg.sum())
+    recs["nelion"][np.nonzero(mrg)[0][::3]] = 1
     contx = np.zeros((17, 26))
     atm = case["atm"]
     xnfpel = atm["xnfdop"] * atm["dopple"]
