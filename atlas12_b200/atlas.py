@@ -273,7 +273,10 @@ class AtlasBatch:
     """
 
     def __init__(self, ctx: Context, operators, nslots, linedata=None, waveset=None, rcoset=None, nrhox=72,
-                 h_tables=None):
+                 h_tables=None, shape="cached"):
+        """shape: "cached" applies the launch shape the autotuner cached for
+        this GPU and workload (autotune.tune_batch), if any; None keeps the
+        library's default; or a (linop_ctas_per_sm, rt_waves) pair."""
         self.ctx = ctx
         ctx.set_operators(operators["xtau8"], operators["coefj"], operators["coefh"], operators["ch_j"],
                           operators["ck_j"])
@@ -295,6 +298,11 @@ class AtlasBatch:
                       ld.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ld.shape[0], _dp(h0), _dp(h1), _dp(h2), 0.0)
         self._h = ctypes.c_void_p()
         ctx.call("atlasgpu_batch_create", ctypes.byref(d), self.nslots, ctypes.byref(self._h))
+        if shape == "cached":
+            from .autotune import cached_shape
+            shape = cached_shape(self)
+        if shape is not None:
+            self.set_shape(*shape)
 
     def load(self, slot, teff, logg, vturb, mh, start, max_iter=60, tol_percent=0.1):
         """Start a model in `slot` from start = dict(t, p, rhox) on TAUSTD."""

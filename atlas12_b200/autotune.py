@@ -51,6 +51,17 @@ def _time_kernels(batch, load):
         batch.run(poll_every=4)
 
 
+def cached_shape(batch):
+    """The cached launch shape for `batch`'s GPU and workload, or None."""
+    path = cache_path()
+    try:
+        with open(path) as f:
+            entry = json.load(f).get(_key(batch, _device_name(batch.ctx.device)))
+    except (OSError, ValueError):
+        return None
+    return tuple(entry["shape"]) if entry else None
+
+
 def tune_batch(batch, params, starts, use_cache=True):
     """Choose and set the fastest launch shape for `batch` on these models
     (params [n, 4], starts: n dicts; the first nslots are loaded).  Returns

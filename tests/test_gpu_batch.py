@@ -99,7 +99,8 @@ def test_batch_rejects_bad_arguments(gpu_ctx, tables, small_grid):
 
 def test_launch_shape_and_autotuner(gpu_ctx, tables, small_grid, singles, tmp_path, monkeypatch):
     """Every launch shape gives the lone model's iteration (relative 1e-8);
-    the autotuner picks one of its candidates and caches it per workload."""
+    the autotuner picks one of its candidates and caches it per workload, and
+    later batches of that workload start from the cached shape."""
     from atlas12_b200 import autotune
     monkeypatch.setenv("XDG_CACHE_HOME", str(tmp_path))
     ws, rc, lines = small_grid
@@ -118,4 +119,11 @@ def test_launch_shape_and_autotuner(gpu_ctx, tables, small_grid, singles, tmp_pa
     assert autotune.tune_batch(b, PARAMS, starts)[:2] == (lc, rw)  # from the cache
     with pytest.raises(_lib.AtlasGPUError, match="RT waves"):
         b.set_shape(16, 0)
+    default = atlas.AtlasBatch(gpu_ctx, tables, nslots=2, linedata=lines, waveset=ws, rcoset=rc, shape=None).shape()
+    b2 = atlas.AtlasBatch(gpu_ctx, tables, nslots=2, linedata=lines, waveset=ws, rcoset=rc)
+    assert b2.shape() == (lc, rw)  # a new batch of this workload starts from the cached shape
+    b2.close()
+    b3 = atlas.AtlasBatch(gpu_ctx, tables, nslots=3, linedata=lines, waveset=ws, rcoset=rc)
+    assert b3.shape() == default  # another workload: nothing cached
+    b3.close()
     b.close()
