@@ -324,7 +324,9 @@ def run_ours(args):
     for _ in range(ne2e):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        b2 = atlas.AtlasBatch(ctx, ops, nslots=CFG["slots"], linedata=W["lines"], waveset=W["ws"], rcoset=W["rc"])
+        # the launch shape the autotuner chose above (also what the batch reads from its cache)
+        b2 = atlas.AtlasBatch(ctx, ops, nslots=CFG["slots"], linedata=W["lines"], waveset=W["ws"], rcoset=W["rc"],
+                              shape=(lc, rw))
         st2, _ = warm_starts(ctx, params, grey)
         res = one_step(b2, st2, keep=True)
         torch.cuda.synchronize()
