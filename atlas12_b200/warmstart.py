@@ -135,24 +135,41 @@ class WarmStart:
             hist = np.concatenate([hist, mlp.train(x, yn, tail_epochs, batch, lr_tail, seed + 2)])
         return cls(mlp, ymean, ystd, residual), hist
 
-    def predict(self, params):
+    def predict(self, params, grey=None):
+        """T, P, XNE [n, 72] for params [n, 4] from one forward pass; grey:
+        the plain grey starts of the same parameters, when the caller has
+        them (the residual network adds to their log T and log P)."""
         params = np.atleast_2d(params)
         y = self.mlp.forward(encode_inputs(params)).astype(np.float64) * self.ystd + self.ymean
         n = NRHOX
         if self.residual:
-            gt, gp = self._grey_logs(params)
+            if grey is None:
+                gt, gp = self._grey_logs(params)
+            else:
+                gt = np.array([np.log10(g["t"]) for g in grey])
+                gp = np.array([np.log10(g["p"]) for g in grey])
             y[:, :n] += gt
             y[:, n:2 * n] += gp
         return 10.0 ** y[:, :n], 10.0 ** y[:, n:2 * n], 10.0 ** y[:, 2 * n:]
 
+    def starts(self, params, grey=None):
+        """Starting structures on TAUSTD for every parameter set: T, P from
+        the network, RHOX = P / g (one forward pass for all of them)."""
+        params = np.atleast_2d(params)
+        t, p, xne = self.predict(params, grey)
+        out = []
+        for i, (teff, logg, mh, vturb) in enumerate(params):
+            ti = t[i].copy()
+            # the network's T need not be monotone; the iteration's own rule applies
+            for j in range(NRHOX - 2, -1, -1):
+                ti[j] = min(ti[j], ti[j + 1] - 1.0)
+            out.append(dict(t=np.maximum(ti, 1200.0), p=p[i], rhox=p[i] / 10.0 ** logg, tauros=TAUSTD.copy(),
+                            xne=xne[i]))
+        return out
+
     def start(self, teff, logg, mh, vturb):
-        """Starting structure on TAUSTD: T, P from the network, RHOX = P / g."""
-        t, p, xne = self.predict([[teff, logg, mh, vturb]])
-        t, p = t[0], p[0]
-        # the network's T need not be monotone; the iteration's own rule applies
-        for j in range(NRHOX - 2, -1, -1):
-            t[j] = min(t[j], t[j + 1] - 1.0)
-        return dict(t=np.maximum(t, 1200.0), p=p, rhox=p / 10.0 ** logg, tauros=TAUSTD.copy(), xne=xne[0])
+        """Starting structure on TAUSTD for one parameter set."""
+        return self.starts([[teff, logg, mh, vturb]])[0]
 
     def save(self, path):
         np.savez(path, params=self.mlp.params(), shape=np.array(self.mlp.shape), ymean=self.ymean,
@@ -206,7 +223,7 @@ def compare_starts(batch, ws, params, max_iter=80, tol=0.1):
     network's start, per parameter set (the unmodified iteration judges both).
     Returns dict of arrays: iters/err for 'grey' and 'mlp'."""
     out = {}
-    for name, starts in (("grey", None), ("mlp", [ws.start(*p) for p in params])):
+    for name, starts in (("grey", None), ("mlp", ws.starts(params))):
         it, er, _, _, _ = run_models(batch, params, starts, max_iter=max_iter, tol=tol)
         out[name] = dict(iters=it, err=er)
     return out

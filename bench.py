@@ -199,8 +199,7 @@ def warm_starts(ctx, params, grey):
         return list(grey), False
     ws = warmstart.WarmStart.load(WARMSTART, ctx)
     starts = []
-    for p, g in zip(params, grey):
-        s = ws.start(*p)
+    for s, g in zip(ws.starts(params, grey), grey):
         good = all(np.all(np.isfinite(s[k])) and np.all(s[k] > 0) for k in ("t", "p", "rhox"))
         starts.append(s if good else g)
     ws.mlp.close()

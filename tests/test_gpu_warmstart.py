@@ -27,6 +27,12 @@ def test_learned_start_converges_more_models_in_the_budget(gpu_ctx, tables):
         pytest.fail("trained warm-start weights are missing")
     params = warmstart.sample_params(32, seed=12)
     ws = warmstart.WarmStart.load(WEIGHTS, gpu_ctx)
+    # one forward pass for many models, with or without the caller's grey starts, = one model at a time
+    grey = [warmstart.grey_start(teff, logg, mh) for teff, logg, mh, _ in params[:4]]
+    for a, b, c in zip(ws.starts(params[:4]), ws.starts(params[:4], grey), [ws.start(*p) for p in params[:4]]):
+        for k in ("t", "p", "rhox"):
+            np.testing.assert_allclose(a[k], c[k], rtol=1e-12)
+            np.testing.assert_array_equal(a[k], b[k])
     batch = warmstart.workload_batch(gpu_ctx, tables, nslots=32)
     r = warmstart.compare_starts(batch, ws, params, max_iter=30, tol=0.1)
     batch.close()
