@@ -218,17 +218,3 @@ def test_driver_order_matches_oracle(sel, po):
         np.testing.assert_array_equal(got, np.concatenate(parts))
         assert st == state
         assert (counts[5] == 0) == (teff > 8000.0)
-
-
-def test_readers_roundtrip(tmp_path, sel):
-    recs = synthetic.selectlines_records(5, 1000, sel["wt"], seed=1)
-    p = tmp_path / "toto.bin"
-    linelists.write_mol2(str(p), recs)
-    back = linelists.read_mol2(str(p))
-    assert back.tobytes() == recs.tobytes()
-    h = synthetic.selectlines_records(6, 1000, sel["wt"], seed=1)
-    q = tmp_path / "h2o.bin"
-    h.tofile(str(q))
-    assert linelists.read_h2o(str(q)).tobytes() == h.tobytes()
-    with pytest.raises(ValueError, match="MOL2"):
-        linelists.read_mol2(str(q))

@@ -232,3 +232,38 @@ def test_host_record_conversion():
         linelists.SelectLines._records(6, t)
     with pytest.raises(ValueError):
         linelists.SelectLines._records(2, np.zeros((5, 3), np.int32))
+
+
+def test_binary_readers_roundtrip(tmp_path, tables):
+    """The MOL2 (header + 32-byte records), H2O (8-byte) and LINEREC readers
+    return the bytes written, memory-mapped; a file without the MOL2 magic is
+    refused; the header count caps the records read (no GPU)."""
+    from atlas12_b200 import linelists
+    wt = tables["wavetab"]
+    mol = synthetic.selectlines_records(5, 1000, wt, seed=1)
+    p = tmp_path / "toto.bin"
+    linelists.write_mol2(str(p), mol)
+    assert linelists.read_mol2(str(p)).tobytes() == mol.tobytes()
+    with open(p, "ab") as f:  # trailing records beyond the header's count are not read
+        f.write(mol[:3].tobytes())
+    assert len(linelists.read_mol2(str(p))) == 1000
+    h = synthetic.selectlines_records(6, 500, wt, seed=2)
+    q = tmp_path / "h2o.bin"
+    h.tofile(str(q))
+    assert linelists.read_h2o(str(q)).tobytes() == h.tobytes()
+    with pytest.raises(ValueError, match="MOL2"):
+        linelists.read_mol2(str(q))
+    ld = synthetic.selectlines_records(1, 700, wt, seed=3)
+    r = tmp_path / "gfpred.bin"
+    ld.tofile(str(r))
+    np.testing.assert_array_equal(linelists.read_linerec(str(r)), ld)
+
+
+def test_driver_order_rules():
+    """SELECTLINES's database order and entry state (no GPU)."""
+    from atlas12_b200 import _lib, linelists
+    kinds = [k for k, _ in linelists.DATABASES]
+    assert kinds == [_lib.SEL_LOWPRED, _lib.SEL_LOWOBS, _lib.SEL_HI, _lib.SEL_DIATOMIC, _lib.SEL_TIO, _lib.SEL_H2O,
+                     _lib.SEL_H3PLUS]
+    st = linelists.initial_state(np.array([9.09, 160000.0]))
+    assert st["nu"] == 1 and st["freq"] == CLIGHT_NMS / 160000.0 and st["igr"] == 0
