@@ -267,3 +267,56 @@ def test_driver_order_rules():
                      _lib.SEL_H3PLUS]
     st = linelists.initial_state(np.array([9.09, 160000.0]))
     assert st["nu"] == 1 and st["freq"] == CLIGHT_NMS / 160000.0 and st["igr"] == 0
+
+
+def test_select_all_threads_the_state(monkeypatch):
+    """select_all on a stub database loop: NU restarts at 1 for every database
+    but LOWOBS, FREQ and IGR carry from one to the next, TiO and H2O are
+    skipped above 8000 K (no GPU)."""
+    from atlas12_b200 import _lib, linelists
+    calls = []
+
+    def fake_select(self, kind, recs, state, cap=None):
+        calls.append((kind, dict(state)))
+        state.update(nu=state["nu"] + 10 * kind, freq=state["freq"] * 2.0, igr=kind)
+        return np.full((len(recs), 4), kind, np.int32)
+
+    monkeypatch.setattr(linelists.SelectLines, "select", fake_select)
+    S = object.__new__(linelists.SelectLines)
+    S.wavetab = np.array([10.0, 20.0])
+    dbs = {k: np.zeros((k, 4), np.int32) for k in range(1, 8)}
+    out, counts, st = S.select_all(dbs, teff=5000.0)
+    assert [c[0] for c in calls] == [1, 2, 3, 4, 5, 6, 7]
+    assert calls[0][1]["nu"] == 1 and calls[1][1]["nu"] == 11  # LOWOBS continues from LOWPRED
+    assert all(c[1]["nu"] == 1 for c in calls[2:])
+    assert calls[0][1]["freq"] == CLIGHT_NMS / 20.0 and calls[3][1]["freq"] == 8.0 * CLIGHT_NMS / 20.0
+    assert [c[1]["igr"] for c in calls] == [0, 1, 2, 3, 4, 5, 6]
+    assert counts == {k: k for k in range(1, 8)} and out.shape == (28, 4)
+    calls.clear()
+    out, counts, st = S.select_all(dbs, teff=9000.0)
+    assert [c[0] for c in calls] == [1, 2, 3, 4, 7] and counts[_lib.SEL_TIO] == 0 and counts[_lib.SEL_H2O] == 0
+
+
+def test_autotune_cache_lookup(tmp_path, monkeypatch):
+    """autotune.cached_shape reads the per-GPU, per-workload entry tune_batch
+    writes, and nothing for another workload (no GPU)."""
+    import json
+    from atlas12_b200 import autotune
+    monkeypatch.setenv("XDG_CACHE_HOME", str(tmp_path))
+    monkeypatch.setattr(autotune, "_device_name", lambda device: "B200")
+
+    class Fake:
+        class ctx:
+            device = 0
+        waveset = np.zeros(30000)
+        nlines, nrhox, nslots = 500000, 72, 32
+
+    assert autotune.cached_shape(Fake) is None
+    path = autotune.cache_path()
+    import os
+    os.makedirs(os.path.dirname(path))
+    with open(path, "w") as f:
+        json.dump({autotune._key(Fake, "B200"): {"shape": [32, 64]}}, f)
+    assert autotune.cached_shape(Fake) == (32, 64)
+    Fake.nslots = 16
+    assert autotune.cached_shape(Fake) is None
