@@ -983,6 +983,281 @@ static void xlinop_wings(const orc_atlas_tables_t *tb, double center, double ada
   }
 }
 
+/* ---- hydrogen line profile (atlas12_modules.f90:20263-21002) ---------- */
+
+/* HFNM: hydrogen oscillator strength f(n,m), :20263-20305 */
+double orc_hfnm(int n, int m) {
+  if (m <= n) return 0.0;
+  const double xn = (double)n;
+  const double ginf = 0.2027 / pow(xn, 0.71);
+  const double gca = 0.124 / xn;
+  const double fkn = xn * 1.9603;
+  const double wtc = 0.45 - 2.4 / orc_powi(xn, 3) * (xn - 1.0);
+  const double xm = (double)m, xmn = (double)(m - n);
+  const double fk = fkn * orc_powi(xm / (xmn * (xm + (double)n)), 3);
+  const double xmn12 = pow(xmn, 1.2);
+  const double wt = (xmn12 - 1.0) / (xmn12 + wtc);
+  return fk * (1.0 - wt * ginf - (0.222 + gca / xm) * (1.0 - wt));
+}
+
+/* STARK_PROFILE: the quasistatic Stark wing S(beta, P), :20376-20514 */
+double orc_stark_profile(const orc_htab_t *h, double b, double p, int n, int m) {
+  int indx = 7;
+  const int mmn = m - n;
+  if (n <= 3 && mmn <= 2) indx = 2 * (n - 1) + mmn;
+  double corr = 1.0;
+  const double b2 = b * b, sb = sqrt(b);
+  if (b > 500.0) return (1.5 / sb + 27.0 / b2) / b2 * corr;
+  int im = (int)(5.0 * p) + 1;
+  if (im > 4) im = 4;
+  const int ip = im + 1;
+  const double wtpp = 5.0 * (p - h->pp[im - 1]);
+  const double wtpm = 1.0 - wtpp;
+  if (b > 25.12) {
+    const double cc = h->c[indx - 1][ip - 1] * wtpp + h->c[indx - 1][im - 1] * wtpm;
+    const double dd = h->d[indx - 1][ip - 1] * wtpp + h->d[indx - 1][im - 1] * wtpm;
+    corr = 1.0 + dd / (cc + b * sb);
+    return (1.5 / sb + 27.0 / b2) / b2 * corr;
+  }
+  int jm = 1;
+  for (int j = 2; j <= 15; ++j)
+    if (b <= h->betagrid[j - 1]) {
+      jm = j - 1;
+      break;
+    }
+  const int jp = jm + 1;
+  const double wtbp = (b - h->betagrid[jm - 1]) / (h->betagrid[jp - 1] - h->betagrid[jm - 1]);
+  const double wtbm = 1.0 - wtbp;
+  const double cbp = h->propbm[indx - 1][jp - 1][ip - 1] * wtpp + h->propbm[indx - 1][jp - 1][im - 1] * wtpm;
+  const double cbm = h->propbm[indx - 1][jm - 1][ip - 1] * wtpp + h->propbm[indx - 1][jm - 1][im - 1] * wtpm;
+  corr = 1.0 + cbp * wtbp + cbm * wtbm;
+  double pr1 = 0.0, pr2 = 0.0;
+  double wt = 0.5 * (10.0 - b);
+  wt = wt < 1.0 ? wt : 1.0;
+  wt = wt > 0.0 ? wt : 0.0;
+  if (b <= 10.0) pr1 = 8.0 / (83.0 + (2.0 + 0.95 * b2) * b);
+  if (b >= 8.0) pr2 = (1.5 / sb + 27.0 / b2) / b2;
+  return (pr1 * wt + pr2 * (1.0 - wt)) * corr;
+}
+
+/* HPROF4's depth vectors (Section 1, :20708-20728) at one depth */
+typedef struct {
+  double xne, pp, fo, y1b, y1s, t3nhe, t3nh2, c1d, c2d, gcon1, gcon2;
+  double xnf1, xnf2, xnfp1, dop1; /* XNF(J,1), XNF(J,2), XNFP(J,1), DOPPLE(J,1) */
+} orc_hdepth_t;
+
+static void orc_hdepth(double xne, double t, double xnfp3, double xnh2, double xnf1, double xnf2, double xnfp1,
+                       double dop1, orc_hdepth_t *d) {
+  const double xne16 = pow(xne, 1.0 / 6.0);
+  d->xne = xne;
+  d->pp = xne16 * 0.08989 / sqrt(t);
+  d->fo = orc_powi(xne16, 4) * 1.25e-9;
+  d->y1b = 2.0 / (1.0 + 0.012 / t * sqrt(xne / t));
+  const double t4 = t / 10000.0;
+  const double t43 = pow(t4, 0.3);
+  d->y1s = t43 / xne16;
+  d->t3nhe = t43 * xnfp3;
+  d->t3nh2 = t43 * xnh2;
+  d->c1d = d->fo * 78940.0 / t;
+  d->c2d = orc_powi(d->fo, 2) / 5.96e-23 / xne;
+  d->gcon1 = 0.2 + 0.09 * sqrt(t4) / (1.0 + xne / 1.0e13);
+  d->gcon2 = 0.2 / (1.0 + xne / 1.0e15);
+  d->xnf1 = xnf1;
+  d->xnf2 = xnf2;
+  d->xnfp1 = xnfp1;
+  d->dop1 = dop1;
+}
+
+/* HPROF4's line constants (Section 2, :20733-20817) */
+typedef struct {
+  int n, m, ifins;
+  double xknm, freqnm, dbeta, wavenm, c1con, c2con, radamp, resont, vdw, starkc, y1num, y1wht;
+  double finest[14], finswt[14];
+} orc_hline_t;
+
+static void orc_hline(const orc_htab_t *h, int n, int m, orc_hline_t *L) {
+  const double FREQ_RYDH = 109677.583403 * 2.99792458e10, CLIGHT_ANGS = 2.99792458e18;
+  const double FOURPI = 4.0 * 3.141592653589793;
+  const int mmn = m - n;
+  const double xn = (double)n, xn2 = xn * xn, xm = (double)m, xm2 = xm * xm;
+  const double xmn2 = xm2 * xn2, xm2mn2 = xm2 - xn2, gnm = xm2mn2 / xmn2;
+  L->n = n;
+  L->m = m;
+  if (mmn <= 3 && n <= 4)
+    L->xknm = h->xknmtb[n - 1][mmn - 1];
+  else
+    L->xknm = 5.5e-5 / gnm * xmn2 / (1.0 + 0.13 / (double)mmn);
+  L->y1num = m == 2 ? 550.0 : m == 3 ? 380.0 : 320.0;
+  L->y1wht = 1.0e13;
+  if (mmn <= 3) L->y1wht = 1.0e14;
+  if (mmn <= 2 && n <= 2) L->y1wht = h->y1wtm[n - 1][mmn - 1];
+  L->freqnm = FREQ_RYDH * gnm;
+  L->dbeta = CLIGHT_ANGS / orc_powi(L->freqnm, 2) / L->xknm;
+  L->wavenm = CLIGHT_ANGS / L->freqnm;
+  L->c1con = L->xknm / L->wavenm * gnm * xm2mn2;
+  L->c2con = orc_powi(L->xknm / L->wavenm, 2);
+  double radamp = h->asum[n - 1] + h->asum[m - 1];
+  if (n == 1) radamp = h->asumlyman[m - 1];
+  radamp = radamp / FOURPI;
+  L->radamp = radamp / L->freqnm;
+  double resont = orc_hfnm(1, m) / xm / (1.0 - 1.0 / xm2);
+  if (n != 1) resont = resont + orc_hfnm(1, n) / xn / (1.0 - 1.0 / xn2);
+  L->resont = resont * 3.92e-24 / gnm;
+  L->vdw = 4.45e-26 / gnm * pow(xm2 * (7.0 * xm2 + 5.0), 0.4);
+  L->starkc = 1.6678e-18 * L->freqnm * L->xknm;
+  if (n > 4 || m > 10) {
+    L->ifins = 1;
+    L->finest[0] = 0.0;
+    L->finswt[0] = 1.0;
+  } else if (mmn != 1) {
+    L->ifins = h->lncomp[n - 1];
+    for (int i = 1; i <= L->ifins; ++i) {
+      L->finest[i - 1] = h->stcomp[i - 1][n - 1] * 1.0e7;
+      L->finswt[i - 1] = h->stcpwt[i - 1][n - 1] / xn2;
+    }
+  } else {
+    L->ifins = h->lnghal[n - 1];
+    const int ipos = h->istal[n - 1];
+    for (int i = 1; i <= L->ifins; ++i) {
+      const int k = ipos - 1 + i;
+      L->finest[i - 1] = h->stalph[k - 1] * 1.0e7;
+      L->finswt[i - 1] = h->stwtal[k - 1] / xn2 / 3.0;
+    }
+  }
+}
+
+/* HPROF4(N, M, J, DELW), Section 3 (:20821-21000), in Voigt normalization */
+static double orc_hprof4(const orc_htab_t *h, const orc_hline_t *L, const orc_hdepth_t *d, double delw) {
+  const double CLIGHT = 2.99792458e10, CLIGHT_ANGS = 2.99792458e18, PI = 3.141592653589793;
+  const double SQRTPI = 1.7724538509055159;
+  const int n = L->n, m = L->m;
+  const double freqnm = L->freqnm;
+  const double delstark = -10.0 * delw / L->wavenm * freqnm;
+  const double wl = L->wavenm + delw * 10.0;
+  const double freq4 = CLIGHT_ANGS / wl;
+  const double del = fabs(freq4 - freqnm);
+  const double hwstk = L->starkc * d->fo;
+  const double hwvdw = L->vdw * d->t3nhe + 2.0 * L->vdw * d->t3nh2;
+  const double hwrad = L->radamp;
+  double hwres = L->resont * d->xnf1;
+  double hwlor = hwres + hwvdw + hwrad;
+  int nwid;
+  if (d->dop1 >= hwstk && d->dop1 >= hwlor)
+    nwid = 1;
+  else if (hwlor >= hwstk)
+    nwid = 2;
+  else
+    nwid = 3;
+  double mx = d->dop1 > hwlor ? d->dop1 : hwlor;
+  mx = mx > hwstk ? mx : hwstk;
+  const double hfwid = freqnm * mx;
+  double hp = 0.0;
+  const int ifcore = fabs(del) <= hfwid;
+  const double dop = freqnm * d->dop1;
+  if (!ifcore || nwid == 1) {
+    for (int i = 0; i < L->ifins; ++i) {
+      const double dd = fabs(freq4 - freqnm - L->finest[i]) / dop;
+      if (dd <= 7.0) hp = hp + exp(-dd * dd) * L->finswt[i];
+    }
+    if (ifcore) return hp;
+  }
+  if (!ifcore || nwid == 2) {
+    if (n == 1 && m == 2) {
+      hwres = hwres * 4.0;
+      hwlor = hwres + hwvdw + hwrad;
+      const double hhw = freqnm * hwlor;
+      double hprofres;
+      if (freq4 > (82259.105 - 4000.0) * CLIGHT) {
+        hprofres = hwres * freqnm / PI / (del * del + hhw * hhw) * SQRTPI * dop;
+      } else {
+        double cutoff = 0.0;
+        if (freq4 >= 50000.0 * CLIGHT) {
+          const double spacing = 200.0 * CLIGHT;
+          const double f22000 = (82259.105 - 22000.0) * CLIGHT;
+          if (freq4 < f22000) {
+            cutoff = (h->cutoffh2[1] - h->cutoffh2[0]) / spacing * (freq4 - f22000) + h->cutoffh2[0];
+          } else {
+            const int icut = (int)((freq4 - f22000) / spacing);
+            const double cutfreq = (double)icut * spacing + f22000;
+            cutoff = (h->cutoffh2[icut + 1] - h->cutoffh2[icut]) / spacing * (freq4 - cutfreq) + h->cutoffh2[icut];
+          }
+          cutoff = pow(10.0, cutoff - 14.0) * d->xnfp1 * 2.0 / CLIGHT;
+        }
+        hprofres = cutoff * SQRTPI * dop;
+      }
+      double hprofrad = hwrad * freqnm / PI / (del * del + hhw * hhw) * SQRTPI * dop;
+      if (freq4 <= 2.463e15) hprofrad = 0.0;
+      double hprofvdw = hwvdw * freqnm / PI / (del * del + hhw * hhw) * SQRTPI * dop;
+      if (freq4 < 1.8e15) hprofvdw = 0.0;
+      hp = hp + (hprofres + hprofrad + hprofvdw);
+    } else {
+      const double hhw = freqnm * hwlor;
+      hp = hp + hhw / PI / (del * del + hhw * hhw) * SQRTPI * dop;
+    }
+    if (ifcore) return hp;
+  }
+  const double wty1 = 1.0 / (1.0 + d->xne / L->y1wht);
+  const double y1scal = L->y1num * d->y1s * wty1 + d->y1b * (1.0 - wty1);
+  const double c1 = d->c1d * L->c1con * y1scal;
+  const double c2 = d->c2d * L->c2con;
+  const double g1 = 6.77 * sqrt(c1);
+  double lg = 0.2114 + log(sqrt(c2) / c1);
+  lg = lg > 0.0 ? lg : 0.0;
+  const double gnot = g1 * lg * (1.0 - d->gcon1 - d->gcon2);
+  const double beta = fabs(delstark) / d->fo * L->dbeta;
+  const double y1 = c1 * beta;
+  const double y2 = c2 * beta * beta;
+  double gam = gnot;
+  if (!(y2 <= 1.0e-4 && y1 <= 1.0e-5)) {
+    const double e = exp(-(y1 < 80.0 ? y1 : 80.0));
+    gam = g1 * (0.5 * e + orc_expi(1, y1) - 0.5 * orc_expi(1, y2)) *
+          (1.0 - d->gcon1 / (1.0 + orc_powi(90.0 * y1, 3)) - d->gcon2 / (1.0 + 2000.0 * y1));
+    if (gam <= 1.0e-20) gam = 0.0;
+  }
+  double prqs = orc_stark_profile(h, beta, d->pp, n, m);
+  if (m <= 2) {
+    prqs = prqs * 0.5;
+    if (freq4 >= (82259.105 - 20000.0) * CLIGHT) {
+      if (freq4 > (82259.105 - 4000.0) * CLIGHT) {
+        const double beta4000 = 4000.0 * CLIGHT / d->fo * L->dbeta;
+        const double prqsp4000 = orc_stark_profile(h, beta4000, d->pp, n, m) * 0.5 / d->fo * L->dbeta;
+        const double cutoff4000 = pow(10.0, -11.07 - 14.0) / CLIGHT * d->xnf2;
+        hp = hp + cutoff4000 / prqsp4000 * prqs / d->fo * L->dbeta * SQRTPI * dop;
+      } else {
+        const double f15000 = (82259.105 - 15000.0) * CLIGHT;
+        const double spacing = 100.0 * CLIGHT;
+        double cutoff;
+        if (freq4 < f15000) {
+          cutoff = (h->cutoffh2plus[1] - h->cutoffh2plus[0]) / spacing * (freq4 - f15000) + h->cutoffh2plus[0];
+        } else {
+          const int icut = (int)((freq4 - f15000) / spacing);
+          const double cutfreq = (double)icut * spacing + f15000;
+          cutoff = (h->cutoffh2plus[icut + 1] - h->cutoffh2plus[icut]) / spacing * (freq4 - cutfreq) +
+                   h->cutoffh2plus[icut];
+        }
+        cutoff = pow(10.0, cutoff - 14.0) / CLIGHT * d->xnf2;
+        hp = hp + cutoff * SQRTPI * dop;
+      }
+    }
+  }
+  double f = 0.0;
+  if (gam > 0.0) f = gam / PI / (gam * gam + beta * beta);
+  const double p1 = orc_powi(0.9 * y1, 2);
+  const double fns = (p1 + 0.03 * sqrt(y1)) / (p1 + 1.0);
+  hp = hp + (prqs * (1.0 + fns) + f) / d->fo * L->dbeta * SQRTPI * dop;
+  return hp;
+}
+
+/* HPROF4 at one point, for the tests: n, m, the depth's inputs, DELW (nm) */
+double orc_hprof4_point(const orc_htab_t *h, int n, int m, double xne, double t, double xnfp3, double xnh2,
+                        double xnf1, double xnf2, double xnfp1, double dop1, double delw) {
+  orc_hdepth_t d;
+  orc_hline_t L;
+  orc_hdepth(xne, t, xnfp3, xnh2, xnf1, xnf2, xnfp1, dop1, &d);
+  orc_hline(h, n, m, &L);
+  return orc_hprof4(h, &L, &d, delw);
+}
+
 /* XLINOP's autoionizing lines (TYPE 1, Fano profile, :20201-20226):
  * CENTER = BSHORE*G*XNFP(J,NELION)/RHO(J) with the two TABCONT gates around
  * the Boltzmann factor, then both wings up to MAX_WING = 2000 points of
@@ -1021,7 +1296,8 @@ int64_t orc_atlas_xlinop(const orc_atlas_tables_t *tb, const orc_nlte_line_t *re
                          const double *xne, const double *txnxn, const double *hckt,
                          const double *tabcont, const int32_t *iwavetab, int nwave,
                          const double *waveset, int numnu, const double *contx, const double *xnfp,
-                         const double *rho, double *xlines) {
+                         const double *rho, const orc_htab_t *htab, const orc_hatm_t *hatm,
+                         double *xlines) {
   const double RYDBERG_INF = 109737.31568157;
   double emerge[KW_MAX];
   for (int j = 0; j < nrhox; ++j) {
@@ -1055,7 +1331,45 @@ int64_t orc_atlas_xlinop(const orc_atlas_tables_t *tb, const orc_nlte_line_t *re
       }
     }
     if (stop) return line;
-    if (r->itype == 2 || r->itype == -1) continue; /* coronal: skipped; hydrogen: not restated */
+    if (r->itype == 2) continue; /* coronal: skipped */
+    if (r->itype == -1) {
+      /* hydrogen (:20177-20199): CENTER = CGF * BOLTH(J, NBLO), BOLTH =
+       * exp(-EH(NBLO)*HCKT)*XNFDOP(J,1); wings in HPROF4 up to MAX_WING, the
+       * red one skipping and the blue one stopping blueward of WCON =
+       * 1e7 / (CONTX(NCON,1) - EMERGE(J)) */
+      const int n = r->nblo, m = r->nbup, ncon = r->ncon;
+      if (!htab || !hatm || !xnfp || n < 1 || m <= n || m > 100 || ncon < 1 || ncon > 25 || nspec < 3) continue;
+      const double RYDBERG_H = 109677.583403;
+      const double eh = n <= 10 ? htab->eh[n - 1] : htab->elim - RYDBERG_H / orc_powi((double)n, 2);
+      orc_hline_t L;
+      orc_hline(htab, n, m, &L);
+      const double cgf = (double)r->gf;
+      for (int J = 1; J <= nrhox; ++J) {
+        const double tc = tabcont[(size_t)(nucont - 1) * kw + J - 1];
+        const double center = cgf * (exp(-eh * hckt[J - 1]) * xnfdop[J - 1]);
+        if (center < tc) continue;
+        const double wcon = 1.0e7 / (contx[ncon - 1] - emerge[J - 1]);
+        orc_hdepth_t d;
+        orc_hdepth(xne[J - 1], hatm->t[J - 1], xnfp[(size_t)2 * kw + J - 1], hatm->xnh2[J - 1],
+                   hatm->xnf1[J - 1], hatm->xnf2[J - 1], xnfp[J - 1], dopple[J - 1], &d);
+        const int hi = nu + 2000 < numnu ? nu + 2000 : numnu;
+        for (int iw = nu; iw <= hi; ++iw) {
+          if (waveset[iw - 1] < wcon) continue;
+          const double cv = center * orc_hprof4(htab, &L, &d, waveset[iw - 1] - wlvac);
+          xlines[(size_t)(iw - 1) * kw + J - 1] += cv;
+          if (cv < tc) break;
+        }
+        for (int i = 1; i <= 2000; ++i) {
+          const int iw = nu - i;
+          if (iw <= 0) break;
+          if (waveset[iw - 1] < wcon) break;
+          const double cv = center * orc_hprof4(htab, &L, &d, waveset[iw - 1] - wlvac);
+          xlines[(size_t)(iw - 1) * kw + J - 1] += cv;
+          if (cv < tc) break;
+        }
+      }
+      continue;
+    }
     if (r->itype != 0 && r->itype != 3) {
       /* autoionizing (TYPE 1) and merged-continuum (any other TYPE, NLAST =
        * TYPE, :20228-20245) records read XNFP(J, NELION) and RHO(J) */

@@ -144,17 +144,45 @@ typedef struct {
   float gammar, gammas, gammaw;
   int32_t nbuff, lim, pad;
 } orc_nlte_line_t;
+/* HPROF4's tables (atlas12_modules.f90:20553-20700) and STARK_PROFILE's
+ * (:20376-20450, data/stark_profile.dat), and XLINOP's hydrogen level
+ * energies (:19964-19975), as the fixture extracted from the source holds
+ * them.  Two-index tables are [first index - 1][second index - 1]. */
+typedef struct {
+  double xknmtb[4][3];  /* XKNMTB(N, M-N) */
+  double y1wtm[2][2];   /* Y1WTM(N, M-N) */
+  double stalph[34], stwtal[34];
+  int32_t istal[4], lnghal[4];
+  double stcomp[5][4], stcpwt[5][4]; /* STCOMP(I, N) */
+  int32_t lncomp[4];
+  double cutoffh2plus[111], cutoffh2[91];
+  double asum[100], asumlyman[100];
+  double betagrid[15], pp[5];
+  double propbm[7][15][5]; /* PROPBM(IP, J, K) at [K-1][J-1][IP-1] */
+  double c[7][5], d[7][5]; /* C(IP, K) at [K-1][IP-1] */
+  double eh[10], elim;
+} orc_htab_t;
+/* the depth vectors HPROF4 reads besides XNE and the XNFP/DOPPLE rows of
+ * species 1 and 3: T(J), XNF(J,1), XNF(J,2), XNH2(J) */
+typedef struct {
+  const double *t, *xnf1, *xnf2, *xnh2;
+} orc_hatm_t;
+double orc_stark_profile(const orc_htab_t *h, double b, double p, int n, int m); /* :20376-20514 */
+double orc_hfnm(int n, int m);                                                  /* :20263-20305 */
+
 /* Adds the TYPE 0/3 records' wings into xlines [numnu][kw]; contx is
  * CONTX(25,16) column-major.  With xnfp [nspec][kw] (XNFP(J,NELION)) and rho
  * [kw] also the autoionizing (TYPE 1) and merged-continuum (other TYPEs)
- * records (:20201-20245); NULL skips them.  Hydrogen (TYPE -1) is not
- * restated.  Returns the number of records read. */
+ * records (:20201-20245); NULL skips them.  With htab and hatm (and xnfp)
+ * also the hydrogen lines (TYPE -1, HPROF4, :20177-20199).  Returns the
+ * number of records read. */
 int64_t orc_atlas_xlinop(const orc_atlas_tables_t *tb, const orc_nlte_line_t *recs, int64_t nrec,
                          int nrhox, int kw, const double *xnfdop, const double *dopple, int nspec,
                          const double *xne, const double *txnxn, const double *hckt,
                          const double *tabcont, const int32_t *iwavetab, int nwave,
                          const double *waveset, int numnu, const double *contx, const double *xnfp,
-                         const double *rho, double *xlines);
+                         const double *rho, const orc_htab_t *htab, const orc_hatm_t *hatm,
+                         double *xlines);
 
 /* ---- SYNTHE compute_line_opacity, normal-metal branch
  *      (synthe_module.f90:3167-3458) and, with xnfpel [nrhox][nspec]

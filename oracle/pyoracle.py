@@ -190,7 +190,14 @@ def _declare2(L):
     L.orc_atlas_linop1.restype = ctypes.c_int64
     L.orc_atlas_xlinop.argtypes = [ctypes.POINTER(_AtlasTables), ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
                                    ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp, _dp, _dp, _ip,
-                                   ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, _dp]
+                                   ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, ctypes.c_void_p,
+                                   ctypes.c_void_p, _dp]
+    L.orc_stark_profile.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+    L.orc_stark_profile.restype = ctypes.c_double
+    L.orc_hfnm.argtypes = [ctypes.c_int, ctypes.c_int]
+    L.orc_hfnm.restype = ctypes.c_double
+    L.orc_hprof4_point.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 9
+    L.orc_hprof4_point.restype = ctypes.c_double
     L.orc_atlas_xlinop.restype = ctypes.c_int64
     L.orc_synthe_nlte_opacity.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -424,10 +431,53 @@ NLTE_LINE = np.dtype([("wlvac", "<f8"), ("elo", "<f4"), ("gf", "<f4"), ("nblo", 
 assert NLTE_LINE.itemsize == 64
 
 
+class HTab(ctypes.Structure):
+    """orc_htab_t: HPROF4's and STARK_PROFILE's tables and XLINOP's hydrogen level energies."""
+    _fields_ = [("xknmtb", ctypes.c_double * 12), ("y1wtm", ctypes.c_double * 4), ("stalph", ctypes.c_double * 34),
+                ("stwtal", ctypes.c_double * 34), ("istal", ctypes.c_int32 * 4), ("lnghal", ctypes.c_int32 * 4),
+                ("stcomp", ctypes.c_double * 20), ("stcpwt", ctypes.c_double * 20), ("lncomp", ctypes.c_int32 * 4),
+                ("cutoffh2plus", ctypes.c_double * 111), ("cutoffh2", ctypes.c_double * 91),
+                ("asum", ctypes.c_double * 100), ("asumlyman", ctypes.c_double * 100),
+                ("betagrid", ctypes.c_double * 15), ("pp", ctypes.c_double * 5), ("propbm", ctypes.c_double * 525),
+                ("c", ctypes.c_double * 35), ("d", ctypes.c_double * 35), ("eh", ctypes.c_double * 10),
+                ("elim", ctypes.c_double)]
+
+    @classmethod
+    def from_tables(cls, t):
+        h = cls()
+        for name in ("xknmtb", "y1wtm", "stalph", "stwtal", "stcomp", "stcpwt", "cutoffh2plus", "cutoffh2", "asum",
+                     "asumlyman", "betagrid", "pp", "propbm", "c", "d", "eh"):
+            v = np.ascontiguousarray(t["h_" + name], np.float64).ravel()  # C order: [first-1][second-1]
+            getattr(h, name)[:] = v.tolist()
+        for name in ("istal", "lnghal", "lncomp"):
+            getattr(h, name)[:] = [int(x) for x in t["h_" + name]]
+        h.elim = float(t["h_elim"][0])
+        return h
+
+
+class _HAtm(ctypes.Structure):
+    _fields_ = [("t", _dp), ("xnf1", _dp), ("xnf2", _dp), ("xnh2", _dp)]
+
+
+def stark_profile(htab, b, p, n, m):
+    return _lib2().orc_stark_profile(ctypes.byref(htab), float(b), float(p), int(n), int(m))
+
+
+def hfnm(n, m):
+    return _lib2().orc_hfnm(int(n), int(m))
+
+
+def hprof4(htab, n, m, xne, t, xnfp3, xnh2, xnf1, xnf2, xnfp1, dop1, delw):
+    return _lib2().orc_hprof4_point(ctypes.byref(htab), int(n), int(m), *[float(v) for v in
+                                                                         (xne, t, xnfp3, xnh2, xnf1, xnf2, xnfp1,
+                                                                          dop1, delw)])
+
+
 def atlas_xlinop(h0, h1, h2, tablog, recs, atm, tabcont, iwavetab, waveset, contx, xlines=None):
     """XLINOP; adds into a copy of xlines [numnu, kw] (zeros when None).  contx: CONTX(25,16) as a
     numpy [16, 25] array (column-major view).  With atm["xnfp"] [nspec, kw] and atm["rho"] [kw] also
-    the autoionizing and merged-continuum records.  Returns (xlines, records read)."""
+    the autoionizing and merged-continuum records; with atm["htab"] (HTab) and atm["t"], atm["xnf1"],
+    atm["xnf2"], atm["xnh2"] [kw] also the hydrogen lines.  Returns (xlines, records read)."""
     h0, h1, h2, tablog = (_d(v) for v in (h0, h1, h2, tablog))
     tb = _AtlasTables(_ptr(h0), _ptr(h1), _ptr(h2), _ptr(tablog))
     rec = np.ascontiguousarray(recs, NLTE_LINE)
@@ -442,10 +492,15 @@ def atlas_xlinop(h0, h1, h2, tablog, recs, atm, tabcont, iwavetab, waveset, cont
     if atm.get("xnfp") is not None:
         xnfp_a, rho_a = _d(atm["xnfp"]), _d(atm["rho"])
         xp, rh = _ptr(xnfp_a), _ptr(rho_a)
+    ht = ha = None
+    if atm.get("htab") is not None:
+        hv = [_d(atm[k]) for k in ("t", "xnf1", "xnf2", "xnh2")]
+        hatm = _HAtm(*[_ptr(v) for v in hv])
+        ht, ha = ctypes.byref(atm["htab"]), ctypes.byref(hatm)
     nread = _lib2().orc_atlas_xlinop(ctypes.byref(tb), rec.ctypes.data_as(ctypes.c_void_p), rec.shape[0], nrhox, kw,
                                      _ptr(xnfdop), _ptr(dopple), nspec, _ptr(xne), _ptr(txnxn), _ptr(hckt),
                                      _ptr(tabcont), _ptr(iw, _ip), iw.size - 1, _ptr(waveset), waveset.size, _ptr(cx),
-                                     xp, rh, _ptr(xl))
+                                     xp, rh, ht, ha, _ptr(xl))
     return xl, nread
 
 

@@ -16,6 +16,16 @@ modified).  Writes tests/golden/reference_tables.npz with:
   molcodes, isox SELECTLINES's diatomic species codes and isotopologue log gf
                  corrections in millidex (atlas12_modules.f90:19182-19202)
   tio_isocorr, h2o_isocorr   the TiO and H2O isotope corrections (:19204, :19207)
+  h_*            the hydrogen line profile's tables (HPROF4, atlas12_modules.f90:20553-21002):
+                 h_xknmtb XKNMTB(4,3) and h_y1wtm Y1WTM(2,2) as [n-1, m-n-1]; the fine
+                 structure h_stalph, h_stwtal (34), h_istal, h_lnghal (4), h_stcomp,
+                 h_stcpwt STCOMP/STCPWT(5,4) as [i-1, n-1], h_lncomp (4); the Lyman alpha
+                 satellite cutoffs h_cutoffh2plus (111), h_cutoffh2 (91); the radiative
+                 damping sums h_asum, h_asumlyman (100); STARK_PROFILE's grids
+                 h_betagrid (15), h_pp (5) (:20376-20514) and its tables from
+                 data/stark_profile.dat: h_propbm [7, 15, 5] (profile, beta, P), h_c,
+                 h_d [7, 5]; XLINOP's hydrogen level energies h_eh (10) and ELIM_HI
+                 h_elim (:19964-19975, :385)
   deck           the reference's converged solar model (workdir/ap00t5777g4.44at12.dat,
                  Teff 5777 K, log g 4.44, 72 depths, iteration 45): READ DECK6
                  columns RHOX, T, P, XNE, ABROSS, ACCRAD, VTURB as printed, [72, 7],
@@ -72,6 +82,21 @@ def fortran_int_array(src, name, count):
     return vals
 
 
+def read_stark(path):
+    """data/stark_profile.dat: per profile K = 1..7 the PROPBM block (15 rows of
+    5), then C (5) and D (5), '#' lines between (STARK_PROFILE's list-directed
+    reads, atlas12_modules.f90:20420-20450)."""
+    vals = []
+    for line in open(path):
+        if line.startswith("#") or not line.strip():
+            continue
+        vals += [float(x.replace("D", "e").replace("d", "e")) for x in line.split()]
+    vals = np.array(vals)
+    assert vals.size == 7 * 85, vals.size
+    v = vals.reshape(7, 85)
+    return v[:, :75].reshape(7, 15, 5), v[:, 75:80], v[:, 80:85]
+
+
 def read_deck(path):
     """READ DECK6 block and PRADK of an ATLAS12 model file."""
     lines = open(path).read().splitlines()
@@ -100,7 +125,26 @@ def main():
         isox=fortran_int_array(mod, "ISOX(NMOL) =", 46),
         tio_isocorr=fortran_int_array(mod, "TIO_ISOCORR(5) =", 5),
         h2o_isocorr=fortran_int_array(mod, "H2O_ISOCORR(4) =", 4),
+        h_xknmtb=fortran_array(mod, "XKNMTB(4,3) =", 12).reshape(4, 3, order="F"),
+        h_y1wtm=fortran_array(mod, "Y1WTM(2,2) =", 4).reshape(2, 2, order="F"),
+        h_stalph=fortran_array(mod, "STALPH(34) =", 34),
+        h_stwtal=fortran_array(mod, "STWTAL(34) =", 34),
+        h_istal=fortran_int_array(mod, "ISTAL(4) =", 4),
+        h_lnghal=fortran_int_array(mod, "LNGHAL(4) =", 4),
+        h_stcomp=fortran_array(mod, "STCOMP(5,4) =", 20).reshape(5, 4, order="F"),
+        h_stcpwt=fortran_array(mod, "STCPWT(5,4) =", 20).reshape(5, 4, order="F"),
+        h_lncomp=fortran_int_array(mod, "LNCOMP(4) =", 4),
+        h_cutoffh2plus=fortran_array(mod, "CUTOFFH2PLUS(111) =", 111),
+        h_cutoffh2=fortran_array(mod, "CUTOFFH2(91) =", 91),
+        h_asum=fortran_array(mod, "ASUM(100) =", 100),
+        h_asumlyman=fortran_array(mod, "ASUMLYMAN(100) =", 100),
+        h_betagrid=fortran_array(mod, "BETAGRID(15) =", 15),
+        h_pp=fortran_array(mod, "PP(5) =", 5),
+        h_eh=np.array([float(re.search(r"EH\(%d\) = ([0-9.D+-]+)" % k, mod).group(1).replace("D", "e"))
+                       for k in range(1, 11)]),
+        h_elim=np.array([float(re.search(r"ELIM_HI = ([0-9.D+-]+)", mod).group(1).replace("D", "e"))]),
     )
+    out["h_propbm"], out["h_c"], out["h_d"] = read_stark(os.path.join(ROOT, "data", "stark_profile.dat"))
     out["deck"], out["deck_pradk"] = read_deck(os.path.join(ROOT, "workdir", "ap00t5777g4.44at12.dat"))
     np.savez(os.path.join(HERE, "reference_tables.npz"), **out)
     for k, v in out.items():

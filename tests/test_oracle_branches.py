@@ -245,3 +245,208 @@ def test_synthe_branches_match_plain_loops(po, small_atm):
     want = py_synthe_other(recs, length, nrhox, g["wbegin"], g["ratio"], 400.8, cont, xnfpel, a["xne"], a["hckt"])
     assert np.count_nonzero(want) > 0.5 * want.size
     np.testing.assert_array_equal(got, want)
+
+
+# ------------------------------------------------------------- hydrogen
+def _powi(x, m):
+    return atlas_powi(x, m)
+
+
+def py_stark(h, b, p, n, m):
+    """STARK_PROFILE (atlas12_modules.f90:20376-20514) in plain Python."""
+    indx = 2 * (n - 1) + (m - n) if (n <= 3 and m - n <= 2) else 7
+    b2, sb = b * b, math.sqrt(b)
+    if b > 500.0:
+        return (1.5 / sb + 27.0 / b2) / b2
+    im = min(int(5.0 * p) + 1, 4)
+    ip = im + 1
+    wtpp = 5.0 * (p - h["h_pp"][im - 1])
+    wtpm = 1.0 - wtpp
+    if b > 25.12:
+        cc = h["h_c"][indx - 1, ip - 1] * wtpp + h["h_c"][indx - 1, im - 1] * wtpm
+        dd = h["h_d"][indx - 1, ip - 1] * wtpp + h["h_d"][indx - 1, im - 1] * wtpm
+        return (1.5 / sb + 27.0 / b2) / b2 * (1.0 + dd / (cc + b * sb))
+    jm = 1
+    for j in range(2, 16):
+        if b <= h["h_betagrid"][j - 1]:
+            jm = j - 1
+            break
+    jp = jm + 1
+    g = h["h_betagrid"]
+    wtbp = (b - g[jm - 1]) / (g[jp - 1] - g[jm - 1])
+    pb = h["h_propbm"][indx - 1]
+    cbp = pb[jp - 1, ip - 1] * wtpp + pb[jp - 1, im - 1] * wtpm
+    cbm = pb[jm - 1, ip - 1] * wtpp + pb[jm - 1, im - 1] * wtpm
+    corr = 1.0 + cbp * wtbp + cbm * (1.0 - wtbp)
+    wt = max(min(0.5 * (10.0 - b), 1.0), 0.0)
+    pr1 = 8.0 / (83.0 + (2.0 + 0.95 * b2) * b) if b <= 10.0 else 0.0
+    pr2 = (1.5 / sb + 27.0 / b2) / b2 if b >= 8.0 else 0.0
+    return (pr1 * wt + pr2 * (1.0 - wt)) * corr
+
+
+def py_hfnm(n, m):
+    if m <= n:
+        return 0.0
+    xn, xm, xmn = float(n), float(m), float(m - n)
+    ginf, gca, fkn = 0.2027 / math.pow(xn, 0.71), 0.124 / xn, xn * 1.9603
+    wtc = 0.45 - 2.4 / _powi(xn, 3) * (xn - 1.0)
+    fk = fkn * _powi(xm / (xmn * (xm + float(n))), 3)
+    x12 = math.pow(xmn, 1.2)
+    wt = (x12 - 1.0) / (x12 + wtc)
+    return fk * (1.0 - wt * ginf - (0.222 + gca / xm) * (1.0 - wt))
+
+
+def py_hprof4(h, n, m, xne, t, xnfp3, xnh2, xnf1, xnf2, xnfp1, dop1, delw, expi):
+    """HPROF4 (atlas12_modules.f90:20553-21002) in plain Python."""
+    c, ca, pi, spi = 2.99792458e10, 2.99792458e18, 3.141592653589793, 1.7724538509055159
+    x16 = math.pow(xne, 1.0 / 6.0)
+    pp, fo = x16 * 0.08989 / math.sqrt(t), _powi(x16, 4) * 1.25e-9
+    y1b = 2.0 / (1.0 + 0.012 / t * math.sqrt(xne / t))
+    t43 = math.pow(t / 10000.0, 0.3)
+    y1s, t3nhe, t3nh2 = t43 / x16, t43 * xnfp3, t43 * xnh2
+    c1d, c2d = fo * 78940.0 / t, _powi(fo, 2) / 5.96e-23 / xne
+    gcon1 = 0.2 + 0.09 * math.sqrt(t / 10000.0) / (1.0 + xne / 1.0e13)
+    gcon2 = 0.2 / (1.0 + xne / 1.0e15)
+    mmn, xn, xm = m - n, float(n), float(m)
+    xn2, xm2 = xn * xn, xm * xm
+    xmn2, xm2mn2 = xm2 * xn2, xm2 - xn2
+    gnm = xm2mn2 / xmn2
+    xknm = h["h_xknmtb"][n - 1, mmn - 1] if (mmn <= 3 and n <= 4) else 5.5e-5 / gnm * xmn2 / (1.0 + 0.13 / mmn)
+    y1num = 550.0 if m == 2 else 380.0 if m == 3 else 320.0
+    y1wht = 1.0e13
+    if mmn <= 3:
+        y1wht = 1.0e14
+    if mmn <= 2 and n <= 2:
+        y1wht = h["h_y1wtm"][n - 1, mmn - 1]
+    freqnm = 109677.583403 * 2.99792458e10 * gnm
+    dbeta = ca / _powi(freqnm, 2) / xknm
+    wavenm = ca / freqnm
+    c1con, c2con = xknm / wavenm * gnm * xm2mn2, _powi(xknm / wavenm, 2)
+    radamp = h["h_asumlyman"][m - 1] if n == 1 else h["h_asum"][n - 1] + h["h_asum"][m - 1]
+    radamp = radamp / (4.0 * pi) / freqnm
+    resont = py_hfnm(1, m) / xm / (1.0 - 1.0 / xm2)
+    if n != 1:
+        resont = resont + py_hfnm(1, n) / xn / (1.0 - 1.0 / xn2)
+    resont = resont * 3.92e-24 / gnm
+    vdw = 4.45e-26 / gnm * math.pow(xm2 * (7.0 * xm2 + 5.0), 0.4)
+    starkc = 1.6678e-18 * freqnm * xknm
+    if n > 4 or m > 10:
+        fs = [(0.0, 1.0)]
+    elif mmn != 1:
+        fs = [(h["h_stcomp"][i, n - 1] * 1.0e7, h["h_stcpwt"][i, n - 1] / xn2) for i in range(h["h_lncomp"][n - 1])]
+    else:
+        k0 = h["h_istal"][n - 1] - 1
+        fs = [(h["h_stalph"][k0 + i] * 1.0e7, h["h_stwtal"][k0 + i] / xn2 / 3.0) for i in range(h["h_lnghal"][n - 1])]
+    dst = -10.0 * delw / wavenm * freqnm
+    freq4 = ca / (wavenm + delw * 10.0)
+    de = abs(freq4 - freqnm)
+    hwstk, hwvdw, hwrad = starkc * fo, vdw * t3nhe + 2.0 * vdw * t3nh2, radamp
+    hwres = resont * xnf1
+    hwlor = hwres + hwvdw + hwrad
+    nwid = 1 if (dop1 >= hwstk and dop1 >= hwlor) else (2 if hwlor >= hwstk else 3)
+    core = abs(de) <= freqnm * max(dop1, hwlor, hwstk)
+    dop = freqnm * dop1
+    hp = 0.0
+    if not core or nwid == 1:
+        for f, w in fs:
+            d = abs(freq4 - freqnm - f) / dop
+            if d <= 7.0:
+                hp = hp + math.exp(-d * d) * w
+        if core:
+            return hp
+    if not core or nwid == 2:
+        if n == 1 and m == 2:
+            hwres = hwres * 4.0
+            hwlor = hwres + hwvdw + hwrad
+            hhw = freqnm * hwlor
+            if freq4 > (82259.105 - 4000.0) * c:
+                res = hwres * freqnm / pi / (de * de + hhw * hhw) * spi * dop
+            else:
+                cut = 0.0
+                if freq4 >= 50000.0 * c:
+                    sp, f0 = 200.0 * c, (82259.105 - 22000.0) * c
+                    tb = h["h_cutoffh2"]
+                    if freq4 < f0:
+                        cut = (tb[1] - tb[0]) / sp * (freq4 - f0) + tb[0]
+                    else:
+                        ic = int((freq4 - f0) / sp)
+                        cut = (tb[ic + 1] - tb[ic]) / sp * (freq4 - (ic * sp + f0)) + tb[ic]
+                    cut = math.pow(10.0, cut - 14.0) * xnfp1 * 2.0 / c
+                res = cut * spi * dop
+            rad = 0.0 if freq4 <= 2.463e15 else hwrad * freqnm / pi / (de * de + hhw * hhw) * spi * dop
+            vd = 0.0 if freq4 < 1.8e15 else hwvdw * freqnm / pi / (de * de + hhw * hhw) * spi * dop
+            hp = hp + (res + rad + vd)
+        else:
+            hhw = freqnm * hwlor
+            hp = hp + hhw / pi / (de * de + hhw * hhw) * spi * dop
+        if core:
+            return hp
+    wty1 = 1.0 / (1.0 + xne / y1wht)
+    y1scal = y1num * y1s * wty1 + y1b * (1.0 - wty1)
+    c1, c2 = c1d * c1con * y1scal, c2d * c2con
+    g1 = 6.77 * math.sqrt(c1)
+    gnot = g1 * max(0.0, 0.2114 + math.log(math.sqrt(c2) / c1)) * (1.0 - gcon1 - gcon2)
+    beta = abs(dst) / fo * dbeta
+    y1, y2 = c1 * beta, c2 * beta * beta
+    gam = gnot
+    if not (y2 <= 1.0e-4 and y1 <= 1.0e-5):
+        gam = g1 * (0.5 * math.exp(-min(80.0, y1)) + expi(1, y1) - 0.5 * expi(1, y2)) * \
+            (1.0 - gcon1 / (1.0 + _powi(90.0 * y1, 3)) - gcon2 / (1.0 + 2000.0 * y1))
+        if gam <= 1.0e-20:
+            gam = 0.0
+    prqs = py_stark(h, beta, pp, n, m)
+    if m <= 2:
+        prqs = prqs * 0.5
+        if freq4 >= (82259.105 - 20000.0) * c:
+            if freq4 > (82259.105 - 4000.0) * c:
+                b4 = 4000.0 * c / fo * dbeta
+                p4 = py_stark(h, b4, pp, n, m) * 0.5 / fo * dbeta
+                c4 = math.pow(10.0, -11.07 - 14.0) / c * xnf2
+                hp = hp + c4 / p4 * prqs / fo * dbeta * spi * dop
+            else:
+                f0, sp = (82259.105 - 15000.0) * c, 100.0 * c
+                tb = h["h_cutoffh2plus"]
+                if freq4 < f0:
+                    cut = (tb[1] - tb[0]) / sp * (freq4 - f0) + tb[0]
+                else:
+                    ic = int((freq4 - f0) / sp)
+                    cut = (tb[ic + 1] - tb[ic]) / sp * (freq4 - (ic * sp + f0)) + tb[ic]
+                hp = hp + math.pow(10.0, cut - 14.0) / c * xnf2 * spi * dop
+    f = gam / pi / (gam * gam + beta * beta) if gam > 0.0 else 0.0
+    p1 = _powi(0.9 * y1, 2)
+    fns = (p1 + 0.03 * math.sqrt(y1)) / (p1 + 1.0)
+    return hp + (prqs * (1.0 + fns) + f) / fo * dbeta * spi * dop
+
+
+def test_stark_profile_and_hfnm_match_plain_loops(po, tables):
+    h = po.HTab.from_tables(tables)
+    rng = np.random.default_rng(8)
+    for _ in range(400):
+        b = float(10.0 ** rng.uniform(-1.0, 3.0))
+        p = float(rng.uniform(0.0, 1.0))
+        n = int(rng.integers(1, 5))
+        m = n + int(rng.integers(1, 8))
+        assert po.stark_profile(h, b, p, n, m) == py_stark(tables, b, p, n, m)
+    for n in range(1, 8):
+        for m in range(1, 30):
+            assert po.hfnm(n, m) == py_hfnm(n, m)
+
+
+@pytest.mark.parametrize("n,m", [(1, 2), (1, 3), (2, 3), (2, 4), (2, 9), (3, 4), (3, 7), (4, 12), (5, 20)])
+def test_hprof4_matches_plain_loops(po, tables, n, m):
+    """HPROF4 over depths of a cool dwarf to a hot giant and both wings: the C
+    oracle and the plain-loop restatement agree bit for bit."""
+    h = po.HTab.from_tables(tables)
+    rng = np.random.default_rng(n * 100 + m)
+    delws = np.concatenate([-np.geomspace(1e-4, 50.0, 40), [0.0], np.geomspace(1e-4, 50.0, 40)])
+    if (n, m) == (1, 2):  # Lyman alpha: far red wing through the H2 and H2+ satellite tables
+        delws = np.concatenate([delws, np.linspace(1.0, 100.0, 60)])
+    for _ in range(6):
+        st = dict(xne=10.0 ** rng.uniform(10.0, 16.0), t=rng.uniform(3500.0, 20000.0),
+                  xnfp3=10.0 ** rng.uniform(10.0, 16.0), xnh2=10.0 ** rng.uniform(0.0, 14.0),
+                  xnf1=10.0 ** rng.uniform(12.0, 17.0), xnf2=10.0 ** rng.uniform(10.0, 15.0),
+                  xnfp1=10.0 ** rng.uniform(10.0, 16.0), dop1=rng.uniform(1e-5, 5e-5))
+        for dw in delws:
+            a = po.hprof4(h, n, m, *st.values(), float(dw))
+            b = py_hprof4(tables, n, m, *st.values(), float(dw), po.expi)
+            assert a == b, (n, m, dw, a, b)
