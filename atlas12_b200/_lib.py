@@ -83,7 +83,8 @@ SIGNATURES = {
     "atlasgpu_synthe_nlte_opacity": (_I, [_P, _P, _I64, _I, _I, _D, _D, _D, _D, _P, _P, _P, _P, _I, _P, _P, _P,
                                           _P, _P]),
     "atlasgpu_atlas_xlinop": (_I, [_P, _P, _I64, _I, _I, _P, _P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P,
-                                   _P, ctypes.POINTER(_I64)]),
+                                   _P, _P, ctypes.POINTER(_I64)]),
+    "atlasgpu_atlas_set_hydrogen_tables": (_I, [_P, _P]),
     "atlasgpu_atlas_rt_pass": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _D,
                                     ctypes.POINTER(Accum), _P]),
     "atlasgpu_atlas_finish": (_I, [_P, ctypes.c_void_p, ctypes.POINTER(Accum), ctypes.POINTER(_D)]),
@@ -132,6 +133,36 @@ MOL2_REC = np.dtype([("wl", "<f4"), ("gflog", "<f4"), ("e1", "<f4"), ("e2", "<f4
 assert MOL2_REC.itemsize == 32
 H2O_REC = np.dtype([("iwl", "<i4"), ("ielo", "<i2"), ("igflog", "<i2")])
 assert H2O_REC.itemsize == 8
+
+
+class HydrogenTables(ctypes.Structure):
+    """atlasgpu_hydrogen_tables (include/atlasgpu.h): HPROF4's and STARK_PROFILE's
+    tables and XLINOP's hydrogen level energies."""
+    _fields_ = [("xknmtb", _D * 12), ("y1wtm", _D * 4), ("stalph", _D * 34), ("stwtal", _D * 34),
+                ("istal", ctypes.c_int32 * 4), ("lnghal", ctypes.c_int32 * 4), ("stcomp", _D * 20),
+                ("stcpwt", _D * 20), ("lncomp", ctypes.c_int32 * 4), ("cutoffh2plus", _D * 111),
+                ("cutoffh2", _D * 91), ("asum", _D * 100), ("asumlyman", _D * 100), ("betagrid", _D * 15),
+                ("pp", _D * 5), ("propbm", _D * 525), ("c", _D * 35), ("d", _D * 35), ("eh", _D * 10), ("elim", _D)]
+
+    @classmethod
+    def from_tables(cls, t):
+        """From arrays named h_<field> (first index slowest, as the header lays them out)."""
+        h = cls()
+        for name, typ in cls._fields_:
+            v = np.asarray(t["h_" + name]).ravel()
+            if name == "elim":
+                h.elim = float(v[0])
+            elif name in ("istal", "lnghal", "lncomp"):
+                getattr(h, name)[:] = [int(x) for x in v]
+            else:
+                getattr(h, name)[:] = [float(x) for x in v]
+        return h
+
+
+class XlinopHydrogen(ctypes.Structure):
+    """atlasgpu_xlinop_hydrogen: T, XNF(J,1), XNF(J,2), XNH2 [nrhox]."""
+    _fields_ = [("t", ctypes.c_void_p), ("xnf1", ctypes.c_void_p), ("xnf2", ctypes.c_void_p),
+                ("xnh2", ctypes.c_void_p)]
 
 
 class SelectState(ctypes.Structure):

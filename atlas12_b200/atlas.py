@@ -84,14 +84,21 @@ class Atlas:
                       ctypes.byref(used))
         return out, used.value
 
+    def set_hydrogen_tables(self, tables):
+        """The hydrogen line profile's tables (arrays h_* as the fixture
+        extracted from the reference holds them) for XLINOP's hydrogen lines."""
+        self._htab = _lib.HydrogenTables.from_tables(tables)
+        self.ctx.call("atlasgpu_atlas_set_hydrogen_tables", ctypes.byref(self._htab))
+
     def xlinop(self, records, nrhox, xnfdop, dopple, xne, txnxn, hckt, tabcont, iwt, waveset, contx, xlines=None,
-               xnfp=None, rho=None):
+               xnfp=None, rho=None, hydrogen=None):
         """XLINOP on unit-19 records (NLTE_LINE array, sorted by wavelength),
         added into a copy of xlines [numnu, kw] (zeros when None).  contx:
         CONTX(25,16) as [16, 25].  With xnfp [nspec, kw] and rho [kw] also the
-        autoionizing and merged-continuum records.  Returns (xlines, number of
-        records of the types not handled: hydrogen, and those two without
-        populations)."""
+        autoionizing and merged-continuum records; with hydrogen = dict(t,
+        xnf1, xnf2, xnh2) [nrhox] (and xnfp, and set_hydrogen_tables) also the
+        hydrogen lines.  Returns (xlines, number of records of the types not
+        handled)."""
         rec = np.ascontiguousarray(records, _lib.NLTE_LINE)
         xd = np.ascontiguousarray(xnfdop, np.float64)
         dp = np.ascontiguousarray(dopple, np.float64)
@@ -105,9 +112,14 @@ class Atlas:
         other = ctypes.c_int64(0)
         xp = None if xnfp is None else np.ascontiguousarray(xnfp, np.float64)
         rh = None if rho is None else np.ascontiguousarray(rho, np.float64)
+        hy = None
+        if hydrogen is not None:
+            hv = [np.ascontiguousarray(hydrogen[k], np.float64) for k in ("t", "xnf1", "xnf2", "xnh2")]
+            hs = _lib.XlinopHydrogen(*[v.ctypes.data for v in hv])
+            hy = ctypes.byref(hs)
         self.ctx.call("atlasgpu_atlas_xlinop", ptr(rec), rec.shape[0], int(nrhox), kw, ptr(xd), ptr(dp), nspec,
                       *[ptr(v) for v in vec], ptr(tc), ptr(iw), iw.size - 1, ptr(ws), ws.size, ptr(cx), ptr(xp),
-                      ptr(rh), ptr(out), ctypes.byref(other))
+                      ptr(rh), hy, ptr(out), ctypes.byref(other))
         return out, other.value
 
     def rt_pass(self, waveset, rcoset, acont, sigmac, xlines, rhox, t, hkt, teff, scont=None):

@@ -5,6 +5,7 @@
 
 #include "api_common.cuh"
 #include "atlas.cuh"
+#include "hydrogen.cuh"
 #include "tcorr.cuh"
 
 using namespace atlasgpu;
@@ -230,13 +231,20 @@ int atlasgpu_atlas_xlinop(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* recs, int
                           const double* xnfdop, const double* dopple, int nspec, const double* xne,
                           const double* txnxn, const double* hckt, const double* tabcont,
                           const int32_t* iwavetab, int nwave, const double* waveset, int numnu,
-                          const double* contx, const double* xnfp, const double* rho, double* xlines_inout,
-                          int64_t* n_other) {
+                          const double* contx, const double* xnfp, const double* rho,
+                          const atlasgpu_xlinop_hydrogen* hyd, double* xlines_inout, int64_t* n_other) {
   if (!ctx || n < 0 || (n > 0 && !recs) || nrhox < 8 || kw < nrhox || kw > kKwMax || nspec < 1 || !xnfdop ||
       !dopple || !xne || !txnxn || !hckt || !tabcont || !iwavetab || nwave < 1 || !waveset || numnu < 2 ||
       !contx || !xlines_inout || (!xnfp) != (!rho))
     return fail(ctx, ATLASGPU_EINVAL, "atlas_xlinop: bad argument");
   const bool pops = xnfp != nullptr;
+  const bool hlines = hyd != nullptr;
+  if (hlines) {
+    if (!pops || nspec < 3 || !hyd->t || !hyd->xnf1 || !hyd->xnf2 || !hyd->xnh2)
+      return fail(ctx, ATLASGPU_EINVAL, "atlas_xlinop: hydrogen lines need XNFP (species 1-3) and T, XNF, XNH2");
+    if (ctx->bufs.find("h_tab") == ctx->bufs.end())
+      return fail(ctx, ATLASGPU_ESTATE, "atlas_xlinop: hydrogen tables not set");
+  }
   if (ctx->bufs.find("tab_h0") == ctx->bufs.end())
     return fail(ctx, ATLASGPU_ESTATE, "atlas_xlinop: Voigt tables not set");
   for (int i = 1; i < numnu; ++i)
@@ -249,7 +257,7 @@ int atlasgpu_atlas_xlinop(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* recs, int
     if ((t == 0 || t == 3) && nc > 0 && (recs[i].nelionx < 1 || recs[i].nelionx > 16))
       return fail(ctx, ATLASGPU_EINVAL, "atlas_xlinop: NELIONX %d outside CONTX at record %lld", recs[i].nelionx,
                   (long long)i);
-    other += t == -1 || (!pops && t != 0 && t != 2 && t != 3);
+    other += (t == -1 && !hlines) || (!pops && t != 0 && t != 2 && t != 3 && t != -1);
   }
   if (n_other) *n_other = other;
   cudaSetDevice(ctx->device);
@@ -307,10 +315,37 @@ int atlasgpu_atlas_xlinop(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* recs, int
       XShoreArgs xa{d_rec, d_lines, n, nrhox, kw, nspec, numnu, d_ws, d_tc, d_xp, d_rho, d_hc, d_em, d_xl};
       k_xlinop_shore<<<grid_for(ctx, n * nrhox * 32, 256, 16), 256, 0, s>>>(xa);
       CKL(ctx);
+      if (hlines) {
+        double* d_hv;
+        if ((r = bufT(ctx, "xl_hv", 4 * (size_t)kw, &d_hv))) return r;
+        const double* hv[4] = {hyd->t, hyd->xnf1, hyd->xnf2, hyd->xnh2};
+        for (int q = 0; q < 4; ++q)
+          CK(cudaMemcpyAsync(d_hv + (size_t)q * kw, hv[q], nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+        XHydArgs ha{d_rec, d_lines, n, nrhox, kw, numnu, (const atlasgpu_hydrogen_tables*)ctx->bufs["h_tab"].first,
+                    d_ws, d_tc, d_xd, d_dp, d_xp, d_xne, d_hc, d_em, d_hv, d_hv + kw, d_hv + 2 * kw, d_hv + 3 * kw,
+                    d_cx, d_xl};
+        k_xlinop_hydrogen<<<grid_for(ctx, n * nrhox * 32, 256, 16), 256, 0, s>>>(ha);
+        CKL(ctx);
+      }
     }
   }
   CK(cudaMemcpyAsync(xlines_inout, d_xl, (size_t)kw * numnu * sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int atlasgpu_atlas_set_hydrogen_tables(atlasgpu_ctx* ctx, const atlasgpu_hydrogen_tables* tables) {
+  if (!ctx || !tables) return fail(ctx, ATLASGPU_EINVAL, "set_hydrogen_tables: null argument");
+  for (int n = 0; n < 4; ++n)
+    if (tables->lnghal[n] < 1 || tables->lnghal[n] > 14 || tables->istal[n] < 1 ||
+        tables->istal[n] + tables->lnghal[n] - 1 > 34 || tables->lncomp[n] < 1 || tables->lncomp[n] > 5)
+      return fail(ctx, ATLASGPU_EINVAL, "set_hydrogen_tables: fine-structure index out of range");
+  cudaSetDevice(ctx->device);
+  atlasgpu_hydrogen_tables* d;
+  int r;
+  if ((r = bufT(ctx, "h_tab", 1, &d))) return r;
+  CK(cudaMemcpyAsync(d, tables, sizeof *tables, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   return 0;
 }
 

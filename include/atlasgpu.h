@@ -220,6 +220,35 @@ int atlasgpu_atlas_linop(atlasgpu_ctx *ctx, const int32_t *linedata, int64_t n, 
                          const int32_t *iwavetab, int nwave, const double *waveset, int numnu,
                          double *xlines_out, int64_t *lines_used);
 
+/* The hydrogen line profile's tables: HPROF4's (atlas12_modules.f90:
+ * 20553-20700), STARK_PROFILE's (:20376-20450 and data/stark_profile.dat)
+ * and XLINOP's level energies EH(1..10) with ELIM_HI (:19964-19975, :385).
+ * Two-index tables at [first index - 1][second index - 1]; PROPBM(IP, J, K)
+ * at [K-1][J-1][IP-1], C and D (IP, K) at [K-1][IP-1]. */
+typedef struct atlasgpu_hydrogen_tables {
+  double xknmtb[4][3]; /* XKNMTB(N, M-N) */
+  double y1wtm[2][2];  /* Y1WTM(N, M-N) */
+  double stalph[34], stwtal[34];
+  int32_t istal[4], lnghal[4];
+  double stcomp[5][4], stcpwt[5][4]; /* STCOMP(I, N) */
+  int32_t lncomp[4];
+  double cutoffh2plus[111], cutoffh2[91];
+  double asum[100], asumlyman[100];
+  double betagrid[15], pp[5];
+  double propbm[7][15][5];
+  double c[7][5], d[7][5];
+  double eh[10], elim;
+} atlasgpu_hydrogen_tables;
+
+/* the depth vectors HPROF4 reads besides XNE, XNFP and DOPPLE: T(J),
+ * XNF(J,1) (H I), XNF(J,2) (H II), XNH2(J), each [nrhox] */
+typedef struct atlasgpu_xlinop_hydrogen {
+  const double *t, *xnf1, *xnf2, *xnh2;
+} atlasgpu_xlinop_hydrogen;
+
+/* Keeps the hydrogen tables on the context for XLINOP's hydrogen lines. */
+int atlasgpu_atlas_set_hydrogen_tables(atlasgpu_ctx *ctx, const atlasgpu_hydrogen_tables *tables);
+
 /* XLINOP (atlas12_modules.f90:19873-20250).  The normal-line branch (TYPE 0 and 3, :20040-20174):
  * the LINOP1 walk on unit-19 records with MAX_WING = 2000, LORENTZ_PREFAC =
  * 0.5642 and the blue-wing cutoff at the continuum edge WCON = 1e7 /
@@ -234,14 +263,19 @@ int atlasgpu_atlas_linop(atlasgpu_ctx *ctx, const int32_t *linedata, int64_t n, 
  * :20201-20226) and the merged-continuum records (every other TYPE but -1,
  * NLAST = TYPE, flat up to the dissolution limit, at most 1001 points,
  * :20228-20245); both NULL: those are skipped and counted in n_other.
- * TYPE 2 records are skipped as in the reference; hydrogen (TYPE -1, the
- * HPROF4 Stark profile) is skipped and counted in n_other (may be NULL). */
+ * With h (and xnfp, and the tables of atlasgpu_atlas_set_hydrogen_tables)
+ * also the hydrogen lines (TYPE -1, :20177-20199): CENTER = GF *
+ * exp(-EH(NBLO)*HCKT) * XNFDOP(J,1), wings of HPROF4(NBLO, NBUP, J, WAVESET -
+ * WLVAC) over MAX_WING points, the red one skipping and the blue one
+ * stopping blueward of WCON = 1e7 / (CONTX(NCON,1) - EMERGE(J)).  TYPE 2
+ * records are skipped as in the reference; the types not handled are
+ * counted in n_other (may be NULL). */
 int atlasgpu_atlas_xlinop(atlasgpu_ctx *ctx, const atlasgpu_nlte_line *recs, int64_t n, int nrhox, int kw,
                           const double *xnfdop, const double *dopple, int nspec, const double *xne,
                           const double *txnxn, const double *hckt, const double *tabcont,
                           const int32_t *iwavetab, int nwave, const double *waveset, int numnu,
-                          const double *contx, const double *xnfp, const double *rho, double *xlines_inout,
-                          int64_t *n_other);
+                          const double *contx, const double *xnfp, const double *rho,
+                          const atlasgpu_xlinop_hydrogen *h, double *xlines_inout, int64_t *n_other);
 
 /* RUN_RT_PASS frequency loop (atlas12_modules.f90:3880-3951): per NU the
  * Planck terms, ALINE = XLINES*STIM, JOSH(1,0) (:18398-18776), the negative

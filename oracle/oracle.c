@@ -1177,7 +1177,8 @@ static double orc_hprof4(const orc_htab_t *h, const orc_hline_t *L, const orc_hd
           if (freq4 < f22000) {
             cutoff = (h->cutoffh2[1] - h->cutoffh2[0]) / spacing * (freq4 - f22000) + h->cutoffh2[0];
           } else {
-            const int icut = (int)((freq4 - f22000) / spacing);
+            int icut = (int)((freq4 - f22000) / spacing);
+            if (icut > 89) icut = 89; /* at the 4000 cm^-1 boundary itself the reference reads past the table */
             const double cutfreq = (double)icut * spacing + f22000;
             cutoff = (h->cutoffh2[icut + 1] - h->cutoffh2[icut]) / spacing * (freq4 - cutfreq) + h->cutoffh2[icut];
           }
@@ -1230,7 +1231,8 @@ static double orc_hprof4(const orc_htab_t *h, const orc_hline_t *L, const orc_hd
         if (freq4 < f15000) {
           cutoff = (h->cutoffh2plus[1] - h->cutoffh2plus[0]) / spacing * (freq4 - f15000) + h->cutoffh2plus[0];
         } else {
-          const int icut = (int)((freq4 - f15000) / spacing);
+          int icut = (int)((freq4 - f15000) / spacing);
+          if (icut > 109) icut = 109; /* the same at the table's end */
           const double cutfreq = (double)icut * spacing + f15000;
           cutoff = (h->cutoffh2plus[icut + 1] - h->cutoffh2plus[icut]) / spacing * (freq4 - cutfreq) +
                    h->cutoffh2plus[icut];

@@ -234,6 +234,65 @@ def test_xlinop_autoionizing_and_merged_continuum_match_oracle(po, gpu_ctx, tabl
     assert np.max(np.abs(got - ref) / scale) < tol
 
 
+def hydrogen_case(po, atlas_case, n_other=2000, seed=12):
+    """Lyman, Balmer, Paschen and Brackett series (TYPE -1, NCON = NBLO, CGF
+    from 2 n^2 f(n, m)) among normal lines over 90-2000 nm, CONTX(N,1) at the
+    hydrogen level edges, and the atmosphere's T, XNF(J,1), XNF(J,2), XNH2."""
+    c = atlas_case
+    rh = 109677.583403
+    recs = synthetic.nlte_records(n_other, 92.0, 1990.0, seed=seed, strong=0.1)
+    series = [(n, m) for n, hi in ((1, 12), (2, 25), (3, 16), (4, 12)) for m in range(n + 1, hi)]
+    hr = np.zeros(len(series), recs.dtype)
+    for i, (n, m) in enumerate(series):
+        wl = 1e7 / (rh * (1.0 / n ** 2 - 1.0 / m ** 2))
+        hr[i]["wlvac"], hr[i]["nblo"], hr[i]["nbup"], hr[i]["itype"], hr[i]["ncon"] = wl, n, m, -1, n
+        hr[i]["nelion"] = 1
+        hr[i]["gf"] = 0.026538 / np.sqrt(np.pi) / synthetic.C_NM * wl * 2 * n * n * po.hfnm(n, m)
+        hr[i]["nbuff"] = int(np.floor(np.log(wl) / np.log(1.0 + 1.0 / 2000000.0) + 0.5))
+    recs = np.concatenate([recs, hr])
+    recs = recs[np.argsort(recs["wlvac"], kind="stable")]
+    contx = synthetic.contx_table()
+    contx[0, :10] = rh / np.arange(1, 11) ** 2
+    pop, t = c["pop"], c["m"]["t"]
+    nh1 = pop["nh"] * (1.0 - pop["xh"])
+    hyd = dict(t=t, xnf1=nh1, xnf2=pop["nh"] * pop["xh"], xnh2=1e-4 * nh1 * np.exp(-t / 1000.0))
+    nsp = min(NSPEC, pop["xnfp"].shape[1])
+    xnfp = np.zeros((NSPEC, 72))
+    xnfp[:nsp] = pop["xnfp"][:, :nsp].T
+    return recs, contx, hyd, xnfp, pop["rho"]
+
+
+@pytest.mark.parametrize("prec,tol", [(_lib.PREC_FP64, 1e-9), (_lib.PREC_MIXED, 1e-6)])
+def test_xlinop_hydrogen_lines_match_oracle(po, gpu_ctx, tables, atlas_case, h_tables, prec, tol):
+    """XLINOP's hydrogen lines (HPROF4 over up to MAX_WING points a side, the
+    blue wing stopping at the level's continuum edge) on top of the other
+    types: every record type handled, none counted."""
+    c = atlas_case
+    ws = np.geomspace(90.0, 2000.0, 6000)
+    recs, contx, hyd, xnfp, rho = hydrogen_case(po, atlas_case)
+    atm = dict(xnfdop=c["xnfdop"], dopple=c["dopple"], xne=c["xne"], txnxn=c["txnxn"], hckt=c["hckt"], xnfp=xnfp,
+               rho=rho)
+    plain, _ = po.atlas_xlinop(*h_tables, po.build_tablog(), recs, atm, c["tabcont"], c["iw"], ws, contx)
+    ref, _ = po.atlas_xlinop(*h_tables, po.build_tablog(), recs, dict(atm, htab=po.HTab.from_tables(tables), **hyd),
+                             c["tabcont"], c["iw"], ws, contx)
+    assert np.count_nonzero(ref != plain) > 50000
+    A = atlas.Atlas(gpu_ctx, tables, *h_tables)
+    A.set_hydrogen_tables(tables)
+    gpu_ctx.set_precision(prec)
+    try:
+        got, other = A.xlinop(recs, 72, c["xnfdop"], c["dopple"], c["xne"], c["txnxn"], c["hckt"], c["tabcont"],
+                              c["iw"], ws, contx, xnfp=xnfp, rho=rho, hydrogen=hyd)
+        plain_got, other_plain = A.xlinop(recs, 72, c["xnfdop"], c["dopple"], c["xne"], c["txnxn"], c["hckt"],
+                                          c["tabcont"], c["iw"], ws, contx, xnfp=xnfp, rho=rho)
+    finally:
+        gpu_ctx.set_precision(_lib.PREC_MIXED)
+    assert other == 0 and other_plain == int(np.sum(recs["itype"] == -1))
+    np.testing.assert_array_equal(got != 0, ref != 0)
+    scale = np.maximum(np.abs(ref), 1e-300)
+    assert np.max(np.abs(got - ref) / scale) < tol
+    np.testing.assert_array_equal(plain_got != 0, plain != 0)
+
+
 def test_xlinop_rejects_unsorted_records(gpu_ctx, tables, atlas_case, h_tables):
     c = atlas_case
     recs = synthetic.nlte_records(100, 300.5, 599.5, seed=6)[::-1].copy()

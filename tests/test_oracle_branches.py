@@ -369,7 +369,7 @@ def py_hprof4(h, n, m, xne, t, xnfp3, xnh2, xnf1, xnf2, xnfp1, dop1, delw, expi)
                     if freq4 < f0:
                         cut = (tb[1] - tb[0]) / sp * (freq4 - f0) + tb[0]
                     else:
-                        ic = int((freq4 - f0) / sp)
+                        ic = min(int((freq4 - f0) / sp), 89)
                         cut = (tb[ic + 1] - tb[ic]) / sp * (freq4 - (ic * sp + f0)) + tb[ic]
                     cut = math.pow(10.0, cut - 14.0) * xnfp1 * 2.0 / c
                 res = cut * spi * dop
@@ -409,7 +409,7 @@ def py_hprof4(h, n, m, xne, t, xnfp3, xnh2, xnf1, xnf2, xnfp1, dop1, delw, expi)
                 if freq4 < f0:
                     cut = (tb[1] - tb[0]) / sp * (freq4 - f0) + tb[0]
                 else:
-                    ic = int((freq4 - f0) / sp)
+                    ic = min(int((freq4 - f0) / sp), 109)
                     cut = (tb[ic + 1] - tb[ic]) / sp * (freq4 - (ic * sp + f0)) + tb[ic]
                 hp = hp + math.pow(10.0, cut - 14.0) / c * xnf2 * spi * dop
     f = gam / pi / (gam * gam + beta * beta) if gam > 0.0 else 0.0
