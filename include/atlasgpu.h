@@ -168,7 +168,7 @@ int atlasgpu_synthe_line_opacity_dev(atlasgpu_ctx *ctx, const atlasgpu_lte_line 
  * tested; and the merged-continuum edges, TYPE = NLAST >= 4 (:3652-3696, vacuum
  * wavelengths): flat from the line to WMERGE, tapering to zero at WTAIL, the
  * grid indices computed on the host with the C library.  xnfpel NULL skips
- * both.  Hydrogen records are skipped. */
+ * both.  Hydrogen records (SYNTHE's hydrogen_line_profile) are skipped. */
 int atlasgpu_synthe_nlte_opacity(atlasgpu_ctx *ctx, const atlasgpu_nlte_line *recs, int64_t n, int length,
                                  int nrhox, double wbegin, double ratio, double wlend, double velshift_kms,
                                  const float *continuum, const double *xnfdop, const double *dopple,
