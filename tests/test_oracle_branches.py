@@ -450,3 +450,98 @@ def test_hprof4_matches_plain_loops(po, tables, n, m):
             a = po.hprof4(h, n, m, *st.values(), float(dw))
             b = py_hprof4(tables, n, m, *st.values(), float(dw), po.expi)
             assert a == b, (n, m, dw, a, b)
+
+
+def py_xlinop_hydrogen(po, h, recs, nrhox, kw, xnfdop1, dopple1, xnfp, xne, hckt, tabcont, iwt, waveset, contx, hatm):
+    """XLINOP's record loop for the hydrogen lines (atlas12_modules.f90:
+    20177-20199) in plain Python, HPROF4 from the oracle's point function."""
+    numnu, nwave = waveset.size, iwt.size - 1
+    xl = np.zeros((numnu, kw))
+    emerge = [RYDBERG_INF / ((1600.0 / math.pow(xne[j], 2.0 / 15.0)) * (1600.0 / math.pow(xne[j], 2.0 / 15.0)))
+              for j in range(nrhox)]
+    nucont, nu = 1, 1
+    for r in recs:
+        wl = float(r["wlvac"])
+        while int(r["nbuff"]) >= iwt[nucont - 1]:
+            nucont += 1
+            if nucont > nwave + 1:
+                nucont = nwave + 1
+                break
+        while wl >= waveset[nu - 1]:
+            nu += 1
+            if nu >= numnu:
+                return xl
+        n, m, ncon = int(r["nblo"]), int(r["nbup"]), int(r["ncon"])
+        if int(r["itype"]) != -1 or n < 1 or m <= n or m > 100 or ncon < 1 or ncon > 25:
+            continue
+        eh = h.eh[n - 1] if n <= 10 else h.elim - 109677.583403 / (n * n)
+        for j in range(nrhox):
+            tc = tabcont[nucont - 1, j]
+            center = float(r["gf"]) * (math.exp(-eh * hckt[j]) * xnfdop1[j])
+            if center < tc:
+                continue
+            wcon = 1.0e7 / (contx.ravel()[ncon - 1] - emerge[j])
+
+            def cv_at(iw):
+                return center * po.hprof4(h, n, m, xne[j], hatm["t"][j], xnfp[2, j], hatm["xnh2"][j],
+                                          hatm["xnf1"][j], hatm["xnf2"][j], xnfp[0, j], dopple1[j],
+                                          waveset[iw - 1] - wl)
+            for iw in range(nu, min(nu + 2000, numnu) + 1):
+                if waveset[iw - 1] < wcon:
+                    continue
+                cv = cv_at(iw)
+                xl[iw - 1, j] += cv
+                if cv < tc:
+                    break
+            for i in range(1, 2001):
+                iw = nu - i
+                if iw <= 0 or waveset[iw - 1] < wcon:
+                    break
+                cv = cv_at(iw)
+                xl[iw - 1, j] += cv
+                if cv < tc:
+                    break
+    return xl
+
+
+def test_xlinop_hydrogen_walk_matches_plain_loops(po, tables, small_atm):
+    """The oracle's hydrogen-line walk (CENTER, the Lyman/Balmer continuum-edge
+    stop of the blue wing, MAX_WING, test after add) against plain loops: bit
+    for bit, Balmer lines on both sides of the Balmer edge at 364.7 nm."""
+    a = small_atm
+    nrhox, kw, nspec = a["nrhox"], a["kw"], a["nspec"]
+    h = po.HTab.from_tables(tables)
+    ws = np.geomspace(350.0, 420.0, 500)
+    cut = atlas.cutoff_grid()
+    iwt = atlas.iwavetab(cut)
+    tabcont = np.full((cut.size + 1, kw), 1.0e-12)
+    rh = 109677.583403
+    series = [(2, m) for m in range(6, 26)] + [(3, 40), (1, 2), (12, 90), (2, 2), (2, 101)]
+    recs = np.zeros(len(series), po.NLTE_LINE)
+    for i, (n, m) in enumerate(series):
+        wl = 1e7 / (rh * (1.0 / n ** 2 - 1.0 / m ** 2)) if m > n else 400.0
+        recs[i]["wlvac"] = wl if 351.0 < wl < 419.0 else 351.0 + i
+        recs[i]["nblo"], recs[i]["nbup"], recs[i]["itype"], recs[i]["ncon"] = n, m, -1, min(n, 25)
+        recs[i]["gf"] = 1.0e-12 * (i + 1)
+        recs[i]["nbuff"] = int(np.floor(np.log(recs[i]["wlvac"]) / np.log(1.0 + 1.0 / 2000000.0) + 0.5))
+    recs = recs[np.argsort(recs["wlvac"], kind="stable")]
+    contx = np.zeros((16, 25))
+    contx[0, :10] = rh / np.arange(1, 11) ** 2
+    rng = np.random.default_rng(21)
+    t = np.linspace(4500.0, 12000.0, kw)
+    hatm = dict(t=t, xnf1=10.0 ** rng.uniform(14.0, 17.0, kw), xnf2=10.0 ** rng.uniform(11.0, 15.0, kw),
+                xnh2=10.0 ** rng.uniform(4.0, 12.0, kw))
+    xnfdop = np.zeros((nspec, kw))
+    xnfdop[0] = 10.0 ** rng.uniform(13.0, 15.0, kw)
+    dopple = np.full((nspec, kw), 1.0)
+    dopple[0] = rng.uniform(1.5e-5, 4e-5, kw)
+    atm = dict(xnfdop=xnfdop, dopple=dopple, xne=a["xne"], txnxn=np.zeros(kw), hckt=a["hckt"], nrhox=nrhox,
+               xnfp=a["xnfp"], rho=a["rho"], htab=h, **hatm)
+    got, _ = po.atlas_xlinop(*po.tabvoigt(tables["tabvi"], tables["tabh1"]), po.build_tablog(), recs, atm, tabcont,
+                             iwt, ws, contx)
+    want = py_xlinop_hydrogen(po, h, recs, nrhox, kw, xnfdop[0], dopple[0], a["xnfp"], a["xne"], a["hckt"], tabcont,
+                              iwt, ws, contx, hatm)
+    assert np.count_nonzero(want) > 1000
+    blue = ws < 1e7 / (rh / 4.0 - 50.0)
+    assert np.count_nonzero(want[blue]) < np.count_nonzero(want[~blue])
+    np.testing.assert_array_equal(got, want)
