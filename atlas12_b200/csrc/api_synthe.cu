@@ -407,7 +407,7 @@ int merged_bins(double wl, int nlast, int nelion, double xne, double wbegin, dou
                 int* n2, int* n3) {
   const double ratiolg = log(ratio);
   const int ixwlbeg = (int)lrint(log(wbegin) / ratiolg);
-  const float inglis = (float)(1600.0 / pow(xne, 2.0 / 15.0));
+  const float inglis = (float)(1600.0 / pow(xne, (double)(2.0f / 15.0f)));
   const float nmerge = inglis - 1.5f;
   const double ryd = nelion == 1 ? 109677.583403 : 109737.31568157;  // RYDBERG_H, RYDBERG_INF
   const double em = ryd / ((double)nmerge * (double)nmerge);
@@ -463,7 +463,7 @@ int atlasgpu_synthe_nlte_opacity(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* re
   // EMERGE(J) = RYDBERG_INF / NMERGE**2 with the reference's REAL(4) INGLIS and NMERGE = INGLIS - 1.5
   std::vector<double> em(nrhox);
   for (int j = 0; j < nrhox; ++j) {
-    const float inglis = (float)(1600.0 / pow(xne[j], 2.0 / 15.0));
+    const float inglis = (float)(1600.0 / pow(xne[j], (double)(2.0f / 15.0f)));
     const float nmerge = inglis - 1.5f;
     em[j] = 109737.31568157 / ((double)nmerge * (double)nmerge);
   }

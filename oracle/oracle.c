@@ -1458,7 +1458,7 @@ static int orc_synthe_merged_bins(double wl, int nlast, int nelion, double xne, 
   const double RYDBERG_INF = 109737.31568157, RYDBERG_H = 109677.583403;
   const double ratiolg = log(ratio);
   const int ixwlbeg = (int)lrint(log(wbegin) / ratiolg);
-  const float inglis = (float)(1600.0 / pow(xne, 2.0 / 15.0));
+  const float inglis = (float)(1600.0 / pow(xne, (double)(2.0f / 15.0f)));
   const float nmerge = inglis - 1.5f;
   const double ryd = nelion == 1 ? RYDBERG_H : RYDBERG_INF;
   const double em = ryd / ((double)nmerge * (double)nmerge);
@@ -1489,7 +1489,7 @@ void orc_synthe_nlte_opacity(const orc_nlte_line_t *recs, int64_t n, int length,
   const double RYDBERG_INF = 109737.31568157, CLIGHT_KMS = 299792.458, CUTOFF = LINE_CUTOFF;
   const double dopratio = 1.0 + velshift_kms / CLIGHT_KMS;
   for (int j = 0; j < nrhox; ++j) {
-    float inglis = (float)(1600.0 / pow(xne[j], 2.0 / 15.0));
+    float inglis = (float)(1600.0 / pow(xne[j], (double)(2.0f / 15.0f)));
     float nmerge = inglis - 1.5f;
     double emerge = RYDBERG_INF / ((double)nmerge * (double)nmerge);
     const float *cont = continuum + (size_t)j * length;

@@ -94,7 +94,7 @@ def py_synthe_other(recs, length, nrhox, wbegin, ratio, wlend, cont, xnfpel, xne
     ixwlbeg = int(round(math.log(wbegin) / ratiolg))
     nspec = xnfpel.shape[1]
     for j in range(nrhox):
-        inglis = np.float32(1600.0 / math.pow(xne[j], 2.0 / 15.0))
+        inglis = np.float32(1600.0 / math.pow(xne[j], float(np.float32(2.0) / np.float32(15.0))))
         nmerge = np.float32(inglis - np.float32(1.5))
         for r in recs:
             t, nel = int(r["itype"]), int(r["nelion"])
