@@ -81,7 +81,8 @@ SIGNATURES = {
     "atlasgpu_atlas_linop": (_I, [_P, _P, _I64, _I, _I, _P, _P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P,
                                   ctypes.POINTER(_I64)]),
     "atlasgpu_synthe_nlte_opacity": (_I, [_P, _P, _I64, _I, _I, _D, _D, _D, _D, _P, _P, _P, _P, _I, _P, _P, _P,
-                                          _P, _P]),
+                                          _P, _P, _P]),
+    "atlasgpu_synthe_set_hydrogen_tables": (_I, [_P, _P, _P]),
     "atlasgpu_atlas_xlinop": (_I, [_P, _P, _I64, _I, _I, _P, _P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P,
                                    _P, _P, ctypes.POINTER(_I64)]),
     "atlasgpu_atlas_set_hydrogen_tables": (_I, [_P, _P]),
@@ -145,11 +146,12 @@ class HydrogenTables(ctypes.Structure):
                 ("pp", _D * 5), ("propbm", _D * 525), ("c", _D * 35), ("d", _D * 35), ("eh", _D * 10), ("elim", _D)]
 
     @classmethod
-    def from_tables(cls, t):
-        """From arrays named h_<field> (first index slowest, as the header lays them out)."""
+    def from_tables(cls, t, prefix="h_"):
+        """From arrays named <prefix><field> (first index slowest, as the header
+        lays them out): "h_" ATLAS12's HPROF4 tables, "s_" SYNTHE's own."""
         h = cls()
         for name, typ in cls._fields_:
-            v = np.asarray(t["h_" + name]).ravel()
+            v = np.asarray(t[prefix + name]).ravel()
             if name == "elim":
                 h.elim = float(v[0])
             elif name in ("istal", "lnghal", "lncomp"):
@@ -157,6 +159,20 @@ class HydrogenTables(ctypes.Structure):
             else:
                 getattr(h, name)[:] = [float(x) for x in v]
         return h
+
+
+class StehleSeries(ctypes.Structure):
+    """atlasgpu_stehle_series: one Stehle Stark-profile series (n_dens 0: not loaded)."""
+    _fields_ = [("n_lower", ctypes.c_int32), ("n_upper_min", ctypes.c_int32), ("n_upper_max", ctypes.c_int32),
+                ("n_dens", ctypes.c_int32), ("density_grid", _D * 20), ("temp_grid", _D * 10),
+                ("log_dalpha_grid", _D * 60), ("max_dens_idx", ctypes.c_void_p), ("k_alpha", ctypes.c_void_p),
+                ("profiles", ctypes.c_void_p)]
+
+
+class SyntheHydrogen(ctypes.Structure):
+    """atlasgpu_synthe_hydrogen: T, XNFPH(J,1), XNFPH(J,2), XNFHE(J,1), XNFH2 [nrhox]."""
+    _fields_ = [("t", ctypes.c_void_p), ("xnfph1", ctypes.c_void_p), ("xnfph2", ctypes.c_void_p),
+                ("xnfhe1", ctypes.c_void_p), ("xnfh2", ctypes.c_void_p)]
 
 
 class XlinopHydrogen(ctypes.Structure):

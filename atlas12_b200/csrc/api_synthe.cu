@@ -4,6 +4,7 @@
 
 #include "api_common.cuh"
 #include "synthe.cuh"
+#include "synthe_h.cuh"
 
 using namespace atlasgpu;
 
@@ -431,15 +432,232 @@ int merged_bins(double wl, int nlast, int nelion, double xne, double wbegin, dou
 }
 }  // namespace
 
+// SYNTHE's hydrogen lines: per hydrogen record the walk's constants, and per
+// (record, depth) the KAPPA0 gates, WCON/WTAIL and whose Doppler width the
+// reference's SAVE'd Stehle convolution was built with (the first record of a
+// run of consecutive records with the same NBLO, NBUP that reach
+// hydrogen_line_profile at that depth)
+static int synthe_hydrogen_launch(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* recs, int64_t n, int length, int nrhox,
+                                  double wbegin, double ratio, double wlend, double dopratio, const float* continuum,
+                                  const double* xnfdop, const float* d_cont, const double* d_xd, const double* d_dp,
+                                  int nspec, const double* xne, const double* d_xne, const double* hckt,
+                                  const double* d_hc, const atlasgpu_synthe_hydrogen* hyd, double* d_acc) {
+  static const double conth[15] = {109678.764, 27419.659, 12186.462, 6854.871, 4387.113, 3046.604, 2238.320, 1713.713,
+                                   1354.044,   1096.776,  906.426,   761.650,  648.980,  559.579,  487.456};
+  const double rydh = 109677.583403, cutoff = 1.0e-3;
+  cudaStream_t s = ctx->stream;
+  atlasgpu_hydrogen_tables tab;
+  CK(cudaMemcpyAsync(&tab, ctx->bufs["sh_tab"].first, sizeof tab, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  double ehyd[100], alphahyd[99];
+  for (int k = 1; k <= 100; ++k) ehyd[k - 1] = k <= 10 ? tab.eh[k - 1] : tab.elim - rydh / ((double)k * (double)k);
+  for (int k = 1; k <= 99; ++k) alphahyd[k - 1] = 1.0e7 / (ehyd[k] - ehyd[k - 1]);
+  std::vector<ShRec> hr;
+  std::vector<int64_t> src;
+  for (int64_t i = 0; i < n; ++i) {
+    const atlasgpu_nlte_line& r = recs[i];
+    if (r.itype != -1 && r.itype != -2) continue;
+    ShRec q;
+    q.wl = r.wlvac * dopratio;
+    q.alpha = alphahyd[r.nblo - 1];
+    q.gf = r.gf;
+    q.elo = r.elo;
+    q.n = r.nblo;
+    q.m = r.nbup;
+    q.nbuff = r.nbuff;
+    q.variant = (r.ncon == 0 || r.nbup == r.nblo + 1) ? 0 : (r.nbup == r.nblo + 2 ? 1 : 2);
+    q.deut = r.itype == -2;
+    hr.push_back(q);
+    src.push_back(i);
+  }
+  const int64_t nh = (int64_t)hr.size();
+  if (nh == 0) return 0;
+  std::vector<ShPair> pairs((size_t)nh * nrhox);
+  for (int j = 0; j < nrhox; ++j) {
+    const float inglis = (float)(1600.0 / pow(xne[j], (double)(2.0f / 15.0f)));
+    const float nmerge = inglis - 1.5f;
+    const double emergeh = rydh / ((double)nmerge * (double)nmerge);
+    const float* cont = continuum + (size_t)j * length;
+    int last_n = 0, last_m = 0, last_deut = 0;
+    for (int64_t k = 0; k < nh; ++k) {
+      const ShRec& q = hr[k];
+      const atlasgpu_nlte_line& r = recs[src[k]];
+      ShPair& p = pairs[(size_t)k * nrhox + j];
+      p.wcon = p.wtail = 0.0;
+      p.flags = p.pad = 0;
+      double kappa0 = (double)q.gf * xnfdop[(size_t)j * nspec];
+      const int ick = q.nbuff < 1 ? 1 : (q.nbuff > length ? length : q.nbuff);
+      const double kapmin = (double)cont[(q.m == 2 ? length : ick) - 1] * cutoff;
+      if (kappa0 < kapmin) continue;
+      kappa0 = kappa0 * exp(-(double)q.elo * hckt[j]);
+      if (kappa0 < kapmin) continue;
+      p.flags = 1;
+      if (q.variant == 2) {
+        const double wshift = 1.0e7 / (conth[r.ncon - 1] - rydh / (81.0 * 81.0));
+        double wmerge = 1.0e7 / (conth[r.ncon - 1] - emergeh);
+        if (wmerge < 0.0) wmerge = wshift + wshift;
+        double wcon = wshift > wmerge ? wshift : wmerge;
+        double wtail = 1.0e7 / (1.0e7 / wcon - 500.0);
+        if (wshift + wshift < wcon) wcon = wshift + wshift;
+        if (wtail < 0.0) wtail = wcon + wcon;
+        if (wcon + wcon < wtail) wtail = wcon + wcon;
+        p.wcon = wcon * dopratio;
+        p.wtail = wtail;
+      }
+      // does the walk reach hydrogen_line_profile at all?
+      const int minred = q.nbuff > 1 ? q.nbuff : 1;
+      const int ib0 = q.nbuff < length + 1 ? q.nbuff : length + 1;
+      bool calls = false, blue = true;
+      if (q.variant == 0) {
+        if (q.wl <= wlend) {
+          calls = minred <= length;
+          if (minred == 1 || q.wl < wbegin) blue = false;
+        }
+      } else if (q.variant == 1) {
+        if (q.wl <= wlend) {
+          if (minred <= length) {
+            if (!(wbegin * powi(ratio, minred - 1) > q.alpha)) calls = true;
+          } else if (minred == 1 || q.wl < wbegin || q.nbuff < 1) {
+            blue = false;
+          }
+        } else if (q.nbuff < 1) {
+          blue = false;
+        }
+      } else {
+        blue = false;
+        if (!(q.wl <= wlend && p.wcon > wlend)) {
+          bool skip = false;
+          if (q.wl <= wlend) {
+            if (wbegin <= q.alpha) {
+              if (wbegin * powi(ratio, minred - 1) >= p.wcon) calls = true;
+              else if (minred == 1) skip = true;
+            }
+            if (!calls && !skip && q.wl < wbegin) skip = true;
+          }
+          if (!calls && !skip && ib0 - 1 >= 1 && !(wbegin * powi(ratio, ib0 - 1) / ratio < p.wcon)) calls = true;
+        }
+      }
+      if (!calls && blue && ib0 - 1 >= 1) calls = true;
+      if (!calls) continue;
+      if (q.n == last_n && q.m == last_m) {
+        if (last_deut) p.flags |= 2;
+      } else {
+        last_n = q.n;
+        last_m = q.m;
+        last_deut = q.deut;
+        if (q.deut) p.flags |= 2;
+      }
+    }
+  }
+  ShRec* d_hr;
+  ShPair* d_pair;
+  double* d_hv;
+  int r;
+  if ((r = bufT(ctx, "sh_rec", (size_t)nh, &d_hr)) || (r = bufT(ctx, "sh_pair", pairs.size(), &d_pair)) ||
+      (r = bufT(ctx, "sh_hv", (size_t)5 * nrhox, &d_hv)))
+    return r;
+  CK(cudaMemcpyAsync(d_hr, hr.data(), (size_t)nh * sizeof(ShRec), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_pair, pairs.data(), pairs.size() * sizeof(ShPair), cudaMemcpyHostToDevice, s));
+  const double* hv[5] = {hyd->t, hyd->xnfph1, hyd->xnfph2, hyd->xnfhe1, hyd->xnfh2};
+  for (int q = 0; q < 5; ++q)
+    CK(cudaMemcpyAsync(d_hv + (size_t)q * nrhox, hv[q], nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  ShArgs a{d_hr, d_pair, nh, nrhox, length, nspec, wbegin, ratio, wlend, d_cont, d_xd, d_dp, d_xne, d_hc,
+           d_hv, d_hv + nrhox, d_hv + 2 * nrhox, d_hv + 3 * nrhox, d_hv + 4 * nrhox,
+           (const atlasgpu_hydrogen_tables*)ctx->bufs["sh_tab"].first,
+           (const StehleDev*)ctx->bufs["sh_stehle"].first, d_acc};
+  const int64_t nwarps = nh * nrhox;
+  const int blocks = grid_for(ctx, nwarps * 32, 32 * kShWarps, 32);
+  k_synthe_hydrogen<<<blocks, 32 * kShWarps, 0, s>>>(a);
+  CKL(ctx);
+  CK(cudaStreamSynchronize(s));  // the host vectors go out of scope
+  return 0;
+}
+
+int atlasgpu_synthe_set_hydrogen_tables(atlasgpu_ctx* ctx, const atlasgpu_hydrogen_tables* tables,
+                                        const atlasgpu_stehle_series* stehle) {
+  if (!ctx || !tables) return fail(ctx, ATLASGPU_EINVAL, "synthe_set_hydrogen_tables: null argument");
+  for (int q = 0; q < 4; ++q)
+    if (tables->lnghal[q] < 1 || tables->lnghal[q] > 14 || tables->istal[q] < 1 ||
+        tables->istal[q] + tables->lnghal[q] - 1 > 34 || tables->lncomp[q] < 1 || tables->lncomp[q] > 5)
+      return fail(ctx, ATLASGPU_EINVAL, "synthe_set_hydrogen_tables: fine-structure index out of range");
+  StehleDev dev[4] = {};
+  if (stehle) {
+    for (int q = 0; q < 4; ++q) {
+      const atlasgpu_stehle_series& S = stehle[q];
+      if (S.n_dens == 0) continue;
+      const int ntr = S.n_upper_max - S.n_upper_min + 1;
+      if (S.n_lower != q + 1 || S.n_upper_min <= S.n_lower || ntr < 1 || S.n_upper_max > 100 || S.n_dens < 2 ||
+          S.n_dens > 20 || !S.max_dens_idx || !S.k_alpha || !S.profiles)
+        return fail(ctx, ATLASGPU_EINVAL, "synthe_set_hydrogen_tables: Stehle series %d malformed", q + 1);
+      for (int t = 0; t < ntr; ++t)
+        if (S.max_dens_idx[t] < 1 || S.max_dens_idx[t] > S.n_dens)
+          return fail(ctx, ATLASGPU_EINVAL, "synthe_set_hydrogen_tables: Stehle series %d density index", q + 1);
+    }
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  atlasgpu_hydrogen_tables* d_tab;
+  StehleDev* d_st;
+  int r;
+  if ((r = bufT(ctx, "sh_tab", 1, &d_tab)) || (r = bufT(ctx, "sh_stehle", 4, &d_st))) return r;
+  CK(cudaMemcpyAsync(d_tab, tables, sizeof *tables, cudaMemcpyHostToDevice, s));
+  for (int q = 0; stehle && q < 4; ++q) {
+    const atlasgpu_stehle_series& S = stehle[q];
+    StehleDev& D = dev[q];
+    if (S.n_dens == 0) continue;
+    const int ntr = S.n_upper_max - S.n_upper_min + 1;
+    const size_t np = (size_t)ntr * S.n_dens * 600;
+    char nm[3][24];
+    snprintf(nm[0], sizeof nm[0], "sh_st_mdi%d", q);
+    snprintf(nm[1], sizeof nm[1], "sh_st_ka%d", q);
+    snprintf(nm[2], sizeof nm[2], "sh_st_pr%d", q);
+    int32_t* d_mdi;
+    double *d_ka, *d_pr;
+    if ((r = bufT(ctx, nm[0], (size_t)ntr, &d_mdi)) || (r = bufT(ctx, nm[1], (size_t)ntr, &d_ka)) ||
+        (r = bufT(ctx, nm[2], np, &d_pr)))
+      return r;
+    CK(cudaMemcpyAsync(d_mdi, S.max_dens_idx, ntr * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_ka, S.k_alpha, ntr * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_pr, S.profiles, np * sizeof(double), cudaMemcpyHostToDevice, s));
+    D.n_lower = S.n_lower;
+    D.n_upper_min = S.n_upper_min;
+    D.n_upper_max = S.n_upper_max;
+    D.n_dens = S.n_dens;
+    memcpy(D.density_grid, S.density_grid, sizeof D.density_grid);
+    memcpy(D.temp_grid, S.temp_grid, sizeof D.temp_grid);
+    memcpy(D.log_dalpha_grid, S.log_dalpha_grid, sizeof D.log_dalpha_grid);
+    D.max_dens_idx = d_mdi;
+    D.k_alpha = d_ka;
+    D.profiles = d_pr;
+  }
+  CK(cudaMemcpyAsync(d_st, dev, sizeof dev, cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
 int atlasgpu_synthe_nlte_opacity(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* recs, int64_t n, int length,
                                  int nrhox, double wbegin, double ratio, double wlend, double velshift_kms,
                                  const float* continuum, const double* xnfdop, const double* dopple,
                                  const double* xnfpel, int nspec, const double* xne, const double* txnxn,
-                                 const double* hckt, const double* contx, float* opacity_inout) {
+                                 const double* hckt, const double* contx, const atlasgpu_synthe_hydrogen* hyd,
+                                 float* opacity_inout) {
   if (!ctx || n < 0 || (n > 0 && !recs) || length < 1 || nrhox < 1 || nrhox > kKwMax || !(wbegin > 0.0) ||
       !(ratio > 1.0) || !continuum || !xnfdop || !dopple || nspec < 1 || !xne || !txnxn || !hckt || !contx ||
       !opacity_inout)
     return fail(ctx, ATLASGPU_EINVAL, "synthe_nlte_opacity: bad argument");
+  if (hyd) {
+    if (!hyd->t || !hyd->xnfph1 || !hyd->xnfph2 || !hyd->xnfhe1 || !hyd->xnfh2)
+      return fail(ctx, ATLASGPU_EINVAL, "synthe_nlte_opacity: hydrogen lines need T, XNFPH, XNFHE, XNFH2");
+    if (ctx->bufs.find("sh_tab") == ctx->bufs.end())
+      return fail(ctx, ATLASGPU_ESTATE, "synthe_nlte_opacity: hydrogen tables not set");
+    for (int64_t i = 0; i < n; ++i) {
+      const atlasgpu_nlte_line& r = recs[i];
+      if ((r.itype == -1 || r.itype == -2) &&
+          (r.nblo < 1 || r.nblo > 99 || r.nbup <= r.nblo || r.nbup > 100 || r.ncon < 0 || r.ncon > 15))
+        return fail(ctx, ATLASGPU_EINVAL, "synthe_nlte_opacity: hydrogen record %lld has NBLO %d NBUP %d NCON %d",
+                    (long long)i, r.nblo, r.nbup, r.ncon);
+    }
+  }
   for (int64_t i = 0; i < n; ++i) {
     const int t = recs[i].itype;
     const bool normal = t == 0 || t == 3 || t <= -3;
@@ -515,6 +733,9 @@ int atlasgpu_synthe_nlte_opacity(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* re
     Timer tm(ctx, "synthe_nlte");
     k_synthe_nlte<<<grid_for(ctx, n * nrhox * 32, 256, 16), 256, 0, s>>>(a);
     CKL(ctx);
+    if (hyd && (r = synthe_hydrogen_launch(ctx, recs, n, length, nrhox, wbegin, ratio, wlend, a.dopratio, continuum,
+                                           xnfdop, d_cont, d_xd, d_dp, nspec, xne, d_xne, hckt, d_hc, hyd, d_acc)))
+      return r;
     k_add_f64_to_f32<<<grid_for(ctx, (int64_t)nm, 256, 8), 256, 0, s>>>(d_acc, d_op, (int64_t)nm);
     CKL(ctx);
   }

@@ -66,6 +66,7 @@ __device__ inline double stark_profile(const atlasgpu_hydrogen_tables& h, double
   if (b > 500.0) return (1.5 / sb + 27.0 / b2) / b2;
   int im = (int)(5.0 * p) + 1;
   if (im > 4) im = 4;
+  if (im < 1) im = 1;  // P >= 0 for any atmosphere; keeps a NaN P inside PP
   const int ip = im + 1;
   const double wtpp = 5.0 * (p - h.pp[im - 1]);
   const double wtpm = 1.0 - wtpp;

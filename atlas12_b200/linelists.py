@@ -156,3 +156,53 @@ class SelectLines:
             counts[kind] = ld.shape[0]
         out = np.concatenate(parts) if parts else np.zeros((0, 4), np.int32)
         return out, counts, state
+
+
+STEHLE_FILES = ("stehle_lyman.bin", "stehle_balmer.bin", "stehle_paschen.bin", "stehle_brackett.bin")
+
+
+def _fortran_records(buf):
+    """The records of a sequential unformatted file (4-byte length markers)."""
+    out, o = [], 0
+    while o < len(buf):
+        n = int(np.frombuffer(buf, "<i4", 1, o)[0])
+        if o + 8 + n > len(buf) or int(np.frombuffer(buf, "<i4", 1, o + 4 + n)[0]) != n:
+            raise ValueError("record markers do not match at byte %d" % o)
+        out.append(buf[o + 4:o + 4 + n])
+        o += 8 + n
+    return out
+
+
+def read_stehle(path):
+    """One Stehle MMM Stark-profile series as INIT_STARK_TABLES reads it
+    (atlas12_modules.f90:17682-17746): record 1 the dimensions (n_lower,
+    n_upper_min, n_upper_max, n_dens, n_temps, n_dalpha), then the density,
+    temperature and log Delta-alpha grids, the per-transition highest valid
+    density index and wing constant, and PROFILES(n_dalpha, n_temps, n_dens,
+    n_trans).  Returns a dict with profiles as [n_trans, n_dens, n_temps,
+    n_dalpha]."""
+    r = _fortran_records(open(path, "rb").read())
+    if len(r) != 7:
+        raise ValueError("%s: %d records, expected 7" % (path, len(r)))
+    n_lower, n_min, n_max, n_dens, n_temps, n_da = (int(x) for x in np.frombuffer(r[0], "<i4", 6))
+    n_trans = n_max - n_min + 1
+    if n_temps != 10 or n_da != 60 or not 2 <= n_dens <= 20 or n_trans < 1:
+        raise ValueError("%s: unexpected dimensions %s" % (path, (n_dens, n_temps, n_da, n_trans)))
+    prof = np.frombuffer(r[6], "<f8", n_da * n_temps * n_dens * n_trans)
+    return dict(n_lower=n_lower, n_upper_min=n_min, n_upper_max=n_max,
+                density_grid=np.frombuffer(r[1], "<f8", n_dens).copy(),
+                temp_grid=np.frombuffer(r[2], "<f8", n_temps).copy(),
+                log_dalpha_grid=np.frombuffer(r[3], "<f8", n_da).copy(),
+                max_dens_idx=np.frombuffer(r[4], "<i4", n_trans).copy(),
+                k_alpha=np.frombuffer(r[5], "<f8", n_trans).copy(),
+                profiles=prof.reshape(n_trans, n_dens, n_temps, n_da).copy())
+
+
+def read_stehle_dir(datadir):
+    """The four series from DATADIR; a missing file leaves its entry None (the
+    reference marks that series not loaded and uses the analytic profile)."""
+    out = []
+    for name in STEHLE_FILES:
+        p = os.path.join(datadir, name)
+        out.append(read_stehle(p) if os.path.exists(p) else None)
+    return out

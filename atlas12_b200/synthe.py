@@ -15,6 +15,8 @@ the memory layout of the reference's (length, nrhox) REAL(4) array.
 Errors raise AtlasGPUError with the library's message (the reference prints
 and calls EXIT(1)).
 """
+import ctypes
+
 import numpy as np
 
 from . import _lib
@@ -95,12 +97,41 @@ class Synthe:
                       ptr(hk), grid["wbegin"], grid["ratio"], grid["length"], ptr(op), ptr(flux), ptr(cont))
         return flux, cont
 
+    def set_hydrogen_tables(self, tables, stehle=None):
+        """SYNTHE's hydrogen_line_profile tables (the s_* arrays extracted from
+        the reference) and the Stehle series (4 dicts as read_stehle gives, None
+        entries not loaded; None: the analytic profile throughout)."""
+        self._shtab = _lib.HydrogenTables.from_tables(tables, "s_")
+        self._stehle_keep = []
+        st = None
+        if stehle is not None:
+            st = (_lib.StehleSeries * 4)()
+            for q, ser in enumerate(stehle):
+                if ser is None:
+                    continue
+                arrs = [np.ascontiguousarray(ser["max_dens_idx"], np.int32),
+                        np.ascontiguousarray(ser["k_alpha"], np.float64),
+                        np.ascontiguousarray(ser["profiles"], np.float64)]
+                self._stehle_keep += arrs
+                a = st[q]
+                a.n_lower, a.n_upper_min, a.n_upper_max = (int(ser[k]) for k in ("n_lower", "n_upper_min",
+                                                                                  "n_upper_max"))
+                a.n_dens = len(ser["density_grid"])
+                a.density_grid[:a.n_dens] = [float(x) for x in ser["density_grid"]]
+                a.temp_grid[:] = [float(x) for x in ser["temp_grid"]]
+                a.log_dalpha_grid[:] = [float(x) for x in ser["log_dalpha_grid"]]
+                a.max_dens_idx, a.k_alpha, a.profiles = (v.ctypes.data for v in arrs)
+        self.ctx.call("atlasgpu_synthe_set_hydrogen_tables", ctypes.byref(self._shtab),
+                      None if st is None else st)
+
     def nlte_opacity(self, records, grid, wlend, continuum, xnfdop, dopple, xne, txnxn, hckt, contx, opacity,
-                     velshift_kms=0.0, xnfpel=None):
+                     velshift_kms=0.0, xnfpel=None, hydrogen=None):
         """compute_line_opacity's normal-metal lines (NLTE_LINE records, nbuff
         = grid index) added into a copy of opacity [nrhox, length] (float32);
         with xnfpel [nrhox, nspec] (populations / RHO) also the autoionizing
-        (Shore) lines.  contx: CONTX(26,17) as [17, 26]."""
+        (Shore) lines; with hydrogen = dict(t, xnfph1, xnfph2, xnfhe1, xnfh2)
+        [nrhox] (and set_hydrogen_tables) also the hydrogen and deuterium
+        lines.  contx: CONTX(26,17) as [17, 26]."""
         rec = np.ascontiguousarray(records, _lib.NLTE_LINE)
         cont = np.ascontiguousarray(continuum, np.float32)
         xd = np.ascontiguousarray(xnfdop, np.float64)
@@ -109,10 +140,15 @@ class Synthe:
         vec = [np.ascontiguousarray(v, np.float64) for v in (xne, txnxn, hckt)]
         out = np.array(opacity, np.float32, copy=True, order="C")
         xp = None if xnfpel is None else np.ascontiguousarray(xnfpel, np.float64)
+        hy = None
+        if hydrogen is not None:
+            hv = [np.ascontiguousarray(hydrogen[k], np.float64) for k in ("t", "xnfph1", "xnfph2", "xnfhe1", "xnfh2")]
+            hs = _lib.SyntheHydrogen(*[v.ctypes.data for v in hv])
+            hy = ctypes.byref(hs)
         self.ctx.call("atlasgpu_synthe_nlte_opacity", ptr(rec), rec.shape[0], int(grid["length"]), nrhox,
                       float(grid["wbegin"]), float(grid["ratio"]), float(wlend), float(velshift_kms), ptr(cont),
                       ptr(xd), ptr(dp), ptr(xp), nspec, *[ptr(v) for v in vec],
-                      ptr(np.ascontiguousarray(contx, np.float64)), ptr(out))
+                      ptr(np.ascontiguousarray(contx, np.float64)), hy, ptr(out))
         return out
 
     def run(self, case):

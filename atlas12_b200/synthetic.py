@@ -316,3 +316,88 @@ def selectlines_records(kind, n, wavetab, seed=12, shuffle_frac=0.0, nspec=1006,
         rec[a] = rec[b]
         rec[b] = tmp
     return rec
+
+
+def stehle_tables(seed=11, series=((1, 2, 30), (2, 3, 30), (3, 4, 30), (4, 5, 7))):
+    """Stehle-format Stark profile tables with the shapes of the published
+    ones (20 densities 1e10..3e19 per half dex, 10 temperatures 2500 K to
+    1.26e6 K, 60 log Delta-alpha points -3.5..5.5) and Holtsmark-like values
+    (flat core, Delta-alpha**-2.5 wings) that are zero above each transition's
+    Inglis-Teller density, for tests of the Stark-convolution path.  Returns
+    4 dicts in the layout the readers give (profiles [n_trans, n_dens, 10, 60])."""
+    rng = np.random.default_rng(seed)
+    out = []
+    lg = np.linspace(-3.5, 5.5, 60)
+    temps = np.array([2500., 5000., 10000., 19950., 39810., 79430., 158500., 316200., 631000., 1259600.])
+    for n_lower, n_min, n_max in series:
+        nd = 20 if n_lower < 4 else 18
+        dens = 10.0 ** (10.0 + 0.5 * np.arange(nd))
+        ntr = n_max - n_min + 1
+        mdi = np.clip(nd - np.arange(ntr) // 2 - rng.integers(0, 3, ntr), 4, nd).astype(np.int32)
+        kal = 10.0 ** rng.uniform(-5.0, 0.5, ntr)
+        da = 10.0 ** lg
+        prof = np.zeros((ntr, nd, 10, 60))
+        for it in range(ntr):
+            w = 0.3 * (1.0 + it) ** 1.5
+            for idn in range(mdi[it]):
+                for itp in range(10):
+                    core = w * (1.0 + 0.05 * idn) * (1.0 + 0.02 * itp)
+                    prof[it, idn, itp] = kal[it] / (core ** 2.5 + da ** 2.5) * (1.0 + 0.1 * np.sin(da + itp))
+        prof[:, :, :, :2][rng.uniform(size=prof[:, :, :, :2].shape) < 0.02] = 0.0
+        out.append(dict(n_lower=n_lower, n_upper_min=n_min, n_upper_max=n_max, density_grid=dens,
+                        temp_grid=temps, log_dalpha_grid=lg, max_dens_idx=mdi, k_alpha=kal, profiles=prof))
+    return out
+
+
+def hydrogen_records(wl_lo, wl_hi, wbegin, ratio, series=((1, 2, 12), (2, 3, 25), (3, 4, 20), (4, 5, 12)),
+                     deuterium=True, scale=1.0):
+    """Unit-19 hydrogen (TYPE -1) and, with `deuterium`, deuterium (TYPE -2,
+    0.027 % bluer, 1.5e-4 of the strength) records for the members n -> m of
+    each (n, m_lo, m_hi) series that fall in [wl_lo, wl_hi] nm: NCON = n for
+    the members past beta (the merged-continuum taper), 0 otherwise; ELO the
+    lower level's energy; CGF from a Kramers-like oscillator strength; NBUFF
+    the SYNTHE grid index of WLVAC on (wbegin, ratio).  Sorted by wavelength."""
+    rh = 109677.583403
+    elev = lambda n: 0.0 if n == 1 else 109678.764 - rh / float(n * n)
+    out = []
+    for n, m_lo, m_hi in series:
+        for m in range(m_lo, m_hi):
+            wl_h = 1e7 / (rh * (1.0 / n ** 2 - 1.0 / m ** 2))
+            for it in ((-1, -2) if deuterium else (-1,)):
+                wl = wl_h * (1.0 - 2.72e-4) if it == -2 else wl_h
+                if not wl_lo <= wl <= wl_hi:
+                    continue
+                f = 1.96 * n * (m / ((m - n) * (m + n))) ** 3 * 0.7
+                r = np.zeros((), _lib_nlte_dtype())
+                r["wlvac"], r["nblo"], r["nbup"], r["itype"] = wl, n, m, it
+                r["ncon"] = n if m > n + 2 else 0
+                r["elo"] = elev(n)
+                r["gf"] = scale * 0.026538 / np.sqrt(np.pi) / C_NM * wl * 2 * n * n * f * (1.5e-4 if it == -2 else 1.0)
+                r["nbuff"] = int(np.floor(np.log(wl / wbegin) / np.log(ratio) + 1.5))
+                out.append(r)
+    recs = np.array(out, _lib_nlte_dtype())
+    return recs[np.argsort(recs["wlvac"], kind="stable")]
+
+
+def _lib_nlte_dtype():
+    from . import _lib
+    return _lib.NLTE_LINE
+
+
+def hydrogen_atmosphere(teff=9500.0, logg=4.0, nspec=3):
+    """A grey atmosphere's hydrogen inputs for SYNTHE's hydrogen lines:
+    xnfdop, dopple [nrhox, nspec] (species 1 = H I), xne, hckt, and the
+    depth vectors T, XNFPH(J,1..2), XNFHE(J,1), XNFH2 [nrhox]."""
+    from . import surrogate as sg
+    m = sg.grey_model(teff, logg)
+    pop = sg.populations(m["t"], m["p"], 2.0)
+    nr = m["t"].size
+    nh1 = pop["nh"] * (1.0 - pop["xh"])
+    xnfdop = np.zeros((nr, nspec))
+    dopple = np.ones((nr, nspec))
+    xnfdop[:, 0] = pop["xnfp"][:, 0] / pop["dopple"][:, 0] / pop["rho"]
+    dopple[:, 0] = pop["dopple"][:, 0]
+    hckt = sg.HPLANCK * sg.CLIGHT / (sg.KBOL * m["t"])
+    return dict(xnfdop=xnfdop, dopple=dopple, xne=pop["xne"], txnxn=np.zeros(nr), hckt=hckt, t=m["t"],
+                xnfph1=nh1, xnfph2=pop["nh"] * pop["xh"], xnfhe1=0.085 * pop["nh"],
+                xnfh2=1e-5 * nh1 * np.exp(-m["t"] / 1500.0))

@@ -151,6 +151,33 @@ int atlasgpu_synthe_line_opacity_dev(atlasgpu_ctx *ctx, const atlasgpu_lte_line 
                                      const double *d_xne, const double *d_txnxn,
                                      const double *d_hckt, int maxprof, float *d_opacity);
 
+/* One Stehle MMM Stark-profile series (INIT_STARK_TABLES,
+ * atlas12_modules.f90:17682-17746: Lyman, Balmer, Paschen, Brackett); n_dens
+ * 0 marks a series that is not loaded.  max_dens_idx [n_trans] (1-based),
+ * k_alpha [n_trans], profiles PROFILES(IA, IT, ID, ITRANS) at
+ * [ITRANS-1][ID-1][IT-1][IA-1] ([n_trans][n_dens][10][60]), n_trans =
+ * n_upper_max - n_upper_min + 1. */
+typedef struct atlasgpu_stehle_series {
+  int32_t n_lower, n_upper_min, n_upper_max, n_dens;
+  double density_grid[20], temp_grid[10], log_dalpha_grid[60];
+  const int32_t *max_dens_idx;
+  const double *k_alpha;
+  const double *profiles;
+} atlasgpu_stehle_series;
+
+/* the depth vectors SYNTHE's hydrogen lines read: T, XNFPH(J,1), XNFPH(J,2),
+ * XNFHE(J,1), XNFH2(J) [nrhox] */
+typedef struct atlasgpu_synthe_hydrogen {
+  const double *t, *xnfph1, *xnfph2, *xnfhe1, *xnfh2;
+} atlasgpu_synthe_hydrogen;
+
+/* Keeps SYNTHE's hydrogen_line_profile tables (its own values, in the layout
+ * of atlasgpu_hydrogen_tables; eh = EHYD(1..10), elim = ELIM_HI) and the four
+ * Stehle series (NULL: none loaded, the analytic profile throughout) on the
+ * context, for atlasgpu_synthe_nlte_opacity. */
+int atlasgpu_synthe_set_hydrogen_tables(atlasgpu_ctx *ctx, const struct atlasgpu_hydrogen_tables *tables,
+                                        const atlasgpu_stehle_series *stehle);
+
 /* The NLTE / complex-profile list's normal-metal lines (TYPE 0, 3 and the He I
  * fallthrough TYPE <= -3) of compute_line_opacity (synthe_module.f90:3167-3458,
  * called per depth at synthe.f90:554): wings walked from the record's grid
@@ -168,12 +195,23 @@ int atlasgpu_synthe_line_opacity_dev(atlasgpu_ctx *ctx, const atlasgpu_lte_line 
  * tested; and the merged-continuum edges, TYPE = NLAST >= 4 (:3652-3696, vacuum
  * wavelengths): flat from the line to WMERGE, tapering to zero at WTAIL, the
  * grid indices computed on the host with the C library.  xnfpel NULL skips
- * both.  Hydrogen records (SYNTHE's hydrogen_line_profile) are skipped. */
+ * both.  With h (and the tables of atlasgpu_synthe_set_hydrogen_tables) also
+ * the hydrogen and deuterium lines, TYPE -1/-2 (:3460-3606): KAPPA0 = GF *
+ * XNFDOP(J,1) * exp(-ELO*HCKT) gated by the continuum, wings of
+ * hydrogen_line_profile(NBLO, NBUP, J, WAVE - WL) (:1032-1980: the Stehle
+ * tables convolved with a Voigt kernel where a loaded series covers the line
+ * and XNE, else the Peterson/Kurucz analytic profile) for the alpha/isolated
+ * lines (NCON 0 or NBUP = NBLO+1), the beta lines (red wing stopping at
+ * ALPHAHYD(NBLO)) and the higher members (tapered between WCON and WTAIL of
+ * the series limit CONTH(NCON), vacuum wavelengths).  NBLO 1..99, NBUP
+ * NBLO+1..100 and NCON 0..15 (the reference aborts or reads outside EHYD,
+ * ALPHAHYD and CONTH otherwise).  h NULL skips them. */
 int atlasgpu_synthe_nlte_opacity(atlasgpu_ctx *ctx, const atlasgpu_nlte_line *recs, int64_t n, int length,
                                  int nrhox, double wbegin, double ratio, double wlend, double velshift_kms,
                                  const float *continuum, const double *xnfdop, const double *dopple,
                                  const double *xnfpel, int nspec, const double *xne, const double *txnxn,
-                                 const double *hckt, const double *contx, float *opacity_inout);
+                                 const double *hckt, const double *contx, const atlasgpu_synthe_hydrogen *h,
+                                 float *opacity_inout);
 
 /* Spectrum: the SYNTHE wavelength loop (synthe.f90:698-718) with
  * setup_opacity_sv and process_wavelength_point (:797-902): per lambda two

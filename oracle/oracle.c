@@ -2223,3 +2223,575 @@ int64_t orc_atlas_selectlines(const orc_select_tables_t *tb, int kind, const voi
   st->igr = igr;
   return ns;
 }
+
+/* ======================================================================
+ * SYNTHE's hydrogen and deuterium lines: compute_line_opacity's TYPE -1/-2
+ * branch (synthe_module.f90:3460-3606) with hydrogen_line_profile
+ * (:1032-1980).  FP64 restatement; the tables are SYNTHE's REAL(4) ones and
+ * the frequency thresholds the reference forms in single precision
+ * ((82259.10 - 4000.0) * REAL(CLIGHT,4) and the like) are formed in float.
+ * ==================================================================== */
+static const double S_CLIGHT = 2.99792458e10, S_CLIGHT_ANGS = 2.99792458e18;
+static const double S_RYDBERG_H = 109677.583403, S_ELIM_HI = 109678.764;
+static const double S_PI = 3.141592653589793;
+/* H_SERIES_LIMITS (atlas12_modules.f90:392-395), CONTH in compute_line_opacity */
+static const double S_CONTH[15] = {109678.764, 27419.659, 12186.462, 6854.871, 4387.113,
+                                   3046.604,   2238.320,  1713.713,  1354.044, 1096.776,
+                                   906.426,    761.650,   648.980,   559.579,  487.456};
+
+/* Lyman alpha's frequency thresholds: (82259.10 - dw) * REAL(CLIGHT,4) in REAL(4) */
+static double s_lya_freq(float dw) { return (double)((82259.10f - dw) * (float)2.99792458e10); }
+
+/* lya_h2_blue_cutoff (:1916-1940): the H2 quasi-molecular satellite on a
+ * 200 cm^-1 grid blueward of 22000 cm^-1 below Lyman alpha; zero below
+ * 50000 cm^-1.  The table index stays inside CUTOFFH2 at the window's edge. */
+static double s_lya_h2_blue(const orc_htab_t *h, double freq, double xnfph1) {
+  const float c4 = (float)2.99792458e10;
+  const float spc = 200.0f * c4, freq22 = (82259.10f - 22000.0f) * c4;
+  if (freq < (double)(50000.0f * c4)) return 0.0;
+  double cval;
+  if (freq < (double)freq22) {
+    cval = (h->cutoffh2[1] - h->cutoffh2[0]) / (double)spc * (freq - (double)freq22) + h->cutoffh2[0];
+  } else {
+    int ic = (int)((freq - (double)freq22) / (double)spc);
+    if (ic > 89) ic = 89;
+    const float cfreq = (float)ic * spc + freq22;
+    cval = (h->cutoffh2[ic + 1] - h->cutoffh2[ic]) / (double)spc * (freq - (double)cfreq) + h->cutoffh2[ic];
+  }
+  return pow(10.0, cval - 14.0) * (double)(float)xnfph1 * 2.0 / (double)c4;
+}
+
+/* lya_h2plus_red_cutoff (:1956-1978): the H2+ satellite, 100 cm^-1 grid */
+static double s_lya_h2plus_red(const orc_htab_t *h, double freq, double xnfph2) {
+  const float c4 = (float)2.99792458e10;
+  const float spc = 100.0f * c4, freq15 = (82259.10f - 15000.0f) * c4;
+  double cval;
+  if (freq < (double)freq15) {
+    cval = (h->cutoffh2plus[1] - h->cutoffh2plus[0]) / (double)spc * (freq - (double)freq15) + h->cutoffh2plus[0];
+  } else {
+    int ic = (int)((freq - (double)freq15) / (double)spc);
+    if (ic > 109) ic = 109;
+    const float cfreq = (float)ic * spc + freq15;
+    cval = (h->cutoffh2plus[ic + 1] - h->cutoffh2plus[ic]) / (double)spc * (freq - (double)cfreq) +
+           h->cutoffh2plus[ic];
+  }
+  return pow(10.0, cval - 14.0) / (double)c4 * (double)(float)xnfph2;
+}
+
+/* expint1 (:731-753): A&S 5.1.56 below 1, a Pade form to 30, zero beyond */
+static double s_expint1(double x) {
+  if (x <= 0.0) return 0.0;
+  if (x <= 1.0)
+    return -log(x) - 0.57721566 +
+           x * (0.99999193 + x * (-0.24991055 + x * (0.05519968 + x * (-0.00976004 + x * 0.00107857))));
+  if (x <= 30.0) return (x * (x + 2.334733) + 0.25062) / (x * (x + 3.330657) + 1.681534) / x * exp(-x);
+  return 0.0;
+}
+
+/* the depth arrays hydrogen_line_profile recomputes when the atmosphere
+ * changes (:1203-1248) */
+typedef struct {
+  double xne, t, pp, fo, y1b, y1s, t3nhe, t3nh2, c1d, c2d, gcon1, gcon2, xnfph1, xnfph2;
+} orc_shdepth_t;
+
+static void orc_shdepth(double xne, double t, double xnfph1, double xnfph2, double xnfhe1, double xnfh2,
+                        orc_shdepth_t *d) {
+  const double xne16 = pow(xne, 1.0 / 6.0);
+  d->xne = xne;
+  d->t = t;
+  d->pp = xne16 * 0.08989 / sqrt(t);
+  d->fo = orc_powi(xne16, 4) * 1.25e-9;
+  d->y1b = 2.0 / (1.0 + 0.012 / t * sqrt(xne / t));
+  const double t4 = t / 10000.0, t43 = pow(t4, 0.3);
+  d->y1s = t43 / xne16;
+  d->t3nhe = t43 * xnfhe1;
+  d->t3nh2 = t43 * xnfh2;
+  d->c1d = d->fo * 78940.0 / t;
+  d->c2d = d->fo * d->fo / 5.96e-23 / xne;
+  d->gcon1 = 0.2 + 0.09 * sqrt(t4) / (1.0 + xne / 1.0e13);
+  d->gcon2 = 0.2 / (1.0 + xne / 1.0e15);
+  d->xnfph1 = xnfph1;
+  d->xnfph2 = xnfph2;
+}
+
+/* the line constants recomputed when N or M changes (:1254-1358) */
+typedef struct {
+  int n, m, ifins;
+  double xknm, freqnm, dbeta, wavenm, c1con, c2con, radamp, resont, vdw, stark, y1num, y1wht;
+  double finest[14], finswt[14];
+} orc_shline_t;
+
+static void orc_shline(const orc_htab_t *h, int n, int m, orc_shline_t *L) {
+  const int mmn = m - n;
+  const double xn = (double)n, xm = (double)m, xn2 = xn * xn, xm2 = xm * xm;
+  const double xmn2 = xm2 * xn2, xm2mn2 = xm2 - xn2, gnm = xm2mn2 / xmn2;
+  L->n = n;
+  L->m = m;
+  L->xknm = (mmn <= 3 && n <= 4) ? h->xknmtb[n - 1][mmn - 1] : 5.5e-5 / gnm * xmn2 / (1.0 + 0.13 / (double)mmn);
+  L->y1num = m == 2 ? 550.0 : (m == 3 ? 380.0 : 320.0);
+  L->y1wht = mmn <= 3 ? 1.0e14 : 1.0e13;
+  if (mmn <= 2 && n <= 2) L->y1wht = h->y1wtm[n - 1][mmn - 1];
+  L->freqnm = S_RYDBERG_H * S_CLIGHT * gnm;
+  L->dbeta = S_CLIGHT_ANGS / (L->freqnm * L->freqnm) / L->xknm;
+  L->wavenm = S_CLIGHT_ANGS / L->freqnm;
+  L->c1con = L->xknm / L->wavenm * gnm * xm2mn2;
+  L->c2con = orc_powi(L->xknm / L->wavenm, 2);
+  double radamp = n == 1 ? h->asumlyman[m - 1] : h->asum[n - 1] + h->asum[m - 1];
+  L->radamp = radamp / (4.0 * S_PI) / L->freqnm;
+  double resont = orc_hfnm(1, m) / xm / (1.0 - 1.0 / xm2);
+  if (n != 1) resont = resont + orc_hfnm(1, n) / xn / (1.0 - 1.0 / xn2);
+  L->resont = resont * 3.579e-24 / gnm;
+  L->vdw = 4.45e-26 / gnm * pow(xm2 * (7.0 * xm2 + 5.0), 0.4);
+  L->stark = 1.6678e-18 * L->freqnm * L->xknm;
+  if (n > 4 || m > 10) {
+    L->ifins = 1;
+    L->finest[0] = 0.0;
+    L->finswt[0] = 1.0;
+  } else if (mmn == 1) {
+    L->ifins = h->lnghal[n - 1];
+    const int ipos = h->istal[n - 1];
+    for (int i = 0; i < L->ifins; ++i) {
+      L->finest[i] = h->stalph[ipos - 1 + i] * 1.0e7;
+      L->finswt[i] = h->stwtal[ipos - 1 + i] / xn2 / 3.0;
+    }
+  } else {
+    L->ifins = h->lncomp[n - 1];
+    for (int i = 0; i < L->ifins; ++i) {
+      L->finest[i] = h->stcomp[i][n - 1] * 1.0e7;
+      L->finswt[i] = h->stcpwt[i][n - 1] / xn2;
+    }
+  }
+}
+
+/* the Peterson/Kurucz analytic profile (:1698-1892): Doppler, Lorentz and
+ * Stark blocks, only the widest inside the core */
+static double orc_shprof_kp(const orc_htab_t *h, const orc_shline_t *L, const orc_shdepth_t *d, double hwdop,
+                            double delw) {
+  const double FREQ_RYDH = S_RYDBERG_H * S_CLIGHT, c4 = (double)(float)2.99792458e10;
+  const int n = L->n, m = L->m;
+  const double freqnm = L->freqnm;
+  const double freq = S_CLIGHT_ANGS / (L->wavenm + delw * 10.0);
+  const double del = fabs(freq - freqnm);
+  const double hwstk = L->stark * d->fo;
+  const double hwvdw = L->vdw * d->t3nhe + 2.0 * L->vdw * d->t3nh2;
+  const double hwrad = L->radamp;
+  const double hwres = L->resont * d->xnfph1 * 2.0;
+  double hwlor = hwres + hwvdw + hwrad;
+  const double dop = freqnm * hwdop;
+  int nwid = 1;
+  if (hwdop < hwstk || hwdop < hwlor) {
+    nwid = 2;
+    if (hwlor < hwstk) nwid = 3;
+  }
+  double mx = hwdop > hwlor ? hwdop : hwlor;
+  if (hwstk > mx) mx = hwstk;
+  const int ifcore = del <= freqnm * mx;
+  double result = 0.0;
+  if (!ifcore || nwid == 1) {
+    for (int i = 0; i < L->ifins; ++i) {
+      const double dd = fabs(freq - freqnm - L->finest[i]) / dop;
+      if (dd <= 7.0) result = result + exp(-dd * dd) * L->finswt[i];
+    }
+    if (ifcore) return result;
+  }
+  if (!ifcore || nwid == 2) {
+    if (n == 1 && m == 2) {
+      const double hwres4 = hwres * 4.0;
+      hwlor = hwres4 + hwvdw + hwrad;
+      const double hhw = freqnm * hwlor;
+      double hprofres;
+      if (freq > s_lya_freq(4000.0f))
+        hprofres = hwres4 * freqnm / S_PI / (del * del + hhw * hhw) * SQRTPI * dop;
+      else
+        hprofres = s_lya_h2_blue(h, freq, d->xnfph1) * SQRTPI * dop;
+      double hprofrad = 0.0;
+      if (freq > (double)2.4190611e15f && freq < (double)0.77f * FREQ_RYDH)
+        hprofrad = hwrad * freqnm / S_PI / (del * del + hhw * hhw) * SQRTPI * dop;
+      double hprofvdw = hwvdw * freqnm / S_PI / (del * del + hhw * hhw) * SQRTPI * dop;
+      if (freq < (double)1.8e15f) hprofvdw = 0.0;
+      result = result + hprofres + hprofrad + hprofvdw;
+    } else {
+      const double hhw = freqnm * hwlor;
+      double top = hhw;
+      if (n == 1 && m <= 5) {
+        if (m == 3 && freq > (double)0.885f * FREQ_RYDH && freq < (double)0.890f * FREQ_RYDH) top = hhw - freqnm * hwrad;
+        if (m == 4 && freq > (double)0.936f * FREQ_RYDH && freq < (double)0.938f * FREQ_RYDH) top = hhw - freqnm * hwrad;
+        if (m == 5 && freq > (double)0.959f * FREQ_RYDH && freq < (double)0.961f * FREQ_RYDH) top = hhw - freqnm * hwrad;
+      }
+      result = result + top / S_PI / (del * del + hhw * hhw) * SQRTPI * dop;
+    }
+    if (ifcore) return result;
+  }
+  const double wty1 = 1.0 / (1.0 + d->xne / L->y1wht);
+  const double y1scal = L->y1num * d->y1s * wty1 + d->y1b * (1.0 - wty1);
+  const double c1 = d->c1d * L->c1con * y1scal, c2 = d->c2d * L->c2con;
+  const double g1 = 6.77 * sqrt(c1);
+  double lg = 0.2114 + log(sqrt(c2) / c1);
+  if (lg < 0.0) lg = 0.0;
+  const double gnot = g1 * lg * (1.0 - d->gcon1 - d->gcon2);
+  const double beta = fabs(del) / d->fo * L->dbeta;
+  const double y1 = c1 * beta, y2 = c2 * (beta * beta);
+  double gam = gnot;
+  if (!(y2 <= 1.0e-4 && y1 <= 1.0e-5)) {
+    gam = g1 * (0.5 * exp(-(y1 < 80.0 ? y1 : 80.0)) + s_expint1(y1) - 0.5 * s_expint1(y2)) *
+          (1.0 - d->gcon1 / (1.0 + orc_powi(90.0 * y1, 3)) - d->gcon2 / (1.0 + 2000.0 * y1));
+    if (gam <= 1.0e-20) gam = 0.0;
+  }
+  double prqs = orc_stark_profile(h, beta, d->pp, n, m);
+  if (m == 2) {
+    prqs = prqs * 0.5;
+    if (freq >= s_lya_freq(20000.0f) && freq <= s_lya_freq(4000.0f)) {
+      result = result + s_lya_h2plus_red(h, freq, d->xnfph2) * SQRTPI * dop;
+    } else if (freq > s_lya_freq(4000.0f)) {
+      const double beta4000 = 4000.0 * c4 / d->fo * L->dbeta;
+      const double prqsp4000 = orc_stark_profile(h, beta4000, d->pp, n, m) * 0.5 / d->fo * L->dbeta;
+      const double cutoff4000 = pow(10.0, -11.07 - 14.0) / c4 * d->xnfph2;
+      result = result + cutoff4000 / prqsp4000 * prqs / d->fo * L->dbeta * SQRTPI * dop;
+    }
+  }
+  const double f = gam > 0.0 ? gam / S_PI / (gam * gam + beta * beta) : 0.0;
+  const double p1 = orc_powi(0.9 * y1, 2);
+  const double fns = (p1 + 0.03 * sqrt(y1)) / (p1 + 1.0);
+  return result + (prqs * (1.0 + fns) + f) / d->fo * L->dbeta * SQRTPI * dop;
+}
+
+double orc_synthe_hprof_kp(const orc_htab_t *h, int n, int m, double xne, double t, double xnfph1,
+                           double xnfph2, double xnfhe1, double xnfh2, double dopph, double delw) {
+  orc_shline_t L;
+  orc_shdepth_t d;
+  orc_shline(h, n, m, &L);
+  orc_shdepth(xne, t, xnfph1, xnfph2, xnfhe1, xnfh2, &d);
+  return orc_shprof_kp(h, &L, &d, dopph, delw);
+}
+
+/* the Stehle-path convolution the reference keeps between calls (SAVE'd
+ * CONV_* variables): rebuilt when N, M or J differ from the last build or
+ * the line constants were recomputed since (another N, M called between) */
+typedef struct {
+  int valid, n, m, last_n, last_m;
+  double F0, lambda0, dop_dalpha, voigt_a;
+  double prof[60];
+} orc_sconv_t;
+
+/* interp_stark_at (:2007-2037): log-log interpolation of the Stark profile */
+static double s_interp_stark(const orc_stehle_t *S, const double *sp, double da) {
+  if (da >= pow(10.0, S->log_dalpha_grid[59])) return sp[59];
+  const double lda = log10(da);
+  int idx;
+  for (idx = 1; idx <= 59; ++idx)
+    if (lda <= S->log_dalpha_grid[idx]) break;
+  if (idx > 59) idx = 59;
+  const double frac = (lda - S->log_dalpha_grid[idx - 1]) / (S->log_dalpha_grid[idx] - S->log_dalpha_grid[idx - 1]);
+  if (sp[idx - 1] > 0.0 && sp[idx] > 0.0) return exp(log(sp[idx - 1]) * (1.0 - frac) + log(sp[idx]) * frac);
+  return sp[idx - 1] * (1.0 - frac) + sp[idx] * frac;
+}
+
+/* the Stark (x) Voigt convolution on the 60-point Delta-alpha grid
+ * (:1427-1640): the table bilinear in (log Ne, T), Ne capped at the
+ * transition's Inglis-Teller density; the kernel on a symmetric grid of the
+ * log points below sigma/3 spacing plus up to 200 wing points at sigma/3 */
+static void orc_sconv_build(const orc_stehle_t *S, const orc_shline_t *L, const orc_shdepth_t *d, double hwdop,
+                            double hwlor_conv, orc_sconv_t *c) {
+  enum { NA = 60, NT = 10, NCONV = 600, NWING = 200 };
+  const int n = L->n, m = L->m;
+  const double xn8 = (double)n, xm8 = (double)m;
+  const double lambda0 = 1.0e8 / S_RYDBERG_H * orc_powi(xn8 * xm8, 2) / ((xm8 - xn8) * (xm8 + xn8));
+  const int itrans = m - S->n_upper_min + 1, nd = S->n_dens;
+  const double dcap = S->density_grid[S->max_dens_idx[itrans - 1] - 1];
+  const double ne_cap = d->xne < dcap ? d->xne : dcap;
+  const double F0 = 1.25e-9 * pow(ne_cap, 2.0 / 3.0);
+  double dag[NA], sp[NA];
+  for (int ia = 0; ia < NA; ++ia) dag[ia] = pow(10.0, S->log_dalpha_grid[ia]);
+  int id1;
+  for (id1 = 1; id1 <= nd - 1; ++id1)
+    if (ne_cap <= S->density_grid[id1]) break;
+  if (id1 > nd - 1) id1 = nd - 1;
+  if (id1 < 1) id1 = 1;
+  const int id2 = id1 + 1;
+  double fd = (log10(ne_cap) - log10(S->density_grid[id1 - 1])) /
+              (log10(S->density_grid[id2 - 1]) - log10(S->density_grid[id1 - 1]));
+  fd = fd < 0.0 ? 0.0 : (fd > 1.0 ? 1.0 : fd);
+  int it1;
+  for (it1 = 1; it1 <= NT - 1; ++it1)
+    if (d->t <= S->temp_grid[it1]) break;
+  if (it1 > NT - 1) it1 = NT - 1;
+  const int it2 = it1 + 1;
+  double ft = (d->t - S->temp_grid[it1 - 1]) / (S->temp_grid[it2 - 1] - S->temp_grid[it1 - 1]);
+  ft = ft < 0.0 ? 0.0 : (ft > 1.0 ? 1.0 : ft);
+  const double *P = S->profiles + (size_t)(itrans - 1) * nd * NT * NA;
+#define SP_AT(ia, it, id) P[((size_t)((id) - 1) * NT + (it) - 1) * NA + (ia)]
+  for (int ia = 0; ia < NA; ++ia) {
+    const double v00 = SP_AT(ia, it1, id1), v01 = SP_AT(ia, it2, id1);
+    const double v10 = SP_AT(ia, it1, id2), v11 = SP_AT(ia, it2, id2);
+    if (v00 > 0 && v01 > 0 && v10 > 0 && v11 > 0)
+      sp[ia] = exp(log(v00) * (1 - fd) * (1 - ft) + log(v01) * (1 - fd) * ft + log(v10) * fd * (1 - ft) +
+                   log(v11) * fd * ft);
+    else
+      sp[ia] = v00 * (1 - fd) * (1 - ft) + v01 * (1 - fd) * ft + v10 * fd * (1 - ft) + v11 * fd * ft;
+  }
+#undef SP_AT
+  const double dop_dalpha = lambda0 * lambda0 / S_CLIGHT_ANGS * L->freqnm * hwdop / F0;
+  const double lor_dalpha = lambda0 * lambda0 / S_CLIGHT_ANGS * L->freqnm * hwlor_conv / F0;
+  const double voigt_a = (double)(float)(lor_dalpha / dop_dalpha);
+  const double dx_wing = dop_dalpha / 3.0;
+  const double d_log = (S->log_dalpha_grid[NA - 1] - S->log_dalpha_grid[0]) / (double)(NA - 1);
+  int n_log = NA;
+  for (int ia = 1; ia <= NA; ++ia)
+    if (dag[ia - 1] * d_log * log(10.0) > dx_wing) {
+      n_log = ia - 1;
+      break;
+    }
+  if (n_log < 1) n_log = 1;
+  const double da_trans = dag[n_log - 1];
+  int n_wing = NWING;
+  double da_wing_max = da_trans + (double)n_wing * dx_wing;
+  if (da_wing_max > dag[NA - 1]) {
+    da_wing_max = dag[NA - 1];
+    n_wing = (int)((da_wing_max - da_trans) / dx_wing);
+    if (n_wing < 0) n_wing = 0;
+  }
+  if (2 * n_wing + 2 * n_log + 1 > NCONV) {
+    n_wing = (NCONV - 2 * n_log - 1) / 2;
+    da_wing_max = da_trans + (double)n_wing * dx_wing;
+  }
+  double cda[NCONV], cpa[NCONV], cst[NCONV];
+  int ic = 0;
+  for (int iw = n_wing; iw >= 1; --iw) {
+    const double da = da_trans + (double)iw * dx_wing;
+    cda[ic] = -da;
+    cpa[ic++] = s_interp_stark(S, sp, da);
+  }
+  for (int ia = n_log; ia >= 1; --ia) {
+    cda[ic] = -dag[ia - 1];
+    cpa[ic++] = sp[ia - 1];
+  }
+  cda[ic] = 0.0;
+  cpa[ic++] = sp[0];
+  for (int ia = 1; ia <= n_log; ++ia) {
+    cda[ic] = dag[ia - 1];
+    cpa[ic++] = sp[ia - 1];
+  }
+  for (int iw = 1; iw <= n_wing; ++iw) {
+    const double da = da_trans + (double)iw * dx_wing;
+    cda[ic] = da;
+    cpa[ic++] = s_interp_stark(S, sp, da);
+  }
+  cst[0] = cda[1] - cda[0];
+  cst[ic - 1] = cda[ic - 1] - cda[ic - 2];
+  for (int iw = 1; iw < ic - 1; ++iw) cst[iw] = 0.5 * (cda[iw + 1] - cda[iw - 1]);
+  for (int ia = 0; ia < NA; ++ia) {
+    const double da_i = dag[ia];
+    if (da_i > da_wing_max && da_wing_max > 0.0) {
+      c->prof[ia] = sp[ia] + voigt_a * dop_dalpha / (S_PI * (da_i * da_i));
+    } else {
+      double gsum = 0.0;
+      for (int iw = 0; iw < ic; ++iw) {
+        const float vv = (float)((da_i - cda[iw]) / dop_dalpha);
+        const double kern = (double)(float)orc_voigt_weideman((double)vv, voigt_a);
+        gsum = gsum + cpa[iw] * kern * cst[iw];
+      }
+      c->prof[ia] = gsum / (dop_dalpha * SQRTPI);
+    }
+  }
+  c->F0 = F0;
+  c->lambda0 = lambda0;
+  c->dop_dalpha = dop_dalpha;
+  c->voigt_a = voigt_a;
+  c->n = n;
+  c->m = m;
+  c->valid = 1;
+}
+
+static int s_use_stehle(const orc_stehle_t *st, int n, int m, double xne) {
+  if (!st || n < 1 || n > 4) return 0;
+  const orc_stehle_t *S = st + (n - 1);
+  return S->n_dens > 0 && m >= S->n_upper_min && m <= S->n_upper_max && xne <= S->density_grid[S->n_dens - 1];
+}
+
+/* hydrogen_line_profile(N, M, J, DELW) with its call-to-call state */
+static double orc_shprof(const orc_htab_t *h, const orc_stehle_t *st, orc_sconv_t *cv, const orc_shline_t *L,
+                         const orc_shdepth_t *d, double hwdop, double delw) {
+  const int n = L->n, m = L->m;
+  if (n != cv->last_n || m != cv->last_m) {
+    cv->last_n = n;
+    cv->last_m = m;
+    cv->valid = 0;
+  }
+  if (!s_use_stehle(st, n, m, d->xne)) return orc_shprof_kp(h, L, d, hwdop, delw);
+  const orc_stehle_t *S = st + (n - 1);
+  const double freq = S_CLIGHT_ANGS / (L->wavenm + delw * 10.0);
+  const double del = fabs(freq - L->freqnm);
+  const double hwvdw = L->vdw * d->t3nhe + 2.0 * L->vdw * d->t3nh2;
+  const double hwres = L->resont * d->xnfph1 * 2.0;
+  const double hwlor = hwres + hwvdw + L->radamp;
+  const double dop = L->freqnm * hwdop;
+  if (!cv->valid || cv->n != n || cv->m != m) {
+    const double hwlor_conv = (n == 1 && m == 2) ? hwres * 4.0 + hwvdw + L->radamp : hwlor;
+    orc_sconv_build(S, L, d, hwdop, hwlor_conv, cv);
+  }
+  const double dac = cv->lambda0 * cv->lambda0 / S_CLIGHT_ANGS * del / cv->F0;
+  double I;
+  if (dac <= pow(10.0, S->log_dalpha_grid[0])) {
+    I = cv->prof[0];
+  } else if (dac >= pow(10.0, S->log_dalpha_grid[59])) {
+    I = S->k_alpha[m - S->n_upper_min] / pow(dac, 2.5) + cv->voigt_a * cv->dop_dalpha / (S_PI * (dac * dac));
+  } else {
+    const double lda = log10(dac);
+    int ia1;
+    for (ia1 = 1; ia1 <= 59; ++ia1)
+      if (lda <= S->log_dalpha_grid[ia1]) break;
+    if (ia1 > 59) ia1 = 59;
+    const double fa = (lda - S->log_dalpha_grid[ia1 - 1]) / (S->log_dalpha_grid[ia1] - S->log_dalpha_grid[ia1 - 1]);
+    const double p1 = cv->prof[ia1 - 1], p2 = cv->prof[ia1];
+    I = (p1 > 0.0 && p2 > 0.0) ? exp(log(p1) * (1.0 - fa) + log(p2) * fa) : p1 * (1.0 - fa) + p2 * fa;
+  }
+  const double phi = I * (cv->lambda0 * cv->lambda0) / (S_CLIGHT_ANGS * cv->F0);
+  double result = phi * SQRTPI * dop;
+  if (n == 1 && m == 2) {
+    if (freq <= s_lya_freq(4000.0f)) result = result + s_lya_h2_blue(h, freq, d->xnfph1) * SQRTPI * dop;
+    if (freq >= s_lya_freq(20000.0f) && freq <= s_lya_freq(4000.0f))
+      result = result + s_lya_h2plus_red(h, freq, d->xnfph2) * SQRTPI * dop;
+    if (freq < (double)(50000.0f * (float)2.99792458e10)) result = 0.0;
+  }
+  return result;
+}
+
+int orc_synthe_hydrogen_opacity(const orc_nlte_line_t *recs, int64_t n, int length, int nrhox,
+                                double wbegin, double ratio, double wlend, double velshift_kms,
+                                const float *continuum, const double *xnfdop, const double *dopple,
+                                int nspec, const double *xne, const double *hckt, const orc_htab_t *tab,
+                                const orc_stehle_t *stehle, const orc_shatm_t *atm, double *out) {
+  const double CUTOFF = LINE_CUTOFF, dopratio = 1.0 + velshift_kms / 299792.458;
+  double ehyd[100], alphahyd[99];
+  for (int k = 1; k <= 100; ++k)
+    ehyd[k - 1] = k <= 10 ? tab->eh[k - 1] : tab->elim - S_RYDBERG_H / ((double)k * (double)k);
+  for (int k = 1; k <= 99; ++k) alphahyd[k - 1] = 1.0e7 / (ehyd[k] - ehyd[k - 1]);
+  for (int64_t i = 0; i < n; ++i) {
+    const orc_nlte_line_t *r = recs + i;
+    if (r->itype != -1 && r->itype != -2) continue;
+    if (r->nblo < 1 || r->nblo > 99 || r->nbup <= r->nblo || r->nbup > 100 || r->ncon < 0 || r->ncon > 15)
+      return -1;
+  }
+  for (int j = 0; j < nrhox; ++j) {
+    const float inglis = (float)(1600.0 / pow(xne[j], (double)(2.0f / 15.0f)));
+    const float nmerge = inglis - 1.5f;
+    const double emergeh = S_RYDBERG_H / ((double)nmerge * (double)nmerge);
+    const float *cont = continuum + (size_t)j * length;
+    double *buf = out + (size_t)j * length;
+    orc_shdepth_t d;
+    orc_shdepth(xne[j], atm->t[j], atm->xnfph1[j], atm->xnfph2[j], atm->xnfhe1[j], atm->xnfh2[j], &d);
+    orc_sconv_t cv;
+    cv.valid = 0;
+    cv.n = cv.m = cv.last_n = cv.last_m = 0;
+    for (int64_t il = 0; il < n; ++il) {
+      const orc_nlte_line_t *r = recs + il;
+      if (r->itype != -1 && r->itype != -2) continue;
+      const int nblo = r->nblo, nbup = r->nbup, ncon = r->ncon, nbuff = r->nbuff;
+      const double wl = r->wlvac * dopratio;
+      double kappa0 = (double)r->gf * xnfdop[(size_t)j * nspec];
+      const int ick = nbuff < 1 ? 1 : (nbuff > length ? length : nbuff);
+      double kapmin = (double)cont[ick - 1] * CUTOFF;
+      if (nbup == 2) kapmin = (double)cont[length - 1] * CUTOFF;
+      if (kappa0 < kapmin) continue;
+      const double bolth = exp(-(double)r->elo * hckt[j]);
+      float dopph = (float)dopple[(size_t)j * nspec];
+      if (r->itype == -2) dopph = dopph / 1.4142f;
+      kappa0 = kappa0 * bolth;
+      if (kappa0 < kapmin) continue;
+      orc_shline_t L;
+      orc_shline(tab, nblo, nbup, &L);
+#define HPROF(w) (kappa0 * orc_shprof(tab, stehle, &cv, &L, &d, (double)dopph, (w) - wl))
+      const int minred = nbuff > 1 ? nbuff : 1;
+      int blue = 1;
+      double wcon = 0.0, wtail = 0.0;
+      const int general = !(ncon == 0 || nbup == nblo + 1) && nbup != nblo + 2;
+      if (!general && (ncon == 0 || nbup == nblo + 1)) {
+        /* alpha / isolated line (:3483-3509) */
+        if (wl <= wlend) {
+          double wave = wbegin * orc_powi(ratio, minred - 1);
+          for (int ib = minred; ib <= length; ++ib) {
+            const double kappa = HPROF(wave);
+            buf[ib - 1] += kappa;
+            if (kappa < (double)cont[ib - 1] * CUTOFF) break;
+            wave = wave * ratio;
+          }
+          if (minred == 1 || wl < wbegin) blue = 0;
+        }
+      } else if (!general) {
+        /* beta line (:3511-3541): the red wing stops at the alpha line */
+        if (wl <= wlend) {
+          double wave = wbegin * orc_powi(ratio, minred - 1);
+          int exited = 0;
+          for (int ib = minred; ib <= length; ++ib) {
+            if (wave > alphahyd[nblo - 1]) {
+              exited = 1;
+              break;
+            }
+            const double kappa = HPROF(wave);
+            buf[ib - 1] += kappa;
+            if (kappa < (double)cont[ib - 1] * CUTOFF) {
+              exited = 1;
+              break;
+            }
+            wave = wave * ratio;
+          }
+          if (!exited && (minred == 1 || wl < wbegin || nbuff < 1)) blue = 0;
+        } else if (nbuff < 1) {
+          blue = 0;
+        }
+      } else {
+        /* higher series members with the merged-continuum taper
+         * (:3543-3606, vacuum wavelengths) */
+        const double wshift = 1.0e7 / (S_CONTH[ncon - 1] - S_RYDBERG_H / (81.0 * 81.0));
+        double wmerge = 1.0e7 / (S_CONTH[ncon - 1] - emergeh);
+        if (wmerge < 0.0) wmerge = wshift + wshift;
+        wcon = wshift > wmerge ? wshift : wmerge;
+        wtail = 1.0e7 / (1.0e7 / wcon - 500.0);
+        if (wshift + wshift < wcon) wcon = wshift + wshift;
+        if (wtail < 0.0) wtail = wcon + wcon;
+        if (wcon + wcon < wtail) wtail = wcon + wcon;
+        wcon = wcon * dopratio;
+        if (wl <= wlend) {
+          if (wcon > wlend) continue;
+          if (wbegin <= alphahyd[nblo - 1]) {
+            double wave = wbegin * orc_powi(ratio, minred - 1);
+            if (wave >= wcon) {
+              double kappa = HPROF(wave);
+              if (kappa >= (double)cont[(minred < length ? minred : length) - 1] * CUTOFF) {
+                if (wave < wtail) kappa = kappa * ((wave - wcon) / (wtail - wcon));
+                if (minred <= length) buf[minred - 1] += kappa; /* the reference's BUFFER(MINRED) */
+                wave = wave * ratio;
+                for (int ib = minred + 1; ib <= length; ++ib) {
+                  if (wave >= wcon) {
+                    kappa = HPROF(wave);
+                    if (wave < wtail) kappa = kappa * ((wave - wcon) / (wtail - wcon));
+                    buf[ib - 1] += kappa;
+                    if (kappa < (double)cont[ib - 1] * CUTOFF) break;
+                  }
+                  wave = wave * ratio;
+                }
+              }
+            }
+            if (minred == 1) continue;
+          }
+          if (wl < wbegin) continue;
+        }
+      }
+      if (!blue) continue;
+      int ib = nbuff < length + 1 ? nbuff : length + 1;
+      const int maxblue = ib - 1;
+      double wave = wbegin * orc_powi(ratio, ib - 1);
+      for (int i = 1; i <= maxblue; ++i) {
+        ib = ib - 1;
+        wave = wave / ratio;
+        if (general && wave < wcon) break;
+        double kappa = HPROF(wave);
+        if (general && wave < wtail) kappa = kappa * ((wave - wcon) / (wtail - wcon));
+        buf[ib - 1] += kappa;
+        if (kappa < (double)cont[ib - 1] * CUTOFF) break;
+      }
+#undef HPROF
+    }
+  }
+  return 0;
+}

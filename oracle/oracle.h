@@ -287,6 +287,41 @@ int64_t orc_atlas_selectlines(const orc_select_tables_t *tb, int kind, const voi
                               const int32_t *iwavetab, const double *wavetab, int nwave,
                               int32_t *out, int64_t cap, int64_t *bad);
 
+/* ---- SYNTHE's hydrogen and deuterium lines (compute_line_opacity TYPE -1/-2,
+ *      synthe_module.f90:3460-3606) with hydrogen_line_profile (:1032-1980):
+ *      the Peterson/Kurucz analytic profile and the Stehle MMM tables
+ *      convolved with a Voigt kernel; FP64 restatement, the REAL(4) tables
+ *      and threshold literals rounded to single precision as declared ------
+ * One Stehle series (INIT_STARK_TABLES, atlas12_modules.f90:17682-17746):
+ * n_dens = 0 marks a series that is not loaded.  profiles holds
+ * PROFILES(IA, IT, ID, ITRANS) at [ITRANS-1][ID-1][IT-1][IA-1]. */
+typedef struct {
+  int32_t n_lower, n_upper_min, n_upper_max, n_dens;
+  double density_grid[20], temp_grid[10], log_dalpha_grid[60];
+  const int32_t *max_dens_idx; /* [n_trans] */
+  const double *k_alpha;       /* [n_trans] */
+  const double *profiles;      /* [n_trans][n_dens][10][60] */
+} orc_stehle_t;
+/* the depth vectors hydrogen_line_profile reads: T, XNFPH(J,1), XNFPH(J,2),
+ * XNFHE(J,1), XNFH2(J) [nrhox] */
+typedef struct {
+  const double *t, *xnfph1, *xnfph2, *xnfhe1, *xnfh2;
+} orc_shatm_t;
+/* hydrogen_line_profile(N, M, J, DELW) at one depth, K-P path (no Stehle
+ * tables); dopph is DOPPH(J).  For tests of the profile alone. */
+double orc_synthe_hprof_kp(const orc_htab_t *h, int n, int m, double xne, double t, double xnfph1,
+                           double xnfph2, double xnfhe1, double xnfh2, double dopph, double delw);
+/* Adds the TYPE -1/-2 records' opacity at every depth into out
+ * [nrhox][length] (double), the other records skipped; stehle [4] (Lyman,
+ * Balmer, Paschen, Brackett) or NULL for the K-P path throughout; tab holds
+ * SYNTHE's own tables (eh: EHYD(1..10)).  Returns 0, or -1 when a record's
+ * NBLO/NBUP/NCON is outside EHYD/ALPHAHYD/CONTH (the reference aborts). */
+int orc_synthe_hydrogen_opacity(const orc_nlte_line_t *recs, int64_t n, int length, int nrhox,
+                                double wbegin, double ratio, double wlend, double velshift_kms,
+                                const float *continuum, const double *xnfdop, const double *dopple,
+                                int nspec, const double *xne, const double *hckt, const orc_htab_t *tab,
+                                const orc_stehle_t *stehle, const orc_shatm_t *atm, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -443,15 +443,16 @@ class HTab(ctypes.Structure):
                 ("elim", ctypes.c_double)]
 
     @classmethod
-    def from_tables(cls, t):
+    def from_tables(cls, t, prefix="h_"):
+        """prefix "h_": ATLAS12's HPROF4 tables; "s_": SYNTHE's hydrogen_line_profile ones."""
         h = cls()
         for name in ("xknmtb", "y1wtm", "stalph", "stwtal", "stcomp", "stcpwt", "cutoffh2plus", "cutoffh2", "asum",
                      "asumlyman", "betagrid", "pp", "propbm", "c", "d", "eh"):
-            v = np.ascontiguousarray(t["h_" + name], np.float64).ravel()  # C order: [first-1][second-1]
+            v = np.ascontiguousarray(t[prefix + name], np.float64).ravel()  # C order: [first-1][second-1]
             getattr(h, name)[:] = v.tolist()
         for name in ("istal", "lnghal", "lncomp"):
-            getattr(h, name)[:] = [int(x) for x in t["h_" + name]]
-        h.elim = float(t["h_elim"][0])
+            getattr(h, name)[:] = [int(x) for x in t[prefix + name]]
+        h.elim = float(t[prefix + "elim"][0])
         return h
 
 
@@ -579,3 +580,69 @@ def selectlines(tables, kind, recs, state, xmax, hckt_last, iwavetab, wavetab, c
         return None, int(r), int(bad.value)
     state.update(nu=st.nu, igr=st.igr, freq=st.freq)
     return out[:r].copy(), 0, -1
+
+
+# ------------------------------------------------------------- SYNTHE hydrogen lines
+class Stehle(ctypes.Structure):
+    """orc_stehle_t: one Stehle series (n_dens = 0: not loaded)."""
+    _fields_ = [("n_lower", ctypes.c_int32), ("n_upper_min", ctypes.c_int32), ("n_upper_max", ctypes.c_int32),
+                ("n_dens", ctypes.c_int32), ("density_grid", ctypes.c_double * 20), ("temp_grid", ctypes.c_double * 10),
+                ("log_dalpha_grid", ctypes.c_double * 60), ("max_dens_idx", ctypes.c_void_p),
+                ("k_alpha", ctypes.c_void_p), ("profiles", ctypes.c_void_p)]
+
+
+def stehle_structs(series):
+    """series: 4 dicts (or None) with n_lower, n_upper_min, n_upper_max, density_grid, temp_grid,
+    log_dalpha_grid, max_dens_idx, k_alpha, profiles [n_trans, n_dens, 10, 60].  Returns the ctypes
+    array and the arrays it points into (keep both alive)."""
+    arr, keep = (Stehle * 4)(), []
+    for i, s in enumerate(series):
+        if s is None:
+            continue
+        mdi = np.ascontiguousarray(s["max_dens_idx"], np.int32)
+        ka = np.ascontiguousarray(s["k_alpha"], np.float64)
+        pr = np.ascontiguousarray(s["profiles"], np.float64)
+        keep += [mdi, ka, pr]
+        a = arr[i]
+        a.n_lower, a.n_upper_min, a.n_upper_max = int(s["n_lower"]), int(s["n_upper_min"]), int(s["n_upper_max"])
+        a.n_dens = len(s["density_grid"])
+        a.density_grid[:a.n_dens] = [float(x) for x in s["density_grid"]]
+        a.temp_grid[:] = [float(x) for x in s["temp_grid"]]
+        a.log_dalpha_grid[:] = [float(x) for x in s["log_dalpha_grid"]]
+        a.max_dens_idx, a.k_alpha, a.profiles = mdi.ctypes.data, ka.ctypes.data, pr.ctypes.data
+    return arr, keep
+
+
+class _SHAtm(ctypes.Structure):
+    _fields_ = [("t", _dp), ("xnfph1", _dp), ("xnfph2", _dp), ("xnfhe1", _dp), ("xnfh2", _dp)]
+
+
+def synthe_hprof_kp(htab, n, m, xne, t, xnfph1, xnfph2, xnfhe1, xnfh2, dopph, delw):
+    """hydrogen_line_profile's K-P path at one depth (SYNTHE's tables in htab)."""
+    f = _lib2().orc_synthe_hprof_kp
+    f.restype = ctypes.c_double
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 8
+    return f(ctypes.byref(htab), n, m, xne, t, xnfph1, xnfph2, xnfhe1, xnfh2, dopph, delw)
+
+
+def synthe_hydrogen_opacity(recs, length, wbegin, ratio, wlend, velshift_kms, continuum, atm, htab, stehle=None):
+    """compute_line_opacity's hydrogen and deuterium lines in FP64: the contribution [nrhox, length].
+    atm: xnfdop, dopple [nrhox, nspec], xne, hckt, t, xnfph1, xnfph2, xnfhe1, xnfh2 [nrhox]; htab: HTab of
+    SYNTHE's tables; stehle: 4 series dicts (None entries: not loaded) or None for the K-P path."""
+    rec = np.ascontiguousarray(recs, NLTE_LINE)
+    cont = np.ascontiguousarray(continuum, np.float32)
+    xnfdop, dopple = _d(atm["xnfdop"]), _d(atm["dopple"])
+    nrhox, nspec = xnfdop.shape
+    hv = [_d(atm[k]) for k in ("t", "xnfph1", "xnfph2", "xnfhe1", "xnfh2")]
+    sa = _SHAtm(*[_ptr(v) for v in hv])
+    st, keep = (None, None) if stehle is None else stehle_structs(stehle)
+    out = np.zeros((nrhox, length))
+    f = _lib2().orc_synthe_hydrogen_opacity
+    f.restype = ctypes.c_int
+    rc = f(rec.ctypes.data_as(ctypes.c_void_p), ctypes.c_int64(rec.shape[0]), length, nrhox, ctypes.c_double(wbegin),
+           ctypes.c_double(ratio), ctypes.c_double(wlend), ctypes.c_double(velshift_kms),
+           cont.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), _ptr(xnfdop), _ptr(dopple), nspec,
+           _ptr(_d(atm["xne"])), _ptr(_d(atm["hckt"])), ctypes.byref(htab), st, ctypes.byref(sa), _ptr(out))
+    if rc != 0:
+        raise ValueError("hydrogen record NBLO/NBUP/NCON outside EHYD/ALPHAHYD/CONTH")
+    return out

@@ -16,6 +16,8 @@ modified).  Writes tests/golden/reference_tables.npz with:
   molcodes, isox SELECTLINES's diatomic species codes and isotopologue log gf
                  corrections in millidex (atlas12_modules.f90:19182-19202)
   tio_isocorr, h2o_isocorr   the TiO and H2O isotope corrections (:19204, :19207)
+  stehle_dims    the four Stehle Stark-profile files' dimensions (stehle_dims)
+  s_*            SYNTHE's hydrogen_line_profile tables, laid out like h_* (synthe_hydrogen_tables)
   h_*            the hydrogen line profile's tables (HPROF4, atlas12_modules.f90:20553-21002):
                  h_xknmtb XKNMTB(4,3) and h_y1wtm Y1WTM(2,2) as [n-1, m-n-1]; the fine
                  structure h_stalph, h_stwtal (34), h_istal, h_lnghal (4), h_stcomp,
@@ -73,9 +75,12 @@ def fortran_array(src, name, count):
 
 
 def fortran_int_array(src, name, count):
-    """INTEGER array constructor (/ ... /) following name, comments dropped."""
+    """INTEGER array constructor (/ ... /) or [ ... ] following name, comments dropped."""
     i = src.index(name)
-    body = src[src.index("(/", i) + 2:src.index("/)", i)]
+    if "(/" in src[i:i + 60]:
+        body = src[src.index("(/", i) + 2:src.index("/)", i)]
+    else:
+        body = src[src.index("[", i) + 1:src.index("]", i)]
     body = re.sub(r"!.*", "", body).replace("&", " ")
     vals = np.array([int(x) for x in re.findall(r"[-+]?\d+", body)], dtype=np.int32)
     assert vals.size == count, (name, vals.size)
@@ -105,6 +110,57 @@ def read_deck(path):
     rows = np.array([[float(x) for x in lines[i + 1 + j].split()[:7]] for j in range(n)])
     pradk = float(next(l for l in lines if l.startswith("PRADK")).split()[1])
     return rows, np.array([pradk])
+
+
+def synthe_hydrogen_tables(syn, mod):
+    """SYNTHE's own hydrogen_line_profile tables (synthe_module.f90:1047-1160),
+    stark_quasistatic_profile's (:776-869) and compute_line_opacity's EHYD
+    (:3299-3310), as s_* arrays laid out like the h_* ones.  They are REAL(4)
+    PARAMETERs, so each value is rounded to single precision.  Y1WHT's four
+    tabulated values are IF branches in the source (:1290-1299), at
+    [N-1, M-N-1]; EHYD(9..10) follow ELIM_HI - RYDBERG_H / N**2."""
+    hp = syn[syn.index("FUNCTION hydrogen_line_profile"):]
+    sq = syn[syn.index("FUNCTION stark_quasistatic_profile"):]
+    f32 = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)
+    const = lambda name: float(re.search(name + r"\s*=\s*([0-9.D+-]+)", mod).group(1).replace("D", "e"))
+    elim, rydh = const(r"ELIM_HI"), const(r"RYDBERG_H  ")
+    ehyd = [float(re.search(r"ehyd\(%d\) = ([0-9.D+-]+)" % k, syn).group(1).replace("D", "e")) for k in range(1, 9)]
+    ehyd += [elim - rydh / float(k) ** 2 for k in (9, 10)]
+    prob = np.stack([fortran_array(sq, "PROB%d(75) =" % k, 75).reshape(15, 5) for k in range(1, 8)])
+    return dict(
+        s_xknmtb=f32(fortran_array(hp, "XKNMTB(4,3) =", 12).reshape(4, 3, order="F")),
+        s_y1wtm=np.array([[1.0e18, 1.0e17], [1.0e16, 1.0e14]]),
+        s_stalph=f32(fortran_array(hp, "STALPH(34) =", 34)),
+        s_stwtal=f32(fortran_array(hp, "STWTAL(34) =", 34)),
+        s_istal=fortran_int_array(hp, "ISTAL(4) =", 4),
+        s_lnghal=fortran_int_array(hp, "LNGHAL(4) =", 4),
+        s_stcomp=f32(fortran_array(hp, "STCOMP(5,4) =", 20).reshape(5, 4, order="F")),
+        s_stcpwt=f32(fortran_array(hp, "STCPWT(5,4) =", 20).reshape(5, 4, order="F")),
+        s_lncomp=fortran_int_array(hp, "LNCOMP(4) =", 4),
+        s_cutoffh2plus=f32(fortran_array(hp, "CUTOFFH2PLUS(111) =", 111)),
+        s_cutoffh2=f32(fortran_array(hp, "CUTOFFH2(91) =", 91)),
+        s_asum=f32(fortran_array(hp, "ASUM(100) =", 100)),
+        s_asumlyman=f32(fortran_array(hp, "ASUMLYMAN(100) =", 100)),
+        s_betagrid=f32(fortran_array(sq, "BETA(15) =", 15)),
+        s_pp=f32(fortran_array(sq, "PP(5)   =", 5)),
+        s_propbm=f32(prob),
+        s_c=f32(fortran_array(sq, "CC(5,7) =", 35).reshape(5, 7, order="F").T),
+        s_d=f32(fortran_array(sq, "DD(5,7) =", 35).reshape(5, 7, order="F").T),
+        s_eh=np.array(ehyd),
+        s_elim=np.array([elim]),
+    )
+
+
+def stehle_dims(datadir):
+    """Per Stehle series (data/stehle_*.bin, read as INIT_STARK_TABLES does):
+    n_lower, n_upper_min, n_upper_max, n_dens, and the number of profile
+    values; the synthetic tables used by the tests have these shapes."""
+    sys.path.insert(0, os.path.join(HERE, "..", ".."))
+    from atlas12_b200 import linelists
+    rows = []
+    for s in linelists.read_stehle_dir(datadir):
+        rows.append([s["n_lower"], s["n_upper_min"], s["n_upper_max"], len(s["density_grid"]), s["profiles"].size])
+    return np.array(rows, dtype=np.int64)
 
 
 def main():
@@ -145,6 +201,8 @@ def main():
         h_elim=np.array([float(re.search(r"ELIM_HI = ([0-9.D+-]+)", mod).group(1).replace("D", "e"))]),
     )
     out["h_propbm"], out["h_c"], out["h_d"] = read_stark(os.path.join(ROOT, "data", "stark_profile.dat"))
+    out.update(synthe_hydrogen_tables(syn, mod))
+    out["stehle_dims"] = stehle_dims(os.path.join(ROOT, "data"))
     out["deck"], out["deck_pradk"] = read_deck(os.path.join(ROOT, "workdir", "ap00t5777g4.44at12.dat"))
     np.savez(os.path.join(HERE, "reference_tables.npz"), **out)
     for k, v in out.items():

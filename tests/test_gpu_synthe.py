@@ -225,6 +225,40 @@ def test_nlte_shore_and_merged_lines_match_fp64_oracle(po, gpu_ctx, tables, prep
     assert err.max() <= 1e-6, err.max()
 
 
+@pytest.mark.parametrize("stehle", [False, True], ids=["analytic", "stehle"])
+@pytest.mark.parametrize("window", ["balmer", "lyman"])
+def test_nlte_hydrogen_lines_match_fp64_oracle(po, gpu_ctx, tables, window, stehle):
+    """compute_line_opacity's hydrogen and deuterium lines: the Lyman series
+    (Lyman alpha with its H2 and H2+ satellites) over 92-130 nm and the Balmer
+    series over 380-700 nm in a 9500 K atmosphere, alpha, beta and the
+    tapered higher members, each deuterium line just before its hydrogen line
+    (which then reuses its Stark convolution), with the analytic profile or
+    Stehle-format tables.  Same tolerance as the other NLTE branches; without
+    the hydrogen inputs the records are skipped."""
+    from atlas12_b200 import surrogate as sg
+    lo, hi, res = (380.0, 700.0, 30000.0) if window == "balmer" else (92.0, 130.0, 20000.0)
+    g = po.synthe_grid(lo, hi, res)
+    length = g["length"]
+    wav = g["wbegin"] * g["ratio"] ** np.arange(length)
+    m = sg.grey_model(9500.0, 4.0)
+    ka, sgm = sg.continuum_opacity(wav, m["t"], m["p"], sg.populations(m["t"], m["p"], 2.0))
+    cont = np.ascontiguousarray((ka + sgm).T, np.float32)
+    atm = synthetic.hydrogen_atmosphere()
+    recs = synthetic.hydrogen_records(lo, hi, g["wbegin"], g["ratio"])
+    assert set(recs["itype"]) == {-1, -2} and len(recs) >= 14
+    st = synthetic.stehle_tables() if stehle else None
+    ref = po.synthe_hydrogen_opacity(recs, length, g["wbegin"], g["ratio"], hi, 0.0, cont, atm,
+                                     po.HTab.from_tables(tables, "s_"), st)
+    assert np.count_nonzero(ref) > 0.3 * ref.size
+    syn = S.Synthe(gpu_ctx, tables)
+    syn.set_hydrogen_tables(tables, st)
+    args = (recs, g, hi, cont, atm["xnfdop"], atm["dopple"], atm["xne"], atm["txnxn"], atm["hckt"],
+            np.zeros((17, 26)), np.zeros((atm["t"].size, length), np.float32))
+    got = syn.nlte_opacity(*args, hydrogen=atm)
+    assert _kappa_err(got, ref, cont) <= 1e-6
+    assert not np.any(syn.nlte_opacity(*args))
+
+
 def test_concurrent_spectra_match_one_at_a_time(gpu_ctx, tables):
     """Spectra of atmospheres with their own windows and line lists on four
     concurrent contexts equal those computed one at a time (flux to 1e-6:
