@@ -153,7 +153,11 @@ class Synthe:
 
     def run(self, case):
         """PROGRAM SYNTHE on a prepared case dict (see synthetic.synthe_case):
-        returns (wavelength_angstrom, flux, continuum_flux, opacity_matrix)."""
+        returns (wavelength_angstrom, flux, continuum_flux, opacity_matrix).
+        With case["nlte"] (NLTE_LINE records, nbuff the grid index) and
+        case["contx"] ([17, 26]) also the unit-19 lines, and with
+        case["xnfpel"] / case["hydrogen"] their Shore and merged-continuum /
+        hydrogen branches (set_hydrogen_tables first for the latter)."""
         grid = synthe_grid(case["wlbeg"], case["wlend"], case["resolu"])
         L = case["lines"]
         nb = self.bin_lines(L["wlvac"], grid)
@@ -162,6 +166,11 @@ class Synthe:
         cont = self.continuum(case["wledge"], case["continall"], grid)
         op = self.line_opacity(lines, grid, case["resolu"], cont, atm["xnfdop"], atm["dopple"], atm["xne"],
                                atm["txnxn"], atm["hckt"])
+        if case.get("nlte") is not None and len(case["nlte"]):
+            # unit-19 lines (compute_line_opacity, called per depth before the LTE loop at synthe.f90:554)
+            op = self.nlte_opacity(case["nlte"], grid, case["wlend"], cont, atm["xnfdop"], atm["dopple"], atm["xne"],
+                                   atm["txnxn"], atm["hckt"], case["contx"], op, xnfpel=case.get("xnfpel"),
+                                   hydrogen=case.get("hydrogen"))
         flux, cflux = self.spectrum(case["wledge"], case["contabs"], case["contscat"], atm["rhox"], atm["hkt"],
                                     grid, op)
         wave = grid["wbegin"] * grid["ratio"] ** np.arange(grid["length"]) * 10.0

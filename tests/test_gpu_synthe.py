@@ -259,6 +259,30 @@ def test_nlte_hydrogen_lines_match_fp64_oracle(po, gpu_ctx, tables, window, steh
     assert not np.any(syn.nlte_opacity(*args))
 
 
+def test_run_adds_the_unit19_lines(po, gpu_ctx, tables, small_case):
+    """PROGRAM SYNTHE with hydrogen records: the opacity matrix is the LTE
+    lines' plus compute_line_opacity's, and the Balmer line deepens the
+    spectrum against the run without them."""
+    case = dict(small_case)
+    g = po.synthe_grid(case["wlbeg"], case["wlend"], case["resolu"])
+    syn = S.Synthe(gpu_ctx, tables)
+    syn.set_hydrogen_tables(tables)
+    atm = case["atm"]
+    nr = atm["xne"].size
+    recs = synthetic.hydrogen_records(395.0, 415.0, g["wbegin"], g["ratio"], series=((2, 6, 7),))
+    hy = synthetic.hydrogen_atmosphere()
+    hyd = {k: hy[k][:nr] for k in ("t", "xnfph1", "xnfph2", "xnfhe1", "xnfh2")}
+    _, flux0, _, op0 = syn.run(case)
+    case.update(nlte=recs, contx=np.zeros((17, 26)), hydrogen=hyd)
+    _, flux1, _, op1 = syn.run(case)
+    cont = syn.continuum(case["wledge"], case["continall"], g)
+    alone = syn.nlte_opacity(recs, g, case["wlend"], cont, atm["xnfdop"], atm["dopple"], atm["xne"], atm["txnxn"],
+                             atm["hckt"], case["contx"], np.zeros_like(op0), hydrogen=hyd)
+    assert np.count_nonzero(alone) > 0.1 * alone.size  # H delta's blue wing over the deeper layers
+    np.testing.assert_allclose(op1, op0 + alone, rtol=1e-6)
+    assert np.all(flux1 <= flux0 * (1 + 1e-6)) and np.mean(flux1) < np.mean(flux0)
+
+
 def test_concurrent_spectra_match_one_at_a_time(gpu_ctx, tables):
     """Spectra of atmospheres with their own windows and line lists on four
     concurrent contexts equal those computed one at a time (flux to 1e-6:
