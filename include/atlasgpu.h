@@ -171,6 +171,8 @@ typedef struct atlasgpu_synthe_hydrogen {
   const double *t, *xnfph1, *xnfph2, *xnfhe1, *xnfh2;
 } atlasgpu_synthe_hydrogen;
 
+struct atlasgpu_hydrogen_tables; /* defined with XLINOP's entry points below */
+
 /* Keeps SYNTHE's hydrogen_line_profile tables (its own values, in the layout
  * of atlasgpu_hydrogen_tables; eh = EHYD(1..10), elim = ELIM_HI) and the four
  * Stehle series (NULL: none loaded, the analytic profile throughout) on the

@@ -27,6 +27,31 @@ def test_library_exports_declared_symbols():
     assert not unbound, unbound
 
 
+def test_header_compiles_as_c_and_cxx(tmp_path):
+    """include/atlasgpu.h is plain C: it compiles warning-free as C11 and C++17,
+    and the structs a caller fills have the sizes the ctypes binding uses."""
+    import ctypes
+    import shutil
+    import subprocess
+    from atlas12_b200 import _lib
+    src = tmp_path / "use.c"
+    src.write_text('#include <stdio.h>\n#include "atlasgpu.h"\n'
+                   "int main(void) {\n"
+                   '  printf("%zu %zu %zu %zu\\n", sizeof(atlasgpu_hydrogen_tables), sizeof(atlasgpu_stehle_series),\n'
+                   "         sizeof(atlasgpu_synthe_hydrogen), sizeof(atlasgpu_nlte_line));\n"
+                   "  return 0;\n}\n")
+    inc = "-I" + os.path.join(ROOT, "include")
+    for cc, std in (("gcc", "-std=c11"), ("g++", "-std=c++17")):
+        if shutil.which(cc) is None:
+            continue
+        exe = tmp_path / ("use_" + cc.replace("+", "x"))
+        lang = ["-x", "c++"] if cc == "g++" else []
+        subprocess.run([cc, std, "-Wall", "-Wextra", "-Werror", inc] + lang + [str(src), "-o", str(exe)], check=True)
+        sizes = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+        assert sizes == [ctypes.sizeof(_lib.HydrogenTables), ctypes.sizeof(_lib.StehleSeries),
+                         ctypes.sizeof(_lib.SyntheHydrogen), _lib.NLTE_LINE.itemsize]
+
+
 def test_grid_is_host_only():
     from atlas12_b200 import synthe
     g = synthe.synthe_grid(400.0, 410.0, 500000.0)
