@@ -272,3 +272,143 @@ def test_synthe_analytic_profile_matches_plain_loops(po, tables, n, m):
             a = po.synthe_hprof_kp(h, n, m, *st, float(dw))
             b = py_synthe_kp(tables, n, m, *st, float(dw))
             assert a == b, (n, m, dw, a, b)
+
+
+def py_synthe_hydrogen_walk(po, h, recs, length, wbegin, ratio, wlend, cont, atm):
+    """compute_line_opacity's TYPE -1/-2 walks (synthe_module.f90:3460-3606)
+    in plain Python with the oracle's analytic profile point function."""
+    import math
+    rydh, cutoff = 109677.583403, 1.0e-3
+    conth = [109678.764, 27419.659, 12186.462, 6854.871, 4387.113, 3046.604, 2238.320, 1713.713, 1354.044,
+             1096.776, 906.426, 761.650, 648.980, 559.579, 487.456]
+    eh = [h.eh[k] for k in range(10)] + [h.elim - rydh / (float(k) * float(k)) for k in range(11, 101)]
+    alphahyd = [1.0e7 / (eh[k + 1] - eh[k]) for k in range(99)]
+    nrhox = atm["xne"].size
+    out = np.zeros((nrhox, length))
+    from test_oracle_branches import atlas_powi
+    for j in range(nrhox):
+        inglis = np.float32(1600.0 / math.pow(atm["xne"][j], float(np.float32(2.0) / np.float32(15.0))))
+        nmerge = np.float32(inglis - np.float32(1.5))
+        emergeh = rydh / (float(nmerge) * float(nmerge))
+        c = cont[j].astype(np.float64)
+        for r in recs:
+            n, m, ncon, nbuff = int(r["nblo"]), int(r["nbup"]), int(r["ncon"]), int(r["nbuff"])
+            wl = float(r["wlvac"])
+            kappa0 = float(r["gf"]) * atm["xnfdop"][j, 0]
+            kapmin = c[(length if m == 2 else min(max(nbuff, 1), length)) - 1] * cutoff
+            if kappa0 < kapmin:
+                continue
+            dopph = np.float32(atm["dopple"][j, 0])
+            if r["itype"] == -2:
+                dopph = np.float32(dopph / np.float32(1.4142))
+            kappa0 = kappa0 * math.exp(-float(r["elo"]) * atm["hckt"][j])
+            if kappa0 < kapmin:
+                continue
+
+            def K(wave):
+                return kappa0 * po.synthe_hprof_kp(h, n, m, atm["xne"][j], atm["t"][j], atm["xnfph1"][j],
+                                                   atm["xnfph2"][j], atm["xnfhe1"][j], atm["xnfh2"][j], float(dopph),
+                                                   wave - wl)
+            minred = max(1, nbuff)
+            general = not (ncon == 0 or m == n + 1) and m != n + 2
+            wcon = wtail = 0.0
+            blue = True
+            if ncon == 0 or m == n + 1:
+                if wl <= wlend:
+                    wave = wbegin * atlas_powi(ratio, minred - 1)
+                    for ib in range(minred, length + 1):
+                        k = K(wave)
+                        out[j, ib - 1] += k
+                        if k < c[ib - 1] * cutoff:
+                            break
+                        wave = wave * ratio
+                    blue = not (minred == 1 or wl < wbegin)
+            elif m == n + 2:
+                if wl <= wlend:
+                    wave = wbegin * atlas_powi(ratio, minred - 1)
+                    exited = False
+                    for ib in range(minred, length + 1):
+                        if wave > alphahyd[n - 1]:
+                            exited = True
+                            break
+                        k = K(wave)
+                        out[j, ib - 1] += k
+                        if k < c[ib - 1] * cutoff:
+                            exited = True
+                            break
+                        wave = wave * ratio
+                    if not exited and (minred == 1 or wl < wbegin or nbuff < 1):
+                        blue = False
+                elif nbuff < 1:
+                    blue = False
+            else:
+                wshift = 1.0e7 / (conth[ncon - 1] - rydh / (81.0 * 81.0))
+                wmerge = 1.0e7 / (conth[ncon - 1] - emergeh)
+                if wmerge < 0.0:
+                    wmerge = wshift + wshift
+                wcon = max(wshift, wmerge)
+                wtail = 1.0e7 / (1.0e7 / wcon - 500.0)
+                wcon = min(wshift + wshift, wcon)
+                if wtail < 0.0:
+                    wtail = wcon + wcon
+                wtail = min(wcon + wcon, wtail)
+                if wl <= wlend:
+                    if wcon > wlend:
+                        continue
+                    if wbegin <= alphahyd[n - 1]:
+                        wave = wbegin * atlas_powi(ratio, minred - 1)
+                        if wave >= wcon:
+                            k = K(wave)
+                            if k >= c[min(minred, length) - 1] * cutoff:
+                                if wave < wtail:
+                                    k = k * ((wave - wcon) / (wtail - wcon))
+                                if minred <= length:
+                                    out[j, minred - 1] += k
+                                wave = wave * ratio
+                                for ib in range(minred + 1, length + 1):
+                                    if wave >= wcon:
+                                        k = K(wave)
+                                        if wave < wtail:
+                                            k = k * ((wave - wcon) / (wtail - wcon))
+                                        out[j, ib - 1] += k
+                                        if k < c[ib - 1] * cutoff:
+                                            break
+                                    wave = wave * ratio
+                        if minred == 1:
+                            continue
+                    if wl < wbegin:
+                        continue
+            if not blue:
+                continue
+            ib = min(length + 1, nbuff)
+            wave = wbegin * atlas_powi(ratio, ib - 1)
+            for _ in range(ib - 1):
+                ib -= 1
+                wave = wave / ratio
+                if general and wave < wcon:
+                    break
+                k = K(wave)
+                if general and wave < wtail:
+                    k = k * ((wave - wcon) / (wtail - wcon))
+                out[j, ib - 1] += k
+                if k < c[ib - 1] * cutoff:
+                    break
+    return out
+
+
+def test_synthe_hydrogen_walks_match_plain_loops(po, tables):
+    """The oracle's alpha, beta and tapered walks (the analytic profile)
+    against plain loops, bit for bit: Balmer lines with deuterium partners on
+    a window cut through the series limit and H alpha's red wing."""
+    g = po.synthe_grid(362.0, 420.0, 8000.0)
+    atm = synthetic.hydrogen_atmosphere()
+    atm = {k: (v[::6] if np.ndim(v) else v) for k, v in atm.items()}
+    nr = atm["xne"].size
+    rng = np.random.default_rng(4)
+    cont = (10.0 ** rng.uniform(-1.0, 0.5, (nr, g["length"]))).astype(np.float32)
+    recs = synthetic.hydrogen_records(300.0, 700.0, g["wbegin"], g["ratio"], series=((2, 3, 14),))
+    h = po.HTab.from_tables(tables, "s_")
+    got = po.synthe_hydrogen_opacity(recs, g["length"], g["wbegin"], g["ratio"], 420.0, 0.0, cont, atm, h)
+    want = py_synthe_hydrogen_walk(po, h, recs, g["length"], g["wbegin"], g["ratio"], 420.0, cont, atm)
+    assert np.count_nonzero(want) > 0.2 * want.size
+    np.testing.assert_array_equal(got, want)
