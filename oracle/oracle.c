@@ -2656,6 +2656,22 @@ static double orc_shprof(const orc_htab_t *h, const orc_stehle_t *st, orc_sconv_
   return result;
 }
 
+double orc_synthe_hprof_stehle(const orc_htab_t *h, const orc_stehle_t *stehle, int n, int m, double xne,
+                               double t, double xnfph1, double xnfph2, double xnfhe1, double xnfh2,
+                               double dopph_conv, double dopph, double delw) {
+  orc_shline_t L;
+  orc_shdepth_t d;
+  orc_sconv_t cv;
+  orc_shline(h, n, m, &L);
+  orc_shdepth(xne, t, xnfph1, xnfph2, xnfhe1, xnfh2, &d);
+  const orc_stehle_t *st = stehle;
+  cv.valid = 0;
+  cv.n = cv.m = cv.last_n = cv.last_m = 0;
+  if (!s_use_stehle(st, n, m, xne)) return orc_shprof_kp(h, &L, &d, dopph, delw);
+  orc_shprof(h, st, &cv, &L, &d, dopph_conv, delw); /* builds the convolution */
+  return orc_shprof(h, st, &cv, &L, &d, dopph, delw);
+}
+
 int orc_synthe_hydrogen_opacity(const orc_nlte_line_t *recs, int64_t n, int length, int nrhox,
                                 double wbegin, double ratio, double wlend, double velshift_kms,
                                 const float *continuum, const double *xnfdop, const double *dopple,

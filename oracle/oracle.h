@@ -311,6 +311,13 @@ typedef struct {
  * tables); dopph is DOPPH(J).  For tests of the profile alone. */
 double orc_synthe_hprof_kp(const orc_htab_t *h, int n, int m, double xne, double t, double xnfph1,
                            double xnfph2, double xnfhe1, double xnfh2, double dopph, double delw);
+/* hydrogen_line_profile(N, M, J, DELW) on the Stehle path at one depth: the
+ * convolution built with Doppler width dopph_conv (the line that built it),
+ * evaluated with dopph (this line's); stehle [4].  For tests of the profile
+ * alone. */
+double orc_synthe_hprof_stehle(const orc_htab_t *h, const orc_stehle_t *stehle, int n, int m, double xne,
+                               double t, double xnfph1, double xnfph2, double xnfhe1, double xnfh2,
+                               double dopph_conv, double dopph, double delw);
 /* Adds the TYPE -1/-2 records' opacity at every depth into out
  * [nrhox][length] (double), the other records skipped; stehle [4] (Lyman,
  * Balmer, Paschen, Brackett) or NULL for the K-P path throughout; tab holds

@@ -625,6 +625,16 @@ def synthe_hprof_kp(htab, n, m, xne, t, xnfph1, xnfph2, xnfhe1, xnfh2, dopph, de
     return f(ctypes.byref(htab), n, m, xne, t, xnfph1, xnfph2, xnfhe1, xnfh2, dopph, delw)
 
 
+def synthe_hprof_stehle(htab, stehle, n, m, xne, t, xnfph1, xnfph2, xnfhe1, xnfh2, dopph_conv, dopph, delw):
+    """hydrogen_line_profile on the Stehle path at one depth (the analytic one where no series covers the
+    line): the convolution built with dopph_conv, evaluated with dopph.  stehle: 4 series dicts."""
+    st, keep = stehle_structs(stehle)
+    f = _lib2().orc_synthe_hprof_stehle
+    f.restype = ctypes.c_double
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 9
+    return f(ctypes.byref(htab), st, n, m, xne, t, xnfph1, xnfph2, xnfhe1, xnfh2, dopph_conv, dopph, delw)
+
+
 def synthe_hydrogen_opacity(recs, length, wbegin, ratio, wlend, velshift_kms, continuum, atm, htab, stehle=None):
     """compute_line_opacity's hydrogen and deuterium lines in FP64: the contribution [nrhox, length].
     atm: xnfdop, dopple [nrhox, nspec], xne, hckt, t, xnfph1, xnfph2, xnfhe1, xnfh2 [nrhox]; htab: HTab of

@@ -412,3 +412,128 @@ def test_synthe_hydrogen_walks_match_plain_loops(po, tables):
     want = py_synthe_hydrogen_walk(po, h, recs, g["length"], g["wbegin"], g["ratio"], 420.0, cont, atm)
     assert np.count_nonzero(want) > 0.2 * want.size
     np.testing.assert_array_equal(got, want)
+
+
+def py_synthe_stehle(po, h, stl, n, m, xne, t, xnfph1, xnfph2, xnfhe1, xnfh2, dconv, dopph, delw):
+    """hydrogen_line_profile's Stehle path (synthe_module.f90:1414-1696, with
+    interp_stark_at :2007-2037) in plain Python: the table bilinear in
+    (log Ne, T), the Stark (x) Voigt convolution on its two-zone grid built
+    with Doppler width dconv, then the log-log evaluation with dopph.  The
+    Voigt kernel is the oracle's (pinned on its own)."""
+    import math
+    from test_oracle_branches import py_hfnm
+    rydh, cang, pi, sqrtpi = 109677.583403, 2.99792458e18, 3.141592653589793, 1.7724538509055159
+    S = stl[n - 1]
+    xn, xm = float(n), float(m)
+    xn2, xm2 = xn * xn, xm * xm
+    gnm = (xm2 - xn2) / (xm2 * xn2)
+    freqnm = rydh * 2.99792458e10 * gnm
+    wavenm = cang / freqnm
+    radamp = (h["s_asumlyman"][m - 1] if n == 1 else h["s_asum"][n - 1] + h["s_asum"][m - 1]) / (4.0 * pi) / freqnm
+    resont = py_hfnm(1, m) / xm / (1.0 - 1.0 / xm2)
+    if n != 1:
+        resont = resont + py_hfnm(1, n) / xn / (1.0 - 1.0 / xn2)
+    resont = resont * 3.579e-24 / gnm
+    vdw = 4.45e-26 / gnm * math.pow(xm2 * (7.0 * xm2 + 5.0), 0.4)
+    t43 = math.pow(t / 10000.0, 0.3)
+    hwvdw = vdw * (t43 * xnfhe1) + 2.0 * vdw * (t43 * xnfh2)
+    hwres = resont * xnfph1 * 2.0
+    hwlor_conv = hwres * 4.0 + hwvdw + radamp if (n == 1 and m == 2) else hwres + hwvdw + radamp
+    lam0 = 1.0e8 / rydh * ((xn * xm) * (xn * xm)) / ((xm - xn) * (xm + xn))
+    itr = m - S["n_upper_min"] + 1
+    dg, tg, lg = S["density_grid"], S["temp_grid"], S["log_dalpha_grid"]
+    nd = len(dg)
+    dcap = dg[S["max_dens_idx"][itr - 1] - 1]
+    ne = xne if xne < dcap else dcap
+    F0 = 1.25e-9 * math.pow(ne, 2.0 / 3.0)
+    dag = [math.pow(10.0, x) for x in lg]
+    id1 = next((i for i in range(1, nd) if ne <= dg[i]), nd)
+    id1 = max(1, min(nd - 1, id1))
+    fd = (math.log10(ne) - math.log10(dg[id1 - 1])) / (math.log10(dg[id1]) - math.log10(dg[id1 - 1]))
+    fd = min(max(fd, 0.0), 1.0)
+    it1 = min(next((i for i in range(1, 10) if t <= tg[i]), 10), 9)
+    ft = min(max((t - tg[it1 - 1]) / (tg[it1] - tg[it1 - 1]), 0.0), 1.0)
+    P = S["profiles"][itr - 1]
+    sp = []
+    for ia in range(60):
+        v00, v01, v10, v11 = P[id1 - 1, it1 - 1, ia], P[id1 - 1, it1, ia], P[id1, it1 - 1, ia], P[id1, it1, ia]
+        if v00 > 0 and v01 > 0 and v10 > 0 and v11 > 0:
+            sp.append(math.exp(math.log(v00) * (1 - fd) * (1 - ft) + math.log(v01) * (1 - fd) * ft +
+                               math.log(v10) * fd * (1 - ft) + math.log(v11) * fd * ft))
+        else:
+            sp.append(v00 * (1 - fd) * (1 - ft) + v01 * (1 - fd) * ft + v10 * fd * (1 - ft) + v11 * fd * ft)
+
+    def interp(da):
+        if da >= math.pow(10.0, lg[59]):
+            return sp[59]
+        x = math.log10(da)
+        i = min(next((k for k in range(1, 60) if x <= lg[k]), 60), 59)
+        fr = (x - lg[i - 1]) / (lg[i] - lg[i - 1])
+        if sp[i - 1] > 0.0 and sp[i] > 0.0:
+            return math.exp(math.log(sp[i - 1]) * (1.0 - fr) + math.log(sp[i]) * fr)
+        return sp[i - 1] * (1.0 - fr) + sp[i] * fr
+    dopd = lam0 * lam0 / cang * freqnm * dconv / F0
+    lord = lam0 * lam0 / cang * freqnm * hwlor_conv / F0
+    va = float(np.float32(lord / dopd))
+    dx = dopd / 3.0
+    dlog = (lg[59] - lg[0]) / 59.0
+    nlog = max(next((ia - 1 for ia in range(1, 61) if dag[ia - 1] * dlog * math.log(10.0) > dx), 60), 1)
+    dtr = dag[nlog - 1]
+    nw, dwm = 200, dtr + 200.0 * dx
+    if dwm > dag[59]:
+        dwm = dag[59]
+        nw = max(int((dwm - dtr) / dx), 0)
+    if 2 * nw + 2 * nlog + 1 > 600:
+        nw = (600 - 2 * nlog - 1) // 2
+        dwm = dtr + float(nw) * dx
+    grid = [(-(dtr + float(iw) * dx), interp(dtr + float(iw) * dx)) for iw in range(nw, 0, -1)]
+    grid += [(-dag[ia - 1], sp[ia - 1]) for ia in range(nlog, 0, -1)] + [(0.0, sp[0])]
+    grid += [(dag[ia - 1], sp[ia - 1]) for ia in range(1, nlog + 1)]
+    grid += [(dtr + float(iw) * dx, interp(dtr + float(iw) * dx)) for iw in range(1, nw + 1)]
+    cda = [g[0] for g in grid]
+    ic = len(cda)
+    cst = [cda[1] - cda[0]] + [0.5 * (cda[k + 1] - cda[k - 1]) for k in range(1, ic - 1)] + [cda[-1] - cda[-2]]
+    prof = []
+    for ia in range(60):
+        da = dag[ia]
+        if da > dwm and dwm > 0.0:
+            prof.append(sp[ia] + va * dopd / (pi * (da * da)))
+        else:
+            s = 0.0
+            for (x, pv), w in zip(grid, cst):
+                kern = float(np.float32(po.voigt_weideman(float(np.float32((da - x) / dopd)), va)))
+                s = s + pv * kern * w
+            prof.append(s / (dopd * sqrtpi))
+    freq = cang / (wavenm + delw * 10.0)
+    dac = lam0 * lam0 / cang * abs(freq - freqnm) / F0
+    if dac <= math.pow(10.0, lg[0]):
+        I = prof[0]
+    elif dac >= math.pow(10.0, lg[59]):
+        I = S["k_alpha"][m - S["n_upper_min"]] / math.pow(dac, 2.5) + va * dopd / (pi * (dac * dac))
+    else:
+        x = math.log10(dac)
+        i = min(next((k for k in range(1, 60) if x <= lg[k]), 60), 59)
+        fa = (x - lg[i - 1]) / (lg[i] - lg[i - 1])
+        p1, p2 = prof[i - 1], prof[i]
+        I = math.exp(math.log(p1) * (1.0 - fa) + math.log(p2) * fa) if (p1 > 0.0 and p2 > 0.0) else \
+            p1 * (1.0 - fa) + p2 * fa
+    return I * (lam0 * lam0) / (cang * F0) * sqrtpi * (freqnm * dopph)
+
+
+@pytest.mark.parametrize("n,m", [(2, 3), (2, 7), (3, 5), (4, 6)])
+def test_synthe_stehle_profile_matches_plain_loops(po, tables, n, m):
+    """The oracle's Stehle path (tables, convolution grid, Voigt kernel sums,
+    log-log evaluation) against the plain-Python restatement, bit for bit,
+    with the convolution built from another line's Doppler width."""
+    h = po.HTab.from_tables(tables, "s_")
+    stl = synthetic.stehle_tables()
+    rng = np.random.default_rng(10 * n + m)
+    for _ in range(3):
+        xne = 10.0 ** rng.uniform(10.5, 15.5)
+        st = (xne, rng.uniform(4000.0, 30000.0), 10.0 ** rng.uniform(12.0, 17.0), 10.0 ** rng.uniform(10.0, 15.0),
+              10.0 ** rng.uniform(11.0, 16.0), 10.0 ** rng.uniform(0.0, 12.0))
+        dconv, dop = float(np.float32(rng.uniform(1e-5, 5e-5))), float(np.float32(rng.uniform(1e-5, 5e-5)))
+        for dw in (0.0, 1e-4, 3e-3, 0.05, 0.4, 2.0, 12.0, -0.02, -1.5):
+            a = po.synthe_hprof_stehle(h, stl, n, m, *st, dconv, dop, dw)
+            b = py_synthe_stehle(po, tables, stl, n, m, *st, dconv, dop, dw)
+            assert a == b, (n, m, dw, a, b)
