@@ -537,3 +537,20 @@ def test_synthe_stehle_profile_matches_plain_loops(po, tables, n, m):
             a = po.synthe_hprof_stehle(h, stl, n, m, *st, dconv, dop, dw)
             b = py_synthe_stehle(po, tables, stl, n, m, *st, dconv, dop, dw)
             assert a == b, (n, m, dw, a, b)
+
+
+def test_hydrogen_records_follow_the_rydberg_series(po):
+    """The synthetic unit-19 hydrogen records: Rydberg wavelengths, deuterium
+    just blueward, NCON set past beta, grid indices that bracket WLVAC."""
+    g = po.synthe_grid(90.0, 2000.0, 5000.0)
+    recs = synthetic.hydrogen_records(90.0, 2000.0, g["wbegin"], g["ratio"])
+    h = recs[recs["itype"] == -1]
+    n, m = h["nblo"].astype(float), h["nbup"].astype(float)
+    np.testing.assert_allclose(h["wlvac"], 1e7 / (109677.583403 * (1 / n ** 2 - 1 / m ** 2)), rtol=1e-12)
+    assert np.all(np.diff(recs["wlvac"]) >= 0)
+    assert np.all((recs["ncon"] > 0) == (recs["nbup"] > recs["nblo"] + 2))
+    d = recs[recs["itype"] == -2]
+    assert len(d) == len(h) and np.all(d["gf"] < 1e-3 * np.max(h["gf"]))
+    lo = g["wbegin"] * g["ratio"] ** (recs["nbuff"].astype(float) - 1.5)
+    hi = g["wbegin"] * g["ratio"] ** (recs["nbuff"].astype(float) - 0.5)
+    assert np.all((lo <= recs["wlvac"] * (1 + 1e-12)) & (recs["wlvac"] <= hi * (1 + 1e-12)))
