@@ -19,8 +19,13 @@ from . import synthe as S
 
 
 class SyntheBatch:
-    def __init__(self, device, operators, lanes=8, precision=_lib.PREC_MIXED):
+    def __init__(self, device, operators, lanes=8, precision=_lib.PREC_MIXED, hydrogen_tables=None, stehle=None):
+        """hydrogen_tables (the s_* arrays) and stehle (read_stehle_dir's list)
+        go to every lane, for cases that carry unit-19 hydrogen records."""
         self.lanes = [S.Synthe(_lib.Context(device, precision), operators) for _ in range(max(1, int(lanes)))]
+        if hydrogen_tables is not None:
+            for syn in self.lanes:
+                syn.set_hydrogen_tables(hydrogen_tables, stehle)
 
     def run(self, cases, keep_opacity=False):
         """Spectra of every case (synthetic.synthe_case dicts), in order."""
