@@ -92,6 +92,7 @@ SIGNATURES = {
     "atlasgpu_model_create": (_I, [_P, ctypes.c_void_p, ctypes.POINTER(_P)]),
     "atlasgpu_model_iterate": (_I, [_P, _P, _I, _D, _I, ctypes.POINTER(_I), _P]),
     "atlasgpu_model_get": (_I, [_P, _P, _P, _P, _P, _P, _P, _P]),
+    "atlasgpu_model_get_tables": (_I, [_P, _P, _P, _P, _P, _P]),
     "atlasgpu_model_set_structure": (_I, [_P, _P, _P, _P, _P]),
     "atlasgpu_model_destroy": (_I, [_P, _P]),
     "atlasgpu_model_set_params": (_I, [_P, _P, _D, _D, _D, _D]),

@@ -232,6 +232,16 @@ class AtlasModel:
         out["hsurf"] = hs
         return out
 
+    def tables(self):
+        """The last iteration's TABCONT [nwave+1, nrhox], XLINES, ACONT and
+        SIGMAC [numnu, nrhox] (KAPCONT's cutoff table, LINOP1's output and
+        the RT pass's continuum)."""
+        kw, nn = self.nrhox, self.waveset.size
+        tc = np.zeros((self.cutwave.size + 1, kw))
+        xl, ac, sg = np.zeros((nn, kw)), np.zeros((nn, kw)), np.zeros((nn, kw))
+        self.ctx.call("atlasgpu_model_get_tables", self._h, ptr(tc), ptr(xl), ptr(ac), ptr(sg))
+        return dict(tabcont=tc, xlines=xl, acont=ac, sigmac=sg)
+
     def set_params(self, teff, logg, vturb, mh=0.0):
         """New stellar parameters on the same line list and grid; follow with set_structure."""
         self.teff = teff

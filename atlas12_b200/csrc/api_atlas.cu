@@ -36,56 +36,104 @@ constexpr int kTabN = 2001;
 
 }  // namespace
 
+namespace {
+
+// the flagged LINEDATA records and their device-prepared lines, gathered
+// into compact arrays
+__global__ void k_prep_gather(const int4* __restrict__ ld, const AtlasLine* __restrict__ lines,
+                              const int64_t* __restrict__ idx, int64_t n, int4* __restrict__ rec,
+                              AtlasLine* __restrict__ fix) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    rec[k] = ld[idx[k]];
+    fix[k] = lines[idx[k]];
+  }
+}
+
+// the host-recomputed lines back to their places
+__global__ void k_prep_scatter(const AtlasLine* __restrict__ fix, const int64_t* __restrict__ idx, int64_t n,
+                               AtlasLine* __restrict__ lines) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    lines[idx[k]] = fix[k];
+}
+
+}  // namespace
+
 namespace atlasgpu {
-// Line preparation with the host fix of near-tie frequency brackets.
+// Line preparation (k_atlas_prep) with the host fix of near-tie frequency
+// brackets: a line whose device wavelength lies within a few ulps of a grid
+// point is recomputed with the C library's exp and pow, the functions the
+// reference's EXP and ** call.  The flagged records are gathered on the
+// device and crossed in one copy each way; when more lines are flagged than
+// the flag buffer holds, the buffer grows to the count and the pass runs
+// again.
 int atlas_prep_lines(atlasgpu_ctx* ctx, const int32_t* d_ld, const int32_t* h_ld, int64_t n,
-               const double* d_tablog, const double* d_ws, const double* h_ws, int numnu,
-               const int32_t* d_iwt, int nwave, int nspec, AtlasLine* d_lines) {
+                     const double* d_tablog, const double* d_ws, const double* h_ws, int numnu,
+                     const int32_t* d_iwt, int nwave, int nspec, AtlasLine* d_lines) {
+  (void)h_ld;
   unsigned long long* d_nf;
-  int64_t* d_fl;
-  const int64_t cap = 1 << 16;
   int r;
-  if ((r = bufT(ctx, "ap_nflag", 1, &d_nf)) || (r = bufT(ctx, "ap_flag", cap, &d_fl))) return r;
-  CK(cudaMemsetAsync(d_nf, 0, sizeof(unsigned long long), ctx->stream));
-  AtlasPrepArgs a{d_ld, n, d_tablog, d_ws, numnu, d_iwt, nwave, nspec, d_lines, d_fl, d_nf, cap};
-  {
-    Timer tm(ctx, "atlas_prep");
-    k_atlas_prep<<<grid_for(ctx, n, 256, 16), 256, 0, ctx->stream>>>(a);
-    CKL(ctx);
-  }
+  if ((r = bufT(ctx, "ap_nflag", 1, &d_nf))) return r;
+  int64_t cap = 1 << 12;
   unsigned long long nf = 0;
-  CK(cudaMemcpyAsync(&nf, d_nf, sizeof nf, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  if ((int64_t)nf > cap) return fail(ctx, ATLASGPU_EINVAL, "prep: %llu near-tie lines", nf);
-  if (nf) {
-    std::vector<int64_t> fl(nf);
-    CK(cudaMemcpy(fl.data(), d_fl, nf * sizeof(int64_t), cudaMemcpyDeviceToHost));
-    const double RATIOLG = log(1.0 + 1.0 / 2000000.0);
-    for (unsigned long long k = 0; k < nf; ++k) {
-      const int64_t i = fl[k];
-      int32_t rec[4];
-      if (h_ld) memcpy(rec, h_ld + 4 * i, sizeof rec);
-      else CK(cudaMemcpy(rec, d_ld + 4 * i, sizeof rec, cudaMemcpyDeviceToHost));
-      AtlasLine L;
-      CK(cudaMemcpy(&L, d_lines + i, sizeof L, cudaMemcpyDeviceToHost));
-      const double wl = exp(rec[0] * RATIOLG);  // the reference's EXP
-      int nu = 1;
-      while (nu < numnu && wl >= h_ws[nu - 1]) ++nu;
-      auto tablog = [](int32_t word, int hi) {
-        const int16_t v = (int16_t)(hi ? ((uint32_t)word >> 16) : (word & 0xffff));
-        return pow(10.0, (double)((int)v - 16384) * 0.001);
-      };
-      const double CEN_PREFAC4 = 0.026538 / kSqrtPi / kClightNms;
-      const double FOURPI_C_INV = 1.0 / (4.0 * kPi * kClightNms);
-      L.cgf = CEN_PREFAC4 * wl * tablog(rec[2], 0);
-      L.gr = tablog(rec[2], 1) * wl * FOURPI_C_INV;
-      L.gs = tablog(rec[3], 0) * wl * FOURPI_C_INV;
-      L.gw = tablog(rec[3], 1) * wl * FOURPI_C_INV;
-      L.wlvac = wl;
-      L.nu = nu;
-      CK(cudaMemcpy(d_lines + i, &L, sizeof L, cudaMemcpyHostToDevice));
+  int64_t* d_fl = nullptr;
+  for (int pass = 0; pass < 2; ++pass) {
+    if ((r = bufT(ctx, "ap_flag", cap, &d_fl))) return r;
+    CK(cudaMemsetAsync(d_nf, 0, sizeof(unsigned long long), ctx->stream));
+    AtlasPrepArgs a{d_ld, n, d_tablog, d_ws, numnu, d_iwt, nwave, nspec, d_lines, d_fl, d_nf, cap};
+    {
+      Timer tm(ctx, "atlas_prep");
+      k_atlas_prep<<<grid_for(ctx, n, 256, 16), 256, 0, ctx->stream>>>(a);
+      CKL(ctx);
     }
+    CK(cudaMemcpyAsync(&nf, d_nf, sizeof nf, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if ((int64_t)nf <= cap) break;
+    cap = (int64_t)nf;  // every flag fits on the second pass
   }
+  if (nf == 0) return 0;
+  int4* d_rec;
+  AtlasLine* d_fix;
+  if ((r = bufT(ctx, "ap_rec", nf, &d_rec)) || (r = bufT(ctx, "ap_fix", nf, &d_fix))) return r;
+  const int g = grid_for(ctx, (int64_t)nf, 256, 4);
+  k_prep_gather<<<g, 256, 0, ctx->stream>>>(reinterpret_cast<const int4*>(d_ld), d_lines, d_fl, (int64_t)nf,
+                                            d_rec, d_fix);
+  CKL(ctx);
+  std::vector<int4> rec(nf);
+  std::vector<AtlasLine> fix(nf);
+  CK(cudaMemcpyAsync(rec.data(), d_rec, nf * sizeof(int4), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(fix.data(), d_fix, nf * sizeof(AtlasLine), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const double RATIOLG = log(1.0 + 1.0 / 2000000.0);
+  const double CEN_PREFAC4 = 0.026538 / kSqrtPi / kClightNms;
+  const double FOURPI_C_INV = 1.0 / (4.0 * kPi * kClightNms);
+  auto tablog = [](int32_t word, int hi) {
+    const int16_t v = (int16_t)(hi ? ((uint32_t)word >> 16) : (word & 0xffff));
+    return pow(10.0, (double)((int)v - 16384) * 0.001);
+  };
+  for (unsigned long long k = 0; k < nf; ++k) {
+    const int32_t r0 = rec[k].x, r2 = rec[k].z, r3 = rec[k].w;
+    const double wl = exp(r0 * RATIOLG);  // the reference's EXP
+    // NU = first grid point with WLVAC < WAVESET(NU), clamped at NUMNU
+    int lo = 1, hi = numnu;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (wl < h_ws[mid - 1]) hi = mid;
+      else lo = mid + 1;
+    }
+    AtlasLine& L = fix[k];
+    L.cgf = CEN_PREFAC4 * wl * tablog(r2, 0);
+    L.gr = tablog(r2, 1) * wl * FOURPI_C_INV;
+    L.gs = tablog(r3, 0) * wl * FOURPI_C_INV;
+    L.gw = tablog(r3, 1) * wl * FOURPI_C_INV;
+    L.wlvac = wl;
+    L.nu = lo;
+  }
+  CK(cudaMemcpyAsync(d_fix, fix.data(), nf * sizeof(AtlasLine), cudaMemcpyHostToDevice, ctx->stream));
+  k_prep_scatter<<<g, 256, 0, ctx->stream>>>(d_fix, d_fl, (int64_t)nf, d_lines);
+  CKL(ctx);
+  // the host vectors are pageable: the copy has consumed them when it returns,
+  // but wait so that the caller's next step sees the fixed lines
+  CK(cudaStreamSynchronize(ctx->stream));
   return 0;
 }
 }  // namespace atlasgpu

@@ -459,6 +459,22 @@ int atlasgpu_model_get(atlasgpu_ctx* ctx, atlasgpu_model* m, double* t, double* 
   return 0;
 }
 
+int atlasgpu_model_get_tables(atlasgpu_ctx* ctx, atlasgpu_model* m, double* tabcont, double* xlines, double* acont,
+                              double* sigmac) {
+  if (!ctx || !m) return fail(ctx, ATLASGPU_EINVAL, "model_get_tables: null");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const size_t nn = (size_t)m->numnu * m->kw * sizeof(double);
+  if (tabcont)
+    CK(cudaMemcpyAsync(tabcont, m->tabcont, (size_t)(m->nwave + 1) * m->kw * sizeof(double), cudaMemcpyDeviceToHost,
+                       s));
+  if (xlines) CK(cudaMemcpyAsync(xlines, m->xl, nn, cudaMemcpyDeviceToHost, s));
+  if (acont) CK(cudaMemcpyAsync(acont, m->acont, nn, cudaMemcpyDeviceToHost, s));
+  if (sigmac) CK(cudaMemcpyAsync(sigmac, m->sigmac, nn, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
 int atlasgpu_model_set_structure(atlasgpu_ctx* ctx, atlasgpu_model* m, const double* t, const double* p,
                                  const double* rhox) {
   if (!ctx || !m || !t || !p || !rhox) return fail(ctx, ATLASGPU_EINVAL, "model_set_structure: null");

@@ -13,10 +13,13 @@
 // That array is part of the library image: every GPU that loads the library
 // holds it (kNoAllocRows x (8*kKwMax + 1) doubles = 6.6 MB) until the
 // process exits.  All calls share it and it keeps the last call's contents;
-// every row a call reads is written by that call first, so nothing needs
-// clearing, but two calls that overlap on the GPU (different streams, or
-// different host threads on one device) race on it and must be serialised by
-// the caller.
+// every row a call reads is written whole by that call first (the depths
+// between nrhox and kw as zeros), so nothing needs clearing, but two calls
+// that overlap on the GPU (different streams, or different host threads on
+// one device) race on it and must be serialised by the caller.  The
+// per-device address lookup itself is safe from several host threads.
+#include <atomic>
+
 #include "api_common.cuh"
 #include "atlas.cuh"
 
@@ -30,7 +33,9 @@ constexpr int kNoAllocRow = kAcc * kKwMax + 1;    // one row: 8 sums per depth +
 static __device__ __align__(256) double g_noalloc_partial[(size_t)kNoAllocRows * kNoAllocRow];
 
 constexpr int kMaxDevices = 64;
-double* g_partial_addr[kMaxDevices] = {nullptr};  // device address of the array, per device
+// device address of the array, per device; host threads making their first
+// call at once may both look it up, and both store the same address
+std::atomic<double*> g_partial_addr[kMaxDevices];
 
 }  // namespace
 
@@ -56,14 +61,15 @@ int atlasgpu_atlas_rt_pass_noalloc(atlasgpu_ctx* ctx, int numnu, const double* d
   CK(cudaSetDevice(ctx->device));
   // set-up, once per device, with that device current: the host-side name of
   // the array is not a device address, so ask the runtime for the address
-  if (!g_partial_addr[ctx->device]) {
+  double* partial = g_partial_addr[ctx->device].load(std::memory_order_acquire);
+  if (!partial) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partial);
     if (e != cudaSuccess || !p)
       return fail(ctx, ATLASGPU_ECUDA, "rt_pass_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-    g_partial_addr[ctx->device] = (double*)p;
+    partial = (double*)p;
+    g_partial_addr[ctx->device].store(partial, std::memory_order_release);
   }
-  double* partial = g_partial_addr[ctx->device];
   // launch shape: at most kNoAllocRows thread groups (rows of partials),
   // contiguous frequencies per group
   const size_t smem = rt_smem_bytes();

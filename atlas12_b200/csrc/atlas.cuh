@@ -279,7 +279,9 @@ template <bool F32>
 __device__ __forceinline__ double linop_cv(const LinopArgs& a, double center, double adamp, double dl, double rdop) {
   const double vv = dl * rdop;
   if (adamp > 0.20) return center * linop_full_voigt(a, vv, adamp);
-  if (vv > 10.0) {
+  // written as !(vv <= 10): a V that is not a number (a non-finite model
+  // structure) takes the Lorentz branch and never reaches the table index
+  if (!(vv <= 10.0)) {
     if (F32) return (double)((float)center * ((float)(a.lorentz * adamp) * __frcp_rn((float)(vv * vv))));
     return center * a.lorentz * adamp / (vv * vv);
   }
@@ -476,40 +478,6 @@ template <bool F32>
 static __global__ void __launch_bounds__(256, 3) k_atlas_linop(LinopArgs a) { linop_body<F32>(a); }
 
 // ---------------------------------------------------------------- RT pass
-__device__ __forceinline__ double expi3(double x) {
-  // EXPI(3, x), atlas12_modules.f90:21103-21225 (Cody & Thacher 1968)
-  const double ex = exp(-x);
-  double e1;
-  if (x > 4.0) {
-    e1 = (ex + ex * (-0.999999999998447 +
-                     (-26.6271060431811 +
-                      (-241.055827097015 +
-                       (-895.927957772937 + (-1298.85688746484 + (-545.374158883133 + -5.66575206533869 / x) / x) / x) / x) /
-                          x) /
-                         x) /
-                   (x + 28.6271060422192 +
-                    (292.310039388533 + (1332.78537748257 + (2777.61949509163 + (2404.01713225909 + 631.657483280800 / x) / x) / x) / x) /
-                        x)) /
-         x;
-  } else if (x > 1.0) {
-    e1 = ex *
-         (0.430967839469389 +
-          (6.90522522784444 + (23.0192559391333 + (24.3784088791317 + (9.04161556946329 + (0.999979577051595 + 4.65627107975096e-7 * x) * x) * x) * x) * x) * x) /
-         (0.103400130404874 +
-          (3.31909213593302 + (20.4494785013794 + (41.2807841891424 + (32.4264210695138 + (10.0411643829054 + x) * x) * x) * x) * x) * x);
-  } else if (x > 0.0) {
-    e1 = (-44178.5471728217 + (57721.7247139444 + (9938.31388962037 + (1842.11088668000 + (101.093806161906 + 5.03416184097568 * x) * x) * x) * x) * x) /
-             (76537.3323337614 + (32597.1881290275 + (6106.10794245759 + (635.419418378382 + (37.2298352833327 + x) * x) * x) * x) * x) -
-         log(x);
-  } else {
-    e1 = 0.0;
-  }
-  double r = e1;
-  r = (ex - x * r) / 1.0;
-  r = (ex - x * r) / 2.0;
-  return r;
-}
-
 constexpr int kAcc = 8;  // rjmins, rdabh, rdiagj, flxrad, raden, h_total, accrad, abross
 
 struct RtArgs {
@@ -648,13 +616,15 @@ static __device__ __forceinline__ void rt_body(const RtArgs& a) {
     pradk0 += S.f.knu1 * rcowt;
     g.sync();
   }
+  // the whole row is written: depths nrhox..kw-1 (padding when kw > nrhox)
+  // get zeros, so the fixed-order reduction never sums stale entries
   double* out = a.partial + (size_t)gw * (kAcc * a.kw + 1);
 #pragma unroll
   for (int c = 0; c < C; ++c) {
     const int j = g.r + c * RtG::N;
-    if (j < nr) {
+    if (j < a.kw) {
 #pragma unroll
-      for (int q = 0; q < kAcc; ++q) out[q * a.kw + j] = acc[q][c];
+      for (int q = 0; q < kAcc; ++q) out[q * a.kw + j] = j < nr ? acc[q][c] : 0.0;
     }
   }
   if (g.r == 0) out[kAcc * a.kw] = pradk0;

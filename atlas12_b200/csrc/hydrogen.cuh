@@ -9,41 +9,6 @@
 
 namespace atlasgpu {
 
-// EXPI(1, x) (atlas12_modules.f90:21103-21225, Cody & Thacher 1968)
-__device__ __forceinline__ double expi1(double x) {
-  const double ex = exp(-x);
-  if (x > 4.0) {
-    return (ex + ex * (-0.999999999998447 +
-                       (-26.6271060431811 +
-                        (-241.055827097015 +
-                         (-895.927957772937 + (-1298.85688746484 + (-545.374158883133 + -5.66575206533869 / x) / x) / x) /
-                             x) /
-                            x) /
-                           x) /
-                     (x + 28.6271060422192 +
-                      (292.310039388533 +
-                       (1332.78537748257 + (2777.61949509163 + (2404.01713225909 + 631.657483280800 / x) / x) / x) / x) /
-                          x)) /
-           x;
-  } else if (x > 1.0) {
-    return ex *
-           (0.430967839469389 +
-            (6.90522522784444 +
-             (23.0192559391333 + (24.3784088791317 + (9.04161556946329 + (0.999979577051595 + 4.65627107975096e-7 * x) * x) * x) * x) *
-                 x) *
-                x) /
-           (0.103400130404874 +
-            (3.31909213593302 + (20.4494785013794 + (41.2807841891424 + (32.4264210695138 + (10.0411643829054 + x) * x) * x) * x) * x) *
-                x);
-  } else if (x > 0.0) {
-    return (-44178.5471728217 +
-            (57721.7247139444 + (9938.31388962037 + (1842.11088668000 + (101.093806161906 + 5.03416184097568 * x) * x) * x) * x) * x) /
-               (76537.3323337614 + (32597.1881290275 + (6106.10794245759 + (635.419418378382 + (37.2298352833327 + x) * x) * x) * x) * x) -
-           log(x);
-  }
-  return 0.0;
-}
-
 __device__ inline double hfnm(int n, int m) {
   if (m <= n) return 0.0;
   const double xn = (double)n;

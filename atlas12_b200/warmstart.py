@@ -238,7 +238,6 @@ def main(argv=None):
     python -m atlas12_b200.warmstart evaluate --weights warmstart.npz --n 200 --seed 12 --out heldout.npz
     """
     import argparse
-    import os
     import time
 
     ap = argparse.ArgumentParser()
@@ -253,9 +252,8 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=3000)
     ap.add_argument("--lr", type=float, default=1e-3)
     a = ap.parse_args(argv)
-    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    t = np.load(os.path.join(root, "tests", "golden", "reference_tables.npz"))
-    tables = {k: t[k] for k in t.files}
+    from . import operators
+    tables = operators.load()
     ctx = _lib.Context(0, _lib.PREC_MIXED)
     t0 = time.time()
     if a.cmd == "generate":

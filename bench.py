@@ -89,8 +89,9 @@ def workload():
 
 
 def operators():
-    t = np.load(os.path.join(ROOT, "tests", "golden", "reference_tables.npz"))
-    return {k: t[k] for k in t.files}
+    """The operator data a caller passes (package data, from the reference's files)."""
+    from atlas12_b200 import operators as op
+    return op.load()
 
 
 class Clocks:

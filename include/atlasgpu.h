@@ -4,8 +4,8 @@
  * The reference (cconroy20/atlas12, Fortran 90) keeps these loops inside its
  * drivers; this library replaces them.  Each entry point names the reference
  * code it stands in for (file:line inside the reference tree).  The Fortran
- * side binds them with BIND(C) interfaces; Python binds
- * them with ctypes (atlas12_b200/_lib.py).
+ * side binds them with BIND(C) interfaces; Python binds them with ctypes
+ * (atlas12_b200/_lib.py).
  *
  * Conventions
  *   - Every call returns 0 or a negative ATLASGPU_E* status; it never aborts.
@@ -17,7 +17,10 @@
  *     whose name ends in _dev take device pointers instead and do no host
  *     transfer; they run on the context's stream and return without waiting.
  *   - One context per host thread; calls on one context serialise on its
- *     stream.  No global mutable state.
+ *     stream.  All state lives in contexts and the objects made on them,
+ *     with one exception: atlasgpu_atlas_rt_pass_noalloc keeps its scratch
+ *     in one fixed device array shared by every call in the process (its
+ *     declaration says how calls must be serialised).
  */
 #ifndef ATLASGPU_H
 #define ATLASGPU_H
@@ -434,6 +437,14 @@ int atlasgpu_model_iterate(atlasgpu_ctx *ctx, atlasgpu_model *m, int max_iter, d
  * iteration's HNU(1) per frequency ([numnu], may be NULL). */
 int atlasgpu_model_get(atlasgpu_ctx *ctx, atlasgpu_model *m, double *t, double *rhox, double *p,
                        double *xne, double *flxerr, double *hsurf);
+/* Copy the model's tables of the last iteration: TABCONT [nwave+1][kw]
+ * (KAPCONT's line-cutoff table, atlas12_modules.f90:19072-19138, built on
+ * the model's first iteration), XLINES [numnu][kw] (LINOP1's output,
+ * :18132-18374) and the continuum ACONT, SIGMAC [numnu][kw] of the RT pass
+ * (any may be NULL; depths j >= nrhox are padding).  What the Fortran
+ * driver holds in the module arrays TABCONT and XLINES after RUN_RT_PASS. */
+int atlasgpu_model_get_tables(atlasgpu_ctx *ctx, atlasgpu_model *m, double *tabcont, double *xlines,
+                              double *acont, double *sigmac);
 /* Overwrite the structure (T, P, RHOX [nrhox]) and restart the iteration
  * count (a warm start). */
 int atlasgpu_model_set_structure(atlasgpu_ctx *ctx, atlasgpu_model *m, const double *t,
@@ -467,15 +478,17 @@ int atlasgpu_model_destroy(atlasgpu_ctx *ctx, atlasgpu_model *m);
  * [numnu][kw] (d_scont may be NULL: SCONT = BNU); d_xlines_t = XLINES
  * transposed, [kw][numnu] (the layout the device LINOP1 writes); d_rhox,
  * d_t, d_hkt [nrhox]; d_sums [8*kw + 1] receives RJMINS, RDABH, RDIAGJ,
- * FLXRAD, RADEN, H_TOTAL, ACCRAD, ABROSS ([q*kw + j]) and PRADK0 ([8*kw]);
- * d_hsurf [numnu] receives HNU(1) per frequency.
+ * FLXRAD, RADEN, H_TOTAL, ACCRAD, ABROSS ([q*kw + j], zero for depths
+ * nrhox <= j < kw) and PRADK0 ([8*kw]); d_hsurf [numnu] receives HNU(1) per
+ * frequency.
  * The call allocates nothing: its scratch is a fixed device array of
  * 1024 x 801 doubles (6.6 MB) in the library image, held by every GPU that
  * loads the library until the process exits.  kw above 100 is rejected.
  * The first call on a device looks the array's address up once (make that
- * first call before any stream capture).  All calls share the array, so calls
- * that overlap on the GPU race: serialise them.  Runs on the context stream
- * and returns without waiting. */
+ * first call before any stream capture); that lookup is safe from several
+ * host threads at once.  All calls share the array, so calls that overlap on
+ * the GPU race: serialise them.  Runs on the context stream and returns
+ * without waiting. */
 int atlasgpu_atlas_rt_pass_noalloc(atlasgpu_ctx *ctx, int numnu, const double *d_waveset,
                                    const double *d_rcoset, const double *d_acont,
                                    const double *d_sigmac, const double *d_scont, int kw,

@@ -14,7 +14,8 @@ ACC = ("rjmins", "rdabh", "rdiagj", "flxrad", "raden", "h_total", "accrad", "abr
 
 
 class OracleIteration:
-    def __init__(self, po, atlas, tables, waveset, rcoset, lines, start, teff, vturb_kms, nu0=1, nu1=None):
+    def __init__(self, po, atlas, tables, waveset, rcoset, lines, start, teff, vturb_kms, nu0=1, nu1=None, mh=0.0,
+                 grav=None):
         from atlas12_b200 import surrogate as sg
         self.po, self.atlas, self.sg = po, atlas, sg
         self.ops = po.Ops.from_tables(tables)
@@ -23,13 +24,13 @@ class OracleIteration:
         self.cut = atlas.cutoff_grid()
         self.iw = atlas.iwavetab(self.cut)
         self.ws, self.rc, self.lines = waveset, rcoset, lines
-        self.teff, self.vturb = teff, vturb_kms
+        self.teff, self.vturb, self.mh = teff, vturb_kms, mh
         self.nu0, self.nu1 = nu0, (waveset.size if nu1 is None else nu1)
         nr = start["t"].size
         self.st = dict(t=start["t"].copy(), rhox=start["rhox"].copy(), p=start["p"].copy(), xne=np.zeros(nr),
                        abross=np.zeros(nr), prad=np.zeros(nr), vturb=np.full(nr, vturb_kms * 1e5),
                        pturb=np.zeros(nr), tauros=start["tauros"].copy(), accrad=np.zeros(nr), raden=np.zeros(nr),
-                       oldt1=np.zeros(nr), teff=teff, grav=start["grav"])
+                       oldt1=np.zeros(nr), teff=teff, grav=start["grav"] if grav is None else grav)
         self.store = po.RossStore()
         self.it = 0
         self.tabcont = None
@@ -42,7 +43,7 @@ class OracleIteration:
         if self.it > 1:
             p = st["grav"] * st["rhox"] - st["prad"]
             st["p"] = np.where(p <= 0, np.maximum(st["grav"] * st["rhox"] * 1e-4, 1e-10), p)
-        pop = sg.populations(st["t"], st["p"], self.vturb, sg.ATLAS_LINE_POP)
+        pop = sg.populations(st["t"], st["p"], self.vturb, sg.ATLAS_LINE_POP, mh=self.mh)
         t = st["t"]
         xd = np.zeros((270, nr))
         dp = np.ones((270, nr))
@@ -54,12 +55,17 @@ class OracleIteration:
         txnxn = (pop["nh"] * (1 - pop["xh"]) + 0.42 * 0.085 * pop["nh"]) * (t / 1e4) ** 0.3
         st["xne"] = pop["xne"]
         if self.tabcont is None:
+            # KAPCONT (atlas12_modules.f90:19072-19138): ACONT = 1e10 and no
+            # KAPP call at cutoff wavelengths not redward of WAVESET(1)
             ka, sgm = sg.continuum_opacity(self.cut, t, st["p"], pop)
+            below = self.cut <= self.ws[0]
+            ka[below], sgm[below] = 1.0e10, 0.0
             stc = 1 - np.exp(-(sg.CLIGHT_NMS / self.cut)[:, None] * hkt[None, :])
             tab = (ka + sgm) * 1e-3 / stc
             self.tabcont = np.vstack([tab, tab[-1:]])
         atm = dict(xnfdop=xd, dopple=dp, xne=pop["xne"], txnxn=txnxn, hckt=hckt)
         xl, _ = po.atlas_linop1(*self.h, self.tl, self.lines, atm, self.tabcont, self.iw, self.ws)
+        self.xlines = xl
         ac, sgm = sg.continuum_opacity(self.ws, t, st["p"], pop)
         acc, _ = po.atlas_rt_pass(self.ops, self.ws, self.rc, ac, sgm, xl, st["rhox"], t, hkt, self.teff,
                                   nu0=self.nu0, nu1=self.nu1)

@@ -34,7 +34,15 @@ modified).  Writes tests/golden/reference_tables.npz with:
                  plus deck_pradk = PRADK -- output of the reference itself, used
                  to pin INTEG / ROSSTAB / TTAUP
 
-Usage:  python tests/golden/make_golden.py [reference_root]
+It also writes atlas12_b200/data/operators.npz: the subset that a caller
+passes to the library as its operator data (the JOSH operators and grids,
+TABVOIGT's table, WAVETAB, the SELECTLINES tables and both programs'
+hydrogen tables), the way a Fortran driver passes what BLOCKJ/BLOCKH and its
+DATA statements hold.  Test-only entries (the Weideman coefficients, the
+converged deck) stay in the fixture.
+
+Usage:  python tests/golden/make_golden.py <reference_root>
+        (or set ATLAS12_REFERENCE to the reference checkout)
 """
 import ctypes
 import os
@@ -43,8 +51,10 @@ import sys
 
 import numpy as np
 
-ROOT = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+ROOT = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ATLAS12_REFERENCE")
 HERE = os.path.dirname(os.path.abspath(__file__))
+PACKAGE_DATA = os.path.join(HERE, "..", "..", "atlas12_b200", "data", "operators.npz")
+TEST_ONLY = ("awei", "lwei", "deck", "deck_pradk", "stehle_dims")
 
 _libc = ctypes.CDLL(None)
 _libc.strtof.restype = ctypes.c_float
@@ -164,6 +174,8 @@ def stehle_dims(datadir):
 
 
 def main():
+    if not ROOT or not os.path.isdir(ROOT):
+        sys.exit("usage: make_golden.py <reference_root>  (or ATLAS12_REFERENCE=<reference_root>)")
     mod = open(os.path.join(ROOT, "src", "atlas12_modules.f90")).read()
     syn = open(os.path.join(ROOT, "src", "synthe_module.f90")).read()
     out = dict(
@@ -205,6 +217,7 @@ def main():
     out["stehle_dims"] = stehle_dims(os.path.join(ROOT, "data"))
     out["deck"], out["deck_pradk"] = read_deck(os.path.join(ROOT, "workdir", "ap00t5777g4.44at12.dat"))
     np.savez(os.path.join(HERE, "reference_tables.npz"), **out)
+    np.savez(PACKAGE_DATA, **{k: v for k, v in out.items() if k not in TEST_ONLY})
     for k, v in out.items():
         print(k, v.shape)
 

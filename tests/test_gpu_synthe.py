@@ -4,8 +4,15 @@ Tolerances:
   * nbuff (binning): bit-exact.
   * continuum (REAL(4)): 2 ulp (device exp10 vs the C library powf).
   * kappa_line: |GPU - oracle_fp64| <= 1e-5 * (kappa_line + kappa_cont) per bin
-    for both precisions (typically ~1e-7 mixed, ~1e-12 fp64); against the
-    reference's REAL(4) sequential sums (oracle ref32) <= 1e-4 * (k + k_c).
+    for both precisions (typically ~1e-7 mixed, ~1e-12 fp64).  Against the
+    reference's REAL(4) sequential sums (oracle ref32): <= 1e-5 * (k + k_c)
+    on the small case.  At the C1 size (20,000 lines) the reference's own
+    REAL(4) accumulation is further than that from the exact sum: the FP64
+    oracle itself differs from ref32 by 1.8e-5 there (the strongest line
+    cores, where hundreds of REAL(4) additions land in one bin and
+    kappa_line >> kappa_cont).  The C1 bound is therefore derived: the GPU's
+    distance from ref32 may exceed the FP64 oracle's distance from ref32 by
+    at most 1e-6 (the GPU adds nothing beyond the reference's rounding).
   * flux: relative 1e-4 against the oracle on the same opacity.
 """
 import numpy as np
@@ -77,7 +84,7 @@ def test_line_opacity_matches_fp64_oracle(prepared, gpu_ctx, tables, prec):
     e64 = _kappa_err(got, p["fp64"], p["cont"])
     e32 = _kappa_err(got, p["ref32"], p["cont"])
     assert e64 <= 1e-5, e64
-    assert e32 <= 1e-4, e32
+    assert e32 <= 1e-5, e32
     assert np.all(np.isfinite(got)) and got.max() > 0
 
 
@@ -136,6 +143,14 @@ def test_full_c1_pipeline(po, gpu_ctx, tables):
     ref = po.synthe_line_opacity(po.FP64, lines, g["length"], case["atm"], cont, case["resolu"])[1]
     assert _kappa_err(op, ref, cont) <= 1e-5
     assert np.all(np.isfinite(flux)) and np.all(flux > 0)
+    # against the reference's REAL(4) sequential order: no further than the
+    # exact (FP64) sums are from it, plus 1e-6
+    r32 = po.synthe_line_opacity(po.REF32, lines, g["length"], case["atm"], cont, case["resolu"])[1]
+    e_exact = _kappa_err(ref.astype(np.float32), r32, cont)
+    e_gpu = _kappa_err(op, r32, cont)
+    print(f"C1 kappa_line vs REAL(4) order: GPU {e_gpu:.3e}, FP64 oracle {e_exact:.3e}")
+    assert e_exact <= 3e-5, e_exact
+    assert e_gpu <= e_exact + 1e-6, (e_gpu, e_exact)
 
 
 def _nlte_records(po, case, g, seed=8):
