@@ -67,6 +67,7 @@ SIGNATURES = {
     "atlasgpu_launch_count": (_I64, [_P]),
     "atlasgpu_enable_timing": (_I, [_P, _I]),
     "atlasgpu_kernel_ms": (_D, [_P, ctypes.c_char_p]),
+    "atlasgpu_kernel_work": (_D, [_P, ctypes.c_char_p]),
     "atlasgpu_set_operators": (_I, [_P, _P, _P, _P, _P, _P]),
     "atlasgpu_synthe_grid": (_I, [_D, _D, _D, ctypes.POINTER(Grid)]),
     "atlasgpu_synthe_bin": (_I, [_P, _P, _I64, _D, _I32, _P]),
@@ -312,6 +313,10 @@ class Context:
 
     def kernel_ms(self, name):
         return float(lib().atlasgpu_kernel_ms(self._h, name.encode()))
+
+    def kernel_work(self, name):
+        """Work units the last timed launch of `name` counted (-1 if none)."""
+        return float(lib().atlasgpu_kernel_work(self._h, name.encode()))
 
     def set_operators(self, xtau8, coefj, coefh, ch_j, ck_j):
         """coefj/coefh as 2-D arrays COEF[L-1, M-1]; passed column-major."""

@@ -143,7 +143,7 @@ namespace {
 int rt_launch(atlasgpu_ctx* ctx, RtArgs& a, double* d_sum, int* nwarps_out) {
   const size_t smem = rt_smem_bytes();
   // enough groups to fill every SM several times, frequencies contiguous per group
-  const int target = ctx->nsm * 3 * kRtGroups * 4;
+  const int target = ctx->nsm * kRtMinBlocks * kRtGroups * 4;
   a.nu_per_warp = std::max(1, (a.numnu + target - 1) / target);
   const int ng = (a.numnu + a.nu_per_warp - 1) / a.nu_per_warp;
   const int blocks = (ng + kRtGroups - 1) / kRtGroups;
@@ -262,10 +262,14 @@ int atlasgpu_atlas_linop(atlasgpu_ctx* ctx, const int32_t* linedata, int64_t n, 
                 (const double*)ctx->bufs["tab_h0"].first, (const double*)ctx->bufs["tab_h1"].first,
                 (const double*)ctx->bufs["tab_h2"].first, (const float4*)ctx->bufs["tab_hf"].first, d_xl, d_cnt,
                 d_cnt + 1};
-    Timer tm(ctx, "atlas_linop");
-    if (ctx->precision == ATLASGPU_PREC_MIXED) k_atlas_linop<true><<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
-    else k_atlas_linop<false><<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
-    CKL(ctx);
+    a.work = work_counters(ctx, 1);
+    {
+      Timer tm(ctx, "atlas_linop");
+      if (ctx->precision == ATLASGPU_PREC_MIXED) k_atlas_linop<true><<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
+      else k_atlas_linop<false><<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
+      CKL(ctx);
+    }
+    work_collect(ctx, a.work, {"atlas_linop_points"});
   }
   CK(cudaMemcpyAsync(xlines_out, d_xl, (size_t)kw * numnu * sizeof(double), cudaMemcpyDeviceToHost, s));
   unsigned long long cnt[2];

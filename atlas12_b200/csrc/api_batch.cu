@@ -81,10 +81,12 @@ __global__ void k_batch_kapp(BatchDev d) {
 }
 
 template <bool F32>
-__global__ void __launch_bounds__(256, 3) k_batch_linop(const LinopArgs* __restrict__ args, const BatchCtl* ctl) {
+__global__ void __launch_bounds__(256, 3) k_batch_linop(const LinopArgs* __restrict__ args, const BatchCtl* ctl,
+                                                        unsigned long long* work) {
   const int b = blockIdx.y;
   if (!running(ctl, b)) return;
-  const LinopArgs a = args[b];
+  LinopArgs a = args[b];
+  a.work = work;
   linop_body<F32>(a);
 }
 
@@ -181,12 +183,16 @@ int enqueue_batch(atlasgpu_ctx* ctx, atlasgpu_batch* B, bool timed) {
     CKL(ctx);
   }
   if (B->nlines > 0) {
-    Timer tm(ctx, "batch_linop");
-    if (ctx->precision == ATLASGPU_PREC_MIXED)
-      k_batch_linop<true><<<dim3(B->grid_linop, nb), 256, 0, s>>>(B->la, B->d.ctl);
-    else
-      k_batch_linop<false><<<dim3(B->grid_linop, nb), 256, 0, s>>>(B->la, B->d.ctl);
-    CKL(ctx);
+    unsigned long long* work = work_counters(ctx, 1);
+    {
+      Timer tm(ctx, "batch_linop");
+      if (ctx->precision == ATLASGPU_PREC_MIXED)
+        k_batch_linop<true><<<dim3(B->grid_linop, nb), 256, 0, s>>>(B->la, B->d.ctl, work);
+      else
+        k_batch_linop<false><<<dim3(B->grid_linop, nb), 256, 0, s>>>(B->la, B->d.ctl, work);
+      CKL(ctx);
+    }
+    work_collect(ctx, work, {"batch_linop_points"});
   }
   {
     Timer tm(ctx, "batch_rt");
@@ -216,7 +222,7 @@ int enqueue_batch(atlasgpu_ctx* ctx, atlasgpu_batch* B, bool timed) {
 int apply_shape(atlasgpu_ctx* ctx, atlasgpu_batch* B, int linop_ctas_per_sm, int rt_waves) {
   const int nb = B->nslots;
   const size_t stride = (size_t)kAcc * B->kw + 1;
-  const int target = ctx->nsm * 3 * kRtGroups * rt_waves;
+  const int target = ctx->nsm * kRtMinBlocks * kRtGroups * rt_waves;
   const int groups_per_slot = std::max(1, (target + nb - 1) / nb);
   const int nu_per = std::max(1, (B->numnu + groups_per_slot - 1) / groups_per_slot);
   const int ng = (B->numnu + nu_per - 1) / nu_per;

@@ -4,6 +4,7 @@
 
 #include <cstdarg>
 #include <cstring>
+#include <initializer_list>
 #include <map>
 #include <string>
 #include <vector>
@@ -19,6 +20,7 @@ struct atlasgpu_ctx {
   int64_t launches = 0;
   bool timing = false;
   std::map<std::string, double> kms;
+  std::map<std::string, double> kwork;  // counted work units of timed launches
   // named device buffers, grow-only
   std::map<std::string, std::pair<void*, size_t>> bufs;
   atlasgpu::JoshOps* ops = nullptr;  // device
@@ -93,11 +95,14 @@ inline int bufT(atlasgpu_ctx* ctx, const char* name, size_t count, T** out) {
 }
 
 // CUDA-event timing of one named launch family (only when enabled)
+// (accumulate = true adds to the family's time instead of replacing it: the
+// caller clears the entry once per call for launches made in several parts)
 struct Timer {
   atlasgpu_ctx* ctx;
   const char* name;
+  bool acc;
   cudaEvent_t a = nullptr, b = nullptr;
-  Timer(atlasgpu_ctx* c, const char* n) : ctx(c), name(n) {
+  Timer(atlasgpu_ctx* c, const char* n, bool accumulate = false) : ctx(c), name(n), acc(accumulate) {
     if (ctx->timing) {
       cudaEventCreate(&a);
       cudaEventCreate(&b);
@@ -110,7 +115,8 @@ struct Timer {
       cudaEventSynchronize(b);
       float ms = 0.f;
       cudaEventElapsedTime(&ms, a, b);
-      ctx->kms[name] = ms;
+      if (acc) ctx->kms[name] += ms;
+      else ctx->kms[name] = ms;
       cudaEventDestroy(a);
       cudaEventDestroy(b);
       a = b = nullptr;
@@ -118,6 +124,30 @@ struct Timer {
   }
   ~Timer() { stop(); }
 };
+
+// Work counters of a timed launch family: a zeroed device array of n
+// counters while timing is enabled, null otherwise (kernels then count
+// nothing).  work_collect copies them back into ctx->kwork under the names.
+inline unsigned long long* work_counters(atlasgpu_ctx* ctx, int n) {
+  if (!ctx->timing) return nullptr;
+  unsigned long long* p;
+  if (bufT(ctx, "work_cnt", (size_t)n, &p)) return nullptr;
+  if (cudaMemsetAsync(p, 0, n * sizeof(unsigned long long), ctx->stream) != cudaSuccess) return nullptr;
+  return p;
+}
+inline void work_collect(atlasgpu_ctx* ctx, const unsigned long long* d, std::initializer_list<const char*> names) {
+  if (!d) return;
+  unsigned long long h[8] = {0};
+  const int n = (int)names.size() < 8 ? (int)names.size() : 8;
+  if (cudaMemcpyAsync(h, d, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+    return;
+  int k = 0;
+  for (const char* nm : names) {
+    if (k >= n) break;
+    ctx->kwork[nm] = (double)h[k++];
+  }
+}
 
 inline int grid_for(atlasgpu_ctx* ctx, int64_t work, int threads, int per_sm = 8) {
   int64_t g = (work + threads - 1) / threads;

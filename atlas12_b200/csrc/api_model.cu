@@ -105,7 +105,7 @@ __global__ void k_surrogate_eval(int nrhox, const double* t, const double* p, do
 void rt_shape(atlasgpu_ctx* ctx, atlasgpu_model* m) {
   const int last = m->nu_last > 0 ? m->nu_last : m->numnu;
   const int len = last - m->nu_first + 1;
-  const int target = ctx->nsm * 3 * kRtGroups * 4;
+  const int target = ctx->nsm * kRtMinBlocks * kRtGroups * 4;
   m->nu_per_group = std::max(1, (len + target - 1) / target);
   const int ng = (len + m->nu_per_group - 1) / m->nu_per_group;
   m->blocks_rt = (ng + kRtGroups - 1) / kRtGroups;
@@ -137,12 +137,16 @@ int enqueue_begin(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
     LinopArgs la{m->lines, m->nlines, m->nrhox, m->kw, m->nspec, m->numnu, m->xnfdop, m->dopple,
                  m->xne_eos, m->txnxn, m->hckt, m->tabcont, m->waveset, m->h0, m->h1, m->h2, m->hf, m->xl,
                  nullptr, m->cnt, m->nu_first, m->nu_last};
-    Timer tm(ctx, "atlas_linop");
-    if (ctx->precision == ATLASGPU_PREC_MIXED)
-      k_atlas_linop<true><<<grid_for(ctx, m->nlines * 32, 256, 16), 256, 0, s>>>(la);
-    else
-      k_atlas_linop<false><<<grid_for(ctx, m->nlines * 32, 256, 16), 256, 0, s>>>(la);
-    CKL(ctx);
+    la.work = work_counters(ctx, 1);
+    {
+      Timer tm(ctx, "atlas_linop");
+      if (ctx->precision == ATLASGPU_PREC_MIXED)
+        k_atlas_linop<true><<<grid_for(ctx, m->nlines * 32, 256, 16), 256, 0, s>>>(la);
+      else
+        k_atlas_linop<false><<<grid_for(ctx, m->nlines * 32, 256, 16), 256, 0, s>>>(la);
+      CKL(ctx);
+    }
+    work_collect(ctx, la.work, {"atlas_linop_points"});
   }
   {
     Timer tm(ctx, "model_kapp");
@@ -304,7 +308,7 @@ int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlas
   rt_shape(ctx, m);
   {
     // any shard launches at most min(NUMNU, target) groups (rt_shape): size the partials for that
-    const int target = ctx->nsm * 3 * kRtGroups * 4;
+    const int target = ctx->nsm * kRtMinBlocks * kRtGroups * 4;
     const int gmax = std::min(m->numnu, target);
     m->nwl = ((gmax + kRtGroups - 1) / kRtGroups) * kRtGroups;
   }

@@ -73,7 +73,7 @@ int atlasgpu_atlas_rt_pass_noalloc(atlasgpu_ctx* ctx, int numnu, const double* d
   // launch shape: at most kNoAllocRows thread groups (rows of partials),
   // contiguous frequencies per group
   const size_t smem = rt_smem_bytes();
-  int target = ctx->nsm * 3 * kRtGroups * 4;
+  int target = ctx->nsm * kRtMinBlocks * kRtGroups * 4;
   if (target > kNoAllocRows) target = kNoAllocRows;
   const int npw = (numnu + target - 1) / target;
   const int ng = (numnu + npw - 1) / npw;

@@ -118,6 +118,12 @@ double atlasgpu_kernel_ms(atlasgpu_ctx* ctx, const char* name) {
   return it == ctx->kms.end() ? -1.0 : it->second;
 }
 
+double atlasgpu_kernel_work(atlasgpu_ctx* ctx, const char* name) {
+  if (!ctx || !name) return -1.0;
+  auto it = ctx->kwork.find(name);
+  return it == ctx->kwork.end() ? -1.0 : it->second;
+}
+
 int atlasgpu_set_operators(atlasgpu_ctx* ctx, const double* xtau8, const double* coefj,
                            const double* coefh, const double* ch_j, const double* ck_j) {
   if (!ctx || !xtau8 || !coefj || !coefh || !ch_j || !ck_j)
@@ -286,14 +292,18 @@ int atlasgpu_synthe_line_opacity_dev(atlasgpu_ctx* ctx, const atlasgpu_lte_line*
       (r = bufT(ctx, "lo_base", nj, &base)))
     return r;
   std::vector<int64_t> htot(nj), hbase(nj);
+  unsigned long long* work = work_counters(ctx, 2);
+  // the families run once per depth batch: their times add up over the call
+  if (ctx->timing)
+    for (const char* f : {"synthe_core", "synthe_farfill", "synthe_farwing"}) ctx->kms[f] = 0.0;
   for (int j0 = 0; j0 < nrhox; j0 += nj) {
     const int nb = std::min(nj, nrhox - j0);
     CK(cudaMemsetAsync(nfar, 0, nb * sizeof(unsigned), ctx->stream));
     CK(cudaMemsetAsync(tdiff, 0, (size_t)nb * (ntiles + 1) * sizeof(int), ctx->stream));
     if (n > 0) {
       CoreArgs a{d_lines, n, length, nrhox, nspec, maxprof, j0, nb, resolu, d_cont, d_xnfdop,
-                 d_dopple, d_xne, d_txnxn, d_hckt, acc, far, nfar, tdiff, ntiles};
-      Timer tm(ctx, "synthe_core");
+                 d_dopple, d_xne, d_txnxn, d_hckt, acc, far, nfar, tdiff, ntiles, work};
+      Timer tm(ctx, "synthe_core", true);
       const int64_t groups = n * nb;
       k_core<8><<<grid_for(ctx, groups * 8, 256, 16), 256, 0, ctx->stream>>>(a);
       CKL(ctx);
@@ -311,13 +321,13 @@ int atlasgpu_synthe_line_opacity_dev(atlasgpu_ctx* ctx, const atlasgpu_lte_line*
     if ((r = bufT(ctx, "lo_csr", (size_t)std::max<int64_t>(run, 1), &csr))) return r;
     CK(cudaMemcpyAsync(base, hbase.data(), nb * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
     {
-      Timer tm(ctx, "synthe_farfill");
+      Timer tm(ctx, "synthe_farfill", true);
       dim3 g(std::max(1, std::min(ctx->nsm * 4 / std::max(1, nb) + 1, 1024)), nb);
       k_far_fill<<<g, 256, 0, ctx->stream>>>(far, nfar, nn, length, base, fillptr, ntiles, csr);
       CKL(ctx);
     }
     {
-      Timer tm(ctx, "synthe_farwing");
+      Timer tm(ctx, "synthe_farwing", true);
       dim3 g(ntiles, nb);
       if (ctx->precision == ATLASGPU_PREC_MIXED)
         k_farwing<true><<<g, kFarThreads, 0, ctx->stream>>>(far, nn, off, base, csr, ntiles, length, j0, acc, d_opac);
@@ -326,6 +336,7 @@ int atlasgpu_synthe_line_opacity_dev(atlasgpu_ctx* ctx, const atlasgpu_lte_line*
       CKL(ctx);
     }
   }
+  work_collect(ctx, work, {"synthe_voigt_evals", "synthe_farwing_updates"});
   return 0;
 }
 

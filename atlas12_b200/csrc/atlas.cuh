@@ -261,6 +261,8 @@ struct LinopArgs {
   double lorentz = kInvSqrtPi;
   const double* lcontx = nullptr;
   const double* emerge = nullptr;
+  // work counter (timed launches only, else null): wing points added into XLINES
+  unsigned long long* work = nullptr;
 };
 
 // LINOP1's profile value at one wing point, V = (distance in nm) * RDOP with
@@ -308,9 +310,10 @@ __device__ __forceinline__ bool linop_below(const LinopArgs& a, double cv, doubl
 // whole warp (lanes over wing points), add-then-test as in the reference:
 // red points rnext..iwmax unless rdone, blue offsets bnext..100 unless bdone.
 template <bool F32>
-static __device__ __noinline__ void linop_finish_warp(const LinopArgs& a, int J, double center, double adamp,
-                                                      double rdop, double wlvac, int nu, double tc, int rnext,
-                                                      bool rdone, int bnext, bool bdone, double wcon, int lane) {
+static __device__ __noinline__ unsigned linop_finish_warp(const LinopArgs& a, int J, double center, double adamp,
+                                                          double rdop, double wlvac, int nu, double tc, int rnext,
+                                                          bool rdone, int bnext, bool bdone, double wcon, int lane) {
+  unsigned added = 0;  // points this lane added
   double* xl = a.xl + (J - 1);
   const int iwmax = min(nu + a.max_wing, a.numnu);
   const int nuh = a.nu_hi > 0 ? a.nu_hi : a.numnu;
@@ -327,7 +330,10 @@ static __device__ __noinline__ void linop_finish_warp(const LinopArgs& a, int J,
       }
       const unsigned stop = __ballot_sync(0xffffffffu, valid && below);
       const int last = stop ? base + __ffs(stop) - 1 : iwmax;
-      if (valid && iw <= last && iw >= a.nu_lo && iw <= nuh) atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
+      if (valid && iw <= last && iw >= a.nu_lo && iw <= nuh) {
+        atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
+        ++added;
+      }
       if (stop) break;
     }
   }
@@ -347,10 +353,14 @@ static __device__ __noinline__ void linop_finish_warp(const LinopArgs& a, int J,
       const unsigned stop = __ballot_sync(0xffffffffu, valid && below);
       const unsigned inval = __ballot_sync(0xffffffffu, !valid);
       const int ilast = stop ? i0 + __ffs(stop) - 1 : a.max_wing;
-      if (valid && i <= ilast && iw >= a.nu_lo && iw <= nuh) atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
+      if (valid && i <= ilast && iw >= a.nu_lo && iw <= nuh) {
+        atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
+        ++added;
+      }
       if (stop || inval) break;
     }
   }
+  return added;
 }
 
 // Warp per line, lane per depth.  Most (line, depth) wing walks stop after a
@@ -365,7 +375,7 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
   const int lane = threadIdx.x & 31;
   const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned long long walked = 0;
+  unsigned long long walked = 0, points = 0;
   const int nuh = a.nu_hi > 0 ? a.nu_hi : a.numnu;
   for (int64_t il = w0; il < a.n; il += nw) {
     const AtlasLine L = a.lines[il];
@@ -433,7 +443,10 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
           const int iw = rnext;
           const double dl = a.waveset[iw - 1] - L.wlvac;
           const double cv = linop_cv<F32>(a, center, adamp, dl, rdop);
-          if (iw >= a.nu_lo && iw <= nuh) atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
+          if (iw >= a.nu_lo && iw <= nuh) {
+            atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
+            ++points;
+          }
           if (linop_below<F32>(a, cv, tc, center, adamp, dl, rdop) || iw >= iwmax) rdone = true;
           else rnext = iw + 1;
         }
@@ -444,7 +457,10 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
           } else {
             const double dl = L.wlvac - a.waveset[iw - 1];
             const double cv = linop_cv<F32>(a, center, adamp, dl, rdop);
-            if (iw >= a.nu_lo && iw <= nuh) atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
+            if (iw >= a.nu_lo && iw <= nuh) {
+              atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
+              ++points;
+            }
             if (linop_below<F32>(a, cv, tc, center, adamp, dl, rdop) || bnext >= a.max_wing) bdone = true;
             else bnext = bnext + 1;
           }
@@ -465,13 +481,17 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
         const bool rd = __shfl_sync(0xffffffffu, (int)rdone, src) != 0;
         const bool bd = __shfl_sync(0xffffffffu, (int)bdone, src) != 0;
         const double wc = __shfl_sync(0xffffffffu, wcon, src);
-        linop_finish_warp<F32>(a, Js, cs, as, ds, L.wlvac, L.nu, ts, rn, rd, bn, bd, wc, lane);
+        points += linop_finish_warp<F32>(a, Js, cs, as, ds, L.wlvac, L.nu, ts, rn, rd, bn, bd, wc, lane);
       }
     }
   }
   // walked (line, depth) pairs, summed over the warp's lanes
   for (int o = 16; o > 0; o >>= 1) walked += __shfl_xor_sync(0xffffffffu, walked, o);
   if (lane == 0 && walked && a.npairs) atomicAdd(a.npairs, walked);
+  if (a.work) {
+    for (int o = 16; o > 0; o >>= 1) points += __shfl_xor_sync(0xffffffffu, points, o);
+    if (lane == 0) atomicAdd(a.work, points);
+  }
 }
 
 template <bool F32>
@@ -502,16 +522,17 @@ struct RtWS {
   JoshWSFull f;
   double acont[kKwMax], sigmac[kKwMax], aline[kKwMax], stim[kKwMax];
   double dab[kKwMax];           // SCONT while JOSH runs (when given), then d(abtot)/d(rhox)
-  alignas(16) double U[kNx * (kNx + 1)];  // pivot rows of the 51x51 factorisation (rows 16-byte aligned)
+  alignas(16) double U[kNx * kU2];  // pivot rows of the 51x51 factorisation (row stride kU2)
 };
 
-// One pair group (64 threads) per frequency, kRtGroups groups per CTA.  The
-// group's 51 matrix rows live in registers (pair elimination), so the
-// shared-memory footprint is the depth vectors and the pivot rows.
-using RtG = PairG;
+// One four-warp group (128 threads) per frequency, kRtGroups groups per CTA.
+// The group's 51x52 system lives in registers, spread block-cyclically over
+// its threads (scatter_solve_2d), so the shared-memory footprint is the
+// depth vectors and the pivot rows; depth loops cover 72 depths in one pass.
+using RtG = QuadG;
 constexpr int kRtGroups = 2;
 constexpr int kRtThreads = kRtGroups * RtG::N;
-constexpr int kRtMinBlocks = 3;
+constexpr int kRtMinBlocks = 2;
 
 // shared memory: RHOX and a zero vector (SIGMAL) for the CTA, then the groups' workspaces
 __host__ __device__ inline size_t rt_smem_bytes() { return 2 * sizeof(double) * kKwMax + kRtGroups * sizeof(RtWS); }

@@ -88,6 +88,9 @@ struct CoreArgs {
   unsigned int* nfar;    // [nj]
   int* tdiff;            // [nj][ntiles+1]
   int ntiles;
+  // work counters (timed launches only, else null): [0] Voigt evaluations,
+  // [1] far-wing bin updates the gather will make
+  unsigned long long* work = nullptr;
 };
 
 template <int G>
@@ -99,6 +102,7 @@ static __global__ void __launch_bounds__(256) k_core(CoreArgs a) {
   const int64_t npairs = a.n * a.nj;
   const int64_t gid0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
   const int64_t gstride = (int64_t)gridDim.x * blockDim.x / G;
+  unsigned long long nev = 0, nfw = 0;  // counted only when a.work is set
   for (int64_t p = gid0; p < npairs; p += gstride) {
     const int jj = (int)(p / a.n);
     const int64_t il = p - (int64_t)jj * a.n;
@@ -121,6 +125,7 @@ static __global__ void __launch_bounds__(256) k_core(CoreArgs a) {
     double* accj = a.acc + (size_t)j * a.length;
     if (g == 0 && nb >= 1 && nb <= a.length)
       atomicAdd(accj + nb - 1, kappa0 * voigt_weideman(0.0, adamp));
+    nev += (g == 0 && nb >= 1 && nb <= a.length);
     const double dv = 1.0 / dp / a.resolu;
     // With MAXPROF < n10dop the reference scatters only min(n10dop, maxstep)
     // core points when no point falls below kapmin; that limit is known only
@@ -133,6 +138,7 @@ static __global__ void __launch_bounds__(256) k_core(CoreArgs a) {
       const bool valid = s <= n10;
       double pv = 0.0;
       if (valid) pv = kappa0 * voigt_weideman((double)s * dv, adamp);
+      nev += valid;
       const unsigned below = __ballot_sync(gmask, valid && pv < kapmin) & gmask;
       int slim = n10;
       if (below) {
@@ -150,6 +156,7 @@ static __global__ void __launch_bounds__(256) k_core(CoreArgs a) {
       const int lim = nstop ? nstop : a.maxprof;
       for (int s = 1 + g; s <= lim; s += G) {
         const double pv = kappa0 * voigt_weideman((double)s * dv, adamp);
+        ++nev;
         const int r = nb + s, b = nb - s;
         if (r >= 1 && r <= a.length) atomicAdd(accj + r - 1, pv);
         if (b >= 1 && b <= a.length) atomicAdd(accj + b - 1, pv);
@@ -177,7 +184,21 @@ static __global__ void __launch_bounds__(256) k_core(CoreArgs a) {
         int* td = a.tdiff + (size_t)jj * (a.ntiles + 1);
         atomicAdd(td + (lo - 1) / kTile, 1);
         atomicAdd(td + (hi - 1) / kTile + 1, -1);
+        // bins n10 < |i - nb| <= maxstep inside the grid
+        const int r0 = max(nb + n10 + 1, 1), r1 = min(nb + maxstep, a.length);
+        const int b0 = max(nb - maxstep, 1), b1 = min(nb - n10 - 1, a.length);
+        nfw += (unsigned long long)(r1 >= r0 ? r1 - r0 + 1 : 0) + (unsigned long long)(b1 >= b0 ? b1 - b0 + 1 : 0);
       }
+    }
+  }
+  if (a.work) {
+    for (int o = 16; o > 0; o >>= 1) {
+      nev += __shfl_xor_sync(0xffffffffu, nev, o);
+      nfw += __shfl_xor_sync(0xffffffffu, nfw, o);
+    }
+    if (lane == 0) {
+      atomicAdd(a.work, nev);
+      atomicAdd(a.work + 1, nfw);
     }
   }
 }

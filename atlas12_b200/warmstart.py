@@ -140,7 +140,12 @@ class WarmStart:
         the plain grey starts of the same parameters, when the caller has
         them (the residual network adds to their log T and log P)."""
         params = np.atleast_2d(params)
-        y = self.mlp.forward(encode_inputs(params)).astype(np.float64) * self.ystd + self.ymean
+        return self.destandardise(self.mlp.forward(encode_inputs(params)), params, grey)
+
+    def destandardise(self, yn, params, grey=None):
+        """T, P, XNE [n, 72] from the network's standardised outputs yn [n, 216]."""
+        params = np.atleast_2d(params)
+        y = np.asarray(yn, np.float64) * self.ystd + self.ymean
         n = NRHOX
         if self.residual:
             if grey is None:
@@ -156,16 +161,7 @@ class WarmStart:
         """Starting structures on TAUSTD for every parameter set: T, P from
         the network, RHOX = P / g (one forward pass for all of them)."""
         params = np.atleast_2d(params)
-        t, p, xne = self.predict(params, grey)
-        out = []
-        for i, (teff, logg, mh, vturb) in enumerate(params):
-            ti = t[i].copy()
-            # the network's T need not be monotone; the iteration's own rule applies
-            for j in range(NRHOX - 2, -1, -1):
-                ti[j] = min(ti[j], ti[j + 1] - 1.0)
-            out.append(dict(t=np.maximum(ti, 1200.0), p=p[i], rhox=p[i] / 10.0 ** logg, tauros=TAUSTD.copy(),
-                            xne=xne[i]))
-        return out
+        return structures(params, *self.predict(params, grey))
 
     def start(self, teff, logg, mh, vturb):
         """Starting structure on TAUSTD for one parameter set."""
@@ -181,6 +177,20 @@ class WarmStart:
         mlp = MLP(ctx, shape=tuple(int(s) for s in d["shape"]))
         mlp.set_params(d["params"])
         return cls(mlp, d["ymean"], d["ystd"], bool(d["residual"]) if "residual" in d.files else False)
+
+
+def structures(params, t, p, xne):
+    """Starting structures on TAUSTD from predicted T, P, XNE [n, 72]: T made
+    monotone (each depth at least 1 K below the next, the iteration's own
+    rule) and floored at 1200 K, RHOX = P / g."""
+    out = []
+    for i, (teff, logg, mh, vturb) in enumerate(np.atleast_2d(params)):
+        ti = t[i].copy()
+        for j in range(NRHOX - 2, -1, -1):
+            ti[j] = min(ti[j], ti[j + 1] - 1.0)
+        out.append(dict(t=np.maximum(ti, 1200.0), p=p[i], rhox=p[i] / 10.0 ** logg, tauros=TAUSTD.copy(),
+                        xne=xne[i]))
+    return out
 
 
 _ross_cache = {}

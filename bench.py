@@ -23,9 +23,14 @@ public API from host buffers (batch creation with the line list upload,
 warm-start prediction, iteration, read-back of every structure).
 
 --impl reference times the CPU restatement of the same path (oracle/, the
-reference's own Fortran cannot be built in this image) on all host threads:
-each step is one full iteration of the grey-start solar model; models/hr
-uses the mean iteration count the plain method needs on the step's models.
+reference's own Fortran cannot be built in this image) on all host threads,
+on the same configuration: the step's 32 models from the same starting
+structures (the network's predictions evaluated on the host in FP64, grey
+where they are not usable), each iterated by the oracle until it converges
+or reaches 30 iterations.  A reference step is a bounded sample of that
+work -- 12 oracle iterations of the model queue, carried over from step to
+step -- and converged models/hr is measured on the models the timed steps
+complete: converged count x 3600 / the seconds spent on them.
 """
 import argparse
 import json
@@ -40,16 +45,17 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# mean iterations per model (converged or capped at 30) that the plain
-# grey-start method spends on the step's 32 models, and the fraction of them
-# it converges, measured on B200 by this bench's plain_fp64 arm; they turn the
-# reference arm's per-iteration time into converged models/hr
-PLAIN_ITERS_PER_MODEL = 29.6
-PLAIN_CONVERGED_FRACTION = 3.0 / 32.0  # measured: 3 of the 32 within 30 iterations
 CFG = dict(workload="atlas12-opacity-sampling model set", numnu=30000, wl_lo=9.0, wl_hi=160000.0, nrhox=72,
            nlines=500000, line_seed=2, models_per_step=32, param_seed=13,
            params="Teff U(3500,8000) K, log g U(1,5), [M/H] U(-2,0.5), vturb U(0.5,3) km/s", tol_percent=0.1,
-           max_iter=30, slots=32, vturb_solar=1.5)
+           max_iter=30, slots=32, vturb_solar=1.5,
+           # the surrogate's line populations are 0.01 of full strength (a
+           # purely radiative model with 500,000 full-strength lines has no
+           # reachable radiative-equilibrium solution from the grey start)
+           atlas_line_pop=0.01, populations="synthetic surrogate EOS and continuum",
+           start="learned warm start (trained network), grey where its structure is not usable")
+# oracle iterations per reference step (a bounded sample of the model queue)
+REF_ITERS_PER_STEP = 12
 WARMSTART = os.path.join(ROOT, "atlas12_b200", "data", "warmstart_c2.npz")
 # FP64 flops counted per frequency in the RT kernel: LU 2/3 51^3, triangular
 # solves 2*51^2, system build 2*51^2, J/H/K operators 4*51^2 + 2*51,
@@ -59,6 +65,11 @@ FLOPS_PER_NU = int(2 / 3 * 51 ** 3 + 8 * 51 ** 2 + 2 * 51 + 110 * 72)
 # workload at the tuned shape): ACONT, SIGMAC, XLINES read (52.7 MB) plus the
 # partial sums written (8.1 MB per model at 32 slots and 64 waves)
 RT_TRAFFIC_PER_MODEL = 60.8e6
+# bytes of one prepared LINOP1 line record on the device (AtlasLine)
+LINE_RECORD_BYTES = 56
+# FP64 operations of one SYNTHE Weideman Voigt evaluation (31 complex Horner
+# steps of 8, plus the setup and the closing terms)
+WEIDEMAN_FLOP = 278
 
 
 def parse():
@@ -69,7 +80,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 GPU comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--synthe-c3", action="store_true", help="also measure the 20M-line full-optical SYNTHE case")
+    ap.add_argument("--no-synthe-c3", action="store_true", help="skip the 20M-line full-optical SYNTHE case")
     ap.add_argument("--slots", type=int, default=None, help="batch slots (default: one per model of a step)")
     ap.add_argument("--no-select", action="store_true", help="skip the SELECTLINES line-database rates")
     ap.add_argument("--synthe-grid", type=int, default=0,
@@ -147,49 +158,135 @@ def dist_setup(args):
     return rank, world, local
 
 
+def host_starts(params, grey):
+    """The GPU arm's starting structures computed on the host: the trained
+    network evaluated in FP64 by the numpy restatement of the network
+    (oracle/mlp_ref.py), grey where its structure is not finite and positive."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import mlp_ref
+    from atlas12_b200 import warmstart
+    if not os.path.exists(WARMSTART):
+        return list(grey)
+    d = np.load(WARMSTART)
+    shape = tuple(int(x) for x in d["shape"])
+    ws = warmstart.WarmStart(None, d["ymean"], d["ystd"], bool(d["residual"]) if "residual" in d.files else False)
+    yn = mlp_ref.forward(d["params"].astype(np.float64), warmstart.encode_inputs(params), shape)[2]
+    out = []
+    for s_, g in zip(warmstart.structures(params, *ws.destandardise(yn, params, grey)), grey):
+        good = all(np.all(np.isfinite(s_[k])) and np.all(s_[k] > 0) for k in ("t", "p", "rhox"))
+        out.append(s_ if good else g)
+    return out
+
+
+class OracleQueue:
+    """The step's models on the CPU oracle, one after another: each from its
+    start until max |FLXERR| <= tol or max_iter iterations (the reference's
+    grid scripts run one model per process in the same way).  run(k) runs k
+    more oracle iterations of the queue and times each; a model's time is
+    the sum of its iterations'."""
+
+    def __init__(self, W, tables, starts):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po
+        from atlas12_b200 import atlas
+        self.po, self.atlas, self.W, self.tables, self.starts = po, atlas, W, tables, starts
+        self.next_model = 0
+        self.cur = None
+        self.done = []  # (model, converged, iterations, seconds)
+
+    def _open(self):
+        from iteration import OracleIteration
+        i = self.next_model % len(self.W["params"])
+        self.next_model += 1
+        teff, logg, mh, vt = self.W["params"][i]
+        it = OracleIteration(self.po, self.atlas, self.tables, self.W["ws"], self.W["rc"], self.W["lines"],
+                             self.starts[i], teff, vt, mh=mh, grav=10.0 ** logg)
+        self.cur = dict(model=i, it=it, n=0, sec=0.0)
+
+    def run(self, k):
+        for _ in range(k):
+            if self.cur is None:
+                self._open()
+            c = self.cur
+            t0 = time.perf_counter()
+            err = c["it"].step()
+            c["sec"] += time.perf_counter() - t0
+            c["n"] += 1
+            conv = bool(err <= CFG["tol_percent"])
+            if conv or not np.isfinite(err) or c["n"] >= CFG["max_iter"]:
+                self.done.append((c["model"], conv, c["n"], c["sec"]))
+                self.cur = None
+
+    def rate(self):
+        """(converged models/hr over the completed models, completed, converged, seconds, iterations)."""
+        sec = sum(d[3] for d in self.done)
+        conv = sum(d[1] for d in self.done)
+        its = sum(d[2] for d in self.done)
+        return (conv * 3600.0 / sec if sec > 0 else 0.0), len(self.done), conv, sec, its
+
+
 def run_reference(args):
-    """CPU restatement of the same path on all host threads."""
+    """The CPU restatement of the same path on all host threads, on the
+    same models and starting structures as the GPU arm (rank 0 only)."""
     rank, world, local = dist_setup(args)
     if rank != 0:
         return 0
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle as po
-    from atlas12_b200 import atlas
-    W = workload()
-    t = operators()
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    step = oracle_iteration_factory(po, atlas, t, W)
-    for _ in range(args.warmup):
-        step()
+    W = workload()
+    starts = host_starts(W["params"], W["grey"])
+    q = OracleQueue(W, operators(), starts)
+    q.run(max(args.warmup, 1))  # warm-up: the first iterations (threads, caches); the queue restarts after
+    q = OracleQueue(W, operators(), starts)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        step()
+        q.run(REF_ITERS_PER_STEP)
         times.append(time.perf_counter() - t0)
-    t_it = float(np.mean(times))
-    v = 3600.0 * PLAIN_CONVERGED_FRACTION / (t_it * PLAIN_ITERS_PER_MODEL)
+    v, ncomp, nconv, sec, its = q.rate()
+    sample = (f"{args.steps} steps of {REF_ITERS_PER_STEP} oracle iterations over the step's model queue (same 32 "
+              f"models and starting structures as the GPU arm, each to max|FLXERR| <= 0.1 % or 30 iterations): "
+              f"{ncomp} models completed, {nconv} converged, {its} iterations in {sec:.1f} s on "
+              f"{os.environ['OMP_NUM_THREADS']} threads")
     line = {"impl": "reference", "metric": "converged models/hr (dF/F<=1e-3)", "value": v, "unit": "models/hr",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_it * 1e3,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": float(np.mean(times)) * 1e3 if times else None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(CFG, parallelism="host threads", flush="host"),
+            "config": dict(CFG, parallelism=f"replicas x{args.gpus}"),
+            "execution": "CPU oracle (C restatement of the reference's iteration), OpenMP over the host threads",
             "cpu_baseline": {"value": v, "unit": "models/hr", "cores": int(os.environ["OMP_NUM_THREADS"]),
-                             "kind": "port",
-                             "sample": f"one full ATLAS12 iteration per step (LINOP1 + 30,000-frequency RT pass + "
-                                       f"TCORR(3)) of the grey-start solar model on the host; converged models/hr "
-                                       f"= 3600 x {PLAIN_CONVERGED_FRACTION:.4f} / (t_iteration x "
-                                       f"{PLAIN_ITERS_PER_MODEL} iterations per model): the grey-start method's "
-                                       f"converged fraction and iterations on the step's models)"},
+                             "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "models/hr", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def oracle_iteration_factory(po, atlas, tables, W):
-    """One ATLAS12 iteration of the oracle on the grey-start solar model (state carried)."""
-    from iteration import OracleIteration
-    it = OracleIteration(po, atlas, tables, W["ws"], W["rc"], W["lines"], W["solar"], 5777.0, CFG["vturb_solar"])
-    return it.step
+def atlas_mixed_error(ctx, batch, params, starts):
+    """One step of the same models from the same starts in all-FP64 and in
+    mixed precision: how many converge each way, and for the models that
+    converge both ways the largest relative T and P difference and the
+    largest FLXERR difference (percent points) of the converged structures."""
+    from atlas12_b200 import _lib
+    out = {}
+    res = {}
+    for name, prec in (("fp64", _lib.PREC_FP64), ("mixed", _lib.PREC_MIXED)):
+        ctx.set_precision(prec)
+        res[name] = batch.run_queue(params, starts, max_iter=CFG["max_iter"], tol_percent=CFG["tol_percent"],
+                                    keep=True)
+    ctx.set_precision(_lib.PREC_MIXED)
+    conv = {k: [r["status"] == _lib.SLOT_CONVERGED for r in v] for k, v in res.items()}
+    both = [i for i in range(len(params)) if conv["fp64"][i] and conv["mixed"][i]]
+    out["converged_fp64"] = int(sum(conv["fp64"]))
+    out["converged_mixed"] = int(sum(conv["mixed"]))
+    out["compared"] = len(both)
+    if both:
+        a, b = res["mixed"], res["fp64"]
+        out["max_rel_T"] = float(max(np.max(np.abs(a[i]["t"] / b[i]["t"] - 1)) for i in both))
+        out["max_rel_P"] = float(max(np.max(np.abs(a[i]["p"] / b[i]["p"] - 1)) for i in both))
+        out["max_abs_flxerr_percent"] = float(max(np.max(np.abs(a[i]["flxerr"] - b[i]["flxerr"])) for i in both))
+        out["iterations_fp64"] = int(sum(b[i]["iters"] for i in both))
+        out["iterations_mixed"] = int(sum(a[i]["iters"] for i in both))
+    return out
 
 
 def warm_starts(ctx, params, grey):
@@ -275,6 +372,7 @@ def run_ours(args):
     batch.step(1)
     names = ("eos", "kapcont", "kapp", "linop", "rt", "reduce", "finish")
     kms = {k: ctx.kernel_ms("batch_" + k) for k in names}
+    linop_points = ctx.kernel_work("batch_linop_points")
     ctx.enable_timing(False)
     batch.run()
     per_model = {k: v / CFG["slots"] for k, v in kms.items()}
@@ -288,6 +386,22 @@ def run_ours(args):
             "peak_source": "measured DFMA loop on this GPU (atlasgpu_fp64_peak_tflops); MEASURED_PEAKS.json has no FP64 figure",
             "work": f"{FLOPS_PER_NU} FP64 flop per frequency x {CFG['numnu']} frequencies x {CFG['slots']} models per launch",
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_batch_rt launch (profiles/)"}
+    # LINOP1 over the batch: wing points added into XLINES per second, and the
+    # algorithmic bytes (prepared line records read once per slot, XLINES
+    # read and written once) against HBM
+    hbm, hbm_src = hbm_peak()
+    linop_bytes = CFG["slots"] * (CFG["nlines"] * LINE_RECORD_BYTES + 2 * 8 * CFG["numnu"] * CFG["nrhox"])
+    rooflines = [{"kernel": "k_batch_linop (LINOP1 wing walks)", "bound": "hbm", "unit": "GB/s",
+                  "achieved": linop_bytes / (kms["linop"] * 1e-3) / 1e9, "peak": hbm, "peak_source": hbm_src,
+                  "frac": linop_bytes / (kms["linop"] * 1e-3) / 1e9 / hbm,
+                  "points_per_s": linop_points / (kms["linop"] * 1e-3) if linop_points > 0 else None,
+                  "points": linop_points,
+                  "work": f"{LINE_RECORD_BYTES} B per prepared line x {CFG['nlines']} lines + XLINES "
+                          f"({CFG['numnu']} x {CFG['nrhox']} FP64) read and written, per slot"}]
+
+    # ATLAS mixed precision against the plain all-FP64 arithmetic on the same
+    # models from the same starts (north star (1)): converged structures
+    mx_err = atlas_mixed_error(ctx, batch, params, starts)
 
     # plain FP64 GPU path: the same models one at a time, FP64, grey start, per-launch host loop
     plain = None
@@ -358,10 +472,11 @@ def run_ours(args):
     syn = None
     if rank == 0 and world == 1:
         # C1: 20,000 atomic lines, 400-410 nm at R = 500,000, 72 depths
-        syn = {"c1": synthe_rates(ctx, ops, 20000, 400.0, 410.0, 0.0)}
-        if args.synthe_c3:
+        syn = {"c1": synthe_rates(ctx, ops, 20000, 400.0, 410.0, 0.0, fp64_peak=fp64_peak)}
+        if not args.no_synthe_c3:
             # C3: 20M lines (30 % molecular), 300-1000 nm at R = 500,000
-            syn["c3"] = synthe_rates(ctx, ops, 20000000, 300.0, 1000.0, 0.3)
+            syn["c3"] = synthe_rates(ctx, ops, 20000000, 300.0, 1000.0, 0.3, fp64_peak=fp64_peak)
+            rooflines += syn["c3"]["rooflines"]
         if args.synthe_grid:
             syn["grid"] = synthe_grid_rate(local, ops, args.synthe_grid)
 
@@ -371,20 +486,21 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(W, ops, plain["mean_iterations"] if plain else PLAIN_ITERS_PER_MODEL,
-                           plain["converged"] / plain["models"] if plain else PLAIN_CONVERGED_FRACTION)
+        cpu = cpu_baseline(W, ops, starts, sum(iters) / args.steps, converged / args.steps)
     if rank == 0:
         line = {"metric": "converged models/hr (dF/F<=1e-3)", "value": value, "unit": "models/hr",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded lines and stellar parameters, surrogate populations/continuum)",
                 "launch_shape": {"linop_ctas_per_sm": lc, "rt_waves": rw, "autotune": tuned},
-                "config": dict(CFG, parallelism=f"replicas x{world}", start="learned warm start, grey fallback"
-                               if learned else "grey (no trained network found)",
-                               l2="flushed between steps (256 MB write)"),
+                "config": dict(CFG, parallelism=f"replicas x{world}"),
+                "execution": "batched models (one captured graph per iteration), mixed-precision LINOP1, FP64 "
+                             "transfer" + ("" if learned else "; no trained network found: grey starts"),
+                "l2": "flushed between steps (256 MB write)",
                 "converged_per_step": float(conv_all.item()) / args.steps / world,
                 "mean_iterations_per_model": float(np.mean(iters)),
-                "kernel_ms_per_model_iteration": per_model, "roofline": roof, "cpu_baseline": cpu,
+                "kernel_ms_per_model_iteration": per_model, "roofline": roof, "rooflines": rooflines,
+                "atlas": {"mixed_error_vs_fp64": mx_err}, "cpu_baseline": cpu,
                 "plain_fp64": plain, "vs_plain_fp64": (value / plain["value"]) if plain and plain["value"] else None,
                 "single_model": single, "synthe": syn, "selectlines": sel,
                 "e2e": {"value": e2e_value, "unit": "models/hr", "h2d_bytes_per_step": int(h2d),
@@ -475,11 +591,14 @@ def selectlines_rates(ctx, ops, cpu=True, reps=3):
     return out
 
 
-def synthe_rates(ctx, ops, nlines, wlbeg, wlend, mol_frac, seed=1):
+def synthe_rates(ctx, ops, nlines, wlbeg, wlend, mol_frac, seed=1, fp64_peak=None):
     """SYNTHE line opacity and spectrum on a synthetic case (CUDA events in the
     library, second run of each precision): line-depth evaluations per second
     of the line-opacity kernels (binning and continuum excluded) in mixed
-    precision and all-FP64, and the spectrum's two JOSH solves per lambda."""
+    precision and all-FP64, and the spectrum's two JOSH solves per lambda.
+    Rooflines (mixed precision): the core pass against the FP64 pipe (counted
+    Weideman evaluations x 278 flop), and the far-wing gather's bin updates
+    per second."""
     from atlas12_b200 import _lib, synthe, synthetic
     case = synthetic.synthe_case(nlines=nlines, wlbeg=wlbeg, wlend=wlend, seed=seed, mol_frac=mol_frac)
     S = synthe.Synthe(ctx, ops)
@@ -492,10 +611,11 @@ def synthe_rates(ctx, ops, nlines, wlbeg, wlend, mol_frac, seed=1):
         _, flux, _, op = S.run(case)
         res[name] = (flux, op)
         ms = {k: ctx.kernel_ms(k) for k in ("synthe_core", "synthe_farfill", "synthe_farwing", "josh_spectrum")}
+        work = {k: ctx.kernel_work(k) for k in ("synthe_voigt_evals", "synthe_farwing_updates")}
         ctx.enable_timing(False)
         line_ms = ms["synthe_core"] + ms["synthe_farfill"] + ms["synthe_farwing"]
         out[name] = {"line_depth_evals_per_s": nlines * 72 / (line_ms * 1e-3), "line_opacity_ms": line_ms,
-                     "spectrum_ms": ms["josh_spectrum"], "kernel_ms": ms}
+                     "spectrum_ms": ms["josh_spectrum"], "kernel_ms": ms, "work": work}
         out["points"] = int(flux.size)
     ctx.set_precision(_lib.PREC_MIXED)
     out["mixed_vs_fp64_line_opacity"] = out["fp64"]["line_opacity_ms"] / out["mixed"]["line_opacity_ms"]
@@ -506,6 +626,21 @@ def synthe_rates(ctx, ops, nlines, wlbeg, wlend, mol_frac, seed=1):
         "kappa_line_max_rel_to_kappa_plus_cont": float(np.max(np.abs(om.astype(np.float64) - o64) /
                                                               (o64.astype(np.float64) + cont))),
         "flux_max_rel": float(np.max(np.abs(fm - f64) / np.abs(f64)))}
+    m = out["mixed"]
+    tag = f"{nlines // 1000000}M lines" if nlines >= 1000000 else f"{nlines // 1000}k lines"
+    rl = []
+    if m["work"]["synthe_voigt_evals"] > 0 and m["kernel_ms"]["synthe_core"] > 0:
+        ach = m["work"]["synthe_voigt_evals"] * WEIDEMAN_FLOP / (m["kernel_ms"]["synthe_core"] * 1e-3) / 1e12
+        rl.append({"kernel": f"k_core (SYNTHE Weideman core, {tag})", "bound": "fp64", "unit": "TFLOP/s",
+                   "achieved": ach, "peak": fp64_peak, "frac": ach / fp64_peak if fp64_peak else None,
+                   "peak_source": "measured DFMA loop on this GPU (atlasgpu_fp64_peak_tflops)",
+                   "work": f"{int(m['work']['synthe_voigt_evals'])} Voigt evaluations x {WEIDEMAN_FLOP} flop"})
+    if m["work"]["synthe_farwing_updates"] > 0 and m["kernel_ms"]["synthe_farwing"] > 0:
+        rl.append({"kernel": f"k_farwing (SYNTHE far-wing gather, {tag})", "bound": "issue",
+                   "unit": "bin updates/s",
+                   "achieved": m["work"]["synthe_farwing_updates"] / (m["kernel_ms"]["synthe_farwing"] * 1e-3),
+                   "work": f"{int(m['work']['synthe_farwing_updates'])} far-wing bin updates (x/n^2 terms)"})
+    out["rooflines"] = rl
     return out
 
 
@@ -539,25 +674,31 @@ def synthe_grid_rate(device, ops, n, lanes=8):
             "timing": "host wall clock around the public API calls (host inputs, host outputs)"}
 
 
-def cpu_baseline(W, ops_t, iters_gpu, conv_fraction):
-    """The oracle on the host: two iterations of the grey-start solar model,
-    all host threads; converged models/hr with the grey-start method's
-    converged fraction and iterations per model on the step's models."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle as po
-    from atlas12_b200 import atlas
+def cpu_baseline(W, ops_t, starts, step_iters, step_converged, steps=2):
+    """The oracle on the host cores on a bounded sample of the same work:
+    `steps` reference steps (12 oracle iterations each) of the step's model
+    queue from the GPU arm's starting structures, all host threads.  The
+    sample gives the oracle's seconds per model iteration; the step's own
+    work (the iterations and converged models the GPU arm's step ran, the
+    same iteration within the parity tolerances) at that rate gives
+    converged models/hr."""
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    step = oracle_iteration_factory(po, atlas, ops_t, W)
-    step()
+    q = OracleQueue(W, ops_t, starts)
+    q.run(1)  # warm-up
+    q = OracleQueue(W, ops_t, starts)
     t0 = time.perf_counter()
-    step()
-    t_it = time.perf_counter() - t0
-    return {"value": 3600.0 * conv_fraction / (t_it * iters_gpu), "unit": "models/hr",
-            "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
-            "sample": f"one ATLAS12 iteration on the host ({t_it:.2f} s); converged models/hr = 3600 x "
-                      f"{conv_fraction:.4f} (converged fraction of the grey-start method within 30 iterations) / "
-                      f"({iters_gpu:.1f} iterations per model x t_iteration)"}
+    q.run(steps * REF_ITERS_PER_STEP)
+    dt = time.perf_counter() - t0
+    t_it = dt / (steps * REF_ITERS_PER_STEP)
+    v = step_converged * 3600.0 / (t_it * step_iters) if step_iters else 0.0
+    _, ncomp, nconv, _, _ = q.rate()
+    return {"value": v, "unit": "models/hr", "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
+            "seconds_per_iteration": t_it,
+            "sample": f"{steps * REF_ITERS_PER_STEP} oracle iterations of the step's model queue from the same "
+                      f"starts ({dt:.1f} s, {t_it:.3f} s per iteration; {ncomp} models completed, {nconv} "
+                      f"converged); converged models/hr = the step's {step_converged:g} converged models x 3600 / "
+                      f"(its {step_iters:g} model iterations x the oracle's seconds per iteration)"}
 
 
 def main():

@@ -106,6 +106,13 @@ int64_t atlasgpu_launch_count(atlasgpu_ctx *ctx);
  * only while enabled. */
 int atlasgpu_enable_timing(atlasgpu_ctx *ctx, int on);
 double atlasgpu_kernel_ms(atlasgpu_ctx *ctx, const char *name);
+/* Algorithmic work units counted by the last timed launch of a kernel
+ * family while timing is enabled, or -1: "synthe_voigt_evals" (SYNTHE core
+ * Voigt evaluations), "synthe_farwing_updates" (far-wing bin updates),
+ * "atlas_linop_points" (LINOP1 wing points added into XLINES), and the
+ * batched iteration's "batch_linop_points".  No reference counterpart:
+ * these are the numerators of the kernels' rooflines. */
+double atlasgpu_kernel_work(atlasgpu_ctx *ctx, const char *name);
 
 /* JOSH operator set: BLOCKJ/BLOCKH matrices (atlas12_modules.f90:18792-18860)
  * plus JOSH's fixed 51-point tau grid XTAU8 and surface weights CH_J, CK_J
