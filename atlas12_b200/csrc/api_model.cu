@@ -484,17 +484,29 @@ int atlasgpu_model_set_structure(atlasgpu_ctx* ctx, atlasgpu_model* m, const dou
   if (!ctx || !m || !t || !p || !rhox) return fail(ctx, ATLASGPU_EINVAL, "model_set_structure: null");
   cudaSetDevice(ctx->device);
   const int kw = m->kw;
+  CK(cudaStreamSynchronize(ctx->stream));
+  // a fresh model, as atlasgpu_model_create leaves it: every state vector
+  // zero except T, RHOX, P, VTURB (kept) and TAUROS = TAUSTD, so nothing of
+  // the previous model (or of a failed, non-finite one) carries over
   std::vector<double> h(kNState * kw);
   CK(cudaMemcpy(h.data(), m->state, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int q = 0; q < kNState; ++q)
+    if (q != 6)
+      for (int j = 0; j < kw; ++j) h[q * kw + j] = 0.0;
   for (int j = 0; j < m->nrhox; ++j) {
     h[0 * kw + j] = t[j];
     h[1 * kw + j] = rhox[j];
     h[2 * kw + j] = p[j];
-    h[5 * kw + j] = 0.0;   // PRAD
-    h[11 * kw + j] = 0.0;  // OLDT1
     h[8 * kw + j] = pow(10.0, -6.875 + 0.125 * j);
   }
   CK(cudaMemcpy(m->state, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  {
+    ModelState ms;
+    CK(cudaMemcpy(&ms, m->ms, sizeof ms, cudaMemcpyDeviceToHost));
+    ms.pradk0 = 0.0;
+    ms.maxerr = 0.0;
+    CK(cudaMemcpy(m->ms, &ms, sizeof ms, cudaMemcpyHostToDevice));
+  }
   CK(cudaMemset(m->iter_dev, 0, sizeof(int)));
   m->kapcont_done = false;  // KAPCONT runs again on the new structure's first iteration
   RossStore R0{0, kRossMax, 0.0, 1.0, 0.0, 1.0, m->ross, m->ross + kRossMax, m->ross + 2 * kRossMax};

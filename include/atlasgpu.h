@@ -452,8 +452,10 @@ int atlasgpu_model_get(atlasgpu_ctx *ctx, atlasgpu_model *m, double *t, double *
  * driver holds in the module arrays TABCONT and XLINES after RUN_RT_PASS. */
 int atlasgpu_model_get_tables(atlasgpu_ctx *ctx, atlasgpu_model *m, double *tabcont, double *xlines,
                               double *acont, double *sigmac);
-/* Overwrite the structure (T, P, RHOX [nrhox]) and restart the iteration
- * count (a warm start). */
+/* Start the model again from a structure (T, P, RHOX [nrhox]), a warm
+ * start: every other state vector (except VTURB), the ROSSTAB history, the
+ * iteration count and KAPCONT's table start afresh, as after
+ * atlasgpu_model_create, so nothing of the previous model carries over. */
 int atlasgpu_model_set_structure(atlasgpu_ctx *ctx, atlasgpu_model *m, const double *t,
                                  const double *p, const double *rhox);
 /* New stellar parameters for the next model on the same line list and grid
