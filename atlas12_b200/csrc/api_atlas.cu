@@ -262,11 +262,28 @@ int atlasgpu_atlas_linop(atlasgpu_ctx* ctx, const int32_t* linedata, int64_t n, 
                 (const double*)ctx->bufs["tab_h0"].first, (const double*)ctx->bufs["tab_h1"].first,
                 (const double*)ctx->bufs["tab_h2"].first, (const float4*)ctx->bufs["tab_hf"].first, d_xl, d_cnt,
                 d_cnt + 1};
+    // exact fixed-point sums (fix_add): per-species CGF maxima, per-depth scales
+    unsigned long long *d_fix, *d_cgf;
+    double *d_fs, *d_fu;
+    if ((r = bufT(ctx, "al_fix", (size_t)kFixWords * kw * numnu, &d_fix)) || (r = bufT(ctx, "al_cgf", nspec, &d_cgf)) ||
+        (r = bufT(ctx, "al_fs", kw, &d_fs)) || (r = bufT(ctx, "al_fu", kw, &d_fu)))
+      return r;
+    CK(cudaMemsetAsync(d_fix, 0, (size_t)kFixWords * kw * numnu * sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(d_cgf, 0, (size_t)nspec * sizeof(unsigned long long), s));
+    k_cgf_max<<<grid_for(ctx, n, 256, 8), 256, 0, s>>>(d_lines, n, nspec, d_cgf);
+    CKL(ctx);
+    k_fix_scale<<<1, 128, 0, s>>>(d_xd, nspec, kw, nrhox, (const double*)d_cgf, d_fs, d_fu);
+    CKL(ctx);
+    a.xfix = d_fix;
+    a.fscale = d_fs;
     a.work = work_counters(ctx, 1);
     {
       Timer tm(ctx, "atlas_linop");
       if (ctx->precision == ATLASGPU_PREC_MIXED) k_atlas_linop<true><<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
       else k_atlas_linop<false><<<grid_for(ctx, n * 32, 256, 16), 256, 0, s>>>(a);
+      CKL(ctx);
+      k_fix_finalize<<<grid_for(ctx, (int64_t)numnu * nrhox, 256, 8), 256, 0, s>>>(d_fix, d_fu, numnu, nrhox, kw,
+                                                                                     d_xl);
       CKL(ctx);
     }
     work_collect(ctx, a.work, {"atlas_linop_points"});

@@ -44,6 +44,9 @@ struct BatchDev {
   double *xne_eos, *txnxn, *hkt, *hckt, *rho;  // [B][kw]
   ContCoef* cc;                                // [B][kw]
   double *acont, *sigmac, *xl;                 // [B][numnu][kw]
+  unsigned long long* xfix;                    // [B][numnu][3][kw] LINOP1's exact sums
+  double *fscale, *funscale;                   // [B][kw] their per-depth scale
+  const double* cgfmax;                        // [nspec] largest CGF per species (shared line list)
   double* tabcont;                             // [B][nwave+1][kw]
   double* partial;                             // [B][nwl][kAcc*kw+1]
   double* sum;                                 // [B][kAcc*kw+1]
@@ -62,6 +65,15 @@ __global__ void k_batch_eos(BatchDev d) {
   const size_t o = (size_t)b * d.kw, os = (size_t)b * d.nspec * d.kw;
   model_eos_depth(d.ms + b, c.iter + 1, j, d.kw, c.grav, c.vturb_cms, c.mh, d.xnfdop + os, d.dopple + os,
                   d.xne_eos + o, d.txnxn + o, d.hkt + o, d.hckt + o, d.rho + o, d.cc + o);
+  fix_scale_depth(d.xnfdop + os, d.nspec, d.kw, j, d.cgfmax, d.fscale + o, d.funscale + o);
+}
+
+// XLINES of every running slot from its fixed-point sums
+__global__ void k_batch_fixfin(BatchDev d) {
+  const int b = blockIdx.y;
+  if (!running(d.ctl, b)) return;
+  const size_t on = (size_t)b * d.numnu * d.kw;
+  fix_finalize_range(d.xfix + kFixWords * on, d.funscale + (size_t)b * d.kw, d.numnu, d.nrhox, d.kw, d.xl + on);
 }
 
 // KAPCONT on a slot's first iteration only (atlas12c.f90:562)
@@ -193,6 +205,11 @@ int enqueue_batch(atlasgpu_ctx* ctx, atlasgpu_batch* B, bool timed) {
       CKL(ctx);
     }
     work_collect(ctx, work, {"batch_linop_points"});
+    {
+      Timer tm(ctx, "batch_fixfin");
+      k_batch_fixfin<<<dim3(B->grid_kapp, nb), 256, 0, s>>>(B->d);
+      CKL(ctx);
+    }
   }
   {
     Timer tm(ctx, "batch_rt");
@@ -269,7 +286,8 @@ int atlasgpu_batch_destroy(atlasgpu_ctx* ctx, atlasgpu_batch* B) {
   if (B->gexec) cudaGraphExecDestroy(B->gexec);
   if (B->graph) cudaGraphDestroy(B->graph);
   const BatchDev& d = B->d;
-  void* ps[] = {d.ctl, d.ms, d.R, d.xnfdop, d.dopple, d.xne_eos, d.txnxn, d.hkt, d.hckt, d.rho, d.cc, d.acont,
+  void* ps[] = {d.xfix, d.fscale, d.funscale, (void*)d.cgfmax,
+                d.ctl, d.ms, d.R, d.xnfdop, d.dopple, d.xne_eos, d.txnxn, d.hkt, d.hckt, d.rho, d.cc, d.acont,
                 d.sigmac, d.xl, d.tabcont, d.partial, d.sum, d.hist, d.hsurf, B->waveset, B->rcoset, B->cutwave, B->h0,
                 B->h1, B->h2, B->hf, B->ross, B->state, B->iwavetab, B->linedata, B->lines, B->la, B->ra, B->cnt};
   for (void* p : ps)
@@ -324,7 +342,9 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
       (r = balloc(ctx, &B->h1, 2001)) || (r = balloc(ctx, &B->h2, 2001)) || (r = balloc(ctx, &B->hf, 2001)) ||
       (r = balloc(ctx, &B->ross, (size_t)nb * 3 * kRossMax)) || (r = balloc(ctx, &B->state, (size_t)nb * kNState * kw)) ||
       (r = balloc(ctx, &B->linedata, (size_t)B->nlines * 4)) || (r = balloc(ctx, &B->lines, (size_t)B->nlines)) ||
-      (r = balloc(ctx, &B->la, nb)) || (r = balloc(ctx, &B->ra, nb)) || (r = balloc(ctx, &B->cnt, 2))) {
+      (r = balloc(ctx, &B->la, nb)) || (r = balloc(ctx, &B->ra, nb)) || (r = balloc(ctx, &B->cnt, 2)) ||
+      (r = balloc(ctx, &d.xfix, (size_t)kFixWords * nb * nnk)) || (r = balloc(ctx, &d.fscale, (size_t)nb * kw)) ||
+      (r = balloc(ctx, &d.funscale, (size_t)nb * kw)) || (r = balloc(ctx, (double**)&d.cgfmax, (size_t)B->nspec))) {
     atlasgpu_batch_destroy(ctx, B);
     return r;
   }
@@ -360,6 +380,8 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
     la[b] = LinopArgs{B->lines, B->nlines, B->nrhox, kw, B->nspec, B->numnu, d.xnfdop + os, d.dopple + os,
                       d.xne_eos + o, d.txnxn + o, d.hckt + o, d.tabcont + (size_t)b * (B->nwave + 1) * kw,
                       B->waveset, B->h0, B->h1, B->h2, B->hf, d.xl + on, nullptr, B->cnt};
+    la[b].xfix = d.xfix + kFixWords * on;
+    la[b].fscale = d.fscale + o;
     ra[b] = RtArgs{ctx->ops, B->numnu, B->nrhox, kw, B->waveset, B->rcoset, d.acont + on, d.sigmac + on, nullptr,
                    d.xl + on, ms[b].rhox, ms[b].t, d.hkt + o, 0.0, 1, 1, kw, nullptr,
                    d.hsurf + (size_t)b * B->numnu, nullptr};
@@ -414,6 +436,14 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
                                               dsc->waveset, B->numnu, B->iwavetab, B->nwave, B->nspec, B->lines))) {
     atlasgpu_batch_destroy(ctx, B);
     return r;
+  }
+  // exact XLINES sums: zeroed words, the largest CGF per species for the scales
+  CK(cudaMemsetAsync(d.xfix, 0, (size_t)kFixWords * nb * nnk * sizeof(unsigned long long), s));
+  CK(cudaMemsetAsync((void*)d.cgfmax, 0, (size_t)B->nspec * sizeof(double), s));
+  if (B->nlines > 0) {
+    k_cgf_max<<<grid_for(ctx, B->nlines, 256, 8), 256, 0, s>>>(B->lines, B->nlines, B->nspec,
+                                                                (unsigned long long*)d.cgfmax);
+    CKL(ctx);
   }
   CK(cudaStreamSynchronize(s));
   if ((r = apply_shape(ctx, B, B->linop_ctas_per_sm, B->rt_waves))) {
@@ -514,7 +544,7 @@ int atlasgpu_batch_step(atlasgpu_ctx* ctx, atlasgpu_batch* B, int n) {
       ctx->launches = l0;  // counted when replayed
     }
     CK(cudaGraphLaunch(B->gexec, s));
-    ctx->launches += B->nlines > 0 ? 7 : 6;
+    ctx->launches += B->nlines > 0 ? 8 : 6;
   }
   return 0;
 }

@@ -26,6 +26,9 @@ struct atlasgpu_model {
   int32_t* linedata;
   AtlasLine* lines;
   double* xl;            // XLINES(J, NU): [numnu][kw]
+  unsigned long long* xfix;  // LINOP1's exact fixed-point sums [numnu][3][kw]
+  double *fscale, *funscale;  // their per-depth scale [kw]
+  unsigned long long* cgfmax;  // largest CGF per species [nspec] (FP64 bit patterns)
   double *partial, *sum, *hsurf;
   double *h0, *h1, *h2, *ross;  // ross: ROSSTAB points [3][kRossMax]
   float4* hf;                    // FP32 (H0, H1, H2, 0)
@@ -48,11 +51,13 @@ namespace {
 // hydrostatics (iteration > 1), surrogate EOS / populations, Planck factors
 __global__ void k_model_eos(ModelState* ms, const int* iter_dev, int nrhox, int kw, double grav,
                             double vturb_cms, double mh, double* xnfdop, double* dopple, double* xne_eos,
-                            double* txnxn, double* hkt, double* hckt, double* rho, ContCoef* cc) {
+                            double* txnxn, double* hkt, double* hckt, double* rho, ContCoef* cc, int nspec,
+                            const double* cgfmax, double* fscale, double* funscale) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nrhox) return;
   model_eos_depth(ms, *iter_dev + 1, j, kw, grav, vturb_cms, mh, xnfdop, dopple, xne_eos, txnxn, hkt, hckt, rho,
                   cc);
+  fix_scale_depth(xnfdop, nspec, kw, j, cgfmax, fscale, funscale);
 }
 
 // KAPCONT (atlas12_modules.f90:19072-19138) on the surrogate continuum
@@ -124,7 +129,8 @@ int enqueue_begin(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
     Timer tm(ctx, "model_eos");
     k_model_eos<<<1, 128, 0, s>>>(m->ms, m->iter_dev, m->nrhox, m->kw, m->grav, m->vturb * 1.0e5, m->mh,
                                   m->xnfdop,
-                                  m->dopple, m->xne_eos, m->txnxn, m->hkt, m->hckt, m->rho, m->cc);
+                                  m->dopple, m->xne_eos, m->txnxn, m->hkt, m->hckt, m->rho, m->cc, m->nspec,
+                                  (const double*)m->cgfmax, m->fscale, m->funscale);
     CKL(ctx);
   }
   if (!m->kapcont_done) {
@@ -132,18 +138,23 @@ int enqueue_begin(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
                                              m->cc, m->tabcont);
     CKL(ctx);
   }
-  CK(cudaMemsetAsync(m->xl, 0, (size_t)m->kw * m->numnu * sizeof(double), s));
+  if (m->nlines == 0) CK(cudaMemsetAsync(m->xl, 0, (size_t)m->kw * m->numnu * sizeof(double), s));
   if (m->nlines > 0) {
     LinopArgs la{m->lines, m->nlines, m->nrhox, m->kw, m->nspec, m->numnu, m->xnfdop, m->dopple,
                  m->xne_eos, m->txnxn, m->hckt, m->tabcont, m->waveset, m->h0, m->h1, m->h2, m->hf, m->xl,
                  nullptr, m->cnt, m->nu_first, m->nu_last};
     la.work = work_counters(ctx, 1);
+    la.xfix = m->xfix;
+    la.fscale = m->fscale;
     {
       Timer tm(ctx, "atlas_linop");
       if (ctx->precision == ATLASGPU_PREC_MIXED)
         k_atlas_linop<true><<<grid_for(ctx, m->nlines * 32, 256, 16), 256, 0, s>>>(la);
       else
         k_atlas_linop<false><<<grid_for(ctx, m->nlines * 32, 256, 16), 256, 0, s>>>(la);
+      CKL(ctx);
+      k_fix_finalize<<<grid_for(ctx, (int64_t)m->numnu * m->nrhox, 256, 8), 256, 0, s>>>(
+          m->xfix, m->funscale, m->numnu, m->nrhox, m->kw, m->xl);
       CKL(ctx);
     }
     work_collect(ctx, la.work, {"atlas_linop_points"});
@@ -296,6 +307,8 @@ int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlas
       (r = dalloc(ctx, &m->cutwave, m->nwave)) || (r = dalloc(ctx, &m->tabcont, (size_t)(m->nwave + 1) * kw)) ||
       (r = dalloc(ctx, &m->iwavetab, m->nwave + 1)) || (r = dalloc(ctx, &m->linedata, (size_t)m->nlines * 4)) ||
       (r = dalloc(ctx, &m->lines, (size_t)m->nlines)) || (r = dalloc(ctx, &m->xl, (size_t)kw * m->numnu)) ||
+      (r = dalloc(ctx, &m->xfix, (size_t)kFixWords * kw * m->numnu)) || (r = dalloc(ctx, &m->fscale, kw)) ||
+      (r = dalloc(ctx, &m->funscale, kw)) || (r = dalloc(ctx, &m->cgfmax, (size_t)m->nspec)) ||
       (r = dalloc(ctx, &m->sum, kAcc * kw + 1)) ||
       (r = dalloc(ctx, &m->hsurf, m->numnu)) || (r = dalloc(ctx, &m->h0, 2001)) || (r = dalloc(ctx, &m->h1, 2001)) ||
       (r = dalloc(ctx, &m->h2, 2001)) || (r = dalloc(ctx, &m->hf, 2001)) || (r = dalloc(ctx, &m->ross, nr)) || (r = dalloc(ctx, &m->R, 1)) || (r = dalloc(ctx, &m->iter_dev, 1)) ||
@@ -391,6 +404,13 @@ int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlas
     atlasgpu_model_destroy(ctx, m);
     return r;
   }
+  // exact XLINES sums: zeroed words, the largest CGF per species for the scales
+  CK(cudaMemsetAsync(m->xfix, 0, (size_t)kFixWords * kw * m->numnu * sizeof(unsigned long long), s));
+  CK(cudaMemsetAsync(m->cgfmax, 0, (size_t)m->nspec * sizeof(unsigned long long), s));
+  if (m->nlines > 0) {
+    k_cgf_max<<<grid_for(ctx, m->nlines, 256, 8), 256, 0, s>>>(m->lines, m->nlines, m->nspec, m->cgfmax);
+    CKL(ctx);
+  }
   CK(cudaStreamSynchronize(s));
   *out = m;
   return 0;
@@ -429,7 +449,7 @@ int atlasgpu_model_iterate(atlasgpu_ctx* ctx, atlasgpu_model* m, int max_iter, d
         ctx->launches = l0;  // counted when replayed
       }
       CK(cudaGraphLaunch(m->gexec, s));
-      ctx->launches += 6;
+      ctx->launches += m->nlines > 0 ? 7 : 5;
     } else {
       if ((r = enqueue_iteration(ctx, m, true))) return r;
     }
@@ -588,6 +608,7 @@ int atlasgpu_model_destroy(atlasgpu_ctx* ctx, atlasgpu_model* m) {
   void* ps[] = {m->state, m->ms, m->xnfdop, m->dopple, m->xne_eos, m->txnxn, m->hkt, m->hckt, m->rho, m->cc,
                 m->acont, m->sigmac,
                 m->waveset, m->rcoset, m->cutwave, m->tabcont, m->iwavetab, m->linedata, m->lines, m->xl,
+                m->xfix, m->fscale, m->funscale, m->cgfmax,
                 m->partial, m->sum, m->hsurf, m->h0, m->h1, m->h2, m->hf, m->ross, m->R, m->iter_dev,
                 m->maxerr_dev, m->cnt};
   for (void* p : ps)

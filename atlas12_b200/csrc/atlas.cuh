@@ -235,6 +235,100 @@ static __global__ void __launch_bounds__(256) k_xlinop_shore(XShoreArgs a) {
   }
 }
 
+// ------------------------------------------------------ exact XLINES sums
+// LINOP1 adds each wing value into XLINES(J, NU).  In the reference the adds
+// come one at a time in line order; here thousands of warps add at once, and
+// FP64 atomics would make the sum depend on their order.  So each value is
+// added as a fixed-point integer instead: y = value * 2^k_J (k_J per depth,
+// from a bound on the largest value there) split into three 48-bit chunks,
+// each added to its own unsigned 64-bit word (16 bits of headroom: 65,536
+// adds of the largest value per bin).  Integer sums do not depend on the
+// order, and the words hold the exact sum (values below 2^-k_J, i.e. about
+// 2^-137 of the depth's bound, round to that unit), so XLINES is the exact
+// sum rounded once to FP64: bit-identical from run to run and within an
+// ulp of any order of FP64 additions.  Layout [numnu][3][kw] (word w of
+// (J, NU) at ((NU-1)*3 + w)*kw + J-1): a warp's lanes at consecutive
+// depths add to consecutive words.
+constexpr int kFixWords = 3;
+constexpr double kFixTop = 0x1p-96, kFixMid = 0x1p-48;
+
+__device__ __forceinline__ void fix_add(unsigned long long* w, int wstride, double y) {
+  const double t2 = floor(y * kFixTop);
+  const double r2 = y - t2 * 0x1p96;  // exact: the bits of y below 2^96
+  const double t1 = floor(r2 * kFixMid);
+  const double r1 = r2 - t1 * 0x1p48;  // exact: the bits below 2^48
+  const double t0 = rint(r1);          // the one rounding, to the unit 2^-k
+  if (t2 > 0.0) atomicAdd(w + 2 * wstride, (unsigned long long)t2);
+  if (t1 > 0.0) atomicAdd(w + wstride, (unsigned long long)t1);
+  if (t0 > 0.0) atomicAdd(w, (unsigned long long)t0);
+}
+
+// The exact integer x2 2^96 + x1 2^48 + x0, rounded to nearest FP64, times unscale (a power of 2)
+__host__ __device__ inline double fix_to_double(unsigned long long x0, unsigned long long x1, unsigned long long x2,
+                                                double unscale) {
+  constexpr unsigned long long m48 = (1ull << 48) - 1;
+  x1 += x0 >> 48;
+  x0 &= m48;
+  x2 += x1 >> 48;
+  x1 &= m48;
+  // 64-bit limbs of the value (at most 160 bits)
+  const unsigned long long lo = x0 | (x1 << 48);
+  const unsigned long long mid = (x1 >> 16) | (x2 << 32);
+  const unsigned long long hi = x2 >> 32;
+  unsigned long long top;
+  bool sticky;
+  int e;  // value = (top with sticky) * 2^e
+  if (hi) {
+#ifdef __CUDA_ARCH__
+    const int z = __clzll((long long)hi);
+#else
+    const int z = __builtin_clzll(hi);
+#endif
+    top = (hi << z) | (mid >> (64 - z));  // z >= 32 (hi < 2^32)
+    sticky = (mid << z) != 0 || lo != 0;
+    e = 128 - z;
+  } else if (mid) {
+#ifdef __CUDA_ARCH__
+    const int z = __clzll((long long)mid);
+#else
+    const int z = __builtin_clzll(mid);
+#endif
+    top = z ? (mid << z) | (lo >> (64 - z)) : mid;
+    sticky = z ? (lo << z) != 0 : lo != 0;
+    e = 64 - z;
+  } else {
+    top = lo;
+    sticky = false;
+    e = 0;
+  }
+  // the sticky bit in bit 0 keeps the round-to-nearest of the 64-bit top exact
+#ifdef __CUDA_ARCH__
+  const double d = __ull2double_rn(top | (sticky ? 1ull : 0ull));
+#else
+  const double d = (double)(top | (sticky ? 1ull : 0ull));
+#endif
+  return ldexp(d, e) * unscale;
+}
+
+// The scale 2^k of depth j: every value added there is at most
+// CGF(line) * XNFDOP(J, NELION) (the Boltzmann factor and the profile are at
+// most 1; 8x margin), so the largest value maps below 2^140 and a bin's
+// words stay below 2^64.  cgfmax: the largest CGF of each species' lines.
+__device__ inline void fix_scale_depth(const double* xnfdop, int nspec, int kw, int j, const double* cgfmax,
+                                       double* scale, double* unscale) {
+  double bound = 0.0;
+  for (int s = 0; s < nspec; ++s) bound = fmax(bound, cgfmax[s] * xnfdop[(size_t)s * kw + j]);
+  if (!(bound > 0.0) || !(bound < 1e300)) {
+    scale[j] = 1.0;
+    unscale[j] = 1.0;
+    return;
+  }
+  int e;
+  frexp(bound, &e);  // bound < 2^e
+  scale[j] = ldexp(1.0, 137 - e);
+  unscale[j] = ldexp(1.0, e - 137);
+}
+
 struct LinopArgs {
   const AtlasLine* lines;
   int64_t n;
@@ -263,7 +357,16 @@ struct LinopArgs {
   const double* emerge = nullptr;
   // work counter (timed launches only, else null): wing points added into XLINES
   unsigned long long* work = nullptr;
+  // exact fixed-point XLINES (see fix_add): words [numnu][3][kw] and the
+  // per-depth scale; null: FP64 atomics into xl (XLINOP adds to a caller's XLINES)
+  unsigned long long* xfix = nullptr;
+  const double* fscale = nullptr;
 };
+
+__device__ __forceinline__ void linop_add(const LinopArgs& a, int J, int iw, double cv) {
+  if (a.xfix) fix_add(a.xfix + ((size_t)(iw - 1) * kFixWords) * a.kw + (J - 1), a.kw, cv * a.fscale[J - 1]);
+  else atomicAdd(a.xl + (size_t)(iw - 1) * a.kw + (J - 1), cv);
+}
 
 // LINOP1's profile value at one wing point, V = (distance in nm) * RDOP with
 // RDOP = 1 / (DOPPLE * WLVAC) taken once per (line, depth): tabulated H(v, a)
@@ -314,7 +417,6 @@ static __device__ __noinline__ unsigned linop_finish_warp(const LinopArgs& a, in
                                                           double rdop, double wlvac, int nu, double tc, int rnext,
                                                           bool rdone, int bnext, bool bdone, double wcon, int lane) {
   unsigned added = 0;  // points this lane added
-  double* xl = a.xl + (J - 1);
   const int iwmax = min(nu + a.max_wing, a.numnu);
   const int nuh = a.nu_hi > 0 ? a.nu_hi : a.numnu;
   if (!rdone) {
@@ -331,7 +433,7 @@ static __device__ __noinline__ unsigned linop_finish_warp(const LinopArgs& a, in
       const unsigned stop = __ballot_sync(0xffffffffu, valid && below);
       const int last = stop ? base + __ffs(stop) - 1 : iwmax;
       if (valid && iw <= last && iw >= a.nu_lo && iw <= nuh) {
-        atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
+        linop_add(a, J, iw, cv);
         ++added;
       }
       if (stop) break;
@@ -354,7 +456,7 @@ static __device__ __noinline__ unsigned linop_finish_warp(const LinopArgs& a, in
       const unsigned inval = __ballot_sync(0xffffffffu, !valid);
       const int ilast = stop ? i0 + __ffs(stop) - 1 : a.max_wing;
       if (valid && i <= ilast && iw >= a.nu_lo && iw <= nuh) {
-        atomicAdd(xl + (size_t)(iw - 1) * a.kw, cv);
+        linop_add(a, J, iw, cv);
         ++added;
       }
       if (stop || inval) break;
@@ -401,6 +503,13 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
     if (lane == 0 && a.used) atomicAdd(a.used, 1ull);
     const int iwmax = min(L.nu + a.max_wing, a.numnu);
     for (int J0 = 1; J0 <= a.nrhox; J0 += 32) {
+      // a round of 32 depths can walk only where its coarse blocks, or the
+      // block just above its first, passed: skip it before any load if none did
+      {
+        const int kl = (J0 + 7) / 8 - 1, kh = (min(J0 + 31, a.nrhox) + 7) / 8 - 1;
+        const unsigned rmask = ((2u << kh) - 1u) & ~((1u << (kl > 0 ? kl - 1 : 0)) - 1u);
+        if (!(ifj & rmask)) continue;
+      }
       const int J = J0 + lane;
       bool walk = false;
       double center = 0.0, tc = 0.0;
@@ -434,7 +543,6 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
         rdop = 1.0 / (dpn[J - 1] * L.wlvac);
         ++walked;
       }
-      double* xlj = a.xl + (J - 1);
       bool rdone = !walk, bdone = !walk;
       int rnext = L.nu, bnext = 1;
 #pragma unroll 1
@@ -444,7 +552,7 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
           const double dl = a.waveset[iw - 1] - L.wlvac;
           const double cv = linop_cv<F32>(a, center, adamp, dl, rdop);
           if (iw >= a.nu_lo && iw <= nuh) {
-            atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
+            linop_add(a, J, iw, cv);
             ++points;
           }
           if (linop_below<F32>(a, cv, tc, center, adamp, dl, rdop) || iw >= iwmax) rdone = true;
@@ -458,7 +566,7 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
             const double dl = L.wlvac - a.waveset[iw - 1];
             const double cv = linop_cv<F32>(a, center, adamp, dl, rdop);
             if (iw >= a.nu_lo && iw <= nuh) {
-              atomicAdd(xlj + (size_t)(iw - 1) * a.kw, cv);
+              linop_add(a, J, iw, cv);
               ++points;
             }
             if (linop_below<F32>(a, cv, tc, center, adamp, dl, rdop) || bnext >= a.max_wing) bdone = true;
@@ -497,6 +605,45 @@ static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
 template <bool F32>
 static __global__ void __launch_bounds__(256, 3) k_atlas_linop(LinopArgs a) { linop_body<F32>(a); }
 
+// XLINES(J, NU) from the fixed-point words, which are cleared for the next
+// accumulation (grid-stride over NU, threads over depths J < nrhox)
+__device__ inline void fix_finalize_range(unsigned long long* __restrict__ xfix, const double* __restrict__ unscale,
+                                          int numnu, int nrhox, int kw, double* __restrict__ xl) {
+  const int64_t n = (int64_t)numnu * nrhox;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t nu = e / nrhox;
+    const int j = (int)(e - nu * nrhox);
+    unsigned long long* w = xfix + (size_t)nu * kFixWords * kw + j;
+    const unsigned long long x0 = w[0], x1 = w[kw], x2 = w[2 * kw];
+    xl[(size_t)nu * kw + j] = (x0 | x1 | x2) ? fix_to_double(x0, x1, x2, unscale[j]) : 0.0;
+    if (x0) w[0] = 0ull;
+    if (x1) w[kw] = 0ull;
+    if (x2) w[2 * kw] = 0ull;
+  }
+}
+
+static __global__ void k_fix_finalize(unsigned long long* xfix, const double* unscale, int numnu, int nrhox, int kw,
+                                      double* xl) {
+  fix_finalize_range(xfix, unscale, numnu, nrhox, kw, xl);
+}
+
+// the largest CGF of each species' lines (CGF > 0: the bit patterns order as the values)
+static __global__ void k_cgf_max(const AtlasLine* __restrict__ lines, int64_t n, int nspec,
+                                 unsigned long long* __restrict__ cgfmax) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const AtlasLine L = lines[i];
+    if (L.nelion >= 1 && L.nelion <= nspec && L.cgf > 0.0)
+      atomicMax(cgfmax + L.nelion - 1, (unsigned long long)__double_as_longlong(L.cgf));
+  }
+}
+
+// the per-depth scales of a model (threads over depths)
+static __global__ void k_fix_scale(const double* xnfdop, int nspec, int kw, int nrhox, const double* cgfmax,
+                                   double* scale, double* unscale) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < nrhox) fix_scale_depth(xnfdop, nspec, kw, j, cgfmax, scale, unscale);
+}
+
 // ---------------------------------------------------------------- RT pass
 constexpr int kAcc = 8;  // rjmins, rdabh, rdiagj, flxrad, raden, h_total, accrad, abross
 
@@ -522,17 +669,20 @@ struct RtWS {
   JoshWSFull f;
   double acont[kKwMax], sigmac[kKwMax], aline[kKwMax], stim[kKwMax];
   double dab[kKwMax];           // SCONT while JOSH runs (when given), then d(abtot)/d(rhox)
-  alignas(16) double U[kNx * kU2];  // pivot rows of the 51x51 factorisation (row stride kU2)
+  alignas(16) double U[kNx * (kNx + 1)];  // pivot rows of the 51x51 factorisation (rows 16-byte aligned)
 };
 
-// One four-warp group (128 threads) per frequency, kRtGroups groups per CTA.
-// The group's 51x52 system lives in registers, spread block-cyclically over
-// its threads (scatter_solve_2d), so the shared-memory footprint is the
-// depth vectors and the pivot rows; depth loops cover 72 depths in one pass.
-using RtG = QuadG;
+// One pair group (64 threads) per frequency, kRtGroups groups per CTA.  The
+// group's 51 matrix rows live in registers (pair elimination), so the
+// shared-memory footprint is the depth vectors and the pivot rows.  (A
+// 128-thread group holding the system block-cyclically, 28 entries per
+// thread and one barrier per step, measured slower: 3.62 ms against 3.34 ms
+// for the 30,000-frequency pass unrolled, 5.79 ms with the step loop
+// rolled; four groups fit per SM against six.)
+using RtG = PairG;
+constexpr int kRtMinBlocks = 3;
 constexpr int kRtGroups = 2;
 constexpr int kRtThreads = kRtGroups * RtG::N;
-constexpr int kRtMinBlocks = 2;
 
 // shared memory: RHOX and a zero vector (SIGMAL) for the CTA, then the groups' workspaces
 __host__ __device__ inline size_t rt_smem_bytes() { return 2 * sizeof(double) * kKwMax + kRtGroups * sizeof(RtWS); }

@@ -81,7 +81,6 @@ struct JoshWS {
   double t1[kKwMax], t2[kKwMax], t3[kKwMax];  // scratch (PARCOE a,b,c / terms)
   double red[8];                              // group reductions (multi-warp groups)
   double piv[kNx];                            // pivots of the elimination without interchanges
-  double lcol[2][kNx + 1];                    // pivot-column entries of the 2-D elimination (two steps)
   int lidx[kKwMax + 4];                       // MAP1 bracket indices
   unsigned pk[4][3];                          // pivot key exchange between a group's warps
 };
@@ -610,171 +609,6 @@ static __device__ __forceinline__ bool scatter_solve_nopivot(PairG& g, const Jos
 
 __device__ __forceinline__ void solve_scatter(PairG& g, const JoshOps& ops, JoshWS& ws, double* U) {
   if (!scatter_solve_nopivot(g, ops, ws, U)) scatter_solve(g, ops, ws, U);
-}
-
-// ------------------------------------------------ 2-D elimination (128 threads)
-// The same system by a four-warp group with the matrix [AMAT | rhs] spread
-// block-cyclically: thread t holds rows R = r + 16k (r = t / 8, k = 0..3)
-// and columns C = c + 8q (c = t % 8, q = 0..6; column 51 is the right-hand
-// side) in registers, 28 entries.  Step i publishes the pivot row (its
-// holders, r = i % 16) and the raw pivot column (c = i % 8) to shared
-// memory with the reciprocal pivot, one barrier, and every thread updates
-// its entries of the trailing block, A(R,C) -= (A(R,i) * (1/pivot)) *
-// A(i,C): SOLVIT's multipliers and row updates, element by element in its
-// order, without interchanges (checked as in scatter_solve_nopivot).  Each
-// thread does at most 28 FMAs a step, and the static loop bounds skip the
-// row and column blocks that are finished.  The reciprocal of the next
-// pivot is taken by its holder right after that entry's update, so it
-// overlaps the rest of the step.  The pivot rows stay in U (row stride kU2,
-// 1/pivot on the diagonal, rhs in column 51) for the back substitution.
-using QuadG = MultiG<4>;
-constexpr int kU2 = kNx + 2;  // U row stride: 53 doubles keep column reads free of bank conflicts
-constexpr int kR2 = 4, kC2 = 7;
-
-struct Lu2d {
-  double a[kR2][kC2];
-  int r, c;
-  bool swap;
-  double rnext;  // reciprocal of the next pivot, by its holder
-};
-
-__device__ __forceinline__ double clamp_pivot(double v) {
-  return fabs(v) < kPivotTol ? copysign(kPivotTol, v) : v;
-}
-
-template <int I>
-__device__ __forceinline__ void lu2d_step(QuadG& g, Lu2d& s, JoshWS& ws, double* __restrict__ U) {
-  constexpr int ri = I % 16, ki = I / 16, ci = I % 8, qi = I / 8;
-  constexpr int klo = (I + 1) / 16;  // first local row block with a row > I
-  constexpr int qlo = I / 8;         // first local column block with a column >= I
-  constexpr int qul = (I + 1) / 8;   // first local column block with a column > I
-  double* ur = U + I * kU2;
-  double* lc = ws.lcol[I & 1];
-  // publication: pivot row (columns > I; 1/pivot on the diagonal), raw pivot column (rows > I)
-  if (s.r == ri) {
-#pragma unroll
-    for (int q = qlo; q < kC2; ++q) {
-      const int C = s.c + 8 * q;
-      if (C > I && C <= kNx) ur[C] = s.a[ki][q];
-    }
-    if (s.c == ci) {
-      ws.piv[I] = s.a[ki][qi];
-      ur[I] = s.rnext;
-    }
-  }
-  if (s.c == ci) {
-#pragma unroll
-    for (int k = klo; k < kR2; ++k) {
-      const int R = s.r + 16 * k;
-      if (R > I && R < kNx) lc[R] = s.a[k][qi];
-    }
-  }
-  g.sync();
-  // update of the trailing block
-  const double rp = ur[I];
-  double l[kR2], u[kC2];
-#pragma unroll
-  for (int k = klo; k < kR2; ++k) {
-    const int R = s.r + 16 * k;
-    const bool act = R > I && R < kNx;
-    l[k] = act ? lc[R] * rp : 0.0;
-    if (s.c == ci && act) s.swap |= fabs(s.a[k][qi]) > fabs(ws.piv[I]);
-  }
-#pragma unroll
-  for (int q = qul; q < kC2; ++q) {
-    const int C = s.c + 8 * q;
-    u[q] = (C > I && C <= kNx) ? ur[C] : 0.0;
-  }
-  if constexpr (I + 1 < kNx) {
-    // the next pivot first, so that its reciprocal overlaps the other updates
-    constexpr int kn = (I + 1) / 16, qn = (I + 1) / 8;
-    s.a[kn][qn] = s.a[kn][qn] - l[kn] * u[qn];
-    if (s.r == (I + 1) % 16 && s.c == (I + 1) % 8) s.rnext = 1.0 / clamp_pivot(s.a[kn][qn]);
-#pragma unroll
-    for (int k = klo; k < kR2; ++k)
-#pragma unroll
-      for (int q = qul; q < kC2; ++q)
-        if (!(k == kn && q == qn)) s.a[k][q] = s.a[k][q] - l[k] * u[q];
-  }
-}
-
-template <int I>
-__device__ __forceinline__ void lu2d_steps(QuadG& g, Lu2d& s, JoshWS& ws, double* U) {
-  if constexpr (I < kNx - 1) {
-    lu2d_step<I>(g, s, ws, U);
-    lu2d_steps<I + 1>(g, s, ws, U);
-  }
-}
-
-// Back substitution from U (row k: 1/pivot at column k, A(k,j) at j > k,
-// the rhs at column 51) by the group's first warp, in SOLVIT's order.
-__device__ __forceinline__ void u2d_back_substitute(int r, const double* U, double* xs) {
-  constexpr int n = kNx;
-  if (r >= 32) return;
-  const int k0 = r, k1 = r + 32;
-  double b0 = U[k0 * kU2 + n];
-  double b1 = k1 < n ? U[k1 * kU2 + n] : 0.0;
-  for (int j = n - 1; j >= 0; --j) {
-    const int src = j & 31;
-    double x = (j < 32 ? b0 : b1) * U[j * kU2 + j];
-    x = __shfl_sync(0xffffffffu, x, src);
-    if (r == src) xs[j] = x;
-    if (k0 < j) b0 = b0 - U[k0 * kU2 + j] * x;
-    if (k1 < j) b1 = b1 - U[k1 * kU2 + j] * x;
-  }
-}
-
-// Returns false if SOLVIT would have interchanged rows at some step.
-static __device__ __noinline__ bool scatter_solve_2d(QuadG& g, const JoshOps& ops, JoshWS& ws, double* U) {
-  Lu2d s;
-  s.r = g.r >> 3;
-  s.c = g.r & 7;
-  s.swap = false;
-  s.rnext = 0.0;
-#pragma unroll
-  for (int k = 0; k < kR2; ++k) {
-    const int R = s.r + 16 * k;
-    const bool rv = R < kNx;
-    const double xa = rv ? ws.xalpha[R] : 0.0;
-#pragma unroll
-    for (int q = 0; q < kC2; ++q) {
-      const int C = s.c + 8 * q;
-      double v = 0.0;
-      if (rv && C < kNx) {
-        v = -xa * ops.coefj[C * kNx + R];
-        if (R == C) v = v + 1.0;
-      } else if (rv && C == kNx) {
-        v = (1.0 - xa) * ws.xsbar[R];
-      }
-      s.a[k][q] = v;
-    }
-  }
-  if (s.r == 0 && s.c == 0) s.rnext = 1.0 / clamp_pivot(s.a[0][0]);
-  lu2d_steps<0>(g, s, ws, U);
-  // the last row, 50 = 2 + 16*3: 1/pivot (column 50 = 2 + 8*6) and the rhs (column 51 = 3 + 8*6)
-  if (s.r == (kNx - 1) % 16) {
-    if (s.c == (kNx - 1) % 8) U[(kNx - 1) * kU2 + kNx - 1] = 1.0 / clamp_pivot(s.a[3][6]);
-    if (s.c == kNx % 8) U[(kNx - 1) * kU2 + kNx] = s.a[3][6];
-  }
-  if (g.any(s.swap)) return false;
-  u2d_back_substitute(g.r, U, ws.xs);
-  g.sync();
-  return true;
-}
-
-// SOLVIT with interchanges for the rare system where the 2-D elimination
-// found a larger entry below a pivot: the first warp factors the matrix in U
-// (column-major, leading dimension kLd) while the others wait.
-static __device__ __noinline__ void scatter_solve_pivoting(QuadG& g, const JoshOps& ops, JoshWS& ws, double* A) {
-  if (g.r < 32) {
-    WarpG w(g.r);
-    scatter_solve(w, ops, ws, A);
-  }
-  g.sync();
-}
-
-__device__ __forceinline__ void solve_scatter(QuadG& g, const JoshOps& ops, JoshWS& ws, double* U) {
-  if (!scatter_solve_2d(g, ops, ws, U)) scatter_solve_pivoting(g, ops, ws, U);
 }
 __device__ __forceinline__ void solve_scatter(WarpG& g, const JoshOps& ops, JoshWS& ws, double* A) {
   scatter_solve(g, ops, ws, A);

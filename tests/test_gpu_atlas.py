@@ -79,6 +79,22 @@ def test_linop_matches_oracle(gpu_ctx, tables, atlas_case, h_tables, oracle_lino
     assert np.max(np.abs(xl - ref) / scale) < tol
 
 
+def test_linop_bit_identical_run_to_run(gpu_ctx, tables, atlas_case, h_tables):
+    """XLINES is an exact fixed-point sum rounded once: the same inputs give
+    the same bits however the GPU orders the adds (both precisions)."""
+    c = atlas_case
+    A = atlas.Atlas(gpu_ctx, tables, *h_tables)
+    for prec in (_lib.PREC_FP64, _lib.PREC_MIXED):
+        gpu_ctx.set_precision(prec)
+        try:
+            runs = [A.linop1(c["lines"], 72, c["xnfdop"], c["dopple"], c["xne"], c["txnxn"], c["hckt"],
+                             c["tabcont"], c["iw"], c["ws"])[0] for _ in range(3)]
+        finally:
+            gpu_ctx.set_precision(_lib.PREC_MIXED)
+        for r in runs[1:]:
+            assert np.array_equal(r.view(np.uint64), runs[0].view(np.uint64))
+
+
 def test_linop_empty_and_out_of_grid(gpu_ctx, tables, atlas_case, h_tables, po):
     c = atlas_case
     A = atlas.Atlas(gpu_ctx, tables, *h_tables)

@@ -127,3 +127,18 @@ def test_launch_shape_and_autotuner(gpu_ctx, tables, small_grid, singles, tmp_pa
     assert b3.shape() == default  # another workload: nothing cached
     b3.close()
     b.close()
+
+
+def test_batch_runs_are_bit_identical(gpu_ctx, tables, small_grid):
+    """Two runs of the same models give the same bits: LINOP1's sums are
+    exact (order-free) and every other reduction has a fixed order, so
+    convergence no longer depends on the run."""
+    ws, rc, lines = small_grid
+    starts = [_start(teff, logg, mh) for teff, logg, mh, _ in PARAMS]
+    b = atlas.AtlasBatch(gpu_ctx, tables, nslots=3, linedata=lines, waveset=ws, rcoset=rc, shape=None)
+    r1 = b.run_queue(PARAMS, starts, max_iter=NIT, tol_percent=0.0, poll_every=1)
+    r2 = b.run_queue(PARAMS, starts, max_iter=NIT, tol_percent=0.0, poll_every=1)
+    b.close()
+    for a, c in zip(r1, r2):
+        for k in ("t", "p", "rhox", "flxerr", "hist"):
+            assert np.array_equal(np.asarray(a[k]).view(np.uint64), np.asarray(c[k]).view(np.uint64)), k
