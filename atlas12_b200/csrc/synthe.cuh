@@ -243,7 +243,12 @@ static __global__ void k_far_fill(const FarLine* __restrict__ far, const unsigne
   }
 }
 
-// far-wing gather + core accumulator -> REAL(4) opacity; zeroes acc for reuse
+// far-wing gather + core accumulator -> REAL(4) opacity; zeroes acc for reuse.
+// The tile's far lines are staged kFarThreads at a time in shared memory
+// (one line record per thread, loaded together), then every thread runs
+// over the staged lines in list order for its kPer bins: the record loads
+// are no longer a dependent global-load chain per line, and each bin's sum
+// takes its terms in the same order as before.
 template <bool kMixed>
 static __global__ void __launch_bounds__(kFarThreads) k_farwing(const FarLine* __restrict__ far,
                                                          int64_t nlines,
@@ -253,6 +258,8 @@ static __global__ void __launch_bounds__(kFarThreads) k_farwing(const FarLine* _
                                                          int length, int j0,
                                                          double* __restrict__ acc,
                                                          float* __restrict__ opac) {
+  __shared__ int4 s_l[kFarThreads];     // (c, n10, m, -) of the staged lines
+  __shared__ double s_x[kFarThreads];   // their x_wing
   const int jj = blockIdx.y, t = blockIdx.x, j = j0 + jj;
   constexpr int kPer = kTile / kFarThreads;
   const int i0 = t * kTile + threadIdx.x + 1;  // 1-based bins i0 + k*kFarThreads
@@ -262,28 +269,39 @@ static __global__ void __launch_bounds__(kFarThreads) k_farwing(const FarLine* _
   const int64_t* o = off + (size_t)jj * (ntiles + 1);
   const int64_t e0 = base[jj] + o[t], e1 = base[jj] + o[t + 1];
   const FarLine* fj = far + (size_t)jj * nlines;
-  for (int64_t e = e0; e < e1; ++e) {
-    const FarLine f = fj[csr[e]];
-    if (kMixed) {
-      const float xf = (float)f.x;
+  for (int64_t c0 = e0; c0 < e1; c0 += kFarThreads) {
+    const int nc = (int)min((int64_t)kFarThreads, e1 - c0);
+    if (threadIdx.x < nc) {
+      const FarLine f = fj[csr[c0 + threadIdx.x]];
+      s_l[threadIdx.x] = make_int4(f.c, f.n10, f.m, 0);
+      s_x[threadIdx.x] = f.x;
+    }
+    __syncthreads();
+    for (int q = 0; q < nc; ++q) {
+      const int4 l = s_l[q];
+      if (kMixed) {
+        const float xf = (float)s_x[q];
 #pragma unroll
-      for (int k = 0; k < kPer; ++k) {
-        const int d = abs(i0 + k * kFarThreads - f.c);
-        if (d > f.n10 && d <= f.m) {
-          const float df = (float)d;
-          sum[k] += (double)(xf * __frcp_rn(df * df));
+        for (int k = 0; k < kPer; ++k) {
+          const int d = abs(i0 + k * kFarThreads - l.x);
+          if (d > l.y && d <= l.z) {
+            const float df = (float)d;
+            sum[k] += (double)(xf * __frcp_rn(df * df));
+          }
         }
-      }
-    } else {
+      } else {
+        const double x = s_x[q];
 #pragma unroll
-      for (int k = 0; k < kPer; ++k) {
-        const int d = abs(i0 + k * kFarThreads - f.c);
-        if (d > f.n10 && d <= f.m) {
-          const double dd = (double)d;
-          sum[k] += f.x / (dd * dd);
+        for (int k = 0; k < kPer; ++k) {
+          const int d = abs(i0 + k * kFarThreads - l.x);
+          if (d > l.y && d <= l.z) {
+            const double dd = (double)d;
+            sum[k] += x / (dd * dd);
+          }
         }
       }
     }
+    __syncthreads();
   }
   double* accj = acc + (size_t)j * length;
   float* oj = opac + (size_t)j * length;
