@@ -175,3 +175,38 @@ class Synthe:
                                     grid, op)
         wave = grid["wbegin"] * grid["ratio"] ** np.arange(grid["length"]) * 10.0
         return wave, flux, cflux, op
+
+
+def main(argv=None):
+    """One synthesis of a synthetic case with the kernel times, e.g.
+
+        python -m atlas12_b200.synthe --lines 20000 --wlbeg 400 --wlend 410
+
+    (the 20,000-line window is the CPU-runnable configuration; 20M lines over
+    300-1000 nm with --mol 0.3 the full-optical one)."""
+    import argparse
+    import json
+
+    from . import operators, synthetic
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--lines", type=int, default=20000)
+    ap.add_argument("--wlbeg", type=float, default=400.0)
+    ap.add_argument("--wlend", type=float, default=410.0)
+    ap.add_argument("--mol", type=float, default=0.0, help="fraction of molecular lines")
+    ap.add_argument("--fp64", action="store_true", help="all-FP64 line opacity")
+    ap.add_argument("--reps", type=int, default=2)
+    a = ap.parse_args(argv)
+    case = synthetic.synthe_case(nlines=a.lines, wlbeg=a.wlbeg, wlend=a.wlend, seed=1, mol_frac=a.mol)
+    ctx = Context(0, _lib.PREC_FP64 if a.fp64 else _lib.PREC_MIXED)
+    S = Synthe(ctx, operators.load())
+    for _ in range(max(a.reps, 1)):
+        ctx.enable_timing(True)
+        wave, flux, cflux, op = S.run(case)
+        ms = {k: ctx.kernel_ms(k) for k in ("synthe_core", "synthe_farfill", "synthe_farwing", "josh_spectrum")}
+        ctx.enable_timing(False)
+    print(json.dumps({"points": int(flux.size), "lines": a.lines, "kernel_ms": ms}))
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()
