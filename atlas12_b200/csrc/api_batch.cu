@@ -93,7 +93,7 @@ __global__ void k_batch_kapp(BatchDev d) {
 }
 
 template <bool F32>
-__global__ void __launch_bounds__(256, 3) k_batch_linop(const LinopArgs* __restrict__ args, const BatchCtl* ctl,
+__global__ void __launch_bounds__(256, kLinopMinBlocks) k_batch_linop(const LinopArgs* __restrict__ args, const BatchCtl* ctl,
                                                         unsigned long long* work) {
   const int b = blockIdx.y;
   if (!running(ctl, b)) return;
