@@ -292,7 +292,7 @@ int atlasgpu_synthe_line_opacity_dev(atlasgpu_ctx* ctx, const atlasgpu_lte_line*
       (r = bufT(ctx, "lo_base", nj, &base)))
     return r;
   std::vector<int64_t> htot(nj), hbase(nj);
-  unsigned long long* work = work_counters(ctx, 2);
+  unsigned long long* work = work_counters(ctx, 4);
   // the families run once per depth batch: their times add up over the call
   if (ctx->timing)
     for (const char* f : {"synthe_core", "synthe_farfill", "synthe_farwing"}) ctx->kms[f] = 0.0;
@@ -328,15 +328,18 @@ int atlasgpu_synthe_line_opacity_dev(atlasgpu_ctx* ctx, const atlasgpu_lte_line*
     }
     {
       Timer tm(ctx, "synthe_farwing", true);
-      dim3 g(ntiles, nb);
+      dim3 g(ntiles * kSubs, nb);
       if (ctx->precision == ATLASGPU_PREC_MIXED)
-        k_farwing<true><<<g, kFarThreads, 0, ctx->stream>>>(far, nn, off, base, csr, ntiles, length, j0, acc, d_opac);
+        k_farwing<true><<<g, 32, 0, ctx->stream>>>(far, nn, off, base, csr, ntiles, length, j0, acc, d_opac,
+                                                            work);
       else
-        k_farwing<false><<<g, kFarThreads, 0, ctx->stream>>>(far, nn, off, base, csr, ntiles, length, j0, acc, d_opac);
+        k_farwing<false><<<g, 32, 0, ctx->stream>>>(far, nn, off, base, csr, ntiles, length, j0, acc, d_opac,
+                                                             work);
       CKL(ctx);
     }
   }
-  work_collect(ctx, work, {"synthe_voigt_evals", "synthe_farwing_updates"});
+  work_collect(ctx, work, {"synthe_voigt_evals", "synthe_farwing_updates", "synthe_farwing_expansions",
+                           "synthe_farwing_direct_pairs"});
   return 0;
 }
 

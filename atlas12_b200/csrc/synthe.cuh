@@ -19,7 +19,6 @@
 namespace atlasgpu {
 
 constexpr int kTile = 1024;      // bins per far-wing tile
-constexpr int kFarThreads = 256; // threads per far-wing tile CTA
 
 struct FarLine {
   int c;    // line centre nbuff (1-based)
@@ -244,73 +243,164 @@ static __global__ void k_far_fill(const FarLine* __restrict__ far, const unsigne
 }
 
 // far-wing gather + core accumulator -> REAL(4) opacity; zeroes acc for reuse.
-// The tile's far lines are staged kFarThreads at a time in shared memory
-// (one line record per thread, loaded together), then every thread runs
-// over the staged lines in list order for its kPer bins: the record loads
-// are no longer a dependent global-load chain per line, and each bin's sum
-// takes its terms in the same order as before.
+//
+// One warp (one CTA) takes one sub-tile of kSub bins at one depth, lane l
+// the bins lane + 32k; it walks the CSR list of the kTile-bin tile the
+// sub-tile belongs to, 32 lines at a time (one line record per lane, the
+// next group's records already in flight), and classifies each line
+// against the sub-tile:
+//   * distant: the whole sub-tile lies inside one far wing of the line
+//     (n10 < |i - c| <= m for every bin i) and the sub-tile centre is at
+//     least kFarSep bins from c.  The line's terms x/(i - c)^2 are then the
+//     Taylor series in v = (i - centre)/h (h = kSub/2) about the centre,
+//       x/(D + h v)^2 = sum_k (x/D^2) (k+1) (-h/D)^k v^k,  D = centre - c,
+//     |h v / D| < 1/4, and the lane adds the first kFarTerms coefficients
+//     (relative truncation below 1e-8);
+//   * otherwise, if any of its bins is in the line's far wing, the line is
+//     broadcast to the warp (shuffles) and every bin takes x/n^2 itself,
+//     the lines in list order.
+// At the end the warp adds its lanes' coefficients and each bin evaluates
+// the polynomial.  Most of the C3 far-wing terms come from strong lines
+// thousands of bins away, so the direct work drops to a few per cent of
+// the terms.  Warps share nothing, so a sub-tile next to strong line
+// centres (long direct list) holds up no other sub-tile.
+constexpr int kSub = 128;       // bins per sub-tile (one warp)
+constexpr int kSubs = kTile / kSub;
+constexpr int kFarSep = 256;    // minimum |centre - c| for an expansion
+constexpr int kFarTerms = 16;   // Taylor terms
+
 template <bool kMixed>
-static __global__ void __launch_bounds__(kFarThreads) k_farwing(const FarLine* __restrict__ far,
-                                                         int64_t nlines,
-                                                         const int64_t* __restrict__ off,
-                                                         const int64_t* __restrict__ base,
-                                                         const int* __restrict__ csr, int ntiles,
-                                                         int length, int j0,
-                                                         double* __restrict__ acc,
-                                                         float* __restrict__ opac) {
-  __shared__ int4 s_l[kFarThreads];     // (c, n10, m, -) of the staged lines
-  __shared__ double s_x[kFarThreads];   // their x_wing
-  const int jj = blockIdx.y, t = blockIdx.x, j = j0 + jj;
-  constexpr int kPer = kTile / kFarThreads;
-  const int i0 = t * kTile + threadIdx.x + 1;  // 1-based bins i0 + k*kFarThreads
+static __global__ void __launch_bounds__(32) k_farwing(const FarLine* __restrict__ far, int64_t nlines,
+                                                 const int64_t* __restrict__ off,
+                                                 const int64_t* __restrict__ base,
+                                                 const int* __restrict__ csr, int ntiles, int length,
+                                                 int j0, double* __restrict__ acc,
+                                                 float* __restrict__ opac,
+                                                 unsigned long long* __restrict__ work) {
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr int kPer = kSub / 32;
+  const int jj = blockIdx.y, t = blockIdx.x / kSubs, j = j0 + jj;
+  const int lane = threadIdx.x;
+  const int lo = t * kTile + (blockIdx.x % kSubs) * kSub + 1;  // first bin of the sub-tile (1-based)
+  if (lo > length) return;
+  const int hi = min(lo + kSub - 1, length);                   // last bin inside the grid
+  const double centre = lo + 0.5 * (kSub - 1);                 // expansion centre
+  const int i0 = lo + lane;                                    // bins i0 + 32k
   double sum[kPer];
 #pragma unroll
   for (int k = 0; k < kPer; ++k) sum[k] = 0.0;
+  double b[kFarTerms];
+#pragma unroll
+  for (int k = 0; k < kFarTerms; ++k) b[k] = 0.0;
+  unsigned nexp = 0, ndir = 0;
   const int64_t* o = off + (size_t)jj * (ntiles + 1);
   const int64_t e0 = base[jj] + o[t], e1 = base[jj] + o[t + 1];
   const FarLine* fj = far + (size_t)jj * nlines;
-  for (int64_t c0 = e0; c0 < e1; c0 += kFarThreads) {
-    const int nc = (int)min((int64_t)kFarThreads, e1 - c0);
-    if (threadIdx.x < nc) {
-      const FarLine f = fj[csr[c0 + threadIdx.x]];
-      s_l[threadIdx.x] = make_int4(f.c, f.n10, f.m, 0);
-      s_x[threadIdx.x] = f.x;
+  const FarLine none{0, 0, 0, 0, 0.0};
+  // two-stage prefetch: the record of the next group, the index of the one after
+  int idx = e0 + lane < e1 ? csr[e0 + lane] : -1;
+  FarLine f = idx >= 0 ? fj[idx] : none;
+  idx = e0 + 32 + lane < e1 ? csr[e0 + 32 + lane] : -1;
+  for (int64_t c0 = e0; c0 < e1; c0 += 32) {
+    const FarLine fn = idx >= 0 ? fj[idx] : none;
+    idx = c0 + 64 + lane < e1 ? csr[c0 + 64 + lane] : -1;
+    bool direct = false;
+    if (c0 + lane < e1) {
+      int dmin, dmax;
+      bool outside = true;
+      if (f.c < lo) {
+        dmin = lo - f.c;
+        dmax = hi - f.c;
+      } else if (f.c > hi) {
+        dmin = f.c - hi;
+        dmax = f.c - lo;
+      } else {
+        outside = false;
+        dmin = 0;
+        dmax = max(f.c - lo, hi - f.c);
+      }
+      const double D = centre - (double)f.c;
+      if (outside && dmin > f.n10 && dmax <= f.m && fabs(D) >= (double)kFarSep) {
+        // 1/D from the single-precision reciprocal and one Newton-Raphson
+        // step (relative error ~1e-14, far below the truncation)
+        const double r0 = (double)__frcp_rn((float)D);
+        const double r = fma(r0, fma(-D, r0, 1.0), r0);
+        const double g = -0.5 * kSub * r, g2 = g * g, g4 = g2 * g2;
+        // powers p*g^k in four independent chains (k mod 4)
+        double p0 = f.x * r * r, p1 = p0 * g, p2 = p0 * g2, p3 = p1 * g2;
+#pragma unroll
+        for (int k = 0; k < kFarTerms; k += 4) {
+          b[k] = fma((double)(k + 1), p0, b[k]);
+          b[k + 1] = fma((double)(k + 2), p1, b[k + 1]);
+          b[k + 2] = fma((double)(k + 3), p2, b[k + 2]);
+          b[k + 3] = fma((double)(k + 4), p3, b[k + 3]);
+          p0 *= g4;
+          p1 *= g4;
+          p2 *= g4;
+          p3 *= g4;
+        }
+        ++nexp;
+      } else {
+        direct = dmax > f.n10 && dmin <= f.m;
+      }
     }
-    __syncthreads();
-    for (int q = 0; q < nc; ++q) {
-      const int4 l = s_l[q];
+    // the direct lines of this group, in list order, broadcast to every bin
+    unsigned bal = __ballot_sync(FULL, direct);
+    ndir += __popc(bal);
+    while (bal) {
+      const int src = __ffs(bal) - 1;
+      bal &= bal - 1u;
+      const int c = __shfl_sync(FULL, f.c, src);
+      const int n10 = __shfl_sync(FULL, f.n10, src);
+      const int m = __shfl_sync(FULL, f.m, src);
+      const double x = __shfl_sync(FULL, f.x, src);
       if (kMixed) {
-        const float xf = (float)s_x[q];
+        const float xf = (float)x;
+        const float fb = (float)(i0 - c);  // exact: |i - c| < 2^24
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
-          const int d = abs(i0 + k * kFarThreads - l.x);
-          if (d > l.y && d <= l.z) {
-            const float df = (float)d;
+          const int d = abs(i0 + 32 * k - c);
+          if (d > n10 && d <= m) {
+            const float df = fb + (float)(32 * k);
             sum[k] += (double)(xf * __frcp_rn(df * df));
           }
         }
       } else {
-        const double x = s_x[q];
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
-          const int d = abs(i0 + k * kFarThreads - l.x);
-          if (d > l.y && d <= l.z) {
+          const int d = abs(i0 + 32 * k - c);
+          if (d > n10 && d <= m) {
             const double dd = (double)d;
             sum[k] += x / (dd * dd);
           }
         }
       }
     }
-    __syncthreads();
+    f = fn;
   }
+  // the warp's expansion: lane sums, then the polynomial at each bin
+#pragma unroll
+  for (int k = 0; k < kFarTerms; ++k)
+    for (int sh = 16; sh > 0; sh >>= 1) b[k] += __shfl_xor_sync(FULL, b[k], sh);
   double* accj = acc + (size_t)j * length;
   float* oj = opac + (size_t)j * length;
 #pragma unroll
   for (int k = 0; k < kPer; ++k) {
-    const int i = i0 + k * kFarThreads;
+    const int i = i0 + 32 * k;
     if (i <= length) {
-      oj[i - 1] = (float)(accj[i - 1] + sum[k]);
+      const double v = ((double)i - centre) * (2.0 / kSub);
+      double pv = b[kFarTerms - 1];
+#pragma unroll
+      for (int q = kFarTerms - 2; q >= 0; --q) pv = fma(pv, v, b[q]);
+      oj[i - 1] = (float)(accj[i - 1] + (sum[k] + pv));
       accj[i - 1] = 0.0;
+    }
+  }
+  if (work) {
+    for (int sh = 16; sh > 0; sh >>= 1) nexp += __shfl_xor_sync(FULL, nexp, sh);
+    if (lane == 0) {
+      atomicAdd(work + 2, (unsigned long long)nexp);
+      atomicAdd(work + 3, (unsigned long long)ndir);
     }
   }
 }

@@ -203,8 +203,11 @@ def main(argv=None):
         ctx.enable_timing(True)
         wave, flux, cflux, op = S.run(case)
         ms = {k: ctx.kernel_ms(k) for k in ("synthe_core", "synthe_farfill", "synthe_farwing", "josh_spectrum")}
+        work = {k: ctx.kernel_work(k) for k in ("synthe_voigt_evals", "synthe_farwing_updates",
+                                                "synthe_farwing_expansions", "synthe_farwing_direct_pairs")}
         ctx.enable_timing(False)
-    print(json.dumps({"points": int(flux.size), "lines": a.lines, "kernel_ms": ms}))
+    print(json.dumps({"points": int(flux.size), "lines": a.lines, "kernel_ms": ms, "work": work,
+                      "flux_sum": float(np.sum(flux)), "cflux_sum": float(np.sum(cflux))}))
     ctx.close()
 
 

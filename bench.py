@@ -611,7 +611,8 @@ def synthe_rates(ctx, ops, nlines, wlbeg, wlend, mol_frac, seed=1, fp64_peak=Non
         _, flux, _, op = S.run(case)
         res[name] = (flux, op)
         ms = {k: ctx.kernel_ms(k) for k in ("synthe_core", "synthe_farfill", "synthe_farwing", "josh_spectrum")}
-        work = {k: ctx.kernel_work(k) for k in ("synthe_voigt_evals", "synthe_farwing_updates")}
+        work = {k: ctx.kernel_work(k) for k in ("synthe_voigt_evals", "synthe_farwing_updates",
+                                                "synthe_farwing_expansions", "synthe_farwing_direct_pairs")}
         ctx.enable_timing(False)
         line_ms = ms["synthe_core"] + ms["synthe_farfill"] + ms["synthe_farwing"]
         out[name] = {"line_depth_evals_per_s": nlines * 72 / (line_ms * 1e-3), "line_opacity_ms": line_ms,
@@ -639,7 +640,9 @@ def synthe_rates(ctx, ops, nlines, wlbeg, wlend, mol_frac, seed=1, fp64_peak=Non
         rl.append({"kernel": f"k_farwing (SYNTHE far-wing gather, {tag})", "bound": "issue",
                    "unit": "bin updates/s",
                    "achieved": m["work"]["synthe_farwing_updates"] / (m["kernel_ms"]["synthe_farwing"] * 1e-3),
-                   "work": f"{int(m['work']['synthe_farwing_updates'])} far-wing bin updates (x/n^2 terms)"})
+                   "work": f"{int(m['work']['synthe_farwing_updates'])} far-wing bin updates (x/n^2 terms): "
+                           f"{int(m['work']['synthe_farwing_expansions'])} (line, 128-bin sub-tile) pairs summed "
+                           f"as Taylor expansions, {int(m['work']['synthe_farwing_direct_pairs'])} bin by bin"})
     out["rooflines"] = rl
     return out
 
