@@ -305,7 +305,7 @@ int atlasgpu_synthe_line_opacity_dev(atlasgpu_ctx* ctx, const atlasgpu_lte_line*
                  d_dopple, d_xne, d_txnxn, d_hckt, acc, far, nfar, tdiff, ntiles, work};
       Timer tm(ctx, "synthe_core", true);
       const int64_t groups = n * nb;
-      k_core<8><<<grid_for(ctx, groups * 8, 256, 16), 256, 0, ctx->stream>>>(a);
+      k_core<<<grid_for(ctx, groups, 256, 4), 256, 0, ctx->stream>>>(a);
       CKL(ctx);
     }
     k_far_scan<<<nb, 32, 0, ctx->stream>>>(tdiff, ntiles, off, fillptr, tot);

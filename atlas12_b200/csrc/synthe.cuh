@@ -3,12 +3,14 @@
 //  k_bin        line -> grid index (mod_mklinelist.f90:898-899)
 //  k_continuum  continuum per depth on the grid (synthe.f90:483-516)
 //  k_core       gates, line centre and Voigt core walk of every (line, depth)
-//               pair (synthe.f90:559-640), core values scattered with FP64
-//               atomics; far-wing lines recorded for k_farwing
+//               pair (synthe.f90:559-640), one pair per lane at a time,
+//               core values scattered with FP64 atomics; far-wing lines
+//               recorded for k_farwing
 //  k_far_*      per-(depth, tile) inverted index of the far-wing lines
-//  k_farwing    gather of the x_wing/n^2 far wings (synthe.f90:641-650)
-//               tile by tile in registers, plus the core accumulator, written
-//               as the REAL(4) opacity matrix
+//  k_farwing    the x_wing/n^2 far wings (synthe.f90:641-650) per 128-bin
+//               sub-tile: distant lines as Taylor expansions about the
+//               sub-tile centre, near ones bin by bin; plus the core
+//               accumulator, written as the REAL(4) opacity matrix
 //  k_spectrum   the wavelength loop (synthe.f90:698-718, 797-902): two
 //               warp-cooperative JOSH(1,1) solves per wavelength
 #pragma once
@@ -92,86 +94,103 @@ struct CoreArgs {
   unsigned long long* work = nullptr;
 };
 
-template <int G>
+// Every lane walks (line, depth) pairs on its own, one Voigt evaluation per
+// trip of the loop: the centre point first, then the core points
+// s = 1, 2, ... until the first value below kapmin (scattered too, as the
+// reference's loop does) or s = n10dop; a lane whose walk has ended takes
+// the next pair of the grid-stride sequence (a few tries per trip, so that
+// the gated-out pairs of a lane cost little).  The evaluation is the only
+// expensive step and all lanes with a pair run it together, whatever the
+// lengths of their walks.
+// With MAXPROF < n10dop the reference scatters only min(n10dop, maxstep)
+// core points when no point falls below kapmin; that limit is known only
+// after the walk, so such pairs walk once to decide (phase 1) and once to
+// scatter (phase 2).
+// A walk that reaches n10dop without a point below kapmin records its far
+// wing x_wing/n^2 (n10dop < n <= maxstep) for k_farwing.
+constexpr int kCoreTries = 4;  // pair fetches per trip for an idle lane
+
 static __global__ void __launch_bounds__(256) k_core(CoreArgs a) {
-  const int lane = threadIdx.x & 31;
-  const int g = lane % G;                 // lane within the group
-  const int gbase = lane - g;             // first lane of the group
-  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << gbase);
   const int64_t npairs = a.n * a.nj;
-  const int64_t gid0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
-  const int64_t gstride = (int64_t)gridDim.x * blockDim.x / G;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // next pair to fetch
   unsigned long long nev = 0, nfw = 0;  // counted only when a.work is set
-  for (int64_t p = gid0; p < npairs; p += gstride) {
-    const int jj = (int)(p / a.n);
-    const int64_t il = p - (int64_t)jj * a.n;
-    const int j = a.j0 + jj;
-    const atlasgpu_lte_line L = a.lines[il];
-    const int nb = L.nbuff;
-    const int nel = L.nelion - 1;
-    if (nel < 0 || nel >= a.nspec) continue;  // invalid species: no opacity
-    const int ic = nb < 1 ? 1 : (nb > a.length ? a.length : nb);
-    const double xd = a.xnfdop[(size_t)j * a.nspec + nel];
-    const double dp = a.dopple[(size_t)j * a.nspec + nel];
-    double kappa0 = (double)L.cgf * xd;
-    const double kapmin = (double)a.cont[(size_t)j * a.length + ic - 1] * kLineCutoff;
-    if (kappa0 < kapmin) continue;
-    kappa0 = kappa0 * exp(-(double)L.elo * a.hckt[j]);
-    if (kappa0 < kapmin) continue;
-    const double adamp =
-        ((double)L.gamrf + (double)L.gamsf * a.xne[j] + (double)L.gamwf * a.txnxn[j]) / dp;
-    const int n10 = (int)(10.0 * dp * a.resolu);
-    double* accj = a.acc + (size_t)j * a.length;
-    if (g == 0 && nb >= 1 && nb <= a.length)
-      atomicAdd(accj + nb - 1, kappa0 * voigt_weideman(0.0, adamp));
-    nev += (g == 0 && nb >= 1 && nb <= a.length);
-    const double dv = 1.0 / dp / a.resolu;
-    // With MAXPROF < n10dop the reference scatters only min(n10dop, maxstep)
-    // core points when no point falls below kapmin; that limit is known only
-    // after the walk, so such pairs walk once to decide and once to scatter.
-    const bool defer = a.maxprof < n10;
-    int nstop = 0;  // 0: no sub-threshold point in the core
-    double plast = 0.0;
-    for (int s0 = 1; s0 <= n10 && nstop == 0; s0 += G) {
-      const int s = s0 + g;
-      const bool valid = s <= n10;
-      double pv = 0.0;
-      if (valid) pv = kappa0 * voigt_weideman((double)s * dv, adamp);
-      nev += valid;
-      const unsigned below = __ballot_sync(gmask, valid && pv < kapmin) & gmask;
-      int slim = n10;
-      if (below) {
-        nstop = s0 + (__ffs(below >> gbase) - 1);
-        slim = nstop;
-      }
-      if (!defer && valid && s <= slim) {
-        const int r = nb + s, b = nb - s;
-        if (r >= 1 && r <= a.length) atomicAdd(accj + r - 1, pv);
-        if (b >= 1 && b <= a.length) atomicAdd(accj + b - 1, pv);
-      }
-      if (s == n10) plast = pv;
+  bool act = false;
+  int phase = 0, s = 0, lim = 0, nb = 0, n10 = 0, jj = 0;
+  double kappa0 = 0.0, adamp = 0.0, dv = 0.0, kapmin = 0.0;
+  double* accj = nullptr;
+  while (act || p < npairs) {
+    for (int k = 0; !act && p < npairs && k < kCoreTries; ++k, p += stride) {
+      const int jp = (int)(p / a.n);
+      const int64_t il = p - (int64_t)jp * a.n;
+      const int j = a.j0 + jp;
+      const atlasgpu_lte_line L = a.lines[il];
+      const int nel = L.nelion - 1;
+      if (nel < 0 || nel >= a.nspec) continue;  // invalid species: no opacity
+      const int ic = L.nbuff < 1 ? 1 : (L.nbuff > a.length ? a.length : L.nbuff);
+      const double xd = a.xnfdop[(size_t)j * a.nspec + nel];
+      const double dp = a.dopple[(size_t)j * a.nspec + nel];
+      double k0 = (double)L.cgf * xd;
+      const double km = (double)a.cont[(size_t)j * a.length + ic - 1] * kLineCutoff;
+      if (k0 < km) continue;
+      k0 = k0 * exp(-(double)L.elo * a.hckt[j]);
+      if (k0 < km) continue;
+      act = true;
+      kappa0 = k0;
+      kapmin = km;
+      adamp = ((double)L.gamrf + (double)L.gamsf * a.xne[j] + (double)L.gamwf * a.txnxn[j]) / dp;
+      n10 = (int)(10.0 * dp * a.resolu);
+      dv = 1.0 / dp / a.resolu;
+      nb = L.nbuff;
+      jj = jp;
+      accj = a.acc + (size_t)j * a.length;
+      s = 0;
+      phase = a.maxprof < n10 ? 1 : 0;
     }
-    if (defer) {
-      const int lim = nstop ? nstop : a.maxprof;
-      for (int s = 1 + g; s <= lim; s += G) {
-        const double pv = kappa0 * voigt_weideman((double)s * dv, adamp);
-        ++nev;
-        const int r = nb + s, b = nb - s;
-        if (r >= 1 && r <= a.length) atomicAdd(accj + r - 1, pv);
-        if (b >= 1 && b <= a.length) atomicAdd(accj + b - 1, pv);
+    if (!act) continue;
+    const double pv = kappa0 * voigt_weideman((double)s * dv, adamp);
+    ++nev;
+    bool far = false;
+    if (s == 0) {
+      // the line centre, then the core walk (none when n10dop < 1)
+      if (nb >= 1 && nb <= a.length) atomicAdd(accj + nb - 1, pv);
+      s = 1;
+      act = n10 >= 1;
+    } else if (phase == 1) {
+      // deciding walk: the scatter limit, then the walk again from s = 1
+      const bool below = pv < kapmin;
+      if (below || s == n10) {
+        lim = below ? s : a.maxprof;
+        phase = 2;
+        s = 1;
+      } else {
+        ++s;
+      }
+    } else {
+      const int r = nb + s, b = nb - s;
+      if (r >= 1 && r <= a.length) atomicAdd(accj + r - 1, pv);
+      if (b >= 1 && b <= a.length) atomicAdd(accj + b - 1, pv);
+      if (phase == 2) {
+        act = s < lim;
+        ++s;
+      } else if (pv < kapmin) {
+        act = false;
+      } else if (s == n10) {
+        act = false;
+        far = true;
+      } else {
+        ++s;
       }
     }
-    if (nstop == 0 && n10 >= 1) {
+    if (far) {
       // far wing: x_wing/n**2 for n10dop < n <= maxstep
-      const int src = gbase + ((n10 - 1) % G);
-      plast = __shfl_sync(gmask, plast, src);
-      const double xw = plast * ((double)n10 * (double)n10);
+      const double xw = pv * ((double)n10 * (double)n10);
       // INT(SQRT(x_wing/kapmin))+1 capped at MAXPROF; saturate before the
       // integer conversion (the reference's INT overflows for huge ratios)
       const double q = sqrt(xw / kapmin);
       const int maxstep = q >= (double)a.maxprof ? a.maxprof : min((int)q + 1, a.maxprof);
       const int lo = max(nb - maxstep, 1), hi = min(nb + maxstep, a.length);
-      if (maxstep > n10 && lo <= hi && g == 0) {
+      if (maxstep > n10 && lo <= hi) {
         const unsigned slot = atomicAdd(a.nfar + jj, 1u);
         FarLine f;
         f.c = nb;
@@ -195,7 +214,7 @@ static __global__ void __launch_bounds__(256) k_core(CoreArgs a) {
       nev += __shfl_xor_sync(0xffffffffu, nev, o);
       nfw += __shfl_xor_sync(0xffffffffu, nfw, o);
     }
-    if (lane == 0) {
+    if ((threadIdx.x & 31) == 0) {
       atomicAdd(a.work, nev);
       atomicAdd(a.work + 1, nfw);
     }
