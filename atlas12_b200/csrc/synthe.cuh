@@ -97,56 +97,105 @@ struct CoreArgs {
 // Every lane walks (line, depth) pairs on its own, one Voigt evaluation per
 // trip of the loop: the centre point first, then the core points
 // s = 1, 2, ... until the first value below kapmin (scattered too, as the
-// reference's loop does) or s = n10dop; a lane whose walk has ended takes
-// the next pair of the grid-stride sequence (a few tries per trip, so that
-// the gated-out pairs of a lane cost little).  The evaluation is the only
-// expensive step and all lanes with a pair run it together, whatever the
-// lengths of their walks.
+// reference's loop does) or s = n10dop.  The evaluation is the only
+// expensive step, and all lanes with a pair run it together whatever the
+// lengths of their walks, so the warp keeps every lane supplied: it gates
+// the pairs 32 at a time (a chunk of its grid-stride sequence, one pair per
+// lane), a pair that passes both kapmin gates stays with its lane as a
+// pending candidate, and a lane whose walk has ended takes the next pending
+// candidate of the warp (k-th idle lane, k-th candidate, by shuffles).
 // With MAXPROF < n10dop the reference scatters only min(n10dop, maxstep)
 // core points when no point falls below kapmin; that limit is known only
 // after the walk, so such pairs walk once to decide (phase 1) and once to
 // scatter (phase 2).
 // A walk that reaches n10dop without a point below kapmin records its far
 // wing x_wing/n^2 (n10dop < n <= maxstep) for k_farwing.
-constexpr int kCoreTries = 4;  // pair fetches per trip for an idle lane
-
-static __global__ void __launch_bounds__(256) k_core(CoreArgs a) {
+static __global__ void __launch_bounds__(256, 4) k_core(CoreArgs a) {
+  constexpr unsigned FULL = 0xffffffffu;
   const int64_t npairs = a.n * a.nj;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // next pair to fetch
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  int64_t chunk = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;  // next chunk of 32 pairs
   unsigned long long nev = 0, nfw = 0;  // counted only when a.work is set
+  // the lane's walk
   bool act = false;
   int phase = 0, s = 0, lim = 0, nb = 0, n10 = 0, jj = 0;
   double kappa0 = 0.0, adamp = 0.0, dv = 0.0, kapmin = 0.0;
   double* accj = nullptr;
-  while (act || p < npairs) {
-    for (int k = 0; !act && p < npairs && k < kCoreTries; ++k, p += stride) {
-      const int jp = (int)(p / a.n);
-      const int64_t il = p - (int64_t)jp * a.n;
-      const int j = a.j0 + jp;
-      const atlasgpu_lte_line L = a.lines[il];
-      const int nel = L.nelion - 1;
-      if (nel < 0 || nel >= a.nspec) continue;  // invalid species: no opacity
-      const int ic = L.nbuff < 1 ? 1 : (L.nbuff > a.length ? a.length : L.nbuff);
-      const double xd = a.xnfdop[(size_t)j * a.nspec + nel];
-      const double dp = a.dopple[(size_t)j * a.nspec + nel];
-      double k0 = (double)L.cgf * xd;
-      const double km = (double)a.cont[(size_t)j * a.length + ic - 1] * kLineCutoff;
-      if (k0 < km) continue;
-      k0 = k0 * exp(-(double)L.elo * a.hckt[j]);
-      if (k0 < km) continue;
-      act = true;
-      kappa0 = k0;
-      kapmin = km;
-      adamp = ((double)L.gamrf + (double)L.gamsf * a.xne[j] + (double)L.gamwf * a.txnxn[j]) / dp;
-      n10 = (int)(10.0 * dp * a.resolu);
-      dv = 1.0 / dp / a.resolu;
-      nb = L.nbuff;
-      jj = jp;
-      accj = a.acc + (size_t)j * a.length;
-      s = 0;
-      phase = a.maxprof < n10 ? 1 : 0;
+  // the lane's pending candidate
+  bool pend = false;
+  int c_nb = 0, c_n10 = 0, c_jj = 0;
+  double c_k0 = 0.0, c_km = 0.0, c_ad = 0.0, c_dv = 0.0;
+  while (true) {
+    // refill the idle lanes: pending candidates first, new chunks when none is left
+    while (true) {
+      const unsigned idle = __ballot_sync(FULL, !act);
+      if (!idle) break;
+      const unsigned pm = __ballot_sync(FULL, pend);
+      if (!pm) {
+        if (chunk * 32 >= npairs) break;
+        const int64_t pp = chunk * 32 + lane;
+        chunk += nw;
+        if (pp < npairs) {
+          const int jp = (int)(pp / a.n);
+          const int64_t il = pp - (int64_t)jp * a.n;
+          const int j = a.j0 + jp;
+          const atlasgpu_lte_line L = a.lines[il];
+          const int nel = L.nelion - 1;
+          if (nel >= 0 && nel < a.nspec) {  // invalid species: no opacity
+            const int ic = L.nbuff < 1 ? 1 : (L.nbuff > a.length ? a.length : L.nbuff);
+            const double xd = a.xnfdop[(size_t)j * a.nspec + nel];
+            const double dp = a.dopple[(size_t)j * a.nspec + nel];
+            double k0 = (double)L.cgf * xd;
+            const double km = (double)a.cont[(size_t)j * a.length + ic - 1] * kLineCutoff;
+            if (k0 >= km) {
+              k0 = k0 * exp(-(double)L.elo * a.hckt[j]);
+              if (k0 >= km) {
+                pend = true;
+                c_k0 = k0;
+                c_km = km;
+                c_ad = ((double)L.gamrf + (double)L.gamsf * a.xne[j] + (double)L.gamwf * a.txnxn[j]) / dp;
+                c_n10 = (int)(10.0 * dp * a.resolu);
+                c_dv = 1.0 / dp / a.resolu;
+                c_nb = L.nbuff;
+                c_jj = jp;
+              }
+            }
+          }
+        }
+        continue;
+      }
+      // the k-th idle lane takes the k-th pending candidate
+      const int npend = __popc(pm), nidle = __popc(idle);
+      const int rank = __popc(idle & lt);
+      const bool take = !act && rank < npend;
+      int src = lane;
+      if (take) {
+        unsigned m = pm;
+        for (int q = 0; q < rank; ++q) m &= m - 1u;
+        src = __ffs(m) - 1;
+      }
+      const double t_k0 = __shfl_sync(FULL, c_k0, src), t_km = __shfl_sync(FULL, c_km, src);
+      const double t_ad = __shfl_sync(FULL, c_ad, src), t_dv = __shfl_sync(FULL, c_dv, src);
+      const int t_n10 = __shfl_sync(FULL, c_n10, src), t_nb = __shfl_sync(FULL, c_nb, src);
+      const int t_jj = __shfl_sync(FULL, c_jj, src);
+      if (pend && __popc(pm & lt) < nidle) pend = false;  // this candidate was taken
+      if (take) {
+        act = true;
+        kappa0 = t_k0;
+        kapmin = t_km;
+        adamp = t_ad;
+        dv = t_dv;
+        n10 = t_n10;
+        nb = t_nb;
+        jj = t_jj;
+        accj = a.acc + (size_t)(a.j0 + jj) * a.length;
+        s = 0;
+        phase = a.maxprof < n10 ? 1 : 0;
+      }
     }
+    if (!__any_sync(FULL, act)) break;
     if (!act) continue;
     const double pv = kappa0 * voigt_weideman((double)s * dv, adamp);
     ++nev;
