@@ -141,21 +141,25 @@ int atlas_prep_lines(atlasgpu_ctx* ctx, const int32_t* d_ld, const int32_t* h_ld
 namespace {
 
 int rt_launch(atlasgpu_ctx* ctx, RtArgs& a, double* d_sum, int* nwarps_out) {
-  const size_t smem = rt_smem_bytes();
-  // enough groups to fill every SM several times, frequencies contiguous per group
-  const int target = ctx->nsm * kRtMinBlocks * kRtGroups * 4;
-  a.nu_per_warp = std::max(1, (a.numnu + target - 1) / target);
-  const int ng = (a.numnu + a.nu_per_warp - 1) / a.nu_per_warp;
-  const int blocks = (ng + kRtGroups - 1) / kRtGroups;
-  const int nwl = blocks * kRtGroups;
-  double* part;
+  // the split pass (k_rt_pre, k_rt_solve, k_rt_post): enough warps and pair
+  // groups to fill every SM several times, frequencies contiguous per unit
+  const RtSplitShape sh = rt_split_shape(a.numnu, ctx->nsm, 1, 4);
+  rt_split_args(a, sh);
+  const int nwl = sh.rows();
+  double *part, *rec;
   int r;
   if ((r = bufT(ctx, "rt_part", (size_t)nwl * (kAcc * a.kw + 1), &part))) return r;
+  if ((r = bufT(ctx, "rt_rec", (size_t)a.numnu * a.rec_stride, &rec))) return r;
   a.partial = part;
-  CK(cudaFuncSetAttribute(k_atlas_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  a.rec = rec;
+  CK(rt_split_attributes(a.nrhox));
   {
     Timer tm(ctx, "atlas_rt");
-    k_atlas_rt<<<blocks, kRtThreads, smem, ctx->stream>>>(a);
+    k_rt_pre<<<sh.pre_blocks, kRtSplitWarps * 32, rt_pre_smem_bytes(), ctx->stream>>>(a);
+    CKL(ctx);
+    k_rt_solve<<<sh.solve_blocks, kRtSolveThreads, rt_solve_smem_bytes(), ctx->stream>>>(a);
+    CKL(ctx);
+    k_rt_post<<<sh.post_blocks, kRtSplitWarps * 32, rt_post_smem_bytes(a.nrhox), ctx->stream>>>(a);
     CKL(ctx);
   }
   {

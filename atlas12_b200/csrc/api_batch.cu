@@ -49,6 +49,7 @@ struct BatchDev {
   const double* cgfmax;                        // [nspec] largest CGF per species (shared line list)
   double* tabcont;                             // [B][nwave+1][kw]
   double* partial;                             // [B][nwl][kAcc*kw+1]
+  double* rt_rec;                              // [B][numnu][rt_rec_stride(kw)] split RT pass records
   double* sum;                                 // [B][kAcc*kw+1]
   double* hist;                                // [B][kHist]
   double* hsurf;                               // [B][numnu] HNU(1) of the last iteration
@@ -102,12 +103,29 @@ __global__ void __launch_bounds__(256, kLinopMinBlocks) k_batch_linop(const Lino
   linop_body<F32>(a);
 }
 
-__global__ void __launch_bounds__(kRtThreads, kRtMinBlocks) k_batch_rt(const RtArgs* __restrict__ args, const BatchCtl* ctl) {
+// the split RT pass (k_rt_pre / k_rt_solve / k_rt_post bodies) per running slot
+__global__ void __launch_bounds__(kRtSplitWarps * 32, 6) k_batch_rt_pre(const RtArgs* __restrict__ args,
+                                                                       const BatchCtl* ctl) {
+  const int b = blockIdx.y;
+  if (!running(ctl, b)) return;
+  rt_pre_body(args[b]);
+}
+__global__ void __launch_bounds__(kRtSolveThreads, kRtSolveMinBlocks) k_batch_rt_solve(const RtArgs* __restrict__ args,
+                                                                                    const BatchCtl* ctl,
+                                                                                    unsigned long long* work) {
+  const int b = blockIdx.y;
+  if (!running(ctl, b)) return;
+  RtArgs a = args[b];
+  a.work = work;
+  rt_solve_body(a);
+}
+__global__ void __launch_bounds__(kRtSplitWarps * 32, 4) k_batch_rt_post(const RtArgs* __restrict__ args,
+                                                                        const BatchCtl* ctl) {
   const int b = blockIdx.y;
   if (!running(ctl, b)) return;
   RtArgs a = args[b];
   a.teff = ctl[b].teff;
-  rt_body(a);
+  rt_post_body(a);
 }
 
 __global__ void __launch_bounds__(kRedCols* kRedRows) k_batch_reduce(BatchDev d) {
@@ -163,11 +181,12 @@ struct atlasgpu_batch {
   LinopArgs* la = nullptr;
   RtArgs* ra = nullptr;
   unsigned long long* cnt = nullptr;
-  int grid_linop = 1, grid_kapp = 1, blocks_rt = 1;
+  int grid_linop = 1, grid_kapp = 1;
+  RtSplitShape rt_sh;                         // launch shape of the split RT pass
   int linop_ctas_per_sm = 16, rt_waves = 32;  // launch shape (atlasgpu_batch_set_shape)
   size_t partial_rows = 0;                    // allocated partial-sum rows per slot
   std::vector<RtArgs> ra_host;                // per-slot RT arguments (rebuilt with the shape)
-  size_t smem_rt = 0, smem_fin = 0;
+  size_t smem_fin = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
 };
@@ -213,8 +232,28 @@ int enqueue_batch(atlasgpu_ctx* ctx, atlasgpu_batch* B, bool timed) {
   }
   {
     Timer tm(ctx, "batch_rt");
-    k_batch_rt<<<dim3(B->blocks_rt, nb), kRtThreads, B->smem_rt, s>>>(B->ra, B->d.ctl);
-    CKL(ctx);
+    const RtSplitShape& sh = B->rt_sh;
+    {
+      Timer t1(ctx, "batch_rt_pre");
+      k_batch_rt_pre<<<dim3(sh.pre_blocks, nb), kRtSplitWarps * 32, rt_pre_smem_bytes(), s>>>(B->ra, B->d.ctl);
+      CKL(ctx);
+    }
+    {
+      unsigned long long* work = work_counters(ctx, 3);
+      {
+        Timer t2(ctx, "batch_rt_solve");
+        k_batch_rt_solve<<<dim3(sh.solve_blocks, nb), kRtSolveThreads, rt_solve_smem_bytes(), s>>>(B->ra,
+                                                                                                 B->d.ctl, work);
+        CKL(ctx);
+      }
+      work_collect(ctx, work, {"batch_rt_eliminated", "batch_rt_series", "batch_rt_series_steps"});
+    }
+    {
+      Timer t3(ctx, "batch_rt_post");
+      k_batch_rt_post<<<dim3(sh.post_blocks, nb), kRtSplitWarps * 32, rt_post_smem_bytes(B->nrhox), s>>>(
+          B->ra, B->d.ctl);
+      CKL(ctx);
+    }
   }
   {
     Timer tm(ctx, "batch_reduce");
@@ -231,20 +270,16 @@ int enqueue_batch(atlasgpu_ctx* ctx, atlasgpu_batch* B, bool timed) {
   return 0;
 }
 
-// Launch shape: LINOP1 CTAs per SM over the whole batch, and RT pair groups
-// sized for about rt_waves resident waves over the batch (each group takes a
-// contiguous run of one slot's frequencies).  Grows the partial-sum buffer
-// when a shape needs more rows, rewrites the per-slot RT arguments and drops
-// the captured graph.
+// Launch shape: LINOP1 CTAs per SM over the whole batch, and the split RT
+// pass's warps and pair groups sized for about rt_waves resident waves over
+// the batch (each takes a contiguous run of one slot's frequencies).  Grows
+// the partial-sum buffer when a shape needs more rows, rewrites the per-slot
+// RT arguments and drops the captured graph.
 int apply_shape(atlasgpu_ctx* ctx, atlasgpu_batch* B, int linop_ctas_per_sm, int rt_waves) {
   const int nb = B->nslots;
   const size_t stride = (size_t)kAcc * B->kw + 1;
-  const int target = ctx->nsm * kRtMinBlocks * kRtGroups * rt_waves;
-  const int groups_per_slot = std::max(1, (target + nb - 1) / nb);
-  const int nu_per = std::max(1, (B->numnu + groups_per_slot - 1) / groups_per_slot);
-  const int ng = (B->numnu + nu_per - 1) / nu_per;
-  const int blocks = (ng + kRtGroups - 1) / kRtGroups;
-  const size_t rows = (size_t)blocks * kRtGroups;
+  const RtSplitShape sh = rt_split_shape(B->numnu, ctx->nsm, nb, rt_waves);
+  const size_t rows = (size_t)sh.rows();
   CK(cudaStreamSynchronize(ctx->stream));
   if (rows > B->partial_rows) {
     if (B->d.partial) cudaFree(B->d.partial);
@@ -256,13 +291,13 @@ int apply_shape(atlasgpu_ctx* ctx, atlasgpu_batch* B, int linop_ctas_per_sm, int
     }
     B->partial_rows = rows;
   }
-  B->blocks_rt = blocks;
+  B->rt_sh = sh;
   B->d.nwl = (int)rows;
   B->grid_linop = std::max(1, ctx->nsm * linop_ctas_per_sm / nb);
   B->linop_ctas_per_sm = linop_ctas_per_sm;
   B->rt_waves = rt_waves;
   for (int b = 0; b < nb; ++b) {
-    B->ra_host[b].nu_per_warp = nu_per;
+    rt_split_args(B->ra_host[b], sh);
     B->ra_host[b].partial = B->d.partial + (size_t)b * rows * stride;
   }
   CK(cudaMemcpy(B->ra, B->ra_host.data(), nb * sizeof(RtArgs), cudaMemcpyHostToDevice));
@@ -288,7 +323,7 @@ int atlasgpu_batch_destroy(atlasgpu_ctx* ctx, atlasgpu_batch* B) {
   const BatchDev& d = B->d;
   void* ps[] = {d.xfix, d.fscale, d.funscale, (void*)d.cgfmax,
                 d.ctl, d.ms, d.R, d.xnfdop, d.dopple, d.xne_eos, d.txnxn, d.hkt, d.hckt, d.rho, d.cc, d.acont,
-                d.sigmac, d.xl, d.tabcont, d.partial, d.sum, d.hist, d.hsurf, B->waveset, B->rcoset, B->cutwave, B->h0,
+                d.sigmac, d.xl, d.tabcont, d.partial, d.rt_rec, d.sum, d.hist, d.hsurf, B->waveset, B->rcoset, B->cutwave, B->h0,
                 B->h1, B->h2, B->hf, B->ross, B->state, B->iwavetab, B->linedata, B->lines, B->la, B->ra, B->cnt};
   for (void* p : ps)
     if (p) cudaFree(p);
@@ -334,7 +369,7 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
       (r = balloc(ctx, &d.rho, (size_t)nb * kw)) || (r = balloc(ctx, &d.cc, (size_t)nb * kw)) ||
       (r = balloc(ctx, &d.acont, nb * nnk)) || (r = balloc(ctx, &d.sigmac, nb * nnk)) ||
       (r = balloc(ctx, &d.xl, nb * nnk)) || (r = balloc(ctx, &d.tabcont, (size_t)nb * (B->nwave + 1) * kw)) ||
-      (r = balloc(ctx, &d.sum, nb * stride)) ||
+      (r = balloc(ctx, &d.sum, nb * stride)) || (r = balloc(ctx, &d.rt_rec, nb * (size_t)B->numnu * rt_rec_stride(kw))) ||
       (r = balloc(ctx, &d.hist, (size_t)nb * kHist)) || (r = balloc(ctx, &d.hsurf, nb * (size_t)B->numnu)) ||
       (r = balloc(ctx, &B->waveset, B->numnu)) ||
       (r = balloc(ctx, &B->rcoset, B->numnu)) || (r = balloc(ctx, &B->cutwave, B->nwave)) ||
@@ -350,13 +385,15 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
   }
   d.waveset = B->waveset;
   d.cutwave = B->cutwave;
-  B->smem_rt = rt_smem_bytes();
   B->smem_fin = fin_smem_bytes(kw, kRossMax);
   if (B->smem_fin > (size_t)ctx->smem_optin) {
     atlasgpu_batch_destroy(ctx, B);
     return fail(ctx, ATLASGPU_EINVAL, "batch_create: finish needs %zu B of shared memory", B->smem_fin);
   }
-  CK(cudaFuncSetAttribute(k_batch_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_rt));
+  CK(cudaFuncSetAttribute(k_batch_rt_pre, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rt_pre_smem_bytes()));
+  CK(cudaFuncSetAttribute(k_batch_rt_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rt_solve_smem_bytes()));
+  CK(cudaFuncSetAttribute(k_batch_rt_post, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)rt_post_smem_bytes(B->nrhox)));
   CK(cudaFuncSetAttribute(k_batch_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_fin));
   cudaStream_t s = ctx->stream;
   // slots start idle; state pointers, ROSSTAB stores and per-slot kernel arguments are fixed for life
@@ -385,6 +422,7 @@ int atlasgpu_batch_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* dsc, int
     ra[b] = RtArgs{ctx->ops, B->numnu, B->nrhox, kw, B->waveset, B->rcoset, d.acont + on, d.sigmac + on, nullptr,
                    d.xl + on, ms[b].rhox, ms[b].t, d.hkt + o, 0.0, 1, 1, kw, nullptr,
                    d.hsurf + (size_t)b * B->numnu, nullptr};
+    ra[b].rec = d.rt_rec + (size_t)b * B->numnu * rt_rec_stride(kw);
   }
   B->ra_host = ra;
   CK(cudaMemcpyAsync(d.ctl, ctl.data(), nb * sizeof(BatchCtl), cudaMemcpyHostToDevice, s));

@@ -36,8 +36,9 @@ struct atlasgpu_model {
   int* iter_dev;         // iterations completed
   double* maxerr_dev;    // last max |FLXERR|
   unsigned long long* cnt;
-  int blocks_rt, nwl, nu_per_group;
-  size_t smem_rt;
+  int nwl;                 // partial-sum rows allocated
+  RtSplitShape rt_sh;      // launch shape of the split RT pass over the shard
+  double* rt_rec;          // the split pass's per-frequency records [numnu][rt_rec_stride(kw)]
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   int graph_precision = -1;  // precision the captured graph was built with
@@ -105,15 +106,11 @@ __global__ void k_surrogate_eval(int nrhox, const double* t, const double* p, do
   }
 }
 
-// RT launch shape for the model's frequency shard: enough pair groups to fill
-// every SM several times, frequencies contiguous per group
+// RT launch shape for the model's frequency shard: enough warps and pair
+// groups to fill every SM several times, frequencies contiguous per unit
 void rt_shape(atlasgpu_ctx* ctx, atlasgpu_model* m) {
   const int last = m->nu_last > 0 ? m->nu_last : m->numnu;
-  const int len = last - m->nu_first + 1;
-  const int target = ctx->nsm * kRtMinBlocks * kRtGroups * 4;
-  m->nu_per_group = std::max(1, (len + target - 1) / target);
-  const int ng = (len + m->nu_per_group - 1) / m->nu_per_group;
-  m->blocks_rt = (ng + kRtGroups - 1) / kRtGroups;
+  m->rt_sh = rt_split_shape(last - m->nu_first + 1, ctx->nsm, 1, 4);
 }
 
 // The first part of one iteration on the context stream, up to the reduced
@@ -167,16 +164,23 @@ int enqueue_begin(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
   }
   RtArgs ra{ctx->ops, m->numnu, m->nrhox, m->kw, m->waveset, m->rcoset, m->acont, m->sigmac, nullptr,
             m->xl, (const double*)m->state + 1 * m->kw, (const double*)m->state + 0 * m->kw, m->hkt,
-            m->teff, m->nu_per_group, 1, m->kw, m->partial, m->hsurf, nullptr, m->nu_first, m->nu_last};
+            m->teff, 1, 1, m->kw, m->partial, m->hsurf, nullptr, m->nu_first, m->nu_last};
+  const RtSplitShape& sh = m->rt_sh;
+  rt_split_args(ra, sh);
+  ra.rec = m->rt_rec;
   double* sums = m->ext_sums ? m->ext_sums : m->sum;
   {
     Timer tm(ctx, "atlas_rt");
-    k_atlas_rt<<<m->blocks_rt, kRtThreads, m->smem_rt, s>>>(ra);
+    k_rt_pre<<<sh.pre_blocks, kRtSplitWarps * 32, rt_pre_smem_bytes(), s>>>(ra);
+    CKL(ctx);
+    k_rt_solve<<<sh.solve_blocks, kRtSolveThreads, rt_solve_smem_bytes(), s>>>(ra);
+    CKL(ctx);
+    k_rt_post<<<sh.post_blocks, kRtSplitWarps * 32, rt_post_smem_bytes(m->nrhox), s>>>(ra);
     CKL(ctx);
   }
   {
     Timer tm(ctx, "atlas_reduce");
-    launch_reduce(m->partial, m->blocks_rt * kRtGroups, m->kw, sums, s);
+    launch_reduce(m->partial, sh.rows(), m->kw, sums, s);
     CKL(ctx);
   }
   ctx->timing = was;
@@ -316,20 +320,15 @@ int atlasgpu_model_create(atlasgpu_ctx* ctx, const atlasgpu_model_desc* d, atlas
     atlasgpu_model_destroy(ctx, m);
     return r;
   }
-  // RT launch shape
-  m->smem_rt = rt_smem_bytes();
+  // RT launch shape, partial sums for the most rows any shard can need, records
   rt_shape(ctx, m);
-  {
-    // any shard launches at most min(NUMNU, target) groups (rt_shape): size the partials for that
-    const int target = ctx->nsm * kRtMinBlocks * kRtGroups * 4;
-    const int gmax = std::min(m->numnu, target);
-    m->nwl = ((gmax + kRtGroups - 1) / kRtGroups) * kRtGroups;
-  }
-  if ((r = dalloc(ctx, &m->partial, (size_t)m->nwl * (kAcc * kw + 1)))) {
+  m->nwl = rt_split_rows_max(m->numnu, ctx->nsm, 4);
+  if ((r = dalloc(ctx, &m->partial, (size_t)m->nwl * (kAcc * kw + 1))) ||
+      (r = dalloc(ctx, &m->rt_rec, (size_t)m->numnu * rt_rec_stride(kw)))) {
     atlasgpu_model_destroy(ctx, m);
     return r;
   }
-  CK(cudaFuncSetAttribute(k_atlas_rt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->smem_rt));
+  CK(rt_split_attributes(m->nrhox));
   if (fin_smem_bytes(kw, kRossMax) > (size_t)ctx->smem_optin) {
     atlasgpu_model_destroy(ctx, m);
     return fail(ctx, ATLASGPU_EINVAL, "model_create: finish needs %zu B of shared memory",
@@ -609,7 +608,7 @@ int atlasgpu_model_destroy(atlasgpu_ctx* ctx, atlasgpu_model* m) {
                 m->acont, m->sigmac,
                 m->waveset, m->rcoset, m->cutwave, m->tabcont, m->iwavetab, m->linedata, m->lines, m->xl,
                 m->xfix, m->fscale, m->funscale, m->cgfmax,
-                m->partial, m->sum, m->hsurf, m->h0, m->h1, m->h2, m->hf, m->ross, m->R, m->iter_dev,
+                m->partial, m->rt_rec, m->sum, m->hsurf, m->h0, m->h1, m->h2, m->hf, m->ross, m->R, m->iter_dev,
                 m->maxerr_dev, m->cnt};
   for (void* p : ps)
     if (p) cudaFree(p);

@@ -671,6 +671,16 @@ struct RtArgs {
   int* sweeps;       // [numnu] Eddington sweeps (diagnostic; may be null)
   // frequency shard NU_FIRST..NU_LAST (1-based; 0 => NUMNU): groups start at NU_FIRST
   int nu_first = 1, nu_last = 0;
+  // split pass (k_rt_pre / k_rt_solve / k_rt_post): per-frequency records
+  // handed from stage to stage, rec_stride doubles per frequency at
+  // (NU - NU_FIRST) * rec_stride; frequencies per pre warp and per solve
+  // group (nu_per_warp is the post warps', one partial row per post warp)
+  double* rec = nullptr;
+  int rec_stride = 0;
+  int nu_per_pre = 1, nu_per_solve = 1;
+  // work counters of the solve stage (timed launches only, else null):
+  // [0] systems eliminated, [1] systems summed as a series, [2] series steps
+  unsigned long long* work = nullptr;
 };
 
 struct RtWS {
@@ -695,6 +705,88 @@ constexpr int kRtThreads = kRtGroups * RtG::N;
 
 // shared memory: RHOX and a zero vector (SIGMAL) for the CTA, then the groups' workspaces
 __host__ __device__ inline size_t rt_smem_bytes() { return 2 * sizeof(double) * kKwMax + kRtGroups * sizeof(RtWS); }
+
+// After JOSH: the negative floor (RUN_RT_PASS :3926-3937), HNU(1) for the
+// .flux record, and the TCORR / RADIAP / ROSS mode-2 terms of this frequency
+// added into the group's accumulators (threads over depths, C per thread).
+// add(q, c, j, v) adds term q of depth j (the thread's c-th depth) to its sum.
+template <class G, class WS, int C, class Add>
+static __device__ __forceinline__ void rt_accumulate(G& g, const RtArgs& a, WS& S, const double* rhox_s, int nu,
+                                                     double freq, double rcowt, Add&& add, double& pradk0) {
+  const int nr = a.nrhox;
+  // negative floor (RUN_RT_PASS :3926-3937)
+  bool neg = false;
+  for (int j = g.r; j < nr; j += G::N) neg |= (S.f.snu[j] < 0.0 || S.f.jnu[j] < 0.0 || S.f.hnu[j] < 0.0);
+  if (g.any(neg)) {
+    for (int j = g.r; j < nr; j += G::N) {
+      S.f.jnu[j] = fmax(S.f.jnu[j], 1.0e-99);
+      S.f.snu[j] = fmax(S.f.snu[j], 1.0e-99);
+      S.f.hnu[j] = fmax(S.f.hnu[j], 1.0e-99);
+    }
+    g.sync();
+  }
+  if (g.r == 0) a.hsurf[nu - 1] = S.f.hnu[0];
+  // TCORR mode 2: d(abtot)/d(rhox)
+  g_deriv(g, rhox_s, S.w.abtot, S.dab, nr);
+  // TERM2 per depth (E3 diagonal of Lambda); D(NRHOX) repeats D(NRHOX-1)
+  for (int j = g.r; j < nr; j += G::N) {
+    const int jd = j < nr - 1 ? j : nr - 2;
+    double d = S.w.taunu[jd + 1] - S.w.taunu[jd];
+    d = fmax(1.0e-10, d);
+    double term2;
+    if (d <= 0.01) {
+      term2 = (kEulerM1 - log(d)) * d / 4.0 + (d * d) / 12.0 - (d * d * d) / 96.0 +
+              ((d * d) * (d * d)) / 720.0;
+    } else {
+      double ex = 0.0;
+      if (d < 10.0) ex = expi3(d);
+      if (a.teff <= 4250.0 && d > 0.005 && d < 0.02) ex = 0.0;
+      term2 = 0.5 * (d + ex - 0.5) / d;
+    }
+    S.w.t1[j] = term2;
+  }
+  g.sync();
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const int j = g.r + c * G::N;
+    if (j >= nr) break;
+    const double ab = S.w.abtot[j], al = S.w.alpha[j], h = S.f.hnu[j];
+    const double rab = 1.0 / ab;
+    add(1, c, j, S.dab[j] * rab * h * rcowt);                // RDABH
+    add(0, c, j, ab * S.f.jmins[j] * rcowt);                 // RJMINS
+    add(3, c, j, h * rcowt);                                 // FLXRAD
+    const double diagj = (j > 0 ? S.w.t1[j - 1] : 0.0) + S.w.t1[j];
+    const double hk = a.hkt[j], tt = a.t[j];
+    // dB/dT = BNU * freq * HKT / T / STIM (floored at 1e-30 for RDIAGJ, as the reference)
+    const double bft = S.f.bnu[j] * freq * hk / tt;
+    const double dbdt = bft / fmax(S.stim[j], 1.0e-30);
+    add(2, c, j, ab * (diagj - 1.0) / (1.0 - al * diagj) * (1.0 - al) * dbdt * rcowt);  // RDIAGJ
+    add(4, c, j, S.f.jnu[j] * rcowt);                        // RADEN
+    add(5, c, j, h * rcowt);                                 // H_TOTAL
+    add(6, c, j, ab * h * rcowt);                            // ACCRAD
+    const double dbdt2 = (S.stim[j] >= 1.0e-30) ? dbdt : bft / S.stim[j];
+    add(7, c, j, dbdt2 * rab * rcowt);                       // ABROSS
+  }
+  pradk0 += S.f.knu1 * rcowt;
+}
+
+// A group's partial-sum row.  The whole row is written: depths nrhox..kw-1
+// (padding when kw > nrhox) get zeros, so the fixed-order reduction never
+// sums stale entries.
+template <class G, int C>
+static __device__ __forceinline__ void rt_write_partial(G& g, const RtArgs& a, int row, const double (&acc)[kAcc][C],
+                                                        double pradk0) {
+  double* out = a.partial + (size_t)row * (kAcc * a.kw + 1);
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const int j = g.r + c * G::N;
+    if (j < a.kw) {
+#pragma unroll
+      for (int q = 0; q < kAcc; ++q) out[q * a.kw + j] = j < a.nrhox ? acc[q][c] : 0.0;
+    }
+  }
+  if (g.r == 0) out[kAcc * a.kw] = pradk0;
+}
 
 static __device__ __forceinline__ void rt_body(const RtArgs& a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -740,77 +832,381 @@ static __device__ __forceinline__ void rt_body(const RtArgs& a) {
     const int sw = g_josh(g, ops, rhox_s, nr, S.acont, S.aline, S.sigmac, zero_s, a.scont ? S.dab : S.f.bnu,
                           S.f.bnu, S.f.bnu, S.w, S.U, &S.f, nullptr);
     if (a.sweeps && g.r == 0) a.sweeps[nu - 1] = sw;
-    // negative floor (RUN_RT_PASS :3926-3937)
-    bool neg = false;
-    for (int j = g.r; j < nr; j += RtG::N) neg |= (S.f.snu[j] < 0.0 || S.f.jnu[j] < 0.0 || S.f.hnu[j] < 0.0);
-    if (g.any(neg)) {
-      for (int j = g.r; j < nr; j += RtG::N) {
-        S.f.jnu[j] = fmax(S.f.jnu[j], 1.0e-99);
-        S.f.snu[j] = fmax(S.f.snu[j], 1.0e-99);
-        S.f.hnu[j] = fmax(S.f.hnu[j], 1.0e-99);
-      }
-      g.sync();
-    }
-    if (g.r == 0) a.hsurf[nu - 1] = S.f.hnu[0];
-    // TCORR mode 2: d(abtot)/d(rhox)
-    g_deriv(g, rhox_s, S.w.abtot, S.dab, nr);
-    // TERM2 per depth (E3 diagonal of Lambda); D(NRHOX) repeats D(NRHOX-1)
-    for (int j = g.r; j < nr; j += RtG::N) {
-      const int jd = j < nr - 1 ? j : nr - 2;
-      double d = S.w.taunu[jd + 1] - S.w.taunu[jd];
-      d = fmax(1.0e-10, d);
-      double term2;
-      if (d <= 0.01) {
-        term2 = (kEulerM1 - log(d)) * d / 4.0 + (d * d) / 12.0 - (d * d * d) / 96.0 +
-                ((d * d) * (d * d)) / 720.0;
-      } else {
-        double ex = 0.0;
-        if (d < 10.0) ex = expi3(d);
-        if (a.teff <= 4250.0 && d > 0.005 && d < 0.02) ex = 0.0;
-        term2 = 0.5 * (d + ex - 0.5) / d;
-      }
-      S.w.t1[j] = term2;
-    }
-    g.sync();
-#pragma unroll
-    for (int c = 0; c < C; ++c) {
-      const int j = g.r + c * RtG::N;
-      if (j >= nr) break;
-      const double ab = S.w.abtot[j], al = S.w.alpha[j], h = S.f.hnu[j];
-      const double rab = 1.0 / ab;
-      acc[1][c] += S.dab[j] * rab * h * rcowt;                // RDABH
-      acc[0][c] += ab * S.f.jmins[j] * rcowt;                 // RJMINS
-      acc[3][c] += h * rcowt;                                 // FLXRAD
-      const double diagj = (j > 0 ? S.w.t1[j - 1] : 0.0) + S.w.t1[j];
-      const double hk = a.hkt[j], tt = a.t[j];
-      // dB/dT = BNU * freq * HKT / T / STIM (floored at 1e-30 for RDIAGJ, as the reference)
-      const double bft = S.f.bnu[j] * freq * hk / tt;
-      const double dbdt = bft / fmax(S.stim[j], 1.0e-30);
-      acc[2][c] += ab * (diagj - 1.0) / (1.0 - al * diagj) * (1.0 - al) * dbdt * rcowt;  // RDIAGJ
-      acc[4][c] += S.f.jnu[j] * rcowt;                        // RADEN
-      acc[5][c] += h * rcowt;                                 // H_TOTAL
-      acc[6][c] += ab * h * rcowt;                            // ACCRAD
-      const double dbdt2 = (S.stim[j] >= 1.0e-30) ? dbdt : bft / S.stim[j];
-      acc[7][c] += dbdt2 * rab * rcowt;                       // ABROSS
-    }
-    pradk0 += S.f.knu1 * rcowt;
+    rt_accumulate<RtG, RtWS, C>(
+        g, a, S, rhox_s, nu, freq, rcowt, [&](int q, int c, int, double v) { acc[q][c] += v; }, pradk0);
     g.sync();
   }
-  // the whole row is written: depths nrhox..kw-1 (padding when kw > nrhox)
-  // get zeros, so the fixed-order reduction never sums stale entries
-  double* out = a.partial + (size_t)gw * (kAcc * a.kw + 1);
-#pragma unroll
-  for (int c = 0; c < C; ++c) {
-    const int j = g.r + c * RtG::N;
-    if (j < a.kw) {
-#pragma unroll
-      for (int q = 0; q < kAcc; ++q) out[q * a.kw + j] = j < nr ? acc[q][c] : 0.0;
-    }
-  }
-  if (g.r == 0) out[kAcc * a.kw] = pradk0;
+  rt_write_partial(g, a, gw, acc, pradk0);
 }
 
 static __global__ void __launch_bounds__(kRtThreads, kRtMinBlocks) k_atlas_rt(RtArgs a) { rt_body(a); }
+
+// ---------------------------------------------------------------- split RT pass
+// The same pass in three launches.  JOSH's 51x51 solve needs ~100 registers
+// of matrix row per thread, which caps the fused kernel at six frequencies
+// per SM; its vector work (INTEG, the MAP1s, the Eddington sweeps, the
+// operator products, DERIV and the mode-2 sums) is a chain of short
+// barrier-separated steps that wants many frequencies in flight instead.
+//   k_rt_pre    warp per frequency: STIM, BNU, ABTOT, ALPHA, SNUBAR, TAUNU,
+//               MAXJ, XSBAR and XALPHA on the 51-point grid
+//   k_rt_solve  pair group per frequency that needs it: the scattering system
+//   k_rt_post   warp per frequency: the rest of JOSH and the mode-2 sums,
+//               one partial-sum row per warp (reduced in fixed order)
+// Each frequency's record goes from stage to stage through device memory,
+// rec_stride doubles: TAUNU [kw], then on the 51-point grid XALPHA, XSBAR
+// and XS, then MAXJ and the solve flag.  Every value is computed by the same
+// expressions as in the fused kernel.  (Forming J - S and H in the solve
+// stage as well, where COEFJ and COEFH stay in L1, measured slower: 2.00
+// against 1.85 ms per model-iteration.)
+struct RtRec {
+  int kw;
+  __host__ __device__ int xalpha() const { return kw; }
+  __host__ __device__ int xsbar() const { return kw + kNx; }
+  __host__ __device__ int xs() const { return kw + 2 * kNx; }
+  __host__ __device__ int maxj() const { return kw + 3 * kNx; }
+  __host__ __device__ int solve() const { return kw + 3 * kNx + 1; }
+};
+__host__ __device__ inline int rt_rec_stride(int kw) { return (kw + 3 * kNx + 2 + 1) & ~1; }
+
+// STIM, BNU and JOSH's ABTOT, ALPHA, SNUBAR (SIGMAL = 0, SLINE = BNU) of one
+// depth at frequency NU, as the fused kernel forms them (RUN_RT_PASS
+// :3905-3922, JOSH :18491-18500)
+struct RtDepth {
+  double stim, bnu, abtot, alpha, snubar;
+};
+__device__ __forceinline__ RtDepth rt_depth(const RtArgs& a, int nu, double freq, double f3, int j) {
+  const double ehvkt = exp(-freq * a.hkt[j]);
+  const double stim = 1.0 - ehvkt;
+  const double bnu = kBnuPrefac * f3 * ehvkt / stim;
+  const double ac = a.acont[(size_t)(nu - 1) * a.kw + j];
+  const double sg = a.sigmac[(size_t)(nu - 1) * a.kw + j];
+  const double sc = a.scont ? a.scont[(size_t)(nu - 1) * a.kw + j] : bnu;
+  const double al = 0.0 + a.xl[(size_t)j * a.xl_sj + (size_t)(nu - 1) * a.xl_snu] * stim;
+  const double sl = 0.0;
+  RtDepth d;
+  d.stim = stim;
+  d.bnu = bnu;
+  d.abtot = ac + al + sg + sl;
+  d.alpha = (sg + sl) / d.abtot;
+  d.snubar = (ac * sc + al * bnu) / (ac + al);
+  return d;
+}
+
+constexpr int kRtSplitWarps = 4;      // warps per CTA of the pre and post stages
+constexpr int kRtSolveGroups = 2;     // pair groups per CTA of the solve stage
+constexpr int kRtSolveThreads = kRtSolveGroups * PairG::N;
+constexpr int kRtSolveMinBlocks = 4;  // 8 systems per SM (128 registers per thread)
+
+struct RtPreWS {
+  double abtot[kKwMax], alpha[kKwMax], snubar[kKwMax], taunu[kKwMax];
+  double t1[kKwMax], t2[kKwMax], t3[kKwMax];
+  double xsbar[kNx], xalpha[kNx], xs[kNx];
+  int lidx[kKwMax + 4];
+};
+struct RtSolveWS {
+  double xs[kNx], xsbar[kNx], xalpha[kNx], piv[kNx];
+  double rowabs[kNx], xb[kNx];  // row sums of |COEFJ|; the series' second buffer
+  double red[8];
+  unsigned pk[4][3];
+  alignas(16) double U[kNx * (kNx + 1)];
+};
+// The post stage's workspace: one warp's vectors carved from shared memory
+// at a stride of kv >= NRHOX doubles (rt_post_kv), its 51-point vectors, the
+// mode-2 sums of the warp's depths (kAcc x kv) and two scalars.
+struct RtPostFull {
+  double *snu, *hnu, *jmins, *jnu, *bnu;
+  double& knu1;
+  int& maxj;
+};
+struct RtPostVec {
+  double *abtot, *alpha, *snubar, *taunu, *t1, *t2, *t3, *xs, *xsbar, *xw;
+  int* lidx;
+};
+struct RtPostView {
+  RtPostVec w;
+  RtPostFull f;
+  double *stim, *dab, *acc;
+};
+__host__ __device__ inline int rt_post_kv(int nrhox) { return (nrhox + 1) & ~1; }
+__host__ __device__ inline size_t rt_post_warp_doubles(int kv) {
+  return (size_t)(12 + kAcc) * kv + 3 * kNx + 2 + (kv + 4 + 1) / 2 + 1;
+}
+__host__ __device__ inline size_t rt_pre_smem_bytes() { return sizeof(double) * kKwMax + kRtSplitWarps * sizeof(RtPreWS); }
+__host__ __device__ inline size_t rt_solve_smem_bytes() { return kRtSolveGroups * sizeof(RtSolveWS); }
+__host__ __device__ inline size_t rt_post_smem_bytes(int nrhox) {
+  return sizeof(double) * (kKwMax + kRtSplitWarps * rt_post_warp_doubles(rt_post_kv(nrhox)));
+}
+
+__device__ __forceinline__ double* rt_rec(const RtArgs& a, int nu) {
+  return a.rec + (size_t)(nu - a.nu_first) * a.rec_stride;
+}
+
+static __device__ __forceinline__ void rt_pre_body(const RtArgs& a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* rhox_s = reinterpret_cast<double*>(smem_raw);
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  RtPreWS& S = reinterpret_cast<RtPreWS*>(smem_raw + sizeof(double) * kKwMax)[wid];
+  for (int j = threadIdx.x; j < a.nrhox; j += blockDim.x) rhox_s[j] = a.rhox[j];
+  __syncthreads();
+  WarpG g(lane);
+  const JoshOps& ops = *a.ops;
+  const int nr = a.nrhox, kw = a.kw;
+  const int w = blockIdx.x * kRtSplitWarps + wid;
+  const int nu0 = a.nu_first + w * a.nu_per_pre;
+  const int nu1 = min(nu0 + a.nu_per_pre - 1, a.nu_last > 0 ? a.nu_last : a.numnu);
+  for (int nu = nu0; nu <= nu1; ++nu) {
+    const double freq = kClightNms / a.waveset[nu - 1];
+    const double f3 = powi(freq / 1.0e15, 3);
+    for (int j = lane; j < nr; j += 32) {
+      const RtDepth d = rt_depth(a, nu, freq, f3, j);
+      S.abtot[j] = d.abtot;
+      S.alpha[j] = d.alpha;
+      S.snubar[j] = d.snubar;
+    }
+    g.sync();
+    bool mapped, solve;
+    // (with IFSURF = 0 a mapped surface with MAXJ = 1 ends as an unmapped
+    // one: the sweeps overwrite SNU at every depth, so XS is not needed)
+    const int maxj = g_josh_prepare(g, ops, rhox_s, nr, S, mapped, solve);
+    (void)mapped;
+    double* rec = rt_rec(a, nu);
+    const RtRec R{kw};
+    for (int j = lane; j < nr; j += 32) rec[j] = S.taunu[j];
+    if (maxj != 1) {
+      for (int l = lane; l < kNx; l += 32) {
+        rec[R.xalpha() + l] = S.xalpha[l];
+        rec[R.xsbar() + l] = S.xsbar[l];
+        if (!solve) rec[R.xs() + l] = S.xs[l];
+      }
+    }
+    if (lane == 0) {
+      rec[R.maxj()] = (double)maxj;
+      rec[R.solve()] = (solve && maxj != 1) ? 1.0 : 0.0;
+    }
+    g.sync();
+  }
+}
+
+// The scattering system X = (1 - XALPHA) XSBAR + XALPHA (COEFJ X) is a
+// contraction with factor q = max_l XALPHA(l) sum_m |COEFJ(l,m)| (the
+// infinity norm of diag(XALPHA) COEFJ).  Where q <= kRtSeriesQ the solve
+// stage sums its Neumann series instead of eliminating: K steps of
+// X <- (1 - XALPHA) XSBAR + XALPHA (COEFJ X) from X = (1 - XALPHA) XSBAR
+// leave an error of at most q^(K+1) |X|, and K is taken so that
+// q^(K+1) <= 2^-60, far below the rounding of the elimination itself (the
+// two solutions agree to rounding).  A step is one matrix-vector product
+// with no sequential dependence between rows: about 1/20 of the
+// elimination's latency, so the series is cheaper up to q ~ 0.5.  Systems
+// with larger q (strongly scattering layers) are eliminated as SOLVIT does.
+constexpr double kRtSeriesQ = 0.5;
+constexpr int kRtSeriesMaxSteps = 64;
+
+__device__ __forceinline__ int rt_series_steps(double q) {
+  if (!(q > 0.0)) return 1;
+  const int k = (int)ceil(-60.0 * 0.6931471805599453 / log(q)) - 1;
+  return k < 1 ? 1 : (k > kRtSeriesMaxSteps ? kRtSeriesMaxSteps : k);
+}
+
+// K series steps by a pair group, thread l < 51 owning X(l); two buffers in
+// shared memory (one barrier per step).  Result in ws.xs.
+template <class G>
+__device__ __forceinline__ void rt_solve_series(G& g, const JoshOps& ops, RtSolveWS& S, int K) {
+  const int l = g.r;
+  const bool own = l < kNx;
+  const double al = own ? S.xalpha[l] : 0.0;
+  const double b = own ? (1.0 - al) * S.xsbar[l] : 0.0;
+  double* cur = S.xs;
+  double* nxt = S.xb;
+  if (own) cur[l] = b;
+  for (int k = 0; k < K; ++k) {
+    g.sync();
+    if (own) {
+      double s4[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 3
+      for (int m0 = 0; m0 < kNx - kNx % 4; m0 += 4) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) s4[q] = s4[q] + ops.coefj[(m0 + q) * kNx + l] * cur[m0 + q];
+      }
+#pragma unroll
+      for (int q = 0; q < kNx % 4; ++q) {
+        const int m = kNx - kNx % 4 + q;
+        s4[q] = s4[q] + ops.coefj[m * kNx + l] * cur[m];
+      }
+      nxt[l] = b + al * ((s4[0] + s4[1]) + (s4[2] + s4[3]));
+    }
+    double* t = cur;
+    cur = nxt;
+    nxt = t;
+  }
+  g.sync();
+  if (own && cur != S.xs) S.xs[l] = cur[l];
+  g.sync();
+}
+
+static __device__ __forceinline__ void rt_solve_body(const RtArgs& a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int gid = threadIdx.x / PairG::N;
+  RtSolveWS& S = reinterpret_cast<RtSolveWS*>(smem_raw)[gid];
+  PairG g(threadIdx.x % PairG::N, 1 + gid, S.red);
+  const JoshOps& ops = *a.ops;
+  const int kw = a.kw;
+  const int grp = blockIdx.x * kRtSolveGroups + gid;
+  const int nu0 = a.nu_first + grp * a.nu_per_solve;
+  const int nu1 = min(nu0 + a.nu_per_solve - 1, a.nu_last > 0 ? a.nu_last : a.numnu);
+  for (int l = g.r; l < kNx; l += PairG::N) {
+    double r = 0.0;
+    for (int m = 0; m < kNx; ++m) r += fabs(ops.coefj[m * kNx + l]);
+    S.rowabs[l] = r;
+  }
+  g.sync();
+  unsigned long long nelim = 0, nseries = 0, nsteps = 0;
+  const RtRec R{kw};
+  for (int nu = nu0; nu <= nu1; ++nu) {
+    double* rec = rt_rec(a, nu);
+    if (rec[R.solve()] == 0.0) continue;  // the same word for the whole group
+    {
+      double qv = 0.0;
+      for (int l = g.r; l < kNx; l += PairG::N) {
+        const double xa = rec[R.xalpha() + l];
+        S.xalpha[l] = xa;
+        S.xsbar[l] = rec[R.xsbar() + l];
+        qv = fmax(qv, xa * S.rowabs[l]);
+      }
+      const double q = g.max(qv);  // (its barrier also publishes XALPHA, XSBAR)
+      if (q <= kRtSeriesQ) {
+        const int K = rt_series_steps(q);
+        rt_solve_series(g, ops, S, K);
+        ++nseries;
+        nsteps += K;
+      } else {
+        solve_scatter(g, ops, S, S.U);
+        ++nelim;
+      }
+    }
+    for (int l = g.r; l < kNx; l += PairG::N) rec[R.xs() + l] = S.xs[l];
+    g.sync();
+  }
+  if (a.work && g.r == 0 && (nelim | nseries)) {
+    atomicAdd(a.work, nelim);
+    atomicAdd(a.work + 1, nseries);
+    atomicAdd(a.work + 2, nsteps);
+  }
+}
+
+static __device__ __forceinline__ void rt_post_body(const RtArgs& a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* rhox_s = reinterpret_cast<double*>(smem_raw);
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nr = a.nrhox, kw = a.kw, kv = rt_post_kv(nr);
+  double* p = rhox_s + kKwMax + (size_t)wid * rt_post_warp_doubles(kv);
+  auto take = [&](size_t n) {
+    double* q = p;
+    p += n;
+    return q;
+  };
+  double *abtot = take(kv), *alpha = take(kv), *snubar = take(kv), *taunu = take(kv), *t1 = take(kv);
+  double *snu = take(kv), *hnu = take(kv), *jmins = take(kv), *jnu = take(kv), *bnu = take(kv);
+  double *stim = take(kv), *dab = take(kv), *acc = take((size_t)kAcc * kv);
+  double *xs = take(kNx), *xsbar = take(kNx), *xw = take(kNx);
+  double* knu1 = take(1);
+  int* maxj_s = reinterpret_cast<int*>(take(1));
+  int* lidx = reinterpret_cast<int*>(take((kv + 4 + 1) / 2));
+  // t2 and t3 serve JOSH only with IFSURF = 1, which this stage never runs
+  RtPostView S{RtPostVec{abtot, alpha, snubar, taunu, t1, t1, t1, xs, xsbar, xw, lidx},
+               RtPostFull{snu, hnu, jmins, jnu, bnu, *knu1, *maxj_s}, stim, dab, acc};
+  for (int j = threadIdx.x; j < nr; j += blockDim.x) rhox_s[j] = a.rhox[j];
+  for (int e = lane; e < kAcc * kv; e += 32) acc[e] = 0.0;
+  __syncthreads();
+  WarpG g(lane);
+  constexpr int C = (kKwMax + 31) / 32;
+  const JoshOps& ops = *a.ops;
+  const int w = blockIdx.x * kRtSplitWarps + wid;  // partial-sum row of this warp
+  const int nu0 = a.nu_first + w * a.nu_per_warp;
+  const int nu1 = min(nu0 + a.nu_per_warp - 1, a.nu_last > 0 ? a.nu_last : a.numnu);
+  double pradk0 = 0.0;
+  for (int nu = nu0; nu <= nu1; ++nu) {
+    const double freq = kClightNms / a.waveset[nu - 1];
+    const double rcowt = a.rcoset[nu - 1];
+    const double f3 = powi(freq / 1.0e15, 3);
+    const double* rec = rt_rec(a, nu);
+    const RtRec R{kw};
+    const int maxj = (int)rec[R.maxj()];
+    for (int j = lane; j < nr; j += 32) {
+      const RtDepth d = rt_depth(a, nu, freq, f3, j);
+      abtot[j] = d.abtot;
+      alpha[j] = d.alpha;
+      snubar[j] = d.snubar;
+      stim[j] = d.stim;
+      bnu[j] = d.bnu;
+      taunu[j] = rec[j];
+    }
+    if (maxj != 1)
+      for (int l = lane; l < kNx; l += 32) xs[l] = rec[R.xs() + l];
+    g.sync();
+    const int sw = g_josh_finish(g, ops, nr, maxj, maxj != 1, S.w, &S.f, bnu, (double*)nullptr);
+    if (a.sweeps && lane == 0) a.sweeps[nu - 1] = sw;
+    rt_accumulate<WarpG, RtPostView, C>(
+        g, a, S, rhox_s, nu, freq, rcowt, [&](int q, int, int j, double v) { acc[q * kv + j] += v; }, pradk0);
+    g.sync();
+  }
+  double* out = a.partial + (size_t)w * (kAcc * kw + 1);
+  for (int j = lane; j < kw; j += 32) {
+#pragma unroll
+    for (int q = 0; q < kAcc; ++q) out[q * kw + j] = j < nr ? acc[q * kv + j] : 0.0;
+  }
+  if (lane == 0) out[kAcc * kw] = pradk0;
+}
+
+static __global__ void __launch_bounds__(kRtSplitWarps * 32, 6) k_rt_pre(RtArgs a) { rt_pre_body(a); }
+static __global__ void __launch_bounds__(kRtSolveThreads, kRtSolveMinBlocks) k_rt_solve(RtArgs a) { rt_solve_body(a); }
+static __global__ void __launch_bounds__(kRtSplitWarps * 32, 4) k_rt_post(RtArgs a) { rt_post_body(a); }
+
+// Launch shape of the split pass over LEN frequencies with 1/NB of the GPU
+// (NB slots of a batch share it): every stage gets about WAVES resident waves
+// of its units (warps or pair groups), frequencies contiguous per unit.
+struct RtSplitShape {
+  int pre_per = 1, pre_blocks = 1, solve_per = 1, solve_blocks = 1, post_per = 1, post_blocks = 1;
+  int rows() const { return post_blocks * kRtSplitWarps; }
+};
+inline void rt_split_fit(int len, int units, int per_block, int& per, int& blocks) {
+  per = (len + units - 1) / units;
+  if (per < 1) per = 1;
+  const int n = (len + per - 1) / per;
+  blocks = (n + per_block - 1) / per_block;
+}
+inline RtSplitShape rt_split_shape(int len, int nsm, int nb, int waves) {
+  RtSplitShape sh;
+  auto units = [&](int per_sm) {
+    const long long u = (long long)nsm * per_sm * waves / (nb > 0 ? nb : 1);
+    return (int)(u < 1 ? 1 : u);
+  };
+  rt_split_fit(len, units(16), kRtSplitWarps, sh.pre_per, sh.pre_blocks);
+  rt_split_fit(len, units(8), kRtSolveGroups, sh.solve_per, sh.solve_blocks);
+  rt_split_fit(len, units(16), kRtSplitWarps, sh.post_per, sh.post_blocks);
+  return sh;
+}
+// the most partial-sum rows any frequency range of a model can need
+// (rt_split_shape never makes more post warps than frequencies or units)
+inline int rt_split_rows_max(int numnu, int nsm, int waves) {
+  const long long units = (long long)nsm * 16 * waves;
+  const long long n = numnu < units ? numnu : units;
+  return (int)((n + kRtSplitWarps - 1) / kRtSplitWarps * kRtSplitWarps);
+}
+// shared-memory opt-in of the three stages (nrhox <= kKwMax)
+inline cudaError_t rt_split_attributes(int nrhox) {
+  cudaError_t e = cudaFuncSetAttribute(k_rt_pre, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rt_pre_smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_rt_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rt_solve_smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_rt_post, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rt_post_smem_bytes(nrhox));
+  return e;
+}
+inline void rt_split_args(RtArgs& a, const RtSplitShape& sh) {
+  a.nu_per_pre = sh.pre_per;
+  a.nu_per_solve = sh.solve_per;
+  a.nu_per_warp = sh.post_per;
+  a.rec_stride = rt_rec_stride(a.kw);
+}
 
 // fixed-order sum of the per-warp partials: out[kAcc*kw + 1].  A block owns
 // 32 consecutive sums (threadIdx.x) and splits the rows over 32 row groups

@@ -153,9 +153,9 @@ __device__ inline void g_parcoe(G& g, const double* f, const double* x, double* 
 }
 
 // fint = running parabolic integral of f over x, fint[0] = start
-template <class G>
+template <class G, class WS>
 __device__ inline void g_integ(G& g, const double* x, const double* f, double* fint, int n, double start,
-                               JoshWS& ws) {
+                               WS& ws) {
   double *a = ws.t1, *b = ws.t2, *c = ws.t3;
   g_parcoe(g, f, x, a, b, c, n);
   for (int i = g.r; i < n - 1; i += G::N) {
@@ -478,7 +478,8 @@ __device__ __forceinline__ void u_back_substitute(int r, const double* U, double
 // for the other rows' update and for the back substitution.
 // The pivot search reduces a 64-bit key (|a| bits, then position) with
 // redux.sync per warp and one exchange between the two warps.
-static __device__ __forceinline__ void scatter_solve(PairG& g, const JoshOps& ops, JoshWS& ws, double* U) {
+template <class WS>
+static __device__ __forceinline__ void scatter_solve(PairG& g, const JoshOps& ops, WS& ws, double* U) {
   constexpr int n = kNx, W = kNx + 1;
   constexpr unsigned FULL = 0xffffffffu;
   const bool own = g.r < n;
@@ -562,7 +563,8 @@ static __device__ __forceinline__ void scatter_solve(PairG& g, const JoshOps& op
 // happened; otherwise the operations were exactly SOLVIT's, in its order.
 // (For these systems it does not happen: AMAT is column diagonally dominant
 // because the columns of COEFJ sum to at most 1 and XALPHA < 1.)
-static __device__ __forceinline__ bool scatter_solve_nopivot(PairG& g, const JoshOps& ops, JoshWS& ws, double* U) {
+template <class WS>
+static __device__ __forceinline__ bool scatter_solve_nopivot(PairG& g, const JoshOps& ops, WS& ws, double* U) {
   constexpr int n = kNx, W = kNx + 1;
   const bool own = g.r < n;
   double a[W];
@@ -607,7 +609,8 @@ static __device__ __forceinline__ bool scatter_solve_nopivot(PairG& g, const Jos
 }
 
 
-__device__ __forceinline__ void solve_scatter(PairG& g, const JoshOps& ops, JoshWS& ws, double* U) {
+template <class WS>
+__device__ __forceinline__ void solve_scatter(PairG& g, const JoshOps& ops, WS& ws, double* U) {
   if (!scatter_solve_nopivot(g, ops, ws, U)) scatter_solve(g, ops, ws, U);
 }
 __device__ __forceinline__ void solve_scatter(WarpG& g, const JoshOps& ops, JoshWS& ws, double* A) {
@@ -615,16 +618,20 @@ __device__ __forceinline__ void solve_scatter(WarpG& g, const JoshOps& ops, Josh
 }
 
 // ---------------------------------------------------------------- JOSH
-// Inputs in ws.*: abtot/alpha/snubar are formed here from the opacity
-// vectors.  rhox is shared by the CTA.  ifsurf = 1 returns H(1); ifsurf = 0
-// fills full (SNU, JNU, HNU, JMINS, KNU(1), MAXJ) as the reference does.
-// A: shared-memory matrix for a warp group, the U rows for a pair group.
-// Returns the number of Eddington sweeps run (0 if none).
-template <class G>
-__device__ inline int g_josh(G& g, const JoshOps& ops, const double* rhox, int nr, const double* acont,
-                             const double* aline, const double* sigmac, const double* sigmal,
-                             const double* scont, const double* sline, const double* bnu, JoshWS& ws,
-                             double* A, JoshWSFull* full, double* hsurf) {
+// JOSH in three parts, so that a caller may run them in separate launches
+// (the ATLAS12 RT pass runs the 51x51 solve in its own kernel):
+//   g_josh_prepare  TAUNU = INTEG(ABTOT dRHOX), MAXJ, and for MAXJ != 1 XSBAR
+//                   and XALPHA on the 51-point grid with their floors
+//                   (atlas12_modules.f90:18491-18570); solve = max XALPHA > 0,
+//                   otherwise XS = XSBAR
+//   solve_scatter   (I - diag(XALPHA) COEFJ) XS = (1 - XALPHA) XSBAR
+//   g_josh_finish   XS floor, IFSURF = 1 surface flux or SNU = MAP1(XS),
+//                   the Eddington sweeps below MAXJ, J/H/K from the operators
+//                   mapped back onto the depths (:18571-18776)
+// ws.abtot, ws.alpha and ws.snubar are formed by the caller (g_josh_fill).
+template <class G, class WS>
+__device__ inline void g_josh_fill(G& g, int nr, const double* acont, const double* aline, const double* sigmac,
+                                   const double* sigmal, const double* scont, const double* sline, WS& ws) {
   for (int j = g.r; j < nr; j += G::N) {
     const double ab = acont[j] + aline[j] + sigmac[j] + sigmal[j];
     ws.abtot[j] = ab;
@@ -632,10 +639,19 @@ __device__ inline int g_josh(G& g, const JoshOps& ops, const double* rhox, int n
     ws.snubar[j] = (acont[j] * scont[j] + aline[j] * sline[j]) / (acont[j] + aline[j]);
   }
   g.sync();
+}
+
+// mapped: the surface is optically thin enough for the 51-point grid (MAP1
+// may still return MAXJ = 1 there, and IFSURF = 1 then takes H(1) from XS).
+template <class G, class WS>
+__device__ inline int g_josh_prepare(G& g, const JoshOps& ops, const double* rhox, int nr, WS& ws, bool& mapped,
+                                     bool& solve) {
   g_integ(g, rhox, ws.abtot, ws.taunu, nr, ws.abtot[0] * rhox[0], ws);
   int maxj = 0;
+  solve = false;
   if (ws.taunu[0] > ops.xtau[kNx - 1]) maxj = 1;
-  if (maxj != 1) {
+  mapped = maxj != 1;
+  if (mapped) {
     maxj = g_map1(g, ws.taunu, ws.snubar, nr, ops.xtau, ws.xsbar, kNx, ws.lidx);
     maxj = g_map1(g, ws.taunu, ws.alpha, nr, ops.xtau, ws.xalpha, kNx, ws.lidx);
     const double tau1 = ws.taunu[0];
@@ -653,11 +669,63 @@ __device__ inline int g_josh(G& g, const JoshOps& ops, const double* rhox, int n
     }
     amax = g.max(amax);
     g.sync();
-    if (amax <= 0.0) {
-      for (int l = g.r; l < kNx; l += G::N) ws.xs[l] = fmax(ws.xsbar[l], 1.0e-37);
+    solve = amax > 0.0;
+    if (!solve) {
+      for (int l = g.r; l < kNx; l += G::N) ws.xs[l] = ws.xsbar[l];
       g.sync();
-    } else {
-      solve_scatter(g, ops, ws, A);
+    }
+  }
+  return maxj;
+}
+
+// J - S and H on the 51-point grid from XS (COEFJ.XS - XS into xw, COEFH.XS
+// into xh), four interleaved partial sums per product (instruction-level
+// parallelism instead of one 51-long dependent chain; the grouping differs
+// from the reference's sequential sum only at rounding level), and
+// KNU(1) = CK.XS in the reference order (:18700-18735)
+template <class G>
+__device__ __forceinline__ void josh_operators(G& g, const JoshOps& ops, const double* xs, double* xw, double* xh,
+                                               double* knu1) {
+  for (int l = g.r; l < kNx; l += G::N) {
+    double sj[4] = {0.0, 0.0, 0.0, 0.0}, sh[4] = {0.0, 0.0, 0.0, 0.0};
+    // sum k takes the terms mm = k, k+4, k+8, ... in that order
+#pragma unroll 2
+    for (int m0 = 0; m0 < kNx - kNx % 4; m0 += 4) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const double x = xs[m0 + k];
+        sj[k] = sj[k] + ops.coefj[(m0 + k) * kNx + l] * x;
+        sh[k] = sh[k] + ops.coefh[(m0 + k) * kNx + l] * x;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kNx % 4; ++k) {
+      const int mm = kNx - kNx % 4 + k;
+      const double x = xs[mm];
+      sj[k] = sj[k] + ops.coefj[mm * kNx + l] * x;
+      sh[k] = sh[k] + ops.coefh[mm * kNx + l] * x;
+    }
+    xw[l] = -xs[l] + ((sj[0] + sj[1]) + (sj[2] + sj[3]));
+    xh[l] = (sh[0] + sh[1]) + (sh[2] + sh[3]);
+  }
+  if (g.r == 0) {
+    double xk = 0.0;
+    for (int mm = 0; mm < kNx; ++mm) xk = xk + ops.ck[mm] * xs[mm];
+    *knu1 = xk;
+  }
+}
+
+// ws.xs holds the solution (or XSBAR); ws.taunu, ws.alpha, ws.snubar as
+// g_josh_prepare left them.  full (JoshWSFull or a view with the same
+// members in shared memory) receives SNU, HNU, JMINS, JNU, KNU(1), MAXJ, or
+// is null for IFSURF = 1.  Returns the number of Eddington sweeps run.
+// kOpsGiven: the caller has floored XS and formed XW (J - S), XH (in
+// ws.xsbar) and KNU(1) with josh_operators already.
+template <bool kOpsGiven = false, class G, class WS, class FullT>
+__device__ inline int g_josh_finish(G& g, const JoshOps& ops, int nr, int maxj, bool mapped, WS& ws, FullT* full,
+                                    const double* bnu, double* hsurf) {
+  if (mapped) {
+    if (!kOpsGiven) {
       for (int l = g.r; l < kNx; l += G::N) ws.xs[l] = fmax(ws.xs[l], 1.0e-37);
       g.sync();
     }
@@ -676,7 +744,7 @@ __device__ inline int g_josh(G& g, const JoshOps& ops, const double* rhox, int n
   // JOSH with IFSURF = 1 and MAXJ = 1 falls through to the Eddington sweep
   // IFSURF = 1 with an optically thick surface borrows the scratch vectors
   // t1..t3 for SNU/HNU/JMINS (JNU is not needed beyond HNU(1)).
-  JoshWSFull* F = full;
+  FullT* F = full;
   int sweeps = 0;
   double* snu = F ? F->snu : ws.t1;
   double* hnu = F ? F->hnu : ws.t2;
@@ -741,36 +809,37 @@ __device__ inline int g_josh(G& g, const JoshOps& ops, const double* rhox, int n
     return sweeps;
   }
   // (IFSURF = 1 never reaches here with MAXJ != 1: it returned above.)
-  // J - S and H on the 51-point grid, mapped back onto the first MAXJ depths
-  // four interleaved partial sums per product (instruction-level parallelism
-  // instead of one 51-long dependent chain; the grouping differs from the
-  // reference's sequential sum only at rounding level)
-  for (int l = g.r; l < kNx; l += G::N) {
-    double sj[4] = {0.0, 0.0, 0.0, 0.0}, sh[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int mm = 0; mm < kNx; ++mm) {
-      const double x = ws.xs[mm];
-      sj[mm & 3] = sj[mm & 3] + ops.coefj[mm * kNx + l] * x;
-      sh[mm & 3] = sh[mm & 3] + ops.coefh[mm * kNx + l] * x;
-    }
-    ws.xw[l] = -ws.xs[l] + ((sj[0] + sj[1]) + (sj[2] + sj[3]));
-    ws.xsbar[l] = (sh[0] + sh[1]) + (sh[2] + sh[3]);  // XSBAR no longer needed: holds XH
+  if (!kOpsGiven) {
+    josh_operators(g, ops, ws.xs, ws.xw, ws.xsbar, &F->knu1);  // XSBAR no longer needed: holds XH
+    g.sync();
   }
-  g.sync();
   g_map1(g, ops.xtau, ws.xw, kNx, ws.taunu, F->jmins, maxj, ws.lidx);
   g_map1(g, ops.xtau, ws.xsbar, kNx, ws.taunu, F->hnu, maxj, ws.lidx);
-  if (g.r == 0) {
-    double xk = 0.0;
-    for (int mm = 0; mm < kNx; ++mm) xk = xk + ops.ck[mm] * ws.xs[mm];
-    F->knu1 = xk;
-    F->maxj = maxj;
-  }
+  if (g.r == 0) F->maxj = maxj;
   for (int j = g.r; j < maxj; j += G::N) {
     F->snu[j] = fmax(F->snu[j], 1.0e-38);
     F->jnu[j] = fmax(F->jmins[j] + F->snu[j], 1.0e-38);
   }
   g.sync();
   return sweeps;
+}
+
+// The whole of JOSH by one group.  Inputs in ws.*: abtot/alpha/snubar are
+// formed here from the opacity vectors.  rhox is shared by the CTA.
+// ifsurf = 1 returns H(1); ifsurf = 0 fills full (SNU, JNU, HNU, JMINS,
+// KNU(1), MAXJ) as the reference does.  A: shared-memory matrix for a warp
+// group, the U rows for a pair group.  Returns the number of Eddington
+// sweeps run (0 if none).
+template <class G>
+__device__ inline int g_josh(G& g, const JoshOps& ops, const double* rhox, int nr, const double* acont,
+                             const double* aline, const double* sigmac, const double* sigmal,
+                             const double* scont, const double* sline, const double* bnu, JoshWS& ws,
+                             double* A, JoshWSFull* full, double* hsurf) {
+  g_josh_fill(g, nr, acont, aline, sigmac, sigmal, scont, sline, ws);
+  bool mapped, solve;
+  const int maxj = g_josh_prepare(g, ops, rhox, nr, ws, mapped, solve);
+  if (solve) solve_scatter(g, ops, ws, A);
+  return g_josh_finish(g, ops, nr, maxj, mapped, ws, full, bnu, hsurf);
 }
 
 }  // namespace atlasgpu

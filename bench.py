@@ -370,9 +370,10 @@ def run_ours(args):
     batch.step(1)
     ctx.enable_timing(True)
     batch.step(1)
-    names = ("eos", "kapcont", "kapp", "linop", "rt", "reduce", "finish")
+    names = ("eos", "kapcont", "kapp", "linop", "rt", "rt_pre", "rt_solve", "rt_post", "reduce", "finish")
     kms = {k: ctx.kernel_ms("batch_" + k) for k in names}
     linop_points = ctx.kernel_work("batch_linop_points")
+    rt_solves = {k: ctx.kernel_work("batch_rt_" + k) for k in ("eliminated", "series", "series_steps")}
     ctx.enable_timing(False)
     batch.run()
     per_model = {k: v / CFG["slots"] for k, v in kms.items()}
@@ -499,7 +500,8 @@ def run_ours(args):
                 "l2": "flushed between steps (256 MB write)",
                 "converged_per_step": float(conv_all.item()) / args.steps / world,
                 "mean_iterations_per_model": float(np.mean(iters)),
-                "kernel_ms_per_model_iteration": per_model, "roofline": roof, "rooflines": rooflines,
+                "kernel_ms_per_model_iteration": per_model, "rt_solves_per_iteration": rt_solves,
+                "roofline": roof, "rooflines": rooflines,
                 "atlas": {"mixed_error_vs_fp64": mx_err}, "cpu_baseline": cpu,
                 "plain_fp64": plain, "vs_plain_fp64": (value / plain["value"]) if plain and plain["value"] else None,
                 "single_model": single, "synthe": syn, "selectlines": sel,
