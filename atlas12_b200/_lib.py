@@ -87,6 +87,8 @@ SIGNATURES = {
     "atlasgpu_atlas_xlinop": (_I, [_P, _P, _I64, _I, _I, _P, _P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P,
                                    _P, _P, ctypes.POINTER(_I64)]),
     "atlasgpu_atlas_set_hydrogen_tables": (_I, [_P, _P]),
+    "atlasgpu_atlas_set_kapp_tables": (_I, [_P, _P]),
+    "atlasgpu_atlas_kapp_hydrogen": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "atlasgpu_atlas_rt_pass": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _D,
                                     ctypes.POINTER(Accum), _P]),
     "atlasgpu_atlas_finish": (_I, [_P, ctypes.c_void_p, ctypes.POINTER(Accum), ctypes.POINTER(_D)]),
@@ -161,6 +163,31 @@ class HydrogenTables(ctypes.Structure):
             else:
                 getattr(h, name)[:] = [float(x) for x in v]
         return h
+
+
+class KappTables(ctypes.Structure):
+    """atlasgpu_kapp_tables (include/atlasgpu.h): KAPP's hydrogen continuum
+    tables (Karzas-Latter, van Hoof g_ff, Holtsmark Q, HOP's level energies,
+    HMINOP's, H2PLOP's and HRAYOP's tables)."""
+    _F = ctypes.c_float
+    _fields_ = [("freqn", _F * 435), ("xn", _F * 435), ("xl", _F * 1044), ("ekarzas", _F * 29),
+                ("gff", _D * 11826), ("q_holtsmark", _D * 150), ("hop_elev", _D * 15), ("hmin_wbf", _D * 116),
+                ("hmin_bf", _D * 116), ("hmin_thetaff", _D * 11), ("hmin_wavek", _D * 22), ("hmin_ff", _D * 242),
+                ("h2p_fr", _D * 5), ("h2p_es", _D * 6), ("ray_m", _D * 74), ("ray_ab", _D * 27), ("ray_bc", _D * 24),
+                ("ray_cd", _D * 22), ("ray_ly", _D * 64), ("ray_fly", _D * 64)]
+
+    @classmethod
+    def from_tables(cls, t):
+        """From the arrays k_<field> of the reference tables, each flattened in
+        Fortran (column-major) order, which is the header's layout."""
+        k = cls()
+        for name, typ in cls._fields_:
+            v = np.asarray(t["k_" + name]).ravel()
+            arr = getattr(k, name)
+            if len(arr) != v.size:
+                raise ValueError(f"kapp table {name}: {v.size} values, expected {len(arr)}")
+            arr[:] = [float(x) for x in v]
+        return k
 
 
 class StehleSeries(ctypes.Structure):

@@ -90,6 +90,31 @@ class Atlas:
         self._htab = _lib.HydrogenTables.from_tables(tables)
         self.ctx.call("atlasgpu_atlas_set_hydrogen_tables", ctypes.byref(self._htab))
 
+    def set_kapp_tables(self, tables):
+        """KAPP's hydrogen continuum tables (arrays k_* as the fixture
+        extracted from the reference's data files and source holds them)."""
+        self._ktab = _lib.KappTables.from_tables(tables)
+        self.ctx.call("atlasgpu_atlas_set_kapp_tables", ctypes.byref(self._ktab))
+
+    def kapp_hydrogen(self, waveset, t, xne, rho, xnfp1, xnfp2, bhyd=None, bmin=None, kw=None, parts=False):
+        """KAPP with its hydrogen, H-, H2+, Rayleigh and electron-scattering
+        sources at every (frequency, depth): (acont, sigmac, scont) [numnu, kw],
+        and with parts=True also [numnu, 7, kw] (AHYD, SHYD, AH2P, AHMIN,
+        SHMIN, SIGH, SIGEL).  bhyd [6, kw] and bmin [kw]: None for LTE."""
+        ws = np.ascontiguousarray(waveset, np.float64)
+        vec = [np.ascontiguousarray(v, np.float64) for v in (t, xne, rho, xnfp1, xnfp2)]
+        nrhox = vec[0].size
+        kw = nrhox if kw is None else int(kw)
+        bh = None if bhyd is None else np.ascontiguousarray(bhyd, np.float64)
+        if bh is not None and bh.shape != (6, kw):
+            raise ValueError("bhyd must be [6, kw]")
+        bm = None if bmin is None else np.ascontiguousarray(bmin, np.float64)
+        out = [np.zeros((ws.size, kw)) for _ in range(3)]
+        pt = np.zeros((ws.size, 7, kw)) if parts else None
+        self.ctx.call("atlasgpu_atlas_kapp_hydrogen", ws.size, ptr(ws), nrhox, kw, *[ptr(v) for v in vec], ptr(bh),
+                      ptr(bm), *[ptr(o) for o in out], ptr(pt))
+        return (*out, pt) if parts else tuple(out)
+
     def xlinop(self, records, nrhox, xnfdop, dopple, xne, txnxn, hckt, tabcont, iwt, waveset, contx, xlines=None,
                xnfp=None, rho=None, hydrogen=None):
         """XLINOP on unit-19 records (NLTE_LINE array, sorted by wavelength),

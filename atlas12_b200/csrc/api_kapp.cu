@@ -1,0 +1,169 @@
+// api_kapp.cu -- C-ABI entry points of KAPP's hydrogen continuum sources
+// (atlas12_modules.f90:11202-11324 with HOP, H2PLOP, HMINOP, HRAYOP, ELECOP;
+// kernels in kapp.cuh).
+#include <cmath>
+#include <vector>
+
+#include "api_common.cuh"
+#include "kapp.cuh"
+
+using namespace atlasgpu;
+
+namespace {
+
+// H_SERIES_LIMITS (atlas12_modules.f90:392-395): HOP's cascade exits at the
+// same thresholds as the reference's
+constexpr double kSeriesLimits[15] = {109678.764, 27419.659, 12186.462, 6854.871, 4387.113,
+                                      3046.604,   2238.320,  1713.713,  1354.044, 1096.776,
+                                      906.426,    761.650,   648.980,   559.579,  487.456};
+
+bool finite_f(const float* p, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(p[i])) return false;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int atlasgpu_atlas_set_kapp_tables(atlasgpu_ctx* ctx, const atlasgpu_kapp_tables* t) {
+  if (!ctx || !t) return fail(ctx, ATLASGPU_EINVAL, "set_kapp_tables: null argument");
+  if (!finite_f(&t->freqn[0][0], 15 * 29) || !finite_f(&t->xn[0][0], 15 * 29) || !finite_f(&t->xl[0][0][0], 36 * 29) ||
+      !finite_f(t->ekarzas, 29) || !finite_all(&t->gff[0][0], 146 * 81) || !finite_all(t->q_holtsmark, 150) ||
+      !finite_all(t->hop_elev, 15) || !finite_all(t->hmin_wbf, 116) || !finite_all(t->hmin_bf, 116) ||
+      !finite_all(t->hmin_thetaff, 11) || !finite_all(t->hmin_wavek, 22) || !finite_all(&t->hmin_ff[0][0], 242) ||
+      !finite_all(t->h2p_fr, 5) || !finite_all(t->h2p_es, 6) || !finite_all(t->ray_m, 74) ||
+      !finite_all(t->ray_ab, 27) || !finite_all(t->ray_bc, 24) || !finite_all(t->ray_cd, 22) ||
+      !finite_all(t->ray_ly, 64) || !finite_all(t->ray_fly, 64))
+    return fail(ctx, ATLASGPU_ENONFINITE, "set_kapp_tables: non-finite table entry");
+  for (int i = 0; i < 146 * 81; ++i)
+    if (!((&t->gff[0][0])[i] > 0.0)) return fail(ctx, ATLASGPU_EINVAL, "set_kapp_tables: g_ff entry not positive");
+  for (int i = 0; i < 242; ++i)
+    if (!((&t->hmin_ff[0][0])[i] > 0.0)) return fail(ctx, ATLASGPU_EINVAL, "set_kapp_tables: FF entry not positive");
+  for (int i = 0; i < 22; ++i)
+    if (!(t->hmin_wavek[i] > 0.0)) return fail(ctx, ATLASGPU_EINVAL, "set_kapp_tables: WAVEK entry not positive");
+  std::vector<KappDev> h(1);
+  KappDev& k = h[0];
+  std::copy(&t->freqn[0][0], &t->freqn[0][0] + 15 * 29, k.freqn);
+  std::copy(&t->xn[0][0], &t->xn[0][0] + 15 * 29, k.xn);
+  std::copy(&t->xl[0][0][0], &t->xl[0][0][0] + 36 * 29, k.xl);
+  std::copy(t->ekarzas, t->ekarzas + 29, k.ekarzas);
+  // COULFF's reader (:12162-12165): GFF_LOGTAB = log10 of the tabulated g_ff
+  for (int i = 0; i < 146 * 81; ++i) k.gff_log[i] = std::log10((&t->gff[0][0])[i]);
+  std::copy(t->q_holtsmark, t->q_holtsmark + 150, k.q);
+  std::copy(t->hop_elev, t->hop_elev + 15, k.hop_elev);
+  std::copy(t->hmin_wbf, t->hmin_wbf + 116, k.wbf);
+  std::copy(t->hmin_bf, t->hmin_bf + 116, k.bf);
+  std::copy(t->hmin_thetaff, t->hmin_thetaff + 11, k.thetaff);
+  // HMINOP's first call (:12488-12497): WFFLOG = log(91.134 / WAVEK),
+  // FFLOG(IWAVE, ITHETA) = log(FF(ITHETA, IWAVE) * 1e-26)
+  for (int iw = 0; iw < 22; ++iw) {
+    k.wfflog[iw] = std::log(91.134 / t->hmin_wavek[iw]);
+    for (int it = 0; it < 11; ++it) k.fflog[it * 22 + iw] = std::log(t->hmin_ff[iw][it] * 1.0e-26);
+  }
+  std::copy(t->h2p_fr, t->h2p_fr + 5, k.h2p_fr);
+  std::copy(t->h2p_es, t->h2p_es + 6, k.h2p_es);
+  std::copy(t->ray_m, t->ray_m + 74, k.ray_m);
+  std::copy(t->ray_ab, t->ray_ab + 27, k.ray_ab);
+  std::copy(t->ray_bc, t->ray_bc + 24, k.ray_bc);
+  std::copy(t->ray_cd, t->ray_cd + 22, k.ray_cd);
+  std::copy(t->ray_ly, t->ray_ly + 64, k.ray_ly);
+  std::copy(t->ray_fly, t->ray_fly + 64, k.ray_fly);
+  std::copy(kSeriesLimits, kSeriesLimits + 15, k.series_limits);
+  cudaSetDevice(ctx->device);
+  KappDev* d;
+  int r;
+  if ((r = bufT(ctx, "kapp_tab", 1, &d))) return r;
+  CK(cudaMemcpyAsync(d, &k, sizeof k, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->kapp_set = true;
+  return 0;
+}
+
+int atlasgpu_atlas_kapp_hydrogen(atlasgpu_ctx* ctx, int numnu, const double* waveset, int nrhox, int kw,
+                                 const double* t, const double* xne, const double* rho, const double* xnfp1,
+                                 const double* xnfp2, const double* bhyd, const double* bmin, double* acont,
+                                 double* sigmac, double* scont, double* parts) {
+  if (!ctx) return ATLASGPU_EINVAL;
+  if (!ctx->kapp_set) return fail(ctx, ATLASGPU_ESTATE, "kapp_hydrogen: tables not set");
+  if (numnu < 1 || nrhox < 1 || kw < nrhox || !waveset || !t || !xne || !rho || !xnfp1 || !xnfp2 || !acont ||
+      !sigmac || !scont)
+    return fail(ctx, ATLASGPU_EINVAL, "kapp_hydrogen: bad argument (numnu %d, nrhox %d, kw %d)", numnu, nrhox, kw);
+  for (int i = 0; i < numnu; ++i)
+    if (!(waveset[i] > 0.0) || !std::isfinite(waveset[i]))
+      return fail(ctx, ATLASGPU_EINVAL, "kapp_hydrogen: WAVESET(%d) = %g", i + 1, waveset[i]);
+  if (!finite_all(t, nrhox) || !finite_all(xne, nrhox) || !finite_all(rho, nrhox) || !finite_all(xnfp1, nrhox) ||
+      !finite_all(xnfp2, nrhox) || (bmin && !finite_all(bmin, nrhox)))
+    return fail(ctx, ATLASGPU_ENONFINITE, "kapp_hydrogen: non-finite depth vector");
+  for (int j = 0; j < nrhox; ++j)
+    if (!(t[j] > 0.0) || !(rho[j] > 0.0))
+      return fail(ctx, ATLASGPU_EINVAL, "kapp_hydrogen: T or RHO not positive at depth %d", j + 1);
+  if (bhyd)
+    for (int n = 0; n < 6; ++n)
+      if (!finite_all(bhyd + (size_t)n * kw, nrhox))
+        return fail(ctx, ATLASGPU_ENONFINITE, "kapp_hydrogen: non-finite BHYD");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const size_t nt = (size_t)numnu * kw;
+  double *d_ws, *d_in, *d_dep, *d_out, *d_parts = nullptr;
+  int r;
+  // inputs: T, XNE, RHO, XNFP1, XNFP2, BMIN [kw] and BHYD [6][kw]
+  if ((r = bufT(ctx, "kp_ws", numnu, &d_ws)) || (r = bufT(ctx, "kp_in", (size_t)12 * kw, &d_in)) ||
+      (r = bufT(ctx, "kp_dep", (size_t)(6 + 2 * kHLev + 9) * kw, &d_dep)) ||
+      (r = bufT(ctx, "kp_out", 3 * nt, &d_out)) || (parts && (r = bufT(ctx, "kp_parts", 7 * nt, &d_parts))))
+    return r;
+  CK(cudaMemsetAsync(d_in, 0, (size_t)12 * kw * sizeof(double), s));
+  CK(cudaMemcpyAsync(d_ws, waveset, numnu * sizeof(double), cudaMemcpyHostToDevice, s));
+  const double* src[5] = {t, xne, rho, xnfp1, xnfp2};
+  for (int q = 0; q < 5; ++q)
+    CK(cudaMemcpyAsync(d_in + (size_t)q * kw, src[q], nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (bmin) CK(cudaMemcpyAsync(d_in + (size_t)5 * kw, bmin, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (bhyd) CK(cudaMemcpyAsync(d_in + (size_t)6 * kw, bhyd, (size_t)6 * kw * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(d_out, 0, 3 * nt * sizeof(double), s));
+  if (d_parts) CK(cudaMemsetAsync(d_parts, 0, 7 * nt * sizeof(double), s));
+  KappArgs a{};
+  a.tb = (const KappDev*)ctx->bufs["kapp_tab"].first;
+  a.numnu = numnu;
+  a.nrhox = nrhox;
+  a.kw = kw;
+  a.waveset = d_ws;
+  a.t = d_in;
+  a.xne = d_in + kw;
+  a.rho = d_in + 2 * kw;
+  a.xnfp1 = d_in + 3 * kw;
+  a.xnfp2 = d_in + 4 * kw;
+  a.bmin = bmin ? d_in + 5 * kw : nullptr;
+  a.bhyd = bhyd ? d_in + 6 * kw : nullptr;
+  double* p = d_dep;
+  double** dv[6] = {&a.d.hkt, &a.d.hckt, &a.d.tkev, &a.d.tlog, &a.d.theta, &a.d.xhmin};
+  for (int q = 0; q < 6; ++q) {
+    *dv[q] = p;
+    p += kw;
+  }
+  a.d.w = p;
+  p += (size_t)kHLev * kw;
+  a.d.bz = p;
+  p += (size_t)kHLev * kw;
+  a.d.bp = p;
+  a.acont = d_out;
+  a.sigmac = d_out + nt;
+  a.scont = d_out + 2 * nt;
+  a.parts = d_parts;
+  {
+    Timer tm(ctx, "kapp_hydrogen");
+    k_kapp_depth<<<(nrhox + 127) / 128, 128, 0, s>>>(a);
+    CKL(ctx);
+    const int blocks = std::min((numnu + kKappWarps - 1) / kKappWarps, ctx->nsm * 8);
+    k_kapp_nu<<<blocks, kKappWarps * 32, 0, s>>>(a);
+    CKL(ctx);
+  }
+  CK(cudaMemcpyAsync(acont, a.acont, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(sigmac, a.sigmac, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(scont, a.scont, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (parts) CK(cudaMemcpyAsync(parts, d_parts, 7 * nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+}  // extern "C"

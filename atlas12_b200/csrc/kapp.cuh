@@ -1,0 +1,354 @@
+// kapp.cuh -- KAPP's hydrogen continuum sources on the device (sm_100a).
+//
+// KAPP (atlas12_modules.f90:11202-11324) is called once per frequency inside
+// RUN_RT_PASS's loop and evaluates every source at every depth.  Here the
+// work is split by what it depends on:
+//   k_kapp_depth  once per call, per depth: the temperature and density
+//                 factors, the Hummer-Mihalas occupation probabilities w_n of
+//                 n = 1..80 (occupation_prob :22549-22567, holtsmark_Q
+//                 :22492-22519) and the level populations' Boltzmann factors
+//                 exp(-E_n HCKT) -- none depends on the frequency
+//   k_kapp_nu     warp per frequency: the per-frequency parts first (XKARZAS
+//                 :11635-11804 for n = 1..80 in its REAL(4) arithmetic,
+//                 HMINOP's free-free table at this wavelength and its
+//                 bound-free cross-section, HRAYOP's and H2PLOP's factors),
+//                 then lanes over depths: HOP (:11359-11608), H2PLOP
+//                 (:12224-12252), HMINOP (:12360-12558), HRAYOP (:12740-12906),
+//                 ELECOP (:17212-17222) and KAPP's totals.
+// Every output is the reference's expression in its order; where the
+// reference evaluates a depth-only factor inside the frequency loop, the
+// factor is the same function of the same inputs.
+#pragma once
+#include "common.cuh"
+#include "tcorr.cuh"
+
+namespace atlasgpu {
+
+// mod_constants (atlas12_modules.f90:315-464)
+constexpr double kKbol = 1.380649e-16;
+constexpr double kEvErg = 1.602176634e-12;
+constexpr double kEmass = 9.1093837139e-28;
+constexpr double kSigmaThomson = 6.6524587051e-25;
+constexpr double kLn10 = 2.30258509299405;
+constexpr double kCoeffFF = 3.69196e8;
+constexpr double kRydbergH = 109677.583403;
+constexpr double kElimHI = 109678.764;
+constexpr double kHminusEA = 0.75419;
+constexpr double kBetaHM88 = 8.798905203085208e+14;
+constexpr double kLogBetaMin = -2.0, kLogBetaStep = 2.4825302042523617e-02;
+constexpr int kHLev = 80;  // HOP's NMAX_HLEVELS
+
+// the tables on the device (set by atlasgpu_atlas_set_kapp_tables)
+struct KappDev {
+  float freqn[15 * 29], xn[15 * 29], xl[36 * 29], ekarzas[29];
+  double gff_log[146 * 81];  // log10 g_ff, GFF_LOGTAB(I, J) at (J-1)*81 + I-1
+  double q[150];
+  double hop_elev[15];
+  double wbf[116], bf[116], thetaff[11], wfflog[22], fflog[11 * 22];  // FFLOG(IWAVE, ITHETA) at it*22 + iw
+  double h2p_fr[5], h2p_es[6];
+  double ray_m[74], ray_ab[27], ray_bc[24], ray_cd[22], ray_ly[64], ray_fly[64];
+  double series_limits[15];  // H_SERIES_LIMITS
+};
+
+// per-depth factors (k_kapp_depth), each [kw]; w, bz: [kHLev][kw] (level n at
+// (n-1)*kw), bp: [9][kw] for the pseudo-continuum's n = 7..15
+struct KappDepth {
+  double *hkt, *hckt, *tkev, *tlog, *theta, *xhmin;
+  double *w, *bz, *bp;
+};
+
+struct KappArgs {
+  const KappDev* tb;
+  int numnu, nrhox, kw;
+  const double* waveset;
+  const double *t, *xne, *rho, *xnfp1, *xnfp2, *bhyd, *bmin;  // bhyd [6][kw], bmin [kw]; may be null
+  KappDepth d;
+  double *acont, *sigmac, *scont;  // [numnu][kw]
+  double* parts;                   // [numnu][7][kw] or null
+};
+
+__host__ __device__ inline double kapp_kbol_ev() { return kKbol / kEvErg; }
+__host__ __device__ inline double kapp_freq_rydh() { return kRydbergH * kClight; }
+__host__ __device__ inline double kapp_hoverk() { return kHplanck / kKbol; }
+
+// holtsmark_Q and occupation_prob; DBLE(n)**5 is exact for n <= 80
+__device__ inline double kapp_occupation(const KappDev& tb, int n, double xne, double xne23) {
+  if (n <= 1 || xne <= 0.0) return 1.0;
+  const double dn = (double)n;
+  const double beta = kBetaHM88 / (dn * dn * dn * dn * dn * xne23);
+  if (beta <= 0.01) return 0.0;
+  if (beta >= 50.0) return 1.0;
+  const double idx_f = (log10(beta) - kLogBetaMin) / kLogBetaStep;
+  int idx = (int)idx_f;
+  idx = idx > 148 ? 148 : (idx < 0 ? 0 : idx);
+  const double frac = idx_f - (double)idx;
+  return tb.q[idx] + frac * (tb.q[idx + 1] - tb.q[idx]);
+}
+
+// XKARZAS(FREQ, 1, N, N): level-averaged Karzas-Latter cross-section, the
+// interpolation in REAL(4) with every operation rounded as written (no
+// contraction)
+__device__ inline double kapp_xkarzas(const KappDev& tb, double freq, int n) {
+  constexpr int NPTS = 29, NMAX = 15;
+  const float fl = __double2float_rn(log10(freq));
+  float x;
+  if (n > NMAX) {
+    const float rn = (float)n;
+    const float rn2 = __fmul_rn(rn, rn);
+    const float flast = __double2float_rn(log10(kapp_freq_rydh() / (double)rn2));
+    if (fl < flast) return 0.0;
+    const float r = __fdiv_rn(1.0f, rn2);
+    float fprev = 0.0f, fcur = flast;
+    int i;
+    for (i = 2; i <= NPTS - 1; ++i) {
+      fcur = __double2float_rn(log10((double)__fadd_rn(tb.ekarzas[i - 1], r) * kapp_freq_rydh()));
+      if (fl > fcur) break;
+    }
+    if (i > NPTS - 1) {
+      i = NPTS;
+      fprev = fcur;  // FREQN15(NPTS-1), set by the loop's last pass
+      fcur = flast;
+    } else {
+      // FREQN15(I-1): the previous pass's value, or (I = 2, only above
+      // 1.5e19 Hz) formed like the others
+      fprev = __double2float_rn(log10((double)__fadd_rn(tb.ekarzas[i - 2], r) * kapp_freq_rydh()));
+    }
+    const float* xn = tb.xn + (NMAX - 1) * NPTS;
+    x = __fadd_rn(__fmul_rn(__fdiv_rn(__fsub_rn(fl, fcur), __fsub_rn(fprev, fcur)), __fsub_rn(xn[i - 2], xn[i - 1])),
+                  xn[i - 1]);
+  } else {
+    const float* fn = tb.freqn + (n - 1) * NPTS;
+    const float* xn = tb.xn + (n - 1) * NPTS;
+    if (fl < fn[NPTS - 1]) return 0.0;
+    int i;
+    for (i = 2; i <= NPTS; ++i)
+      if (fl > fn[i - 1]) break;
+    if (i > NPTS) i = NPTS;
+    x = __fadd_rn(__fmul_rn(__fdiv_rn(__fsub_rn(fl, fn[i - 1]), __fsub_rn(fn[i - 2], fn[i - 1])),
+                            __fsub_rn(xn[i - 2], xn[i - 1])),
+                  xn[i - 1]);
+  }
+  return exp((double)x * kLn10);
+}
+
+// COULFF(J, 1) (:11995-12196): bilinear interpolation in log g_ff
+__device__ inline double kapp_coulff(const KappDev& tb, double freqlg, double tlog) {
+  constexpr int NG = 81, NU = 146;
+  const double l10ryk = log10(kapp_freq_rydh() * kapp_hoverk());
+  const double l10kh = -log10(kapp_hoverk());
+  const double lgam2 = 0.0 + l10ryk - tlog / kLn10;
+  const double lu = (freqlg - tlog) / kLn10 - l10kh;
+  const double xi = (lgam2 - -6.0) / 0.2 + 1.0;
+  const double xj = (lu - -16.0) / 0.2 + 1.0;
+  int i0 = (int)xi, j0 = (int)xj;
+  i0 = i0 > NG - 1 ? NG - 1 : (i0 < 1 ? 1 : i0);
+  j0 = j0 > NU - 1 ? NU - 1 : (j0 < 1 ? 1 : j0);
+  const double fi = fmax(0.0, fmin(xi - (double)i0, 1.0));
+  const double fj = fmax(0.0, fmin(xj - (double)j0, 1.0));
+  const double* g = tb.gff_log;
+  const double lg00 = g[(j0 - 1) * NG + i0 - 1], lg01 = g[j0 * NG + i0 - 1];
+  const double lg10 = g[(j0 - 1) * NG + i0], lg11 = g[j0 * NG + i0];
+  const double lg = (1.0 - fi) * ((1.0 - fj) * lg00 + fj * lg01) + fi * ((1.0 - fj) * lg10 + fj * lg11);
+  return pow(10.0, lg);
+}
+
+// LINTER (:5859-5880)
+__device__ inline double kapp_linter(const double* xo, const double* yo, int n, double x) {
+  int i;
+  for (i = 2; i <= n; ++i)
+    if (x < xo[i - 1]) break;
+  if (i > n) i = n;
+  return yo[i - 2] + (yo[i - 1] - yo[i - 2]) / (xo[i - 1] - xo[i - 2]) * (x - xo[i - 2]);
+}
+
+// HRAYOP's cross-section at FREQ (:12793-12900)
+__device__ inline double kapp_rayleigh(const KappDev& tb, double freq) {
+  const double fr = kapp_freq_rydh();
+  const double d1 = 0.01 * fr, dab = 0.005 * fr, dbc = 0.002 * fr, dcd = 0.001 * fr;
+  int i;
+  double g;
+  if (freq < d1) return kSigmaThomson * powi(tb.ray_m[0], 2) * powi(freq / d1, 4);
+  if (freq <= 0.74 * fr) {
+    i = min((int)(freq / d1) + 1, 74);
+    g = tb.ray_m[i - 2] + (tb.ray_m[i - 1] - tb.ray_m[i - 2]) / d1 * (freq - (double)(i - 1) * d1);
+    return kSigmaThomson * powi(g, 2);
+  }
+  if (freq < 0.77 * fr) return 0.0;
+  if (freq <= 0.885 * fr) {
+    i = min((int)((freq - 0.755 * fr) / dab) + 1 + 1, 27);
+    g = tb.ray_ab[i - 2] + (tb.ray_ab[i - 1] - tb.ray_ab[i - 2]) / dab * (freq - (0.755 * fr + (double)(i - 2) * dab));
+    return kSigmaThomson * powi(g, 2);
+  }
+  if (freq < 0.890 * fr) return 0.0;
+  if (freq <= 0.936 * fr) {
+    i = min((int)((freq - 0.890 * fr) / dbc) + 1 + 1, 24);
+    g = tb.ray_bc[i - 2] + (tb.ray_bc[i - 1] - tb.ray_bc[i - 2]) / dbc * (freq - (0.890 * fr + (double)(i - 2) * dbc));
+    return kSigmaThomson * powi(g, 2);
+  }
+  if (freq < 0.938 * fr) return 0.0;
+  if (freq <= 0.959 * fr) {
+    i = min((int)((freq - 0.938 * fr) / dcd) + 1 + 1, 22);
+    g = tb.ray_cd[i - 2] + (tb.ray_cd[i - 1] - tb.ray_cd[i - 2]) / dcd * (freq - (0.938 * fr + (double)(i - 2) * dcd));
+    return kSigmaThomson * powi(g, 2);
+  }
+  if (freq < 0.961 * fr) return 0.0;
+  if (freq <= fr) return kSigmaThomson * tb.ray_ly[0];
+  const double xnew = freq / fr;
+  double fnew;
+  s_map1(tb.ray_fly, tb.ray_ly, 64, &xnew, &fnew, 1);
+  return kSigmaThomson * fnew;
+}
+
+// per-depth factors; threads over depths
+static __global__ void k_kapp_depth(KappArgs a) {
+  const KappDev& tb = *a.tb;
+  const int kw = a.kw;
+  const double saha = 2.0 * pow(2.0 * kPi * kEmass * kKbol / (kHplanck * kHplanck), 1.5);
+  const double theta_c = 0.4342944819032518 / kapp_kbol_ev();
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < a.nrhox; j += gridDim.x * blockDim.x) {
+    const double T = a.t[j];
+    const double tk = kKbol * T;
+    const double hkt = kHplanck / tk, hckt = hkt * kClight;
+    const double tkev = kapp_kbol_ev() * T;
+    a.d.hkt[j] = hkt;
+    a.d.hckt[j] = hckt;
+    a.d.tkev[j] = tkev;
+    a.d.tlog[j] = log(T);
+    a.d.theta[j] = theta_c / T;
+    const double bm = a.bmin ? a.bmin[j] : 1.0, bh1 = a.bhyd ? a.bhyd[j] : 1.0;
+    // XHMIN (HMINOP :12505-12509)
+    a.d.xhmin[j] = exp(kHminusEA / tkev) / (saha * T * sqrt(T)) * bm * bh1 * a.xnfp1[j] * a.xne[j];
+    const double xne = a.xne[j];
+    const double xne23 = pow(xne, 2.0 / 3.0);
+    for (int n = 1; n <= kHLev; ++n) {
+      a.d.w[(size_t)(n - 1) * kw + j] = kapp_occupation(tb, n, xne, xne23);
+      const double dn2 = powi((double)n, 2);
+      const double en = n <= 15 ? tb.hop_elev[n - 1] : kElimHI - kRydbergH / dn2;
+      a.d.bz[(size_t)(n - 1) * kw + j] = exp(-en * hckt);
+      if (n >= 7 && n <= 15) a.d.bp[(size_t)(n - 7) * kw + j] = exp(-(kElimHI - kRydbergH / dn2) * hckt);
+    }
+  }
+}
+
+constexpr int kKappWarps = 8;  // warps per CTA of k_kapp_nu
+
+// warp per frequency (grid-stride), lanes over depths
+static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) {
+  __shared__ double s_xk[kKappWarps][kHLev + 1];
+  __shared__ double s_fftt[kKappWarps][11];
+  const KappDev& tb = *a.tb;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int kw = a.kw;
+  const double fr = kapp_freq_rydh();
+  const double theta_c = 0.4342944819032518 / kapp_kbol_ev();
+  double* xk = s_xk[wid];
+  double* fftt = s_fftt[wid];
+  for (int nu = blockIdx.x * kKappWarps + wid; nu < a.numnu; nu += gridDim.x * kKappWarps) {
+    // RUN_RT_PASS's frequency quantities (:3907-3917)
+    const double wave = a.waveset[nu];
+    const double freq = kClightNms / wave;
+    const double waveno = 1.0e7 / wave;
+    const double freqlg = log(freq);
+    const double f3 = powi(freq / 1.0e15, 3);
+    // XKARZAS(FREQ, 1, n, n) of n = 1..80, HMINOP's free-free table at this wavelength
+    for (int n = lane + 1; n <= kHLev; n += 32) xk[n] = kapp_xkarzas(tb, freq, n);
+    if (lane < 11)
+      fftt[lane] = exp(kapp_linter(tb.wfflog, tb.fflog + lane * 22, 22, log(wave))) / tb.thetaff[lane] * theta_c *
+                   kKbol;
+    double hminbf = 0.0;
+    if (freq > 1.82365e14) s_map1(tb.wbf, tb.bf, 116, &wave, &hminbf, 1);
+    const double xray = kapp_rayleigh(tb, freq);
+    const double* c = tb.h2p_fr;
+    const double* e = tb.h2p_es;
+    const double frh2 = c[0] + (c[1] + (c[2] + (c[3] + c[4] * freqlg) * freqlg) * freqlg) * freqlg;
+    const double esh2 = e[0] + (e[1] + (e[2] + (e[3] + (e[4] + e[5] * freq) * freq) * freq) * freq) * freq;
+    const double freq3_inv = 1.0 / (freq * freq * freq);
+    __syncwarp();
+    for (int j = lane; j < a.nrhox; j += 32) {
+      const double T = a.t[j];
+      const double ehvkt = exp(-freq * a.d.hkt[j]);
+      const double stim = 1.0 - ehvkt;
+      const double bnu = kBnuPrefac * f3 * ehvkt / stim;
+      const double xne = a.xne[j], rho = a.rho[j], x1 = a.xnfp1[j], x2 = a.xnfp2[j];
+      const double bm = a.bmin ? a.bmin[j] : 1.0;
+      const double* W = a.d.w + j;
+      const double* BZ = a.d.bz + j;
+      const double* BP = a.d.bp + j;
+      // HOP: explicit levels n = 15 .. 1, each exit below its series limit
+      double H = 0.0, S = 0.0, A;
+      for (int n = 15; n >= 1; --n) {
+        if (waveno < tb.series_limits[n - 1]) break;
+        if (n >= 7) {
+          A = W[(n - 1) * kw] * xk[n] * (double)(2 * n * n) * BZ[(n - 1) * kw] * stim;
+          H = H + A;
+          S = S + A * bnu;
+        } else {
+          const double bh = a.bhyd ? a.bhyd[(size_t)(n - 1) * kw + j] : 1.0;
+          if (n >= 2) A = xk[n] * (double)(2 * n * n) * BZ[(n - 1) * kw] * (bh - ehvkt);
+          else A = xk[1] * 2.0 * 1.0 * (bh - ehvkt);
+          H = H + A;
+          S = S + A * bnu * stim / (bh - ehvkt);
+        }
+      }
+      // n = 16..80 from XKARZAS's n = 15 rescaling
+      for (int n = 16; n <= kHLev; ++n) {
+        const double dn2 = powi((double)n, 2);
+        if (waveno < kElimHI / dn2) continue;
+        const double w = W[(n - 1) * kw];
+        if (w < 1.0e-6) continue;
+        A = w * xk[n] * 2.0 * dn2 * BZ[(n - 1) * kw] * stim;
+        H = H + A;
+        S = S + A * bnu;
+      }
+      // the dissolved fraction 1 - w_n of n = 7..80 as a Kramers pseudo-continuum
+      for (int n = 7; n <= kHLev; ++n) {
+        const double w = W[(n - 1) * kw];
+        if (1.0 - w < 1.0e-6) continue;
+        const double bz = n <= 15 ? BP[(n - 7) * kw] : BZ[(n - 1) * kw];
+        A = (1.0 - w) * 2.815e29 * freq3_inv * 2.0 / powi((double)n, 3) * bz * stim;
+        H = H + A;
+        S = S + A * bnu;
+      }
+      H = H * x1 / rho;
+      S = S * x1 / rho;
+      A = kCoeffFF / sqrt(T) * kapp_coulff(tb, freqlg, a.d.tlog[j]) / freq * xne / freq * x2 / freq * stim / rho;
+      H = H + A;
+      S = S + A * bnu;
+      const double ahyd = H, shyd = H > 0.0 ? S / H : 0.0;
+      const double bh1 = a.bhyd ? a.bhyd[j] : 1.0;
+      // H2PLOP
+      const double ah2p = freq > fr ? 0.0 : exp(-esh2 / a.d.tkev[j] + frh2) * x1 * 2.0 * bh1 * x2 / rho * stim;
+      // HMINOP
+      const double ffth = kapp_linter(tb.thetaff, fftt, 11, a.d.theta[j]);
+      const double hminff = ffth * x1 * 2.0 * bh1 * xne / rho;
+      const double hbf = hminbf * 1.0e-18 * (1.0 - ehvkt / bm) * a.d.xhmin[j] / rho;
+      const double ahmin = hbf + hminff;
+      const double shmin = (hbf * bnu * stim / (bm - ehvkt) + hminff * bnu) / ahmin;
+      // HRAYOP, ELECOP
+      const double sigh = xray * x1 * 2.0 * bh1 / rho;
+      const double sigel = kSigmaThomson * xne / rho;
+      // KAPP's totals (:11300-11320); the sources not built here are zero
+      const double av = ah2p + 0.0 + 0.0 + 0.0 + 0.0 + 0.0 + 0.0;
+      const double acont = av + ahyd + ahmin;
+      double scont = bnu;
+      if (acont > 0.0) scont = (av * bnu + ahyd * shyd + ahmin * shmin) / acont;
+      const size_t o = (size_t)nu * kw + j;
+      a.acont[o] = acont;
+      a.scont[o] = scont;
+      a.sigmac[o] = sigh + 0.0 + sigel + 0.0 + 0.0;
+      if (a.parts) {
+        double* p = a.parts + (size_t)nu * 7 * kw + j;
+        p[0] = ahyd;
+        p[kw] = shyd;
+        p[2 * kw] = ah2p;
+        p[3 * kw] = ahmin;
+        p[4 * kw] = shmin;
+        p[5 * kw] = sigh;
+        p[6 * kw] = sigel;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace atlasgpu

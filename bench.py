@@ -61,9 +61,14 @@ WARMSTART = os.path.join(ROOT, "atlas12_b200", "data", "warmstart_c2.npz")
 # solves 2*51^2, system build 2*51^2, J/H/K operators 4*51^2 + 2*51,
 # INTEG/MAP1/DERIV and the mode-2 sums ~ 110 per depth (72 depths)
 FLOPS_PER_NU = int(2 / 3 * 51 ** 3 + 8 * 51 ** 2 + 2 * 51 + 110 * 72)
-# DRAM bytes per model of one batched RT launch (ncu, 4-slot capture of this
-# workload at the tuned shape): ACONT, SIGMAC, XLINES read (52.7 MB) plus the
-# partial sums written (8.1 MB per model at 32 slots and 64 waves)
+# the part of FLOPS_PER_NU that is the scattering solve (LU, triangular
+# solves, system build) and the FP64 operations of one Neumann-series step
+# (a 51x51 matrix-vector product and the update)
+FLOPS_PER_SOLVE = int(2 / 3 * 51 ** 3 + 4 * 51 ** 2)
+FLOPS_PER_SERIES_STEP = 2 * 51 ** 2 + 3 * 51
+# DRAM bytes per model of the three batched RT launches (ncu, 4-slot capture
+# of this workload): ACONT, SIGMAC, XLINES read and the per-frequency records
+# written and read back
 RT_TRAFFIC_PER_MODEL = 60.8e6
 # bytes of one prepared LINOP1 line record on the device (AtlasLine)
 LINE_RECORD_BYTES = 56
@@ -379,14 +384,22 @@ def run_ours(args):
     per_model = {k: v / CFG["slots"] for k, v in kms.items()}
     fp64_peak = float(_lib.lib().atlasgpu_fp64_peak_tflops(ctx.handle))
     ach = CFG["slots"] * CFG["numnu"] * FLOPS_PER_NU / (kms["rt"] * 1e-3) / 1e12
-    roof = {"kernel": "k_batch_rt (JOSH per frequency, FP64)", "bound": "fp64", "achieved": ach, "peak": fp64_peak,
+    # FP64 operations the pass executed: the per-frequency work outside the
+    # solve, each eliminated system's LU, each series step's matrix-vector product
+    nfreq = CFG["slots"] * CFG["numnu"]
+    executed = (nfreq * (FLOPS_PER_NU - FLOPS_PER_SOLVE) + rt_solves["eliminated"] * FLOPS_PER_SOLVE
+                + rt_solves["series_steps"] * FLOPS_PER_SERIES_STEP)
+    roof = {"kernel": "RT pass (k_batch_rt_pre + k_batch_rt_solve + k_batch_rt_post, JOSH per frequency, FP64)",
+            "bound": "fp64", "achieved": ach, "peak": fp64_peak,
             "unit": "TFLOP/s", "frac": ach / fp64_peak if fp64_peak > 0 else None,
+            "executed_tflops": executed / (kms["rt"] * 1e-3) / 1e12,
             "traffic": RT_TRAFFIC_PER_MODEL * CFG["slots"],
-            "traffic_scaling": "ncu capture of a 4-slot launch (90.2 MB per model incl. 37.5 MB of partial sums), "
-                               "read traffic scaled by slots, partial sums at this batch's 8.1 MB per model",
+            "traffic_scaling": "ncu capture of the three launches of a 4-slot batch, per model, times slots",
             "peak_source": "measured DFMA loop on this GPU (atlasgpu_fp64_peak_tflops); MEASURED_PEAKS.json has no FP64 figure",
-            "work": f"{FLOPS_PER_NU} FP64 flop per frequency x {CFG['numnu']} frequencies x {CFG['slots']} models per launch",
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_batch_rt launch (profiles/)"}
+            "work": f"{FLOPS_PER_NU} FP64 flop per frequency (the reference's elimination counted for every "
+                    f"system) x {CFG['numnu']} frequencies x {CFG['slots']} models per pass; executed_tflops counts "
+                    "the series steps and eliminations actually run",
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the three RT launches (profiles/)"}
     # LINOP1 over the batch: wing points added into XLINES per second, and the
     # algorithmic bytes (prepared line records read once per slot, XLINES
     # read and written once) against HBM
@@ -481,6 +494,10 @@ def run_ours(args):
         if args.synthe_grid:
             syn["grid"] = synthe_grid_rate(local, ops, args.synthe_grid)
 
+    kp = None
+    if rank == 0 and world == 1:
+        kp = kapp_rate(ctx, ops, W)
+
     sel = None
     if rank == 0 and world == 1 and not args.no_select:
         sel = selectlines_rates(ctx, ops, cpu=not args.no_cpu)
@@ -504,7 +521,7 @@ def run_ours(args):
                 "roofline": roof, "rooflines": rooflines,
                 "atlas": {"mixed_error_vs_fp64": mx_err}, "cpu_baseline": cpu,
                 "plain_fp64": plain, "vs_plain_fp64": (value / plain["value"]) if plain and plain["value"] else None,
-                "single_model": single, "synthe": syn, "selectlines": sel,
+                "single_model": single, "synthe": syn, "selectlines": sel, "kapp_hydrogen": kp,
                 "e2e": {"value": e2e_value, "unit": "models/hr", "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h)},
                 "gpu_launches": int(gpu_launches), "clocks": clk}
@@ -523,6 +540,28 @@ SELECT_CASES = [("gfpred LINEREC (16 B)", 1, 20_000_000), ("TiO MOL2 (32 B)", 5,
 # DRAM bytes of one 12M-record LINEREC call, all its kernels (ncu): 437 MB,
 # 36.4 B per record (the tile-maximum pass reads the records a second time)
 SELECT_TRAFFIC_PER_LINEREC = 36.4
+
+
+def kapp_rate(ctx, ops, W):
+    """KAPP's hydrogen continuum sources (atlasgpu_atlas_kapp_hydrogen) over the
+    workload's 30,000 frequencies and 72 depths of the grey solar model:
+    kernel time (CUDA events, after a warm-up call) and (frequency, depth)
+    evaluations per second; the call's host copies are outside the kernel time."""
+    from atlas12_b200 import atlas, surrogate
+    A = atlas.Atlas(ctx, ops)
+    A.set_kapp_tables(ops)
+    m = W["solar"]
+    e = surrogate.eos(m["t"], m["p"])
+    args = (W["ws"], m["t"], e["xne"], e["rho"], e["nh"] * (1 - e["xh"]) / 2, e["nh"] * e["xh"])
+    A.kapp_hydrogen(*args)
+    ctx.enable_timing(True)
+    A.kapp_hydrogen(*args)
+    ms = ctx.kernel_ms("kapp_hydrogen")
+    ctx.enable_timing(False)
+    n = W["ws"].size * m["t"].size
+    return {"frequencies": int(W["ws"].size), "depths": int(m["t"].size), "kernel_ms": ms,
+            "evals_per_s": n / (ms * 1e-3) if ms > 0 else None,
+            "sources": "HOP (n = 1..80), H2PLOP, HMINOP, HRAYOP, ELECOP and KAPP's totals"}
 
 
 def hbm_peak():

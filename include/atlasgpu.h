@@ -327,6 +327,52 @@ int atlasgpu_atlas_xlinop(atlasgpu_ctx *ctx, const atlasgpu_nlte_line *recs, int
                           const double *contx, const double *xnfp, const double *rho,
                           const atlasgpu_xlinop_hydrogen *h, double *xlines_inout, int64_t *n_other);
 
+/* KAPP's hydrogen continuum tables, as the reference reads them from its data
+ * files and DATA statements (Fortran arrays column-major):
+ *   XKARZAS (atlas12_modules.f90:11635-11804): data/karzas_freqn.dat,
+ *     karzas_xn.dat, karzas_xl.dat, karzas_ekarzas.dat (REAL(4));
+ *   COULFF (:11995-12196): data/gauntff_vanhoof.dat, the 146 rows of 81
+ *     thermally averaged g_ff (the library takes log10 as the reader does);
+ *   holtsmark_Q (:425-464): Q_HOLTSMARK;
+ *   HOP (:11359-11608): the level energies E_n of n = 1..15 (cm^-1; E_1 = 0);
+ *   HMINOP (:12360-12558): WBF, BF, THETAFF, WAVEK, FF (FF holds REAL(4)
+ *     literals, so its values are single-precision roundings);
+ *   H2PLOP (:12224-12252): the FR and ES fit coefficients, signed, lowest
+ *     order first;
+ *   HRAYOP (:12740-12906): GAVRILAM, GAVRILAMAB, GAVRILAMBC, GAVRILAMCD,
+ *     GAVRILALYMANCONT, FGAVRILALYMANCONT. */
+typedef struct atlasgpu_kapp_tables {
+  float freqn[15][29], xn[15][29], xl[6][6][29], ekarzas[29];
+  double gff[146][81];
+  double q_holtsmark[150];
+  double hop_elev[15];
+  double hmin_wbf[116], hmin_bf[116], hmin_thetaff[11], hmin_wavek[22], hmin_ff[22][11];
+  double h2p_fr[5], h2p_es[6];
+  double ray_m[74], ray_ab[27], ray_bc[24], ray_cd[22], ray_ly[64], ray_fly[64];
+} atlasgpu_kapp_tables;
+
+/* Keeps KAPP's hydrogen tables on the context for atlasgpu_atlas_kapp_hydrogen
+ * (COULFF's log10 of g_ff and HMINOP's log tables are taken here, once, as the
+ * reference's first calls do). */
+int atlasgpu_atlas_set_kapp_tables(atlasgpu_ctx *ctx, const atlasgpu_kapp_tables *tables);
+
+/* KAPP (atlas12_modules.f90:11202-11324) with its hydrogen, H-, H2+ and
+ * scattering sources, per frequency and depth: HOP (:11359-11608: bound-free
+ * from n = 1..15 with Karzas-Latter cross-sections and the occupation
+ * probabilities of Hummer & Mihalas, n = 16..80, the dissolved-level
+ * pseudo-continuum, free-free with COULFF), H2PLOP, HMINOP (McLaughlin
+ * bound-free, Bell & Berrington free-free), HRAYOP (Gavrila), ELECOP; the
+ * totals ACONT, SCONT, SIGMAC as KAPP forms them with the helium, metal, H2
+ * and line sources zero.  WAVESET (nm) [numnu]; depth vectors [nrhox]: T, XNE,
+ * RHO, XNFP(J,1) (H I number density over its partition function), XNFP(J,2)
+ * (H II); bhyd BHYD(J,1..6) as [6][kw] and bmin BMIN(J) [kw], or NULL for LTE
+ * (1).  Outputs [numnu][kw]; parts, if not NULL, [numnu][7][kw]: AHYD, SHYD,
+ * AH2P, AHMIN, SHMIN, SIGH, SIGEL. */
+int atlasgpu_atlas_kapp_hydrogen(atlasgpu_ctx *ctx, int numnu, const double *waveset, int nrhox, int kw,
+                                 const double *t, const double *xne, const double *rho, const double *xnfp1,
+                                 const double *xnfp2, const double *bhyd, const double *bmin, double *acont,
+                                 double *sigmac, double *scont, double *parts);
+
 /* RUN_RT_PASS frequency loop (atlas12_modules.f90:3880-3951): per NU the
  * Planck terms, ALINE = XLINES*STIM, JOSH(1,0) (:18398-18776), the negative
  * floor and the TCORR/RADIAP/ROSS mode-2 sums.  acont/sigmac [numnu][kw]

@@ -329,6 +329,37 @@ int orc_synthe_hydrogen_opacity(const orc_nlte_line_t *recs, int64_t n, int leng
                                 int nspec, const double *xne, const double *hckt, const orc_htab_t *tab,
                                 const orc_stehle_t *stehle, const orc_shatm_t *atm, double *out);
 
+/* ---- KAPP's hydrogen continuum sources (oracle/kapp.c) ---- */
+/* Tables of HOP/XKARZAS/COULFF/occupation_prob, HMINOP, H2PLOP and HRAYOP,
+ * as the reference reads them from its data files and DATA statements.
+ * Fortran arrays column-major. */
+typedef struct {
+  const float *freqn, *xn, *xl, *ekarzas; /* FREQN(29,15), XN(29,15), XL(29,6,6), EKARZAS(29): REAL(4) */
+  const double *gff_logtab;               /* GFF_LOGTAB(81,146): log10 of van Hoof's g_ff */
+  const double *q_holtsmark;              /* Q_HOLTSMARK(150) */
+  const double *hop_elev;                 /* HOP's level energies E_n (cm^-1), n = 1..15 */
+  const double *hmin_wbf, *hmin_bf;       /* HMINOP WBF(116), BF(116) */
+  const double *hmin_thetaff;             /* THETAFF(11) */
+  const double *hmin_wavek;               /* WAVEK(22) */
+  const double *hmin_ff;                  /* FF(11,22) (REAL(4) literals) */
+  const double *h2p_fr, *h2p_es;          /* H2PLOP's fits: FR coefficients [5], ES [6], signed */
+  const double *ray_m, *ray_ab, *ray_bc, *ray_cd; /* GAVRILAM(74), AB(27), BC(24), CD(22) */
+  const double *ray_ly, *ray_fly;         /* GAVRILALYMANCONT(64), FGAVRILALYMANCONT(64) */
+} orc_kapp_tables;
+
+enum {
+  ORC_KAPP_AHYD, ORC_KAPP_SHYD, ORC_KAPP_AH2P, ORC_KAPP_AHMIN, ORC_KAPP_SHMIN, ORC_KAPP_SIGH, ORC_KAPP_SIGEL,
+  ORC_KAPP_ACONT, ORC_KAPP_SCONT, ORC_KAPP_SIGMAC, ORC_KAPP_NOUT
+};
+
+double orc_occupation_prob(const orc_kapp_tables *tb, int n, double xne);
+void orc_log10_array(const double *in, double *out, int n);
+double orc_xkarzas(const orc_kapp_tables *tb, double freq, double zeff2, int n, int l);
+/* out[q * nrhox + j], q = ORC_KAPP_*; bhyd BHYD(J,n) at [(n-1)*nrhox + j] or NULL (1); bmin or NULL (1) */
+void orc_kapp_hydrogen(const orc_kapp_tables *tb, double wave, int nrhox, const double *t, const double *xne,
+                       const double *rho, const double *xnfp1, const double *xnfp2, const double *bhyd,
+                       const double *bmin, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -656,3 +656,60 @@ def synthe_hydrogen_opacity(recs, length, wbegin, ratio, wlend, velshift_kms, co
     if rc != 0:
         raise ValueError("hydrogen record NBLO/NBUP/NCON outside EHYD/ALPHAHYD/CONTH")
     return out
+
+
+# ---------------------------------------------------------------- KAPP (hydrogen sources)
+KAPP_NAMES = ("ahyd", "shyd", "ah2p", "ahmin", "shmin", "sigh", "sigel", "acont", "scont", "sigmac")
+
+
+class KappTables(ctypes.Structure):
+    """orc_kapp_tables; keeps its arrays alive (built by kapp_tables)."""
+    _fields_ = [(k, _fp) for k in ("freqn", "xn", "xl", "ekarzas")] + \
+               [(k, _dp) for k in ("gff_logtab", "q_holtsmark", "hop_elev", "hmin_wbf", "hmin_bf", "hmin_thetaff",
+                                   "hmin_wavek", "hmin_ff", "h2p_fr", "h2p_es", "ray_m", "ray_ab", "ray_bc", "ray_cd",
+                                   "ray_ly", "ray_fly")]
+
+
+def _lib_kapp():
+    L = lib()
+    if not getattr(L, "_kapp_declared", False):
+        L.orc_log10_array.argtypes = [_dp, _dp, ctypes.c_int]
+        L.orc_occupation_prob.argtypes = [ctypes.POINTER(KappTables), ctypes.c_int, ctypes.c_double]
+        L.orc_occupation_prob.restype = ctypes.c_double
+        L.orc_xkarzas.argtypes = [ctypes.POINTER(KappTables), ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                  ctypes.c_int]
+        L.orc_xkarzas.restype = ctypes.c_double
+        L.orc_kapp_hydrogen.argtypes = [ctypes.POINTER(KappTables), ctypes.c_double, ctypes.c_int] + [_dp] * 8
+        L._kapp_declared = True
+    return L
+
+
+def kapp_tables(tables):
+    """KappTables from the k_* entries of the reference tables (GFF as its
+    reader stores it: log10 by the C library)."""
+    L = _lib_kapp()
+    keep = {}
+    for k in ("freqn", "xn", "xl", "ekarzas"):
+        keep[k] = np.ascontiguousarray(tables["k_" + k], np.float32)
+    gff = _d(tables["k_gff"])
+    keep["gff_logtab"] = np.empty_like(gff)
+    L.orc_log10_array(_ptr(gff), _ptr(keep["gff_logtab"]), gff.size)
+    for k in ("q_holtsmark", "hop_elev", "hmin_wbf", "hmin_bf", "hmin_thetaff", "hmin_wavek", "hmin_ff", "h2p_fr",
+              "h2p_es", "ray_m", "ray_ab", "ray_bc", "ray_cd", "ray_ly", "ray_fly"):
+        keep[k] = _d(tables["k_" + k])
+    kt = KappTables(*[_ptr(keep[n], _fp if t is _fp else _dp) for n, t in KappTables._fields_])
+    kt._keep = keep
+    return kt
+
+
+def kapp_hydrogen(kt, wave, t, xne, rho, xnfp1, xnfp2, bhyd=None, bmin=None):
+    """KAPP's hydrogen sources and totals at one wavelength (nm): dict of [nrhox] arrays (KAPP_NAMES)."""
+    L = _lib_kapp()
+    nr = len(t)
+    out = np.zeros((len(KAPP_NAMES), nr))
+    v = [_d(a) for a in (t, xne, rho, xnfp1, xnfp2)]
+    bh = None if bhyd is None else _d(bhyd)
+    bm = None if bmin is None else _d(bmin)
+    L.orc_kapp_hydrogen(ctypes.byref(kt), float(wave), nr, *[_ptr(a) for a in v],
+                        _ptr(bh) if bh is not None else None, _ptr(bm) if bm is not None else None, _ptr(out))
+    return dict(zip(KAPP_NAMES, out))

@@ -173,6 +173,76 @@ def stehle_dims(datadir):
     return np.array(rows, dtype=np.int64)
 
 
+def read_real4_lines(path, skip, count):
+    """One REAL(4) per list-directed READ after `skip` header lines (XKARZAS's
+    read_karzas_tables, atlas12_modules.f90:11730-11802)."""
+    lines = open(path).read().splitlines()[skip:skip + count]
+    vals = np.array([_libc.strtof(l.split()[0].encode(), None) for l in lines], dtype=np.float32)
+    assert vals.size == count, path
+    return vals
+
+
+def read_gauntff(path):
+    """data/gauntff_vanhoof.dat as COULFF's reader takes it (:12098-12194):
+    five header values after the '#' comments, then 146 rows of 81 g_ff
+    (read into REAL(8)); returned as GFF(81,146) column-major, the raw values
+    (the library and the oracle take log10 themselves)."""
+    rows = []
+    for line in open(path):
+        line = line.split("#", 1)[0].strip()
+        if line:
+            rows.append(line)
+    head, data = rows[:5], rows[5:5 + 146]  # (the uncertainty table after it is not read)
+    assert int(head[0]) == 20140210 and head[1].split() == ["81", "146"], head
+    vals = np.array([[float(x.replace("D", "e").replace("d", "e")) for x in r.split()] for r in data])
+    assert vals.shape == (146, 81), vals.shape
+    return vals.reshape(-1)  # [J][I]: GFF(I, J) at J * 81 + I
+
+
+def kapp_tables(mod, datadir):
+    """KAPP's hydrogen continuum tables: XKARZAS's Karzas-Latter files,
+    COULFF's van Hoof table, Q_HOLTSMARK, HOP's level energies, HMINOP's
+    bound-free and Bell & Berrington free-free tables (FF is written with
+    REAL(4) literals, so each value is rounded to single precision), H2PLOP's
+    fits and HRAYOP's Gavrila factors (atlas12_modules.f90:425-464,
+    :11359-11608, :12224-12252, :12360-12558, :12740-12906)."""
+    hop = mod[mod.index("SUBROUTINE HOP"):mod.index("END SUBROUTINE HOP")]
+    elev = [float(x) for x in re.findall(r"EXP\(-([0-9.]+)D0 \* HCKT\(J\)\)", hop)]
+    assert len(elev) == 14, len(elev)  # n = 15 .. 2
+    hmin = mod[mod.index("SUBROUTINE HMINOP"):mod.index("END SUBROUTINE HMINOP")]
+    h2p = mod[mod.index("SUBROUTINE H2PLOP"):mod.index("END SUBROUTINE H2PLOP")]
+    ray = mod[mod.index("SUBROUTINE HRAYOP"):mod.index("END SUBROUTINE HRAYOP")]
+    num = r"([-+]?[0-9.]+D[-+]?[0-9]+)"
+    f = lambda x: float(x.replace("D", "e"))
+    fr = re.search(r"FR = " + num + r" \+ \(" + num + r" \+ \(" + num + r" &\s*\+ \(" + num + r" - " + num +
+                   r" \* FREQLG\)", h2p)
+    es = re.search(r"ES = " + num + r" \+ \(" + num + r" \+ \(" + num + r" &\s*\+ \(" + num + r" \+ \(" + num +
+                   r" - " + num + r" \* FREQ\)", h2p)
+    f32 = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)
+    return dict(
+        k_freqn=read_real4_lines(os.path.join(datadir, "karzas_freqn.dat"), 2, 29 * 15),
+        k_xn=read_real4_lines(os.path.join(datadir, "karzas_xn.dat"), 3, 29 * 15),
+        k_xl=read_real4_lines(os.path.join(datadir, "karzas_xl.dat"), 3, 29 * 36),
+        k_ekarzas=read_real4_lines(os.path.join(datadir, "karzas_ekarzas.dat"), 2, 29),
+        k_gff=read_gauntff(os.path.join(datadir, "gauntff_vanhoof.dat")),
+        k_q_holtsmark=fortran_array(mod, "Q_HOLTSMARK(150) =", 150),
+        k_hop_elev=np.array([0.0] + elev[::-1]),
+        k_hmin_wbf=fortran_array(hmin, ":: WBF(116) =", 116),
+        k_hmin_bf=fortran_array(hmin, ":: BF(116) =", 116),
+        k_hmin_thetaff=fortran_array(hmin, ":: THETAFF(11) =", 11),
+        k_hmin_wavek=fortran_array(hmin, ":: WAVEK(22) =", 22),
+        k_hmin_ff=f32(fortran_array(hmin, ":: FF(11, 22) =", 242)),
+        k_h2p_fr=np.array([f(fr.group(1)), f(fr.group(2)), f(fr.group(3)), f(fr.group(4)), -f(fr.group(5))]),
+        k_h2p_es=np.array([f(es.group(k)) for k in range(1, 6)] + [-f(es.group(6))]),
+        k_ray_m=fortran_array(ray, ":: GAVRILAM(74) =", 74),
+        k_ray_ab=fortran_array(ray, ":: GAVRILAMAB(27) =", 27),
+        k_ray_bc=fortran_array(ray, ":: GAVRILAMBC(24) =", 24),
+        k_ray_cd=fortran_array(ray, ":: GAVRILAMCD(22) =", 22),
+        k_ray_ly=fortran_array(ray, ":: GAVRILALYMANCONT(64) =", 64),
+        k_ray_fly=fortran_array(ray, ":: FGAVRILALYMANCONT(64) =", 64),
+    )
+
+
 def main():
     if not ROOT or not os.path.isdir(ROOT):
         sys.exit("usage: make_golden.py <reference_root>  (or ATLAS12_REFERENCE=<reference_root>)")
@@ -215,6 +285,7 @@ def main():
     out["h_propbm"], out["h_c"], out["h_d"] = read_stark(os.path.join(ROOT, "data", "stark_profile.dat"))
     out.update(synthe_hydrogen_tables(syn, mod))
     out["stehle_dims"] = stehle_dims(os.path.join(ROOT, "data"))
+    out.update(kapp_tables(mod, os.path.join(ROOT, "data")))
     out["deck"], out["deck_pradk"] = read_deck(os.path.join(ROOT, "workdir", "ap00t5777g4.44at12.dat"))
     np.savez(os.path.join(HERE, "reference_tables.npz"), **out)
     np.savez(PACKAGE_DATA, **{k: v for k, v in out.items() if k not in TEST_ONLY})
