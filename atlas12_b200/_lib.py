@@ -105,6 +105,7 @@ SIGNATURES = {
     "atlasgpu_model_iterate_end": (_I, [_P, _P, ctypes.POINTER(_D)]),
     "atlasgpu_surrogate_eval": (_I, [_P, _I, _P, _P, _D, _I, _P, _P, _P, _P, _P]),
     "atlasgpu_fp64_peak_tflops": (_D, [_P]),
+    "atlasgpu_u64_atomic_peak": (_D, [_P]),
     "atlasgpu_mlp_create": (_I, [_P, _I, _I, _I, _I, ctypes.c_uint64, ctypes.POINTER(_P)]),
     "atlasgpu_mlp_destroy": (_I, [_P, _P]),
     "atlasgpu_mlp_nparam": (_I64, [_P]),

@@ -231,6 +231,18 @@ __global__ void k_fp64_fma(double* out, int iters) {
   if (s == 12345.678) out[0] = s;  // keep the chains alive
 }
 
+// 64-bit integer atomic adds at L2, lanes of a warp on 32 consecutive words
+// (as LINOP1's lanes at consecutive depths), warps scattered over the region
+__global__ void k_u64_atomics(unsigned long long* w, size_t nwords, int iters) {
+  const size_t warp = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const size_t nrows = nwords / 32;
+  for (int i = 0; i < iters; ++i) {
+    const size_t row = (warp * 7919u + (size_t)i * 104729u) % nrows;
+    atomicAdd(w + row * 32 + lane, 1ull);
+  }
+}
+
 template <class T>
 int dalloc(atlasgpu_ctx* ctx, T** p, size_t n) {
   if (cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
@@ -637,6 +649,29 @@ double atlasgpu_fp64_peak_tflops(atlasgpu_ctx* ctx) {
   if (cudaGetLastError() != cudaSuccess || ms <= 0.f) return -1.0;
   const double flops = 2.0 * 8.0 * iters * (double)threads * blocks;
   return flops / (ms * 1e-3) / 1e12;
+}
+
+double atlasgpu_u64_atomic_peak(atlasgpu_ctx* ctx) {
+  if (!ctx) return -1.0;
+  cudaSetDevice(ctx->device);
+  const size_t nwords = (size_t)1 << 23;  // 64 MB: LINOP1's fixed-point words of one model
+  unsigned long long* w;
+  if (bufT(ctx, "atom_peak", nwords, &w)) return -1.0;
+  const int iters = 256, threads = 256, blocks = ctx->nsm * 8;
+  k_u64_atomics<<<blocks, threads, 0, ctx->stream>>>(w, nwords, 16);  // warm-up
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, ctx->stream);
+  k_u64_atomics<<<blocks, threads, 0, ctx->stream>>>(w, nwords, iters);
+  cudaEventRecord(b, ctx->stream);
+  cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (cudaGetLastError() != cudaSuccess || ms <= 0.f) return -1.0;
+  return (double)iters * threads * blocks / (ms * 1e-3) / 1e9;
 }
 
 }  // extern "C"

@@ -363,9 +363,23 @@ struct LinopArgs {
   const double* fscale = nullptr;
 };
 
-__device__ __forceinline__ void linop_add(const LinopArgs& a, int J, int iw, double cv) {
+// Adds one wing value into XLINES(J, IW).  kDry: adds nothing and returns
+// the number of atomics the add would issue (the counting pass of a timed
+// measurement; the walk is the same), else returns 0.
+template <bool kDry>
+__device__ __forceinline__ int linop_add(const LinopArgs& a, int J, int iw, double cv) {
+  if (kDry) {
+    if (!a.xfix) return 1;
+    const double y = cv * a.fscale[J - 1];
+    const double t2 = floor(y * kFixTop);
+    const double r2 = y - t2 * 0x1p96;
+    const double t1 = floor(r2 * kFixMid);
+    const double t0 = rint(r2 - t1 * 0x1p48);
+    return (t2 > 0.0) + (t1 > 0.0) + (t0 > 0.0);
+  }
   if (a.xfix) fix_add(a.xfix + ((size_t)(iw - 1) * kFixWords) * a.kw + (J - 1), a.kw, cv * a.fscale[J - 1]);
   else atomicAdd(a.xl + (size_t)(iw - 1) * a.kw + (J - 1), cv);
+  return 0;
 }
 
 // LINOP1's profile value at one wing point, V = (distance in nm) * RDOP with
@@ -412,10 +426,11 @@ __device__ __forceinline__ bool linop_below(const LinopArgs& a, double cv, doubl
 // The rest of one (line, depth) walk after a lane gave up on it, by the
 // whole warp (lanes over wing points), add-then-test as in the reference:
 // red points rnext..iwmax unless rdone, blue offsets bnext..100 unless bdone.
-template <bool F32>
+template <bool F32, bool kDry>
 static __device__ __noinline__ unsigned linop_finish_warp(const LinopArgs& a, int J, double center, double adamp,
                                                           double rdop, double wlvac, int nu, double tc, int rnext,
-                                                          bool rdone, int bnext, bool bdone, double wcon, int lane) {
+                                                          bool rdone, int bnext, bool bdone, double wcon, int lane,
+                                                          unsigned long long& atoms) {
   unsigned added = 0;  // points this lane added
   const int iwmax = min(nu + a.max_wing, a.numnu);
   const int nuh = a.nu_hi > 0 ? a.nu_hi : a.numnu;
@@ -433,7 +448,7 @@ static __device__ __noinline__ unsigned linop_finish_warp(const LinopArgs& a, in
       const unsigned stop = __ballot_sync(0xffffffffu, valid && below);
       const int last = stop ? base + __ffs(stop) - 1 : iwmax;
       if (valid && iw <= last && iw >= a.nu_lo && iw <= nuh) {
-        linop_add(a, J, iw, cv);
+        atoms += linop_add<kDry>(a, J, iw, cv);
         ++added;
       }
       if (stop) break;
@@ -456,7 +471,7 @@ static __device__ __noinline__ unsigned linop_finish_warp(const LinopArgs& a, in
       const unsigned inval = __ballot_sync(0xffffffffu, !valid);
       const int ilast = stop ? i0 + __ffs(stop) - 1 : a.max_wing;
       if (valid && i <= ilast && iw >= a.nu_lo && iw <= nuh) {
-        linop_add(a, J, iw, cv);
+        atoms += linop_add<kDry>(a, J, iw, cv);
         ++added;
       }
       if (stop || inval) break;
@@ -475,140 +490,179 @@ static __device__ __noinline__ unsigned linop_finish_warp(const LinopArgs& a, in
 // share the WAVESET window and the XLINES lines they touch in cache.
 // Measured on the 500,000-line, 30,000-frequency pass (solar / cool model):
 // 4 points per lane and one line per warp 4.45 / 5.49 ms; 16 points, chunks
-// of 8 lines and four CTAs per SM (64 registers) 3.74 / 4.80 ms.
+// of 8 lines and four CTAs per SM (64 registers) 3.74 / 4.80 ms.  In the
+// 32-slot batch of one model (per model-iteration, solar / cool giant): 16
+// points 2.42 / 3.39 ms, 32 points 2.36 / 3.39, 64 points 2.31 / 3.39; but on
+// the bench's mixed 32-model batch 64 points took 2.37 ms against 2.27 for 16.
 constexpr int kLinopLanePts = 16;
 constexpr int kLinopChunk = 8;
 constexpr int kLinopMinBlocks = 4;
 
-template <bool F32>
-static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
-  const int lane = threadIdx.x & 31;
-  const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned long long walked = 0, points = 0;
+// One stored line by one warp (lanes over depths): the coarse and fine
+// depth gates and the red and blue wing walks of LINOP1 (:18236-18370).
+// walked / points count the walked (line, depth) pairs and the wing points
+// this lane added.
+template <bool F32, bool kDry = false>
+static __device__ __forceinline__ void linop_line(const LinopArgs& a, int64_t il, int lane, unsigned long long& walked,
+                                                  unsigned long long& points, unsigned long long& atoms) {
   const int nuh = a.nu_hi > 0 ? a.nu_hi : a.numnu;
-  for (int64_t il0 = w0 * kLinopChunk; il0 < a.n; il0 += nw * kLinopChunk)
-  for (int64_t il = il0; il < il0 + kLinopChunk && il < a.n; ++il) {
-    const AtlasLine L = a.lines[il];
-    if (L.nelion == 0 || L.nu + a.max_wing < a.nu_lo || L.nu - a.max_wing > nuh) continue;
-    const double cx = a.lcontx ? a.lcontx[il] : 0.0;
-    const double* xdn = a.xnfdop + (size_t)(L.nelion - 1) * a.kw;
-    const double* dpn = a.dopple + (size_t)(L.nelion - 1) * a.kw;
-    const double* tcv = a.tabcont + (size_t)(L.nucont - 1) * a.kw;
-    // coarse gates: depths 8, 16, ... (lane k -> depth 8(k+1)); bit k = IFJ at depth 8(k+1)
-    int pass = 0;
-    {
-      const int J = 8 * (lane + 1);
-      if (J <= a.nrhox) {
-        double c = L.cgf * xdn[J - 1];
-        if (c >= tcv[J - 1]) {
-          c = c * exp(-L.elo * a.hckt[J - 1]);
-          pass = c >= tcv[J - 1];
-        }
-      }
-    }
-    const unsigned ifj = __ballot_sync(0xffffffffu, pass);
-    if (ifj == 0) continue;
-    if (lane == 0 && a.used) atomicAdd(a.used, 1ull);
-    const int iwmax = min(L.nu + a.max_wing, a.numnu);
-    for (int J0 = 1; J0 <= a.nrhox; J0 += 32) {
-      // a round of 32 depths can walk only where its coarse blocks, or the
-      // block just above its first, passed: skip it before any load if none did
-      {
-        const int kl = (J0 + 7) / 8 - 1, kh = (min(J0 + 31, a.nrhox) + 7) / 8 - 1;
-        const unsigned rmask = ((2u << kh) - 1u) & ~((1u << (kl > 0 ? kl - 1 : 0)) - 1u);
-        if (!(ifj & rmask)) continue;
-      }
-      const int J = J0 + lane;
-      bool walk = false;
-      double center = 0.0, tc = 0.0;
-      const int K = 8 * ((J + 7) / 8);  // the coarse depth closing J's block
-      if (J <= a.nrhox && K <= a.nrhox) {
-        const int k = K / 8 - 1;
-        const bool cur = (ifj >> k) & 1u;
-        tc = tcv[J - 1];
-        if (J == K) {
-          walk = cur;
-          if (walk) center = L.cgf * xdn[J - 1] * exp(-L.elo * a.hckt[J - 1]);
-        } else if (cur || (k > 0 && ((ifj >> (k - 1)) & 1u))) {
-          // fine depth K-7..K-1 of a block next to a passing coarse depth
-          center = L.cgf * xdn[J - 1];
-          if (center >= tc) {
-            center = center * exp(-L.elo * a.hckt[J - 1]);
-            walk = center >= tc;
-          }
-        }
-      }
-      if (!__any_sync(0xffffffffu, walk)) continue;
-      // XLINOP: no walk at a depth whose continuum edge lies redward of the line
-      double wcon = 0.0;
-      if (walk && cx > 0.0) {
-        wcon = 1.0e7 / (cx - a.emerge[J - 1]);
-        if (L.wlvac < wcon) walk = false;
-      }
-      double adamp = 0.0, rdop = 1.0;
-      if (walk) {
-        adamp = (L.gr + L.gs * a.xne[J - 1] + L.gw * a.txnxn[J - 1]) / dpn[J - 1];
-        rdop = 1.0 / (dpn[J - 1] * L.wlvac);
-        ++walked;
-      }
-      bool rdone = !walk, bdone = !walk;
-      int rnext = L.nu, bnext = 1;
-#pragma unroll 1
-      for (int s = 0; s < kLinopLanePts && __any_sync(0xffffffffu, !rdone || !bdone); ++s) {
-        if (!rdone) {
-          const int iw = rnext;
-          const double dl = a.waveset[iw - 1] - L.wlvac;
-          const double cv = linop_cv<F32>(a, center, adamp, dl, rdop);
-          if (iw >= a.nu_lo && iw <= nuh) {
-            linop_add(a, J, iw, cv);
-            ++points;
-          }
-          if (linop_below<F32>(a, cv, tc, center, adamp, dl, rdop) || iw >= iwmax) rdone = true;
-          else rnext = iw + 1;
-        }
-        if (!bdone) {
-          const int iw = L.nu - bnext;
-          if (iw < 1 || a.waveset[iw - 1] < wcon) {
-            bdone = true;
-          } else {
-            const double dl = L.wlvac - a.waveset[iw - 1];
-            const double cv = linop_cv<F32>(a, center, adamp, dl, rdop);
-            if (iw >= a.nu_lo && iw <= nuh) {
-              linop_add(a, J, iw, cv);
-              ++points;
-            }
-            if (linop_below<F32>(a, cv, tc, center, adamp, dl, rdop) || bnext >= a.max_wing) bdone = true;
-            else bnext = bnext + 1;
-          }
-        }
-      }
-      // walks still going: the warp finishes them one at a time
-      unsigned ov = __ballot_sync(0xffffffffu, !rdone || !bdone);
-      while (ov) {
-        const int src = __ffs(ov) - 1;
-        ov &= ov - 1;
-        const int Js = __shfl_sync(0xffffffffu, J, src);
-        const double cs = __shfl_sync(0xffffffffu, center, src);
-        const double as = __shfl_sync(0xffffffffu, adamp, src);
-        const double ds = __shfl_sync(0xffffffffu, rdop, src);
-        const double ts = __shfl_sync(0xffffffffu, tc, src);
-        const int rn = __shfl_sync(0xffffffffu, rnext, src);
-        const int bn = __shfl_sync(0xffffffffu, bnext, src);
-        const bool rd = __shfl_sync(0xffffffffu, (int)rdone, src) != 0;
-        const bool bd = __shfl_sync(0xffffffffu, (int)bdone, src) != 0;
-        const double wc = __shfl_sync(0xffffffffu, wcon, src);
-        points += linop_finish_warp<F32>(a, Js, cs, as, ds, L.wlvac, L.nu, ts, rn, rd, bn, bd, wc, lane);
+  const AtlasLine L = a.lines[il];
+  if (L.nelion == 0 || L.nu + a.max_wing < a.nu_lo || L.nu - a.max_wing > nuh) return;
+  const double cx = a.lcontx ? a.lcontx[il] : 0.0;
+  const double* xdn = a.xnfdop + (size_t)(L.nelion - 1) * a.kw;
+  const double* dpn = a.dopple + (size_t)(L.nelion - 1) * a.kw;
+  const double* tcv = a.tabcont + (size_t)(L.nucont - 1) * a.kw;
+  // coarse gates: depths 8, 16, ... (lane k -> depth 8(k+1)); bit k = IFJ at depth 8(k+1)
+  int pass = 0;
+  {
+    const int J = 8 * (lane + 1);
+    if (J <= a.nrhox) {
+      double c = L.cgf * xdn[J - 1];
+      if (c >= tcv[J - 1]) {
+        c = c * exp(-L.elo * a.hckt[J - 1]);
+        pass = c >= tcv[J - 1];
       }
     }
   }
-  // walked (line, depth) pairs, summed over the warp's lanes
+  const unsigned ifj = __ballot_sync(0xffffffffu, pass);
+  if (ifj == 0) return;
+  if (lane == 0 && a.used) atomicAdd(a.used, 1ull);
+  const int iwmax = min(L.nu + a.max_wing, a.numnu);
+  for (int J0 = 1; J0 <= a.nrhox; J0 += 32) {
+    // a round of 32 depths can walk only where its coarse blocks, or the
+    // block just above its first, passed: skip it before any load if none did
+    {
+      const int kl = (J0 + 7) / 8 - 1, kh = (min(J0 + 31, a.nrhox) + 7) / 8 - 1;
+      const unsigned rmask = ((2u << kh) - 1u) & ~((1u << (kl > 0 ? kl - 1 : 0)) - 1u);
+      if (!(ifj & rmask)) continue;
+    }
+    const int J = J0 + lane;
+    bool walk = false;
+    double center = 0.0, tc = 0.0;
+    const int K = 8 * ((J + 7) / 8);  // the coarse depth closing J's block
+    if (J <= a.nrhox && K <= a.nrhox) {
+      const int k = K / 8 - 1;
+      const bool cur = (ifj >> k) & 1u;
+      tc = tcv[J - 1];
+      if (J == K) {
+        walk = cur;
+        if (walk) center = L.cgf * xdn[J - 1] * exp(-L.elo * a.hckt[J - 1]);
+      } else if (cur || (k > 0 && ((ifj >> (k - 1)) & 1u))) {
+        // fine depth K-7..K-1 of a block next to a passing coarse depth
+        center = L.cgf * xdn[J - 1];
+        if (center >= tc) {
+          center = center * exp(-L.elo * a.hckt[J - 1]);
+          walk = center >= tc;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, walk)) continue;
+    // XLINOP: no walk at a depth whose continuum edge lies redward of the line
+    double wcon = 0.0;
+    if (walk && cx > 0.0) {
+      wcon = 1.0e7 / (cx - a.emerge[J - 1]);
+      if (L.wlvac < wcon) walk = false;
+    }
+    double adamp = 0.0, rdop = 1.0;
+    if (walk) {
+      adamp = (L.gr + L.gs * a.xne[J - 1] + L.gw * a.txnxn[J - 1]) / dpn[J - 1];
+      rdop = 1.0 / (dpn[J - 1] * L.wlvac);
+      ++walked;
+    }
+    bool rdone = !walk, bdone = !walk;
+    int rnext = L.nu, bnext = 1;
+    // each walk's next grid wavelength is loaded one point ahead, so the load
+    // is in flight while the current point is evaluated (the last load of a
+    // walk goes unused; every index stays inside WAVESET)
+    double wr = walk ? a.waveset[rnext - 1] : 0.0;
+    double wb = (walk && L.nu >= 2) ? a.waveset[L.nu - 2] : 0.0;
+#pragma unroll 1
+    for (int s = 0; s < kLinopLanePts && __any_sync(0xffffffffu, !rdone || !bdone); ++s) {
+      if (!rdone) {
+        const int iw = rnext;
+        const double wr_next = iw < a.numnu ? a.waveset[iw] : 0.0;
+        const double dl = wr - L.wlvac;
+        const double cv = linop_cv<F32>(a, center, adamp, dl, rdop);
+        if (iw >= a.nu_lo && iw <= nuh) {
+          atoms += linop_add<kDry>(a, J, iw, cv);
+          ++points;
+        }
+        if (linop_below<F32>(a, cv, tc, center, adamp, dl, rdop) || iw >= iwmax) {
+          rdone = true;
+        } else {
+          rnext = iw + 1;
+          wr = wr_next;
+        }
+      }
+      if (!bdone) {
+        const int iw = L.nu - bnext;
+        if (iw < 1 || wb < wcon) {
+          bdone = true;
+        } else {
+          const double wb_next = iw >= 2 ? a.waveset[iw - 2] : 0.0;
+          const double dl = L.wlvac - wb;
+          const double cv = linop_cv<F32>(a, center, adamp, dl, rdop);
+          if (iw >= a.nu_lo && iw <= nuh) {
+            atoms += linop_add<kDry>(a, J, iw, cv);
+            ++points;
+          }
+          if (linop_below<F32>(a, cv, tc, center, adamp, dl, rdop) || bnext >= a.max_wing) {
+            bdone = true;
+          } else {
+            bnext = bnext + 1;
+            wb = wb_next;
+          }
+        }
+      }
+    }
+    // walks still going: the warp finishes them one at a time
+    unsigned ov = __ballot_sync(0xffffffffu, !rdone || !bdone);
+    while (ov) {
+      const int src = __ffs(ov) - 1;
+      ov &= ov - 1;
+      const int Js = __shfl_sync(0xffffffffu, J, src);
+      const double cs = __shfl_sync(0xffffffffu, center, src);
+      const double as = __shfl_sync(0xffffffffu, adamp, src);
+      const double ds = __shfl_sync(0xffffffffu, rdop, src);
+      const double ts = __shfl_sync(0xffffffffu, tc, src);
+      const int rn = __shfl_sync(0xffffffffu, rnext, src);
+      const int bn = __shfl_sync(0xffffffffu, bnext, src);
+      const bool rd = __shfl_sync(0xffffffffu, (int)rdone, src) != 0;
+      const bool bd = __shfl_sync(0xffffffffu, (int)bdone, src) != 0;
+      const double wc = __shfl_sync(0xffffffffu, wcon, src);
+      points += linop_finish_warp<F32, kDry>(a, Js, cs, as, ds, L.wlvac, L.nu, ts, rn, rd, bn, bd, wc, lane, atoms);
+    }
+  }
+}
+
+// walked (line, depth) pairs, wing points and XLINES atomics, summed over
+// the warp's lanes (work[0] points, work[1] atomics)
+__device__ __forceinline__ void linop_counts(const LinopArgs& a, int lane, unsigned long long walked,
+                                             unsigned long long points, unsigned long long atoms) {
   for (int o = 16; o > 0; o >>= 1) walked += __shfl_xor_sync(0xffffffffu, walked, o);
   if (lane == 0 && walked && a.npairs) atomicAdd(a.npairs, walked);
   if (a.work) {
     for (int o = 16; o > 0; o >>= 1) points += __shfl_xor_sync(0xffffffffu, points, o);
-    if (lane == 0) atomicAdd(a.work, points);
+    for (int o = 16; o > 0; o >>= 1) atoms += __shfl_xor_sync(0xffffffffu, atoms, o);
+    if (lane == 0) {
+      atomicAdd(a.work, points);
+      if (atoms) atomicAdd(a.work + 1, atoms);
+    }
   }
+}
+
+// kDry: the counting pass (walks, counts the wing points and the atomics the
+// adds would issue, adds nothing)
+template <bool F32, bool kDry = false>
+static __device__ __forceinline__ void linop_body(const LinopArgs& a) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long walked = 0, points = 0, atoms = 0;
+  for (int64_t il0 = w0 * kLinopChunk; il0 < a.n; il0 += nw * kLinopChunk)
+    for (int64_t il = il0; il < il0 + kLinopChunk && il < a.n; ++il)
+      linop_line<F32, kDry>(a, il, lane, walked, points, atoms);
+  linop_counts(a, lane, walked, points, atoms);
 }
 
 template <bool F32>

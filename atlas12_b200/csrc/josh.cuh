@@ -179,7 +179,7 @@ __device__ inline void g_integ(G& g, const double* x, const double* f, double* f
 
 // ---------------------------------------------------------------- DERIV
 template <class G>
-__device__ inline void g_deriv(G& g, const double* x, const double* f, double* dfdx, int n) {
+__device__ __noinline__ void g_deriv(G& g, const double* x, const double* f, double* dfdx, int n) {
   constexpr int C = (kKwMax + G::N - 1) / G::N;
   const double s = fabs(x[1] - x[0]) / (x[1] - x[0]);
   double v[C];
@@ -233,7 +233,7 @@ __device__ __forceinline__ void map1_for(const double* xo, const double* fo, int
 
 // Returns MAP1 (index of the last old interval used).  xnew ascending.
 template <class G>
-__device__ inline int g_map1(G& g, const double* xo, const double* fo, int nold, const double* xn,
+__device__ __noinline__ int g_map1(G& g, const double* xo, const double* fo, int nold, const double* xn,
                              double* fn, int nnew, int* lidx) {
   // bracket: L_k = min{L >= 2 : XOLD(L) > XNEW(k)}, nold+1 when past the end
   for (int k = g.r; k < nnew; k += G::N) {

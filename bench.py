@@ -67,9 +67,15 @@ FLOPS_PER_NU = int(2 / 3 * 51 ** 3 + 8 * 51 ** 2 + 2 * 51 + 110 * 72)
 FLOPS_PER_SOLVE = int(2 / 3 * 51 ** 3 + 4 * 51 ** 2)
 FLOPS_PER_SERIES_STEP = 2 * 51 ** 2 + 3 * 51
 # DRAM bytes per model of the three batched RT launches (ncu, 4-slot capture
-# of this workload): ACONT, SIGMAC, XLINES read and the per-frequency records
-# written and read back
-RT_TRAFFIC_PER_MODEL = 60.8e6
+# of this workload: 337 MB per model, of which 138 MB are the post stage's
+# partial-sum rows, one per frequency at 4 slots; at 32 slots a post warp
+# takes 6-7 frequencies and its rows are 22 MB per model): ACONT, SIGMAC and
+# XLINES read by the prepare and finish stages, the per-frequency records
+# written and read back, the partial sums
+RT_TRAFFIC_PER_MODEL = 221e6
+# DRAM bytes per model of one batched LINOP1 launch (ncu, 4-slot capture of
+# this workload): the prepared line records and the fixed-point XLINES words
+LINOP_TRAFFIC_PER_MODEL = 60.4e6
 # bytes of one prepared LINOP1 line record on the device (AtlasLine)
 LINE_RECORD_BYTES = 56
 # FP64 operations of one SYNTHE Weideman Voigt evaluation (31 complex Horner
@@ -378,6 +384,7 @@ def run_ours(args):
     names = ("eos", "kapcont", "kapp", "linop", "rt", "rt_pre", "rt_solve", "rt_post", "reduce", "finish")
     kms = {k: ctx.kernel_ms("batch_" + k) for k in names}
     linop_points = ctx.kernel_work("batch_linop_points")
+    linop_atomics = ctx.kernel_work("batch_linop_atomics")
     rt_solves = {k: ctx.kernel_work("batch_rt_" + k) for k in ("eliminated", "series", "series_steps")}
     ctx.enable_timing(False)
     batch.run()
@@ -394,24 +401,41 @@ def run_ours(args):
             "unit": "TFLOP/s", "frac": ach / fp64_peak if fp64_peak > 0 else None,
             "executed_tflops": executed / (kms["rt"] * 1e-3) / 1e12,
             "traffic": RT_TRAFFIC_PER_MODEL * CFG["slots"],
-            "traffic_scaling": "ncu capture of the three launches of a 4-slot batch, per model, times slots",
+            "traffic_scaling": "ncu capture of the three launches of a 4-slot batch (337 MB per model), its "
+                               "partial-sum rows rescaled to this batch's 6-7 frequencies per post warp, times slots",
             "peak_source": "measured DFMA loop on this GPU (atlasgpu_fp64_peak_tflops); MEASURED_PEAKS.json has no FP64 figure",
             "work": f"{FLOPS_PER_NU} FP64 flop per frequency (the reference's elimination counted for every "
                     f"system) x {CFG['numnu']} frequencies x {CFG['slots']} models per pass; executed_tflops counts "
                     "the series steps and eliminations actually run",
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the three RT launches (profiles/)"}
-    # LINOP1 over the batch: wing points added into XLINES per second, and the
-    # algorithmic bytes (prepared line records read once per slot, XLINES
-    # read and written once) against HBM
+    # LINOP1 over the batch: its bound is the L2 atomics of the exact XLINES
+    # sums (each wing point adds 1-3 64-bit words, the access pattern of the
+    # measured atomic peak); the algorithmic bytes (prepared line records read
+    # once per slot, XLINES read and written once) against HBM beside it
     hbm, hbm_src = hbm_peak()
+    atom_peak = float(_lib.lib().atlasgpu_u64_atomic_peak(ctx.handle))  # 1e9 atomics/s
+    linop_s = kms["linop"] * 1e-3
     linop_bytes = CFG["slots"] * (CFG["nlines"] * LINE_RECORD_BYTES + 2 * 8 * CFG["numnu"] * CFG["nrhox"])
-    rooflines = [{"kernel": "k_batch_linop (LINOP1 wing walks)", "bound": "hbm", "unit": "GB/s",
-                  "achieved": linop_bytes / (kms["linop"] * 1e-3) / 1e9, "peak": hbm, "peak_source": hbm_src,
-                  "frac": linop_bytes / (kms["linop"] * 1e-3) / 1e9 / hbm,
-                  "points_per_s": linop_points / (kms["linop"] * 1e-3) if linop_points > 0 else None,
-                  "points": linop_points,
-                  "work": f"{LINE_RECORD_BYTES} B per prepared line x {CFG['nlines']} lines + XLINES "
-                          f"({CFG['numnu']} x {CFG['nrhox']} FP64) read and written, per slot"}]
+    linop_roof = {"kernel": "k_batch_linop (LINOP1 wing walks, exact fixed-point XLINES sums)", "bound": "l2_atomics",
+                  "unit": "G atomics/s", "achieved": linop_atomics / linop_s / 1e9 if linop_atomics > 0 else None,
+                  "peak": atom_peak, "peak_source": "measured 64-bit atomic-add loop on this GPU "
+                                                    "(atlasgpu_u64_atomic_peak; warps on 32 consecutive words)",
+                  "frac": (linop_atomics / linop_s / 1e9 / atom_peak) if linop_atomics > 0 and atom_peak > 0 else None,
+                  "atomics": linop_atomics, "points": linop_points,
+                  "points_per_s": linop_points / linop_s if linop_points > 0 else None,
+                  "hbm": {"achieved": linop_bytes / linop_s / 1e9, "peak": hbm, "peak_source": hbm_src,
+                          "frac": linop_bytes / linop_s / 1e9 / hbm, "unit": "GB/s",
+                          "work": f"{LINE_RECORD_BYTES} B per prepared line x {CFG['nlines']} lines + XLINES "
+                                  f"({CFG['numnu']} x {CFG['nrhox']} FP64) read and written, per slot"},
+                  "traffic": LINOP_TRAFFIC_PER_MODEL * CFG["slots"],
+                  "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 4-slot k_batch_linop "
+                                    "launch (profiles/), per model, times slots",
+                  "work": "counted 64-bit atomic adds of one batched launch (32 slots)"}
+    # the dominant kernel of the step carries the line's roofline key
+    if kms["linop"] > kms["rt"]:
+        roof, rooflines = linop_roof, [roof]
+    else:
+        rooflines = [linop_roof]
 
     # ATLAS mixed precision against the plain all-FP64 arithmetic on the same
     # models from the same starts (north star (1)): converged structures

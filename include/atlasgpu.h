@@ -109,9 +109,12 @@ double atlasgpu_kernel_ms(atlasgpu_ctx *ctx, const char *name);
 /* Algorithmic work units counted by the last timed launch of a kernel
  * family while timing is enabled, or -1: "synthe_voigt_evals" (SYNTHE core
  * Voigt evaluations), "synthe_farwing_updates" (far-wing bin updates),
- * "atlas_linop_points" (LINOP1 wing points added into XLINES), and the
- * batched iteration's "batch_linop_points".  No reference counterpart:
- * these are the numerators of the kernels' rooflines. */
+ * "atlas_linop_points" (LINOP1 wing points added into XLINES), the batched
+ * iteration's "batch_linop_points" and "batch_linop_atomics" (the atomics
+ * its exact sums issue, counted by a pass that walks without adding), the batched
+ * RT solve stage's "batch_rt_eliminated", "batch_rt_series" (systems solved
+ * each way) and "batch_rt_series_steps".  No reference counterpart: these
+ * are the numerators of the kernels' rooflines. */
 double atlasgpu_kernel_work(atlasgpu_ctx *ctx, const char *name);
 
 /* JOSH operator set: BLOCKJ/BLOCKH matrices (atlas12_modules.f90:18792-18860)
@@ -634,6 +637,12 @@ int atlasgpu_mlp_train(atlasgpu_ctx *ctx, atlasgpu_mlp *p, const float *x, const
  * the denominator of the FP64-pipe roofline of the transfer kernels.  No
  * reference counterpart.  Returns a negative value on failure. */
 double atlasgpu_fp64_peak_tflops(atlasgpu_ctx *ctx);
+
+/* Measured rate of 64-bit integer atomic adds at L2 (billions per second),
+ * warps adding to 32 consecutive words at scattered places of a 64 MB
+ * region, the access pattern of LINOP1's exact XLINES sums: the denominator
+ * of LINOP1's roofline.  No reference counterpart.  Negative on failure. */
+double atlasgpu_u64_atomic_peak(atlasgpu_ctx *ctx);
 
 /* The surrogate physics on the device for given T, P [nrhox]: continuum
  * absorption and scattering kabs, sigma [nw][nrhox] at wave [nw] (nm),

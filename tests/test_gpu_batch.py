@@ -142,3 +142,37 @@ def test_batch_runs_are_bit_identical(gpu_ctx, tables, small_grid):
     for a, c in zip(r1, r2):
         for k in ("t", "p", "rhox", "flxerr", "hist"):
             assert np.array_equal(np.asarray(a[k]).view(np.uint64), np.asarray(c[k]).view(np.uint64)), k
+
+
+def test_timed_iteration_counts_without_changing_results(gpu_ctx, tables, small_grid):
+    """A timed iteration also runs LINOP1's counting pass (the same walks,
+    counting the atomics the exact sums issue, adding nothing): the counts are
+    consistent (1-3 atomics per wing point) and the models' structure is the
+    same bits as an untimed iteration's."""
+    ws, rc, lines = small_grid
+    starts = [_start(teff, logg, mh) for teff, logg, mh, _ in PARAMS]
+    out = []
+    for timed in (False, True):
+        b = atlas.AtlasBatch(gpu_ctx, tables, nslots=3, linedata=lines, waveset=ws, rcoset=rc, shape=None)
+        for s, (teff, logg, mh, vt) in enumerate(PARAMS):
+            b.load(s, teff, logg, vt, mh, starts[s], max_iter=4, tol_percent=0.0)
+        b.step(1)
+        gpu_ctx.enable_timing(timed)
+        b.step(1)
+        if timed:
+            pts = gpu_ctx.kernel_work("batch_linop_points")
+            atoms = gpu_ctx.kernel_work("batch_linop_atomics")
+            assert pts > 0 and pts <= atoms <= 3 * pts, (pts, atoms)
+        gpu_ctx.enable_timing(False)
+        b.step(2)
+        out.append([b.structure(s) for s in range(3)])
+        b.close()
+    for a, c in zip(*out):
+        for k in ("t", "p", "rhox", "flxerr"):
+            assert np.array_equal(np.asarray(a[k]).view(np.uint64), np.asarray(c[k]).view(np.uint64)), k
+
+
+def test_atomic_peak_probe(gpu_ctx):
+    """The denominator of LINOP1's roofline: a positive rate of 64-bit atomics."""
+    rate = float(_lib.lib().atlasgpu_u64_atomic_peak(gpu_ctx.handle))
+    assert rate > 10.0, rate  # billions per second
