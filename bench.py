@@ -74,8 +74,9 @@ FLOPS_PER_SERIES_STEP = 2 * 51 ** 2 + 3 * 51
 # written and read back, the partial sums
 RT_TRAFFIC_PER_MODEL = 221e6
 # DRAM bytes per model of one batched LINOP1 launch (ncu, 4-slot capture of
-# this workload): the prepared line records and the fixed-point XLINES words
-LINOP_TRAFFIC_PER_MODEL = 60.4e6
+# this workload: 959 MB): the prepared line records and the fixed-point XLINES
+# words, whose write-backs dominate once several models' words exceed L2
+LINOP_TRAFFIC_PER_MODEL = 240e6
 # bytes of one prepared LINOP1 line record on the device (AtlasLine)
 LINE_RECORD_BYTES = 56
 # FP64 operations of one SYNTHE Weideman Voigt evaluation (31 complex Horner
