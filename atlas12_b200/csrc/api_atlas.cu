@@ -157,6 +157,8 @@ int rt_launch(atlasgpu_ctx* ctx, RtArgs& a, double* d_sum, int* nwarps_out) {
     Timer tm(ctx, "atlas_rt");
     k_rt_pre<<<sh.pre_blocks, kRtSplitWarps * 32, rt_pre_smem_bytes(), ctx->stream>>>(a);
     CKL(ctx);
+    k_rt_series<<<sh.solve_blocks, kRtSolveThreads, 0, ctx->stream>>>(a);
+    CKL(ctx);
     k_rt_solve<<<sh.solve_blocks, kRtSolveThreads, rt_solve_smem_bytes(), ctx->stream>>>(a);
     CKL(ctx);
     k_rt_post<<<sh.post_blocks, kRtSplitWarps * 32, rt_post_smem_bytes(a.nrhox), ctx->stream>>>(a);

@@ -124,6 +124,15 @@ __global__ void __launch_bounds__(kRtSolveThreads, kRtSolveMinBlocks) k_batch_rt
   a.work = work;
   rt_solve_body(a);
 }
+__global__ void __launch_bounds__(kRtSolveThreads, kRtSeriesMinBlocks) k_batch_rt_series(const RtArgs* __restrict__ args,
+                                                                                      const BatchCtl* ctl,
+                                                                                      unsigned long long* work) {
+  const int b = blockIdx.y;
+  if (!running(ctl, b)) return;
+  RtArgs a = args[b];
+  a.work = work;
+  rt_series_body(a);
+}
 __global__ void __launch_bounds__(kRtSplitWarps * 32, 4) k_batch_rt_post(const RtArgs* __restrict__ args,
                                                                         const BatchCtl* ctl) {
   const int b = blockIdx.y;
@@ -265,6 +274,8 @@ int enqueue_batch(atlasgpu_ctx* ctx, atlasgpu_batch* B, bool timed) {
       unsigned long long* work = work_counters(ctx, 3);
       {
         Timer t2(ctx, "batch_rt_solve");
+        k_batch_rt_series<<<dim3(sh.solve_blocks, nb), kRtSolveThreads, 0, s>>>(B->ra, B->d.ctl, work);
+        CKL(ctx);
         k_batch_rt_solve<<<dim3(sh.solve_blocks, nb), kRtSolveThreads, rt_solve_smem_bytes(), s>>>(B->ra,
                                                                                                  B->d.ctl, work);
         CKL(ctx);

@@ -173,6 +173,8 @@ int enqueue_begin(atlasgpu_ctx* ctx, atlasgpu_model* m, bool timed) {
     Timer tm(ctx, "atlas_rt");
     k_rt_pre<<<sh.pre_blocks, kRtSplitWarps * 32, rt_pre_smem_bytes(), s>>>(ra);
     CKL(ctx);
+    k_rt_series<<<sh.solve_blocks, kRtSolveThreads, 0, s>>>(ra);
+    CKL(ctx);
     k_rt_solve<<<sh.solve_blocks, kRtSolveThreads, rt_solve_smem_bytes(), s>>>(ra);
     CKL(ctx);
     k_rt_post<<<sh.post_blocks, kRtSplitWarps * 32, rt_post_smem_bytes(m->nrhox), s>>>(ra);

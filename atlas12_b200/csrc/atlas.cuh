@@ -959,7 +959,7 @@ struct RtPreWS {
 };
 struct RtSolveWS {
   double xs[kNx], xsbar[kNx], xalpha[kNx], piv[kNx];
-  double rowabs[kNx], xb[kNx];  // row sums of |COEFJ|; the series' second buffer
+  double rowabs[kNx];  // row sums of |COEFJ| (the contraction bound's factors)
   double red[8];
   unsigned pk[4][3];
   alignas(16) double U[kNx * (kNx + 1)];
@@ -1049,9 +1049,10 @@ static __device__ __forceinline__ void rt_pre_body(const RtArgs& a) {
 // leave an error of at most q^(K+1) |X|, and K is taken so that
 // q^(K+1) <= 2^-60, far below the rounding of the elimination itself (the
 // two solutions agree to rounding).  A step is one matrix-vector product
-// with no sequential dependence between rows: about 1/20 of the
-// elimination's latency, so the series is cheaper up to q ~ 0.5.  Systems
-// with larger q (strongly scattering layers) are eliminated as SOLVIT does.
+// with no sequential dependence between rows and one barrier, against the
+// elimination's 50 dependent pivot steps, so the series is cheaper up to
+// q ~ 0.5.  Systems with larger q (strongly scattering layers) are
+// eliminated as SOLVIT does.
 constexpr double kRtSeriesQ = 0.5;
 constexpr int kRtSeriesMaxSteps = 64;
 
@@ -1059,42 +1060,6 @@ __device__ __forceinline__ int rt_series_steps(double q) {
   if (!(q > 0.0)) return 1;
   const int k = (int)ceil(-60.0 * 0.6931471805599453 / log(q)) - 1;
   return k < 1 ? 1 : (k > kRtSeriesMaxSteps ? kRtSeriesMaxSteps : k);
-}
-
-// K series steps by a pair group, thread l < 51 owning X(l); two buffers in
-// shared memory (one barrier per step).  Result in ws.xs.
-template <class G>
-__device__ __forceinline__ void rt_solve_series(G& g, const JoshOps& ops, RtSolveWS& S, int K) {
-  const int l = g.r;
-  const bool own = l < kNx;
-  const double al = own ? S.xalpha[l] : 0.0;
-  const double b = own ? (1.0 - al) * S.xsbar[l] : 0.0;
-  double* cur = S.xs;
-  double* nxt = S.xb;
-  if (own) cur[l] = b;
-  for (int k = 0; k < K; ++k) {
-    g.sync();
-    if (own) {
-      double s4[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 3
-      for (int m0 = 0; m0 < kNx - kNx % 4; m0 += 4) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) s4[q] = s4[q] + ops.coefj[(m0 + q) * kNx + l] * cur[m0 + q];
-      }
-#pragma unroll
-      for (int q = 0; q < kNx % 4; ++q) {
-        const int m = kNx - kNx % 4 + q;
-        s4[q] = s4[q] + ops.coefj[m * kNx + l] * cur[m];
-      }
-      nxt[l] = b + al * ((s4[0] + s4[1]) + (s4[2] + s4[3]));
-    }
-    double* t = cur;
-    cur = nxt;
-    nxt = t;
-  }
-  g.sync();
-  if (own && cur != S.xs) S.xs[l] = cur[l];
-  g.sync();
 }
 
 static __device__ __forceinline__ void rt_solve_body(const RtArgs& a) {
@@ -1127,21 +1092,86 @@ static __device__ __forceinline__ void rt_solve_body(const RtArgs& a) {
         qv = fmax(qv, xa * S.rowabs[l]);
       }
       const double q = g.max(qv);  // (its barrier also publishes XALPHA, XSBAR)
-      if (q <= kRtSeriesQ) {
-        const int K = rt_series_steps(q);
-        rt_solve_series(g, ops, S, K);
-        ++nseries;
-        nsteps += K;
-      } else {
-        solve_scatter(g, ops, S, S.U);
-        ++nelim;
-      }
+      if (q <= kRtSeriesQ) continue;  // summed by k_rt_series
+      solve_scatter(g, ops, S, S.U);
+      ++nelim;
     }
     for (int l = g.r; l < kNx; l += PairG::N) rec[R.xs() + l] = S.xs[l];
     g.sync();
   }
   if (a.work && g.r == 0 && (nelim | nseries)) {
     atomicAdd(a.work, nelim);
+    atomicAdd(a.work + 1, nseries);
+    atomicAdd(a.work + 2, nsteps);
+  }
+}
+
+// The Neumann series of the systems with q <= kRtSeriesQ, by their own
+// kernel (k_rt_series; k_rt_solve eliminates the rest): thread l of a pair
+// group keeps row l of COEFJ in registers for the whole launch (it is the
+// same for every frequency), so a step is 51 FMAs on registers and the
+// broadcast reads of X from shared memory, with no loads of COEFJ.  Sum k of
+// the four partial sums takes the terms m = k, k+4, ... in that order; q is
+// formed as in rt_solve_body, so the two kernels split the systems the same
+// way.  (The series inside k_rt_solve, reading COEFJ from L1 every step,
+// took 2.6k cycles per step at eight groups per SM.)
+constexpr int kRtSeriesMinBlocks = 3;
+struct RtSeriesWS {
+  alignas(16) double xa[kNx + 1];
+  alignas(16) double xb[kNx + 1];
+  double red[8];
+};
+
+static __device__ __forceinline__ void rt_series_body(const RtArgs& a) {
+  __shared__ RtSeriesWS s_ws[kRtSolveGroups];
+  const int gid = threadIdx.x / PairG::N;
+  RtSeriesWS& S = s_ws[gid];
+  PairG g(threadIdx.x % PairG::N, 1 + gid, S.red);
+  const JoshOps& ops = *a.ops;
+  const int kw = a.kw, l = g.r;
+  const bool own = l < kNx;
+  double c[kNx];
+  double rowabs = 0.0;
+#pragma unroll
+  for (int m = 0; m < kNx; ++m) c[m] = own ? ops.coefj[m * kNx + l] : 0.0;
+  for (int m = 0; m < kNx; ++m) rowabs += fabs(own ? ops.coefj[m * kNx + l] : 0.0);
+  const int grp = blockIdx.x * kRtSolveGroups + gid;
+  const int nu0 = a.nu_first + grp * a.nu_per_solve;
+  const int nu1 = min(nu0 + a.nu_per_solve - 1, a.nu_last > 0 ? a.nu_last : a.numnu);
+  unsigned long long nseries = 0, nsteps = 0;
+  const RtRec R{kw};
+  for (int nu = nu0; nu <= nu1; ++nu) {
+    double* rec = rt_rec(a, nu);
+    if (rec[R.solve()] == 0.0) continue;  // the same word for the whole group
+    const double al = own ? rec[R.xalpha() + l] : 0.0;
+    const double xb = own ? rec[R.xsbar() + l] : 0.0;
+    double qv = 0.0;
+    if (own) qv = fmax(qv, al * rowabs);
+    const double q = g.max(qv);
+    if (q > kRtSeriesQ) continue;  // eliminated by k_rt_solve
+    const int K = rt_series_steps(q);
+    const double b = own ? (1.0 - al) * xb : 0.0;
+    double* cur = S.xa;
+    double* nxt = S.xb;
+    if (own) cur[l] = b;
+    for (int k = 0; k < K; ++k) {
+      g.sync();
+      if (own) {
+        double s4[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int m = 0; m < kNx; ++m) s4[m & 3] = s4[m & 3] + c[m] * cur[m];
+        nxt[l] = b + al * ((s4[0] + s4[1]) + (s4[2] + s4[3]));
+      }
+      double* t = cur;
+      cur = nxt;
+      nxt = t;
+    }
+    g.sync();
+    if (own) rec[R.xs() + l] = cur[l];
+    ++nseries;
+    nsteps += K;
+  }
+  if (a.work && g.r == 0 && nseries) {
     atomicAdd(a.work + 1, nseries);
     atomicAdd(a.work + 2, nsteps);
   }
@@ -1213,6 +1243,7 @@ static __device__ __forceinline__ void rt_post_body(const RtArgs& a) {
 
 static __global__ void __launch_bounds__(kRtSplitWarps * 32, 6) k_rt_pre(RtArgs a) { rt_pre_body(a); }
 static __global__ void __launch_bounds__(kRtSolveThreads, kRtSolveMinBlocks) k_rt_solve(RtArgs a) { rt_solve_body(a); }
+static __global__ void __launch_bounds__(kRtSolveThreads, kRtSeriesMinBlocks) k_rt_series(RtArgs a) { rt_series_body(a); }
 static __global__ void __launch_bounds__(kRtSplitWarps * 32, 4) k_rt_post(RtArgs a) { rt_post_body(a); }
 
 // Launch shape of the split pass over LEN frequencies with 1/NB of the GPU
