@@ -89,6 +89,7 @@ SIGNATURES = {
     "atlasgpu_atlas_set_hydrogen_tables": (_I, [_P, _P]),
     "atlasgpu_atlas_set_kapp_tables": (_I, [_P, _P]),
     "atlasgpu_atlas_kapp_hydrogen": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "atlasgpu_atlas_kapp": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _P]),
     "atlasgpu_atlas_rt_pass": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _D,
                                     ctypes.POINTER(Accum), _P]),
     "atlasgpu_atlas_finish": (_I, [_P, ctypes.c_void_p, ctypes.POINTER(Accum), ctypes.POINTER(_D)]),
@@ -169,13 +170,19 @@ class HydrogenTables(ctypes.Structure):
 class KappTables(ctypes.Structure):
     """atlasgpu_kapp_tables (include/atlasgpu.h): KAPP's hydrogen continuum
     tables (Karzas-Latter, van Hoof g_ff, Holtsmark Q, HOP's level energies,
-    HMINOP's, H2PLOP's and HRAYOP's tables)."""
+    HMINOP's, H2PLOP's and HRAYOP's tables) and the helium ones (HE1OP's
+    levels, CROSSHE, the 2s/2p fits, HEMIOP's table)."""
     _F = ctypes.c_float
     _fields_ = [("freqn", _F * 435), ("xn", _F * 435), ("xl", _F * 1044), ("ekarzas", _F * 29),
                 ("gff", _D * 11826), ("q_holtsmark", _D * 150), ("hop_elev", _D * 15), ("hmin_wbf", _D * 116),
                 ("hmin_bf", _D * 116), ("hmin_thetaff", _D * 11), ("hmin_wavek", _D * 22), ("hmin_ff", _D * 242),
                 ("h2p_fr", _D * 5), ("h2p_es", _D * 6), ("ray_m", _D * 74), ("ray_ab", _D * 27), ("ray_bc", _D * 24),
-                ("ray_cd", _D * 22), ("ray_ly", _D * 64), ("ray_fly", _D * 64)]
+                ("ray_cd", _D * 22), ("ray_ly", _D * 64), ("ray_fly", _D * 64),
+                ("he1_chi", _D * 10), ("he1_freq", _D * 10), ("he1_g", _D * 10), ("he_x505", _D * 92),
+                ("he_x50", _D * 16), ("he_x20", _D * 11), ("he_x10", _D * 21)] + \
+        [(k, _D * 16) for k in ("he2s1s_f", "he2s1s_x", "he2s3s_f", "he2s3s_x", "he2p1p_f", "he2p1p_x",
+                                "he2p3p_f", "he2p3p_x")] + \
+        [("hem_w", _D * 17), ("hem_t", _D * 12), ("hem_k", _D * 204)]
 
     @classmethod
     def from_tables(cls, t):
@@ -189,6 +196,12 @@ class KappTables(ctypes.Structure):
                 raise ValueError(f"kapp table {name}: {v.size} values, expected {len(arr)}")
             arr[:] = [float(x) for x in v]
         return k
+
+
+class KappPops(ctypes.Structure):
+    """atlasgpu_kapp_pops: the depth vectors of atlasgpu_atlas_kapp (addresses)."""
+    _fields_ = [(k, ctypes.c_void_p) for k in ("t", "xne", "rho", "xnfp_h1", "xnfp_h2", "xnfp_he1", "xnfp_he2",
+                                               "xnfp_he3", "xnf_he2", "bhyd", "bmin")]
 
 
 class StehleSeries(ctypes.Structure):

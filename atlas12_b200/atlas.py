@@ -115,6 +115,29 @@ class Atlas:
                       ptr(bm), *[ptr(o) for o in out], ptr(pt))
         return (*out, pt) if parts else tuple(out)
 
+    def kapp(self, waveset, t, xne, rho, xnfp1, xnfp2, xnfp3, xnfp4, xnfp5, xnf4, bhyd=None, bmin=None, kw=None,
+             parts=False):
+        """KAPP with the hydrogen sources of kapp_hydrogen and the helium ones
+        (HE1OP, HE2OP, HEMIOP, HERAOP): (acont, sigmac, scont) [numnu, kw], and
+        with parts=True also [numnu, 11, kw] (AHYD, SHYD, AH2P, AHMIN, SHMIN,
+        SIGH, SIGEL, AHE1, AHE2, AHEMIN, SIGHE).  xnfp1..5 = XNFP(J,1..5),
+        xnf4 = XNF(J,4) (He II number density), each [nrhox]."""
+        ws = np.ascontiguousarray(waveset, np.float64)
+        vec = [np.ascontiguousarray(v, np.float64) for v in (t, xne, rho, xnfp1, xnfp2, xnfp3, xnfp4, xnfp5, xnf4)]
+        nrhox = vec[0].size
+        kw = nrhox if kw is None else int(kw)
+        bh = None if bhyd is None else np.ascontiguousarray(bhyd, np.float64)
+        if bh is not None and bh.shape != (6, kw):
+            raise ValueError("bhyd must be [6, kw]")
+        bm = None if bmin is None else np.ascontiguousarray(bmin, np.float64)
+        pops = _lib.KappPops(*[v.ctypes.data for v in vec], None if bh is None else bh.ctypes.data,
+                             None if bm is None else bm.ctypes.data)
+        out = [np.zeros((ws.size, kw)) for _ in range(3)]
+        pt = np.zeros((ws.size, 11, kw)) if parts else None
+        self.ctx.call("atlasgpu_atlas_kapp", ws.size, ptr(ws), nrhox, kw, ctypes.byref(pops),
+                      *[ptr(o) for o in out], ptr(pt))
+        return (*out, pt) if parts else tuple(out)
+
     def xlinop(self, records, nrhox, xnfdop, dopple, xne, txnxn, hckt, tabcont, iwt, waveset, contx, xlines=None,
                xnfp=None, rho=None, hydrogen=None):
         """XLINOP on unit-19 records (NLTE_LINE array, sorted by wavelength),

@@ -1,6 +1,6 @@
-// api_kapp.cu -- C-ABI entry points of KAPP's hydrogen continuum sources
-// (atlas12_modules.f90:11202-11324 with HOP, H2PLOP, HMINOP, HRAYOP, ELECOP;
-// kernels in kapp.cuh).
+// api_kapp.cu -- C-ABI entry points of KAPP's hydrogen and helium continuum
+// sources (atlas12_modules.f90:11202-11324 with HOP, H2PLOP, HMINOP, HRAYOP,
+// ELECOP, HE1OP, HE2OP, HEMIOP, HERAOP; kernels in kapp.cuh).
 #include <cmath>
 #include <vector>
 
@@ -35,8 +35,22 @@ int atlasgpu_atlas_set_kapp_tables(atlasgpu_ctx* ctx, const atlasgpu_kapp_tables
       !finite_all(t->hmin_thetaff, 11) || !finite_all(t->hmin_wavek, 22) || !finite_all(&t->hmin_ff[0][0], 242) ||
       !finite_all(t->h2p_fr, 5) || !finite_all(t->h2p_es, 6) || !finite_all(t->ray_m, 74) ||
       !finite_all(t->ray_ab, 27) || !finite_all(t->ray_bc, 24) || !finite_all(t->ray_cd, 22) ||
-      !finite_all(t->ray_ly, 64) || !finite_all(t->ray_fly, 64))
+      !finite_all(t->ray_ly, 64) || !finite_all(t->ray_fly, 64) || !finite_all(t->he1_chi, 10) ||
+      !finite_all(t->he1_freq, 10) || !finite_all(t->he1_g, 10) || !finite_all(t->he_x505, 92) ||
+      !finite_all(t->he_x50, 16) || !finite_all(t->he_x20, 11) || !finite_all(t->he_x10, 21) ||
+      !finite_all(t->he2s1s_f, 16) || !finite_all(t->he2s1s_x, 16) || !finite_all(t->he2s3s_f, 16) ||
+      !finite_all(t->he2s3s_x, 16) || !finite_all(t->he2p1p_f, 16) || !finite_all(t->he2p1p_x, 16) ||
+      !finite_all(t->he2p3p_f, 16) || !finite_all(t->he2p3p_x, 16) || !finite_all(t->hem_w, 17) ||
+      !finite_all(t->hem_t, 12) || !finite_all(&t->hem_k[0][0], 12 * 17))
     return fail(ctx, ATLASGPU_ENONFINITE, "set_kapp_tables: non-finite table entry");
+  for (int i = 0; i < 12 * 17; ++i)
+    if (!((&t->hem_k[0][0])[i] > 0.0)) return fail(ctx, ATLASGPU_EINVAL, "set_kapp_tables: KHEM entry not positive");
+  for (int i = 0; i < 17; ++i)
+    if (!(t->hem_w[i] > 0.0) || (i > 0 && !(t->hem_w[i] > t->hem_w[i - 1])))
+      return fail(ctx, ATLASGPU_EINVAL, "set_kapp_tables: WHEM not positive and increasing");
+  for (int i = 0; i < 12; ++i)
+    if (!(t->hem_t[i] > 0.0) || (i > 0 && !(t->hem_t[i] > t->hem_t[i - 1])))
+      return fail(ctx, ATLASGPU_EINVAL, "set_kapp_tables: THEM not positive and increasing");
   for (int i = 0; i < 146 * 81; ++i)
     if (!((&t->gff[0][0])[i] > 0.0)) return fail(ctx, ATLASGPU_EINVAL, "set_kapp_tables: g_ff entry not positive");
   for (int i = 0; i < 242; ++i)
@@ -71,6 +85,23 @@ int atlasgpu_atlas_set_kapp_tables(atlasgpu_ctx* ctx, const atlasgpu_kapp_tables
   std::copy(t->ray_ly, t->ray_ly + 64, k.ray_ly);
   std::copy(t->ray_fly, t->ray_fly + 64, k.ray_fly);
   std::copy(kSeriesLimits, kSeriesLimits + 15, k.series_limits);
+  std::copy(t->he1_chi, t->he1_chi + 10, k.he1_chi);
+  std::copy(t->he1_freq, t->he1_freq + 10, k.he1_freq);
+  std::copy(t->he1_g, t->he1_g + 10, k.he1_g);
+  std::copy(t->he_x505, t->he_x505 + 92, k.he_x505);
+  std::copy(t->he_x50, t->he_x50 + 16, k.he_x50);
+  std::copy(t->he_x20, t->he_x20 + 11, k.he_x20);
+  std::copy(t->he_x10, t->he_x10 + 21, k.he_x10);
+  const double* knots[8] = {t->he2s1s_f, t->he2s1s_x, t->he2s3s_f, t->he2s3s_x,
+                            t->he2p1p_f, t->he2p1p_x, t->he2p3p_f, t->he2p3p_x};
+  double* kd[8] = {k.he2s1s_f, k.he2s1s_x, k.he2s3s_f, k.he2s3s_x, k.he2p1p_f, k.he2p1p_x, k.he2p3p_f, k.he2p3p_x};
+  for (int q = 0; q < 8; ++q) std::copy(knots[q], knots[q] + 16, kd[q]);
+  // HEMIOP's first call (:13788-13798): LOGW, LOGT, LOGK = log of the table
+  std::copy(t->hem_w, t->hem_w + 17, k.hem_w);
+  std::copy(t->hem_t, t->hem_t + 12, k.hem_t);
+  for (int i = 0; i < 17; ++i) k.hem_logw[i] = std::log(t->hem_w[i]);
+  for (int i = 0; i < 12; ++i) k.hem_logt[i] = std::log(t->hem_t[i]);
+  for (int i = 0; i < 12 * 17; ++i) k.hem_logk[i] = std::log((&t->hem_k[0][0])[i]);
   cudaSetDevice(ctx->device);
   KappDev* d;
   int r;
@@ -81,47 +112,61 @@ int atlasgpu_atlas_set_kapp_tables(atlasgpu_ctx* ctx, const atlasgpu_kapp_tables
   return 0;
 }
 
-int atlasgpu_atlas_kapp_hydrogen(atlasgpu_ctx* ctx, int numnu, const double* waveset, int nrhox, int kw,
-                                 const double* t, const double* xne, const double* rho, const double* xnfp1,
-                                 const double* xnfp2, const double* bhyd, const double* bmin, double* acont,
-                                 double* sigmac, double* scont, double* parts) {
+}  // extern "C"
+
+namespace {
+
+// both entry points: validate, stage the depth vectors, launch the two
+// kernels, copy the totals (and the per-source parts) back
+int kapp_run(atlasgpu_ctx* ctx, const char* name, int numnu, const double* waveset, int nrhox, int kw,
+             const atlasgpu_kapp_pops& pp, bool helium, double* acont, double* sigmac, double* scont, double* parts) {
   if (!ctx) return ATLASGPU_EINVAL;
-  if (!ctx->kapp_set) return fail(ctx, ATLASGPU_ESTATE, "kapp_hydrogen: tables not set");
-  if (numnu < 1 || nrhox < 1 || kw < nrhox || !waveset || !t || !xne || !rho || !xnfp1 || !xnfp2 || !acont ||
-      !sigmac || !scont)
-    return fail(ctx, ATLASGPU_EINVAL, "kapp_hydrogen: bad argument (numnu %d, nrhox %d, kw %d)", numnu, nrhox, kw);
+  if (!ctx->kapp_set) return fail(ctx, ATLASGPU_ESTATE, "%s: tables not set", name);
+  if (numnu < 1 || nrhox < 1 || kw < nrhox || !waveset || !pp.t || !pp.xne || !pp.rho || !pp.xnfp_h1 ||
+      !pp.xnfp_h2 || !acont || !sigmac || !scont ||
+      (helium && (!pp.xnfp_he1 || !pp.xnfp_he2 || !pp.xnfp_he3 || !pp.xnf_he2)))
+    return fail(ctx, ATLASGPU_EINVAL, "%s: bad argument (numnu %d, nrhox %d, kw %d)", name, numnu, nrhox, kw);
   for (int i = 0; i < numnu; ++i)
     if (!(waveset[i] > 0.0) || !std::isfinite(waveset[i]))
-      return fail(ctx, ATLASGPU_EINVAL, "kapp_hydrogen: WAVESET(%d) = %g", i + 1, waveset[i]);
-  if (!finite_all(t, nrhox) || !finite_all(xne, nrhox) || !finite_all(rho, nrhox) || !finite_all(xnfp1, nrhox) ||
-      !finite_all(xnfp2, nrhox) || (bmin && !finite_all(bmin, nrhox)))
-    return fail(ctx, ATLASGPU_ENONFINITE, "kapp_hydrogen: non-finite depth vector");
+      return fail(ctx, ATLASGPU_EINVAL, "%s: WAVESET(%d) = %g", name, i + 1, waveset[i]);
+  if (!finite_all(pp.t, nrhox) || !finite_all(pp.xne, nrhox) || !finite_all(pp.rho, nrhox) ||
+      !finite_all(pp.xnfp_h1, nrhox) || !finite_all(pp.xnfp_h2, nrhox) || (pp.bmin && !finite_all(pp.bmin, nrhox)) ||
+      (helium && (!finite_all(pp.xnfp_he1, nrhox) || !finite_all(pp.xnfp_he2, nrhox) ||
+                  !finite_all(pp.xnfp_he3, nrhox) || !finite_all(pp.xnf_he2, nrhox))))
+    return fail(ctx, ATLASGPU_ENONFINITE, "%s: non-finite depth vector", name);
   for (int j = 0; j < nrhox; ++j)
-    if (!(t[j] > 0.0) || !(rho[j] > 0.0))
-      return fail(ctx, ATLASGPU_EINVAL, "kapp_hydrogen: T or RHO not positive at depth %d", j + 1);
-  if (bhyd)
+    if (!(pp.t[j] > 0.0) || !(pp.rho[j] > 0.0))
+      return fail(ctx, ATLASGPU_EINVAL, "%s: T or RHO not positive at depth %d", name, j + 1);
+  if (pp.bhyd)
     for (int n = 0; n < 6; ++n)
-      if (!finite_all(bhyd + (size_t)n * kw, nrhox))
-        return fail(ctx, ATLASGPU_ENONFINITE, "kapp_hydrogen: non-finite BHYD");
+      if (!finite_all(pp.bhyd + (size_t)n * kw, nrhox)) return fail(ctx, ATLASGPU_ENONFINITE, "%s: non-finite BHYD", name);
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
   const size_t nt = (size_t)numnu * kw;
+  const int nparts = helium ? 11 : 7;
   double *d_ws, *d_in, *d_dep, *d_out, *d_parts = nullptr;
   int r;
-  // inputs: T, XNE, RHO, XNFP1, XNFP2, BMIN [kw] and BHYD [6][kw]
-  if ((r = bufT(ctx, "kp_ws", numnu, &d_ws)) || (r = bufT(ctx, "kp_in", (size_t)12 * kw, &d_in)) ||
-      (r = bufT(ctx, "kp_dep", (size_t)(6 + 2 * kHLev + 9) * kw, &d_dep)) ||
-      (r = bufT(ctx, "kp_out", 3 * nt, &d_out)) || (parts && (r = bufT(ctx, "kp_parts", 7 * nt, &d_parts))))
+  // inputs: T, XNE, RHO, XNFP1, XNFP2, BMIN [kw], BHYD [6][kw], XNFP3..5, XNF4 [kw]
+  const size_t ndep = (size_t)(6 + 2 * kHLev + 9 + 10 + 24 + 3) * kw;
+  if ((r = bufT(ctx, "kp_ws", numnu, &d_ws)) || (r = bufT(ctx, "kp_in", (size_t)16 * kw, &d_in)) ||
+      (r = bufT(ctx, "kp_dep", ndep, &d_dep)) || (r = bufT(ctx, "kp_out", 3 * nt, &d_out)) ||
+      (parts && (r = bufT(ctx, "kp_parts", (size_t)nparts * nt, &d_parts))))
     return r;
-  CK(cudaMemsetAsync(d_in, 0, (size_t)12 * kw * sizeof(double), s));
+  CK(cudaMemsetAsync(d_in, 0, (size_t)16 * kw * sizeof(double), s));
   CK(cudaMemcpyAsync(d_ws, waveset, numnu * sizeof(double), cudaMemcpyHostToDevice, s));
-  const double* src[5] = {t, xne, rho, xnfp1, xnfp2};
+  const double* src[5] = {pp.t, pp.xne, pp.rho, pp.xnfp_h1, pp.xnfp_h2};
   for (int q = 0; q < 5; ++q)
     CK(cudaMemcpyAsync(d_in + (size_t)q * kw, src[q], nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
-  if (bmin) CK(cudaMemcpyAsync(d_in + (size_t)5 * kw, bmin, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
-  if (bhyd) CK(cudaMemcpyAsync(d_in + (size_t)6 * kw, bhyd, (size_t)6 * kw * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (pp.bmin) CK(cudaMemcpyAsync(d_in + (size_t)5 * kw, pp.bmin, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (pp.bhyd)
+    CK(cudaMemcpyAsync(d_in + (size_t)6 * kw, pp.bhyd, (size_t)6 * kw * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (helium) {
+    const double* hsrc[4] = {pp.xnfp_he1, pp.xnfp_he2, pp.xnfp_he3, pp.xnf_he2};
+    for (int q = 0; q < 4; ++q)
+      CK(cudaMemcpyAsync(d_in + (size_t)(12 + q) * kw, hsrc[q], nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  }
   CK(cudaMemsetAsync(d_out, 0, 3 * nt * sizeof(double), s));
-  if (d_parts) CK(cudaMemsetAsync(d_parts, 0, 7 * nt * sizeof(double), s));
+  if (d_parts) CK(cudaMemsetAsync(d_parts, 0, (size_t)nparts * nt * sizeof(double), s));
   KappArgs a{};
   a.tb = (const KappDev*)ctx->bufs["kapp_tab"].first;
   a.numnu = numnu;
@@ -133,8 +178,14 @@ int atlasgpu_atlas_kapp_hydrogen(atlasgpu_ctx* ctx, int numnu, const double* wav
   a.rho = d_in + 2 * kw;
   a.xnfp1 = d_in + 3 * kw;
   a.xnfp2 = d_in + 4 * kw;
-  a.bmin = bmin ? d_in + 5 * kw : nullptr;
-  a.bhyd = bhyd ? d_in + 6 * kw : nullptr;
+  a.bmin = pp.bmin ? d_in + 5 * kw : nullptr;
+  a.bhyd = pp.bhyd ? d_in + 6 * kw : nullptr;
+  if (helium) {
+    a.xnfp3 = d_in + 12 * kw;
+    a.xnfp4 = d_in + 13 * kw;
+    a.xnfp5 = d_in + 14 * kw;
+    a.xnf4 = d_in + 15 * kw;
+  }
   double* p = d_dep;
   double** dv[6] = {&a.d.hkt, &a.d.hckt, &a.d.tkev, &a.d.tlog, &a.d.theta, &a.d.xhmin};
   for (int q = 0; q < 6; ++q) {
@@ -146,24 +197,61 @@ int atlasgpu_atlas_kapp_hydrogen(atlasgpu_ctx* ctx, int numnu, const double* wav
   a.d.bz = p;
   p += (size_t)kHLev * kw;
   a.d.bp = p;
+  p += (size_t)9 * kw;
+  a.d.he_bolt = p;
+  p += (size_t)10 * kw;
+  a.d.he_boltn = p;
+  p += (size_t)24 * kw;
+  a.d.he_freet = p;
+  a.d.he_boltex = p + kw;
+  a.d.he_exlim = p + 2 * kw;
   a.acont = d_out;
   a.sigmac = d_out + nt;
   a.scont = d_out + 2 * nt;
   a.parts = d_parts;
+  a.nparts = nparts;
   {
-    Timer tm(ctx, "kapp_hydrogen");
+    Timer tm(ctx, name);
     k_kapp_depth<<<(nrhox + 127) / 128, 128, 0, s>>>(a);
     CKL(ctx);
     const int blocks = std::min((numnu + kKappWarps - 1) / kKappWarps, ctx->nsm * 8);
-    k_kapp_nu<<<blocks, kKappWarps * 32, 0, s>>>(a);
+    if (helium)
+      k_kapp_nu<true><<<blocks, kKappWarps * 32, 0, s>>>(a);
+    else
+      k_kapp_nu<false><<<blocks, kKappWarps * 32, 0, s>>>(a);
     CKL(ctx);
   }
   CK(cudaMemcpyAsync(acont, a.acont, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(sigmac, a.sigmac, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(scont, a.scont, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
-  if (parts) CK(cudaMemcpyAsync(parts, d_parts, 7 * nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (parts) CK(cudaMemcpyAsync(parts, d_parts, (size_t)nparts * nt * sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int atlasgpu_atlas_kapp_hydrogen(atlasgpu_ctx* ctx, int numnu, const double* waveset, int nrhox, int kw,
+                                 const double* t, const double* xne, const double* rho, const double* xnfp1,
+                                 const double* xnfp2, const double* bhyd, const double* bmin, double* acont,
+                                 double* sigmac, double* scont, double* parts) {
+  atlasgpu_kapp_pops pp{};
+  pp.t = t;
+  pp.xne = xne;
+  pp.rho = rho;
+  pp.xnfp_h1 = xnfp1;
+  pp.xnfp_h2 = xnfp2;
+  pp.bhyd = bhyd;
+  pp.bmin = bmin;
+  return kapp_run(ctx, "kapp_hydrogen", numnu, waveset, nrhox, kw, pp, false, acont, sigmac, scont, parts);
+}
+
+int atlasgpu_atlas_kapp(atlasgpu_ctx* ctx, int numnu, const double* waveset, int nrhox, int kw,
+                        const atlasgpu_kapp_pops* pops, double* acont, double* sigmac, double* scont, double* parts) {
+  if (!pops) return fail(ctx, ATLASGPU_EINVAL, "kapp: null populations");
+  return kapp_run(ctx, "kapp", numnu, waveset, nrhox, kw, *pops, true, acont, sigmac, scont, parts);
 }
 
 }  // extern "C"

@@ -1,4 +1,4 @@
-// kapp.cuh -- KAPP's hydrogen continuum sources on the device (sm_100a).
+// kapp.cuh -- KAPP's hydrogen and helium continuum sources on the device (sm_100a).
 //
 // KAPP (atlas12_modules.f90:11202-11324) is called once per frequency inside
 // RUN_RT_PASS's loop and evaluates every source at every depth.  Here the
@@ -14,7 +14,10 @@
 //                 bound-free cross-section, HRAYOP's and H2PLOP's factors),
 //                 then lanes over depths: HOP (:11359-11608), H2PLOP
 //                 (:12224-12252), HMINOP (:12360-12558), HRAYOP (:12740-12906),
-//                 ELECOP (:17212-17222) and KAPP's totals.
+//                 ELECOP (:17212-17222) and KAPP's totals; with helium
+//                 populations also HE1OP (:12939-13143, its cross-sections
+//                 per frequency on lanes), HE2OP (:13569-13674), HEMIOP
+//                 (:13716-13833) and HERAOP (:13918-13941).
 // Every output is the reference's expression in its order; where the
 // reference evaluates a depth-only factor inside the frequency loop, the
 // factor is the same function of the same inputs.
@@ -35,6 +38,8 @@ constexpr double kRydbergH = 109677.583403;
 constexpr double kElimHI = 109678.764;
 constexpr double kHminusEA = 0.75419;
 constexpr double kBetaHM88 = 8.798905203085208e+14;
+constexpr double kRydbergHe = 109722.277609;
+constexpr double kClightAngs = 2.99792458e18;
 constexpr double kLogBetaMin = -2.0, kLogBetaStep = 2.4825302042523617e-02;
 constexpr int kHLev = 80;  // HOP's NMAX_HLEVELS
 
@@ -48,13 +53,22 @@ struct KappDev {
   double h2p_fr[5], h2p_es[6];
   double ray_m[74], ray_ab[27], ray_bc[24], ray_cd[22], ray_ly[64], ray_fly[64];
   double series_limits[15];  // H_SERIES_LIMITS
+  // helium: HE1OP's levels, CROSSHE, the 2s/2p fits (log10 knots), HEMIOP's
+  // table and its logs (LOGK(IW, IT) at it*17 + iw)
+  double he1_chi[10], he1_freq[10], he1_g[10];
+  double he_x505[92], he_x50[16], he_x20[11], he_x10[21];
+  double he2s1s_f[16], he2s1s_x[16], he2s3s_f[16], he2s3s_x[16];
+  double he2p1p_f[16], he2p1p_x[16], he2p3p_f[16], he2p3p_x[16];
+  double hem_w[17], hem_t[12], hem_logw[17], hem_logt[12], hem_logk[12 * 17];
 };
 
 // per-depth factors (k_kapp_depth), each [kw]; w, bz: [kHLev][kw] (level n at
-// (n-1)*kw), bp: [9][kw] for the pseudo-continuum's n = 7..15
+// (n-1)*kw), bp: [9][kw] for the pseudo-continuum's n = 7..15; HE1OP's BOLT
+// [10][kw], BOLTN of n = 4..27 [24][kw], FREET, BOLTEX, EXLIM (helium only)
 struct KappDepth {
   double *hkt, *hckt, *tkev, *tlog, *theta, *xhmin;
   double *w, *bz, *bp;
+  double *he_bolt, *he_boltn, *he_freet, *he_boltex, *he_exlim;
 };
 
 struct KappArgs {
@@ -62,9 +76,11 @@ struct KappArgs {
   int numnu, nrhox, kw;
   const double* waveset;
   const double *t, *xne, *rho, *xnfp1, *xnfp2, *bhyd, *bmin;  // bhyd [6][kw], bmin [kw]; may be null
+  const double *xnfp3, *xnfp4, *xnfp5, *xnf4;  // helium populations; xnfp3 null: no helium sources
   KappDepth d;
   double *acont, *sigmac, *scont;  // [numnu][kw]
-  double* parts;                   // [numnu][7][kw] or null
+  double* parts;                   // [numnu][nparts][kw] or null
+  int nparts;                      // 7 (hydrogen) or 11 (with helium)
 };
 
 __host__ __device__ inline double kapp_kbol_ev() { return kKbol / kEvErg; }
@@ -85,58 +101,72 @@ __device__ inline double kapp_occupation(const KappDev& tb, int n, double xne, d
   return tb.q[idx] + frac * (tb.q[idx + 1] - tb.q[idx]);
 }
 
-// XKARZAS(FREQ, 1, N, N): level-averaged Karzas-Latter cross-section, the
-// interpolation in REAL(4) with every operation rounded as written (no
-// contraction)
-__device__ inline double kapp_xkarzas(const KappDev& tb, double freq, int n) {
-  constexpr int NPTS = 29, NMAX = 15;
-  const float fl = __double2float_rn(log10(freq));
+// XKARZAS(FREQ, ZEFF2, N, L): the Karzas-Latter cross-section, level-averaged
+// (L >= N or N > 6) or l-resolved, the interpolation in REAL(4) with every
+// operation rounded as written (no contraction)
+__device__ inline double kapp_xkarzas(const KappDev& tb, double freq, double zeff2, int n, int l) {
+  constexpr int NPTS = 29, NMAX = 15, NLMAX = 6;
+  const float fl = __double2float_rn(log10(freq / zeff2));
   float x;
-  if (n > NMAX) {
-    const float rn = (float)n;
-    const float rn2 = __fmul_rn(rn, rn);
-    const float flast = __double2float_rn(log10(kapp_freq_rydh() / (double)rn2));
-    if (fl < flast) return 0.0;
-    const float r = __fdiv_rn(1.0f, rn2);
-    float fprev = 0.0f, fcur = flast;
-    int i;
-    for (i = 2; i <= NPTS - 1; ++i) {
-      fcur = __double2float_rn(log10((double)__fadd_rn(tb.ekarzas[i - 1], r) * kapp_freq_rydh()));
-      if (fl > fcur) break;
-    }
-    if (i > NPTS - 1) {
-      i = NPTS;
-      fprev = fcur;  // FREQN15(NPTS-1), set by the loop's last pass
-      fcur = flast;
+  if (l >= n || n > NLMAX) {
+    if (n > NMAX) {
+      const float rn = (float)n;
+      const float rn2 = __fmul_rn(rn, rn);
+      const float flast = __double2float_rn(log10(kapp_freq_rydh() / (double)rn2));
+      if (fl < flast) return 0.0;
+      const float r = __fdiv_rn(1.0f, rn2);
+      float fprev = 0.0f, fcur = flast;
+      int i;
+      for (i = 2; i <= NPTS - 1; ++i) {
+        fcur = __double2float_rn(log10((double)__fadd_rn(tb.ekarzas[i - 1], r) * kapp_freq_rydh()));
+        if (fl > fcur) break;
+      }
+      if (i > NPTS - 1) {
+        i = NPTS;
+        fprev = fcur;  // FREQN15(NPTS-1), set by the loop's last pass
+        fcur = flast;
+      } else {
+        // FREQN15(I-1): the previous pass's value, or (I = 2, only above
+        // 1.5e19 Hz) formed like the others
+        fprev = __double2float_rn(log10((double)__fadd_rn(tb.ekarzas[i - 2], r) * kapp_freq_rydh()));
+      }
+      const float* xn = tb.xn + (NMAX - 1) * NPTS;
+      x = __fadd_rn(__fmul_rn(__fdiv_rn(__fsub_rn(fl, fcur), __fsub_rn(fprev, fcur)), __fsub_rn(xn[i - 2], xn[i - 1])),
+                    xn[i - 1]);
     } else {
-      // FREQN15(I-1): the previous pass's value, or (I = 2, only above
-      // 1.5e19 Hz) formed like the others
-      fprev = __double2float_rn(log10((double)__fadd_rn(tb.ekarzas[i - 2], r) * kapp_freq_rydh()));
+      const float* fn = tb.freqn + (n - 1) * NPTS;
+      const float* xn = tb.xn + (n - 1) * NPTS;
+      if (fl < fn[NPTS - 1]) return 0.0;
+      int i;
+      for (i = 2; i <= NPTS; ++i)
+        if (fl > fn[i - 1]) break;
+      if (i > NPTS) i = NPTS;
+      x = __fadd_rn(__fmul_rn(__fdiv_rn(__fsub_rn(fl, fn[i - 1]), __fsub_rn(fn[i - 2], fn[i - 1])),
+                              __fsub_rn(xn[i - 2], xn[i - 1])),
+                    xn[i - 1]);
     }
-    const float* xn = tb.xn + (NMAX - 1) * NPTS;
-    x = __fadd_rn(__fmul_rn(__fdiv_rn(__fsub_rn(fl, fcur), __fsub_rn(fprev, fcur)), __fsub_rn(xn[i - 2], xn[i - 1])),
-                  xn[i - 1]);
   } else {
     const float* fn = tb.freqn + (n - 1) * NPTS;
-    const float* xn = tb.xn + (n - 1) * NPTS;
+    const float* xl = tb.xl + ((n - 1) * NLMAX + l) * NPTS;  // XL(I, L+1, N)
     if (fl < fn[NPTS - 1]) return 0.0;
     int i;
     for (i = 2; i <= NPTS; ++i)
       if (fl > fn[i - 1]) break;
     if (i > NPTS) i = NPTS;
     x = __fadd_rn(__fmul_rn(__fdiv_rn(__fsub_rn(fl, fn[i - 1]), __fsub_rn(fn[i - 2], fn[i - 1])),
-                            __fsub_rn(xn[i - 2], xn[i - 1])),
-                  xn[i - 1]);
+                            __fsub_rn(xl[i - 2], xl[i - 1])),
+                  xl[i - 1]);
   }
-  return exp((double)x * kLn10);
+  return exp((double)x * kLn10) / zeff2;
 }
 
-// COULFF(J, 1) (:11995-12196): bilinear interpolation in log g_ff
-__device__ inline double kapp_coulff(const KappDev& tb, double freqlg, double tlog) {
+// COULFF(J, NZ) (:11995-12196): bilinear interpolation in log g_ff; z2log is
+// Z2LOG(NZ) (0 for H, 0.60206 for He II)
+__device__ inline double kapp_coulff(const KappDev& tb, double freqlg, double tlog, double z2log = 0.0) {
   constexpr int NG = 81, NU = 146;
   const double l10ryk = log10(kapp_freq_rydh() * kapp_hoverk());
   const double l10kh = -log10(kapp_hoverk());
-  const double lgam2 = 0.0 + l10ryk - tlog / kLn10;
+  const double lgam2 = z2log + l10ryk - tlog / kLn10;
   const double lu = (freqlg - tlog) / kLn10 - l10kh;
   const double xi = (lgam2 - -6.0) / 0.2 + 1.0;
   const double xj = (lu - -16.0) / 0.2 + 1.0;
@@ -199,6 +229,182 @@ __device__ inline double kapp_rayleigh(const KappDev& tb, double freq) {
   return kSigmaThomson * fnew;
 }
 
+// CROSSHE (:13160-13236): Marr & West's He I ground-state cross-section on
+// four uniform wavelength grids
+__device__ inline double kapp_crosshe(const KappDev& tb, double freq) {
+  if (freq < 5.945209e15) return 0.0;
+  const double wave = kClightAngs / freq;
+  int i;
+  if (wave > 50.0) {
+    i = min(92, max(2, (int)(93.0 - (wave - 50.0) / 5.0)));
+    return ((wave - (double)(92 - i) * 5.0 - 50.0) / 5.0 * (tb.he_x505[i - 2] - tb.he_x505[i - 1]) +
+            tb.he_x505[i - 1]) *
+           1.0e-18;
+  }
+  if (wave > 20.0) {
+    i = min(16, max(2, (int)(17.0 - (wave - 20.0) / 2.0)));
+    return ((wave - (double)(16 - i) * 2.0 - 20.0) / 2.0 * (tb.he_x50[i - 2] - tb.he_x50[i - 1]) +
+            tb.he_x50[i - 1]) *
+           1.0e-18;
+  }
+  if (wave > 10.0) {
+    i = min(11, max(2, (int)(12.0 - (wave - 10.0) / 1.0)));
+    return ((wave - (double)(11 - i) * 1.0 - 10.0) / 1.0 * (tb.he_x20[i - 2] - tb.he_x20[i - 1]) +
+            tb.he_x20[i - 1]) *
+           1.0e-18;
+  }
+  i = min(21, max(2, (int)(22.0 - wave / 0.5)));
+  return ((wave - (double)(21 - i) * 0.5) / 0.5 * (tb.he_x10[i - 2] - tb.he_x10[i - 1]) + tb.he_x10[i - 1]) * 1.0e-18;
+}
+
+// the knot interpolation in log10 frequency shared by HE12S1S, HE12S3S,
+// HE12P1P and HE12P3P (:13299-13545)
+__device__ inline double kapp_he_knots(const double* f, const double* x, double freq) {
+  const double freqlg = log10(freq);
+  int i;
+  for (i = 2; i <= 16; ++i)
+    if (freqlg > f[i - 1]) break;
+  if (i > 16) i = 16;
+  const double v = (freqlg - f[i - 1]) / (f[i - 2] - f[i - 1]) * (x[i - 2] - x[i - 1]) + x[i - 1];
+  return exp(v * kLn10);
+}
+
+// HE1OP's TRANS(N) (:13006-13097): the level's own cross-section when
+// IMIN <= N, plus its inner-shell term to He II n = 2 (N = 2..5) or n = 3
+// (N = 6..10) when IMIN >= 1 and every threshold of the nested tests is
+// reached
+__device__ __noinline__ double kapp_he1_trans(const KappDev& tb, double freq, int n, int imin) {
+  double tr = 0.0;
+  if (imin > 0 && imin <= n) {
+    switch (n) {
+      case 1: tr = kapp_crosshe(tb, freq); break;
+      case 2:  // HE12S3S
+        if (freq >= 38454.691 * kClight) {
+          if (freq > 2.4 * kRydbergHe * kClight) {
+            const double wavno = freq / kClight;
+            const double ek = (wavno - 38454.691) / kRydbergHe;
+            const double eps = 2.0 * (ek - 2.47898) / 0.000780;
+            tr = 0.01521 * pow(470310.0 / wavno, 3.12) * 8.067e-18 * powi(eps - 122.4, 2) / (1.0 + powi(eps, 2));
+          } else {
+            tr = kapp_he_knots(tb.he2s3s_f, tb.he2s3s_x, freq);
+          }
+        }
+        break;
+      case 3:  // HE12S1S
+        if (freq >= 32033.214 * kClight) {
+          if (freq > 2.4 * kRydbergHe * kClight) {
+            const double wavno = freq / kClight;
+            const double ek = (wavno - 32033.214) / kRydbergHe;
+            const double eps = 2.0 * (ek - 2.612316) / 0.00322;
+            tr = 0.008175 * pow(484940.0 / wavno, 2.71) * 8.067e-18 * powi(eps + 76.21, 2) / (1.0 + powi(eps, 2));
+          } else {
+            tr = kapp_he_knots(tb.he2s1s_f, tb.he2s1s_x, freq);
+          }
+        }
+        break;
+      case 4:  // HE12P3P
+        if (freq >= 29223.753 * kClight) tr = kapp_he_knots(tb.he2p3p_f, tb.he2p3p_x, freq);
+        break;
+      case 5:  // HE12P1P
+        if (freq >= 27175.76 * kClight) {
+          if (freq > 2.4 * kRydbergHe * kClight) {
+            const double wavno = freq / kClight;
+            const double ek = (wavno - 27175.76) / kRydbergHe;
+            const double eps1s = 2.0 * (ek - 2.446534) / 0.01037;
+            const double eps1d = 2.0 * (ek - 2.59427) / 0.00538;
+            tr = 0.0009487 * pow(466750.0 / wavno, 3.69) * 8.067e-18 *
+                 (powi(eps1s - 29.30, 2) / (1.0 + powi(eps1s, 2)) + powi(eps1d + 172.4, 2) / (1.0 + powi(eps1d, 2)));
+          } else {
+            tr = kapp_he_knots(tb.he2p1p_f, tb.he2p1p_x, freq);
+          }
+        }
+        break;
+      case 6: tr = kapp_xkarzas(tb, freq, 1.236439, 3, 0); break;
+      case 7: tr = kapp_xkarzas(tb, freq, 1.102898, 3, 0); break;
+      case 8: tr = kapp_xkarzas(tb, freq, 1.045499, 3, 1); break;
+      case 9: tr = kapp_xkarzas(tb, freq, 1.001427, 3, 2); break;
+      default: tr = kapp_xkarzas(tb, freq, 0.9926, 3, 1); break;
+    }
+  }
+  if (imin >= 1 && n >= 2) {
+    const double ryd = kRydbergHe * kClight;
+    // excited-level energies (cm^-1) of the nested tests: N = 5, 4, 3, 2 below
+    // ELIM 527490.06 (He II n = 2), N = 10 .. 6 below ELIM 588451.59 (n = 3)
+    const double elim = n <= 5 ? 527490.06 : 588451.59;
+    const int top = n <= 5 ? 5 : 10;
+    for (int k = top; k >= n; --k) {
+      double e;
+      switch (k) {
+        case 5: e = 171135.000; break;
+        case 4: e = 169087.0; break;
+        case 3: e = 166277.546; break;
+        case 2: e = 159856.069; break;
+        case 10: e = 186209.471; break;
+        case 9: e = 186101.0; break;
+        case 8: e = 185564.0; break;
+        case 7: e = 184864.0; break;
+        default: e = 183236.0; break;
+      }
+      const double freqhe = (elim - e) * kClight;
+      if (!(freq >= freqhe)) break;
+      if (k == n) tr = tr + kapp_xkarzas(tb, freq, freqhe / ryd, 1, 0);
+    }
+  }
+  return tr;
+}
+
+// HE2OP (:13569-13674) at one depth: He II bound-free (dissolved levels
+// n >= 10, n = 9..1 down to the frequency's threshold) and free-free
+__device__ __noinline__ double kapp_he2op(const KappDev& tb, double freq, double freqlg, double waveno, double T,
+                                    double tlog, double hckt, double stim, double xne, double rho, double x4,
+                                    double x5) {
+  const double freq3 = 2.815e29 / freq / freq / freq;
+  const double xnfprho = x4 / rho;
+  double H = freq3 * 16.0 * 2.0 / 2.0 / (438889.068 * hckt) *
+             (exp(-fmax(434519.959, 438908.85 - waveno) * hckt) - exp(-438908.85 * hckt)) * stim * xnfprho;
+  double X, A;
+  do {
+    if (waveno < 5418.390) break;
+    X = freq3 / 59049.0 * 16.0;
+    A = X * 162.0 * exp(-433490.46 * hckt) * stim * xnfprho;
+    H = H + A;
+    if (waveno < 6857.660) break;
+    X = freq3 * 16.0 / 32768.0;
+    A = X * 128.0 * exp(-432051.19 * hckt) * stim * xnfprho;
+    H = H + A;
+    if (waveno < 8956.950) break;
+    X = freq3 * 16.0 / 16807.0;
+    A = X * 98.0 * exp(-429951.90 * hckt) * stim * xnfprho;
+    H = H + A;
+    if (waveno < 12191.437) break;
+    X = freq3 * 16.0 / 7776.0 * (1.0986 + (-2.704e13 + 1.229e27 / freq) / freq);
+    A = X * 72.0 * exp(-426717.413 * hckt) * stim * xnfprho;
+    H = H + A;
+    if (waveno < 17555.715) break;
+    X = freq3 * 16.0 / 3125.0 * (1.102 + (-3.909e13 + 2.371e27 / freq) / freq);
+    A = X * 50.0 * exp(-421353.135 * hckt) * stim * xnfprho;
+    H = H + A;
+    if (waveno < 27430.925) break;
+    X = freq3 * 16.0 / 1024.0 * (1.101 + (-5.765e13 + 4.593e27 / freq) / freq);
+    A = X * 32.0 * exp(-411477.925 * hckt) * stim * xnfprho;
+    H = H + A;
+    if (waveno < 48766.491) break;
+    X = freq3 * 16.0 / 243.0 * (1.101 + (-9.863e13 + 1.035e28 / freq) / freq);
+    A = X * 18.0 * exp(-390142.359 * hckt) * stim * xnfprho;
+    H = H + A;
+    if (waveno < 109726.529) break;
+    X = freq3 * 16.0 / 32.0 * (1.105 + (-2.375e14 + 4.077e28 / freq) / freq);
+    A = X * 8.0 * exp(-329182.321 * hckt) * stim * xnfprho;
+    H = H + A;
+    if (waveno < 438908.850) break;
+    X = freq3 * 16.0 / 1.0 * (0.9916 + (2.719e13 - 2.268e30 / freq) / freq);
+    A = X * 2.0 * stim * xnfprho;
+    H = H + A;
+  } while (false);
+  A = kCoeffFF * 4.0 / sqrt(T) * kapp_coulff(tb, freqlg, tlog, 0.60206) / freq * xne / freq * x5 / freq * stim / rho;
+  return H + A;
+}
+
 // per-depth factors; threads over depths
 static __global__ void k_kapp_depth(KappArgs a) {
   const KappDev& tb = *a.tb;
@@ -227,15 +433,32 @@ static __global__ void k_kapp_depth(KappArgs a) {
       a.d.bz[(size_t)(n - 1) * kw + j] = exp(-en * hckt);
       if (n >= 7 && n <= 15) a.d.bp[(size_t)(n - 7) * kw + j] = exp(-(kElimHI - kRydbergH / dn2) * hckt);
     }
+    if (a.xnfp3) {
+      // HE1OP's temperature block (:12978-12995)
+      const double x3 = a.xnfp3[j], rho = a.rho[j];
+      for (int n = 1; n <= 10; ++n)
+        a.d.he_bolt[(size_t)(n - 1) * kw + j] = exp(-tb.he1_chi[n - 1] / tkev) * tb.he1_g[n - 1] * x3 / rho;
+      for (int n = 4; n <= 27; ++n) {
+        const double dn2 = powi((double)n, 2);
+        a.d.he_boltn[(size_t)(n - 4) * kw + j] = exp(-24.587 * (1.0 - 1.0 / dn2) / tkev) * 4.0 * dn2 * x3 / rho;
+      }
+      a.d.he_freet[j] = xne * a.xnf4[j] / rho / sqrt(T);
+      const double xr = x3 * (4.0 / 2.0 / 13.595) * tkev / rho;
+      a.d.he_boltex[j] = exp(-23.730 / tkev) * xr;
+      a.d.he_exlim[j] = exp(-24.587 / tkev) * xr;
+    }
   }
 }
 
 constexpr int kKappWarps = 8;  // warps per CTA of k_kapp_nu
 
-// warp per frequency (grid-stride), lanes over depths
+// warp per frequency (grid-stride), lanes over depths; kHelium adds the
+// helium sources (a separate instantiation keeps the hydrogen one lean)
+template <bool kHelium>
 static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) {
   __shared__ double s_xk[kKappWarps][kHLev + 1];
   __shared__ double s_fftt[kKappWarps][11];
+  __shared__ double s_he[kKappWarps][10 + 24 + 12];  // HE1OP's TRANS, TRANSN of n = 4..27; HEMIOP's KT
   const KappDev& tb = *a.tb;
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int kw = a.kw;
@@ -243,6 +466,10 @@ static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) 
   const double theta_c = 0.4342944819032518 / kapp_kbol_ev();
   double* xk = s_xk[wid];
   double* fftt = s_fftt[wid];
+  double* trans = s_he[wid];
+  double* transn = trans + 10;
+  double* hem_kt = transn + 24;
+  constexpr bool helium = kHelium;
   for (int nu = blockIdx.x * kKappWarps + wid; nu < a.numnu; nu += gridDim.x * kKappWarps) {
     // RUN_RT_PASS's frequency quantities (:3907-3917)
     const double wave = a.waveset[nu];
@@ -251,7 +478,7 @@ static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) 
     const double freqlg = log(freq);
     const double f3 = powi(freq / 1.0e15, 3);
     // XKARZAS(FREQ, 1, n, n) of n = 1..80, HMINOP's free-free table at this wavelength
-    for (int n = lane + 1; n <= kHLev; n += 32) xk[n] = kapp_xkarzas(tb, freq, n);
+    for (int n = lane + 1; n <= kHLev; n += 32) xk[n] = kapp_xkarzas(tb, freq, 1.0, n, n);
     if (lane < 11)
       fftt[lane] = exp(kapp_linter(tb.wfflog, tb.fflog + lane * 22, 22, log(wave))) / tb.thetaff[lane] * theta_c *
                    kKbol;
@@ -263,6 +490,35 @@ static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) 
     const double frh2 = c[0] + (c[1] + (c[2] + (c[3] + c[4] * freqlg) * freqlg) * freqlg) * freqlg;
     const double esh2 = e[0] + (e[1] + (e[2] + (e[3] + (e[4] + e[5] * freq) * freq) * freq) * freq) * freq;
     const double freq3_inv = 1.0 / (freq * freq * freq);
+    // helium per frequency: HE1OP's IMIN and cross-sections (lanes over the
+    // levels), HEMIOP's log k at this wavelength for the twelve temperatures,
+    // HERAOP's cross-section
+    int imin = 0;
+    double sighe_x = 0.0;
+    const double freq3he = powi(freq, 3);
+    if (helium) {
+      for (int n = 1; n <= 10; ++n)
+        if (tb.he1_freq[n - 1] <= freq) {
+          imin = n;
+          break;
+        }
+      if (lane < 10) trans[lane] = kapp_he1_trans(tb, freq, lane + 1, imin);
+      if (lane < 24) {
+        const double zeff2 = 4.0 - 3.0 / powi((double)(lane + 4), 2);
+        transn[lane] = freq >= 1.25408e16 ? kapp_xkarzas(tb, freq, zeff2, 1, 0) : 0.0;
+      }
+      double wl = wave;
+      if (wl > tb.hem_w[16]) wl = tb.hem_w[16];
+      int iw = 1;
+      for (int i = 1; i <= 16; ++i)
+        if (wl >= tb.hem_w[i - 1]) iw = i;
+      const double xw = (log(wl) - tb.hem_logw[iw - 1]) / (tb.hem_logw[iw] - tb.hem_logw[iw - 1]);
+      if (lane < 12)
+        hem_kt[lane] = tb.hem_logk[lane * 17 + iw - 1] * (1.0 - xw) + tb.hem_logk[lane * 17 + iw] * xw;
+      const double w = kClightAngs / fmin(freq, 5.15e15);
+      const double ww = powi(w, 2);
+      sighe_x = 5.484e-14 / ww / ww * powi(1.0 + (2.44e5 + 5.94e10 / (ww - 2.90e5)) / ww, 2);
+    }
     __syncwarp();
     for (int j = lane; j < a.nrhox; j += 32) {
       const double T = a.t[j];
@@ -311,7 +567,8 @@ static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) 
       }
       H = H * x1 / rho;
       S = S * x1 / rho;
-      A = kCoeffFF / sqrt(T) * kapp_coulff(tb, freqlg, a.d.tlog[j]) / freq * xne / freq * x2 / freq * stim / rho;
+      const double gff1 = kapp_coulff(tb, freqlg, a.d.tlog[j]);  // COULFF(J, 1), also HE1OP's
+      A = kCoeffFF / sqrt(T) * gff1 / freq * xne / freq * x2 / freq * stim / rho;
       H = H + A;
       S = S + A * bnu;
       const double ahyd = H, shyd = H > 0.0 ? S / H : 0.0;
@@ -327,17 +584,41 @@ static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) 
       // HRAYOP, ELECOP
       const double sigh = xray * x1 * 2.0 * bh1 / rho;
       const double sigel = kSigmaThomson * xne / rho;
-      // KAPP's totals (:11300-11320); the sources not built here are zero
-      const double av = ah2p + 0.0 + 0.0 + 0.0 + 0.0 + 0.0 + 0.0;
+      // helium: HE1OP (:13108-13140), HE2OP, HEMIOP, HERAOP
+      double ahe1 = 0.0, ahe2 = 0.0, ahemin = 0.0, sighe = 0.0;
+      if (helium) {
+        const double exlim = a.d.he_exlim[j];
+        double ex = a.d.he_boltex[j];
+        if (freq < 2.055e14) ex = exlim / ehvkt;
+        double he1 = (ex - exlim) * (2.815e29 / freq3he);
+        if (imin > 0)
+          for (int n = imin; n <= 10; ++n) he1 = he1 + trans[n - 1] * a.d.he_bolt[(size_t)(n - 1) * kw + j];
+        if (freq >= 1.25408e16)
+          for (int n = 4; n <= 27; ++n) he1 = he1 + transn[n - 4] * a.d.he_boltn[(size_t)(n - 4) * kw + j];
+        ahe1 = (he1 + gff1 * a.d.he_freet[j] * (kCoeffFF / freq3he)) * stim;
+        ahe2 = kapp_he2op(tb, freq, freqlg, waveno, T, a.d.tlog[j], a.d.hckt[j], stim, xne, rho, a.xnfp4[j],
+                          a.xnfp5[j]);
+        int it = 1;
+        for (int i = 1; i <= 11; ++i)
+          if (T >= tb.hem_t[i - 1]) it = i;
+        double xt = (log(fmax(T, 1.0)) - tb.hem_logt[it - 1]) / (tb.hem_logt[it] - tb.hem_logt[it - 1]);
+        xt = fmax(0.0, fmin(1.0, xt));
+        const double lkv = hem_kt[it - 1] * (1.0 - xt) + hem_kt[it] * xt;
+        const double x3 = a.xnfp3[j];
+        ahemin = exp(lkv) * xne * kKbol * T * x3 / rho;
+        sighe = sighe_x * x3 / rho;
+      }
+      // KAPP's totals (:11300-11320); the metal, H2 and line sources are zero
+      const double av = ah2p + ahe1 + ahe2 + ahemin + 0.0 + 0.0 + 0.0;
       const double acont = av + ahyd + ahmin;
       double scont = bnu;
       if (acont > 0.0) scont = (av * bnu + ahyd * shyd + ahmin * shmin) / acont;
       const size_t o = (size_t)nu * kw + j;
       a.acont[o] = acont;
       a.scont[o] = scont;
-      a.sigmac[o] = sigh + 0.0 + sigel + 0.0 + 0.0;
+      a.sigmac[o] = sigh + sighe + sigel + 0.0 + 0.0;
       if (a.parts) {
-        double* p = a.parts + (size_t)nu * 7 * kw + j;
+        double* p = a.parts + (size_t)nu * a.nparts * kw + j;
         p[0] = ahyd;
         p[kw] = shyd;
         p[2 * kw] = ah2p;
@@ -345,6 +626,12 @@ static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) 
         p[4 * kw] = shmin;
         p[5 * kw] = sigh;
         p[6 * kw] = sigel;
+        if (a.nparts > 7) {
+          p[7 * kw] = ahe1;
+          p[8 * kw] = ahe2;
+          p[9 * kw] = ahemin;
+          p[10 * kw] = sighe;
+        }
       }
     }
     __syncwarp();

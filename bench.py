@@ -569,8 +569,9 @@ SELECT_TRAFFIC_PER_LINEREC = 36.4
 
 
 def kapp_rate(ctx, ops, W):
-    """KAPP's hydrogen continuum sources (atlasgpu_atlas_kapp_hydrogen) over the
-    workload's 30,000 frequencies and 72 depths of the grey solar model:
+    """KAPP's hydrogen continuum sources (atlasgpu_atlas_kapp_hydrogen), and with
+    the helium ones (atlasgpu_atlas_kapp), over the workload's 30,000
+    frequencies and 72 depths of the grey solar model:
     kernel time (CUDA events, after a warm-up call) and (frequency, depth)
     evaluations per second; the call's host copies are outside the kernel time."""
     from atlas12_b200 import atlas, surrogate
@@ -585,9 +586,24 @@ def kapp_rate(ctx, ops, W):
     ms = ctx.kernel_ms("kapp_hydrogen")
     ctx.enable_timing(False)
     n = W["ws"].size * m["t"].size
+    # the same with the helium sources (atlasgpu_atlas_kapp): helium at 0.0851
+    # of hydrogen by number, its ionisation split by smooth functions of T
+    t = m["t"]
+    nhe = 0.0851 * e["nh"]
+    f1 = 1.0 / (1.0 + np.exp(-(t - 12000.0) / 1500.0))
+    f2 = 1.0 / (1.0 + np.exp(-(t - 22000.0) / 2500.0))
+    xnf4 = nhe * f1 * (1.0 - f2)
+    hargs = args + (nhe * (1.0 - f1), xnf4 / 2.0, nhe * f1 * f2, xnf4)
+    A.kapp(*hargs)
+    ctx.enable_timing(True)
+    A.kapp(*hargs)
+    ms_he = ctx.kernel_ms("kapp")
+    ctx.enable_timing(False)
     return {"frequencies": int(W["ws"].size), "depths": int(m["t"].size), "kernel_ms": ms,
             "evals_per_s": n / (ms * 1e-3) if ms > 0 else None,
-            "sources": "HOP (n = 1..80), H2PLOP, HMINOP, HRAYOP, ELECOP and KAPP's totals"}
+            "sources": "HOP (n = 1..80), H2PLOP, HMINOP, HRAYOP, ELECOP and KAPP's totals",
+            "with_helium": {"kernel_ms": ms_he, "evals_per_s": n / (ms_he * 1e-3) if ms_he > 0 else None,
+                            "sources": "the above and HE1OP, HE2OP, HEMIOP, HERAOP"}}
 
 
 def hbm_peak():

@@ -343,7 +343,15 @@ int atlasgpu_atlas_xlinop(atlasgpu_ctx *ctx, const atlasgpu_nlte_line *recs, int
  *   H2PLOP (:12224-12252): the FR and ES fit coefficients, signed, lowest
  *     order first;
  *   HRAYOP (:12740-12906): GAVRILAM, GAVRILAMAB, GAVRILAMBC, GAVRILAMCD,
- *     GAVRILALYMANCONT, FGAVRILALYMANCONT. */
+ *     GAVRILALYMANCONT, FGAVRILALYMANCONT;
+ * and the helium ones:
+ *   HE1OP (:12939-13143): CHI, HEFREQ, G of its ten resolved levels;
+ *   CROSSHE (:13160-13236): X505, X50, X20, X10 (1e-18 cm^2);
+ *   HE12S1S, HE12S3S, HE12P1P, HE12P3P (:13299-13545): log10 frequency and
+ *     log10 cross-section knots (FREQ1S/X1S, FREQ3S/X3S, FREQ1P/X1P,
+ *     FREQ3P/X3P);
+ *   HEMIOP (:13716-13833): WHEM (nm), THEM (K), KHEM(17,12) (cm^4/dyn; the
+ *     library takes the logs as the reference's first call does). */
 typedef struct atlasgpu_kapp_tables {
   float freqn[15][29], xn[15][29], xl[6][6][29], ekarzas[29];
   double gff[146][81];
@@ -352,6 +360,11 @@ typedef struct atlasgpu_kapp_tables {
   double hmin_wbf[116], hmin_bf[116], hmin_thetaff[11], hmin_wavek[22], hmin_ff[22][11];
   double h2p_fr[5], h2p_es[6];
   double ray_m[74], ray_ab[27], ray_bc[24], ray_cd[22], ray_ly[64], ray_fly[64];
+  double he1_chi[10], he1_freq[10], he1_g[10];
+  double he_x505[92], he_x50[16], he_x20[11], he_x10[21];
+  double he2s1s_f[16], he2s1s_x[16], he2s3s_f[16], he2s3s_x[16];
+  double he2p1p_f[16], he2p1p_x[16], he2p3p_f[16], he2p3p_x[16];
+  double hem_w[17], hem_t[12], hem_k[12][17];
 } atlasgpu_kapp_tables;
 
 /* Keeps KAPP's hydrogen tables on the context for atlasgpu_atlas_kapp_hydrogen
@@ -375,6 +388,31 @@ int atlasgpu_atlas_kapp_hydrogen(atlasgpu_ctx *ctx, int numnu, const double *wav
                                  const double *t, const double *xne, const double *rho, const double *xnfp1,
                                  const double *xnfp2, const double *bhyd, const double *bmin, double *acont,
                                  double *sigmac, double *scont, double *parts);
+
+/* Depth vectors [nrhox] for atlasgpu_atlas_kapp: the hydrogen ones as for
+ * atlasgpu_atlas_kapp_hydrogen, and the helium populations the helium
+ * sources read: XNFP(J,3) (He I over its partition function), XNFP(J,4)
+ * (He II), XNFP(J,5) (He III) and XNF(J,4) (the He II number density, which
+ * HE1OP's free-free term takes). */
+typedef struct atlasgpu_kapp_pops {
+  const double *t, *xne, *rho;
+  const double *xnfp_h1, *xnfp_h2;
+  const double *xnfp_he1, *xnfp_he2, *xnfp_he3, *xnf_he2;
+  const double *bhyd, *bmin; /* NULL for LTE, as for atlasgpu_atlas_kapp_hydrogen */
+} atlasgpu_kapp_pops;
+
+/* KAPP (atlas12_modules.f90:11202-11324) with the hydrogen sources of
+ * atlasgpu_atlas_kapp_hydrogen and the helium ones: HE1OP (:12939-13143: the
+ * ten resolved levels with CROSSHE, the 2s/2p fits and XKARZAS for the n = 3
+ * levels, the inner-shell thresholds to He II n = 2 and 3, n = 4..27, the
+ * dissolved-level term, free-free), HE2OP (:13569-13674), HEMIOP
+ * (:13716-13833), HERAOP (:13918-13941); ACONT, SCONT and SIGMAC as KAPP
+ * forms them with the metal, H2 and line sources zero.  Outputs as for
+ * atlasgpu_atlas_kapp_hydrogen; parts, if not NULL, [numnu][11][kw]: AHYD,
+ * SHYD, AH2P, AHMIN, SHMIN, SIGH, SIGEL, AHE1, AHE2, AHEMIN, SIGHE. */
+int atlasgpu_atlas_kapp(atlasgpu_ctx *ctx, int numnu, const double *waveset, int nrhox, int kw,
+                        const atlasgpu_kapp_pops *pops, double *acont, double *sigmac, double *scont,
+                        double *parts);
 
 /* RUN_RT_PASS frequency loop (atlas12_modules.f90:3880-3951): per NU the
  * Planck terms, ALINE = XLINES*STIM, JOSH(1,0) (:18398-18776), the negative

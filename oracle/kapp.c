@@ -1,6 +1,6 @@
-/* kapp.c -- CPU oracle (test infrastructure) of KAPP's hydrogen continuum
- * sources: the checker of atlasgpu_atlas_kapp_hydrogen.  Never part of the
- * product; only tests/ load it.
+/* kapp.c -- CPU oracle (test infrastructure) of KAPP's hydrogen and helium
+ * continuum sources: the checker of atlasgpu_atlas_kapp_hydrogen and
+ * atlasgpu_atlas_kapp.  Never part of the product; only tests/ load it.
  *
  * Restates, per frequency and depth, the reference's (src/atlas12_modules.f90):
  *   KAPP assembly        :11202-11324 (ACONT, SCONT, SIGMAC from the sources built here;
@@ -15,6 +15,11 @@
  *   HRAYOP               :12740-12906
  *   ELECOP               :17212-17222
  *   occupation_prob      :22549-22567, holtsmark_Q :22492-22519
+ *   HE1OP                :12939-13143 (with CROSSHE :13160-13236 and the 2s/2p fits
+ *                                      HE12S1S, HE12S3S, HE12P1P, HE12P3P :13299-13545)
+ *   HE2OP                :13569-13674
+ *   HEMIOP               :13716-13833
+ *   HERAOP               :13918-13941
  * Constants from mod_constants (:315-464).  The tables come from the
  * reference's data files and DATA statements (tests/golden/make_golden.py).
  */
@@ -39,6 +44,8 @@
 #define K_BETA_COEFF_HM88 8.798905203085208e+14
 #define K_LOG_BETA_MIN (-2.0)
 #define K_LOG_BETA_STEP 2.4825302042523617e-02
+#define K_RYDBERG_HE 109722.277609
+#define K_CLIGHT_ANGS 2.99792458e18
 
 static const double H_SERIES_LIMITS[15] = {109678.764, 27419.659, 12186.462, 6854.871, 4387.113,
                                            3046.604,   2238.320,  1713.713,  1354.044, 1096.776,
@@ -122,13 +129,13 @@ double orc_xkarzas(const orc_kapp_tables *tb, double freq, double zeff2, int n, 
   return exp((double)x * K_LN10) / zeff2;
 }
 
-/* COULFF(J, 1) (:11995-12196): GFF_LOGTAB(81,146) column-major, log10 of the
- * tabulated g_ff as the reader stores it */
-static double coulff_h(const orc_kapp_tables *tb, double freqlg, double tlog) {
+/* COULFF(J, NZ) (:11995-12196): GFF_LOGTAB(81,146) column-major, log10 of
+ * the tabulated g_ff as the reader stores it; z2log = Z2LOG(NZ) */
+static double coulff(const orc_kapp_tables *tb, double freqlg, double tlog, double z2log) {
   enum { NG = 81, NU = 146 };
   const double log10_ryh_over_k = log10(freq_rydh() * hoverk());
   const double log10_k_over_h = -log10(hoverk());
-  const double lgam2 = 0.0 + log10_ryh_over_k - tlog / K_LN10;
+  const double lgam2 = z2log + log10_ryh_over_k - tlog / K_LN10;
   const double lu = (freqlg - tlog) / K_LN10 - log10_k_over_h;
   const double xi = (lgam2 - -6.0) / 0.2 + 1.0;
   const double xj = (lu - -16.0) / 0.2 + 1.0;
@@ -295,7 +302,7 @@ void orc_kapp_hydrogen(const orc_kapp_tables *tb, double wave, int nrhox, const 
     }
     H = H * xnfp1[j] / rho[j];
     S = S * xnfp1[j] / rho[j];
-    A = K_COEFF_FF / sqrt(T) * coulff_h(tb, freqlg, tlog) / freq * xne[j] / freq * xnfp2[j] / freq * stim / rho[j];
+    A = K_COEFF_FF / sqrt(T) * coulff(tb, freqlg, tlog, 0.0) / freq * xne[j] / freq * xnfp2[j] / freq * stim / rho[j];
     H = H + A;
     S = S + A * bnu;
     const double ahyd = H, shyd = H > 0.0 ? S / H : 0.0;
@@ -320,6 +327,273 @@ void orc_kapp_hydrogen(const orc_kapp_tables *tb, double wave, int nrhox, const 
     const double sigmac = sigh + 0.0 + sigel + 0.0 + 0.0;
     const double q[ORC_KAPP_NOUT] = {ahyd, shyd, ah2p, ahmin, shmin, sigh, sigel, acont, scont, sigmac};
     for (int k = 0; k < ORC_KAPP_NOUT; ++k) out[(size_t)k * nrhox + j] = q[k];
+  }
+}
+
+/* ---- helium ---- */
+
+/* CROSSHE (:13160-13236) */
+double orc_crosshe(const orc_kapp_tables *tb, double freq) {
+  if (freq < 5.945209e15) return 0.0;
+  const double wave = K_CLIGHT_ANGS / freq;
+  int i;
+  if (wave > 50.0) {
+    i = (int)(93.0 - (wave - 50.0) / 5.0);
+    i = i < 2 ? 2 : (i > 92 ? 92 : i);
+    return ((wave - (92 - i) * 5.0 - 50.0) / 5.0 * (tb->he_x505[i - 2] - tb->he_x505[i - 1]) + tb->he_x505[i - 1]) *
+           1.e-18;
+  } else if (wave > 20.0) {
+    i = (int)(17.0 - (wave - 20.0) / 2.0);
+    i = i < 2 ? 2 : (i > 16 ? 16 : i);
+    return ((wave - (16 - i) * 2.0 - 20.0) / 2.0 * (tb->he_x50[i - 2] - tb->he_x50[i - 1]) + tb->he_x50[i - 1]) *
+           1.e-18;
+  } else if (wave > 10.0) {
+    i = (int)(12.0 - (wave - 10.0) / 1.0);
+    i = i < 2 ? 2 : (i > 11 ? 11 : i);
+    return ((wave - (11 - i) * 1.0 - 10.0) / 1.0 * (tb->he_x20[i - 2] - tb->he_x20[i - 1]) + tb->he_x20[i - 1]) *
+           1.e-18;
+  }
+  i = (int)(22.0 - wave / 0.5);
+  i = i < 2 ? 2 : (i > 21 ? 21 : i);
+  return ((wave - (21 - i) * 0.5) / 0.5 * (tb->he_x10[i - 2] - tb->he_x10[i - 1]) + tb->he_x10[i - 1]) * 1.e-18;
+}
+
+/* the log10-knot branch of HE12S1S, HE12S3S, HE12P1P, HE12P3P */
+static double he_knots(const double *fk, const double *xk, double freq) {
+  const double freqlg = log10(freq);
+  int i;
+  for (i = 2; i <= 16; ++i)
+    if (freqlg > fk[i - 1]) break;
+  if (i > 16) i = 16;
+  const double x = (freqlg - fk[i - 1]) / (fk[i - 2] - fk[i - 1]) * (xk[i - 2] - xk[i - 1]) + xk[i - 1];
+  return exp(x * K_LN10);
+}
+
+/* HE12S1S (:13299-13343) */
+static double he12s1s(const orc_kapp_tables *tb, double freq) {
+  if (freq < 32033.214 * K_CLIGHT) return 0.0;
+  if (freq > 2.4 * K_RYDBERG_HE * K_CLIGHT) {
+    const double wavno = freq / K_CLIGHT;
+    const double ek = (wavno - 32033.214) / K_RYDBERG_HE;
+    const double eps = 2.0 * (ek - 2.612316) / 0.00322;
+    return 0.008175 * pow(484940.0 / wavno, 2.71) * 8.067e-18 * ipow(eps + 76.21, 2) / (1.0 + ipow(eps, 2));
+  }
+  return he_knots(tb->he2s1s_f, tb->he2s1s_x, freq);
+}
+
+/* HE12S3S (:13346-13390) */
+static double he12s3s(const orc_kapp_tables *tb, double freq) {
+  if (freq < 38454.691 * K_CLIGHT) return 0.0;
+  if (freq > 2.4 * K_RYDBERG_HE * K_CLIGHT) {
+    const double wavno = freq / K_CLIGHT;
+    const double ek = (wavno - 38454.691) / K_RYDBERG_HE;
+    const double eps = 2.0 * (ek - 2.47898) / 0.000780;
+    return 0.01521 * pow(470310.0 / wavno, 3.12) * 8.067e-18 * ipow(eps - 122.4, 2) / (1.0 + ipow(eps, 2));
+  }
+  return he_knots(tb->he2s3s_f, tb->he2s3s_x, freq);
+}
+
+/* HE12P1P (:13393-13440) */
+static double he12p1p(const orc_kapp_tables *tb, double freq) {
+  if (freq < 27175.76 * K_CLIGHT) return 0.0;
+  if (freq > 2.4 * K_RYDBERG_HE * K_CLIGHT) {
+    const double wavno = freq / K_CLIGHT;
+    const double ek = (wavno - 27175.76) / K_RYDBERG_HE;
+    const double eps1s = 2.0 * (ek - 2.446534) / 0.01037;
+    const double eps1d = 2.0 * (ek - 2.59427) / 0.00538;
+    return 0.0009487 * pow(466750.0 / wavno, 3.69) * 8.067e-18 *
+           (ipow(eps1s - 29.30, 2) / (1.0 + ipow(eps1s, 2)) + ipow(eps1d + 172.4, 2) / (1.0 + ipow(eps1d, 2)));
+  }
+  return he_knots(tb->he2p1p_f, tb->he2p1p_x, freq);
+}
+
+/* HE12P3P (:13443-13480) */
+static double he12p3p(const orc_kapp_tables *tb, double freq) {
+  if (freq < 29223.753 * K_CLIGHT) return 0.0;
+  return he_knots(tb->he2p3p_f, tb->he2p3p_x, freq);
+}
+
+/* HE1OP (:12939-13143) at one frequency, all depths, into ahe1[] */
+static void he1op(const orc_kapp_tables *tb, double freq, int nrhox, const double *t, const double *xne,
+                  const double *rho, const double *xnfp3, const double *xnf4, double *ahe1) {
+  const double ryd = K_RYDBERG_HE * K_CLIGHT;
+  const double freq3 = ipow(freq, 3);
+  const double cfree = K_COEFF_FF / freq3;
+  const double c = 2.815e29 / freq3;
+  int imin = 0;
+  for (int n = 1; n <= 10; ++n)
+    if (tb->he1_freq[n - 1] <= freq) {
+      imin = n;
+      break;
+    }
+  double trans[11] = {0};
+  if (imin > 0 && imin <= 1) trans[1] = orc_crosshe(tb, freq);
+  if (imin > 0 && imin <= 2) trans[2] = he12s3s(tb, freq);
+  if (imin > 0 && imin <= 3) trans[3] = he12s1s(tb, freq);
+  if (imin > 0 && imin <= 4) trans[4] = he12p3p(tb, freq);
+  if (imin > 0 && imin <= 5) trans[5] = he12p1p(tb, freq);
+  if (imin > 0 && imin <= 6) trans[6] = orc_xkarzas(tb, freq, 1.236439, 3, 0);
+  if (imin > 0 && imin <= 7) trans[7] = orc_xkarzas(tb, freq, 1.102898, 3, 0);
+  if (imin > 0 && imin <= 8) trans[8] = orc_xkarzas(tb, freq, 1.045499, 3, 1);
+  if (imin > 0 && imin <= 9) trans[9] = orc_xkarzas(tb, freq, 1.001427, 3, 2);
+  if (imin > 0 && imin <= 10) trans[10] = orc_xkarzas(tb, freq, 0.9926, 3, 1);
+  if (imin >= 1) {
+    /* inner shell to He II n = 2: 1s2p 1P, 1s2p 3P, 1s2s 1S, 1s2s 3S */
+    double elim = 527490.06, fhe;
+    fhe = (elim - 171135.000) * K_CLIGHT;
+    if (freq >= fhe) {
+      trans[5] = trans[5] + orc_xkarzas(tb, freq, fhe / ryd, 1, 0);
+      fhe = (elim - 169087.0) * K_CLIGHT;
+      if (freq >= fhe) {
+        trans[4] = trans[4] + orc_xkarzas(tb, freq, fhe / ryd, 1, 0);
+        fhe = (elim - 166277.546) * K_CLIGHT;
+        if (freq >= fhe) {
+          trans[3] = trans[3] + orc_xkarzas(tb, freq, fhe / ryd, 1, 0);
+          fhe = (elim - 159856.069) * K_CLIGHT;
+          if (freq >= fhe) trans[2] = trans[2] + orc_xkarzas(tb, freq, fhe / ryd, 1, 0);
+        }
+      }
+    }
+    /* inner shell to He II n = 3: levels 10, 9, 8, 7, 6 */
+    elim = 588451.59;
+    const double e3[5] = {186209.471, 186101.0, 185564.0, 184864.0, 183236.0};
+    for (int k = 0; k < 5; ++k) {
+      fhe = (elim - e3[k]) * K_CLIGHT;
+      if (!(freq >= fhe)) break;
+      trans[10 - k] = trans[10 - k] + orc_xkarzas(tb, freq, fhe / ryd, 1, 0);
+    }
+  }
+  double transn[28] = {0};
+  if (freq >= 1.25408e16)
+    for (int n = 4; n <= 27; ++n) transn[n] = orc_xkarzas(tb, freq, 4.0 - 3.0 / ipow((double)n, 2), 1, 0);
+  const double freqlg = log(freq);
+  for (int j = 0; j < nrhox; ++j) {
+    const double T = t[j], tkev = kbol_ev() * T, tlog = log(T);
+    const double hkt = K_HPLANCK / (K_KBOL * T);
+    const double ehvkt = exp(-freq * hkt), stim = 1.0 - ehvkt;
+    const double xr = xnfp3[j] * (4.0 / 2.0 / 13.595) * tkev / rho[j];
+    const double boltex = exp(-23.730 / tkev) * xr;
+    const double exlim = exp(-24.587 / tkev) * xr;
+    const double freet = xne[j] * xnf4[j] / rho[j] / sqrt(T);
+    double ex = boltex;
+    if (freq < 2.055e14) ex = exlim / ehvkt;
+    double he1 = (ex - exlim) * c;
+    if (imin > 0)
+      for (int n = imin; n <= 10; ++n) {
+        const double bolt = exp(-tb->he1_chi[n - 1] / tkev) * tb->he1_g[n - 1] * xnfp3[j] / rho[j];
+        he1 = he1 + trans[n] * bolt;
+      }
+    if (freq >= 1.25408e16)
+      for (int n = 4; n <= 27; ++n) {
+        const double boltn =
+            exp(-24.587 * (1.0 - 1.0 / ipow((double)n, 2)) / tkev) * 4.0 * ipow((double)n, 2) * xnfp3[j] / rho[j];
+        he1 = he1 + transn[n] * boltn;
+      }
+    ahe1[j] = (he1 + coulff(tb, freqlg, tlog, 0.0) * freet * cfree) * stim;
+  }
+}
+
+/* HE2OP (:13569-13674) at one frequency, all depths (AHE2 only: KAPP weights
+ * it by BNU, so SHE2 is not formed) */
+static void he2op(const orc_kapp_tables *tb, double freq, double waveno, int nrhox, const double *t,
+                  const double *xne, const double *rho, const double *xnfp4, const double *xnfp5, double *ahe2) {
+  /* levels n = 9..1: threshold (cm^-1), X's denominator n^5, g = 2n^2, E_n (cm^-1), Gaunt fit (none for n >= 7) */
+  static const double thr[9] = {5418.390, 6857.660, 8956.950, 12191.437, 17555.715,
+                                27430.925, 48766.491, 109726.529, 438908.850};
+  static const double g[9] = {162.0, 128.0, 98.0, 72.0, 50.0, 32.0, 18.0, 8.0, 2.0};
+  static const double en[9] = {433490.46, 432051.19, 429951.90, 426717.413, 421353.135,
+                               411477.925, 390142.359, 329182.321, 0.0};
+  static const double ga[9] = {0, 0, 0, 1.0986, 1.102, 1.101, 1.101, 1.105, 0.9916};
+  static const double gb[9] = {0, 0, 0, -2.704e13, -3.909e13, -5.765e13, -9.863e13, -2.375e14, 2.719e13};
+  static const double gc[9] = {0, 0, 0, 1.229e27, 2.371e27, 4.593e27, 1.035e28, 4.077e28, -2.268e30};
+  static const double den[9] = {59049.0, 32768.0, 16807.0, 7776.0, 3125.0, 1024.0, 243.0, 32.0, 1.0};
+  const double freq3 = 2.815e29 / freq / freq / freq;
+  const double freqlg = log(freq);
+  for (int j = 0; j < nrhox; ++j) {
+    const double T = t[j], tlog = log(T);
+    const double hkt = K_HPLANCK / (K_KBOL * T), hckt = hkt * K_CLIGHT;
+    const double stim = 1.0 - exp(-freq * hkt);
+    const double xnfprho = xnfp4[j] / rho[j];
+    double h = freq3 * 16.0 * 2.0 / 2.0 / (438889.068 * hckt) *
+               (exp(-fmax(434519.959, 438908.85 - waveno) * hckt) - exp(-438908.85 * hckt)) * stim * xnfprho;
+    for (int k = 0; k < 9; ++k) {
+      if (waveno < thr[k]) break;
+      double x;
+      if (k == 0) x = freq3 / den[k] * 16.0;
+      else if (k < 3) x = freq3 * 16.0 / den[k];
+      else x = freq3 * 16.0 / den[k] * (ga[k] + (gb[k] + gc[k] / freq) / freq);
+      const double a = k < 8 ? x * g[k] * exp(-en[k] * hckt) * stim * xnfprho : x * g[k] * stim * xnfprho;
+      h = h + a;
+    }
+    const double a = K_COEFF_FF * 4.0 / sqrt(T) * coulff(tb, freqlg, tlog, 0.60206) / freq * xne[j] / freq *
+                     xnfp5[j] / freq * stim / rho[j];
+    ahe2[j] = h + a;
+  }
+}
+
+/* HEMIOP (:13716-13833); wave in nm */
+static void hemiop(const orc_kapp_tables *tb, double wave, int nrhox, const double *t, const double *xne,
+                   const double *rho, const double *xnfp3, double *ahemin) {
+  double logw[17], logt[12], kt[12];
+  for (int i = 0; i < 17; ++i) logw[i] = log(tb->hem_w[i]);
+  for (int i = 0; i < 12; ++i) logt[i] = log(tb->hem_t[i]);
+  double wl = wave;
+  if (wl > tb->hem_w[16]) wl = tb->hem_w[16];
+  int iw = 1;
+  for (int i = 1; i <= 16; ++i)
+    if (wl >= tb->hem_w[i - 1]) iw = i;
+  const double xw = (log(wl) - logw[iw - 1]) / (logw[iw] - logw[iw - 1]);
+  for (int jt = 0; jt < 12; ++jt)
+    kt[jt] = log(tb->hem_k[jt * 17 + iw - 1]) * (1.0 - xw) + log(tb->hem_k[jt * 17 + iw]) * xw;
+  for (int j = 0; j < nrhox; ++j) {
+    int it = 1;
+    for (int i = 1; i <= 11; ++i)
+      if (t[j] >= tb->hem_t[i - 1]) it = i;
+    double xt = (log(fmax(t[j], 1.0)) - logt[it - 1]) / (logt[it] - logt[it - 1]);
+    xt = fmax(0.0, fmin(1.0, xt));
+    const double lkv = kt[it - 1] * (1.0 - xt) + kt[it] * xt;
+    ahemin[j] = exp(lkv) * xne[j] * K_KBOL * t[j] * xnfp3[j] / rho[j];
+  }
+}
+
+/* HERAOP (:13918-13941) */
+static double heraop_sig(double freq) {
+  const double w = K_CLIGHT_ANGS / fmin(freq, 5.15e15);
+  const double ww = ipow(w, 2);
+  return 5.484e-14 / ww / ww * ipow(1.0 + (2.44e5 + 5.94e10 / (ww - 2.90e5)) / ww, 2);
+}
+
+void orc_kapp(const orc_kapp_tables *tb, double wave, int nrhox, const double *t, const double *xne,
+              const double *rho, const double *xnfp1, const double *xnfp2, const double *xnfp3,
+              const double *xnfp4, const double *xnfp5, const double *xnf4, const double *bhyd, const double *bmin,
+              double *out) {
+  const double freq = K_CLIGHT_NMS / wave;
+  const double waveno = 1.0e7 / wave;
+  const double f3 = ipow(freq / 1.0e15, 3);
+  double *ahe1 = out + (size_t)ORC_KAPP_AHE1 * nrhox, *ahe2 = out + (size_t)ORC_KAPP_AHE2 * nrhox;
+  double *ahemin = out + (size_t)ORC_KAPP_AHEMIN * nrhox, *sighe = out + (size_t)ORC_KAPP_SIGHE * nrhox;
+  orc_kapp_hydrogen(tb, wave, nrhox, t, xne, rho, xnfp1, xnfp2, bhyd, bmin, out);
+  he1op(tb, freq, nrhox, t, xne, rho, xnfp3, xnf4, ahe1);
+  he2op(tb, freq, waveno, nrhox, t, xne, rho, xnfp4, xnfp5, ahe2);
+  hemiop(tb, wave, nrhox, t, xne, rho, xnfp3, ahemin);
+  const double sig = heraop_sig(freq);
+  for (int j = 0; j < nrhox; ++j) sighe[j] = sig * xnfp3[j] / rho[j];
+  /* KAPP's totals (:11300-11320) again, with the helium sources */
+  for (int j = 0; j < nrhox; ++j) {
+    const double hkt = K_HPLANCK / (K_KBOL * t[j]);
+    const double ehvkt = exp(-freq * hkt), stim = 1.0 - ehvkt;
+    const double bnu = bnu_prefac() * f3 * ehvkt / stim;
+    const double ahyd = out[(size_t)ORC_KAPP_AHYD * nrhox + j], shyd = out[(size_t)ORC_KAPP_SHYD * nrhox + j];
+    const double ahmin = out[(size_t)ORC_KAPP_AHMIN * nrhox + j], shmin = out[(size_t)ORC_KAPP_SHMIN * nrhox + j];
+    const double ah2p = out[(size_t)ORC_KAPP_AH2P * nrhox + j];
+    const double a = ah2p + ahe1[j] + ahe2[j] + ahemin[j] + 0.0 + 0.0 + 0.0;
+    const double acont = a + ahyd + ahmin;
+    double scont = bnu;
+    if (acont > 0.0) scont = (a * bnu + ahyd * shyd + ahmin * shmin) / acont;
+    out[(size_t)ORC_KAPP_ACONT * nrhox + j] = acont;
+    out[(size_t)ORC_KAPP_SCONT * nrhox + j] = scont;
+    out[(size_t)ORC_KAPP_SIGMAC * nrhox + j] =
+        out[(size_t)ORC_KAPP_SIGH * nrhox + j] + sighe[j] + out[(size_t)ORC_KAPP_SIGEL * nrhox + j] + 0.0 + 0.0;
   }
 }
 

@@ -345,11 +345,19 @@ typedef struct {
   const double *h2p_fr, *h2p_es;          /* H2PLOP's fits: FR coefficients [5], ES [6], signed */
   const double *ray_m, *ray_ab, *ray_bc, *ray_cd; /* GAVRILAM(74), AB(27), BC(24), CD(22) */
   const double *ray_ly, *ray_fly;         /* GAVRILALYMANCONT(64), FGAVRILALYMANCONT(64) */
+  /* helium */
+  const double *he1_chi, *he1_freq, *he1_g;                 /* HE1OP CHI(10), HEFREQ(10), G(10) */
+  const double *he_x505, *he_x50, *he_x20, *he_x10;         /* CROSSHE X505(92), X50(16), X20(11), X10(21) */
+  const double *he2s1s_f, *he2s1s_x, *he2s3s_f, *he2s3s_x;  /* HE12S1S, HE12S3S knots (16 each) */
+  const double *he2p1p_f, *he2p1p_x, *he2p3p_f, *he2p3p_x;  /* HE12P1P, HE12P3P knots (16 each) */
+  const double *hem_w, *hem_t, *hem_k;                      /* HEMIOP WHEM(17), THEM(12), KHEM(17,12) */
 } orc_kapp_tables;
 
 enum {
   ORC_KAPP_AHYD, ORC_KAPP_SHYD, ORC_KAPP_AH2P, ORC_KAPP_AHMIN, ORC_KAPP_SHMIN, ORC_KAPP_SIGH, ORC_KAPP_SIGEL,
-  ORC_KAPP_ACONT, ORC_KAPP_SCONT, ORC_KAPP_SIGMAC, ORC_KAPP_NOUT
+  ORC_KAPP_ACONT, ORC_KAPP_SCONT, ORC_KAPP_SIGMAC, ORC_KAPP_NOUT,
+  /* orc_kapp's helium rows after the ten above */
+  ORC_KAPP_AHE1 = ORC_KAPP_NOUT, ORC_KAPP_AHE2, ORC_KAPP_AHEMIN, ORC_KAPP_SIGHE, ORC_KAPP_NOUT_HE
 };
 
 double orc_occupation_prob(const orc_kapp_tables *tb, int n, double xne);
@@ -359,6 +367,14 @@ double orc_xkarzas(const orc_kapp_tables *tb, double freq, double zeff2, int n, 
 void orc_kapp_hydrogen(const orc_kapp_tables *tb, double wave, int nrhox, const double *t, const double *xne,
                        const double *rho, const double *xnfp1, const double *xnfp2, const double *bhyd,
                        const double *bmin, double *out);
+/* orc_kapp_hydrogen with the helium sources (HE1OP, HE2OP, HEMIOP, HERAOP):
+ * xnfp3..5 = XNFP(J,3..5), xnf4 = XNF(J,4); out[q * nrhox + j] for
+ * q < ORC_KAPP_NOUT_HE */
+void orc_kapp(const orc_kapp_tables *tb, double wave, int nrhox, const double *t, const double *xne,
+              const double *rho, const double *xnfp1, const double *xnfp2, const double *xnfp3,
+              const double *xnfp4, const double *xnfp5, const double *xnf4, const double *bhyd, const double *bmin,
+              double *out);
+double orc_crosshe(const orc_kapp_tables *tb, double freq);
 
 #ifdef __cplusplus
 }

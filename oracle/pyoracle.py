@@ -660,6 +660,9 @@ def synthe_hydrogen_opacity(recs, length, wbegin, ratio, wlend, velshift_kms, co
 
 # ---------------------------------------------------------------- KAPP (hydrogen sources)
 KAPP_NAMES = ("ahyd", "shyd", "ah2p", "ahmin", "shmin", "sigh", "sigel", "acont", "scont", "sigmac")
+KAPP_NAMES_HE = KAPP_NAMES + ("ahe1", "ahe2", "ahemin", "sighe")
+_KAPP_HE_TABLES = ("he1_chi", "he1_freq", "he1_g", "he_x505", "he_x50", "he_x20", "he_x10", "he2s1s_f", "he2s1s_x",
+                   "he2s3s_f", "he2s3s_x", "he2p1p_f", "he2p1p_x", "he2p3p_f", "he2p3p_x", "hem_w", "hem_t", "hem_k")
 
 
 class KappTables(ctypes.Structure):
@@ -667,7 +670,7 @@ class KappTables(ctypes.Structure):
     _fields_ = [(k, _fp) for k in ("freqn", "xn", "xl", "ekarzas")] + \
                [(k, _dp) for k in ("gff_logtab", "q_holtsmark", "hop_elev", "hmin_wbf", "hmin_bf", "hmin_thetaff",
                                    "hmin_wavek", "hmin_ff", "h2p_fr", "h2p_es", "ray_m", "ray_ab", "ray_bc", "ray_cd",
-                                   "ray_ly", "ray_fly")]
+                                   "ray_ly", "ray_fly") + _KAPP_HE_TABLES]
 
 
 def _lib_kapp():
@@ -680,6 +683,9 @@ def _lib_kapp():
                                   ctypes.c_int]
         L.orc_xkarzas.restype = ctypes.c_double
         L.orc_kapp_hydrogen.argtypes = [ctypes.POINTER(KappTables), ctypes.c_double, ctypes.c_int] + [_dp] * 8
+        L.orc_kapp.argtypes = [ctypes.POINTER(KappTables), ctypes.c_double, ctypes.c_int] + [_dp] * 12
+        L.orc_crosshe.argtypes = [ctypes.POINTER(KappTables), ctypes.c_double]
+        L.orc_crosshe.restype = ctypes.c_double
         L._kapp_declared = True
     return L
 
@@ -695,7 +701,7 @@ def kapp_tables(tables):
     keep["gff_logtab"] = np.empty_like(gff)
     L.orc_log10_array(_ptr(gff), _ptr(keep["gff_logtab"]), gff.size)
     for k in ("q_holtsmark", "hop_elev", "hmin_wbf", "hmin_bf", "hmin_thetaff", "hmin_wavek", "hmin_ff", "h2p_fr",
-              "h2p_es", "ray_m", "ray_ab", "ray_bc", "ray_cd", "ray_ly", "ray_fly"):
+              "h2p_es", "ray_m", "ray_ab", "ray_bc", "ray_cd", "ray_ly", "ray_fly") + _KAPP_HE_TABLES:
         keep[k] = _d(tables["k_" + k])
     kt = KappTables(*[_ptr(keep[n], _fp if t is _fp else _dp) for n, t in KappTables._fields_])
     kt._keep = keep
@@ -713,3 +719,22 @@ def kapp_hydrogen(kt, wave, t, xne, rho, xnfp1, xnfp2, bhyd=None, bmin=None):
     L.orc_kapp_hydrogen(ctypes.byref(kt), float(wave), nr, *[_ptr(a) for a in v],
                         _ptr(bh) if bh is not None else None, _ptr(bm) if bm is not None else None, _ptr(out))
     return dict(zip(KAPP_NAMES, out))
+
+
+def kapp(kt, wave, t, xne, rho, xnfp1, xnfp2, xnfp3, xnfp4, xnfp5, xnf4, bhyd=None, bmin=None):
+    """KAPP's hydrogen and helium sources and totals at one wavelength (nm):
+    dict of [nrhox] arrays (KAPP_NAMES_HE)."""
+    L = _lib_kapp()
+    nr = len(t)
+    out = np.zeros((len(KAPP_NAMES_HE), nr))
+    v = [_d(a) for a in (t, xne, rho, xnfp1, xnfp2, xnfp3, xnfp4, xnfp5, xnf4)]
+    bh = None if bhyd is None else _d(bhyd)
+    bm = None if bmin is None else _d(bmin)
+    L.orc_kapp(ctypes.byref(kt), float(wave), nr, *[_ptr(a) for a in v],
+               _ptr(bh) if bh is not None else None, _ptr(bm) if bm is not None else None, _ptr(out))
+    return dict(zip(KAPP_NAMES_HE, out))
+
+
+def crosshe(kt, freq):
+    """CROSSHE(FREQ): He I ground-state cross-section (cm^2)."""
+    return _lib_kapp().orc_crosshe(ctypes.byref(kt), float(freq))

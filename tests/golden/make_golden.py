@@ -243,6 +243,38 @@ def kapp_tables(mod, datadir):
     )
 
 
+def kapp_helium_tables(mod):
+    """KAPP's helium tables: HE1OP's level energies, threshold frequencies and
+    statistical weights, CROSSHE's Marr & West cross-sections, the 2s/2p fits
+    of HE12S1S, HE12S3S, HE12P1P, HE12P3P and HEMIOP's John (1994) free-free
+    table (atlas12_modules.f90:12939-13143, :13160-13236, :13299-13545,
+    :13716-13833)."""
+    def body(name):
+        return mod[mod.index(name):mod.index("END " + name)]
+    he1 = body("SUBROUTINE HE1OP")
+    cross = body("FUNCTION CROSSHE")
+    hem = body("SUBROUTINE HEMIOP")
+    out = dict(
+        k_he1_chi=fortran_array(he1, ":: CHI(10) =", 10),
+        k_he1_freq=fortran_array(he1, ":: HEFREQ(10) =", 10),
+        k_he1_g=fortran_array(he1, ":: G(10) =", 10),
+        k_he_x505=fortran_array(cross, ":: X505(92) =", 92),
+        k_he_x50=fortran_array(cross, ":: X50(16) =", 16),
+        k_he_x20=fortran_array(cross, ":: X20(11) =", 11),
+        k_he_x10=fortran_array(cross, ":: X10(21) =", 21),
+        k_hem_w=fortran_array(hem, ":: WHEM(NWHEM) =", 17),
+        k_hem_t=fortran_array(hem, ":: THEM(NTHEM) =", 12),
+        k_hem_k=fortran_array(hem, ":: KHEM(NWHEM, NTHEM) =", 17 * 12),  # [it][iw]
+    )
+    for fn, f, x in (("HE12S1S", "FREQ1S", "X1S"), ("HE12S3S", "FREQ3S", "X3S"),
+                     ("HE12P1P", "FREQ1P", "X1P"), ("HE12P3P", "FREQ3P", "X3P")):
+        src = body("FUNCTION " + fn)
+        key = fn[3:].lower()
+        out["k_he%s_f" % key] = fortran_array(src, ":: %s(16) =" % f, 16)
+        out["k_he%s_x" % key] = fortran_array(src, ":: %s(16) =" % x, 16)
+    return out
+
+
 def main():
     if not ROOT or not os.path.isdir(ROOT):
         sys.exit("usage: make_golden.py <reference_root>  (or ATLAS12_REFERENCE=<reference_root>)")
@@ -286,6 +318,7 @@ def main():
     out.update(synthe_hydrogen_tables(syn, mod))
     out["stehle_dims"] = stehle_dims(os.path.join(ROOT, "data"))
     out.update(kapp_tables(mod, os.path.join(ROOT, "data")))
+    out.update(kapp_helium_tables(mod))
     out["deck"], out["deck_pradk"] = read_deck(os.path.join(ROOT, "workdir", "ap00t5777g4.44at12.dat"))
     np.savez(os.path.join(HERE, "reference_tables.npz"), **out)
     np.savez(PACKAGE_DATA, **{k: v for k, v in out.items() if k not in TEST_ONLY})

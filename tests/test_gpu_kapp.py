@@ -1,7 +1,8 @@
-"""KAPP's hydrogen continuum sources on the GPU (atlasgpu_atlas_kapp_hydrogen,
-through the C ABI) against the CPU oracle (oracle/kapp.c), which restates
-HOP, XKARZAS, COULFF, H2PLOP, HMINOP, HRAYOP, ELECOP and KAPP's totals
-(atlas12_modules.f90:11202-12906, :17212-17222).
+"""KAPP's hydrogen and helium continuum sources on the GPU
+(atlasgpu_atlas_kapp_hydrogen and atlasgpu_atlas_kapp, through the C ABI)
+against the CPU oracle (oracle/kapp.c), which restates HOP, XKARZAS, COULFF,
+H2PLOP, HMINOP, HRAYOP, ELECOP, HE1OP, HE2OP, HEMIOP, HERAOP and KAPP's
+totals (atlas12_modules.f90:11202-13941, :17212-17222).
 
 Tolerance: relative 1e-10 per element of every source and total.  Both sides
 are FP64 (XKARZAS's REAL(4) interpolation in single precision, rounded as
@@ -28,6 +29,7 @@ pytestmark = pytest.mark.gpu
 
 RTOL = 1e-10
 NAMES = ("ahyd", "shyd", "ah2p", "ahmin", "shmin", "sigh", "sigel")
+NAMES_HE = NAMES + ("ahe1", "ahe2", "ahemin", "sighe")
 
 
 def atmosphere(teff, logg):
@@ -79,6 +81,74 @@ def test_kapp_hydrogen_matches_oracle(po, tables, kapp, teff, logg, nlte):
     # the padding depths nrhox..kw-1 are zero
     assert not np.any(ac[:, nr:]) and not np.any(sg[:, nr:]) and not np.any(sc[:, nr:])
     assert np.all(ac[:, :nr] > 0) and np.all(np.isfinite(sc[:, :nr]))
+
+
+def helium_atmosphere(teff, logg):
+    """atmosphere() with helium at 0.0851 of hydrogen by number, its
+    ionisation split by smooth functions of T."""
+    at = atmosphere(teff, logg)
+    t = at["t"]
+    e = surrogate.eos(t, surrogate.grey_model(teff, logg)["p"])
+    nhe = 0.0851 * e["nh"]
+    f1 = 1.0 / (1.0 + np.exp(-(t - 12000.0) / 1500.0))
+    f2 = 1.0 / (1.0 + np.exp(-(t - 22000.0) / 2500.0))
+    xnf4 = nhe * f1 * (1.0 - f2)
+    return dict(at, x3=nhe * (1.0 - f1), x4=xnf4 / 2.0, x5=nhe * f1 * f2, xnf4=xnf4)
+
+
+HE_EDGES = np.array([22.78, 50.43, 91.13, 205.06, 260.0, 312.1, 331.2, 342.2, 364.6, 569.6, 820.3, 1116.5, 1458.2,
+                     1845.6, 23.905, 1458.8, 506.441, 58.21])
+
+
+@pytest.mark.parametrize("teff,logg,nlte", [(15000.0, 4.0, False), (25000.0, 4.5, True), (6000.0, 4.0, False)])
+def test_kapp_helium_matches_oracle(po, tables, kapp, teff, logg, nlte):
+    at = helium_atmosphere(teff, logg)
+    nr, kw = at["t"].size, 80
+    ws, _ = synthetic.geometric_waveset(5.0, 300000.0, 600)
+    ws = np.sort(np.concatenate([ws, HE_EDGES * (1 - 1e-6), HE_EDGES * (1 + 1e-6)]))
+    bhyd = bmin = None
+    if nlte:
+        rng = np.random.default_rng(7)
+        bhyd = np.zeros((6, kw))
+        bhyd[:, :nr] = rng.uniform(0.7, 1.4, (6, nr))
+        bmin = np.zeros(kw)
+        bmin[:nr] = rng.uniform(0.8, 1.2, nr)
+    pops = (at["t"], at["xne"], at["rho"], at["x1"], at["x2"], at["x3"], at["x4"], at["x5"], at["xnf4"])
+    ac, sg, sc, parts = kapp.kapp(ws, *pops, bhyd=bhyd, bmin=bmin, kw=kw, parts=True)
+    kt = po.kapp_tables(tables)
+    worst = {}
+    for i, w in enumerate(ws):
+        ref = po.kapp(kt, w, *pops, None if bhyd is None else bhyd[:, :nr], None if bmin is None else bmin[:nr])
+        got = dict(acont=ac[i, :nr], sigmac=sg[i, :nr], scont=sc[i, :nr],
+                   **{k: parts[i, q, :nr] for q, k in enumerate(NAMES_HE)})
+        for k, v in got.items():
+            worst[k] = max(worst.get(k, 0.0), rel_err(v, ref[k]))
+    print("max relative error", worst)
+    assert max(worst.values()) <= RTOL, worst
+    assert not np.any(ac[:, nr:]) and not np.any(sg[:, nr:]) and not np.any(parts[:, :, nr:])
+    # the hydrogen sources are those of kapp_hydrogen, bit for bit; helium only adds
+    ach, sgh, sch, ph = kapp.kapp_hydrogen(ws, *pops[:5], bhyd=bhyd, bmin=bmin, kw=kw, parts=True)
+    np.testing.assert_array_equal(parts[:, :7], ph)
+    assert np.all(ac >= ach) and np.all(sg >= sgh)
+    if teff >= 15000.0:
+        assert np.max(parts[:, 7:11, :nr]) > 0 and np.max(ac - ach) > 0
+
+
+def test_kapp_helium_rejects_bad_input(gpu_ctx, tables, kapp):
+    at = helium_atmosphere(15000.0, 4.0)
+    ws = np.array([50.0, 500.0])
+    pops = [at[k] for k in ("t", "xne", "rho", "x1", "x2", "x3", "x4", "x5", "xnf4")]
+    bad = [p.copy() for p in pops]
+    bad[5][4] = np.inf
+    with pytest.raises(RuntimeError, match="non-finite"):
+        kapp.kapp(ws, *bad)
+    pp = _lib.KappPops(*[p.ctypes.data for p in pops[:5]], None, None, None, None, None, None)
+    out = [np.zeros((2, pops[0].size)) for _ in range(3)]
+    with pytest.raises(RuntimeError, match="bad argument"):
+        gpu_ctx.call("atlasgpu_atlas_kapp", 2, ws.ctypes.data, pops[0].size, pops[0].size, ctypes.byref(pp),
+                     *[o.ctypes.data for o in out], None)
+    ac, sg, sc = kapp.kapp(ws, *pops)
+    assert np.all(ac > 0)
 
 
 def test_kapp_hydrogen_rejects_bad_input(gpu_ctx, tables):
