@@ -90,6 +90,7 @@ SIGNATURES = {
     "atlasgpu_atlas_set_kapp_tables": (_I, [_P, _P]),
     "atlasgpu_atlas_kapp_hydrogen": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "atlasgpu_atlas_kapp": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _P]),
+    "atlasgpu_atlas_set_kapp_h2_tables": (_I, [_P, _P]),
     "atlasgpu_atlas_rt_pass": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _D,
                                     ctypes.POINTER(Accum), _P]),
     "atlasgpu_atlas_finish": (_I, [_P, ctypes.c_void_p, ctypes.POINTER(Accum), ctypes.POINTER(_D)]),
@@ -201,7 +202,38 @@ class KappTables(ctypes.Structure):
 class KappPops(ctypes.Structure):
     """atlasgpu_kapp_pops: the depth vectors of atlasgpu_atlas_kapp (addresses)."""
     _fields_ = [(k, ctypes.c_void_p) for k in ("t", "xne", "rho", "xnfp_h1", "xnfp_h2", "xnfp_he1", "xnfp_he2",
-                                               "xnfp_he3", "xnf_he2", "bhyd", "bmin")]
+                                               "xnfp_he3", "xnf_he2", "bhyd", "bmin", "xnf_he1")]
+
+
+class KappH2Tables(ctypes.Structure):
+    """atlasgpu_kapp_h2_tables: H2MINOP's table, PARTFNH2's values, H2COLLOP's
+    CIA grid (the two large arrays by address; from_tables keeps them alive)."""
+    _I32 = ctypes.c_int32
+    _fields_ = [("h2m_w", _D * 10), ("h2m_t", _D * 7), ("h2m_k", _D * 70), ("pf_n", _I32), ("pf_tstart", _D),
+                ("pf_tstep", _D), ("pf", ctypes.c_void_p), ("cia_nnu", _I32), ("cia_ntmax", _I32),
+                ("cia_nt", _I32 * 4), ("use_pair", _I32 * 4), ("cia_nu0", _D), ("cia_dnu", _D),
+                ("cia_temp", ctypes.c_void_p), ("cia_tab", ctypes.c_void_p)]
+
+    @classmethod
+    def from_tables(cls, t, use_pair=(1, 1, 1, 1)):
+        """From the k_h2m_*, k_pf_h2*, k_cia_* arrays of the reference tables."""
+        k = cls()
+        k.h2m_w[:] = [float(x) for x in np.asarray(t["k_h2m_w"]).ravel()]
+        k.h2m_t[:] = [float(x) for x in np.asarray(t["k_h2m_t"]).ravel()]
+        k.h2m_k[:] = [float(x) for x in np.asarray(t["k_h2m_k"]).ravel()]
+        pf = np.ascontiguousarray(t["k_pf_h2"], np.float64)
+        tpf = np.asarray(t["k_pf_h2_t"], np.float64)
+        temp = np.ascontiguousarray(t["k_cia_temp"], np.float64)
+        tab = np.ascontiguousarray(t["k_cia_tab"], np.float64)
+        grid = np.asarray(t["k_cia_grid"], np.float64)
+        k.pf_n, k.pf_tstart, k.pf_tstep, k.pf = pf.size, float(tpf[0]), float(tpf[1] - tpf[0]), pf.ctypes.data
+        k.cia_nnu, k.cia_ntmax = int(grid[0]), temp.shape[1]
+        k.cia_nt[:] = [int(x) for x in np.asarray(t["k_cia_nt"]).ravel()]
+        k.use_pair[:] = [int(bool(x)) for x in use_pair]
+        k.cia_nu0, k.cia_dnu = float(grid[1]), float(grid[2])
+        k.cia_temp, k.cia_tab = temp.ctypes.data, tab.ctypes.data
+        k._keep = (pf, temp, tab)
+        return k
 
 
 class StehleSeries(ctypes.Structure):

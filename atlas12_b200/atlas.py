@@ -115,15 +115,25 @@ class Atlas:
                       ptr(bm), *[ptr(o) for o in out], ptr(pt))
         return (*out, pt) if parts else tuple(out)
 
+    def set_kapp_h2_tables(self, tables, use_pair=(1, 1, 1, 1)):
+        """Keep KAPP's H2 tables (H2MINOP, PARTFNH2, H2COLLOP's CIA grid) on the
+        context; use_pair = USE_CIA_PAIR for H2-H2, H2-He, H2-H, H-He."""
+        t = _lib.KappH2Tables.from_tables(tables, use_pair)
+        self.ctx.call("atlasgpu_atlas_set_kapp_h2_tables", ctypes.byref(t))
+
     def kapp(self, waveset, t, xne, rho, xnfp1, xnfp2, xnfp3, xnfp4, xnfp5, xnf4, bhyd=None, bmin=None, kw=None,
-             parts=False):
+             parts=False, xnf3=None):
         """KAPP with the hydrogen sources of kapp_hydrogen and the helium ones
         (HE1OP, HE2OP, HEMIOP, HERAOP): (acont, sigmac, scont) [numnu, kw], and
         with parts=True also [numnu, 11, kw] (AHYD, SHYD, AH2P, AHMIN, SHMIN,
         SIGH, SIGEL, AHE1, AHE2, AHEMIN, SIGHE).  xnfp1..5 = XNFP(J,1..5),
-        xnf4 = XNF(J,4) (He II number density), each [nrhox]."""
+        xnf4 = XNF(J,4) (He II number density), each [nrhox].  With xnf3 =
+        XNF(J,3) (He I number density; set_kapp_h2_tables first) also the H2
+        sources (H2MINOP, H2COLLOP, H2RAOP), and parts [numnu, 14, kw] with
+        AH2MIN, AH2COLL, SIGH2 appended."""
         ws = np.ascontiguousarray(waveset, np.float64)
         vec = [np.ascontiguousarray(v, np.float64) for v in (t, xne, rho, xnfp1, xnfp2, xnfp3, xnfp4, xnfp5, xnf4)]
+        x3 = None if xnf3 is None else np.ascontiguousarray(xnf3, np.float64)
         nrhox = vec[0].size
         kw = nrhox if kw is None else int(kw)
         bh = None if bhyd is None else np.ascontiguousarray(bhyd, np.float64)
@@ -131,9 +141,9 @@ class Atlas:
             raise ValueError("bhyd must be [6, kw]")
         bm = None if bmin is None else np.ascontiguousarray(bmin, np.float64)
         pops = _lib.KappPops(*[v.ctypes.data for v in vec], None if bh is None else bh.ctypes.data,
-                             None if bm is None else bm.ctypes.data)
+                             None if bm is None else bm.ctypes.data, None if x3 is None else x3.ctypes.data)
         out = [np.zeros((ws.size, kw)) for _ in range(3)]
-        pt = np.zeros((ws.size, 11, kw)) if parts else None
+        pt = np.zeros((ws.size, 11 if x3 is None else 14, kw)) if parts else None
         self.ctx.call("atlasgpu_atlas_kapp", ws.size, ptr(ws), nrhox, kw, ctypes.byref(pops),
                       *[ptr(o) for o in out], ptr(pt))
         return (*out, pt) if parts else tuple(out)

@@ -25,7 +25,8 @@ struct atlasgpu_ctx {
   std::map<std::string, std::pair<void*, size_t>> bufs;
   atlasgpu::JoshOps* ops = nullptr;  // device
   bool ops_set = false;
-  bool kapp_set = false;  // atlasgpu_atlas_set_kapp_tables done
+  bool kapp_set = false;     // atlasgpu_atlas_set_kapp_tables done
+  bool kapp_h2_set = false;  // atlasgpu_atlas_set_kapp_h2_tables done
   int nsm = 148;
   size_t smem_optin = 0;
   // SELECTLINES tables (atlasgpu_atlas_select_tables)

@@ -1,6 +1,7 @@
-// api_kapp.cu -- C-ABI entry points of KAPP's hydrogen and helium continuum
-// sources (atlas12_modules.f90:11202-11324 with HOP, H2PLOP, HMINOP, HRAYOP,
-// ELECOP, HE1OP, HE2OP, HEMIOP, HERAOP; kernels in kapp.cuh).
+// api_kapp.cu -- C-ABI entry points of KAPP's hydrogen, helium and H2
+// continuum sources (atlas12_modules.f90:11202-11324 with HOP, H2PLOP, HMINOP,
+// HRAYOP, ELECOP, HE1OP, HE2OP, HEMIOP, HERAOP, H2MINOP, H2COLLOP, H2RAOP;
+// kernels in kapp.cuh).
 #include <cmath>
 #include <vector>
 
@@ -112,6 +113,88 @@ int atlasgpu_atlas_set_kapp_tables(atlasgpu_ctx* ctx, const atlasgpu_kapp_tables
   return 0;
 }
 
+int atlasgpu_atlas_set_kapp_h2_tables(atlasgpu_ctx* ctx, const atlasgpu_kapp_h2_tables* t) {
+  if (!ctx || !t) return fail(ctx, ATLASGPU_EINVAL, "set_kapp_h2_tables: null argument");
+  if (t->pf_n < 3 || t->pf_n > 100000 || !t->pf || !(t->pf_tstep > 0.0) || !std::isfinite(t->pf_tstart) ||
+      t->cia_nnu < 2 || t->cia_ntmax < 2 || !t->cia_temp || !t->cia_tab || !(t->cia_dnu > 0.0) ||
+      !std::isfinite(t->cia_nu0) || (size_t)t->cia_nnu * t->cia_ntmax * 4 > ((size_t)1 << 27))
+    return fail(ctx, ATLASGPU_EINVAL, "set_kapp_h2_tables: bad sizes (pf_n %d, cia %d x %d)", t->pf_n, t->cia_ntmax,
+                t->cia_nnu);
+  for (int p = 0; p < 4; ++p)
+    if (t->cia_nt[p] < 2 || t->cia_nt[p] > t->cia_ntmax)
+      return fail(ctx, ATLASGPU_EINVAL, "set_kapp_h2_tables: pair %d has %d temperatures", p + 1, t->cia_nt[p]);
+  const size_t ntab = (size_t)4 * t->cia_ntmax * t->cia_nnu;
+  if (!finite_all(t->h2m_w, 10) || !finite_all(t->h2m_t, 7) || !finite_all(&t->h2m_k[0][0], 70) ||
+      !finite_all(t->pf, t->pf_n) || !finite_all(t->cia_temp, (size_t)4 * t->cia_ntmax) ||
+      !finite_all(t->cia_tab, ntab))
+    return fail(ctx, ATLASGPU_ENONFINITE, "set_kapp_h2_tables: non-finite table entry");
+  for (int i = 0; i < 70; ++i)
+    if (!((&t->h2m_k[0][0])[i] > 0.0)) return fail(ctx, ATLASGPU_EINVAL, "set_kapp_h2_tables: KH2M entry not positive");
+  for (int i = 0; i < 10; ++i)
+    if (!(t->h2m_w[i] > 0.0) || (i > 0 && !(t->h2m_w[i] > t->h2m_w[i - 1])))
+      return fail(ctx, ATLASGPU_EINVAL, "set_kapp_h2_tables: WH2M not positive and increasing");
+  for (int i = 0; i < 7; ++i)
+    if (!(t->h2m_t[i] > 0.0) || (i > 0 && !(t->h2m_t[i] > t->h2m_t[i - 1])))
+      return fail(ctx, ATLASGPU_EINVAL, "set_kapp_h2_tables: TH2M not positive and increasing");
+  for (int p = 0; p < 4; ++p)
+    for (int i = 1; i < t->cia_nt[p]; ++i)
+      if (!(t->cia_temp[(size_t)p * t->cia_ntmax + i] > t->cia_temp[(size_t)p * t->cia_ntmax + i - 1]))
+        return fail(ctx, ATLASGPU_EINVAL, "set_kapp_h2_tables: CIA temperatures of pair %d not increasing", p + 1);
+  std::vector<KappH2Dev> hv(1);
+  KappH2Dev& h = hv[0];
+  std::copy(t->h2m_w, t->h2m_w + 10, h.h2m_w);
+  std::copy(t->h2m_t, t->h2m_t + 7, h.h2m_t);
+  // H2MINOP's first call (:12650-12660): LOGW, LOGT, LOGK
+  for (int i = 0; i < 10; ++i) h.h2m_logw[i] = std::log(t->h2m_w[i]);
+  for (int i = 0; i < 7; ++i) h.h2m_logt[i] = std::log(t->h2m_t[i]);
+  for (int i = 0; i < 70; ++i) h.h2m_logk[i] = std::log((&t->h2m_k[0][0])[i]);
+  h.pf_n = t->pf_n;
+  h.pf_tstart = t->pf_tstart;
+  h.pf_tstep = t->pf_tstep;
+  h.cia_nnu = t->cia_nnu;
+  h.cia_ntmax = t->cia_ntmax;
+  for (int p = 0; p < 4; ++p) {
+    h.cia_nt[p] = t->cia_nt[p];
+    h.use_pair[p] = t->use_pair[p] ? 1 : 0;
+  }
+  h.cia_nu0 = t->cia_nu0;
+  h.cia_dnu = t->cia_dnu;
+  h.cia_numax = t->cia_nu0 + t->cia_dnu * (double)(t->cia_nnu - 1);  // CIANUMAX (:16408)
+  // EQUILH2's PARAMETERs (:22449-22455)
+  const double mh = 1.008 * kAmu;
+  h.equil_d0 = 36118.11 * (kHplanck * kClight / kKbol);
+  h.equil_pref = std::pow(2.0, 1.5) / 4.0 / std::pow(2.0 * kPi * mh * kKbol / (kHplanck * kHplanck), 1.5);
+  // PARTFNH2's natural cubic spline (:22370-22384)
+  const int n = t->pf_n;
+  std::vector<double> pf2(n, 0.0), cwk(n, 0.0);
+  const double* pf = t->pf;
+  for (int k = 2; k <= n - 1; ++k) {
+    pf2[k - 1] = (6.0 * (pf[k] - 2.0 * pf[k - 1] + pf[k - 2]) / (t->pf_tstep * t->pf_tstep) - pf2[k - 2]) /
+                 (4.0 - cwk[k - 2]);
+    cwk[k - 1] = 1.0 / (4.0 - cwk[k - 2]);
+  }
+  for (int k = n - 1; k >= 2; --k) pf2[k - 1] = pf2[k - 1] - cwk[k - 1] * pf2[k];
+  cudaSetDevice(ctx->device);
+  const size_t nd = 2 * (size_t)n + (size_t)4 * t->cia_ntmax + ntab;
+  double* d;
+  KappH2Dev* dh;
+  int r;
+  if ((r = bufT(ctx, "kapp_h2_data", nd, &d)) || (r = bufT(ctx, "kapp_h2_tab", 1, &dh))) return r;
+  h.pf = d;
+  h.pf2 = d + n;
+  h.cia_temp = d + 2 * (size_t)n;
+  h.cia_tab = d + 2 * (size_t)n + (size_t)4 * t->cia_ntmax;
+  CK(cudaMemcpyAsync((void*)h.pf, pf, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync((void*)h.pf2, pf2.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync((void*)h.cia_temp, t->cia_temp, (size_t)4 * t->cia_ntmax * sizeof(double),
+                     cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync((void*)h.cia_tab, t->cia_tab, ntab * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(dh, &h, sizeof h, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->kapp_h2_set = true;
+  return 0;
+}
+
 }  // extern "C"
 
 namespace {
@@ -122,6 +205,8 @@ int kapp_run(atlasgpu_ctx* ctx, const char* name, int numnu, const double* waves
              const atlasgpu_kapp_pops& pp, bool helium, double* acont, double* sigmac, double* scont, double* parts) {
   if (!ctx) return ATLASGPU_EINVAL;
   if (!ctx->kapp_set) return fail(ctx, ATLASGPU_ESTATE, "%s: tables not set", name);
+  const bool h2 = helium && pp.xnf_he1;
+  if (h2 && !ctx->kapp_h2_set) return fail(ctx, ATLASGPU_ESTATE, "%s: H2 tables not set", name);
   if (numnu < 1 || nrhox < 1 || kw < nrhox || !waveset || !pp.t || !pp.xne || !pp.rho || !pp.xnfp_h1 ||
       !pp.xnfp_h2 || !acont || !sigmac || !scont ||
       (helium && (!pp.xnfp_he1 || !pp.xnfp_he2 || !pp.xnfp_he3 || !pp.xnf_he2)))
@@ -132,7 +217,8 @@ int kapp_run(atlasgpu_ctx* ctx, const char* name, int numnu, const double* waves
   if (!finite_all(pp.t, nrhox) || !finite_all(pp.xne, nrhox) || !finite_all(pp.rho, nrhox) ||
       !finite_all(pp.xnfp_h1, nrhox) || !finite_all(pp.xnfp_h2, nrhox) || (pp.bmin && !finite_all(pp.bmin, nrhox)) ||
       (helium && (!finite_all(pp.xnfp_he1, nrhox) || !finite_all(pp.xnfp_he2, nrhox) ||
-                  !finite_all(pp.xnfp_he3, nrhox) || !finite_all(pp.xnf_he2, nrhox))))
+                  !finite_all(pp.xnfp_he3, nrhox) || !finite_all(pp.xnf_he2, nrhox))) ||
+      (h2 && !finite_all(pp.xnf_he1, nrhox)))
     return fail(ctx, ATLASGPU_ENONFINITE, "%s: non-finite depth vector", name);
   for (int j = 0; j < nrhox; ++j)
     if (!(pp.t[j] > 0.0) || !(pp.rho[j] > 0.0))
@@ -143,16 +229,16 @@ int kapp_run(atlasgpu_ctx* ctx, const char* name, int numnu, const double* waves
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
   const size_t nt = (size_t)numnu * kw;
-  const int nparts = helium ? 11 : 7;
+  const int nparts = h2 ? 14 : (helium ? 11 : 7);
   double *d_ws, *d_in, *d_dep, *d_out, *d_parts = nullptr;
   int r;
-  // inputs: T, XNE, RHO, XNFP1, XNFP2, BMIN [kw], BHYD [6][kw], XNFP3..5, XNF4 [kw]
-  const size_t ndep = (size_t)(6 + 2 * kHLev + 9 + 10 + 24 + 3) * kw;
-  if ((r = bufT(ctx, "kp_ws", numnu, &d_ws)) || (r = bufT(ctx, "kp_in", (size_t)16 * kw, &d_in)) ||
+  // inputs: T, XNE, RHO, XNFP1, XNFP2, BMIN [kw], BHYD [6][kw], XNFP3..5, XNF4, XNF3 [kw]
+  const size_t ndep = (size_t)(6 + 2 * kHLev + 9 + 10 + 24 + 3 + 14) * kw;
+  if ((r = bufT(ctx, "kp_ws", numnu, &d_ws)) || (r = bufT(ctx, "kp_in", (size_t)17 * kw, &d_in)) ||
       (r = bufT(ctx, "kp_dep", ndep, &d_dep)) || (r = bufT(ctx, "kp_out", 3 * nt, &d_out)) ||
       (parts && (r = bufT(ctx, "kp_parts", (size_t)nparts * nt, &d_parts))))
     return r;
-  CK(cudaMemsetAsync(d_in, 0, (size_t)16 * kw * sizeof(double), s));
+  CK(cudaMemsetAsync(d_in, 0, (size_t)17 * kw * sizeof(double), s));
   CK(cudaMemcpyAsync(d_ws, waveset, numnu * sizeof(double), cudaMemcpyHostToDevice, s));
   const double* src[5] = {pp.t, pp.xne, pp.rho, pp.xnfp_h1, pp.xnfp_h2};
   for (int q = 0; q < 5; ++q)
@@ -165,6 +251,7 @@ int kapp_run(atlasgpu_ctx* ctx, const char* name, int numnu, const double* waves
     for (int q = 0; q < 4; ++q)
       CK(cudaMemcpyAsync(d_in + (size_t)(12 + q) * kw, hsrc[q], nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
   }
+  if (h2) CK(cudaMemcpyAsync(d_in + (size_t)16 * kw, pp.xnf_he1, nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(d_out, 0, 3 * nt * sizeof(double), s));
   if (d_parts) CK(cudaMemsetAsync(d_parts, 0, (size_t)nparts * nt * sizeof(double), s));
   KappArgs a{};
@@ -186,6 +273,10 @@ int kapp_run(atlasgpu_ctx* ctx, const char* name, int numnu, const double* waves
     a.xnfp5 = d_in + 14 * kw;
     a.xnf4 = d_in + 15 * kw;
   }
+  if (h2) {
+    a.xnf3 = d_in + 16 * kw;
+    a.h2 = (const KappH2Dev*)ctx->bufs["kapp_h2_tab"].first;
+  }
   double* p = d_dep;
   double** dv[6] = {&a.d.hkt, &a.d.hckt, &a.d.tkev, &a.d.tlog, &a.d.theta, &a.d.xhmin};
   for (int q = 0; q < 6; ++q) {
@@ -205,6 +296,12 @@ int kapp_run(atlasgpu_ctx* ctx, const char* name, int numnu, const double* waves
   a.d.he_freet = p;
   a.d.he_boltex = p + kw;
   a.d.he_exlim = p + 2 * kw;
+  p += (size_t)3 * kw;
+  a.d.xnh2m = p;
+  a.d.xnh2 = p + kw;
+  a.d.ciaden = p + 2 * kw;
+  a.d.ciait = p + 6 * kw;
+  a.d.ciawt = p + 10 * kw;
   a.acont = d_out;
   a.sigmac = d_out + nt;
   a.scont = d_out + 2 * nt;
@@ -215,10 +312,12 @@ int kapp_run(atlasgpu_ctx* ctx, const char* name, int numnu, const double* waves
     k_kapp_depth<<<(nrhox + 127) / 128, 128, 0, s>>>(a);
     CKL(ctx);
     const int blocks = std::min((numnu + kKappWarps - 1) / kKappWarps, ctx->nsm * 8);
-    if (helium)
-      k_kapp_nu<true><<<blocks, kKappWarps * 32, 0, s>>>(a);
+    if (h2)
+      k_kapp_nu<true, true><<<blocks, kKappWarps * 32, 0, s>>>(a);
+    else if (helium)
+      k_kapp_nu<true, false><<<blocks, kKappWarps * 32, 0, s>>>(a);
     else
-      k_kapp_nu<false><<<blocks, kKappWarps * 32, 0, s>>>(a);
+      k_kapp_nu<false, false><<<blocks, kKappWarps * 32, 0, s>>>(a);
     CKL(ctx);
   }
   CK(cudaMemcpyAsync(acont, a.acont, nt * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -1,4 +1,4 @@
-// kapp.cuh -- KAPP's hydrogen and helium continuum sources on the device (sm_100a).
+// kapp.cuh -- KAPP's hydrogen, helium and H2 continuum sources on the device (sm_100a).
 //
 // KAPP (atlas12_modules.f90:11202-11324) is called once per frequency inside
 // RUN_RT_PASS's loop and evaluates every source at every depth.  Here the
@@ -17,7 +17,10 @@
 //                 ELECOP (:17212-17222) and KAPP's totals; with helium
 //                 populations also HE1OP (:12939-13143, its cross-sections
 //                 per frequency on lanes), HE2OP (:13569-13674), HEMIOP
-//                 (:13716-13833) and HERAOP (:13918-13941).
+//                 (:13716-13833) and HERAOP (:13918-13941); with the H2
+//                 tables also H2MINOP (:12611-12708), H2COLLOP (:16371-16527)
+//                 and H2RAOP (:17289-17338), their H2 densities from
+//                 EQUILH2 (:22437-22469) and PARTFNH2 (:22324-22418) per depth.
 // Every output is the reference's expression in its order; where the
 // reference evaluates a depth-only factor inside the frequency loop, the
 // factor is the same function of the same inputs.
@@ -40,6 +43,7 @@ constexpr double kHminusEA = 0.75419;
 constexpr double kBetaHM88 = 8.798905203085208e+14;
 constexpr double kRydbergHe = 109722.277609;
 constexpr double kClightAngs = 2.99792458e18;
+constexpr double kAmu = 1.66053906892e-24;
 constexpr double kLogBetaMin = -2.0, kLogBetaStep = 2.4825302042523617e-02;
 constexpr int kHLev = 80;  // HOP's NMAX_HLEVELS
 
@@ -62,13 +66,28 @@ struct KappDev {
   double hem_w[17], hem_t[12], hem_logw[17], hem_logt[12], hem_logk[12 * 17];
 };
 
+// the H2 tables on the device (set by atlasgpu_atlas_set_kapp_h2_tables):
+// H2MINOP's table and logs (LOGK(IW, IT) at it*10 + iw), PARTFNH2's values
+// and spline second derivatives, H2COLLOP's CIA grid (pf, pf2, cia_temp,
+// cia_tab point into the same allocation), EQUILH2's two constants
+struct KappH2Dev {
+  double h2m_w[10], h2m_t[7], h2m_logw[10], h2m_logt[7], h2m_logk[7 * 10];
+  int pf_n, cia_nnu, cia_ntmax, cia_nt[4], use_pair[4];
+  double pf_tstart, pf_tstep, cia_nu0, cia_dnu, cia_numax;
+  double equil_pref, equil_d0;  // EQUILH2's trans_prefactor and D0_over_kT_coeff
+  const double *pf, *pf2, *cia_temp, *cia_tab;
+};
+
 // per-depth factors (k_kapp_depth), each [kw]; w, bz: [kHLev][kw] (level n at
 // (n-1)*kw), bp: [9][kw] for the pseudo-continuum's n = 7..15; HE1OP's BOLT
-// [10][kw], BOLTN of n = 4..27 [24][kw], FREET, BOLTEX, EXLIM (helium only)
+// [10][kw], BOLTN of n = 4..27 [24][kw], FREET, BOLTEX, EXLIM (helium only);
+// H2MINOP's XNH2M, XNH2, H2COLLOP's CIADEN, CIAIT (as doubles), CIAWT [4][kw]
+// each (H2 only)
 struct KappDepth {
   double *hkt, *hckt, *tkev, *tlog, *theta, *xhmin;
   double *w, *bz, *bp;
   double *he_bolt, *he_boltn, *he_freet, *he_boltex, *he_exlim;
+  double *xnh2m, *xnh2, *ciaden, *ciait, *ciawt;
 };
 
 struct KappArgs {
@@ -77,10 +96,12 @@ struct KappArgs {
   const double* waveset;
   const double *t, *xne, *rho, *xnfp1, *xnfp2, *bhyd, *bmin;  // bhyd [6][kw], bmin [kw]; may be null
   const double *xnfp3, *xnfp4, *xnfp5, *xnf4;  // helium populations; xnfp3 null: no helium sources
+  const double* xnf3;                           // XNF(J,3); null: no H2 sources
+  const KappH2Dev* h2;
   KappDepth d;
   double *acont, *sigmac, *scont;  // [numnu][kw]
   double* parts;                   // [numnu][nparts][kw] or null
-  int nparts;                      // 7 (hydrogen) or 11 (with helium)
+  int nparts;                      // 7 (hydrogen), 11 (with helium) or 14 (with H2)
 };
 
 __host__ __device__ inline double kapp_kbol_ev() { return kKbol / kEvErg; }
@@ -405,6 +426,29 @@ __device__ __noinline__ double kapp_he2op(const KappDev& tb, double freq, double
   return H + A;
 }
 
+// H2COLLOP's sum over the pairs at one depth (:16510-16522): the wavenumber
+// interpolation of the two temperature rows that bracket the depth, then the
+// temperature interpolation, in log10
+__device__ __noinline__ double kapp_h2coll(const KappH2Dev* __restrict__ h, const double* __restrict__ ciaden,
+                                           const double* __restrict__ ciait, const double* __restrict__ ciawt, int kw,
+                                           int j, double rho, int inu, double delnu, double dlow) {
+  double s = 0.0;
+  for (int ip = 0; ip < 4; ++ip) {
+    if (!h->use_pair[ip]) continue;
+    const double den = ciaden[(size_t)ip * kw + j];
+    if (den <= 0.0) continue;
+    const int ic = (int)ciait[(size_t)ip * kw + j];
+    const double wt = ciawt[(size_t)ip * kw + j];
+    const double* r0 = h->cia_tab + ((size_t)ip * h->cia_ntmax + ic - 1) * h->cia_nnu + inu - 1;
+    const double* r1 = r0 + h->cia_nnu;
+    const double c0 = r0[0] * (1.0 - delnu) + r0[1] * delnu + dlow;
+    const double c1 = r1[0] * (1.0 - delnu) + r1[1] * delnu + dlow;
+    const double xlog = c0 * (1.0 - wt) + c1 * wt;
+    s = s + pow(10.0, xlog) * den / rho;
+  }
+  return s;
+}
+
 // per-depth factors; threads over depths
 static __global__ void k_kapp_depth(KappArgs a) {
   const KappDev& tb = *a.tb;
@@ -447,18 +491,51 @@ static __global__ void k_kapp_depth(KappArgs a) {
       a.d.he_boltex[j] = exp(-23.730 / tkev) * xr;
       a.d.he_exlim[j] = exp(-24.587 / tkev) * xr;
     }
+    if (a.xnf3) {
+      // PARTFNH2 (:22398-22416), EQUILH2, then H2MINOP's XNH2M (:12668-12673)
+      // and H2COLLOP's densities and temperature brackets (:16457-16481)
+      const KappH2Dev& h = *a.h2;
+      const double tt = fmin(h.pf_tstart + (double)(h.pf_n - 1) * h.pf_tstep, fmax(h.pf_tstart, T));
+      int n = (int)((tt - h.pf_tstart) / h.pf_tstep) + 1;
+      n = min(h.pf_n - 1, max(1, n));
+      const double frac = (tt - (h.pf_tstart + (double)(n - 1) * h.pf_tstep)) / h.pf_tstep;
+      const double q = (1.0 - frac) * h.pf[n - 1] + frac * h.pf[n] +
+                       (powi(1.0 - frac, 3) - (1.0 - frac)) * h.pf2[n - 1] * powi(h.pf_tstep, 2) / 6.0 +
+                       (powi(frac, 3) - frac) * h.pf2[n] * powi(h.pf_tstep, 2) / 6.0;
+      const double equil = q * h.equil_pref / pow(T, 1.5) * exp(h.equil_d0 / T);
+      const double bh1 = a.bhyd ? a.bhyd[j] : 1.0;
+      const double xnhi = a.xnfp1[j] * 2.0 * bh1;
+      a.d.xnh2m[j] = powi(a.xnfp1[j] * 2.0 * bh1, 2) * equil;
+      const double xnh2 = T <= 20000.0 ? powi(xnhi, 2) * equil : 0.0;
+      a.d.xnh2[j] = xnh2;
+      const double x3 = a.xnf3[j];
+      const double den[4] = {xnh2 * xnh2, xnh2 * x3, xnh2 * xnhi, xnhi * x3};
+#pragma unroll
+      for (int ip = 0; ip < 4; ++ip) {
+        const double* tp = h.cia_temp + ip * h.cia_ntmax;
+        const int nt = h.cia_nt[ip];
+        const double tcl = fmax(tp[0], fmin(tp[nt - 1], T));
+        int it = 1;
+        for (int i = 1; i <= nt - 1; ++i)
+          if (tcl >= tp[i - 1]) it = i;
+        a.d.ciaden[(size_t)ip * kw + j] = den[ip];
+        a.d.ciait[(size_t)ip * kw + j] = (double)it;
+        a.d.ciawt[(size_t)ip * kw + j] = (tcl - tp[it - 1]) / (tp[it] - tp[it - 1]);
+      }
+    }
   }
 }
 
 constexpr int kKappWarps = 8;  // warps per CTA of k_kapp_nu
 
 // warp per frequency (grid-stride), lanes over depths; kHelium adds the
-// helium sources (a separate instantiation keeps the hydrogen one lean)
-template <bool kHelium>
+// helium sources and kH2 (with kHelium) the H2 ones (separate instantiations
+// keep the hydrogen one lean)
+template <bool kHelium, bool kH2>
 static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) {
   __shared__ double s_xk[kKappWarps][kHLev + 1];
   __shared__ double s_fftt[kKappWarps][11];
-  __shared__ double s_he[kKappWarps][10 + 24 + 12];  // HE1OP's TRANS, TRANSN of n = 4..27; HEMIOP's KT
+  __shared__ double s_he[kKappWarps][10 + 24 + 12 + 7];  // HE1OP's TRANS, TRANSN of n = 4..27; HEMIOP's and H2MINOP's KT
   const KappDev& tb = *a.tb;
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int kw = a.kw;
@@ -469,6 +546,7 @@ static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) 
   double* trans = s_he[wid];
   double* transn = trans + 10;
   double* hem_kt = transn + 24;
+  double* h2m_kt = hem_kt + 12;
   constexpr bool helium = kHelium;
   for (int nu = blockIdx.x * kKappWarps + wid; nu < a.numnu; nu += gridDim.x * kKappWarps) {
     // RUN_RT_PASS's frequency quantities (:3907-3917)
@@ -518,6 +596,37 @@ static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) 
       const double w = kClightAngs / fmin(freq, 5.15e15);
       const double ww = powi(w, 2);
       sighe_x = 5.484e-14 / ww / ww * powi(1.0 + (2.44e5 + 5.94e10 / (ww - 2.90e5)) / ww, 2);
+    }
+    // H2 per frequency: H2MINOP's log k at this wavelength for its seven
+    // temperatures, H2RAOP's cross-section, H2COLLOP's wavenumber bracket
+    double sigh2_x = 0.0, cia_delnu = 0.0, cia_dlow = 0.0;
+    int cia_inu = 0;
+    bool cia_on = false;
+    if (kH2) {
+      const KappH2Dev& h = *a.h2;
+      double wl = wave;
+      if (wl > h.h2m_w[9]) wl = h.h2m_w[9];
+      int iw = 1;
+      for (int i = 1; i <= 9; ++i)
+        if (wl >= h.h2m_w[i - 1]) iw = i;
+      const double xw = (log(wl) - h.h2m_logw[iw - 1]) / (h.h2m_logw[iw] - h.h2m_logw[iw - 1]);
+      if (lane < 7) h2m_kt[lane] = h.h2m_logk[lane * 10 + iw - 1] * (1.0 - xw) + h.h2m_logk[lane * 10 + iw] * xw;
+      const double w = kClightAngs / fmin(freq, 2.922e15);
+      const double ww = powi(w, 2);
+      sigh2_x = (8.14e-13 + 1.28e-6 / ww + 1.61 / (ww * ww)) / (ww * ww);
+      if (!(waveno > h.cia_numax)) {
+        if (waveno <= h.cia_nu0) {
+          if (waveno > 0.0) {
+            cia_on = true;
+            cia_inu = 1;
+            cia_dlow = 2.0 * log10(waveno / h.cia_nu0);
+          }
+        } else {
+          cia_on = true;
+          cia_inu = min((int)((waveno - h.cia_nu0) / h.cia_dnu) + 1, h.cia_nnu - 1);
+          cia_delnu = (waveno - h.cia_nu0 - h.cia_dnu * (double)(cia_inu - 1)) / h.cia_dnu;
+        }
+      }
     }
     __syncwarp();
     for (int j = lane; j < a.nrhox; j += 32) {
@@ -608,15 +717,30 @@ static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) 
         ahemin = exp(lkv) * xne * kKbol * T * x3 / rho;
         sighe = sighe_x * x3 / rho;
       }
-      // KAPP's totals (:11300-11320); the metal, H2 and line sources are zero
-      const double av = ah2p + ahe1 + ahe2 + ahemin + 0.0 + 0.0 + 0.0;
+      // H2: H2MINOP (:12686-12704), H2COLLOP (:16483-16522), H2RAOP
+      double ah2min = 0.0, ah2coll = 0.0, sigh2 = 0.0;
+      if (kH2) {
+        const KappH2Dev& h = *a.h2;
+        int it = 1;
+        for (int i = 1; i <= 6; ++i)
+          if (T >= h.h2m_t[i - 1]) it = i;
+        double xt = (log(fmax(T, 1.0)) - h.h2m_logt[it - 1]) / (h.h2m_logt[it] - h.h2m_logt[it - 1]);
+        xt = fmax(0.0, fmin(1.0, xt));
+        const double lkv = h2m_kt[it - 1] * (1.0 - xt) + h2m_kt[it] * xt;
+        ah2min = exp(lkv) * xne * kKbol * T * a.d.xnh2m[j] / rho;
+        if (cia_on)
+          ah2coll = kapp_h2coll(a.h2, a.d.ciaden, a.d.ciait, a.d.ciawt, kw, j, rho, cia_inu, cia_delnu, cia_dlow);
+        sigh2 = sigh2_x * a.d.xnh2[j] / rho;
+      }
+      // KAPP's totals (:11300-11320); the metal and line sources are zero
+      const double av = ah2p + ahe1 + ahe2 + ahemin + ah2min + ah2coll + 0.0;
       const double acont = av + ahyd + ahmin;
       double scont = bnu;
       if (acont > 0.0) scont = (av * bnu + ahyd * shyd + ahmin * shmin) / acont;
       const size_t o = (size_t)nu * kw + j;
       a.acont[o] = acont;
       a.scont[o] = scont;
-      a.sigmac[o] = sigh + sighe + sigel + 0.0 + 0.0;
+      a.sigmac[o] = sigh + sighe + sigel + sigh2 + 0.0;
       if (a.parts) {
         double* p = a.parts + (size_t)nu * a.nparts * kw + j;
         p[0] = ahyd;
@@ -631,6 +755,11 @@ static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) 
           p[8 * kw] = ahe2;
           p[9 * kw] = ahemin;
           p[10 * kw] = sighe;
+        }
+        if (a.nparts > 11) {
+          p[11 * kw] = ah2min;
+          p[12 * kw] = ah2coll;
+          p[13 * kw] = sigh2;
         }
       }
     }

@@ -599,11 +599,20 @@ def kapp_rate(ctx, ops, W):
     A.kapp(*hargs)
     ms_he = ctx.kernel_ms("kapp")
     ctx.enable_timing(False)
+    # and with the H2 sources (H2MINOP, H2COLLOP, H2RAOP)
+    A.set_kapp_h2_tables(ops)
+    A.kapp(*hargs, xnf3=hargs[6])
+    ctx.enable_timing(True)
+    A.kapp(*hargs, xnf3=hargs[6])
+    ms_h2 = ctx.kernel_ms("kapp")
+    ctx.enable_timing(False)
     return {"frequencies": int(W["ws"].size), "depths": int(m["t"].size), "kernel_ms": ms,
             "evals_per_s": n / (ms * 1e-3) if ms > 0 else None,
             "sources": "HOP (n = 1..80), H2PLOP, HMINOP, HRAYOP, ELECOP and KAPP's totals",
             "with_helium": {"kernel_ms": ms_he, "evals_per_s": n / (ms_he * 1e-3) if ms_he > 0 else None,
-                            "sources": "the above and HE1OP, HE2OP, HEMIOP, HERAOP"}}
+                            "sources": "the above and HE1OP, HE2OP, HEMIOP, HERAOP"},
+            "with_helium_h2": {"kernel_ms": ms_h2, "evals_per_s": n / (ms_h2 * 1e-3) if ms_h2 > 0 else None,
+                               "sources": "the above and H2MINOP, H2COLLOP, H2RAOP"}}
 
 
 def hbm_peak():

@@ -399,17 +399,47 @@ typedef struct atlasgpu_kapp_pops {
   const double *xnfp_h1, *xnfp_h2;
   const double *xnfp_he1, *xnfp_he2, *xnfp_he3, *xnf_he2;
   const double *bhyd, *bmin; /* NULL for LTE, as for atlasgpu_atlas_kapp_hydrogen */
+  const double *xnf_he1;     /* XNF(J,3), the He I number density: non-NULL adds the H2 sources */
 } atlasgpu_kapp_pops;
+
+/* KAPP's H2 tables, as the reference reads them:
+ *   H2MINOP (atlas12_modules.f90:12611-12708): WH2M (nm), TH2M (K),
+ *     KH2M(10,7) (cm^4/dyn; the library takes the logs);
+ *   PARTFNH2 (:22324-22418): data/partfnh2.dat, Q(H2) at pf_tstart +
+ *     (n-1) pf_tstep, n = 1..pf_n (the library forms the cubic spline's
+ *     second derivatives as the reader does);
+ *   H2COLLOP (:16371-16527): data/h2collop.dat, log10 of the CIA
+ *     coefficients of the pairs H2-H2, H2-He, H2-H, H-He on the wavenumber
+ *     grid cia_nu0 + (i-1) cia_dnu, i = 1..cia_nnu: cia_temp [4][cia_ntmax]
+ *     (cia_nt[p] used), cia_tab [4][cia_ntmax][cia_nnu]; use_pair =
+ *     USE_CIA_PAIR. */
+typedef struct atlasgpu_kapp_h2_tables {
+  double h2m_w[10], h2m_t[7], h2m_k[7][10];
+  int32_t pf_n;
+  double pf_tstart, pf_tstep;
+  const double *pf;
+  int32_t cia_nnu, cia_ntmax, cia_nt[4], use_pair[4];
+  double cia_nu0, cia_dnu;
+  const double *cia_temp, *cia_tab;
+} atlasgpu_kapp_h2_tables;
+
+/* Keeps the H2 tables on the context for atlasgpu_atlas_kapp (pops->xnf_he1
+ * non-NULL). */
+int atlasgpu_atlas_set_kapp_h2_tables(atlasgpu_ctx *ctx, const atlasgpu_kapp_h2_tables *tables);
 
 /* KAPP (atlas12_modules.f90:11202-11324) with the hydrogen sources of
  * atlasgpu_atlas_kapp_hydrogen and the helium ones: HE1OP (:12939-13143: the
  * ten resolved levels with CROSSHE, the 2s/2p fits and XKARZAS for the n = 3
  * levels, the inner-shell thresholds to He II n = 2 and 3, n = 4..27, the
  * dissolved-level term, free-free), HE2OP (:13569-13674), HEMIOP
- * (:13716-13833), HERAOP (:13918-13941); ACONT, SCONT and SIGMAC as KAPP
- * forms them with the metal, H2 and line sources zero.  Outputs as for
- * atlasgpu_atlas_kapp_hydrogen; parts, if not NULL, [numnu][11][kw]: AHYD,
- * SHYD, AH2P, AHMIN, SHMIN, SIGH, SIGEL, AHE1, AHE2, AHEMIN, SIGHE. */
+ * (:13716-13833), HERAOP (:13918-13941); with pops->xnf_he1 also the H2
+ * sources H2MINOP (:12611-12708), H2COLLOP (:16371-16527) and H2RAOP
+ * (:17289-17338) with EQUILH2 (:22437-22469); ACONT, SCONT and SIGMAC as KAPP
+ * forms them with the metal and line sources (and without xnf_he1 the H2
+ * ones) zero.  Outputs as for atlasgpu_atlas_kapp_hydrogen; parts, if not
+ * NULL, [numnu][11][kw] (or [numnu][14][kw] with H2): AHYD, SHYD, AH2P,
+ * AHMIN, SHMIN, SIGH, SIGEL, AHE1, AHE2, AHEMIN, SIGHE (, AH2MIN, AH2COLL,
+ * SIGH2). */
 int atlasgpu_atlas_kapp(atlasgpu_ctx *ctx, int numnu, const double *waveset, int nrhox, int kw,
                         const atlasgpu_kapp_pops *pops, double *acont, double *sigmac, double *scont,
                         double *parts);

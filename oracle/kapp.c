@@ -20,6 +20,10 @@
  *   HE2OP                :13569-13674
  *   HEMIOP               :13716-13833
  *   HERAOP               :13918-13941
+ *   H2MINOP              :12611-12708
+ *   H2COLLOP             :16371-16527
+ *   H2RAOP               :17289-17338
+ *   PARTFNH2             :22324-22418, EQUILH2 :22437-22469
  * Constants from mod_constants (:315-464).  The tables come from the
  * reference's data files and DATA statements (tests/golden/make_golden.py).
  */
@@ -46,6 +50,7 @@
 #define K_LOG_BETA_STEP 2.4825302042523617e-02
 #define K_RYDBERG_HE 109722.277609
 #define K_CLIGHT_ANGS 2.99792458e18
+#define K_AMU 1.66053906892e-24
 
 static const double H_SERIES_LIMITS[15] = {109678.764, 27419.659, 12186.462, 6854.871, 4387.113,
                                            3046.604,   2238.320,  1713.713,  1354.044, 1096.776,
@@ -594,6 +599,139 @@ void orc_kapp(const orc_kapp_tables *tb, double wave, int nrhox, const double *t
     out[(size_t)ORC_KAPP_SCONT * nrhox + j] = scont;
     out[(size_t)ORC_KAPP_SIGMAC * nrhox + j] =
         out[(size_t)ORC_KAPP_SIGH * nrhox + j] + sighe[j] + out[(size_t)ORC_KAPP_SIGEL * nrhox + j] + 0.0 + 0.0;
+  }
+}
+
+/* ---- H2 ---- */
+
+/* PARTFNH2 (:22324-22418): natural cubic spline through the tabulated Q(T),
+ * its second derivatives formed as the reader forms them */
+double orc_partfnh2(const orc_kapp_h2_tables *h2, double t) {
+  const int npf = h2->pf_n;
+  const double *pf = h2->pf, tstart = h2->pf_tstart, tstep = h2->pf_tstep;
+  double pf2[512], cwk[512];
+  pf2[0] = 0.0;
+  pf2[npf - 1] = 0.0;
+  cwk[0] = 0.0;
+  for (int n = 2; n <= npf - 1; ++n) {
+    pf2[n - 1] = (6.0 * (pf[n] - 2.0 * pf[n - 1] + pf[n - 2]) / ipow(tstep, 2) - pf2[n - 2]) / (4.0 - cwk[n - 2]);
+    cwk[n - 1] = 1.0 / (4.0 - cwk[n - 2]);
+  }
+  for (int n = npf - 1; n >= 2; --n) pf2[n - 1] = pf2[n - 1] - cwk[n - 1] * pf2[n];
+  const double tt = fmin(tstart + (npf - 1) * tstep, fmax(tstart, t));
+  int n = (int)((tt - tstart) / tstep) + 1;
+  if (n > npf - 1) n = npf - 1;
+  if (n < 1) n = 1;
+  const double frac = (tt - (tstart + (n - 1) * tstep)) / tstep;
+  return (1.0 - frac) * pf[n - 1] + frac * pf[n] + (ipow(1.0 - frac, 3) - (1.0 - frac)) * pf2[n - 1] * ipow(tstep, 2) / 6.0 +
+         (ipow(frac, 3) - frac) * pf2[n] * ipow(tstep, 2) / 6.0;
+}
+
+/* EQUILH2 (:22437-22469): n(H2) / n(H I)^2 */
+double orc_equilh2(const orc_kapp_h2_tables *h2, double t) {
+  const double m_h = 1.008 * K_AMU;
+  const double d0 = 36118.11 * (K_HPLANCK * K_CLIGHT / K_KBOL);
+  const double pref = pow(2.0, 1.5) / 4.0 / pow(2.0 * K_PI * m_h * K_KBOL / (K_HPLANCK * K_HPLANCK), 1.5);
+  return orc_partfnh2(h2, t) * pref / pow(t, 1.5) * exp(d0 / t);
+}
+
+void orc_kapp_h2(const orc_kapp_tables *tb, const orc_kapp_h2_tables *h2, double wave, int nrhox, const double *t,
+                 const double *xne, const double *rho, const double *xnfp1, const double *xnfp2, const double *xnfp3,
+                 const double *xnfp4, const double *xnfp5, const double *xnf4, const double *xnf3, const double *bhyd,
+                 const double *bmin, double *out) {
+  const double freq = K_CLIGHT_NMS / wave;
+  const double waveno = 1.0e7 / wave;
+  const double f3 = ipow(freq / 1.0e15, 3);
+  orc_kapp(tb, wave, nrhox, t, xne, rho, xnfp1, xnfp2, xnfp3, xnfp4, xnfp5, xnf4, bhyd, bmin, out);
+  double *ah2min = out + (size_t)ORC_KAPP_AH2MIN * nrhox, *ah2coll = out + (size_t)ORC_KAPP_AH2COLL * nrhox;
+  double *sigh2 = out + (size_t)ORC_KAPP_SIGH2 * nrhox;
+  /* H2MINOP: log k at this wavelength for each tabulated temperature */
+  double logw[10], logt[7], kt[7];
+  for (int i = 0; i < 10; ++i) logw[i] = log(h2->h2m_w[i]);
+  for (int i = 0; i < 7; ++i) logt[i] = log(h2->h2m_t[i]);
+  double wl = wave;
+  if (wl > h2->h2m_w[9]) wl = h2->h2m_w[9];
+  int iw = 1;
+  for (int i = 1; i <= 9; ++i)
+    if (wl >= h2->h2m_w[i - 1]) iw = i;
+  const double xw = (log(wl) - logw[iw - 1]) / (logw[iw] - logw[iw - 1]);
+  for (int jt = 0; jt < 7; ++jt)
+    kt[jt] = log(h2->h2m_k[jt * 10 + iw - 1]) * (1.0 - xw) + log(h2->h2m_k[jt * 10 + iw]) * xw;
+  /* H2RAOP's cross-section */
+  const double w = K_CLIGHT_ANGS / fmin(freq, 2.922e15);
+  const double ww = ipow(w, 2);
+  const double sig = (8.14e-13 + 1.28e-6 / ww + 1.61 / (ww * ww)) / (ww * ww);
+  /* H2COLLOP's wavenumber bracket */
+  const double numax = h2->cia_nu0 + h2->cia_dnu * (double)(h2->cia_nnu - 1);
+  int cia = 0, inu = 1;
+  double delnu = 0.0, dlow = 0.0;
+  if (!(waveno > numax)) {
+    if (waveno <= h2->cia_nu0) {
+      if (waveno > 0.0) {
+        cia = 1;
+        dlow = 2.0 * log10(waveno / h2->cia_nu0);
+      }
+    } else {
+      cia = 1;
+      inu = (int)((waveno - h2->cia_nu0) / h2->cia_dnu) + 1;
+      if (inu > h2->cia_nnu - 1) inu = h2->cia_nnu - 1;
+      delnu = (waveno - h2->cia_nu0 - h2->cia_dnu * (double)(inu - 1)) / h2->cia_dnu;
+    }
+  }
+  for (int j = 0; j < nrhox; ++j) {
+    const double T = t[j];
+    const double bh1 = bhyd ? bhyd[j] : 1.0;
+    const double eq = orc_equilh2(h2, T);
+    const double xnh2m = ipow(xnfp1[j] * 2.0 * bh1, 2) * eq;
+    const double xnhi = xnfp1[j] * 2.0 * bh1;
+    const double xnh2 = T <= 20000.0 ? ipow(xnhi, 2) * eq : 0.0;
+    /* H2MINOP */
+    int it = 1;
+    for (int i = 1; i <= 6; ++i)
+      if (T >= h2->h2m_t[i - 1]) it = i;
+    double xt = (log(fmax(T, 1.0)) - logt[it - 1]) / (logt[it] - logt[it - 1]);
+    xt = fmax(0.0, fmin(1.0, xt));
+    ah2min[j] = exp(kt[it - 1] * (1.0 - xt) + kt[it] * xt) * xne[j] * K_KBOL * T * xnh2m / rho[j];
+    /* H2COLLOP */
+    const double den[4] = {xnh2 * xnh2, xnh2 * xnf3[j], xnh2 * xnhi, xnhi * xnf3[j]};
+    double a = 0.0;
+    if (cia)
+      for (int ip = 0; ip < 4; ++ip) {
+        if (!h2->use_pair[ip]) continue;
+        const double *tp = h2->cia_temp + (size_t)ip * h2->cia_ntmax;
+        const int nt = h2->cia_nt[ip];
+        const double tcl = fmax(tp[0], fmin(tp[nt - 1], T));
+        int ic = 1;
+        for (int i = 1; i <= nt - 1; ++i)
+          if (tcl >= tp[i - 1]) ic = i;
+        const double wt = (tcl - tp[ic - 1]) / (tp[ic] - tp[ic - 1]);
+        if (den[ip] <= 0.0) continue;
+        const double *tab = h2->cia_tab + (size_t)ip * h2->cia_ntmax * h2->cia_nnu;
+        const double c0 = tab[(size_t)(ic - 1) * h2->cia_nnu + inu - 1] * (1.0 - delnu) +
+                          tab[(size_t)(ic - 1) * h2->cia_nnu + inu] * delnu + dlow;
+        const double c1 = tab[(size_t)ic * h2->cia_nnu + inu - 1] * (1.0 - delnu) +
+                          tab[(size_t)ic * h2->cia_nnu + inu] * delnu + dlow;
+        a = a + pow(10.0, c0 * (1.0 - wt) + c1 * wt) * den[ip] / rho[j];
+      }
+    ah2coll[j] = a;
+    sigh2[j] = sig * xnh2 / rho[j];
+    /* KAPP's totals with the H2 sources */
+    const double hkt = K_HPLANCK / (K_KBOL * T);
+    const double ehvkt = exp(-freq * hkt), stim = 1.0 - ehvkt;
+    const double bnu = bnu_prefac() * f3 * ehvkt / stim;
+    const double ahyd = out[(size_t)ORC_KAPP_AHYD * nrhox + j], shyd = out[(size_t)ORC_KAPP_SHYD * nrhox + j];
+    const double ahmin = out[(size_t)ORC_KAPP_AHMIN * nrhox + j], shmin = out[(size_t)ORC_KAPP_SHMIN * nrhox + j];
+    const double av = out[(size_t)ORC_KAPP_AH2P * nrhox + j] + out[(size_t)ORC_KAPP_AHE1 * nrhox + j] +
+                      out[(size_t)ORC_KAPP_AHE2 * nrhox + j] + out[(size_t)ORC_KAPP_AHEMIN * nrhox + j] + ah2min[j] +
+                      ah2coll[j] + 0.0;
+    const double acont = av + ahyd + ahmin;
+    double scont = bnu;
+    if (acont > 0.0) scont = (av * bnu + ahyd * shyd + ahmin * shmin) / acont;
+    out[(size_t)ORC_KAPP_ACONT * nrhox + j] = acont;
+    out[(size_t)ORC_KAPP_SCONT * nrhox + j] = scont;
+    out[(size_t)ORC_KAPP_SIGMAC * nrhox + j] = out[(size_t)ORC_KAPP_SIGH * nrhox + j] +
+                                               out[(size_t)ORC_KAPP_SIGHE * nrhox + j] +
+                                               out[(size_t)ORC_KAPP_SIGEL * nrhox + j] + sigh2[j] + 0.0;
   }
 }
 

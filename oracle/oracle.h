@@ -376,6 +376,31 @@ void orc_kapp(const orc_kapp_tables *tb, double wave, int nrhox, const double *t
               double *out);
 double orc_crosshe(const orc_kapp_tables *tb, double freq);
 
+/* KAPP's H2 tables: H2MINOP's WH2M(10), TH2M(7), KH2M(10,7); PARTFNH2's
+ * partfnh2.dat (Q at pf_tstart + (n-1) pf_tstep); H2COLLOP's h2collop.dat
+ * (cia_temp [4][cia_ntmax], cia_tab [4][cia_ntmax][cia_nnu] log10) */
+typedef struct {
+  const double *h2m_w, *h2m_t, *h2m_k;
+  int pf_n;
+  double pf_tstart, pf_tstep;
+  const double *pf;
+  int cia_nnu, cia_ntmax;
+  const int *cia_nt, *use_pair;
+  double cia_nu0, cia_dnu;
+  const double *cia_temp, *cia_tab;
+} orc_kapp_h2_tables;
+
+enum { ORC_KAPP_AH2MIN = ORC_KAPP_NOUT_HE, ORC_KAPP_AH2COLL, ORC_KAPP_SIGH2, ORC_KAPP_NOUT_H2 };
+
+double orc_partfnh2(const orc_kapp_h2_tables *h2, double t);
+double orc_equilh2(const orc_kapp_h2_tables *h2, double t);
+/* orc_kapp with the H2 sources (H2MINOP, H2COLLOP, H2RAOP): xnf3 = XNF(J,3);
+ * out[q * nrhox + j] for q < ORC_KAPP_NOUT_H2 */
+void orc_kapp_h2(const orc_kapp_tables *tb, const orc_kapp_h2_tables *h2, double wave, int nrhox, const double *t,
+                 const double *xne, const double *rho, const double *xnfp1, const double *xnfp2, const double *xnfp3,
+                 const double *xnfp4, const double *xnfp5, const double *xnf4, const double *xnf3, const double *bhyd,
+                 const double *bmin, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -661,6 +661,7 @@ def synthe_hydrogen_opacity(recs, length, wbegin, ratio, wlend, velshift_kms, co
 # ---------------------------------------------------------------- KAPP (hydrogen sources)
 KAPP_NAMES = ("ahyd", "shyd", "ah2p", "ahmin", "shmin", "sigh", "sigel", "acont", "scont", "sigmac")
 KAPP_NAMES_HE = KAPP_NAMES + ("ahe1", "ahe2", "ahemin", "sighe")
+KAPP_NAMES_H2 = KAPP_NAMES_HE + ("ah2min", "ah2coll", "sigh2")
 _KAPP_HE_TABLES = ("he1_chi", "he1_freq", "he1_g", "he_x505", "he_x50", "he_x20", "he_x10", "he2s1s_f", "he2s1s_x",
                    "he2s3s_f", "he2s3s_x", "he2p1p_f", "he2p1p_x", "he2p3p_f", "he2p3p_x", "hem_w", "hem_t", "hem_k")
 
@@ -671,6 +672,15 @@ class KappTables(ctypes.Structure):
                [(k, _dp) for k in ("gff_logtab", "q_holtsmark", "hop_elev", "hmin_wbf", "hmin_bf", "hmin_thetaff",
                                    "hmin_wavek", "hmin_ff", "h2p_fr", "h2p_es", "ray_m", "ray_ab", "ray_bc", "ray_cd",
                                    "ray_ly", "ray_fly") + _KAPP_HE_TABLES]
+
+
+class KappH2Tables(ctypes.Structure):
+    """orc_kapp_h2_tables; keeps its arrays alive (built by kapp_h2_tables)."""
+    _ip = ctypes.POINTER(ctypes.c_int)
+    _fields_ = [("h2m_w", _dp), ("h2m_t", _dp), ("h2m_k", _dp), ("pf_n", ctypes.c_int), ("pf_tstart", ctypes.c_double),
+                ("pf_tstep", ctypes.c_double), ("pf", _dp), ("cia_nnu", ctypes.c_int), ("cia_ntmax", ctypes.c_int),
+                ("cia_nt", _ip), ("use_pair", _ip), ("cia_nu0", ctypes.c_double), ("cia_dnu", ctypes.c_double),
+                ("cia_temp", _dp), ("cia_tab", _dp)]
 
 
 def _lib_kapp():
@@ -686,6 +696,11 @@ def _lib_kapp():
         L.orc_kapp.argtypes = [ctypes.POINTER(KappTables), ctypes.c_double, ctypes.c_int] + [_dp] * 12
         L.orc_crosshe.argtypes = [ctypes.POINTER(KappTables), ctypes.c_double]
         L.orc_crosshe.restype = ctypes.c_double
+        L.orc_kapp_h2.argtypes = [ctypes.POINTER(KappTables), ctypes.POINTER(KappH2Tables), ctypes.c_double,
+                                  ctypes.c_int] + [_dp] * 13
+        for f in (L.orc_partfnh2, L.orc_equilh2):
+            f.argtypes = [ctypes.POINTER(KappH2Tables), ctypes.c_double]
+            f.restype = ctypes.c_double
         L._kapp_declared = True
     return L
 
@@ -733,6 +748,47 @@ def kapp(kt, wave, t, xne, rho, xnfp1, xnfp2, xnfp3, xnfp4, xnfp5, xnf4, bhyd=No
     L.orc_kapp(ctypes.byref(kt), float(wave), nr, *[_ptr(a) for a in v],
                _ptr(bh) if bh is not None else None, _ptr(bm) if bm is not None else None, _ptr(out))
     return dict(zip(KAPP_NAMES_HE, out))
+
+
+def kapp_h2_tables(tables, use_pair=(1, 1, 1, 1)):
+    """KappH2Tables from the k_h2m_*, k_pf_h2*, k_cia_* entries of the reference tables."""
+    _lib_kapp()
+    keep = dict(h2m_w=_d(tables["k_h2m_w"]), h2m_t=_d(tables["k_h2m_t"]), h2m_k=_d(tables["k_h2m_k"]),
+                pf=_d(tables["k_pf_h2"]), cia_temp=_d(tables["k_cia_temp"]), cia_tab=_d(tables["k_cia_tab"]),
+                cia_nt=np.ascontiguousarray(tables["k_cia_nt"], np.int32),
+                use_pair=np.ascontiguousarray(use_pair, np.int32))
+    tpf = np.asarray(tables["k_pf_h2_t"], np.float64)
+    grid = np.asarray(tables["k_cia_grid"], np.float64)
+    assert 3 <= keep["pf"].size <= 512
+    ip = ctypes.POINTER(ctypes.c_int)
+    h = KappH2Tables(_ptr(keep["h2m_w"]), _ptr(keep["h2m_t"]), _ptr(keep["h2m_k"]), keep["pf"].size, float(tpf[0]),
+                     float(tpf[1] - tpf[0]), _ptr(keep["pf"]), int(grid[0]), keep["cia_temp"].shape[1],
+                     keep["cia_nt"].ctypes.data_as(ip), keep["use_pair"].ctypes.data_as(ip), float(grid[1]),
+                     float(grid[2]), _ptr(keep["cia_temp"]), _ptr(keep["cia_tab"]))
+    h._keep = keep
+    return h
+
+
+def kapp_h2(kt, h2, wave, t, xne, rho, xnfp1, xnfp2, xnfp3, xnfp4, xnfp5, xnf4, xnf3, bhyd=None, bmin=None):
+    """KAPP's hydrogen, helium and H2 sources and totals at one wavelength
+    (nm): dict of [nrhox] arrays (KAPP_NAMES_H2)."""
+    L = _lib_kapp()
+    nr = len(t)
+    out = np.zeros((len(KAPP_NAMES_H2), nr))
+    v = [_d(a) for a in (t, xne, rho, xnfp1, xnfp2, xnfp3, xnfp4, xnfp5, xnf4, xnf3)]
+    bh = None if bhyd is None else _d(bhyd)
+    bm = None if bmin is None else _d(bmin)
+    L.orc_kapp_h2(ctypes.byref(kt), ctypes.byref(h2), float(wave), nr, *[_ptr(a) for a in v],
+                  _ptr(bh) if bh is not None else None, _ptr(bm) if bm is not None else None, _ptr(out))
+    return dict(zip(KAPP_NAMES_H2, out))
+
+
+def partfnh2(h2, t):
+    return _lib_kapp().orc_partfnh2(ctypes.byref(h2), float(t))
+
+
+def equilh2(h2, t):
+    return _lib_kapp().orc_equilh2(ctypes.byref(h2), float(t))
 
 
 def crosshe(kt, freq):

@@ -28,6 +28,11 @@ modified).  Writes tests/golden/reference_tables.npz with:
                  data/stark_profile.dat: h_propbm [7, 15, 5] (profile, beta, P), h_c,
                  h_d [7, 5]; XLINOP's hydrogen level energies h_eh (10) and ELIM_HI
                  h_elim (:19964-19975, :385)
+  k_*            KAPP's continuum tables (kapp_tables, kapp_helium_tables, kapp_h2_tables):
+                 the Karzas-Latter files, van Hoof's g_ff, Q_HOLTSMARK, HOP's level energies,
+                 HMINOP's, H2PLOP's and HRAYOP's DATA statements; HE1OP's levels, CROSSHE,
+                 the He I 2s/2p knots, HEMIOP's table; H2MINOP's table, data/partfnh2.dat
+                 and data/h2collop.dat
   deck           the reference's converged solar model (workdir/ap00t5777g4.44at12.dat,
                  Teff 5777 K, log g 4.44, 72 depths, iteration 45): READ DECK6
                  columns RHOX, T, P, XNE, ABROSS, ACCRAD, VTURB as printed, [72, 7],
@@ -36,8 +41,8 @@ modified).  Writes tests/golden/reference_tables.npz with:
 
 It also writes atlas12_b200/data/operators.npz: the subset that a caller
 passes to the library as its operator data (the JOSH operators and grids,
-TABVOIGT's table, WAVETAB, the SELECTLINES tables and both programs'
-hydrogen tables), the way a Fortran driver passes what BLOCKJ/BLOCKH and its
+TABVOIGT's table, WAVETAB, the SELECTLINES tables, both programs'
+hydrogen tables and KAPP's tables), the way a Fortran driver passes what BLOCKJ/BLOCKH and its
 DATA statements hold.  Test-only entries (the Weideman coefficients, the
 converged deck) stay in the fixture.
 
@@ -275,6 +280,59 @@ def kapp_helium_tables(mod):
     return out
 
 
+def kapp_h2_tables(mod, datadir):
+    """KAPP's H2 tables: H2MINOP's H2- free-free table (WH2M, TH2M, KH2M),
+    PARTFNH2's data/partfnh2.dat (T, Q pairs; the reader skips '#' and blank
+    lines) and H2COLLOP's data/h2collop.dat (log10 CIA coefficients of the
+    H2-H2, H2-He, H2-H and H-He pairs on a uniform wavenumber grid), read as
+    the reference reads them (atlas12_modules.f90:12611-12708, :22324-22418,
+    :16371-16527).  CIATAB is returned [pair][temperature][wavenumber] with
+    -99 past a pair's own temperature count, as the reader initialises it."""
+    h2m = mod[mod.index("SUBROUTINE H2MINOP"):mod.index("END SUBROUTINE H2MINOP")]
+    pf = []
+    for line in open(os.path.join(datadir, "partfnh2.dat")):
+        line = line.strip()
+        if not line or line.startswith("#"):
+            continue
+        t, q = line.split()[:2]
+        pf.append((float(t), float(q)))
+    pf = np.array(pf)
+    assert np.all(np.diff(pf[:, 0]) == pf[1, 0] - pf[0, 0]), "partfnh2.dat: T not uniform"
+    toks, names = [], []
+    lines = [l for l in open(os.path.join(datadir, "h2collop.dat")) if not l.startswith("#")]
+    npair, ntmax = (int(x) for x in lines[0].split()[:2])
+    ncianu, nu0, dnu = lines[1].split()[:3]
+    ncianu, nu0, dnu = int(ncianu), float(nu0), float(dnu)
+    temps = np.zeros((npair, ntmax))
+    tab = np.full((npair, ntmax, ncianu), -99.0)
+    nciat = np.zeros(npair, np.int32)
+    body = lines[2:]
+    ip = -1
+    for line in body:
+        if line[:1].isalpha():
+            ip += 1
+            name, n = line.split()[:2]
+            names.append(name)
+            nciat[ip] = int(n)
+            toks.append([])
+        else:
+            toks[ip].extend(float(x.replace("D", "e").replace("d", "e")) for x in line.split())
+    assert ip + 1 == npair == 4, (ip, npair)
+    for ip in range(npair):
+        n = nciat[ip]
+        v = np.array(toks[ip])
+        assert v.size == n + n * ncianu, (names[ip], v.size)
+        temps[ip, :n] = v[:n]
+        tab[ip, :n] = v[n:].reshape(n, ncianu)
+    return dict(
+        k_h2m_w=fortran_array(h2m, ":: WH2M(NWH2M) =", 10),
+        k_h2m_t=fortran_array(h2m, ":: TH2M(NTH2M) =", 7),
+        k_h2m_k=fortran_array(h2m, ":: KH2M(NWH2M, NTH2M) =", 70),  # [it][iw]
+        k_pf_h2=pf[:, 1], k_pf_h2_t=pf[:, 0],
+        k_cia_grid=np.array([ncianu, nu0, dnu]), k_cia_nt=nciat, k_cia_temp=temps, k_cia_tab=tab,
+    )
+
+
 def main():
     if not ROOT or not os.path.isdir(ROOT):
         sys.exit("usage: make_golden.py <reference_root>  (or ATLAS12_REFERENCE=<reference_root>)")
@@ -319,9 +377,10 @@ def main():
     out["stehle_dims"] = stehle_dims(os.path.join(ROOT, "data"))
     out.update(kapp_tables(mod, os.path.join(ROOT, "data")))
     out.update(kapp_helium_tables(mod))
+    out.update(kapp_h2_tables(mod, os.path.join(ROOT, "data")))
     out["deck"], out["deck_pradk"] = read_deck(os.path.join(ROOT, "workdir", "ap00t5777g4.44at12.dat"))
-    np.savez(os.path.join(HERE, "reference_tables.npz"), **out)
-    np.savez(PACKAGE_DATA, **{k: v for k, v in out.items() if k not in TEST_ONLY})
+    np.savez_compressed(os.path.join(HERE, "reference_tables.npz"), **out)
+    np.savez_compressed(PACKAGE_DATA, **{k: v for k, v in out.items() if k not in TEST_ONLY})
     for k, v in out.items():
         print(k, v.shape)
 

@@ -1,8 +1,9 @@
-"""KAPP's hydrogen and helium continuum sources on the GPU
+"""KAPP's hydrogen, helium and H2 continuum sources on the GPU
 (atlasgpu_atlas_kapp_hydrogen and atlasgpu_atlas_kapp, through the C ABI)
 against the CPU oracle (oracle/kapp.c), which restates HOP, XKARZAS, COULFF,
-H2PLOP, HMINOP, HRAYOP, ELECOP, HE1OP, HE2OP, HEMIOP, HERAOP and KAPP's
-totals (atlas12_modules.f90:11202-13941, :17212-17222).
+H2PLOP, HMINOP, HRAYOP, ELECOP, HE1OP, HE2OP, HEMIOP, HERAOP, H2MINOP,
+H2COLLOP, H2RAOP with PARTFNH2 and EQUILH2, and KAPP's totals
+(atlas12_modules.f90:11202-17338, :22324-22469).
 
 Tolerance: relative 1e-10 per element of every source and total.  Both sides
 are FP64 (XKARZAS's REAL(4) interpolation in single precision, rounded as
@@ -30,6 +31,7 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-10
 NAMES = ("ahyd", "shyd", "ah2p", "ahmin", "shmin", "sigh", "sigel")
 NAMES_HE = NAMES + ("ahe1", "ahe2", "ahemin", "sighe")
+NAMES_H2 = NAMES_HE + ("ah2min", "ah2coll", "sigh2")
 
 
 def atmosphere(teff, logg):
@@ -132,6 +134,66 @@ def test_kapp_helium_matches_oracle(po, tables, kapp, teff, logg, nlte):
     assert np.all(ac >= ach) and np.all(sg >= sgh)
     if teff >= 15000.0:
         assert np.max(parts[:, 7:11, :nr]) > 0 and np.max(ac - ach) > 0
+
+
+@pytest.mark.parametrize("teff,logg,nlte", [(3500.0, 5.0, False), (4500.0, 4.5, True), (9000.0, 4.0, False)])
+def test_kapp_h2_matches_oracle(po, tables, kapp, teff, logg, nlte):
+    kapp.set_kapp_h2_tables(tables)
+    at = helium_atmosphere(teff, logg)
+    nr, kw = at["t"].size, 80
+    xnf3 = at["x3"] * 1.0  # He I partition function 1
+    # 600 frequencies over 9 nm - 400 um (the CIA grid ends at 20,000 cm^-1 = 500 nm), plus points either side
+    # of H2MINOP's and the CIA grid's ends and H2RAOP's cap
+    ws, _ = synthetic.geometric_waveset(9.0, 400000.0, 600)
+    edges = np.array([500.14, 210057.25, 1e7 / 20000.0, 1e7 / 25.0, 102.6, 1e7 / 1012.5])
+    ws = np.sort(np.concatenate([ws, edges * (1 - 1e-6), edges * (1 + 1e-6)]))
+    bhyd = bmin = None
+    if nlte:
+        rng = np.random.default_rng(9)
+        bhyd = np.zeros((6, kw))
+        bhyd[:, :nr] = rng.uniform(0.7, 1.4, (6, nr))
+        bmin = np.zeros(kw)
+        bmin[:nr] = rng.uniform(0.8, 1.2, nr)
+    pops = (at["t"], at["xne"], at["rho"], at["x1"], at["x2"], at["x3"], at["x4"], at["x5"], at["xnf4"])
+    ac, sg, sc, parts = kapp.kapp(ws, *pops, bhyd=bhyd, bmin=bmin, kw=kw, parts=True, xnf3=xnf3)
+    kt, h2 = po.kapp_tables(tables), po.kapp_h2_tables(tables)
+    worst = {}
+    for i, w in enumerate(ws):
+        ref = po.kapp_h2(kt, h2, w, *pops, xnf3, None if bhyd is None else bhyd[:, :nr],
+                         None if bmin is None else bmin[:nr])
+        got = dict(acont=ac[i, :nr], sigmac=sg[i, :nr], scont=sc[i, :nr],
+                   **{k: parts[i, q, :nr] for q, k in enumerate(NAMES_H2)})
+        for k, v in got.items():
+            worst[k] = max(worst.get(k, 0.0), rel_err(v, ref[k]))
+    print("max relative error", worst)
+    assert max(worst.values()) <= RTOL, worst
+    assert not np.any(ac[:, nr:]) and not np.any(parts[:, :, nr:])
+    if teff < 5000.0:
+        assert np.max(parts[:, 11:14, :nr]) > 0
+
+
+def test_kapp_h2_requires_its_tables(gpu_ctx, tables):
+    fresh = _lib.Context(0, _lib.PREC_MIXED)
+    try:
+        a = atlas.Atlas(fresh, tables)
+        a.set_kapp_tables(tables)
+        at = helium_atmosphere(3500.0, 5.0)
+        pops = [at[k] for k in ("t", "xne", "rho", "x1", "x2", "x3", "x4", "x5", "xnf4")]
+        ws = np.array([1000.0, 5000.0])
+        with pytest.raises(RuntimeError, match="H2 tables not set"):
+            a.kapp(ws, *pops, xnf3=at["x3"])
+        t = dict(tables)
+        t["k_cia_tab"] = tables["k_cia_tab"].copy()
+        t["k_cia_tab"][1, 3, 17] = np.nan
+        with pytest.raises(RuntimeError, match="non-finite"):
+            a.set_kapp_h2_tables(t)
+        a.set_kapp_h2_tables(tables)
+        ac, sg, sc = a.kapp(ws, *pops, xnf3=at["x3"])
+        ac0, sg0, sc0 = a.kapp(ws, *pops)
+        # the H2 sources only add (to rounding: the two calls run different kernel instantiations)
+        assert np.all(ac >= ac0 * (1 - 1e-13)) and np.all(sg >= sg0 * (1 - 1e-13)) and np.any(ac > ac0 * (1 + 1e-6))
+    finally:
+        fresh.close()
 
 
 def test_kapp_helium_rejects_bad_input(gpu_ctx, tables, kapp):
