@@ -91,6 +91,8 @@ SIGNATURES = {
     "atlasgpu_atlas_kapp_hydrogen": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "atlasgpu_atlas_kapp": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _P]),
     "atlasgpu_atlas_set_kapp_h2_tables": (_I, [_P, _P]),
+    "atlasgpu_atlas_set_stehle_tables": (_I, [_P, _P]),
+    "atlasgpu_atlas_hlinop": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     "atlasgpu_atlas_rt_pass": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _D,
                                     ctypes.POINTER(Accum), _P]),
     "atlasgpu_atlas_finish": (_I, [_P, ctypes.c_void_p, ctypes.POINTER(Accum), ctypes.POINTER(_D)]),
@@ -183,7 +185,9 @@ class KappTables(ctypes.Structure):
                 ("he_x50", _D * 16), ("he_x20", _D * 11), ("he_x10", _D * 21)] + \
         [(k, _D * 16) for k in ("he2s1s_f", "he2s1s_x", "he2s3s_f", "he2s3s_x", "he2p1p_f", "he2p1p_x",
                                 "he2p3p_f", "he2p3p_x")] + \
-        [("hem_w", _D * 17), ("hem_t", _D * 12), ("hem_k", _D * 204)]
+        [("hem_w", _D * 17), ("hem_t", _D * 12), ("hem_k", _D * 204), ("gf_lyman", _D * 29),
+         ("gf_balmer", _D * 28), ("gf_paschen", _D * 27), ("gf_brackett", _D * 3), ("stark_knm", _D * 20),
+         ("stark_f", _D * 40)]
 
     @classmethod
     def from_tables(cls, t):
@@ -242,6 +246,27 @@ class StehleSeries(ctypes.Structure):
                 ("n_dens", ctypes.c_int32), ("density_grid", _D * 20), ("temp_grid", _D * 10),
                 ("log_dalpha_grid", _D * 60), ("max_dens_idx", ctypes.c_void_p), ("k_alpha", ctypes.c_void_p),
                 ("profiles", ctypes.c_void_p)]
+
+
+def stehle_array(stehle):
+    """(StehleSeries * 4) from 4 dicts as read_stehle / synthetic.stehle_tables
+    give them (None entries: not loaded), and the arrays it points into (keep
+    both alive while the library reads them)."""
+    st, keep = (StehleSeries * 4)(), []
+    for q, ser in enumerate(stehle):
+        if ser is None:
+            continue
+        arrs = [np.ascontiguousarray(ser["max_dens_idx"], np.int32), np.ascontiguousarray(ser["k_alpha"], np.float64),
+                np.ascontiguousarray(ser["profiles"], np.float64)]
+        keep += arrs
+        a = st[q]
+        a.n_lower, a.n_upper_min, a.n_upper_max = (int(ser[k]) for k in ("n_lower", "n_upper_min", "n_upper_max"))
+        a.n_dens = len(ser["density_grid"])
+        a.density_grid[:a.n_dens] = [float(x) for x in ser["density_grid"]]
+        a.temp_grid[:] = [float(x) for x in ser["temp_grid"]]
+        a.log_dalpha_grid[:] = [float(x) for x in ser["log_dalpha_grid"]]
+        a.max_dens_idx, a.k_alpha, a.profiles = (v.ctypes.data for v in arrs)
+    return st, keep
 
 
 class SyntheHydrogen(ctypes.Structure):

@@ -121,6 +121,29 @@ class Atlas:
         t = _lib.KappH2Tables.from_tables(tables, use_pair)
         self.ctx.call("atlasgpu_atlas_set_kapp_h2_tables", ctypes.byref(t))
 
+    def set_stehle_tables(self, stehle):
+        """The four Stehle series STARK_MMM reads (4 dicts as read_stehle or
+        synthetic.stehle_tables give, None entries not loaded); None: STARK's
+        analytic profile throughout."""
+        st, keep = (None, []) if stehle is None else _lib.stehle_array(stehle)
+        self.ctx.call("atlasgpu_atlas_set_stehle_tables", st)
+        del keep  # the library copied the tables
+
+    def hlinop(self, waveset, t, xne, rho, xnfp1, bhyd=None, kw=None):
+        """HLINOP's hydrogen line pseudo-continuum at every (frequency, depth):
+        (AHLINE, SHLINE) [numnu, kw].  bhyd [6, kw]: None for LTE."""
+        ws = np.ascontiguousarray(waveset, np.float64)
+        vec = [np.ascontiguousarray(v, np.float64) for v in (t, xne, rho, xnfp1)]
+        nrhox = vec[0].size
+        kw = nrhox if kw is None else int(kw)
+        bh = None if bhyd is None else np.ascontiguousarray(bhyd, np.float64)
+        if bh is not None and bh.shape != (6, kw):
+            raise ValueError("bhyd must be [6, kw]")
+        out = [np.zeros((ws.size, kw)) for _ in range(2)]
+        self.ctx.call("atlasgpu_atlas_hlinop", ws.size, ptr(ws), nrhox, kw, *[ptr(v) for v in vec], ptr(bh),
+                      *[ptr(o) for o in out])
+        return tuple(out)
+
     def kapp(self, waveset, t, xne, rho, xnfp1, xnfp2, xnfp3, xnfp4, xnfp5, xnf4, bhyd=None, bmin=None, kw=None,
              parts=False, xnf3=None):
         """KAPP with the hydrogen sources of kapp_hydrogen and the helium ones

@@ -16,8 +16,8 @@ import os
 
 from . import _lib
 
-LINOP_CANDIDATES = (8, 16, 32, 64)
-RT_CANDIDATES = (16, 32, 64, 128)
+LINOP_CANDIDATES = (16, 32, 64)
+RT_CANDIDATES = (32, 64, 128, 256)
 
 
 def cache_path():

@@ -27,6 +27,7 @@ struct atlasgpu_ctx {
   bool ops_set = false;
   bool kapp_set = false;     // atlasgpu_atlas_set_kapp_tables done
   bool kapp_h2_set = false;  // atlasgpu_atlas_set_kapp_h2_tables done
+  bool atlas_stehle = false;  // atlasgpu_atlas_set_stehle_tables loaded tables
   int nsm = 148;
   size_t smem_optin = 0;
   // SELECTLINES tables (atlasgpu_atlas_select_tables)
@@ -174,6 +175,11 @@ inline std::vector<float4> pack_voigt_f32(const double* h0, const double* h1, co
 
 // TABLOG (atlas12_modules.f90:2083-2086) for every INTEGER(2), index I + 32768, on the context
 int ensure_tablog(atlasgpu_ctx* ctx, double** out);
+
+// the four Stehle series to the device (api_synthe.cu): buffers named after
+// prefix, *out the StehleDev[4] array; who names the caller in errors
+int stehle_upload(atlasgpu_ctx* ctx, const atlasgpu_stehle_series* stehle, const char* prefix, const char* who,
+                  StehleDev** out);
 
 struct AtlasLine;
 int atlas_prep_lines(atlasgpu_ctx* ctx, const int32_t* d_ld, const int32_t* h_ld, int64_t n,

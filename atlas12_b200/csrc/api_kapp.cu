@@ -1,7 +1,7 @@
 // api_kapp.cu -- C-ABI entry points of KAPP's hydrogen, helium and H2
 // continuum sources (atlas12_modules.f90:11202-11324 with HOP, H2PLOP, HMINOP,
-// HRAYOP, ELECOP, HE1OP, HE2OP, HEMIOP, HERAOP, H2MINOP, H2COLLOP, H2RAOP;
-// kernels in kapp.cuh).
+// HRAYOP, ELECOP, HE1OP, HE2OP, HEMIOP, HERAOP, H2MINOP, H2COLLOP, H2RAOP)
+// and of HLINOP's hydrogen line pseudo-continuum; kernels in kapp.cuh.
 #include <cmath>
 #include <vector>
 
@@ -42,7 +42,9 @@ int atlasgpu_atlas_set_kapp_tables(atlasgpu_ctx* ctx, const atlasgpu_kapp_tables
       !finite_all(t->he2s1s_f, 16) || !finite_all(t->he2s1s_x, 16) || !finite_all(t->he2s3s_f, 16) ||
       !finite_all(t->he2s3s_x, 16) || !finite_all(t->he2p1p_f, 16) || !finite_all(t->he2p1p_x, 16) ||
       !finite_all(t->he2p3p_f, 16) || !finite_all(t->he2p3p_x, 16) || !finite_all(t->hem_w, 17) ||
-      !finite_all(t->hem_t, 12) || !finite_all(&t->hem_k[0][0], 12 * 17))
+      !finite_all(t->hem_t, 12) || !finite_all(&t->hem_k[0][0], 12 * 17) || !finite_all(t->gf_lyman, 29) ||
+      !finite_all(t->gf_balmer, 28) || !finite_all(t->gf_paschen, 27) || !finite_all(t->gf_brackett, 3) ||
+      !finite_all(&t->stark_knm[0][0], 20) || !finite_all(&t->stark_f[0][0], 40))
     return fail(ctx, ATLASGPU_ENONFINITE, "set_kapp_tables: non-finite table entry");
   for (int i = 0; i < 12 * 17; ++i)
     if (!((&t->hem_k[0][0])[i] > 0.0)) return fail(ctx, ATLASGPU_EINVAL, "set_kapp_tables: KHEM entry not positive");
@@ -86,6 +88,12 @@ int atlasgpu_atlas_set_kapp_tables(atlasgpu_ctx* ctx, const atlasgpu_kapp_tables
   std::copy(t->ray_ly, t->ray_ly + 64, k.ray_ly);
   std::copy(t->ray_fly, t->ray_fly + 64, k.ray_fly);
   std::copy(kSeriesLimits, kSeriesLimits + 15, k.series_limits);
+  std::copy(t->gf_lyman, t->gf_lyman + 29, k.gf_lyman);
+  std::copy(t->gf_balmer, t->gf_balmer + 28, k.gf_balmer);
+  std::copy(t->gf_paschen, t->gf_paschen + 27, k.gf_paschen);
+  std::copy(t->gf_brackett, t->gf_brackett + 3, k.gf_brackett);
+  std::copy(&t->stark_knm[0][0], &t->stark_knm[0][0] + 20, k.stark_knm);
+  std::copy(&t->stark_f[0][0], &t->stark_f[0][0] + 40, k.stark_f);
   std::copy(t->he1_chi, t->he1_chi + 10, k.he1_chi);
   std::copy(t->he1_freq, t->he1_freq + 10, k.he1_freq);
   std::copy(t->he1_g, t->he1_g + 10, k.he1_g);
@@ -351,6 +359,92 @@ int atlasgpu_atlas_kapp(atlasgpu_ctx* ctx, int numnu, const double* waveset, int
                         const atlasgpu_kapp_pops* pops, double* acont, double* sigmac, double* scont, double* parts) {
   if (!pops) return fail(ctx, ATLASGPU_EINVAL, "kapp: null populations");
   return kapp_run(ctx, "kapp", numnu, waveset, nrhox, kw, *pops, true, acont, sigmac, scont, parts);
+}
+
+int atlasgpu_atlas_set_stehle_tables(atlasgpu_ctx* ctx, const atlasgpu_stehle_series* stehle) {
+  if (!ctx) return ATLASGPU_EINVAL;
+  StehleDev* d;
+  int r = stehle_upload(ctx, stehle, "ak_stehle", "atlas_set_stehle_tables", &d);
+  if (r) return r;
+  ctx->atlas_stehle = stehle != nullptr;
+  return 0;
+}
+
+int atlasgpu_atlas_hlinop(atlasgpu_ctx* ctx, int numnu, const double* waveset, int nrhox, int kw, const double* t,
+                          const double* xne, const double* rho, const double* xnfp1, const double* bhyd,
+                          double* ahline, double* shline) {
+  if (!ctx) return ATLASGPU_EINVAL;
+  if (!ctx->kapp_set) return fail(ctx, ATLASGPU_ESTATE, "hlinop: tables not set");
+  if (numnu < 1 || nrhox < 1 || kw < nrhox || !waveset || !t || !xne || !rho || !xnfp1 || !ahline || !shline)
+    return fail(ctx, ATLASGPU_EINVAL, "hlinop: bad argument (numnu %d, nrhox %d, kw %d)", numnu, nrhox, kw);
+  for (int i = 0; i < numnu; ++i)
+    if (!(waveset[i] > 0.0) || !std::isfinite(waveset[i]))
+      return fail(ctx, ATLASGPU_EINVAL, "hlinop: WAVESET(%d) = %g", i + 1, waveset[i]);
+  if (!finite_all(t, nrhox) || !finite_all(xne, nrhox) || !finite_all(rho, nrhox) || !finite_all(xnfp1, nrhox))
+    return fail(ctx, ATLASGPU_ENONFINITE, "hlinop: non-finite depth vector");
+  for (int j = 0; j < nrhox; ++j)
+    if (!(t[j] > 0.0) || !(rho[j] > 0.0) || !(xne[j] > 0.0))
+      return fail(ctx, ATLASGPU_EINVAL, "hlinop: T, RHO or XNE not positive at depth %d", j + 1);
+  if (bhyd)
+    for (int n = 0; n < 6; ++n)
+      for (int j = 0; j < nrhox; ++j)
+        if (!std::isfinite(bhyd[(size_t)n * kw + j]) || !(bhyd[(size_t)n * kw + j] > 0.0))
+          return fail(ctx, ATLASGPU_EINVAL, "hlinop: BHYD(%d, %d) not positive", j + 1, n + 1);
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const size_t nt = (size_t)numnu * kw;
+  double *d_ws, *d_in, *d_dep, *d_out;
+  int r;
+  const size_t ndep = (size_t)(6 + 2 * kHLev + 9) * kw;
+  if ((r = bufT(ctx, "kp_ws", numnu, &d_ws)) || (r = bufT(ctx, "hl_in", (size_t)12 * kw, &d_in)) ||
+      (r = bufT(ctx, "hl_dep", ndep, &d_dep)) || (r = bufT(ctx, "hl_out", 2 * nt, &d_out)))
+    return r;
+  CK(cudaMemsetAsync(d_in, 0, (size_t)12 * kw * sizeof(double), s));
+  CK(cudaMemsetAsync(d_out, 0, 2 * nt * sizeof(double), s));
+  CK(cudaMemcpyAsync(d_ws, waveset, numnu * sizeof(double), cudaMemcpyHostToDevice, s));
+  const double* src[4] = {t, xne, rho, xnfp1};
+  for (int q = 0; q < 4; ++q)
+    CK(cudaMemcpyAsync(d_in + (size_t)q * kw, src[q], nrhox * sizeof(double), cudaMemcpyHostToDevice, s));
+  // XNFP(J,2) is not read by HLINOP; its slot stays zero
+  if (bhyd) CK(cudaMemcpyAsync(d_in + (size_t)6 * kw, bhyd, (size_t)6 * kw * sizeof(double), cudaMemcpyHostToDevice, s));
+  KappArgs a{};
+  a.tb = (const KappDev*)ctx->bufs["kapp_tab"].first;
+  a.numnu = numnu;
+  a.nrhox = nrhox;
+  a.kw = kw;
+  a.waveset = d_ws;
+  a.t = d_in;
+  a.xne = d_in + kw;
+  a.rho = d_in + 2 * kw;
+  a.xnfp1 = d_in + 3 * kw;
+  a.xnfp2 = d_in + 4 * kw;
+  a.bhyd = bhyd ? d_in + 6 * kw : nullptr;
+  double* p = d_dep;
+  double** dv[6] = {&a.d.hkt, &a.d.hckt, &a.d.tkev, &a.d.tlog, &a.d.theta, &a.d.xhmin};
+  for (int q = 0; q < 6; ++q) {
+    *dv[q] = p;
+    p += kw;
+  }
+  a.d.w = p;
+  p += (size_t)kHLev * kw;
+  a.d.bz = p;
+  p += (size_t)kHLev * kw;
+  a.d.bp = p;
+  a.ahline = d_out;
+  a.shline = d_out + nt;
+  a.stehle = ctx->atlas_stehle ? (const StehleDev*)ctx->bufs["ak_stehle"].first : nullptr;
+  {
+    Timer tm(ctx, "hlinop");
+    k_kapp_depth<<<(nrhox + 127) / 128, 128, 0, s>>>(a);
+    CKL(ctx);
+    const int blocks = std::min((numnu + kKappWarps - 1) / kKappWarps, ctx->nsm * 8);
+    k_hlinop<<<blocks, kKappWarps * 32, 0, s>>>(a);
+    CKL(ctx);
+  }
+  CK(cudaMemcpyAsync(ahline, a.ahline, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(shline, a.shline, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
 }
 
 }  // extern "C"

@@ -587,13 +587,15 @@ static int synthe_hydrogen_launch(atlasgpu_ctx* ctx, const atlasgpu_nlte_line* r
   return 0;
 }
 
-int atlasgpu_synthe_set_hydrogen_tables(atlasgpu_ctx* ctx, const atlasgpu_hydrogen_tables* tables,
-                                        const atlasgpu_stehle_series* stehle) {
-  if (!ctx || !tables) return fail(ctx, ATLASGPU_EINVAL, "synthe_set_hydrogen_tables: null argument");
-  for (int q = 0; q < 4; ++q)
-    if (tables->lnghal[q] < 1 || tables->lnghal[q] > 14 || tables->istal[q] < 1 ||
-        tables->istal[q] + tables->lnghal[q] - 1 > 34 || tables->lncomp[q] < 1 || tables->lncomp[q] > 5)
-      return fail(ctx, ATLASGPU_EINVAL, "synthe_set_hydrogen_tables: fine-structure index out of range");
+}  // extern "C"
+
+namespace atlasgpu {
+
+// The four Stehle series into device buffers named <prefix>_mdi<q>,
+// <prefix>_ka<q>, <prefix>_pr<q> and the StehleDev array <prefix> (NULL or a
+// series with n_dens 0: not loaded); *out the device array.  Validates first.
+int stehle_upload(atlasgpu_ctx* ctx, const atlasgpu_stehle_series* stehle, const char* prefix, const char* who,
+                  StehleDev** out) {
   StehleDev dev[4] = {};
   if (stehle) {
     for (int q = 0; q < 4; ++q) {
@@ -602,29 +604,27 @@ int atlasgpu_synthe_set_hydrogen_tables(atlasgpu_ctx* ctx, const atlasgpu_hydrog
       const int ntr = S.n_upper_max - S.n_upper_min + 1;
       if (S.n_lower != q + 1 || S.n_upper_min <= S.n_lower || ntr < 1 || S.n_upper_max > 100 || S.n_dens < 2 ||
           S.n_dens > 20 || !S.max_dens_idx || !S.k_alpha || !S.profiles)
-        return fail(ctx, ATLASGPU_EINVAL, "synthe_set_hydrogen_tables: Stehle series %d malformed", q + 1);
+        return fail(ctx, ATLASGPU_EINVAL, "%s: Stehle series %d malformed", who, q + 1);
       for (int t = 0; t < ntr; ++t)
         if (S.max_dens_idx[t] < 1 || S.max_dens_idx[t] > S.n_dens)
-          return fail(ctx, ATLASGPU_EINVAL, "synthe_set_hydrogen_tables: Stehle series %d density index", q + 1);
+          return fail(ctx, ATLASGPU_EINVAL, "%s: Stehle series %d density index", who, q + 1);
     }
   }
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
-  atlasgpu_hydrogen_tables* d_tab;
   StehleDev* d_st;
   int r;
-  if ((r = bufT(ctx, "sh_tab", 1, &d_tab)) || (r = bufT(ctx, "sh_stehle", 4, &d_st))) return r;
-  CK(cudaMemcpyAsync(d_tab, tables, sizeof *tables, cudaMemcpyHostToDevice, s));
+  if ((r = bufT(ctx, prefix, 4, &d_st))) return r;
   for (int q = 0; stehle && q < 4; ++q) {
     const atlasgpu_stehle_series& S = stehle[q];
     StehleDev& D = dev[q];
     if (S.n_dens == 0) continue;
     const int ntr = S.n_upper_max - S.n_upper_min + 1;
     const size_t np = (size_t)ntr * S.n_dens * 600;
-    char nm[3][24];
-    snprintf(nm[0], sizeof nm[0], "sh_st_mdi%d", q);
-    snprintf(nm[1], sizeof nm[1], "sh_st_ka%d", q);
-    snprintf(nm[2], sizeof nm[2], "sh_st_pr%d", q);
+    char nm[3][48];
+    snprintf(nm[0], sizeof nm[0], "%s_mdi%d", prefix, q);
+    snprintf(nm[1], sizeof nm[1], "%s_ka%d", prefix, q);
+    snprintf(nm[2], sizeof nm[2], "%s_pr%d", prefix, q);
     int32_t* d_mdi;
     double *d_ka, *d_pr;
     if ((r = bufT(ctx, nm[0], (size_t)ntr, &d_mdi)) || (r = bufT(ctx, nm[1], (size_t)ntr, &d_ka)) ||
@@ -646,6 +646,28 @@ int atlasgpu_synthe_set_hydrogen_tables(atlasgpu_ctx* ctx, const atlasgpu_hydrog
   }
   CK(cudaMemcpyAsync(d_st, dev, sizeof dev, cudaMemcpyHostToDevice, s));
   CK(cudaStreamSynchronize(s));
+  *out = d_st;
+  return 0;
+}
+
+}  // namespace atlasgpu
+
+extern "C" {
+
+int atlasgpu_synthe_set_hydrogen_tables(atlasgpu_ctx* ctx, const atlasgpu_hydrogen_tables* tables,
+                                        const atlasgpu_stehle_series* stehle) {
+  if (!ctx || !tables) return fail(ctx, ATLASGPU_EINVAL, "synthe_set_hydrogen_tables: null argument");
+  for (int q = 0; q < 4; ++q)
+    if (tables->lnghal[q] < 1 || tables->lnghal[q] > 14 || tables->istal[q] < 1 ||
+        tables->istal[q] + tables->lnghal[q] - 1 > 34 || tables->lncomp[q] < 1 || tables->lncomp[q] > 5)
+      return fail(ctx, ATLASGPU_EINVAL, "synthe_set_hydrogen_tables: fine-structure index out of range");
+  StehleDev* d_st;
+  int r;
+  if ((r = stehle_upload(ctx, stehle, "sh_stehle", "synthe_set_hydrogen_tables", &d_st))) return r;
+  atlasgpu_hydrogen_tables* d_tab;
+  if ((r = bufT(ctx, "sh_tab", 1, &d_tab))) return r;
+  CK(cudaMemcpyAsync(d_tab, tables, sizeof *tables, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   return 0;
 }
 

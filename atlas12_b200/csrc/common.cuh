@@ -36,6 +36,17 @@ struct JoshOps {
 };
 
 // gfortran's REAL(8)**INTEGER (libgcc binary exponentiation), host and device
+// one Stehle Stark-profile series on the device (n_dens 0: not loaded), as
+// INIT_STARK_TABLES reads it (atlas12_modules.f90:17682-17746); SYNTHE's
+// hydrogen lines and ATLAS's STARK_MMM read it
+struct StehleDev {
+  int n_lower, n_upper_min, n_upper_max, n_dens;
+  double density_grid[20], temp_grid[10], log_dalpha_grid[60];
+  const int32_t* max_dens_idx;
+  const double* k_alpha;
+  const double* profiles;  // [n_trans][n_dens][10][60]
+};
+
 __host__ __device__ inline double powi(double x, int m) {
   unsigned n = m < 0 ? (unsigned)(-m) : (unsigned)m;
   double y = (n % 2) ? x : 1.0;

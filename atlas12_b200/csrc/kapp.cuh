@@ -44,6 +44,8 @@ constexpr double kBetaHM88 = 8.798905203085208e+14;
 constexpr double kRydbergHe = 109722.277609;
 constexpr double kClightAngs = 2.99792458e18;
 constexpr double kAmu = 1.66053906892e-24;
+constexpr double kRydAng = 1.0e8 / kRydbergH;  // RYD_ANG
+constexpr double kA0Stark = 0.0265384;         // STARK's A0 = pi e^2 / (m_e c)
 constexpr double kLogBetaMin = -2.0, kLogBetaStep = 2.4825302042523617e-02;
 constexpr int kHLev = 80;  // HOP's NMAX_HLEVELS
 
@@ -64,6 +66,10 @@ struct KappDev {
   double he2s1s_f[16], he2s1s_x[16], he2s3s_f[16], he2s3s_x[16];
   double he2p1p_f[16], he2p1p_x[16], he2p3p_f[16], he2p3p_x[16];
   double hem_w[17], hem_t[12], hem_logw[17], hem_logt[12], hem_logk[12 * 17];
+  // HLINOP: hydrogen_f_value's gf tables, STARK's KNMTAB(MMINN, N) at
+  // (N-1)*5 + MMINN-1 and FSTARK(MMINN, N) at (N-1)*10 + MMINN-1
+  double gf_lyman[29], gf_balmer[28], gf_paschen[27], gf_brackett[3];
+  double stark_knm[20], stark_f[40];
 };
 
 // the H2 tables on the device (set by atlasgpu_atlas_set_kapp_h2_tables):
@@ -102,6 +108,8 @@ struct KappArgs {
   double *acont, *sigmac, *scont;  // [numnu][kw]
   double* parts;                   // [numnu][nparts][kw] or null
   int nparts;                      // 7 (hydrogen), 11 (with helium) or 14 (with H2)
+  double *ahline, *shline;         // HLINOP's outputs [numnu][kw] (k_hlinop)
+  const StehleDev* stehle;         // [4] or null: STARK throughout
 };
 
 __host__ __device__ inline double kapp_kbol_ev() { return kKbol / kEvErg; }
@@ -764,6 +772,228 @@ static __global__ void __launch_bounds__(kKappWarps * 32) k_kapp_nu(KappArgs a) 
       }
     }
     __syncwarp();
+  }
+}
+
+// ------------------------------------------------------------------ HLINOP
+// hydrogen_f_value (:17760-17829): tabulated gf of the first members, a
+// Kramers estimate with an average Gaunt factor beyond
+__device__ inline double kapp_hf_value(const KappDev& tb, int n, int m) {
+  if (m <= n) return 0.0;
+  const double xn = (double)n, xm = (double)m;
+  const int idx = m - n;
+  double gf;
+  if (n == 1 && idx <= 29) gf = tb.gf_lyman[idx - 1];
+  else if (n == 2 && idx <= 28) gf = tb.gf_balmer[idx - 1];
+  else if (n == 3 && idx <= 27) gf = tb.gf_paschen[idx - 1];
+  else if (n == 4 && idx <= 3) gf = tb.gf_brackett[idx - 1];
+  else {
+    gf = 1.9603 * powi(xn, 2) / (powi(xm, 3) * powi(1.0 / powi(xn, 2) - 1.0 / powi(xm, 2), 3));
+    gf = gf * 0.80;
+  }
+  return gf / (2.0 * powi(xn, 2));
+}
+
+// STARK's EXINT (:17650-17655)
+__device__ inline double kapp_exint(double x) {
+  return -log(x) - 0.57516 + (0.97996 + (-0.21654 + (0.033572 + (-0.0029222 + 1.05439e-4 * x) * x) * x) * x) * x;
+}
+
+// STARK(N, M, J) (:17528-17659): Griem's quasi-static profile with the
+// impact correction; f0 = 1.25e-9 XNE^(2/3) of the depth
+__device__ __noinline__ double kapp_stark(const KappDev& tb, int n, int m, double freq, double xne, double hkt,
+                                          double f0) {
+  const double xn = (double)n, xm = (double)m;
+  const double x = xn / xm;
+  const double xx = powi(x, 2);
+  const double nn = xn * xn, mm = xm * xm;
+  const int mminn = m - n;
+  const double knm = mminn <= 5 ? tb.stark_knm[(n - 1) * 5 + mminn - 1] : 5.5e-5 * powi(nn * mm, 2) / (mm - nn);
+  const double fnm = mminn <= 10 ? tb.stark_f[(n - 1) * 10 + mminn - 1]
+                                 : tb.stark_f[(n - 1) * 10 + 9] *
+                                       powi((20.0 * xn + 100.0) / ((xn + 10.0) * xm * (1.0 - xx)), 3);
+  const double ryd = kapp_freq_rydh();
+  const double freqnm = ryd * (1.0 / nn - 1.0 / mm);
+  const double del = fabs(freq - freqnm);
+  const double dbeta = kClightAngs / powi(freqnm, 2) / f0 / knm;
+  const double beta = dbeta * del;
+  const double y1 = mm * del * hkt / 2.0;
+  const double y2 = (kPi * kPi / 2.0 / kA0Stark / kClight) * powi(del, 2) / xne;
+  const double qstat = 1.5 + 0.5 * (powi(y1, 2) - 1.384) / (powi(y1, 2) + 1.384);
+  double impact = 0.0;
+  if (y1 < 8.0 && y1 < y2) {
+    double exy2 = 0.0;
+    if (y2 <= 8.0) exy2 = kapp_exint(y2);
+    impact = 1.438 * sqrt(y1 * (1.0 - xx)) * (0.4 * exp(-y1) + kapp_exint(y1) - 0.5 * exy2);
+  }
+  double prof, ratio;
+  if (beta <= 20.0) {
+    prof = 8.0 / (80.0 + powi(beta, 3));
+    ratio = qstat + impact;
+  } else {
+    prof = 1.5 / beta / beta / sqrt(beta);
+    const double dioi = 6.28 * 1.48e-25 * (2.0 * mm * ryd / del) * xne *
+                        (sqrt(2.0 * mm * ryd / del) * (1.3 * qstat + 0.30 * impact) - 3.9 * ryd * hkt);
+    ratio = qstat * fmin(1.0 + dioi, 1.25) + impact;
+  }
+  return kA0Stark * fnm * prof * dbeta * ratio;
+}
+
+// STARK_MMM(N, M, J) (:17854-18106): the Stehle table of the series, trilinear
+// in (log Delta-alpha, log T, log Ne) on log profile values (linear where one
+// of the eight corners is not positive), the Delta-alpha^-2.5 wing past the
+// table; STARK where the series, the transition, the density or the
+// temperature is off the table
+__device__ __noinline__ double kapp_stark_mmm(const KappDev& tb, const StehleDev* st, int n, int m, double freq,
+                                              double T, double xne, double hkt, double f0) {
+  if (n < 1 || n > 4 || m <= n || !st) return kapp_stark(tb, n, m, freq, xne, hkt, f0);
+  const StehleDev& S = st[n - 1];
+  if (S.n_dens == 0 || m < S.n_upper_min || m > S.n_upper_max) return kapp_stark(tb, n, m, freq, xne, hkt, f0);
+  const int itrans = m - S.n_upper_min + 1;
+  if (xne > S.density_grid[S.n_dens - 1]) return kapp_stark(tb, n, m, freq, xne, hkt, f0);
+  const double ne_eff = fmin(xne, S.density_grid[S.max_dens_idx[itrans - 1] - 1]);
+  const double xn = (double)n, xm = (double)m;
+  const double lambda0 = kRydAng * powi(xn * xm, 2) / ((xm - xn) * (xm + xn));
+  const double freq_nm = kClightAngs / lambda0;
+  const double del_freq = fabs(freq - freq_nm);
+  const double F0 = 1.25e-9 * pow(ne_eff, 2.0 / 3.0);
+  if (F0 <= 0.0) return kapp_stark(tb, n, m, freq, xne, hkt, f0);
+  const double dalpha = powi(lambda0, 2) / kClightAngs * del_freq / F0;
+  const int nd = S.n_dens, nt = 10, na = 60;
+  const double log_ne = log10(ne_eff);
+  if (T < S.temp_grid[0] * 0.5 || T > S.temp_grid[nt - 1] * 2.0) return kapp_stark(tb, n, m, freq, xne, hkt, f0);
+  int id1;
+  for (id1 = 1; id1 <= nd - 1; ++id1)
+    if (ne_eff <= S.density_grid[id1]) break;
+  id1 = max(1, min(nd - 1, id1));
+  const int id2 = id1 + 1;
+  double frac_d = (log_ne - log10(S.density_grid[id1 - 1])) /
+                  (log10(S.density_grid[id2 - 1]) - log10(S.density_grid[id1 - 1]));
+  frac_d = fmax(0.0, fmin(1.0, frac_d));
+  int it1;
+  for (it1 = 1; it1 <= nt - 1; ++it1)
+    if (T <= S.temp_grid[it1]) break;
+  it1 = max(1, min(nt - 1, it1));
+  const int it2 = it1 + 1;
+  double frac_t = (log(T) - log(S.temp_grid[it1 - 1])) / (log(S.temp_grid[it2 - 1]) - log(S.temp_grid[it1 - 1]));
+  frac_t = fmax(0.0, fmin(1.0, frac_t));
+  int ia1 = 1, ia2 = 1;
+  double frac_a = 0.0;
+  if (dalpha > 0.0) {
+    const double log_dalpha = log10(dalpha);
+    if (log_dalpha <= S.log_dalpha_grid[0]) {
+    } else if (log_dalpha >= S.log_dalpha_grid[na - 1]) {
+      const double f_nm = kapp_hf_value(tb, n, m);
+      const double I = S.k_alpha[itrans - 1] / pow(dalpha, 2.5);
+      return kA0Stark * f_nm * I * powi(lambda0, 2) / (kClightAngs * F0);
+    } else {
+      for (ia1 = 1; ia1 <= na - 1; ++ia1)
+        if (log_dalpha <= S.log_dalpha_grid[ia1]) break;
+      ia1 = max(1, min(na - 1, ia1));
+      ia2 = ia1 + 1;
+      frac_a = (log_dalpha - S.log_dalpha_grid[ia1 - 1]) / (S.log_dalpha_grid[ia2 - 1] - S.log_dalpha_grid[ia1 - 1]);
+      frac_a = fmax(0.0, fmin(1.0, frac_a));
+    }
+  }
+  const double* P = S.profiles + (size_t)(itrans - 1) * nd * nt * na;
+  auto pv = [&](int ia, int it, int id) { return P[((size_t)(id - 1) * nt + (it - 1)) * na + ia - 1]; };
+  double v000 = pv(ia1, it1, id1), v001 = pv(ia2, it1, id1), v010 = pv(ia1, it2, id1), v011 = pv(ia2, it2, id1);
+  double v100 = pv(ia1, it1, id2), v101 = pv(ia2, it1, id2), v110 = pv(ia1, it2, id2), v111 = pv(ia2, it2, id2);
+  double I;
+  if (v000 <= 0.0 || v001 <= 0.0 || v010 <= 0.0 || v011 <= 0.0 || v100 <= 0.0 || v101 <= 0.0 || v110 <= 0.0 ||
+      v111 <= 0.0) {
+    const double v00 = v000 + frac_a * (v001 - v000), v01 = v010 + frac_a * (v011 - v010);
+    const double v10 = v100 + frac_a * (v101 - v100), v11 = v110 + frac_a * (v111 - v110);
+    const double v0 = v00 + frac_t * (v01 - v00), v1 = v10 + frac_t * (v11 - v10);
+    I = v0 + frac_d * (v1 - v0);
+  } else {
+    v000 = log(v000);
+    v001 = log(v001);
+    v010 = log(v010);
+    v011 = log(v011);
+    v100 = log(v100);
+    v101 = log(v101);
+    v110 = log(v110);
+    v111 = log(v111);
+    const double v00 = v000 + frac_a * (v001 - v000), v01 = v010 + frac_a * (v011 - v010);
+    const double v10 = v100 + frac_a * (v101 - v100), v11 = v110 + frac_a * (v111 - v110);
+    const double v0 = v00 + frac_t * (v01 - v00), v1 = v10 + frac_t * (v11 - v10);
+    I = exp(v0 + frac_d * (v1 - v0));
+  }
+  I = fmax(I, 0.0);
+  const double f_nm = kapp_hf_value(tb, n, m);
+  return kA0Stark * f_nm * I * powi(lambda0, 2) / (kClightAngs * F0);
+}
+
+// HLINOP (:17381-17503): warp per frequency (grid-stride), lanes over depths;
+// reads the occupation probabilities k_kapp_depth left in d.w
+static __global__ void __launch_bounds__(kKappWarps * 32) k_hlinop(KappArgs a) {
+  const KappDev& tb = *a.tb;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int kw = a.kw;
+  const double nu_lyman = kapp_freq_rydh();
+  for (int nu = blockIdx.x * kKappWarps + wid; nu < a.numnu; nu += gridDim.x * kKappWarps) {
+    const double wave = a.waveset[nu];
+    const double freq = kClightNms / wave;
+    const double f3 = powi(freq / 1.0e15, 3);
+    const int n = (int)sqrt(nu_lyman / freq);
+    bool none = n == 0 || n > 4 || (n == 1 && freq < 2.0e15) || (n == 2 && freq < 4.44e14);
+    // MFREQ = NINT(SQRT(NU_LYMAN / (NU_LYMAN / N^2 - FREQ))); at the series
+    // limit itself the argument is infinite and every upper level is past
+    // the dissolved-level cut, as any MFREQ above 80 gives
+    int mfreq = 1000000;
+    if (!none) {
+      const double q = sqrt(nu_lyman / (nu_lyman / powi((double)n, 2) - freq));
+      if (q < 1.0e6) mfreq = (int)round(q);
+    }
+    for (int j = lane; j < a.nrhox; j += 32) {
+      const size_t o = (size_t)nu * kw + j;
+      if (none) {
+        a.ahline[o] = 0.0;
+        a.shline[o] = 0.0;
+        continue;
+      }
+      const double T = a.t[j], xne = a.xne[j];
+      const double hkt = a.d.hkt[j];
+      const double ehvkt = exp(-freq * hkt);
+      const double stim = 1.0 - ehvkt;
+      const double bnu = kBnuPrefac * f3 * ehvkt / stim;
+      const double f0 = 1.25e-9 * pow(xne, 2.0 / 3.0);
+      const double* W = a.d.w + j;  // w_n at (n-1)*kw
+      auto bh = [&](int k) { return a.bhyd ? a.bhyd[(size_t)(k - 1) * kw + j] : 1.0; };
+      auto bolt = [&](int k) {
+        const double dk2 = powi((double)k, 2);
+        return exp(-(13.595 - 13.595 / dk2) / a.d.tkev[j]) * 2.0 * dk2 * bh(k) * a.xnfp1[j] / a.rho[j];
+      };
+      int m1 = mfreq, m2 = m1 + 1;
+      m1 = max(m1, n + 1);
+      double H = 0.0, S = 0.0;
+      if (m1 > 6) {
+        if (m1 > kHLev || W[(size_t)(m1 - 1) * kw] < 1.0e-3) {
+          a.ahline[o] = 0.0;
+          a.shline[o] = bnu;
+          continue;
+        }
+        m1 = m1 - 1;
+        m2 = m2 + 3;
+        if (n >= 4 && m1 <= 8) {
+          H = kapp_stark_mmm(tb, a.stehle, 3, 4, freq, T, xne, hkt, f0) * (1.0 - ehvkt * bh(4) / bh(3)) * bolt(3);
+          S = H * bnu * stim / (bh(3) / bh(4) - ehvkt);
+        }
+      }
+      const double bn = bh(n), boltn = bolt(n);
+      for (int m = m1; m <= m2; ++m) {
+        const double bm = m <= 6 ? bh(m) : 1.0;
+        double w = 1.0;
+        if (m >= 2 && m <= kHLev) w = W[(size_t)(m - 1) * kw];
+        if (m > kHLev) w = 0.0;
+        const double A = w * kapp_stark_mmm(tb, a.stehle, n, m, freq, T, xne, hkt, f0) * (1.0 - ehvkt * bm / bn) * boltn;
+        H = H + A;
+        S = S + A * bnu * stim / (bn / bm - ehvkt);
+      }
+      a.ahline[o] = H;
+      a.shline[o] = H > 0.0 ? S / H : bnu;
+    }
   }
 }
 

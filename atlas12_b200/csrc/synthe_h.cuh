@@ -18,14 +18,6 @@ namespace atlasgpu {
 
 constexpr int kShWarps = 2;  // warps per block; each owns one ShConv slot
 
-// one Stehle series on the device (n_dens 0: not loaded)
-struct StehleDev {
-  int n_lower, n_upper_min, n_upper_max, n_dens;
-  double density_grid[20], temp_grid[10], log_dalpha_grid[60];
-  const int32_t* max_dens_idx;
-  const double* k_alpha;
-  const double* profiles;  // [n_trans][n_dens][10][60]
-};
 
 // a hydrogen record as the walk needs it (prepared on the host)
 struct ShRec {

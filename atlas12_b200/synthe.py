@@ -102,25 +102,7 @@ class Synthe:
         the reference) and the Stehle series (4 dicts as read_stehle gives, None
         entries not loaded; None: the analytic profile throughout)."""
         self._shtab = _lib.HydrogenTables.from_tables(tables, "s_")
-        self._stehle_keep = []
-        st = None
-        if stehle is not None:
-            st = (_lib.StehleSeries * 4)()
-            for q, ser in enumerate(stehle):
-                if ser is None:
-                    continue
-                arrs = [np.ascontiguousarray(ser["max_dens_idx"], np.int32),
-                        np.ascontiguousarray(ser["k_alpha"], np.float64),
-                        np.ascontiguousarray(ser["profiles"], np.float64)]
-                self._stehle_keep += arrs
-                a = st[q]
-                a.n_lower, a.n_upper_min, a.n_upper_max = (int(ser[k]) for k in ("n_lower", "n_upper_min",
-                                                                                  "n_upper_max"))
-                a.n_dens = len(ser["density_grid"])
-                a.density_grid[:a.n_dens] = [float(x) for x in ser["density_grid"]]
-                a.temp_grid[:] = [float(x) for x in ser["temp_grid"]]
-                a.log_dalpha_grid[:] = [float(x) for x in ser["log_dalpha_grid"]]
-                a.max_dens_idx, a.k_alpha, a.profiles = (v.ctypes.data for v in arrs)
+        st, self._stehle_keep = (None, []) if stehle is None else _lib.stehle_array(stehle)
         self.ctx.call("atlasgpu_synthe_set_hydrogen_tables", ctypes.byref(self._shtab),
                       None if st is None else st)
 

@@ -351,7 +351,9 @@ int atlasgpu_atlas_xlinop(atlasgpu_ctx *ctx, const atlasgpu_nlte_line *recs, int
  *     log10 cross-section knots (FREQ1S/X1S, FREQ3S/X3S, FREQ1P/X1P,
  *     FREQ3P/X3P);
  *   HEMIOP (:13716-13833): WHEM (nm), THEM (K), KHEM(17,12) (cm^4/dyn; the
- *     library takes the logs as the reference's first call does). */
+ *     library takes the logs as the reference's first call does);
+ * and HLINOP's: hydrogen_f_value's (:17760-17829) GF_LYMAN, GF_BALMER,
+ *   GF_PASCHEN, GF_BRACKETT; STARK's (:17528-17659) KNMTAB(5,4), FSTARK(10,4). */
 typedef struct atlasgpu_kapp_tables {
   float freqn[15][29], xn[15][29], xl[6][6][29], ekarzas[29];
   double gff[146][81];
@@ -365,6 +367,8 @@ typedef struct atlasgpu_kapp_tables {
   double he2s1s_f[16], he2s1s_x[16], he2s3s_f[16], he2s3s_x[16];
   double he2p1p_f[16], he2p1p_x[16], he2p3p_f[16], he2p3p_x[16];
   double hem_w[17], hem_t[12], hem_k[12][17];
+  double gf_lyman[29], gf_balmer[28], gf_paschen[27], gf_brackett[3];
+  double stark_knm[4][5], stark_f[4][10];
 } atlasgpu_kapp_tables;
 
 /* Keeps KAPP's hydrogen tables on the context for atlasgpu_atlas_kapp_hydrogen
@@ -443,6 +447,27 @@ int atlasgpu_atlas_set_kapp_h2_tables(atlasgpu_ctx *ctx, const atlasgpu_kapp_h2_
 int atlasgpu_atlas_kapp(atlasgpu_ctx *ctx, int numnu, const double *waveset, int nrhox, int kw,
                         const atlasgpu_kapp_pops *pops, double *acont, double *sigmac, double *scont,
                         double *parts);
+
+/* Keeps the four Stehle series (Lyman, Balmer, Paschen, Brackett) that
+ * STARK_MMM (atlas12_modules.f90:17854-18106) reads on the context for
+ * atlasgpu_atlas_hlinop; NULL (or a series with n_dens 0): STARK's analytic
+ * profile throughout, as when the reference finds no table file. */
+int atlasgpu_atlas_set_stehle_tables(atlasgpu_ctx *ctx, const atlasgpu_stehle_series *stehle);
+
+/* HLINOP (atlas12_modules.f90:17381-17503): the hydrogen line
+ * pseudo-continuum of KAPP, per frequency and depth -- the lines of the
+ * series whose lower level n = int(sqrt(nu_Lyman / nu)) (n <= 4; Lyman only
+ * above 2e15 Hz, Balmer above 4.44e14 Hz) nearest the frequency, their Stark
+ * profiles from STARK_MMM (Stehle tables where loaded, else STARK
+ * :17528-17659) with the occupation probabilities and departure
+ * coefficients.  Depth vectors [nrhox] T, XNE, RHO, XNFP(J,1); bhyd
+ * BHYD(J,1..6) as [6][kw] or NULL (LTE).  Outputs AHLINE, SHLINE
+ * [numnu][kw] (frequencies outside the four series: 0 and 0, as KAPP's
+ * zeroed arrays; depths past the dissolved-level cut: 0 and BNU).  The
+ * tables of atlasgpu_atlas_set_kapp_tables must be set. */
+int atlasgpu_atlas_hlinop(atlasgpu_ctx *ctx, int numnu, const double *waveset, int nrhox, int kw, const double *t,
+                          const double *xne, const double *rho, const double *xnfp1, const double *bhyd,
+                          double *ahline, double *shline);
 
 /* RUN_RT_PASS frequency loop (atlas12_modules.f90:3880-3951): per NU the
  * Planck terms, ALINE = XLINES*STIM, JOSH(1,0) (:18398-18776), the negative

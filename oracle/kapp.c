@@ -24,6 +24,8 @@
  *   H2COLLOP             :16371-16527
  *   H2RAOP               :17289-17338
  *   PARTFNH2             :22324-22418, EQUILH2 :22437-22469
+ *   HLINOP               :17381-17503 (with STARK :17528-17659, STARK_MMM
+ *                                      :17854-18106, hydrogen_f_value :17760-17829)
  * Constants from mod_constants (:315-464).  The tables come from the
  * reference's data files and DATA statements (tests/golden/make_golden.py).
  */
@@ -732,6 +734,185 @@ void orc_kapp_h2(const orc_kapp_tables *tb, const orc_kapp_h2_tables *h2, double
     out[(size_t)ORC_KAPP_SIGMAC * nrhox + j] = out[(size_t)ORC_KAPP_SIGH * nrhox + j] +
                                                out[(size_t)ORC_KAPP_SIGHE * nrhox + j] +
                                                out[(size_t)ORC_KAPP_SIGEL * nrhox + j] + sigh2[j] + 0.0;
+  }
+}
+
+/* ---- HLINOP ---- */
+
+/* hydrogen_f_value (:17760-17829) */
+static double hf_value(const orc_kapp_tables *tb, int n, int m) {
+  if (m <= n) return 0.0;
+  const double xn = n, xm = m;
+  const int idx = m - n;
+  double gf;
+  if (n == 1 && idx <= 29) gf = tb->gf_lyman[idx - 1];
+  else if (n == 2 && idx <= 28) gf = tb->gf_balmer[idx - 1];
+  else if (n == 3 && idx <= 27) gf = tb->gf_paschen[idx - 1];
+  else if (n == 4 && idx <= 3) gf = tb->gf_brackett[idx - 1];
+  else {
+    gf = 1.9603 * ipow(xn, 2) / (ipow(xm, 3) * ipow(1.0 / ipow(xn, 2) - 1.0 / ipow(xm, 2), 3));
+    gf = gf * 0.80;
+  }
+  return gf / (2.0 * ipow(xn, 2));
+}
+
+static double exint(double x) {
+  return -log(x) - 0.57516 + (0.97996 + (-0.21654 + (0.033572 + (-0.0029222 + 1.05439e-4 * x) * x) * x) * x) * x;
+}
+
+/* STARK (:17528-17659) at one depth */
+static double stark(const orc_kapp_tables *tb, int n, int m, double freq, double t, double xne) {
+  const double f0 = 1.25e-9 * pow(xne, 2.0 / 3.0);
+  const double hkt = K_HPLANCK / (K_KBOL * t);
+  const double xn = n, xm = m, x = xn / xm, xx = ipow(x, 2), nn = xn * xn, mm = xm * xm;
+  const int mminn = m - n;
+  double knm, fnm;
+  if (mminn <= 5) knm = tb->stark_knm[(n - 1) * 5 + mminn - 1];
+  else knm = 5.5e-5 * ipow(nn * mm, 2) / (mm - nn);
+  if (mminn <= 10) fnm = tb->stark_f[(n - 1) * 10 + mminn - 1];
+  else fnm = tb->stark_f[(n - 1) * 10 + 9] * ipow((20.0 * xn + 100.0) / ((xn + 10.0) * xm * (1.0 - xx)), 3);
+  const double ryd = freq_rydh();
+  const double freqnm = ryd * (1.0 / nn - 1.0 / mm);
+  const double del = fabs(freq - freqnm);
+  const double dbeta = K_CLIGHT_ANGS / ipow(freqnm, 2) / f0 / knm;
+  const double beta = dbeta * del;
+  const double y1 = mm * del * hkt / 2.0;
+  const double y2 = (K_PI * K_PI / 2.0 / 0.0265384 / K_CLIGHT) * ipow(del, 2) / xne;
+  const double qstat = 1.5 + 0.5 * (ipow(y1, 2) - 1.384) / (ipow(y1, 2) + 1.384);
+  double impact = 0.0;
+  if (y1 < 8.0 && y1 < y2) {
+    const double exy2 = y2 <= 8.0 ? exint(y2) : 0.0;
+    impact = 1.438 * sqrt(y1 * (1.0 - xx)) * (0.4 * exp(-y1) + exint(y1) - 0.5 * exy2);
+  }
+  double prof, ratio;
+  if (beta <= 20.0) {
+    prof = 8.0 / (80.0 + ipow(beta, 3));
+    ratio = qstat + impact;
+  } else {
+    prof = 1.5 / beta / beta / sqrt(beta);
+    const double dioi = 6.28 * 1.48e-25 * (2.0 * mm * ryd / del) * xne *
+                        (sqrt(2.0 * mm * ryd / del) * (1.3 * qstat + 0.30 * impact) - 3.9 * ryd * hkt);
+    ratio = qstat * fmin(1.0 + dioi, 1.25) + impact;
+  }
+  return 0.0265384 * fnm * prof * dbeta * ratio;
+}
+
+/* STARK_MMM (:17854-18106) */
+double orc_stark_mmm(const orc_kapp_tables *tb, const orc_stehle_t *stehle, int n, int m, double freq, double t,
+                     double xne) {
+  if (n < 1 || n > 4 || m <= n || !stehle) return stark(tb, n, m, freq, t, xne);
+  const orc_stehle_t *S = &stehle[n - 1];
+  if (S->n_dens == 0 || m < S->n_upper_min || m > S->n_upper_max) return stark(tb, n, m, freq, t, xne);
+  const int itrans = m - S->n_upper_min + 1;
+  if (xne > S->density_grid[S->n_dens - 1]) return stark(tb, n, m, freq, t, xne);
+  const double ne_eff = fmin(xne, S->density_grid[S->max_dens_idx[itrans - 1] - 1]);
+  const double xn = n, xm = m;
+  const double lambda0 = (1.0e8 / K_RYDBERG_H) * ipow(xn * xm, 2) / ((xm - xn) * (xm + xn));
+  const double del_freq = fabs(freq - K_CLIGHT_ANGS / lambda0);
+  const double f0 = 1.25e-9 * pow(ne_eff, 2.0 / 3.0);
+  if (f0 <= 0.0) return stark(tb, n, m, freq, t, xne);
+  const double dalpha = ipow(lambda0, 2) / K_CLIGHT_ANGS * del_freq / f0;
+  const int nd = S->n_dens, nt = 10, na = 60;
+  const double log_ne = log10(ne_eff);
+  if (t < S->temp_grid[0] * 0.5 || t > S->temp_grid[nt - 1] * 2.0) return stark(tb, n, m, freq, t, xne);
+  int id1;
+  for (id1 = 1; id1 <= nd - 1; ++id1)
+    if (ne_eff <= S->density_grid[id1]) break;
+  if (id1 > nd - 1) id1 = nd - 1;
+  const int id2 = id1 + 1;
+  double frac_d =
+      (log_ne - log10(S->density_grid[id1 - 1])) / (log10(S->density_grid[id2 - 1]) - log10(S->density_grid[id1 - 1]));
+  frac_d = fmax(0.0, fmin(1.0, frac_d));
+  int it1;
+  for (it1 = 1; it1 <= nt - 1; ++it1)
+    if (t <= S->temp_grid[it1]) break;
+  if (it1 > nt - 1) it1 = nt - 1;
+  const int it2 = it1 + 1;
+  double frac_t = (log(t) - log(S->temp_grid[it1 - 1])) / (log(S->temp_grid[it2 - 1]) - log(S->temp_grid[it1 - 1]));
+  frac_t = fmax(0.0, fmin(1.0, frac_t));
+  int ia1 = 1, ia2 = 1;
+  double frac_a = 0.0;
+  if (dalpha > 0.0) {
+    const double lda = log10(dalpha);
+    if (lda >= S->log_dalpha_grid[na - 1]) {
+      const double i_da = S->k_alpha[itrans - 1] / pow(dalpha, 2.5);
+      return 0.0265384 * hf_value(tb, n, m) * i_da * ipow(lambda0, 2) / (K_CLIGHT_ANGS * f0);
+    }
+    if (lda > S->log_dalpha_grid[0]) {
+      for (ia1 = 1; ia1 <= na - 1; ++ia1)
+        if (lda <= S->log_dalpha_grid[ia1]) break;
+      if (ia1 > na - 1) ia1 = na - 1;
+      ia2 = ia1 + 1;
+      frac_a = (lda - S->log_dalpha_grid[ia1 - 1]) / (S->log_dalpha_grid[ia2 - 1] - S->log_dalpha_grid[ia1 - 1]);
+      frac_a = fmax(0.0, fmin(1.0, frac_a));
+    }
+  }
+#define PV(IA, IT, ID) S->profiles[(((size_t)(itrans - 1) * nd + (ID)-1) * nt + (IT)-1) * na + (IA)-1]
+  double v[8] = {PV(ia1, it1, id1), PV(ia2, it1, id1), PV(ia1, it2, id1), PV(ia2, it2, id1),
+                 PV(ia1, it1, id2), PV(ia2, it1, id2), PV(ia1, it2, id2), PV(ia2, it2, id2)};
+#undef PV
+  int pos = 1;
+  for (int k = 0; k < 8; ++k)
+    if (v[k] <= 0.0) pos = 0;
+  if (pos)
+    for (int k = 0; k < 8; ++k) v[k] = log(v[k]);
+  const double v00 = v[0] + frac_a * (v[1] - v[0]), v01 = v[2] + frac_a * (v[3] - v[2]);
+  const double v10 = v[4] + frac_a * (v[5] - v[4]), v11 = v[6] + frac_a * (v[7] - v[6]);
+  const double v0 = v00 + frac_t * (v01 - v00), v1 = v10 + frac_t * (v11 - v10);
+  double i_da = pos ? exp(v0 + frac_d * (v1 - v0)) : v0 + frac_d * (v1 - v0);
+  i_da = fmax(i_da, 0.0);
+  return 0.0265384 * hf_value(tb, n, m) * i_da * ipow(lambda0, 2) / (K_CLIGHT_ANGS * f0);
+}
+
+void orc_hlinop(const orc_kapp_tables *tb, const orc_stehle_t *stehle, double wave, int nrhox, const double *t,
+                const double *xne, const double *rho, const double *xnfp1, const double *bhyd, double *ahline,
+                double *shline) {
+  const double nu_lyman = freq_rydh();
+  const double freq = K_CLIGHT_NMS / wave;
+  const double f3 = ipow(freq / 1.0e15, 3);
+  for (int j = 0; j < nrhox; ++j) ahline[j] = shline[j] = 0.0;
+  const int n = (int)sqrt(nu_lyman / freq);
+  if (n == 0 || n > 4) return;
+  if (n == 1 && freq < 2.0e15) return;
+  if (n == 2 && freq < 4.44e14) return;
+  const double q = sqrt(nu_lyman / (nu_lyman / ipow((double)n, 2) - freq));
+  const int mfreq = q < 1.0e6 ? (int)round(q) : 1000000; /* the series limit itself: past every level */
+  for (int j = 0; j < nrhox; ++j) {
+    const double T = t[j], tkev = kbol_ev() * T;
+    const double ehvkt = exp(-freq * (K_HPLANCK / (K_KBOL * T))), stim = 1.0 - ehvkt;
+    const double bnu = bnu_prefac() * f3 * ehvkt / stim;
+#define BH(K) (bhyd ? bhyd[(size_t)((K)-1) * nrhox + j] : 1.0)
+    double bolt[5];
+    for (int k = 1; k <= 4; ++k)
+      bolt[k] = exp(-(13.595 - 13.595 / ipow((double)k, 2)) / tkev) * 2.0 * ipow((double)k, 2) * BH(k) * xnfp1[j] / rho[j];
+    int m1 = mfreq, m2 = m1 + 1;
+    if (m1 < n + 1) m1 = n + 1;
+    double h = 0.0, s = 0.0;
+    if (m1 > 6) {
+      if (m1 > 80 || orc_occupation_prob(tb, m1, xne[j]) < 1.0e-3) {
+        ahline[j] = 0.0;
+        shline[j] = bnu;
+        continue;
+      }
+      m1 = m1 - 1;
+      m2 = m2 + 3;
+      if (n >= 4 && m1 <= 8) {
+        h = orc_stark_mmm(tb, stehle, 3, 4, freq, T, xne[j]) * (1.0 - ehvkt * BH(4) / BH(3)) * bolt[3];
+        s = h * bnu * stim / (BH(3) / BH(4) - ehvkt);
+      }
+    }
+    for (int m = m1; m <= m2; ++m) {
+      const double bm = m <= 6 ? BH(m) : 1.0;
+      double w = 1.0;
+      if (m >= 2 && m <= 80) w = orc_occupation_prob(tb, m, xne[j]);
+      if (m > 80) w = 0.0;
+      const double a = w * orc_stark_mmm(tb, stehle, n, m, freq, T, xne[j]) * (1.0 - ehvkt * bm / BH(n)) * bolt[n];
+      h = h + a;
+      s = s + a * bnu * stim / (BH(n) / bm - ehvkt);
+    }
+#undef BH
+    ahline[j] = h;
+    shline[j] = h > 0.0 ? s / h : bnu;
   }
 }
 

@@ -351,6 +351,9 @@ typedef struct {
   const double *he2s1s_f, *he2s1s_x, *he2s3s_f, *he2s3s_x;  /* HE12S1S, HE12S3S knots (16 each) */
   const double *he2p1p_f, *he2p1p_x, *he2p3p_f, *he2p3p_x;  /* HE12P1P, HE12P3P knots (16 each) */
   const double *hem_w, *hem_t, *hem_k;                      /* HEMIOP WHEM(17), THEM(12), KHEM(17,12) */
+  /* HLINOP: hydrogen_f_value's GF_LYMAN(29), GF_BALMER(28), GF_PASCHEN(27), GF_BRACKETT(3);
+   * STARK's KNMTAB(5,4), FSTARK(10,4) */
+  const double *gf_lyman, *gf_balmer, *gf_paschen, *gf_brackett, *stark_knm, *stark_f;
 } orc_kapp_tables;
 
 enum {
@@ -391,6 +394,15 @@ typedef struct {
 } orc_kapp_h2_tables;
 
 enum { ORC_KAPP_AH2MIN = ORC_KAPP_NOUT_HE, ORC_KAPP_AH2COLL, ORC_KAPP_SIGH2, ORC_KAPP_NOUT_H2 };
+
+/* HLINOP (atlas12_modules.f90:17381-17503) at one wavelength (nm), all
+ * depths: ahline[j], shline[j]; bhyd BHYD(J,n) at [(n-1)*nrhox + j] or NULL;
+ * stehle [4] or NULL (STARK throughout) */
+void orc_hlinop(const orc_kapp_tables *tb, const orc_stehle_t *stehle, double wave, int nrhox, const double *t,
+                const double *xne, const double *rho, const double *xnfp1, const double *bhyd, double *ahline,
+                double *shline);
+double orc_stark_mmm(const orc_kapp_tables *tb, const orc_stehle_t *stehle, int n, int m, double freq, double t,
+                     double xne);
 
 double orc_partfnh2(const orc_kapp_h2_tables *h2, double t);
 double orc_equilh2(const orc_kapp_h2_tables *h2, double t);

@@ -663,7 +663,8 @@ KAPP_NAMES = ("ahyd", "shyd", "ah2p", "ahmin", "shmin", "sigh", "sigel", "acont"
 KAPP_NAMES_HE = KAPP_NAMES + ("ahe1", "ahe2", "ahemin", "sighe")
 KAPP_NAMES_H2 = KAPP_NAMES_HE + ("ah2min", "ah2coll", "sigh2")
 _KAPP_HE_TABLES = ("he1_chi", "he1_freq", "he1_g", "he_x505", "he_x50", "he_x20", "he_x10", "he2s1s_f", "he2s1s_x",
-                   "he2s3s_f", "he2s3s_x", "he2p1p_f", "he2p1p_x", "he2p3p_f", "he2p3p_x", "hem_w", "hem_t", "hem_k")
+                   "he2s3s_f", "he2s3s_x", "he2p1p_f", "he2p1p_x", "he2p3p_f", "he2p3p_x", "hem_w", "hem_t", "hem_k",
+                   "gf_lyman", "gf_balmer", "gf_paschen", "gf_brackett", "stark_knm", "stark_f")
 
 
 class KappTables(ctypes.Structure):
@@ -698,6 +699,11 @@ def _lib_kapp():
         L.orc_crosshe.restype = ctypes.c_double
         L.orc_kapp_h2.argtypes = [ctypes.POINTER(KappTables), ctypes.POINTER(KappH2Tables), ctypes.c_double,
                                   ctypes.c_int] + [_dp] * 13
+        L.orc_hlinop.argtypes = [ctypes.POINTER(KappTables), ctypes.c_void_p, ctypes.c_double, ctypes.c_int] + \
+            [_dp] * 7
+        L.orc_stark_mmm.argtypes = [ctypes.POINTER(KappTables), ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + \
+            [ctypes.c_double] * 3
+        L.orc_stark_mmm.restype = ctypes.c_double
         for f in (L.orc_partfnh2, L.orc_equilh2):
             f.argtypes = [ctypes.POINTER(KappH2Tables), ctypes.c_double]
             f.restype = ctypes.c_double
@@ -781,6 +787,25 @@ def kapp_h2(kt, h2, wave, t, xne, rho, xnfp1, xnfp2, xnfp3, xnfp4, xnfp5, xnf4, 
     L.orc_kapp_h2(ctypes.byref(kt), ctypes.byref(h2), float(wave), nr, *[_ptr(a) for a in v],
                   _ptr(bh) if bh is not None else None, _ptr(bm) if bm is not None else None, _ptr(out))
     return dict(zip(KAPP_NAMES_H2, out))
+
+
+def hlinop(kt, wave, t, xne, rho, xnfp1, bhyd=None, stehle=None):
+    """HLINOP at one wavelength (nm): (ahline, shline) [nrhox].  stehle: the
+    ctypes array of stehle_structs, or None (STARK throughout)."""
+    L = _lib_kapp()
+    nr = len(t)
+    ah, sh = np.zeros(nr), np.zeros(nr)
+    v = [_d(a) for a in (t, xne, rho, xnfp1)]
+    bh = None if bhyd is None else _d(bhyd)
+    L.orc_hlinop(ctypes.byref(kt), None if stehle is None else ctypes.addressof(stehle), float(wave), nr,
+                 *[_ptr(a) for a in v], _ptr(bh) if bh is not None else None, _ptr(ah), _ptr(sh))
+    return ah, sh
+
+
+def stark_mmm(kt, n, m, freq, t, xne, stehle=None):
+    """STARK_MMM(N, M, J) at one (frequency, T, XNE)."""
+    return _lib_kapp().orc_stark_mmm(ctypes.byref(kt), None if stehle is None else ctypes.addressof(stehle), n, m,
+                                     float(freq), float(t), float(xne))
 
 
 def partfnh2(h2, t):

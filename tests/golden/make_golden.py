@@ -271,6 +271,16 @@ def kapp_helium_tables(mod):
         k_hem_t=fortran_array(hem, ":: THEM(NTHEM) =", 12),
         k_hem_k=fortran_array(hem, ":: KHEM(NWHEM, NTHEM) =", 17 * 12),  # [it][iw]
     )
+    # HLINOP's oscillator strengths and Stark parameters (hydrogen_f_value
+    # :17760-17829, STARK :17528-17659; KNMTAB(5,4), FSTARK(10,4) column-major)
+    hfv = body("FUNCTION hydrogen_f_value")
+    stark = mod[mod.index("\nFUNCTION STARK(N, M, J)") + 1:mod.index("END FUNCTION STARK\n")]
+    out.update(k_gf_lyman=fortran_array(hfv, ":: GF_LYMAN(29) =", 29),
+               k_gf_balmer=fortran_array(hfv, ":: GF_BALMER(28) =", 28),
+               k_gf_paschen=fortran_array(hfv, ":: GF_PASCHEN(27) =", 27),
+               k_gf_brackett=fortran_array(hfv, ":: GF_BRACKETT(3) =", 3),
+               k_stark_knm=fortran_array(stark, ":: KNMTAB(5,4) =", 20),
+               k_stark_f=fortran_array(stark, ":: FSTARK(10,4) =", 40))
     for fn, f, x in (("HE12S1S", "FREQ1S", "X1S"), ("HE12S3S", "FREQ3S", "X3S"),
                      ("HE12P1P", "FREQ1P", "X1P"), ("HE12P3P", "FREQ3P", "X3P")):
         src = body("FUNCTION " + fn)

@@ -196,6 +196,42 @@ def test_kapp_h2_requires_its_tables(gpu_ctx, tables):
         fresh.close()
 
 
+@pytest.mark.parametrize("use_stehle,nlte", [(False, False), (True, False), (True, True)])
+def test_hlinop_matches_oracle(po, tables, kapp, use_stehle, nlte):
+    """HLINOP (atlasgpu_atlas_hlinop) against orc_hlinop: AHLINE and SHLINE at
+    every (frequency, depth) over 80-2300 nm with the Lyman, Balmer, Paschen
+    and Brackett members and limits, on seeded Stehle tables or STARK alone,
+    LTE and with departure coefficients (which make SHLINE differ from BNU)."""
+    rng = np.random.default_rng(4)
+    nr, kw = 40, 48
+    t = np.geomspace(3000.0, 60000.0, nr)
+    xne = np.geomspace(1e9, 3e17, nr)
+    rho = np.geomspace(1e-11, 1e-5, nr)
+    x1 = rho / 1.67e-24 * rng.uniform(0.05, 0.5, nr)
+    ws, _ = synthetic.geometric_waveset(80.0, 2300.0, 700)
+    lines = np.array([97.25, 102.57, 121.57, 364.6, 383.54, 410.17, 486.13, 656.28, 820.4, 1005.2, 1875.1, 1458.2,
+                      2166.1])
+    ws = np.sort(np.concatenate([ws, lines * (1 - 1e-5), lines * (1 + 1e-5)]))
+    st_dicts = synthetic.stehle_tables() if use_stehle else None
+    kapp.set_stehle_tables(st_dicts)
+    bhyd = None
+    if nlte:
+        bhyd = np.ones((6, kw))
+        bhyd[:, :nr] = rng.uniform(0.6, 1.5, (6, nr))
+    ah, sh = kapp.hlinop(ws, t, xne, rho, x1, bhyd=bhyd, kw=kw)
+    st = po.stehle_structs(st_dicts)[0] if use_stehle else None
+    worst = {"ahline": 0.0, "shline": 0.0}
+    kt = po.kapp_tables(tables)
+    for i, w in enumerate(ws):
+        ra, rs = po.hlinop(kt, w, t, xne, rho, x1, None if bhyd is None else np.ascontiguousarray(bhyd[:, :nr]), st)
+        worst["ahline"] = max(worst["ahline"], rel_err(ah[i, :nr], ra))
+        worst["shline"] = max(worst["shline"], rel_err(sh[i, :nr], rs))
+    print("max relative error", worst)
+    assert max(worst.values()) <= RTOL, worst
+    assert np.count_nonzero(ah[:, :nr]) > 0.3 * ah[:, :nr].size and not np.any(ah[:, nr:])
+    kapp.set_stehle_tables(None)
+
+
 def test_kapp_helium_rejects_bad_input(gpu_ctx, tables, kapp):
     at = helium_atmosphere(15000.0, 4.0)
     ws = np.array([50.0, 500.0])
