@@ -66,13 +66,24 @@ FLOPS_PER_NU = int(2 / 3 * 51 ** 3 + 8 * 51 ** 2 + 2 * 51 + 110 * 72)
 # (a 51x51 matrix-vector product and the update)
 FLOPS_PER_SOLVE = int(2 / 3 * 51 ** 3 + 4 * 51 ** 2)
 FLOPS_PER_SERIES_STEP = 2 * 51 ** 2 + 3 * 51
-# DRAM bytes per model of the three batched RT launches (ncu, 4-slot capture
-# of this workload: 337 MB per model, of which 138 MB are the post stage's
-# partial-sum rows, one per frequency at 4 slots; at 32 slots a post warp
-# takes 6-7 frequencies and its rows are 22 MB per model): ACONT, SIGMAC and
-# XLINES read by the prepare and finish stages, the per-frequency records
-# written and read back, the partial sums
-RT_TRAFFIC_PER_MODEL = 221e6
+# DRAM bytes per model of the three batched RT launches that do not depend on
+# the launch shape (ncu, 4-slot capture of this workload: 337 MB per model
+# less the 138 MB of partial-sum rows it wrote, one per frequency at 4 slots):
+# ACONT, SIGMAC and XLINES read by the prepare and finish stages, the
+# per-frequency records written and read back.  The finish stage's
+# partial-sum rows (one 577-double row per finish warp) are added for the
+# tuned shape (rt_partial_rows).
+RT_TRAFFIC_FIXED_PER_MODEL = 199e6
+
+
+def rt_partial_rows(numnu, nsm, slots, waves, warps_per_block=4):
+    """Partial-sum rows per model of the split RT pass's finish stage at a
+    launch shape (rt_split_shape in csrc/atlas.cuh: 16 warps per SM per wave
+    over the batch, each a contiguous run of one slot's frequencies)."""
+    units = max(1, nsm * 16 * waves // max(slots, 1))
+    per = max(1, -(-numnu // units))
+    n = -(-numnu // per)
+    return -(-n // warps_per_block) * warps_per_block
 # DRAM bytes per model of one batched LINOP1 launch (ncu, 4-slot capture of
 # this workload: 959 MB): the prepared line records and the fixed-point XLINES
 # words, whose write-backs dominate once several models' words exceed L2
@@ -397,14 +408,19 @@ def run_ours(args):
     nfreq = CFG["slots"] * CFG["numnu"]
     executed = (nfreq * (FLOPS_PER_NU - FLOPS_PER_SOLVE) + rt_solves["eliminated"] * FLOPS_PER_SOLVE
                 + rt_solves["series_steps"] * FLOPS_PER_SERIES_STEP)
+    import torch
+    rows = rt_partial_rows(CFG["numnu"], torch.cuda.get_device_properties(0).multi_processor_count, CFG["slots"],
+                           batch.shape()[1])
+    rt_traffic = RT_TRAFFIC_FIXED_PER_MODEL + rows * (8 * CFG["nrhox"] + 1) * 8
     roof = {"kernel": "RT pass (k_batch_rt_pre + k_batch_rt_series + k_batch_rt_solve + k_batch_rt_post, JOSH per "
                       "frequency, FP64)",
             "bound": "fp64", "achieved": ach, "peak": fp64_peak,
             "unit": "TFLOP/s", "frac": ach / fp64_peak if fp64_peak > 0 else None,
             "executed_tflops": executed / (kms["rt"] * 1e-3) / 1e12,
-            "traffic": RT_TRAFFIC_PER_MODEL * CFG["slots"],
-            "traffic_scaling": "ncu capture of the three launches of a 4-slot batch (337 MB per model), its "
-                               "partial-sum rows rescaled to this batch's 6-7 frequencies per post warp, times slots",
+            "traffic": rt_traffic * CFG["slots"],
+            "traffic_scaling": f"ncu capture of the three launches of a 4-slot batch (337 MB per model, 138 MB of "
+                               f"them partial-sum rows); the rows rescaled to this shape's {rows} per model "
+                               f"({rows * (8 * CFG['nrhox'] + 1) * 8 / 1e6:.0f} MB), times slots",
             "peak_source": "measured DFMA loop on this GPU (atlasgpu_fp64_peak_tflops); MEASURED_PEAKS.json has no FP64 figure",
             "work": f"{FLOPS_PER_NU} FP64 flop per frequency (the reference's elimination counted for every "
                     f"system) x {CFG['numnu']} frequencies x {CFG['slots']} models per pass; executed_tflops counts "
@@ -606,13 +622,24 @@ def kapp_rate(ctx, ops, W):
     A.kapp(*hargs, xnf3=hargs[6])
     ms_h2 = ctx.kernel_ms("kapp")
     ctx.enable_timing(False)
+    # HLINOP with STARK_MMM on seeded Stehle-format tables of the published shapes
+    from atlas12_b200 import synthetic
+    A.set_stehle_tables(synthetic.stehle_tables())
+    hl_args = (W["ws"], m["t"], e["xne"], e["rho"], args[4])
+    A.hlinop(*hl_args)
+    ctx.enable_timing(True)
+    A.hlinop(*hl_args)
+    ms_hl = ctx.kernel_ms("hlinop")
+    ctx.enable_timing(False)
     return {"frequencies": int(W["ws"].size), "depths": int(m["t"].size), "kernel_ms": ms,
             "evals_per_s": n / (ms * 1e-3) if ms > 0 else None,
             "sources": "HOP (n = 1..80), H2PLOP, HMINOP, HRAYOP, ELECOP and KAPP's totals",
             "with_helium": {"kernel_ms": ms_he, "evals_per_s": n / (ms_he * 1e-3) if ms_he > 0 else None,
                             "sources": "the above and HE1OP, HE2OP, HEMIOP, HERAOP"},
             "with_helium_h2": {"kernel_ms": ms_h2, "evals_per_s": n / (ms_h2 * 1e-3) if ms_h2 > 0 else None,
-                               "sources": "the above and H2MINOP, H2COLLOP, H2RAOP"}}
+                               "sources": "the above and H2MINOP, H2COLLOP, H2RAOP"},
+            "hlinop": {"kernel_ms": ms_hl, "evals_per_s": n / (ms_hl * 1e-3) if ms_hl > 0 else None,
+                       "sources": "HLINOP, STARK_MMM on seeded Stehle-format tables"}}
 
 
 def hbm_peak():
