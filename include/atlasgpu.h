@@ -460,8 +460,9 @@ int atlasgpu_atlas_set_stehle_tables(atlasgpu_ctx *ctx, const atlasgpu_stehle_se
  * above 2e15 Hz, Balmer above 4.44e14 Hz) nearest the frequency, their Stark
  * profiles from STARK_MMM (Stehle tables where loaded, else STARK
  * :17528-17659) with the occupation probabilities and departure
- * coefficients.  Depth vectors [nrhox] T, XNE, RHO, XNFP(J,1); bhyd
- * BHYD(J,1..6) as [6][kw] or NULL (LTE).  Outputs AHLINE, SHLINE
+ * coefficients.  Depth vectors [nrhox] T, XNE, RHO, XNFP(J,1), each positive
+ * but XNFP (STARK divides by XNE); bhyd BHYD(J,1..6) as [6][kw], positive, or
+ * NULL (LTE).  Outputs AHLINE, SHLINE
  * [numnu][kw] (frequencies outside the four series: 0 and 0, as KAPP's
  * zeroed arrays; depths past the dissolved-level cut: 0 and BNU).  The
  * tables of atlasgpu_atlas_set_kapp_tables must be set. */
