@@ -37,8 +37,9 @@ def test_header_compiles_as_c_and_cxx(tmp_path):
     src = tmp_path / "use.c"
     src.write_text('#include <stdio.h>\n#include "atlasgpu.h"\n'
                    "int main(void) {\n"
-                   '  printf("%zu %zu %zu %zu\\n", sizeof(atlasgpu_hydrogen_tables), sizeof(atlasgpu_stehle_series),\n'
-                   "         sizeof(atlasgpu_synthe_hydrogen), sizeof(atlasgpu_nlte_line));\n"
+                   '  printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(atlasgpu_hydrogen_tables),\n'
+                   "         sizeof(atlasgpu_stehle_series), sizeof(atlasgpu_synthe_hydrogen), sizeof(atlasgpu_nlte_line),\n"
+                   "         sizeof(atlasgpu_kapp_tables), sizeof(atlasgpu_kapp_pops), sizeof(atlasgpu_kapp_h2_tables));\n"
                    "  return 0;\n}\n")
     inc = "-I" + os.path.join(ROOT, "include")
     for cc, std in (("gcc", "-std=c11"), ("g++", "-std=c++17")):
@@ -49,7 +50,9 @@ def test_header_compiles_as_c_and_cxx(tmp_path):
         subprocess.run([cc, std, "-Wall", "-Wextra", "-Werror", inc] + lang + [str(src), "-o", str(exe)], check=True)
         sizes = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
         assert sizes == [ctypes.sizeof(_lib.HydrogenTables), ctypes.sizeof(_lib.StehleSeries),
-                         ctypes.sizeof(_lib.SyntheHydrogen), _lib.NLTE_LINE.itemsize]
+                         ctypes.sizeof(_lib.SyntheHydrogen), _lib.NLTE_LINE.itemsize,
+                         ctypes.sizeof(_lib.KappTables), ctypes.sizeof(_lib.KappPops),
+                         ctypes.sizeof(_lib.KappH2Tables)]
 
 
 def test_grid_is_host_only():
